@@ -1,0 +1,221 @@
+"""B200-native structured PCG velocity solve for CISM's Glissade higher-order solver.
+
+Python mirror of the reference solver interface
+(libglissade/glissade_velo_higher_pcg.F90, public list :56-58).  Each function
+calls the compiled sm_100a library ``_lib/libcismgpu.so`` through its C ABI
+(include/cismgpu.h); there is no Python or CPU fallback: if the library or a
+B200 is missing, the call raises.
+
+Array arguments use the memory layout the Fortran caller passes.  Either give
+arrays with the reference's dimensions in Fortran order, e.g. Auu of shape
+(27, nz, nx-1, ny-1) with order='F', or the same memory as C-order arrays with the
+dimensions reversed, e.g. shape (ny-1, nx-1, nz, 27).  xu and xv are updated in
+place (intent(inout)), and (err, niters) is returned.  A nonzero library status
+raises CismGpuError, which is where the reference calls
+write_log(..., GM_FATAL).
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import os
+
+import numpy as np
+
+__all__ = [
+    "ParallelType", "CismGpuError", "load_library", "pcg_solver_standard_3d", "pcg_solver_chrongear_3d",
+    "pcg_solver_standard_2d", "pcg_solver_chrongear_2d", "matvec_multiply_structured_3d",
+    "matvec_multiply_structured_2d", "HO_PRECOND_NONE", "HO_PRECOND_DIAG", "HO_PRECOND_SIA",
+    "HO_PRECOND_TRIDIAG_LOCAL", "HO_PRECOND_TRIDIAG_GLOBAL",
+]
+
+# libglide/glide_types.F90:342-346
+HO_PRECOND_NONE = 0
+HO_PRECOND_DIAG = 1
+HO_PRECOND_SIA = 2
+HO_PRECOND_TRIDIAG_LOCAL = 3
+HO_PRECOND_TRIDIAG_GLOBAL = 4
+
+STATUS_NAMES = {
+    0: "CISMGPU_OK", 1: "CISMGPU_EBREAKDOWN_ETA1", 2: "CISMGPU_EBREAKDOWN_ALPHA", 3: "CISMGPU_EUNSUPPORTED",
+    4: "CISMGPU_EINVAL", 5: "CISMGPU_ECUDA", 6: "CISMGPU_ETIMEOUT", 7: "CISMGPU_ENOMEM", 8: "CISMGPU_ENODEV",
+}
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libcismgpu.so")
+
+
+class CismGpuError(RuntimeError):
+    """A nonzero status from the library (the reference's GM_FATAL cases and GPU errors)."""
+
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+
+
+class CParallel(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in (
+        "staggered_ilo", "staggered_ihi", "staggered_jlo", "staggered_jhi", "periodic_bc", "outflow_bc",
+        "no_ice_bc", "reprosum", "tasks_row", "tasks_col")]
+
+
+@dataclasses.dataclass
+class ParallelType:
+    """The fields of type(parallel_type) read on this path (libglimmer/parallel_mpi.F90:78-153)."""
+    staggered_ilo: int
+    staggered_ihi: int
+    staggered_jlo: int
+    staggered_jhi: int
+    periodic_bc: bool = True
+    outflow_bc: bool = False
+    no_ice_bc: bool = False
+    reprosum: bool = False
+    tasks_row: int = 1
+    tasks_col: int = 1
+
+    @classmethod
+    def from_dict(cls, d: dict) -> "ParallelType":
+        return cls(**{f.name: d[f.name] for f in dataclasses.fields(cls) if f.name in d})
+
+    def to_c(self) -> CParallel:
+        return CParallel(*(int(getattr(self, f.name)) for f in dataclasses.fields(self)))
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load libcismgpu.so (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with cism_b200.build.build() (no CPU fallback exists)")
+    lib = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    d, i32, dbl = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+    par = P(CParallel)
+    common_tail = [d, d, d, d, d, d, d, d, i32, i32, dbl, i32, P(dbl), P(i32), i32, i32, i32]
+    lib.cismgpu_pcg_standard_3d.argtypes = [i32, i32, i32, par, d, d, d] + common_tail
+    lib.cismgpu_pcg_chrongear_3d.argtypes = [i32, i32, i32, par, d, d, d] + common_tail
+    lib.cismgpu_pcg_standard_2d.argtypes = [i32, i32, par, d, d] + common_tail
+    lib.cismgpu_pcg_chrongear_2d.argtypes = [i32, i32, par, d, d] + common_tail
+    for f in ("cismgpu_pcg_standard_3d", "cismgpu_pcg_chrongear_3d", "cismgpu_pcg_standard_2d",
+              "cismgpu_pcg_chrongear_2d"):
+        getattr(lib, f).restype = ctypes.c_int
+    lib.cismgpu_matvec_structured_3d.argtypes = [i32, i32, i32, par, d, d, d, d, d, d, d, d, d, d]
+    lib.cismgpu_matvec_structured_3d.restype = ctypes.c_int
+    lib.cismgpu_matvec_structured_2d.argtypes = [i32, i32, par, d, d, d, d, d, d, d, d, d, d]
+    lib.cismgpu_matvec_structured_2d.restype = ctypes.c_int
+    lib.cismgpu_last_error.restype = ctypes.c_char_p
+    lib.cismgpu_version.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray, dtype, n: int, writable: bool = False):
+    if not isinstance(a, np.ndarray) or a.dtype != dtype:
+        raise TypeError(f"expected a numpy array of {np.dtype(dtype).name}")
+    if a.size != n:
+        raise ValueError(f"array has {a.size} elements, expected {n}")
+    if not (a.flags.c_contiguous or a.flags.f_contiguous):
+        raise ValueError("array must be contiguous in the caller's layout")
+    if writable and not a.flags.writeable:
+        raise ValueError("output array is read-only")
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _par(parallel) -> CParallel:
+    if isinstance(parallel, ParallelType):
+        return parallel.to_c()
+    if isinstance(parallel, dict):
+        return ParallelType.from_dict(parallel).to_c()
+    raise TypeError("parallel must be a ParallelType or dict")
+
+
+def _check(lib, status: int):
+    if status != 0:
+        raise CismGpuError(status, lib.cismgpu_last_error().decode())
+
+
+def _solve(fname: str, is3d: bool, nx, ny, nz, parallel, indxA_2d, indxA_3d, active_vertex, Auu, Auv, Avu, Avv,
+           bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, itest, jtest, rtest):
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    nvec = nv * (nz if is3d else 1)
+    nblk = nvec * (27 if is3d else 9)
+    err = ctypes.c_double(0.0)
+    niters = ctypes.c_int(0)
+    par = _par(parallel)
+    i2 = _ptr(np.ascontiguousarray(indxA_2d, dtype=np.int32), np.int32, 9)
+    head = [nx, ny] + ([nz] if is3d else []) + [ctypes.byref(par), i2]
+    if is3d:
+        head.append(_ptr(np.ascontiguousarray(indxA_3d, dtype=np.int32), np.int32, 27))
+    args = head + [
+        _ptr(active_vertex, np.int32, nv),
+        _ptr(Auu, np.float64, nblk), _ptr(Auv, np.float64, nblk), _ptr(Avu, np.float64, nblk),
+        _ptr(Avv, np.float64, nblk), _ptr(bu, np.float64, nvec), _ptr(bv, np.float64, nvec),
+        _ptr(xu, np.float64, nvec, True), _ptr(xv, np.float64, nvec, True),
+        int(precond), int(linear_solve_ncheck), float(tolerance), int(maxiters), ctypes.byref(err),
+        ctypes.byref(niters), int(itest), int(jtest), int(rtest)]
+    _check(lib, getattr(lib, fname)(*args))
+    return err.value, niters.value
+
+
+def pcg_solver_standard_3d(nx, ny, nz, parallel, indxA_2d, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, bu, bv,
+                           xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, itest=1, jtest=1, rtest=0):
+    """Mirrors pcg_solver_standard_3d (glissade_velo_higher_pcg.F90:827-1537)."""
+    return _solve("cismgpu_pcg_standard_3d", True, nx, ny, nz, parallel, indxA_2d, indxA_3d, active_vertex, Auu,
+                  Auv, Avu, Avv, bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, itest, jtest,
+                  rtest)
+
+
+def pcg_solver_chrongear_3d(nx, ny, nz, parallel, indxA_2d, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, bu, bv,
+                            xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, itest=1, jtest=1, rtest=0):
+    """Mirrors pcg_solver_chrongear_3d (glissade_velo_higher_pcg.F90:2632-3594)."""
+    return _solve("cismgpu_pcg_chrongear_3d", True, nx, ny, nz, parallel, indxA_2d, indxA_3d, active_vertex, Auu,
+                  Auv, Avu, Avv, bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, itest, jtest,
+                  rtest)
+
+
+def pcg_solver_standard_2d(nx, ny, parallel, indxA_2d, active_vertex, Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond,
+                           linear_solve_ncheck, tolerance, maxiters, itest=1, jtest=1, rtest=0):
+    """Mirrors pcg_solver_standard_2d (glissade_velo_higher_pcg.F90:67-823)."""
+    return _solve("cismgpu_pcg_standard_2d", False, nx, ny, 1, parallel, indxA_2d, None, active_vertex, Auu, Auv,
+                  Avu, Avv, bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, itest, jtest, rtest)
+
+
+def pcg_solver_chrongear_2d(nx, ny, parallel, indxA_2d, active_vertex, Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond,
+                            linear_solve_ncheck, tolerance, maxiters, itest=1, jtest=1, rtest=0):
+    """Mirrors pcg_solver_chrongear_2d (glissade_velo_higher_pcg.F90:1541-2628)."""
+    return _solve("cismgpu_pcg_chrongear_2d", False, nx, ny, 1, parallel, indxA_2d, None, active_vertex, Auu, Auv,
+                  Avu, Avv, bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, itest, jtest, rtest)
+
+
+def matvec_multiply_structured_3d(nx, ny, nz, parallel, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, xu, xv):
+    """Mirrors matvec_multiply_structured_3d (glissade_velo_higher_pcg.F90:5528-5652); returns (yu, yv)."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    nvec, nblk = nv * nz, nv * nz * 27
+    yu, yv = np.empty_like(xu), np.empty_like(xv)
+    par = _par(parallel)
+    _check(lib, lib.cismgpu_matvec_structured_3d(
+        nx, ny, nz, ctypes.byref(par), _ptr(np.ascontiguousarray(indxA_3d, dtype=np.int32), np.int32, 27),
+        _ptr(active_vertex, np.int32, nv), _ptr(Auu, np.float64, nblk), _ptr(Auv, np.float64, nblk),
+        _ptr(Avu, np.float64, nblk), _ptr(Avv, np.float64, nblk), _ptr(xu, np.float64, nvec),
+        _ptr(xv, np.float64, nvec), _ptr(yu, np.float64, nvec, True), _ptr(yv, np.float64, nvec, True)))
+    return yu, yv
+
+
+def matvec_multiply_structured_2d(nx, ny, parallel, indxA_2d, active_vertex, Auu, Auv, Avu, Avv, xu, xv):
+    """Mirrors matvec_multiply_structured_2d (glissade_velo_higher_pcg.F90:5656-5773); returns (yu, yv)."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    yu, yv = np.empty_like(xu), np.empty_like(xv)
+    par = _par(parallel)
+    _check(lib, lib.cismgpu_matvec_structured_2d(
+        nx, ny, ctypes.byref(par), _ptr(np.ascontiguousarray(indxA_2d, dtype=np.int32), np.int32, 9),
+        _ptr(active_vertex, np.int32, nv), _ptr(Auu, np.float64, nv * 9), _ptr(Auv, np.float64, nv * 9),
+        _ptr(Avu, np.float64, nv * 9), _ptr(Avv, np.float64, nv * 9), _ptr(xu, np.float64, nv),
+        _ptr(xv, np.float64, nv), _ptr(yu, np.float64, nv, True), _ptr(yv, np.float64, nv, True)))
+    return yu, yv

@@ -1,0 +1,446 @@
+// pcg_fp64.cu -- plain FP64 structured PCG on B200 (sm_100a), reference-faithful.
+//
+// Each kernel restates one or more consecutive whole-array statements of
+// libglissade/glissade_velo_higher_pcg.F90 with the same floating-point operation
+// order (the library is compiled with --fmad=false, so a*b+c is never contracted),
+// and global sums go through the fixed double-double tree of common.cuh.  The
+// kernels never read the CPU; scalars (alpha, beta, ...) live in SolveState in HBM
+// and are produced by the last CTA of the reducing kernel.
+#include "common.cuh"
+#include "../../include/cismgpu.h"
+
+namespace cismgpu {
+
+// ---------------------------------------------------------------------------
+// reduction: per-CTA dd partials -> last CTA finishes with the fixed tree and
+// runs the scalar epilogue
+// ---------------------------------------------------------------------------
+struct RedCtx {
+    DD *partials;        // [gridDim.x][2]
+    SolveState *st;
+    int epi;
+    int iter;
+};
+
+__device__ void epilogue(SolveState *st, int epi, int iter, double S0, double S1) {
+    switch (epi) {
+    case EPI_L2RHS:
+        st->L2_rhs = sqrt(S0);
+        break;
+    case EPI_STD_ETA1: {  // :1325-1337
+        st->eta1 = S0;
+        if (S0 != S0) { st->status = CISMGPU_EBREAKDOWN_ETA1; st->done = 1; st->niters = iter; break; }
+        st->beta = st->eta1 / st->eta0;
+        break;
+    }
+    case EPI_STD_ETA2: {  // :1371-1394
+        st->eta0 = st->eta1;
+        st->eta2 = S0;
+        st->alpha = st->eta1 / st->eta2;
+        if (st->alpha != st->alpha) { st->status = CISMGPU_EBREAKDOWN_ALPHA; st->done = 1; st->niters = iter; }
+        break;
+    }
+    case EPI_CHECK: {     // :1466-1513, :3516-3563
+        st->err = sqrt(S0) / st->L2_rhs;
+        st->checks += 1;
+        if (st->err < st->tol) { st->niters = iter; st->done = 1; }
+        break;
+    }
+    case EPI_CG_RHO0:     // (r,z) of the first pass, kept until (d,q) is known (:3215, :3258)
+        st->rho_old = S0;
+        break;
+    case EPI_CG_FIRST: {  // :3258-3266
+        st->sigma = S0;
+        st->alpha = st->rho_old / st->sigma;
+        if (st->alpha != st->alpha) { st->status = CISMGPU_EBREAKDOWN_ALPHA; st->done = 1; st->niters = iter; }
+        break;
+    }
+    case EPI_CG_ITER: {   // :3426-3437
+        st->rho = S0;
+        st->delta = S1;
+        st->beta = st->rho / st->rho_old;
+        st->sigma = st->delta - st->beta * st->rho / st->alpha;
+        st->alpha = st->rho / st->sigma;
+        st->rho_old = st->rho;
+        if (st->alpha != st->alpha) { st->status = CISMGPU_EBREAKDOWN_ALPHA; st->done = 1; st->niters = iter; }
+        break;
+    }
+    default:
+        break;
+    }
+}
+
+// Called by all threads of every CTA with the thread's column partials.
+template <int NF>
+__device__ void reduce_and_finish(const RedCtx &rc, DD v0, DD v1) {
+    __shared__ DD sm[8];
+    __shared__ bool last;
+    DD b0 = block_tree(v0, sm);
+    DD b1 = DD{0.0, 0.0};
+    if (NF > 1) b1 = block_tree(v1, sm);
+    if (threadIdx.x == 0) {
+        rc.partials[2 * blockIdx.x + 0] = b0;
+        rc.partials[2 * blockIdx.x + 1] = b1;
+        __threadfence();
+        unsigned int t = atomicAdd(&rc.st->ticket[0], 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    DD a0{0.0, 0.0}, a1{0.0, 0.0};
+    for (unsigned int c = threadIdx.x; c < gridDim.x; c += kBlock) {
+        DD p0, p1;
+        p0.hi = __ldcg(&rc.partials[2 * c].hi);
+        p0.lo = __ldcg(&rc.partials[2 * c].lo);
+        a0 = dd_add(a0, p0);
+        if (NF > 1) {
+            p1.hi = __ldcg(&rc.partials[2 * c + 1].hi);
+            p1.lo = __ldcg(&rc.partials[2 * c + 1].lo);
+            a1 = dd_add(a1, p1);
+        }
+    }
+    DD r0 = block_tree(a0, sm);
+    DD r1 = DD{0.0, 0.0};
+    if (NF > 1) r1 = block_tree(a1, sm);
+    if (threadIdx.x == 0) {
+        rc.st->ticket[0] = 0u;
+        epilogue(rc.st, rc.epi, rc.iter, r0.hi + r0.lo, r1.hi + r1.lo);
+    }
+}
+
+__device__ __forceinline__ void col_of(const Geom &g, long long q, int &i, int &j) {
+    j = (int)(q / g.NX);
+    i = (int)(q - (long long)j * g.NX);
+}
+
+// ---------------------------------------------------------------------------
+// structured matvec row (matvec_multiply_structured_3d :5612-5650, _2d :5739-5771)
+// ---------------------------------------------------------------------------
+template <int NC>
+__device__ __forceinline__ void mv_row(const Geom &g, const double *__restrict__ A, const double *__restrict__ xu,
+                                       const double *__restrict__ xv, int i, int j, long long q, int k,
+                                       double &yu, double &yv) {
+    const long long plane = (long long)g.nz * g.NQ;
+    const double *Auu = A, *Auv = A + NC * plane, *Avu = A + 2 * NC * plane, *Avv = A + 3 * NC * plane;
+    double su = 0.0, sv = 0.0;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
+        if (k + kA >= 0 && k + kA < g.nz && i + iA >= 0 && i + iA < g.NX && j + jA >= 0 && j + jA < g.NY) {
+            const long long a = (long long)c * plane + (long long)k * g.NQ + q;
+            const long long n = (long long)(k + kA) * g.NQ + q + iA + (long long)jA * g.NX;
+            const double x1 = xu[n], x2 = xv[n];
+            su = __dadd_rn(__dadd_rn(su, __dmul_rn(Auu[a], x1)), __dmul_rn(Auv[a], x2));
+            sv = __dadd_rn(__dadd_rn(sv, __dmul_rn(Avu[a], x1)), __dmul_rn(Avv[a], x2));
+        }
+    }
+    yu = su;
+    yv = sv;
+}
+
+enum MvMode { MV_PLAIN = 0, MV_RESID, MV_DQ, MV_CG_AZ };
+
+// y = A x over owned active columns, 0 elsewhere; optional fused statements:
+//   MV_RESID : r = b - y (whole array); S0 = (r,r)             [:1454-1466, :3504-3516]
+//   MV_DQ    : S0 = (x,y) with x = d, y = q                    [:1376-1381, :3241-3248]
+//   MV_CG_AZ : S0 = (r,z), S1 = (y,z) with x = z, y = Az       [:3401-3413]
+template <int NC, int MODE>
+__global__ void __launch_bounds__(kBlock) k_mv(Geom g, const double *__restrict__ A, const int32_t *__restrict__ act,
+                                               const double *__restrict__ xu, const double *__restrict__ xv,
+                                               double *__restrict__ yu, double *__restrict__ yv,
+                                               const double *__restrict__ bu, const double *__restrict__ bv,
+                                               double *__restrict__ ru, double *__restrict__ rv, RedCtx rc) {
+    if (rc.st->done) return;
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    DD s0{0.0, 0.0}, s1{0.0, 0.0};
+    if (q < g.NQ) {
+        int i, j;
+        col_of(g, q, i, j);
+        const bool own = owned(g, i, j);
+        const bool on = own && act[q] != 0;
+        for (int k = 0; k < g.nz; ++k) {
+            const long long e = (long long)k * g.NQ + q;
+            double a = 0.0, b = 0.0;
+            if (on) mv_row<NC>(g, A, xu, xv, i, j, q, k, a, b);
+            yu[e] = a;
+            yv[e] = b;
+            if (MODE == MV_RESID) {
+                const double r1 = __dsub_rn(bu[e], a), r2 = __dsub_rn(bv[e], b);
+                ru[e] = r1;
+                rv[e] = r2;
+                if (own) s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(r1, r1), __dmul_rn(r2, r2)));
+            } else if (MODE == MV_DQ) {
+                if (own) s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(xu[e], a), __dmul_rn(xv[e], b)));
+            } else if (MODE == MV_CG_AZ) {
+                if (own) {
+                    const double z1 = xu[e], z2 = xv[e];
+                    s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(ru[e], z1), __dmul_rn(rv[e], z2)));
+                    s1 = dd_add_d(s1, __dadd_rn(__dmul_rn(a, z1), __dmul_rn(b, z2)));
+                }
+            }
+        }
+    }
+    if (MODE == MV_RESID || MODE == MV_DQ) reduce_and_finish<1>(rc, s0, s1);
+    if (MODE == MV_CG_AZ) reduce_and_finish<2>(rc, s0, s1);
+}
+
+// ---------------------------------------------------------------------------
+// preconditioner apply over the whole array (halo included)
+// ---------------------------------------------------------------------------
+// tridiag_solver (:5870-5922) on one column of the SIA matrix (easy_sia_solver :5777-5866).
+// M(-1), M(0), M(+1) are the A planes of offsets (0,0,-1), (0,0,0), (0,0,+1).
+constexpr int kMaxNz = 64;
+
+__device__ void sia_column(const Geom &g, const double *__restrict__ Mlo, const double *__restrict__ Mdi,
+                           const double *__restrict__ Mup, const double *__restrict__ r, double *__restrict__ z,
+                           long long q) {
+    const int nz = g.nz;
+    const long long NQ = g.NQ;
+    double gam[kMaxNz];
+    double sol[kMaxNz];
+    // top layer: sbdiag = 0, diag = M(0), spdiag = M(+1); bottom layer: spdiag = 0
+    double beta = Mdi[q];
+    sol[0] = r[q] / beta;
+    for (int k = 1; k < nz; ++k) {
+        const double sp_prev = Mup[(long long)(k - 1) * NQ + q];  // spdiag(k-1), k-1 <= nz-1
+        const double sb = Mlo[(long long)k * NQ + q];
+        const double dg = Mdi[(long long)k * NQ + q];
+        gam[k] = sp_prev / beta;
+        beta = __dsub_rn(dg, __dmul_rn(sb, gam[k]));
+        sol[k] = __dsub_rn(r[(long long)k * NQ + q], __dmul_rn(sb, sol[k - 1])) / beta;
+    }
+    for (int k = nz - 2; k >= 0; --k) sol[k] = __dsub_rn(sol[k], __dmul_rn(gam[k + 1], sol[k + 1]));
+    for (int k = 0; k < nz; ++k) z[(long long)k * NQ + q] = sol[k];
+}
+
+enum PreMode { PRE_ONLY = 0, PRE_STD, PRE_CG_FIRST };
+
+// z = PC(r) over the whole array, then optionally:
+//   PRE_STD      : S0 = (r,z)                      [:1320-1326]
+//   PRE_CG_FIRST : S0 = (r,z) kept for the first-pass epilogue; d = z   [:3215-3223]
+// kind: 0 none (z = r), 1 diag, 2 sia (3D only), anything else: z unchanged.
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_precond(Geom g, int kind, const double *__restrict__ A,
+                                                    int NC, const int32_t *__restrict__ act,
+                                                    const double *__restrict__ ru, const double *__restrict__ rv,
+                                                    double *__restrict__ zu, double *__restrict__ zv,
+                                                    double *__restrict__ du, double *__restrict__ dv,
+                                                    RedCtx rc) {
+    if (rc.st->done) return;
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    DD s0{0.0, 0.0};
+    if (q < g.NQ) {
+        int i, j;
+        col_of(g, q, i, j);
+        const long long plane = (long long)g.nz * g.NQ;
+        const int cdiag = (NC == 27) ? 13 : 4;
+        const double *Auu = A, *Avv = A + 3LL * NC * plane;
+        if (kind == CISMGPU_PRECOND_NONE) {
+            for (int k = 0; k < g.nz; ++k) {
+                const long long e = (long long)k * g.NQ + q;
+                zu[e] = ru[e];
+                zv[e] = rv[e];
+            }
+        } else if (kind == CISMGPU_PRECOND_DIAG) {  // :1238-1253 (3D), :467-480 (2D)
+            for (int k = 0; k < g.nz; ++k) {
+                const long long e = (long long)k * g.NQ + q;
+                const double a = Auu[(long long)cdiag * plane + e], b = Avv[(long long)cdiag * plane + e];
+                zu[e] = (a != 0.0) ? ru[e] / a : 0.0;
+                zv[e] = (b != 0.0) ? rv[e] / b : 0.0;
+            }
+        } else if (kind == CISMGPU_PRECOND_SIA && NC == 27) {  // :1255-1263
+            if (act[q] != 0) {
+                sia_column(g, Auu + 4 * plane, Auu + 13 * plane, Auu + 22 * plane, ru, zu, q);
+                sia_column(g, Avv + 4 * plane, Avv + 13 * plane, Avv + 22 * plane, rv, zv, q);
+            }
+        }
+        if (MODE == PRE_STD || MODE == PRE_CG_FIRST) {
+            const bool own = owned(g, i, j);
+            for (int k = 0; k < g.nz; ++k) {
+                const long long e = (long long)k * g.NQ + q;
+                const double z1 = zu[e], z2 = zv[e];
+                if (own) s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(ru[e], z1), __dmul_rn(rv[e], z2)));
+                if (MODE == PRE_CG_FIRST) { du[e] = z1; dv[e] = z2; }
+            }
+        }
+    }
+    if (MODE == PRE_STD || MODE == PRE_CG_FIRST) reduce_and_finish<1>(rc, s0, s0);
+}
+
+// ---------------------------------------------------------------------------
+// whole-array vector statements
+// ---------------------------------------------------------------------------
+enum VecOp {
+    OP_STD_INIT = 0,  // r = b - z; d = 0; z = 0; S0 = (b,b)           [:1190-1216]
+    OP_STD_D,         // d = z + beta*d                                  [:1340-1341]
+    OP_XR,            // x = x + alpha*d; r = r - alpha*q                [:1399-1403, :3272-3276]
+    OP_CG_INIT,       // r = b - z                                       [:3115-3116]
+    OP_CG_UPD,        // d = z + beta*d; q = Az + beta*q; x += alpha*d; r -= alpha*q  [:3444-3459]
+    OP_DOT_BB,        // S0 = (b,b)                                      [:3067-3074]
+};
+
+struct VecArgs {
+    const double *bu, *bv;
+    double *xu, *xv, *ru, *rv, *du, *dv, *qu, *qv, *zu, *zv;
+    const double *Azu, *Azv;
+};
+
+template <int OP>
+__global__ void __launch_bounds__(kBlock) k_vec(Geom g, VecArgs v, RedCtx rc) {
+    if (rc.st->done) return;
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    DD s0{0.0, 0.0};
+    const double alpha = rc.st->alpha, beta = rc.st->beta;
+    if (q < g.NQ) {
+        int i, j;
+        col_of(g, q, i, j);
+        const bool own = owned(g, i, j);
+        for (int k = 0; k < g.nz; ++k) {
+            const long long e = (long long)k * g.NQ + q;
+            if (OP == OP_STD_INIT) {
+                v.ru[e] = __dsub_rn(v.bu[e], v.zu[e]);
+                v.rv[e] = __dsub_rn(v.bv[e], v.zv[e]);
+                v.du[e] = 0.0; v.dv[e] = 0.0;
+                v.zu[e] = 0.0; v.zv[e] = 0.0;
+                if (own) s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(v.bu[e], v.bu[e]), __dmul_rn(v.bv[e], v.bv[e])));
+            } else if (OP == OP_DOT_BB) {
+                if (own) s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(v.bu[e], v.bu[e]), __dmul_rn(v.bv[e], v.bv[e])));
+            } else if (OP == OP_STD_D) {
+                v.du[e] = __dadd_rn(v.zu[e], __dmul_rn(beta, v.du[e]));
+                v.dv[e] = __dadd_rn(v.zv[e], __dmul_rn(beta, v.dv[e]));
+            } else if (OP == OP_XR) {
+                v.xu[e] = __dadd_rn(v.xu[e], __dmul_rn(alpha, v.du[e]));
+                v.xv[e] = __dadd_rn(v.xv[e], __dmul_rn(alpha, v.dv[e]));
+                v.ru[e] = __dsub_rn(v.ru[e], __dmul_rn(alpha, v.qu[e]));
+                v.rv[e] = __dsub_rn(v.rv[e], __dmul_rn(alpha, v.qv[e]));
+            } else if (OP == OP_CG_INIT) {
+                v.ru[e] = __dsub_rn(v.bu[e], v.zu[e]);
+                v.rv[e] = __dsub_rn(v.bv[e], v.zv[e]);
+            } else if (OP == OP_CG_UPD) {
+                const double d1 = __dadd_rn(v.zu[e], __dmul_rn(beta, v.du[e]));
+                const double d2 = __dadd_rn(v.zv[e], __dmul_rn(beta, v.dv[e]));
+                const double q1 = __dadd_rn(v.Azu[e], __dmul_rn(beta, v.qu[e]));
+                const double q2 = __dadd_rn(v.Azv[e], __dmul_rn(beta, v.qv[e]));
+                v.du[e] = d1; v.dv[e] = d2;
+                v.qu[e] = q1; v.qv[e] = q2;
+                v.xu[e] = __dadd_rn(v.xu[e], __dmul_rn(alpha, d1));
+                v.xv[e] = __dadd_rn(v.xv[e], __dmul_rn(alpha, d2));
+                v.ru[e] = __dsub_rn(v.ru[e], __dmul_rn(alpha, q1));
+                v.rv[e] = __dsub_rn(v.rv[e], __dmul_rn(alpha, q2));
+            }
+        }
+    }
+    if (OP == OP_STD_INIT || OP == OP_DOT_BB) reduce_and_finish<1>(rc, s0, s0);
+}
+
+// ---------------------------------------------------------------------------
+// staggered halo on one rank (parallel_mpi.F90:10772-10936)
+// ---------------------------------------------------------------------------
+// Threads enumerate the ring columns: rows j in {0,1,NY-2,NY-1} (all i), then
+// columns i in {0,1,NX-2,NX-1} for 2 <= j <= NY-3.  A periodic halo position
+// (i in {0,1,NX-1} or j in {0,1,NY-1}) takes the value at (pi(i), pj(j)) with
+// pi(0)=NX-3, pi(1)=NX-2, pi(NX-1)=2 (identity otherwise): the composite of the
+// east-west exchange on owned rows followed by the north-south exchange on all
+// columns.  Sources are never halo positions, so one pass is race free.  Outflow
+// then zeroes i,j in {0, N-1}; no_ice zeroes i,j in {0,1,N-2,N-1}.
+__device__ __forceinline__ int pmap(int i, int N) {
+    if (i == 0) return N - 3;
+    if (i == 1) return N - 2;
+    if (i == N - 1) return 2;
+    return i;
+}
+
+__global__ void __launch_bounds__(kBlock) k_halo(Geom g, double *__restrict__ au, double *__restrict__ av,
+                                                 const SolveState *st) {
+    if (st && st->done) return;
+    const int NX = g.NX, NY = g.NY;
+    const long long nring = 4LL * NX + 4LL * (NY - 4);
+    const long long t = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (t >= nring) return;
+    int i, j;
+    if (t < 4LL * NX) {
+        const int r = (int)(t / NX);
+        i = (int)(t - (long long)r * NX);
+        j = (r < 2) ? r : NY - 4 + r;  // 0,1,NY-2,NY-1
+    } else {
+        const long long u = t - 4LL * NX;
+        const int r = (int)(u / (NY - 4));
+        j = 2 + (int)(u - (long long)r * (NY - 4));
+        i = (r < 2) ? r : NX - 4 + r;
+    }
+    bool zero = false;
+    if (g.outflow) zero = (i == 0 || i == NX - 1 || j == 0 || j == NY - 1);
+    else if (g.no_ice) zero = (i <= 1 || i >= NX - 2 || j <= 1 || j >= NY - 2);
+    const long long q = (long long)j * NX + i;
+    if (zero) {
+        for (int k = 0; k < g.nz; ++k) {
+            au[(long long)k * g.NQ + q] = 0.0;
+            av[(long long)k * g.NQ + q] = 0.0;
+        }
+        return;
+    }
+    if (g.periodic) {
+        const bool halo = (i <= 1 || i == NX - 1 || j <= 1 || j == NY - 1);
+        if (!halo) return;
+        const long long s = (long long)pmap(j, NY) * NX + pmap(i, NX);
+        for (int k = 0; k < g.nz; ++k) {
+            au[(long long)k * g.NQ + q] = au[(long long)k * g.NQ + s];
+            av[(long long)k * g.NQ + q] = av[(long long)k * g.NQ + s];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// layout conversion between the caller's Fortran arrays and device planes
+// ---------------------------------------------------------------------------
+// 3D block A(27,nz,NX,NY) raw -> planes [c][k][q]; canonical c reads m = indxA(c)
+__global__ void k_perm_block3(Geom g, const double *__restrict__ raw, double *__restrict__ dst,
+                              const int32_t *__restrict__ map27) {
+    const long long node = (long long)blockIdx.x * blockDim.x + threadIdx.x;  // Fortran order k + nz*q
+    const long long n = (long long)g.nz * g.NQ;
+    if (node >= n) return;
+    const long long q = node / g.nz;
+    const int k = (int)(node - q * g.nz);
+    const double *src = raw + 27LL * node;
+    for (int c = 0; c < 27; ++c) dst[(long long)c * n + (long long)k * g.NQ + q] = src[map27[c] - 1];
+}
+
+// 2D block A(NX,NY,9) raw (already planes) -> canonical planes
+__global__ void k_perm_block2(Geom g, const double *__restrict__ raw, double *__restrict__ dst,
+                              const int32_t *__restrict__ map9) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.NQ) return;
+    for (int c = 0; c < 9; ++c) dst[(long long)c * g.NQ + q] = raw[(long long)(map9[c] - 1) * g.NQ + q];
+}
+
+// vector (nz,NX,NY) Fortran <-> level-major planes
+__global__ void k_vec_in(Geom g, const double *__restrict__ raw, double *__restrict__ dst) {
+    const long long node = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)g.nz * g.NQ;
+    if (node >= n) return;
+    const long long q = node / g.nz;
+    const int k = (int)(node - q * g.nz);
+    dst[(long long)k * g.NQ + q] = raw[node];
+}
+
+__global__ void k_vec_out(Geom g, const double *__restrict__ src, double *__restrict__ raw) {
+    const long long node = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)g.nz * g.NQ;
+    if (node >= n) return;
+    const long long q = node / g.nz;
+    const int k = (int)(node - q * g.nz);
+    raw[node] = src[(long long)k * g.NQ + q];
+}
+
+__global__ void k_init_state(SolveState *st, double tol, int maxiters) {
+    st->eta0 = 1.0; st->eta1 = 0.0; st->eta2 = 0.0; st->alpha = 0.0; st->beta = 0.0;
+    st->rho_old = 0.0; st->sigma = 0.0; st->rho = 0.0; st->delta = 0.0;
+    st->L2_rhs = 0.0;
+    st->err = __longlong_as_double(0x7ff8000000000000LL);  // NaN until the first check
+    st->tol = tol;
+    st->done = 0; st->status = 0; st->niters = maxiters; st->checks = 0;
+    for (int t = 0; t < 4; ++t) st->ticket[t] = 0u;
+}
+
+}  // namespace cismgpu

@@ -1,0 +1,158 @@
+/*
+ * cismgpu.h -- C ABI of the B200 (sm_100a) native structured PCG velocity solve.
+ *
+ * These entry points replace the four native PCG solvers of CISM's Glissade
+ * higher-order velocity solver,
+ *   libglissade/glissade_velo_higher_pcg.F90
+ *     pcg_solver_standard_2d   (:67-823)
+ *     pcg_solver_standard_3d   (:827-1537)
+ *     pcg_solver_chrongear_2d  (:1541-2628)
+ *     pcg_solver_chrongear_3d  (:2632-3594)
+ * called from glissade_velo_higher_solve (libglissade/glissade_velo_higher.F90:3229-3322).
+ *
+ * Argument lists keep the Fortran order and meaning.  Arrays are Fortran
+ * column-major, exactly as the Fortran caller holds them:
+ *   3D blocks   A(27, nz, nx-1, ny-1): element (m,k,i,j) at (m-1)+27*((k-1)+nz*((i-1)+(nx-1)*(j-1)))
+ *   3D vectors  b(nz, nx-1, ny-1)
+ *   2D blocks   A(nx-1, ny-1, 9):      element (i,j,m) at (i-1)+(nx-1)*((j-1)+(ny-1)*(m-1))
+ *   2D vectors  b(nx-1, ny-1)
+ *   indxA_3d(-1:1,-1:1,-1:1) and indxA_2d(-1:1,-1:1) as 27 / 9 int32 (iA fastest)
+ *   active_vertex(nx-1, ny-1) as Fortran default logical (4 bytes, nonzero = .true.)
+ * nx, ny are the *cell* dimensions of the haloed local grid (velocity arrays are
+ * (nx-1) x (ny-1) vertices), as in the reference.
+ *
+ * type(parallel_type) is not C-interoperable, so the Fortran wrapper copies the
+ * fields the path reads (libglimmer/parallel_mpi.F90:78-153) into cismgpu_par_t.
+ *
+ * Return value: CISMGPU_OK (0) on success, INCLUDING non-convergence (the
+ * reference returns niters = maxiters and the last err, :1514-1520).  Nonzero
+ * codes stand for the cases where the reference calls write_log(..., GM_FATAL)
+ * (NaN breakdown, :637-639,697-700,1331,1391,2196,2467,3263,3434) or where the
+ * GPU path cannot run the call.  The Fortran wrapper maps nonzero to GM_FATAL.
+ *
+ * Every call is synchronous: on return xu/xv hold the solution (including the
+ * halo values the reference leaves in them), err and niters are set, and the
+ * library holds no pointer to caller memory.
+ */
+#ifndef CISMGPU_H
+#define CISMGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define CISMGPU_OK                0
+#define CISMGPU_EBREAKDOWN_ETA1   1  /* eta1 = (r,z) is NaN   (reference :637, :1331)            */
+#define CISMGPU_EBREAKDOWN_ALPHA  2  /* alpha is NaN           (reference :697, :1391, :2196, :2467, :3263, :3434) */
+#define CISMGPU_EUNSUPPORTED      3  /* tridiagonal precond (3,4) or tasks_row*tasks_col > 1     */
+#define CISMGPU_EINVAL            4  /* bad sizes, null pointers, inconsistent owned bounds     */
+#define CISMGPU_ECUDA             5  /* CUDA runtime error (message via cismgpu_last_error)     */
+#define CISMGPU_ETIMEOUT          6  /* a bounded device wait gave up                           */
+#define CISMGPU_ENOMEM            7  /* device allocation failed or HBM budget exceeded         */
+#define CISMGPU_ENODEV            8  /* no CUDA device / not an sm_100 device                   */
+
+/* preconditioner options, libglide/glide_types.F90:342-346 */
+#define CISMGPU_PRECOND_NONE            0
+#define CISMGPU_PRECOND_DIAG            1
+#define CISMGPU_PRECOND_SIA             2
+#define CISMGPU_PRECOND_TRIDIAG_LOCAL   3
+#define CISMGPU_PRECOND_TRIDIAG_GLOBAL  4
+
+/* Fields of type(parallel_type) read on this path (libglimmer/parallel_mpi.F90:78-153).
+ * Indices are 1-based, as in Fortran.  On one rank: periodic/no_penetration and
+ * no_ice have staggered_ilo = jlo = 3, outflow has 2; staggered_ihi = nx-2,
+ * staggered_jhi = ny-2 (parallel_mpi.F90:2640-2653). */
+typedef struct cismgpu_par {
+    int32_t staggered_ilo, staggered_ihi;
+    int32_t staggered_jlo, staggered_jhi;
+    int32_t periodic_bc;   /* logical: doubly periodic (also no_penetration, parallel_mpi.F90:2498) */
+    int32_t outflow_bc;    /* logical: zero beyond the global boundary                              */
+    int32_t no_ice_bc;     /* logical: zero the halo and the last owned row                         */
+    int32_t reprosum;      /* logical: reproducible sums requested                                  */
+    int32_t tasks_row;     /* tasks on this row    (must be 1: whole domain on one GPU)            */
+    int32_t tasks_col;     /* tasks on this column (must be 1)                                      */
+} cismgpu_par_t;
+
+/* Replaces pcg_solver_standard_3d, glissade_velo_higher_pcg.F90:827-838 (decls :895-949). */
+int cismgpu_pcg_standard_3d(int nx, int ny, int nz, const cismgpu_par_t *par,
+                            const int32_t *indxA_2d, const int32_t *indxA_3d,
+                            const int32_t *active_vertex,
+                            const double *Auu, const double *Auv,
+                            const double *Avu, const double *Avv,
+                            const double *bu, const double *bv,
+                            double *xu, double *xv,
+                            int precond, int linear_solve_ncheck,
+                            double tolerance, int maxiters,
+                            double *err, int *niters,
+                            int itest, int jtest, int rtest);
+
+/* Replaces pcg_solver_chrongear_3d, glissade_velo_higher_pcg.F90:2632-2643 (decls :2751-2805). */
+int cismgpu_pcg_chrongear_3d(int nx, int ny, int nz, const cismgpu_par_t *par,
+                             const int32_t *indxA_2d, const int32_t *indxA_3d,
+                             const int32_t *active_vertex,
+                             const double *Auu, const double *Auv,
+                             const double *Avu, const double *Avv,
+                             const double *bu, const double *bv,
+                             double *xu, double *xv,
+                             int precond, int linear_solve_ncheck,
+                             double tolerance, int maxiters,
+                             double *err, int *niters,
+                             int itest, int jtest, int rtest);
+
+/* Replaces pcg_solver_standard_2d, glissade_velo_higher_pcg.F90:67-77 (decls :109-158). */
+int cismgpu_pcg_standard_2d(int nx, int ny, const cismgpu_par_t *par,
+                            const int32_t *indxA_2d, const int32_t *active_vertex,
+                            const double *Auu, const double *Auv,
+                            const double *Avu, const double *Avv,
+                            const double *bu, const double *bv,
+                            double *xu, double *xv,
+                            int precond, int linear_solve_ncheck,
+                            double tolerance, int maxiters,
+                            double *err, int *niters,
+                            int itest, int jtest, int rtest);
+
+/* Replaces pcg_solver_chrongear_2d, glissade_velo_higher_pcg.F90:1541-1551 (decls :1581-1630). */
+int cismgpu_pcg_chrongear_2d(int nx, int ny, const cismgpu_par_t *par,
+                             const int32_t *indxA_2d, const int32_t *active_vertex,
+                             const double *Auu, const double *Auv,
+                             const double *Avu, const double *Avv,
+                             const double *bu, const double *bv,
+                             double *xu, double *xv,
+                             int precond, int linear_solve_ncheck,
+                             double tolerance, int maxiters,
+                             double *err, int *niters,
+                             int itest, int jtest, int rtest);
+
+/* Replaces matvec_multiply_structured_3d, glissade_velo_higher_pcg.F90:5528-5652
+ * (public in the reference module, :58).  y = A x on locally owned, active
+ * vertices; 0 elsewhere.  Bit-identical to the reference loop order. */
+int cismgpu_matvec_structured_3d(int nx, int ny, int nz, const cismgpu_par_t *par,
+                                 const int32_t *indxA_3d, const int32_t *active_vertex,
+                                 const double *Auu, const double *Auv,
+                                 const double *Avu, const double *Avv,
+                                 const double *xu, const double *xv,
+                                 double *yu, double *yv);
+
+/* Mirrors matvec_multiply_structured_2d, glissade_velo_higher_pcg.F90:5656-5773. */
+int cismgpu_matvec_structured_2d(int nx, int ny, const cismgpu_par_t *par,
+                                 const int32_t *indxA_2d, const int32_t *active_vertex,
+                                 const double *Auu, const double *Auv,
+                                 const double *Avu, const double *Avv,
+                                 const double *xu, const double *xv,
+                                 double *yu, double *yv);
+
+/* Message for the last nonzero status on the calling thread ("" if none). */
+const char *cismgpu_last_error(void);
+
+/* Library version string. */
+const char *cismgpu_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CISMGPU_H */

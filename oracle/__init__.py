@@ -1,0 +1,141 @@
+"""CPU oracle for the structured PCG solve -- TEST INFRASTRUCTURE ONLY.
+
+Loads oracle/_build/liboracle.so (built from oracle/pcg_oracle.cpp by
+oracle/Makefile), a loop-for-loop C++ restatement of
+libglissade/glissade_velo_higher_pcg.F90 and the one-rank semantics of
+libglimmer/parallel_mpi.F90's global sum and staggered halo.  Only tests/,
+__graft_entry__.smoke() and bench.py's CPU-baseline arm may use it, and only as
+the checker or the timed CPU baseline.
+
+Parity is unpinned against reference outputs (no Fortran compiler here and no
+golden vectors in the reference); see pcg_oracle.cpp's header.
+
+Sum modes: SUM_SEQ (the reference's order), SUM_EXACT (exact, reproducible),
+SUM_DDTREE (restatement of the GPU library's reduction tree).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+SUM_SEQ, SUM_EXACT, SUM_DDTREE = 0, 1, 2
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+
+class _Par(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int32) for n in (
+        "staggered_ilo", "staggered_ihi", "staggered_jlo", "staggered_jhi", "periodic_bc", "outflow_bc",
+        "no_ice_bc", "reprosum", "tasks_row", "tasks_col")]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        d, i, dbl = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        P = ctypes.POINTER
+        tail = [d, d, d, d, d, d, d, d, i, i, dbl, i, P(dbl), P(i), i, i, i, i]
+        L.oracle_pcg_standard_3d.argtypes = [i, i, i, P(_Par), d, d, d] + tail
+        L.oracle_pcg_chrongear_3d.argtypes = [i, i, i, P(_Par), d, d, d] + tail
+        L.oracle_pcg_standard_2d.argtypes = [i, i, P(_Par), d, d] + tail
+        L.oracle_pcg_chrongear_2d.argtypes = [i, i, P(_Par), d, d] + tail
+        L.oracle_matvec_3d.argtypes = [i, i, i, P(_Par), d, d, d, d, d, d, d, d, d, d]
+        L.oracle_matvec_2d.argtypes = [i, i, P(_Par), d, d, d, d, d, d, d, d, d, d]
+        L.oracle_halo.argtypes = [i, i, i, P(_Par), d]
+        L.oracle_global_sum.argtypes = [i, i, i, P(_Par), d, d, i]
+        L.oracle_global_sum.restype = dbl
+        L.oracle_easy_sia.argtypes = [i, i, i, d, d, d, d]
+        L.oracle_exact_sum.argtypes = [d, ctypes.c_long]
+        L.oracle_exact_sum.restype = dbl
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    assert isinstance(a, np.ndarray) and (a.flags.c_contiguous or a.flags.f_contiguous)
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def _par(par: dict) -> _Par:
+    return _Par(*(int(par[f]) for f, _ in _Par._fields_))
+
+
+def indx3():
+    return np.arange(1, 28, dtype=np.int32)
+
+
+def indx2():
+    return np.arange(1, 10, dtype=np.int32)
+
+
+def pcg(alg: str, prob, precond: int, ncheck: int = 5, tol: float = 1e-8, maxiters: int = 200,
+        summode: int = SUM_SEQ, x0=None):
+    """Run one oracle solve on a cism_b200.assembly.Problem; returns (status, xu, xv, err, niters)."""
+    L = lib()
+    xu = np.array(prob.bu * 0.0 if x0 is None else x0[0], dtype=np.float64, copy=True)
+    xv = np.array(prob.bv * 0.0 if x0 is None else x0[1], dtype=np.float64, copy=True)
+    err = ctypes.c_double(0.0)
+    nit = ctypes.c_int(0)
+    par = _par(prob.par)
+    i2 = indx2()
+    i3 = indx3()
+    common = [_p(prob.active_vertex), _p(prob.Auu), _p(prob.Auv), _p(prob.Avu), _p(prob.Avv), _p(prob.bu),
+              _p(prob.bv), _p(xu), _p(xv), precond, ncheck, tol, maxiters, ctypes.byref(err), ctypes.byref(nit),
+              1, 1, 0, summode]
+    if prob.kind == "3d":
+        f = L.oracle_pcg_standard_3d if alg == "standard" else L.oracle_pcg_chrongear_3d
+        st = f(prob.nx, prob.ny, prob.nz, ctypes.byref(par), _p(i2), _p(i3), *common)
+    else:
+        f = L.oracle_pcg_standard_2d if alg == "standard" else L.oracle_pcg_chrongear_2d
+        st = f(prob.nx, prob.ny, ctypes.byref(par), _p(i2), *common)
+    return st, xu, xv, err.value, nit.value
+
+
+def matvec(prob, xu, xv):
+    L = lib()
+    yu, yv = np.empty_like(xu), np.empty_like(xv)
+    par = _par(prob.par)
+    if prob.kind == "3d":
+        L.oracle_matvec_3d(prob.nx, prob.ny, prob.nz, ctypes.byref(par), _p(indx3()), _p(prob.active_vertex),
+                           _p(prob.Auu), _p(prob.Auv), _p(prob.Avu), _p(prob.Avv), _p(xu), _p(xv), _p(yu), _p(yv))
+    else:
+        L.oracle_matvec_2d(prob.nx, prob.ny, ctypes.byref(par), _p(indx2()), _p(prob.active_vertex),
+                           _p(prob.Auu), _p(prob.Auv), _p(prob.Avu), _p(prob.Avv), _p(xu), _p(xv), _p(yu), _p(yv))
+    return yu, yv
+
+
+def halo(nx, ny, nz, par: dict, a: np.ndarray) -> np.ndarray:
+    out = np.array(a, dtype=np.float64, copy=True)
+    p = _par(par)
+    lib().oracle_halo(nx, ny, nz, ctypes.byref(p), _p(out))
+    return out
+
+
+def global_sum(nx, ny, nz, par: dict, a1, a2, summode=SUM_SEQ) -> float:
+    p = _par(par)
+    return lib().oracle_global_sum(nx, ny, nz, ctypes.byref(p), _p(np.ascontiguousarray(a1)),
+                                   _p(np.ascontiguousarray(a2)), summode)
+
+
+def easy_sia(nx, ny, nz, active, M, b, x):
+    out = np.array(x, dtype=np.float64, copy=True)
+    lib().oracle_easy_sia(nx, ny, nz, _p(active), _p(np.ascontiguousarray(M)), _p(np.ascontiguousarray(b)),
+                          _p(out))
+    return out
+
+
+def exact_sum(a) -> float:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return lib().oracle_exact_sum(_p(a), a.size)

@@ -1,0 +1,778 @@
+// pcg_oracle.cpp -- CPU restatement of CISM's native structured PCG solve.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is the correctness oracle and the timed
+// CPU baseline for the B200 library; nothing in the product links or calls it.
+// It may be used only by tests/, __graft_entry__.smoke() and bench.py's CPU
+// baseline arm.
+//
+// PARITY STATUS: the reference is Fortran 90 and no Fortran compiler exists in
+// this build environment, and the reference ships no golden vectors or
+// known-answer tests for this path.  This restatement is therefore *unpinned*
+// against reference outputs; it is pinned against mathematical known answers
+// (dense solves, dense matvecs, Thomas vs dense) in tests/test_oracle_kat.py.
+//
+// It restates, loop for loop and in the same floating-point operation order:
+//   libglissade/glissade_velo_higher_pcg.F90
+//     pcg_solver_standard_2d          :67-823
+//     pcg_solver_standard_3d          :827-1537
+//     pcg_solver_chrongear_2d         :1541-2628
+//     pcg_solver_chrongear_3d         :2632-3594
+//     setup_preconditioner_diag_3d    :3598-3643
+//     setup_preconditioner_sia_3d     :3647-3733
+//     setup_preconditioner_diag_2d    :4199-4243
+//     matvec_multiply_structured_3d   :5528-5652
+//     matvec_multiply_structured_2d   :5656-5773
+//     easy_sia_solver                 :5777-5866
+//     tridiag_solver                  :5870-5922
+//   libglimmer/parallel_mpi.F90
+//     parallel_global_sum_stagger_*   :6537-7063  (one rank: mpi_allreduce is the identity)
+//     staggered_parallel_halo_real8_* :10609-11099 (one rank: periodic self-exchange, BC zero fill)
+//
+// Compile with -O2 -ffp-contract=off (gfortran on x86-64 does not contract a*b+c
+// into an FMA; the reference Linux build uses -O2).
+//
+// Global sums have three modes:
+//   ORACLE_SUM_SEQ    : the reference's non-reprosum order: local_sum = local_sum + arr1 + arr2,
+//                       j outer, i, k inner over owned vertices (parallel_mpi.F90:6760-6790).
+//   ORACLE_SUM_EXACT  : the exact sum of fl(arr1+arr2) over owned vertices, rounded once to
+//                       nearest-even: an order-independent reproducible sum in the spirit of
+//                       the reprosum branch (parallel_mpi.F90:6702-6758, cism_reprosum_mod.F90).
+//   ORACLE_SUM_DDTREE : a restatement of the B200 library's fixed reduction tree (double-double
+//                       column chunks of 256, warp and block trees); with it the whole solve is
+//                       bit-identical to the GPU, which isolates summation order as the only
+//                       source of difference against ORACLE_SUM_SEQ.
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+
+#include "../include/cismgpu.h"
+
+namespace {
+
+enum { ORACLE_SUM_SEQ = 0, ORACLE_SUM_EXACT = 1, ORACLE_SUM_DDTREE = 2 };
+
+// ---------------------------------------------------------------------------
+// Exact summation: a Kulisch-style fixed-point accumulator over the whole
+// double range, radix 2^32 digits held in int64 limbs (bit 0 = 2^-1074).
+// ---------------------------------------------------------------------------
+struct ExactAcc {
+    static const int NLIMB = 72;  // 72*32 = 2304 bits > 1074 + 1024 + 64 headroom
+    int64_t limb[NLIMB];
+    ExactAcc() { std::memset(limb, 0, sizeof(limb)); }
+    void add(double v) {
+        if (v == 0.0) return;
+        int e;
+        double f = std::frexp(std::fabs(v), &e);  // |v| = f * 2^e, f in [0.5,1)
+        // integer mantissa m = f*2^53, |v| = m * 2^(e-53); lsb exponent e-53 >= -1074
+        int64_t m = (int64_t)std::ldexp(f, 53);
+        int lsb = e - 53;
+        if (lsb < -1074) {  // subnormal: shift mantissa so that lsb = -1074 (exact)
+            m >>= (-1074 - lsb);
+            lsb = -1074;
+        }
+        int shift = lsb + 1074;
+        int li = shift / 32, off = shift % 32;
+        unsigned __int128 w = ((unsigned __int128)(uint64_t)m) << off;
+        int64_t sgn = v < 0 ? -1 : 1;
+        for (int t = 0; t < 3 && li + t < NLIMB; ++t) {
+            int64_t digit = (int64_t)(uint64_t)(w & 0xffffffffu);
+            limb[li + t] += sgn * digit;
+            w >>= 32;
+        }
+    }
+    double result() const {
+        // propagate carries into canonical signed digits
+        std::vector<int64_t> d(limb, limb + NLIMB);
+        for (int t = 0; t < NLIMB - 1; ++t) {
+            int64_t c = d[t] >> 32;      // arithmetic shift: floor division
+            d[t] -= c * ((int64_t)1 << 32);
+            d[t + 1] += c;
+        }
+        bool neg = d[NLIMB - 1] < 0;
+        if (neg) {  // negate the whole number: two's complement over digits
+            for (int t = 0; t < NLIMB; ++t) d[t] = -d[t];
+            for (int t = 0; t < NLIMB - 1; ++t) {
+                int64_t c = d[t] >> 32;
+                d[t] -= c * ((int64_t)1 << 32);
+                d[t + 1] += c;
+            }
+        }
+        // now all digits in [0, 2^32)
+        int top = -1;
+        for (int t = NLIMB - 1; t >= 0; --t) if (d[t] != 0) { top = t; break; }
+        if (top < 0) return 0.0;
+        int hb = 31;
+        while (!((d[top] >> hb) & 1)) --hb;
+        long P = (long)top * 32 + hb;  // index of the most significant set bit
+        auto bit = [&](long idx) -> int {
+            if (idx < 0) return 0;
+            return (int)((d[idx / 32] >> (idx % 32)) & 1);
+        };
+        double res;
+        if (P < 53) {
+            uint64_t M = 0;
+            for (long b = P; b >= 0; --b) M = (M << 1) | (uint64_t)bit(b);
+            res = std::ldexp((double)M, -1074);
+        } else {
+            uint64_t M = 0;
+            for (long b = P; b > P - 53; --b) M = (M << 1) | (uint64_t)bit(b);
+            long low = P - 53;  // bits low..0 are the remainder
+            int g = bit(low);
+            bool sticky = false;
+            for (long b = low - 1; b >= 0; --b)
+                if (bit(b)) { sticky = true; break; }
+            if (g && (sticky || (M & 1))) M += 1;
+            res = std::ldexp((double)M, (int)(P - 52 - 1074));
+        }
+        return neg ? -res : res;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Double-double arithmetic, operation order identical to the device code.
+// ---------------------------------------------------------------------------
+struct DD { double hi, lo; };
+
+inline DD dd_add_d(DD a, double x) {
+    double s = a.hi + x;
+    double bb = s - a.hi;
+    double e = (a.hi - (s - bb)) + (x - bb);
+    e = e + a.lo;
+    double hi = s + e;
+    double lo = e - (hi - s);
+    return DD{hi, lo};
+}
+
+inline DD dd_add(DD a, DD b) {
+    double s = a.hi + b.hi;
+    double bb = s - a.hi;
+    double e = (a.hi - (s - bb)) + (b.hi - bb);
+    e = e + (a.lo + b.lo);
+    double hi = s + e;
+    double lo = e - (hi - s);
+    return DD{hi, lo};
+}
+
+// Restatement of the device reduction tree.  'col_sum(q)' must return, for
+// column q (0-based, q = (i-1) + NX*(j-1)), the dd accumulation over its levels
+// k = 1..nz in order; non-owned columns return {0,0}.
+//   chunk = 256 columns; thread t of chunk c handles column c*256+t;
+//   warp tree: for off = 16,8,4,2,1: v[l] = v[l] + v[l+off]  (l+off < 32 else own)
+//   block tree over the 8 warp sums: for off = 4,2,1 (lanes >= 8 hold 0)
+//   final: 256 "threads" accumulate chunk partials c = t, t+256, ... in order,
+//          then the same warp and block trees.
+template <class F>
+double ddtree_reduce(long nq, F col_sum) {
+    const int B = 256;
+    long nchunk = (nq + B - 1) / B;
+    auto block_tree = [](std::vector<DD> &v) -> DD {
+        // v has 256 entries
+        DD w[8];
+        for (int wp = 0; wp < 8; ++wp) {
+            DD lane[32];
+            for (int l = 0; l < 32; ++l) lane[l] = v[wp * 32 + l];
+            for (int off = 16; off >= 1; off >>= 1) {
+                DD nxt[32];
+                for (int l = 0; l < 32; ++l)
+                    nxt[l] = (l + off < 32) ? dd_add(lane[l], lane[l + off]) : lane[l];
+                std::memcpy(lane, nxt, sizeof(lane));
+            }
+            w[wp] = lane[0];
+        }
+        DD lane[32];
+        for (int l = 0; l < 32; ++l) lane[l] = (l < 8) ? w[l] : DD{0.0, 0.0};
+        for (int off = 4; off >= 1; off >>= 1) {
+            DD nxt[32];
+            for (int l = 0; l < 32; ++l)
+                nxt[l] = (l + off < 32) ? dd_add(lane[l], lane[l + off]) : lane[l];
+            std::memcpy(lane, nxt, sizeof(lane));
+        }
+        return lane[0];
+    };
+    std::vector<DD> partial(nchunk);
+    std::vector<DD> v(B);
+    for (long c = 0; c < nchunk; ++c) {
+        for (int t = 0; t < B; ++t) {
+            long q = c * B + t;
+            v[t] = (q < nq) ? col_sum(q) : DD{0.0, 0.0};
+        }
+        partial[c] = block_tree(v);
+    }
+    for (int t = 0; t < B; ++t) {
+        DD acc{0.0, 0.0};
+        for (long c = t; c < nchunk; c += B) acc = dd_add(acc, partial[c]);
+        v[t] = acc;
+    }
+    DD r = block_tree(v);
+    return r.hi + r.lo;
+}
+
+// ---------------------------------------------------------------------------
+// Grid and index helpers (Fortran column-major, 1-based)
+// ---------------------------------------------------------------------------
+struct Geom {
+    int nz, NX, NY;  // NX = nx-1, NY = ny-1 vertices; nz = 1 for 2D
+    long nq() const { return (long)NX * NY; }
+    long ntot() const { return (long)nz * NX * NY; }
+    // 3D vector element (k,i,j)
+    long v3(int k, int i, int j) const { return (k - 1) + (long)nz * ((i - 1) + (long)NX * (j - 1)); }
+    // 3D block element (m,k,i,j)
+    long a3(int m, int k, int i, int j) const { return (m - 1) + 27L * v3(k, i, j); }
+    // 2D vector element (i,j)
+    long v2(int i, int j) const { return (i - 1) + (long)NX * (j - 1); }
+    // 2D block element (i,j,m)
+    long a2(int i, int j, int m) const { return (i - 1) + (long)NX * ((j - 1) + (long)NY * (m - 1)); }
+};
+
+struct Ctx {
+    Geom g;
+    cismgpu_par_t par;
+    int summode;
+    const int32_t *indx2;  // indxA_2d(-1:1,-1:1): (iA+1) + 3*(jA+1)
+    const int32_t *indx3;  // indxA_3d(-1:1,-1:1,-1:1)
+    const int32_t *active; // active_vertex(NX,NY)
+    int I2(int iA, int jA) const { return indx2[(iA + 1) + 3 * (jA + 1)]; }
+    int I3(int iA, int jA, int kA) const { return indx3[(iA + 1) + 3 * (jA + 1) + 9 * (kA + 1)]; }
+    bool act(int i, int j) const { return active[(i - 1) + (long)g.NX * (j - 1)] != 0; }
+    bool owned_col(long q) const {
+        int i = (int)(q % g.NX) + 1, j = (int)(q / g.NX) + 1;
+        return i >= par.staggered_ilo && i <= par.staggered_ihi &&
+               j >= par.staggered_jlo && j <= par.staggered_jhi;
+    }
+};
+
+typedef std::vector<double> Vec;
+
+// parallel_global_sum_stagger (3D and 2D; nz = 1 for 2D), one field with arr2.
+// Vectors are in Fortran layout (nz, NX, NY), so element (k, q) is at k-1 + nz*q.
+double global_sum(const Ctx &c, const Vec &a1, const Vec &a2) {
+    const Geom &g = c.g;
+    const cismgpu_par_t &p = c.par;
+    if (c.summode == ORACLE_SUM_SEQ) {
+        double local_sum = 0.0;
+        for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+            for (int i = p.staggered_ilo; i <= p.staggered_ihi; ++i)
+                for (int k = 1; k <= g.nz; ++k) {
+                    long e = g.v3(k, i, j);
+                    local_sum = local_sum + a1[e] + a2[e];
+                }
+        return local_sum;  // parallel_reduce_sum on one rank
+    } else if (c.summode == ORACLE_SUM_EXACT) {
+        ExactAcc acc;
+        for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+            for (int i = p.staggered_ilo; i <= p.staggered_ihi; ++i)
+                for (int k = 1; k <= g.nz; ++k) {
+                    long e = g.v3(k, i, j);
+                    acc.add(a1[e] + a2[e]);
+                }
+        return acc.result();
+    } else {
+        return ddtree_reduce(g.nq(), [&](long q) -> DD {
+            if (!c.owned_col(q)) return DD{0.0, 0.0};
+            DD acc{0.0, 0.0};
+            for (int k = 0; k < g.nz; ++k) {
+                long e = k + (long)g.nz * q;
+                acc = dd_add_d(acc, a1[e] + a2[e]);
+            }
+            return acc;
+        });
+    }
+}
+
+// staggered_parallel_halo on one rank (parallel_mpi.F90:10772-10936), nz = 1 for 2D.
+void halo(const Ctx &c, Vec &a) {
+    const Geom &g = c.g;
+    const cismgpu_par_t &p = c.par;
+    const int NX = g.NX, NY = g.NY, nz = g.nz;
+    const int lh = 2, uh = 1;
+    if (p.periodic_bc) {
+        // east-west over owned rows j = jlo..jhi; sends are captured before receives land
+        std::vector<double> wsend, esend;
+        for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+            for (int k = 1; k <= nz; ++k) wsend.push_back(a[g.v3(k, 1 + lh, j)]);
+        for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+            for (int ii = NX - uh - lh + 1; ii <= NX - uh; ++ii)
+                for (int k = 1; k <= nz; ++k) esend.push_back(a[g.v3(k, ii, j)]);
+        size_t n = 0;
+        for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+            for (int k = 1; k <= nz; ++k) a[g.v3(k, NX, j)] = wsend[n++];
+        n = 0;
+        for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+            for (int ii = 1; ii <= lh; ++ii)
+                for (int k = 1; k <= nz; ++k) a[g.v3(k, ii, j)] = esend[n++];
+        // north-south over the full i range (after the east-west update)
+        std::vector<double> ssend, nsend;
+        for (int i = 1; i <= NX; ++i)
+            for (int k = 1; k <= nz; ++k) ssend.push_back(a[g.v3(k, i, 1 + lh)]);
+        for (int jj = NY - uh - lh + 1; jj <= NY - uh; ++jj)
+            for (int i = 1; i <= NX; ++i)
+                for (int k = 1; k <= nz; ++k) nsend.push_back(a[g.v3(k, i, jj)]);
+        n = 0;
+        for (int i = 1; i <= NX; ++i)
+            for (int k = 1; k <= nz; ++k) a[g.v3(k, i, NY)] = ssend[n++];
+        n = 0;
+        for (int jj = 1; jj <= lh; ++jj)
+            for (int i = 1; i <= NX; ++i)
+                for (int k = 1; k <= nz; ++k) a[g.v3(k, i, jj)] = nsend[n++];
+    }
+    if (p.outflow_bc) {
+        for (int j = 1; j <= NY; ++j)
+            for (int k = 1; k <= nz; ++k) { a[g.v3(k, 1, j)] = 0.0; a[g.v3(k, NX, j)] = 0.0; }
+        for (int i = 1; i <= NX; ++i)
+            for (int k = 1; k <= nz; ++k) { a[g.v3(k, i, 1)] = 0.0; a[g.v3(k, i, NY)] = 0.0; }
+    } else if (p.no_ice_bc) {
+        for (int j = 1; j <= NY; ++j)
+            for (int k = 1; k <= nz; ++k) {
+                a[g.v3(k, 1, j)] = 0.0; a[g.v3(k, 2, j)] = 0.0;
+                a[g.v3(k, NX - 1, j)] = 0.0; a[g.v3(k, NX, j)] = 0.0;
+            }
+        for (int i = 1; i <= NX; ++i)
+            for (int k = 1; k <= nz; ++k) {
+                a[g.v3(k, i, 1)] = 0.0; a[g.v3(k, i, 2)] = 0.0;
+                a[g.v3(k, i, NY - 1)] = 0.0; a[g.v3(k, i, NY)] = 0.0;
+            }
+        // corner flags are false on a single rank (parallel_mpi.F90:2619-2622)
+    }
+}
+
+// matvec_multiply_structured_3d, :5528-5652
+void matvec3(const Ctx &c, const double *Auu, const double *Auv, const double *Avu, const double *Avv,
+             const Vec &xu, const Vec &xv, Vec &yu, Vec &yv) {
+    const Geom &g = c.g;
+    const cismgpu_par_t &p = c.par;
+    std::fill(yu.begin(), yu.end(), 0.0);
+    std::fill(yv.begin(), yv.end(), 0.0);
+    for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+        for (int i = p.staggered_ilo; i <= p.staggered_ihi; ++i) {
+            if (!c.act(i, j)) continue;
+            for (int k = 1; k <= g.nz; ++k) {
+                long e = g.v3(k, i, j);
+                for (int kA = -1; kA <= 1; ++kA)
+                    for (int jA = -1; jA <= 1; ++jA)
+                        for (int iA = -1; iA <= 1; ++iA) {
+                            if ((k + kA >= 1 && k + kA <= g.nz) && (i + iA >= 1 && i + iA <= g.NX) &&
+                                (j + jA >= 1 && j + jA <= g.NY)) {
+                                int m = c.I3(iA, jA, kA);
+                                long a = g.a3(m, k, i, j);
+                                long n = g.v3(k + kA, i + iA, j + jA);
+                                yu[e] = yu[e] + Auu[a] * xu[n] + Auv[a] * xv[n];
+                                yv[e] = yv[e] + Avu[a] * xu[n] + Avv[a] * xv[n];
+                            }
+                        }
+            }
+        }
+}
+
+// matvec_multiply_structured_2d, :5656-5773 (jA, iA outer; j, i inner)
+void matvec2(const Ctx &c, const double *Auu, const double *Auv, const double *Avu, const double *Avv,
+             const Vec &xu, const Vec &xv, Vec &yu, Vec &yv) {
+    const Geom &g = c.g;
+    const cismgpu_par_t &p = c.par;
+    std::fill(yu.begin(), yu.end(), 0.0);
+    std::fill(yv.begin(), yv.end(), 0.0);
+    for (int jA = -1; jA <= 1; ++jA)
+        for (int iA = -1; iA <= 1; ++iA) {
+            int m = c.I2(iA, jA);
+            for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+                for (int i = p.staggered_ilo; i <= p.staggered_ihi; ++i) {
+                    if (!c.act(i, j)) continue;
+                    if ((i + iA >= 1 && i + iA <= g.NX) && (j + jA >= 1 && j + jA <= g.NY)) {
+                        long e = g.v2(i, j);
+                        long a = g.a2(i, j, m);
+                        long n = g.v2(i + iA, j + jA);
+                        yu[e] = yu[e] + Auu[a] * xu[n] + Auv[a] * xv[n];
+                        yv[e] = yv[e] + Avu[a] * xu[n] + Avv[a] * xv[n];
+                    }
+                }
+        }
+}
+
+// tridiag_solver, :5870-5922
+void tridiag_solver(int order, const double *sbdiag, const double *diag, const double *spdiag,
+                    const double *rhs, double *soln) {
+    std::vector<double> gamma(order + 1);
+    double beta = diag[0];
+    soln[0] = rhs[0] / beta;
+    for (int k = 2; k <= order; ++k) {
+        gamma[k - 1] = spdiag[k - 2] / beta;
+        beta = diag[k - 1] - sbdiag[k - 1] * gamma[k - 1];
+        soln[k - 1] = (rhs[k - 1] - sbdiag[k - 1] * soln[k - 2]) / beta;
+    }
+    for (int k = order - 1; k >= 1; --k) soln[k - 1] = soln[k - 1] - gamma[k] * soln[k];
+}
+
+// easy_sia_solver, :5777-5866.  M is (-1:1, nz, NX, NY): element (l,k,i,j) at (l+1) + 3*v3(k,i,j).
+void easy_sia_solver(const Ctx &c, const Vec &M, const Vec &b, Vec &x) {
+    const Geom &g = c.g;
+    const int nz = g.nz;
+    std::vector<double> sb(nz), dg(nz), sp(nz), rhs(nz), soln(nz);
+    for (int j = 1; j <= g.NY; ++j)
+        for (int i = 1; i <= g.NX; ++i) {
+            if (!c.act(i, j)) continue;
+            for (int k = 1; k <= nz; ++k) { rhs[k - 1] = b[g.v3(k, i, j)]; soln[k - 1] = x[g.v3(k, i, j)]; }
+            int k = 1;
+            sb[k - 1] = 0.0;
+            dg[k - 1] = M[1 + 3 * g.v3(k, i, j)];
+            sp[k - 1] = M[2 + 3 * g.v3(k, i, j)];
+            for (k = 2; k <= nz - 1; ++k) {
+                sb[k - 1] = M[0 + 3 * g.v3(k, i, j)];
+                dg[k - 1] = M[1 + 3 * g.v3(k, i, j)];
+                sp[k - 1] = M[2 + 3 * g.v3(k, i, j)];
+            }
+            k = nz;
+            sb[k - 1] = M[0 + 3 * g.v3(k, i, j)];
+            dg[k - 1] = M[1 + 3 * g.v3(k, i, j)];
+            sp[k - 1] = 0.0;
+            tridiag_solver(nz, sb.data(), dg.data(), sp.data(), rhs.data(), soln.data());
+            for (int kk = 1; kk <= nz; ++kk) x[g.v3(kk, i, j)] = soln[kk - 1];
+        }
+}
+
+// Preconditioner state for one solve.
+struct Precond {
+    int kind;      // 0 none, 1 diag, 2 sia, other: no branch taken
+    Vec Adu, Adv;  // diagonal entries (diag)
+    Vec Muu, Mvv;  // (-1:1, nz, NX, NY) (sia)
+};
+
+void setup_precond(const Ctx &c, bool is3d, int precond, const double *Auu, const double *Avv, Precond &P) {
+    const Geom &g = c.g;
+    P.kind = precond;
+    if (precond == CISMGPU_PRECOND_DIAG) {
+        P.Adu.assign(g.ntot(), 0.0);
+        P.Adv.assign(g.ntot(), 0.0);
+        if (is3d) {  // setup_preconditioner_diag_3d :3639-3641
+            int m = c.I3(0, 0, 0);
+            for (int j = 1; j <= g.NY; ++j)
+                for (int i = 1; i <= g.NX; ++i)
+                    for (int k = 1; k <= g.nz; ++k) {
+                        P.Adu[g.v3(k, i, j)] = Auu[g.a3(m, k, i, j)];
+                        P.Adv[g.v3(k, i, j)] = Avv[g.a3(m, k, i, j)];
+                    }
+        } else {     // setup_preconditioner_diag_2d :4239-4241
+            int m = c.I2(0, 0);
+            for (int j = 1; j <= g.NY; ++j)
+                for (int i = 1; i <= g.NX; ++i) {
+                    P.Adu[g.v2(i, j)] = Auu[g.a2(i, j, m)];
+                    P.Adv[g.v2(i, j)] = Avv[g.a2(i, j, m)];
+                }
+        }
+    } else if (precond == CISMGPU_PRECOND_SIA && is3d) {  // setup_preconditioner_sia_3d :3686-3727
+        P.Muu.assign(3 * g.ntot(), 0.0);
+        P.Mvv.assign(3 * g.ntot(), 0.0);
+        for (int j = 1; j <= g.NY; ++j)
+            for (int i = 1; i <= g.NX; ++i)
+                for (int k = 1; k <= g.nz; ++k) {
+                    long e = g.v3(k, i, j);
+                    int m = c.I3(0, 0, -1);
+                    P.Muu[0 + 3 * e] = Auu[g.a3(m, k, i, j)];
+                    P.Mvv[0 + 3 * e] = Avv[g.a3(m, k, i, j)];
+                    m = c.I3(0, 0, 0);
+                    P.Muu[1 + 3 * e] = Auu[g.a3(m, k, i, j)];
+                    P.Mvv[1 + 3 * e] = Avv[g.a3(m, k, i, j)];
+                    m = c.I3(0, 0, 1);
+                    P.Muu[2 + 3 * e] = Auu[g.a3(m, k, i, j)];
+                    P.Mvv[2 + 3 * e] = Avv[g.a3(m, k, i, j)];
+                }
+    }
+}
+
+// z = PC(r), applied over the whole array (halo included), :1231-1263 / :460-480.
+void apply_precond(const Ctx &c, bool is3d, const Precond &P, const Vec &ru, const Vec &rv, Vec &zu, Vec &zv) {
+    const long n = c.g.ntot();
+    if (P.kind == CISMGPU_PRECOND_NONE) {
+        zu = ru;
+        zv = rv;
+    } else if (P.kind == CISMGPU_PRECOND_DIAG) {
+        for (long e = 0; e < n; ++e) {
+            zu[e] = (P.Adu[e] != 0.0) ? ru[e] / P.Adu[e] : 0.0;
+            zv[e] = (P.Adv[e] != 0.0) ? rv[e] / P.Adv[e] : 0.0;
+        }
+    } else if (P.kind == CISMGPU_PRECOND_SIA && is3d) {
+        easy_sia_solver(c, P.Muu, ru, zu);
+        easy_sia_solver(c, P.Mvv, rv, zv);
+    }
+    // any other value: no branch taken, z keeps its contents (as in the reference)
+}
+
+inline void mul(const Vec &a, const Vec &b, Vec &out) {
+    for (size_t e = 0; e < a.size(); ++e) out[e] = a[e] * b[e];
+}
+
+int check_args(int nx, int ny, int nz, const cismgpu_par_t *par, int precond, int ncheck, int maxiters) {
+    if (!par || nx < 5 || ny < 5 || nz < 1) return CISMGPU_EINVAL;
+    if (ncheck < 1) return CISMGPU_EINVAL;
+    if (maxiters < 0) return CISMGPU_EINVAL;
+    if (par->tasks_row * par->tasks_col != 1) return CISMGPU_EUNSUPPORTED;
+    if (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL)
+        return CISMGPU_EUNSUPPORTED;
+    if (par->staggered_ilo < 1 || par->staggered_ihi > nx - 1 || par->staggered_ilo > par->staggered_ihi ||
+        par->staggered_jlo < 1 || par->staggered_jhi > ny - 1 || par->staggered_jlo > par->staggered_jhi)
+        return CISMGPU_EINVAL;
+    return CISMGPU_OK;
+}
+
+// pcg_solver_standard_{2d,3d}: :67-823 and :827-1537
+int standard(bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indx2,
+             const int32_t *indx3, const int32_t *active, const double *Auu, const double *Auv,
+             const double *Avu, const double *Avv, const double *bu_, const double *bv_, double *xu_,
+             double *xv_, int precond, int ncheck, double tol, int maxiters, double *err, int *niters,
+             int summode) {
+    int st = check_args(nx, ny, nz, par, precond, ncheck, maxiters);
+    if (st) return st;
+    Ctx c{Geom{is3d ? nz : 1, nx - 1, ny - 1}, *par, summode, indx2, indx3, active};
+    const long n = c.g.ntot();
+    Vec bu(bu_, bu_ + n), bv(bv_, bv_ + n), xu(xu_, xu_ + n), xv(xv_, xv_ + n);
+    Vec ru(n), rv(n), du(n), dv(n), qu(n), qv(n), zu(n, 0.0), zv(n, 0.0), w0u(n), w0v(n);
+    Precond P;
+    setup_precond(c, is3d, precond, Auu, Avv, P);
+    auto matvec = [&](const Vec &a, const Vec &b, Vec &ya, Vec &yb) {
+        if (is3d) matvec3(c, Auu, Auv, Avu, Avv, a, b, ya, yb);
+        else matvec2(c, Auu, Auv, Avu, Avv, a, b, ya, yb);
+    };
+    *err = NAN;  // intent(out) and never set when no check runs; NaN makes that visible
+    int status = CISMGPU_OK;
+
+    halo(c, xu); halo(c, xv);
+    matvec(xu, xv, zu, zv);
+    for (long e = 0; e < n; ++e) { ru[e] = bu[e] - zu[e]; rv[e] = bv[e] - zv[e]; }
+    *niters = maxiters;
+    double eta0 = 1.0, eta1, eta2, alpha, beta;
+    std::fill(du.begin(), du.end(), 0.0); std::fill(dv.begin(), dv.end(), 0.0);
+    std::fill(zu.begin(), zu.end(), 0.0); std::fill(zv.begin(), zv.end(), 0.0);
+    mul(bu, bu, w0u); mul(bv, bv, w0v);
+    double L2_rhs = std::sqrt(global_sum(c, w0u, w0v));
+
+    for (int iter = 1; iter <= maxiters; ++iter) {
+        apply_precond(c, is3d, P, ru, rv, zu, zv);
+        mul(ru, zu, w0u); mul(rv, zv, w0v);
+        eta1 = global_sum(c, w0u, w0v);
+        if (eta1 != eta1) { status = CISMGPU_EBREAKDOWN_ETA1; *niters = iter; break; }
+        beta = eta1 / eta0;
+        for (long e = 0; e < n; ++e) { du[e] = zu[e] + beta * du[e]; dv[e] = zv[e] + beta * dv[e]; }
+        halo(c, du); halo(c, dv);
+        matvec(du, dv, qu, qv);
+        eta0 = eta1;
+        mul(du, qu, w0u); mul(dv, qv, w0v);
+        eta2 = global_sum(c, w0u, w0v);
+        alpha = eta1 / eta2;
+        if (alpha != alpha) { status = CISMGPU_EBREAKDOWN_ALPHA; *niters = iter; break; }
+        for (long e = 0; e < n; ++e) {
+            xu[e] = xu[e] + alpha * du[e]; xv[e] = xv[e] + alpha * dv[e];
+            ru[e] = ru[e] - alpha * qu[e]; rv[e] = rv[e] - alpha * qv[e];
+        }
+        if (iter % ncheck == 0 || iter == 5) {
+            halo(c, xu); halo(c, xv);
+            matvec(xu, xv, zu, zv);
+            for (long e = 0; e < n; ++e) { ru[e] = bu[e] - zu[e]; rv[e] = bv[e] - zv[e]; }
+            mul(ru, ru, w0u); mul(rv, rv, w0v);
+            double L2_resid = std::sqrt(global_sum(c, w0u, w0v));
+            *err = L2_resid / L2_rhs;
+            if (*err < tol) { *niters = iter; break; }
+        }
+    }
+    std::memcpy(xu_, xu.data(), n * sizeof(double));
+    std::memcpy(xv_, xv.data(), n * sizeof(double));
+    return status;
+}
+
+// pcg_solver_chrongear_{2d,3d}: :1541-2628 and :2632-3594
+int chrongear(bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indx2,
+              const int32_t *indx3, const int32_t *active, const double *Auu, const double *Auv,
+              const double *Avu, const double *Avv, const double *bu_, const double *bv_, double *xu_,
+              double *xv_, int precond, int ncheck, double tol, int maxiters, double *err, int *niters,
+              int summode) {
+    int st = check_args(nx, ny, nz, par, precond, ncheck, maxiters);
+    if (st) return st;
+    Ctx c{Geom{is3d ? nz : 1, nx - 1, ny - 1}, *par, summode, indx2, indx3, active};
+    const long n = c.g.ntot();
+    Vec bu(bu_, bu_ + n), bv(bv_, bv_ + n), xu(xu_, xu_ + n), xv(xv_, xv_ + n);
+    Vec ru(n, 0.0), rv(n, 0.0), du(n, 0.0), dv(n, 0.0), zu(n, 0.0), zv(n, 0.0), qu(n, 0.0), qv(n, 0.0);
+    Vec Azu(n, 0.0), Azv(n, 0.0), wu(n, 0.0), wv(n, 0.0), w1u(n), w1v(n), w2u(n), w2v(n);
+    Precond P;
+    setup_precond(c, is3d, precond, Auu, Avv, P);
+    auto matvec = [&](const Vec &a, const Vec &b, Vec &ya, Vec &yb) {
+        if (is3d) matvec3(c, Auu, Auv, Avu, Avv, a, b, ya, yb);
+        else matvec2(c, Auu, Auv, Avu, Avv, a, b, ya, yb);
+    };
+    *err = NAN;
+    int status = CISMGPU_OK;
+    const int maxiters_chrongear = maxiters;  // tridiag override (2D :1728-1732) is unsupported here
+    *niters = maxiters_chrongear;
+
+    mul(bu, bu, wu); mul(bv, bv, wv);
+    double bb = global_sum(c, wu, wv);
+    double L2_rhs = std::sqrt(bb);
+
+    // first pass
+    halo(c, xu); halo(c, xv);
+    matvec(xu, xv, zu, zv);
+    for (long e = 0; e < n; ++e) { ru[e] = bu[e] - zu[e]; rv[e] = bv[e] - zv[e]; }
+    halo(c, ru); halo(c, rv);
+    apply_precond(c, is3d, P, ru, rv, zu, zv);
+    mul(ru, zu, w1u); mul(rv, zv, w1v);
+    du = zu; dv = zv;
+    matvec(du, dv, qu, qv);
+    mul(du, qu, w2u); mul(dv, qv, w2v);
+    double rho_old = global_sum(c, w1u, w1v);
+    double sigma = global_sum(c, w2u, w2v);
+    halo(c, qu); halo(c, qv);
+    double alpha = rho_old / sigma;
+    if (alpha != alpha) {
+        status = CISMGPU_EBREAKDOWN_ALPHA;
+        *niters = 1;
+    } else {
+        for (long e = 0; e < n; ++e) {
+            xu[e] = xu[e] + alpha * du[e]; xv[e] = xv[e] + alpha * dv[e];
+            ru[e] = ru[e] - alpha * qu[e]; rv[e] = rv[e] - alpha * qv[e];
+        }
+        for (int iter = 2; iter <= maxiters_chrongear; ++iter) {
+            apply_precond(c, is3d, P, ru, rv, zu, zv);
+            matvec(zu, zv, Azu, Azv);
+            mul(ru, zu, w1u); mul(rv, zv, w1v);
+            mul(Azu, zu, w2u); mul(Azv, zv, w2v);
+            double rho = global_sum(c, w1u, w1v);
+            double delta = global_sum(c, w2u, w2v);
+            halo(c, Azu); halo(c, Azv);
+            double beta = rho / rho_old;
+            sigma = delta - beta * rho / alpha;
+            alpha = rho / sigma;
+            rho_old = rho;
+            if (alpha != alpha) { status = CISMGPU_EBREAKDOWN_ALPHA; *niters = iter; break; }
+            for (long e = 0; e < n; ++e) {
+                du[e] = zu[e] + beta * du[e]; dv[e] = zv[e] + beta * dv[e];
+                qu[e] = Azu[e] + beta * qu[e]; qv[e] = Azv[e] + beta * qv[e];
+                xu[e] = xu[e] + alpha * du[e]; xv[e] = xv[e] + alpha * dv[e];
+                ru[e] = ru[e] - alpha * qu[e]; rv[e] = rv[e] - alpha * qv[e];
+            }
+            if (iter % ncheck == 0 || iter == 5) {
+                matvec(xu, xv, zu, zv);
+                for (long e = 0; e < n; ++e) { ru[e] = bu[e] - zu[e]; rv[e] = bv[e] - zv[e]; }
+                mul(ru, ru, wu); mul(rv, rv, wv);
+                double rr = global_sum(c, wu, wv);
+                *err = std::sqrt(rr) / L2_rhs;
+                if (*err < tol) { *niters = iter; break; }
+                halo(c, ru); halo(c, rv);
+            }
+        }
+    }
+    std::memcpy(xu_, xu.data(), n * sizeof(double));
+    std::memcpy(xv_, xv.data(), n * sizeof(double));
+    return status;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI of the oracle (same argument lists as include/cismgpu.h plus a sum mode)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int oracle_pcg_standard_3d(int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indxA_2d,
+                           const int32_t *indxA_3d, const int32_t *active_vertex, const double *Auu,
+                           const double *Auv, const double *Avu, const double *Avv, const double *bu,
+                           const double *bv, double *xu, double *xv, int precond, int ncheck,
+                           double tolerance, int maxiters, double *err, int *niters, int itest, int jtest,
+                           int rtest, int summode) {
+    (void)itest; (void)jtest; (void)rtest;
+    return standard(true, nx, ny, nz, par, indxA_2d, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, bu, bv,
+                    xu, xv, precond, ncheck, tolerance, maxiters, err, niters, summode);
+}
+
+int oracle_pcg_chrongear_3d(int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indxA_2d,
+                            const int32_t *indxA_3d, const int32_t *active_vertex, const double *Auu,
+                            const double *Auv, const double *Avu, const double *Avv, const double *bu,
+                            const double *bv, double *xu, double *xv, int precond, int ncheck,
+                            double tolerance, int maxiters, double *err, int *niters, int itest, int jtest,
+                            int rtest, int summode) {
+    (void)itest; (void)jtest; (void)rtest;
+    return chrongear(true, nx, ny, nz, par, indxA_2d, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, bu, bv,
+                     xu, xv, precond, ncheck, tolerance, maxiters, err, niters, summode);
+}
+
+int oracle_pcg_standard_2d(int nx, int ny, const cismgpu_par_t *par, const int32_t *indxA_2d,
+                           const int32_t *active_vertex, const double *Auu, const double *Auv,
+                           const double *Avu, const double *Avv, const double *bu, const double *bv,
+                           double *xu, double *xv, int precond, int ncheck, double tolerance, int maxiters,
+                           double *err, int *niters, int itest, int jtest, int rtest, int summode) {
+    (void)itest; (void)jtest; (void)rtest;
+    return standard(false, nx, ny, 1, par, indxA_2d, nullptr, active_vertex, Auu, Auv, Avu, Avv, bu, bv,
+                    xu, xv, precond, ncheck, tolerance, maxiters, err, niters, summode);
+}
+
+int oracle_pcg_chrongear_2d(int nx, int ny, const cismgpu_par_t *par, const int32_t *indxA_2d,
+                            const int32_t *active_vertex, const double *Auu, const double *Auv,
+                            const double *Avu, const double *Avv, const double *bu, const double *bv,
+                            double *xu, double *xv, int precond, int ncheck, double tolerance, int maxiters,
+                            double *err, int *niters, int itest, int jtest, int rtest, int summode) {
+    (void)itest; (void)jtest; (void)rtest;
+    return chrongear(false, nx, ny, 1, par, indxA_2d, nullptr, active_vertex, Auu, Auv, Avu, Avv, bu, bv,
+                     xu, xv, precond, ncheck, tolerance, maxiters, err, niters, summode);
+}
+
+int oracle_matvec_3d(int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indxA_3d,
+                     const int32_t *active_vertex, const double *Auu, const double *Auv, const double *Avu,
+                     const double *Avv, const double *xu, const double *xv, double *yu, double *yv) {
+    Ctx c{Geom{nz, nx - 1, ny - 1}, *par, 0, nullptr, indxA_3d, active_vertex};
+    long n = c.g.ntot();
+    Vec a(xu, xu + n), b(xv, xv + n), ya(n), yb(n);
+    matvec3(c, Auu, Auv, Avu, Avv, a, b, ya, yb);
+    std::memcpy(yu, ya.data(), n * sizeof(double));
+    std::memcpy(yv, yb.data(), n * sizeof(double));
+    return 0;
+}
+
+int oracle_matvec_2d(int nx, int ny, const cismgpu_par_t *par, const int32_t *indxA_2d,
+                     const int32_t *active_vertex, const double *Auu, const double *Auv, const double *Avu,
+                     const double *Avv, const double *xu, const double *xv, double *yu, double *yv) {
+    Ctx c{Geom{1, nx - 1, ny - 1}, *par, 0, indxA_2d, nullptr, active_vertex};
+    long n = c.g.ntot();
+    Vec a(xu, xu + n), b(xv, xv + n), ya(n), yb(n);
+    matvec2(c, Auu, Auv, Avu, Avv, a, b, ya, yb);
+    std::memcpy(yu, ya.data(), n * sizeof(double));
+    std::memcpy(yv, yb.data(), n * sizeof(double));
+    return 0;
+}
+
+// staggered_parallel_halo on a (nz, nx-1, ny-1) array in place (nz = 1 for 2D)
+int oracle_halo(int nx, int ny, int nz, const cismgpu_par_t *par, double *a) {
+    Ctx c{Geom{nz, nx - 1, ny - 1}, *par, 0, nullptr, nullptr, nullptr};
+    long n = c.g.ntot();
+    Vec v(a, a + n);
+    halo(c, v);
+    std::memcpy(a, v.data(), n * sizeof(double));
+    return 0;
+}
+
+// parallel_global_sum_stagger(arr1, parallel, arr2) in the given mode
+double oracle_global_sum(int nx, int ny, int nz, const cismgpu_par_t *par, const double *a1, const double *a2,
+                         int summode) {
+    Ctx c{Geom{nz, nx - 1, ny - 1}, *par, summode, nullptr, nullptr, nullptr};
+    long n = c.g.ntot();
+    Vec x(a1, a1 + n), y(a2, a2 + n);
+    return global_sum(c, x, y);
+}
+
+// easy_sia_solver on a (-1:1, nz, nx-1, ny-1) matrix
+int oracle_easy_sia(int nx, int ny, int nz, const int32_t *active_vertex, const double *M, const double *b,
+                    double *x) {
+    cismgpu_par_t par{};
+    Ctx c{Geom{nz, nx - 1, ny - 1}, par, 0, nullptr, nullptr, active_vertex};
+    long n = c.g.ntot();
+    Vec MM(M, M + 3 * n), bb(b, b + n), xx(x, x + n);
+    easy_sia_solver(c, MM, bb, xx);
+    std::memcpy(x, xx.data(), n * sizeof(double));
+    return 0;
+}
+
+// exact correctly-rounded sum of n doubles
+double oracle_exact_sum(const double *a, long n) {
+    ExactAcc acc;
+    for (long e = 0; e < n; ++e) acc.add(a[e]);
+    return acc.result();
+}
+
+}  // extern "C"

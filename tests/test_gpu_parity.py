@@ -1,0 +1,190 @@
+"""Parity of the B200 library against the CPU oracle, called through the C ABI.
+
+Two bars, both on the same seeded inputs:
+  * bit-exact (x including halo entries, err, niters, status) against the oracle run
+    with its restatement of the device reduction tree (oracle.SUM_DDTREE): every
+    matvec, preconditioner, halo and vector statement is an exact restatement;
+  * against the reference's own sequential summation order (oracle.SUM_SEQ): with
+    the SIA preconditioner (the reference default) x agrees within 1e-10 relative
+    through convergence; with diagonal or no preconditioning CG trajectories are
+    sensitive to summation order, so the bar there is a converged err < tol on both
+    sides and x within 1e-6 relative.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import cism_b200 as cg
+import oracle
+from cism_b200 import assembly as asm
+from tests import problems
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_solve(alg, P, precond, ncheck=5, tol=1e-8, maxiters=200, x0=None):
+    xu = np.zeros_like(P.bu) if x0 is None else x0[0].copy()
+    xv = np.zeros_like(P.bv) if x0 is None else x0[1].copy()
+    try:
+        if P.kind == "3d":
+            f = cg.pcg_solver_standard_3d if alg == "standard" else cg.pcg_solver_chrongear_3d
+            err, nit = f(P.nx, P.ny, P.nz, P.par, asm.indxA_2d(), asm.indxA_3d(), P.active_vertex, P.Auu, P.Auv,
+                         P.Avu, P.Avv, P.bu, P.bv, xu, xv, precond, ncheck, tol, maxiters)
+        else:
+            f = cg.pcg_solver_standard_2d if alg == "standard" else cg.pcg_solver_chrongear_2d
+            err, nit = f(P.nx, P.ny, P.par, asm.indxA_2d(), P.active_vertex, P.Auu, P.Auv, P.Avu, P.Avv, P.bu,
+                         P.bv, xu, xv, precond, ncheck, tol, maxiters)
+        st = 0
+    except cg.CismGpuError as e:
+        st, err, nit = e.status, float("nan"), -1
+    return st, xu, xv, err, nit
+
+
+def rel(a, b):
+    num = np.linalg.norm(np.concatenate([(a[0] - b[0]).ravel(), (a[1] - b[1]).ravel()]))
+    den = np.linalg.norm(np.concatenate([b[0].ravel(), b[1].ravel()]))
+    return num / den
+
+
+def assert_bitexact(g, o):
+    assert g[0] == o[0], ("status", g[0], o[0])
+    if g[0] != 0:
+        return
+    np.testing.assert_array_equal(g[1], o[1])
+    np.testing.assert_array_equal(g[2], o[2])
+    assert g[4] == o[4], ("niters", g[4], o[4])
+    assert (math.isnan(g[3]) and math.isnan(o[3])) or g[3] == o[3], ("err", g[3], o[3])
+
+
+CASES_3D = [
+    ("interior-periodic", dict(seed=1)),
+    ("boundary-periodic", dict(seed=2, boundary_ice=True, bc="periodic")),
+    ("boundary-outflow", dict(seed=3, boundary_ice=True, bc="outflow")),
+    ("boundary-noice", dict(seed=4, boundary_ice=True, bc="no_ice")),
+    ("noslip", dict(seed=5, sliding=False)),
+]
+
+
+@pytest.mark.parametrize("alg", ["standard", "chrongear"])
+@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("case", CASES_3D, ids=[c[0] for c in CASES_3D])
+def test_3d_bitexact_vs_device_tree_oracle(gpu_lib, alg, precond, case):
+    P = problems.slab_3d(**case[1])
+    x0 = problems.random_x0(P, seed=7, scale=10.0)
+    o = oracle.pcg(alg, P, precond, tol=1e-8, maxiters=300, summode=oracle.SUM_DDTREE, x0=x0)
+    g = gpu_solve(alg, P, precond, tol=1e-8, maxiters=300, x0=x0)
+    assert_bitexact(g, o)
+
+
+CASES_2D = [
+    ("interior-periodic", dict(seed=1)),
+    ("boundary-periodic", dict(seed=2, boundary_ice=True, bc="periodic")),
+    ("boundary-outflow", dict(seed=3, boundary_ice=True, bc="outflow")),
+    ("boundary-noice", dict(seed=4, boundary_ice=True, bc="no_ice")),
+]
+
+
+@pytest.mark.parametrize("alg", ["standard", "chrongear"])
+@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("case", CASES_2D, ids=[c[0] for c in CASES_2D])
+def test_2d_bitexact_vs_device_tree_oracle(gpu_lib, alg, precond, case):
+    # precond 2 in 2D takes no branch in the reference (z unchanged): reproduced, not rejected
+    P = problems.slab_2d(**case[1])
+    x0 = problems.random_x0(P, seed=8, scale=10.0)
+    o = oracle.pcg(alg, P, precond, tol=1e-8, maxiters=400, summode=oracle.SUM_DDTREE, x0=x0)
+    g = gpu_solve(alg, P, precond, tol=1e-8, maxiters=400, x0=x0)
+    assert_bitexact(g, o)
+
+
+@pytest.mark.parametrize("alg,precond", [("standard", 1), ("chrongear", 2), ("standard", 2), ("chrongear", 1)])
+def test_dome_vs_reference_order(gpu_lib, alg, precond):
+    """The 31x31x11 dome (the reference's CPU case) against the reference summation order."""
+    P = asm.dome()
+    seq = oracle.pcg(alg, P, precond, maxiters=400, summode=oracle.SUM_SEQ)
+    tree = oracle.pcg(alg, P, precond, maxiters=400, summode=oracle.SUM_DDTREE)
+    g = gpu_solve(alg, P, precond, maxiters=400)
+    assert_bitexact(g, tree)
+    assert g[0] == seq[0] == 0
+    assert g[3] < 1e-8 and seq[3] < 1e-8
+    bound = 1e-10 if precond == 2 else 1e-6
+    assert rel(g[1:3], seq[1:3]) < bound
+
+
+def test_dome_trajectory_vs_reference_order(gpu_lib):
+    """At a fixed iteration count early in the solve, the diag-preconditioned trajectory
+    agrees with the reference order to 1e-10."""
+    P = asm.dome()
+    for n in (5, 20, 50):
+        seq = oracle.pcg("standard", P, 1, tol=0.0, maxiters=n, summode=oracle.SUM_SEQ)
+        g = gpu_solve("standard", P, 1, tol=0.0, maxiters=n)
+        assert g[4] == n and rel(g[1:3], seq[1:3]) < 1e-10
+
+
+def test_matvec_3d_bitexact(gpu_lib):
+    P = problems.slab_3d(seed=9, boundary_ice=True, bc="periodic")
+    rng = np.random.default_rng(3)
+    xu, xv = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bv.shape)
+    yu, yv = cg.matvec_multiply_structured_3d(P.nx, P.ny, P.nz, P.par, asm.indxA_3d(), P.active_vertex, P.Auu,
+                                              P.Auv, P.Avu, P.Avv, xu, xv)
+    eu, ev = oracle.matvec(P, xu, xv)
+    np.testing.assert_array_equal(yu, eu)
+    np.testing.assert_array_equal(yv, ev)
+
+
+def test_matvec_2d_bitexact(gpu_lib):
+    P = problems.slab_2d(seed=9, boundary_ice=True, bc="outflow")
+    rng = np.random.default_rng(4)
+    xu, xv = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bv.shape)
+    yu, yv = cg.matvec_multiply_structured_2d(P.nx, P.ny, P.par, asm.indxA_2d(), P.active_vertex, P.Auu, P.Auv,
+                                              P.Avu, P.Avv, xu, xv)
+    eu, ev = oracle.matvec(P, xu, xv)
+    np.testing.assert_array_equal(yu, eu)
+    np.testing.assert_array_equal(yv, ev)
+
+
+def test_error_statuses(gpu_lib):
+    P = problems.slab_3d(seed=2)
+    assert gpu_solve("standard", P, 3)[0] == 3
+    assert gpu_solve("chrongear", P, 4)[0] == 3
+    Q = problems.slab_3d(seed=2)
+    Q.par = dict(Q.par, tasks_col=2)
+    assert gpu_solve("standard", Q, 1)[0] == 3
+    Z = problems.slab_3d(seed=2)
+    Z.bu[:] = 0.0
+    Z.bv[:] = 0.0
+    assert gpu_solve("standard", Z, 1)[0] == oracle.pcg("standard", Z, 1)[0] == 2
+    assert gpu_solve("chrongear", Z, 2)[0] == oracle.pcg("chrongear", Z, 2)[0] == 2
+    assert gpu_solve("standard", P, 1, ncheck=0)[0] == 4
+
+
+def test_no_check_leaves_err_nan(gpu_lib):
+    P = problems.slab_3d(seed=2)
+    st, xu, xv, err, nit = gpu_solve("standard", P, 1, ncheck=10, maxiters=3)
+    assert st == 0 and nit == 3 and math.isnan(err)
+
+
+def test_golden_dense_solutions(gpu_lib):
+    import os
+    data = np.load(os.path.join(os.path.dirname(__file__), "golden", "dense_kat.npz"))
+    from tests.test_oracle_kat import owned_active_mask
+    for name in ("slab3d", "slab2d"):
+        P = problems.slab_3d(seed=21, nz=4) if name == "slab3d" else problems.slab_2d(seed=22)
+        m = owned_active_mask(P)
+        for alg in ("standard", "chrongear"):
+            st, xu, xv, err, nit = gpu_solve(alg, P, 1, tol=1e-10, maxiters=10000)
+            assert st == 0 and err < 1e-10
+            xs_u, xs_v = data[f"{name}_xu"], data[f"{name}_xv"]
+            r = np.linalg.norm(np.concatenate([(xu - xs_u)[m], (xv - xs_v)[m]])) / \
+                np.linalg.norm(np.concatenate([xs_u[m], xs_v[m]]))
+            assert r < float(data[f"{name}_bound"])
+
+
+def test_repeated_calls_reuse_workspace(gpu_lib):
+    """Same call twice (as the Picard loop does) and a size change in between give identical results."""
+    P = problems.slab_3d(seed=6)
+    a = gpu_solve("chrongear", P, 2)
+    Q = problems.slab_2d(seed=6)
+    gpu_solve("chrongear", Q, 1)
+    b = gpu_solve("chrongear", P, 2)
+    assert_bitexact(a, b)

@@ -1,0 +1,271 @@
+"""Known-answer tests that pin the CPU oracle (no GPU needed).
+
+The reference ships no golden vectors for this path and its Fortran cannot be
+compiled here, so the oracle is pinned against independent mathematics:
+dense assembly of the block stencil (matvec), a dense tridiagonal solve
+(easy_sia_solver/tridiag_solver), dense direct solves (the converged PCG
+solution), exact rational sums (global sums), hand-checked halo cases, and the
+committed fixtures under tests/golden/ (made by tests/golden/make_golden.py with
+numpy/scipy only).
+"""
+import fractions
+import math
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from cism_b200 import assembly as asm
+from tests import problems
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_matvec_3d_matches_dense_product():
+    P = problems.slab_3d(seed=3, boundary_ice=True, bc="periodic")
+    rng = np.random.default_rng(0)
+    xu, xv = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bv.shape)
+    yu, yv = oracle.matvec(P, xu, xv)
+    NY, NX, nz = P.bu.shape
+    p = P.par
+    eu, ev = np.zeros_like(yu), np.zeros_like(yv)
+    for j in range(p["staggered_jlo"] - 1, p["staggered_jhi"]):
+        for i in range(p["staggered_ilo"] - 1, p["staggered_ihi"]):
+            if not P.active_vertex[j, i]:
+                continue
+            for k in range(nz):
+                su = sv = 0.0
+                for m in range(27):
+                    iA, jA, kA = m % 3 - 1, (m // 3) % 3 - 1, m // 9 - 1
+                    jj, ii, kk = j + jA, i + iA, k + kA
+                    if 0 <= jj < NY and 0 <= ii < NX and 0 <= kk < nz:
+                        # left to right, as the reference: (y + Auu*xu) + Auv*xv
+                        su = su + P.Auu[j, i, k, m] * xu[jj, ii, kk] + P.Auv[j, i, k, m] * xv[jj, ii, kk]
+                        sv = sv + P.Avu[j, i, k, m] * xu[jj, ii, kk] + P.Avv[j, i, k, m] * xv[jj, ii, kk]
+                eu[j, i, k], ev[j, i, k] = su, sv
+    np.testing.assert_array_equal(yu, eu)  # same loop order -> bit identical
+    np.testing.assert_array_equal(yv, ev)
+
+
+def test_matvec_2d_matches_dense_product():
+    P = problems.slab_2d(seed=4, boundary_ice=True, bc="outflow")
+    rng = np.random.default_rng(1)
+    xu, xv = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bv.shape)
+    yu, yv = oracle.matvec(P, xu, xv)
+    NY, NX = P.bu.shape
+    p = P.par
+    eu, ev = np.zeros_like(yu), np.zeros_like(yv)
+    for m in range(9):  # jA, iA outer as in the reference
+        iA, jA = m % 3 - 1, m // 3 - 1
+        for j in range(p["staggered_jlo"] - 1, p["staggered_jhi"]):
+            for i in range(p["staggered_ilo"] - 1, p["staggered_ihi"]):
+                if P.active_vertex[j, i] and 0 <= i + iA < NX and 0 <= j + jA < NY:
+                    eu[j, i] = eu[j, i] + P.Auu[m, j, i] * xu[j + jA, i + iA] + P.Auv[m, j, i] * xv[j + jA, i + iA]
+                    ev[j, i] = ev[j, i] + P.Avu[m, j, i] * xu[j + jA, i + iA] + P.Avv[m, j, i] * xv[j + jA, i + iA]
+    np.testing.assert_array_equal(yu, eu)
+    np.testing.assert_array_equal(yv, ev)
+
+
+def test_easy_sia_matches_dense_tridiagonal_solve():
+    rng = np.random.default_rng(5)
+    nx, ny, nz = 7, 6, 9
+    NX, NY = nx - 1, ny - 1
+    M = rng.standard_normal((NY, NX, nz, 3))
+    M[..., 1] = 4.0 + np.abs(M[..., 1])
+    active = (rng.random((NY, NX)) > 0.3).astype(np.int32)
+    b = rng.standard_normal((NY, NX, nz))
+    x0 = rng.standard_normal((NY, NX, nz))
+    x = oracle.easy_sia(nx, ny, nz, active, M, b, x0)
+    for j in range(NY):
+        for i in range(NX):
+            if not active[j, i]:
+                np.testing.assert_array_equal(x[j, i], x0[j, i])  # inactive columns keep x
+                continue
+            T = np.zeros((nz, nz))
+            for k in range(nz):
+                T[k, k] = M[j, i, k, 1]
+                if k > 0:
+                    T[k, k - 1] = M[j, i, k, 0]
+                if k < nz - 1:
+                    T[k, k + 1] = M[j, i, k, 2]
+            np.testing.assert_allclose(x[j, i], np.linalg.solve(T, b[j, i]), rtol=1e-12, atol=1e-12)
+
+
+def test_exact_sum_is_correctly_rounded():
+    rng = np.random.default_rng(7)
+    for trial in range(20):
+        a = rng.standard_normal(500) * np.exp(rng.uniform(-40, 40, 500))
+        a[::7] *= -1e-17
+        exact = sum(fractions.Fraction(float(v)) for v in a)
+        assert oracle.exact_sum(a) == float(exact)
+        assert oracle.exact_sum(a) == math.fsum(a)
+    # cancellation and subnormals
+    a = np.array([1e308, 1.0, -1e308, 5e-324, 5e-324])
+    assert oracle.exact_sum(a) == math.fsum(a)
+    assert oracle.exact_sum(np.array([0.1] * 10)) == math.fsum([0.1] * 10)
+
+
+def test_global_sum_modes_owned_range():
+    P = problems.slab_3d(seed=1)
+    rng = np.random.default_rng(2)
+    a1, a2 = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bu.shape)
+    p = P.par
+    sl = (slice(p["staggered_jlo"] - 1, p["staggered_jhi"]), slice(p["staggered_ilo"] - 1, p["staggered_ihi"]))
+    seq = 0.0
+    for j in range(p["staggered_jlo"] - 1, p["staggered_jhi"]):
+        for i in range(p["staggered_ilo"] - 1, p["staggered_ihi"]):
+            for k in range(P.nz):
+                seq = seq + a1[j, i, k] + a2[j, i, k]
+    assert oracle.global_sum(P.nx, P.ny, P.nz, p, a1, a2, oracle.SUM_SEQ) == seq
+    summ = (a1[sl] + a2[sl]).ravel()
+    assert oracle.global_sum(P.nx, P.ny, P.nz, p, a1, a2, oracle.SUM_EXACT) == math.fsum(summ)
+    assert oracle.global_sum(P.nx, P.ny, P.nz, p, a1, a2, oracle.SUM_DDTREE) == math.fsum(summ)
+
+
+@pytest.mark.parametrize("bc", ["periodic", "outflow", "no_ice"])
+def test_halo_semantics(bc):
+    nx, ny, nz = 9, 8, 2
+    par = asm.default_par(nx, ny, bc)
+    NX, NY = nx - 1, ny - 1
+    a = np.arange(NY * NX * nz, dtype=np.float64).reshape(NY, NX, nz) + 1.0
+    h = oracle.halo(nx, ny, nz, par, a)
+    if bc == "periodic":
+        src_i = {0: NX - 3, 1: NX - 2, NX - 1: 2}
+        for j in range(NY):
+            for i in range(NX):
+                si, sj = src_i.get(i, i), {0: NY - 3, 1: NY - 2, NY - 1: 2}.get(j, j)
+                np.testing.assert_array_equal(h[j, i], a[sj, si])
+    elif bc == "outflow":
+        assert np.all(h[:, 0] == 0) and np.all(h[:, -1] == 0) and np.all(h[0] == 0) and np.all(h[-1] == 0)
+        np.testing.assert_array_equal(h[1:-1, 1:-1], a[1:-1, 1:-1])
+    else:
+        for z in (0, 1, NX - 2, NX - 1):
+            assert np.all(h[:, z] == 0)
+        for z in (0, 1, NY - 2, NY - 1):
+            assert np.all(h[z] == 0)
+        np.testing.assert_array_equal(h[2:-2, 2:-2], a[2:-2, 2:-2])
+
+
+def owned_active_mask(P):
+    p = P.par
+    m = np.zeros(P.active_vertex.shape, dtype=bool)
+    m[p["staggered_jlo"] - 1:p["staggered_jhi"], p["staggered_ilo"] - 1:p["staggered_ihi"]] = True
+    m &= P.active_vertex != 0
+    return np.broadcast_to(m[..., None], P.bu.shape) if P.kind == "3d" else m
+
+
+def _owned_active_dense(P):
+    """Dense operator of the PCG on owned active nodes with zero halo values (interior-ice cases)."""
+    nz = P.nz
+    p = P.par
+    idx = {}
+    for j in range(p["staggered_jlo"] - 1, p["staggered_jhi"]):
+        for i in range(p["staggered_ilo"] - 1, p["staggered_ihi"]):
+            if P.active_vertex[j, i]:
+                for k in range(nz):
+                    idx[(j, i, k)] = len(idx)
+    n = len(idx)
+    A = np.zeros((2 * n, 2 * n))
+    b = np.zeros(2 * n)
+    for (j, i, k), r in idx.items():
+        b[r], b[n + r] = (P.bu[j, i, k], P.bv[j, i, k]) if P.kind == "3d" else (P.bu[j, i], P.bv[j, i])
+        for m in range(27 if P.kind == "3d" else 9):
+            iA, jA = m % 3 - 1, (m // 3) % 3 - 1
+            kA = m // 9 - 1 if P.kind == "3d" else 0
+            c = idx.get((j + jA, i + iA, k + kA))
+            if c is None:
+                continue
+            if P.kind == "3d":
+                A[r, c] += P.Auu[j, i, k, m]; A[r, n + c] += P.Auv[j, i, k, m]
+                A[n + r, c] += P.Avu[j, i, k, m]; A[n + r, n + c] += P.Avv[j, i, k, m]
+            else:
+                A[r, c] += P.Auu[m, j, i]; A[r, n + c] += P.Auv[m, j, i]
+                A[n + r, c] += P.Avu[m, j, i]; A[n + r, n + c] += P.Avv[m, j, i]
+    return idx, A, b
+
+
+@pytest.mark.parametrize("alg", ["standard", "chrongear"])
+@pytest.mark.parametrize("precond", [0, 1, 2])
+def test_pcg_converges_to_dense_solution_3d(alg, precond):
+    P = problems.slab_3d(seed=11, nz=4)
+    idx, A, b = _owned_active_dense(P)
+    assert np.allclose(A, A.T, rtol=1e-10, atol=1e-12 * np.abs(A).max())
+    xs = np.linalg.solve(A, b)
+    # attainable accuracy of CG is about eps * cond(A) ~ 1e-10 here; the reference
+    # algorithm (residual replacement without restart) diverges if asked for more
+    # Chronopoulos-Gear without preconditioning stagnates near 1e-8 on this system
+    # (q is not recomputed after residual replacement, :3482-3579)
+    tol = 1e-7 if (alg, precond) == ("chrongear", 0) else 1e-10
+    st, xu, xv, err, nit = oracle.pcg(alg, P, precond, tol=tol, maxiters=5000)
+    assert st == 0 and err < tol and nit < 5000
+    n = len(idx)
+    got = np.zeros(2 * n)
+    for (j, i, k), r in idx.items():
+        got[r], got[n + r] = xu[j, i, k], xv[j, i, k]
+    cond = np.linalg.cond(A)
+    assert np.linalg.norm(got - xs) / np.linalg.norm(xs) < tol * cond * 10
+
+
+@pytest.mark.parametrize("alg", ["standard", "chrongear"])
+def test_pcg_converges_to_dense_solution_2d(alg):
+    P = problems.slab_2d(seed=12)
+    idx, A, b = _owned_active_dense(P)
+    xs = np.linalg.solve(A, b)
+    st, xu, xv, err, nit = oracle.pcg(alg, P, 1, tol=1e-10, maxiters=5000)
+    assert st == 0 and err < 1e-10
+    n = len(idx)
+    got = np.zeros(2 * n)
+    for (j, i, k), r in idx.items():
+        got[r], got[n + r] = xu[j, i], xv[j, i]
+    assert np.linalg.norm(got - xs) / np.linalg.norm(xs) < 1e-10 * np.linalg.cond(A) * 10
+
+
+def test_sum_modes_agree_in_trajectory_for_sia():
+    """Only summation order differs between the modes: with the SIA preconditioner the
+    iterates stay within 1e-10 of the reference order through convergence."""
+    P = asm.dome()
+    ref = oracle.pcg("chrongear", P, 2, summode=oracle.SUM_SEQ)
+    for mode in (oracle.SUM_EXACT, oracle.SUM_DDTREE):
+        got = oracle.pcg("chrongear", P, 2, summode=mode)
+        assert got[0] == ref[0] == 0 and got[4] == ref[4]
+        num = np.linalg.norm(np.concatenate([(got[1] - ref[1]).ravel(), (got[2] - ref[2]).ravel()]))
+        den = np.linalg.norm(np.concatenate([ref[1].ravel(), ref[2].ravel()]))
+        assert num / den < 1e-10
+
+
+def test_error_statuses():
+    P = problems.slab_3d(seed=2)
+    assert oracle.pcg("standard", P, 3)[0] == 3          # tridiagonal precond: unsupported
+    par = dict(P.par, tasks_row=2)
+    Q = problems.slab_3d(seed=2)
+    Q.par = par
+    assert oracle.pcg("chrongear", Q, 1)[0] == 3          # more than one task
+    Z = problems.slab_3d(seed=2)
+    Z.bu[:] = 0.0
+    Z.bv[:] = 0.0
+    assert oracle.pcg("standard", Z, 1)[0] == 2           # b = x0 = 0: eta2 = 0, alpha = NaN
+    assert oracle.pcg("chrongear", Z, 1)[0] == 2
+
+
+def test_no_check_leaves_err_nan():
+    P = problems.slab_3d(seed=2)
+    st, xu, xv, err, nit = oracle.pcg("standard", P, 1, ncheck=10, maxiters=3)
+    assert st == 0 and nit == 3 and math.isnan(err)
+
+
+def test_golden_dense_solutions():
+    """Committed fixtures: dense-LU solutions of small assembled systems."""
+    path = os.path.join(GOLDEN, "dense_kat.npz")
+    data = np.load(path)
+    for name in ("slab3d", "slab2d"):
+        P = problems.slab_3d(seed=21, nz=4) if name == "slab3d" else problems.slab_2d(seed=22)
+        np.testing.assert_array_equal(P.bu, data[f"{name}_bu"])  # generator unchanged
+        xs_u, xs_v = data[f"{name}_xu"], data[f"{name}_xv"]
+        for alg in ("standard", "chrongear"):
+            st, xu, xv, err, nit = oracle.pcg(alg, P, 1, tol=1e-10, maxiters=10000)
+            assert st == 0
+            m = owned_active_mask(P)  # halo entries of x hold periodic copies, as in the reference
+            rel = np.linalg.norm(np.concatenate([(xu - xs_u)[m], (xv - xs_v)[m]])) / \
+                np.linalg.norm(np.concatenate([xs_u[m], xs_v[m]]))
+            assert rel < float(data[f"{name}_bound"]), (name, alg, rel)
