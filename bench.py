@@ -1,0 +1,399 @@
+"""Benchmark: solves/sec (and p50/p99 latency) to a 1e-8 FP64 relative residual.
+
+Workload (default, one GPU): the 401x401-node 2D SSA system, Chronopoulos-Gear PCG
+with the diagonal (Jacobi) preconditioner, first-Picard assembly of a seeded
+smooth random thickness field (500-2000 m) and log-normal basal friction
+(mu = ln 1e3 Pa yr/m, sigma = 1), dx = 1 km.  Synthetic data: the reference runs
+no public dataset for this path.
+
+Our arm ("ours"): the mixed-precision persistent Chronopoulos-Gear solver
+(FP32 recurrences, FP64 x, FP64 residual replacement every 5 iterations) on a
+device-resident handle; the plain FP64 GPU PCG (the reference algorithm statement
+by statement, bit-identical to the oracle) is timed beside it on the same handle.
+L2 is flushed (256 MiB write) before every timed solve.
+`e2e` is the same metric through the reference-signature C-ABI call
+(cismgpu_pcg_chrongear_2d) with pinned host buffers: upload of A, b, x0 and the
+download of x inside the timed region.
+
+Reference arm (`--impl reference`): the CPU restatement of the reference PCG
+(oracle/, FP64, reference summation order) on all host cores, one independent
+solve per core; each timed step runs a bounded number of iterations per core and
+is scaled to a full solve by the iteration count of a full solve.
+
+Launch: python bench.py [--gpus N --steps K --warmup W] (torchrun for N > 1:
+each rank solves its own replica, scaling "weak").
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "solves/sec and p50/p99 latency at 1e-8 rel. residual vs plain FP64 GPU PCG"
+UNIT = "solves/s"
+WORKLOAD = "cfg2: 2D SSA 401x401 nodes, dx=1 km, Chronopoulos-Gear PCG + diagonal (Jacobi) precond, tol 1e-8"
+TOL, NCHECK, MAXITERS, PRECOND = 1e-8, 5, 20000, 1
+PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def make_problem(workload="cfg2"):
+    from cism_b200 import assembly as asm
+    if workload == "cfg2":
+        return asm.ssa_random(ewn=401, nsn=401, dx=1000.0, seed=7)
+    if workload == "cfg3":   # 201x201x11 ice stream, no-slip bed
+        return asm.ice_stream(ewn=201, nsn=201, nz=11, dx=2000.0)
+    if workload == "dome":   # cfg1: 31x31x11 dome
+        return asm.dome()
+    raise ValueError(workload)
+
+
+PROFILE_PRECOND = {"cfg2": 1, "cfg3": 2, "dome": 2}
+
+
+def run_profile(args):
+    """Only the product path (mixed solves) on one workload: the command ncu captures."""
+    import torch
+    import cism_b200 as cg
+    from cism_b200 import build
+    build.build()
+    P = make_problem(args.workload)
+    S = cg.DeviceSolver(P)
+    pc = PROFILE_PRECOND[args.workload]
+    for k in range(args.warmup + args.steps):
+        e, n = S.solve(cg.ALG_MIXED_CHRONGEAR, pc, NCHECK, TOL, MAXITERS)
+    torch.cuda.synchronize()
+    print(f"profile workload={args.workload} precond={pc} niters={n} err={e:.3e} unknowns={P.n_unknowns}")
+    return 0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+def ncu_traffic(kernel_key):
+    """Per-launch DRAM bytes of a kernel from the committed ncu summary (profiles/*.md), or None."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel_key)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU restatement on all host cores
+# ---------------------------------------------------------------------------
+_WORKER_PROBLEM = None
+
+
+def _ref_worker(niters):
+    global _WORKER_PROBLEM
+    import oracle
+    if _WORKER_PROBLEM is None:
+        _WORKER_PROBLEM = make_problem()
+    P = _WORKER_PROBLEM
+    t0 = time.perf_counter()
+    oracle.pcg("chrongear", P, PRECOND, ncheck=NCHECK, tol=0.0, maxiters=niters, summode=oracle.SUM_SEQ)
+    return time.perf_counter() - t0
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    import oracle
+    oracle.build()
+    cores = os.cpu_count() or 1
+    # full-solve iteration count of the reference algorithm (one full solve, untimed)
+    P = make_problem()
+    st, xu, xv, err, nfull = oracle.pcg("chrongear", P, PRECOND, ncheck=NCHECK, tol=TOL, maxiters=MAXITERS,
+                                        summode=oracle.SUM_SEQ)
+    sample_iters = 100
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(cores) as pool:
+        for _ in range(max(args.warmup, 0)):
+            pool.map(_ref_worker, [10] * cores)
+        rates = []
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            times = pool.map(_ref_worker, [sample_iters] * cores)
+            per_iter = max(times) / sample_iters      # all cores run concurrently
+            rates.append(cores / (per_iter * nfull))  # full solves per second, all cores
+        wall = time.perf_counter() - t0
+    value = float(np.median(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(args.steps, 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "solver": "reference PCG restated in C++ (oracle/), FP64, sequential sums"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{sample_iters} Chronopoulos-Gear iterations per core per step, scaled to the "
+                                   f"{nfull} iterations of a full solve to 1e-8 (err {err:.2e})"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def cpu_baseline_sample(P, niters_full):
+    """The oracle (reference order, FP64) on one core, a bounded sample scaled to a full solve."""
+    import oracle
+    oracle.build()
+    sample = 600
+    t0 = time.perf_counter()
+    oracle.pcg("chrongear", P, PRECOND, ncheck=NCHECK, tol=0.0, maxiters=sample, summode=oracle.SUM_SEQ)
+    dt = time.perf_counter() - t0
+    per_iter = dt / sample
+    return {"value": 1.0 / (per_iter * niters_full), "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{sample} Chronopoulos-Gear iterations ({dt:.1f} s) on 1 core, scaled to the {niters_full} "
+                      f"iterations the FP64 reference algorithm takes to reach 1e-8"}
+
+
+def run_ours(args):
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    import cism_b200 as cg
+    from cism_b200 import build
+    build.build()
+    cg.load_library()
+    P = make_problem()
+    stream = torch.cuda.Stream()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    S = cg.DeviceSolver(P, stream=stream.cuda_stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg:
+            pg.barrier()
+
+    # --- warm-up of the product path ---
+    for _ in range(max(args.warmup, 3)):
+        with torch.cuda.stream(stream):
+            S.solve(cg.ALG_MIXED_CHRONGEAR, PRECOND, NCHECK, TOL, MAXITERS)
+    stream.synchronize()
+
+    # --- timed region ---
+    S.profile(True)
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    errs, nits = [], []
+    with torch.cuda.stream(stream):
+        t_start.record(stream)
+        for k in range(args.steps):
+            flush.fill_(float(k))
+            evs[k][0].record(stream)
+            e, n = S.solve(cg.ALG_MIXED_CHRONGEAR, PRECOND, NCHECK, TOL, MAXITERS)
+            evs[k][1].record(stream)
+            errs.append(e)
+            nits.append(n)
+        t_end.record(stream)
+    stream.synchronize()
+    barrier()
+    clk = clocks.stop()
+    total_ms = t_start.elapsed_time(t_end)
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    if pg:
+        t = torch.tensor([total_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        total_ms = float(t.item())
+    prof_ms, prof_n, prof_bytes = S.profile_read()
+    S.profile(False)
+    # --- plain FP64 GPU PCG (reference algorithm, bit-identical to the oracle) ---
+    with torch.cuda.stream(stream):
+        e64, n64 = S.solve(cg.ALG_CHRONGEAR, PRECOND, NCHECK, TOL, MAXITERS)  # warm
+    x64 = S.x()
+    fp64_ms = []
+    for _ in range(2):
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            ev0.record(stream)
+            S.solve(cg.ALG_CHRONGEAR, PRECOND, NCHECK, TOL, MAXITERS)
+            ev1.record(stream)
+        stream.synchronize()
+        fp64_ms.append(ev0.elapsed_time(ev1))
+    fp64_solve_ms = float(np.median(fp64_ms))
+
+    xm = S.x()
+    num = math.sqrt(float(np.sum((xm[0] - x64[0]) ** 2) + np.sum((xm[1] - x64[1]) ** 2)))
+    den = math.sqrt(float(np.sum(x64[0] ** 2) + np.sum(x64[1] ** 2)))
+    err_vs_fp64 = num / den
+
+    value = world * args.steps / (total_ms / 1e3)
+    peak, peak_kind = hbm_peak()
+    avg_launch_ms = prof_ms / max(prof_n, 1)
+    achieved = prof_bytes / (avg_launch_ms / 1e3) / 1e9 if prof_n else None
+    traffic = ncu_traffic("k_mixed<9,1>:cfg2")
+
+    # --- end to end through the reference-signature C-ABI call, pinned host buffers ---
+    e2e = None
+    if True:
+        pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+        Auu, Auv, Avu, Avv = pin(P.Auu), pin(P.Auv), pin(P.Avu), pin(P.Avv)
+        bu, bv, act = pin(P.bu), pin(P.bv), pin(P.active_vertex)
+        xu, xv = pin(np.zeros_like(P.bu)), pin(np.zeros_like(P.bv))
+        from cism_b200 import assembly as asm
+        i2 = asm.indxA_2d()
+        prev = cg.set_oneshot_algorithm(cg.ALG_MIXED_CHRONGEAR)
+        e2e_ms = []
+        try:
+            for k in range(max(2, args.steps // 2) + 1):
+                xu[...] = 0.0
+                xv[...] = 0.0
+                flush.fill_(1.0)
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                cg.pcg_solver_chrongear_2d(P.nx, P.ny, P.par, i2, act, Auu, Auv, Avu, Avv, bu, bv, xu, xv, PRECOND,
+                                           NCHECK, TOL, MAXITERS)
+                dt = time.perf_counter() - t0
+                if k > 0:  # the first call allocates the workspace
+                    e2e_ms.append(1e3 * dt)
+        finally:
+            cg.set_oneshot_algorithm(prev)
+        h2d = sum(a.nbytes for a in (Auu, Auv, Avu, Avv, bu, bv, xu, xv, act)) + 9 * 4
+        d2h = xu.nbytes + xv.nbytes
+        e2e = {"value": world * 1e3 / float(np.mean(e2e_ms)), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_solve": float(np.mean(e2e_ms)),
+               "path": "cismgpu_pcg_chrongear_2d (reference signature), mixed algorithm, pinned host buffers"}
+
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return 0
+    cpu = cpu_baseline_sample(P, n64) if world == 1 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 recurrences + f64 x/dots/residual", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "solver": "mixed-precision persistent Chronopoulos-Gear (one launch per solve)",
+                   "l2": "flushed (256 MiB write) before every solve", "parallelism": f"replicas x{world}",
+                   "unknowns": P.n_unknowns},
+        "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
+        "niters": int(np.median(nits)), "err": float(max(errs)), "err_vs_fp64_solution": err_vs_fp64,
+        "fp64_plain": {"solves_per_s": 1e3 / fp64_solve_ms, "ms_per_solve": fp64_solve_ms, "niters": n64,
+                       "err": e64, "solver": "reference Chronopoulos-Gear statement by statement, FP64"},
+        "speedup_vs_fp64_plain": value / world / (1e3 / fp64_solve_ms),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                     "kernel": "k_mixed<9,1> (whole solve in one cooperative launch)",
+                     "peak_kind": peak_kind,
+                     "note": "algorithmic bytes = FP32 iterations x 264 B + FP64 checks x 328 B per active vertex; "
+                             "the 2D working set (~40 MB) stays in L2 across iterations"},
+        "cpu_baseline": cpu, "e2e": e2e,
+        "gpu_launches": 3 * args.steps, "clocks": clk,
+    }
+    print(json.dumps(line))
+    if pg:
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--mode", default="bench", choices=["bench", "profile"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "dome"])
+    args = ap.parse_args()
+    if args.mode == "profile":
+        return run_profile(args)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -26,8 +26,11 @@ __all__ = [
     "ParallelType", "CismGpuError", "load_library", "pcg_solver_standard_3d", "pcg_solver_chrongear_3d",
     "pcg_solver_standard_2d", "pcg_solver_chrongear_2d", "matvec_multiply_structured_3d",
     "matvec_multiply_structured_2d", "HO_PRECOND_NONE", "HO_PRECOND_DIAG", "HO_PRECOND_SIA",
-    "HO_PRECOND_TRIDIAG_LOCAL", "HO_PRECOND_TRIDIAG_GLOBAL",
+    "HO_PRECOND_TRIDIAG_LOCAL", "HO_PRECOND_TRIDIAG_GLOBAL", "DeviceSolver", "solve_batch",
+    "ALG_STANDARD", "ALG_CHRONGEAR", "ALG_MIXED_CHRONGEAR",
 ]
+
+ALG_STANDARD, ALG_CHRONGEAR, ALG_MIXED_CHRONGEAR = 0, 1, 2
 
 # libglide/glide_types.F90:342-346
 HO_PRECOND_NONE = 0
@@ -107,6 +110,25 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_matvec_structured_3d.restype = ctypes.c_int
     lib.cismgpu_matvec_structured_2d.argtypes = [i32, i32, par, d, d, d, d, d, d, d, d, d, d]
     lib.cismgpu_matvec_structured_2d.restype = ctypes.c_int
+    vp = ctypes.c_void_p
+    lib.cismgpu_solver_create.argtypes = [P(vp), i32, i32, i32, i32, par, d, d, d, d, d, d, d, d, d, d, vp]
+    lib.cismgpu_solver_create.restype = ctypes.c_int
+    lib.cismgpu_solver_solve.argtypes = [vp, i32, i32, i32, dbl, i32, P(dbl), P(i32)]
+    lib.cismgpu_solver_solve.restype = ctypes.c_int
+    lib.cismgpu_solver_solve_batch.argtypes = [P(vp), i32, i32, i32, i32, dbl, i32, P(dbl), P(i32), P(i32), vp]
+    lib.cismgpu_solver_solve_batch.restype = ctypes.c_int
+    lib.cismgpu_solver_get_x.argtypes = [vp, d, d]
+    lib.cismgpu_solver_get_x.restype = ctypes.c_int
+    lib.cismgpu_solver_profile.argtypes = [vp, i32]
+    lib.cismgpu_solver_profile.restype = ctypes.c_int
+    lib.cismgpu_solver_profile_read.argtypes = [vp, P(dbl), P(i32), P(dbl)]
+    lib.cismgpu_solver_profile_read.restype = ctypes.c_int
+    lib.cismgpu_solver_device_bytes.argtypes = [vp]
+    lib.cismgpu_solver_device_bytes.restype = ctypes.c_size_t
+    lib.cismgpu_solver_destroy.argtypes = [vp]
+    lib.cismgpu_solver_destroy.restype = ctypes.c_int
+    lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
+    lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
     lib.cismgpu_last_error.restype = ctypes.c_char_p
     lib.cismgpu_version.restype = ctypes.c_char_p
     _lib = lib
@@ -160,6 +182,11 @@ def _solve(fname: str, is3d: bool, nx, ny, nz, parallel, indxA_2d, indxA_3d, act
         ctypes.byref(niters), int(itest), int(jtest), int(rtest)]
     _check(lib, getattr(lib, fname)(*args))
     return err.value, niters.value
+
+
+def set_oneshot_algorithm(algorithm: int = -1) -> int:
+    """Select the algorithm of the reference-signature calls (-1: the one each call names, FP64)."""
+    return int(load_library().cismgpu_set_oneshot_algorithm(int(algorithm)))
 
 
 def pcg_solver_standard_3d(nx, ny, nz, parallel, indxA_2d, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, bu, bv,
@@ -219,3 +246,94 @@ def matvec_multiply_structured_2d(nx, ny, parallel, indxA_2d, active_vertex, Auu
         _ptr(Avu, np.float64, nv * 9), _ptr(Avv, np.float64, nv * 9), _ptr(xu, np.float64, nv),
         _ptr(xv, np.float64, nv), _ptr(yu, np.float64, nv, True), _ptr(yv, np.float64, nv, True)))
     return yu, yv
+
+
+class DeviceSolver:
+    """A device-resident linear system (cismgpu_solver_create): A, b and x0 live in HBM.
+
+    ``problem`` is a cism_b200.assembly.Problem (or any object with the same fields).
+    ``stream`` is a CUDA stream handle (int) or None for a private stream.
+    """
+
+    def __init__(self, problem, x0=None, stream=None):
+        lib = load_library()
+        self._lib = lib
+        P = problem
+        self.problem = P
+        is3d = P.kind == "3d"
+        nv = (P.nx - 1) * (P.ny - 1)
+        nvec = nv * (P.nz if is3d else 1)
+        nblk = nvec * (27 if is3d else 9)
+        indx = np.arange(1, 28 if is3d else 10, dtype=np.int32)
+        self._keep = [indx]
+        par = _par(P.par)
+        self._par = par
+        h = ctypes.c_void_p()
+        xu0 = xv0 = None
+        if x0 is not None:
+            xu0, xv0 = _ptr(x0[0], np.float64, nvec), _ptr(x0[1], np.float64, nvec)
+            self._keep += [x0]
+        st = lib.cismgpu_solver_create(
+            ctypes.byref(h), 3 if is3d else 2, P.nx, P.ny, P.nz if is3d else 1, ctypes.byref(par),
+            _ptr(indx, np.int32, indx.size), _ptr(P.active_vertex, np.int32, nv), _ptr(P.Auu, np.float64, nblk),
+            _ptr(P.Auv, np.float64, nblk), _ptr(P.Avu, np.float64, nblk), _ptr(P.Avv, np.float64, nblk),
+            _ptr(P.bu, np.float64, nvec), _ptr(P.bv, np.float64, nvec), xu0, xv0,
+            ctypes.c_void_p(stream) if stream else None)
+        _check(lib, st)
+        self.handle = h
+        self._shape = P.bu.shape
+
+    def solve(self, algorithm=ALG_CHRONGEAR, precond=HO_PRECOND_DIAG, ncheck=5, tol=1e-8, maxiters=200):
+        """Returns (err, niters); raises CismGpuError on a nonzero status."""
+        err = ctypes.c_double(0.0)
+        nit = ctypes.c_int(0)
+        _check(self._lib, self._lib.cismgpu_solver_solve(self.handle, algorithm, precond, ncheck, tol, maxiters,
+                                                          ctypes.byref(err), ctypes.byref(nit)))
+        return err.value, nit.value
+
+    def x(self):
+        xu = np.empty(self._shape)
+        xv = np.empty(self._shape)
+        _check(self._lib, self._lib.cismgpu_solver_get_x(self.handle, ctypes.c_void_p(xu.ctypes.data),
+                                                         ctypes.c_void_p(xv.ctypes.data)))
+        return xu, xv
+
+    def profile(self, enable=True):
+        _check(self._lib, self._lib.cismgpu_solver_profile(self.handle, int(enable)))
+
+    def profile_read(self):
+        ms, n, by = ctypes.c_double(), ctypes.c_int(), ctypes.c_double()
+        _check(self._lib, self._lib.cismgpu_solver_profile_read(self.handle, ctypes.byref(ms), ctypes.byref(n),
+                                                                ctypes.byref(by)))
+        return ms.value, n.value, by.value
+
+    def device_bytes(self) -> int:
+        return int(self._lib.cismgpu_solver_device_bytes(self.handle))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.cismgpu_solver_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def solve_batch(solvers, algorithm=ALG_MIXED_CHRONGEAR, precond=HO_PRECOND_DIAG, ncheck=5, tol=1e-8, maxiters=200,
+                stream=None):
+    """One persistent launch over many DeviceSolvers; returns (errs, niters, statuses) arrays."""
+    lib = load_library()
+    n = len(solvers)
+    hs = (ctypes.c_void_p * n)(*[s.handle for s in solvers])
+    errs = (ctypes.c_double * n)()
+    nits = (ctypes.c_int * n)()
+    sts = (ctypes.c_int * n)()
+    rc = lib.cismgpu_solver_solve_batch(hs, n, algorithm, precond, ncheck, tol, maxiters, errs, nits, sts,
+                                        ctypes.c_void_p(stream) if stream else None)
+    statuses = np.array(list(sts), dtype=np.int32)
+    if rc != 0 and not np.any(statuses):
+        _check(lib, rc)
+    return np.array(list(errs)), np.array(list(nits), dtype=np.int32), statuses

@@ -1,16 +1,22 @@
 // cismgpu.cu -- host driver and C ABI of the B200 structured PCG library.
 //
-// One translation unit: the FP64 reference-faithful kernels (pcg_fp64.cu) plus the
-// host code that uploads the caller's Fortran arrays, re-lays them into coefficient
-// planes, enqueues the solver's kernel sequence on one stream and polls the
-// device-side convergence flag with one check period of look-ahead.
+// One translation unit: the FP64 reference-faithful kernels (pcg_fp64.cu), the
+// mixed-precision kernels (pcg_mixed.cu) and the host code.  A Solver owns the
+// device copy of one linear system (coefficient planes, level-major vectors) and
+// one stream; it enqueues a solver's kernel sequence and polls the device-side
+// convergence flag with one check period of look-ahead, so the GPU never idles
+// waiting for the host.  The one-shot reference-signature calls reuse one cached
+// Solver (the Picard loop calls them repeatedly with the same sizes).
 #include <cstdio>
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
 
 #include "pcg_fp64.cu"
+#include "pcg_mixed.cu"
 
 namespace cismgpu {
 
@@ -29,39 +35,37 @@ static int fail(int code, const std::string &msg) {
                         std::string(#call) + ": " + cudaGetErrorString(e_));                 \
     } while (0)
 
+#define TRY(expr)                \
+    do {                         \
+        int rc_ = (expr);        \
+        if (rc_) return rc_;     \
+    } while (0)
+
 struct DevBuf {
     void *p = nullptr;
     size_t n = 0;
     cudaError_t ensure(size_t bytes) {
         if (bytes <= n) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e == cudaSuccess) n = bytes;
+        else p = nullptr;
+        return e;
+    }
+    void release() {
         if (p) cudaFree(p);
         p = nullptr;
         n = 0;
-        cudaError_t e = cudaMalloc(&p, bytes);
-        if (e == cudaSuccess) n = bytes;
-        return e;
     }
     template <class T> T *as() const { return static_cast<T *>(p); }
 };
 
 // Vectors of one solve, level-major planes of nz*NQ doubles each.
-enum VecId { VB_U, VB_V, VX_U, VX_V, VR_U, VR_V, VD_U, VD_V, VQ_U, VQ_V, VZ_U, VZ_V, VAZ_U, VAZ_V, NVEC };
-
-struct Workspace {
-    int device = -1;
-    bool ready = false;
-    cudaStream_t stream = nullptr;
-    DevBuf A, raw, vec, act, partials, state, map;
-    int *h_done = nullptr;          // pinned, 2 slots for look-ahead polling
-    SolveState *h_state = nullptr;  // pinned
-    cudaEvent_t ev[2];
+enum VecId {
+    VB_U, VB_V, VX_U, VX_V, VR_U, VR_V, VD_U, VD_V, VQ_U, VQ_V, VZ_U, VZ_V, VAZ_U, VAZ_V, VX0_U, VX0_V, NVEC
 };
 
-static std::mutex g_mu;
-static Workspace g_ws;
-
-static int init_device(Workspace &ws) {
-    if (ws.ready) return CISMGPU_OK;
+static int check_device() {
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
     if (e != cudaSuccess || n == 0) return fail(CISMGPU_ENODEV, "no CUDA device");
@@ -70,33 +74,570 @@ static int init_device(Workspace &ws) {
     cudaDeviceProp prop;
     CU(cudaGetDeviceProperties(&prop, dev));
     if (prop.major != 10) return fail(CISMGPU_ENODEV, std::string("not an sm_100 device: ") + prop.name);
-    CU(cudaStreamCreateWithFlags(&ws.stream, cudaStreamNonBlocking));
-    CU(cudaMallocHost(&ws.h_done, 2 * sizeof(int)));
-    CU(cudaMallocHost(&ws.h_state, sizeof(SolveState)));
-    CU(cudaEventCreateWithFlags(&ws.ev[0], cudaEventDisableTiming));
-    CU(cudaEventCreateWithFlags(&ws.ev[1], cudaEventDisableTiming));
-    ws.device = dev;
-    ws.ready = true;
     return CISMGPU_OK;
+}
+
+static inline unsigned nblocks(long long n, int b = kBlock) { return (unsigned)((n + b - 1) / b); }
+static inline bool is_check(int iter, int ncheck) { return (iter % ncheck == 0) || iter == 5; }
+
+struct Ptrs {
+    double *bu, *bv, *xu, *xv, *ru, *rv, *du, *dv, *qu, *qv, *zu, *zv, *Azu, *Azv, *x0u, *x0v;
+};
+
+struct Solver {
+    Geom g{};
+    bool is3d = false;
+    int NC = 27;
+    long long nvec = 0;
+    long long n_active_owned = 0;  // active owned columns
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    DevBuf A, raw, vec, act, partials, state, map;
+    MixedBufs mixed;  // FP32 copies, created on first mixed solve
+    int *h_done = nullptr;          // pinned, 2 slots for look-ahead polling
+    SolveState *h_state = nullptr;  // pinned
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    // profiling of matvec launches
+    bool prof = false;
+    std::vector<cudaEvent_t> pev;
+    int pused = 0;
+    double prof_ms = 0.0;
+    int prof_n = 0;
+    double prof_bytes = 0.0;
+
+    ~Solver() { destroy(); }
+
+    void destroy() {
+        A.release(); raw.release(); vec.release(); act.release(); partials.release(); state.release(); map.release();
+        mixed.release();
+        if (h_done) cudaFreeHost(h_done);
+        if (h_state) cudaFreeHost(h_state);
+        h_done = nullptr;
+        h_state = nullptr;
+        for (auto &e : ev) if (e) cudaEventDestroy(e), e = nullptr;
+        for (auto &e : pev) cudaEventDestroy(e);
+        pev.clear();
+        if (own_stream && stream) cudaStreamDestroy(stream);
+        stream = nullptr;
+        own_stream = false;
+    }
+
+    int init(cudaStream_t s) {
+        if (h_done) return CISMGPU_OK;
+        TRY(check_device());
+        if (s) {
+            stream = s;
+            own_stream = false;
+        } else {
+            CU(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+            own_stream = true;
+        }
+        CU(cudaMallocHost(&h_done, 2 * sizeof(int)));
+        CU(cudaMallocHost(&h_state, sizeof(SolveState)));
+        CU(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+        CU(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming));
+        return CISMGPU_OK;
+    }
+
+    Ptrs ptrs() const {
+        double *V = vec.as<double>();
+        auto P = [&](int id) { return V + (size_t)id * nvec; };
+        return Ptrs{P(VB_U), P(VB_V), P(VX_U), P(VX_V), P(VR_U), P(VR_V), P(VD_U), P(VD_V),
+                    P(VQ_U), P(VQ_V), P(VZ_U), P(VZ_V), P(VAZ_U), P(VAZ_V), P(VX0_U), P(VX0_V)};
+    }
+
+    VecArgs vargs() const {
+        const Ptrs p = ptrs();
+        VecArgs v;
+        v.bu = p.bu; v.bv = p.bv; v.xu = p.xu; v.xv = p.xv; v.ru = p.ru; v.rv = p.rv;
+        v.du = p.du; v.dv = p.dv; v.qu = p.qu; v.qv = p.qv; v.zu = p.zu; v.zv = p.zv;
+        v.Azu = p.Azu; v.Azv = p.Azv;
+        return v;
+    }
+
+    // Upload the caller's arrays: coefficient planes, level-major vectors.  x0 may be null.
+    int upload(const Geom &geom, bool three_d, const int32_t *indx, const int32_t *active,
+               const double *const blocks[4], const double *bu, const double *bv, const double *xu,
+               const double *xv) {
+        g = geom;
+        is3d = three_d;
+        NC = is3d ? 27 : 9;
+        nvec = (long long)g.nz * g.NQ;
+        mixed.valid = false;
+        n_active_owned = 0;
+        for (int j = g.jlo; j <= g.jhi; ++j)
+            for (int i = g.ilo; i <= g.ihi; ++i) n_active_owned += active[(long long)j * g.NX + i] != 0;
+        const size_t blk_bytes = (size_t)NC * nvec * sizeof(double);
+        CU(A.ensure(4 * blk_bytes));
+        CU(raw.ensure(blk_bytes));
+        CU(vec.ensure((size_t)NVEC * nvec * sizeof(double)));
+        CU(act.ensure((size_t)g.NQ * sizeof(int32_t)));
+        CU(partials.ensure((size_t)nblocks(g.NQ) * 2 * sizeof(DD)));
+        CU(state.ensure(sizeof(SolveState)));
+        CU(map.ensure(32 * sizeof(int32_t)));
+        cudaStream_t s = stream;
+        CU(cudaMemcpyAsync(map.p, indx, NC * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(act.p, active, (size_t)g.NQ * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+        for (int b = 0; b < 4; ++b) {
+            CU(cudaMemcpyAsync(raw.p, blocks[b], blk_bytes, cudaMemcpyHostToDevice, s));
+            double *dst = A.as<double>() + (size_t)b * NC * nvec;
+            if (is3d)
+                k_perm_block3<<<nblocks(nvec), kBlock, 0, s>>>(g, raw.as<double>(), dst, map.as<int32_t>());
+            else
+                k_perm_block2<<<nblocks(g.NQ), kBlock, 0, s>>>(g, raw.as<double>(), dst, map.as<int32_t>());
+            CU(cudaGetLastError());
+        }
+        double *V = vec.as<double>();
+        const double *src[4] = {bu, bv, xu, xv};
+        const int dst_id[4] = {VB_U, VB_V, VX0_U, VX0_V};
+        for (int t = 0; t < 4; ++t) {
+            double *dst = V + (size_t)dst_id[t] * nvec;
+            if (!src[t]) {
+                CU(cudaMemsetAsync(dst, 0, nvec * sizeof(double), s));
+            } else if (is3d) {
+                CU(cudaMemcpyAsync(raw.p, src[t], nvec * sizeof(double), cudaMemcpyHostToDevice, s));
+                k_vec_in<<<nblocks(nvec), kBlock, 0, s>>>(g, raw.as<double>(), dst);
+                CU(cudaGetLastError());
+            } else {
+                CU(cudaMemcpyAsync(dst, src[t], nvec * sizeof(double), cudaMemcpyHostToDevice, s));
+            }
+        }
+        return CISMGPU_OK;
+    }
+
+    int download(int id_u, int id_v, double *xu, double *xv) {
+        double *V = vec.as<double>();
+        double *out[2] = {xu, xv};
+        const int id[2] = {id_u, id_v};
+        for (int t = 0; t < 2; ++t) {
+            if (is3d) {
+                k_vec_out<<<nblocks(nvec), kBlock, 0, stream>>>(g, V + (size_t)id[t] * nvec, raw.as<double>());
+                CU(cudaGetLastError());
+                CU(cudaMemcpyAsync(out[t], raw.p, nvec * sizeof(double), cudaMemcpyDeviceToHost, stream));
+            } else {
+                CU(cudaMemcpyAsync(out[t], V + (size_t)id[t] * nvec, nvec * sizeof(double), cudaMemcpyDeviceToHost,
+                                   stream));
+            }
+        }
+        CU(cudaStreamSynchronize(stream));
+        return CISMGPU_OK;
+    }
+
+    // ---- profiling of matvec launches (CUDA events on this stream) ----
+    template <class F>
+    int timed(F launch) {
+        if (prof) {
+            if (pused + 2 > (int)pev.size() && pev.size() < 16384) {
+                for (int t = 0; t < 256; ++t) {
+                    cudaEvent_t e;
+                    CU(cudaEventCreate(&e));
+                    pev.push_back(e);
+                }
+            }
+            if (pused + 2 <= (int)pev.size()) {
+                CU(cudaEventRecord(pev[pused], stream));
+                launch();
+                CU(cudaEventRecord(pev[pused + 1], stream));
+                pused += 2;
+                return CISMGPU_OK;
+            }
+        }
+        launch();
+        return CISMGPU_OK;
+    }
+
+    int collect_profile() {
+        if (!prof) return CISMGPU_OK;
+        CU(cudaStreamSynchronize(stream));
+        for (int t = 0; t + 1 < pused; t += 2) {
+            float ms = 0.f;
+            CU(cudaEventElapsedTime(&ms, pev[t], pev[t + 1]));
+            prof_ms += ms;
+            prof_n += 1;
+        }
+        pused = 0;
+        return CISMGPU_OK;
+    }
+
+    // ---- convergence polling with one check period of look-ahead ----
+    struct Poller {
+        Solver &s;
+        int pending = -1, slot = 0;
+        explicit Poller(Solver &sv) : s(sv) {}
+        int after_check() {
+            SolveState *st = s.state.as<SolveState>();
+            if (cudaMemcpyAsync(&s.h_done[slot], &st->done, sizeof(int), cudaMemcpyDeviceToHost, s.stream) !=
+                cudaSuccess)
+                return -1;
+            if (cudaEventRecord(s.ev[slot], s.stream) != cudaSuccess) return -1;
+            int finished = 0;
+            if (pending >= 0) {
+                if (cudaEventSynchronize(s.ev[pending]) != cudaSuccess) return -1;
+                finished = s.h_done[pending];
+            }
+            pending = slot;
+            slot ^= 1;
+            return finished;
+        }
+    };
+
+    int begin_solve() {
+        const Ptrs p = ptrs();
+        CU(cudaMemcpyAsync(p.xu, p.x0u, 2 * nvec * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        return CISMGPU_OK;
+    }
+
+    int finish_solve(double *err, int *niters) {
+        CU(cudaMemcpyAsync(h_state, state.p, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        TRY(collect_profile());
+        *err = h_state->err;
+        *niters = h_state->niters;
+        if (h_state->status == CISMGPU_EBREAKDOWN_ETA1)
+            return fail(CISMGPU_EBREAKDOWN_ETA1, "PCG solver has failed, eta1 = NaN");
+        if (h_state->status == CISMGPU_EBREAKDOWN_ALPHA)
+            return fail(CISMGPU_EBREAKDOWN_ALPHA, "PCG solver has failed, alpha = NaN");
+        return CISMGPU_OK;
+    }
+
+    double mv_bytes(int extra_vec_streams) const {
+        // per active owned node: 4 blocks x NC coefficients + vector streams of 2 components
+        return (double)n_active_owned * g.nz * (4.0 * NC * 8.0 + 2.0 * 8.0 * (2 + extra_vec_streams));
+    }
+
+    template <int NCC> int run_standard(int precond, int ncheck, double tol, int maxiters);
+    template <int NCC> int run_chrongear(int precond, int ncheck, double tol, int maxiters);
+    template <int NCC> int run_mixed(int precond, int ncheck, double tol, int maxiters);
+};
+
+// pcg_solver_standard_{2d,3d} launch sequence (:1169-1524 / :392-808)
+template <int NCC>
+int Solver::run_standard(int precond, int ncheck, double tol, int maxiters) {
+    cudaStream_t s = stream;
+    SolveState *st = state.as<SolveState>();
+    DD *part = partials.as<DD>();
+    const Ptrs p = ptrs();
+    const VecArgs v = vargs();
+    const double *Ad = A.as<double>();
+    const int32_t *ac = act.as<int32_t>();
+    const unsigned nb = nblocks(g.NQ);
+    const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
+    auto rc = [&](int epi, int iter) { return RedCtx{part, st, epi, iter}; };
+    const Geom gg = g;
+    prof_bytes = mv_bytes(0);
+
+    k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
+    k_mv<NCC, MV_PLAIN><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
+                                              nullptr, rc(EPI_NONE, 0));
+    k_vec<OP_STD_INIT><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_L2RHS, 0));
+    CU(cudaGetLastError());
+    Poller poll(*this);
+    for (int iter = 1; iter <= maxiters; ++iter) {
+        k_precond<PRE_STD><<<nb, kBlock, 0, s>>>(gg, precond, Ad, NCC, ac, p.ru, p.rv, p.zu, p.zv, nullptr, nullptr,
+                                                 rc(EPI_STD_ETA1, iter));
+        k_vec<OP_STD_D><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, iter));
+        k_halo<<<hb, kBlock, 0, s>>>(gg, p.du, p.dv, st);
+        TRY(timed([&] {
+            k_mv<NCC, MV_DQ><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr,
+                                                   nullptr, rc(EPI_STD_ETA2, iter));
+        }));
+        k_vec<OP_XR><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, iter));
+        if (is_check(iter, ncheck)) {
+            k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
+            k_mv<NCC, MV_RESID><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
+                                                      rc(EPI_CHECK, iter));
+            CU(cudaGetLastError());
+            int f = poll.after_check();
+            if (f < 0) return fail(CISMGPU_ECUDA, "polling the convergence flag failed");
+            if (f) break;
+        }
+    }
+    CU(cudaGetLastError());
+    return CISMGPU_OK;
+}
+
+// pcg_solver_chrongear_{2d,3d} launch sequence (:3066-3581 / :1913-2613)
+template <int NCC>
+int Solver::run_chrongear(int precond, int ncheck, double tol, int maxiters) {
+    cudaStream_t s = stream;
+    SolveState *st = state.as<SolveState>();
+    DD *part = partials.as<DD>();
+    const Ptrs p = ptrs();
+    const VecArgs v = vargs();
+    const double *Ad = A.as<double>();
+    const int32_t *ac = act.as<int32_t>();
+    const unsigned nb = nblocks(g.NQ);
+    const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
+    auto rc = [&](int epi, int iter) { return RedCtx{part, st, epi, iter}; };
+    const Geom gg = g;
+    prof_bytes = mv_bytes(1);  // the fused (r,z) dot also reads r
+
+    k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
+    // r = d = z = q = Az = 0 (:3048-3061)
+    CU(cudaMemsetAsync(p.ru, 0, (size_t)(VAZ_V - VR_U + 1) * nvec * sizeof(double), s));
+    k_vec<OP_DOT_BB><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_L2RHS, 0));
+    // first pass (:3085-3290)
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
+    k_mv<NCC, MV_PLAIN><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
+                                              nullptr, rc(EPI_NONE, 1));
+    k_vec<OP_CG_INIT><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, 1));
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
+    k_precond<PRE_CG_FIRST><<<nb, kBlock, 0, s>>>(gg, precond, Ad, NCC, ac, p.ru, p.rv, p.zu, p.zv, p.du, p.dv,
+                                                  rc(EPI_CG_RHO0, 1));
+    k_mv<NCC, MV_DQ><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr,
+                                           rc(EPI_CG_FIRST, 1));
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.qu, p.qv, st);
+    k_vec<OP_XR><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, 1));
+    CU(cudaGetLastError());
+    Poller poll(*this);
+    for (int iter = 2; iter <= maxiters; ++iter) {
+        k_precond<PRE_ONLY><<<nb, kBlock, 0, s>>>(gg, precond, Ad, NCC, ac, p.ru, p.rv, p.zu, p.zv, nullptr, nullptr,
+                                                  rc(EPI_NONE, iter));
+        TRY(timed([&] {
+            k_mv<NCC, MV_CG_AZ><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.zu, p.zv, p.Azu, p.Azv, nullptr, nullptr, p.ru,
+                                                      p.rv, rc(EPI_CG_ITER, iter));
+        }));
+        k_halo<<<hb, kBlock, 0, s>>>(gg, p.Azu, p.Azv, st);
+        k_vec<OP_CG_UPD><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, iter));
+        if (is_check(iter, ncheck)) {
+            k_mv<NCC, MV_RESID><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
+                                                      rc(EPI_CHECK, iter));
+            k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
+            CU(cudaGetLastError());
+            int f = poll.after_check();
+            if (f < 0) return fail(CISMGPU_ECUDA, "polling the convergence flag failed");
+            if (f) break;
+        }
+    }
+    CU(cudaGetLastError());
+    return CISMGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// mixed-precision persistent solver (pcg_mixed.cu): host side
+// ---------------------------------------------------------------------------
+__global__ void k_mstate_to_solve(const MState *ms, SolveState *st, const GridBar *bar) {
+    st->err = ms->err;
+    st->niters = ms->niters;
+    st->status = (bar->abort && !ms->done) ? CISMGPU_ETIMEOUT : ms->status;
+    st->checks = ms->checks;
+    st->done = 1;
+}
+
+static int mixed_nzm(const Geom &g, bool is3d) { return !is3d ? 1 : (g.nz <= 16 ? 16 : 32); }
+
+// Allocate and fill the FP32 copy of the matrix and the preconditioner factors.
+static int mixed_prepare(Solver &sv, int precond) {
+    if (sv.g.nz > kMixedMaxNz) return fail(CISMGPU_EUNSUPPORTED, "mixed solver supports nz <= 32");
+    if (!(precond == 0 || precond == 1 || (precond == 2 && sv.is3d)))
+        return fail(CISMGPU_EUNSUPPORTED, "mixed solver preconditioners: 0, 1, or 2 (3D only)");
+    MixedBufs &m = sv.mixed;
+    const long long nvec = sv.nvec;
+    const int NC = sv.NC;
+    const Geom &g = sv.g;
+    const int tiles_x = (g.ihi - g.ilo + kTX) / kTX, tiles_y = (g.jhi - g.jlo + kTY) / kTY;
+    const int ntiles = tiles_x * tiles_y;
+    if (!m.valid) {
+        m.release();
+        size_t bytes = 0;
+        auto alloc = [&](void **p, size_t n) -> cudaError_t {
+            bytes += n;
+            return cudaMalloc(p, n);
+        };
+        CU(alloc((void **)&m.A32, (size_t)4 * NC * nvec * sizeof(float)));
+        CU(alloc((void **)&m.pre, (size_t)6 * nvec * sizeof(float)));
+        CU(alloc((void **)&m.vec, (size_t)16 * nvec * sizeof(float)));
+        CU(alloc((void **)&m.partials, (size_t)ntiles * 3 * sizeof(DD)));
+        CU(alloc((void **)&m.state, sizeof(MState)));
+        CU(alloc((void **)&m.desc, sizeof(MDesc)));
+        CU(alloc((void **)&m.tiles, (size_t)ntiles * sizeof(MTile)));
+        CU(alloc((void **)&m.bar, sizeof(GridBar)));
+        m.nbytes = bytes;
+        m.ntiles = ntiles;
+        const long long n = 4LL * NC * nvec;
+        k_to_f32<<<1184, kBlock, 0, sv.stream>>>(sv.A.as<double>(), m.A32, n);
+        CU(cudaGetLastError());
+        std::vector<MTile> tl(ntiles);
+        for (int t = 0; t < ntiles; ++t) tl[t] = MTile{0, t};
+        CU(cudaMemcpyAsync(m.tiles, tl.data(), ntiles * sizeof(MTile), cudaMemcpyHostToDevice, sv.stream));
+        CU(cudaStreamSynchronize(sv.stream));  // tl goes out of scope
+        m.valid = true;
+        m.precond = -1;
+    }
+    if (m.precond != precond) {
+        if (NC == 27)
+            k_mixed_precond_setup<27><<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, precond, sv.A.as<double>(), m.pre);
+        else
+            k_mixed_precond_setup<9><<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, precond, sv.A.as<double>(), m.pre);
+        CU(cudaGetLastError());
+        m.precond = precond;
+    }
+    return CISMGPU_OK;
+}
+
+static MDesc mixed_desc(const Solver &sv, int precond) {
+    const MixedBufs &m = sv.mixed;
+    const long long nvec = sv.nvec;
+    const Ptrs p = sv.ptrs();
+    MDesc D;
+    D.g = sv.g;
+    D.NC = sv.NC;
+    D.precond = precond;
+    D.tiles_x = (sv.g.ihi - sv.g.ilo + kTX) / kTX;
+    D.tiles_y = (sv.g.jhi - sv.g.jlo + kTY) / kTY;
+    D.ntiles = D.tiles_x * D.tiles_y;
+    D.A32 = m.A32;
+    D.A64 = sv.A.as<double>();
+    D.pre = m.pre;
+    D.act = sv.act.as<int32_t>();
+    D.b = p.bu;
+    D.x = p.xu;
+    float *V = m.vec;
+    const size_t vs = (size_t)2 * nvec;  // one vector = u and v planes
+    D.r[0] = V + 0 * vs; D.r[1] = V + 1 * vs;
+    D.q[0] = V + 2 * vs; D.q[1] = V + 3 * vs;
+    D.Az[0] = V + 4 * vs; D.Az[1] = V + 5 * vs;
+    D.z = V + 6 * vs;
+    D.d = V + 7 * vs;
+    D.partials = m.partials;
+    return D;
+}
+
+static MState mixed_init_state(double tol, int maxiters, int ncheck) {
+    MState S;
+    std::memset(&S, 0, sizeof(S));
+    S.tol = tol;
+    S.maxiters = maxiters;
+    S.ncheck = ncheck;
+    S.niters = maxiters;
+    S.step = MS_INIT;
+    S.err = std::nan("");
+    return S;
+}
+
+// x = x0 and all FP32 recurrence vectors = 0 (the reference zeroes its work vectors, :3048-3061)
+static int mixed_reset(Solver &sv, cudaStream_t s) {
+    const Ptrs p = sv.ptrs();
+    CU(cudaMemcpyAsync(p.xu, p.x0u, 2 * sv.nvec * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CU(cudaMemsetAsync(sv.mixed.vec, 0, (size_t)16 * sv.nvec * sizeof(float), s));
+    return CISMGPU_OK;
+}
+
+template <int NC, int NZM>
+static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_tiles, int ntiles, GridBar *d_bar,
+                        int max_steps, cudaStream_t s) {
+    const size_t smem = sizeof(MShared<NZM>);
+    static bool attr_set = false;
+    if (!attr_set) {
+        CU(cudaFuncSetAttribute(k_mixed<NC, NZM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        attr_set = true;
+    }
+    int dev = 0, nsm = 0, occ = 0;
+    CU(cudaGetDevice(&dev));
+    CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mixed<NC, NZM>, kBlock, smem));
+    if (occ < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM");
+    int grid = nsm * occ;
+    if (grid > ntiles) grid = ntiles;
+    void *args[] = {(void *)&d_descs, (void *)&d_states, (void *)&d_tiles, (void *)&ntiles, (void *)&d_bar,
+                    (void *)&max_steps};
+    CU(cudaLaunchCooperativeKernel((const void *)k_mixed<NC, NZM>, dim3(grid), dim3(kBlock), args, smem, s));
+    return CISMGPU_OK;
+}
+
+static int mixed_dispatch(bool is3d, int nzm, const MDesc *d, MState *st, const MTile *t, int nt, GridBar *bar,
+                          int max_steps, cudaStream_t s) {
+    if (!is3d) return mixed_launch<9, 1>(d, st, t, nt, bar, max_steps, s);
+    if (nzm == 16) return mixed_launch<27, 16>(d, st, t, nt, bar, max_steps, s);
+    return mixed_launch<27, 32>(d, st, t, nt, bar, max_steps, s);
+}
+
+static double mixed_iter_bytes(const Solver &sv, int precond) {
+    const double pre = precond == 2 ? 24.0 : (precond == 1 ? 8.0 : 0.0);
+    return (double)sv.n_active_owned * sv.g.nz * (4.0 * sv.NC * 4.0 + 40.0 + 32.0 + 40.0 + pre);
+}
+
+static double mixed_check_bytes(const Solver &sv) {
+    return (double)sv.n_active_owned * sv.g.nz * (4.0 * sv.NC * 8.0 + 16.0 + 16.0 + 8.0);
+}
+
+template <int NCC>
+int Solver::run_mixed(int precond, int ncheck, double tol, int maxiters) {
+    TRY(mixed_prepare(*this, precond));
+    TRY(mixed_reset(*this, stream));
+    MixedBufs &m = mixed;
+    const MDesc D = mixed_desc(*this, precond);
+    const MState S0 = mixed_init_state(tol, maxiters, ncheck);
+    GridBar B{0u, 0u, 0, 1};
+    CU(cudaMemcpyAsync(m.desc, &D, sizeof(MDesc), cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(m.state, &S0, sizeof(MState), cudaMemcpyHostToDevice, stream));
+    CU(cudaMemcpyAsync(m.bar, &B, sizeof(GridBar), cudaMemcpyHostToDevice, stream));
+    const int max_steps = 4 * maxiters + 16;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (prof) {
+        CU(cudaEventCreate(&e0));
+        CU(cudaEventCreate(&e1));
+        CU(cudaEventRecord(e0, stream));
+    }
+    TRY(mixed_dispatch(is3d, mixed_nzm(g, is3d), m.desc, m.state, m.tiles, m.ntiles, m.bar, max_steps, stream));
+    if (prof) CU(cudaEventRecord(e1, stream));
+    const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
+    const Ptrs p = ptrs();
+    k_mstate_to_solve<<<1, 1, 0, stream>>>(m.state, state.as<SolveState>(), m.bar);
+    k_halo<<<hb, kBlock, 0, stream>>>(g, p.xu, p.xv, nullptr);  // the caller's x carries halo values
+    CU(cudaGetLastError());
+    if (prof) {
+        MState hs;
+        CU(cudaMemcpyAsync(&hs, m.state, sizeof(MState), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        float ms = 0.f;
+        CU(cudaEventElapsedTime(&ms, e0, e1));
+        prof_ms += ms;
+        prof_n += 1;
+        prof_bytes = hs.fp32_matvecs * mixed_iter_bytes(*this, precond) + hs.fp64_matvecs * mixed_check_bytes(*this);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    return CISMGPU_OK;
+}
+
+enum Algo { ALG_STANDARD = CISMGPU_ALG_STANDARD, ALG_CHRONGEAR = CISMGPU_ALG_CHRONGEAR,
+            ALG_MIXED = CISMGPU_ALG_MIXED_CHRONGEAR };
+
+static int run_algorithm(Solver &sv, int alg, int precond, int ncheck, double tol, int maxiters) {
+    if (alg == ALG_STANDARD)
+        return sv.is3d ? sv.run_standard<27>(precond, ncheck, tol, maxiters)
+                       : sv.run_standard<9>(precond, ncheck, tol, maxiters);
+    if (alg == ALG_CHRONGEAR)
+        return sv.is3d ? sv.run_chrongear<27>(precond, ncheck, tol, maxiters)
+                       : sv.run_chrongear<9>(precond, ncheck, tol, maxiters);
+    if (alg == ALG_MIXED)
+        return sv.is3d ? sv.run_mixed<27>(precond, ncheck, tol, maxiters)
+                       : sv.run_mixed<9>(precond, ncheck, tol, maxiters);
+    return fail(CISMGPU_EINVAL, "unknown algorithm");
 }
 
 static int validate(int nx, int ny, int nz, const cismgpu_par_t *par, const void *indx, const void *act,
                     const void *A0, const void *A1, const void *A2, const void *A3, const void *bu,
-                    const void *bv, const void *xu, const void *xv, int precond, int ncheck, int maxiters,
-                    const void *err, const void *niters) {
-    if (!par || !indx || !act || !A0 || !A1 || !A2 || !A3 || !bu || !bv || !xu || !xv || !err || !niters)
+                    const void *bv) {
+    if (!par || !indx || !act || !A0 || !A1 || !A2 || !A3 || !bu || !bv)
         return fail(CISMGPU_EINVAL, "null pointer argument");
     if (nx < 6 || ny < 6 || nz < 1 || nz > kMaxNz)
         return fail(CISMGPU_EINVAL, "grid too small or nz outside 1..64");
-    if (ncheck < 1) return fail(CISMGPU_EINVAL, "linear_solve_ncheck must be >= 1");
-    if (maxiters < 0) return fail(CISMGPU_EINVAL, "maxiters must be >= 0");
     if (par->tasks_row * par->tasks_col != 1)
         return fail(CISMGPU_EUNSUPPORTED, "the whole domain must be on one GPU (tasks_row*tasks_col == 1)");
-    if (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL)
-        return fail(CISMGPU_EUNSUPPORTED, "tridiagonal preconditioners (3, 4) are not implemented");
     if (par->staggered_ilo < 1 || par->staggered_ihi > nx - 1 || par->staggered_ilo > par->staggered_ihi ||
         par->staggered_jlo < 1 || par->staggered_jhi > ny - 1 || par->staggered_jlo > par->staggered_jhi)
         return fail(CISMGPU_EINVAL, "owned vertex bounds outside the array");
+    return CISMGPU_OK;
+}
+
+static int validate_solve_args(int precond, int ncheck, int maxiters) {
+    if (ncheck < 1) return fail(CISMGPU_EINVAL, "linear_solve_ncheck must be >= 1");
+    if (maxiters < 0) return fail(CISMGPU_EINVAL, "maxiters must be >= 0");
+    if (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL)
+        return fail(CISMGPU_EUNSUPPORTED, "tridiagonal preconditioners (3, 4) are not implemented");
     return CISMGPU_OK;
 }
 
@@ -123,281 +664,60 @@ static Geom make_geom(int nx, int ny, int nz, const cismgpu_par_t *par) {
     return g;
 }
 
-static inline unsigned nblocks(long long n, int b = kBlock) { return (unsigned)((n + b - 1) / b); }
+static std::mutex g_mu;
+static Solver *g_oneshot = nullptr;  // cached Solver of the one-shot calls
+static int g_oneshot_alg = -1;       // -1: the reference algorithm each call names
 
-// Upload the caller's arrays into the workspace (coefficient planes, level-major vectors).
-static int upload(Workspace &ws, const Geom &g, bool is3d, const int32_t *indx, const int32_t *act,
-                  const double *const blocks[4], const double *bu, const double *bv, const double *xu,
-                  const double *xv) {
-    const int NC = is3d ? 27 : 9;
-    const long long nvec = (long long)g.nz * g.NQ;
-    const size_t blk_bytes = (size_t)NC * nvec * sizeof(double);
-    CU(ws.A.ensure(4 * blk_bytes));
-    CU(ws.raw.ensure(blk_bytes));
-    CU(ws.vec.ensure((size_t)NVEC * nvec * sizeof(double)));
-    CU(ws.act.ensure((size_t)g.NQ * sizeof(int32_t)));
-    CU(ws.partials.ensure((size_t)nblocks(g.NQ) * 2 * sizeof(DD)));
-    CU(ws.state.ensure(sizeof(SolveState)));
-    CU(ws.map.ensure(32 * sizeof(int32_t)));
-    cudaStream_t s = ws.stream;
-    CU(cudaMemcpyAsync(ws.map.p, indx, NC * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(ws.act.p, act, (size_t)g.NQ * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    for (int b = 0; b < 4; ++b) {
-        CU(cudaMemcpyAsync(ws.raw.p, blocks[b], blk_bytes, cudaMemcpyHostToDevice, s));
-        double *dst = ws.A.as<double>() + (size_t)b * NC * nvec;
-        if (is3d)
-            k_perm_block3<<<nblocks(nvec), kBlock, 0, s>>>(g, ws.raw.as<double>(), dst, ws.map.as<int32_t>());
-        else
-            k_perm_block2<<<nblocks(g.NQ), kBlock, 0, s>>>(g, ws.raw.as<double>(), dst, ws.map.as<int32_t>());
-        CU(cudaGetLastError());
-    }
-    double *V = ws.vec.as<double>();
-    const double *src[4] = {bu, bv, xu, xv};
-    const int dst_id[4] = {VB_U, VB_V, VX_U, VX_V};
-    for (int t = 0; t < 4; ++t) {
-        double *dst = V + (size_t)dst_id[t] * nvec;
-        if (is3d) {
-            CU(cudaMemcpyAsync(ws.raw.p, src[t], nvec * sizeof(double), cudaMemcpyHostToDevice, s));
-            k_vec_in<<<nblocks(nvec), kBlock, 0, s>>>(g, ws.raw.as<double>(), dst);
-            CU(cudaGetLastError());
-        } else {
-            CU(cudaMemcpyAsync(dst, src[t], nvec * sizeof(double), cudaMemcpyHostToDevice, s));
-        }
-    }
-    return CISMGPU_OK;
-}
-
-static int download_x(Workspace &ws, const Geom &g, bool is3d, double *xu, double *xv) {
-    const long long nvec = (long long)g.nz * g.NQ;
-    double *V = ws.vec.as<double>();
-    cudaStream_t s = ws.stream;
-    double *out[2] = {xu, xv};
-    const int id[2] = {VX_U, VX_V};
-    for (int t = 0; t < 2; ++t) {
-        if (is3d) {
-            k_vec_out<<<nblocks(nvec), kBlock, 0, s>>>(g, V + (size_t)id[t] * nvec, ws.raw.as<double>());
-            CU(cudaGetLastError());
-            CU(cudaMemcpyAsync(out[t], ws.raw.p, nvec * sizeof(double), cudaMemcpyDeviceToHost, s));
-        } else {
-            CU(cudaMemcpyAsync(out[t], V + (size_t)id[t] * nvec, nvec * sizeof(double), cudaMemcpyDeviceToHost, s));
-        }
-    }
-    CU(cudaMemcpyAsync(ws.h_state, ws.state.p, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
-    CU(cudaStreamSynchronize(s));
-    return CISMGPU_OK;
-}
-
-// Enqueue-and-poll helper: after the kernels of a check iteration are enqueued,
-// copy 'done' to pinned memory; wait for the *previous* check's copy so the GPU
-// always has one check period of work queued.
-struct Poller {
-    Workspace &ws;
-    SolveState *st;
-    int pending = -1;  // slot index of the outstanding copy, -1 if none
-    int slot = 0;
-    explicit Poller(Workspace &w, SolveState *s) : ws(w), st(s) {}
-    // returns 1 when the solve is finished, 0 to continue, <0 on CUDA error
-    int after_check() {
-        cudaStream_t s = ws.stream;
-        if (cudaMemcpyAsync(&ws.h_done[slot], &st->done, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess)
-            return -1;
-        if (cudaEventRecord(ws.ev[slot], s) != cudaSuccess) return -1;
-        int finished = 0;
-        if (pending >= 0) {
-            if (cudaEventSynchronize(ws.ev[pending]) != cudaSuccess) return -1;
-            finished = ws.h_done[pending];
-        }
-        pending = slot;
-        slot ^= 1;
-        return finished;
-    }
-};
-
-static inline bool is_check(int iter, int ncheck) { return (iter % ncheck == 0) || iter == 5; }
-
-struct Ptrs {
-    double *bu, *bv, *xu, *xv, *ru, *rv, *du, *dv, *qu, *qv, *zu, *zv, *Azu, *Azv;
-};
-
-static Ptrs ptrs(Workspace &ws, const Geom &g) {
-    const long long nvec = (long long)g.nz * g.NQ;
-    double *V = ws.vec.as<double>();
-    auto P = [&](int id) { return V + (size_t)id * nvec; };
-    return Ptrs{P(VB_U), P(VB_V), P(VX_U), P(VX_V), P(VR_U), P(VR_V), P(VD_U), P(VD_V),
-                P(VQ_U), P(VQ_V), P(VZ_U), P(VZ_V), P(VAZ_U), P(VAZ_V)};
-}
-
-static VecArgs vargs(const Ptrs &p) {
-    VecArgs v;
-    v.bu = p.bu; v.bv = p.bv; v.xu = p.xu; v.xv = p.xv; v.ru = p.ru; v.rv = p.rv;
-    v.du = p.du; v.dv = p.dv; v.qu = p.qu; v.qv = p.qv; v.zu = p.zu; v.zv = p.zv;
-    v.Azu = p.Azu; v.Azv = p.Azv;
-    return v;
-}
-
-// pcg_solver_standard_{2d,3d} launch sequence (:1169-1524 / :392-808)
-template <int NC>
-static int run_standard(Workspace &ws, const Geom &g, int precond, int ncheck, double tol, int maxiters) {
-    cudaStream_t s = ws.stream;
-    SolveState *st = ws.state.as<SolveState>();
-    DD *part = ws.partials.as<DD>();
-    const Ptrs p = ptrs(ws, g);
-    const VecArgs v = vargs(p);
-    const double *A = ws.A.as<double>();
-    const int32_t *act = ws.act.as<int32_t>();
-    const unsigned nb = nblocks(g.NQ);
-    const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
-    auto rc = [&](int epi, int iter) { return RedCtx{part, st, epi, iter}; };
-
-    k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
-    k_halo<<<hb, kBlock, 0, s>>>(g, p.xu, p.xv, st);
-    k_mv<NC, MV_PLAIN><<<nb, kBlock, 0, s>>>(g, A, act, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
-                                             nullptr, rc(EPI_NONE, 0));
-    k_vec<OP_STD_INIT><<<nb, kBlock, 0, s>>>(g, v, rc(EPI_L2RHS, 0));
-    CU(cudaGetLastError());
-    Poller poll(ws, st);
-    for (int iter = 1; iter <= maxiters; ++iter) {
-        k_precond<PRE_STD><<<nb, kBlock, 0, s>>>(g, precond, A, NC, act, p.ru, p.rv, p.zu, p.zv, nullptr, nullptr,
-                                                 rc(EPI_STD_ETA1, iter));
-        k_vec<OP_STD_D><<<nb, kBlock, 0, s>>>(g, v, rc(EPI_NONE, iter));
-        k_halo<<<hb, kBlock, 0, s>>>(g, p.du, p.dv, st);
-        k_mv<NC, MV_DQ><<<nb, kBlock, 0, s>>>(g, A, act, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr,
-                                              nullptr, rc(EPI_STD_ETA2, iter));
-        k_vec<OP_XR><<<nb, kBlock, 0, s>>>(g, v, rc(EPI_NONE, iter));
-        if (is_check(iter, ncheck)) {
-            k_halo<<<hb, kBlock, 0, s>>>(g, p.xu, p.xv, st);
-            k_mv<NC, MV_RESID><<<nb, kBlock, 0, s>>>(g, A, act, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
-                                                     rc(EPI_CHECK, iter));
-            CU(cudaGetLastError());
-            int f = poll.after_check();
-            if (f < 0) return fail(CISMGPU_ECUDA, "polling the convergence flag failed");
-            if (f) break;
-        }
-    }
-    CU(cudaGetLastError());
-    return CISMGPU_OK;
-}
-
-// pcg_solver_chrongear_{2d,3d} launch sequence (:3066-3581 / :1913-2613)
-template <int NC>
-static int run_chrongear(Workspace &ws, const Geom &g, int precond, int ncheck, double tol, int maxiters) {
-    cudaStream_t s = ws.stream;
-    SolveState *st = ws.state.as<SolveState>();
-    DD *part = ws.partials.as<DD>();
-    const Ptrs p = ptrs(ws, g);
-    const VecArgs v = vargs(p);
-    const double *A = ws.A.as<double>();
-    const int32_t *act = ws.act.as<int32_t>();
-    const unsigned nb = nblocks(g.NQ);
-    const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
-    auto rc = [&](int epi, int iter) { return RedCtx{part, st, epi, iter}; };
-    const long long nvec = (long long)g.nz * g.NQ;
-
-    k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
-    // r = d = z = q = Az = 0 (:3048-3061)
-    CU(cudaMemsetAsync(p.ru, 0, (size_t)(NVEC - VR_U) * nvec * sizeof(double), s));
-    k_vec<OP_DOT_BB><<<nb, kBlock, 0, s>>>(g, v, rc(EPI_L2RHS, 0));
-    // first pass (:3085-3290)
-    k_halo<<<hb, kBlock, 0, s>>>(g, p.xu, p.xv, st);
-    k_mv<NC, MV_PLAIN><<<nb, kBlock, 0, s>>>(g, A, act, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
-                                             nullptr, rc(EPI_NONE, 1));
-    k_vec<OP_CG_INIT><<<nb, kBlock, 0, s>>>(g, v, rc(EPI_NONE, 1));
-    k_halo<<<hb, kBlock, 0, s>>>(g, p.ru, p.rv, st);
-    k_precond<PRE_CG_FIRST><<<nb, kBlock, 0, s>>>(g, precond, A, NC, act, p.ru, p.rv, p.zu, p.zv, p.du, p.dv,
-                                                  rc(EPI_CG_RHO0, 1));
-    k_mv<NC, MV_DQ><<<nb, kBlock, 0, s>>>(g, A, act, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr,
-                                          rc(EPI_CG_FIRST, 1));
-    k_halo<<<hb, kBlock, 0, s>>>(g, p.qu, p.qv, st);
-    k_vec<OP_XR><<<nb, kBlock, 0, s>>>(g, v, rc(EPI_NONE, 1));
-    CU(cudaGetLastError());
-    Poller poll(ws, st);
-    for (int iter = 2; iter <= maxiters; ++iter) {
-        k_precond<PRE_ONLY><<<nb, kBlock, 0, s>>>(g, precond, A, NC, act, p.ru, p.rv, p.zu, p.zv, nullptr, nullptr,
-                                                  rc(EPI_NONE, iter));
-        k_mv<NC, MV_CG_AZ><<<nb, kBlock, 0, s>>>(g, A, act, p.zu, p.zv, p.Azu, p.Azv, nullptr, nullptr, p.ru,
-                                                 p.rv, rc(EPI_CG_ITER, iter));
-        k_halo<<<hb, kBlock, 0, s>>>(g, p.Azu, p.Azv, st);
-        k_vec<OP_CG_UPD><<<nb, kBlock, 0, s>>>(g, v, rc(EPI_NONE, iter));
-        if (is_check(iter, ncheck)) {
-            k_mv<NC, MV_RESID><<<nb, kBlock, 0, s>>>(g, A, act, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
-                                                     rc(EPI_CHECK, iter));
-            k_halo<<<hb, kBlock, 0, s>>>(g, p.ru, p.rv, st);
-            CU(cudaGetLastError());
-            int f = poll.after_check();
-            if (f < 0) return fail(CISMGPU_ECUDA, "polling the convergence flag failed");
-            if (f) break;
-        }
-    }
-    CU(cudaGetLastError());
-    return CISMGPU_OK;
-}
-
-enum Algo { ALG_STANDARD, ALG_CHRONGEAR };
-
-static int solve(Algo alg, bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indx2,
-                 const int32_t *indx3, const int32_t *act, const double *Auu, const double *Auv, const double *Avu,
-                 const double *Avv, const double *bu, const double *bv, double *xu, double *xv, int precond,
-                 int ncheck, double tol, int maxiters, double *err, int *niters) {
+static int oneshot_solve(int alg, bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indx2,
+                         const int32_t *indx3, const int32_t *act, const double *Auu, const double *Auv,
+                         const double *Avu, const double *Avv, const double *bu, const double *bv, double *xu,
+                         double *xv, int precond, int ncheck, double tol, int maxiters, double *err, int *niters) {
     std::lock_guard<std::mutex> lk(g_mu);
     g_last_error.clear();
     const int32_t *indx = is3d ? indx3 : indx2;
-    int rc = validate(nx, ny, is3d ? nz : 1, par, indx, act, Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond, ncheck,
-                      maxiters, err, niters);
-    if (rc) return rc;
-    if ((rc = validate_indx(indx, is3d ? 27 : 9))) return rc;
-    Workspace &ws = g_ws;
-    if ((rc = init_device(ws))) return rc;
-    const Geom g = make_geom(nx, ny, is3d ? nz : 1, par);
+    if (!xu || !xv || !err || !niters) return fail(CISMGPU_EINVAL, "null pointer argument");
+    TRY(validate(nx, ny, is3d ? nz : 1, par, indx, act, Auu, Auv, Avu, Avv, bu, bv));
+    TRY(validate_solve_args(precond, ncheck, maxiters));
+    TRY(validate_indx(indx, is3d ? 27 : 9));
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
     const double *blocks[4] = {Auu, Auv, Avu, Avv};
-    if ((rc = upload(ws, g, is3d, indx, act, blocks, bu, bv, xu, xv))) return rc;
-    if (alg == ALG_STANDARD)
-        rc = is3d ? run_standard<27>(ws, g, precond, ncheck, tol, maxiters)
-                  : run_standard<9>(ws, g, precond, ncheck, tol, maxiters);
-    else
-        rc = is3d ? run_chrongear<27>(ws, g, precond, ncheck, tol, maxiters)
-                  : run_chrongear<9>(ws, g, precond, ncheck, tol, maxiters);
-    if (rc) return rc;
-    if ((rc = download_x(ws, g, is3d, xu, xv))) return rc;
-    *err = ws.h_state->err;
-    *niters = ws.h_state->niters;
-    if (ws.h_state->status == CISMGPU_EBREAKDOWN_ETA1)
-        return fail(CISMGPU_EBREAKDOWN_ETA1, "PCG solver has failed, eta1 = NaN");
-    if (ws.h_state->status == CISMGPU_EBREAKDOWN_ALPHA)
-        return fail(CISMGPU_EBREAKDOWN_ALPHA, "PCG solver has failed, alpha = NaN");
-    return CISMGPU_OK;
+    TRY(sv.upload(make_geom(nx, ny, is3d ? nz : 1, par), is3d, indx, act, blocks, bu, bv, xu, xv));
+    TRY(sv.begin_solve());
+    TRY(run_algorithm(sv, g_oneshot_alg >= 0 ? g_oneshot_alg : alg, precond, ncheck, tol, maxiters));
+    int rc = sv.finish_solve(err, niters);
+    TRY(sv.download(VX_U, VX_V, xu, xv));
+    return rc;
 }
 
-static int matvec(bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indx,
-                  const int32_t *act, const double *Auu, const double *Auv, const double *Avu, const double *Avv,
-                  const double *xu, const double *xv, double *yu, double *yv) {
+static int oneshot_matvec(bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indx,
+                          const int32_t *act, const double *Auu, const double *Auv, const double *Avu,
+                          const double *Avv, const double *xu, const double *xv, double *yu, double *yv) {
     std::lock_guard<std::mutex> lk(g_mu);
     g_last_error.clear();
-    int dummy_i = 0;
-    double dummy_d = 0.0;
-    int rc = validate(nx, ny, is3d ? nz : 1, par, indx, act, Auu, Auv, Avu, Avv, xu, xv, xu, xv, 0, 1, 0,
-                      &dummy_d, &dummy_i);
-    if (rc) return rc;
-    if ((rc = validate_indx(indx, is3d ? 27 : 9))) return rc;
+    TRY(validate(nx, ny, is3d ? nz : 1, par, indx, act, Auu, Auv, Avu, Avv, xu, xv));
+    TRY(validate_indx(indx, is3d ? 27 : 9));
     if (!yu || !yv) return fail(CISMGPU_EINVAL, "null output pointer");
-    Workspace &ws = g_ws;
-    if ((rc = init_device(ws))) return rc;
-    const Geom g = make_geom(nx, ny, is3d ? nz : 1, par);
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
     const double *blocks[4] = {Auu, Auv, Avu, Avv};
-    // x is uploaded into the b slots and the product lands in the x slots
-    if ((rc = upload(ws, g, is3d, indx, act, blocks, xu, xv, xu, xv))) return rc;
-    const Ptrs p = ptrs(ws, g);
-    SolveState *st = ws.state.as<SolveState>();
-    cudaStream_t s = ws.stream;
-    k_init_state<<<1, 1, 0, s>>>(st, 0.0, 0);
-    RedCtx rc0{ws.partials.as<DD>(), st, EPI_NONE, 0};
+    TRY(sv.upload(make_geom(nx, ny, is3d ? nz : 1, par), is3d, indx, act, blocks, xu, xv, nullptr, nullptr));
+    const Ptrs p = sv.ptrs();
+    SolveState *st = sv.state.as<SolveState>();
+    k_init_state<<<1, 1, 0, sv.stream>>>(st, 0.0, 0);
+    RedCtx rc0{sv.partials.as<DD>(), st, EPI_NONE, 0};
     if (is3d)
-        k_mv<27, MV_PLAIN><<<nblocks(g.NQ), kBlock, 0, s>>>(g, ws.A.as<double>(), ws.act.as<int32_t>(), p.bu, p.bv,
-                                                           p.xu, p.xv, nullptr, nullptr, nullptr, nullptr, rc0);
+        k_mv<27, MV_PLAIN><<<nblocks(sv.g.NQ), kBlock, 0, sv.stream>>>(sv.g, sv.A.as<double>(), sv.act.as<int32_t>(),
+                                                                      p.bu, p.bv, p.xu, p.xv, nullptr, nullptr,
+                                                                      nullptr, nullptr, rc0);
     else
-        k_mv<9, MV_PLAIN><<<nblocks(g.NQ), kBlock, 0, s>>>(g, ws.A.as<double>(), ws.act.as<int32_t>(), p.bu, p.bv,
-                                                          p.xu, p.xv, nullptr, nullptr, nullptr, nullptr, rc0);
+        k_mv<9, MV_PLAIN><<<nblocks(sv.g.NQ), kBlock, 0, sv.stream>>>(sv.g, sv.A.as<double>(), sv.act.as<int32_t>(),
+                                                                     p.bu, p.bv, p.xu, p.xv, nullptr, nullptr,
+                                                                     nullptr, nullptr, rc0);
     CU(cudaGetLastError());
-    return download_x(ws, g, is3d, yu, yv);
+    return sv.download(VX_U, VX_V, yu, yv);
 }
 
 }  // namespace cismgpu
@@ -406,6 +726,11 @@ static int matvec(bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, c
 // C ABI (include/cismgpu.h)
 // ---------------------------------------------------------------------------
 using namespace cismgpu;
+
+struct cismgpu_solver {
+    Solver sv;
+    std::mutex mu;
+};
 
 extern "C" {
 
@@ -416,8 +741,8 @@ int cismgpu_pcg_standard_3d(int nx, int ny, int nz, const cismgpu_par_t *par, co
                             double tolerance, int maxiters, double *err, int *niters, int itest, int jtest,
                             int rtest) {
     (void)itest; (void)jtest; (void)rtest;  // debug-print location only (verbose_pcg = .false.)
-    return solve(ALG_STANDARD, true, nx, ny, nz, par, indxA_2d, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, bu,
-                 bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, err, niters);
+    return oneshot_solve(ALG_STANDARD, true, nx, ny, nz, par, indxA_2d, indxA_3d, active_vertex, Auu, Auv, Avu, Avv,
+                         bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, err, niters);
 }
 
 int cismgpu_pcg_chrongear_3d(int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indxA_2d,
@@ -427,8 +752,8 @@ int cismgpu_pcg_chrongear_3d(int nx, int ny, int nz, const cismgpu_par_t *par, c
                              double tolerance, int maxiters, double *err, int *niters, int itest, int jtest,
                              int rtest) {
     (void)itest; (void)jtest; (void)rtest;
-    return solve(ALG_CHRONGEAR, true, nx, ny, nz, par, indxA_2d, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, bu,
-                 bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, err, niters);
+    return oneshot_solve(ALG_CHRONGEAR, true, nx, ny, nz, par, indxA_2d, indxA_3d, active_vertex, Auu, Auv, Avu,
+                         Avv, bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, err, niters);
 }
 
 int cismgpu_pcg_standard_2d(int nx, int ny, const cismgpu_par_t *par, const int32_t *indxA_2d,
@@ -437,8 +762,8 @@ int cismgpu_pcg_standard_2d(int nx, int ny, const cismgpu_par_t *par, const int3
                             int precond, int linear_solve_ncheck, double tolerance, int maxiters, double *err,
                             int *niters, int itest, int jtest, int rtest) {
     (void)itest; (void)jtest; (void)rtest;
-    return solve(ALG_STANDARD, false, nx, ny, 1, par, indxA_2d, nullptr, active_vertex, Auu, Auv, Avu, Avv, bu, bv,
-                 xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, err, niters);
+    return oneshot_solve(ALG_STANDARD, false, nx, ny, 1, par, indxA_2d, nullptr, active_vertex, Auu, Auv, Avu, Avv,
+                         bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, err, niters);
 }
 
 int cismgpu_pcg_chrongear_2d(int nx, int ny, const cismgpu_par_t *par, const int32_t *indxA_2d,
@@ -447,26 +772,196 @@ int cismgpu_pcg_chrongear_2d(int nx, int ny, const cismgpu_par_t *par, const int
                              int precond, int linear_solve_ncheck, double tolerance, int maxiters, double *err,
                              int *niters, int itest, int jtest, int rtest) {
     (void)itest; (void)jtest; (void)rtest;
-    return solve(ALG_CHRONGEAR, false, nx, ny, 1, par, indxA_2d, nullptr, active_vertex, Auu, Auv, Avu, Avv, bu,
-                 bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, err, niters);
+    return oneshot_solve(ALG_CHRONGEAR, false, nx, ny, 1, par, indxA_2d, nullptr, active_vertex, Auu, Auv, Avu, Avv,
+                         bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, err, niters);
 }
 
 int cismgpu_matvec_structured_3d(int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indxA_3d,
                                  const int32_t *active_vertex, const double *Auu, const double *Auv,
                                  const double *Avu, const double *Avv, const double *xu, const double *xv,
                                  double *yu, double *yv) {
-    return matvec(true, nx, ny, nz, par, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, xu, xv, yu, yv);
+    return oneshot_matvec(true, nx, ny, nz, par, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, xu, xv, yu, yv);
 }
 
 int cismgpu_matvec_structured_2d(int nx, int ny, const cismgpu_par_t *par, const int32_t *indxA_2d,
                                  const int32_t *active_vertex, const double *Auu, const double *Auv,
                                  const double *Avu, const double *Avv, const double *xu, const double *xv,
                                  double *yu, double *yv) {
-    return matvec(false, nx, ny, 1, par, indxA_2d, active_vertex, Auu, Auv, Avu, Avv, xu, xv, yu, yv);
+    return oneshot_matvec(false, nx, ny, 1, par, indxA_2d, active_vertex, Auu, Auv, Avu, Avv, xu, xv, yu, yv);
+}
+
+int cismgpu_solver_create(cismgpu_solver_t **out, int dims, int nx, int ny, int nz, const cismgpu_par_t *par,
+                          const int32_t *indxA, const int32_t *active_vertex, const double *Auu, const double *Auv,
+                          const double *Avu, const double *Avv, const double *bu, const double *bv,
+                          const double *xu0, const double *xv0, void *cuda_stream) {
+    g_last_error.clear();
+    if (!out) return fail(CISMGPU_EINVAL, "null handle pointer");
+    *out = nullptr;
+    if (dims != 2 && dims != 3) return fail(CISMGPU_EINVAL, "dims must be 2 or 3");
+    const bool is3d = dims == 3;
+    TRY(validate(nx, ny, is3d ? nz : 1, par, indxA, active_vertex, Auu, Auv, Avu, Avv, bu, bv));
+    TRY(validate_indx(indxA, is3d ? 27 : 9));
+    cismgpu_solver *h = new cismgpu_solver();
+    int rc = h->sv.init((cudaStream_t)cuda_stream);
+    const double *blocks[4] = {Auu, Auv, Avu, Avv};
+    if (!rc) rc = h->sv.upload(make_geom(nx, ny, is3d ? nz : 1, par), is3d, indxA, active_vertex, blocks, bu, bv,
+                               xu0, xv0);
+    if (!rc && cudaStreamSynchronize(h->sv.stream) != cudaSuccess) rc = fail(CISMGPU_ECUDA, "upload failed");
+    if (rc) {
+        delete h;
+        return rc;
+    }
+    *out = h;
+    return CISMGPU_OK;
+}
+
+int cismgpu_solver_solve(cismgpu_solver_t *h, int algorithm, int precond, int linear_solve_ncheck, double tolerance,
+                         int maxiters, double *err, int *niters) {
+    g_last_error.clear();
+    if (!h || !err || !niters) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    TRY(validate_solve_args(precond, linear_solve_ncheck, maxiters));
+    Solver &sv = h->sv;
+    TRY(sv.begin_solve());
+    TRY(run_algorithm(sv, algorithm, precond, linear_solve_ncheck, tolerance, maxiters));
+    return sv.finish_solve(err, niters);
+}
+
+int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm, int precond, int linear_solve_ncheck,
+                               double tolerance, int maxiters, double *errs, int *niters, int *statuses,
+                               void *cuda_stream) {
+    g_last_error.clear();
+    if (!solvers || n < 1 || !errs || !niters || !statuses) return fail(CISMGPU_EINVAL, "null argument");
+    TRY(validate_solve_args(precond, linear_solve_ncheck, maxiters));
+    if (algorithm != CISMGPU_ALG_MIXED_CHRONGEAR) {  // FP64 reference algorithms: one solve after another
+        int first = CISMGPU_OK;
+        for (int t = 0; t < n; ++t) {
+            statuses[t] = cismgpu_solver_solve(solvers[t], algorithm, precond, linear_solve_ncheck, tolerance,
+                                               maxiters, &errs[t], &niters[t]);
+            if (statuses[t] && !first) first = statuses[t];
+        }
+        return first;
+    }
+    std::vector<std::unique_lock<std::mutex>> locks;
+    for (int t = 0; t < n; ++t) {
+        if (!solvers[t]) return fail(CISMGPU_EINVAL, "null handle in batch");
+        locks.emplace_back(solvers[t]->mu);
+    }
+    Solver &s0 = solvers[0]->sv;
+    const int nzm = mixed_nzm(s0.g, s0.is3d);
+    for (int t = 0; t < n; ++t) {
+        Solver &sv = solvers[t]->sv;
+        if (sv.is3d != s0.is3d || mixed_nzm(sv.g, sv.is3d) != nzm)
+            return fail(CISMGPU_EINVAL, "batch members must share dims and the nz class (<=16 or <=32)");
+        TRY(mixed_prepare(sv, precond));
+        TRY(mixed_reset(sv, sv.stream));
+    }
+    for (int t = 0; t < n; ++t) CU(cudaStreamSynchronize(solvers[t]->sv.stream));
+    cudaStream_t s = cuda_stream ? (cudaStream_t)cuda_stream : s0.stream;
+    // one descriptor, state and tile list for the whole batch
+    std::vector<MDesc> descs(n);
+    std::vector<MState> states(n, mixed_init_state(tolerance, maxiters, linear_solve_ncheck));
+    std::vector<MTile> tiles;
+    for (int t = 0; t < n; ++t) {
+        descs[t] = mixed_desc(solvers[t]->sv, precond);
+        for (int k = 0; k < descs[t].ntiles; ++k) tiles.push_back(MTile{t, k});
+    }
+    // interleave tiles of different solves so that each CTA's share mixes sizes (round robin by tile index)
+    std::stable_sort(tiles.begin(), tiles.end(), [](const MTile &a, const MTile &b) { return a.tile < b.tile; });
+    GridBar B{0u, 0u, 0, n};
+    void *dmem = nullptr;
+    const size_t off_s = ((n * sizeof(MDesc)) + 255) / 256 * 256;
+    const size_t off_t = off_s + ((n * sizeof(MState)) + 255) / 256 * 256;
+    const size_t off_b = off_t + ((tiles.size() * sizeof(MTile)) + 255) / 256 * 256;
+    CU(cudaMallocAsync(&dmem, off_b + sizeof(GridBar), s));
+    char *base = static_cast<char *>(dmem);
+    MDesc *d_descs = reinterpret_cast<MDesc *>(base);
+    MState *d_states = reinterpret_cast<MState *>(base + off_s);
+    MTile *d_tiles = reinterpret_cast<MTile *>(base + off_t);
+    GridBar *d_bar = reinterpret_cast<GridBar *>(base + off_b);
+    CU(cudaMemcpyAsync(d_descs, descs.data(), n * sizeof(MDesc), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(d_states, states.data(), n * sizeof(MState), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(MTile), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(d_bar, &B, sizeof(GridBar), cudaMemcpyHostToDevice, s));
+    int rc = mixed_dispatch(s0.is3d, nzm, d_descs, d_states, d_tiles, (int)tiles.size(), d_bar, 4 * maxiters + 16, s);
+    if (rc) {
+        cudaFreeAsync(dmem, s);
+        return rc;
+    }
+    for (int t = 0; t < n; ++t) {
+        Solver &sv = solvers[t]->sv;
+        const Ptrs p = sv.ptrs();
+        k_mstate_to_solve<<<1, 1, 0, s>>>(d_states + t, sv.state.as<SolveState>(), d_bar);
+        k_halo<<<nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4)), kBlock, 0, s>>>(sv.g, p.xu, p.xv, nullptr);
+    }
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(states.data(), d_states, n * sizeof(MState), cudaMemcpyDeviceToHost, s));
+    GridBar hb;
+    CU(cudaMemcpyAsync(&hb, d_bar, sizeof(GridBar), cudaMemcpyDeviceToHost, s));
+    CU(cudaFreeAsync(dmem, s));
+    CU(cudaStreamSynchronize(s));
+    int first = CISMGPU_OK;
+    for (int t = 0; t < n; ++t) {
+        errs[t] = states[t].err;
+        niters[t] = states[t].niters;
+        statuses[t] = (hb.abort && !states[t].done) ? CISMGPU_ETIMEOUT : states[t].status;
+        if (statuses[t] && !first) first = statuses[t];
+    }
+    if (first) return fail(first, "batch member failed (see statuses)");
+    return CISMGPU_OK;
+}
+
+int cismgpu_solver_get_x(cismgpu_solver_t *h, double *xu, double *xv) {
+    g_last_error.clear();
+    if (!h || !xu || !xv) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    return h->sv.download(VX_U, VX_V, xu, xv);
+}
+
+int cismgpu_solver_profile(cismgpu_solver_t *h, int enable) {
+    if (!h) return fail(CISMGPU_EINVAL, "null handle");
+    std::lock_guard<std::mutex> lk(h->mu);
+    h->sv.prof = enable != 0;
+    h->sv.prof_ms = 0.0;
+    h->sv.prof_n = 0;
+    h->sv.pused = 0;
+    return CISMGPU_OK;
+}
+
+int cismgpu_solver_profile_read(cismgpu_solver_t *h, double *total_ms, int *launches, double *bytes_per_launch) {
+    if (!h || !total_ms || !launches || !bytes_per_launch) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    *total_ms = h->sv.prof_ms;
+    *launches = h->sv.prof_n;
+    *bytes_per_launch = h->sv.prof_bytes;
+    return CISMGPU_OK;
+}
+
+size_t cismgpu_solver_device_bytes(const cismgpu_solver_t *h) {
+    if (!h) return 0;
+    const Solver &s = h->sv;
+    return s.A.n + s.raw.n + s.vec.n + s.act.n + s.partials.n + s.state.n + s.map.n + s.mixed.bytes();
+}
+
+int cismgpu_solver_destroy(cismgpu_solver_t *h) {
+    if (!h) return CISMGPU_OK;
+    {
+        std::lock_guard<std::mutex> lk(h->mu);
+        if (h->sv.stream) cudaStreamSynchronize(h->sv.stream);
+    }
+    delete h;
+    return CISMGPU_OK;
+}
+
+int cismgpu_set_oneshot_algorithm(int algorithm) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    const int prev = g_oneshot_alg;
+    g_oneshot_alg = (algorithm >= CISMGPU_ALG_STANDARD && algorithm <= CISMGPU_ALG_MIXED_CHRONGEAR) ? algorithm : -1;
+    return prev;
 }
 
 const char *cismgpu_last_error(void) { return g_last_error.c_str(); }
 
-const char *cismgpu_version(void) { return "cismgpu 0.1 (sm_100a)"; }
+const char *cismgpu_version(void) { return "cismgpu 0.2 (sm_100a)"; }
 
 }  // extern "C"

@@ -145,6 +145,67 @@ int cismgpu_matvec_structured_2d(int nx, int ny, const cismgpu_par_t *par,
                                  const double *xu, const double *xv,
                                  double *yu, double *yv);
 
+/* ------------------------------------------------------------------------
+ * Device-resident solver handles (no reference counterpart: the reference
+ * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps
+ * them, and all Krylov state, in HBM, so repeated solves (benchmarking, the
+ * serving loop, batched ensembles) pay no host<->device traffic.  Each handle
+ * owns its buffers and runs on the stream given at creation (NULL: a new
+ * non-blocking stream), so handles on different streams run concurrently.
+ * ------------------------------------------------------------------------ */
+typedef struct cismgpu_solver cismgpu_solver_t;
+
+/* algorithms */
+#define CISMGPU_ALG_STANDARD        0  /* pcg_solver_standard_*  (FP64, reference statements)        */
+#define CISMGPU_ALG_CHRONGEAR       1  /* pcg_solver_chrongear_* (FP64, reference statements)        */
+#define CISMGPU_ALG_MIXED_CHRONGEAR 2  /* FP32 inner Chronopoulos-Gear + FP64 iterative refinement  */
+
+/* dims = 3 (27-point blocks, indxA = indxA_3d) or 2 (9-point blocks, indxA = indxA_2d, nz = 1).
+ * Array arguments as for the solver calls above; x0 may be NULL (zero initial guess). */
+int cismgpu_solver_create(cismgpu_solver_t **out, int dims, int nx, int ny, int nz,
+                          const cismgpu_par_t *par, const int32_t *indxA, const int32_t *active_vertex,
+                          const double *Auu, const double *Auv, const double *Avu, const double *Avv,
+                          const double *bu, const double *bv, const double *xu0, const double *xv0,
+                          void *cuda_stream);
+
+/* Solve from the stored x0; err/niters as in the reference calls (for the mixed
+ * algorithm: err is the FP64 true relative residual, niters the total inner
+ * iterations).  Blocks until the solve has finished. */
+int cismgpu_solver_solve(cismgpu_solver_t *s, int algorithm, int precond, int linear_solve_ncheck,
+                         double tolerance, int maxiters, double *err, int *niters);
+
+/* Solve n independent systems (uneven sizes allowed) in ONE persistent cooperative
+ * launch on cuda_stream (NULL: the first handle's stream).  algorithm must be
+ * CISMGPU_ALG_MIXED_CHRONGEAR; all handles must have the same dims, and nz <= 32.
+ * Every system's result is bit-identical to solving it alone.  Per-system
+ * err/niters/status arrays of length n; returns the first nonzero status. */
+int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm, int precond,
+                               int linear_solve_ncheck, double tolerance, int maxiters,
+                               double *errs, int *niters, int *statuses, void *cuda_stream);
+
+/* Copy the current solution (caller's Fortran layout, halo entries included) to host memory. */
+int cismgpu_solver_get_x(cismgpu_solver_t *s, double *xu, double *xv);
+
+/* Per-kernel CUDA-event timing of the structured matvec launches (off by default).
+ * read: total device milliseconds, launch count, and algorithmic bytes per launch
+ * (active owned nodes x (4*NC*sizeof(A) + vector streams)). */
+int cismgpu_solver_profile(cismgpu_solver_t *s, int enable);
+int cismgpu_solver_profile_read(cismgpu_solver_t *s, double *total_ms, int *launches, double *bytes_per_launch);
+
+/* Device bytes held by the handle. */
+size_t cismgpu_solver_device_bytes(const cismgpu_solver_t *s);
+
+int cismgpu_solver_destroy(cismgpu_solver_t *s);
+
+/* Algorithm used by the four reference-signature calls above.  Default (-1): the
+ * reference algorithm each call names, in FP64 (bit-reproducible, parity-tested).
+ * CISMGPU_ALG_MIXED_CHRONGEAR: all four calls run the mixed-precision persistent
+ * Chronopoulos-Gear solver instead (same system, same err definition, FP64 true
+ * residual below the tolerance; x agrees with the FP64 solution to the accuracy the
+ * tolerance implies).  No reference counterpart: a configuration switch of this
+ * library.  Returns the previous setting. */
+int cismgpu_set_oneshot_algorithm(int algorithm);
+
 /* Message for the last nonzero status on the calling thread ("" if none). */
 const char *cismgpu_last_error(void);
 

@@ -1,0 +1,125 @@
+"""Mixed-precision persistent Chronopoulos-Gear (FP32 recurrences, FP64 x, FP64 residual
+replacement) and its batched form.  Every result is checked against the FP64 oracle:
+the FP64 true relative residual must reach the tolerance, and x must agree with the
+oracle's FP64 solution within the accuracy a 1e-8 residual implies (bound in each test).
+"""
+import numpy as np
+import pytest
+
+import cism_b200 as cg
+import oracle
+from cism_b200 import assembly as asm
+from tests import problems
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    num = np.linalg.norm(np.concatenate([(a[0] - b[0]).ravel(), (a[1] - b[1]).ravel()]))
+    den = np.linalg.norm(np.concatenate([b[0].ravel(), b[1].ravel()]))
+    return num / den
+
+
+def true_residual(P, xu, xv):
+    yu, yv = oracle.matvec(P, oracle.halo(P.nx, P.ny, P.nz, P.par, xu), oracle.halo(P.nx, P.ny, P.nz, P.par, xv))
+    p = P.par
+    sl = (slice(p["staggered_jlo"] - 1, p["staggered_jhi"]), slice(p["staggered_ilo"] - 1, p["staggered_ihi"]))
+    ru, rv = (P.bu - yu)[sl], (P.bv - yv)[sl]
+    return np.sqrt(np.sum(ru * ru) + np.sum(rv * rv)) / np.sqrt(np.sum(P.bu[sl] ** 2) + np.sum(P.bv[sl] ** 2))
+
+
+CASES = [
+    ("dome-sia", lambda: asm.dome(), 2, 1e-7),
+    ("dome-diag", lambda: asm.dome(), 1, 1e-6),
+    ("slab3d-noslip-diag", lambda: problems.slab_3d(seed=5, sliding=False), 1, 1e-6),
+    ("slab3d-sliding-sia", lambda: problems.slab_3d(seed=1, ewn=20, nsn=17), 2, 1e-5),
+    ("ssa2d-diag", lambda: asm.ssa_random(ewn=61, nsn=57, seed=3), 1, 1e-5),
+    ("ssa2d-none", lambda: problems.slab_2d(seed=1), 0, 1e-5),
+]
+
+
+@pytest.mark.parametrize("name,make,precond,xbound", CASES, ids=[c[0] for c in CASES])
+def test_mixed_reaches_fp64_tolerance(gpu_lib, name, make, precond, xbound):
+    P = make()
+    S = cg.DeviceSolver(P)
+    err, nit = S.solve(cg.ALG_MIXED_CHRONGEAR, precond, 5, 1e-8, 5000)
+    xu, xv = S.x()
+    assert err < 1e-8
+    assert true_residual(P, xu, xv) < 1.5e-8        # independent FP64 residual on the CPU
+    st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, precond, tol=1e-8, maxiters=5000)
+    assert st == 0 and oerr < 1e-8
+    assert rel((xu, xv), (ou, ov)) < xbound
+    # the FP64 reference algorithm needs about as many iterations
+    assert nit <= 2.0 * onit + 10
+
+
+def test_mixed_is_deterministic(gpu_lib):
+    P = asm.ssa_random(ewn=61, nsn=57, seed=4)
+    S = cg.DeviceSolver(P)
+    a = S.solve(cg.ALG_MIXED_CHRONGEAR, 1, 5, 1e-8, 5000), S.x()
+    b = S.solve(cg.ALG_MIXED_CHRONGEAR, 1, 5, 1e-8, 5000), S.x()
+    assert a[0] == b[0]
+    np.testing.assert_array_equal(a[1][0], b[1][0])
+    np.testing.assert_array_equal(a[1][1], b[1][1])
+
+
+def test_batch_equals_alone(gpu_lib):
+    """Uneven 3D solves in one persistent launch give bit-identical results to solving each alone."""
+    probs = [problems.slab_3d(seed=s, ewn=8 + 5 * s, nsn=9 + 3 * s, nz=5 + (s % 3)) for s in range(5)]
+    solvers = [cg.DeviceSolver(P) for P in probs]
+    alone = []
+    for S in solvers:
+        e, n = S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 3000)
+        alone.append((e, n, S.x()))
+    errs, nits, sts = cg.solve_batch(solvers, cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 3000)
+    assert not np.any(sts)
+    for t, S in enumerate(solvers):
+        xu, xv = S.x()
+        assert errs[t] == alone[t][0] and nits[t] == alone[t][1]
+        np.testing.assert_array_equal(xu, alone[t][2][0])
+        np.testing.assert_array_equal(xv, alone[t][2][1])
+        assert errs[t] < 1e-8
+
+
+def test_batch_mixed_2d_sizes(gpu_lib):
+    probs = [asm.ssa_random(ewn=40 + 9 * s, nsn=33 + 7 * s, seed=10 + s) for s in range(4)]
+    solvers = [cg.DeviceSolver(P) for P in probs]
+    errs, nits, sts = cg.solve_batch(solvers, cg.ALG_MIXED_CHRONGEAR, 1, 5, 1e-8, 5000)
+    assert not np.any(sts) and np.all(errs < 1e-8)
+    for t, P in enumerate(probs):
+        st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, 1, tol=1e-8, maxiters=5000)
+        assert rel(solvers[t].x(), (ou, ov)) < 1e-5
+
+
+def test_handle_fp64_matches_oneshot(gpu_lib):
+    """The device-resident handle runs the same FP64 kernels as the one-shot C-ABI call."""
+    P = asm.dome()
+    S = cg.DeviceSolver(P)
+    e, n = S.solve(cg.ALG_CHRONGEAR, 2, 5, 1e-8, 200)
+    st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, 2, summode=oracle.SUM_DDTREE)
+    xu, xv = S.x()
+    assert e == oerr and n == onit
+    np.testing.assert_array_equal(xu, ou)
+    np.testing.assert_array_equal(xv, ov)
+
+
+def test_mixed_boundary_conditions(gpu_lib):
+    for bc in ("outflow", "no_ice"):
+        P = problems.slab_3d(seed=3, boundary_ice=True, bc=bc, sliding=False)
+        st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, 1, tol=1e-8, maxiters=3000)
+        S = cg.DeviceSolver(P)
+        try:
+            err, nit = S.solve(cg.ALG_MIXED_CHRONGEAR, 1, 5, 1e-8, 3000)
+        except cg.CismGpuError as e:
+            err = None
+        if st == 0 and oerr < 1e-8:
+            assert err is not None and err < 1e-8
+            assert rel(S.x(), (ou, ov)) < 1e-5
+
+
+def test_mixed_rejects_unsupported(gpu_lib):
+    P = problems.slab_2d(seed=1)
+    S = cg.DeviceSolver(P)
+    with pytest.raises(cg.CismGpuError) as e:
+        S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 100)  # SIA in 2D
+    assert e.value.status == 3
