@@ -70,10 +70,21 @@ def run_profile(args):
     P = make_problem(args.workload)
     S = cg.DeviceSolver(P)
     pc = PROFILE_PRECOND[args.workload]
-    for k in range(args.warmup + args.steps):
+    for k in range(args.warmup):
+        e, n = S.solve(cg.ALG_MIXED_CHRONGEAR, pc, NCHECK, TOL, MAXITERS)
+    S.profile(True)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
         e, n = S.solve(cg.ALG_MIXED_CHRONGEAR, pc, NCHECK, TOL, MAXITERS)
     torch.cuda.synchronize()
-    print(f"profile workload={args.workload} precond={pc} niters={n} err={e:.3e} unknowns={P.n_unknowns}")
+    wall = (time.perf_counter() - t0) / max(args.steps, 1)
+    ms, nl, by = S.profile_read()
+    print(f"profile workload={args.workload} precond={pc} niters={n} err={e:.3e} unknowns={P.n_unknowns} "
+          f"kernel_ms={ms / max(nl, 1):.3f} wall_ms={1e3 * wall:.3f} GB/s={by / (ms / max(nl, 1) / 1e3) / 1e9:.1f}")
+    if args.fp64:
+        t0 = time.perf_counter()
+        e, n = S.solve(cg.ALG_CHRONGEAR, pc, NCHECK, TOL, MAXITERS)
+        print(f"fp64 plain: niters={n} err={e:.3e} wall_ms={1e3 * (time.perf_counter() - t0):.3f}")
     return 0
 
 
@@ -289,6 +300,7 @@ def run_ours(args):
         total_ms = float(t.item())
     prof_ms, prof_n, prof_bytes = S.profile_read()
     S.profile(False)
+    xm = S.x()  # the mixed solution, before the FP64 solves below overwrite x
     # --- plain FP64 GPU PCG (reference algorithm, bit-identical to the oracle) ---
     with torch.cuda.stream(stream):
         e64, n64 = S.solve(cg.ALG_CHRONGEAR, PRECOND, NCHECK, TOL, MAXITERS)  # warm
@@ -305,7 +317,6 @@ def run_ours(args):
         fp64_ms.append(ev0.elapsed_time(ev1))
     fp64_solve_ms = float(np.median(fp64_ms))
 
-    xm = S.x()
     num = math.sqrt(float(np.sum((xm[0] - x64[0]) ** 2) + np.sum((xm[1] - x64[1]) ** 2)))
     den = math.sqrt(float(np.sum(x64[0] ** 2) + np.sum(x64[1] ** 2)))
     err_vs_fp64 = num / den
@@ -387,6 +398,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="bench", choices=["bench", "profile"])
     ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "dome"])
+    ap.add_argument("--fp64", action="store_true", help="profile mode: also time one plain FP64 solve")
     args = ap.parse_args()
     if args.mode == "profile":
         return run_profile(args)

@@ -163,7 +163,7 @@ struct Solver {
         is3d = three_d;
         NC = is3d ? 27 : 9;
         nvec = (long long)g.nz * g.NQ;
-        mixed.valid = false;
+        mixed.stale = true;  // new matrix: FP32 copy and factors must be rebuilt
         n_active_owned = 0;
         for (int j = g.jlo; j <= g.jhi; ++j)
             for (int i = g.ilo; i <= g.ihi; ++i) n_active_owned += active[(long long)j * g.NX + i] != 0;
@@ -427,7 +427,21 @@ __global__ void k_mstate_to_solve(const MState *ms, SolveState *st, const GridBa
 
 static int mixed_nzm(const Geom &g, bool is3d) { return !is3d ? 1 : (g.nz <= 16 ? 16 : 32); }
 
-// Allocate and fill the FP32 copy of the matrix and the preconditioner factors.
+static MDesc mixed_desc(const Solver &sv, int precond);
+
+template <int NC>
+static int mixed_build_maps(Solver &sv) {
+    constexpr int TX = TileShape<NC>::TX, TY = TileShape<NC>::TY;
+    const MDesc D = mixed_desc(sv, sv.mixed.precond < 0 ? 0 : sv.mixed.precond);
+    const long long n = (long long)D.ntiles * (TX + 2) * (TY + 2);
+    k_slot_maps<TX, TY><<<nblocks(n), kBlock, 0, sv.stream>>>(D, sv.mixed.maps);
+    k_to_f32<NC><<<1184, kBlock, 0, sv.stream>>>(sv.g, sv.A.as<double>(), sv.mixed.A32);
+    CU(cudaGetLastError());
+    return CISMGPU_OK;
+}
+
+// Allocate and fill the FP32 copy of the matrix, the tile slot maps and the
+// preconditioner factors.
 static int mixed_prepare(Solver &sv, int precond) {
     if (sv.g.nz > kMixedMaxNz) return fail(CISMGPU_EUNSUPPORTED, "mixed solver supports nz <= 32");
     if (!(precond == 0 || precond == 1 || (precond == 2 && sv.is3d)))
@@ -436,9 +450,11 @@ static int mixed_prepare(Solver &sv, int precond) {
     const long long nvec = sv.nvec;
     const int NC = sv.NC;
     const Geom &g = sv.g;
-    const int tiles_x = (g.ihi - g.ilo + kTX) / kTX, tiles_y = (g.jhi - g.jlo + kTY) / kTY;
+    const int TX = NC == 27 ? TileShape<27>::TX : TileShape<9>::TX, TY = NC == 27 ? TileShape<27>::TY : TileShape<9>::TY;
+    const int tiles_x = (g.ihi - g.ilo + TX) / TX, tiles_y = (g.jhi - g.jlo + TY) / TY;
     const int ntiles = tiles_x * tiles_y;
-    if (!m.valid) {
+    const bool same_shape = m.valid && m.shape_nvec == nvec && m.shape_nc == NC && m.ntiles == ntiles;
+    if (!same_shape) {
         m.release();
         size_t bytes = 0;
         auto alloc = [&](void **p, size_t n) -> cudaError_t {
@@ -448,21 +464,27 @@ static int mixed_prepare(Solver &sv, int precond) {
         CU(alloc((void **)&m.A32, (size_t)4 * NC * nvec * sizeof(float)));
         CU(alloc((void **)&m.pre, (size_t)6 * nvec * sizeof(float)));
         CU(alloc((void **)&m.vec, (size_t)16 * nvec * sizeof(float)));
-        CU(alloc((void **)&m.partials, (size_t)ntiles * 3 * sizeof(DD)));
+        CU(alloc((void **)&m.partials, (size_t)ntiles * 2 * 3 * sizeof(DD)));
+        CU(alloc((void **)&m.maps, (size_t)ntiles * (TX + 2) * (TY + 2) * sizeof(int)));
         CU(alloc((void **)&m.state, sizeof(MState)));
         CU(alloc((void **)&m.desc, sizeof(MDesc)));
         CU(alloc((void **)&m.tiles, (size_t)ntiles * sizeof(MTile)));
         CU(alloc((void **)&m.bar, sizeof(GridBar)));
         m.nbytes = bytes;
         m.ntiles = ntiles;
-        const long long n = 4LL * NC * nvec;
-        k_to_f32<<<1184, kBlock, 0, sv.stream>>>(sv.A.as<double>(), m.A32, n);
-        CU(cudaGetLastError());
+        m.shape_nvec = nvec;
+        m.shape_nc = NC;
         std::vector<MTile> tl(ntiles);
         for (int t = 0; t < ntiles; ++t) tl[t] = MTile{0, t};
         CU(cudaMemcpyAsync(m.tiles, tl.data(), ntiles * sizeof(MTile), cudaMemcpyHostToDevice, sv.stream));
         CU(cudaStreamSynchronize(sv.stream));  // tl goes out of scope
         m.valid = true;
+        m.stale = true;
+    }
+    if (m.stale) {  // new matrix or active mask: FP32 copy and slot maps
+        if (NC == 27) TRY(mixed_build_maps<27>(sv));
+        else TRY(mixed_build_maps<9>(sv));
+        m.stale = false;
         m.precond = -1;
     }
     if (m.precond != precond) {
@@ -484,8 +506,10 @@ static MDesc mixed_desc(const Solver &sv, int precond) {
     D.g = sv.g;
     D.NC = sv.NC;
     D.precond = precond;
-    D.tiles_x = (sv.g.ihi - sv.g.ilo + kTX) / kTX;
-    D.tiles_y = (sv.g.jhi - sv.g.jlo + kTY) / kTY;
+    const int TX = sv.NC == 27 ? TileShape<27>::TX : TileShape<9>::TX;
+    const int TY = sv.NC == 27 ? TileShape<27>::TY : TileShape<9>::TY;
+    D.tiles_x = (sv.g.ihi - sv.g.ilo + TX) / TX;
+    D.tiles_y = (sv.g.jhi - sv.g.jlo + TY) / TY;
     D.ntiles = D.tiles_x * D.tiles_y;
     D.A32 = m.A32;
     D.A64 = sv.A.as<double>();
@@ -501,6 +525,7 @@ static MDesc mixed_desc(const Solver &sv, int precond) {
     D.z = V + 6 * vs;
     D.d = V + 7 * vs;
     D.partials = m.partials;
+    D.maps = m.maps;
     return D;
 }
 
@@ -517,17 +542,22 @@ static MState mixed_init_state(double tol, int maxiters, int ncheck) {
 }
 
 // x = x0 and all FP32 recurrence vectors = 0 (the reference zeroes its work vectors, :3048-3061)
+// The reference starts with halo(x) (:3094-3097) and, with inactive halo vertices and the
+// diagonal or SIA preconditioner, never changes x there again; the mixed kernel writes
+// only owned unknowns, so x leaves with the same halo values.
 static int mixed_reset(Solver &sv, cudaStream_t s) {
     const Ptrs p = sv.ptrs();
     CU(cudaMemcpyAsync(p.xu, p.x0u, 2 * sv.nvec * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    k_halo<<<nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4)), kBlock, 0, s>>>(sv.g, p.xu, p.xv, nullptr);
+    CU(cudaGetLastError());
     CU(cudaMemsetAsync(sv.mixed.vec, 0, (size_t)16 * sv.nvec * sizeof(float), s));
     return CISMGPU_OK;
 }
 
 template <int NC, int NZM>
 static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_tiles, int ntiles, GridBar *d_bar,
-                        int max_steps, cudaStream_t s) {
-    const size_t smem = sizeof(MShared<NZM>);
+                        int max_steps, cudaStream_t s, const std::vector<MTile> *host_tiles) {
+    const size_t smem = sizeof(MShared<NC, NZM>);
     static bool attr_set = false;
     if (!attr_set) {
         CU(cudaFuncSetAttribute(k_mixed<NC, NZM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -540,6 +570,17 @@ static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_t
     if (occ < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM");
     int grid = nsm * occ;
     if (grid > ntiles) grid = ntiles;
+    if (host_tiles) {  // each CTA caches the state of at most kMaxCtaSolves solves
+        for (int b = 0; b < grid; ++b) {
+            std::vector<int> seen;
+            for (int w = b; w < ntiles; w += grid) {
+                const int sv = (*host_tiles)[w].solve;
+                if (std::find(seen.begin(), seen.end(), sv) == seen.end()) seen.push_back(sv);
+            }
+            if ((int)seen.size() > kMaxCtaSolves)
+                return fail(CISMGPU_EUNSUPPORTED, "batch too fragmented for one launch (solves per CTA > 32)");
+        }
+    }
     void *args[] = {(void *)&d_descs, (void *)&d_states, (void *)&d_tiles, (void *)&ntiles, (void *)&d_bar,
                     (void *)&max_steps};
     CU(cudaLaunchCooperativeKernel((const void *)k_mixed<NC, NZM>, dim3(grid), dim3(kBlock), args, smem, s));
@@ -547,10 +588,10 @@ static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_t
 }
 
 static int mixed_dispatch(bool is3d, int nzm, const MDesc *d, MState *st, const MTile *t, int nt, GridBar *bar,
-                          int max_steps, cudaStream_t s) {
-    if (!is3d) return mixed_launch<9, 1>(d, st, t, nt, bar, max_steps, s);
-    if (nzm == 16) return mixed_launch<27, 16>(d, st, t, nt, bar, max_steps, s);
-    return mixed_launch<27, 32>(d, st, t, nt, bar, max_steps, s);
+                          int max_steps, cudaStream_t s, const std::vector<MTile> *host_tiles = nullptr) {
+    if (!is3d) return mixed_launch<9, 1>(d, st, t, nt, bar, max_steps, s, host_tiles);
+    if (nzm == 16) return mixed_launch<27, 16>(d, st, t, nt, bar, max_steps, s, host_tiles);
+    return mixed_launch<27, 32>(d, st, t, nt, bar, max_steps, s, host_tiles);
 }
 
 static double mixed_iter_bytes(const Solver &sv, int precond) {
@@ -582,10 +623,7 @@ int Solver::run_mixed(int precond, int ncheck, double tol, int maxiters) {
     }
     TRY(mixed_dispatch(is3d, mixed_nzm(g, is3d), m.desc, m.state, m.tiles, m.ntiles, m.bar, max_steps, stream));
     if (prof) CU(cudaEventRecord(e1, stream));
-    const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
-    const Ptrs p = ptrs();
     k_mstate_to_solve<<<1, 1, 0, stream>>>(m.state, state.as<SolveState>(), m.bar);
-    k_halo<<<hb, kBlock, 0, stream>>>(g, p.xu, p.xv, nullptr);  // the caller's x carries halo values
     CU(cudaGetLastError());
     if (prof) {
         MState hs;
@@ -866,8 +904,8 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
         descs[t] = mixed_desc(solvers[t]->sv, precond);
         for (int k = 0; k < descs[t].ntiles; ++k) tiles.push_back(MTile{t, k});
     }
-    // interleave tiles of different solves so that each CTA's share mixes sizes (round robin by tile index)
-    std::stable_sort(tiles.begin(), tiles.end(), [](const MTile &a, const MTile &b) { return a.tile < b.tile; });
+    // tiles in (solve, tile) order; CTAs take them round robin, so a solve's tiles spread over
+    // consecutive CTAs and each CTA holds tiles of only a few solves
     GridBar B{0u, 0u, 0, n};
     void *dmem = nullptr;
     const size_t off_s = ((n * sizeof(MDesc)) + 255) / 256 * 256;
@@ -883,17 +921,14 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
     CU(cudaMemcpyAsync(d_states, states.data(), n * sizeof(MState), cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(MTile), cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(d_bar, &B, sizeof(GridBar), cudaMemcpyHostToDevice, s));
-    int rc = mixed_dispatch(s0.is3d, nzm, d_descs, d_states, d_tiles, (int)tiles.size(), d_bar, 4 * maxiters + 16, s);
+    int rc = mixed_dispatch(s0.is3d, nzm, d_descs, d_states, d_tiles, (int)tiles.size(), d_bar, 4 * maxiters + 16, s,
+                            &tiles);
     if (rc) {
         cudaFreeAsync(dmem, s);
         return rc;
     }
-    for (int t = 0; t < n; ++t) {
-        Solver &sv = solvers[t]->sv;
-        const Ptrs p = sv.ptrs();
-        k_mstate_to_solve<<<1, 1, 0, s>>>(d_states + t, sv.state.as<SolveState>(), d_bar);
-        k_halo<<<nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4)), kBlock, 0, s>>>(sv.g, p.xu, p.xv, nullptr);
-    }
+    for (int t = 0; t < n; ++t)
+        k_mstate_to_solve<<<1, 1, 0, s>>>(d_states + t, solvers[t]->sv.state.as<SolveState>(), d_bar);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(states.data(), d_states, n * sizeof(MState), cudaMemcpyDeviceToHost, s));
     GridBar hb;

@@ -29,8 +29,6 @@
 
 namespace cismgpu {
 
-constexpr int kTX = 32, kTY = 8;                 // tile of columns (one thread per column)
-constexpr int kSlots = (kTX + 2) * (kTY + 2);    // tile + one-column halo ring
 constexpr int kMixedMaxNz = 32;                  // shared-memory bound of the mixed kernel (levels)
 
 enum MStep { MS_INIT = 0, MS_A, MS_MERGED, MS_B, MS_CHECK, MS_DONE };
@@ -49,7 +47,8 @@ struct MDesc {
     double *x;           // [2][nz][NQ]
     float *r[2], *q[2], *Az[2];  // [2][nz][NQ] each (u, v planes)
     float *z, *d;                // [2][nz][NQ]
-    DD *partials;        // [ntiles][3]
+    DD *partials;        // [ntiles][2 step parities][3]
+    const int *maps;     // [ntiles][(TX+2)*(TY+2)] slot maps (k_slot_maps)
 };
 
 struct MState {
@@ -214,12 +213,29 @@ __device__ void advance_state(MState &S, const MDesc &D, double S0, double S1, d
 // ---------------------------------------------------------------------------
 // tile work
 // ---------------------------------------------------------------------------
-template <int NZM>
+// Tile shapes: one CTA of 256 threads per tile.  2D: 64 x 16 columns (4 per thread);
+// 3D: 32 x 8 columns with nz levels each.
+template <int NC> struct TileShape;
+template <> struct TileShape<9> { static constexpr int TX = 64, TY = 16; };
+template <> struct TileShape<27> { static constexpr int TX = 32, TY = 8; };
+
+constexpr int kMaxCtaSolves = 32;  // distinct solves whose tiles one CTA may hold in a launch
+
+template <int NC, int NZM>
 struct MShared {
-    float z[2][NZM][kSlots];       // preconditioned residual on tile + halo
-    float rt[2][NZM][kTX * kTY];   // new residual on the tile columns
-    DD red[8];
-    bool last;
+    static constexpr int TX = TileShape<NC>::TX, TY = TileShape<NC>::TY;
+    static constexpr int NS = (TX + 2) * (TY + 2), NT = TX * TY;
+    static constexpr int KP = (NC == 27) ? NZM + 2 : 1;  // z levels with a zero row above and below
+    float z[2][KP][NS];        // preconditioned residual on tile + halo
+    float rt[2][NZM][NT];      // new residual on the tile columns
+    int map[NS];               // slot map of the current tile (k_slot_maps)
+    MDesc D;                   // descriptor of the current tile's solve
+    MState st[kMaxCtaSolves];  // this CTA's copy of the state of every solve it holds
+    int sid[kMaxCtaSolves];    // solve index of each cached state
+    int owner[kMaxCtaSolves];  // 1 if this CTA holds tile 0 of the solve (reports it)
+    int nsolve;
+    int cur;                   // cache slot described by D
+    DD red[8][3];
 };
 
 // Loads of data that other CTAs wrote earlier in the same launch go through L2
@@ -227,78 +243,147 @@ struct MShared {
 __device__ __forceinline__ float ldf(const float *p) { return __ldcg(p); }
 __device__ __forceinline__ double ldd(const double *p) { return __ldcg(p); }
 
-__device__ __forceinline__ MState load_state(const MState *p) {
-    MState s;
-    const unsigned long long *src = reinterpret_cast<const unsigned long long *>(p);
-    unsigned long long *dst = reinterpret_cast<unsigned long long *>(&s);
+// Block tree over 256 threads for three dd fields at once; result in thread 0.
+__device__ __forceinline__ void block_tree3(DD &a, DD &b, DD &c, DD (*sm)[3]) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int w = 0; w < (int)(sizeof(MState) / 8); ++w) dst[w] = __ldcg(src + w);
-    return s;
-}
-
-// z = M^-1 r on one column, in place in smem (s = slot), FP32.
-template <int NZM>
-__device__ __forceinline__ void precond_col(const MDesc &D, float (*zc)[NZM][kSlots], int s, long long q) {
-    const int nz = D.g.nz;
-    const long long plane = (long long)nz * D.g.NQ;
-    for (int c = 0; c < 2; ++c) {
-        float (*z)[kSlots] = zc[c];
-        if (D.precond == 1) {
-            const float *inv = D.pre + c * plane;
-            for (int k = 0; k < nz; ++k) z[k][s] = z[k][s] * inv[(long long)k * D.g.NQ + q];
-        } else if (D.precond == 2) {
-            const float *ib = D.pre + (c * 3 + 0) * plane, *sb = D.pre + (c * 3 + 1) * plane,
-                        *gm = D.pre + (c * 3 + 2) * plane;
-            // forward: y_1 = r_1/beta_1; y_k = (r_k - sb_k y_{k-1})/beta_k ; back: z_k = y_k - gamma_{k+1} z_{k+1}
-            float prev = z[0][s] * ib[q];
-            z[0][s] = prev;
-            for (int k = 1; k < nz; ++k) {
-                const long long e = (long long)k * D.g.NQ + q;
-                prev = (z[k][s] - sb[e] * prev) * ib[e];
-                z[k][s] = prev;
-            }
-            for (int k = nz - 2; k >= 0; --k)
-                z[k][s] = z[k][s] - gm[(long long)(k + 1) * D.g.NQ + q] * z[k + 1][s];
+    for (int off = 16; off >= 1; off >>= 1) {
+        DD oa = dd_shfl_down(a, off), ob = dd_shfl_down(b, off), oc = dd_shfl_down(c, off);
+        if (lane + off < 32) { a = dd_add(a, oa); b = dd_add(b, ob); c = dd_add(c, oc); }
+    }
+    __syncthreads();
+    if (lane == 0) { sm[warp][0] = a; sm[warp][1] = b; sm[warp][2] = c; }
+    __syncthreads();
+    if (warp == 0) {
+        const DD z0{0.0, 0.0};
+        a = lane < 8 ? sm[lane][0] : z0;
+        b = lane < 8 ? sm[lane][1] : z0;
+        c = lane < 8 ? sm[lane][2] : z0;
+#pragma unroll
+        for (int off = 4; off >= 1; off >>= 1) {
+            DD oa = dd_shfl_down(a, off), ob = dd_shfl_down(b, off), oc = dd_shfl_down(c, off);
+            if (lane + off < 32) { a = dd_add(a, oa); b = dd_add(b, ob); c = dd_add(c, oc); }
         }
-        // precond 0: z = r
     }
 }
 
-// One tile of one solve for the solve's current step.  Returns the three partials.
-template <int NC, int NZM>
-__device__ void tile_step(const MDesc &D, const MState &S, int tile, MShared<NZM> &sh, DD &p0, DD &p1, DD &p2) {
+// Slot map entry: (halo source column + 1) << 2 | live | mine << 1.  Source -1 means the
+// slot holds zero (zero boundary condition or outside the array).
+__device__ __forceinline__ int map_src(int v) { return (v >> 2) - 1; }
+__device__ __forceinline__ bool map_live(int v) { return (v & 1) != 0; }
+__device__ __forceinline__ bool map_mine(int v) { return (v & 2) != 0; }
+
+template <int TX, int TY>
+__global__ void k_slot_maps(MDesc D, int *maps) {
+    constexpr int NS = (TX + 2) * (TY + 2);
+    const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (id >= (long long)D.ntiles * NS) return;
+    const int tile = (int)(id / NS), sl = (int)(id % NS);
     const Geom &g = D.g;
-    const int nz = g.nz;
+    const int tx = tile % D.tiles_x, ty = tile / D.tiles_x;
+    const int i0 = g.ilo + tx * TX, j0 = g.jlo + ty * TY;
+    const int li = sl % (TX + 2), lj = sl / (TX + 2);
+    const int i = i0 - 1 + li, j = j0 - 1 + lj;
+    const long long m = src_col(g, i, j);
+    int v = (int)(m + 1) << 2;
+    if (m >= 0) {
+        const int mi = (int)(m % g.NX), mj = (int)(m / g.NX);
+        const bool live = live_col(D, mi, mj, m);
+        const bool interior = li >= 1 && li <= TX && lj >= 1 && lj <= TY;
+        if (live) v |= 1;
+        if (live && interior && m == (long long)j * g.NX + i) v |= 2;
+    }
+    maps[id] = v;
+}
+
+// z = M^-1 r on one column of the SIA tridiagonal, in place in smem (slot s), FP32.
+// The column's factors are loaded in one batch first: a load inside the recurrence
+// would cost one memory round trip per level.
+template <int KP, int NS, int NZM>
+__device__ __forceinline__ void sia_col(const MDesc &D, float (*zc)[KP][NS], int s, long long q) {
+    const int nz = D.g.nz;
+    const long long NQ = D.g.NQ;
+    const long long plane = (long long)nz * NQ;
+    for (int c = 0; c < 2; ++c) {
+        float (*z)[NS] = zc[c] + 1;  // level k is row k+1 (rows 0 and nz+1 are zero padding)
+        const float *ib = D.pre + (c * 3 + 0) * plane, *sb = D.pre + (c * 3 + 1) * plane,
+                    *gm = D.pre + (c * 3 + 2) * plane;
+        float fib[NZM], fsb[NZM], fgm[NZM];
+#pragma unroll
+        for (int k = 0; k < NZM; ++k) {
+            const bool in = k < nz;
+            fib[k] = in ? __ldg(ib + (long long)k * NQ + q) : 0.0f;
+            fsb[k] = in ? __ldg(sb + (long long)k * NQ + q) : 0.0f;
+            fgm[k] = in ? __ldg(gm + (long long)k * NQ + q) : 0.0f;
+        }
+        // forward: y_1 = r_1/beta_1; y_k = (r_k - sb_k y_{k-1})/beta_k; back: z_k = y_k - gamma_{k+1} z_{k+1}
+        float prev = z[0][s] * fib[0];
+        z[0][s] = prev;
+#pragma unroll
+        for (int k = 1; k < NZM; ++k) {
+            if (k < nz) {
+                prev = (z[k][s] - fsb[k] * prev) * fib[k];
+                z[k][s] = prev;
+            }
+        }
+        float next = z[nz - 1][s];
+#pragma unroll
+        for (int k = NZM - 2; k >= 0; --k) {
+            if (k < nz - 1) {
+                next = z[k][s] - fgm[k + 1] * next;
+                z[k][s] = next;
+            }
+        }
+    }
+}
+
+// One tile of one solve for the solve's current step; writes the tile's partials.
+template <int NC, int NZM>
+__device__ void tile_step(const MState &S, int tile, int pbuf, MShared<NC, NZM> &sh) {
+    using SH = MShared<NC, NZM>;
+    constexpr int TX = SH::TX, TY = SH::TY, NS = SH::NS, NT = SH::NT, KP = SH::KP;
+    constexpr int OFF = (NC == 27) ? 1 : 0;  // z row of level 0
+    const MDesc &D = sh.D;
+    const Geom &g = D.g;
+    const int nz = (NC == 27) ? g.nz : 1;
     const long long NQ = g.NQ;
     const long long plane = (long long)nz * NQ;
     const int tx = tile % D.tiles_x, ty = tile / D.tiles_x;
-    const int i0 = g.ilo + tx * kTX, j0 = g.jlo + ty * kTY;
+    const int i0 = g.ilo + tx * TX, j0 = g.jlo + ty * TY;
     const int t = threadIdx.x;
     const int step = S.step;
     const int par = S.par;
-    p0 = p1 = p2 = DD{0.0, 0.0};
+    DD p0{0.0, 0.0}, p1{0.0, 0.0}, p2{0.0, 0.0};
+
+    const int *tmap = D.maps + (long long)tile * NS;
+    for (int sl = t; sl < NS; sl += kBlock) sh.map[sl] = tmap[sl];
+    __syncthreads();
 
     if (step == MS_INIT || step == MS_CHECK) {
         // r = b - A64 x (FP64, x read through the halo map); r32 = r on live columns
-        const int ti = t % kTX, tj = t / kTX;
-        const int i = i0 + ti, j = j0 + tj;
-        if (i <= g.ihi && j <= g.jhi) {
+        const double *Auu = D.A64, *Auv = D.A64 + NC * plane, *Avu = D.A64 + 2 * NC * plane,
+                     *Avv = D.A64 + 3 * NC * plane;
+        const double *xu = D.x, *xv = D.x + plane;
+        for (int it = t; it < NT; it += kBlock) {
+            const int ti = it % TX, tj = it / TX;
+            const int i = i0 + ti, j = j0 + tj;
+            if (i > g.ihi || j > g.jhi) continue;
             const long long q = (long long)j * g.NX + i;
+            const int s = (ti + 1) + (TX + 2) * (tj + 1);
             const bool on = D.act[q] != 0;
-            const bool live = live_col(D, i, j, q);
-            const double *Auu = D.A64, *Auv = D.A64 + NC * plane, *Avu = D.A64 + 2 * NC * plane,
-                         *Avv = D.A64 + 3 * NC * plane;
-            const double *xu = D.x, *xv = D.x + plane;
+            const bool live = map_live(sh.map[s]);
+            int nb[9];
+#pragma unroll
+            for (int h = 0; h < 9; ++h) nb[h] = map_src(sh.map[s + (h % 3 - 1) + (TX + 2) * (h / 3 - 1)]);
             for (int k = 0; k < nz; ++k) {
                 const long long e = (long long)k * NQ + q;
                 double yu = 0.0, yv = 0.0;
                 if (on) {
 #pragma unroll
                     for (int c = 0; c < NC; ++c) {
-                        const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
-                        if (k + kA < 0 || k + kA >= nz) continue;
-                        const long long sc = src_col(g, i + iA, j + jA);
-                        if (sc < 0) continue;
+                        const int kA = (NC == 27) ? c / 9 - 1 : 0;
+                        const int sc = nb[c % 9];
+                        if (k + kA < 0 || k + kA >= nz || sc < 0) continue;
                         const long long n = (long long)(k + kA) * NQ + sc;
                         const long long a = (long long)c * plane + e;
                         const double x1 = ldd(xu + n), x2 = ldd(xv + n);
@@ -308,185 +393,247 @@ __device__ void tile_step(const MDesc &D, const MState &S, int tile, MShared<NZM
                         yv = fma(Avv[a], x2, yv);
                     }
                 }
-                const double ru = D.b[e] - yu, rv = D.b[plane + e] - yv;
+                const double bu = D.b[e], bv = D.b[plane + e];
+                const double ru = bu - yu, rv = bv - yv;
                 p1 = dd_add_d(p1, ru * ru + rv * rv);
-                if (step == MS_INIT) p0 = dd_add_d(p0, D.b[e] * D.b[e] + D.b[plane + e] * D.b[plane + e]);
-                else p0 = p1;
+                if (step == MS_INIT) p0 = dd_add_d(p0, bu * bu + bv * bv);
                 D.r[par][e] = live ? (float)ru : 0.0f;
                 D.r[par][plane + e] = live ? (float)rv : 0.0f;
             }
         }
         if (step == MS_CHECK) { p0 = p1; p1 = DD{0.0, 0.0}; }
-        return;
-    }
+    } else {
+        const float alpha = (float)S.alpha, beta = (float)S.beta;
+        const double alpha64 = S.alpha;
+        const bool do_b = (step == MS_MERGED || step == MS_B);
+        const bool do_a = (step == MS_MERGED || step == MS_A);
+        const int rin = par, rout = do_b ? (par ^ 1) : par;  // buffers holding r_i / r_{i+1}
 
-    const float alpha = (float)S.alpha, beta = (float)S.beta;
-    const bool do_b = (step == MS_MERGED || step == MS_B);
-    const bool do_a = (step == MS_MERGED || step == MS_A);
-    const int rin = par, rout = do_b ? (par ^ 1) : par;  // buffers holding r_i / r_{i+1}
-
-    // ---- pass 1: update (B) on the tile, new residual and z on tile + halo ----
-    for (int s = t; s < kSlots; s += blockDim.x) {
-        const int li = s % (kTX + 2), lj = s / (kTX + 2);
-        const int i = i0 - 1 + li, j = j0 - 1 + lj;
-        const bool interior = li >= 1 && li <= kTX && lj >= 1 && lj <= kTY;
-        long long m = src_col(g, i, j);
-        const bool mine = interior && m >= 0 && owned(g, i, j) && m == (long long)j * g.NX + i;
-        bool live = false;
-        if (m >= 0) {
-            const int mi = (int)(m % g.NX), mj = (int)(m / g.NX);
-            live = live_col(D, mi, mj, m);
-        }
-        if (!live) {
-            for (int k = 0; k < nz; ++k) { sh.z[0][k][s] = 0.0f; sh.z[1][k][s] = 0.0f; }
-            if (mine && do_b) {  // keep dead columns at zero
-                for (int k = 0; k < nz; ++k)
-                    for (int c = 0; c < 2; ++c) {
-                        const long long e = c * plane + (long long)k * NQ + m;
-                        D.q[rout][e] = 0.0f;
-                        D.r[rout][e] = 0.0f;
+        // ---- pass 1: update (B) on the tile, new residual (and diag z) on tile + halo ----
+        constexpr int P1 = (2 * NS + kBlock - 1) / kBlock;  // items per thread and level
+        for (int k = 0; k < nz; ++k) {
+#pragma unroll
+            for (int r = 0; r < P1; ++r) {
+                const int it = t + r * kBlock;
+                if (it >= 2 * NS) break;
+                const int c = it / NS, sl = it - c * NS;
+                const int v = sh.map[sl];
+                const int m = map_live(v) ? map_src(v) : -1;
+                float rn = 0.0f;
+                if (m >= 0) {
+                    const long long e = c * plane + (long long)k * NQ + m;
+                    if (do_b) {
+                        const float qo = ldf(D.q[rin] + e), az = ldf(D.Az[rin] + e), ro = ldf(D.r[rin] + e);
+                        const float qn = fmaf(beta, qo, az);  // q_i = Az_i + beta q_{i-1}
+                        rn = fmaf(-alpha, qn, ro);             // r_{i+1} = r_i - alpha q_i
+                        if (map_mine(v)) {
+                            const float dn = fmaf(beta, D.d[e], D.z[e]);  // d_i = z_i + beta d_{i-1}
+                            D.d[e] = dn;
+                            D.q[rout][e] = qn;
+                            D.r[rout][e] = rn;
+                            D.x[e] = fma(alpha64, (double)dn, D.x[e]);  // x += alpha d_i (FP64)
+                        }
+                    } else {
+                        rn = ldf(D.r[rin] + e);
                     }
-            }
-            if (interior && do_a) {
-                const int it = (li - 1) + kTX * (lj - 1);
-                for (int k = 0; k < nz; ++k) { sh.rt[0][k][it] = 0.0f; sh.rt[1][k][it] = 0.0f; }
-            }
-            continue;
-        }
-        for (int c = 0; c < 2; ++c) {
-            for (int k = 0; k < nz; ++k) {
-                const long long e = c * plane + (long long)k * NQ + m;
-                float rn;
-                if (do_b) {
-                    const float qn = fmaf(beta, ldf(D.q[rin] + e), ldf(D.Az[rin] + e));  // q_i = Az_i + beta q_{i-1}
-                    rn = fmaf(-alpha, qn, ldf(D.r[rin] + e));                          // r_{i+1} = r_i - alpha q_i
-                    if (mine) {
-                        const float dn = fmaf(beta, D.d[e], D.z[e]);           // d_i = z_i + beta d_{i-1}
-                        D.d[e] = dn;
-                        D.q[rout][e] = qn;
-                        D.r[rout][e] = rn;
-                        D.x[e] = fma(S.alpha, (double)dn, D.x[e]);            // x += alpha d_i (FP64)
-                    }
-                } else {
-                    rn = ldf(D.r[rin] + e);
                 }
-                sh.z[c][k][s] = rn;
-                if (interior && do_a) sh.rt[c][k][(li - 1) + kTX * (lj - 1)] = rn;
+                if (do_a) {
+                    const int li = sl % (TX + 2), lj = sl / (TX + 2);
+                    if (li >= 1 && li <= TX && lj >= 1 && lj <= TY) sh.rt[c][k][(li - 1) + TX * (lj - 1)] = rn;
+                    float zv = rn;
+                    if (D.precond == 1 && m >= 0) zv = rn * D.pre[c * plane + (long long)k * NQ + m];
+                    sh.z[c][k + OFF][sl] = zv;
+                }
             }
         }
-        if (do_a) precond_col<NZM>(D, sh.z, s, m);
-    }
-    if (!do_a) return;
-    __syncthreads();
+        if (do_a) {
+            if (NC == 27) {  // zero padding rows (levels -1 and nz)
+                for (int it = t; it < 2 * NS; it += kBlock) {
+                    const int c = it / NS, sl = it - c * NS;
+                    sh.z[c][0][sl] = 0.0f;
+                    sh.z[c][nz + 1][sl] = 0.0f;
+                }
+            }
+            __syncthreads();
+            if (NC == 27 && D.precond == 2) {  // column tridiagonal solves on tile + halo
+                for (int sl = t; sl < NS; sl += kBlock) {
+                    const int v = sh.map[sl];
+                    if (map_live(v)) sia_col<KP, NS, NZM>(D, sh.z, sl, map_src(v));
+                }
+                __syncthreads();
+            }
 
-    // ---- pass 2: Az = A z on the tile columns, partial dots ----
-    {
-        const int ti = t % kTX, tj = t / kTX;
-        const int i = i0 + ti, j = j0 + tj;
-        const int s = (ti + 1) + (kTX + 2) * (tj + 1);
-        const int it = ti + kTX * tj;
-        if (t < kTX * kTY && i <= g.ihi && j <= g.jhi) {
-            const long long q = (long long)j * g.NX + i;
-            const bool live = live_col(D, i, j, q);
+            // ---- pass 2: Az = A z on the tile columns, z to HBM, partial dots ----
+            // Couplings that leave the grid are zero in the FP32 copy and the padded z rows
+            // and out-of-grid halo slots are zero, so every column sums all NC terms.
             const float *Auu = D.A32, *Auv = D.A32 + NC * plane, *Avu = D.A32 + 2 * NC * plane,
                         *Avv = D.A32 + 3 * NC * plane;
             float *Azu = D.Az[rout], *Azv = D.Az[rout] + plane;
-            for (int k = 0; k < nz; ++k) {
-                const long long e = (long long)k * NQ + q;
-                float yu = 0.0f, yv = 0.0f;
-                if (live) {
 #pragma unroll
-                    for (int c = 0; c < NC; ++c) {
-                        const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
-                        const int kk = k + kA;
-                        if (kk < 0 || kk >= nz) continue;
-                        const int sn = s + iA + (kTX + 2) * jA;
-                        const float zu = sh.z[0][kk][sn], zv = sh.z[1][kk][sn];
-                        const long long a = (long long)c * plane + e;
-                        yu = fmaf(Auu[a], zu, yu);
-                        yu = fmaf(Auv[a], zv, yu);
-                        yv = fmaf(Avu[a], zu, yv);
-                        yv = fmaf(Avv[a], zv, yv);
+            for (int r = 0; r < NT / kBlock; ++r) {
+                const int it = t + r * kBlock;
+                const int ti = it % TX, tj = it / TX;
+                const int i = i0 + ti, j = j0 + tj;
+                if (i > g.ihi || j > g.jhi) continue;
+                const int s = (ti + 1) + (TX + 2) * (tj + 1);
+                const long long q = (long long)j * g.NX + i;
+                const bool live = map_live(sh.map[s]);
+                for (int k = 0; k < nz; ++k) {
+                    const long long e = (long long)k * NQ + q;
+                    float yu = 0.0f, yv = 0.0f;
+                    if (live) {
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
+                            const int sn = s + iA + (TX + 2) * jA;
+                            const float zu = sh.z[0][k + OFF + kA][sn], zv = sh.z[1][k + OFF + kA][sn];
+                            const long long a = (long long)c * plane + e;
+                            yu = fmaf(__ldg(Auu + a), zu, yu);
+                            yu = fmaf(__ldg(Auv + a), zv, yu);
+                            yv = fmaf(__ldg(Avu + a), zu, yv);
+                            yv = fmaf(__ldg(Avv + a), zv, yv);
+                        }
                     }
+                    Azu[e] = yu;
+                    Azv[e] = yv;
+                    const float zu = sh.z[0][k + OFF][s], zv = sh.z[1][k + OFF][s];
+                    D.z[e] = zu;
+                    D.z[plane + e] = zv;
+                    const double ru = sh.rt[0][k][it], rv = sh.rt[1][k][it];
+                    p0 = dd_add_d(p0, ru * (double)zu + rv * (double)zv);
+                    p1 = dd_add_d(p1, (double)yu * zu + (double)yv * zv);
+                    p2 = dd_add_d(p2, ru * ru + rv * rv);
                 }
-                Azu[e] = yu;
-                Azv[e] = yv;
-                const double zu = sh.z[0][k][s], zv = sh.z[1][k][s];
-                D.z[e] = (float)zu;
-                D.z[plane + e] = (float)zv;
-                const double ru = sh.rt[0][k][it], rv = sh.rt[1][k][it];
-                p0 = dd_add_d(p0, ru * zu + rv * zv);
-                p1 = dd_add_d(p1, (double)yu * zu + (double)yv * zv);
-                p2 = dd_add_d(p2, ru * ru + rv * rv);
             }
         }
+    }
+    block_tree3(p0, p1, p2, sh.red);
+    if (t == 0) {
+        DD *pp = D.partials + ((long long)tile * 2 + pbuf) * 3;
+        pp[0] = p0;
+        pp[1] = p1;
+        pp[2] = p2;
+    }
+    __syncthreads();
+}
+
+// Reduce the partials (buffer pbuf) of every running solve this CTA holds and advance
+// its cached state.  Every CTA holding a solve does this with the same inputs and the
+// same fixed tree, so all copies of a solve's state stay bit-identical.  The CTA holding
+// tile 0 publishes a finished solve and decrements n_active before its next barrier.
+template <int NC, int NZM>
+__device__ void reduce_cached(MShared<NC, NZM> &sh, const MDesc *__restrict__ descs, int pbuf, MState *gstates,
+                              GridBar *bar) {
+    for (int cs = 0; cs < sh.nsolve; ++cs) {
+        if (sh.st[cs].done) continue;
+        const MDesc &D = descs[sh.sid[cs]];
+        const int ntl = D.ntiles;
+        const DD *P = D.partials;
+        DD a0{0.0, 0.0}, a1{0.0, 0.0}, a2{0.0, 0.0};
+        for (int c = threadIdx.x; c < ntl; c += kBlock) {
+            const DD *pp = P + ((long long)c * 2 + pbuf) * 3;
+            DD v0, v1, v2;
+            v0.hi = __ldcg(&pp[0].hi); v0.lo = __ldcg(&pp[0].lo);
+            v1.hi = __ldcg(&pp[1].hi); v1.lo = __ldcg(&pp[1].lo);
+            v2.hi = __ldcg(&pp[2].hi); v2.lo = __ldcg(&pp[2].lo);
+            a0 = dd_add(a0, v0);
+            a1 = dd_add(a1, v1);
+            a2 = dd_add(a2, v2);
+        }
+        block_tree3(a0, a1, a2, sh.red);
+        if (threadIdx.x == 0) {
+            MState &S = sh.st[cs];
+            advance_state(S, D, a0.hi + a0.lo, a1.hi + a1.lo, a2.hi + a2.lo);
+            if (S.done && sh.owner[cs]) {
+                gstates[sh.sid[cs]] = S;
+                __threadfence();
+                atomicSub(&bar->n_active, 1);
+            }
+        }
+        __syncthreads();
     }
 }
 
 template <int NC, int NZM>
-__global__ void __launch_bounds__(kBlock) k_mixed(const MDesc *__restrict__ descs, MState *states,
-                                                  const MTile *__restrict__ tiles, int ntiles, GridBar *bar,
-                                                  int max_steps) {
+__global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ descs, MState *states,
+                                                     const MTile *__restrict__ tiles, int ntiles, GridBar *bar,
+                                                     int max_steps) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    MShared<NZM> &sh = *reinterpret_cast<MShared<NZM> *>(smem_raw);
-    for (int step = 0; step < max_steps; ++step) {
-        if (((volatile GridBar *)bar)->n_active <= 0) break;
+    MShared<NC, NZM> &sh = *reinterpret_cast<MShared<NC, NZM> *>(smem_raw);
+    // cache the states of the solves this CTA holds (round robin over the tile list)
+    if (threadIdx.x == 0) {
+        int n = 0;
         for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
             const MTile T = tiles[w];
-            const MDesc &D = descs[T.solve];
-            MState *Sp = &states[T.solve];
-            const MState S = load_state(Sp);
-            if (S.done || S.step == MS_DONE) continue;
-            DD p0, p1, p2;
-            tile_step<NC, NZM>(D, S, T.tile, sh, p0, p1, p2);
-            DD b0 = block_tree(p0, sh.red);
-            DD b1 = block_tree(p1, sh.red);
-            DD b2 = block_tree(p2, sh.red);
-            if (threadIdx.x == 0) {
-                D.partials[3 * T.tile + 0] = b0;
-                D.partials[3 * T.tile + 1] = b1;
-                D.partials[3 * T.tile + 2] = b2;
-                __threadfence();
-                const unsigned tk = atomicAdd(&Sp->ticket, 1u);
-                sh.last = (tk == (unsigned)D.ntiles - 1);
+            int u = 0;
+            while (u < n && sh.sid[u] != T.solve) ++u;
+            if (u == n && n < kMaxCtaSolves) {
+                sh.sid[n] = T.solve;
+                sh.owner[n] = 0;
+                const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&states[T.solve]);
+                unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sh.st[n]);
+                for (int w8 = 0; w8 < (int)(sizeof(MState) / 8); ++w8) dst[w8] = __ldcg(src + w8);
+                ++n;
             }
-            __syncthreads();
-            if (sh.last) {
-                __threadfence();
-                DD a0{0.0, 0.0}, a1{0.0, 0.0}, a2{0.0, 0.0};
-                for (int c = threadIdx.x; c < D.ntiles; c += kBlock) {
-                    DD v0, v1, v2;
-                    v0.hi = __ldcg(&D.partials[3 * c].hi); v0.lo = __ldcg(&D.partials[3 * c].lo);
-                    v1.hi = __ldcg(&D.partials[3 * c + 1].hi); v1.lo = __ldcg(&D.partials[3 * c + 1].lo);
-                    v2.hi = __ldcg(&D.partials[3 * c + 2].hi); v2.lo = __ldcg(&D.partials[3 * c + 2].lo);
-                    a0 = dd_add(a0, v0);
-                    a1 = dd_add(a1, v1);
-                    a2 = dd_add(a2, v2);
-                }
-                DD r0 = block_tree(a0, sh.red);
-                DD r1 = block_tree(a1, sh.red);
-                DD r2 = block_tree(a2, sh.red);
+            if (u < n && T.tile == 0) sh.owner[u] = 1;
+        }
+        sh.nsolve = n;
+        sh.cur = -1;
+    }
+    __syncthreads();
+    bool finished = false;
+    int step = 0;
+    for (; step < max_steps; ++step) {
+        const int pbuf = step & 1;
+        if (step > 0) reduce_cached<NC, NZM>(sh, descs, pbuf ^ 1, states, bar);  // previous step's sums
+        for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
+            const MTile T = tiles[w];
+            int cs = 0;
+            while (cs < sh.nsolve && sh.sid[cs] != T.solve) ++cs;
+            if (cs >= sh.nsolve || sh.st[cs].done) continue;
+            if (sh.cur != cs) {
+                __syncthreads();
                 if (threadIdx.x == 0) {
-                    MState NS = load_state(Sp);
-                    NS.ticket = 0u;
-                    advance_state(NS, D, r0.hi + r0.lo, r1.hi + r1.lo, r2.hi + r2.lo);
-                    *Sp = NS;
-                    if (NS.done) atomicSub(&bar->n_active, 1);
-                    __threadfence();
+                    sh.D = descs[T.solve];
+                    sh.cur = cs;
                 }
+                __syncthreads();
             }
-            __syncthreads();
+            tile_step<NC, NZM>(sh.st[cs], T.tile, pbuf, sh);
         }
         if (!grid_barrier(bar, gridDim.x)) return;
+        if (((volatile GridBar *)bar)->n_active <= 0) {
+            finished = true;
+            break;
+        }
     }
+    // out of steps: fold in the last step's sums so that the next launch resumes exactly
+    if (!finished && step > 0) reduce_cached<NC, NZM>(sh, descs, (step - 1) & 1, states, bar);
+    if (threadIdx.x == 0)
+        for (int cs = 0; cs < sh.nsolve; ++cs)
+            if (sh.owner[cs]) states[sh.sid[cs]] = sh.st[cs];
 }
 
 // ---------------------------------------------------------------------------
 // setup kernels: FP32 matrix copy and FP32 preconditioner factors
 // ---------------------------------------------------------------------------
-__global__ void k_to_f32(const double *__restrict__ src, float *__restrict__ dst, long long n) {
-    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
-        dst[e] = (float)src[e];
+// FP32 copy of the coefficient planes; couplings whose neighbour lies outside the
+// array (which the reference skips) are stored as zero so the FP32 stencil loop needs
+// no bounds tests.
+template <int NC>
+__global__ void k_to_f32(Geom g, const double *__restrict__ src, float *__restrict__ dst) {
+    const long long plane = (long long)g.nz * g.NQ;
+    const long long n = 4LL * NC * plane;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)((e / plane) % NC);
+        const long long r = e % plane;
+        const int k = (int)(r / g.NQ);
+        const long long q = r % g.NQ;
+        const int i = (int)(q % g.NX), j = (int)(q / g.NX);
+        const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
+        const bool in = i + iA >= 0 && i + iA < g.NX && j + jA >= 0 && j + jA < g.NY && k + kA >= 0 && k + kA < g.nz;
+        dst[e] = in ? (float)src[e] : 0.0f;
+    }
 }
 
 // diag: inverse of the diagonal coefficient (0 where the diagonal is 0), per component
@@ -528,8 +675,12 @@ __global__ void k_mixed_precond_setup(Geom g, int precond, const double *__restr
 // Device buffers of the mixed solver for one system (owned by the host Solver).
 struct MixedBufs {
     bool valid = false;
+    bool stale = false;        // the FP64 matrix changed since the FP32 copy was made
+    long long shape_nvec = 0;
+    int shape_nc = 0;
     int precond = -1;
     float *A32 = nullptr, *pre = nullptr, *vec = nullptr;
+    int *maps = nullptr;
     DD *partials = nullptr;
     MState *state = nullptr;
     MDesc *desc = nullptr;
@@ -539,9 +690,10 @@ struct MixedBufs {
     int ntiles = 0;
     void release() {
         for (void *p : {(void *)A32, (void *)pre, (void *)vec, (void *)partials, (void *)state, (void *)desc,
-                        (void *)tiles, (void *)bar})
+                        (void *)tiles, (void *)bar, (void *)maps})
             if (p) cudaFree(p);
         A32 = pre = vec = nullptr;
+        maps = nullptr;
         partials = nullptr;
         state = nullptr;
         desc = nullptr;
