@@ -67,6 +67,7 @@ def run_profile(args):
     import cism_b200 as cg
     from cism_b200 import build
     build.build()
+    torch.zeros(1, device="cuda")  # CUDA context up before any timing
     P = make_problem(args.workload)
     S = cg.DeviceSolver(P)
     pc = PROFILE_PRECOND[args.workload]

@@ -9,7 +9,9 @@
 // Solver (the Picard loop calls them repeatedly with the same sizes).
 #include <cstdio>
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -21,6 +23,21 @@
 namespace cismgpu {
 
 static thread_local std::string g_last_error;
+
+// CISMGPU_TRACE=1: host-side phase timestamps on stderr (diagnostics only).
+static bool trace_on() {
+    static const bool on = [] {
+        const char *e = std::getenv("CISMGPU_TRACE");
+        return e && e[0] == '1';
+    }();
+    return on;
+}
+static void trace(const char *what) {
+    if (!trace_on()) return;
+    static auto t0 = std::chrono::steady_clock::now();
+    const double us = std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+    std::fprintf(stderr, "[cismgpu %12.1f us] %s\n", us, what);
+}
 
 static int fail(int code, const std::string &msg) {
     g_last_error = msg;
@@ -104,6 +121,7 @@ struct Solver {
     double prof_ms = 0.0;
     int prof_n = 0;
     double prof_bytes = 0.0;
+    int last_ty = 0;  // tile height of the last mixed solve
 
     ~Solver() { destroy(); }
 
@@ -288,8 +306,10 @@ struct Solver {
     }
 
     int finish_solve(double *err, int *niters) {
+        trace("finish_solve: begin");
         CU(cudaMemcpyAsync(h_state, state.p, sizeof(SolveState), cudaMemcpyDeviceToHost, stream));
         CU(cudaStreamSynchronize(stream));
+        trace("finish_solve: synchronized");
         TRY(collect_profile());
         *err = h_state->err;
         *niters = h_state->niters;
@@ -425,80 +445,11 @@ __global__ void k_mstate_to_solve(const MState *ms, SolveState *st, const GridBa
     st->done = 1;
 }
 
-static int mixed_nzm(const Geom &g, bool is3d) { return !is3d ? 1 : (g.nz <= 16 ? 16 : 32); }
-
-static MDesc mixed_desc(const Solver &sv, int precond);
-
-template <int NC>
-static int mixed_build_maps(Solver &sv) {
-    constexpr int TX = TileShape<NC>::TX, TY = TileShape<NC>::TY;
-    const MDesc D = mixed_desc(sv, sv.mixed.precond < 0 ? 0 : sv.mixed.precond);
-    const long long n = (long long)D.ntiles * (TX + 2) * (TY + 2);
-    k_slot_maps<TX, TY><<<nblocks(n), kBlock, 0, sv.stream>>>(D, sv.mixed.maps);
-    k_to_f32<NC><<<1184, kBlock, 0, sv.stream>>>(sv.g, sv.A.as<double>(), sv.mixed.A32);
-    CU(cudaGetLastError());
-    return CISMGPU_OK;
+static int tiles_for(const Geom &g, int TY) {
+    return ((g.ihi - g.ilo + kTX) / kTX) * ((g.jhi - g.jlo + TY) / TY);
 }
 
-// Allocate and fill the FP32 copy of the matrix, the tile slot maps and the
-// preconditioner factors.
-static int mixed_prepare(Solver &sv, int precond) {
-    if (sv.g.nz > kMixedMaxNz) return fail(CISMGPU_EUNSUPPORTED, "mixed solver supports nz <= 32");
-    if (!(precond == 0 || precond == 1 || (precond == 2 && sv.is3d)))
-        return fail(CISMGPU_EUNSUPPORTED, "mixed solver preconditioners: 0, 1, or 2 (3D only)");
-    MixedBufs &m = sv.mixed;
-    const long long nvec = sv.nvec;
-    const int NC = sv.NC;
-    const Geom &g = sv.g;
-    const int TX = NC == 27 ? TileShape<27>::TX : TileShape<9>::TX, TY = NC == 27 ? TileShape<27>::TY : TileShape<9>::TY;
-    const int tiles_x = (g.ihi - g.ilo + TX) / TX, tiles_y = (g.jhi - g.jlo + TY) / TY;
-    const int ntiles = tiles_x * tiles_y;
-    const bool same_shape = m.valid && m.shape_nvec == nvec && m.shape_nc == NC && m.ntiles == ntiles;
-    if (!same_shape) {
-        m.release();
-        size_t bytes = 0;
-        auto alloc = [&](void **p, size_t n) -> cudaError_t {
-            bytes += n;
-            return cudaMalloc(p, n);
-        };
-        CU(alloc((void **)&m.A32, (size_t)4 * NC * nvec * sizeof(float)));
-        CU(alloc((void **)&m.pre, (size_t)6 * nvec * sizeof(float)));
-        CU(alloc((void **)&m.vec, (size_t)16 * nvec * sizeof(float)));
-        CU(alloc((void **)&m.partials, (size_t)ntiles * 2 * 3 * sizeof(DD)));
-        CU(alloc((void **)&m.maps, (size_t)ntiles * (TX + 2) * (TY + 2) * sizeof(int)));
-        CU(alloc((void **)&m.state, sizeof(MState)));
-        CU(alloc((void **)&m.desc, sizeof(MDesc)));
-        CU(alloc((void **)&m.tiles, (size_t)ntiles * sizeof(MTile)));
-        CU(alloc((void **)&m.bar, sizeof(GridBar)));
-        m.nbytes = bytes;
-        m.ntiles = ntiles;
-        m.shape_nvec = nvec;
-        m.shape_nc = NC;
-        std::vector<MTile> tl(ntiles);
-        for (int t = 0; t < ntiles; ++t) tl[t] = MTile{0, t};
-        CU(cudaMemcpyAsync(m.tiles, tl.data(), ntiles * sizeof(MTile), cudaMemcpyHostToDevice, sv.stream));
-        CU(cudaStreamSynchronize(sv.stream));  // tl goes out of scope
-        m.valid = true;
-        m.stale = true;
-    }
-    if (m.stale) {  // new matrix or active mask: FP32 copy and slot maps
-        if (NC == 27) TRY(mixed_build_maps<27>(sv));
-        else TRY(mixed_build_maps<9>(sv));
-        m.stale = false;
-        m.precond = -1;
-    }
-    if (m.precond != precond) {
-        if (NC == 27)
-            k_mixed_precond_setup<27><<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, precond, sv.A.as<double>(), m.pre);
-        else
-            k_mixed_precond_setup<9><<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, precond, sv.A.as<double>(), m.pre);
-        CU(cudaGetLastError());
-        m.precond = precond;
-    }
-    return CISMGPU_OK;
-}
-
-static MDesc mixed_desc(const Solver &sv, int precond) {
+static MDesc mixed_desc(const Solver &sv, int precond, int TY) {
     const MixedBufs &m = sv.mixed;
     const long long nvec = sv.nvec;
     const Ptrs p = sv.ptrs();
@@ -506,9 +457,7 @@ static MDesc mixed_desc(const Solver &sv, int precond) {
     D.g = sv.g;
     D.NC = sv.NC;
     D.precond = precond;
-    const int TX = sv.NC == 27 ? TileShape<27>::TX : TileShape<9>::TX;
-    const int TY = sv.NC == 27 ? TileShape<27>::TY : TileShape<9>::TY;
-    D.tiles_x = (sv.g.ihi - sv.g.ilo + TX) / TX;
+    D.tiles_x = (sv.g.ihi - sv.g.ilo + kTX) / kTX;
     D.tiles_y = (sv.g.jhi - sv.g.jlo + TY) / TY;
     D.ntiles = D.tiles_x * D.tiles_y;
     D.A32 = m.A32;
@@ -529,6 +478,141 @@ static MDesc mixed_desc(const Solver &sv, int precond) {
     return D;
 }
 
+// Shared memory of the mixed kernel for a tile height (resident: 2D launches with one tile
+// per CTA keep the tile's FP32 matrix in shared memory).
+static size_t mixed_smem(bool is3d, int nzm, int TY, bool resident = false) {
+    if (!is3d) return MLayout<9, 1>(TY, resident).bytes();
+    if (nzm == 16) return MLayout<27, 16>(TY, false).bytes();
+    return MLayout<27, 32>(TY, false).bytes();
+}
+
+static int mixed_nzm(const Geom &g, bool is3d) { return !is3d ? 1 : (g.nz <= 16 ? 16 : 32); }
+
+static const void *mixed_kernel(bool is3d, int nzm) {
+    if (!is3d) return (const void *)k_mixed<9, 1>;
+    if (nzm == 16) return (const void *)k_mixed<27, 16>;
+    return (const void *)k_mixed<27, 32>;
+}
+
+// Co-resident CTAs of the mixed kernel at tile height TY (0 if it does not fit).
+static int mixed_grid(bool is3d, int nzm, int TY, bool resident = false) {
+    const size_t smem = mixed_smem(is3d, nzm, TY, resident);
+    if (smem > 227 * 1024 - 64) return 0;
+    const void *k = mixed_kernel(is3d, nzm);
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    int dev = 0, nsm = 0, occ = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kBlock, smem) != cudaSuccess) return 0;
+    return nsm * occ;
+}
+
+// Tile autotuner: the smallest tile height whose tiles (summed over the batch) fit in
+// the co-resident CTAs, so every CTA holds at most one tile per solve step; if no
+// height fits (large batches), 16 rows (8 for nz > 16), the best load balance measured
+// for streaming-bound batches.
+static int mixed_choose_ty(const std::vector<const Geom *> &gs, bool is3d, int nzm, bool *resident) {
+    *resident = false;
+    if (!is3d) {  // 2D: first try one tile per CTA with the tile's matrix resident in shared memory
+        for (int TY = 1; TY <= kMaxTY; ++TY) {
+            const int G = mixed_grid(is3d, nzm, TY, true);
+            if (G == 0) break;
+            long long nt = 0;
+            for (const Geom *g : gs) nt += tiles_for(*g, TY);
+            if (nt <= G) {
+                *resident = true;
+                return TY;
+            }
+        }
+    }
+    for (int TY = 1; TY <= kMaxTY; ++TY) {
+        const int G = mixed_grid(is3d, nzm, TY);
+        if (G == 0) break;
+        long long nt = 0;
+        for (const Geom *g : gs) nt += tiles_for(*g, TY);
+        if (nt <= G) return TY;
+    }
+    int TY = (nzm == 32) ? 8 : 16;
+    while (TY > 1 && mixed_grid(is3d, nzm, TY) == 0) --TY;
+    return TY;
+}
+
+// Allocate and fill the FP32 copy of the matrix, the preconditioner factors and, for tile
+// height TY, the tile slot maps and partial sums.
+static int mixed_prepare(Solver &sv, int precond, int TY) {
+    if (sv.g.nz > kMixedMaxNz) return fail(CISMGPU_EUNSUPPORTED, "mixed solver supports nz <= 32");
+    if (!(precond == 0 || precond == 1 || (precond == 2 && sv.is3d)))
+        return fail(CISMGPU_EUNSUPPORTED, "mixed solver preconditioners: 0, 1, or 2 (3D only)");
+    MixedBufs &m = sv.mixed;
+    const long long nvec = sv.nvec;
+    const int NC = sv.NC;
+    const Geom &g = sv.g;
+    if (!(m.valid && m.shape_nvec == nvec && m.shape_nc == NC)) {
+        m.release();
+        size_t bytes = 0;
+        auto alloc = [&](void **p, size_t n) -> cudaError_t {
+            bytes += n;
+            return cudaMalloc(p, n);
+        };
+        CU(alloc((void **)&m.A32, (size_t)4 * NC * nvec * sizeof(float)));
+        CU(alloc((void **)&m.pre, (size_t)6 * nvec * sizeof(float)));
+        CU(alloc((void **)&m.vec, (size_t)16 * nvec * sizeof(float)));
+        CU(alloc((void **)&m.state, sizeof(MState)));
+        CU(alloc((void **)&m.desc, sizeof(MDesc)));
+        CU(alloc((void **)&m.bar, sizeof(GridBar)));
+        m.nbytes = bytes;
+        m.shape_nvec = nvec;
+        m.shape_nc = NC;
+        m.valid = true;
+        m.stale = true;
+        m.TY = 0;
+        m.ntiles = 0;
+    }
+    if (m.stale) {  // new matrix: FP32 copy (couplings leaving the grid set to zero)
+        if (NC == 27) k_to_f32<27><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32);
+        else k_to_f32<9><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32);
+        CU(cudaGetLastError());
+        m.stale = false;
+        m.precond = -1;
+        m.TY = 0;  // the active mask may have changed: rebuild the slot maps
+    }
+    if (m.TY != TY) {
+        const int ntiles = tiles_for(g, TY);
+        const int NS = (kTX + 2) * (TY + 2);
+        if (ntiles > m.ntiles_cap || (long long)ntiles * NS > m.maps_cap) {
+            if (m.partials) cudaFree(m.partials);
+            if (m.maps) cudaFree(m.maps);
+            if (m.tiles) cudaFree(m.tiles);
+            m.partials = nullptr;
+            m.maps = nullptr;
+            m.tiles = nullptr;
+            CU(cudaMalloc((void **)&m.partials, (size_t)ntiles * 2 * 3 * sizeof(DD)));
+            CU(cudaMalloc((void **)&m.maps, (size_t)ntiles * NS * sizeof(int)));
+            CU(cudaMalloc((void **)&m.tiles, (size_t)ntiles * sizeof(MTile)));
+            m.ntiles_cap = ntiles;
+            m.maps_cap = (long long)ntiles * NS;
+        }
+        m.ntiles = ntiles;
+        const MDesc D = mixed_desc(sv, precond, TY);
+        k_slot_maps<<<nblocks((long long)ntiles * NS), kBlock, 0, sv.stream>>>(D, TY, m.maps);
+        CU(cudaGetLastError());
+        std::vector<MTile> tl(ntiles);
+        for (int t = 0; t < ntiles; ++t) tl[t] = MTile{0, t};
+        CU(cudaMemcpyAsync(m.tiles, tl.data(), ntiles * sizeof(MTile), cudaMemcpyHostToDevice, sv.stream));
+        CU(cudaStreamSynchronize(sv.stream));  // tl goes out of scope
+        m.TY = TY;
+    }
+    if (m.precond != precond) {
+        if (NC == 27)
+            k_mixed_precond_setup<27><<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, precond, sv.A.as<double>(), m.pre);
+        else
+            k_mixed_precond_setup<9><<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, precond, sv.A.as<double>(), m.pre);
+        CU(cudaGetLastError());
+        m.precond = precond;
+    }
+    return CISMGPU_OK;
+}
+
 static MState mixed_init_state(double tol, int maxiters, int ncheck) {
     MState S;
     std::memset(&S, 0, sizeof(S));
@@ -541,7 +625,6 @@ static MState mixed_init_state(double tol, int maxiters, int ncheck) {
     return S;
 }
 
-// x = x0 and all FP32 recurrence vectors = 0 (the reference zeroes its work vectors, :3048-3061)
 // The reference starts with halo(x) (:3094-3097) and, with inactive halo vertices and the
 // diagonal or SIA preconditioner, never changes x there again; the mixed kernel writes
 // only owned unknowns, so x leaves with the same halo values.
@@ -555,20 +638,13 @@ static int mixed_reset(Solver &sv, cudaStream_t s) {
 }
 
 template <int NC, int NZM>
-static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_tiles, int ntiles, GridBar *d_bar,
-                        int max_steps, cudaStream_t s, const std::vector<MTile> *host_tiles) {
-    const size_t smem = sizeof(MShared<NC, NZM>);
-    static bool attr_set = false;
-    if (!attr_set) {
-        CU(cudaFuncSetAttribute(k_mixed<NC, NZM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        attr_set = true;
-    }
-    int dev = 0, nsm = 0, occ = 0;
-    CU(cudaGetDevice(&dev));
-    CU(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mixed<NC, NZM>, kBlock, smem));
-    if (occ < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM");
-    int grid = nsm * occ;
+static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_tiles, int ntiles, int TY,
+                        int resident, GridBar *d_bar, int max_steps, cudaStream_t s,
+                        const std::vector<MTile> *host_tiles) {
+    const size_t smem = MLayout<NC, NZM>(TY, resident != 0).bytes();
+    int grid = mixed_grid(NC == 27, NZM, TY, resident != 0);
+    if (grid < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM at this tile height");
+    if (resident && grid < ntiles) return fail(CISMGPU_EUNSUPPORTED, "resident launch needs one tile per CTA");
     if (grid > ntiles) grid = ntiles;
     if (host_tiles) {  // each CTA caches the state of at most kMaxCtaSolves solves
         for (int b = 0; b < grid; ++b) {
@@ -581,17 +657,19 @@ static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_t
                 return fail(CISMGPU_EUNSUPPORTED, "batch too fragmented for one launch (solves per CTA > 32)");
         }
     }
-    void *args[] = {(void *)&d_descs, (void *)&d_states, (void *)&d_tiles, (void *)&ntiles, (void *)&d_bar,
-                    (void *)&max_steps};
+    void *args[] = {(void *)&d_descs, (void *)&d_states, (void *)&d_tiles, (void *)&ntiles, (void *)&TY,
+                    (void *)&resident, (void *)&d_bar, (void *)&max_steps};
     CU(cudaLaunchCooperativeKernel((const void *)k_mixed<NC, NZM>, dim3(grid), dim3(kBlock), args, smem, s));
     return CISMGPU_OK;
 }
 
-static int mixed_dispatch(bool is3d, int nzm, const MDesc *d, MState *st, const MTile *t, int nt, GridBar *bar,
-                          int max_steps, cudaStream_t s, const std::vector<MTile> *host_tiles = nullptr) {
-    if (!is3d) return mixed_launch<9, 1>(d, st, t, nt, bar, max_steps, s, host_tiles);
-    if (nzm == 16) return mixed_launch<27, 16>(d, st, t, nt, bar, max_steps, s, host_tiles);
-    return mixed_launch<27, 32>(d, st, t, nt, bar, max_steps, s, host_tiles);
+static int mixed_dispatch(bool is3d, int nzm, const MDesc *d, MState *st, const MTile *t, int nt, int TY,
+                          bool resident, GridBar *bar, int max_steps, cudaStream_t s,
+                          const std::vector<MTile> *host_tiles = nullptr) {
+    const int res = resident ? 1 : 0;
+    if (!is3d) return mixed_launch<9, 1>(d, st, t, nt, TY, res, bar, max_steps, s, host_tiles);
+    if (nzm == 16) return mixed_launch<27, 16>(d, st, t, nt, TY, 0, bar, max_steps, s, host_tiles);
+    return mixed_launch<27, 32>(d, st, t, nt, TY, 0, bar, max_steps, s, host_tiles);
 }
 
 static double mixed_iter_bytes(const Solver &sv, int precond) {
@@ -605,10 +683,17 @@ static double mixed_check_bytes(const Solver &sv) {
 
 template <int NCC>
 int Solver::run_mixed(int precond, int ncheck, double tol, int maxiters) {
-    TRY(mixed_prepare(*this, precond));
+    trace("run_mixed: begin");
+    const int nzm = mixed_nzm(g, is3d);
+    bool resident = false;
+    const int TY = mixed_choose_ty({&g}, is3d, nzm, &resident);
+    trace("run_mixed: tile height chosen");
+    TRY(mixed_prepare(*this, precond, TY));
+    trace("run_mixed: prepared");
     TRY(mixed_reset(*this, stream));
+    trace("run_mixed: reset enqueued");
     MixedBufs &m = mixed;
-    const MDesc D = mixed_desc(*this, precond);
+    const MDesc D = mixed_desc(*this, precond, TY);
     const MState S0 = mixed_init_state(tol, maxiters, ncheck);
     GridBar B{0u, 0u, 0, 1};
     CU(cudaMemcpyAsync(m.desc, &D, sizeof(MDesc), cudaMemcpyHostToDevice, stream));
@@ -621,10 +706,13 @@ int Solver::run_mixed(int precond, int ncheck, double tol, int maxiters) {
         CU(cudaEventCreate(&e1));
         CU(cudaEventRecord(e0, stream));
     }
-    TRY(mixed_dispatch(is3d, mixed_nzm(g, is3d), m.desc, m.state, m.tiles, m.ntiles, m.bar, max_steps, stream));
+    trace("run_mixed: descriptors copied");
+    TRY(mixed_dispatch(is3d, nzm, m.desc, m.state, m.tiles, m.ntiles, TY, resident, m.bar, max_steps, stream));
+    trace("run_mixed: kernel launched");
     if (prof) CU(cudaEventRecord(e1, stream));
     k_mstate_to_solve<<<1, 1, 0, stream>>>(m.state, state.as<SolveState>(), m.bar);
     CU(cudaGetLastError());
+    last_ty = TY;
     if (prof) {
         MState hs;
         CU(cudaMemcpyAsync(&hs, m.state, sizeof(MState), cudaMemcpyDeviceToHost, stream));
@@ -858,6 +946,7 @@ int cismgpu_solver_solve(cismgpu_solver_t *h, int algorithm, int precond, int li
     g_last_error.clear();
     if (!h || !err || !niters) return fail(CISMGPU_EINVAL, "null argument");
     std::lock_guard<std::mutex> lk(h->mu);
+    trace("solver_solve: begin");
     TRY(validate_solve_args(precond, linear_solve_ncheck, maxiters));
     Solver &sv = h->sv;
     TRY(sv.begin_solve());
@@ -887,11 +976,18 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
     }
     Solver &s0 = solvers[0]->sv;
     const int nzm = mixed_nzm(s0.g, s0.is3d);
+    std::vector<const Geom *> geoms;
     for (int t = 0; t < n; ++t) {
         Solver &sv = solvers[t]->sv;
         if (sv.is3d != s0.is3d || mixed_nzm(sv.g, sv.is3d) != nzm)
             return fail(CISMGPU_EINVAL, "batch members must share dims and the nz class (<=16 or <=32)");
-        TRY(mixed_prepare(sv, precond));
+        geoms.push_back(&sv.g);
+    }
+    bool resident = false;
+    const int TY = mixed_choose_ty(geoms, s0.is3d, nzm, &resident);
+    for (int t = 0; t < n; ++t) {
+        Solver &sv = solvers[t]->sv;
+        TRY(mixed_prepare(sv, precond, TY));
         TRY(mixed_reset(sv, sv.stream));
     }
     for (int t = 0; t < n; ++t) CU(cudaStreamSynchronize(solvers[t]->sv.stream));
@@ -901,7 +997,7 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
     std::vector<MState> states(n, mixed_init_state(tolerance, maxiters, linear_solve_ncheck));
     std::vector<MTile> tiles;
     for (int t = 0; t < n; ++t) {
-        descs[t] = mixed_desc(solvers[t]->sv, precond);
+        descs[t] = mixed_desc(solvers[t]->sv, precond, TY);
         for (int k = 0; k < descs[t].ntiles; ++k) tiles.push_back(MTile{t, k});
     }
     // tiles in (solve, tile) order; CTAs take them round robin, so a solve's tiles spread over
@@ -921,8 +1017,8 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
     CU(cudaMemcpyAsync(d_states, states.data(), n * sizeof(MState), cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(MTile), cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(d_bar, &B, sizeof(GridBar), cudaMemcpyHostToDevice, s));
-    int rc = mixed_dispatch(s0.is3d, nzm, d_descs, d_states, d_tiles, (int)tiles.size(), d_bar, 4 * maxiters + 16, s,
-                            &tiles);
+    int rc = mixed_dispatch(s0.is3d, nzm, d_descs, d_states, d_tiles, (int)tiles.size(), TY, resident, d_bar,
+                            4 * maxiters + 16, s, &tiles);
     if (rc) {
         cudaFreeAsync(dmem, s);
         return rc;

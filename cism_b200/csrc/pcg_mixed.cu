@@ -48,7 +48,7 @@ struct MDesc {
     float *r[2], *q[2], *Az[2];  // [2][nz][NQ] each (u, v planes)
     float *z, *d;                // [2][nz][NQ]
     DD *partials;        // [ntiles][2 step parities][3]
-    const int *maps;     // [ntiles][(TX+2)*(TY+2)] slot maps (k_slot_maps)
+    const int *maps;     // [ntiles][(kTX+2)*(TY+2)] slot maps (k_slot_maps)
 };
 
 struct MState {
@@ -213,29 +213,41 @@ __device__ void advance_state(MState &S, const MDesc &D, double S0, double S1, d
 // ---------------------------------------------------------------------------
 // tile work
 // ---------------------------------------------------------------------------
-// Tile shapes: one CTA of 256 threads per tile.  2D: 64 x 16 columns (4 per thread);
-// 3D: 32 x 8 columns with nz levels each.
-template <int NC> struct TileShape;
-template <> struct TileShape<9> { static constexpr int TX = 64, TY = 16; };
-template <> struct TileShape<27> { static constexpr int TX = 32, TY = 8; };
-
+// Tiles are kTX columns wide (one warp per tile row: coalesced 128-byte FP32 rows) and
+// TY rows high; TY is chosen per launch by the host (mixed_choose_ty) so that a solve has
+// no more tiles than there are co-resident CTAs.
+constexpr int kTX = 32;
 constexpr int kMaxCtaSolves = 32;  // distinct solves whose tiles one CTA may hold in a launch
+constexpr int kMaxTY = 64;
 
-template <int NC, int NZM>
-struct MShared {
-    static constexpr int TX = TileShape<NC>::TX, TY = TileShape<NC>::TY;
-    static constexpr int NS = (TX + 2) * (TY + 2), NT = TX * TY;
-    static constexpr int KP = (NC == 27) ? NZM + 2 : 1;  // z levels with a zero row above and below
-    float z[2][KP][NS];        // preconditioned residual on tile + halo
-    float rt[2][NZM][NT];      // new residual on the tile columns
-    int map[NS];               // slot map of the current tile (k_slot_maps)
+struct MHead {
     MDesc D;                   // descriptor of the current tile's solve
     MState st[kMaxCtaSolves];  // this CTA's copy of the state of every solve it holds
     int sid[kMaxCtaSolves];    // solve index of each cached state
     int owner[kMaxCtaSolves];  // 1 if this CTA holds tile 0 of the solve (reports it)
     int nsolve;
     int cur;                   // cache slot described by D
-    DD red[8][3];
+    double red[8][3];
+};
+
+// Dynamic shared memory: head | map[NS] | z[2][KP][NS] | rt[2][NZM][NT] | stage[kStage] DD
+//                        | (resident launches) A[4][NC][NT] FP32 matrix of the CTA's tile
+constexpr int kStage = 2 * kBlock;  // tile partials staged for the cross-tile sum (per field chunk)
+
+template <int NC, int NZM>
+struct MLayout {
+    static constexpr int KP = (NC == 27) ? NZM + 2 : 1;  // z levels with a zero row above and below
+    int NS, NT;
+    bool resA;
+    __host__ __device__ MLayout(int TY, bool resident) : NS((kTX + 2) * (TY + 2)), NT(kTX * TY), resA(resident) {}
+    __host__ __device__ size_t off_map() const { return (sizeof(MHead) + 15) / 16 * 16; }
+    __host__ __device__ size_t off_z() const { return (off_map() + 4 * (size_t)NS + 15) / 16 * 16; }
+    __host__ __device__ size_t off_rt() const { return off_z() + 4 * (size_t)2 * KP * NS; }
+    __host__ __device__ size_t off_stage() const { return (off_rt() + 4 * (size_t)2 * NZM * NT + 15) / 16 * 16; }
+    __host__ __device__ size_t off_A() const { return off_stage() + sizeof(DD) * kStage; }
+    __host__ __device__ size_t bytes() const {
+        return off_A() + (resA ? 4 * (size_t)4 * NC * NZM * NT : 0);
+    }
 };
 
 // Loads of data that other CTAs wrote earlier in the same launch go through L2
@@ -243,27 +255,23 @@ struct MShared {
 __device__ __forceinline__ float ldf(const float *p) { return __ldcg(p); }
 __device__ __forceinline__ double ldd(const double *p) { return __ldcg(p); }
 
-// Block tree over 256 threads for three dd fields at once; result in thread 0.
-__device__ __forceinline__ void block_tree3(DD &a, DD &b, DD &c, DD (*sm)[3]) {
+// Sum of three doubles over the 256 threads in a fixed order (warp shuffle tree, then the
+// 8 warp sums in order); result in thread 0.
+__device__ __forceinline__ void block_sum3(double &a, double &b, double &c, double (*sm)[3]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) {
-        DD oa = dd_shfl_down(a, off), ob = dd_shfl_down(b, off), oc = dd_shfl_down(c, off);
-        if (lane + off < 32) { a = dd_add(a, oa); b = dd_add(b, ob); c = dd_add(c, oc); }
+        a += __shfl_down_sync(0xffffffffu, a, off);
+        b += __shfl_down_sync(0xffffffffu, b, off);
+        c += __shfl_down_sync(0xffffffffu, c, off);
     }
     __syncthreads();
     if (lane == 0) { sm[warp][0] = a; sm[warp][1] = b; sm[warp][2] = c; }
     __syncthreads();
-    if (warp == 0) {
-        const DD z0{0.0, 0.0};
-        a = lane < 8 ? sm[lane][0] : z0;
-        b = lane < 8 ? sm[lane][1] : z0;
-        c = lane < 8 ? sm[lane][2] : z0;
+    if (threadIdx.x == 0) {
+        a = sm[0][0]; b = sm[0][1]; c = sm[0][2];
 #pragma unroll
-        for (int off = 4; off >= 1; off >>= 1) {
-            DD oa = dd_shfl_down(a, off), ob = dd_shfl_down(b, off), oc = dd_shfl_down(c, off);
-            if (lane + off < 32) { a = dd_add(a, oa); b = dd_add(b, ob); c = dd_add(c, oc); }
-        }
+        for (int w = 1; w < kBlock / 32; ++w) { a += sm[w][0]; b += sm[w][1]; c += sm[w][2]; }
     }
 }
 
@@ -273,39 +281,39 @@ __device__ __forceinline__ int map_src(int v) { return (v >> 2) - 1; }
 __device__ __forceinline__ bool map_live(int v) { return (v & 1) != 0; }
 __device__ __forceinline__ bool map_mine(int v) { return (v & 2) != 0; }
 
-template <int TX, int TY>
-__global__ void k_slot_maps(MDesc D, int *maps) {
-    constexpr int NS = (TX + 2) * (TY + 2);
+__global__ void k_slot_maps(MDesc D, int TY, int *maps) {
+    const int NS = (kTX + 2) * (TY + 2);
     const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= (long long)D.ntiles * NS) return;
     const int tile = (int)(id / NS), sl = (int)(id % NS);
     const Geom &g = D.g;
     const int tx = tile % D.tiles_x, ty = tile / D.tiles_x;
-    const int i0 = g.ilo + tx * TX, j0 = g.jlo + ty * TY;
-    const int li = sl % (TX + 2), lj = sl / (TX + 2);
+    const int i0 = g.ilo + tx * kTX, j0 = g.jlo + ty * TY;
+    const int li = sl % (kTX + 2), lj = sl / (kTX + 2);
     const int i = i0 - 1 + li, j = j0 - 1 + lj;
     const long long m = src_col(g, i, j);
     int v = (int)(m + 1) << 2;
     if (m >= 0) {
         const int mi = (int)(m % g.NX), mj = (int)(m / g.NX);
         const bool live = live_col(D, mi, mj, m);
-        const bool interior = li >= 1 && li <= TX && lj >= 1 && lj <= TY;
+        const bool interior = li >= 1 && li <= kTX && lj >= 1 && lj <= TY;
         if (live) v |= 1;
         if (live && interior && m == (long long)j * g.NX + i) v |= 2;
     }
     maps[id] = v;
 }
 
-// z = M^-1 r on one column of the SIA tridiagonal, in place in smem (slot s), FP32.
-// The column's factors are loaded in one batch first: a load inside the recurrence
-// would cost one memory round trip per level.
-template <int KP, int NS, int NZM>
-__device__ __forceinline__ void sia_col(const MDesc &D, float (*zc)[KP][NS], int s, long long q) {
+// z = M^-1 r on one column of the SIA tridiagonal, in place in smem (zc = z[c][0][0],
+// row stride NS; level k at row k+1), FP32.  The column's factors are loaded in one
+// batch first: a load inside the recurrence would cost a memory round trip per level.
+template <int NZM>
+__device__ __forceinline__ void sia_col(const MDesc &D, float *zc, int NS, int s, long long q) {
     const int nz = D.g.nz;
     const long long NQ = D.g.NQ;
     const long long plane = (long long)nz * NQ;
+    constexpr int KP = NZM + 2;
     for (int c = 0; c < 2; ++c) {
-        float (*z)[NS] = zc[c] + 1;  // level k is row k+1 (rows 0 and nz+1 are zero padding)
+        float *z = zc + (size_t)c * KP * NS + NS + s;  // z[k * NS] is level k
         const float *ib = D.pre + (c * 3 + 0) * plane, *sb = D.pre + (c * 3 + 1) * plane,
                     *gm = D.pre + (c * 3 + 2) * plane;
         float fib[NZM], fsb[NZM], fgm[NZM];
@@ -317,91 +325,93 @@ __device__ __forceinline__ void sia_col(const MDesc &D, float (*zc)[KP][NS], int
             fgm[k] = in ? __ldg(gm + (long long)k * NQ + q) : 0.0f;
         }
         // forward: y_1 = r_1/beta_1; y_k = (r_k - sb_k y_{k-1})/beta_k; back: z_k = y_k - gamma_{k+1} z_{k+1}
-        float prev = z[0][s] * fib[0];
-        z[0][s] = prev;
+        float prev = z[0] * fib[0];
+        z[0] = prev;
 #pragma unroll
-        for (int k = 1; k < NZM; ++k) {
+        for (int k = 1; k < NZM; ++k)
             if (k < nz) {
-                prev = (z[k][s] - fsb[k] * prev) * fib[k];
-                z[k][s] = prev;
+                prev = (z[(size_t)k * NS] - fsb[k] * prev) * fib[k];
+                z[(size_t)k * NS] = prev;
             }
-        }
-        float next = z[nz - 1][s];
+        float next = prev;
 #pragma unroll
-        for (int k = NZM - 2; k >= 0; --k) {
+        for (int k = NZM - 2; k >= 0; --k)
             if (k < nz - 1) {
-                next = z[k][s] - fgm[k + 1] * next;
-                z[k][s] = next;
+                next = z[(size_t)k * NS] - fgm[k + 1] * next;
+                z[(size_t)k * NS] = next;
             }
-        }
     }
 }
 
 // One tile of one solve for the solve's current step; writes the tile's partials.
 template <int NC, int NZM>
-__device__ void tile_step(const MState &S, int tile, int pbuf, MShared<NC, NZM> &sh) {
-    using SH = MShared<NC, NZM>;
-    constexpr int TX = SH::TX, TY = SH::TY, NS = SH::NS, NT = SH::NT, KP = SH::KP;
+__device__ void tile_step(const MState &S, int tile, int pbuf, int TY, bool resident, MHead &hd, unsigned char *smem) {
+    using LY = MLayout<NC, NZM>;
+    constexpr int KP = LY::KP;
     constexpr int OFF = (NC == 27) ? 1 : 0;  // z row of level 0
-    const MDesc &D = sh.D;
+    const LY ly(TY, resident);
+    const int NS = ly.NS, NT = ly.NT;
+    int *smap = reinterpret_cast<int *>(smem + ly.off_map());
+    float *sz = reinterpret_cast<float *>(smem + ly.off_z());   // [2][KP][NS]
+    float *srt = reinterpret_cast<float *>(smem + ly.off_rt()); // [2][NZM][NT]
+    const MDesc &D = hd.D;
     const Geom &g = D.g;
     const int nz = (NC == 27) ? g.nz : 1;
     const long long NQ = g.NQ;
     const long long plane = (long long)nz * NQ;
     const int tx = tile % D.tiles_x, ty = tile / D.tiles_x;
-    const int i0 = g.ilo + tx * TX, j0 = g.jlo + ty * TY;
+    const int i0 = g.ilo + tx * kTX, j0 = g.jlo + ty * TY;
     const int t = threadIdx.x;
     const int step = S.step;
     const int par = S.par;
-    DD p0{0.0, 0.0}, p1{0.0, 0.0}, p2{0.0, 0.0};
+    double p0 = 0.0, p1 = 0.0, p2 = 0.0;
 
-    const int *tmap = D.maps + (long long)tile * NS;
-    for (int sl = t; sl < NS; sl += kBlock) sh.map[sl] = tmap[sl];
-    __syncthreads();
+    if (!resident) {  // resident launches keep their single tile's map for the whole launch
+        const int *tmap = D.maps + (long long)tile * NS;
+        for (int sl = t; sl < NS; sl += kBlock) smap[sl] = tmap[sl];
+        __syncthreads();
+    }
 
     if (step == MS_INIT || step == MS_CHECK) {
         // r = b - A64 x (FP64, x read through the halo map); r32 = r on live columns
         const double *Auu = D.A64, *Auv = D.A64 + NC * plane, *Avu = D.A64 + 2 * NC * plane,
                      *Avv = D.A64 + 3 * NC * plane;
         const double *xu = D.x, *xv = D.x + plane;
-        for (int it = t; it < NT; it += kBlock) {
-            const int ti = it % TX, tj = it / TX;
+        const int nitems = NT * nz;
+        for (int it = t; it < nitems; it += kBlock) {
+            const int col = it % NT, k = it / NT;
+            const int ti = col % kTX, tj = col / kTX;
             const int i = i0 + ti, j = j0 + tj;
             if (i > g.ihi || j > g.jhi) continue;
             const long long q = (long long)j * g.NX + i;
-            const int s = (ti + 1) + (TX + 2) * (tj + 1);
+            const int s = (ti + 1) + (kTX + 2) * (tj + 1);
             const bool on = D.act[q] != 0;
-            const bool live = map_live(sh.map[s]);
-            int nb[9];
+            const bool live = map_live(smap[s]);
+            const long long e = (long long)k * NQ + q;
+            double yu = 0.0, yv = 0.0;
+            if (on) {
 #pragma unroll
-            for (int h = 0; h < 9; ++h) nb[h] = map_src(sh.map[s + (h % 3 - 1) + (TX + 2) * (h / 3 - 1)]);
-            for (int k = 0; k < nz; ++k) {
-                const long long e = (long long)k * NQ + q;
-                double yu = 0.0, yv = 0.0;
-                if (on) {
-#pragma unroll
-                    for (int c = 0; c < NC; ++c) {
-                        const int kA = (NC == 27) ? c / 9 - 1 : 0;
-                        const int sc = nb[c % 9];
-                        if (k + kA < 0 || k + kA >= nz || sc < 0) continue;
-                        const long long n = (long long)(k + kA) * NQ + sc;
-                        const long long a = (long long)c * plane + e;
-                        const double x1 = ldd(xu + n), x2 = ldd(xv + n);
-                        yu = fma(Auu[a], x1, yu);
-                        yu = fma(Auv[a], x2, yu);
-                        yv = fma(Avu[a], x1, yv);
-                        yv = fma(Avv[a], x2, yv);
-                    }
+                for (int c = 0; c < NC; ++c) {
+                    const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
+                    const int sc = map_src(smap[s + iA + (kTX + 2) * jA]);
+                    if (k + kA < 0 || k + kA >= nz || sc < 0) continue;
+                    const long long n = (long long)(k + kA) * NQ + sc;
+                    const long long a = (long long)c * plane + e;
+                    const double x1 = ldd(xu + n), x2 = ldd(xv + n);
+                    yu = fma(Auu[a], x1, yu);
+                    yu = fma(Auv[a], x2, yu);
+                    yv = fma(Avu[a], x1, yv);
+                    yv = fma(Avv[a], x2, yv);
                 }
-                const double bu = D.b[e], bv = D.b[plane + e];
-                const double ru = bu - yu, rv = bv - yv;
-                p1 = dd_add_d(p1, ru * ru + rv * rv);
-                if (step == MS_INIT) p0 = dd_add_d(p0, bu * bu + bv * bv);
-                D.r[par][e] = live ? (float)ru : 0.0f;
-                D.r[par][plane + e] = live ? (float)rv : 0.0f;
             }
+            const double bu = D.b[e], bv = D.b[plane + e];
+            const double ru = bu - yu, rv = bv - yv;
+            p1 += ru * ru + rv * rv;
+            p0 += bu * bu + bv * bv;
+            D.r[par][e] = live ? (float)ru : 0.0f;
+            D.r[par][plane + e] = live ? (float)rv : 0.0f;
         }
-        if (step == MS_CHECK) { p0 = p1; p1 = DD{0.0, 0.0}; }
+        if (step == MS_CHECK) { p0 = p1; p1 = 0.0; }
     } else {
         const float alpha = (float)S.alpha, beta = (float)S.beta;
         const double alpha64 = S.alpha;
@@ -410,83 +420,102 @@ __device__ void tile_step(const MState &S, int tile, int pbuf, MShared<NC, NZM> 
         const int rin = par, rout = do_b ? (par ^ 1) : par;  // buffers holding r_i / r_{i+1}
 
         // ---- pass 1: update (B) on the tile, new residual (and diag z) on tile + halo ----
-        constexpr int P1 = (2 * NS + kBlock - 1) / kBlock;  // items per thread and level
+        const int n1 = 2 * NS;
         for (int k = 0; k < nz; ++k) {
-#pragma unroll
-            for (int r = 0; r < P1; ++r) {
-                const int it = t + r * kBlock;
-                if (it >= 2 * NS) break;
-                const int c = it / NS, sl = it - c * NS;
-                const int v = sh.map[sl];
+#pragma unroll 4
+            for (int it = t; it < n1; it += kBlock) {
+                const int c = it >= NS ? 1 : 0, sl = it - c * NS;
+                const int v = smap[sl];
                 const int m = map_live(v) ? map_src(v) : -1;
                 float rn = 0.0f;
                 if (m >= 0) {
                     const long long e = c * plane + (long long)k * NQ + m;
                     if (do_b) {
+                        // the owner's d, z, x are loaded with the halo values (one round trip);
+                        // every live slot maps to an owned column, so the addresses are valid
                         const float qo = ldf(D.q[rin] + e), az = ldf(D.Az[rin] + e), ro = ldf(D.r[rin] + e);
+                        const bool mine = map_mine(v);
+                        const float dold = mine ? D.d[e] : 0.0f, zold = mine ? D.z[e] : 0.0f;
+                        const double xold = mine ? D.x[e] : 0.0;
                         const float qn = fmaf(beta, qo, az);  // q_i = Az_i + beta q_{i-1}
                         rn = fmaf(-alpha, qn, ro);             // r_{i+1} = r_i - alpha q_i
-                        if (map_mine(v)) {
-                            const float dn = fmaf(beta, D.d[e], D.z[e]);  // d_i = z_i + beta d_{i-1}
+                        if (mine) {
+                            const float dn = fmaf(beta, dold, zold);  // d_i = z_i + beta d_{i-1}
                             D.d[e] = dn;
                             D.q[rout][e] = qn;
                             D.r[rout][e] = rn;
-                            D.x[e] = fma(alpha64, (double)dn, D.x[e]);  // x += alpha d_i (FP64)
+                            D.x[e] = fma(alpha64, (double)dn, xold);  // x += alpha d_i (FP64)
                         }
                     } else {
                         rn = ldf(D.r[rin] + e);
                     }
                 }
                 if (do_a) {
-                    const int li = sl % (TX + 2), lj = sl / (TX + 2);
-                    if (li >= 1 && li <= TX && lj >= 1 && lj <= TY) sh.rt[c][k][(li - 1) + TX * (lj - 1)] = rn;
+                    const int li = sl % (kTX + 2), lj = sl / (kTX + 2);
+                    if (li >= 1 && li <= kTX && lj >= 1 && lj <= TY)
+                        srt[((size_t)c * NZM + k) * NT + (li - 1) + kTX * (lj - 1)] = rn;
                     float zv = rn;
-                    if (D.precond == 1 && m >= 0) zv = rn * D.pre[c * plane + (long long)k * NQ + m];
-                    sh.z[c][k + OFF][sl] = zv;
+                    if (D.precond == 1 && m >= 0) zv = rn * __ldg(D.pre + c * plane + (long long)k * NQ + m);
+                    sz[((size_t)c * KP + k + OFF) * NS + sl] = zv;
                 }
             }
         }
         if (do_a) {
             if (NC == 27) {  // zero padding rows (levels -1 and nz)
-                for (int it = t; it < 2 * NS; it += kBlock) {
-                    const int c = it / NS, sl = it - c * NS;
-                    sh.z[c][0][sl] = 0.0f;
-                    sh.z[c][nz + 1][sl] = 0.0f;
+                for (int it = t; it < n1; it += kBlock) {
+                    const int c = it >= NS ? 1 : 0, sl = it - c * NS;
+                    sz[((size_t)c * KP + 0) * NS + sl] = 0.0f;
+                    sz[((size_t)c * KP + nz + 1) * NS + sl] = 0.0f;
                 }
             }
             __syncthreads();
             if (NC == 27 && D.precond == 2) {  // column tridiagonal solves on tile + halo
                 for (int sl = t; sl < NS; sl += kBlock) {
-                    const int v = sh.map[sl];
-                    if (map_live(v)) sia_col<KP, NS, NZM>(D, sh.z, sl, map_src(v));
+                    const int v = smap[sl];
+                    if (map_live(v)) sia_col<NZM>(D, sz, NS, sl, map_src(v));
                 }
                 __syncthreads();
             }
 
-            // ---- pass 2: Az = A z on the tile columns, z to HBM, partial dots ----
+            // ---- pass 2: Az = A z on (column, level) items, z to HBM, partial dots ----
             // Couplings that leave the grid are zero in the FP32 copy and the padded z rows
-            // and out-of-grid halo slots are zero, so every column sums all NC terms.
+            // and out-of-grid halo slots are zero, so every node sums all NC terms.
             const float *Auu = D.A32, *Auv = D.A32 + NC * plane, *Avu = D.A32 + 2 * NC * plane,
                         *Avv = D.A32 + 3 * NC * plane;
+            const float *sA = reinterpret_cast<const float *>(smem + ly.off_A());  // [4][NC][nz*NT]
+            const int NN = nz * NT;
             float *Azu = D.Az[rout], *Azv = D.Az[rout] + plane;
-#pragma unroll
-            for (int r = 0; r < NT / kBlock; ++r) {
-                const int it = t + r * kBlock;
-                const int ti = it % TX, tj = it / TX;
+            const float *szu = sz, *szv = sz + (size_t)KP * NS;
+            const int nitems = NT * nz;
+#pragma unroll 2
+            for (int it = t; it < nitems; it += kBlock) {
+                const int col = it % NT, k = it / NT;
+                const int ti = col % kTX, tj = col / kTX;
                 const int i = i0 + ti, j = j0 + tj;
                 if (i > g.ihi || j > g.jhi) continue;
-                const int s = (ti + 1) + (TX + 2) * (tj + 1);
+                const int s = (ti + 1) + (kTX + 2) * (tj + 1);
                 const long long q = (long long)j * g.NX + i;
-                const bool live = map_live(sh.map[s]);
-                for (int k = 0; k < nz; ++k) {
-                    const long long e = (long long)k * NQ + q;
-                    float yu = 0.0f, yv = 0.0f;
-                    if (live) {
+                const long long e = (long long)k * NQ + q;
+                float yu = 0.0f, yv = 0.0f;
+                if (map_live(smap[s])) {
+                    if (resident) {
 #pragma unroll
                         for (int c = 0; c < NC; ++c) {
                             const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
-                            const int sn = s + iA + (TX + 2) * jA;
-                            const float zu = sh.z[0][k + OFF + kA][sn], zv = sh.z[1][k + OFF + kA][sn];
+                            const int zi = (k + OFF + kA) * NS + s + iA + (kTX + 2) * jA;
+                            const float zu = szu[zi], zv = szv[zi];
+                            const int a = c * NN + it;
+                            yu = fmaf(sA[a], zu, yu);
+                            yu = fmaf(sA[NC * NN + a], zv, yu);
+                            yv = fmaf(sA[2 * NC * NN + a], zu, yv);
+                            yv = fmaf(sA[3 * NC * NN + a], zv, yv);
+                        }
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
+                            const int zi = (k + OFF + kA) * NS + s + iA + (kTX + 2) * jA;
+                            const float zu = szu[zi], zv = szv[zi];
                             const long long a = (long long)c * plane + e;
                             yu = fmaf(__ldg(Auu + a), zu, yu);
                             yu = fmaf(__ldg(Auv + a), zv, yu);
@@ -494,112 +523,158 @@ __device__ void tile_step(const MState &S, int tile, int pbuf, MShared<NC, NZM> 
                             yv = fmaf(__ldg(Avv + a), zv, yv);
                         }
                     }
-                    Azu[e] = yu;
-                    Azv[e] = yv;
-                    const float zu = sh.z[0][k + OFF][s], zv = sh.z[1][k + OFF][s];
-                    D.z[e] = zu;
-                    D.z[plane + e] = zv;
-                    const double ru = sh.rt[0][k][it], rv = sh.rt[1][k][it];
-                    p0 = dd_add_d(p0, ru * (double)zu + rv * (double)zv);
-                    p1 = dd_add_d(p1, (double)yu * zu + (double)yv * zv);
-                    p2 = dd_add_d(p2, ru * ru + rv * rv);
                 }
+                Azu[e] = yu;
+                Azv[e] = yv;
+                const float zu = szu[(k + OFF) * NS + s], zv = szv[(k + OFF) * NS + s];
+                D.z[e] = zu;
+                D.z[plane + e] = zv;
+                const double ru = srt[(size_t)k * NT + col], rv = srt[((size_t)NZM + k) * NT + col];
+                p0 += ru * (double)zu + rv * (double)zv;
+                p1 += (double)yu * zu + (double)yv * zv;
+                p2 += ru * ru + rv * rv;
             }
         }
     }
-    block_tree3(p0, p1, p2, sh.red);
+    block_sum3(p0, p1, p2, hd.red);
     if (t == 0) {
         DD *pp = D.partials + ((long long)tile * 2 + pbuf) * 3;
-        pp[0] = p0;
-        pp[1] = p1;
-        pp[2] = p2;
+        pp[0] = DD{p0, 0.0};
+        pp[1] = DD{p1, 0.0};
+        pp[2] = DD{p2, 0.0};
     }
     __syncthreads();
 }
 
 // Reduce the partials (buffer pbuf) of every running solve this CTA holds and advance
-// its cached state.  Every CTA holding a solve does this with the same inputs and the
-// same fixed tree, so all copies of a solve's state stay bit-identical.  The CTA holding
-// tile 0 publishes a finished solve and decrements n_active before its next barrier.
-template <int NC, int NZM>
-__device__ void reduce_cached(MShared<NC, NZM> &sh, const MDesc *__restrict__ descs, int pbuf, MState *gstates,
+// its cached state.  All threads stage the tile partials in shared memory (one memory
+// round trip per kStage tiles); warp 0 sums them in double-double in a fixed order
+// (lane l takes tiles l, l+32, ...; then a shuffle tree).  Every CTA holding a solve does
+// this with the same inputs, so all copies of a solve's state stay bit-identical.  The
+// CTA holding tile 0 publishes a finished solve and decrements n_active before its next
+// barrier.
+__device__ void reduce_cached(MHead &hd, DD *stage, const MDesc *__restrict__ descs, int pbuf, MState *gstates,
                               GridBar *bar) {
-    for (int cs = 0; cs < sh.nsolve; ++cs) {
-        if (sh.st[cs].done) continue;
-        const MDesc &D = descs[sh.sid[cs]];
+    const int lane = threadIdx.x & 31;
+    for (int cs = 0; cs < hd.nsolve; ++cs) {
+        if (hd.st[cs].done) continue;  // uniform: only thread 0 writes st, before a barrier
+        const MDesc &D = descs[hd.sid[cs]];
         const int ntl = D.ntiles;
         const DD *P = D.partials;
         DD a0{0.0, 0.0}, a1{0.0, 0.0}, a2{0.0, 0.0};
-        for (int c = threadIdx.x; c < ntl; c += kBlock) {
-            const DD *pp = P + ((long long)c * 2 + pbuf) * 3;
-            DD v0, v1, v2;
-            v0.hi = __ldcg(&pp[0].hi); v0.lo = __ldcg(&pp[0].lo);
-            v1.hi = __ldcg(&pp[1].hi); v1.lo = __ldcg(&pp[1].lo);
-            v2.hi = __ldcg(&pp[2].hi); v2.lo = __ldcg(&pp[2].lo);
-            a0 = dd_add(a0, v0);
-            a1 = dd_add(a1, v1);
-            a2 = dd_add(a2, v2);
+        const int chunk = kStage / 3 / 32 * 32;  // tiles per staging round, a multiple of 32
+        for (int base = 0; base < ntl; base += chunk) {
+            const int n = min(chunk, ntl - base);
+            __syncthreads();
+            for (int w = threadIdx.x; w < 3 * n; w += kBlock) {
+                const DD *pp = P + ((long long)(base + w / 3) * 2 + pbuf) * 3 + (w % 3);
+                DD v;
+                v.hi = __ldcg(&pp->hi);
+                v.lo = __ldcg(&pp->lo);
+                stage[w] = v;
+            }
+            __syncthreads();
+            if (threadIdx.x < 32)
+                for (int c = lane; c < n; c += 32) {
+                    a0 = dd_add(a0, stage[3 * c + 0]);
+                    a1 = dd_add(a1, stage[3 * c + 1]);
+                    a2 = dd_add(a2, stage[3 * c + 2]);
+                }
         }
-        block_tree3(a0, a1, a2, sh.red);
-        if (threadIdx.x == 0) {
-            MState &S = sh.st[cs];
-            advance_state(S, D, a0.hi + a0.lo, a1.hi + a1.lo, a2.hi + a2.lo);
-            if (S.done && sh.owner[cs]) {
-                gstates[sh.sid[cs]] = S;
-                __threadfence();
-                atomicSub(&bar->n_active, 1);
+        if (threadIdx.x < 32) {
+#pragma unroll
+            for (int off = 16; off >= 1; off >>= 1) {
+                DD o0 = dd_shfl_down(a0, off), o1 = dd_shfl_down(a1, off), o2 = dd_shfl_down(a2, off);
+                if (lane + off < 32) { a0 = dd_add(a0, o0); a1 = dd_add(a1, o1); a2 = dd_add(a2, o2); }
+            }
+            if (lane == 0) {
+                MState &S = hd.st[cs];
+                advance_state(S, D, a0.hi + a0.lo, a1.hi + a1.lo, a2.hi + a2.lo);
+                if (S.done && hd.owner[cs]) {
+                    gstates[hd.sid[cs]] = S;
+                    __threadfence();
+                    atomicSub(&bar->n_active, 1);
+                }
             }
         }
         __syncthreads();
     }
 }
 
+// resident != 0: the launch has exactly one tile per CTA; the CTA keeps that tile's slot
+// map and (2D) its FP32 matrix coefficients in shared memory for the whole launch.
 template <int NC, int NZM>
 __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ descs, MState *states,
-                                                     const MTile *__restrict__ tiles, int ntiles, GridBar *bar,
-                                                     int max_steps) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    MShared<NC, NZM> &sh = *reinterpret_cast<MShared<NC, NZM> *>(smem_raw);
+                                                     const MTile *__restrict__ tiles, int ntiles, int TY,
+                                                     int resident, GridBar *bar, int max_steps) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    MHead &hd = *reinterpret_cast<MHead *>(smem);
+    const MLayout<NC, NZM> ly(TY, resident != 0);
+    DD *stage = reinterpret_cast<DD *>(smem + ly.off_stage());
     // cache the states of the solves this CTA holds (round robin over the tile list)
     if (threadIdx.x == 0) {
         int n = 0;
         for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
             const MTile T = tiles[w];
             int u = 0;
-            while (u < n && sh.sid[u] != T.solve) ++u;
+            while (u < n && hd.sid[u] != T.solve) ++u;
             if (u == n && n < kMaxCtaSolves) {
-                sh.sid[n] = T.solve;
-                sh.owner[n] = 0;
+                hd.sid[n] = T.solve;
+                hd.owner[n] = 0;
                 const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&states[T.solve]);
-                unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sh.st[n]);
+                unsigned long long *dst = reinterpret_cast<unsigned long long *>(&hd.st[n]);
                 for (int w8 = 0; w8 < (int)(sizeof(MState) / 8); ++w8) dst[w8] = __ldcg(src + w8);
                 ++n;
             }
-            if (u < n && T.tile == 0) sh.owner[u] = 1;
+            if (u < n && T.tile == 0) hd.owner[u] = 1;
         }
-        sh.nsolve = n;
-        sh.cur = -1;
+        hd.nsolve = n;
+        hd.cur = -1;
     }
     __syncthreads();
+    if (resident && blockIdx.x < ntiles) {  // the CTA's only tile: slot map and FP32 matrix
+        const MTile T = tiles[blockIdx.x];
+        const MDesc &D = descs[T.solve];
+        const int NS = ly.NS, NT = ly.NT;
+        int *smap = reinterpret_cast<int *>(smem + ly.off_map());
+        const int *tmap = D.maps + (long long)T.tile * NS;
+        for (int sl = threadIdx.x; sl < NS; sl += kBlock) smap[sl] = tmap[sl];
+        float *sA = reinterpret_cast<float *>(smem + ly.off_A());
+        const int nz = (NC == 27) ? D.g.nz : 1;
+        const long long plane = (long long)nz * D.g.NQ;
+        const int tx = T.tile % D.tiles_x, ty = T.tile / D.tiles_x;
+        const int i0 = D.g.ilo + tx * kTX, j0 = D.g.jlo + ty * TY;
+        const int NN = nz * NT;
+        for (int w = threadIdx.x; w < 4 * NC * NN; w += kBlock) {
+            const int it = w % NN, bc = w / NN;  // bc = block * NC + c
+            const int col = it % NT, k = it / NT;
+            const int i = i0 + col % kTX, j = j0 + col / kTX;
+            float a = 0.0f;
+            if (i <= D.g.ihi && j <= D.g.jhi)
+                a = D.A32[(long long)bc * plane + (long long)k * D.g.NQ + (long long)j * D.g.NX + i];
+            sA[w] = a;
+        }
+        __syncthreads();
+    }
     bool finished = false;
     int step = 0;
     for (; step < max_steps; ++step) {
         const int pbuf = step & 1;
-        if (step > 0) reduce_cached<NC, NZM>(sh, descs, pbuf ^ 1, states, bar);  // previous step's sums
+        if (step > 0) reduce_cached(hd, stage, descs, pbuf ^ 1, states, bar);  // previous step's sums
         for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
             const MTile T = tiles[w];
             int cs = 0;
-            while (cs < sh.nsolve && sh.sid[cs] != T.solve) ++cs;
-            if (cs >= sh.nsolve || sh.st[cs].done) continue;
-            if (sh.cur != cs) {
+            while (cs < hd.nsolve && hd.sid[cs] != T.solve) ++cs;
+            if (cs >= hd.nsolve || hd.st[cs].done) continue;
+            if (hd.cur != cs) {
                 __syncthreads();
                 if (threadIdx.x == 0) {
-                    sh.D = descs[T.solve];
-                    sh.cur = cs;
+                    hd.D = descs[T.solve];
+                    hd.cur = cs;
                 }
                 __syncthreads();
             }
-            tile_step<NC, NZM>(sh.st[cs], T.tile, pbuf, sh);
+            tile_step<NC, NZM>(hd.st[cs], T.tile, pbuf, TY, resident != 0, hd, smem);
         }
         if (!grid_barrier(bar, gridDim.x)) return;
         if (((volatile GridBar *)bar)->n_active <= 0) {
@@ -608,10 +683,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
         }
     }
     // out of steps: fold in the last step's sums so that the next launch resumes exactly
-    if (!finished && step > 0) reduce_cached<NC, NZM>(sh, descs, (step - 1) & 1, states, bar);
+    if (!finished && step > 0) reduce_cached(hd, stage, descs, (step - 1) & 1, states, bar);
     if (threadIdx.x == 0)
-        for (int cs = 0; cs < sh.nsolve; ++cs)
-            if (sh.owner[cs]) states[sh.sid[cs]] = sh.st[cs];
+        for (int cs = 0; cs < hd.nsolve; ++cs)
+            if (hd.owner[cs]) states[hd.sid[cs]] = hd.st[cs];
 }
 
 // ---------------------------------------------------------------------------
@@ -675,6 +750,7 @@ __global__ void k_mixed_precond_setup(Geom g, int precond, const double *__restr
 // Device buffers of the mixed solver for one system (owned by the host Solver).
 struct MixedBufs {
     bool valid = false;
+    int TY = 0;                // tile height the slot maps were built for
     bool stale = false;        // the FP64 matrix changed since the FP32 copy was made
     long long shape_nvec = 0;
     int shape_nc = 0;
@@ -688,12 +764,17 @@ struct MixedBufs {
     GridBar *bar = nullptr;
     size_t nbytes = 0;
     int ntiles = 0;
+    int ntiles_cap = 0;
+    long long maps_cap = 0;
     void release() {
         for (void *p : {(void *)A32, (void *)pre, (void *)vec, (void *)partials, (void *)state, (void *)desc,
                         (void *)tiles, (void *)bar, (void *)maps})
             if (p) cudaFree(p);
         A32 = pre = vec = nullptr;
         maps = nullptr;
+        ntiles = ntiles_cap = 0;
+        maps_cap = 0;
+        TY = 0;
         partials = nullptr;
         state = nullptr;
         desc = nullptr;
