@@ -127,6 +127,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_solver_device_bytes.restype = ctypes.c_size_t
     lib.cismgpu_solver_destroy.argtypes = [vp]
     lib.cismgpu_solver_destroy.restype = ctypes.c_int
+    lib.cismgpu_global_sum_stagger.argtypes = [i32, i32, i32, par, d, d, P(dbl)]
+    lib.cismgpu_global_sum_stagger.restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
     lib.cismgpu_last_error.restype = ctypes.c_char_p
@@ -182,6 +184,18 @@ def _solve(fname: str, is3d: bool, nx, ny, nz, parallel, indxA_2d, indxA_3d, act
         ctypes.byref(niters), int(itest), int(jtest), int(rtest)]
     _check(lib, getattr(lib, fname)(*args))
     return err.value, niters.value
+
+
+def parallel_global_sum_stagger(nx, ny, nz, parallel, arr1, arr2) -> float:
+    """Mirrors parallel_global_sum_stagger(arr1, parallel, arr2) (libglimmer/parallel_mpi.F90:6537-6794)
+    on one rank: the sum over owned vertices of arr1 + arr2 (nz = 1 for 2D fields)."""
+    lib = load_library()
+    n = (nx - 1) * (ny - 1) * nz
+    out = ctypes.c_double(0.0)
+    par = _par(parallel)
+    _check(lib, lib.cismgpu_global_sum_stagger(nx, ny, nz, ctypes.byref(par), _ptr(arr1, np.float64, n),
+                                               _ptr(arr2, np.float64, n), ctypes.byref(out)))
+    return out.value
 
 
 def set_oneshot_algorithm(algorithm: int = -1) -> int:

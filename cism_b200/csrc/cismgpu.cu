@@ -846,6 +846,36 @@ static int oneshot_matvec(bool is3d, int nx, int ny, int nz, const cismgpu_par_t
     return sv.download(VX_U, VX_V, yu, yv);
 }
 
+static int oneshot_global_sum(int nx, int ny, int nz, const cismgpu_par_t *par, const double *a1, const double *a2,
+                              double *sum) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_error.clear();
+    if (!par || !a1 || !a2 || !sum) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (nx < 6 || ny < 6 || nz < 1) return fail(CISMGPU_EINVAL, "grid too small");
+    if (par->staggered_ilo < 1 || par->staggered_ihi > nx - 1 || par->staggered_ilo > par->staggered_ihi ||
+        par->staggered_jlo < 1 || par->staggered_jhi > ny - 1 || par->staggered_jlo > par->staggered_jhi)
+        return fail(CISMGPU_EINVAL, "owned vertex bounds outside the array");
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
+    const Geom g = make_geom(nx, ny, nz, par);
+    const long long n = (long long)nz * g.NQ;
+    const unsigned nb = nblocks(g.NQ);
+    CU(sv.raw.ensure((size_t)2 * n * sizeof(double)));
+    CU(sv.partials.ensure((size_t)nb * 2 * sizeof(DD)));
+    CU(sv.state.ensure(sizeof(SolveState)));
+    double *d1 = sv.raw.as<double>(), *d2 = d1 + n;
+    SolveState *st = sv.state.as<SolveState>();
+    CU(cudaMemcpyAsync(d1, a1, n * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
+    CU(cudaMemcpyAsync(d2, a2, n * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
+    CU(cudaMemsetAsync(st, 0, sizeof(SolveState), sv.stream));
+    k_gsum<true><<<nb, kBlock, 0, sv.stream>>>(g, d1, d2, sv.partials.as<DD>(), &st->ticket[0], &st->err);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(sum, &st->err, sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
+    CU(cudaStreamSynchronize(sv.stream));
+    return CISMGPU_OK;
+}
+
 }  // namespace cismgpu
 
 // ---------------------------------------------------------------------------
@@ -914,6 +944,11 @@ int cismgpu_matvec_structured_2d(int nx, int ny, const cismgpu_par_t *par, const
                                  const double *Avu, const double *Avv, const double *xu, const double *xv,
                                  double *yu, double *yv) {
     return oneshot_matvec(false, nx, ny, 1, par, indxA_2d, active_vertex, Auu, Auv, Avu, Avv, xu, xv, yu, yv);
+}
+
+int cismgpu_global_sum_stagger(int nx, int ny, int nz, const cismgpu_par_t *par, const double *arr1,
+                               const double *arr2, double *sum) {
+    return oneshot_global_sum(nx, ny, nz, par, arr1, arr2, sum);
 }
 
 int cismgpu_solver_create(cismgpu_solver_t **out, int dims, int nx, int ny, int nz, const cismgpu_par_t *par,

@@ -392,6 +392,54 @@ __global__ void __launch_bounds__(kBlock) k_halo(Geom g, double *__restrict__ au
 }
 
 // ---------------------------------------------------------------------------
+// owned-vertex global sum of arr1 + arr2 (parallel_global_sum_stagger on one rank)
+// ---------------------------------------------------------------------------
+// FORTRAN_LAYOUT: element (k, q) at k + nz*q (the caller's arrays); otherwise k*NQ + q.
+// Same tree as every solver reduction: column dd sums over k, block tree per chunk of
+// 256 columns, chunk partials, fixed final tree by the last CTA (which also resets the
+// ticket for the next use).
+template <bool FORTRAN_LAYOUT>
+__global__ void __launch_bounds__(kBlock) k_gsum(Geom g, const double *__restrict__ a1, const double *__restrict__ a2,
+                                                 DD *partials, unsigned int *ticket, double *out) {
+    __shared__ DD sm[8];
+    __shared__ bool last;
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    DD acc{0.0, 0.0};
+    if (q < g.NQ) {
+        int i, j;
+        j = (int)(q / g.NX);
+        i = (int)(q - (long long)j * g.NX);
+        if (owned(g, i, j))
+            for (int k = 0; k < g.nz; ++k) {
+                const long long e = FORTRAN_LAYOUT ? (long long)k + (long long)g.nz * q : (long long)k * g.NQ + q;
+                acc = dd_add_d(acc, __dadd_rn(a1[e], a2[e]));
+            }
+    }
+    DD b = block_tree(acc, sm);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = b;
+        __threadfence();
+        const unsigned int t = atomicAdd(ticket, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    DD a{0.0, 0.0};
+    for (unsigned int c = threadIdx.x; c < gridDim.x; c += kBlock) {
+        DD p;
+        p.hi = __ldcg(&partials[c].hi);
+        p.lo = __ldcg(&partials[c].lo);
+        a = dd_add(a, p);
+    }
+    DD r = block_tree(a, sm);
+    if (threadIdx.x == 0) {
+        *ticket = 0u;
+        *out = r.hi + r.lo;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // layout conversion between the caller's Fortran arrays and device planes
 // ---------------------------------------------------------------------------
 // 3D block A(27,nz,NX,NY) raw -> planes [c][k][q]; canonical c reads m = indxA(c)

@@ -188,3 +188,19 @@ def test_repeated_calls_reuse_workspace(gpu_lib):
     gpu_solve("chrongear", Q, 1)
     b = gpu_solve("chrongear", P, 2)
     assert_bitexact(a, b)
+
+
+@pytest.mark.parametrize("nz,bc", [(11, "periodic"), (1, "outflow"), (7, "no_ice")])
+def test_global_sum_stagger(gpu_lib, nz, bc):
+    """parallel_global_sum_stagger: bit-identical to the oracle's restatement of the device tree,
+    equal to the exact sum, and within rounding of the reference's sequential order."""
+    nx, ny = 37, 29
+    par = asm.default_par(nx, ny, bc)
+    rng = np.random.default_rng(nz)
+    a1 = rng.standard_normal((ny - 1, nx - 1, nz)) * np.exp(rng.uniform(-20, 20, (ny - 1, nx - 1, nz)))
+    a2 = rng.standard_normal((ny - 1, nx - 1, nz))
+    g = cg.parallel_global_sum_stagger(nx, ny, nz, par, a1, a2)
+    assert g == oracle.global_sum(nx, ny, nz, par, a1, a2, oracle.SUM_DDTREE)
+    assert g == oracle.global_sum(nx, ny, nz, par, a1, a2, oracle.SUM_EXACT)
+    seq = oracle.global_sum(nx, ny, nz, par, a1, a2, oracle.SUM_SEQ)
+    assert abs(g - seq) <= 1e-12 * np.sum(np.abs(a1 + a2))
