@@ -1,0 +1,262 @@
+!+++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++
+!
+!   glissade_velo_higher_pcg_gpu.F90
+!
+!   Drop-in replacements for the four native PCG solvers of
+!   libglissade/glissade_velo_higher_pcg.F90 that run on a B200 through the
+!   C ABI of libcismgpu.so (include/cismgpu.h).  Every subroutine keeps the
+!   reference argument list, intents and meaning:
+!     pcg_solver_standard_2d   (:67-823)     pcg_solver_standard_3d   (:827-1537)
+!     pcg_solver_chrongear_2d  (:1541-2628)  pcg_solver_chrongear_3d  (:2632-3594)
+!   A nonzero library status is reported the way the reference reports a failed
+!   solve: write_log(message, GM_FATAL).
+!
+!   type(parallel_type) is not interoperable, so the fields the path reads
+!   (libglimmer/parallel_mpi.F90:78-153) are copied into a bind(C) struct.
+!   logical arrays are passed as the 4-byte Fortran default logical; the library
+!   treats any nonzero value as .true.
+!
+!   Build: compile with the CISM sources and link libcismgpu.so, e.g. add
+!   "-L<path>/cism_b200/_lib -lcismgpu" to CISM_EXTRA_LIBS
+!   (builds/linux-gnu/linux-gnu-cmake:56).
+!
+!+++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++++
+
+  module glissade_velo_higher_pcg_gpu
+
+    use, intrinsic :: iso_c_binding
+    use glimmer_global, only: dp
+    use glimmer_log
+    use cism_parallel, only: parallel_type
+
+    implicit none
+    private
+    public :: pcg_solver_standard_2d, pcg_solver_standard_3d, &
+              pcg_solver_chrongear_2d, pcg_solver_chrongear_3d, &
+              cismgpu_use_mixed_precision
+
+    type, bind(C) :: cismgpu_par_t
+       integer(c_int32_t) :: staggered_ilo, staggered_ihi
+       integer(c_int32_t) :: staggered_jlo, staggered_jhi
+       integer(c_int32_t) :: periodic_bc, outflow_bc, no_ice_bc
+       integer(c_int32_t) :: reprosum
+       integer(c_int32_t) :: tasks_row, tasks_col
+    end type cismgpu_par_t
+
+    interface
+       integer(c_int) function c_pcg_standard_3d(nx, ny, nz, par, indxA_2d, indxA_3d, active_vertex, &
+            Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond, ncheck, tol, maxiters, err, niters,        &
+            itest, jtest, rtest) bind(C, name="cismgpu_pcg_standard_3d")
+         import :: c_int, c_double, c_int32_t, cismgpu_par_t
+         integer(c_int), value :: nx, ny, nz
+         type(cismgpu_par_t), intent(in) :: par
+         integer(c_int32_t), intent(in) :: indxA_2d(*), indxA_3d(*), active_vertex(*)
+         real(c_double), intent(in) :: Auu(*), Auv(*), Avu(*), Avv(*), bu(*), bv(*)
+         real(c_double), intent(inout) :: xu(*), xv(*)
+         integer(c_int), value :: precond, ncheck, maxiters, itest, jtest, rtest
+         real(c_double), value :: tol
+         real(c_double), intent(out) :: err
+         integer(c_int), intent(out) :: niters
+       end function c_pcg_standard_3d
+
+       integer(c_int) function c_pcg_chrongear_3d(nx, ny, nz, par, indxA_2d, indxA_3d, active_vertex, &
+            Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond, ncheck, tol, maxiters, err, niters,         &
+            itest, jtest, rtest) bind(C, name="cismgpu_pcg_chrongear_3d")
+         import :: c_int, c_double, c_int32_t, cismgpu_par_t
+         integer(c_int), value :: nx, ny, nz
+         type(cismgpu_par_t), intent(in) :: par
+         integer(c_int32_t), intent(in) :: indxA_2d(*), indxA_3d(*), active_vertex(*)
+         real(c_double), intent(in) :: Auu(*), Auv(*), Avu(*), Avv(*), bu(*), bv(*)
+         real(c_double), intent(inout) :: xu(*), xv(*)
+         integer(c_int), value :: precond, ncheck, maxiters, itest, jtest, rtest
+         real(c_double), value :: tol
+         real(c_double), intent(out) :: err
+         integer(c_int), intent(out) :: niters
+       end function c_pcg_chrongear_3d
+
+       integer(c_int) function c_pcg_standard_2d(nx, ny, par, indxA_2d, active_vertex,               &
+            Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond, ncheck, tol, maxiters, err, niters,        &
+            itest, jtest, rtest) bind(C, name="cismgpu_pcg_standard_2d")
+         import :: c_int, c_double, c_int32_t, cismgpu_par_t
+         integer(c_int), value :: nx, ny
+         type(cismgpu_par_t), intent(in) :: par
+         integer(c_int32_t), intent(in) :: indxA_2d(*), active_vertex(*)
+         real(c_double), intent(in) :: Auu(*), Auv(*), Avu(*), Avv(*), bu(*), bv(*)
+         real(c_double), intent(inout) :: xu(*), xv(*)
+         integer(c_int), value :: precond, ncheck, maxiters, itest, jtest, rtest
+         real(c_double), value :: tol
+         real(c_double), intent(out) :: err
+         integer(c_int), intent(out) :: niters
+       end function c_pcg_standard_2d
+
+       integer(c_int) function c_pcg_chrongear_2d(nx, ny, par, indxA_2d, active_vertex,              &
+            Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond, ncheck, tol, maxiters, err, niters,        &
+            itest, jtest, rtest) bind(C, name="cismgpu_pcg_chrongear_2d")
+         import :: c_int, c_double, c_int32_t, cismgpu_par_t
+         integer(c_int), value :: nx, ny
+         type(cismgpu_par_t), intent(in) :: par
+         integer(c_int32_t), intent(in) :: indxA_2d(*), active_vertex(*)
+         real(c_double), intent(in) :: Auu(*), Auv(*), Avu(*), Avv(*), bu(*), bv(*)
+         real(c_double), intent(inout) :: xu(*), xv(*)
+         integer(c_int), value :: precond, ncheck, maxiters, itest, jtest, rtest
+         real(c_double), value :: tol
+         real(c_double), intent(out) :: err
+         integer(c_int), intent(out) :: niters
+       end function c_pcg_chrongear_2d
+
+       integer(c_int) function c_set_oneshot_algorithm(algorithm) &
+            bind(C, name="cismgpu_set_oneshot_algorithm")
+         import :: c_int
+         integer(c_int), value :: algorithm
+       end function c_set_oneshot_algorithm
+
+       type(c_ptr) function c_last_error() bind(C, name="cismgpu_last_error")
+         import :: c_ptr
+       end function c_last_error
+    end interface
+
+  contains
+
+    !-----------------------------------------------------------------------
+    ! .true.: all four solvers run the mixed-precision persistent
+    ! Chronopoulos-Gear solver (FP32 recurrences, FP64 solution and residual
+    ! checks); .false. (default): the reference algorithms in FP64.
+    subroutine cismgpu_use_mixed_precision(on)
+      logical, intent(in) :: on
+      integer(c_int) :: prev
+      if (on) then
+         prev = c_set_oneshot_algorithm(2_c_int)
+      else
+         prev = c_set_oneshot_algorithm(-1_c_int)
+      endif
+    end subroutine cismgpu_use_mixed_precision
+
+    function to_c(parallel) result(p)
+      type(parallel_type), intent(in) :: parallel
+      type(cismgpu_par_t) :: p
+      p%staggered_ilo = parallel%staggered_ilo
+      p%staggered_ihi = parallel%staggered_ihi
+      p%staggered_jlo = parallel%staggered_jlo
+      p%staggered_jhi = parallel%staggered_jhi
+      p%periodic_bc = merge(1, 0, parallel%periodic_bc)
+      p%outflow_bc  = merge(1, 0, parallel%outflow_bc)
+      p%no_ice_bc   = merge(1, 0, parallel%no_ice_bc)
+      p%reprosum    = merge(1, 0, parallel%reprosum)
+      p%tasks_row   = parallel%tasks_row
+      p%tasks_col   = parallel%tasks_col
+    end function to_c
+
+    subroutine check(status)
+      integer(c_int), intent(in) :: status
+      character(kind=c_char), pointer :: msg(:)
+      character(len=256) :: text
+      integer :: n
+      if (status == 0) return
+      call c_f_pointer(c_last_error(), msg, [256])
+      text = ' '
+      do n = 1, 256
+         if (msg(n) == c_null_char) exit
+         text(n:n) = msg(n)
+      enddo
+      call write_log('GPU PCG solver has failed: '//trim(text), GM_FATAL)
+    end subroutine check
+
+    !-----------------------------------------------------------------------
+    subroutine pcg_solver_standard_3d(nx, ny, nz, parallel, indxA_2d, indxA_3d, active_vertex, &
+                                      Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond,             &
+                                      linear_solve_ncheck, tolerance, maxiters, err, niters,   &
+                                      itest, jtest, rtest)
+      integer, intent(in) :: nx, ny, nz
+      type(parallel_type), intent(in) :: parallel
+      integer, dimension(-1:1,-1:1), intent(in) :: indxA_2d
+      integer, dimension(-1:1,-1:1,-1:1), intent(in) :: indxA_3d
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      real(dp), dimension(27,nz,nx-1,ny-1), intent(in) :: Auu, Auv, Avu, Avv
+      real(dp), dimension(nz,nx-1,ny-1), intent(in) :: bu, bv
+      real(dp), dimension(nz,nx-1,ny-1), intent(inout) :: xu, xv
+      integer, intent(in) :: precond, linear_solve_ncheck, maxiters
+      real(dp), intent(in) :: tolerance
+      real(dp), intent(out) :: err
+      integer, intent(out) :: niters
+      integer, intent(in) :: itest, jtest, rtest
+      integer(c_int32_t) :: act(nx-1,ny-1)
+      act = merge(1, 0, active_vertex)
+      call check(c_pcg_standard_3d(nx, ny, nz, to_c(parallel), indxA_2d, indxA_3d, act, Auu, Auv, Avu, Avv, &
+                                   bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters,      &
+                                   err, niters, itest, jtest, rtest))
+    end subroutine pcg_solver_standard_3d
+
+    !-----------------------------------------------------------------------
+    subroutine pcg_solver_chrongear_3d(nx, ny, nz, parallel, indxA_2d, indxA_3d, active_vertex, &
+                                       Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond,             &
+                                       linear_solve_ncheck, tolerance, maxiters, err, niters,   &
+                                       itest, jtest, rtest)
+      integer, intent(in) :: nx, ny, nz
+      type(parallel_type), intent(in) :: parallel
+      integer, dimension(-1:1,-1:1), intent(in) :: indxA_2d
+      integer, dimension(-1:1,-1:1,-1:1), intent(in) :: indxA_3d
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      real(dp), dimension(27,nz,nx-1,ny-1), intent(in) :: Auu, Auv, Avu, Avv
+      real(dp), dimension(nz,nx-1,ny-1), intent(in) :: bu, bv
+      real(dp), dimension(nz,nx-1,ny-1), intent(inout) :: xu, xv
+      integer, intent(in) :: precond, linear_solve_ncheck, maxiters
+      real(dp), intent(in) :: tolerance
+      real(dp), intent(out) :: err
+      integer, intent(out) :: niters
+      integer, intent(in) :: itest, jtest, rtest
+      integer(c_int32_t) :: act(nx-1,ny-1)
+      act = merge(1, 0, active_vertex)
+      call check(c_pcg_chrongear_3d(nx, ny, nz, to_c(parallel), indxA_2d, indxA_3d, act, Auu, Auv, Avu, Avv, &
+                                    bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters,      &
+                                    err, niters, itest, jtest, rtest))
+    end subroutine pcg_solver_chrongear_3d
+
+    !-----------------------------------------------------------------------
+    subroutine pcg_solver_standard_2d(nx, ny, parallel, indxA_2d, active_vertex,            &
+                                      Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond,          &
+                                      linear_solve_ncheck, tolerance, maxiters, err, niters, &
+                                      itest, jtest, rtest)
+      integer, intent(in) :: nx, ny
+      type(parallel_type), intent(in) :: parallel
+      integer, dimension(-1:1,-1:1), intent(in) :: indxA_2d
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      real(dp), dimension(nx-1,ny-1,9), intent(in) :: Auu, Auv, Avu, Avv
+      real(dp), dimension(nx-1,ny-1), intent(in) :: bu, bv
+      real(dp), dimension(nx-1,ny-1), intent(inout) :: xu, xv
+      integer, intent(in) :: precond, linear_solve_ncheck, maxiters
+      real(dp), intent(in) :: tolerance
+      real(dp), intent(out) :: err
+      integer, intent(out) :: niters
+      integer, intent(in) :: itest, jtest, rtest
+      integer(c_int32_t) :: act(nx-1,ny-1)
+      act = merge(1, 0, active_vertex)
+      call check(c_pcg_standard_2d(nx, ny, to_c(parallel), indxA_2d, act, Auu, Auv, Avu, Avv,            &
+                                   bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, &
+                                   err, niters, itest, jtest, rtest))
+    end subroutine pcg_solver_standard_2d
+
+    !-----------------------------------------------------------------------
+    subroutine pcg_solver_chrongear_2d(nx, ny, parallel, indxA_2d, active_vertex,            &
+                                       Auu, Auv, Avu, Avv, bu, bv, xu, xv, precond,          &
+                                       linear_solve_ncheck, tolerance, maxiters, err, niters, &
+                                       itest, jtest, rtest)
+      integer, intent(in) :: nx, ny
+      type(parallel_type), intent(in) :: parallel
+      integer, dimension(-1:1,-1:1), intent(in) :: indxA_2d
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      real(dp), dimension(nx-1,ny-1,9), intent(in) :: Auu, Auv, Avu, Avv
+      real(dp), dimension(nx-1,ny-1), intent(in) :: bu, bv
+      real(dp), dimension(nx-1,ny-1), intent(inout) :: xu, xv
+      integer, intent(in) :: precond, linear_solve_ncheck, maxiters
+      real(dp), intent(in) :: tolerance
+      real(dp), intent(out) :: err
+      integer, intent(out) :: niters
+      integer, intent(in) :: itest, jtest, rtest
+      integer(c_int32_t) :: act(nx-1,ny-1)
+      act = merge(1, 0, active_vertex)
+      call check(c_pcg_chrongear_2d(nx, ny, to_c(parallel), indxA_2d, act, Auu, Auv, Avu, Avv,            &
+                                    bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, &
+                                    err, niters, itest, jtest, rtest))
+    end subroutine pcg_solver_chrongear_2d
+
+  end module glissade_velo_higher_pcg_gpu
