@@ -129,6 +129,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_solver_destroy.restype = ctypes.c_int
     lib.cismgpu_global_sum_stagger.argtypes = [i32, i32, i32, par, d, d, P(dbl)]
     lib.cismgpu_global_sum_stagger.restype = ctypes.c_int
+    lib.cismgpu_global_sum_stagger_noalloc.argtypes = [i32, i32, i32, par, vp, vp, vp, vp]
+    lib.cismgpu_global_sum_stagger_noalloc.restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
     lib.cismgpu_last_error.restype = ctypes.c_char_p
@@ -196,6 +198,24 @@ def parallel_global_sum_stagger(nx, ny, nz, parallel, arr1, arr2) -> float:
     _check(lib, lib.cismgpu_global_sum_stagger(nx, ny, nz, ctypes.byref(par), _ptr(arr1, np.float64, n),
                                                _ptr(arr2, np.float64, n), ctypes.byref(out)))
     return out.value
+
+
+NOALLOC_MAX_COLUMNS = 4194304  # CISMGPU_NOALLOC_MAX_COLUMNS
+
+
+def parallel_global_sum_stagger_noalloc(nx, ny, nz, parallel, arr1_dev: int, arr2_dev: int, sum_dev: int,
+                                        stream: int = 0) -> None:
+    """The owned-vertex sum of parallel_global_sum_stagger for callers that cannot let the
+    library allocate device memory: arr1_dev, arr2_dev and sum_dev are device addresses (e.g. a
+    torch tensor's data_ptr()), the kernel is enqueued on `stream` (a cudaStream_t as an int, 0 for
+    the default stream) and writes the sum to sum_dev without synchronizing.  The scratch is a fixed
+    array inside the library, shared by every call on a device, so calls that overlap on the GPU race;
+    grids with more than NOALLOC_MAX_COLUMNS vertex columns are rejected."""
+    lib = load_library()
+    par = _par(parallel)
+    _check(lib, lib.cismgpu_global_sum_stagger_noalloc(nx, ny, nz, ctypes.byref(par), ctypes.c_void_p(arr1_dev),
+                                                       ctypes.c_void_p(arr2_dev), ctypes.c_void_p(sum_dev),
+                                                       ctypes.c_void_p(stream)))
 
 
 def set_oneshot_algorithm(algorithm: int = -1) -> int:

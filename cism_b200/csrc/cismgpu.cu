@@ -1131,3 +1131,5 @@ const char *cismgpu_last_error(void) { return g_last_error.c_str(); }
 const char *cismgpu_version(void) { return "cismgpu 0.2 (sm_100a)"; }
 
 }  // extern "C"
+
+#include "noalloc.cu"

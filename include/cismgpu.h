@@ -155,6 +155,24 @@ int cismgpu_matvec_structured_2d(int nx, int ny, const cismgpu_par_t *par,
 int cismgpu_global_sum_stagger(int nx, int ny, int nz, const cismgpu_par_t *par,
                                const double *arr1, const double *arr2, double *sum);
 
+/* No counterpart in the reference: the sum above for callers that cannot let a
+ * library allocate device memory -- a host whose own allocator has reserved the
+ * device, code that must not stall the device mid-step the way cudaMalloc/cudaFree
+ * can, or code that only holds device pointers another component gave it.
+ * arr1_dev, arr2_dev (layout (nz, nx-1, ny-1)) and sum_dev are device-accessible
+ * pointers; the kernel is enqueued on cuda_stream (NULL: the default stream) and
+ * *sum_dev is written asynchronously, identical to cismgpu_global_sum_stagger's result.
+ * It allocates nothing: its scratch is a fixed array in the library's device memory,
+ * sized for at most CISMGPU_NOALLOC_MAX_COLUMNS vertex columns (nx-1)*(ny-1) (any nz);
+ * larger grids return CISMGPU_EINVAL.  All calls on a device share that array: calls
+ * whose kernels overlap on the GPU race and give wrong sums, so order them (one stream).
+ * The first call on each device looks up the array's address (and may load the
+ * library's kernels onto the device): make it before any stream capture begins. */
+#define CISMGPU_NOALLOC_MAX_COLUMNS 4194304
+int cismgpu_global_sum_stagger_noalloc(int nx, int ny, int nz, const cismgpu_par_t *par,
+                                       const double *arr1_dev, const double *arr2_dev,
+                                       double *sum_dev, void *cuda_stream);
+
 /* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps
