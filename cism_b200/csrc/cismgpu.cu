@@ -437,10 +437,10 @@ int Solver::run_chrongear(int precond, int ncheck, double tol, int maxiters) {
 // ---------------------------------------------------------------------------
 // mixed-precision persistent solver (pcg_mixed.cu): host side
 // ---------------------------------------------------------------------------
-__global__ void k_mstate_to_solve(const MState *ms, SolveState *st, const GridBar *bar) {
+__global__ void k_mstate_to_solve(const MState *ms, SolveState *st, const MCtl *ctl) {
     st->err = ms->err;
     st->niters = ms->niters;
-    st->status = (bar->abort && !ms->done) ? CISMGPU_ETIMEOUT : ms->status;
+    st->status = (ctl->abort && !ms->done) ? CISMGPU_ETIMEOUT : ms->status;
     st->checks = ms->checks;
     st->done = 1;
 }
@@ -449,7 +449,7 @@ static int tiles_for(const Geom &g, int TY) {
     return ((g.ihi - g.ilo + kTX) / kTX) * ((g.jhi - g.jlo + TY) / TY);
 }
 
-static MDesc mixed_desc(const Solver &sv, int precond, int TY) {
+static MDesc mixed_desc(const Solver &sv, int precond, int TY) {  // TY: the solve's tile height
     const MixedBufs &m = sv.mixed;
     const long long nvec = sv.nvec;
     const Ptrs p = sv.ptrs();
@@ -457,6 +457,7 @@ static MDesc mixed_desc(const Solver &sv, int precond, int TY) {
     D.g = sv.g;
     D.NC = sv.NC;
     D.precond = precond;
+    D.TY = TY;
     D.tiles_x = (sv.g.ihi - sv.g.ilo + kTX) / kTX;
     D.tiles_y = (sv.g.jhi - sv.g.jlo + TY) / TY;
     D.ntiles = D.tiles_x * D.tiles_y;
@@ -473,7 +474,7 @@ static MDesc mixed_desc(const Solver &sv, int precond, int TY) {
     D.Az[0] = V + 4 * vs; D.Az[1] = V + 5 * vs;
     D.z = V + 6 * vs;
     D.d = V + 7 * vs;
-    D.partials = m.partials;
+    D.recs = m.recs;
     D.maps = m.maps;
     return D;
 }
@@ -507,40 +508,42 @@ static int mixed_grid(bool is3d, int nzm, int TY, bool resident = false) {
     return nsm * occ;
 }
 
-// Tile autotuner: the smallest tile height whose tiles (summed over the batch) fit in
-// the co-resident CTAs, so every CTA holds at most one tile per solve step; if no
-// height fits (large batches), 16 rows (8 for nz > 16), the best load balance measured
-// for streaming-bound batches.
-static int mixed_choose_ty(const std::vector<const Geom *> &gs, bool is3d, int nzm, bool *resident) {
-    *resident = false;
-    if (!is3d) {  // 2D: first try one tile per CTA with the tile's matrix resident in shared memory
+// Tile autotuner, per solve (a solve's tiling, and so its rounding, never depends on what
+// else shares a launch): the smallest tile height whose tiles fit in the co-resident
+// CTAs, so that alone every CTA holds one tile per step; 2D first tries the layout that
+// keeps the tile's FP32 matrix in shared memory.  If no height fits (very large grids),
+// 16 rows (8 for nz > 16), the best load balance measured for streaming-bound solves.
+static int mixed_solve_ty(const Geom &g, bool is3d, int nzm) {
+    if (!is3d)
         for (int TY = 1; TY <= kMaxTY; ++TY) {
             const int G = mixed_grid(is3d, nzm, TY, true);
             if (G == 0) break;
-            long long nt = 0;
-            for (const Geom *g : gs) nt += tiles_for(*g, TY);
-            if (nt <= G) {
-                *resident = true;
-                return TY;
-            }
+            if (tiles_for(g, TY) <= G) return TY;
         }
-    }
     for (int TY = 1; TY <= kMaxTY; ++TY) {
         const int G = mixed_grid(is3d, nzm, TY);
         if (G == 0) break;
-        long long nt = 0;
-        for (const Geom *g : gs) nt += tiles_for(*g, TY);
-        if (nt <= G) return TY;
+        if (tiles_for(g, TY) <= G) return TY;
     }
     int TY = (nzm == 32) ? 8 : 16;
     while (TY > 1 && mixed_grid(is3d, nzm, TY) == 0) --TY;
     return TY;
 }
 
+// A launch keeps the FP32 matrix in shared memory (2D only) when its tiles fit one per
+// co-resident CTA with the shared-memory layout of its tallest tile.
+static bool mixed_resident(bool is3d, int nzm, int TYmax, long long ntiles) {
+    if (is3d) return false;
+    const int G = mixed_grid(is3d, nzm, TYmax, true);
+    return G > 0 && ntiles <= G;
+}
+
 // Allocate and fill the FP32 copy of the matrix, the preconditioner factors and, for tile
 // height TY, the tile slot maps and partial sums.
 static int mixed_prepare(Solver &sv, int precond, int TY) {
     if (sv.g.nz > kMixedMaxNz) return fail(CISMGPU_EUNSUPPORTED, "mixed solver supports nz <= 32");
+    if (8LL * sv.nvec >= (1LL << 31))  // the kernel indexes vector planes with 32-bit offsets
+        return fail(CISMGPU_EUNSUPPORTED, "mixed solver supports nz*(nx-1)*(ny-1) < 2^28");
     if (!(precond == 0 || precond == 1 || (precond == 2 && sv.is3d)))
         return fail(CISMGPU_EUNSUPPORTED, "mixed solver preconditioners: 0, 1, or 2 (3D only)");
     MixedBufs &m = sv.mixed;
@@ -559,7 +562,7 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
         CU(alloc((void **)&m.vec, (size_t)16 * nvec * sizeof(float)));
         CU(alloc((void **)&m.state, sizeof(MState)));
         CU(alloc((void **)&m.desc, sizeof(MDesc)));
-        CU(alloc((void **)&m.bar, sizeof(GridBar)));
+        CU(alloc((void **)&m.ctl, sizeof(MCtl)));
         m.nbytes = bytes;
         m.shape_nvec = nvec;
         m.shape_nc = NC;
@@ -580,13 +583,13 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
         const int ntiles = tiles_for(g, TY);
         const int NS = (kTX + 2) * (TY + 2);
         if (ntiles > m.ntiles_cap || (long long)ntiles * NS > m.maps_cap) {
-            if (m.partials) cudaFree(m.partials);
+            if (m.recs) cudaFree(m.recs);
             if (m.maps) cudaFree(m.maps);
             if (m.tiles) cudaFree(m.tiles);
-            m.partials = nullptr;
+            m.recs = nullptr;
             m.maps = nullptr;
             m.tiles = nullptr;
-            CU(cudaMalloc((void **)&m.partials, (size_t)ntiles * 2 * 3 * sizeof(DD)));
+            CU(cudaMalloc((void **)&m.recs, (size_t)ntiles * 2 * sizeof(TileRec)));
             CU(cudaMalloc((void **)&m.maps, (size_t)ntiles * NS * sizeof(int)));
             CU(cudaMalloc((void **)&m.tiles, (size_t)ntiles * sizeof(MTile)));
             m.ntiles_cap = ntiles;
@@ -594,7 +597,7 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
         }
         m.ntiles = ntiles;
         const MDesc D = mixed_desc(sv, precond, TY);
-        k_slot_maps<<<nblocks((long long)ntiles * NS), kBlock, 0, sv.stream>>>(D, TY, m.maps);
+        k_slot_maps<<<nblocks((long long)ntiles * NS), kBlock, 0, sv.stream>>>(D, m.maps);
         CU(cudaGetLastError());
         std::vector<MTile> tl(ntiles);
         for (int t = 0; t < ntiles; ++t) tl[t] = MTile{0, t};
@@ -634,12 +637,13 @@ static int mixed_reset(Solver &sv, cudaStream_t s) {
     k_halo<<<nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4)), kBlock, 0, s>>>(sv.g, p.xu, p.xv, nullptr);
     CU(cudaGetLastError());
     CU(cudaMemsetAsync(sv.mixed.vec, 0, (size_t)16 * sv.nvec * sizeof(float), s));
+    CU(cudaMemsetAsync(sv.mixed.recs, 0, (size_t)sv.mixed.ntiles * 2 * sizeof(TileRec), s));  // tags restart at 1
     return CISMGPU_OK;
 }
 
 template <int NC, int NZM>
 static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_tiles, int ntiles, int TY,
-                        int resident, GridBar *d_bar, int max_steps, cudaStream_t s,
+                        int resident, MCtl *d_ctl, int max_steps, cudaStream_t s,
                         const std::vector<MTile> *host_tiles) {
     const size_t smem = MLayout<NC, NZM>(TY, resident != 0).bytes();
     int grid = mixed_grid(NC == 27, NZM, TY, resident != 0);
@@ -654,17 +658,17 @@ static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_t
                 if (std::find(seen.begin(), seen.end(), sv) == seen.end()) seen.push_back(sv);
             }
             if ((int)seen.size() > kMaxCtaSolves)
-                return fail(CISMGPU_EUNSUPPORTED, "batch too fragmented for one launch (solves per CTA > 32)");
+                return fail(CISMGPU_EUNSUPPORTED, "batch too fragmented for one launch (solves per CTA > 64)");
         }
     }
     void *args[] = {(void *)&d_descs, (void *)&d_states, (void *)&d_tiles, (void *)&ntiles, (void *)&TY,
-                    (void *)&resident, (void *)&d_bar, (void *)&max_steps};
+                    (void *)&resident, (void *)&d_ctl, (void *)&max_steps};
     CU(cudaLaunchCooperativeKernel((const void *)k_mixed<NC, NZM>, dim3(grid), dim3(kBlock), args, smem, s));
     return CISMGPU_OK;
 }
 
 static int mixed_dispatch(bool is3d, int nzm, const MDesc *d, MState *st, const MTile *t, int nt, int TY,
-                          bool resident, GridBar *bar, int max_steps, cudaStream_t s,
+                          bool resident, MCtl *bar, int max_steps, cudaStream_t s,
                           const std::vector<MTile> *host_tiles = nullptr) {
     const int res = resident ? 1 : 0;
     if (!is3d) return mixed_launch<9, 1>(d, st, t, nt, TY, res, bar, max_steps, s, host_tiles);
@@ -685,20 +689,19 @@ template <int NCC>
 int Solver::run_mixed(int precond, int ncheck, double tol, int maxiters) {
     trace("run_mixed: begin");
     const int nzm = mixed_nzm(g, is3d);
-    bool resident = false;
-    const int TY = mixed_choose_ty({&g}, is3d, nzm, &resident);
+    const int TY = mixed_solve_ty(g, is3d, nzm);
     trace("run_mixed: tile height chosen");
     TRY(mixed_prepare(*this, precond, TY));
     trace("run_mixed: prepared");
     TRY(mixed_reset(*this, stream));
     trace("run_mixed: reset enqueued");
     MixedBufs &m = mixed;
+    const bool resident = mixed_resident(is3d, nzm, TY, m.ntiles);
     const MDesc D = mixed_desc(*this, precond, TY);
     const MState S0 = mixed_init_state(tol, maxiters, ncheck);
-    GridBar B{0u, 0u, 0, 1};
     CU(cudaMemcpyAsync(m.desc, &D, sizeof(MDesc), cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(m.state, &S0, sizeof(MState), cudaMemcpyHostToDevice, stream));
-    CU(cudaMemcpyAsync(m.bar, &B, sizeof(GridBar), cudaMemcpyHostToDevice, stream));
+    CU(cudaMemsetAsync(m.ctl, 0, sizeof(MCtl), stream));
     const int max_steps = 4 * maxiters + 16;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (prof) {
@@ -707,10 +710,10 @@ int Solver::run_mixed(int precond, int ncheck, double tol, int maxiters) {
         CU(cudaEventRecord(e0, stream));
     }
     trace("run_mixed: descriptors copied");
-    TRY(mixed_dispatch(is3d, nzm, m.desc, m.state, m.tiles, m.ntiles, TY, resident, m.bar, max_steps, stream));
+    TRY(mixed_dispatch(is3d, nzm, m.desc, m.state, m.tiles, m.ntiles, TY, resident, m.ctl, max_steps, stream));
     trace("run_mixed: kernel launched");
     if (prof) CU(cudaEventRecord(e1, stream));
-    k_mstate_to_solve<<<1, 1, 0, stream>>>(m.state, state.as<SolveState>(), m.bar);
+    k_mstate_to_solve<<<1, 1, 0, stream>>>(m.state, state.as<SolveState>(), m.ctl);
     CU(cudaGetLastError());
     last_ty = TY;
     if (prof) {
@@ -1018,13 +1021,18 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
             return fail(CISMGPU_EINVAL, "batch members must share dims and the nz class (<=16 or <=32)");
         geoms.push_back(&sv.g);
     }
-    bool resident = false;
-    const int TY = mixed_choose_ty(geoms, s0.is3d, nzm, &resident);
+    std::vector<int> tys(n);
+    int TYmax = 1;
+    long long ntot = 0;
     for (int t = 0; t < n; ++t) {
         Solver &sv = solvers[t]->sv;
-        TRY(mixed_prepare(sv, precond, TY));
+        tys[t] = mixed_solve_ty(sv.g, sv.is3d, nzm);
+        TYmax = std::max(TYmax, tys[t]);
+        ntot += tiles_for(sv.g, tys[t]);
+        TRY(mixed_prepare(sv, precond, tys[t]));
         TRY(mixed_reset(sv, sv.stream));
     }
+    const bool resident = mixed_resident(s0.is3d, nzm, TYmax, ntot);
     for (int t = 0; t < n; ++t) CU(cudaStreamSynchronize(solvers[t]->sv.stream));
     cudaStream_t s = cuda_stream ? (cudaStream_t)cuda_stream : s0.stream;
     // one descriptor, state and tile list for the whole batch
@@ -1032,27 +1040,26 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
     std::vector<MState> states(n, mixed_init_state(tolerance, maxiters, linear_solve_ncheck));
     std::vector<MTile> tiles;
     for (int t = 0; t < n; ++t) {
-        descs[t] = mixed_desc(solvers[t]->sv, precond, TY);
+        descs[t] = mixed_desc(solvers[t]->sv, precond, tys[t]);
         for (int k = 0; k < descs[t].ntiles; ++k) tiles.push_back(MTile{t, k});
     }
     // tiles in (solve, tile) order; CTAs take them round robin, so a solve's tiles spread over
     // consecutive CTAs and each CTA holds tiles of only a few solves
-    GridBar B{0u, 0u, 0, n};
     void *dmem = nullptr;
     const size_t off_s = ((n * sizeof(MDesc)) + 255) / 256 * 256;
     const size_t off_t = off_s + ((n * sizeof(MState)) + 255) / 256 * 256;
     const size_t off_b = off_t + ((tiles.size() * sizeof(MTile)) + 255) / 256 * 256;
-    CU(cudaMallocAsync(&dmem, off_b + sizeof(GridBar), s));
+    CU(cudaMallocAsync(&dmem, off_b + sizeof(MCtl), s));
     char *base = static_cast<char *>(dmem);
     MDesc *d_descs = reinterpret_cast<MDesc *>(base);
     MState *d_states = reinterpret_cast<MState *>(base + off_s);
     MTile *d_tiles = reinterpret_cast<MTile *>(base + off_t);
-    GridBar *d_bar = reinterpret_cast<GridBar *>(base + off_b);
+    MCtl *d_bar = reinterpret_cast<MCtl *>(base + off_b);
     CU(cudaMemcpyAsync(d_descs, descs.data(), n * sizeof(MDesc), cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(d_states, states.data(), n * sizeof(MState), cudaMemcpyHostToDevice, s));
     CU(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(MTile), cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(d_bar, &B, sizeof(GridBar), cudaMemcpyHostToDevice, s));
-    int rc = mixed_dispatch(s0.is3d, nzm, d_descs, d_states, d_tiles, (int)tiles.size(), TY, resident, d_bar,
+    CU(cudaMemsetAsync(d_bar, 0, sizeof(MCtl), s));
+    int rc = mixed_dispatch(s0.is3d, nzm, d_descs, d_states, d_tiles, (int)tiles.size(), TYmax, resident, d_bar,
                             4 * maxiters + 16, s, &tiles);
     if (rc) {
         cudaFreeAsync(dmem, s);
@@ -1062,8 +1069,8 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
         k_mstate_to_solve<<<1, 1, 0, s>>>(d_states + t, solvers[t]->sv.state.as<SolveState>(), d_bar);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(states.data(), d_states, n * sizeof(MState), cudaMemcpyDeviceToHost, s));
-    GridBar hb;
-    CU(cudaMemcpyAsync(&hb, d_bar, sizeof(GridBar), cudaMemcpyDeviceToHost, s));
+    MCtl hb;
+    CU(cudaMemcpyAsync(&hb, d_bar, sizeof(MCtl), cudaMemcpyDeviceToHost, s));
     CU(cudaFreeAsync(dmem, s));
     CU(cudaStreamSynchronize(s));
     int first = CISMGPU_OK;

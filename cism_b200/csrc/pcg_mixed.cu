@@ -4,7 +4,7 @@
 // pcg_solver_chrongear_* (glissade_velo_higher_pcg.F90:3296-3581) with the
 // matrix, z, d, q, Az and the recursive residual r stored and multiplied in FP32,
 // the solution x accumulated in FP64, every dot product accumulated in FP64
-// double-double, and the reference's periodic residual replacement
+// (double-double across tiles), and the reference's periodic residual replacement
 // (:3482-3579) done in FP64: at every check iteration r = b - A x is computed
 // with the FP64 matrix, the FP64 norm gives err, and the FP32 recurrences
 // continue from the true residual (a "reliable update": the Krylov directions
@@ -13,16 +13,19 @@
 //
 // Execution: one cooperative persistent kernel runs any number of independent
 // solves (a batch, or the slots of the serving loop).  The owned vertices of each
-// solve are cut into tiles of TX x TY columns; a CTA processes tiles round robin.
-// Per step a tile computes, for its columns and a one-column halo ring, the
-// pointwise update of iteration i and the preconditioner of iteration i+1 (the
-// halo values are recomputed from the previous step's vectors, which is why r, q
-// and Az are double buffered), then the FP32 stencil product of iteration i+1 and
-// the tile's partial dot products.  The last CTA to finish a solve's tiles in a
-// step reduces that solve's partials with a fixed tree and advances the solve's
-// state machine, so every solve needs exactly one grid barrier per iteration and
-// its results do not depend on which CTA ran which tile or on what else is in the
-// batch.  Grid barriers spin with a clock64 limit and report CISMGPU_ETIMEOUT.
+// solve are cut into tiles of kTX x TY columns (TY fixed per solve); a CTA
+// processes tiles round robin.  Per step a tile computes, for its columns and a
+// one-column halo ring, the pointwise update of iteration i and the
+// preconditioner of iteration i+1 (the halo values are recomputed from the
+// previous step's vectors, which is why r, q and Az are double buffered), then the
+// FP32 stencil product of iteration i+1 and the tile's partial dot products, and
+// publishes them in a record stamped with the solve's step number.  There is no
+// grid barrier: before its next step every CTA holding a tile of a solve waits
+// for all of that solve's records of the step, and sums them in one fixed order,
+// so all CTAs advance identical copies of the solve's scalars, a solve never waits
+// for another solve, and its results do not depend on which CTA ran which tile or
+// on what else is in the launch.  Every wait is bounded (clock64) and reports
+// CISMGPU_ETIMEOUT.
 #pragma once
 
 #include "common.cuh"
@@ -33,11 +36,18 @@ constexpr int kMixedMaxNz = 32;                  // shared-memory bound of the m
 
 enum MStep { MS_INIT = 0, MS_A, MS_MERGED, MS_B, MS_CHECK, MS_DONE };
 
+// A tile's partial sums of one step, stamped with the step number (tag) last.
+struct TileRec {
+    double p0, p1, p2;
+    unsigned tag, pad;
+};
+
 // device-visible description of one solve
 struct MDesc {
     Geom g;
     int NC;          // 27 (3D) or 9 (2D)
     int precond;     // 0 none, 1 diag, 2 sia
+    int TY;          // tile height of this solve
     int tiles_x, tiles_y, ntiles;
     const float *A32;    // [4][NC][nz][NQ]
     const double *A64;   // [4][NC][nz][NQ]
@@ -47,7 +57,7 @@ struct MDesc {
     double *x;           // [2][nz][NQ]
     float *r[2], *q[2], *Az[2];  // [2][nz][NQ] each (u, v planes)
     float *z, *d;                // [2][nz][NQ]
-    DD *partials;        // [ntiles][2 step parities][3]
+    TileRec *recs;       // [ntiles][2 step parities]
     const int *maps;     // [ntiles][(kTX+2)*(TY+2)] slot maps (k_slot_maps)
 };
 
@@ -58,16 +68,14 @@ struct MState {
     int maxiters, ncheck;
     int done, status, niters;
     int checks, fp32_matvecs, fp64_matvecs;
-    unsigned ticket;
+    unsigned tick;       // steps completed (the tag of the last records summed)
 };
 
 struct MTile { int solve, tile; };
 
-struct GridBar {
-    unsigned count;
-    unsigned gen;
-    int abort;          // set on a barrier timeout; every CTA leaves at its next wait
-    int n_active;       // solves not yet done
+struct MCtl {
+    int abort;          // set on a wait timeout; every CTA leaves at its next wait
+    int pad[3];
 };
 
 // ---------------------------------------------------------------------------
@@ -101,44 +109,23 @@ __device__ __forceinline__ bool live_col(const MDesc &D, int i, int j, long long
     return owned(D.g, i, j) && D.act[q] != 0 && !zero_pos(D.g, i, j);
 }
 
-__device__ bool grid_barrier(GridBar *bar, unsigned nblocks) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ok = 1;
-        volatile unsigned *vgen = &bar->gen;
-        volatile int *vabort = &bar->abort;
-        const unsigned gen = *vgen;
-        __threadfence();
-        const unsigned arrived = atomicAdd(&bar->count, 1u);
-        if (arrived == nblocks - 1) {
-            bar->count = 0u;
-            __threadfence();
-            atomicAdd(&bar->gen, 1u);
-        } else {
-            const long long t0 = clock64();
-            while (*vgen == gen) {
-                if (*vabort) { ok = 0; break; }
-                if (clock64() - t0 > (1LL << 32)) {  // ~2 s at 2 GHz: give up, report
-                    atomicExch(&bar->abort, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return ok != 0;
-}
-
 __device__ __forceinline__ bool is_check_it(int iter, int ncheck) { return (iter % ncheck == 0) || iter == 5; }
 
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+constexpr long long kWaitCycles = 1LL << 31;  // ~1 s at 2 GHz: a wait longer than this is a failure
+
 // ---------------------------------------------------------------------------
-// per-solve state machine, run by the last CTA of a step (thread 0)
+// per-solve state machine, run by thread 0 of every CTA holding the solve
 // ---------------------------------------------------------------------------
-__device__ void advance_state(MState &S, const MDesc &D, double S0, double S1, double S2) {
+__device__ void advance_state(MState &S, double S0, double S1, double S2) {
     switch (S.step) {
     case MS_INIT:  // S0 = (b,b), S1 = (r,r) of r = b - A x0
         S.L2_rhs = sqrt(S0);
@@ -214,11 +201,12 @@ __device__ void advance_state(MState &S, const MDesc &D, double S0, double S1, d
 // tile work
 // ---------------------------------------------------------------------------
 // Tiles are kTX columns wide (one warp per tile row: coalesced 128-byte FP32 rows) and
-// TY rows high; TY is chosen per launch by the host (mixed_choose_ty) so that a solve has
-// no more tiles than there are co-resident CTAs.
+// TY rows high; TY is chosen per solve by the host (mixed_solve_ty).
 constexpr int kTX = 32;
-constexpr int kMaxCtaSolves = 32;  // distinct solves whose tiles one CTA may hold in a launch
+constexpr int kMaxCtaSolves = 64;  // distinct solves whose tiles one CTA may hold in a launch
 constexpr int kMaxTY = 64;
+constexpr int kCh2 = 4;            // stencil items per load batch
+constexpr int kChR = 4;            // FP64 residual items per load batch
 
 struct MHead {
     MDesc D;                   // descriptor of the current tile's solve
@@ -228,12 +216,12 @@ struct MHead {
     int nsolve;
     int cur;                   // cache slot described by D
     double red[8][3];
+    DD rdd[8][3];
 };
 
-// Dynamic shared memory: head | map[NS] | z[2][KP][NS] | rt[2][NZM][NT] | stage[kStage] DD
-//                        | (resident launches) A[4][NC][NT] FP32 matrix of the CTA's tile
-constexpr int kStage = 2 * kBlock;  // tile partials staged for the cross-tile sum (per field chunk)
-
+// Dynamic shared memory: head | map[NS] | z[2][KP][NS] | rt[2][NZM][NT]
+//                        | (resident launches) A[4][NC][NZM*NT] FP32 matrix of the CTA's tile
+// sized for the launch's largest tile height.
 template <int NC, int NZM>
 struct MLayout {
     static constexpr int KP = (NC == 27) ? NZM + 2 : 1;  // z levels with a zero row above and below
@@ -243,8 +231,7 @@ struct MLayout {
     __host__ __device__ size_t off_map() const { return (sizeof(MHead) + 15) / 16 * 16; }
     __host__ __device__ size_t off_z() const { return (off_map() + 4 * (size_t)NS + 15) / 16 * 16; }
     __host__ __device__ size_t off_rt() const { return off_z() + 4 * (size_t)2 * KP * NS; }
-    __host__ __device__ size_t off_stage() const { return (off_rt() + 4 * (size_t)2 * NZM * NT + 15) / 16 * 16; }
-    __host__ __device__ size_t off_A() const { return off_stage() + sizeof(DD) * kStage; }
+    __host__ __device__ size_t off_A() const { return (off_rt() + 4 * (size_t)2 * NZM * NT + 15) / 16 * 16; }
     __host__ __device__ size_t bytes() const {
         return off_A() + (resA ? 4 * (size_t)4 * NC * NZM * NT : 0);
     }
@@ -281,7 +268,8 @@ __device__ __forceinline__ int map_src(int v) { return (v >> 2) - 1; }
 __device__ __forceinline__ bool map_live(int v) { return (v & 1) != 0; }
 __device__ __forceinline__ bool map_mine(int v) { return (v & 2) != 0; }
 
-__global__ void k_slot_maps(MDesc D, int TY, int *maps) {
+__global__ void k_slot_maps(MDesc D, int *maps) {
+    const int TY = D.TY;
     const int NS = (kTX + 2) * (TY + 2);
     const long long id = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (id >= (long long)D.ntiles * NS) return;
@@ -307,22 +295,22 @@ __global__ void k_slot_maps(MDesc D, int TY, int *maps) {
 // row stride NS; level k at row k+1), FP32.  The column's factors are loaded in one
 // batch first: a load inside the recurrence would cost a memory round trip per level.
 template <int NZM>
-__device__ __forceinline__ void sia_col(const MDesc &D, float *zc, int NS, int s, long long q) {
+__device__ __forceinline__ void sia_col(const MDesc &D, float *zc, int NS, int s, int q) {
     const int nz = D.g.nz;
-    const long long NQ = D.g.NQ;
-    const long long plane = (long long)nz * NQ;
+    const int NQ = (int)D.g.NQ;
+    const int plane = nz * NQ;
     constexpr int KP = NZM + 2;
     for (int c = 0; c < 2; ++c) {
-        float *z = zc + (size_t)c * KP * NS + NS + s;  // z[k * NS] is level k
+        float *z = zc + c * KP * NS + NS + s;  // z[k * NS] is level k
         const float *ib = D.pre + (c * 3 + 0) * plane, *sb = D.pre + (c * 3 + 1) * plane,
                     *gm = D.pre + (c * 3 + 2) * plane;
         float fib[NZM], fsb[NZM], fgm[NZM];
 #pragma unroll
         for (int k = 0; k < NZM; ++k) {
             const bool in = k < nz;
-            fib[k] = in ? __ldg(ib + (long long)k * NQ + q) : 0.0f;
-            fsb[k] = in ? __ldg(sb + (long long)k * NQ + q) : 0.0f;
-            fgm[k] = in ? __ldg(gm + (long long)k * NQ + q) : 0.0f;
+            fib[k] = in ? __ldg(ib + k * NQ + q) : 0.0f;
+            fsb[k] = in ? __ldg(sb + k * NQ + q) : 0.0f;
+            fgm[k] = in ? __ldg(gm + k * NQ + q) : 0.0f;
         }
         // forward: y_1 = r_1/beta_1; y_k = (r_k - sb_k y_{k-1})/beta_k; back: z_k = y_k - gamma_{k+1} z_{k+1}
         float prev = z[0] * fib[0];
@@ -330,35 +318,108 @@ __device__ __forceinline__ void sia_col(const MDesc &D, float *zc, int NS, int s
 #pragma unroll
         for (int k = 1; k < NZM; ++k)
             if (k < nz) {
-                prev = (z[(size_t)k * NS] - fsb[k] * prev) * fib[k];
-                z[(size_t)k * NS] = prev;
+                prev = (z[k * NS] - fsb[k] * prev) * fib[k];
+                z[k * NS] = prev;
             }
         float next = prev;
 #pragma unroll
         for (int k = NZM - 2; k >= 0; --k)
             if (k < nz - 1) {
-                next = z[(size_t)k * NS] - fgm[k + 1] * next;
-                z[(size_t)k * NS] = next;
+                next = z[k * NS] - fgm[k + 1] * next;
+                z[k * NS] = next;
             }
     }
 }
 
-// One tile of one solve for the solve's current step; writes the tile's partials.
+// FP64 r = b - A64 x on the tile (x read through the halo map); r32 = r on live columns.
+// Partials: p0 = (b,b), p1 = (r,r).  Loads of kChR items are issued before any store.
+template <int NC>
+__device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, int TY, int i0, int j0, int par,
+                                              double &p0, double &p1) {
+    const Geom &g = D.g;
+    const int nz = (NC == 27) ? g.nz : 1;
+    const int NQ = (int)g.NQ;
+    const int plane = nz * NQ;
+    const int NT = kTX * TY;
+    const double *__restrict__ Auu = D.A64;
+    const double *__restrict__ Auv = D.A64 + (size_t)NC * plane;
+    const double *__restrict__ Avu = D.A64 + (size_t)2 * NC * plane;
+    const double *__restrict__ Avv = D.A64 + (size_t)3 * NC * plane;
+    const double *__restrict__ xu = D.x;
+    const double *__restrict__ xv = D.x + plane;
+    float *__restrict__ ru32 = D.r[par];
+    float *__restrict__ rv32 = D.r[par] + plane;
+    const int nitems = NT * nz;
+#pragma unroll 1
+    for (int base = threadIdx.x; base < nitems; base += kChR * kBlock) {
+        double yu[kChR], yv[kChR], bu[kChR], bv[kChR];
+        int ee[kChR];
+        bool ok[kChR], lv[kChR];
+#pragma unroll
+        for (int u = 0; u < kChR; ++u) {
+            const int it = base + u * kBlock;
+            yu[u] = 0.0; yv[u] = 0.0; bu[u] = 0.0; bv[u] = 0.0;
+            ee[u] = 0; ok[u] = false; lv[u] = false;
+            if (it < nitems) {
+                const int col = it % NT, k = it / NT;
+                const int ti = col % kTX, tj = col / kTX;
+                const int i = i0 + ti, j = j0 + tj;
+                if (i <= g.ihi && j <= g.jhi) {
+                    const int q = j * g.NX + i;
+                    const int s = (ti + 1) + (kTX + 2) * (tj + 1);
+                    const int e = k * NQ + q;
+                    ok[u] = true;
+                    ee[u] = e;
+                    lv[u] = map_live(smap[s]);
+                    bu[u] = D.b[e];
+                    bv[u] = D.b[plane + e];
+                    if (D.act[q] != 0) {
+#pragma unroll
+                        for (int c = 0; c < NC; ++c) {
+                            const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
+                            const int sc = map_src(smap[s + iA + (kTX + 2) * jA]);
+                            if (k + kA < 0 || k + kA >= nz || sc < 0) continue;
+                            const int n = (k + kA) * NQ + sc;
+                            const size_t a = (size_t)c * plane + e;
+                            const double x1 = ldd(xu + n), x2 = ldd(xv + n);
+                            yu[u] = fma(Auu[a], x1, yu[u]);
+                            yu[u] = fma(Auv[a], x2, yu[u]);
+                            yv[u] = fma(Avu[a], x1, yv[u]);
+                            yv[u] = fma(Avv[a], x2, yv[u]);
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kChR; ++u) {
+            if (!ok[u]) continue;
+            const double ru = bu[u] - yu[u], rv = bv[u] - yv[u];
+            p1 += ru * ru + rv * rv;
+            p0 += bu[u] * bu[u] + bv[u] * bv[u];
+            ru32[ee[u]] = lv[u] ? (float)ru : 0.0f;
+            rv32[ee[u]] = lv[u] ? (float)rv : 0.0f;
+        }
+    }
+}
+
+// One tile of one solve for the solve's current step; publishes the tile's record.
 template <int NC, int NZM>
-__device__ void tile_step(const MState &S, int tile, int pbuf, int TY, bool resident, MHead &hd, unsigned char *smem) {
+__device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, MHead &hd, unsigned char *smem) {
     using LY = MLayout<NC, NZM>;
     constexpr int KP = LY::KP;
     constexpr int OFF = (NC == 27) ? 1 : 0;  // z row of level 0
-    const LY ly(TY, resident);
-    const int NS = ly.NS, NT = ly.NT;
+    const LY ly(TYmax, resident);
+    const MDesc &D = hd.D;
+    const int TY = D.TY;
+    const int NS = (kTX + 2) * (TY + 2), NT = kTX * TY;
     int *smap = reinterpret_cast<int *>(smem + ly.off_map());
     float *sz = reinterpret_cast<float *>(smem + ly.off_z());   // [2][KP][NS]
     float *srt = reinterpret_cast<float *>(smem + ly.off_rt()); // [2][NZM][NT]
-    const MDesc &D = hd.D;
     const Geom &g = D.g;
     const int nz = (NC == 27) ? g.nz : 1;
-    const long long NQ = g.NQ;
-    const long long plane = (long long)nz * NQ;
+    const int NQ = (int)g.NQ;
+    const int plane = nz * NQ;
     const int tx = tile % D.tiles_x, ty = tile / D.tiles_x;
     const int i0 = g.ilo + tx * kTX, j0 = g.jlo + ty * TY;
     const int t = threadIdx.x;
@@ -367,50 +428,13 @@ __device__ void tile_step(const MState &S, int tile, int pbuf, int TY, bool resi
     double p0 = 0.0, p1 = 0.0, p2 = 0.0;
 
     if (!resident) {  // resident launches keep their single tile's map for the whole launch
-        const int *tmap = D.maps + (long long)tile * NS;
+        const int *tmap = D.maps + (size_t)tile * NS;
         for (int sl = t; sl < NS; sl += kBlock) smap[sl] = tmap[sl];
         __syncthreads();
     }
 
     if (step == MS_INIT || step == MS_CHECK) {
-        // r = b - A64 x (FP64, x read through the halo map); r32 = r on live columns
-        const double *Auu = D.A64, *Auv = D.A64 + NC * plane, *Avu = D.A64 + 2 * NC * plane,
-                     *Avv = D.A64 + 3 * NC * plane;
-        const double *xu = D.x, *xv = D.x + plane;
-        const int nitems = NT * nz;
-        for (int it = t; it < nitems; it += kBlock) {
-            const int col = it % NT, k = it / NT;
-            const int ti = col % kTX, tj = col / kTX;
-            const int i = i0 + ti, j = j0 + tj;
-            if (i > g.ihi || j > g.jhi) continue;
-            const long long q = (long long)j * g.NX + i;
-            const int s = (ti + 1) + (kTX + 2) * (tj + 1);
-            const bool on = D.act[q] != 0;
-            const bool live = map_live(smap[s]);
-            const long long e = (long long)k * NQ + q;
-            double yu = 0.0, yv = 0.0;
-            if (on) {
-#pragma unroll
-                for (int c = 0; c < NC; ++c) {
-                    const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
-                    const int sc = map_src(smap[s + iA + (kTX + 2) * jA]);
-                    if (k + kA < 0 || k + kA >= nz || sc < 0) continue;
-                    const long long n = (long long)(k + kA) * NQ + sc;
-                    const long long a = (long long)c * plane + e;
-                    const double x1 = ldd(xu + n), x2 = ldd(xv + n);
-                    yu = fma(Auu[a], x1, yu);
-                    yu = fma(Auv[a], x2, yu);
-                    yv = fma(Avu[a], x1, yv);
-                    yv = fma(Avv[a], x2, yv);
-                }
-            }
-            const double bu = D.b[e], bv = D.b[plane + e];
-            const double ru = bu - yu, rv = bv - yv;
-            p1 += ru * ru + rv * rv;
-            p0 += bu * bu + bv * bv;
-            D.r[par][e] = live ? (float)ru : 0.0f;
-            D.r[par][plane + e] = live ? (float)rv : 0.0f;
-        }
+        residual_pass<NC>(D, smap, TY, i0, j0, par, p0, p1);
         if (step == MS_CHECK) { p0 = p1; p1 = 0.0; }
     } else {
         const float alpha = (float)S.alpha, beta = (float)S.beta;
@@ -418,54 +442,104 @@ __device__ void tile_step(const MState &S, int tile, int pbuf, int TY, bool resi
         const bool do_b = (step == MS_MERGED || step == MS_B);
         const bool do_a = (step == MS_MERGED || step == MS_A);
         const int rin = par, rout = do_b ? (par ^ 1) : par;  // buffers holding r_i / r_{i+1}
+        const float *__restrict__ q_in = D.q[rin];
+        const float *__restrict__ az_in = D.Az[rin];
+        const float *__restrict__ r_in = D.r[rin];
+        float *__restrict__ q_out = D.q[rout];
+        float *__restrict__ r_out = D.r[rout];
+        float *__restrict__ dvec = D.d;
+        const float *__restrict__ zvec = D.z;
+        double *__restrict__ xvec = D.x;
+        const float *__restrict__ dinv = D.pre;
+        const bool diag = D.precond == 1;
 
         // ---- pass 1: update (B) on the tile, new residual (and diag z) on tile + halo ----
-        const int n1 = 2 * NS;
-        for (int k = 0; k < nz; ++k) {
-#pragma unroll 4
-            for (int it = t; it < n1; it += kBlock) {
-                const int c = it >= NS ? 1 : 0, sl = it - c * NS;
-                const int v = smap[sl];
-                const int m = map_live(v) ? map_src(v) : -1;
+        // items (k, c, slot) in the order k, c, slot; kCh1 items' loads are issued together
+        constexpr int kCh1 = (NC == 27) ? 4 : 6;  // items per load batch (register budget)
+        const int per_k = 2 * NS;
+        const int n1 = per_k * nz;
+#pragma unroll 1
+        for (int base = t; base < n1; base += kCh1 * kBlock) {
+            float qo[kCh1], az[kCh1], ro[kCh1], dold[kCh1], zold[kCh1], pr[kCh1];
+            double xold[kCh1];
+            int ee[kCh1], vv[kCh1], ss[kCh1], sr[kCh1];
+            int k = base / per_k;
+            int rem = base - k * per_k;
+#pragma unroll
+            for (int u = 0; u < kCh1; ++u) {
+                if (u > 0) {
+                    rem += kBlock;
+                    while (rem >= per_k) { rem -= per_k; ++k; }
+                }
+                ss[u] = -1;
+                sr[u] = -1;
+                vv[u] = 0;
+                ee[u] = 0;
+                qo[u] = az[u] = ro[u] = dold[u] = zold[u] = 0.0f;
+                pr[u] = 1.0f;
+                xold[u] = 0.0;
+                if (k < nz) {
+                    const int c = rem >= NS ? 1 : 0, sl = rem - c * NS;
+                    ss[u] = (c * KP + k + OFF) * NS + sl;  // the item's z slot in smem
+                    const int li = sl % (kTX + 2), lj = sl / (kTX + 2);
+                    if (li >= 1 && li <= kTX && lj >= 1 && lj <= TY)  // tile column: keep r for the dots
+                        sr[u] = (c * NZM + k) * NT + (li - 1) + kTX * (lj - 1);
+                    const int v = smap[sl];
+                    vv[u] = v;
+                    const int m = map_live(v) ? map_src(v) : -1;
+                    if (m >= 0) {
+                        const int e = c * plane + k * NQ + m;
+                        ee[u] = e;
+                        if (do_b) {
+                            qo[u] = ldf(q_in + e);
+                            az[u] = ldf(az_in + e);
+                            ro[u] = ldf(r_in + e);
+                            if (map_mine(v)) {
+                                dold[u] = ldf(dvec + e);
+                                zold[u] = ldf(zvec + e);
+                                xold[u] = ldd(xvec + e);
+                            }
+                        } else {
+                            ro[u] = ldf(r_in + e);
+                        }
+                        if (do_a && diag) pr[u] = __ldg(dinv + e);
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kCh1; ++u) {
+                if (ss[u] < 0) continue;
+                const int v = vv[u];
+                const bool live = map_live(v);
                 float rn = 0.0f;
-                if (m >= 0) {
-                    const long long e = c * plane + (long long)k * NQ + m;
+                if (live) {
+                    const int e = ee[u];
                     if (do_b) {
-                        // the owner's d, z, x are loaded with the halo values (one round trip);
-                        // every live slot maps to an owned column, so the addresses are valid
-                        const float qo = ldf(D.q[rin] + e), az = ldf(D.Az[rin] + e), ro = ldf(D.r[rin] + e);
-                        const bool mine = map_mine(v);
-                        const float dold = mine ? D.d[e] : 0.0f, zold = mine ? D.z[e] : 0.0f;
-                        const double xold = mine ? D.x[e] : 0.0;
-                        const float qn = fmaf(beta, qo, az);  // q_i = Az_i + beta q_{i-1}
-                        rn = fmaf(-alpha, qn, ro);             // r_{i+1} = r_i - alpha q_i
-                        if (mine) {
-                            const float dn = fmaf(beta, dold, zold);  // d_i = z_i + beta d_{i-1}
-                            D.d[e] = dn;
-                            D.q[rout][e] = qn;
-                            D.r[rout][e] = rn;
-                            D.x[e] = fma(alpha64, (double)dn, xold);  // x += alpha d_i (FP64)
+                        const float qn = fmaf(beta, qo[u], az[u]);  // q_i = Az_i + beta q_{i-1}
+                        rn = fmaf(-alpha, qn, ro[u]);              // r_{i+1} = r_i - alpha q_i
+                        if (map_mine(v)) {
+                            const float dn = fmaf(beta, dold[u], zold[u]);  // d_i = z_i + beta d_{i-1}
+                            dvec[e] = dn;
+                            q_out[e] = qn;
+                            r_out[e] = rn;
+                            xvec[e] = fma(alpha64, (double)dn, xold[u]);  // x += alpha d_i (FP64)
                         }
                     } else {
-                        rn = ldf(D.r[rin] + e);
+                        rn = ro[u];
                     }
                 }
                 if (do_a) {
-                    const int li = sl % (kTX + 2), lj = sl / (kTX + 2);
-                    if (li >= 1 && li <= kTX && lj >= 1 && lj <= TY)
-                        srt[((size_t)c * NZM + k) * NT + (li - 1) + kTX * (lj - 1)] = rn;
-                    float zv = rn;
-                    if (D.precond == 1 && m >= 0) zv = rn * __ldg(D.pre + c * plane + (long long)k * NQ + m);
-                    sz[((size_t)c * KP + k + OFF) * NS + sl] = zv;
+                    if (sr[u] >= 0) srt[sr[u]] = rn;
+                    sz[ss[u]] = (diag && live) ? rn * pr[u] : rn;
                 }
             }
         }
         if (do_a) {
             if (NC == 27) {  // zero padding rows (levels -1 and nz)
-                for (int it = t; it < n1; it += kBlock) {
+                for (int it = t; it < 2 * NS; it += kBlock) {
                     const int c = it >= NS ? 1 : 0, sl = it - c * NS;
-                    sz[((size_t)c * KP + 0) * NS + sl] = 0.0f;
-                    sz[((size_t)c * KP + nz + 1) * NS + sl] = 0.0f;
+                    sz[(c * KP + 0) * NS + sl] = 0.0f;
+                    sz[(c * KP + nz + 1) * NS + sl] = 0.0f;
                 }
             }
             __syncthreads();
@@ -480,137 +554,177 @@ __device__ void tile_step(const MState &S, int tile, int pbuf, int TY, bool resi
             // ---- pass 2: Az = A z on (column, level) items, z to HBM, partial dots ----
             // Couplings that leave the grid are zero in the FP32 copy and the padded z rows
             // and out-of-grid halo slots are zero, so every node sums all NC terms.
-            const float *Auu = D.A32, *Auv = D.A32 + NC * plane, *Avu = D.A32 + 2 * NC * plane,
-                        *Avv = D.A32 + 3 * NC * plane;
+            const float *__restrict__ Auu = D.A32;
+            const float *__restrict__ Auv = D.A32 + (size_t)NC * plane;
+            const float *__restrict__ Avu = D.A32 + (size_t)2 * NC * plane;
+            const float *__restrict__ Avv = D.A32 + (size_t)3 * NC * plane;
             const float *sA = reinterpret_cast<const float *>(smem + ly.off_A());  // [4][NC][nz*NT]
             const int NN = nz * NT;
-            float *Azu = D.Az[rout], *Azv = D.Az[rout] + plane;
-            const float *szu = sz, *szv = sz + (size_t)KP * NS;
-            const int nitems = NT * nz;
-#pragma unroll 2
-            for (int it = t; it < nitems; it += kBlock) {
-                const int col = it % NT, k = it / NT;
-                const int ti = col % kTX, tj = col / kTX;
-                const int i = i0 + ti, j = j0 + tj;
-                if (i > g.ihi || j > g.jhi) continue;
-                const int s = (ti + 1) + (kTX + 2) * (tj + 1);
-                const long long q = (long long)j * g.NX + i;
-                const long long e = (long long)k * NQ + q;
-                float yu = 0.0f, yv = 0.0f;
-                if (map_live(smap[s])) {
-                    if (resident) {
+            float *__restrict__ Azu = D.Az[rout];
+            float *__restrict__ Azv = D.Az[rout] + plane;
+            float *__restrict__ zu_out = D.z;
+            float *__restrict__ zv_out = D.z + plane;
+            const float *szu = sz, *szv = sz + KP * NS;
+#pragma unroll 1
+            for (int base = t; base < NN; base += kCh2 * kBlock) {
+                float yu[kCh2], yv[kCh2], zu[kCh2], zv[kCh2];
+                int ee[kCh2], cc[kCh2];
+                bool ok[kCh2];
 #pragma unroll
-                        for (int c = 0; c < NC; ++c) {
-                            const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
-                            const int zi = (k + OFF + kA) * NS + s + iA + (kTX + 2) * jA;
-                            const float zu = szu[zi], zv = szv[zi];
-                            const int a = c * NN + it;
-                            yu = fmaf(sA[a], zu, yu);
-                            yu = fmaf(sA[NC * NN + a], zv, yu);
-                            yv = fmaf(sA[2 * NC * NN + a], zu, yv);
-                            yv = fmaf(sA[3 * NC * NN + a], zv, yv);
-                        }
-                    } else {
+                for (int u = 0; u < kCh2; ++u) {
+                    const int it = base + u * kBlock;
+                    yu[u] = yv[u] = zu[u] = zv[u] = 0.0f;
+                    ok[u] = false;
+                    ee[u] = 0;
+                    cc[u] = 0;
+                    if (it < NN) {
+                        const int col = it % NT, k = it / NT;
+                        const int ti = col % kTX, tj = col / kTX;
+                        const int i = i0 + ti, j = j0 + tj;
+                        if (i <= g.ihi && j <= g.jhi) {
+                            const int s = (ti + 1) + (kTX + 2) * (tj + 1);
+                            const int e = k * NQ + j * g.NX + i;
+                            ok[u] = true;
+                            ee[u] = e;
+                            cc[u] = k * NT + col;
+                            zu[u] = szu[(k + OFF) * NS + s];
+                            zv[u] = szv[(k + OFF) * NS + s];
+                            if (map_live(smap[s])) {
+                                if (resident) {
 #pragma unroll
-                        for (int c = 0; c < NC; ++c) {
-                            const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
-                            const int zi = (k + OFF + kA) * NS + s + iA + (kTX + 2) * jA;
-                            const float zu = szu[zi], zv = szv[zi];
-                            const long long a = (long long)c * plane + e;
-                            yu = fmaf(__ldg(Auu + a), zu, yu);
-                            yu = fmaf(__ldg(Auv + a), zv, yu);
-                            yv = fmaf(__ldg(Avu + a), zu, yv);
-                            yv = fmaf(__ldg(Avv + a), zv, yv);
+                                    for (int c = 0; c < NC; ++c) {
+                                        const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
+                                        const int zi = (k + OFF + kA) * NS + s + iA + (kTX + 2) * jA;
+                                        const float z1 = szu[zi], z2 = szv[zi];
+                                        const int a = c * NN + it;
+                                        yu[u] = fmaf(sA[a], z1, yu[u]);
+                                        yu[u] = fmaf(sA[NC * NN + a], z2, yu[u]);
+                                        yv[u] = fmaf(sA[2 * NC * NN + a], z1, yv[u]);
+                                        yv[u] = fmaf(sA[3 * NC * NN + a], z2, yv[u]);
+                                    }
+                                } else {
+#pragma unroll
+                                    for (int c = 0; c < NC; ++c) {
+                                        const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
+                                        const int zi = (k + OFF + kA) * NS + s + iA + (kTX + 2) * jA;
+                                        const float z1 = szu[zi], z2 = szv[zi];
+                                        const size_t a = (size_t)c * plane + e;
+                                        yu[u] = fmaf(__ldg(Auu + a), z1, yu[u]);
+                                        yu[u] = fmaf(__ldg(Auv + a), z2, yu[u]);
+                                        yv[u] = fmaf(__ldg(Avu + a), z1, yv[u]);
+                                        yv[u] = fmaf(__ldg(Avv + a), z2, yv[u]);
+                                    }
+                                }
+                            }
                         }
                     }
                 }
-                Azu[e] = yu;
-                Azv[e] = yv;
-                const float zu = szu[(k + OFF) * NS + s], zv = szv[(k + OFF) * NS + s];
-                D.z[e] = zu;
-                D.z[plane + e] = zv;
-                const double ru = srt[(size_t)k * NT + col], rv = srt[((size_t)NZM + k) * NT + col];
-                p0 += ru * (double)zu + rv * (double)zv;
-                p1 += (double)yu * zu + (double)yv * zv;
-                p2 += ru * ru + rv * rv;
+#pragma unroll
+                for (int u = 0; u < kCh2; ++u) {
+                    if (!ok[u]) continue;
+                    const int e = ee[u];
+                    Azu[e] = yu[u];
+                    Azv[e] = yv[u];
+                    zu_out[e] = zu[u];
+                    zv_out[e] = zv[u];
+                    const double ru = srt[cc[u]], rv = srt[NZM * NT + cc[u]];
+                    p0 += ru * (double)zu[u] + rv * (double)zv[u];
+                    p1 += (double)yu[u] * zu[u] + (double)yv[u] * zv[u];
+                    p2 += ru * ru + rv * rv;
+                }
             }
         }
     }
     block_sum3(p0, p1, p2, hd.red);
     if (t == 0) {
-        DD *pp = D.partials + ((long long)tile * 2 + pbuf) * 3;
-        pp[0] = DD{p0, 0.0};
-        pp[1] = DD{p1, 0.0};
-        pp[2] = DD{p2, 0.0};
+        const unsigned tag = S.tick + 1u;
+        TileRec *rp = D.recs + 2 * (size_t)tile + (tag & 1u);
+        rp->p0 = p0;
+        rp->p1 = p1;
+        rp->p2 = p2;
+        __threadfence();
+        st_release(&rp->tag, tag);
     }
     __syncthreads();
 }
 
-// Reduce the partials (buffer pbuf) of every running solve this CTA holds and advance
-// its cached state.  All threads stage the tile partials in shared memory (one memory
-// round trip per kStage tiles); warp 0 sums them in double-double in a fixed order
-// (lane l takes tiles l, l+32, ...; then a shuffle tree).  Every CTA holding a solve does
-// this with the same inputs, so all copies of a solve's state stay bit-identical.  The
-// CTA holding tile 0 publishes a finished solve and decrements n_active before its next
-// barrier.
-__device__ void reduce_cached(MHead &hd, DD *stage, const MDesc *__restrict__ descs, int pbuf, MState *gstates,
-                              GridBar *bar) {
-    const int lane = threadIdx.x & 31;
+// Wait for the records of the step just taken by every running solve this CTA holds, sum
+// them and advance the solve's cached state.  All threads take part: thread t waits for and
+// accumulates tiles t, t+256, ... in double-double, then a fixed shuffle/warp tree.  Every
+// CTA holding a solve does this with the same inputs in the same order, so all copies of a
+// solve's state stay bit-identical.  The CTA holding tile 0 publishes a finished solve.
+// Returns false if a wait gave up (here or in another CTA).
+__device__ bool reduce_wait(MHead &hd, const MDesc *__restrict__ descs, MState *gstates, MCtl *ctl) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int cs = 0; cs < hd.nsolve; ++cs) {
         if (hd.st[cs].done) continue;  // uniform: only thread 0 writes st, before a barrier
         const MDesc &D = descs[hd.sid[cs]];
         const int ntl = D.ntiles;
-        const DD *P = D.partials;
+        const unsigned tag = hd.st[cs].tick + 1u;
+        const TileRec *R = D.recs + (tag & 1u);
         DD a0{0.0, 0.0}, a1{0.0, 0.0}, a2{0.0, 0.0};
-        const int chunk = kStage / 3 / 32 * 32;  // tiles per staging round, a multiple of 32
-        for (int base = 0; base < ntl; base += chunk) {
-            const int n = min(chunk, ntl - base);
-            __syncthreads();
-            for (int w = threadIdx.x; w < 3 * n; w += kBlock) {
-                const DD *pp = P + ((long long)(base + w / 3) * 2 + pbuf) * 3 + (w % 3);
-                DD v;
-                v.hi = __ldcg(&pp->hi);
-                v.lo = __ldcg(&pp->lo);
-                stage[w] = v;
-            }
-            __syncthreads();
-            if (threadIdx.x < 32)
-                for (int c = lane; c < n; c += 32) {
-                    a0 = dd_add(a0, stage[3 * c + 0]);
-                    a1 = dd_add(a1, stage[3 * c + 1]);
-                    a2 = dd_add(a2, stage[3 * c + 2]);
+        int bad = 0;
+        for (int w = threadIdx.x; w < ntl && !bad; w += kBlock) {
+            const TileRec *rp = R + 2 * (size_t)w;
+            if (ld_acquire(&rp->tag) != tag) {
+                const long long t0 = clock64();
+                unsigned spins = 0;
+                while (ld_acquire(&rp->tag) != tag) {
+                    __nanosleep(spins < 16 ? 20 : 100);
+                    if ((++spins & 31u) == 0) {
+                        if (*(volatile int *)&ctl->abort) { bad = 1; break; }
+                        if (clock64() - t0 > kWaitCycles) {
+                            atomicExch(&ctl->abort, 1);
+                            bad = 1;
+                            break;
+                        }
+                    }
                 }
+                if (bad) break;
+            }
+            a0 = dd_add_d(a0, __ldcg(&rp->p0));
+            a1 = dd_add_d(a1, __ldcg(&rp->p1));
+            a2 = dd_add_d(a2, __ldcg(&rp->p2));
         }
-        if (threadIdx.x < 32) {
+        if (__syncthreads_or(bad)) return false;
 #pragma unroll
-            for (int off = 16; off >= 1; off >>= 1) {
-                DD o0 = dd_shfl_down(a0, off), o1 = dd_shfl_down(a1, off), o2 = dd_shfl_down(a2, off);
-                if (lane + off < 32) { a0 = dd_add(a0, o0); a1 = dd_add(a1, o1); a2 = dd_add(a2, o2); }
+        for (int off = 16; off >= 1; off >>= 1) {
+            const DD o0 = dd_shfl_down(a0, off), o1 = dd_shfl_down(a1, off), o2 = dd_shfl_down(a2, off);
+            if (lane + off < 32) { a0 = dd_add(a0, o0); a1 = dd_add(a1, o1); a2 = dd_add(a2, o2); }
+        }
+        if (lane == 0) { hd.rdd[warp][0] = a0; hd.rdd[warp][1] = a1; hd.rdd[warp][2] = a2; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            DD s0 = hd.rdd[0][0], s1 = hd.rdd[0][1], s2 = hd.rdd[0][2];
+            for (int w = 1; w < kBlock / 32; ++w) {
+                s0 = dd_add(s0, hd.rdd[w][0]);
+                s1 = dd_add(s1, hd.rdd[w][1]);
+                s2 = dd_add(s2, hd.rdd[w][2]);
             }
-            if (lane == 0) {
-                MState &S = hd.st[cs];
-                advance_state(S, D, a0.hi + a0.lo, a1.hi + a1.lo, a2.hi + a2.lo);
-                if (S.done && hd.owner[cs]) {
-                    gstates[hd.sid[cs]] = S;
-                    __threadfence();
-                    atomicSub(&bar->n_active, 1);
-                }
+            MState &S = hd.st[cs];
+            advance_state(S, s0.hi + s0.lo, s1.hi + s1.lo, s2.hi + s2.lo);
+            S.tick = tag;
+            if (S.done && hd.owner[cs]) {
+                gstates[hd.sid[cs]] = S;
+                __threadfence();
             }
         }
         __syncthreads();
     }
+    return true;
 }
 
 // resident != 0: the launch has exactly one tile per CTA; the CTA keeps that tile's slot
 // map and (2D) its FP32 matrix coefficients in shared memory for the whole launch.
+// A CTA leaves when every solve it holds is done, or after max_steps steps (a serving
+// epoch); then it folds in the last step's sums so that the next launch resumes exactly.
 template <int NC, int NZM>
 __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ descs, MState *states,
-                                                     const MTile *__restrict__ tiles, int ntiles, int TY,
-                                                     int resident, GridBar *bar, int max_steps) {
+                                                     const MTile *__restrict__ tiles, int ntiles, int TYmax,
+                                                     int resident, MCtl *ctl, int max_steps) {
     extern __shared__ __align__(16) unsigned char smem[];
     MHead &hd = *reinterpret_cast<MHead *>(smem);
-    const MLayout<NC, NZM> ly(TY, resident != 0);
-    DD *stage = reinterpret_cast<DD *>(smem + ly.off_stage());
+    const MLayout<NC, NZM> ly(TYmax, resident != 0);
     // cache the states of the solves this CTA holds (round robin over the tile list)
     if (threadIdx.x == 0) {
         int n = 0;
@@ -635,13 +749,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
     if (resident && blockIdx.x < ntiles) {  // the CTA's only tile: slot map and FP32 matrix
         const MTile T = tiles[blockIdx.x];
         const MDesc &D = descs[T.solve];
-        const int NS = ly.NS, NT = ly.NT;
+        const int TY = D.TY;
+        const int NS = (kTX + 2) * (TY + 2), NT = kTX * TY;
         int *smap = reinterpret_cast<int *>(smem + ly.off_map());
-        const int *tmap = D.maps + (long long)T.tile * NS;
+        const int *tmap = D.maps + (size_t)T.tile * NS;
         for (int sl = threadIdx.x; sl < NS; sl += kBlock) smap[sl] = tmap[sl];
         float *sA = reinterpret_cast<float *>(smem + ly.off_A());
         const int nz = (NC == 27) ? D.g.nz : 1;
-        const long long plane = (long long)nz * D.g.NQ;
+        const int NQ = (int)D.g.NQ;
+        const int plane = nz * NQ;
         const int tx = T.tile % D.tiles_x, ty = T.tile / D.tiles_x;
         const int i0 = D.g.ilo + tx * kTX, j0 = D.g.jlo + ty * TY;
         const int NN = nz * NT;
@@ -650,8 +766,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
             const int col = it % NT, k = it / NT;
             const int i = i0 + col % kTX, j = j0 + col / kTX;
             float a = 0.0f;
-            if (i <= D.g.ihi && j <= D.g.jhi)
-                a = D.A32[(long long)bc * plane + (long long)k * D.g.NQ + (long long)j * D.g.NX + i];
+            if (i <= D.g.ihi && j <= D.g.jhi) a = D.A32[(size_t)bc * plane + k * NQ + j * D.g.NX + i];
             sA[w] = a;
         }
         __syncthreads();
@@ -659,8 +774,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
     bool finished = false;
     int step = 0;
     for (; step < max_steps; ++step) {
-        const int pbuf = step & 1;
-        if (step > 0) reduce_cached(hd, stage, descs, pbuf ^ 1, states, bar);  // previous step's sums
+        if (step > 0 && !reduce_wait(hd, descs, states, ctl)) return;  // previous step's sums
+        bool running = false;
+        for (int cs = 0; cs < hd.nsolve; ++cs) running |= !hd.st[cs].done;
+        if (!running) {
+            finished = true;
+            break;
+        }
         for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
             const MTile T = tiles[w];
             int cs = 0;
@@ -674,16 +794,11 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
                 }
                 __syncthreads();
             }
-            tile_step<NC, NZM>(hd.st[cs], T.tile, pbuf, TY, resident != 0, hd, smem);
-        }
-        if (!grid_barrier(bar, gridDim.x)) return;
-        if (((volatile GridBar *)bar)->n_active <= 0) {
-            finished = true;
-            break;
+            tile_step<NC, NZM>(hd.st[cs], T.tile, resident != 0, TYmax, hd, smem);
         }
     }
     // out of steps: fold in the last step's sums so that the next launch resumes exactly
-    if (!finished && step > 0) reduce_cached(hd, stage, descs, (step - 1) & 1, states, bar);
+    if (!finished && step > 0 && !reduce_wait(hd, descs, states, ctl)) return;
     if (threadIdx.x == 0)
         for (int cs = 0; cs < hd.nsolve; ++cs)
             if (hd.owner[cs]) states[hd.sid[cs]] = hd.st[cs];
@@ -757,29 +872,29 @@ struct MixedBufs {
     int precond = -1;
     float *A32 = nullptr, *pre = nullptr, *vec = nullptr;
     int *maps = nullptr;
-    DD *partials = nullptr;
+    TileRec *recs = nullptr;
     MState *state = nullptr;
     MDesc *desc = nullptr;
     MTile *tiles = nullptr;
-    GridBar *bar = nullptr;
+    MCtl *ctl = nullptr;
     size_t nbytes = 0;
     int ntiles = 0;
     int ntiles_cap = 0;
     long long maps_cap = 0;
     void release() {
-        for (void *p : {(void *)A32, (void *)pre, (void *)vec, (void *)partials, (void *)state, (void *)desc,
-                        (void *)tiles, (void *)bar, (void *)maps})
+        for (void *p : {(void *)A32, (void *)pre, (void *)vec, (void *)recs, (void *)state, (void *)desc,
+                        (void *)tiles, (void *)ctl, (void *)maps})
             if (p) cudaFree(p);
         A32 = pre = vec = nullptr;
         maps = nullptr;
         ntiles = ntiles_cap = 0;
         maps_cap = 0;
         TY = 0;
-        partials = nullptr;
+        recs = nullptr;
         state = nullptr;
         desc = nullptr;
         tiles = nullptr;
-        bar = nullptr;
+        ctl = nullptr;
         nbytes = 0;
         valid = false;
         precond = -1;
