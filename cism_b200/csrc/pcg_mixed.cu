@@ -116,8 +116,8 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
-__device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
-    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+__device__ __forceinline__ void st_relaxed(unsigned *p, unsigned v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 constexpr long long kWaitCycles = 1LL << 31;  // ~1 s at 2 GHz: a wait longer than this is a failure
@@ -642,8 +642,8 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
         rp->p0 = p0;
         rp->p1 = p1;
         rp->p2 = p2;
-        __threadfence();
-        st_release(&rp->tag, tag);
+        __threadfence();            // orders the record and the tile's vector stores before the tag
+        st_relaxed(&rp->tag, tag);  // (fence + relaxed store: a release without a second fence)
     }
     __syncthreads();
 }
