@@ -196,6 +196,7 @@ def assemble_bp_3d(thck, usrf, dx, dy, nz, flwa=1.0e-16, beta=None, bc="periodic
     yv = np.arange(NY, dtype=np.float64) * dy
 
     A = np.zeros((4, NY, NX, nz, 27))  # uu, uv, vu, vv
+    Af = A.reshape(4, -1)               # flat views for the element scatter
     cj, ci = np.nonzero(ac)
     # elements: every active cell x every layer
     ecj = np.repeat(cj, nz - 1)
@@ -218,23 +219,27 @@ def assemble_bp_3d(thck, usrf, dx, dy, nz, flwa=1.0e-16, beta=None, bc="periodic
         dphi = np.einsum("epba,pna->epnb", jinv, DPHIR3)  # (E, qp, node, xyz)
         f = efvs * 1.0 * det / VOL0                       # efvs * wqp * detJ / vol0
         dx_, dy_, dz_ = dphi[..., 0], dphi[..., 1], dphi[..., 2]
-        Kuu = np.einsum("ep,epr,epc->erc", f, dx_, dx_) * 4 + np.einsum("ep,epr,epc->erc", f, dy_, dy_) \
-            + np.einsum("ep,epr,epc->erc", f, dz_, dz_)
-        Kvv = np.einsum("ep,epr,epc->erc", f, dy_, dy_) * 4 + np.einsum("ep,epr,epc->erc", f, dx_, dx_) \
-            + np.einsum("ep,epr,epc->erc", f, dz_, dz_)
-        Kuv = np.einsum("ep,epr,epc->erc", f, dx_, dy_) * 2 + np.einsum("ep,epr,epc->erc", f, dy_, dx_)
-        Kvu = np.einsum("ep,epr,epc->erc", f, dy_, dx_) * 2 + np.einsum("ep,epr,epc->erc", f, dx_, dy_)
+        Kxx = np.einsum("ep,epr,epc->erc", f, dx_, dx_)
+        Kyy = np.einsum("ep,epr,epc->erc", f, dy_, dy_)
+        Kzz = np.einsum("ep,epr,epc->erc", f, dz_, dz_)
+        Kxy = np.einsum("ep,epr,epc->erc", f, dx_, dy_)
+        Kyx = np.einsum("ep,epr,epc->erc", f, dy_, dx_)
+        Kuu = Kxx * 4 + Kyy + Kzz
+        Kvv = Kyy * 4 + Kxx + Kzz
+        Kuv = Kxy * 2 + Kyx
+        Kvu = Kyx * 2 + Kxy
+        node = ((vj * NX + vi) * nz + kk) * 27                 # flat (j, i, k, m=0) offsets, (E, 8)
         for nr in range(8):
-            rj, ri, rk = vj[:, nr], vi[:, nr], kk[:, nr]
+            base = node[:, nr]
             for nc in range(8):
                 iA = ISH3[nc] - ISH3[nr]
                 jA = JSH3[nc] - JSH3[nr]
                 kA = KSH3[nc] - KSH3[nr]
-                m = (iA + 1) + 3 * (jA + 1) + 9 * (kA + 1)
-                A[0, rj, ri, rk, m] += Kuu[:, nr, nc]
-                A[1, rj, ri, rk, m] += Kuv[:, nr, nc]
-                A[2, rj, ri, rk, m] += Kvu[:, nr, nc]
-                A[3, rj, ri, rk, m] += Kvv[:, nr, nc]
+                fi = base + ((iA + 1) + 3 * (jA + 1) + 9 * (kA + 1))  # unique within the chunk
+                Af[0][fi] += Kuu[:, nr, nc]
+                Af[1][fi] += Kuv[:, nr, nc]
+                Af[2][fi] += Kvu[:, nr, nc]
+                Af[3][fi] += Kvv[:, nr, nc]
 
     # load vector, local driving stress (:4243-4262)
     dsdx, dsdy = vertex_gradient(usrf, dx, dy)
