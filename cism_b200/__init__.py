@@ -117,6 +117,14 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_solver_solve.restype = ctypes.c_int
     lib.cismgpu_solver_solve_batch.argtypes = [P(vp), i32, i32, i32, i32, dbl, i32, P(dbl), P(i32), P(i32), vp]
     lib.cismgpu_solver_solve_batch.restype = ctypes.c_int
+    lib.cismgpu_batch_create.argtypes = [P(vp), P(vp), i32, i32, i32, dbl, i32, vp]
+    lib.cismgpu_batch_create.restype = ctypes.c_int
+    lib.cismgpu_batch_run.argtypes = [vp]
+    lib.cismgpu_batch_run.restype = ctypes.c_int
+    lib.cismgpu_batch_wait.argtypes = [vp, P(dbl), P(i32), P(i32)]
+    lib.cismgpu_batch_wait.restype = ctypes.c_int
+    lib.cismgpu_batch_destroy.argtypes = [vp]
+    lib.cismgpu_batch_destroy.restype = ctypes.c_int
     lib.cismgpu_solver_get_x.argtypes = [vp, d, d]
     lib.cismgpu_solver_get_x.restype = ctypes.c_int
     lib.cismgpu_solver_profile.argtypes = [vp, i32]
@@ -371,3 +379,45 @@ def solve_batch(solvers, algorithm=ALG_MIXED_CHRONGEAR, precond=HO_PRECOND_DIAG,
     if rc != 0 and not np.any(statuses):
         _check(lib, rc)
     return np.array(list(errs)), np.array(list(nits), dtype=np.int32), statuses
+
+
+class GraphBatch:
+    """A batched mixed-precision solve over DeviceSolvers captured in a CUDA graph
+    (cismgpu_batch_create): run() replays it asynchronously, wait() returns
+    (errs, niters, statuses).  The members are locked until close()."""
+
+    def __init__(self, solvers, precond=HO_PRECOND_DIAG, ncheck=5, tol=1e-8, maxiters=200, stream=None):
+        lib = load_library()
+        self._lib = lib
+        self.solvers = list(solvers)
+        n = len(self.solvers)
+        self.n = n
+        hs = (ctypes.c_void_p * n)(*[s.handle for s in self.solvers])
+        h = ctypes.c_void_p()
+        _check(lib, lib.cismgpu_batch_create(ctypes.byref(h), hs, n, precond, ncheck, tol, maxiters,
+                                             ctypes.c_void_p(stream) if stream else None))
+        self.handle = h.value
+
+    def run(self):
+        _check(self._lib, self._lib.cismgpu_batch_run(self.handle))
+
+    def wait(self):
+        n = self.n
+        errs, nits, sts = (ctypes.c_double * n)(), (ctypes.c_int * n)(), (ctypes.c_int * n)()
+        rc = self._lib.cismgpu_batch_wait(self.handle, errs, nits, sts)
+        statuses = np.array(list(sts), dtype=np.int32)
+        if rc != 0 and not np.any(statuses):
+            _check(self._lib, rc)
+        return np.array(list(errs)), np.array(list(nits), dtype=np.int32), statuses
+
+    def close(self):
+        if self.handle:
+            self._lib.cismgpu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

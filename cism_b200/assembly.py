@@ -407,3 +407,17 @@ def ssa_random(ewn=401, nsn=401, dx=1000.0, seed=7, corr_km=20.0, name="ssa") ->
 def lognormal_beta(shape, seed, mu=math.log(1.0e3), sd=1.0):
     rng = np.random.default_rng(seed)
     return np.exp(mu + sd * rng.standard_normal(shape))
+
+
+def batch_member(n, seed, nz=11, dx=2000.0) -> Problem:
+    """One member of the batched 3D workload: an n x n x nz ice stream (seeded bed roughness)
+    sliding on its own seeded log-normal basal friction field (mu = ln 1e3 Pa yr/m, sigma = 1)."""
+    shape = (n + 2 * NHALO - 1, n + 2 * NHALO - 1)
+    return ice_stream(ewn=n, nsn=n, nz=nz, dx=dx, seed=seed, beta=lognormal_beta(shape, 1000 + seed),
+                      name=f"member{seed}_{n}")
+
+
+def batch_sizes(count=64, seed=11, lo=64, hi=256):
+    """Seeded horizontal sizes, uniform on lo..hi vertices per side."""
+    return [int(v) for v in np.random.default_rng(seed).integers(lo, hi + 1, count)]
+

@@ -445,6 +445,18 @@ __global__ void k_mstate_to_solve(const MState *ms, SolveState *st, const MCtl *
     st->done = 1;
 }
 
+// Batched form: member t's result into its handle's SolveState.
+__global__ void k_mstates_to_solves(const MState *ms, SolveState *const *dst, int n, const MCtl *ctl) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    SolveState *st = dst[t];
+    st->err = ms[t].err;
+    st->niters = ms[t].niters;
+    st->status = (ctl->abort && !ms[t].done) ? CISMGPU_ETIMEOUT : ms[t].status;
+    st->checks = ms[t].checks;
+    st->done = 1;
+}
+
 static int tiles_for(const Geom &g, int TY) {
     return ((g.ihi - g.ilo + kTX) / kTX) * ((g.jhi - g.jlo + TY) / TY);
 }
@@ -641,26 +653,47 @@ static int mixed_reset(Solver &sv, cudaStream_t s) {
     return CISMGPU_OK;
 }
 
-template <int NC, int NZM>
-static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_tiles, int ntiles, int TY,
-                        int resident, MCtl *d_ctl, int max_steps, cudaStream_t s,
-                        const std::vector<MTile> *host_tiles) {
-    const size_t smem = MLayout<NC, NZM>(TY, resident != 0).bytes();
-    int grid = mixed_grid(NC == 27, NZM, TY, resident != 0);
-    if (grid < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM at this tile height");
-    if (resident && grid < ntiles) return fail(CISMGPU_EUNSUPPORTED, "resident launch needs one tile per CTA");
-    if (grid > ntiles) grid = ntiles;
-    if (host_tiles) {  // each CTA caches the state of at most kMaxCtaSolves solves
+// Co-resident grid of a launch (sets the kernel's shared-memory attribute; call outside any
+// stream capture).  0 if the kernel does not fit.
+static int mixed_launch_grid(bool is3d, int nzm, int TY, bool resident, int ntiles) {
+    const int grid = mixed_grid(is3d, nzm, TY, resident);
+    if (grid < 1) return 0;
+    if (resident && grid < ntiles) return 0;
+    return std::min(grid, ntiles);
+}
+
+// Launch order of a tile list on `grid` CTAs (CTA b takes entries b, b + grid, ...).  With
+// more tiles than CTAs, each CTA gets a contiguous run of the (solve, tile) list, so that it
+// holds tiles of few solves; padding entries have solve = -1.  Fails if a CTA would hold
+// tiles of more than kMaxCtaSolves solves.
+static int mixed_tile_order(const std::vector<MTile> &in, int grid, std::vector<MTile> &out) {
+    const int T = (int)in.size();
+    if (T <= grid) {
+        out = in;
+    } else {
+        const int per = (T + grid - 1) / grid;
+        out.assign((size_t)per * grid, MTile{-1, -1});
         for (int b = 0; b < grid; ++b) {
-            std::vector<int> seen;
-            for (int w = b; w < ntiles; w += grid) {
-                const int sv = (*host_tiles)[w].solve;
-                if (std::find(seen.begin(), seen.end(), sv) == seen.end()) seen.push_back(sv);
-            }
-            if ((int)seen.size() > kMaxCtaSolves)
-                return fail(CISMGPU_EUNSUPPORTED, "batch too fragmented for one launch (solves per CTA > 64)");
+            const long long lo = (long long)b * T / grid, hi = (long long)(b + 1) * T / grid;
+            for (long long w = lo; w < hi; ++w) out[(size_t)(w - lo) * grid + b] = in[(size_t)w];
         }
     }
+    for (int b = 0; b < grid; ++b) {
+        std::vector<int> seen;
+        for (size_t w = b; w < out.size(); w += grid) {
+            const int sv = out[w].solve;
+            if (sv >= 0 && std::find(seen.begin(), seen.end(), sv) == seen.end()) seen.push_back(sv);
+        }
+        if ((int)seen.size() > kMaxCtaSolves)
+            return fail(CISMGPU_EUNSUPPORTED, "batch too fragmented for one launch (solves per CTA > 64)");
+    }
+    return CISMGPU_OK;
+}
+
+template <int NC, int NZM>
+static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_tiles, int ntiles, int TY,
+                        int resident, MCtl *d_ctl, int max_steps, int grid, cudaStream_t s) {
+    const size_t smem = MLayout<NC, NZM>(TY, resident != 0).bytes();
     void *args[] = {(void *)&d_descs, (void *)&d_states, (void *)&d_tiles, (void *)&ntiles, (void *)&TY,
                     (void *)&resident, (void *)&d_ctl, (void *)&max_steps};
     CU(cudaLaunchCooperativeKernel((const void *)k_mixed<NC, NZM>, dim3(grid), dim3(kBlock), args, smem, s));
@@ -668,12 +701,11 @@ static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_t
 }
 
 static int mixed_dispatch(bool is3d, int nzm, const MDesc *d, MState *st, const MTile *t, int nt, int TY,
-                          bool resident, MCtl *bar, int max_steps, cudaStream_t s,
-                          const std::vector<MTile> *host_tiles = nullptr) {
+                          bool resident, MCtl *ctl, int max_steps, int grid, cudaStream_t s) {
     const int res = resident ? 1 : 0;
-    if (!is3d) return mixed_launch<9, 1>(d, st, t, nt, TY, res, bar, max_steps, s, host_tiles);
-    if (nzm == 16) return mixed_launch<27, 16>(d, st, t, nt, TY, 0, bar, max_steps, s, host_tiles);
-    return mixed_launch<27, 32>(d, st, t, nt, TY, 0, bar, max_steps, s, host_tiles);
+    if (!is3d) return mixed_launch<9, 1>(d, st, t, nt, TY, res, ctl, max_steps, grid, s);
+    if (nzm == 16) return mixed_launch<27, 16>(d, st, t, nt, TY, 0, ctl, max_steps, grid, s);
+    return mixed_launch<27, 32>(d, st, t, nt, TY, 0, ctl, max_steps, grid, s);
 }
 
 static double mixed_iter_bytes(const Solver &sv, int precond) {
@@ -710,7 +742,9 @@ int Solver::run_mixed(int precond, int ncheck, double tol, int maxiters) {
         CU(cudaEventRecord(e0, stream));
     }
     trace("run_mixed: descriptors copied");
-    TRY(mixed_dispatch(is3d, nzm, m.desc, m.state, m.tiles, m.ntiles, TY, resident, m.ctl, max_steps, stream));
+    const int grid = mixed_launch_grid(is3d, nzm, TY, resident, m.ntiles);
+    if (grid < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM at this tile height");
+    TRY(mixed_dispatch(is3d, nzm, m.desc, m.state, m.tiles, m.ntiles, TY, resident, m.ctl, max_steps, grid, stream));
     trace("run_mixed: kernel launched");
     if (prof) CU(cudaEventRecord(e1, stream));
     k_mstate_to_solve<<<1, 1, 0, stream>>>(m.state, state.as<SolveState>(), m.ctl);
@@ -879,6 +913,118 @@ static int oneshot_global_sum(int nx, int ny, int nz, const cismgpu_par_t *par, 
     return CISMGPU_OK;
 }
 
+// A prepared launch of the mixed solver over several handles (one persistent kernel).  The
+// device block holds, 256-byte aligned: descriptors, running states, initial states, the
+// tile list, the SolveState pointers of the members and the control word; results come back
+// into pinned host memory, so the whole sequence can be captured in a CUDA graph.
+struct MixedBatch {
+    std::vector<Solver *> svs;
+    bool is3d = false, resident = false;
+    int nzm = 0, TYmax = 1, grid = 0, ntl = 0, max_steps = 0;
+    void *dmem = nullptr;
+    MDesc *d_descs = nullptr;
+    MState *d_states = nullptr, *d_states0 = nullptr;
+    MTile *d_tiles = nullptr;
+    SolveState **d_dst = nullptr;
+    MCtl *d_ctl = nullptr;
+    MState *h_states = nullptr;  // pinned
+    MCtl *h_ctl = nullptr;       // pinned
+    void release() {
+        if (dmem) cudaFree(dmem);
+        if (h_states) cudaFreeHost(h_states);
+        if (h_ctl) cudaFreeHost(h_ctl);
+        dmem = nullptr;
+        h_states = nullptr;
+        h_ctl = nullptr;
+    }
+    ~MixedBatch() { release(); }
+};
+
+// Prepare every member (FP32 matrix, maps, preconditioner; its own tile height), plan the
+// launch and upload the descriptors, initial states and the tile list.
+static int batch_prepare(MixedBatch &B, int precond, int ncheck, double tol, int maxiters) {
+    const int n = (int)B.svs.size();
+    Solver &s0 = *B.svs[0];
+    B.is3d = s0.is3d;
+    B.nzm = mixed_nzm(s0.g, s0.is3d);
+    std::vector<int> tys(n);
+    std::vector<MTile> tl;
+    for (int t = 0; t < n; ++t) {
+        Solver &sv = *B.svs[t];
+        if (sv.is3d != s0.is3d || mixed_nzm(sv.g, sv.is3d) != B.nzm)
+            return fail(CISMGPU_EINVAL, "batch members must share dims and the nz class (<=16 or <=32)");
+        tys[t] = mixed_solve_ty(sv.g, sv.is3d, B.nzm);
+        B.TYmax = std::max(B.TYmax, tys[t]);
+        TRY(mixed_prepare(sv, precond, tys[t]));
+        for (int k = 0; k < tiles_for(sv.g, tys[t]); ++k) tl.push_back(MTile{t, k});
+    }
+    for (int t = 0; t < n; ++t) CU(cudaStreamSynchronize(B.svs[t]->stream));
+    B.resident = mixed_resident(B.is3d, B.nzm, B.TYmax, (long long)tl.size());
+    B.grid = mixed_launch_grid(B.is3d, B.nzm, B.TYmax, B.resident, (int)tl.size());
+    if (B.grid < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM at this tile height");
+    std::vector<MTile> order;
+    TRY(mixed_tile_order(tl, B.grid, order));
+    B.ntl = (int)order.size();
+    B.max_steps = 4 * maxiters + 16;
+    std::vector<MDesc> descs(n);
+    std::vector<SolveState *> dst(n);
+    for (int t = 0; t < n; ++t) {
+        descs[t] = mixed_desc(*B.svs[t], precond, tys[t]);
+        dst[t] = B.svs[t]->state.as<SolveState>();
+    }
+    const std::vector<MState> states(n, mixed_init_state(tol, maxiters, ncheck));
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t o_desc = 0, o_st = al(n * sizeof(MDesc)), o_st0 = o_st + al(n * sizeof(MState)),
+                 o_tl = o_st0 + al(n * sizeof(MState)), o_dst = o_tl + al(order.size() * sizeof(MTile)),
+                 o_ctl = o_dst + al(n * sizeof(SolveState *)), total = o_ctl + al(sizeof(MCtl));
+    CU(cudaMalloc(&B.dmem, total));
+    char *base = static_cast<char *>(B.dmem);
+    B.d_descs = reinterpret_cast<MDesc *>(base + o_desc);
+    B.d_states = reinterpret_cast<MState *>(base + o_st);
+    B.d_states0 = reinterpret_cast<MState *>(base + o_st0);
+    B.d_tiles = reinterpret_cast<MTile *>(base + o_tl);
+    B.d_dst = reinterpret_cast<SolveState **>(base + o_dst);
+    B.d_ctl = reinterpret_cast<MCtl *>(base + o_ctl);
+    CU(cudaMallocHost((void **)&B.h_states, n * sizeof(MState)));
+    CU(cudaMallocHost((void **)&B.h_ctl, sizeof(MCtl)));
+    CU(cudaMemcpy(B.d_descs, descs.data(), n * sizeof(MDesc), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(B.d_states0, states.data(), n * sizeof(MState), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(B.d_tiles, order.data(), order.size() * sizeof(MTile), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(B.d_dst, dst.data(), n * sizeof(SolveState *), cudaMemcpyHostToDevice));
+    return CISMGPU_OK;
+}
+
+// One batched solve on stream s: member resets, initial states, the persistent launch, and
+// the results (each handle's SolveState, and pinned host copies).  No host synchronization
+// and no allocation, so it can be captured.
+static int batch_enqueue(MixedBatch &B, cudaStream_t s) {
+    const int n = (int)B.svs.size();
+    for (Solver *sv : B.svs) TRY(mixed_reset(*sv, s));
+    CU(cudaMemcpyAsync(B.d_states, B.d_states0, n * sizeof(MState), cudaMemcpyDeviceToDevice, s));
+    CU(cudaMemsetAsync(B.d_ctl, 0, sizeof(MCtl), s));
+    TRY(mixed_dispatch(B.is3d, B.nzm, B.d_descs, B.d_states, B.d_tiles, B.ntl, B.TYmax, B.resident, B.d_ctl,
+                       B.max_steps, B.grid, s));
+    k_mstates_to_solves<<<(n + 127) / 128, 128, 0, s>>>(B.d_states, B.d_dst, n, B.d_ctl);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(B.h_states, B.d_states, n * sizeof(MState), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(B.h_ctl, B.d_ctl, sizeof(MCtl), cudaMemcpyDeviceToHost, s));
+    return CISMGPU_OK;
+}
+
+// Per-member results of the last completed batch_enqueue (after the stream is synchronized).
+static int batch_results(const MixedBatch &B, double *errs, int *niters, int *statuses) {
+    int first = CISMGPU_OK;
+    for (size_t t = 0; t < B.svs.size(); ++t) {
+        const MState &S = B.h_states[t];
+        errs[t] = S.err;
+        niters[t] = S.niters;
+        statuses[t] = (B.h_ctl->abort && !S.done) ? CISMGPU_ETIMEOUT : S.status;
+        if (statuses[t] && !first) first = statuses[t];
+    }
+    if (first) return fail(first, "batch member failed (see statuses)");
+    return CISMGPU_OK;
+}
+
 }  // namespace cismgpu
 
 // ---------------------------------------------------------------------------
@@ -889,7 +1035,19 @@ using namespace cismgpu;
 struct cismgpu_solver {
     Solver sv;
     std::mutex mu;
+    bool in_batch = false;               // a graph batch replays this handle's buffers
+    cudaStream_t batch_stream = nullptr; // that batch's stream
 };
+
+struct cismgpu_batch {
+    cismgpu::MixedBatch b;
+    std::vector<cismgpu_solver *> members;  // marked in_batch while the batch exists
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
 
 extern "C" {
 
@@ -984,6 +1142,7 @@ int cismgpu_solver_solve(cismgpu_solver_t *h, int algorithm, int precond, int li
     g_last_error.clear();
     if (!h || !err || !niters) return fail(CISMGPU_EINVAL, "null argument");
     std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
     trace("solver_solve: begin");
     TRY(validate_solve_args(precond, linear_solve_ncheck, maxiters));
     Solver &sv = h->sv;
@@ -991,6 +1150,7 @@ int cismgpu_solver_solve(cismgpu_solver_t *h, int algorithm, int precond, int li
     TRY(run_algorithm(sv, algorithm, precond, linear_solve_ncheck, tolerance, maxiters));
     return sv.finish_solve(err, niters);
 }
+
 
 int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm, int precond, int linear_solve_ncheck,
                                double tolerance, int maxiters, double *errs, int *niters, int *statuses,
@@ -1008,79 +1168,107 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
         return first;
     }
     std::vector<std::unique_lock<std::mutex>> locks;
+    MixedBatch B;
     for (int t = 0; t < n; ++t) {
         if (!solvers[t]) return fail(CISMGPU_EINVAL, "null handle in batch");
         locks.emplace_back(solvers[t]->mu);
+        if (solvers[t]->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch");
+        B.svs.push_back(&solvers[t]->sv);
     }
-    Solver &s0 = solvers[0]->sv;
-    const int nzm = mixed_nzm(s0.g, s0.is3d);
-    std::vector<const Geom *> geoms;
+    TRY(batch_prepare(B, precond, linear_solve_ncheck, tolerance, maxiters));
+    cudaStream_t s = cuda_stream ? (cudaStream_t)cuda_stream : B.svs[0]->stream;
+    TRY(batch_enqueue(B, s));
+    CU(cudaStreamSynchronize(s));
+    return batch_results(B, errs, niters, statuses);
+}
+
+int cismgpu_batch_create(cismgpu_batch_t **out, cismgpu_solver_t **solvers, int n, int precond,
+                         int linear_solve_ncheck, double tolerance, int maxiters, void *cuda_stream) {
+    g_last_error.clear();
+    if (!out || !solvers || n < 1) return fail(CISMGPU_EINVAL, "null argument");
+    *out = nullptr;
+    TRY(validate_solve_args(precond, linear_solve_ncheck, maxiters));
     for (int t = 0; t < n; ++t) {
-        Solver &sv = solvers[t]->sv;
-        if (sv.is3d != s0.is3d || mixed_nzm(sv.g, sv.is3d) != nzm)
-            return fail(CISMGPU_EINVAL, "batch members must share dims and the nz class (<=16 or <=32)");
-        geoms.push_back(&sv.g);
+        if (!solvers[t]) return fail(CISMGPU_EINVAL, "null handle in batch");
+        for (int u = 0; u < t; ++u)
+            if (solvers[u] == solvers[t]) return fail(CISMGPU_EINVAL, "handle listed twice in batch");
     }
-    std::vector<int> tys(n);
-    int TYmax = 1;
-    long long ntot = 0;
-    for (int t = 0; t < n; ++t) {
-        Solver &sv = solvers[t]->sv;
-        tys[t] = mixed_solve_ty(sv.g, sv.is3d, nzm);
-        TYmax = std::max(TYmax, tys[t]);
-        ntot += tiles_for(sv.g, tys[t]);
-        TRY(mixed_prepare(sv, precond, tys[t]));
-        TRY(mixed_reset(sv, sv.stream));
+    cismgpu_batch *h = new cismgpu_batch();
+    int rc = CISMGPU_OK;
+    {
+        std::vector<std::unique_lock<std::mutex>> locks;  // held during preparation only
+        for (int t = 0; t < n && !rc; ++t) {
+            locks.emplace_back(solvers[t]->mu);
+            if (solvers[t]->in_batch) rc = fail(CISMGPU_EINVAL, "handle already belongs to a graph batch");
+            h->b.svs.push_back(&solvers[t]->sv);
+        }
+        if (!rc) rc = batch_prepare(h->b, precond, linear_solve_ncheck, tolerance, maxiters);
+        if (!rc) {
+            if (cuda_stream) {
+                h->stream = (cudaStream_t)cuda_stream;
+            } else if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) == cudaSuccess) {
+                h->own_stream = true;
+            } else {
+                rc = fail(CISMGPU_ECUDA, "stream creation failed");
+            }
+        }
+        if (!rc) {  // capture one batched solve into a graph
+            cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) rc = fail(CISMGPU_ECUDA, std::string("begin capture: ") + cudaGetErrorString(e));
+            if (!rc) {
+                const int rce = batch_enqueue(h->b, h->stream);
+                cudaGraph_t g = nullptr;
+                e = cudaStreamEndCapture(h->stream, &g);
+                h->graph = g;
+                if (rce) rc = rce;
+                else if (e != cudaSuccess) rc = fail(CISMGPU_ECUDA, std::string("end capture: ") + cudaGetErrorString(e));
+            }
+            if (!rc) {
+                e = cudaGraphInstantiate(&h->exec, h->graph, 0);
+                if (e != cudaSuccess) rc = fail(CISMGPU_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            }
+        }
+        if (!rc)
+            for (int t = 0; t < n; ++t) {
+                solvers[t]->in_batch = true;
+                solvers[t]->batch_stream = h->stream;
+                h->members.push_back(solvers[t]);
+            }
     }
-    const bool resident = mixed_resident(s0.is3d, nzm, TYmax, ntot);
-    for (int t = 0; t < n; ++t) CU(cudaStreamSynchronize(solvers[t]->sv.stream));
-    cudaStream_t s = cuda_stream ? (cudaStream_t)cuda_stream : s0.stream;
-    // one descriptor, state and tile list for the whole batch
-    std::vector<MDesc> descs(n);
-    std::vector<MState> states(n, mixed_init_state(tolerance, maxiters, linear_solve_ncheck));
-    std::vector<MTile> tiles;
-    for (int t = 0; t < n; ++t) {
-        descs[t] = mixed_desc(solvers[t]->sv, precond, tys[t]);
-        for (int k = 0; k < descs[t].ntiles; ++k) tiles.push_back(MTile{t, k});
-    }
-    // tiles in (solve, tile) order; CTAs take them round robin, so a solve's tiles spread over
-    // consecutive CTAs and each CTA holds tiles of only a few solves
-    void *dmem = nullptr;
-    const size_t off_s = ((n * sizeof(MDesc)) + 255) / 256 * 256;
-    const size_t off_t = off_s + ((n * sizeof(MState)) + 255) / 256 * 256;
-    const size_t off_b = off_t + ((tiles.size() * sizeof(MTile)) + 255) / 256 * 256;
-    CU(cudaMallocAsync(&dmem, off_b + sizeof(MCtl), s));
-    char *base = static_cast<char *>(dmem);
-    MDesc *d_descs = reinterpret_cast<MDesc *>(base);
-    MState *d_states = reinterpret_cast<MState *>(base + off_s);
-    MTile *d_tiles = reinterpret_cast<MTile *>(base + off_t);
-    MCtl *d_bar = reinterpret_cast<MCtl *>(base + off_b);
-    CU(cudaMemcpyAsync(d_descs, descs.data(), n * sizeof(MDesc), cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(d_states, states.data(), n * sizeof(MState), cudaMemcpyHostToDevice, s));
-    CU(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(MTile), cudaMemcpyHostToDevice, s));
-    CU(cudaMemsetAsync(d_bar, 0, sizeof(MCtl), s));
-    int rc = mixed_dispatch(s0.is3d, nzm, d_descs, d_states, d_tiles, (int)tiles.size(), TYmax, resident, d_bar,
-                            4 * maxiters + 16, s, &tiles);
     if (rc) {
-        cudaFreeAsync(dmem, s);
+        cismgpu_batch_destroy(h);
         return rc;
     }
-    for (int t = 0; t < n; ++t)
-        k_mstate_to_solve<<<1, 1, 0, s>>>(d_states + t, solvers[t]->sv.state.as<SolveState>(), d_bar);
-    CU(cudaGetLastError());
-    CU(cudaMemcpyAsync(states.data(), d_states, n * sizeof(MState), cudaMemcpyDeviceToHost, s));
-    MCtl hb;
-    CU(cudaMemcpyAsync(&hb, d_bar, sizeof(MCtl), cudaMemcpyDeviceToHost, s));
-    CU(cudaFreeAsync(dmem, s));
-    CU(cudaStreamSynchronize(s));
-    int first = CISMGPU_OK;
-    for (int t = 0; t < n; ++t) {
-        errs[t] = states[t].err;
-        niters[t] = states[t].niters;
-        statuses[t] = (hb.abort && !states[t].done) ? CISMGPU_ETIMEOUT : states[t].status;
-        if (statuses[t] && !first) first = statuses[t];
+    *out = h;
+    return CISMGPU_OK;
+}
+
+int cismgpu_batch_run(cismgpu_batch_t *h) {
+    g_last_error.clear();
+    if (!h || !h->exec) return fail(CISMGPU_EINVAL, "null batch");
+    CU(cudaGraphLaunch(h->exec, h->stream));
+    return CISMGPU_OK;
+}
+
+int cismgpu_batch_wait(cismgpu_batch_t *h, double *errs, int *niters, int *statuses) {
+    g_last_error.clear();
+    if (!h || !errs || !niters || !statuses) return fail(CISMGPU_EINVAL, "null argument");
+    CU(cudaStreamSynchronize(h->stream));
+    return batch_results(h->b, errs, niters, statuses);
+}
+
+int cismgpu_batch_destroy(cismgpu_batch_t *h) {
+    if (!h) return CISMGPU_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (cismgpu_solver *m : h->members) {
+        std::lock_guard<std::mutex> lk(m->mu);
+        m->in_batch = false;
+        m->batch_stream = nullptr;
     }
-    if (first) return fail(first, "batch member failed (see statuses)");
+    if (h->exec) cudaGraphExecDestroy(h->exec);
+    if (h->graph) cudaGraphDestroy(h->graph);
+    if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+    delete h;
     return CISMGPU_OK;
 }
 
@@ -1088,6 +1276,7 @@ int cismgpu_solver_get_x(cismgpu_solver_t *h, double *xu, double *xv) {
     g_last_error.clear();
     if (!h || !xu || !xv) return fail(CISMGPU_EINVAL, "null argument");
     std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) CU(cudaStreamSynchronize(h->batch_stream));  // the batch may be writing x
     return h->sv.download(VX_U, VX_V, xu, xv);
 }
 
@@ -1120,6 +1309,7 @@ int cismgpu_solver_destroy(cismgpu_solver_t *h) {
     if (!h) return CISMGPU_OK;
     {
         std::lock_guard<std::mutex> lk(h->mu);
+        if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
         if (h->sv.stream) cudaStreamSynchronize(h->sv.stream);
     }
     delete h;

@@ -730,6 +730,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
         int n = 0;
         for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
             const MTile T = tiles[w];
+            if (T.solve < 0) continue;  // padding of a blocked tile order
             int u = 0;
             while (u < n && hd.sid[u] != T.solve) ++u;
             if (u == n && n < kMaxCtaSolves) {

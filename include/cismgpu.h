@@ -211,6 +211,27 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
                                int linear_solve_ncheck, double tolerance, int maxiters,
                                double *errs, int *niters, int *statuses, void *cuda_stream);
 
+/* ------------------------------------------------------------------------
+ * Graph-captured batches (no reference counterpart).  cismgpu_batch_create
+ * prepares the mixed solver on every member (FP32 matrix, preconditioner,
+ * per-member tile height), plans one persistent launch over all their tiles
+ * and captures a whole batched solve -- resets to each member's x0, the launch,
+ * the results -- into a CUDA graph.  cismgpu_batch_run replays it
+ * (asynchronously, on the batch's stream); cismgpu_batch_wait synchronizes and
+ * returns per-member err/niters/status.  Until cismgpu_batch_destroy the
+ * members belong to the batch: cismgpu_solver_solve, _solve_batch, _destroy
+ * and another batch_create on them return CISMGPU_EINVAL; cismgpu_solver_get_x
+ * first waits for the batch's stream.  A changed matrix needs a new batch.
+ * Results are bit-identical to cismgpu_solver_solve_batch and to solving each
+ * member alone.  cuda_stream NULL: the batch creates its own stream.
+ * ------------------------------------------------------------------------ */
+typedef struct cismgpu_batch cismgpu_batch_t;
+int cismgpu_batch_create(cismgpu_batch_t **out, cismgpu_solver_t **solvers, int n, int precond,
+                         int linear_solve_ncheck, double tolerance, int maxiters, void *cuda_stream);
+int cismgpu_batch_run(cismgpu_batch_t *b);
+int cismgpu_batch_wait(cismgpu_batch_t *b, double *errs, int *niters, int *statuses);
+int cismgpu_batch_destroy(cismgpu_batch_t *b);
+
 /* Copy the current solution (caller's Fortran layout, halo entries included) to host memory. */
 int cismgpu_solver_get_x(cismgpu_solver_t *s, double *xu, double *xv);
 

@@ -131,3 +131,48 @@ def test_mixed_rejects_unsupported(gpu_lib):
     with pytest.raises(cg.CismGpuError) as e:
         S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 100)  # SIA in 2D
     assert e.value.status == 3
+
+
+def test_graph_batch_replays_bit_identical(gpu_lib):
+    """A CUDA-graph batch (sliding 3D members, each with its own log-normal friction) gives the
+    same bits as solving each member alone, on every replay."""
+    probs = [asm.batch_member(n, seed=s, nz=7) for s, n in enumerate((20, 27, 33, 24))]
+    solvers = [cg.DeviceSolver(P) for P in probs]
+    alone = []
+    for S in solvers:
+        e, n = S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 3000)
+        alone.append((e, n, S.x()))
+    B = cg.GraphBatch(solvers, precond=2, ncheck=5, tol=1e-8, maxiters=3000)
+    try:
+        with pytest.raises(cg.CismGpuError) as e:  # members belong to the batch until it is closed
+            solvers[1].solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 3000)
+        assert e.value.status == 4
+        for rep in range(2):
+            B.run()
+            errs, nits, sts = B.wait()
+            assert not np.any(sts)
+            for t, S in enumerate(solvers):
+                assert errs[t] == alone[t][0] and nits[t] == alone[t][1] and errs[t] < 1e-8
+                xu, xv = S.x()
+                np.testing.assert_array_equal(xu, alone[t][2][0])
+                np.testing.assert_array_equal(xv, alone[t][2][1])
+    finally:
+        B.close()
+
+
+def test_batch_more_tiles_than_ctas(gpu_lib):
+    """Thousands of tiles over a few hundred CTAs (blocked tile order with padding): every
+    member bit-identical to its solve alone, and within tolerance of the FP64 oracle."""
+    probs = [asm.ssa_random(ewn=90 + 7 * (s % 5), nsn=80 + 5 * (s % 3), seed=30 + s) for s in range(24)]
+    solvers = [cg.DeviceSolver(P) for P in probs]
+    errs, nits, sts = cg.solve_batch(solvers, cg.ALG_MIXED_CHRONGEAR, 1, 5, 1e-8, 5000)
+    assert not np.any(sts) and np.all(errs < 1e-8)
+    xb = [S.x() for S in solvers]
+    for t in (0, 7, 23):
+        e, n = solvers[t].solve(cg.ALG_MIXED_CHRONGEAR, 1, 5, 1e-8, 5000)
+        assert e == errs[t] and n == nits[t]
+        xu, xv = solvers[t].x()
+        np.testing.assert_array_equal(xu, xb[t][0])
+        np.testing.assert_array_equal(xv, xb[t][1])
+    st, ou, ov, oerr, onit = oracle.pcg("chrongear", probs[3], 1, tol=1e-8, maxiters=5000)
+    assert rel(xb[3], (ou, ov), probs[3]) < 1e-5
