@@ -487,6 +487,8 @@ static MDesc mixed_desc(const Solver &sv, int precond, int TY) {  // TY: the sol
     D.z = V + 6 * vs;
     D.d = V + 7 * vs;
     D.recs = m.recs;
+    D.bc = m.bc;
+    D.dflag = reinterpret_cast<int *>(m.bc + 2 * kBcastCopies);
     D.maps = m.maps;
     return D;
 }
@@ -542,6 +544,16 @@ static int mixed_solve_ty(const Geom &g, bool is3d, int nzm) {
     return TY;
 }
 
+// Tile height of a solve in batched and served launches (dynamic kernel): the single-solve
+// height, but at least 4 rows (3D) or 16 rows (2D), so that a tile carries enough work to
+// hide its fixed costs (descriptor, map, broadcast, record).  Depends on the solve only, so a
+// system gives the same bits alone and in any mix.
+static int mixed_batch_ty(const Geom &g, bool is3d, int nzm) {
+    int ty = std::max(mixed_solve_ty(g, is3d, nzm), is3d ? 4 : 16);
+    while (ty > 1 && mixed_grid(is3d, nzm, ty) == 0) --ty;
+    return ty;
+}
+
 // A launch keeps the FP32 matrix in shared memory (2D only) when its tiles fit one per
 // co-resident CTA with the shared-memory layout of its tallest tile.
 static bool mixed_resident(bool is3d, int nzm, int TYmax, long long ntiles) {
@@ -573,6 +585,7 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
         CU(alloc((void **)&m.pre, (size_t)6 * nvec * sizeof(float)));
         CU(alloc((void **)&m.vec, (size_t)16 * nvec * sizeof(float)));
         CU(alloc((void **)&m.state, sizeof(MState)));
+        CU(alloc((void **)&m.bc, (2 * kBcastCopies + 1) * sizeof(Bcast)));  // + the done-flag line
         CU(alloc((void **)&m.desc, sizeof(MDesc)));
         CU(alloc((void **)&m.ctl, sizeof(MCtl)));
         m.nbytes = bytes;
@@ -650,6 +663,7 @@ static int mixed_reset(Solver &sv, cudaStream_t s) {
     CU(cudaGetLastError());
     CU(cudaMemsetAsync(sv.mixed.vec, 0, (size_t)16 * sv.nvec * sizeof(float), s));
     CU(cudaMemsetAsync(sv.mixed.recs, 0, (size_t)sv.mixed.ntiles * 2 * sizeof(TileRec), s));  // tags restart at 1
+    CU(cudaMemsetAsync(sv.mixed.bc, 0, (2 * kBcastCopies + 1) * sizeof(Bcast), s));       // broadcast tag 0 = x0 state
     return CISMGPU_OK;
 }
 
@@ -698,6 +712,44 @@ static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_t
                     (void *)&resident, (void *)&d_ctl, (void *)&max_steps};
     CU(cudaLaunchCooperativeKernel((const void *)k_mixed<NC, NZM>, dim3(grid), dim3(kBlock), args, smem, s));
     return CISMGPU_OK;
+}
+
+template <int NC, int NZM>
+static int mixed_dyn_launch(const MDesc *d_descs, MState *d_states, const unsigned *d_tick0, int nsolve,
+                            const MTile *d_tiles, int ntiles, int TY, MCtl *d_ctl, int max_steps, int grid,
+                            cudaStream_t s) {
+    const size_t smem = MLayout<NC, NZM>(TY, false).bytes();
+    void *args[] = {(void *)&d_descs, (void *)&d_states, (void *)&d_tick0, (void *)&nsolve, (void *)&d_tiles,
+                    (void *)&ntiles, (void *)&TY, (void *)&d_ctl, (void *)&max_steps};
+    CU(cudaLaunchCooperativeKernel((const void *)k_mixed_dyn<NC, NZM>, dim3(grid), dim3(kBlock), args, smem, s));
+    return CISMGPU_OK;
+}
+
+static const void *mixed_dyn_kernel(bool is3d, int nzm) {
+    if (!is3d) return (const void *)k_mixed_dyn<9, 1>;
+    if (nzm == 16) return (const void *)k_mixed_dyn<27, 16>;
+    return (const void *)k_mixed_dyn<27, 32>;
+}
+
+// Co-resident CTAs of the dynamic kernel at tile height TY (sets its shared-memory attribute;
+// call outside any stream capture).
+static int mixed_dyn_grid(bool is3d, int nzm, int TY) {
+    const size_t smem = mixed_smem(is3d, nzm, TY, false);
+    if (smem > 227 * 1024 - 64) return 0;
+    const void *k = mixed_dyn_kernel(is3d, nzm);
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    int dev = 0, nsm = 0, occ = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kBlock, smem) != cudaSuccess) return 0;
+    return nsm * occ;
+}
+
+static int mixed_dyn_dispatch(bool is3d, int nzm, const MDesc *d, MState *st, const unsigned *tick0, int nsolve,
+                              const MTile *t, int nt, int TY, MCtl *ctl, int max_steps, int grid, cudaStream_t s) {
+    if (!is3d) return mixed_dyn_launch<9, 1>(d, st, tick0, nsolve, t, nt, TY, ctl, max_steps, grid, s);
+    if (nzm == 16) return mixed_dyn_launch<27, 16>(d, st, tick0, nsolve, t, nt, TY, ctl, max_steps, grid, s);
+    return mixed_dyn_launch<27, 32>(d, st, tick0, nsolve, t, nt, TY, ctl, max_steps, grid, s);
 }
 
 static int mixed_dispatch(bool is3d, int nzm, const MDesc *d, MState *st, const MTile *t, int nt, int TY,
@@ -913,20 +965,22 @@ static int oneshot_global_sum(int nx, int ny, int nz, const cismgpu_par_t *par, 
     return CISMGPU_OK;
 }
 
-// A prepared launch of the mixed solver over several handles (one persistent kernel).  The
-// device block holds, 256-byte aligned: descriptors, running states, initial states, the
-// tile list, the SolveState pointers of the members and the control word; results come back
-// into pinned host memory, so the whole sequence can be captured in a CUDA graph.
+// A prepared launch of the mixed solver over several handles: one dynamic persistent kernel
+// (k_mixed_dyn) over all their tiles.  The device block holds, 256-byte aligned: descriptors,
+// running states, initial states, launch-start ticks, the tile list, the SolveState pointers
+// of the members and the control word with its initial value; results come back into pinned
+// host memory, so the whole sequence can be captured in a CUDA graph.
 struct MixedBatch {
     std::vector<Solver *> svs;
-    bool is3d = false, resident = false;
+    bool is3d = false;
     int nzm = 0, TYmax = 1, grid = 0, ntl = 0, max_steps = 0;
     void *dmem = nullptr;
     MDesc *d_descs = nullptr;
     MState *d_states = nullptr, *d_states0 = nullptr;
+    unsigned *d_tick0 = nullptr;
     MTile *d_tiles = nullptr;
     SolveState **d_dst = nullptr;
-    MCtl *d_ctl = nullptr;
+    MCtl *d_ctl = nullptr, *d_ctl0 = nullptr;
     MState *h_states = nullptr;  // pinned
     MCtl *h_ctl = nullptr;       // pinned
     void release() {
@@ -940,8 +994,8 @@ struct MixedBatch {
     ~MixedBatch() { release(); }
 };
 
-// Prepare every member (FP32 matrix, maps, preconditioner; its own tile height), plan the
-// launch and upload the descriptors, initial states and the tile list.
+// Prepare every member (FP32 matrix, maps, preconditioner; its own batch tile height), plan
+// the launch and upload the descriptors, initial states and the tile list.
 static int batch_prepare(MixedBatch &B, int precond, int ncheck, double tol, int maxiters) {
     const int n = (int)B.svs.size();
     Solver &s0 = *B.svs[0];
@@ -953,18 +1007,17 @@ static int batch_prepare(MixedBatch &B, int precond, int ncheck, double tol, int
         Solver &sv = *B.svs[t];
         if (sv.is3d != s0.is3d || mixed_nzm(sv.g, sv.is3d) != B.nzm)
             return fail(CISMGPU_EINVAL, "batch members must share dims and the nz class (<=16 or <=32)");
-        tys[t] = mixed_solve_ty(sv.g, sv.is3d, B.nzm);
+        tys[t] = mixed_batch_ty(sv.g, sv.is3d, B.nzm);
         B.TYmax = std::max(B.TYmax, tys[t]);
         TRY(mixed_prepare(sv, precond, tys[t]));
         for (int k = 0; k < tiles_for(sv.g, tys[t]); ++k) tl.push_back(MTile{t, k});
     }
     for (int t = 0; t < n; ++t) CU(cudaStreamSynchronize(B.svs[t]->stream));
-    B.resident = mixed_resident(B.is3d, B.nzm, B.TYmax, (long long)tl.size());
-    B.grid = mixed_launch_grid(B.is3d, B.nzm, B.TYmax, B.resident, (int)tl.size());
+    B.grid = mixed_dyn_grid(B.is3d, B.nzm, B.TYmax);
     if (B.grid < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM at this tile height");
-    std::vector<MTile> order;
-    TRY(mixed_tile_order(tl, B.grid, order));
-    B.ntl = (int)order.size();
+    if ((long long)n > (long long)B.grid * kMaxCtaSolves)
+        return fail(CISMGPU_EUNSUPPORTED, "too many systems for one launch");
+    B.ntl = (int)tl.size();
     B.max_steps = 4 * maxiters + 16;
     std::vector<MDesc> descs(n);
     std::vector<SolveState *> dst(n);
@@ -973,37 +1026,46 @@ static int batch_prepare(MixedBatch &B, int precond, int ncheck, double tol, int
         dst[t] = B.svs[t]->state.as<SolveState>();
     }
     const std::vector<MState> states(n, mixed_init_state(tol, maxiters, ncheck));
+    const std::vector<unsigned> tick0(n, 0u);
+    MCtl c0;
+    std::memset(&c0, 0, sizeof(c0));
+    c0.active = n;
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     const size_t o_desc = 0, o_st = al(n * sizeof(MDesc)), o_st0 = o_st + al(n * sizeof(MState)),
-                 o_tl = o_st0 + al(n * sizeof(MState)), o_dst = o_tl + al(order.size() * sizeof(MTile)),
-                 o_ctl = o_dst + al(n * sizeof(SolveState *)), total = o_ctl + al(sizeof(MCtl));
+                 o_tk = o_st0 + al(n * sizeof(MState)), o_tl = o_tk + al(n * sizeof(unsigned)),
+                 o_dst = o_tl + al(tl.size() * sizeof(MTile)), o_ctl = o_dst + al(n * sizeof(SolveState *)),
+                 o_ctl0 = o_ctl + al(sizeof(MCtl)), total = o_ctl0 + al(sizeof(MCtl));
     CU(cudaMalloc(&B.dmem, total));
     char *base = static_cast<char *>(B.dmem);
     B.d_descs = reinterpret_cast<MDesc *>(base + o_desc);
     B.d_states = reinterpret_cast<MState *>(base + o_st);
     B.d_states0 = reinterpret_cast<MState *>(base + o_st0);
+    B.d_tick0 = reinterpret_cast<unsigned *>(base + o_tk);
     B.d_tiles = reinterpret_cast<MTile *>(base + o_tl);
     B.d_dst = reinterpret_cast<SolveState **>(base + o_dst);
     B.d_ctl = reinterpret_cast<MCtl *>(base + o_ctl);
+    B.d_ctl0 = reinterpret_cast<MCtl *>(base + o_ctl0);
     CU(cudaMallocHost((void **)&B.h_states, n * sizeof(MState)));
     CU(cudaMallocHost((void **)&B.h_ctl, sizeof(MCtl)));
     CU(cudaMemcpy(B.d_descs, descs.data(), n * sizeof(MDesc), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(B.d_states0, states.data(), n * sizeof(MState), cudaMemcpyHostToDevice));
-    CU(cudaMemcpy(B.d_tiles, order.data(), order.size() * sizeof(MTile), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(B.d_tick0, tick0.data(), n * sizeof(unsigned), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(B.d_tiles, tl.data(), tl.size() * sizeof(MTile), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(B.d_dst, dst.data(), n * sizeof(SolveState *), cudaMemcpyHostToDevice));
+    CU(cudaMemcpy(B.d_ctl0, &c0, sizeof(MCtl), cudaMemcpyHostToDevice));
     return CISMGPU_OK;
 }
 
-// One batched solve on stream s: member resets, initial states, the persistent launch, and
-// the results (each handle's SolveState, and pinned host copies).  No host synchronization
-// and no allocation, so it can be captured.
+// One batched solve on stream s: member resets, initial states and control word, the
+// persistent launch, and the results (each handle's SolveState, and pinned host copies).  No
+// host synchronization and no allocation, so it can be captured.
 static int batch_enqueue(MixedBatch &B, cudaStream_t s) {
     const int n = (int)B.svs.size();
     for (Solver *sv : B.svs) TRY(mixed_reset(*sv, s));
     CU(cudaMemcpyAsync(B.d_states, B.d_states0, n * sizeof(MState), cudaMemcpyDeviceToDevice, s));
-    CU(cudaMemsetAsync(B.d_ctl, 0, sizeof(MCtl), s));
-    TRY(mixed_dispatch(B.is3d, B.nzm, B.d_descs, B.d_states, B.d_tiles, B.ntl, B.TYmax, B.resident, B.d_ctl,
-                       B.max_steps, B.grid, s));
+    CU(cudaMemcpyAsync(B.d_ctl, B.d_ctl0, sizeof(MCtl), cudaMemcpyDeviceToDevice, s));
+    TRY(mixed_dyn_dispatch(B.is3d, B.nzm, B.d_descs, B.d_states, B.d_tick0, n, B.d_tiles, B.ntl, B.TYmax, B.d_ctl,
+                           B.max_steps, B.grid, s));
     k_mstates_to_solves<<<(n + 127) / 128, 128, 0, s>>>(B.d_states, B.d_dst, n, B.d_ctl);
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(B.h_states, B.d_states, n * sizeof(MState), cudaMemcpyDeviceToHost, s));

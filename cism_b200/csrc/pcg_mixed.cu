@@ -42,6 +42,16 @@ struct TileRec {
     unsigned tag, pad;
 };
 
+// The scalars a solve's leader broadcasts after summing a step's records (dynamic launches):
+// word = tag << 32 | done << 9 | par << 8 | step, written last.  Replicated kBcastCopies
+// times, one 256-byte line each, so that polls spread over several L2 slices.
+struct __align__(256) Bcast {
+    unsigned long long word;
+    double alpha, beta;
+    double pad[29];
+};
+constexpr int kBcastCopies = 8;
+
 // device-visible description of one solve
 struct MDesc {
     Geom g;
@@ -58,6 +68,8 @@ struct MDesc {
     float *r[2], *q[2], *Az[2];  // [2][nz][NQ] each (u, v planes)
     float *z, *d;                // [2][nz][NQ]
     TileRec *recs;       // [ntiles][2 step parities]
+    Bcast *bc;           // [2 step parities][kBcastCopies] (dynamic launches)
+    int *dflag;          // set once the solve is done (dynamic launches)
     const int *maps;     // [ntiles][(kTX+2)*(TY+2)] slot maps (k_slot_maps)
 };
 
@@ -74,8 +86,9 @@ struct MState {
 struct MTile { int solve, tile; };
 
 struct MCtl {
-    int abort;          // set on a wait timeout; every CTA leaves at its next wait
-    int pad[3];
+    int abort;                 // set on a wait timeout; every CTA leaves at its next wait
+    int active;                // dynamic launches: solves not yet done
+    unsigned long long next;   // dynamic launches: work counter (step * ntiles + tile list position)
 };
 
 // ---------------------------------------------------------------------------
@@ -118,6 +131,19 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 }
 __device__ __forceinline__ void st_relaxed(unsigned *p, unsigned v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ int ld_acquire_i(const int *p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
 }
 
 constexpr long long kWaitCycles = 1LL << 31;  // ~1 s at 2 GHz: a wait longer than this is a failure
@@ -806,6 +832,197 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
 }
 
 // ---------------------------------------------------------------------------
+// dynamic launches (batches and the serving loop)
+// ---------------------------------------------------------------------------
+// Leader duties of one step for every running solve this CTA leads: wait for the records
+// of all the solve's tiles, sum them in the same fixed order as reduce_wait (so results are
+// bit-identical to the single-solve kernel), advance the state and broadcast the scalars
+// the tiles need.  A finished solve is published to gstates, flagged and counted down.
+// Returns false if a wait gave up (here or in another CTA).
+__device__ bool lead_duties(MHead &hd, const MDesc *__restrict__ descs, MState *gstates, MCtl *ctl) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int cs = 0; cs < hd.nsolve; ++cs) {
+        if (hd.st[cs].done) continue;  // uniform: only thread 0 writes st, before a barrier
+        const MDesc &D = descs[hd.sid[cs]];
+        const int ntl = D.ntiles;
+        const unsigned tag = hd.st[cs].tick + 1u;
+        const TileRec *R = D.recs + (tag & 1u);
+        DD a0{0.0, 0.0}, a1{0.0, 0.0}, a2{0.0, 0.0};
+        int bad = 0;
+        for (int w = threadIdx.x; w < ntl && !bad; w += kBlock) {
+            const TileRec *rp = R + 2 * (size_t)w;
+            if (ld_acquire(&rp->tag) != tag) {
+                const long long t0 = clock64();
+                unsigned spins = 0;
+                while (ld_acquire(&rp->tag) != tag) {
+                    __nanosleep(spins < 16 ? 20 : 100);
+                    if ((++spins & 31u) == 0) {
+                        if (*(volatile int *)&ctl->abort) { bad = 1; break; }
+                        if (clock64() - t0 > kWaitCycles) {
+                            atomicExch(&ctl->abort, 1);
+                            bad = 1;
+                            break;
+                        }
+                    }
+                }
+                if (bad) break;
+            }
+            a0 = dd_add_d(a0, __ldcg(&rp->p0));
+            a1 = dd_add_d(a1, __ldcg(&rp->p1));
+            a2 = dd_add_d(a2, __ldcg(&rp->p2));
+        }
+        if (__syncthreads_or(bad)) return false;
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            const DD o0 = dd_shfl_down(a0, off), o1 = dd_shfl_down(a1, off), o2 = dd_shfl_down(a2, off);
+            if (lane + off < 32) { a0 = dd_add(a0, o0); a1 = dd_add(a1, o1); a2 = dd_add(a2, o2); }
+        }
+        if (lane == 0) { hd.rdd[warp][0] = a0; hd.rdd[warp][1] = a1; hd.rdd[warp][2] = a2; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            DD s0 = hd.rdd[0][0], s1 = hd.rdd[0][1], s2 = hd.rdd[0][2];
+            for (int w = 1; w < kBlock / 32; ++w) {
+                s0 = dd_add(s0, hd.rdd[w][0]);
+                s1 = dd_add(s1, hd.rdd[w][1]);
+                s2 = dd_add(s2, hd.rdd[w][2]);
+            }
+            MState &S = hd.st[cs];
+            advance_state(S, s0.hi + s0.lo, s1.hi + s1.lo, s2.hi + s2.lo);
+            S.tick = tag;
+            if (S.done) gstates[hd.sid[cs]] = S;
+            Bcast *B = D.bc + (size_t)(tag & 1u) * kBcastCopies;
+            for (int k = 0; k < kBcastCopies; ++k) {
+                B[k].alpha = S.alpha;
+                B[k].beta = S.beta;
+            }
+            __threadfence();  // the state, the scalars and (cumulatively) the records before the word
+            const unsigned long long word = ((unsigned long long)tag << 32) | (unsigned)(S.done << 9) |
+                                            (unsigned)(S.par << 8) | (unsigned)S.step;
+            for (int k = 0; k < kBcastCopies; ++k) st_relaxed64(&B[k].word, word);
+            if (S.done) {
+                st_relaxed(reinterpret_cast<unsigned *>(D.dflag), 1u);
+                atomicSub(&ctl->active, 1);
+            }
+        }
+        __syncthreads();
+    }
+    return true;
+}
+
+// Dynamic persistent kernel.  Work items are (step, tile list position), handed out in
+// order by one atomic counter, so every CTA works on whatever tiles are left: solves that
+// converge early free the GPU for the others.  Solve i is led by CTA i * grid / nsolve,
+// which sums its records and broadcasts its scalars (lead_duties); a CTA that takes a tile
+// of solve X at step s waits for X's broadcast of step s (tag = ltick0[X] + s).  Before a CTA
+// works on any item of step s it finishes its leader duties of every earlier step, so the
+// waits cannot form a cycle.  The per-tile arithmetic is tile_step, and the sums are taken
+// in the same fixed order as the single-solve kernel, so every result is bit-identical to
+// solving the system alone with the same tile height.  Stops when all solves are done or
+// after max_steps steps (a serving epoch), after folding in the last step's sums.
+template <int NC, int NZM>
+__global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict__ descs, MState *states,
+                                                         const unsigned *__restrict__ ltick0, int nsolve,
+                                                         const MTile *__restrict__ tiles, int ntiles, int TYmax,
+                                                         MCtl *ctl, int max_steps) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    MHead &hd = *reinterpret_cast<MHead *>(smem);
+    __shared__ unsigned long long s_item;
+    __shared__ int s_flag;
+    __shared__ MState s_view;
+    if (threadIdx.x == 0) {  // the solves this CTA leads
+        int n = 0;
+        for (int i = 0; i < nsolve && n < kMaxCtaSolves; ++i) {
+            if ((int)((long long)i * gridDim.x / nsolve) != (int)blockIdx.x) continue;
+            hd.sid[n] = i;
+            hd.owner[n] = 1;
+            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&states[i]);
+            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&hd.st[n]);
+            for (int w8 = 0; w8 < (int)(sizeof(MState) / 8); ++w8) dst[w8] = __ldcg(src + w8);
+            ++n;
+        }
+        hd.nsolve = n;
+        hd.cur = -1;
+    }
+    __syncthreads();
+    int duty_step = 0;  // leader duties of steps < duty_step are done
+    bool epoch_end = false;
+    for (;;) {
+        __syncthreads();  // every thread is done with the previous item's shared values
+        if (threadIdx.x == 0) {
+            s_flag = (*(volatile int *)&ctl->active <= 0 || *(volatile int *)&ctl->abort) ? 1 : 0;
+            if (!s_flag) s_item = atomicAdd(&ctl->next, 1ull);
+        }
+        __syncthreads();
+        if (s_flag) break;  // all solves done (or a wait gave up somewhere)
+        const long long step = (long long)(s_item / (unsigned long long)ntiles);
+        const int pos = (int)(s_item % (unsigned long long)ntiles);
+        if (step >= max_steps) {
+            epoch_end = true;
+            break;
+        }
+        while (duty_step < step) {
+            if (!lead_duties(hd, descs, states, ctl)) return;
+            ++duty_step;
+        }
+        const MTile T = tiles[pos];
+        if (T.solve < 0) continue;
+        // the solve's scalars after `step` steps of this launch
+        if (threadIdx.x == 0) {
+            const MDesc *Dp = descs + T.solve;
+            const unsigned tag = ltick0[T.solve] + (unsigned)step;
+            const Bcast *B = Dp->bc + (size_t)(tag & 1u) * kBcastCopies + (blockIdx.x % kBcastCopies);
+            const int *dflag = Dp->dflag;
+            int st = 0;  // 0 ready, 1 solve done, 2 gave up
+            unsigned long long word = ld_acquire64(&B->word);
+            if ((unsigned)(word >> 32) != tag) {
+                const long long t0 = clock64();
+                unsigned spins = 0;
+                while ((unsigned)((word = ld_acquire64(&B->word)) >> 32) != tag) {
+                    if (ld_acquire_i(dflag)) { st = 1; break; }
+                    __nanosleep(spins < 16 ? 20 : 100);
+                    if ((++spins & 31u) == 0) {
+                        if (*(volatile int *)&ctl->abort) { st = 2; break; }
+                        if (clock64() - t0 > kWaitCycles) {
+                            atomicExch(&ctl->abort, 1);
+                            st = 2;
+                            break;
+                        }
+                    }
+                }
+            }
+            if (st == 0 && ((word >> 9) & 1u)) st = 1;
+            if (st == 0) {
+                s_view.step = (int)(word & 0xffu);
+                s_view.par = (int)((word >> 8) & 1u);
+                s_view.alpha = __ldcg(&B->alpha);
+                s_view.beta = __ldcg(&B->beta);
+                s_view.tick = tag;
+                if (hd.cur != T.solve) {
+                    hd.D = *Dp;
+                    hd.cur = T.solve;
+                }
+            }
+            s_flag = st;
+        }
+        __syncthreads();
+        if (s_flag == 2) return;
+        if (s_flag == 1) continue;
+        tile_step<NC, NZM>(s_view, T.tile, false, TYmax, hd, smem);
+    }
+    if (threadIdx.x == 0) s_flag = *(volatile int *)&ctl->abort;
+    __syncthreads();
+    if (s_flag) return;
+    // a serving epoch ends: fold in the sums of the last steps so the next launch resumes exactly
+    if (epoch_end)
+        while (duty_step < max_steps) {
+            if (!lead_duties(hd, descs, states, ctl)) return;
+            ++duty_step;
+        }
+    if (threadIdx.x == 0)
+        for (int cs = 0; cs < hd.nsolve; ++cs) states[hd.sid[cs]] = hd.st[cs];
+}
+
+// ---------------------------------------------------------------------------
 // setup kernels: FP32 matrix copy and FP32 preconditioner factors
 // ---------------------------------------------------------------------------
 // FP32 copy of the coefficient planes; couplings whose neighbour lies outside the
@@ -874,6 +1091,7 @@ struct MixedBufs {
     float *A32 = nullptr, *pre = nullptr, *vec = nullptr;
     int *maps = nullptr;
     TileRec *recs = nullptr;
+    Bcast *bc = nullptr;       // [2][kBcastCopies] broadcast lines, then one line holding the done flag
     MState *state = nullptr;
     MDesc *desc = nullptr;
     MTile *tiles = nullptr;
@@ -884,7 +1102,7 @@ struct MixedBufs {
     long long maps_cap = 0;
     void release() {
         for (void *p : {(void *)A32, (void *)pre, (void *)vec, (void *)recs, (void *)state, (void *)desc,
-                        (void *)tiles, (void *)ctl, (void *)maps})
+                        (void *)tiles, (void *)ctl, (void *)maps, (void *)bc})
             if (p) cudaFree(p);
         A32 = pre = vec = nullptr;
         maps = nullptr;
@@ -892,6 +1110,7 @@ struct MixedBufs {
         maps_cap = 0;
         TY = 0;
         recs = nullptr;
+        bc = nullptr;
         state = nullptr;
         desc = nullptr;
         tiles = nullptr;

@@ -205,7 +205,9 @@ int cismgpu_solver_solve(cismgpu_solver_t *s, int algorithm, int precond, int li
 /* Solve n independent systems (uneven sizes allowed) in ONE persistent cooperative
  * launch on cuda_stream (NULL: the first handle's stream).  algorithm must be
  * CISMGPU_ALG_MIXED_CHRONGEAR; all handles must have the same dims, and nz <= 32.
- * Every system's result is bit-identical to solving it alone.  Per-system
+ * Every system's result is bit-identical to the same system batched alone
+ * (batches use a dynamic persistent kernel with per-system tile heights, so
+ * what else is in the batch never changes a result).  Per-system
  * err/niters/status arrays of length n; returns the first nonzero status. */
 int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm, int precond,
                                int linear_solve_ncheck, double tolerance, int maxiters,
@@ -222,8 +224,8 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
  * members belong to the batch: cismgpu_solver_solve, _solve_batch, _destroy
  * and another batch_create on them return CISMGPU_EINVAL; cismgpu_solver_get_x
  * first waits for the batch's stream.  A changed matrix needs a new batch.
- * Results are bit-identical to cismgpu_solver_solve_batch and to solving each
- * member alone.  cuda_stream NULL: the batch creates its own stream.
+ * Results are bit-identical to cismgpu_solver_solve_batch and to each member
+ * batched alone.  cuda_stream NULL: the batch creates its own stream.
  * ------------------------------------------------------------------------ */
 typedef struct cismgpu_batch cismgpu_batch_t;
 int cismgpu_batch_create(cismgpu_batch_t **out, cismgpu_solver_t **solvers, int n, int precond,

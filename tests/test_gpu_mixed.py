@@ -71,14 +71,22 @@ def test_mixed_is_deterministic(gpu_lib):
     np.testing.assert_array_equal(a[1][1], b[1][1])
 
 
+def batch_alone(S, precond, maxiters):
+    """A system solved alone by the batched kernel (same tile height as in any batch)."""
+    errs, nits, sts = cg.solve_batch([S], cg.ALG_MIXED_CHRONGEAR, precond, 5, 1e-8, maxiters)
+    assert sts[0] == 0
+    return errs[0], nits[0], S.x()
+
+
 def test_batch_equals_alone(gpu_lib):
-    """Uneven 3D solves in one persistent launch give bit-identical results to solving each alone."""
+    """Uneven 3D solves in one dynamic persistent launch give bit-identical results to each
+    system batched alone, and agree with the single-solve kernel within the solve tolerance."""
     probs = [problems.slab_3d(seed=s, ewn=8 + 5 * s, nsn=9 + 3 * s, nz=5 + (s % 3)) for s in range(5)]
     solvers = [cg.DeviceSolver(P) for P in probs]
-    alone = []
-    for S in solvers:
-        e, n = S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 3000)
-        alone.append((e, n, S.x()))
+    alone = [batch_alone(S, 2, 3000) for S in solvers]
+    for S, P in zip(solvers, probs):
+        S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 3000)
+        assert rel(S.x(), alone[solvers.index(S)][2], P) < 1e-6
     errs, nits, sts = cg.solve_batch(solvers, cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 3000)
     assert not np.any(sts)
     for t, S in enumerate(solvers):
@@ -138,10 +146,7 @@ def test_graph_batch_replays_bit_identical(gpu_lib):
     same bits as solving each member alone, on every replay."""
     probs = [asm.batch_member(n, seed=s, nz=7) for s, n in enumerate((20, 27, 33, 24))]
     solvers = [cg.DeviceSolver(P) for P in probs]
-    alone = []
-    for S in solvers:
-        e, n = S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 3000)
-        alone.append((e, n, S.x()))
+    alone = [batch_alone(S, 2, 3000) for S in solvers]
     B = cg.GraphBatch(solvers, precond=2, ncheck=5, tol=1e-8, maxiters=3000)
     try:
         with pytest.raises(cg.CismGpuError) as e:  # members belong to the batch until it is closed
@@ -169,9 +174,8 @@ def test_batch_more_tiles_than_ctas(gpu_lib):
     assert not np.any(sts) and np.all(errs < 1e-8)
     xb = [S.x() for S in solvers]
     for t in (0, 7, 23):
-        e, n = solvers[t].solve(cg.ALG_MIXED_CHRONGEAR, 1, 5, 1e-8, 5000)
+        e, n, (xu, xv) = batch_alone(solvers[t], 1, 5000)
         assert e == errs[t] and n == nits[t]
-        xu, xv = solvers[t].x()
         np.testing.assert_array_equal(xu, xb[t][0])
         np.testing.assert_array_equal(xv, xb[t][1])
     st, ou, ov, oerr, onit = oracle.pcg("chrongear", probs[3], 1, tol=1e-8, maxiters=5000)
