@@ -62,6 +62,17 @@ class CParallel(ctypes.Structure):
         "no_ice_bc", "reprosum", "tasks_row", "tasks_col")]
 
 
+class CRequest(ctypes.Structure):
+    """cismgpu_request_t: one system for the serving loop."""
+    _fields_ = [("dims", ctypes.c_int), ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("par", ctypes.POINTER(CParallel)), ("indxA", ctypes.c_void_p), ("active_vertex", ctypes.c_void_p),
+                ("Auu", ctypes.c_void_p), ("Auv", ctypes.c_void_p), ("Avu", ctypes.c_void_p),
+                ("Avv", ctypes.c_void_p), ("bu", ctypes.c_void_p), ("bv", ctypes.c_void_p),
+                ("xu0", ctypes.c_void_p), ("xv0", ctypes.c_void_p), ("xu", ctypes.c_void_p), ("xv", ctypes.c_void_p),
+                ("precond", ctypes.c_int), ("linear_solve_ncheck", ctypes.c_int), ("tolerance", ctypes.c_double),
+                ("maxiters", ctypes.c_int)]
+
+
 @dataclasses.dataclass
 class ParallelType:
     """The fields of type(parallel_type) read on this path (libglimmer/parallel_mpi.F90:78-153)."""
@@ -125,6 +136,18 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_batch_wait.restype = ctypes.c_int
     lib.cismgpu_batch_destroy.argtypes = [vp]
     lib.cismgpu_batch_destroy.restype = ctypes.c_int
+    lib.cismgpu_server_create.argtypes = [P(vp), ctypes.c_size_t, i32]
+    lib.cismgpu_server_create.restype = ctypes.c_int
+    lib.cismgpu_server_submit.argtypes = [vp, P(CRequest), P(ctypes.c_longlong)]
+    lib.cismgpu_server_submit.restype = ctypes.c_int
+    lib.cismgpu_server_poll.argtypes = [vp, ctypes.c_longlong, P(i32), P(dbl), P(i32), P(i32), P(dbl), P(dbl)]
+    lib.cismgpu_server_poll.restype = ctypes.c_int
+    lib.cismgpu_server_drain.argtypes = [vp]
+    lib.cismgpu_server_drain.restype = ctypes.c_int
+    lib.cismgpu_server_stats.argtypes = [vp, P(ctypes.c_longlong), P(ctypes.c_size_t), P(i32), P(i32)]
+    lib.cismgpu_server_stats.restype = ctypes.c_int
+    lib.cismgpu_server_destroy.argtypes = [vp]
+    lib.cismgpu_server_destroy.restype = ctypes.c_int
     lib.cismgpu_solver_get_x.argtypes = [vp, d, d]
     lib.cismgpu_solver_get_x.restype = ctypes.c_int
     lib.cismgpu_solver_profile.argtypes = [vp, i32]
@@ -413,6 +436,82 @@ class GraphBatch:
     def close(self):
         if self.handle:
             self._lib.cismgpu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The continuous-batching serving loop (cismgpu_server_*): submit() queues a system and
+    returns its id at once; the library's server thread admits it within the HBM budget,
+    solves it alongside whatever else is running, and writes the solution into the arrays
+    returned by result()."""
+
+    def __init__(self, hbm_budget_bytes=150 * 10**9, epoch_steps=64):
+        lib = load_library()
+        self._lib = lib
+        h = ctypes.c_void_p()
+        _check(lib, lib.cismgpu_server_create(ctypes.byref(h), int(hbm_budget_bytes), int(epoch_steps)))
+        self.handle = h.value
+        self._keep = {}
+
+    def submit(self, problem, precond=HO_PRECOND_DIAG, ncheck=5, tol=1e-8, maxiters=20000, x0=None) -> int:
+        P = problem
+        is3d = P.kind == "3d"
+        nv = (P.nx - 1) * (P.ny - 1)
+        nvec = nv * (P.nz if is3d else 1)
+        nblk = nvec * (27 if is3d else 9)
+        indx = np.arange(1, 28 if is3d else 10, dtype=np.int32)
+        par = _par(P.par)
+        xu = np.zeros_like(P.bu)
+        xv = np.zeros_like(P.bv)
+        keep = [P, indx, par, xu, xv]
+        rq = CRequest(3 if is3d else 2, P.nx, P.ny, P.nz if is3d else 1, ctypes.pointer(par),
+                      _ptr(indx, np.int32, indx.size), _ptr(P.active_vertex, np.int32, nv),
+                      _ptr(P.Auu, np.float64, nblk), _ptr(P.Auv, np.float64, nblk), _ptr(P.Avu, np.float64, nblk),
+                      _ptr(P.Avv, np.float64, nblk), _ptr(P.bu, np.float64, nvec), _ptr(P.bv, np.float64, nvec),
+                      None, None, _ptr(xu, np.float64, nvec, True), _ptr(xv, np.float64, nvec, True),
+                      precond, ncheck, tol, maxiters)
+        if x0 is not None:
+            rq.xu0 = _ptr(x0[0], np.float64, nvec)
+            rq.xv0 = _ptr(x0[1], np.float64, nvec)
+            keep.append(x0)
+        rid = ctypes.c_longlong()
+        _check(self._lib, self._lib.cismgpu_server_submit(self.handle, ctypes.byref(rq), ctypes.byref(rid)))
+        self._keep[rid.value] = keep
+        return rid.value
+
+    def poll(self, rid):
+        """dict(done, err, niters, status, latency_ms, queue_ms)."""
+        d, e, n, st, lat, q = (ctypes.c_int(), ctypes.c_double(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double(),
+                               ctypes.c_double())
+        _check(self._lib, self._lib.cismgpu_server_poll(self.handle, rid, d, e, n, st, lat, q))
+        return {"done": bool(d.value), "err": e.value, "niters": n.value, "status": st.value,
+                "latency_ms": lat.value, "queue_ms": q.value}
+
+    def result(self, rid):
+        """(xu, xv, poll dict) of a finished request."""
+        info = self.poll(rid)
+        if not info["done"]:
+            raise RuntimeError(f"request {rid} is not done")
+        keep = self._keep[rid]
+        return keep[3], keep[4], info
+
+    def drain(self):
+        _check(self._lib, self._lib.cismgpu_server_drain(self.handle))
+
+    def stats(self):
+        ep, by, ac, qu = ctypes.c_longlong(), ctypes.c_size_t(), ctypes.c_int(), ctypes.c_int()
+        _check(self._lib, self._lib.cismgpu_server_stats(self.handle, ep, by, ac, qu))
+        return {"epochs": ep.value, "bytes_in_use": by.value, "active": ac.value, "queued": qu.value}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.cismgpu_server_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -229,6 +229,7 @@ struct Solver {
         const int id[2] = {id_u, id_v};
         for (int t = 0; t < 2; ++t) {
             if (is3d) {
+                CU(raw.ensure((size_t)nvec * sizeof(double)));  // staging for the layout change
                 k_vec_out<<<nblocks(nvec), kBlock, 0, stream>>>(g, V + (size_t)id[t] * nvec, raw.as<double>());
                 CU(cudaGetLastError());
                 CU(cudaMemcpyAsync(out[t], raw.p, nvec * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -715,7 +716,7 @@ static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_t
 }
 
 template <int NC, int NZM>
-static int mixed_dyn_launch(const MDesc *d_descs, MState *d_states, const unsigned *d_tick0, int nsolve,
+static int mixed_dyn_launch(const MDesc *d_descs, MState *const *d_states, const unsigned *d_tick0, int nsolve,
                             const MTile *d_tiles, int ntiles, int TY, MCtl *d_ctl, int max_steps, int grid,
                             cudaStream_t s) {
     const size_t smem = MLayout<NC, NZM>(TY, false).bytes();
@@ -745,7 +746,7 @@ static int mixed_dyn_grid(bool is3d, int nzm, int TY) {
     return nsm * occ;
 }
 
-static int mixed_dyn_dispatch(bool is3d, int nzm, const MDesc *d, MState *st, const unsigned *tick0, int nsolve,
+static int mixed_dyn_dispatch(bool is3d, int nzm, const MDesc *d, MState *const *st, const unsigned *tick0, int nsolve,
                               const MTile *t, int nt, int TY, MCtl *ctl, int max_steps, int grid, cudaStream_t s) {
     if (!is3d) return mixed_dyn_launch<9, 1>(d, st, tick0, nsolve, t, nt, TY, ctl, max_steps, grid, s);
     if (nzm == 16) return mixed_dyn_launch<27, 16>(d, st, tick0, nsolve, t, nt, TY, ctl, max_steps, grid, s);
@@ -977,6 +978,7 @@ struct MixedBatch {
     void *dmem = nullptr;
     MDesc *d_descs = nullptr;
     MState *d_states = nullptr, *d_states0 = nullptr;
+    MState **d_sptr = nullptr;   // d_sptr[t] = d_states + t
     unsigned *d_tick0 = nullptr;
     MTile *d_tiles = nullptr;
     SolveState **d_dst = nullptr;
@@ -1032,7 +1034,8 @@ static int batch_prepare(MixedBatch &B, int precond, int ncheck, double tol, int
     c0.active = n;
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     const size_t o_desc = 0, o_st = al(n * sizeof(MDesc)), o_st0 = o_st + al(n * sizeof(MState)),
-                 o_tk = o_st0 + al(n * sizeof(MState)), o_tl = o_tk + al(n * sizeof(unsigned)),
+                 o_sp = o_st0 + al(n * sizeof(MState)), o_tk = o_sp + al(n * sizeof(MState *)),
+                 o_tl = o_tk + al(n * sizeof(unsigned)),
                  o_dst = o_tl + al(tl.size() * sizeof(MTile)), o_ctl = o_dst + al(n * sizeof(SolveState *)),
                  o_ctl0 = o_ctl + al(sizeof(MCtl)), total = o_ctl0 + al(sizeof(MCtl));
     CU(cudaMalloc(&B.dmem, total));
@@ -1040,6 +1043,7 @@ static int batch_prepare(MixedBatch &B, int precond, int ncheck, double tol, int
     B.d_descs = reinterpret_cast<MDesc *>(base + o_desc);
     B.d_states = reinterpret_cast<MState *>(base + o_st);
     B.d_states0 = reinterpret_cast<MState *>(base + o_st0);
+    B.d_sptr = reinterpret_cast<MState **>(base + o_sp);
     B.d_tick0 = reinterpret_cast<unsigned *>(base + o_tk);
     B.d_tiles = reinterpret_cast<MTile *>(base + o_tl);
     B.d_dst = reinterpret_cast<SolveState **>(base + o_dst);
@@ -1050,6 +1054,9 @@ static int batch_prepare(MixedBatch &B, int precond, int ncheck, double tol, int
     CU(cudaMemcpy(B.d_descs, descs.data(), n * sizeof(MDesc), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(B.d_states0, states.data(), n * sizeof(MState), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(B.d_tick0, tick0.data(), n * sizeof(unsigned), cudaMemcpyHostToDevice));
+    std::vector<MState *> sptr(n);
+    for (int t = 0; t < n; ++t) sptr[t] = B.d_states + t;
+    CU(cudaMemcpy(B.d_sptr, sptr.data(), n * sizeof(MState *), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(B.d_tiles, tl.data(), tl.size() * sizeof(MTile), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(B.d_dst, dst.data(), n * sizeof(SolveState *), cudaMemcpyHostToDevice));
     CU(cudaMemcpy(B.d_ctl0, &c0, sizeof(MCtl), cudaMemcpyHostToDevice));
@@ -1064,7 +1071,7 @@ static int batch_enqueue(MixedBatch &B, cudaStream_t s) {
     for (Solver *sv : B.svs) TRY(mixed_reset(*sv, s));
     CU(cudaMemcpyAsync(B.d_states, B.d_states0, n * sizeof(MState), cudaMemcpyDeviceToDevice, s));
     CU(cudaMemcpyAsync(B.d_ctl, B.d_ctl0, sizeof(MCtl), cudaMemcpyDeviceToDevice, s));
-    TRY(mixed_dyn_dispatch(B.is3d, B.nzm, B.d_descs, B.d_states, B.d_tick0, n, B.d_tiles, B.ntl, B.TYmax, B.d_ctl,
+    TRY(mixed_dyn_dispatch(B.is3d, B.nzm, B.d_descs, B.d_sptr, B.d_tick0, n, B.d_tiles, B.ntl, B.TYmax, B.d_ctl,
                            B.max_steps, B.grid, s));
     k_mstates_to_solves<<<(n + 127) / 128, 128, 0, s>>>(B.d_states, B.d_dst, n, B.d_ctl);
     CU(cudaGetLastError());
@@ -1391,4 +1398,5 @@ const char *cismgpu_version(void) { return "cismgpu 0.2 (sm_100a)"; }
 
 }  // extern "C"
 
+#include "server.cu"
 #include "noalloc.cu"

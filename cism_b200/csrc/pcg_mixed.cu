@@ -839,7 +839,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
 // bit-identical to the single-solve kernel), advance the state and broadcast the scalars
 // the tiles need.  A finished solve is published to gstates, flagged and counted down.
 // Returns false if a wait gave up (here or in another CTA).
-__device__ bool lead_duties(MHead &hd, const MDesc *__restrict__ descs, MState *gstates, MCtl *ctl) {
+__device__ bool lead_duties(MHead &hd, const MDesc *__restrict__ descs, MState *const *gstates, MCtl *ctl) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int cs = 0; cs < hd.nsolve; ++cs) {
         if (hd.st[cs].done) continue;  // uniform: only thread 0 writes st, before a barrier
@@ -889,7 +889,7 @@ __device__ bool lead_duties(MHead &hd, const MDesc *__restrict__ descs, MState *
             MState &S = hd.st[cs];
             advance_state(S, s0.hi + s0.lo, s1.hi + s1.lo, s2.hi + s2.lo);
             S.tick = tag;
-            if (S.done) gstates[hd.sid[cs]] = S;
+            if (S.done) *gstates[hd.sid[cs]] = S;
             Bcast *B = D.bc + (size_t)(tag & 1u) * kBcastCopies;
             for (int k = 0; k < kBcastCopies; ++k) {
                 B[k].alpha = S.alpha;
@@ -920,7 +920,7 @@ __device__ bool lead_duties(MHead &hd, const MDesc *__restrict__ descs, MState *
 // solving the system alone with the same tile height.  Stops when all solves are done or
 // after max_steps steps (a serving epoch), after folding in the last step's sums.
 template <int NC, int NZM>
-__global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict__ descs, MState *states,
+__global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict__ descs, MState *const *states,
                                                          const unsigned *__restrict__ ltick0, int nsolve,
                                                          const MTile *__restrict__ tiles, int ntiles, int TYmax,
                                                          MCtl *ctl, int max_steps) {
@@ -935,7 +935,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict
             if ((int)((long long)i * gridDim.x / nsolve) != (int)blockIdx.x) continue;
             hd.sid[n] = i;
             hd.owner[n] = 1;
-            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(&states[i]);
+            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(states[i]);
             unsigned long long *dst = reinterpret_cast<unsigned long long *>(&hd.st[n]);
             for (int w8 = 0; w8 < (int)(sizeof(MState) / 8); ++w8) dst[w8] = __ldcg(src + w8);
             ++n;
@@ -1019,7 +1019,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict
             ++duty_step;
         }
     if (threadIdx.x == 0)
-        for (int cs = 0; cs < hd.nsolve; ++cs) states[hd.sid[cs]] = hd.st[cs];
+        for (int cs = 0; cs < hd.nsolve; ++cs) *states[hd.sid[cs]] = hd.st[cs];
 }
 
 // ---------------------------------------------------------------------------

@@ -1,0 +1,383 @@
+// server.cu -- continuous-batching serving loop for the mixed-precision solver.
+//
+// Requests (one linear system each, in the caller's Fortran layout) are queued by
+// cismgpu_server_submit and served by one host thread:
+//   * admission: in arrival order while the HBM budget allows; an admitted request gets
+//     its own device-resident handle (matrix, FP32 copy, preconditioner, Krylov vectors),
+//     uploaded on the handle's own stream while the GPU runs the current epoch;
+//   * epochs: every active request of a kernel class (2D, 3D nz <= 16, 3D nz <= 32) takes
+//     part in one launch of the dynamic persistent kernel (k_mixed_dyn) for up to
+//     epoch_steps steps; a request's state (scalars in its MState, vectors in its buffers)
+//     stays on the device between epochs, so a request joins and leaves between any two
+//     epochs without restarting anyone;
+//   * retirement: a finished request's x is copied into the caller's arrays, its handle
+//     freed and its bytes returned to the budget.
+// Tile heights and the order of every sum depend on the request only, so a result is
+// bit-identical whether the request is served alone or in any mix.
+#pragma once
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <thread>
+#include <unordered_map>
+
+namespace cismgpu {
+
+__global__ void k_gather_states(MState *const *src, MState *dst, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) dst[t] = *src[t];
+}
+
+struct SrvReq {
+    long long id = 0;
+    cismgpu_request_t rq{};
+    cismgpu_par_t par{};
+    int phase = 0;  // 0 queued, 1 admitted, 2 done
+    int status = CISMGPU_OK, niters = 0, checks = 0;
+    double err = 0.0;
+    double t_submit = 0.0, t_admit = 0.0, t_done = 0.0;  // ms since the server started
+    cismgpu_solver *h = nullptr;
+    size_t bytes = 0;
+    int cls = 0;       // kernel class: 0 2D, 1 3D nz <= 16, 2 3D nz <= 32
+    int TY = 0;
+    unsigned tick = 0; // steps completed, as of the last epoch
+};
+
+// Device bytes a request's handle holds at most (the FP64 system, its staging block, the
+// FP64 and FP32 vectors, the FP32 matrix and factors, tile maps and records).
+static size_t request_bytes(const cismgpu_request_t &r) {
+    const long long NQ = (long long)(r.nx - 1) * (r.ny - 1);
+    const long long nvec = NQ * (r.dims == 3 ? r.nz : 1);
+    const long long NC = r.dims == 3 ? 27 : 9;
+    const long long per = 4 * NC * 8 + NC * 8 + NVEC * 8 + 4 * NC * 4 + 6 * 4 + 16 * 4;
+    return (size_t)(nvec * per + NQ * 16 + (8 << 20));
+}
+
+static int request_class(const cismgpu_request_t &r) {
+    if (r.dims != 3) return 0;
+    return r.nz <= 16 ? 1 : 2;
+}
+
+}  // namespace cismgpu
+
+struct cismgpu_server {
+    size_t budget = 0, used = 0;
+    int epoch_steps = 64;
+    std::mutex mu;
+    std::condition_variable cv;     // work arrived / a request finished
+    std::deque<cismgpu::SrvReq *> queued;
+    std::vector<cismgpu::SrvReq *> active;
+    std::unordered_map<long long, cismgpu::SrvReq *> reqs;
+    long long next_id = 1;
+    long long inflight = 0;         // submitted and not yet done
+    long long epochs = 0;
+    bool stop = false;
+    int device = 0;
+    std::thread th;
+    cudaStream_t es = nullptr;      // epoch stream
+    std::chrono::steady_clock::time_point t0;
+    double now() const {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace cismgpu {
+
+// Per-class launch scratch, reused across epochs.
+struct SrvLaunch {
+    DevBuf blk;                 // descriptors | state pointers | ticks | tiles | ctl | gathered states
+    char *h_blk = nullptr;      // pinned staging of the same layout (rewritten only after the epoch)
+    size_t h_cap = 0;
+    MState *h_states = nullptr; // pinned
+    MCtl *h_ctl = nullptr;      // pinned
+    int cap = 0;
+    std::vector<SrvReq *> members;
+    ~SrvLaunch() {
+        blk.release();
+        if (h_blk) cudaFreeHost(h_blk);
+        if (h_states) cudaFreeHost(h_states);
+        if (h_ctl) cudaFreeHost(h_ctl);
+    }
+};
+
+// Create, upload and prepare the handle of an admitted request (on the handle's stream).
+static int srv_admit(SrvReq &r) {
+    const cismgpu_request_t &q = r.rq;
+    cismgpu_solver_t *h = nullptr;
+    TRY(cismgpu_solver_create(&h, q.dims, q.nx, q.ny, q.nz, &r.par, q.indxA, q.active_vertex, q.Auu, q.Auv,
+                              q.Avu, q.Avv, q.bu, q.bv, q.xu0, q.xv0, nullptr));
+    r.h = h;
+    Solver &sv = h->sv;
+    const int nzm = mixed_nzm(sv.g, sv.is3d);
+    r.TY = mixed_batch_ty(sv.g, sv.is3d, nzm);
+    TRY(mixed_prepare(sv, q.precond, r.TY));
+    TRY(mixed_reset(sv, sv.stream));
+    const MState S0 = mixed_init_state(q.tolerance, q.maxiters, q.linear_solve_ncheck);
+    CU(cudaMemcpyAsync(sv.mixed.state, &S0, sizeof(MState), cudaMemcpyHostToDevice, sv.stream));
+    CU(cudaStreamSynchronize(sv.stream));
+    r.tick = 0;
+    return CISMGPU_OK;
+}
+
+// Launch one epoch of class cls over its active requests (asynchronous on the epoch stream).
+static int srv_launch(cismgpu_server *S, SrvLaunch &L, int cls) {
+    const int n = (int)L.members.size();
+    if (n == 0) return CISMGPU_OK;
+    const bool is3d = cls != 0;
+    const int nzm = cls == 0 ? 1 : (cls == 1 ? 16 : 32);
+    int TYmax = 1;
+    std::vector<MDesc> descs(n);
+    std::vector<MState *> sptr(n);
+    std::vector<unsigned> tick(n);
+    std::vector<MTile> tl;
+    for (int t = 0; t < n; ++t) {
+        SrvReq &r = *L.members[t];
+        Solver &sv = r.h->sv;
+        descs[t] = mixed_desc(sv, r.rq.precond, r.TY);
+        sptr[t] = sv.mixed.state;
+        tick[t] = r.tick;
+        TYmax = std::max(TYmax, r.TY);
+        for (int k = 0; k < descs[t].ntiles; ++k) tl.push_back(MTile{t, k});
+    }
+    const int grid = mixed_dyn_grid(is3d, nzm, TYmax);
+    if (grid < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM at this tile height");
+    if ((long long)n > (long long)grid * kMaxCtaSolves) return fail(CISMGPU_EUNSUPPORTED, "too many requests");
+    auto al = [](size_t x) { return (x + 255) / 256 * 256; };
+    const size_t o_d = 0, o_p = al(n * sizeof(MDesc)), o_t = o_p + al(n * sizeof(MState *)),
+                 o_l = o_t + al(n * sizeof(unsigned)), o_c = o_l + al(tl.size() * sizeof(MTile)),
+                 o_g = o_c + al(sizeof(MCtl)), total = o_g + al(n * sizeof(MState));
+    CU(L.blk.ensure(total));
+    if (total > L.h_cap) {
+        if (L.h_blk) cudaFreeHost(L.h_blk);
+        L.h_blk = nullptr;
+        L.h_cap = 0;
+        CU(cudaMallocHost((void **)&L.h_blk, total));
+        L.h_cap = total;
+    }
+    if (n > L.cap) {
+        if (L.h_states) cudaFreeHost(L.h_states);
+        L.h_states = nullptr;
+        CU(cudaMallocHost((void **)&L.h_states, n * sizeof(MState)));
+        L.cap = n;
+    }
+    if (!L.h_ctl) CU(cudaMallocHost((void **)&L.h_ctl, sizeof(MCtl)));
+    char *base = static_cast<char *>(L.blk.p);
+    MCtl c0;
+    std::memset(&c0, 0, sizeof(c0));
+    c0.active = n;
+    cudaStream_t s = S->es;
+    std::memcpy(L.h_blk + o_d, descs.data(), n * sizeof(MDesc));
+    std::memcpy(L.h_blk + o_p, sptr.data(), n * sizeof(MState *));
+    std::memcpy(L.h_blk + o_t, tick.data(), n * sizeof(unsigned));
+    std::memcpy(L.h_blk + o_l, tl.data(), tl.size() * sizeof(MTile));
+    std::memcpy(L.h_blk + o_c, &c0, sizeof(MCtl));
+    CU(cudaMemcpyAsync(base, L.h_blk, o_g, cudaMemcpyHostToDevice, s));
+    TRY(mixed_dyn_dispatch(is3d, nzm, reinterpret_cast<MDesc *>(base + o_d), reinterpret_cast<MState **>(base + o_p),
+                           reinterpret_cast<unsigned *>(base + o_t), n, reinterpret_cast<MTile *>(base + o_l),
+                           (int)tl.size(), TYmax, reinterpret_cast<MCtl *>(base + o_c), S->epoch_steps, grid, s));
+    k_gather_states<<<(n + 127) / 128, 128, 0, s>>>(reinterpret_cast<MState **>(base + o_p),
+                                                   reinterpret_cast<MState *>(base + o_g), n);
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(L.h_states, base + o_g, n * sizeof(MState), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(L.h_ctl, base + o_c, sizeof(MCtl), cudaMemcpyDeviceToHost, s));
+    return CISMGPU_OK;
+}
+
+// Finish a request: x to the caller, handle freed, budget returned, waiters woken.
+static void srv_retire(cismgpu_server *S, SrvReq &r, int status, double err, int niters, int checks) {
+    if (r.h) {
+        const int rc = cismgpu_solver_get_x(r.h, r.rq.xu, r.rq.xv);
+        if (rc && status == CISMGPU_OK) status = rc;
+        cismgpu_solver_destroy(r.h);
+        r.h = nullptr;
+    }
+    std::lock_guard<std::mutex> lk(S->mu);
+    r.status = status;
+    r.err = err;
+    r.niters = niters;
+    r.checks = checks;
+    r.t_done = S->now();
+    r.phase = 2;
+    S->used -= r.bytes;
+    S->inflight -= 1;
+    S->cv.notify_all();
+}
+
+static void srv_loop(cismgpu_server *S) {
+    cudaSetDevice(S->device);
+    SrvLaunch L[3];
+    for (;;) {
+        std::vector<SrvReq *> admit;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv.wait(lk, [&] { return S->stop || !S->queued.empty() || !S->active.empty(); });
+            if (S->stop && S->queued.empty() && S->active.empty()) break;
+            while (!S->queued.empty()) {  // arrival order, within the HBM budget
+                SrvReq *r = S->queued.front();
+                const bool idle = S->active.empty() && admit.empty();
+                if (S->used + r->bytes > S->budget && !idle) break;
+                S->queued.pop_front();
+                S->used += r->bytes;
+                admit.push_back(r);
+            }
+        }
+        // 1. one epoch per kernel class over the requests already active
+        for (int c = 0; c < 3; ++c) L[c].members.clear();
+        for (SrvReq *r : S->active) L[r->cls].members.push_back(r);
+        int launched = 0;
+        for (int c = 0; c < 3; ++c) {
+            if (L[c].members.empty()) continue;
+            const int rc = srv_launch(S, L[c], c);
+            if (rc) {  // the class cannot run: fail its requests
+                for (SrvReq *r : L[c].members) srv_retire(S, *r, rc, std::nan(""), 0, 0);
+                L[c].members.clear();
+            } else {
+                ++launched;
+            }
+        }
+        // 2. admissions, overlapping the epochs on the GPU
+        for (SrvReq *r : admit) {
+            if (r->bytes > S->budget) {
+                srv_retire(S, *r, fail(CISMGPU_ENOMEM, "request larger than the HBM budget"), std::nan(""), 0, 0);
+                continue;
+            }
+            const int rc = srv_admit(*r);
+            if (rc) {
+                srv_retire(S, *r, rc, std::nan(""), 0, 0);
+                continue;
+            }
+            std::lock_guard<std::mutex> lk(S->mu);
+            r->t_admit = S->now();
+            r->phase = 1;
+        }
+        // 3. the epochs' results
+        if (launched) {
+            cudaStreamSynchronize(S->es);
+            ++S->epochs;
+        }
+        std::vector<SrvReq *> still;
+        for (int c = 0; c < 3; ++c) {
+            const bool aborted = L[c].h_ctl && !L[c].members.empty() && L[c].h_ctl->abort;
+            for (size_t t = 0; t < L[c].members.size(); ++t) {
+                SrvReq *r = L[c].members[t];
+                const MState &st = L[c].h_states[t];
+                r->tick = st.tick;
+                if (st.done) srv_retire(S, *r, st.status, st.err, st.niters, st.checks);
+                else if (aborted) srv_retire(S, *r, CISMGPU_ETIMEOUT, st.err, st.niters, st.checks);
+                else still.push_back(r);
+            }
+        }
+        for (SrvReq *r : admit)
+            if (r->phase == 1) still.push_back(r);
+        S->active.swap(still);
+    }
+}
+
+}  // namespace cismgpu
+
+extern "C" {
+
+int cismgpu_server_create(cismgpu_server_t **out, size_t hbm_budget_bytes, int epoch_steps) {
+    using namespace cismgpu;
+    g_last_error.clear();
+    if (!out) return fail(CISMGPU_EINVAL, "null argument");
+    *out = nullptr;
+    if (hbm_budget_bytes == 0 || epoch_steps < 1) return fail(CISMGPU_EINVAL, "budget and epoch_steps must be > 0");
+    TRY(check_device());
+    cismgpu_server *S = new cismgpu_server();
+    S->budget = hbm_budget_bytes;
+    S->epoch_steps = epoch_steps;
+    S->t0 = std::chrono::steady_clock::now();
+    cudaGetDevice(&S->device);
+    const cudaError_t e = cudaStreamCreateWithFlags(&S->es, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete S;
+        return fail(CISMGPU_ECUDA, std::string("server stream creation failed: ") + cudaGetErrorString(e));
+    }
+    S->th = std::thread(srv_loop, S);
+    *out = S;
+    return CISMGPU_OK;
+}
+
+int cismgpu_server_submit(cismgpu_server_t *S, const cismgpu_request_t *rq, long long *id) {
+    using namespace cismgpu;
+    g_last_error.clear();
+    if (!S || !rq || !id || !rq->par || !rq->xu || !rq->xv) return fail(CISMGPU_EINVAL, "null argument");
+    if (rq->dims != 2 && rq->dims != 3) return fail(CISMGPU_EINVAL, "dims must be 2 or 3");
+    TRY(validate_solve_args(rq->precond, rq->linear_solve_ncheck, rq->maxiters));
+    if (!(rq->precond == 0 || rq->precond == 1 || (rq->precond == 2 && rq->dims == 3)))
+        return fail(CISMGPU_EUNSUPPORTED, "mixed solver preconditioners: 0, 1, or 2 (3D only)");
+    if (rq->dims == 3 && (rq->nz < 1 || rq->nz > kMixedMaxNz)) return fail(CISMGPU_EUNSUPPORTED, "nz must be 1..32");
+    SrvReq *r = new SrvReq();
+    r->rq = *rq;
+    r->par = *rq->par;
+    r->rq.par = &r->par;
+    if (rq->dims == 2) r->rq.nz = 1;
+    r->bytes = request_bytes(r->rq);
+    r->cls = request_class(r->rq);
+    std::lock_guard<std::mutex> lk(S->mu);
+    r->id = S->next_id++;
+    r->t_submit = S->now();
+    S->reqs[r->id] = r;
+    S->queued.push_back(r);
+    S->inflight += 1;
+    *id = r->id;
+    S->cv.notify_all();
+    return CISMGPU_OK;
+}
+
+int cismgpu_server_poll(cismgpu_server_t *S, long long id, int *done, double *err, int *niters, int *status,
+                        double *latency_ms, double *queue_ms) {
+    using namespace cismgpu;
+    if (!S || !done) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(id);
+    if (it == S->reqs.end()) return fail(CISMGPU_EINVAL, "unknown request id");
+    const SrvReq &r = *it->second;
+    *done = r.phase == 2;
+    if (err) *err = r.err;
+    if (niters) *niters = r.niters;
+    if (status) *status = r.status;
+    if (latency_ms) *latency_ms = r.phase == 2 ? r.t_done - r.t_submit : S->now() - r.t_submit;
+    if (queue_ms) *queue_ms = r.phase >= 1 ? r.t_admit - r.t_submit : S->now() - r.t_submit;
+    return CISMGPU_OK;
+}
+
+int cismgpu_server_drain(cismgpu_server_t *S) {
+    using namespace cismgpu;
+    if (!S) return fail(CISMGPU_EINVAL, "null argument");
+    std::unique_lock<std::mutex> lk(S->mu);
+    S->cv.wait(lk, [&] { return S->inflight == 0; });
+    return CISMGPU_OK;
+}
+
+int cismgpu_server_stats(cismgpu_server_t *S, long long *epochs, size_t *bytes_in_use, int *active, int *queued) {
+    using namespace cismgpu;
+    if (!S) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (epochs) *epochs = S->epochs;
+    if (bytes_in_use) *bytes_in_use = S->used;
+    if (active) *active = (int)S->active.size();
+    if (queued) *queued = (int)S->queued.size();
+    return CISMGPU_OK;
+}
+
+int cismgpu_server_destroy(cismgpu_server_t *S) {
+    if (!S) return CISMGPU_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        S->cv.notify_all();
+    }
+    if (S->th.joinable()) S->th.join();
+    for (auto &kv : S->reqs) {
+        if (kv.second->h) cismgpu_solver_destroy(kv.second->h);
+        delete kv.second;
+    }
+    if (S->es) cudaStreamDestroy(S->es);
+    delete S;
+    return CISMGPU_OK;
+}
+
+}  // extern "C"

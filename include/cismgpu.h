@@ -234,6 +234,44 @@ int cismgpu_batch_run(cismgpu_batch_t *b);
 int cismgpu_batch_wait(cismgpu_batch_t *b, double *errs, int *niters, int *statuses);
 int cismgpu_batch_destroy(cismgpu_batch_t *b);
 
+/* ------------------------------------------------------------------------
+ * Serving loop (no reference counterpart): continuous batching of independent
+ * solves with the mixed-precision solver.  A host thread admits requests in
+ * arrival order within an HBM budget (each admitted request holds its own
+ * device-resident matrix and Krylov state), runs every admitted request in
+ * epochs of at most epoch_steps steps of one persistent launch per kernel class
+ * (2D, 3D nz <= 16, 3D nz <= 32), and between epochs retires finished requests
+ * (x copied to the caller, device memory freed) and admits new ones, whose
+ * upload overlaps the running epoch.  A request's result is bit-identical
+ * whether it is served alone or in any mix.
+ * The arrays a request points to must stay valid until it is done; xu/xv
+ * receive the solution (caller's layout) when it completes.
+ * ------------------------------------------------------------------------ */
+typedef struct cismgpu_server cismgpu_server_t;
+typedef struct cismgpu_request {
+    int dims;                        /* 2 or 3                                  */
+    int nx, ny, nz;                  /* nz ignored (1) for dims = 2             */
+    const cismgpu_par_t *par;        /* copied at submit                        */
+    const int32_t *indxA;            /* indxA_3d (27) or indxA_2d (9)           */
+    const int32_t *active_vertex;
+    const double *Auu, *Auv, *Avu, *Avv;
+    const double *bu, *bv;
+    const double *xu0, *xv0;         /* initial guess, NULL: zero               */
+    double *xu, *xv;                 /* solution, written on completion         */
+    int precond, linear_solve_ncheck;
+    double tolerance;
+    int maxiters;
+} cismgpu_request_t;
+int cismgpu_server_create(cismgpu_server_t **out, size_t hbm_budget_bytes, int epoch_steps);
+int cismgpu_server_submit(cismgpu_server_t *s, const cismgpu_request_t *req, long long *id);
+/* done: 1 once xu/xv hold the result; latency_ms: submit to completion (or to now);
+ * queue_ms: submit to admission. */
+int cismgpu_server_poll(cismgpu_server_t *s, long long id, int *done, double *err, int *niters, int *status,
+                        double *latency_ms, double *queue_ms);
+int cismgpu_server_drain(cismgpu_server_t *s);  /* wait until every submitted request is done */
+int cismgpu_server_stats(cismgpu_server_t *s, long long *epochs, size_t *bytes_in_use, int *active, int *queued);
+int cismgpu_server_destroy(cismgpu_server_t *s); /* finishes the queued requests first */
+
 /* Copy the current solution (caller's Fortran layout, halo entries included) to host memory. */
 int cismgpu_solver_get_x(cismgpu_solver_t *s, double *xu, double *xv);
 
