@@ -197,6 +197,134 @@ def run_batch(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# served workload: a Poisson stream of 2D SSA and 3D BP requests
+# ---------------------------------------------------------------------------
+def _make_served(args):
+    from cism_b200 import assembly as asm
+    kind, n, nz, seed = args
+    if kind == "2d":
+        return asm.ssa_random(ewn=n, nsn=n, dx=1000.0, seed=seed, name=f"ssa{n}")
+    return asm.ice_stream(ewn=n, nsn=n, nz=nz, dx=2000.0, seed=seed, name=f"bp{n}x{nz}")
+
+
+def _fifo(arrivals, service):
+    """Completion latencies of one FIFO server with the given service times."""
+    t, lat = 0.0, []
+    for a, s in zip(arrivals, service):
+        t = max(t, a) + s
+        lat.append(t - a)
+    return lat
+
+
+def run_serve(args):
+    """A seeded Poisson stream (mean 200 req/s) of 2D SSA (96^2..1025^2 vertices, diagonal
+    precond) and 3D BP ice streams (48^2..384^2 vertices x 5..21 levels, no-slip bed, SIA
+    precond), served by the continuous-batching loop under a 150 GB HBM budget; latency is
+    submit to x back in host memory.  Requests draw from a seeded pool of distinct systems
+    (every request gets its own device copy).  Beside it: the same stream through a FIFO
+    queue of one-shot reference-signature calls, plain FP64 and mixed, with service times
+    measured per pool system."""
+    import multiprocessing as mp
+    rng = np.random.default_rng(2024)
+    pool_spec = [("2d", int(rng.integers(96, 1026)), 1, 100 + k) for k in range(args.pool)]
+    pool_spec += [("3d", int(rng.integers(48, 385)), int(rng.integers(5, 22)), 200 + k) for k in range(args.pool)]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(min(len(pool_spec), os.cpu_count() or 1)) as pool:
+        probs = pool.map(_make_served, pool_spec)
+    t_gen = time.perf_counter() - t0
+    import cism_b200 as cg
+    from cism_b200 import build
+    from cism_b200 import assembly as asm
+    build.build()
+    pcs = [1 if P.kind == "2d" else 2 for P in probs]
+    nreq = args.requests
+    arrivals = np.cumsum(rng.exponential(1.0 / 200.0, nreq))
+    arrivals -= arrivals[0]
+    which = rng.integers(0, len(probs), nreq)
+    maxit = 20000
+
+    def oneshot(P, pc, alg):
+        prev = cg.set_oneshot_algorithm(alg)
+        try:
+            xu, xv = np.zeros_like(P.bu), np.zeros_like(P.bv)
+            t = time.perf_counter()
+            if P.kind == "3d":
+                cg.pcg_solver_chrongear_3d(P.nx, P.ny, P.nz, P.par, asm.indxA_2d(), asm.indxA_3d(), P.active_vertex,
+                                           P.Auu, P.Auv, P.Avu, P.Avv, P.bu, P.bv, xu, xv, pc, NCHECK, TOL, maxit)
+            else:
+                cg.pcg_solver_chrongear_2d(P.nx, P.ny, P.par, asm.indxA_2d(), P.active_vertex, P.Auu, P.Auv, P.Avu,
+                                           P.Avv, P.bu, P.bv, xu, xv, pc, NCHECK, TOL, maxit)
+            return time.perf_counter() - t, (xu, xv)
+        finally:
+            cg.set_oneshot_algorithm(prev)
+
+    svc64, svcmx, x64 = [], [], []
+    for P, pc in zip(probs, pcs):
+        oneshot(P, pc, cg.ALG_CHRONGEAR)  # warm the workspace
+        dt, x = oneshot(P, pc, cg.ALG_CHRONGEAR)
+        svc64.append(dt)
+        x64.append(x)
+        oneshot(P, pc, cg.ALG_MIXED_CHRONGEAR)
+        svcmx.append(oneshot(P, pc, cg.ALG_MIXED_CHRONGEAR)[0])
+    S = cg.Server(hbm_budget_bytes=150 * 10**9, epoch_steps=args.epoch_steps)
+    clocks = ClockSampler(0)
+    clocks.start()
+    time.sleep(0.3)
+    ids = []
+    start = time.perf_counter()
+    for k in range(nreq):
+        dt = arrivals[k] - (time.perf_counter() - start)
+        if dt > 0:
+            time.sleep(dt)
+        ids.append(S.submit(probs[which[k]], precond=pcs[which[k]], tol=TOL, maxiters=maxit))
+    S.drain()
+    wall = time.perf_counter() - start
+    clk = clocks.stop()
+    infos = [S.poll(i) for i in ids]
+    bad = [i["status"] for i in infos if i["status"] != 0]
+    if bad:
+        raise RuntimeError(f"served requests failed: {bad[:8]}")
+    lat = np.array([i["latency_ms"] for i in infos])
+    errs = np.array([i["err"] for i in infos])
+    rel = 0.0
+    for k, rid in enumerate(ids):
+        xu, xv, _ = S.result(rid)
+        au, av = x64[which[k]]
+        rel = max(rel, math.sqrt(float(np.sum((xu - au) ** 2) + np.sum((xv - av) ** 2))) /
+                  math.sqrt(float(np.sum(au ** 2) + np.sum(av ** 2))))
+    st = S.stats()
+    S.close()
+    lat64 = 1e3 * np.array(_fifo(arrivals, [svc64[w] for w in which]))
+    latmx = 1e3 * np.array(_fifo(arrivals, [svcmx[w] for w in which]))
+    value = nreq / wall
+    fp64_rate = nreq / max(float(np.max(arrivals + lat64 / 1e3)), 1e-9)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": nreq, "warmup": 0,
+        "ms_per_step": 1e3 * wall / nreq, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 recurrences + f64 x/dots/residual", "data": "synthetic",
+        "config": {"workload": f"cfg5: {nreq} requests, Poisson mean 200 req/s, 2D SSA 96^2..1025^2 (diag) and 3D BP "
+                               f"48^2..384^2 x 5..21 levels (SIA), pool of {len(probs)} seeded systems, "
+                               "HBM budget 150 GB, tol 1e-8",
+                   "solver": f"continuous-batching serving loop, epochs of {args.epoch_steps} steps",
+                   "generation_s": round(t_gen, 1)},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "mean": float(np.mean(lat))},
+        "err_max": float(np.max(errs)), "err_vs_fp64_solution_max": rel,
+        "fp64_plain_fifo": {"solves_per_s": fp64_rate,
+                            "latency_ms": {"p50": float(np.percentile(lat64, 50)), "p99": float(np.percentile(lat64, 99))},
+                            "solver": "one-shot cismgpu_pcg_chrongear_* calls (FP64 reference statements), FIFO"},
+        "mixed_one_at_a_time_fifo": {"solves_per_s": nreq / max(float(np.max(arrivals + latmx / 1e3)), 1e-9),
+                                     "latency_ms": {"p50": float(np.percentile(latmx, 50)),
+                                                    "p99": float(np.percentile(latmx, 99))}},
+        "speedup_vs_fp64_plain": value / fp64_rate,
+        "server": {"epochs": st["epochs"]},
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def hbm_peak():
     try:
         with open(PEAKS) as f:
@@ -507,7 +635,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="bench", choices=["bench", "profile"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "dome", "cfg4"])
+    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "dome", "cfg4", "cfg5"])
+    ap.add_argument("--requests", type=int, default=96, help="cfg5: number of requests")
+    ap.add_argument("--pool", type=int, default=8, help="cfg5: distinct systems per kind")
+    ap.add_argument("--epoch-steps", type=int, default=64, help="cfg5: steps per serving epoch")
     ap.add_argument("--batch", type=int, default=64, help="cfg4: number of systems")
     ap.add_argument("--fp64", action="store_true", help="profile mode: also time one plain FP64 solve")
     args = ap.parse_args()
@@ -515,6 +646,8 @@ def main():
         return run_profile(args)
     if args.workload == "cfg4":
         return run_batch(args)
+    if args.workload == "cfg5":
+        return run_serve(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
