@@ -2,7 +2,7 @@
 //
 // Requests (one linear system each, in the caller's Fortran layout) are queued by
 // cismgpu_server_submit and served by one host thread:
-//   * admission: in arrival order while the HBM budget allows; an admitted request gets
+//   * admission (its own host thread): in arrival order while the HBM budget allows; an admitted request gets
 //     its own device-resident handle (matrix, FP32 copy, preconditioner, Krylov vectors),
 //     uploaded on the handle's own stream while the GPU runs the current epoch;
 //   * epochs: every active request of a kernel class (2D, 3D nz <= 16, 3D nz <= 32) takes
@@ -66,15 +66,18 @@ struct cismgpu_server {
     int epoch_steps = 64;
     std::mutex mu;
     std::condition_variable cv;     // work arrived / a request finished
-    std::deque<cismgpu::SrvReq *> queued;
-    std::vector<cismgpu::SrvReq *> active;
+    std::deque<cismgpu::SrvReq *> queued;   // submitted, waiting for admission
+    std::vector<cismgpu::SrvReq *> ready;   // admitted and uploaded, joining at the next epoch
+    std::vector<cismgpu::SrvReq *> active;  // taking part in epochs
+    int uploading = 0;                      // admitted, upload in progress
     std::unordered_map<long long, cismgpu::SrvReq *> reqs;
     long long next_id = 1;
     long long inflight = 0;         // submitted and not yet done
     long long epochs = 0;
     bool stop = false;
     int device = 0;
-    std::thread th;
+    std::thread th;                 // epoch loop
+    std::thread up;                 // admissions and uploads
     cudaStream_t es = nullptr;      // epoch stream
     std::chrono::steady_clock::time_point t0;
     double now() const {
@@ -204,25 +207,61 @@ static void srv_retire(cismgpu_server *S, SrvReq &r, int status, double err, int
     S->cv.notify_all();
 }
 
+// Admission thread: takes queued requests in arrival order as the HBM budget allows and
+// uploads and prepares each on its own stream, so that uploads run while the epoch loop keeps
+// the GPU busy.  A request larger than the whole budget fails with CISMGPU_ENOMEM.
+static void srv_admit_loop(cismgpu_server *S) {
+    cudaSetDevice(S->device);
+    for (;;) {
+        SrvReq *r = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv.wait(lk, [&] {
+                if (S->queued.empty()) return S->stop;
+                const SrvReq *f = S->queued.front();
+                return f->bytes > S->budget || S->used + f->bytes <= S->budget;
+            });
+            if (S->queued.empty()) break;  // stopping, nothing left to admit
+            r = S->queued.front();
+            S->queued.pop_front();
+            if (r->bytes > S->budget) {
+                r->bytes = 0;  // never counted against the budget
+            } else {
+                S->used += r->bytes;
+            }
+            S->uploading += 1;
+        }
+        int rc = r->bytes == 0 ? fail(CISMGPU_ENOMEM, "request larger than the HBM budget") : srv_admit(*r);
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->uploading -= 1;
+            if (!rc) {
+                r->t_admit = S->now();
+                r->phase = 1;
+                S->ready.push_back(r);
+            }
+            S->cv.notify_all();
+        }
+        if (rc) srv_retire(S, *r, rc, std::nan(""), 0, 0);
+    }
+}
+
+// Epoch loop: one epoch per kernel class over the active requests, then retire the finished
+// ones; requests admitted meanwhile join at the next epoch.
 static void srv_loop(cismgpu_server *S) {
     cudaSetDevice(S->device);
     SrvLaunch L[3];
     for (;;) {
-        std::vector<SrvReq *> admit;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            S->cv.wait(lk, [&] { return S->stop || !S->queued.empty() || !S->active.empty(); });
-            if (S->stop && S->queued.empty() && S->active.empty()) break;
-            while (!S->queued.empty()) {  // arrival order, within the HBM budget
-                SrvReq *r = S->queued.front();
-                const bool idle = S->active.empty() && admit.empty();
-                if (S->used + r->bytes > S->budget && !idle) break;
-                S->queued.pop_front();
-                S->used += r->bytes;
-                admit.push_back(r);
-            }
+            S->cv.wait(lk, [&] {
+                return !S->ready.empty() || !S->active.empty() ||
+                       (S->stop && S->queued.empty() && S->uploading == 0);
+            });
+            if (S->ready.empty() && S->active.empty()) break;  // stopping and nothing left
+            S->active.insert(S->active.end(), S->ready.begin(), S->ready.end());
+            S->ready.clear();
         }
-        // 1. one epoch per kernel class over the requests already active
         for (int c = 0; c < 3; ++c) L[c].members.clear();
         for (SrvReq *r : S->active) L[r->cls].members.push_back(r);
         int launched = 0;
@@ -236,24 +275,9 @@ static void srv_loop(cismgpu_server *S) {
                 ++launched;
             }
         }
-        // 2. admissions, overlapping the epochs on the GPU
-        for (SrvReq *r : admit) {
-            if (r->bytes > S->budget) {
-                srv_retire(S, *r, fail(CISMGPU_ENOMEM, "request larger than the HBM budget"), std::nan(""), 0, 0);
-                continue;
-            }
-            const int rc = srv_admit(*r);
-            if (rc) {
-                srv_retire(S, *r, rc, std::nan(""), 0, 0);
-                continue;
-            }
-            std::lock_guard<std::mutex> lk(S->mu);
-            r->t_admit = S->now();
-            r->phase = 1;
-        }
-        // 3. the epochs' results
         if (launched) {
             cudaStreamSynchronize(S->es);
+            std::lock_guard<std::mutex> lk(S->mu);
             ++S->epochs;
         }
         std::vector<SrvReq *> still;
@@ -268,8 +292,7 @@ static void srv_loop(cismgpu_server *S) {
                 else still.push_back(r);
             }
         }
-        for (SrvReq *r : admit)
-            if (r->phase == 1) still.push_back(r);
+        std::lock_guard<std::mutex> lk(S->mu);
         S->active.swap(still);
     }
 }
@@ -296,6 +319,7 @@ int cismgpu_server_create(cismgpu_server_t **out, size_t hbm_budget_bytes, int e
         return fail(CISMGPU_ECUDA, std::string("server stream creation failed: ") + cudaGetErrorString(e));
     }
     S->th = std::thread(srv_loop, S);
+    S->up = std::thread(srv_admit_loop, S);
     *out = S;
     return CISMGPU_OK;
 }
@@ -370,6 +394,7 @@ int cismgpu_server_destroy(cismgpu_server_t *S) {
         S->stop = true;
         S->cv.notify_all();
     }
+    if (S->up.joinable()) S->up.join();
     if (S->th.joinable()) S->th.join();
     for (auto &kv : S->reqs) {
         if (kv.second->h) cismgpu_solver_destroy(kv.second->h);
