@@ -68,6 +68,20 @@ def run_profile(args):
     from cism_b200 import build
     build.build()
     torch.zeros(1, device="cuda")  # CUDA context up before any timing
+    if args.workload == "cfg4":  # a small batch of cfg4 members through one graph-captured launch
+        from cism_b200 import assembly as asm
+        sizes = asm.batch_sizes(args.batch)
+        solvers = [cg.DeviceSolver(asm.batch_member(n, s)) for s, n in enumerate(sizes)]
+        B = cg.GraphBatch(solvers, precond=2, ncheck=NCHECK, tol=TOL, maxiters=4000)
+        for k in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            B.run()
+            errs, nits, sts = B.wait()
+            wall = time.perf_counter() - t0
+        print(f"profile workload=cfg4 batch={len(sizes)} sizes={sizes} niters={list(nits)} err_max={max(errs):.3e} "
+              f"wall_ms={1e3 * wall:.1f}")
+        B.close()
+        return 0
     P = make_problem(args.workload)
     S = cg.DeviceSolver(P)
     pc = PROFILE_PRECOND[args.workload]
