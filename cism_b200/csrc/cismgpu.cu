@@ -767,7 +767,9 @@ static double mixed_iter_bytes(const Solver &sv, int precond) {
 }
 
 static double mixed_check_bytes(const Solver &sv) {
-    return (double)sv.n_active_owned * sv.g.nz * (4.0 * sv.NC * 8.0 + 16.0 + 16.0 + 8.0);
+    // FP64 residual (matrix, x, b, r32) + the fused update (z, d, q, Az loads, q store) + the
+    // deferred owner writes of the next step (d, z, x loads, d, x stores)
+    return (double)sv.n_active_owned * sv.g.nz * (4.0 * sv.NC * 8.0 + 16.0 + 16.0 + 8.0 + 20.0 + 28.0);
 }
 
 template <int NCC>

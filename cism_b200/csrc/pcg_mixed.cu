@@ -34,7 +34,11 @@ namespace cismgpu {
 
 constexpr int kMixedMaxNz = 32;                  // shared-memory bound of the mixed kernel (levels)
 
-enum MStep { MS_INIT = 0, MS_A, MS_MERGED, MS_B, MS_CHECK, MS_DONE };
+// Step kinds.  A check iteration ends with one MS_BC step (update and FP64 residual
+// replacement together); the owners' in-place d and x writes of that update are deferred
+// to the next step (MS_A_UPD, or MS_FIN when the solve stops there), so that no tile reads
+// a neighbour's half-updated d or x while it recomputes the halo of x.
+enum MStep { MS_INIT = 0, MS_A, MS_MERGED, MS_B, MS_CHECK_UNUSED, MS_DONE, MS_BC, MS_A_UPD, MS_FIN };
 
 // A tile's partial sums of one step, stamped with the step number (tag) last.
 struct TileRec {
@@ -167,6 +171,7 @@ __device__ void advance_state(MState &S, double S0, double S1, double S2) {
         }
         break;
     case MS_A:       // S0 = (r,z), S1 = (Az,z) of iteration iter
+    case MS_A_UPD:
     case MS_MERGED: {
         if (S.step == MS_MERGED) {  // the merged step finished iteration iter's update: advance
             S.par ^= 1;
@@ -187,36 +192,36 @@ __device__ void advance_state(MState &S, double S0, double S1, double S2) {
             S.step = MS_DONE;
             break;
         }
-        // iteration iter's update comes next: alone if a check or the last iteration follows
-        S.step = (is_check_it(S.iter, S.ncheck) || S.iter >= S.maxiters) ? MS_B : MS_MERGED;
+        // iteration iter's update comes next: with the FP64 check at check iterations, alone
+        // at the last iteration, merged with the next iteration's first half otherwise
+        S.step = is_check_it(S.iter, S.ncheck) ? MS_BC : (S.iter >= S.maxiters ? MS_B : MS_MERGED);
         break;
     }
-    case MS_B:
+    case MS_B:  // last iteration without a check
         S.par ^= 1;
-        if (is_check_it(S.iter, S.ncheck)) {
-            S.step = MS_CHECK;
-        } else {  // last iteration without a check
-            S.niters = S.maxiters;
-            S.done = 1;
-            S.step = MS_DONE;
-        }
+        S.niters = S.maxiters;
+        S.done = 1;
+        S.step = MS_DONE;
         break;
-    case MS_CHECK:  // S0 = (r,r) of the FP64 true residual
+    case MS_BC:  // S0 = (r,r) of the FP64 true residual after iteration iter's update
+        S.par ^= 1;
         S.checks += 1;
         S.fp64_matvecs += 1;
         S.err = sqrt(S0) / S.L2_rhs;
         if (S.err < S.tol) {
             S.niters = S.iter;
-            S.done = 1;
-            S.step = MS_DONE;
+            S.step = MS_FIN;
         } else if (S.iter >= S.maxiters) {
             S.niters = S.maxiters;
-            S.done = 1;
-            S.step = MS_DONE;
+            S.step = MS_FIN;
         } else {
             S.iter += 1;
-            S.step = MS_A;
+            S.step = MS_A_UPD;
         }
+        break;
+    case MS_FIN:  // the deferred x and d writes are done
+        S.done = 1;
+        S.step = MS_DONE;
         break;
     default:
         break;
@@ -357,11 +362,14 @@ __device__ __forceinline__ void sia_col(const MDesc &D, float *zc, int NS, int s
     }
 }
 
-// FP64 r = b - A64 x on the tile (x read through the halo map); r32 = r on live columns.
+// FP64 r = b - A64 x on the tile (x read through the halo map); r32 = r on live columns,
+// into buffer rpar.  With sdn (the MS_BC step) the x of every tile and halo slot is first
+// advanced by this iteration's update, x + alpha64 * dn with dn = sdn[c][k][slot] -- the same
+// FP64 fma its owner applies later, so the residual sees exactly the updated x.
 // Partials: p0 = (b,b), p1 = (r,r).  Loads of kChR items are issued before any store.
 template <int NC>
-__device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, int TY, int i0, int j0, int par,
-                                              double &p0, double &p1) {
+__device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, int TY, int i0, int j0, int rpar,
+                                              const float *sdn, double alpha64, double &p0, double &p1) {
     const Geom &g = D.g;
     const int nz = (NC == 27) ? g.nz : 1;
     const int NQ = (int)g.NQ;
@@ -373,8 +381,9 @@ __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, i
     const double *__restrict__ Avv = D.A64 + (size_t)3 * NC * plane;
     const double *__restrict__ xu = D.x;
     const double *__restrict__ xv = D.x + plane;
-    float *__restrict__ ru32 = D.r[par];
-    float *__restrict__ rv32 = D.r[par] + plane;
+    float *__restrict__ ru32 = D.r[rpar];
+    float *__restrict__ rv32 = D.r[rpar] + plane;
+    const int NS = (kTX + 2) * (TY + 2);
     const int nitems = NT * nz;
 #pragma unroll 1
     for (int base = threadIdx.x; base < nitems; base += kChR * kBlock) {
@@ -403,11 +412,16 @@ __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, i
 #pragma unroll
                         for (int c = 0; c < NC; ++c) {
                             const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
-                            const int sc = map_src(smap[s + iA + (kTX + 2) * jA]);
+                            const int sn = s + iA + (kTX + 2) * jA;
+                            const int sc = map_src(smap[sn]);
                             if (k + kA < 0 || k + kA >= nz || sc < 0) continue;
                             const int n = (k + kA) * NQ + sc;
                             const size_t a = (size_t)c * plane + e;
-                            const double x1 = ldd(xu + n), x2 = ldd(xv + n);
+                            double x1 = ldd(xu + n), x2 = ldd(xv + n);
+                            if (sdn) {
+                                x1 = fma(alpha64, (double)sdn[(k + kA) * NS + sn], x1);
+                                x2 = fma(alpha64, (double)sdn[(nz + k + kA) * NS + sn], x2);
+                            }
                             yu[u] = fma(Auu[a], x1, yu[u]);
                             yu[u] = fma(Auv[a], x2, yu[u]);
                             yv[u] = fma(Avu[a], x1, yv[u]);
@@ -459,14 +473,81 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
         __syncthreads();
     }
 
-    if (step == MS_INIT || step == MS_CHECK) {
-        residual_pass<NC>(D, smap, TY, i0, j0, par, p0, p1);
-        if (step == MS_CHECK) { p0 = p1; p1 = 0.0; }
+    if (step == MS_INIT) {
+        residual_pass<NC>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
+    } else if (step == MS_BC) {
+        // update of iteration iter fused with the FP64 check: dn = z + beta d on tile and halo
+        // slots (into shared memory, over the z rows), q for the owned columns; the owners'
+        // d and x writes wait for the next step
+        const float beta = (float)S.beta;
+        float *sdn = sz;  // [2][nz][NS]
+        const float *__restrict__ q_in = D.q[par];
+        const float *__restrict__ az_in = D.Az[par];
+        float *__restrict__ q_out = D.q[par ^ 1];
+        const int n1 = 2 * NS * nz;
+#pragma unroll 1
+        for (int base = t; base < n1; base += 4 * kBlock) {
+            float zo[4], dol[4], qo[4], az[4];
+            int ee[4], vv[4], ix[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int it = base + u * kBlock;
+                ix[u] = -1;
+                vv[u] = 0;
+                ee[u] = 0;
+                zo[u] = dol[u] = qo[u] = az[u] = 0.0f;
+                if (it < n1) {
+                    const int k = it / (2 * NS), rem = it - k * 2 * NS;
+                    const int c = rem >= NS ? 1 : 0, sl = rem - c * NS;
+                    ix[u] = (c * nz + k) * NS + sl;
+                    const int v = smap[sl];
+                    vv[u] = v;
+                    if (map_live(v)) {
+                        const int e = c * plane + k * NQ + map_src(v);
+                        ee[u] = e;
+                        zo[u] = ldf(D.z + e);
+                        dol[u] = ldf(D.d + e);
+                        if (map_mine(v)) {
+                            qo[u] = ldf(q_in + e);
+                            az[u] = ldf(az_in + e);
+                        }
+                    }
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                if (ix[u] < 0) continue;
+                const bool live = map_live(vv[u]);
+                sdn[ix[u]] = live ? fmaf(beta, dol[u], zo[u]) : 0.0f;  // d_i = z_i + beta d_{i-1}
+                if (live && map_mine(vv[u])) q_out[ee[u]] = fmaf(beta, qo[u], az[u]);  // q_i = Az_i + beta q_{i-1}
+            }
+        }
+        __syncthreads();
+        residual_pass<NC>(D, smap, TY, i0, j0, par ^ 1, sdn, S.alpha, p0, p1);
+        p0 = p1;
+        p1 = 0.0;
+    } else if (step == MS_FIN) {
+        // the deferred owner writes of the last (checked) update
+        const float beta = (float)S.beta;
+        const double alpha64 = S.alpha;
+        const int nitems = 2 * NT * nz;
+        for (int it = t; it < nitems; it += kBlock) {
+            const int c = it / (NT * nz), r2 = it - c * NT * nz;
+            const int k = r2 / NT, col = r2 - k * NT;
+            const int s = (col % kTX + 1) + (kTX + 2) * (col / kTX + 1);
+            const int v = smap[s];
+            if (!map_mine(v)) continue;
+            const int e = c * plane + k * NQ + map_src(v);
+            const float dn = fmaf(beta, ldf(D.d + e), ldf(D.z + e));
+            D.d[e] = dn;
+            D.x[e] = fma(alpha64, (double)dn, ldd(D.x + e));
+        }
     } else {
         const float alpha = (float)S.alpha, beta = (float)S.beta;
         const double alpha64 = S.alpha;
         const bool do_b = (step == MS_MERGED || step == MS_B);
-        const bool do_a = (step == MS_MERGED || step == MS_A);
+        const bool do_a = (step == MS_MERGED || step == MS_A || step == MS_A_UPD);
+        const bool upd = (step == MS_A_UPD);  // apply the owners' deferred d and x writes
         const int rin = par, rout = do_b ? (par ^ 1) : par;  // buffers holding r_i / r_{i+1}
         const float *__restrict__ q_in = D.q[rin];
         const float *__restrict__ az_in = D.Az[rin];
@@ -527,6 +608,11 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                             }
                         } else {
                             ro[u] = ldf(r_in + e);
+                            if (upd && map_mine(v)) {
+                                dold[u] = ldf(dvec + e);
+                                zold[u] = ldf(zvec + e);
+                                xold[u] = ldd(xvec + e);
+                            }
                         }
                         if (do_a && diag) pr[u] = __ldg(dinv + e);
                     }
@@ -552,6 +638,11 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                         }
                     } else {
                         rn = ro[u];
+                        if (upd && map_mine(v)) {  // the previous (checked) update's owner writes
+                            const float dn = fmaf(beta, dold[u], zold[u]);
+                            dvec[e] = dn;
+                            xvec[e] = fma(alpha64, (double)dn, xold[u]);
+                        }
                     }
                 }
                 if (do_a) {
