@@ -615,7 +615,7 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
             m.recs = nullptr;
             m.maps = nullptr;
             m.tiles = nullptr;
-            CU(cudaMalloc((void **)&m.recs, (size_t)ntiles * 2 * sizeof(TileRec)));
+            CU(cudaMalloc((void **)&m.recs, (size_t)kRecCopies * ntiles * 2 * sizeof(TileRec)));
             CU(cudaMalloc((void **)&m.maps, (size_t)ntiles * NS * sizeof(int)));
             CU(cudaMalloc((void **)&m.tiles, (size_t)ntiles * sizeof(MTile)));
             m.ntiles_cap = ntiles;
@@ -663,7 +663,7 @@ static int mixed_reset(Solver &sv, cudaStream_t s) {
     k_halo<<<nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4)), kBlock, 0, s>>>(sv.g, p.xu, p.xv, nullptr);
     CU(cudaGetLastError());
     CU(cudaMemsetAsync(sv.mixed.vec, 0, (size_t)16 * sv.nvec * sizeof(float), s));
-    CU(cudaMemsetAsync(sv.mixed.recs, 0, (size_t)sv.mixed.ntiles * 2 * sizeof(TileRec), s));  // tags restart at 1
+    CU(cudaMemsetAsync(sv.mixed.recs, 0, (size_t)kRecCopies * sv.mixed.ntiles * 2 * sizeof(TileRec), s));  // tags restart at 1
     CU(cudaMemsetAsync(sv.mixed.bc, 0, (2 * kBcastCopies + 1) * sizeof(Bcast), s));       // broadcast tag 0 = x0 state
     return CISMGPU_OK;
 }

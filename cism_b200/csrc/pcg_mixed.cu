@@ -40,11 +40,14 @@ constexpr int kMixedMaxNz = 32;                  // shared-memory bound of the m
 // a neighbour's half-updated d or x while it recomputes the halo of x.
 enum MStep { MS_INIT = 0, MS_A, MS_MERGED, MS_B, MS_CHECK_UNUSED, MS_DONE, MS_BC, MS_A_UPD, MS_FIN };
 
-// A tile's partial sums of one step, stamped with the step number (tag) last.
+// A tile's partial sums of one step, stamped with the step number (tag) last.  Each tile
+// writes kRecCopies copies ([copy][tile][parity]); a CTA reads copy blockIdx % kRecCopies,
+// so the all-to-all reads of a step spread over more L2 lines.
 struct TileRec {
     double p0, p1, p2;
     unsigned tag, pad;
 };
+constexpr int kRecCopies = 4;
 
 // The scalars a solve's leader broadcasts after summing a step's records (dynamic launches):
 // word = tag << 32 | done << 9 | par << 8 | step, written last.  Replicated kBcastCopies
@@ -71,7 +74,7 @@ struct MDesc {
     double *x;           // [2][nz][NQ]
     float *r[2], *q[2], *Az[2];  // [2][nz][NQ] each (u, v planes)
     float *z, *d;                // [2][nz][NQ]
-    TileRec *recs;       // [ntiles][2 step parities]
+    TileRec *recs;       // [kRecCopies][ntiles][2 step parities]
     Bcast *bc;           // [2 step parities][kBcastCopies] (dynamic launches)
     int *dflag;          // set once the solve is done (dynamic launches)
     const int *maps;     // [ntiles][(kTX+2)*(TY+2)] slot maps (k_slot_maps)
@@ -756,11 +759,14 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
     if (t == 0) {
         const unsigned tag = S.tick + 1u;
         TileRec *rp = D.recs + 2 * (size_t)tile + (tag & 1u);
-        rp->p0 = p0;
-        rp->p1 = p1;
-        rp->p2 = p2;
-        __threadfence();            // orders the record and the tile's vector stores before the tag
-        st_relaxed(&rp->tag, tag);  // (fence + relaxed store: a release without a second fence)
+        const size_t cstride = 2 * (size_t)D.ntiles;
+        for (int k = 0; k < kRecCopies; ++k) {
+            rp[k * cstride].p0 = p0;
+            rp[k * cstride].p1 = p1;
+            rp[k * cstride].p2 = p2;
+        }
+        __threadfence();  // orders the records and the tile's vector stores before the tags
+        for (int k = 0; k < kRecCopies; ++k) st_relaxed(&rp[k * cstride].tag, tag);  // fence + relaxed = release
     }
     __syncthreads();
 }
@@ -778,7 +784,7 @@ __device__ bool reduce_wait(MHead &hd, const MDesc *__restrict__ descs, MState *
         const MDesc &D = descs[hd.sid[cs]];
         const int ntl = D.ntiles;
         const unsigned tag = hd.st[cs].tick + 1u;
-        const TileRec *R = D.recs + (tag & 1u);
+        const TileRec *R = D.recs + (size_t)(blockIdx.x % kRecCopies) * 2 * ntl + (tag & 1u);
         DD a0{0.0, 0.0}, a1{0.0, 0.0}, a2{0.0, 0.0};
         int bad = 0;
         for (int w = threadIdx.x; w < ntl && !bad; w += kBlock) {
@@ -937,7 +943,7 @@ __device__ bool lead_duties(MHead &hd, const MDesc *__restrict__ descs, MState *
         const MDesc &D = descs[hd.sid[cs]];
         const int ntl = D.ntiles;
         const unsigned tag = hd.st[cs].tick + 1u;
-        const TileRec *R = D.recs + (tag & 1u);
+        const TileRec *R = D.recs + (size_t)(blockIdx.x % kRecCopies) * 2 * ntl + (tag & 1u);
         DD a0{0.0, 0.0}, a1{0.0, 0.0}, a2{0.0, 0.0};
         int bad = 0;
         for (int w = threadIdx.x; w < ntl && !bad; w += kBlock) {
