@@ -180,3 +180,21 @@ def test_batch_more_tiles_than_ctas(gpu_lib):
         np.testing.assert_array_equal(xv, xb[t][1])
     st, ou, ov, oerr, onit = oracle.pcg("chrongear", probs[3], 1, tol=1e-8, maxiters=5000)
     assert rel(xb[3], (ou, ov), probs[3]) < 1e-5
+
+
+@pytest.mark.parametrize("maxiters", [5, 7, 10])
+def test_mixed_stops_with_updated_x(gpu_lib, maxiters):
+    """A solve that stops at maxiters returns niters = maxiters.  When the last iteration is a
+    check iteration (5, 10), err is the FP64 residual of the returned x, so the update whose
+    writes are deferred past the check has been applied; both kernels agree."""
+    P = asm.dome()
+    S = cg.DeviceSolver(P)
+    err, nit = S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-14, maxiters)
+    xu, xv = S.x()
+    assert nit == maxiters and np.all(np.isfinite(xu)) and np.all(np.isfinite(xv))
+    errs, nits, sts = cg.solve_batch([S], cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-14, maxiters)
+    bu, bv = S.x()
+    assert sts[0] == 0 and nits[0] == maxiters
+    if maxiters % 5 == 0:
+        assert abs(true_residual(P, xu, xv) - err) <= 1e-9 * err
+        assert abs(true_residual(P, bu, bv) - errs[0]) <= 1e-9 * errs[0]
