@@ -582,7 +582,7 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
             bytes += n;
             return cudaMalloc(p, n);
         };
-        CU(alloc((void **)&m.A32, (size_t)4 * NC * nvec * sizeof(float)));
+        CU(alloc((void **)&m.A32, (size_t)NC * nvec * sizeof(float4)));
         CU(alloc((void **)&m.pre, (size_t)6 * nvec * sizeof(float)));
         CU(alloc((void **)&m.vec, (size_t)16 * nvec * sizeof(float)));
         CU(alloc((void **)&m.state, sizeof(MState)));

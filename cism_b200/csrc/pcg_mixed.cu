@@ -66,7 +66,7 @@ struct MDesc {
     int precond;     // 0 none, 1 diag, 2 sia
     int TY;          // tile height of this solve
     int tiles_x, tiles_y, ntiles;
-    const float *A32;    // [4][NC][nz][NQ]
+    const float4 *A32;   // [NC][nz][NQ] of (uu, uv, vu, vv): one 16-byte load per coupling
     const double *A64;   // [4][NC][nz][NQ]
     const float *pre;    // diag: [2][nz][NQ] inverse diagonal; sia: [2][3][nz][NQ] (1/beta, sb, gamma)
     const int32_t *act;  // [NQ]
@@ -674,11 +674,8 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
             // ---- pass 2: Az = A z on (column, level) items, z to HBM, partial dots ----
             // Couplings that leave the grid are zero in the FP32 copy and the padded z rows
             // and out-of-grid halo slots are zero, so every node sums all NC terms.
-            const float *__restrict__ Auu = D.A32;
-            const float *__restrict__ Auv = D.A32 + (size_t)NC * plane;
-            const float *__restrict__ Avu = D.A32 + (size_t)2 * NC * plane;
-            const float *__restrict__ Avv = D.A32 + (size_t)3 * NC * plane;
-            const float *sA = reinterpret_cast<const float *>(smem + ly.off_A());  // [4][NC][nz*NT]
+            const float4 *__restrict__ A4 = D.A32;
+            const float4 *sA = reinterpret_cast<const float4 *>(smem + ly.off_A());  // [NC][nz*NT]
             const int NN = nz * NT;
             float *__restrict__ Azu = D.Az[rout];
             float *__restrict__ Azv = D.Az[rout] + plane;
@@ -716,11 +713,11 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                                         const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
                                         const int zi = (k + OFF + kA) * NS + s + iA + (kTX + 2) * jA;
                                         const float z1 = szu[zi], z2 = szv[zi];
-                                        const int a = c * NN + it;
-                                        yu[u] = fmaf(sA[a], z1, yu[u]);
-                                        yu[u] = fmaf(sA[NC * NN + a], z2, yu[u]);
-                                        yv[u] = fmaf(sA[2 * NC * NN + a], z1, yv[u]);
-                                        yv[u] = fmaf(sA[3 * NC * NN + a], z2, yv[u]);
+                                        const float4 a = sA[c * NN + it];
+                                        yu[u] = fmaf(a.x, z1, yu[u]);
+                                        yu[u] = fmaf(a.y, z2, yu[u]);
+                                        yv[u] = fmaf(a.z, z1, yv[u]);
+                                        yv[u] = fmaf(a.w, z2, yv[u]);
                                     }
                                 } else {
 #pragma unroll
@@ -728,11 +725,11 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                                         const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
                                         const int zi = (k + OFF + kA) * NS + s + iA + (kTX + 2) * jA;
                                         const float z1 = szu[zi], z2 = szv[zi];
-                                        const size_t a = (size_t)c * plane + e;
-                                        yu[u] = fmaf(__ldg(Auu + a), z1, yu[u]);
-                                        yu[u] = fmaf(__ldg(Auv + a), z2, yu[u]);
-                                        yv[u] = fmaf(__ldg(Avu + a), z1, yv[u]);
-                                        yv[u] = fmaf(__ldg(Avv + a), z2, yv[u]);
+                                        const float4 a = __ldg(A4 + (size_t)c * plane + e);
+                                        yu[u] = fmaf(a.x, z1, yu[u]);
+                                        yu[u] = fmaf(a.y, z2, yu[u]);
+                                        yv[u] = fmaf(a.z, z1, yv[u]);
+                                        yv[u] = fmaf(a.w, z2, yv[u]);
                                     }
                                 }
                             }
@@ -878,19 +875,19 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
         int *smap = reinterpret_cast<int *>(smem + ly.off_map());
         const int *tmap = D.maps + (size_t)T.tile * NS;
         for (int sl = threadIdx.x; sl < NS; sl += kBlock) smap[sl] = tmap[sl];
-        float *sA = reinterpret_cast<float *>(smem + ly.off_A());
+        float4 *sA = reinterpret_cast<float4 *>(smem + ly.off_A());
         const int nz = (NC == 27) ? D.g.nz : 1;
         const int NQ = (int)D.g.NQ;
         const int plane = nz * NQ;
         const int tx = T.tile % D.tiles_x, ty = T.tile / D.tiles_x;
         const int i0 = D.g.ilo + tx * kTX, j0 = D.g.jlo + ty * TY;
         const int NN = nz * NT;
-        for (int w = threadIdx.x; w < 4 * NC * NN; w += kBlock) {
-            const int it = w % NN, bc = w / NN;  // bc = block * NC + c
+        for (int w = threadIdx.x; w < NC * NN; w += kBlock) {
+            const int it = w % NN, c = w / NN;
             const int col = it % NT, k = it / NT;
             const int i = i0 + col % kTX, j = j0 + col / kTX;
-            float a = 0.0f;
-            if (i <= D.g.ihi && j <= D.g.jhi) a = D.A32[(size_t)bc * plane + k * NQ + j * D.g.NX + i];
+            float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (i <= D.g.ihi && j <= D.g.jhi) a = D.A32[(size_t)c * plane + k * NQ + j * D.g.NX + i];
             sA[w] = a;
         }
         __syncthreads();
@@ -1126,18 +1123,20 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict
 // array (which the reference skips) are stored as zero so the FP32 stencil loop needs
 // no bounds tests.
 template <int NC>
-__global__ void k_to_f32(Geom g, const double *__restrict__ src, float *__restrict__ dst) {
+__global__ void k_to_f32(Geom g, const double *__restrict__ src, float4 *__restrict__ dst) {
     const long long plane = (long long)g.nz * g.NQ;
-    const long long n = 4LL * NC * plane;
+    const long long n = (long long)NC * plane;  // one float4 (uu, uv, vu, vv) per coupling and node
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
-        const int c = (int)((e / plane) % NC);
+        const int c = (int)(e / plane);
         const long long r = e % plane;
         const int k = (int)(r / g.NQ);
         const long long q = r % g.NQ;
         const int i = (int)(q % g.NX), j = (int)(q / g.NX);
         const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
         const bool in = i + iA >= 0 && i + iA < g.NX && j + jA >= 0 && j + jA < g.NY && k + kA >= 0 && k + kA < g.nz;
-        dst[e] = in ? (float)src[e] : 0.0f;
+        const size_t bs = (size_t)NC * plane;  // FP64 planes [4][NC][nz][NQ]
+        dst[e] = in ? make_float4((float)src[e], (float)src[bs + e], (float)src[2 * bs + e], (float)src[3 * bs + e])
+                    : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
 }
 
@@ -1185,7 +1184,8 @@ struct MixedBufs {
     long long shape_nvec = 0;
     int shape_nc = 0;
     int precond = -1;
-    float *A32 = nullptr, *pre = nullptr, *vec = nullptr;
+    float4 *A32 = nullptr;
+    float *pre = nullptr, *vec = nullptr;
     int *maps = nullptr;
     TileRec *recs = nullptr;
     Bcast *bc = nullptr;       // [2][kBcastCopies] broadcast lines, then one line holding the done flag
@@ -1201,7 +1201,8 @@ struct MixedBufs {
         for (void *p : {(void *)A32, (void *)pre, (void *)vec, (void *)recs, (void *)state, (void *)desc,
                         (void *)tiles, (void *)ctl, (void *)maps, (void *)bc})
             if (p) cudaFree(p);
-        A32 = pre = vec = nullptr;
+        A32 = nullptr;
+        pre = vec = nullptr;
         maps = nullptr;
         ntiles = ntiles_cap = 0;
         maps_cap = 0;
