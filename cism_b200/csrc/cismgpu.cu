@@ -349,7 +349,7 @@ int Solver::run_standard(int precond, int ncheck, double tol, int maxiters) {
 
     k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
-    k_mv<NCC, MV_PLAIN><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
+    k_mv<NCC, MV_PLAIN><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
                                               nullptr, rc(EPI_NONE, 0));
     k_vec<OP_STD_INIT><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_L2RHS, 0));
     CU(cudaGetLastError());
@@ -360,13 +360,13 @@ int Solver::run_standard(int precond, int ncheck, double tol, int maxiters) {
         k_vec<OP_STD_D><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, iter));
         k_halo<<<hb, kBlock, 0, s>>>(gg, p.du, p.dv, st);
         TRY(timed([&] {
-            k_mv<NCC, MV_DQ><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr,
+            k_mv<NCC, MV_DQ><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr,
                                                    nullptr, rc(EPI_STD_ETA2, iter));
         }));
         k_vec<OP_XR><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, iter));
         if (is_check(iter, ncheck)) {
             k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
-            k_mv<NCC, MV_RESID><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
+            k_mv<NCC, MV_RESID><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
                                                       rc(EPI_CHECK, iter));
             CU(cudaGetLastError());
             int f = poll.after_check();
@@ -400,13 +400,13 @@ int Solver::run_chrongear(int precond, int ncheck, double tol, int maxiters) {
     k_vec<OP_DOT_BB><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_L2RHS, 0));
     // first pass (:3085-3290)
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
-    k_mv<NCC, MV_PLAIN><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
+    k_mv<NCC, MV_PLAIN><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
                                               nullptr, rc(EPI_NONE, 1));
     k_vec<OP_CG_INIT><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, 1));
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
     k_precond<PRE_CG_FIRST><<<nb, kBlock, 0, s>>>(gg, precond, Ad, NCC, ac, p.ru, p.rv, p.zu, p.zv, p.du, p.dv,
                                                   rc(EPI_CG_RHO0, 1));
-    k_mv<NCC, MV_DQ><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr,
+    k_mv<NCC, MV_DQ><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr,
                                            rc(EPI_CG_FIRST, 1));
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.qu, p.qv, st);
     k_vec<OP_XR><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, 1));
@@ -416,13 +416,13 @@ int Solver::run_chrongear(int precond, int ncheck, double tol, int maxiters) {
         k_precond<PRE_ONLY><<<nb, kBlock, 0, s>>>(gg, precond, Ad, NCC, ac, p.ru, p.rv, p.zu, p.zv, nullptr, nullptr,
                                                   rc(EPI_NONE, iter));
         TRY(timed([&] {
-            k_mv<NCC, MV_CG_AZ><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.zu, p.zv, p.Azu, p.Azv, nullptr, nullptr, p.ru,
+            k_mv<NCC, MV_CG_AZ><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.zu, p.zv, p.Azu, p.Azv, nullptr, nullptr, p.ru,
                                                       p.rv, rc(EPI_CG_ITER, iter));
         }));
         k_halo<<<hb, kBlock, 0, s>>>(gg, p.Azu, p.Azv, st);
         k_vec<OP_CG_UPD><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, iter));
         if (is_check(iter, ncheck)) {
-            k_mv<NCC, MV_RESID><<<nb, kBlock, 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
+            k_mv<NCC, MV_RESID><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
                                                       rc(EPI_CHECK, iter));
             k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
             CU(cudaGetLastError());
@@ -927,11 +927,11 @@ static int oneshot_matvec(bool is3d, int nx, int ny, int nz, const cismgpu_par_t
     k_init_state<<<1, 1, 0, sv.stream>>>(st, 0.0, 0);
     RedCtx rc0{sv.partials.as<DD>(), st, EPI_NONE, 0};
     if (is3d)
-        k_mv<27, MV_PLAIN><<<nblocks(sv.g.NQ), kBlock, 0, sv.stream>>>(sv.g, sv.A.as<double>(), sv.act.as<int32_t>(),
+        k_mv<27, MV_PLAIN><<<nblocks(sv.g.NQ), mv_threads<27>(), 0, sv.stream>>>(sv.g, sv.A.as<double>(), sv.act.as<int32_t>(),
                                                                       p.bu, p.bv, p.xu, p.xv, nullptr, nullptr,
                                                                       nullptr, nullptr, rc0);
     else
-        k_mv<9, MV_PLAIN><<<nblocks(sv.g.NQ), kBlock, 0, sv.stream>>>(sv.g, sv.A.as<double>(), sv.act.as<int32_t>(),
+        k_mv<9, MV_PLAIN><<<nblocks(sv.g.NQ), mv_threads<9>(), 0, sv.stream>>>(sv.g, sv.A.as<double>(), sv.act.as<int32_t>(),
                                                                      p.bu, p.bv, p.xu, p.xv, nullptr, nullptr,
                                                                      nullptr, nullptr, rc0);
     CU(cudaGetLastError());

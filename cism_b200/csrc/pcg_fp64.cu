@@ -109,6 +109,73 @@ __device__ void reduce_and_finish(const RedCtx &rc, DD v0, DD v1) {
     }
 }
 
+// Block tree over the first 256 threads of a block of any size (the other threads pass
+// through the barriers); result in thread 0.  Same order as block_tree.
+__device__ __forceinline__ DD block_tree_first(DD v, DD *sm) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp < kBlock / 32) {
+#pragma unroll
+        for (int off = 16; off >= 1; off >>= 1) {
+            DD o = dd_shfl_down(v, off);
+            if (lane + off < 32) v = dd_add(v, o);
+        }
+    }
+    __syncthreads();  // protect 'sm' reuse across consecutive calls
+    if (warp < kBlock / 32 && lane == 0) sm[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        DD w = (lane < 8) ? sm[lane] : DD{0.0, 0.0};
+#pragma unroll
+        for (int off = 4; off >= 1; off >>= 1) {
+            DD o = dd_shfl_down(w, off);
+            if (lane + off < 32) w = dd_add(w, o);
+        }
+        v = w;
+    }
+    return v;
+}
+
+// reduce_and_finish for blocks of kBlock * L threads whose first kBlock threads hold the
+// values (the column sums); identical order and result to reduce_and_finish.
+template <int NF>
+__device__ void reduce_and_finish_first(const RedCtx &rc, DD v0, DD v1) {
+    __shared__ DD sm[8];
+    __shared__ bool last;
+    DD b0 = block_tree_first(v0, sm);
+    DD b1 = DD{0.0, 0.0};
+    if (NF > 1) b1 = block_tree_first(v1, sm);
+    if (threadIdx.x == 0) {
+        rc.partials[2 * blockIdx.x + 0] = b0;
+        rc.partials[2 * blockIdx.x + 1] = b1;
+        __threadfence();
+        unsigned int t = atomicAdd(&rc.st->ticket[0], 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    DD a0{0.0, 0.0}, a1{0.0, 0.0};
+    if (threadIdx.x < kBlock)
+        for (unsigned int c = threadIdx.x; c < gridDim.x; c += kBlock) {
+            DD p0, p1;
+            p0.hi = __ldcg(&rc.partials[2 * c].hi);
+            p0.lo = __ldcg(&rc.partials[2 * c].lo);
+            a0 = dd_add(a0, p0);
+            if (NF > 1) {
+                p1.hi = __ldcg(&rc.partials[2 * c + 1].hi);
+                p1.lo = __ldcg(&rc.partials[2 * c + 1].lo);
+                a1 = dd_add(a1, p1);
+            }
+        }
+    DD r0 = block_tree_first(a0, sm);
+    DD r1 = DD{0.0, 0.0};
+    if (NF > 1) r1 = block_tree_first(a1, sm);
+    if (threadIdx.x == 0) {
+        rc.st->ticket[0] = 0u;
+        epilogue(rc.st, rc.epi, rc.iter, r0.hi + r0.lo, r1.hi + r1.lo);
+    }
+}
+
 __device__ __forceinline__ void col_of(const Geom &g, long long q, int &i, int &j) {
     j = (int)(q / g.NX);
     i = (int)(q - (long long)j * g.NX);
@@ -145,44 +212,85 @@ enum MvMode { MV_PLAIN = 0, MV_RESID, MV_DQ, MV_CG_AZ };
 //   MV_RESID : r = b - y (whole array); S0 = (r,r)             [:1454-1466, :3504-3516]
 //   MV_DQ    : S0 = (x,y) with x = d, y = q                    [:1376-1381, :3241-3248]
 //   MV_CG_AZ : S0 = (r,z), S1 = (y,z) with x = z, y = Az       [:3401-3413]
+// Level lanes of the structured matvec: 3D blocks have kMvLanes threads per column (levels
+// k = lane, lane + kMvLanes, ...), so a CTA holds 256 columns x 2 lanes and a launch has enough
+// loads in flight to stream the 108 coefficient planes while two CTAs fit on an SM (no
+// second wave of a few CTAs at typical sizes); 2D has one level.
+constexpr int kMvLanes = 2;
+constexpr int kMvChunk = 8;  // levels per shared-memory round of the per-column dot terms
+template <int NC> __host__ __device__ constexpr int mv_threads() { return NC == 27 ? kBlock * kMvLanes : kBlock; }
+
+// y = A x (+ the statement fused with it).  Per column the dot terms are added over k in
+// level order by the column's first lane (through shared memory), then the block tree of
+// the 256 columns: the same order as one thread per column.
 template <int NC, int MODE>
-__global__ void __launch_bounds__(kBlock) k_mv(Geom g, const double *__restrict__ A, const int32_t *__restrict__ act,
-                                               const double *__restrict__ xu, const double *__restrict__ xv,
-                                               double *__restrict__ yu, double *__restrict__ yv,
-                                               const double *__restrict__ bu, const double *__restrict__ bv,
-                                               double *__restrict__ ru, double *__restrict__ rv, RedCtx rc) {
+__global__ void __launch_bounds__(mv_threads<NC>(), NC == 27 ? 2 : 1) k_mv(Geom g, const double *__restrict__ A,
+                                                          const int32_t *__restrict__ act,
+                                                          const double *__restrict__ xu, const double *__restrict__ xv,
+                                                          double *__restrict__ yu, double *__restrict__ yv,
+                                                          const double *__restrict__ bu, const double *__restrict__ bv,
+                                                          double *__restrict__ ru, double *__restrict__ rv, RedCtx rc) {
+    constexpr int L = mv_threads<NC>() / kBlock;
+    constexpr bool RED = (MODE == MV_RESID || MODE == MV_DQ || MODE == MV_CG_AZ);
+    constexpr int NT = (MODE == MV_CG_AZ) ? 2 : 1;
+    __shared__ double terms[RED && L > 1 ? NT * kMvChunk * kBlock : 1];
     if (rc.st->done) return;
-    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    const int col = threadIdx.x % kBlock, lane = threadIdx.x / kBlock;
+    const long long q = (long long)blockIdx.x * kBlock + col;
     DD s0{0.0, 0.0}, s1{0.0, 0.0};
+    int i = 0, j = 0;
+    bool own = false, on = false;
     if (q < g.NQ) {
-        int i, j;
         col_of(g, q, i, j);
-        const bool own = owned(g, i, j);
-        const bool on = own && act[q] != 0;
-        for (int k = 0; k < g.nz; ++k) {
+        own = owned(g, i, j);
+        on = own && act[q] != 0;
+    }
+    for (int k0 = 0; k0 < g.nz; k0 += (L > 1 ? kMvChunk : g.nz)) {
+        const int k1 = (L > 1) ? min(g.nz, k0 + kMvChunk) : g.nz;
+        for (int k = k0 + lane; k < k1; k += L) {
+            if (q >= g.NQ) break;
             const long long e = (long long)k * g.NQ + q;
             double a = 0.0, b = 0.0;
             if (on) mv_row<NC>(g, A, xu, xv, i, j, q, k, a, b);
             yu[e] = a;
             yv[e] = b;
+            double t0 = 0.0, t1 = 0.0;
             if (MODE == MV_RESID) {
                 const double r1 = __dsub_rn(bu[e], a), r2 = __dsub_rn(bv[e], b);
                 ru[e] = r1;
                 rv[e] = r2;
-                if (own) s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(r1, r1), __dmul_rn(r2, r2)));
+                t0 = __dadd_rn(__dmul_rn(r1, r1), __dmul_rn(r2, r2));
             } else if (MODE == MV_DQ) {
-                if (own) s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(xu[e], a), __dmul_rn(xv[e], b)));
+                t0 = __dadd_rn(__dmul_rn(xu[e], a), __dmul_rn(xv[e], b));
             } else if (MODE == MV_CG_AZ) {
-                if (own) {
-                    const double z1 = xu[e], z2 = xv[e];
-                    s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(ru[e], z1), __dmul_rn(rv[e], z2)));
-                    s1 = dd_add_d(s1, __dadd_rn(__dmul_rn(a, z1), __dmul_rn(b, z2)));
+                const double z1 = xu[e], z2 = xv[e];
+                t0 = __dadd_rn(__dmul_rn(ru[e], z1), __dmul_rn(rv[e], z2));
+                t1 = __dadd_rn(__dmul_rn(a, z1), __dmul_rn(b, z2));
+            }
+            if (RED) {
+                if (L == 1) {
+                    if (own) {
+                        s0 = dd_add_d(s0, t0);
+                        if (NT > 1) s1 = dd_add_d(s1, t1);
+                    }
+                } else {
+                    terms[(k - k0) * kBlock + col] = t0;
+                    if (NT > 1) terms[(kMvChunk + k - k0) * kBlock + col] = t1;
                 }
             }
         }
+        if (RED && L > 1) {  // the column's terms of this chunk, in level order
+            __syncthreads();
+            if (lane == 0 && own)
+                for (int k = k0; k < k1; ++k) {
+                    s0 = dd_add_d(s0, terms[(k - k0) * kBlock + col]);
+                    if (NT > 1) s1 = dd_add_d(s1, terms[(kMvChunk + k - k0) * kBlock + col]);
+                }
+            __syncthreads();
+        }
     }
-    if (MODE == MV_RESID || MODE == MV_DQ) reduce_and_finish<1>(rc, s0, s1);
-    if (MODE == MV_CG_AZ) reduce_and_finish<2>(rc, s0, s1);
+    if (MODE == MV_RESID || MODE == MV_DQ) reduce_and_finish_first<1>(rc, s0, s1);
+    if (MODE == MV_CG_AZ) reduce_and_finish_first<2>(rc, s0, s1);
 }
 
 // ---------------------------------------------------------------------------
