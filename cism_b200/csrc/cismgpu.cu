@@ -491,6 +491,7 @@ static MDesc mixed_desc(const Solver &sv, int precond, int TY) {  // TY: the sol
     D.bc = m.bc;
     D.dflag = reinterpret_cast<int *>(m.bc + 2 * kBcastCopies);
     D.maps = m.maps;
+    D.nbrs = m.nbrs;
     return D;
 }
 
@@ -611,12 +612,15 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
         if (ntiles > m.ntiles_cap || (long long)ntiles * NS > m.maps_cap) {
             if (m.recs) cudaFree(m.recs);
             if (m.maps) cudaFree(m.maps);
+            if (m.nbrs) cudaFree(m.nbrs);
             if (m.tiles) cudaFree(m.tiles);
             m.recs = nullptr;
             m.maps = nullptr;
+            m.nbrs = nullptr;
             m.tiles = nullptr;
             CU(cudaMalloc((void **)&m.recs, (size_t)kRecCopies * ntiles * 2 * sizeof(TileRec)));
             CU(cudaMalloc((void **)&m.maps, (size_t)ntiles * NS * sizeof(int)));
+            CU(cudaMalloc((void **)&m.nbrs, (size_t)ntiles * kNbrStride * sizeof(int)));
             CU(cudaMalloc((void **)&m.tiles, (size_t)ntiles * sizeof(MTile)));
             m.ntiles_cap = ntiles;
             m.maps_cap = (long long)ntiles * NS;
@@ -624,6 +628,8 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
         m.ntiles = ntiles;
         const MDesc D = mixed_desc(sv, precond, TY);
         k_slot_maps<<<nblocks((long long)ntiles * NS), kBlock, 0, sv.stream>>>(D, m.maps);
+        CU(cudaGetLastError());
+        k_tile_nbrs<<<nblocks(ntiles), kBlock, 0, sv.stream>>>(D, m.maps, m.nbrs);
         CU(cudaGetLastError());
         std::vector<MTile> tl(ntiles);
         for (int t = 0; t < ntiles; ++t) tl[t] = MTile{0, t};

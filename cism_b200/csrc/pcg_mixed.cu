@@ -4,7 +4,7 @@
 // pcg_solver_chrongear_* (glissade_velo_higher_pcg.F90:3296-3581) with the
 // matrix, z, d, q, Az and the recursive residual r stored and multiplied in FP32,
 // the solution x accumulated in FP64, every dot product accumulated in FP64
-// (double-double across tiles), and the reference's periodic residual replacement
+// (within and across tiles, in one fixed order), and the reference's periodic residual replacement
 // (:3482-3579) done in FP64: at every check iteration r = b - A x is computed
 // with the FP64 matrix, the FP64 norm gives err, and the FP32 recurrences
 // continue from the true residual (a "reliable update": the Krylov directions
@@ -40,14 +40,21 @@ constexpr int kMixedMaxNz = 32;                  // shared-memory bound of the m
 // a neighbour's half-updated d or x while it recomputes the halo of x.
 enum MStep { MS_INIT = 0, MS_A, MS_MERGED, MS_B, MS_CHECK_UNUSED, MS_DONE, MS_BC, MS_A_UPD, MS_FIN };
 
-// A tile's partial sums of one step, stamped with the step number (tag) last.  Each tile
-// writes kRecCopies copies ([copy][tile][parity]); a CTA reads copy blockIdx % kRecCopies,
-// so the all-to-all reads of a step spread over more L2 lines.
-struct TileRec {
-    double p0, p1, p2;
-    unsigned tag, pad;
+// A tile's partial sums of one step.  Every 64-bit word carries the step number (tag) in its
+// high half and one 32-bit half of a sum in its low half (w[2i] low, w[2i+1] high half of
+// sum i), so a reader that finds the tag in all six words has the step's values, with
+// relaxed loads and no fence.  The words are stored after a release fence, so an acquire
+// load of a word also orders the tile's vector stores of the step before the reader's
+// later loads (the halo).  Each tile writes kRecCopies copies ([copy][tile][parity]); a CTA
+// reads copy blockIdx % kRecCopies, so the all-to-all reads of a step spread over more L2
+// lines.
+struct __align__(64) TileRec {
+    unsigned long long w[6];
+    unsigned long long pad[2];
 };
 constexpr int kRecCopies = 4;
+constexpr int kNbrMax = 8;     // tiles whose columns one tile's halo reads (else: fence)
+constexpr int kNbrStride = kNbrMax + 1;  // [count or -1, tiles...] per tile
 
 // The scalars a solve's leader broadcasts after summing a step's records (dynamic launches):
 // word = tag << 32 | done << 9 | par << 8 | step, written last.  Replicated kBcastCopies
@@ -78,6 +85,7 @@ struct MDesc {
     Bcast *bc;           // [2 step parities][kBcastCopies] (dynamic launches)
     int *dflag;          // set once the solve is done (dynamic launches)
     const int *maps;     // [ntiles][(kTX+2)*(TY+2)] slot maps (k_slot_maps)
+    const int *nbrs;     // [ntiles][kNbrStride] tiles owning the tile's live halo columns (k_tile_nbrs)
 };
 
 struct MState {
@@ -146,6 +154,19 @@ __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long l
 }
 __device__ __forceinline__ void st_relaxed64(unsigned long long *p, unsigned long long v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+// The six words of a record, as three 16-byte relaxed loads (each 64-bit element is a
+// single-copy-atomic access).
+__device__ __forceinline__ void ld_rec(const TileRec *rp, unsigned long long (&w)[6]) {
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w[0]), "=l"(w[1]) : "l"(rp->w) : "memory");
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w[2]), "=l"(w[3]) : "l"(rp->w + 2) : "memory");
+    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w[4]), "=l"(w[5]) : "l"(rp->w + 4) : "memory");
 }
 __device__ __forceinline__ int ld_acquire_i(const int *p) {
     int v;
@@ -239,6 +260,7 @@ __device__ void advance_state(MState &S, double S0, double S1, double S2) {
 constexpr int kTX = 32;
 constexpr int kMaxCtaSolves = 64;  // distinct solves whose tiles one CTA may hold in a launch
 constexpr int kMaxTY = 64;
+constexpr int kMaxAcq = 32;        // neighbour tiles a CTA acquires per step (4 tiles x 8)
 constexpr int kCh2 = 4;            // stencil items per load batch
 constexpr int kChR = 4;            // FP64 residual items per load batch
 
@@ -250,7 +272,9 @@ struct MHead {
     int nsolve;
     int cur;                   // cache slot described by D
     double red[8][3];
-    DD rdd[8][3];
+    double rsum[8][3];
+    int nacq;                  // >= 0: the CTA reads the halo of acq[0..nacq) only; -1: fence
+    int acq[kMaxAcq];
 };
 
 // Dynamic shared memory: head | map[NS] | z[2][KP][NS] | rt[2][NZM][NT]
@@ -323,6 +347,34 @@ __global__ void k_slot_maps(MDesc D, int *maps) {
         if (live && interior && m == (long long)j * g.NX + i) v |= 2;
     }
     maps[id] = v;
+}
+
+// For each tile, the other tiles owning a live column its halo slots read ([count, tiles]),
+// or count -1 if there are more than kNbrMax (the readers then fence instead).
+__global__ void k_tile_nbrs(MDesc D, const int *maps, int *nbrs) {
+    const int tile = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tile >= D.ntiles) return;
+    const Geom &g = D.g;
+    const int NS = (kTX + 2) * (D.TY + 2);
+    int list[kNbrMax];
+    int n = 0;
+    bool over = false;
+    for (int sl = 0; sl < NS && !over; ++sl) {
+        const int v = maps[(size_t)tile * NS + sl];
+        if (!map_live(v)) continue;
+        const int m = map_src(v);
+        const int mi = m % g.NX, mj = m / g.NX;
+        const int ot = ((mj - g.jlo) / D.TY) * D.tiles_x + (mi - g.ilo) / kTX;
+        if (ot == tile) continue;
+        bool seen = false;
+        for (int k = 0; k < n; ++k) seen |= (list[k] == ot);
+        if (seen) continue;
+        if (n == kNbrMax) over = true;
+        else list[n++] = ot;
+    }
+    int *out = nbrs + (size_t)tile * kNbrStride;
+    out[0] = over ? -1 : n;
+    for (int k = 0; k < n; ++k) out[1 + k] = list[k];
 }
 
 // z = M^-1 r on one column of the SIA tridiagonal, in place in smem (zc = z[c][0][0],
@@ -753,76 +805,126 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
         }
     }
     block_sum3(p0, p1, p2, hd.red);
-    if (t == 0) {
-        const unsigned tag = S.tick + 1u;
-        TileRec *rp = D.recs + 2 * (size_t)tile + (tag & 1u);
-        const size_t cstride = 2 * (size_t)D.ntiles;
-        for (int k = 0; k < kRecCopies; ++k) {
-            rp[k * cstride].p0 = p0;
-            rp[k * cstride].p1 = p1;
-            rp[k * cstride].p2 = p2;
+    if (t < 32) {  // warp 0: lane c*6+k stores word k of copy c, after a release fence
+        p0 = __shfl_sync(0xffffffffu, p0, 0);
+        p1 = __shfl_sync(0xffffffffu, p1, 0);
+        p2 = __shfl_sync(0xffffffffu, p2, 0);
+        if (t < 6 * kRecCopies) {
+            const unsigned tag = S.tick + 1u;
+            const int c = t / 6, k = t - 6 * (t / 6);
+            const double pv = (k < 2) ? p0 : ((k < 4) ? p1 : p2);
+            const unsigned half = (k & 1) ? (unsigned)__double2hiint(pv) : (unsigned)__double2loint(pv);
+            TileRec *rp = D.recs + (size_t)c * 2 * D.ntiles + 2 * (size_t)tile + (tag & 1u);
+            fence_acq_rel();  // the tile's vector stores (every thread's, via the barrier above) first
+            st_relaxed64(&rp->w[k], ((unsigned long long)tag << 32) | half);
         }
-        __threadfence();  // orders the records and the tile's vector stores before the tags
-        for (int k = 0; k < kRecCopies; ++k) st_relaxed(&rp[k * cstride].tag, tag);  // fence + relaxed = release
     }
     __syncthreads();
 }
 
+// Waits for the step-`tag` records of the ntl tiles at R (one record pair per tile) and sums
+// them in a fixed order: thread t takes tiles t, t + 256, ... in increasing order, then a
+// warp shuffle tree and a tree over the 8 warp sums.  Every CTA summing a solve's records
+// runs this with the same inputs, so all of them get bit-identical sums (in thread 0).
+// Records validate themselves (the tag in every word), so a thread polls its tiles with
+// relaxed loads issued together: one memory round trip once they are there.  Ordering for
+// the loads that follow: with nacq >= 0, threads 0..nacq-1 each take an acquire load of a
+// record of tile acq[t] (the tiles whose columns the CTA's halo reads) alongside; with
+// nacq < 0 every thread ends with an acquire fence (a leader whose sums others rely on).
+// Returns false if a wait gave up.
+constexpr int kRecPerThread = 2;  // tiles a thread polls at once (ntl <= 512 in one round)
+__device__ bool sum_records(const TileRec *R, int ntl, unsigned tag, MCtl *ctl, double (*rsum)[3],
+                            const int *acq, int nacq, double &s0, double &s1, double &s2) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    int bad = 0;
+    const int at = (nacq > 0 && (int)threadIdx.x < nacq) ? acq[threadIdx.x] : -1;
+    bool acq_need = at >= 0;
+    for (int w0 = threadIdx.x; (w0 < ntl || acq_need) && !bad; w0 += kRecPerThread * kBlock) {
+        unsigned need = 0;
+#pragma unroll
+        for (int u = 0; u < kRecPerThread; ++u)
+            if (w0 + u * kBlock < ntl) need |= 1u << u;
+        double v[kRecPerThread][3];
+#pragma unroll
+        for (int u = 0; u < kRecPerThread; ++u) v[u][0] = v[u][1] = v[u][2] = 0.0;
+        const long long t0 = clock64();
+        unsigned spins = 0;
+        for (;;) {
+#pragma unroll
+            for (int u = 0; u < kRecPerThread; ++u) {
+                if (!((need >> u) & 1u)) continue;
+                unsigned long long wd[6];
+                ld_rec(R + 2 * (size_t)(w0 + u * kBlock), wd);
+                bool ok = true;
+#pragma unroll
+                for (int k = 0; k < 6; ++k) ok &= (unsigned)(wd[k] >> 32) == tag;
+                if (ok) {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+                        v[u][k] = __hiloint2double((int)(unsigned)wd[2 * k + 1], (int)(unsigned)wd[2 * k]);
+                    need &= ~(1u << u);
+                }
+            }
+            if (acq_need && (unsigned)(ld_acquire64(&R[2 * (size_t)at].w[5]) >> 32) == tag) acq_need = false;
+            if (!need && !acq_need) break;
+            __nanosleep(spins < 16 ? 20 : 100);
+            if ((++spins & 31u) == 0) {
+                if (*(volatile int *)&ctl->abort) { bad = 1; break; }
+                if (clock64() - t0 > kWaitCycles) {
+                    atomicExch(&ctl->abort, 1);
+                    bad = 1;
+                    break;
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kRecPerThread; ++u)
+            if (w0 + u * kBlock < ntl) { a0 += v[u][0]; a1 += v[u][1]; a2 += v[u][2]; }
+    }
+    if (nacq < 0) fence_acq_rel();
+    if (__syncthreads_or(bad)) return false;
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        const double o0 = __shfl_down_sync(0xffffffffu, a0, off), o1 = __shfl_down_sync(0xffffffffu, a1, off),
+                     o2 = __shfl_down_sync(0xffffffffu, a2, off);
+        if (lane + off < 32) { a0 += o0; a1 += o1; a2 += o2; }
+    }
+    if (lane == 0) { rsum[warp][0] = a0; rsum[warp][1] = a1; rsum[warp][2] = a2; }
+    __syncthreads();
+    if (warp == 0) {
+        constexpr int NW = kBlock / 32;
+        a0 = lane < NW ? rsum[lane][0] : 0.0;
+        a1 = lane < NW ? rsum[lane][1] : 0.0;
+        a2 = lane < NW ? rsum[lane][2] : 0.0;
+#pragma unroll
+        for (int off = NW / 2; off >= 1; off >>= 1) {
+            const double o0 = __shfl_down_sync(0xffffffffu, a0, off), o1 = __shfl_down_sync(0xffffffffu, a1, off),
+                         o2 = __shfl_down_sync(0xffffffffu, a2, off);
+            if (lane + off < NW) { a0 += o0; a1 += o1; a2 += o2; }
+        }
+    }
+    s0 = a0; s1 = a1; s2 = a2;
+    return true;
+}
+
 // Wait for the records of the step just taken by every running solve this CTA holds, sum
-// them and advance the solve's cached state.  All threads take part: thread t waits for and
-// accumulates tiles t, t+256, ... in double-double, then a fixed shuffle/warp tree.  Every
-// CTA holding a solve does this with the same inputs in the same order, so all copies of a
-// solve's state stay bit-identical.  The CTA holding tile 0 publishes a finished solve.
+// them (sum_records) and advance the solve's cached state.  Every CTA holding a solve does
+// this with the same inputs in the same order, so all copies of a solve's state stay
+// bit-identical.  The CTA holding tile 0 publishes a finished solve.
 // Returns false if a wait gave up (here or in another CTA).
 __device__ bool reduce_wait(MHead &hd, const MDesc *__restrict__ descs, MState *gstates, MCtl *ctl) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int cs = 0; cs < hd.nsolve; ++cs) {
         if (hd.st[cs].done) continue;  // uniform: only thread 0 writes st, before a barrier
         const MDesc &D = descs[hd.sid[cs]];
         const int ntl = D.ntiles;
         const unsigned tag = hd.st[cs].tick + 1u;
         const TileRec *R = D.recs + (size_t)(blockIdx.x % kRecCopies) * 2 * ntl + (tag & 1u);
-        DD a0{0.0, 0.0}, a1{0.0, 0.0}, a2{0.0, 0.0};
-        int bad = 0;
-        for (int w = threadIdx.x; w < ntl && !bad; w += kBlock) {
-            const TileRec *rp = R + 2 * (size_t)w;
-            if (ld_acquire(&rp->tag) != tag) {
-                const long long t0 = clock64();
-                unsigned spins = 0;
-                while (ld_acquire(&rp->tag) != tag) {
-                    __nanosleep(spins < 16 ? 20 : 100);
-                    if ((++spins & 31u) == 0) {
-                        if (*(volatile int *)&ctl->abort) { bad = 1; break; }
-                        if (clock64() - t0 > kWaitCycles) {
-                            atomicExch(&ctl->abort, 1);
-                            bad = 1;
-                            break;
-                        }
-                    }
-                }
-                if (bad) break;
-            }
-            a0 = dd_add_d(a0, __ldcg(&rp->p0));
-            a1 = dd_add_d(a1, __ldcg(&rp->p1));
-            a2 = dd_add_d(a2, __ldcg(&rp->p2));
-        }
-        if (__syncthreads_or(bad)) return false;
-#pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) {
-            const DD o0 = dd_shfl_down(a0, off), o1 = dd_shfl_down(a1, off), o2 = dd_shfl_down(a2, off);
-            if (lane + off < 32) { a0 = dd_add(a0, o0); a1 = dd_add(a1, o1); a2 = dd_add(a2, o2); }
-        }
-        if (lane == 0) { hd.rdd[warp][0] = a0; hd.rdd[warp][1] = a1; hd.rdd[warp][2] = a2; }
-        __syncthreads();
+        double s0, s1, s2;
+        if (!sum_records(R, ntl, tag, ctl, hd.rsum, hd.acq, hd.nsolve == 1 ? hd.nacq : -1, s0, s1, s2)) return false;
         if (threadIdx.x == 0) {
-            DD s0 = hd.rdd[0][0], s1 = hd.rdd[0][1], s2 = hd.rdd[0][2];
-            for (int w = 1; w < kBlock / 32; ++w) {
-                s0 = dd_add(s0, hd.rdd[w][0]);
-                s1 = dd_add(s1, hd.rdd[w][1]);
-                s2 = dd_add(s2, hd.rdd[w][2]);
-            }
             MState &S = hd.st[cs];
-            advance_state(S, s0.hi + s0.lo, s1.hi + s1.lo, s2.hi + s2.lo);
+            advance_state(S, s0, s1, s2);
             S.tick = tag;
             if (S.done && hd.owner[cs]) {
                 gstates[hd.sid[cs]] = S;
@@ -865,6 +967,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
         }
         hd.nsolve = n;
         hd.cur = -1;
+        // one solve: acquire only the tiles whose columns this CTA's halo reads
+        int na = (n == 1) ? 0 : -1;
+        for (int w = blockIdx.x; w < ntiles && na >= 0; w += gridDim.x) {
+            const MTile T = tiles[w];
+            if (T.solve < 0) continue;
+            const int *nb = descs[T.solve].nbrs + (size_t)T.tile * kNbrStride;
+            const int cnt = nb[0];
+            if (cnt < 0 || na + cnt > kMaxAcq) { na = -1; break; }
+            for (int k = 0; k < cnt; ++k) hd.acq[na++] = nb[1 + k];
+        }
+        hd.nacq = na;
     }
     __syncthreads();
     if (resident && blockIdx.x < ntiles) {  // the CTA's only tile: slot map and FP32 matrix
@@ -934,54 +1047,17 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
 // the tiles need.  A finished solve is published to gstates, flagged and counted down.
 // Returns false if a wait gave up (here or in another CTA).
 __device__ bool lead_duties(MHead &hd, const MDesc *__restrict__ descs, MState *const *gstates, MCtl *ctl) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int cs = 0; cs < hd.nsolve; ++cs) {
         if (hd.st[cs].done) continue;  // uniform: only thread 0 writes st, before a barrier
         const MDesc &D = descs[hd.sid[cs]];
         const int ntl = D.ntiles;
         const unsigned tag = hd.st[cs].tick + 1u;
         const TileRec *R = D.recs + (size_t)(blockIdx.x % kRecCopies) * 2 * ntl + (tag & 1u);
-        DD a0{0.0, 0.0}, a1{0.0, 0.0}, a2{0.0, 0.0};
-        int bad = 0;
-        for (int w = threadIdx.x; w < ntl && !bad; w += kBlock) {
-            const TileRec *rp = R + 2 * (size_t)w;
-            if (ld_acquire(&rp->tag) != tag) {
-                const long long t0 = clock64();
-                unsigned spins = 0;
-                while (ld_acquire(&rp->tag) != tag) {
-                    __nanosleep(spins < 16 ? 20 : 100);
-                    if ((++spins & 31u) == 0) {
-                        if (*(volatile int *)&ctl->abort) { bad = 1; break; }
-                        if (clock64() - t0 > kWaitCycles) {
-                            atomicExch(&ctl->abort, 1);
-                            bad = 1;
-                            break;
-                        }
-                    }
-                }
-                if (bad) break;
-            }
-            a0 = dd_add_d(a0, __ldcg(&rp->p0));
-            a1 = dd_add_d(a1, __ldcg(&rp->p1));
-            a2 = dd_add_d(a2, __ldcg(&rp->p2));
-        }
-        if (__syncthreads_or(bad)) return false;
-#pragma unroll
-        for (int off = 16; off >= 1; off >>= 1) {
-            const DD o0 = dd_shfl_down(a0, off), o1 = dd_shfl_down(a1, off), o2 = dd_shfl_down(a2, off);
-            if (lane + off < 32) { a0 = dd_add(a0, o0); a1 = dd_add(a1, o1); a2 = dd_add(a2, o2); }
-        }
-        if (lane == 0) { hd.rdd[warp][0] = a0; hd.rdd[warp][1] = a1; hd.rdd[warp][2] = a2; }
-        __syncthreads();
+        double s0, s1, s2;
+        if (!sum_records(R, ntl, tag, ctl, hd.rsum, nullptr, -1, s0, s1, s2)) return false;
         if (threadIdx.x == 0) {
-            DD s0 = hd.rdd[0][0], s1 = hd.rdd[0][1], s2 = hd.rdd[0][2];
-            for (int w = 1; w < kBlock / 32; ++w) {
-                s0 = dd_add(s0, hd.rdd[w][0]);
-                s1 = dd_add(s1, hd.rdd[w][1]);
-                s2 = dd_add(s2, hd.rdd[w][2]);
-            }
             MState &S = hd.st[cs];
-            advance_state(S, s0.hi + s0.lo, s1.hi + s1.lo, s2.hi + s2.lo);
+            advance_state(S, s0, s1, s2);
             S.tick = tag;
             if (S.done) *gstates[hd.sid[cs]] = S;
             Bcast *B = D.bc + (size_t)(tag & 1u) * kBcastCopies;
@@ -1187,6 +1263,7 @@ struct MixedBufs {
     float4 *A32 = nullptr;
     float *pre = nullptr, *vec = nullptr;
     int *maps = nullptr;
+    int *nbrs = nullptr;
     TileRec *recs = nullptr;
     Bcast *bc = nullptr;       // [2][kBcastCopies] broadcast lines, then one line holding the done flag
     MState *state = nullptr;
@@ -1199,11 +1276,12 @@ struct MixedBufs {
     long long maps_cap = 0;
     void release() {
         for (void *p : {(void *)A32, (void *)pre, (void *)vec, (void *)recs, (void *)state, (void *)desc,
-                        (void *)tiles, (void *)ctl, (void *)maps, (void *)bc})
+                        (void *)tiles, (void *)ctl, (void *)maps, (void *)nbrs, (void *)bc})
             if (p) cudaFree(p);
         A32 = nullptr;
         pre = vec = nullptr;
         maps = nullptr;
+        nbrs = nullptr;
         ntiles = ntiles_cap = 0;
         maps_cap = 0;
         TY = 0;
