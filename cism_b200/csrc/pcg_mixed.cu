@@ -261,6 +261,7 @@ constexpr int kTX = 32;
 constexpr int kMaxCtaSolves = 64;  // distinct solves whose tiles one CTA may hold in a launch
 constexpr int kMaxTY = 64;
 constexpr int kMaxAcq = 32;        // neighbour tiles a CTA acquires per step (4 tiles x 8)
+constexpr int kTilesCached = 16;   // tile list entries a CTA keeps in shared memory
 constexpr int kCh2 = 4;            // stencil items per load batch
 constexpr int kChR = 4;            // FP64 residual items per load batch
 
@@ -275,6 +276,8 @@ struct MHead {
     double rsum[8][3];
     int nacq;                  // >= 0: the CTA reads the halo of acq[0..nacq) only; -1: fence
     int acq[kMaxAcq];
+    int ntl;                   // static launches: tile list entries of this CTA
+    MTile tl[kTilesCached];    // the first kTilesCached of them
 };
 
 // Dynamic shared memory: head | map[NS] | z[2][KP][NS] | rt[2][NZM][NT]
@@ -978,6 +981,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
             for (int k = 0; k < cnt; ++k) hd.acq[na++] = nb[1 + k];
         }
         hd.nacq = na;
+        int nt = 0;
+        for (int w = blockIdx.x; w < ntiles; w += gridDim.x, ++nt)
+            if (nt < kTilesCached) hd.tl[nt] = tiles[w];
+        hd.ntl = nt;
     }
     __syncthreads();
     if (resident && blockIdx.x < ntiles) {  // the CTA's only tile: slot map and FP32 matrix
@@ -1015,8 +1022,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
             finished = true;
             break;
         }
-        for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
-            const MTile T = tiles[w];
+        for (int u = 0; u < hd.ntl; ++u) {
+            const MTile T = (u < kTilesCached) ? hd.tl[u] : tiles[blockIdx.x + (size_t)u * gridDim.x];
+            if (T.solve < 0) continue;  // padding of a blocked tile order
             int cs = 0;
             while (cs < hd.nsolve && hd.sid[cs] != T.solve) ++cs;
             if (cs >= hd.nsolve || hd.st[cs].done) continue;
