@@ -492,6 +492,7 @@ static MDesc mixed_desc(const Solver &sv, int precond, int TY) {  // TY: the sol
     D.dflag = reinterpret_cast<int *>(m.bc + 2 * kBcastCopies);
     D.maps = m.maps;
     D.nbrs = m.nbrs;
+    D.stream = (size_t)sv.NC * (size_t)nvec * sizeof(float4) > kStreamBytes ? 1 : 0;
     return D;
 }
 

@@ -53,6 +53,7 @@ struct __align__(64) TileRec {
     unsigned long long pad[2];
 };
 constexpr int kRecCopies = 4;
+constexpr size_t kStreamBytes = 32u << 20;  // FP32 matrix size above which L2 cannot keep a solve's matrix
 constexpr int kNbrMax = 8;     // tiles whose columns one tile's halo reads (else: fence)
 constexpr int kNbrStride = kNbrMax + 1;  // [count or -1, tiles...] per tile
 
@@ -86,6 +87,7 @@ struct MDesc {
     int *dflag;          // set once the solve is done (dynamic launches)
     const int *maps;     // [ntiles][(kTX+2)*(TY+2)] slot maps (k_slot_maps)
     const int *nbrs;     // [ntiles][kNbrStride] tiles owning the tile's live halo columns (k_tile_nbrs)
+    int stream;          // matrix loads evict-first (the FP32 matrix exceeds kStreamBytes)
 };
 
 struct MState {
@@ -298,6 +300,28 @@ struct MLayout {
     }
 };
 
+// Matrix loads (read-only for the launch) carry an L2 policy: evict-first for a solve whose
+// matrix streams through L2 every step (larger than L2 can keep), so that it does not push
+// out the vectors the next pass reads; evict-normal for one L2 can keep between steps.
+__device__ __forceinline__ unsigned long long l2_matrix_policy(bool stream) {
+    unsigned long long pol;
+    if (stream) asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    else asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ float4 ld_stream(const float4 *p, unsigned long long pol) {
+    float4 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+        : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ld_stream(const double *p, unsigned long long pol) {
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 // Loads of data that other CTAs wrote earlier in the same launch go through L2
 // (ld.global.cg): L1 is not coherent across SMs.
 __device__ __forceinline__ float ldf(const float *p) { return __ldcg(p); }
@@ -443,6 +467,7 @@ __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, i
     float *__restrict__ rv32 = D.r[rpar] + plane;
     const int NS = (kTX + 2) * (TY + 2);
     const int nitems = NT * nz;
+    const unsigned long long pol = l2_matrix_policy(D.stream != 0);
 #pragma unroll 1
     for (int base = threadIdx.x; base < nitems; base += kChR * kBlock) {
         double yu[kChR], yv[kChR], bu[kChR], bv[kChR];
@@ -480,10 +505,10 @@ __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, i
                                 x1 = fma(alpha64, (double)sdn[(k + kA) * NS + sn], x1);
                                 x2 = fma(alpha64, (double)sdn[(nz + k + kA) * NS + sn], x2);
                             }
-                            yu[u] = fma(Auu[a], x1, yu[u]);
-                            yu[u] = fma(Auv[a], x2, yu[u]);
-                            yv[u] = fma(Avu[a], x1, yv[u]);
-                            yv[u] = fma(Avv[a], x2, yv[u]);
+                            yu[u] = fma(ld_stream(Auu + a, pol), x1, yu[u]);
+                            yu[u] = fma(ld_stream(Auv + a, pol), x2, yu[u]);
+                            yv[u] = fma(ld_stream(Avu + a, pol), x1, yv[u]);
+                            yv[u] = fma(ld_stream(Avv + a, pol), x2, yv[u]);
                         }
                     }
                 }
@@ -737,6 +762,7 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
             float *__restrict__ zu_out = D.z;
             float *__restrict__ zv_out = D.z + plane;
             const float *szu = sz, *szv = sz + KP * NS;
+            const unsigned long long pol = l2_matrix_policy(D.stream != 0);
 #pragma unroll 1
             for (int base = t; base < NN; base += kCh2 * kBlock) {
                 float yu[kCh2], yv[kCh2], zu[kCh2], zv[kCh2];
@@ -780,7 +806,7 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                                         const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
                                         const int zi = (k + OFF + kA) * NS + s + iA + (kTX + 2) * jA;
                                         const float z1 = szu[zi], z2 = szv[zi];
-                                        const float4 a = __ldg(A4 + (size_t)c * plane + e);
+                                        const float4 a = ld_stream(A4 + (size_t)c * plane + e, pol);
                                         yu[u] = fmaf(a.x, z1, yu[u]);
                                         yu[u] = fmaf(a.y, z2, yu[u]);
                                         yv[u] = fmaf(a.z, z1, yv[u]);
