@@ -42,6 +42,7 @@ HO_PRECOND_TRIDIAG_GLOBAL = 4
 STATUS_NAMES = {
     0: "CISMGPU_OK", 1: "CISMGPU_EBREAKDOWN_ETA1", 2: "CISMGPU_EBREAKDOWN_ALPHA", 3: "CISMGPU_EUNSUPPORTED",
     4: "CISMGPU_EINVAL", 5: "CISMGPU_ECUDA", 6: "CISMGPU_ETIMEOUT", 7: "CISMGPU_ENOMEM", 8: "CISMGPU_ENODEV",
+    9: "CISMGPU_EDIVZERO",
 }
 
 _HERE = os.path.dirname(os.path.abspath(__file__))

@@ -110,6 +110,9 @@ struct Solver {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     DevBuf A, raw, vec, act, partials, state, map;
+    DevBuf tri;       // tridiagonal preconditioner planes (TriPlane), on first use
+    int32_t hindx[27] = {};   // host copy of the uploaded indxA map (27 or 9 entries)
+    int32_t hindx2[9] = {};   // indxA_2d: the uploaded map in 2D; in 3D the caller's, else standard
     MixedBufs mixed;  // FP32 copies, created on first mixed solve
     int *h_done = nullptr;          // pinned, 2 slots for look-ahead polling
     SolveState *h_state = nullptr;  // pinned
@@ -127,6 +130,7 @@ struct Solver {
 
     void destroy() {
         A.release(); raw.release(); vec.release(); act.release(); partials.release(); state.release(); map.release();
+        tri.release();
         mixed.release();
         if (h_done) cudaFreeHost(h_done);
         if (h_state) cudaFreeHost(h_state);
@@ -180,6 +184,8 @@ struct Solver {
         g = geom;
         is3d = three_d;
         NC = is3d ? 27 : 9;
+        for (int c = 0; c < NC; ++c) hindx[c] = indx[c];
+        for (int c = 0; c < 9; ++c) hindx2[c] = is3d ? c + 1 : indx[c];
         nvec = (long long)g.nz * g.NQ;
         mixed.stale = true;  // new matrix: FP32 copy and factors must be rebuilt
         n_active_owned = 0;
@@ -318,12 +324,92 @@ struct Solver {
             return fail(CISMGPU_EBREAKDOWN_ETA1, "PCG solver has failed, eta1 = NaN");
         if (h_state->status == CISMGPU_EBREAKDOWN_ALPHA)
             return fail(CISMGPU_EBREAKDOWN_ALPHA, "PCG solver has failed, alpha = NaN");
+        if (h_state->status == CISMGPU_EDIVZERO)
+            return fail(CISMGPU_EDIVZERO, "divzero in the tridiagonal preconditioner setup");
         return CISMGPU_OK;
     }
 
     double mv_bytes(int extra_vec_streams) const {
         // per active owned node: 4 blocks x NC coefficients + vector streams of 2 components
         return (double)n_active_owned * g.nz * (4.0 * NC * 8.0 + 2.0 * 8.0 * (2 + extra_vec_streams));
+    }
+
+    // Device planes of the line-system couplings for precond 3/4 (TriMap): the raw index m that
+    // indxA_2d gives each coupling, and in 3D the planes holding raw m, m+9, m+18.
+    int tri_map(TriMap &tm) const {
+        static const int geo[2][3] = {{3, 4, 5}, {1, 4, 7}};  // (-1,0),(0,0),(1,0) / (0,-1),(0,0),(0,1)
+        for (int comp = 0; comp < 2; ++comp)
+            for (int e = 0; e < 3; ++e) {
+                const int m = hindx2[geo[comp][e]];
+                if (m < 1 || m > 9) return fail(CISMGPU_EINVAL, "indxA_2d entry outside 1..9");
+                tm.m[comp][e] = m;
+                for (int t = 0; t < 3; ++t) tm.c[comp][e][t] = 0;
+                if (!is3d) {
+                    tm.c[comp][e][0] = geo[comp][e];  // the planes were permuted by this same map
+                } else {
+                    for (int t = 0; t < 3; ++t) {
+                        int c = 0;
+                        while (c < 27 && hindx[c] != m + 9 * t) ++c;
+                        if (c == 27) return fail(CISMGPU_EINVAL, "indxA_3d does not name a coefficient the "
+                                                                 "tridiagonal preconditioner sums");
+                        tm.c[comp][e][t] = c;
+                    }
+                }
+            }
+        return CISMGPU_OK;
+    }
+
+    // Setup of precond 3/4 (after k_init_state: a zero pivot ends the solve with EDIVZERO).
+    int tri_setup(int precond) {
+        CU(tri.ensure((size_t)NTRI * g.NQ * sizeof(double)));
+        TriMap tm;
+        TRY(tri_map(tm));
+        const int global = precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL;
+        if (is3d)
+            k_tri_coef<27><<<nblocks(g.NQ), kBlock, 0, stream>>>(g, A.as<double>(), act.as<int32_t>(), tm, global,
+                                                                tri.as<double>());
+        else
+            k_tri_coef<9><<<nblocks(g.NQ), kBlock, 0, stream>>>(g, A.as<double>(), act.as<int32_t>(), tm, global,
+                                                               tri.as<double>());
+        k_tri_factor<<<(tri_lines(g) + kBlock - 1) / kBlock, kBlock, 0, stream>>>(g, global, tri.as<double>(),
+                                                                                  state.as<SolveState>());
+        CU(cudaGetLastError());
+        return CISMGPU_OK;
+    }
+
+    // z = PC(r) (+ the statement MODE fuses): precond 3/4 first run their line solves
+    // (3D: of the vertically summed residual) and halo update, then k_precond finishes.
+    template <int NCC, int MODE>
+    int apply_precond(int precond, const Ptrs &p, RedCtx rc, double *du, double *dv) {
+        cudaStream_t s = stream;
+        SolveState *st = state.as<SolveState>();
+        const double *zs = nullptr;
+        if (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL) {
+            const int global = precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL;
+            double *T = tri.as<double>();
+            const long long NQ = g.NQ;
+            const unsigned lb = (tri_lines(g) + kBlock - 1) / kBlock;
+            const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
+            if (NCC == 27) {
+                k_tri_vsum<<<nblocks(NQ), kBlock, 0, s>>>(g, p.ru, p.rv, T, st);
+                CU(cudaMemsetAsync(T + TZS_U * NQ, 0, 2 * NQ * sizeof(double), s));
+                k_tri_lines<<<lb, kBlock, 0, s>>>(g, global, T + TRS_U * NQ, T + TRS_V * NQ, T + TZS_U * NQ,
+                                                  T + TZS_V * NQ, T, st);
+                Geom g1 = g;
+                g1.nz = 1;
+                k_halo<<<hb, kBlock, 0, s>>>(g1, T + TZS_U * NQ, T + TZS_V * NQ, st);
+                zs = T + TZS_U * NQ;
+            } else {
+                CU(cudaMemsetAsync(p.zu, 0, NQ * sizeof(double), s));
+                CU(cudaMemsetAsync(p.zv, 0, NQ * sizeof(double), s));
+                k_tri_lines<<<lb, kBlock, 0, s>>>(g, global, p.ru, p.rv, p.zu, p.zv, T, st);
+                k_halo<<<hb, kBlock, 0, s>>>(g, p.zu, p.zv, st);
+            }
+        }
+        k_precond<MODE><<<nblocks(g.NQ), kBlock, 0, s>>>(g, precond, A.as<double>(), NCC, act.as<int32_t>(), p.ru,
+                                                         p.rv, p.zu, p.zv, du, dv, rc, zs);
+        CU(cudaGetLastError());
+        return CISMGPU_OK;
     }
 
     template <int NCC> int run_standard(int precond, int ncheck, double tol, int maxiters);
@@ -348,6 +434,8 @@ int Solver::run_standard(int precond, int ncheck, double tol, int maxiters) {
     prof_bytes = mv_bytes(0);
 
     k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
+    if (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL)
+        TRY(tri_setup(precond));  // pcg_precond_init (:1083-1160 / :263-376)
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
     k_mv<NCC, MV_PLAIN><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
                                               nullptr, rc(EPI_NONE, 0));
@@ -355,8 +443,7 @@ int Solver::run_standard(int precond, int ncheck, double tol, int maxiters) {
     CU(cudaGetLastError());
     Poller poll(*this);
     for (int iter = 1; iter <= maxiters; ++iter) {
-        k_precond<PRE_STD><<<nb, kBlock, 0, s>>>(gg, precond, Ad, NCC, ac, p.ru, p.rv, p.zu, p.zv, nullptr, nullptr,
-                                                 rc(EPI_STD_ETA1, iter));
+        TRY((apply_precond<NCC, PRE_STD>(precond, p, rc(EPI_STD_ETA1, iter), nullptr, nullptr)));
         k_vec<OP_STD_D><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, iter));
         k_halo<<<hb, kBlock, 0, s>>>(gg, p.du, p.dv, st);
         TRY(timed([&] {
@@ -393,8 +480,12 @@ int Solver::run_chrongear(int precond, int ncheck, double tol, int maxiters) {
     auto rc = [&](int epi, int iter) { return RedCtx{part, st, epi, iter}; };
     const Geom gg = g;
     prof_bytes = mv_bytes(1);  // the fused (r,z) dot also reads r
+    // 2D with a tridiagonal preconditioner: at most 100 iterations (:1704-1732); 3D keeps maxiters
+    const bool tri = precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL;
+    if (tri && NCC == 9) maxiters = 100;
 
     k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
+    if (tri) TRY(tri_setup(precond));  // pcg_precond_init (:2916-3040 / :1747-1880)
     // r = d = z = q = Az = 0 (:3048-3061)
     CU(cudaMemsetAsync(p.ru, 0, (size_t)(VAZ_V - VR_U + 1) * nvec * sizeof(double), s));
     k_vec<OP_DOT_BB><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_L2RHS, 0));
@@ -404,8 +495,7 @@ int Solver::run_chrongear(int precond, int ncheck, double tol, int maxiters) {
                                               nullptr, rc(EPI_NONE, 1));
     k_vec<OP_CG_INIT><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, 1));
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
-    k_precond<PRE_CG_FIRST><<<nb, kBlock, 0, s>>>(gg, precond, Ad, NCC, ac, p.ru, p.rv, p.zu, p.zv, p.du, p.dv,
-                                                  rc(EPI_CG_RHO0, 1));
+    TRY((apply_precond<NCC, PRE_CG_FIRST>(precond, p, rc(EPI_CG_RHO0, 1), p.du, p.dv)));
     k_mv<NCC, MV_DQ><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr,
                                            rc(EPI_CG_FIRST, 1));
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.qu, p.qv, st);
@@ -413,8 +503,7 @@ int Solver::run_chrongear(int precond, int ncheck, double tol, int maxiters) {
     CU(cudaGetLastError());
     Poller poll(*this);
     for (int iter = 2; iter <= maxiters; ++iter) {
-        k_precond<PRE_ONLY><<<nb, kBlock, 0, s>>>(gg, precond, Ad, NCC, ac, p.ru, p.rv, p.zu, p.zv, nullptr, nullptr,
-                                                  rc(EPI_NONE, iter));
+        TRY((apply_precond<NCC, PRE_ONLY>(precond, p, rc(EPI_NONE, iter), nullptr, nullptr)));
         TRY(timed([&] {
             k_mv<NCC, MV_CG_AZ><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.zu, p.zv, p.Azu, p.Azv, nullptr, nullptr, p.ru,
                                                       p.rv, rc(EPI_CG_ITER, iter));
@@ -861,8 +950,7 @@ static int validate(int nx, int ny, int nz, const cismgpu_par_t *par, const void
 static int validate_solve_args(int precond, int ncheck, int maxiters) {
     if (ncheck < 1) return fail(CISMGPU_EINVAL, "linear_solve_ncheck must be >= 1");
     if (maxiters < 0) return fail(CISMGPU_EINVAL, "maxiters must be >= 0");
-    if (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL)
-        return fail(CISMGPU_EUNSUPPORTED, "tridiagonal preconditioners (3, 4) are not implemented");
+    (void)precond;  // every value is accepted: 0-4 have branches, others take none (as the reference)
     return CISMGPU_OK;
 }
 
@@ -909,6 +997,8 @@ static int oneshot_solve(int alg, bool is3d, int nx, int ny, int nz, const cismg
     TRY(sv.init(nullptr));
     const double *blocks[4] = {Auu, Auv, Avu, Avv};
     TRY(sv.upload(make_geom(nx, ny, is3d ? nz : 1, par), is3d, indx, act, blocks, bu, bv, xu, xv));
+    if (is3d && indx2)
+        for (int c = 0; c < 9; ++c) sv.hindx2[c] = indx2[c];
     TRY(sv.begin_solve());
     TRY(run_algorithm(sv, g_oneshot_alg >= 0 ? g_oneshot_alg : alg, precond, ncheck, tol, maxiters));
     int rc = sv.finish_solve(err, niters);

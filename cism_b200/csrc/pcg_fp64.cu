@@ -327,14 +327,16 @@ enum PreMode { PRE_ONLY = 0, PRE_STD, PRE_CG_FIRST };
 // z = PC(r) over the whole array, then optionally:
 //   PRE_STD      : S0 = (r,z)                      [:1320-1326]
 //   PRE_CG_FIRST : S0 = (r,z) kept for the first-pass epilogue; d = z   [:3215-3223]
-// kind: 0 none (z = r), 1 diag, 2 sia (3D only), anything else: z unchanged.
+// kind: 0 none (z = r), 1 diag, 2 sia (3D only), 3/4 tridiagonal: in 2D z was written by
+// k_tri_lines and the halo update, in 3D the SIA columns plus the summed line solution zs
+// ([2][NQ], u then v) on every level; anything else: z unchanged.
 template <int MODE>
 __global__ void __launch_bounds__(kBlock) k_precond(Geom g, int kind, const double *__restrict__ A,
                                                     int NC, const int32_t *__restrict__ act,
                                                     const double *__restrict__ ru, const double *__restrict__ rv,
                                                     double *__restrict__ zu, double *__restrict__ zv,
                                                     double *__restrict__ du, double *__restrict__ dv,
-                                                    RedCtx rc) {
+                                                    RedCtx rc, const double *__restrict__ zs = nullptr) {
     if (rc.st->done) return;
     const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
     DD s0{0.0, 0.0};
@@ -362,6 +364,18 @@ __global__ void __launch_bounds__(kBlock) k_precond(Geom g, int kind, const doub
                 sia_column(g, Auu + 4 * plane, Auu + 13 * plane, Auu + 22 * plane, ru, zu, q);
                 sia_column(g, Avv + 4 * plane, Avv + 13 * plane, Avv + 22 * plane, rv, zv, q);
             }
+        } else if ((kind == CISMGPU_PRECOND_TRIDIAG_LOCAL || kind == CISMGPU_PRECOND_TRIDIAG_GLOBAL) && NC == 27) {
+            // tridiag_solver_{local,global}_3d :4617-4655 / :4876-4911: SIA columns, then + zs
+            if (act[q] != 0) {
+                sia_column(g, Auu + 4 * plane, Auu + 13 * plane, Auu + 22 * plane, ru, zu, q);
+                sia_column(g, Avv + 4 * plane, Avv + 13 * plane, Avv + 22 * plane, rv, zv, q);
+            }
+            const double su = zs[q], sv = zs[g.NQ + q];
+            for (int k = 0; k < g.nz; ++k) {
+                const long long e = (long long)k * g.NQ + q;
+                zu[e] = __dadd_rn(zu[e], su);
+                zv[e] = __dadd_rn(zv[e], sv);
+            }
         }
         if (MODE == PRE_STD || MODE == PRE_CG_FIRST) {
             const bool own = owned(g, i, j);
@@ -374,6 +388,181 @@ __global__ void __launch_bounds__(kBlock) k_precond(Geom g, int kind, const doub
         }
     }
     if (MODE == PRE_STD || MODE == PRE_CG_FIRST) reduce_and_finish<1>(rc, s0, s0);
+}
+
+// ---------------------------------------------------------------------------
+// tridiagonal line preconditioners (precond 3 local, 4 global) on one task
+// ---------------------------------------------------------------------------
+// On one task the global form's solution is its particular solution (tasks_rc = 1,
+// tridiag_solver_global_2d :5495-5497), which is the local form's arithmetic on the owned
+// block; the forms differ in the global setup's extra zero-pivot check (:4472-4488), in
+// 3D inactive columns (local zeroes all nine summed couplings, :3823-3833; global only sets
+// the centre, :4025-4032) and in the local back substitution continuing below the owned
+// range (:4999-5001, gamma = omega = 0 there).  Lines: u along rows j (i varies), v along
+// columns i (j varies), one thread per line.  Work planes of NQ doubles:
+enum TriPlane {
+    TU_SUB = 0, TU_DG, TU_SP, TU_ADR, TU_OM, TU_DEN,  // u lines: sub, diag, super, 1/diag, omega, 1/denom
+    TV_SUB, TV_DG, TV_SP, TV_ADR, TV_OM, TV_DEN,      // v lines
+    TRS_U, TRS_V,                                     // 3D: vertical sums of r
+    TZS_U, TZS_V,                                     // 3D: line solution of the summed problem
+    NTRI
+};
+
+// Coefficient planes of the line systems: [u/v][sub, diag, super] -> the device planes of the
+// caller's raw indices m (2D: plane c[..][0]) or m, m+9, m+18 (3D vertical sums), with m the
+// raw index (1..9) indxA_2d gives the coupling.
+struct TriMap {
+    int c[2][3][3];
+    int m[2][3];
+};
+
+// setup_preconditioner_tridiag_{local,global}_{2d,3d}: the line coefficients, zero-diagonal
+// fix (:4306-4313) and 1/diag (:4347), omega = 1/denom = 0 until k_tri_factor.  3D: sums
+// over levels of the three vertical offsets, ((s + A(m)) + A(m+9)) + A(m+18) (:3813-3819).
+template <int NC>
+__global__ void k_tri_coef(Geom g, const double *__restrict__ A, const int32_t *__restrict__ act, TriMap tm,
+                           int global, double *__restrict__ T) {
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (q >= g.NQ) return;
+    const long long plane = (long long)g.nz * g.NQ;
+    for (int comp = 0; comp < 2; ++comp) {
+        const double *B = A + (comp ? 3LL : 0LL) * NC * plane;  // Auu or Avv
+        double v[3];
+        for (int e = 0; e < 3; ++e) {
+            if (NC == 9) {
+                v[e] = B[(long long)tm.c[comp][e][0] * g.NQ + q];
+            } else {
+                double sum = 0.0;
+                for (int k = 0; k < g.nz; ++k) {
+                    const long long o = (long long)k * g.NQ + q;
+                    sum = __dadd_rn(__dadd_rn(__dadd_rn(sum, B[tm.c[comp][e][0] * plane + o]),
+                                              B[tm.c[comp][e][1] * plane + o]),
+                                    B[tm.c[comp][e][2] * plane + o]);
+                }
+                if (act[q] == 0) {
+                    if (tm.m[comp][e] == 5) sum = 1.0;
+                    else if (!global) sum = 0.0;
+                }
+                v[e] = sum;
+            }
+        }
+        if (v[1] == 0.0) { v[1] = 1.0; v[0] = 0.0; v[2] = 0.0; }
+        double *P = T + (comp ? TV_SUB : TU_SUB) * g.NQ;
+        P[0 * g.NQ + q] = v[0];
+        P[1 * g.NQ + q] = v[1];
+        P[2 * g.NQ + q] = v[2];
+        P[3 * g.NQ + q] = __ddiv_rn(1.0, v[1]);
+        P[4 * g.NQ + q] = 0.0;
+        P[5 * g.NQ + q] = 0.0;
+    }
+}
+
+__device__ __forceinline__ void tri_line(const Geom &g, int t, bool &along_i, int &l, int &s0, int &s1) {
+    const int nu = g.jhi - g.jlo + 1;
+    along_i = t < nu;
+    l = along_i ? g.jlo + t : g.ilo + (t - nu);
+    s0 = along_i ? g.ilo : g.jlo;
+    s1 = along_i ? g.ihi : g.jhi;
+}
+__device__ __forceinline__ long long tri_at(const Geom &g, bool along_i, int l, int s) {
+    return along_i ? (long long)l * g.NX + s : (long long)s * g.NX + l;
+}
+__host__ __device__ inline int tri_lines(const Geom &g) { return (g.jhi - g.jlo + 1) + (g.ihi - g.ilo + 1); }
+
+// Forward elimination per owned line (:4324-4342 / :4361-4379; global :4441-4452), and for the
+// global form the reverse recurrence it checks for zero pivots (:4464-4488).  A zero pivot
+// is GM_FATAL in the reference: the solve ends with CISMGPU_EDIVZERO before it starts.
+__global__ void k_tri_factor(Geom g, int global, double *__restrict__ T, SolveState *st) {
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t >= tri_lines(g)) return;
+    bool along_i;
+    int l, s0, s1;
+    tri_line(g, t, along_i, l, s0, s1);
+    double *P = T + (along_i ? TU_SUB : TV_SUB) * g.NQ;
+    const double *sub = P, *dg = P + g.NQ, *sp = P + 2 * g.NQ;
+    double *om = P + 4 * g.NQ, *den = P + 5 * g.NQ;
+    long long e = tri_at(g, along_i, l, s0);
+    double omp = __ddiv_rn(sp[e], dg[e]);
+    om[e] = omp;
+    for (int s = s0 + 1; s <= s1; ++s) {
+        e = tri_at(g, along_i, l, s);
+        const double d = __dsub_rn(dg[e], __dmul_rn(sub[e], omp));
+        if (d == 0.0) {
+            st->status = CISMGPU_EDIVZERO;
+            st->done = 1;
+            return;
+        }
+        const double dn = __ddiv_rn(1.0, d);
+        den[e] = dn;
+        omp = __dmul_rn(sp[e], dn);
+        om[e] = omp;
+    }
+    if (global) {
+        e = tri_at(g, along_i, l, s1);
+        double o = __ddiv_rn(sub[e], dg[e]);
+        for (int s = s1 - 1; s >= s0; --s) {
+            e = tri_at(g, along_i, l, s);
+            const double d = __dsub_rn(dg[e], __dmul_rn(sp[e], o));
+            if (d == 0.0) {
+                st->status = CISMGPU_EDIVZERO;
+                st->done = 1;
+                return;
+            }
+            o = __ddiv_rn(sub[e], d);
+        }
+    }
+}
+
+// sum(ru(:,i,j)) over levels, in level order (tridiag_solver_local_3d :4585-4590)
+__global__ void k_tri_vsum(Geom g, const double *__restrict__ ru, const double *__restrict__ rv,
+                           double *__restrict__ T, const SolveState *st) {
+    if (st->done) return;
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (q >= g.NQ) return;
+    double a = 0.0, b = 0.0;
+    for (int k = 0; k < g.nz; ++k) {
+        a = __dadd_rn(a, ru[(long long)k * g.NQ + q]);
+        b = __dadd_rn(b, rv[(long long)k * g.NQ + q]);
+    }
+    T[TRS_U * g.NQ + q] = a;
+    T[TRS_V * g.NQ + q] = b;
+}
+
+// Line solves of tridiag_solver_local_2d (:4985-5013 u, :5041-5069 v) from planes bu, bv into
+// xu, xv, which hold zeros on entry: gamma forward (stored in x), then back substitution.
+__global__ void k_tri_lines(Geom g, int global, const double *__restrict__ bu, const double *__restrict__ bv,
+                            double *__restrict__ xu, double *__restrict__ xv, const double *__restrict__ T,
+                            const SolveState *st) {
+    if (st->done) return;
+    const int t = blockIdx.x * kBlock + threadIdx.x;
+    if (t >= tri_lines(g)) return;
+    bool along_i;
+    int l, s0, s1;
+    tri_line(g, t, along_i, l, s0, s1);
+    const double *P = T + (along_i ? TU_SUB : TV_SUB) * g.NQ;
+    const double *sub = P, *adr = P + 3 * g.NQ, *om = P + 4 * g.NQ, *den = P + 5 * g.NQ;
+    const double *b = along_i ? bu : bv;
+    double *x = along_i ? xu : xv;
+    long long e = tri_at(g, along_i, l, s0);
+    double gp = __dmul_rn(b[e], adr[e]);
+    x[e] = gp;
+    for (int s = s0 + 1; s <= s1; ++s) {
+        e = tri_at(g, along_i, l, s);
+        gp = __dmul_rn(__dsub_rn(b[e], __dmul_rn(sub[e], gp)), den[e]);
+        x[e] = gp;
+    }
+    double xn = gp;
+    for (int s = s1 - 1; s >= s0; --s) {
+        e = tri_at(g, along_i, l, s);
+        xn = __dsub_rn(x[e], __dmul_rn(om[e], xn));
+        x[e] = xn;
+    }
+    if (!global)
+        for (int s = s0 - 1; s >= 0; --s) {
+            e = tri_at(g, along_i, l, s);
+            xn = __dsub_rn(0.0, __dmul_rn(om[e], xn));
+            x[e] = xn;
+        }
 }
 
 // ---------------------------------------------------------------------------

@@ -48,12 +48,14 @@ extern "C" {
 #define CISMGPU_OK                0
 #define CISMGPU_EBREAKDOWN_ETA1   1  /* eta1 = (r,z) is NaN   (reference :637, :1331)            */
 #define CISMGPU_EBREAKDOWN_ALPHA  2  /* alpha is NaN           (reference :697, :1391, :2196, :2467, :3263, :3434) */
-#define CISMGPU_EUNSUPPORTED      3  /* tridiagonal precond (3,4) or tasks_row*tasks_col > 1     */
+#define CISMGPU_EUNSUPPORTED      3  /* tasks_row*tasks_col > 1; mixed solver with precond 3,4   */
 #define CISMGPU_EINVAL            4  /* bad sizes, null pointers, inconsistent owned bounds     */
 #define CISMGPU_ECUDA             5  /* CUDA runtime error (message via cismgpu_last_error)     */
 #define CISMGPU_ETIMEOUT          6  /* a bounded device wait gave up                           */
 #define CISMGPU_ENOMEM            7  /* device allocation failed or HBM budget exceeded         */
 #define CISMGPU_ENODEV            8  /* no CUDA device / not an sm_100 device                   */
+#define CISMGPU_EDIVZERO          9  /* tridiagonal precond setup met a zero pivot (reference
+                                        GM_FATAL :4339, :4380, :4475, :4492); x is unchanged      */
 
 /* preconditioner options, libglide/glide_types.F90:342-346 */
 #define CISMGPU_PRECOND_NONE            0
@@ -189,7 +191,9 @@ typedef struct cismgpu_solver cismgpu_solver_t;
 #define CISMGPU_ALG_MIXED_CHRONGEAR 2  /* FP32 inner Chronopoulos-Gear + FP64 iterative refinement  */
 
 /* dims = 3 (27-point blocks, indxA = indxA_3d) or 2 (9-point blocks, indxA = indxA_2d, nz = 1).
- * Array arguments as for the solver calls above; x0 may be NULL (zero initial guess). */
+ * Array arguments as for the solver calls above; x0 may be NULL (zero initial guess).
+ * 3D handles use the standard indxA_2d (m = 1 + (iA+1) + 3*(jA+1)) where the tridiagonal
+ * preconditioners (3, 4) read the vertically summed couplings. */
 int cismgpu_solver_create(cismgpu_solver_t **out, int dims, int nx, int ny, int nz,
                           const cismgpu_par_t *par, const int32_t *indxA, const int32_t *active_vertex,
                           const double *Auu, const double *Auv, const double *Avu, const double *Avv,

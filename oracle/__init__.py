@@ -57,6 +57,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_global_sum.argtypes = [i, i, i, P(_Par), d, d, i]
         L.oracle_global_sum.restype = dbl
         L.oracle_easy_sia.argtypes = [i, i, i, d, d, d, d]
+        L.oracle_precond_apply.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, i, d, d, d, d]
         L.oracle_exact_sum.argtypes = [d, ctypes.c_long]
         L.oracle_exact_sum.restype = dbl
         _lib = L
@@ -134,6 +135,21 @@ def easy_sia(nx, ny, nz, active, M, b, x):
     lib().oracle_easy_sia(nx, ny, nz, _p(active), _p(np.ascontiguousarray(M)), _p(np.ascontiguousarray(b)),
                           _p(out))
     return out
+
+
+def precond_apply(prob, precond: int, ru, rv, zu0=None, zv0=None):
+    """z = PC(r) for one preconditioner of prob's matrix (setup + one apply); z starts from
+    zu0/zv0 (default zero), which the SIA column solve keeps on inactive columns.
+    Returns (status, zu, zv)."""
+    is3d = prob.kind == "3d"
+    zu = np.array(np.zeros_like(ru) if zu0 is None else zu0, dtype=np.float64, copy=True)
+    zv = np.array(np.zeros_like(rv) if zv0 is None else zv0, dtype=np.float64, copy=True)
+    par = _par(prob.par)
+    st = lib().oracle_precond_apply(int(is3d), prob.nx, prob.ny, prob.nz if is3d else 1, ctypes.byref(par),
+                                    _p(indx2()), _p(indx3()), _p(prob.active_vertex), _p(prob.Auu), _p(prob.Avv),
+                                    precond, _p(np.ascontiguousarray(ru)), _p(np.ascontiguousarray(rv)), _p(zu),
+                                    _p(zv))
+    return st, zu, zv
 
 
 def exact_sum(a) -> float:

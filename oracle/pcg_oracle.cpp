@@ -20,6 +20,14 @@
 //     setup_preconditioner_diag_3d    :3598-3643
 //     setup_preconditioner_sia_3d     :3647-3733
 //     setup_preconditioner_diag_2d    :4199-4243
+//     setup_preconditioner_tridiag_local_3d   :3737-3926
+//     setup_preconditioner_tridiag_global_3d  :3930-4195
+//     setup_preconditioner_tridiag_local_2d   :4247-4392
+//     setup_preconditioner_tridiag_global_2d  :4396-4520  (one task per row and column)
+//     tridiag_solver_local_3d         :4524-4658
+//     tridiag_solver_global_3d        :4662-4913  (one task: the particular solution)
+//     tridiag_solver_local_2d         :4917-5100
+//     tridiag_solver_global_2d        :5104-5524  (tasks_rc = 1 branch, :5495-5497)
 //     matvec_multiply_structured_3d   :5528-5652
 //     matvec_multiply_structured_2d   :5656-5773
 //     easy_sia_solver                 :5777-5866
@@ -431,16 +439,105 @@ void easy_sia_solver(const Ctx &c, const Vec &M, const Vec &b, Vec &x) {
         }
 }
 
-// Preconditioner state for one solve.
-struct Precond {
-    int kind;      // 0 none, 1 diag, 2 sia, other: no branch taken
-    Vec Adu, Adv;  // diagonal entries (diag)
-    Vec Muu, Mvv;  // (-1:1, nz, NX, NY) (sia)
+// Tridiagonal line factors on an (NX, NY) plane, index v2(i,j): the u system runs along
+// rows (i), the v system along columns (j).  adr = 1/diag after the zero-diagonal fix.
+struct TriLines {
+    Vec sub, dg, sp, adr, omega, denom;
 };
 
-void setup_precond(const Ctx &c, bool is3d, int precond, const double *Auu, const double *Avv, Precond &P) {
+// Preconditioner state for one solve.
+struct Precond {
+    int kind;      // 0 none, 1 diag, 2 sia, 3/4 tridiag local/global, other: no branch taken
+    Vec Adu, Adv;  // diagonal entries (diag)
+    Vec Muu, Mvv;  // (-1:1, nz, NX, NY) (sia; also the vertical part of 3D tridiag)
+    TriLines tu, tv;
+};
+
+// Line factorization over the owned range (setup_preconditioner_tridiag_local_2d
+// :4324-4342 / :4361-4379; the global form :4441-4470 computes the same omega and denom on
+// the owned block and, with one task, also runs the reverse recurrence only for its
+// zero-pivot check :4472-4488).  along_i: lines are rows j, else columns i.
+int tri_factor(const Ctx &c, TriLines &t, bool along_i, bool global) {
+    const Geom &g = c.g;
+    const cismgpu_par_t &p = c.par;
+    const int l0 = along_i ? p.staggered_jlo : p.staggered_ilo, l1 = along_i ? p.staggered_jhi : p.staggered_ihi;
+    const int s0 = along_i ? p.staggered_ilo : p.staggered_jlo, s1 = along_i ? p.staggered_ihi : p.staggered_jhi;
+    auto at = [&](int line, int s) { return along_i ? g.v2(s, line) : g.v2(line, s); };
+    for (int l = l0; l <= l1; ++l) {
+        t.omega[at(l, s0)] = t.sp[at(l, s0)] / t.dg[at(l, s0)];
+        for (int s = s0 + 1; s <= s1; ++s) {
+            const long e = at(l, s);
+            double den = t.dg[e] - t.sub[e] * t.omega[at(l, s - 1)];
+            if (den == 0.0) return CISMGPU_EDIVZERO;
+            t.denom[e] = 1.0 / den;
+            t.omega[e] = t.sp[e] * t.denom[e];
+        }
+        if (global) {
+            double om = t.sub[at(l, s1)] / t.dg[at(l, s1)];
+            for (int s = s1 - 1; s >= s0; --s) {
+                const long e = at(l, s);
+                double den_uh = t.dg[e] - t.sp[e] * om;
+                if (den_uh == 0.0) return CISMGPU_EDIVZERO;
+                om = t.sub[e] / den_uh;
+            }
+        }
+    }
+    return CISMGPU_OK;
+}
+
+// Coefficients of one line system from a 9-entry plane accessor A(i,j,m): sub/diag/super at
+// indxA_2d (-1,0),(0,0),(1,0) for u and (0,-1),(0,0),(0,1) for v; zero diagonals become 1
+// with zero off-diagonals (:4306-4313, :4349-4356); omega = denom = 0; adr = 1/diag (:4347).
+template <class F>
+void tri_coefs(const Ctx &c, TriLines &t, bool along_i, F A) {
+    const Geom &g = c.g;
+    const long n = g.nq();
+    t.sub.assign(n, 0.0); t.dg.assign(n, 0.0); t.sp.assign(n, 0.0);
+    t.adr.assign(n, 0.0); t.omega.assign(n, 0.0); t.denom.assign(n, 0.0);
+    const int ms = along_i ? c.I2(-1, 0) : c.I2(0, -1), md = c.I2(0, 0), mp = along_i ? c.I2(1, 0) : c.I2(0, 1);
+    for (int j = 1; j <= g.NY; ++j)
+        for (int i = 1; i <= g.NX; ++i) {
+            const long e = g.v2(i, j);
+            t.sub[e] = A(i, j, ms);
+            t.dg[e] = A(i, j, md);
+            t.sp[e] = A(i, j, mp);
+            if (t.dg[e] == 0.0) { t.dg[e] = 1.0; t.sub[e] = 0.0; t.sp[e] = 0.0; }
+        }
+    for (long e = 0; e < n; ++e) t.adr[e] = 1.0 / t.dg[e];
+}
+
+// tridiag_solver_local_2d :4985-5013 (u) / :5041-5069 (v) on plane b -> x.  The local form
+// back-substitutes down to index 1 (halo entries below the owned range: gamma = omega = 0);
+// the global form with one task keeps the owned particular solution and zero elsewhere.
+void tri_solve(const Ctx &c, const TriLines &t, bool along_i, bool global, const double *b, double *x) {
+    const Geom &g = c.g;
+    const cismgpu_par_t &p = c.par;
+    const int l0 = along_i ? p.staggered_jlo : p.staggered_ilo, l1 = along_i ? p.staggered_jhi : p.staggered_ihi;
+    const int s0 = along_i ? p.staggered_ilo : p.staggered_jlo, s1 = along_i ? p.staggered_ihi : p.staggered_jhi;
+    auto at = [&](int line, int s) { return along_i ? g.v2(s, line) : g.v2(line, s); };
+    for (long e = 0; e < g.nq(); ++e) x[e] = 0.0;
+    std::vector<double> gam((along_i ? g.NX : g.NY) + 1, 0.0);
+    for (int l = l0; l <= l1; ++l) {
+        std::fill(gam.begin(), gam.end(), 0.0);
+        gam[s0] = b[at(l, s0)] * t.adr[at(l, s0)];
+        for (int s = s0 + 1; s <= s1; ++s) {
+            const long e = at(l, s);
+            gam[s] = (b[e] - t.sub[e] * gam[s - 1]) * t.denom[e];
+        }
+        x[at(l, s1)] = gam[s1];
+        const int send = global ? s0 : 1;
+        for (int s = s1 - 1; s >= send; --s) {
+            const long e = at(l, s);
+            x[e] = gam[s] - t.omega[e] * x[at(l, s + 1)];
+        }
+    }
+}
+
+int setup_precond(const Ctx &c, bool is3d, int precond, const double *Auu, const double *Avv, Precond &P) {
     const Geom &g = c.g;
     P.kind = precond;
+    const bool tri = (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL);
+    const bool global = (precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL);
     if (precond == CISMGPU_PRECOND_DIAG) {
         P.Adu.assign(g.ntot(), 0.0);
         P.Adv.assign(g.ntot(), 0.0);
@@ -460,7 +557,15 @@ void setup_precond(const Ctx &c, bool is3d, int precond, const double *Auu, cons
                     P.Adv[g.v2(i, j)] = Avv[g.a2(i, j, m)];
                 }
         }
-    } else if (precond == CISMGPU_PRECOND_SIA && is3d) {  // setup_preconditioner_sia_3d :3686-3727
+    } else if (tri && !is3d) {  // setup_preconditioner_tridiag_{local,global}_2d
+        tri_coefs(c, P.tu, true, [&](int i, int j, int m) { return Auu[g.a2(i, j, m)]; });
+        tri_coefs(c, P.tv, false, [&](int i, int j, int m) { return Avv[g.a2(i, j, m)]; });
+        int st = tri_factor(c, P.tu, true, global);
+        if (st) return st;
+        st = tri_factor(c, P.tv, false, global);
+        if (st) return st;
+    }
+    if ((precond == CISMGPU_PRECOND_SIA || tri) && is3d) {  // setup_preconditioner_sia_3d :3686-3727
         P.Muu.assign(3 * g.ntot(), 0.0);
         P.Mvv.assign(3 * g.ntot(), 0.0);
         for (int j = 1; j <= g.NY; ++j)
@@ -478,6 +583,41 @@ void setup_precond(const Ctx &c, bool is3d, int precond, const double *Auu, cons
                     P.Mvv[2 + 3 * e] = Avv[g.a3(m, k, i, j)];
                 }
     }
+    if (tri && is3d) {
+        // vertical sums of the 9 horizontal couplings over the 3 vertical offsets and all
+        // levels, raw m, m+9, m+18 (:3809-3821 / :4011-4023); inactive columns: the local form
+        // zeroes the 9 sums and sets m = 5 to 1 (:3823-3833), the global form only sets m = 5
+        // to 1 (:4025-4032); its halo update of the sums (:4034-4037) touches no owned entry
+        const long nq = g.nq();
+        Vec su(9 * nq), sv(9 * nq);
+        for (int j = 1; j <= g.NY; ++j)
+            for (int i = 1; i <= g.NX; ++i)
+                for (int m = 1; m <= 9; ++m) {
+                    double au = 0.0, av = 0.0;
+                    for (int k = 1; k <= g.nz; ++k) {
+                        au = au + Auu[g.a3(m, k, i, j)] + Auu[g.a3(m + 9, k, i, j)] + Auu[g.a3(m + 18, k, i, j)];
+                        av = av + Avv[g.a3(m, k, i, j)] + Avv[g.a3(m + 9, k, i, j)] + Avv[g.a3(m + 18, k, i, j)];
+                    }
+                    su[(m - 1) * nq + g.v2(i, j)] = au;
+                    sv[(m - 1) * nq + g.v2(i, j)] = av;
+                }
+        for (int j = 1; j <= g.NY; ++j)
+            for (int i = 1; i <= g.NX; ++i) {
+                if (c.act(i, j)) continue;
+                for (int m = 1; m <= 9; ++m)
+                    if (!global || m == 5) {
+                        su[(m - 1) * nq + g.v2(i, j)] = (m == 5) ? 1.0 : 0.0;
+                        sv[(m - 1) * nq + g.v2(i, j)] = (m == 5) ? 1.0 : 0.0;
+                    }
+            }
+        tri_coefs(c, P.tu, true, [&](int i, int j, int m) { return su[(m - 1) * nq + g.v2(i, j)]; });
+        tri_coefs(c, P.tv, false, [&](int i, int j, int m) { return sv[(m - 1) * nq + g.v2(i, j)]; });
+        int st = tri_factor(c, P.tu, true, global);
+        if (st) return st;
+        st = tri_factor(c, P.tv, false, global);
+        if (st) return st;
+    }
+    return CISMGPU_OK;
 }
 
 // z = PC(r), applied over the whole array (halo included), :1231-1263 / :460-480.
@@ -494,6 +634,40 @@ void apply_precond(const Ctx &c, bool is3d, const Precond &P, const Vec &ru, con
     } else if (P.kind == CISMGPU_PRECOND_SIA && is3d) {
         easy_sia_solver(c, P.Muu, ru, zu);
         easy_sia_solver(c, P.Mvv, rv, zv);
+    } else if (P.kind == CISMGPU_PRECOND_TRIDIAG_LOCAL || P.kind == CISMGPU_PRECOND_TRIDIAG_GLOBAL) {
+        const bool global = (P.kind == CISMGPU_PRECOND_TRIDIAG_GLOBAL);
+        const Geom &g = c.g;
+        Ctx c2 = c;
+        c2.g.nz = 1;  // (NX, NY) planes
+        if (!is3d) {  // line solves, then halo(z) (:502-531 / :533-617)
+            tri_solve(c2, P.tu, true, global, ru.data(), zu.data());
+            tri_solve(c2, P.tv, false, global, rv.data(), zv.data());
+            halo(c2, zu);
+            halo(c2, zv);
+        } else {  // tridiag_solver_{local,global}_3d: vertical sums of r (sum(ru(:,i,j))), line
+                  // solves, halo of the summed solution, SIA columns, z += summed solution
+            const long nq = g.nq();
+            Vec rsu(nq), rsv(nq), zsu(nq), zsv(nq);
+            for (int j = 1; j <= g.NY; ++j)
+                for (int i = 1; i <= g.NX; ++i) {
+                    double a = 0.0, b = 0.0;
+                    for (int k = 1; k <= g.nz; ++k) { a = a + ru[g.v3(k, i, j)]; b = b + rv[g.v3(k, i, j)]; }
+                    rsu[g.v2(i, j)] = a;
+                    rsv[g.v2(i, j)] = b;
+                }
+            tri_solve(c2, P.tu, true, global, rsu.data(), zsu.data());
+            tri_solve(c2, P.tv, false, global, rsv.data(), zsv.data());
+            halo(c2, zsu);
+            halo(c2, zsv);
+            easy_sia_solver(c, P.Muu, ru, zu);
+            easy_sia_solver(c, P.Mvv, rv, zv);
+            for (int j = 1; j <= g.NY; ++j)
+                for (int i = 1; i <= g.NX; ++i)
+                    for (int k = 1; k <= g.nz; ++k) {
+                        zu[g.v3(k, i, j)] = zu[g.v3(k, i, j)] + zsu[g.v2(i, j)];
+                        zv[g.v3(k, i, j)] = zv[g.v3(k, i, j)] + zsv[g.v2(i, j)];
+                    }
+        }
     }
     // any other value: no branch taken, z keeps its contents (as in the reference)
 }
@@ -503,12 +677,11 @@ inline void mul(const Vec &a, const Vec &b, Vec &out) {
 }
 
 int check_args(int nx, int ny, int nz, const cismgpu_par_t *par, int precond, int ncheck, int maxiters) {
+    (void)precond;  // every value is accepted: 0-4 have branches, others take none
     if (!par || nx < 5 || ny < 5 || nz < 1) return CISMGPU_EINVAL;
     if (ncheck < 1) return CISMGPU_EINVAL;
     if (maxiters < 0) return CISMGPU_EINVAL;
     if (par->tasks_row * par->tasks_col != 1) return CISMGPU_EUNSUPPORTED;
-    if (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL)
-        return CISMGPU_EUNSUPPORTED;
     if (par->staggered_ilo < 1 || par->staggered_ihi > nx - 1 || par->staggered_ilo > par->staggered_ihi ||
         par->staggered_jlo < 1 || par->staggered_jhi > ny - 1 || par->staggered_jlo > par->staggered_jhi)
         return CISMGPU_EINVAL;
@@ -528,12 +701,14 @@ int standard(bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const 
     Vec bu(bu_, bu_ + n), bv(bv_, bv_ + n), xu(xu_, xu_ + n), xv(xv_, xv_ + n);
     Vec ru(n), rv(n), du(n), dv(n), qu(n), qv(n), zu(n, 0.0), zv(n, 0.0), w0u(n), w0v(n);
     Precond P;
-    setup_precond(c, is3d, precond, Auu, Avv, P);
+    *err = NAN;  // intent(out) and never set when no check runs; NaN makes that visible
+    *niters = maxiters;
+    st = setup_precond(c, is3d, precond, Auu, Avv, P);
+    if (st) return st;  // GM_FATAL in the reference: x unchanged
     auto matvec = [&](const Vec &a, const Vec &b, Vec &ya, Vec &yb) {
         if (is3d) matvec3(c, Auu, Auv, Avu, Avv, a, b, ya, yb);
         else matvec2(c, Auu, Auv, Avu, Avv, a, b, ya, yb);
     };
-    *err = NAN;  // intent(out) and never set when no check runs; NaN makes that visible
     int status = CISMGPU_OK;
 
     halo(c, xu); halo(c, xv);
@@ -593,15 +768,19 @@ int chrongear(bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const
     Vec ru(n, 0.0), rv(n, 0.0), du(n, 0.0), dv(n, 0.0), zu(n, 0.0), zv(n, 0.0), qu(n, 0.0), qv(n, 0.0);
     Vec Azu(n, 0.0), Azv(n, 0.0), wu(n, 0.0), wv(n, 0.0), w1u(n), w1v(n), w2u(n), w2v(n);
     Precond P;
-    setup_precond(c, is3d, precond, Auu, Avv, P);
+    // 2D with a tridiagonal preconditioner: at most 100 iterations (:1704-1732); 3D keeps
+    // maxiters (:2896-2909)
+    const bool tri = (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL);
+    const int maxiters_chrongear = (tri && !is3d) ? 100 : maxiters;
+    *err = NAN;
+    *niters = maxiters_chrongear;
+    st = setup_precond(c, is3d, precond, Auu, Avv, P);
+    if (st) return st;  // GM_FATAL in the reference: x unchanged
     auto matvec = [&](const Vec &a, const Vec &b, Vec &ya, Vec &yb) {
         if (is3d) matvec3(c, Auu, Auv, Avu, Avv, a, b, ya, yb);
         else matvec2(c, Auu, Auv, Avu, Avv, a, b, ya, yb);
     };
-    *err = NAN;
     int status = CISMGPU_OK;
-    const int maxiters_chrongear = maxiters;  // tridiag override (2D :1728-1732) is unsupported here
-    *niters = maxiters_chrongear;
 
     mul(bu, bu, wu); mul(bv, bv, wv);
     double bb = global_sum(c, wu, wv);
@@ -766,6 +945,24 @@ int oracle_easy_sia(int nx, int ny, int nz, const int32_t *active_vertex, const 
     easy_sia_solver(c, MM, bb, xx);
     std::memcpy(x, xx.data(), n * sizeof(double));
     return 0;
+}
+
+// z = PC(r) for one preconditioner (setup + apply), is3d ? (nz,nx-1,ny-1) : (nx-1,ny-1)
+// arrays; z holds the previous z on entry (kept where the reference keeps it)
+int oracle_precond_apply(int is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indxA_2d,
+                         const int32_t *indxA_3d, const int32_t *active_vertex, const double *Auu,
+                         const double *Avv, int precond, const double *ru, const double *rv, double *zu,
+                         double *zv) {
+    Ctx c{Geom{is3d ? nz : 1, nx - 1, ny - 1}, *par, 0, indxA_2d, indxA_3d, active_vertex};
+    const long n = c.g.ntot();
+    Precond P;
+    int st = setup_precond(c, is3d != 0, precond, Auu, Avv, P);
+    if (st) return st;
+    Vec a(ru, ru + n), b(rv, rv + n), za(zu, zu + n), zb(zv, zv + n);
+    apply_precond(c, is3d != 0, P, a, b, za, zb);
+    std::memcpy(zu, za.data(), n * sizeof(double));
+    std::memcpy(zv, zb.data(), n * sizeof(double));
+    return CISMGPU_OK;
 }
 
 // exact correctly-rounded sum of n doubles

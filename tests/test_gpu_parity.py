@@ -67,7 +67,7 @@ CASES_3D = [
 
 
 @pytest.mark.parametrize("alg", ["standard", "chrongear"])
-@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("case", CASES_3D, ids=[c[0] for c in CASES_3D])
 def test_3d_bitexact_vs_device_tree_oracle(gpu_lib, alg, precond, case):
     P = problems.slab_3d(**case[1])
@@ -86,10 +86,11 @@ CASES_2D = [
 
 
 @pytest.mark.parametrize("alg", ["standard", "chrongear"])
-@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("case", CASES_2D, ids=[c[0] for c in CASES_2D])
 def test_2d_bitexact_vs_device_tree_oracle(gpu_lib, alg, precond, case):
-    # precond 2 in 2D takes no branch in the reference (z unchanged): reproduced, not rejected
+    # precond 2 in 2D takes no branch in the reference (z unchanged): reproduced, not rejected;
+    # with 3/4 Chronopoulos-Gear stops at 100 iterations on both sides (:1704-1732)
     P = problems.slab_2d(**case[1])
     x0 = problems.random_x0(P, seed=8, scale=10.0)
     o = oracle.pcg(alg, P, precond, tol=1e-8, maxiters=400, summode=oracle.SUM_DDTREE, x0=x0)
@@ -145,8 +146,6 @@ def test_matvec_2d_bitexact(gpu_lib):
 
 def test_error_statuses(gpu_lib):
     P = problems.slab_3d(seed=2)
-    assert gpu_solve("standard", P, 3)[0] == 3
-    assert gpu_solve("chrongear", P, 4)[0] == 3
     Q = problems.slab_3d(seed=2)
     Q.par = dict(Q.par, tasks_col=2)
     assert gpu_solve("standard", Q, 1)[0] == 3
@@ -156,6 +155,31 @@ def test_error_statuses(gpu_lib):
     assert gpu_solve("standard", Z, 1)[0] == oracle.pcg("standard", Z, 1)[0] == 2
     assert gpu_solve("chrongear", Z, 2)[0] == oracle.pcg("chrongear", Z, 2)[0] == 2
     assert gpu_solve("standard", P, 1, ncheck=0)[0] == 4
+
+
+def test_tridiag_zero_pivot(gpu_lib):
+    """A zero pivot in the line factorization: CISMGPU_EDIVZERO (GM_FATAL in the reference,
+    :4339, :4380), x unchanged; the global form's reverse-recurrence check (:4475, :4492)
+    fails precond 4 only."""
+    P = problems.slab_2d(seed=23)
+    p = P.par
+    j, a, b = p["staggered_jlo"] - 1, p["staggered_ilo"] - 1, p["staggered_ihi"] - 1
+    P.Auu[4, j, a], P.Auu[5, j, a] = 1.0, 1.0
+    P.Auu[3, j, a + 1], P.Auu[4, j, a + 1] = 2.0, 2.0
+    x0 = problems.random_x0(P, seed=3, scale=1.0)
+    for alg, pc in (("standard", 3), ("chrongear", 4)):
+        st, xu, xv, err, nit = gpu_solve(alg, P, pc, maxiters=3, x0=x0)
+        assert st == 9 == oracle.pcg(alg, P, pc, maxiters=3)[0]
+        np.testing.assert_array_equal(xu, x0[0])
+        np.testing.assert_array_equal(xv, x0[1])
+    Q = problems.slab_2d(seed=23)
+    Q.Auu[3, j, b], Q.Auu[4, j, b] = 1.0, 1.0
+    Q.Auu[5, j, b - 1], Q.Auu[4, j, b - 1] = 3.0, 3.0
+    for pc in (3, 4):
+        g = gpu_solve("standard", Q, pc, maxiters=3)
+        o = oracle.pcg("standard", Q, pc, maxiters=3, summode=oracle.SUM_DDTREE)
+        assert (g[0] == 9) == (pc == 4)
+        assert_bitexact(g, o)
 
 
 def test_no_check_leaves_err_nan(gpu_lib):

@@ -92,6 +92,110 @@ def test_easy_sia_matches_dense_tridiagonal_solve():
             np.testing.assert_allclose(x[j, i], np.linalg.solve(T, b[j, i]), rtol=1e-12, atol=1e-12)
 
 
+def _line_solve(dg, sub, sp, b):
+    """Dense solve of one tridiagonal line system with the reference's zero-diagonal fix
+    (diag 0 -> 1, off-diagonals 0; setup_preconditioner_tridiag_local_2d :4306-4313)."""
+    dg, sub, sp = dg.copy(), sub.copy(), sp.copy()
+    z = dg == 0.0
+    dg[z], sub[z], sp[z] = 1.0, 0.0, 0.0
+    n = len(dg)
+    T = np.diag(dg) + np.diag(sub[1:], -1) + np.diag(sp[:-1], 1)
+    return np.linalg.solve(T, b)
+
+
+def _owned(P):
+    p = P.par
+    return (range(p["staggered_jlo"] - 1, p["staggered_jhi"]), range(p["staggered_ilo"] - 1, p["staggered_ihi"]))
+
+
+@pytest.mark.parametrize("bc", ["periodic", "outflow", "no_ice"])
+def test_tridiag_precond_2d_matches_dense_line_solves(bc):
+    """Precond 3 and 4 in 2D: u solved along each owned row with Auu's (-1,0),(0,0),(1,0)
+    couplings, v along each owned column with Avv's (0,-1),(0,0),(0,1); z on owned
+    vertices equals dense line solves, and the local and global forms agree bit for bit
+    on one task (tridiag_solver_global_2d keeps the particular solution, :5495-5497)."""
+    P = problems.slab_2d(seed=21, boundary_ice=True, bc=bc)
+    rng = np.random.default_rng(2)
+    ru, rv = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bv.shape)
+    st3, zu3, zv3 = oracle.precond_apply(P, 3, ru, rv)
+    st4, zu4, zv4 = oracle.precond_apply(P, 4, ru, rv)
+    assert st3 == st4 == 0
+    np.testing.assert_array_equal(zu3, zu4)
+    np.testing.assert_array_equal(zv3, zv4)
+    J, I = _owned(P)
+    i0, i1, j0, j1 = I[0], I[-1] + 1, J[0], J[-1] + 1
+    wu, wv = np.zeros_like(zu3), np.zeros_like(zv3)
+    for j in J:  # Auu[m, j, i]: m = (iA+1) + 3*(jA+1)
+        wu[j, i0:i1] = _line_solve(P.Auu[4, j, i0:i1], P.Auu[3, j, i0:i1], P.Auu[5, j, i0:i1], ru[j, i0:i1])
+    for i in I:
+        wv[j0:j1, i] = _line_solve(P.Avv[4, j0:j1, i], P.Avv[1, j0:j1, i], P.Avv[7, j0:j1, i], rv[j0:j1, i])
+    # then the staggered halo update of z (:529-531): periodic copies or boundary zeros
+    wu = oracle.halo(P.nx, P.ny, 1, P.par, wu)
+    wv = oracle.halo(P.nx, P.ny, 1, P.par, wv)
+    np.testing.assert_allclose(zu3, wu, rtol=1e-10, atol=1e-12 * np.abs(wu).max())
+    np.testing.assert_allclose(zv3, wv, rtol=1e-10, atol=1e-12 * np.abs(wv).max())
+
+
+@pytest.mark.parametrize("precond", [3, 4])
+def test_tridiag_precond_3d_matches_dense(precond):
+    """Precond 3/4 in 3D: vertically summed couplings (all 27 folded onto the 9 horizontal
+    ones), line solves of the summed residual, halo, then the SIA column solve of r plus the
+    summed solution on every level (tridiag_solver_local_3d :4524-4658)."""
+    P = problems.slab_3d(seed=22, nz=5)
+    rng = np.random.default_rng(3)
+    ru, rv = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bv.shape)
+    st, zu, zv = oracle.precond_apply(P, precond, ru, rv)
+    assert st == 0
+    NY, NX, nz = P.bu.shape
+    J, I = _owned(P)
+    i0, i1, j0, j1 = I[0], I[-1] + 1, J[0], J[-1] + 1
+
+    def vsum(A, m):  # sum over levels and the three vertical offsets of horizontal coupling m
+        s = A[:, :, :, m] + A[:, :, :, m + 9] + A[:, :, :, m + 18]
+        out = s.sum(axis=2)
+        inact = P.active_vertex == 0
+        out[inact] = 1.0 if m == 4 else (0.0 if precond == 3 else out[inact])
+        return out
+    su = {m: vsum(P.Auu, m) for m in (3, 4, 5)}
+    sv = {m: vsum(P.Avv, m) for m in (1, 4, 7)}
+    rsu, rsv = ru.sum(axis=2), rv.sum(axis=2)
+    zsu, zsv = np.zeros((NY, NX)), np.zeros((NY, NX))
+    for j in J:
+        zsu[j, i0:i1] = _line_solve(su[4][j, i0:i1], su[3][j, i0:i1], su[5][j, i0:i1], rsu[j, i0:i1])
+    for i in I:
+        zsv[j0:j1, i] = _line_solve(sv[4][j0:j1, i], sv[1][j0:j1, i], sv[7][j0:j1, i], rsv[j0:j1, i])
+    zsu = oracle.halo(P.nx, P.ny, 1, P.par, zsu)
+    zsv = oracle.halo(P.nx, P.ny, 1, P.par, zsv)
+    for j in range(NY):
+        for i in range(NX):
+            for A, r, zs, z in ((P.Auu, ru, zsu, zu), (P.Avv, rv, zsv, zv)):
+                if P.active_vertex[j, i]:
+                    T = np.diag(A[j, i, :, 13]) + np.diag(A[j, i, 1:, 4], -1) + np.diag(A[j, i, :-1, 22], 1)
+                    want = np.linalg.solve(T, r[j, i]) + zs[j, i]
+                else:
+                    want = np.zeros(nz) + zs[j, i]  # z keeps its previous value (0) plus the sum
+                np.testing.assert_allclose(z[j, i], want, rtol=1e-9, atol=1e-11 * (1 + np.abs(want).max()))
+
+
+def test_tridiag_precond_zero_pivot():
+    """A zero pivot in the line factorization is GM_FATAL in the reference (:4339, :4380);
+    the global form also checks the reverse recurrence (:4475, :4492), so a pivot that
+    only that recurrence meets fails precond 4 and not precond 3."""
+    P = problems.slab_2d(seed=23)
+    J, I = _owned(P)
+    j, a = J[0], I[0]
+    P.Auu[4, j, a], P.Auu[5, j, a] = 1.0, 1.0        # omega(a) = 1
+    P.Auu[3, j, a + 1], P.Auu[4, j, a + 1] = 2.0, 2.0  # 2 - 2*1 = 0
+    assert oracle.pcg("standard", P, 3, maxiters=3)[0] == 9
+    assert oracle.pcg("chrongear", P, 4, maxiters=3)[0] == 9
+    Q = problems.slab_2d(seed=23)
+    b = I[-1]
+    Q.Auu[3, j, b], Q.Auu[4, j, b] = 1.0, 1.0          # reverse: omega_uh(b) = 1
+    Q.Auu[5, j, b - 1], Q.Auu[4, j, b - 1] = 3.0, 3.0  # 3 - 3*1 = 0
+    assert oracle.pcg("standard", Q, 3, maxiters=3)[0] != 9
+    assert oracle.pcg("standard", Q, 4, maxiters=3)[0] == 9
+
+
 def test_exact_sum_is_correctly_rounded():
     rng = np.random.default_rng(7)
     for trial in range(20):
@@ -186,7 +290,7 @@ def _owned_active_dense(P):
 
 
 @pytest.mark.parametrize("alg", ["standard", "chrongear"])
-@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3, 4])
 def test_pcg_converges_to_dense_solution_3d(alg, precond):
     P = problems.slab_3d(seed=11, nz=4)
     idx, A, b = _owned_active_dense(P)
@@ -208,12 +312,15 @@ def test_pcg_converges_to_dense_solution_3d(alg, precond):
 
 
 @pytest.mark.parametrize("alg", ["standard", "chrongear"])
-def test_pcg_converges_to_dense_solution_2d(alg):
+@pytest.mark.parametrize("precond", [1, 3, 4])
+def test_pcg_converges_to_dense_solution_2d(alg, precond):
     P = problems.slab_2d(seed=12)
     idx, A, b = _owned_active_dense(P)
     xs = np.linalg.solve(A, b)
-    st, xu, xv, err, nit = oracle.pcg(alg, P, 1, tol=1e-10, maxiters=5000)
+    st, xu, xv, err, nit = oracle.pcg(alg, P, precond, tol=1e-10, maxiters=5000)
     assert st == 0 and err < 1e-10
+    if alg == "chrongear" and precond in (3, 4):
+        assert nit <= 100  # Chronopoulos-Gear 2D caps tridiagonal solves at 100 (:1704-1732)
     n = len(idx)
     got = np.zeros(2 * n)
     for (j, i, k), r in idx.items():
@@ -236,7 +343,6 @@ def test_sum_modes_agree_in_trajectory_for_sia():
 
 def test_error_statuses():
     P = problems.slab_3d(seed=2)
-    assert oracle.pcg("standard", P, 3)[0] == 3          # tridiagonal precond: unsupported
     par = dict(P.par, tasks_row=2)
     Q = problems.slab_3d(seed=2)
     Q.par = par
