@@ -163,6 +163,19 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_global_sum_stagger.restype = ctypes.c_int
     lib.cismgpu_global_sum_stagger_noalloc.argtypes = [i32, i32, i32, par, vp, vp, vp, vp]
     lib.cismgpu_global_sum_stagger_noalloc.restype = ctypes.c_int
+    lib.cismgpu_compute_residual_vector_3d.argtypes = [i32, i32, i32, par, d, d, d, d, d, d, d, d, d, d, d, d,
+                                                       P(dbl), P(dbl)]
+    lib.cismgpu_compute_residual_vector_2d.argtypes = [i32, i32, par, d, d, d, d, d, d, d, d, d, d, d, d,
+                                                       P(dbl), P(dbl)]
+    lib.cismgpu_compute_residual_velocity_3d.argtypes = [i32, i32, i32, i32, par, d, d, d, d, P(dbl)]
+    lib.cismgpu_compute_residual_velocity_2d.argtypes = [i32, i32, i32, par, d, d, d, d, P(dbl)]
+    lib.cismgpu_solver_set_system.argtypes = [vp, d, d, d, d, d, d, i32]
+    lib.cismgpu_solver_residual_vector.argtypes = [vp, d, d, P(dbl), P(dbl)]
+    lib.cismgpu_solver_residual_velocity.argtypes = [vp, i32, P(dbl)]
+    for f in ("cismgpu_compute_residual_vector_3d", "cismgpu_compute_residual_vector_2d",
+              "cismgpu_compute_residual_velocity_3d", "cismgpu_compute_residual_velocity_2d",
+              "cismgpu_solver_set_system", "cismgpu_solver_residual_vector", "cismgpu_solver_residual_velocity"):
+        getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
     lib.cismgpu_last_error.restype = ctypes.c_char_p
@@ -314,6 +327,66 @@ def matvec_multiply_structured_2d(nx, ny, parallel, indxA_2d, active_vertex, Auu
     return yu, yv
 
 
+def compute_residual_vector_3d(nx, ny, nz, parallel, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, bu, bv, uvel,
+                               vvel):
+    """Mirrors compute_residual_vector_3d (glissade_velo_higher.F90:9693-9894);
+    returns (resid_u, resid_v, L2_norm, L2_norm_relative)."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    nvec, nblk = nv * nz, nv * nz * 27
+    ru, rv = np.empty_like(bu), np.empty_like(bv)
+    l2, l2r = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    par = _par(parallel)
+    _check(lib, lib.cismgpu_compute_residual_vector_3d(
+        nx, ny, nz, ctypes.byref(par), _ptr(np.ascontiguousarray(indxA_3d, dtype=np.int32), np.int32, 27),
+        _ptr(active_vertex, np.int32, nv), _ptr(Auu, np.float64, nblk), _ptr(Auv, np.float64, nblk),
+        _ptr(Avu, np.float64, nblk), _ptr(Avv, np.float64, nblk), _ptr(bu, np.float64, nvec),
+        _ptr(bv, np.float64, nvec), _ptr(uvel, np.float64, nvec), _ptr(vvel, np.float64, nvec),
+        _ptr(ru, np.float64, nvec, True), _ptr(rv, np.float64, nvec, True), ctypes.byref(l2), ctypes.byref(l2r)))
+    return ru, rv, l2.value, l2r.value
+
+
+def compute_residual_vector_2d(nx, ny, parallel, indxA_2d, active_vertex, Auu, Auv, Avu, Avv, bu, bv, uvel, vvel):
+    """Mirrors compute_residual_vector_2d (glissade_velo_higher.F90:9502-9689);
+    returns (resid_u, resid_v, L2_norm, L2_norm_relative)."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    ru, rv = np.empty_like(bu), np.empty_like(bv)
+    l2, l2r = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    par = _par(parallel)
+    _check(lib, lib.cismgpu_compute_residual_vector_2d(
+        nx, ny, ctypes.byref(par), _ptr(np.ascontiguousarray(indxA_2d, dtype=np.int32), np.int32, 9),
+        _ptr(active_vertex, np.int32, nv), _ptr(Auu, np.float64, nv * 9), _ptr(Auv, np.float64, nv * 9),
+        _ptr(Avu, np.float64, nv * 9), _ptr(Avv, np.float64, nv * 9), _ptr(bu, np.float64, nv),
+        _ptr(bv, np.float64, nv), _ptr(uvel, np.float64, nv), _ptr(vvel, np.float64, nv),
+        _ptr(ru, np.float64, nv, True), _ptr(rv, np.float64, nv, True), ctypes.byref(l2), ctypes.byref(l2r)))
+    return ru, rv, l2.value, l2r.value
+
+
+def compute_residual_velocity_3d(whichresid, nx, ny, nz, parallel, uvel, vvel, usav, vsav) -> float:
+    """Mirrors compute_residual_velocity_3d (glissade_velo_higher.F90:10314-10446)."""
+    lib = load_library()
+    n = (nx - 1) * (ny - 1) * nz
+    out = ctypes.c_double(0.0)
+    par = _par(parallel)
+    _check(lib, lib.cismgpu_compute_residual_velocity_3d(
+        int(whichresid), nx, ny, nz, ctypes.byref(par), _ptr(uvel, np.float64, n), _ptr(vvel, np.float64, n),
+        _ptr(usav, np.float64, n), _ptr(vsav, np.float64, n), ctypes.byref(out)))
+    return out.value
+
+
+def compute_residual_velocity_2d(whichresid, nx, ny, parallel, uvel, vvel, usav, vsav) -> float:
+    """Mirrors compute_residual_velocity_2d (glissade_velo_higher.F90:10188-10310)."""
+    lib = load_library()
+    n = (nx - 1) * (ny - 1)
+    out = ctypes.c_double(0.0)
+    par = _par(parallel)
+    _check(lib, lib.cismgpu_compute_residual_velocity_2d(
+        int(whichresid), nx, ny, ctypes.byref(par), _ptr(uvel, np.float64, n), _ptr(vvel, np.float64, n),
+        _ptr(usav, np.float64, n), _ptr(vsav, np.float64, n), ctypes.byref(out)))
+    return out.value
+
+
 class DeviceSolver:
     """A device-resident linear system (cismgpu_solver_create): A, b and x0 live in HBM.
 
@@ -356,6 +429,40 @@ class DeviceSolver:
         _check(self._lib, self._lib.cismgpu_solver_solve(self.handle, algorithm, precond, ncheck, tol, maxiters,
                                                           ctypes.byref(err), ctypes.byref(nit)))
         return err.value, nit.value
+
+    def set_system(self, Auu, Auv, Avu, Avv, bu, bv, x0_from_solution=True):
+        """New coefficients and right-hand side (same geometry and active vertices) for the next
+        Picard iteration; with x0_from_solution the next solve starts from the last solution,
+        which stays on the device."""
+        P = self.problem
+        is3d = P.kind == "3d"
+        nv = (P.nx - 1) * (P.ny - 1)
+        nvec = nv * (P.nz if is3d else 1)
+        nblk = nvec * (27 if is3d else 9)
+        _check(self._lib, self._lib.cismgpu_solver_set_system(
+            self.handle, _ptr(Auu, np.float64, nblk), _ptr(Auv, np.float64, nblk), _ptr(Avu, np.float64, nblk),
+            _ptr(Avv, np.float64, nblk), _ptr(bu, np.float64, nvec), _ptr(bv, np.float64, nvec),
+            1 if x0_from_solution else 0))
+
+    def residual_vector(self, arrays=True):
+        """compute_residual_vector of the current velocity with the current system:
+        (resid_u, resid_v, L2_norm, L2_norm_relative); resid arrays are None with arrays=False."""
+        l2, l2r = ctypes.c_double(0.0), ctypes.c_double(0.0)
+        ru = rv = None
+        pu = pv = None
+        if arrays:
+            ru, rv = np.empty(self._shape), np.empty(self._shape)
+            pu, pv = ctypes.c_void_p(ru.ctypes.data), ctypes.c_void_p(rv.ctypes.data)
+        _check(self._lib, self._lib.cismgpu_solver_residual_vector(self.handle, pu, pv, ctypes.byref(l2),
+                                                                   ctypes.byref(l2r)))
+        return ru, rv, l2.value, l2r.value
+
+    def residual_velocity(self, whichresid=1):
+        """compute_residual_velocity between the last solution and the guess it started from."""
+        out = ctypes.c_double(0.0)
+        _check(self._lib, self._lib.cismgpu_solver_residual_velocity(self.handle, int(whichresid),
+                                                                     ctypes.byref(out)))
+        return out.value
 
     def x(self):
         xu = np.empty(self._shape)

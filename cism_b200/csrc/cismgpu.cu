@@ -111,6 +111,7 @@ struct Solver {
     bool own_stream = false;
     DevBuf A, raw, vec, act, partials, state, map;
     DevBuf tri;       // tridiagonal preconditioner planes (TriPlane), on first use
+    bool x_current = false;   // the x planes hold a solution (a solve ran since the last upload)
     int32_t hindx[27] = {};   // host copy of the uploaded indxA map (27 or 9 entries)
     int32_t hindx2[9] = {};   // indxA_2d: the uploaded map in 2D; in 3D the caller's, else standard
     MixedBufs mixed;  // FP32 copies, created on first mixed solve
@@ -177,31 +178,44 @@ struct Solver {
         return v;
     }
 
-    // Upload the caller's arrays: coefficient planes, level-major vectors.  x0 may be null.
-    int upload(const Geom &geom, bool three_d, const int32_t *indx, const int32_t *active,
-               const double *const blocks[4], const double *bu, const double *bv, const double *xu,
-               const double *xv) {
+    // Geometry of the arrays that follow, and buffers sized for it.
+    int set_geom(const Geom &geom, bool three_d) {
         g = geom;
         is3d = three_d;
         NC = is3d ? 27 : 9;
-        for (int c = 0; c < NC; ++c) hindx[c] = indx[c];
-        for (int c = 0; c < 9; ++c) hindx2[c] = is3d ? c + 1 : indx[c];
         nvec = (long long)g.nz * g.NQ;
-        mixed.stale = true;  // new matrix: FP32 copy and factors must be rebuilt
-        n_active_owned = 0;
-        for (int j = g.jlo; j <= g.jhi; ++j)
-            for (int i = g.ilo; i <= g.ihi; ++i) n_active_owned += active[(long long)j * g.NX + i] != 0;
+        x_current = false;
+        CU(vec.ensure((size_t)NVEC * nvec * sizeof(double)));
+        CU(raw.ensure((size_t)nvec * sizeof(double)));
+        CU(partials.ensure((size_t)nblocks(g.NQ) * 2 * sizeof(DD)));
+        CU(state.ensure(sizeof(SolveState)));
+        return CISMGPU_OK;
+    }
+
+    // One vector from the caller's layout into level-major planes (null: zeros).
+    int put_vec(int id, const double *src) {
+        double *dst = vec.as<double>() + (size_t)id * nvec;
+        cudaStream_t s = stream;
+        if (!src) {
+            CU(cudaMemsetAsync(dst, 0, nvec * sizeof(double), s));
+        } else if (is3d) {
+            CU(raw.ensure((size_t)nvec * sizeof(double)));
+            CU(cudaMemcpyAsync(raw.p, src, nvec * sizeof(double), cudaMemcpyHostToDevice, s));
+            k_vec_in<<<nblocks(nvec), kBlock, 0, s>>>(g, raw.as<double>(), dst);
+            CU(cudaGetLastError());
+        } else {
+            CU(cudaMemcpyAsync(dst, src, nvec * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
+        return CISMGPU_OK;
+    }
+
+    // The coefficient blocks (permuted by the uploaded indxA map) and the right-hand side.
+    int put_system(const double *const blocks[4], const double *bu, const double *bv) {
         const size_t blk_bytes = (size_t)NC * nvec * sizeof(double);
         CU(A.ensure(4 * blk_bytes));
         CU(raw.ensure(blk_bytes));
-        CU(vec.ensure((size_t)NVEC * nvec * sizeof(double)));
-        CU(act.ensure((size_t)g.NQ * sizeof(int32_t)));
-        CU(partials.ensure((size_t)nblocks(g.NQ) * 2 * sizeof(DD)));
-        CU(state.ensure(sizeof(SolveState)));
-        CU(map.ensure(32 * sizeof(int32_t)));
         cudaStream_t s = stream;
-        CU(cudaMemcpyAsync(map.p, indx, NC * sizeof(int32_t), cudaMemcpyHostToDevice, s));
-        CU(cudaMemcpyAsync(act.p, active, (size_t)g.NQ * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+        mixed.stale = true;  // new matrix: FP32 copy and factors must be rebuilt
         for (int b = 0; b < 4; ++b) {
             CU(cudaMemcpyAsync(raw.p, blocks[b], blk_bytes, cudaMemcpyHostToDevice, s));
             double *dst = A.as<double>() + (size_t)b * NC * nvec;
@@ -211,20 +225,83 @@ struct Solver {
                 k_perm_block2<<<nblocks(g.NQ), kBlock, 0, s>>>(g, raw.as<double>(), dst, map.as<int32_t>());
             CU(cudaGetLastError());
         }
+        TRY(put_vec(VB_U, bu));
+        TRY(put_vec(VB_V, bv));
+        return CISMGPU_OK;
+    }
+
+    // Upload the caller's arrays: coefficient planes, level-major vectors.  x0 may be null.
+    int upload(const Geom &geom, bool three_d, const int32_t *indx, const int32_t *active,
+               const double *const blocks[4], const double *bu, const double *bv, const double *xu,
+               const double *xv) {
+        TRY(set_geom(geom, three_d));
+        for (int c = 0; c < NC; ++c) hindx[c] = indx[c];
+        for (int c = 0; c < 9; ++c) hindx2[c] = is3d ? c + 1 : indx[c];
+        n_active_owned = 0;
+        for (int j = g.jlo; j <= g.jhi; ++j)
+            for (int i = g.ilo; i <= g.ihi; ++i) n_active_owned += active[(long long)j * g.NX + i] != 0;
+        CU(act.ensure((size_t)g.NQ * sizeof(int32_t)));
+        CU(map.ensure(32 * sizeof(int32_t)));
+        cudaStream_t s = stream;
+        CU(cudaMemcpyAsync(map.p, indx, NC * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(act.p, active, (size_t)g.NQ * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+        TRY(put_system(blocks, bu, bv));
+        TRY(put_vec(VX0_U, xu));
+        TRY(put_vec(VX0_V, xv));
+        return CISMGPU_OK;
+    }
+
+    // compute_residual_vector on the device (glissade_velo_higher.F90:9502-9894): resid = A x - b
+    // into the r planes for x = planes (xid, xid+1); L2 = |Ax - b| and |b| over owned active
+    // vertices.  Leaves the stream synchronized.
+    int residual_vector(int xid, double *L2_norm, double *L2_rhs) {
+        const Ptrs p = ptrs();
         double *V = vec.as<double>();
-        const double *src[4] = {bu, bv, xu, xv};
-        const int dst_id[4] = {VB_U, VB_V, VX0_U, VX0_V};
-        for (int t = 0; t < 4; ++t) {
-            double *dst = V + (size_t)dst_id[t] * nvec;
-            if (!src[t]) {
-                CU(cudaMemsetAsync(dst, 0, nvec * sizeof(double), s));
-            } else if (is3d) {
-                CU(cudaMemcpyAsync(raw.p, src[t], nvec * sizeof(double), cudaMemcpyHostToDevice, s));
-                k_vec_in<<<nblocks(nvec), kBlock, 0, s>>>(g, raw.as<double>(), dst);
-                CU(cudaGetLastError());
-            } else {
-                CU(cudaMemcpyAsync(dst, src[t], nvec * sizeof(double), cudaMemcpyHostToDevice, s));
-            }
+        const double *xu = V + (size_t)xid * nvec, *xv = V + (size_t)(xid + 1) * nvec;
+        SolveState *st = state.as<SolveState>();
+        cudaStream_t s = stream;
+        CU(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+        RedCtx rc0{partials.as<DD>(), st, EPI_NONE, 0};
+        RedCtx rc1{partials.as<DD>(), st, EPI_RESID_VEC, 0};
+        const unsigned nb = nblocks(g.NQ);
+        if (is3d)
+            k_mv<27, MV_PLAIN><<<nb, mv_threads<27>(), 0, s>>>(g, A.as<double>(), act.as<int32_t>(), xu, xv, p.zu, p.zv,
+                                                              nullptr, nullptr, nullptr, nullptr, rc0);
+        else
+            k_mv<9, MV_PLAIN><<<nb, mv_threads<9>(), 0, s>>>(g, A.as<double>(), act.as<int32_t>(), xu, xv, p.zu, p.zv,
+                                                            nullptr, nullptr, nullptr, nullptr, rc0);
+        k_resid_vec<<<nb, kBlock, 0, s>>>(g, act.as<int32_t>(), p.zu, p.zv, p.bu, p.bv, p.ru, p.rv, rc1);
+        CU(cudaGetLastError());
+        CU(cudaMemcpyAsync(h_state, st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        *L2_norm = h_state->err;
+        *L2_rhs = h_state->L2_rhs;
+        return CISMGPU_OK;
+    }
+
+    // compute_residual_velocity on the device (:10188-10446) between the planes of id_new
+    // (uvel, vvel) and id_old (usav, vsav).  Leaves the stream synchronized.
+    int residual_velocity(int whichresid, int id_new, int id_old, double *resid_velo) {
+        double *V = vec.as<double>();
+        SolveState *st = state.as<SolveState>();
+        cudaStream_t s = stream;
+        CU(cudaMemsetAsync(st, 0, sizeof(SolveState), s));
+        const int mean = whichresid == CISMGPU_RESID_MEANU;
+        // 3D: the bed level is left out for the "no basal" max and the mean (size(uvel,1) - 1)
+        const int kmax = (is3d && (whichresid == CISMGPU_RESID_MAXU_NO_UBAS || mean)) ? g.nz - 1 : g.nz;
+        RedCtx rc{partials.as<DD>(), st, EPI_SUM, 0};
+        k_resid_velo<<<nblocks(g.NQ), kBlock, 0, s>>>(g, kmax, mean, V + (size_t)id_new * nvec,
+                                                      V + (size_t)(id_new + 1) * nvec, V + (size_t)id_old * nvec,
+                                                      V + (size_t)(id_old + 1) * nvec, rc);
+        CU(cudaGetLastError());
+        CU(cudaMemcpyAsync(h_state, st, sizeof(SolveState), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (mean) {
+            *resid_velo = h_state->count > 0 ? h_state->rho / (double)h_state->count : 0.0;
+        } else {
+            double d;
+            std::memcpy(&d, &h_state->maxbits, sizeof(d));
+            *resid_velo = d;
         }
         return CISMGPU_OK;
     }
@@ -307,6 +384,7 @@ struct Solver {
     };
 
     int begin_solve() {
+        x_current = true;
         const Ptrs p = ptrs();
         CU(cudaMemcpyAsync(p.xu, p.x0u, 2 * nvec * sizeof(double), cudaMemcpyDeviceToDevice, stream));
         return CISMGPU_OK;
@@ -755,6 +833,7 @@ static MState mixed_init_state(double tol, int maxiters, int ncheck) {
 // only owned unknowns, so x leaves with the same halo values.
 static int mixed_reset(Solver &sv, cudaStream_t s) {
     const Ptrs p = sv.ptrs();
+    sv.x_current = true;
     CU(cudaMemcpyAsync(p.xu, p.x0u, 2 * sv.nvec * sizeof(double), cudaMemcpyDeviceToDevice, s));
     k_halo<<<nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4)), kBlock, 0, s>>>(sv.g, p.xu, p.xv, nullptr);
     CU(cudaGetLastError());
@@ -1035,6 +1114,47 @@ static int oneshot_matvec(bool is3d, int nx, int ny, int nz, const cismgpu_par_t
     return sv.download(VX_U, VX_V, yu, yv);
 }
 
+static int oneshot_resid_vec(bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indx,
+                             const int32_t *act, const double *Auu, const double *Auv, const double *Avu,
+                             const double *Avv, const double *bu, const double *bv, const double *uvel,
+                             const double *vvel, double *resid_u, double *resid_v, double *L2_norm,
+                             double *L2_norm_relative) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_error.clear();
+    TRY(validate(nx, ny, is3d ? nz : 1, par, indx, act, Auu, Auv, Avu, Avv, bu, bv));
+    TRY(validate_indx(indx, is3d ? 27 : 9));
+    if (!uvel || !vvel || !resid_u || !resid_v || !L2_norm) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
+    const double *blocks[4] = {Auu, Auv, Avu, Avv};
+    TRY(sv.upload(make_geom(nx, ny, is3d ? nz : 1, par), is3d, indx, act, blocks, bu, bv, uvel, vvel));
+    double l2 = 0.0, l2b = 0.0;
+    TRY(sv.residual_vector(VX0_U, &l2, &l2b));
+    TRY(sv.download(VR_U, VR_V, resid_u, resid_v));
+    *L2_norm = l2;
+    if (L2_norm_relative) *L2_norm_relative = (l2b > 0.0) ? l2 / l2b : 0.0;  // :9886-9890
+    return CISMGPU_OK;
+}
+
+static int oneshot_resid_velo(bool is3d, int whichresid, int nx, int ny, int nz, const cismgpu_par_t *par,
+                              const double *uvel, const double *vvel, const double *usav, const double *vsav,
+                              double *resid_velo) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_error.clear();
+    if (!uvel || !vvel || !usav || !vsav || !resid_velo) return fail(CISMGPU_EINVAL, "null pointer argument");
+    TRY(validate(nx, ny, is3d ? nz : 1, par, uvel, uvel, uvel, uvel, uvel, uvel, uvel, uvel));
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
+    TRY(sv.set_geom(make_geom(nx, ny, is3d ? nz : 1, par), is3d));
+    TRY(sv.put_vec(VX_U, uvel));
+    TRY(sv.put_vec(VX_V, vvel));
+    TRY(sv.put_vec(VX0_U, usav));
+    TRY(sv.put_vec(VX0_V, vsav));
+    return sv.residual_velocity(whichresid, VX_U, VX0_U, resid_velo);
+}
+
 static int oneshot_global_sum(int nx, int ny, int nz, const cismgpu_par_t *par, const double *a1, const double *a2,
                               double *sum) {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -1280,6 +1400,36 @@ int cismgpu_global_sum_stagger(int nx, int ny, int nz, const cismgpu_par_t *par,
     return oneshot_global_sum(nx, ny, nz, par, arr1, arr2, sum);
 }
 
+int cismgpu_compute_residual_vector_3d(int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indxA_3d,
+                                       const int32_t *active_vertex, const double *Auu, const double *Auv,
+                                       const double *Avu, const double *Avv, const double *bu, const double *bv,
+                                       const double *uvel, const double *vvel, double *resid_u, double *resid_v,
+                                       double *L2_norm, double *L2_norm_relative) {
+    return oneshot_resid_vec(true, nx, ny, nz, par, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, bu, bv, uvel,
+                             vvel, resid_u, resid_v, L2_norm, L2_norm_relative);
+}
+
+int cismgpu_compute_residual_vector_2d(int nx, int ny, const cismgpu_par_t *par, const int32_t *indxA_2d,
+                                       const int32_t *active_vertex, const double *Auu, const double *Auv,
+                                       const double *Avu, const double *Avv, const double *bu, const double *bv,
+                                       const double *uvel, const double *vvel, double *resid_u, double *resid_v,
+                                       double *L2_norm, double *L2_norm_relative) {
+    return oneshot_resid_vec(false, nx, ny, 1, par, indxA_2d, active_vertex, Auu, Auv, Avu, Avv, bu, bv, uvel,
+                             vvel, resid_u, resid_v, L2_norm, L2_norm_relative);
+}
+
+int cismgpu_compute_residual_velocity_3d(int whichresid, int nx, int ny, int nz, const cismgpu_par_t *par,
+                                         const double *uvel, const double *vvel, const double *usav,
+                                         const double *vsav, double *resid_velo) {
+    return oneshot_resid_velo(true, whichresid, nx, ny, nz, par, uvel, vvel, usav, vsav, resid_velo);
+}
+
+int cismgpu_compute_residual_velocity_2d(int whichresid, int nx, int ny, const cismgpu_par_t *par,
+                                         const double *uvel, const double *vvel, const double *usav,
+                                         const double *vsav, double *resid_velo) {
+    return oneshot_resid_velo(false, whichresid, nx, ny, 1, par, uvel, vvel, usav, vsav, resid_velo);
+}
+
 int cismgpu_solver_create(cismgpu_solver_t **out, int dims, int nx, int ny, int nz, const cismgpu_par_t *par,
                           const int32_t *indxA, const int32_t *active_vertex, const double *Auu, const double *Auv,
                           const double *Avu, const double *Avv, const double *bu, const double *bv,
@@ -1446,6 +1596,49 @@ int cismgpu_solver_get_x(cismgpu_solver_t *h, double *xu, double *xv) {
     std::lock_guard<std::mutex> lk(h->mu);
     if (h->in_batch) CU(cudaStreamSynchronize(h->batch_stream));  // the batch may be writing x
     return h->sv.download(VX_U, VX_V, xu, xv);
+}
+
+int cismgpu_solver_set_system(cismgpu_solver_t *h, const double *Auu, const double *Auv, const double *Avu,
+                              const double *Avv, const double *bu, const double *bv, int x0_from_solution) {
+    g_last_error.clear();
+    if (!h || !Auu || !Auv || !Avu || !Avv || !bu || !bv) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
+    Solver &sv = h->sv;
+    if (x0_from_solution && sv.x_current) {
+        const Ptrs p = sv.ptrs();
+        CU(cudaMemcpyAsync(p.x0u, p.xu, 2 * sv.nvec * sizeof(double), cudaMemcpyDeviceToDevice, sv.stream));
+    }
+    const double *blocks[4] = {Auu, Auv, Avu, Avv};
+    TRY(sv.put_system(blocks, bu, bv));
+    sv.x_current = false;
+    CU(cudaStreamSynchronize(sv.stream));  // the caller's arrays may be reused on return
+    return CISMGPU_OK;
+}
+
+int cismgpu_solver_residual_vector(cismgpu_solver_t *h, double *resid_u, double *resid_v, double *L2_norm,
+                                   double *L2_norm_relative) {
+    g_last_error.clear();
+    if (!h || !L2_norm || (!resid_u) != (!resid_v)) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
+    Solver &sv = h->sv;
+    double l2 = 0.0, l2b = 0.0;
+    TRY(sv.residual_vector(sv.x_current ? VX_U : VX0_U, &l2, &l2b));
+    if (resid_u) TRY(sv.download(VR_U, VR_V, resid_u, resid_v));
+    *L2_norm = l2;
+    if (L2_norm_relative) *L2_norm_relative = (l2b > 0.0) ? l2 / l2b : 0.0;
+    return CISMGPU_OK;
+}
+
+int cismgpu_solver_residual_velocity(cismgpu_solver_t *h, int whichresid, double *resid_velo) {
+    g_last_error.clear();
+    if (!h || !resid_velo) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
+    Solver &sv = h->sv;
+    if (!sv.x_current) return fail(CISMGPU_EINVAL, "no solve since the system was set");
+    return sv.residual_velocity(whichresid, VX_U, VX0_U, resid_velo);
 }
 
 int cismgpu_solver_profile(cismgpu_solver_t *h, int enable) {

@@ -104,6 +104,8 @@ struct SolveState {
     int niters;
     int checks;                               // number of residual checks done
     unsigned int ticket[4];                   // last-CTA tickets, one per concurrent reduction slot
+    unsigned long long maxbits;               // residual velocity: bits of the largest difference so far
+    unsigned long long count;                 // residual velocity (mean): nonzero speeds counted
 };
 
 enum Epi {
@@ -115,6 +117,8 @@ enum Epi {
     EPI_CG_RHO0,      // rho_old = S0
     EPI_CG_FIRST,     // sigma = S0; alpha = rho_old/sigma; NaN -> fail
     EPI_CG_ITER,      // rho = S0; delta = S1; beta, sigma, alpha, rho_old; NaN -> fail
+    EPI_RESID_VEC,    // err = sqrt(S0) = |Ax - b|; L2_rhs = sqrt(S1) = |b| (owned active)
+    EPI_SUM,          // rho = S0
 };
 
 }  // namespace cismgpu

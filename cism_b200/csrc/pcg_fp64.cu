@@ -65,6 +65,13 @@ __device__ void epilogue(SolveState *st, int epi, int iter, double S0, double S1
         if (st->alpha != st->alpha) { st->status = CISMGPU_EBREAKDOWN_ALPHA; st->done = 1; st->niters = iter; }
         break;
     }
+    case EPI_RESID_VEC:   // glissade_velo_higher.F90:9858-9859, :9883-9884
+        st->err = sqrt(S0);
+        st->L2_rhs = sqrt(S1);
+        break;
+    case EPI_SUM:
+        st->rho = S0;
+        break;
     default:
         break;
     }
@@ -388,6 +395,76 @@ __global__ void __launch_bounds__(kBlock) k_precond(Geom g, int kind, const doub
         }
     }
     if (MODE == PRE_STD || MODE == PRE_CG_FIRST) reduce_and_finish<1>(rc, s0, s0);
+}
+
+// ---------------------------------------------------------------------------
+// nonlinear-iteration diagnostics (glissade_velo_higher.F90)
+// ---------------------------------------------------------------------------
+// compute_residual_vector_{2d,3d} (:9502-9689 / :9693-9894), after y = A u (k_mv MV_PLAIN,
+// the same statements and order): resid = y - b on owned active vertices, 0 elsewhere;
+// S0 = sum of resid_u^2 + resid_v^2, S1 = sum of bu^2 + bv^2 over owned active vertices (the
+// global sums' fixed tree).
+__global__ void __launch_bounds__(kBlock) k_resid_vec(Geom g, const int32_t *__restrict__ act,
+                                                      const double *__restrict__ yu, const double *__restrict__ yv,
+                                                      const double *__restrict__ bu, const double *__restrict__ bv,
+                                                      double *__restrict__ ru, double *__restrict__ rv, RedCtx rc) {
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    DD s0{0.0, 0.0}, s1{0.0, 0.0};
+    if (q < g.NQ) {
+        int i, j;
+        col_of(g, q, i, j);
+        const bool on = owned(g, i, j) && act[q] != 0;
+        for (int k = 0; k < g.nz; ++k) {
+            const long long e = (long long)k * g.NQ + q;
+            if (on) {
+                const double r1 = __dsub_rn(yu[e], bu[e]), r2 = __dsub_rn(yv[e], bv[e]);
+                ru[e] = r1;
+                rv[e] = r2;
+                s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(r1, r1), __dmul_rn(r2, r2)));
+                s1 = dd_add_d(s1, __dadd_rn(__dmul_rn(bu[e], bu[e]), __dmul_rn(bv[e], bv[e])));
+            } else {
+                ru[e] = 0.0;
+                rv[e] = 0.0;
+            }
+        }
+    }
+    reduce_and_finish<2>(rc, s0, s1);
+}
+
+// compute_residual_velocity_{2d,3d} (:10188-10310 / :10314-10446) over owned vertices and
+// levels k < kmax: speed = sqrt(u**2 + v**2); where speed /= 0, d = abs((oldspeed-speed)/speed).
+// Max modes: the largest d, as atomicMax on the bits of a non-negative double (a NaN d never
+// wins, as "d > resid_velo" is false for it; the state's maxbits starts at +0).  Mean mode: the
+// count and the sum of d (the global sums' fixed tree; EPI_SUM).
+__global__ void __launch_bounds__(kBlock) k_resid_velo(Geom g, int kmax, int mean, const double *__restrict__ u,
+                                                       const double *__restrict__ v, const double *__restrict__ us,
+                                                       const double *__restrict__ vs, RedCtx rc) {
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    DD s0{0.0, 0.0};
+    unsigned long long cnt = 0;
+    if (q < g.NQ) {
+        int i, j;
+        col_of(g, q, i, j);
+        if (owned(g, i, j))
+            for (int k = 0; k < kmax; ++k) {
+                const long long e = (long long)k * g.NQ + q;
+                const double speed = __dsqrt_rn(__dadd_rn(__dmul_rn(u[e], u[e]), __dmul_rn(v[e], v[e])));
+                if (speed != 0.0) {
+                    const double old = __dsqrt_rn(__dadd_rn(__dmul_rn(us[e], us[e]), __dmul_rn(vs[e], vs[e])));
+                    const double d = fabs(__ddiv_rn(__dsub_rn(old, speed), speed));
+                    if (mean) {
+                        ++cnt;
+                        s0 = dd_add_d(s0, d);
+                    } else if (d > 0.0) {
+                        atomicMax(&rc.st->maxbits, (unsigned long long)__double_as_longlong(d));
+                    }
+                }
+            }
+    }
+    if (mean) {
+        if (cnt) atomicAdd(&rc.st->count, cnt);
+        reduce_and_finish<1>(rc, s0, s0);
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -176,6 +176,49 @@ int cismgpu_global_sum_stagger_noalloc(int nx, int ny, int nz, const cismgpu_par
                                        double *sum_dev, void *cuda_stream);
 
 /* ------------------------------------------------------------------------
+ * Nonlinear-iteration diagnostics (glissade_velo_higher.F90), one-shot form.
+ * ------------------------------------------------------------------------ */
+
+/* whichresid of compute_residual_velocity (HO_RESID_*, libglide/glide_types.F90:321-325) */
+#define CISMGPU_RESID_MAXU          0  /* max relative speed change, all levels                */
+#define CISMGPU_RESID_MAXU_NO_UBAS  1  /* ... without the bed level (3D)                        */
+#define CISMGPU_RESID_MEANU         2  /* mean relative speed change, without the bed level (3D) */
+
+/* Replaces compute_residual_vector_3d (glissade_velo_higher.F90:9693-9894):
+ * resid = A*uvel - b on owned active vertices (0 elsewhere, same matvec statements as
+ * matvec_multiply_structured_3d), L2_norm = |resid| and, if L2_norm_relative is not NULL,
+ * L2_norm/|b| over owned active vertices (0 when |b| = 0).  Sums use the global sums' fixed
+ * tree.  Arrays in the caller's layout as for the solver calls; itest/jtest/rtest (diagnostic
+ * prints only) are not taken. */
+int cismgpu_compute_residual_vector_3d(int nx, int ny, int nz, const cismgpu_par_t *par,
+                                       const int32_t *indxA_3d, const int32_t *active_vertex,
+                                       const double *Auu, const double *Auv, const double *Avu,
+                                       const double *Avv, const double *bu, const double *bv,
+                                       const double *uvel, const double *vvel, double *resid_u,
+                                       double *resid_v, double *L2_norm, double *L2_norm_relative);
+
+/* Replaces compute_residual_vector_2d (glissade_velo_higher.F90:9502-9689). */
+int cismgpu_compute_residual_vector_2d(int nx, int ny, const cismgpu_par_t *par, const int32_t *indxA_2d,
+                                       const int32_t *active_vertex, const double *Auu, const double *Auv,
+                                       const double *Avu, const double *Avv, const double *bu,
+                                       const double *bv, const double *uvel, const double *vvel,
+                                       double *resid_u, double *resid_v, double *L2_norm,
+                                       double *L2_norm_relative);
+
+/* Replaces compute_residual_velocity_3d (glissade_velo_higher.F90:10314-10446): over owned
+ * vertices, the largest (or, for CISMGPU_RESID_MEANU, the mean) of |(|usav| - |u|)/|u|| where
+ * |u| = sqrt(uvel**2 + vvel**2) /= 0.  Max modes are exact; the mean's sum uses the global
+ * sums' fixed tree.  (The reference's location of the maximum is diagnostic output only.) */
+int cismgpu_compute_residual_velocity_3d(int whichresid, int nx, int ny, int nz, const cismgpu_par_t *par,
+                                         const double *uvel, const double *vvel, const double *usav,
+                                         const double *vsav, double *resid_velo);
+
+/* Replaces compute_residual_velocity_2d (glissade_velo_higher.F90:10188-10310). */
+int cismgpu_compute_residual_velocity_2d(int whichresid, int nx, int ny, const cismgpu_par_t *par,
+                                         const double *uvel, const double *vvel, const double *usav,
+                                         const double *vsav, double *resid_velo);
+
+/* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps
  * them, and all Krylov state, in HBM, so repeated solves (benchmarking, the
@@ -278,6 +321,23 @@ int cismgpu_server_destroy(cismgpu_server_t *s); /* finishes the queued requests
 
 /* Copy the current solution (caller's Fortran layout, halo entries included) to host memory. */
 int cismgpu_solver_get_x(cismgpu_solver_t *s, double *xu, double *xv);
+
+/* The Picard loop on a handle, with A, b and x kept in HBM between nonlinear iterations:
+ *  cismgpu_solver_set_system  new coefficients and right-hand side for the same geometry and
+ *                             active vertices; with x0_from_solution != 0 and a solve done since
+ *                             the last system, the next initial guess is that solution (on the
+ *                             device: nothing crosses PCIe but A and b);
+ *  cismgpu_solver_residual_vector   compute_residual_vector of the current velocity (the last
+ *                             solution, or the stored initial guess if no solve ran since the
+ *                             system was set) with the current A and b; resid_u/resid_v may be
+ *                             NULL (norms only), L2_norm_relative may be NULL;
+ *  cismgpu_solver_residual_velocity compute_residual_velocity between the last solution and
+ *                             the initial guess that solve started from (EINVAL before a solve). */
+int cismgpu_solver_set_system(cismgpu_solver_t *s, const double *Auu, const double *Auv, const double *Avu,
+                              const double *Avv, const double *bu, const double *bv, int x0_from_solution);
+int cismgpu_solver_residual_vector(cismgpu_solver_t *s, double *resid_u, double *resid_v, double *L2_norm,
+                                   double *L2_norm_relative);
+int cismgpu_solver_residual_velocity(cismgpu_solver_t *s, int whichresid, double *resid_velo);
 
 /* Per-kernel CUDA-event timing of the structured matvec launches (off by default).
  * read: total device milliseconds, launch count, and algorithmic bytes per launch

@@ -58,6 +58,10 @@ def lib() -> ctypes.CDLL:
         L.oracle_global_sum.restype = dbl
         L.oracle_easy_sia.argtypes = [i, i, i, d, d, d, d]
         L.oracle_precond_apply.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, i, d, d, d, d]
+        L.oracle_compute_residual_vector.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, d, d, d, d, d, d,
+                                                     P(dbl), P(dbl), i]
+        L.oracle_compute_residual_velocity.argtypes = [i, i, i, i, i, P(_Par), d, d, d, d, i]
+        L.oracle_compute_residual_velocity.restype = dbl
         L.oracle_exact_sum.argtypes = [d, ctypes.c_long]
         L.oracle_exact_sum.restype = dbl
         _lib = L
@@ -150,6 +154,30 @@ def precond_apply(prob, precond: int, ru, rv, zu0=None, zv0=None):
                                     precond, _p(np.ascontiguousarray(ru)), _p(np.ascontiguousarray(rv)), _p(zu),
                                     _p(zv))
     return st, zu, zv
+
+
+def residual_vector(prob, uvel, vvel, summode: int = SUM_SEQ):
+    """compute_residual_vector_{2d,3d} of prob's system at (uvel, vvel):
+    (resid_u, resid_v, L2_norm, L2_norm_relative)."""
+    is3d = prob.kind == "3d"
+    ru, rv = np.empty_like(prob.bu), np.empty_like(prob.bv)
+    l2, l2r = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    par = _par(prob.par)
+    lib().oracle_compute_residual_vector(int(is3d), prob.nx, prob.ny, prob.nz if is3d else 1, ctypes.byref(par),
+                                         _p(indx3() if is3d else indx2()), _p(prob.active_vertex), _p(prob.Auu),
+                                         _p(prob.Auv), _p(prob.Avu), _p(prob.Avv), _p(prob.bu), _p(prob.bv),
+                                         _p(np.ascontiguousarray(uvel)), _p(np.ascontiguousarray(vvel)), _p(ru),
+                                         _p(rv), ctypes.byref(l2), ctypes.byref(l2r), summode)
+    return ru, rv, l2.value, l2r.value
+
+
+def residual_velocity(prob, whichresid: int, uvel, vvel, usav, vsav, summode: int = SUM_SEQ) -> float:
+    """compute_residual_velocity_{2d,3d} on prob's grid."""
+    is3d = prob.kind == "3d"
+    par = _par(prob.par)
+    arrs = [_p(np.ascontiguousarray(a, dtype=np.float64)) for a in (uvel, vvel, usav, vsav)]
+    return lib().oracle_compute_residual_velocity(int(is3d), whichresid, prob.nx, prob.ny, prob.nz if is3d else 1,
+                                                  ctypes.byref(par), *arrs, summode)
 
 
 def exact_sum(a) -> float:

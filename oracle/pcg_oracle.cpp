@@ -28,6 +28,11 @@
 //     tridiag_solver_global_3d        :4662-4913  (one task: the particular solution)
 //     tridiag_solver_local_2d         :4917-5100
 //     tridiag_solver_global_2d        :5104-5524  (tasks_rc = 1 branch, :5495-5497)
+//   libglissade/glissade_velo_higher.F90
+//     compute_residual_vector_2d      :9502-9689
+//     compute_residual_vector_3d      :9693-9894
+//     compute_residual_velocity_2d    :10188-10310
+//     compute_residual_velocity_3d    :10314-10446
 //     matvec_multiply_structured_3d   :5528-5652
 //     matvec_multiply_structured_2d   :5656-5773
 //     easy_sia_solver                 :5777-5866
@@ -843,6 +848,82 @@ int chrongear(bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const
     return status;
 }
 
+// compute_residual_vector_{2d,3d}: resid = A u - b on owned active vertices (the matvec
+// statements of matvec_multiply_structured_*, which the residual loops repeat), the L2 norm
+// of resid and |b| over owned active vertices through the global sum of the given mode.
+void resid_vector(const Ctx &c, bool is3d, const double *Auu, const double *Auv, const double *Avu,
+                  const double *Avv, const Vec &bu, const Vec &bv, const Vec &u, const Vec &v, Vec &ru, Vec &rv,
+                  double *L2, double *L2rel) {
+    const Geom &g = c.g;
+    const cismgpu_par_t &p = c.par;
+    const long n = g.ntot();
+    Vec yu(n, 0.0), yv(n, 0.0);
+    if (is3d) matvec3(c, Auu, Auv, Avu, Avv, u, v, yu, yv);
+    else matvec2(c, Auu, Auv, Avu, Avv, u, v, yu, yv);
+    ru.assign(n, 0.0);
+    rv.assign(n, 0.0);
+    Vec wu(n, 0.0), wv(n, 0.0), bu2(n, 0.0), bv2(n, 0.0);
+    for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+        for (int i = p.staggered_ilo; i <= p.staggered_ihi; ++i) {
+            if (!c.act(i, j)) continue;
+            for (int k = 1; k <= g.nz; ++k) {
+                const long e = g.v3(k, i, j);
+                ru[e] = yu[e] - bu[e];
+                rv[e] = yv[e] - bv[e];
+                wu[e] = ru[e] * ru[e];
+                wv[e] = rv[e] * rv[e];
+                bu2[e] = bu[e] * bu[e];
+                bv2[e] = bv[e] * bv[e];
+            }
+        }
+    *L2 = std::sqrt(global_sum(c, wu, wv));
+    const double L2b = std::sqrt(global_sum(c, bu2, bv2));
+    *L2rel = (L2b > 0.0) ? *L2 / L2b : 0.0;
+}
+
+// compute_residual_velocity_{2d,3d}: whichresid 1 (max, bed left out in 3D), 2 (mean, bed
+// left out in 3D), anything else (max over all levels).  The mean's sum follows the mode:
+// SEQ is the reference's j, i, k order; DDTREE and EXACT as the global sums.
+double resid_velocity(const Ctx &c, bool is3d, int whichresid, const Vec &u, const Vec &v, const Vec &us,
+                      const Vec &vs) {
+    const Geom &g = c.g;
+    const cismgpu_par_t &p = c.par;
+    const bool mean = whichresid == CISMGPU_RESID_MEANU;
+    const int kmax = (is3d && (whichresid == CISMGPU_RESID_MAXU_NO_UBAS || mean)) ? g.nz - 1 : g.nz;
+    auto diff = [&](long e, double &d) {
+        const double speed = std::sqrt(u[e] * u[e] + v[e] * v[e]);
+        if (speed == 0.0) return false;
+        const double old = std::sqrt(us[e] * us[e] + vs[e] * vs[e]);
+        d = std::fabs((old - speed) / speed);
+        return true;
+    };
+    double r = 0.0;
+    if (!mean) {
+        for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+            for (int i = p.staggered_ilo; i <= p.staggered_ihi; ++i)
+                for (int k = 1; k <= kmax; ++k) {
+                    double d;
+                    if (diff(g.v3(k, i, j), d) && d > r) r = d;
+                }
+        return r;
+    }
+    long count = 0;
+    Vec w(g.ntot(), 0.0), z(g.ntot(), 0.0);
+    for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+        for (int i = p.staggered_ilo; i <= p.staggered_ihi; ++i)
+            for (int k = 1; k <= kmax; ++k) {
+                double d;
+                if (diff(g.v3(k, i, j), d)) {
+                    ++count;
+                    r = r + d;
+                    w[g.v3(k, i, j)] = d;
+                }
+            }
+    if (c.summode != ORACLE_SUM_SEQ) r = global_sum(c, w, z);  // the other modes' order (d + 0 = d)
+    if (count > 0) r = r / (double)count;
+    return r;
+}
+
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -963,6 +1044,32 @@ int oracle_precond_apply(int is3d, int nx, int ny, int nz, const cismgpu_par_t *
     std::memcpy(zu, za.data(), n * sizeof(double));
     std::memcpy(zv, zb.data(), n * sizeof(double));
     return CISMGPU_OK;
+}
+
+// compute_residual_vector_{2d,3d} (is3d: (nz,nx-1,ny-1) arrays, indx = indxA_3d; else 2D, indxA_2d)
+int oracle_compute_residual_vector(int is3d, int nx, int ny, int nz, const cismgpu_par_t *par,
+                                   const int32_t *indx, const int32_t *active_vertex, const double *Auu,
+                                   const double *Auv, const double *Avu, const double *Avv, const double *bu,
+                                   const double *bv, const double *uvel, const double *vvel, double *resid_u,
+                                   double *resid_v, double *L2, double *L2rel, int summode) {
+    Ctx c{Geom{is3d ? nz : 1, nx - 1, ny - 1}, *par, summode, is3d ? nullptr : indx, is3d ? indx : nullptr,
+          active_vertex};
+    const long n = c.g.ntot();
+    Vec b1(bu, bu + n), b2(bv, bv + n), x1(uvel, uvel + n), x2(vvel, vvel + n), r1, r2;
+    resid_vector(c, is3d != 0, Auu, Auv, Avu, Avv, b1, b2, x1, x2, r1, r2, L2, L2rel);
+    std::memcpy(resid_u, r1.data(), n * sizeof(double));
+    std::memcpy(resid_v, r2.data(), n * sizeof(double));
+    return 0;
+}
+
+// compute_residual_velocity_{2d,3d}
+double oracle_compute_residual_velocity(int is3d, int whichresid, int nx, int ny, int nz,
+                                        const cismgpu_par_t *par, const double *uvel, const double *vvel,
+                                        const double *usav, const double *vsav, int summode) {
+    Ctx c{Geom{is3d ? nz : 1, nx - 1, ny - 1}, *par, summode, nullptr, nullptr, nullptr};
+    const long n = c.g.ntot();
+    Vec u(uvel, uvel + n), v(vvel, vvel + n), us(usav, usav + n), vs(vsav, vsav + n);
+    return resid_velocity(c, is3d != 0, whichresid, u, v, us, vs);
 }
 
 // exact correctly-rounded sum of n doubles

@@ -196,6 +196,55 @@ def test_tridiag_precond_zero_pivot():
     assert oracle.pcg("standard", Q, 4, maxiters=3)[0] == 9
 
 
+@pytest.mark.parametrize("kind", ["3d", "2d"])
+def test_residual_vector_matches_matvec_minus_b(kind):
+    """compute_residual_vector: A u - b on owned active vertices (zero elsewhere) and its
+    L2 norm and |b| over owned active vertices."""
+    P = problems.slab_3d(seed=31, boundary_ice=True, bc="periodic") if kind == "3d" else \
+        problems.slab_2d(seed=31, boundary_ice=True, bc="outflow")
+    rng = np.random.default_rng(4)
+    u, v = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bv.shape)
+    ru, rv, l2, l2r = oracle.residual_vector(P, u, v)
+    yu, yv = oracle.matvec(P, u, v)
+    m = np.zeros(P.active_vertex.shape, bool)
+    J, I = _owned(P)
+    m[J[0]:J[-1] + 1, I[0]:I[-1] + 1] = P.active_vertex[J[0]:J[-1] + 1, I[0]:I[-1] + 1] != 0
+    mask = m[..., None] if kind == "3d" else m
+    np.testing.assert_array_equal(ru, np.where(mask, yu - P.bu, 0.0))
+    np.testing.assert_array_equal(rv, np.where(mask, yv - P.bv, 0.0))
+    want = math.sqrt(math.fsum((ru * ru + rv * rv).ravel()))
+    bnorm = math.sqrt(math.fsum(np.where(mask, P.bu * P.bu + P.bv * P.bv, 0.0).ravel()))
+    assert abs(l2 - want) <= 1e-13 * want and abs(l2r - want / bnorm) <= 1e-13 * want / bnorm
+
+
+@pytest.mark.parametrize("which", [0, 1, 2, 3])
+@pytest.mark.parametrize("kind", ["3d", "2d"])
+def test_residual_velocity_matches_numpy(kind, which):
+    """compute_residual_velocity: max (or mean) of |(|u_old| - |u|)/|u|| over owned vertices
+    where |u| /= 0; 1 and 2 leave the bed level out in 3D; other values take the default."""
+    P = problems.slab_3d(seed=32) if kind == "3d" else problems.slab_2d(seed=32)
+    rng = np.random.default_rng(5)
+    u, v = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bv.shape)
+    u[..., 0] = v[..., 0] = 0.0  # zero speeds are skipped
+    us, vs = u * (1 + 0.1 * rng.random(u.shape)), v * (1 - 0.1 * rng.random(v.shape))
+    J, I = _owned(P)
+    sl = (slice(J[0], J[-1] + 1), slice(I[0], I[-1] + 1))
+    su, sv_, so_u, so_v = u[sl], v[sl], us[sl], vs[sl]
+    if kind == "3d" and which in (1, 2):
+        su, sv_, so_u, so_v = su[..., :-1], sv_[..., :-1], so_u[..., :-1], so_v[..., :-1]
+    speed = np.sqrt(su * su + sv_ * sv_)
+    old = np.sqrt(so_u * so_u + so_v * so_v)
+    nz = speed != 0
+    d = np.abs((old[nz] - speed[nz]) / speed[nz])
+    got = oracle.residual_velocity(P, which, u, v, us, vs)
+    if which == 2:
+        assert abs(got - math.fsum(d) / d.size) <= 1e-14 * got
+        for mode in (oracle.SUM_DDTREE, oracle.SUM_EXACT):
+            assert abs(oracle.residual_velocity(P, which, u, v, us, vs, summode=mode) - got) <= 1e-14 * got
+    else:
+        assert got == d.max()
+
+
 def test_exact_sum_is_correctly_rounded():
     rng = np.random.default_rng(7)
     for trial in range(20):
