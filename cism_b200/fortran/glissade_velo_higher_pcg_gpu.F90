@@ -8,6 +8,11 @@
 !   reference argument list, intents and meaning:
 !     pcg_solver_standard_2d   (:67-823)     pcg_solver_standard_3d   (:827-1537)
 !     pcg_solver_chrongear_2d  (:1541-2628)  pcg_solver_chrongear_3d  (:2632-3594)
+!   and, for the steps around the solve in the Picard loop of
+!   libglissade/glissade_velo_higher.F90 (module procedures there, so a caller
+!   takes these with "use glissade_velo_higher_pcg_gpu, only: gpu_x => x"):
+!     compute_residual_vector_2d   (:9502-9689)    compute_residual_vector_3d   (:9693-9894)
+!     compute_residual_velocity_2d (:10188-10310)  compute_residual_velocity_3d (:10314-10446)
 !   A nonzero library status is reported the way the reference reports a failed
 !   solve: write_log(message, GM_FATAL).
 !
@@ -33,6 +38,8 @@
     private
     public :: pcg_solver_standard_2d, pcg_solver_standard_3d, &
               pcg_solver_chrongear_2d, pcg_solver_chrongear_3d, &
+              compute_residual_vector_2d, compute_residual_vector_3d, &
+              compute_residual_velocity_2d, compute_residual_velocity_3d, &
               cismgpu_use_mixed_precision
 
     type, bind(C) :: cismgpu_par_t
@@ -113,6 +120,48 @@
        type(c_ptr) function c_last_error() bind(C, name="cismgpu_last_error")
          import :: c_ptr
        end function c_last_error
+
+       integer(c_int) function c_resid_vector_3d(nx, ny, nz, par, indxA_3d, active_vertex, Auu, Auv, Avu, Avv, &
+            bu, bv, uvel, vvel, resid_u, resid_v, L2_norm, L2_norm_relative)                          &
+            bind(C, name="cismgpu_compute_residual_vector_3d")
+         import :: c_int, c_double, c_int32_t, c_ptr, cismgpu_par_t
+         integer(c_int), value :: nx, ny, nz
+         type(cismgpu_par_t), intent(in) :: par
+         integer(c_int32_t), intent(in) :: indxA_3d(*), active_vertex(*)
+         real(c_double), intent(in) :: Auu(*), Auv(*), Avu(*), Avv(*), bu(*), bv(*), uvel(*), vvel(*)
+         real(c_double), intent(out) :: resid_u(*), resid_v(*), L2_norm
+         type(c_ptr), value :: L2_norm_relative
+       end function c_resid_vector_3d
+
+       integer(c_int) function c_resid_vector_2d(nx, ny, par, indxA_2d, active_vertex, Auu, Auv, Avu, Avv, &
+            bu, bv, uvel, vvel, resid_u, resid_v, L2_norm, L2_norm_relative)                      &
+            bind(C, name="cismgpu_compute_residual_vector_2d")
+         import :: c_int, c_double, c_int32_t, c_ptr, cismgpu_par_t
+         integer(c_int), value :: nx, ny
+         type(cismgpu_par_t), intent(in) :: par
+         integer(c_int32_t), intent(in) :: indxA_2d(*), active_vertex(*)
+         real(c_double), intent(in) :: Auu(*), Auv(*), Avu(*), Avv(*), bu(*), bv(*), uvel(*), vvel(*)
+         real(c_double), intent(out) :: resid_u(*), resid_v(*), L2_norm
+         type(c_ptr), value :: L2_norm_relative
+       end function c_resid_vector_2d
+
+       integer(c_int) function c_resid_velocity_3d(whichresid, nx, ny, nz, par, uvel, vvel, usav, vsav, &
+            resid_velo) bind(C, name="cismgpu_compute_residual_velocity_3d")
+         import :: c_int, c_double, cismgpu_par_t
+         integer(c_int), value :: whichresid, nx, ny, nz
+         type(cismgpu_par_t), intent(in) :: par
+         real(c_double), intent(in) :: uvel(*), vvel(*), usav(*), vsav(*)
+         real(c_double), intent(out) :: resid_velo
+       end function c_resid_velocity_3d
+
+       integer(c_int) function c_resid_velocity_2d(whichresid, nx, ny, par, uvel, vvel, usav, vsav, &
+            resid_velo) bind(C, name="cismgpu_compute_residual_velocity_2d")
+         import :: c_int, c_double, cismgpu_par_t
+         integer(c_int), value :: whichresid, nx, ny
+         type(cismgpu_par_t), intent(in) :: par
+         real(c_double), intent(in) :: uvel(*), vvel(*), usav(*), vsav(*)
+         real(c_double), intent(out) :: resid_velo
+       end function c_resid_velocity_2d
     end interface
 
   contains
@@ -258,5 +307,84 @@
                                     bu, bv, xu, xv, precond, linear_solve_ncheck, tolerance, maxiters, &
                                     err, niters, itest, jtest, rtest))
     end subroutine pcg_solver_chrongear_2d
+
+    !-----------------------------------------------------------------------
+    ! indxA_3d(iA,jA,kA) = 1 + (iA+1) + 3*(jA+1) + 9*(kA+1) and indxA_2d(iA,jA) = 1 + (iA+1) + 3*(jA+1):
+    ! the module maps of glissade_velo_higher (glissade_velo_higher.F90:608-640) these routines use.
+    subroutine compute_residual_vector_3d(nx, ny, nz, parallel, itest, jtest, rtest, active_vertex, &
+                                          Auu, Auv, Avu, Avv, bu, bv, uvel, vvel, resid_u, resid_v, &
+                                          L2_norm, L2_norm_relative)
+      integer, intent(in) :: nx, ny, nz
+      type(parallel_type), intent(in) :: parallel
+      integer, intent(in) :: itest, jtest, rtest
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      real(dp), dimension(27,nz,nx-1,ny-1), intent(in) :: Auu, Auv, Avu, Avv
+      real(dp), dimension(nz,nx-1,ny-1), intent(in) :: bu, bv, uvel, vvel
+      real(dp), dimension(nz,nx-1,ny-1), intent(out) :: resid_u, resid_v
+      real(dp), intent(out) :: L2_norm
+      real(dp), intent(out), optional :: L2_norm_relative
+      integer(c_int32_t) :: act(nx-1,ny-1), indx3(27)
+      real(c_double), target :: rel
+      integer :: m
+      act = merge(1, 0, active_vertex)
+      indx3 = [(m, m = 1, 27)]
+      if (present(L2_norm_relative)) then
+         call check(c_resid_vector_3d(nx, ny, nz, to_c(parallel), indx3, act, Auu, Auv, Avu, Avv, bu, bv, &
+                                      uvel, vvel, resid_u, resid_v, L2_norm, c_loc(rel)))
+         L2_norm_relative = rel
+      else
+         call check(c_resid_vector_3d(nx, ny, nz, to_c(parallel), indx3, act, Auu, Auv, Avu, Avv, bu, bv, &
+                                      uvel, vvel, resid_u, resid_v, L2_norm, c_null_ptr))
+      endif
+    end subroutine compute_residual_vector_3d
+
+    !-----------------------------------------------------------------------
+    subroutine compute_residual_vector_2d(nx, ny, parallel, itest, jtest, rtest, active_vertex, &
+                                          Auu, Auv, Avu, Avv, bu, bv, uvel, vvel, resid_u, resid_v, &
+                                          L2_norm, L2_norm_relative)
+      integer, intent(in) :: nx, ny
+      type(parallel_type), intent(in) :: parallel
+      integer, intent(in) :: itest, jtest, rtest
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      real(dp), dimension(nx-1,ny-1,9), intent(in) :: Auu, Auv, Avu, Avv
+      real(dp), dimension(nx-1,ny-1), intent(in) :: bu, bv, uvel, vvel
+      real(dp), dimension(nx-1,ny-1), intent(out) :: resid_u, resid_v
+      real(dp), intent(out) :: L2_norm
+      real(dp), intent(out), optional :: L2_norm_relative
+      integer(c_int32_t) :: act(nx-1,ny-1), indx2(9)
+      real(c_double), target :: rel
+      integer :: m
+      act = merge(1, 0, active_vertex)
+      indx2 = [(m, m = 1, 9)]
+      if (present(L2_norm_relative)) then
+         call check(c_resid_vector_2d(nx, ny, to_c(parallel), indx2, act, Auu, Auv, Avu, Avv, bu, bv, &
+                                      uvel, vvel, resid_u, resid_v, L2_norm, c_loc(rel)))
+         L2_norm_relative = rel
+      else
+         call check(c_resid_vector_2d(nx, ny, to_c(parallel), indx2, act, Auu, Auv, Avu, Avv, bu, bv, &
+                                      uvel, vvel, resid_u, resid_v, L2_norm, c_null_ptr))
+      endif
+    end subroutine compute_residual_vector_2d
+
+    !-----------------------------------------------------------------------
+    ! The arrays are (nz, nx-1, ny-1) as everywhere on this path.
+    subroutine compute_residual_velocity_3d(whichresid, parallel, uvel, vvel, usav, vsav, resid_velo)
+      integer, intent(in) :: whichresid
+      type(parallel_type), intent(in) :: parallel
+      real(dp), dimension(:,:,:), intent(in) :: uvel, vvel, usav, vsav
+      real(dp), intent(out) :: resid_velo
+      call check(c_resid_velocity_3d(whichresid, size(uvel,2) + 1, size(uvel,3) + 1, size(uvel,1), &
+                                     to_c(parallel), uvel, vvel, usav, vsav, resid_velo))
+    end subroutine compute_residual_velocity_3d
+
+    !-----------------------------------------------------------------------
+    subroutine compute_residual_velocity_2d(whichresid, parallel, uvel, vvel, usav, vsav, resid_velo)
+      integer, intent(in) :: whichresid
+      type(parallel_type), intent(in) :: parallel
+      real(dp), dimension(:,:), intent(in) :: uvel, vvel, usav, vsav
+      real(dp), intent(out) :: resid_velo
+      call check(c_resid_velocity_2d(whichresid, size(uvel,1) + 1, size(uvel,2) + 1, to_c(parallel), &
+                                     uvel, vvel, usav, vsav, resid_velo))
+    end subroutine compute_residual_velocity_2d
 
   end module glissade_velo_higher_pcg_gpu
