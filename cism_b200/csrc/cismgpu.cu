@@ -265,10 +265,10 @@ struct Solver {
         RedCtx rc1{partials.as<DD>(), st, EPI_RESID_VEC, 0};
         const unsigned nb = nblocks(g.NQ);
         if (is3d)
-            k_mv<27, MV_PLAIN><<<nb, mv_threads<27>(), 0, s>>>(g, A.as<double>(), act.as<int32_t>(), xu, xv, p.zu, p.zv,
+            launch_mv<27, MV_PLAIN>(s, g, A.as<double>(), act.as<int32_t>(), xu, xv, p.zu, p.zv,
                                                               nullptr, nullptr, nullptr, nullptr, rc0);
         else
-            k_mv<9, MV_PLAIN><<<nb, mv_threads<9>(), 0, s>>>(g, A.as<double>(), act.as<int32_t>(), xu, xv, p.zu, p.zv,
+            launch_mv<9, MV_PLAIN>(s, g, A.as<double>(), act.as<int32_t>(), xu, xv, p.zu, p.zv,
                                                             nullptr, nullptr, nullptr, nullptr, rc0);
         k_resid_vec<<<nb, kBlock, 0, s>>>(g, act.as<int32_t>(), p.zu, p.zv, p.bu, p.bv, p.ru, p.rv, rc1);
         CU(cudaGetLastError());
@@ -515,7 +515,7 @@ int Solver::run_standard(int precond, int ncheck, double tol, int maxiters) {
     if (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL)
         TRY(tri_setup(precond));  // pcg_precond_init (:1083-1160 / :263-376)
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
-    k_mv<NCC, MV_PLAIN><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
+    launch_mv<NCC, MV_PLAIN>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
                                               nullptr, rc(EPI_NONE, 0));
     k_vec<OP_STD_INIT><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_L2RHS, 0));
     CU(cudaGetLastError());
@@ -525,13 +525,13 @@ int Solver::run_standard(int precond, int ncheck, double tol, int maxiters) {
         k_vec<OP_STD_D><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, iter));
         k_halo<<<hb, kBlock, 0, s>>>(gg, p.du, p.dv, st);
         TRY(timed([&] {
-            k_mv<NCC, MV_DQ><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr,
+            launch_mv<NCC, MV_DQ>(s, gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr,
                                                    nullptr, rc(EPI_STD_ETA2, iter));
         }));
         k_vec<OP_XR><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, iter));
         if (is_check(iter, ncheck)) {
             k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
-            k_mv<NCC, MV_RESID><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
+            launch_mv<NCC, MV_RESID>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
                                                       rc(EPI_CHECK, iter));
             CU(cudaGetLastError());
             int f = poll.after_check();
@@ -569,12 +569,12 @@ int Solver::run_chrongear(int precond, int ncheck, double tol, int maxiters) {
     k_vec<OP_DOT_BB><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_L2RHS, 0));
     // first pass (:3085-3290)
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
-    k_mv<NCC, MV_PLAIN><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
+    launch_mv<NCC, MV_PLAIN>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr,
                                               nullptr, rc(EPI_NONE, 1));
     k_vec<OP_CG_INIT><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, 1));
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
     TRY((apply_precond<NCC, PRE_CG_FIRST>(precond, p, rc(EPI_CG_RHO0, 1), p.du, p.dv)));
-    k_mv<NCC, MV_DQ><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr,
+    launch_mv<NCC, MV_DQ>(s, gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr,
                                            rc(EPI_CG_FIRST, 1));
     k_halo<<<hb, kBlock, 0, s>>>(gg, p.qu, p.qv, st);
     k_vec<OP_XR><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, 1));
@@ -583,13 +583,13 @@ int Solver::run_chrongear(int precond, int ncheck, double tol, int maxiters) {
     for (int iter = 2; iter <= maxiters; ++iter) {
         TRY((apply_precond<NCC, PRE_ONLY>(precond, p, rc(EPI_NONE, iter), nullptr, nullptr)));
         TRY(timed([&] {
-            k_mv<NCC, MV_CG_AZ><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.zu, p.zv, p.Azu, p.Azv, nullptr, nullptr, p.ru,
+            launch_mv<NCC, MV_CG_AZ>(s, gg, Ad, ac, p.zu, p.zv, p.Azu, p.Azv, nullptr, nullptr, p.ru,
                                                       p.rv, rc(EPI_CG_ITER, iter));
         }));
         k_halo<<<hb, kBlock, 0, s>>>(gg, p.Azu, p.Azv, st);
         k_vec<OP_CG_UPD><<<nb, kBlock, 0, s>>>(gg, v, rc(EPI_NONE, iter));
         if (is_check(iter, ncheck)) {
-            k_mv<NCC, MV_RESID><<<nb, mv_threads<NCC>(), 0, s>>>(gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
+            launch_mv<NCC, MV_RESID>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv,
                                                       rc(EPI_CHECK, iter));
             k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
             CU(cudaGetLastError());
@@ -1103,11 +1103,11 @@ static int oneshot_matvec(bool is3d, int nx, int ny, int nz, const cismgpu_par_t
     k_init_state<<<1, 1, 0, sv.stream>>>(st, 0.0, 0);
     RedCtx rc0{sv.partials.as<DD>(), st, EPI_NONE, 0};
     if (is3d)
-        k_mv<27, MV_PLAIN><<<nblocks(sv.g.NQ), mv_threads<27>(), 0, sv.stream>>>(sv.g, sv.A.as<double>(), sv.act.as<int32_t>(),
+        launch_mv<27, MV_PLAIN>(sv.stream, sv.g, sv.A.as<double>(), sv.act.as<int32_t>(),
                                                                       p.bu, p.bv, p.xu, p.xv, nullptr, nullptr,
                                                                       nullptr, nullptr, rc0);
     else
-        k_mv<9, MV_PLAIN><<<nblocks(sv.g.NQ), mv_threads<9>(), 0, sv.stream>>>(sv.g, sv.A.as<double>(), sv.act.as<int32_t>(),
+        launch_mv<9, MV_PLAIN>(sv.stream, sv.g, sv.A.as<double>(), sv.act.as<int32_t>(),
                                                                      p.bu, p.bv, p.xu, p.xv, nullptr, nullptr,
                                                                      nullptr, nullptr, rc0);
     CU(cudaGetLastError());

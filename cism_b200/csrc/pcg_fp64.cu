@@ -219,85 +219,114 @@ enum MvMode { MV_PLAIN = 0, MV_RESID, MV_DQ, MV_CG_AZ };
 //   MV_RESID : r = b - y (whole array); S0 = (r,r)             [:1454-1466, :3504-3516]
 //   MV_DQ    : S0 = (x,y) with x = d, y = q                    [:1376-1381, :3241-3248]
 //   MV_CG_AZ : S0 = (r,z), S1 = (y,z) with x = z, y = Az       [:3401-3413]
-// Level lanes of the structured matvec: 3D blocks have kMvLanes threads per column (levels
-// k = lane, lane + kMvLanes, ...), so a CTA holds 256 columns x 2 lanes and a launch has enough
-// loads in flight to stream the 108 coefficient planes while two CTAs fit on an SM (no
-// second wave of a few CTAs at typical sizes); 2D has one level.
-constexpr int kMvLanes = 2;
-constexpr int kMvChunk = 8;  // levels per shared-memory round of the per-column dot terms
-template <int NC> __host__ __device__ constexpr int mv_threads() { return NC == 27 ? kBlock * kMvLanes : kBlock; }
-
-// y = A x (+ the statement fused with it).  Per column the dot terms are added over k in
-// level order by the column's first lane (through shared memory), then the block tree of
-// the 256 columns: the same order as one thread per column.
+// The structured matvec runs as two kernels in 3D.  k_mv_nodes: one thread per node (column
+// q, level k = blockIdx.y), y = A x with the reference's statements (mv_row), and for MV_RESID
+// also r = b - y: every (column, level) is independent, so a launch has nz * NQ/256 CTAs and
+// enough loads in flight to stream the 108 coefficient planes.  k_mv_dots (modes with dot
+// products): one thread per column adds its terms over k in level order, then the block tree
+// of the 256 columns and the last-CTA tree: the order the reduction has always had.  In 2D a
+// column has one level, so k_mv_nodes adds the terms and reduces itself.
 template <int NC, int MODE>
-__global__ void __launch_bounds__(mv_threads<NC>(), NC == 27 ? 2 : 1) k_mv(Geom g, const double *__restrict__ A,
-                                                          const int32_t *__restrict__ act,
-                                                          const double *__restrict__ xu, const double *__restrict__ xv,
-                                                          double *__restrict__ yu, double *__restrict__ yv,
-                                                          const double *__restrict__ bu, const double *__restrict__ bv,
-                                                          double *__restrict__ ru, double *__restrict__ rv, RedCtx rc) {
-    constexpr int L = mv_threads<NC>() / kBlock;
-    constexpr bool RED = (MODE == MV_RESID || MODE == MV_DQ || MODE == MV_CG_AZ);
-    constexpr int NT = (MODE == MV_CG_AZ) ? 2 : 1;
-    __shared__ double terms[RED && L > 1 ? NT * kMvChunk * kBlock : 1];
-    if (rc.st->done) return;
-    const int col = threadIdx.x % kBlock, lane = threadIdx.x / kBlock;
-    const long long q = (long long)blockIdx.x * kBlock + col;
+__global__ void __launch_bounds__(kBlock) k_mv_nodes(Geom g, const double *__restrict__ A,
+                                                     const int32_t *__restrict__ act,
+                                                     const double *__restrict__ xu, const double *__restrict__ xv,
+                                                     double *__restrict__ yu, double *__restrict__ yv,
+                                                     const double *__restrict__ bu, const double *__restrict__ bv,
+                                                     double *__restrict__ ru, double *__restrict__ rv, RedCtx rc) {
+    // 2D (one level per column): the column's dot terms and the reduction in this kernel
+    constexpr bool FUSED = (NC == 9) && (MODE == MV_RESID || MODE == MV_DQ || MODE == MV_CG_AZ);
+    if (rc.st && rc.st->done) return;
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    const int k = blockIdx.y;
     DD s0{0.0, 0.0}, s1{0.0, 0.0};
-    int i = 0, j = 0;
-    bool own = false, on = false;
     if (q < g.NQ) {
+        int i, j;
         col_of(g, q, i, j);
-        own = owned(g, i, j);
-        on = own && act[q] != 0;
-    }
-    for (int k0 = 0; k0 < g.nz; k0 += (L > 1 ? kMvChunk : g.nz)) {
-        const int k1 = (L > 1) ? min(g.nz, k0 + kMvChunk) : g.nz;
-        for (int k = k0 + lane; k < k1; k += L) {
-            if (q >= g.NQ) break;
-            const long long e = (long long)k * g.NQ + q;
-            double a = 0.0, b = 0.0;
-            if (on) mv_row<NC>(g, A, xu, xv, i, j, q, k, a, b);
-            yu[e] = a;
-            yv[e] = b;
-            double t0 = 0.0, t1 = 0.0;
+        const bool own = owned(g, i, j);
+        const bool on = own && act[q] != 0;
+        const long long e = (long long)k * g.NQ + q;
+        double a = 0.0, b = 0.0;
+        if (on) mv_row<NC>(g, A, xu, xv, i, j, q, k, a, b);
+        yu[e] = a;
+        yv[e] = b;
+        double r1 = 0.0, r2 = 0.0;
+        if (MODE == MV_RESID) {
+            r1 = __dsub_rn(bu[e], a);
+            r2 = __dsub_rn(bv[e], b);
+            ru[e] = r1;
+            rv[e] = r2;
+        }
+        if (FUSED && own) {
             if (MODE == MV_RESID) {
-                const double r1 = __dsub_rn(bu[e], a), r2 = __dsub_rn(bv[e], b);
-                ru[e] = r1;
-                rv[e] = r2;
-                t0 = __dadd_rn(__dmul_rn(r1, r1), __dmul_rn(r2, r2));
+                s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(r1, r1), __dmul_rn(r2, r2)));
             } else if (MODE == MV_DQ) {
-                t0 = __dadd_rn(__dmul_rn(xu[e], a), __dmul_rn(xv[e], b));
+                s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(xu[e], a), __dmul_rn(xv[e], b)));
             } else if (MODE == MV_CG_AZ) {
                 const double z1 = xu[e], z2 = xv[e];
-                t0 = __dadd_rn(__dmul_rn(ru[e], z1), __dmul_rn(rv[e], z2));
-                t1 = __dadd_rn(__dmul_rn(a, z1), __dmul_rn(b, z2));
+                s0 = dd_add_d(s0, __dadd_rn(__dmul_rn(ru[e], z1), __dmul_rn(rv[e], z2)));
+                s1 = dd_add_d(s1, __dadd_rn(__dmul_rn(a, z1), __dmul_rn(b, z2)));
             }
-            if (RED) {
-                if (L == 1) {
-                    if (own) {
-                        s0 = dd_add_d(s0, t0);
-                        if (NT > 1) s1 = dd_add_d(s1, t1);
+        }
+    }
+    if (FUSED) {
+        if (MODE == MV_CG_AZ) reduce_and_finish_first<2>(rc, s0, s1);
+        else reduce_and_finish_first<1>(rc, s0, s1);
+    }
+}
+
+constexpr int kDotChunk = 8;  // levels whose loads k_mv_dots issues together
+
+template <int MODE>
+__global__ void __launch_bounds__(kBlock) k_mv_dots(Geom g, const double *__restrict__ xu,
+                                                    const double *__restrict__ xv, const double *__restrict__ yu,
+                                                    const double *__restrict__ yv, const double *__restrict__ ru,
+                                                    const double *__restrict__ rv, RedCtx rc) {
+    if (rc.st->done) return;
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    DD s0{0.0, 0.0}, s1{0.0, 0.0};
+    if (q < g.NQ) {
+        int i, j;
+        col_of(g, q, i, j);
+        if (owned(g, i, j))
+            for (int k0 = 0; k0 < g.nz; k0 += kDotChunk) {  // a chunk's loads together, then its terms in order
+                double t0[kDotChunk], t1[kDotChunk];
+#pragma unroll
+                for (int u = 0; u < kDotChunk; ++u) {
+                    t0[u] = t1[u] = 0.0;
+                    if (k0 + u >= g.nz) continue;
+                    const long long e = (long long)(k0 + u) * g.NQ + q;
+                    if (MODE == MV_RESID) {
+                        const double r1 = ru[e], r2 = rv[e];
+                        t0[u] = __dadd_rn(__dmul_rn(r1, r1), __dmul_rn(r2, r2));
+                    } else if (MODE == MV_DQ) {
+                        t0[u] = __dadd_rn(__dmul_rn(xu[e], yu[e]), __dmul_rn(xv[e], yv[e]));
+                    } else if (MODE == MV_CG_AZ) {
+                        const double z1 = xu[e], z2 = xv[e];
+                        t0[u] = __dadd_rn(__dmul_rn(ru[e], z1), __dmul_rn(rv[e], z2));
+                        t1[u] = __dadd_rn(__dmul_rn(yu[e], z1), __dmul_rn(yv[e], z2));
                     }
-                } else {
-                    terms[(k - k0) * kBlock + col] = t0;
-                    if (NT > 1) terms[(kMvChunk + k - k0) * kBlock + col] = t1;
                 }
+#pragma unroll
+                for (int u = 0; u < kDotChunk; ++u)
+                    if (k0 + u < g.nz) {
+                        s0 = dd_add_d(s0, t0[u]);
+                        if (MODE == MV_CG_AZ) s1 = dd_add_d(s1, t1[u]);
+                    }
             }
-        }
-        if (RED && L > 1) {  // the column's terms of this chunk, in level order
-            __syncthreads();
-            if (lane == 0 && own)
-                for (int k = k0; k < k1; ++k) {
-                    s0 = dd_add_d(s0, terms[(k - k0) * kBlock + col]);
-                    if (NT > 1) s1 = dd_add_d(s1, terms[(kMvChunk + k - k0) * kBlock + col]);
-                }
-            __syncthreads();
-        }
     }
     if (MODE == MV_RESID || MODE == MV_DQ) reduce_and_finish_first<1>(rc, s0, s1);
     if (MODE == MV_CG_AZ) reduce_and_finish_first<2>(rc, s0, s1);
+}
+
+// y = A x (+ the statement MODE fuses with it, see MvMode) on stream s.
+template <int NC, int MODE>
+inline void launch_mv(cudaStream_t s, const Geom &g, const double *A, const int32_t *act, const double *xu,
+                      const double *xv, double *yu, double *yv, const double *bu, const double *bv, double *ru,
+                      double *rv, const RedCtx &rc) {
+    const dim3 grid((unsigned)((g.NQ + kBlock - 1) / kBlock), (unsigned)g.nz);
+    k_mv_nodes<NC, MODE><<<grid, kBlock, 0, s>>>(g, A, act, xu, xv, yu, yv, bu, bv, ru, rv, rc);
+    if (NC == 27 && MODE != MV_PLAIN)
+        k_mv_dots<MODE><<<grid.x, kBlock, 0, s>>>(g, xu, xv, yu, yv, ru, rv, rc);
 }
 
 // ---------------------------------------------------------------------------
