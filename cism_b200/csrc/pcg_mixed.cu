@@ -40,17 +40,17 @@ constexpr int kMixedMaxNz = 32;                  // shared-memory bound of the m
 // a neighbour's half-updated d or x while it recomputes the halo of x.
 enum MStep { MS_INIT = 0, MS_A, MS_MERGED, MS_B, MS_CHECK_UNUSED, MS_DONE, MS_BC, MS_A_UPD, MS_FIN };
 
-// A tile's partial sums of one step.  Every 64-bit word carries the step number (tag) in its
-// high half and one 32-bit half of a sum in its low half (w[2i] low, w[2i+1] high half of
-// sum i), so a reader that finds the tag in all six words has the step's values, with
+// A tile's partial sums of one step (two sums).  Every 64-bit word carries the step number
+// (tag) in its high half and one 32-bit half of a sum in its low half (w[2i] low, w[2i+1]
+// high half of sum i), so a reader that finds the tag in all four words has the step's values, with
 // relaxed loads and no fence.  The words are stored after a release fence, so an acquire
 // load of a word also orders the tile's vector stores of the step before the reader's
 // later loads (the halo).  Each tile writes kRecCopies copies ([copy][tile][parity]); a CTA
 // reads copy blockIdx % kRecCopies, so the all-to-all reads of a step spread over more L2
 // lines.
 struct __align__(64) TileRec {
-    unsigned long long w[6];
-    unsigned long long pad[2];
+    unsigned long long w[4];
+    unsigned long long pad[4];
 };
 constexpr int kRecCopies = 4;
 constexpr size_t kStreamBytes = 32u << 20;  // FP32 matrix size above which L2 cannot keep a solve's matrix
@@ -92,7 +92,6 @@ struct MDesc {
 
 struct MState {
     double alpha, beta, rho_old, sigma, L2_rhs, err, tol;
-    double rr_inner;     // (r,r) of the recursive FP32 residual, for diagnostics
     int step, iter, par;
     int maxiters, ncheck;
     int done, status, niters;
@@ -163,12 +162,11 @@ __device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
     return v;
 }
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
-// The six words of a record, as three 16-byte relaxed loads (each 64-bit element is a
+// The four words of a record, as two 16-byte relaxed loads (each 64-bit element is a
 // single-copy-atomic access).
-__device__ __forceinline__ void ld_rec(const TileRec *rp, unsigned long long (&w)[6]) {
+__device__ __forceinline__ void ld_rec(const TileRec *rp, unsigned long long (&w)[4]) {
     asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w[0]), "=l"(w[1]) : "l"(rp->w) : "memory");
     asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w[2]), "=l"(w[3]) : "l"(rp->w + 2) : "memory");
-    asm volatile("ld.relaxed.gpu.global.v2.u64 {%0, %1}, [%2];" : "=l"(w[4]), "=l"(w[5]) : "l"(rp->w + 4) : "memory");
 }
 __device__ __forceinline__ int ld_acquire_i(const int *p) {
     int v;
@@ -181,7 +179,7 @@ constexpr long long kWaitCycles = 1LL << 31;  // ~1 s at 2 GHz: a wait longer th
 // ---------------------------------------------------------------------------
 // per-solve state machine, run by thread 0 of every CTA holding the solve
 // ---------------------------------------------------------------------------
-__device__ void advance_state(MState &S, double S0, double S1, double S2) {
+__device__ void advance_state(MState &S, double S0, double S1) {
     switch (S.step) {
     case MS_INIT:  // S0 = (b,b), S1 = (r,r) of r = b - A x0
         S.L2_rhs = sqrt(S0);
@@ -206,7 +204,6 @@ __device__ void advance_state(MState &S, double S0, double S1, double S2) {
         S.fp32_matvecs += 1;
         const bool first = (S.iter == 1);
         const double rho = S0, delta = S1;
-        S.rr_inner = S2;
         S.beta = first ? 0.0 : rho / S.rho_old;
         S.sigma = first ? delta : delta - S.beta * rho / S.alpha;
         S.alpha = rho / S.sigma;
@@ -274,8 +271,8 @@ struct MHead {
     int owner[kMaxCtaSolves];  // 1 if this CTA holds tile 0 of the solve (reports it)
     int nsolve;
     int cur;                   // cache slot described by D
-    double red[8][3];
-    double rsum[8][3];
+    double red[8][2];
+    double rsum[8][2];
     int nacq;                  // >= 0: the CTA reads the halo of acq[0..nacq) only; -1: fence
     int acq[kMaxAcq];
     int ntl;                   // static launches: tile list entries of this CTA
@@ -327,23 +324,22 @@ __device__ __forceinline__ double ld_stream(const double *p, unsigned long long 
 __device__ __forceinline__ float ldf(const float *p) { return __ldcg(p); }
 __device__ __forceinline__ double ldd(const double *p) { return __ldcg(p); }
 
-// Sum of three doubles over the 256 threads in a fixed order (warp shuffle tree, then the
+// Sum of two doubles over the 256 threads in a fixed order (warp shuffle tree, then the
 // 8 warp sums in order); result in thread 0.
-__device__ __forceinline__ void block_sum3(double &a, double &b, double &c, double (*sm)[3]) {
+__device__ __forceinline__ void block_sum2(double &a, double &b, double (*sm)[2]) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) {
         a += __shfl_down_sync(0xffffffffu, a, off);
         b += __shfl_down_sync(0xffffffffu, b, off);
-        c += __shfl_down_sync(0xffffffffu, c, off);
     }
     __syncthreads();
-    if (lane == 0) { sm[warp][0] = a; sm[warp][1] = b; sm[warp][2] = c; }
+    if (lane == 0) { sm[warp][0] = a; sm[warp][1] = b; }
     __syncthreads();
     if (threadIdx.x == 0) {
-        a = sm[0][0]; b = sm[0][1]; c = sm[0][2];
+        a = sm[0][0]; b = sm[0][1];
 #pragma unroll
-        for (int w = 1; w < kBlock / 32; ++w) { a += sm[w][0]; b += sm[w][1]; c += sm[w][2]; }
+        for (int w = 1; w < kBlock / 32; ++w) { a += sm[w][0]; b += sm[w][1]; }
     }
 }
 
@@ -500,7 +496,10 @@ __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, i
                             if (k + kA < 0 || k + kA >= nz || sc < 0) continue;
                             const int n = (k + kA) * NQ + sc;
                             const size_t a = (size_t)c * plane + e;
-                            double x1 = ldd(xu + n), x2 = ldd(xv + n);
+                            // x is not written during this step (owner writes are deferred) and the step
+                            // starts after the acquire of the tiles' records and a barrier: plain
+                            // loads, so the neighbour reuse of x hits in L1
+                            double x1 = xu[n], x2 = xv[n];
                             if (sdn) {
                                 x1 = fma(alpha64, (double)sdn[(k + kA) * NS + sn], x1);
                                 x2 = fma(alpha64, (double)sdn[(nz + k + kA) * NS + sn], x2);
@@ -548,7 +547,7 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
     const int t = threadIdx.x;
     const int step = S.step;
     const int par = S.par;
-    double p0 = 0.0, p1 = 0.0, p2 = 0.0;
+    double p0 = 0.0, p1 = 0.0;
 
     if (!resident) {  // resident launches keep their single tile's map for the whole launch
         const int *tmap = D.maps + (size_t)tile * NS;
@@ -828,20 +827,18 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                     const double ru = srt[cc[u]], rv = srt[NZM * NT + cc[u]];
                     p0 += ru * (double)zu[u] + rv * (double)zv[u];
                     p1 += (double)yu[u] * zu[u] + (double)yv[u] * zv[u];
-                    p2 += ru * ru + rv * rv;
                 }
             }
         }
     }
-    block_sum3(p0, p1, p2, hd.red);
-    if (t < 32) {  // warp 0: lane c*6+k stores word k of copy c, after a release fence
+    block_sum2(p0, p1, hd.red);
+    if (t < 32) {  // warp 0: lane c*4+k stores word k of copy c, after a release fence
         p0 = __shfl_sync(0xffffffffu, p0, 0);
         p1 = __shfl_sync(0xffffffffu, p1, 0);
-        p2 = __shfl_sync(0xffffffffu, p2, 0);
-        if (t < 6 * kRecCopies) {
+        if (t < 4 * kRecCopies) {
             const unsigned tag = S.tick + 1u;
-            const int c = t / 6, k = t - 6 * (t / 6);
-            const double pv = (k < 2) ? p0 : ((k < 4) ? p1 : p2);
+            const int c = t / 4, k = t - 4 * (t / 4);
+            const double pv = (k < 2) ? p0 : p1;
             const unsigned half = (k & 1) ? (unsigned)__double2hiint(pv) : (unsigned)__double2loint(pv);
             TileRec *rp = D.recs + (size_t)c * 2 * D.ntiles + 2 * (size_t)tile + (tag & 1u);
             fence_acq_rel();  // the tile's vector stores (every thread's, via the barrier above) first
@@ -862,10 +859,10 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
 // nacq < 0 every thread ends with an acquire fence (a leader whose sums others rely on).
 // Returns false if a wait gave up.
 constexpr int kRecPerThread = 2;  // tiles a thread polls at once (ntl <= 512 in one round)
-__device__ bool sum_records(const TileRec *R, int ntl, unsigned tag, MCtl *ctl, double (*rsum)[3],
-                            const int *acq, int nacq, double &s0, double &s1, double &s2) {
+__device__ bool sum_records(const TileRec *R, int ntl, unsigned tag, MCtl *ctl, double (*rsum)[2],
+                            const int *acq, int nacq, double &s0, double &s1) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+    double a0 = 0.0, a1 = 0.0;
     int bad = 0;
     const int at = (nacq > 0 && (int)threadIdx.x < nacq) ? acq[threadIdx.x] : -1;
     bool acq_need = at >= 0;
@@ -874,28 +871,28 @@ __device__ bool sum_records(const TileRec *R, int ntl, unsigned tag, MCtl *ctl, 
 #pragma unroll
         for (int u = 0; u < kRecPerThread; ++u)
             if (w0 + u * kBlock < ntl) need |= 1u << u;
-        double v[kRecPerThread][3];
+        double v[kRecPerThread][2];
 #pragma unroll
-        for (int u = 0; u < kRecPerThread; ++u) v[u][0] = v[u][1] = v[u][2] = 0.0;
+        for (int u = 0; u < kRecPerThread; ++u) v[u][0] = v[u][1] = 0.0;
         const long long t0 = clock64();
         unsigned spins = 0;
         for (;;) {
 #pragma unroll
             for (int u = 0; u < kRecPerThread; ++u) {
                 if (!((need >> u) & 1u)) continue;
-                unsigned long long wd[6];
+                unsigned long long wd[4];
                 ld_rec(R + 2 * (size_t)(w0 + u * kBlock), wd);
                 bool ok = true;
 #pragma unroll
-                for (int k = 0; k < 6; ++k) ok &= (unsigned)(wd[k] >> 32) == tag;
+                for (int k = 0; k < 4; ++k) ok &= (unsigned)(wd[k] >> 32) == tag;
                 if (ok) {
 #pragma unroll
-                    for (int k = 0; k < 3; ++k)
+                    for (int k = 0; k < 2; ++k)
                         v[u][k] = __hiloint2double((int)(unsigned)wd[2 * k + 1], (int)(unsigned)wd[2 * k]);
                     need &= ~(1u << u);
                 }
             }
-            if (acq_need && (unsigned)(ld_acquire64(&R[2 * (size_t)at].w[5]) >> 32) == tag) acq_need = false;
+            if (acq_need && (unsigned)(ld_acquire64(&R[2 * (size_t)at].w[3]) >> 32) == tag) acq_need = false;
             if (!need && !acq_need) break;
             __nanosleep(spins < 16 ? 20 : 100);
             if ((++spins & 31u) == 0) {
@@ -909,31 +906,28 @@ __device__ bool sum_records(const TileRec *R, int ntl, unsigned tag, MCtl *ctl, 
         }
 #pragma unroll
         for (int u = 0; u < kRecPerThread; ++u)
-            if (w0 + u * kBlock < ntl) { a0 += v[u][0]; a1 += v[u][1]; a2 += v[u][2]; }
+            if (w0 + u * kBlock < ntl) { a0 += v[u][0]; a1 += v[u][1]; }
     }
     if (nacq < 0) fence_acq_rel();
     if (__syncthreads_or(bad)) return false;
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1) {
-        const double o0 = __shfl_down_sync(0xffffffffu, a0, off), o1 = __shfl_down_sync(0xffffffffu, a1, off),
-                     o2 = __shfl_down_sync(0xffffffffu, a2, off);
-        if (lane + off < 32) { a0 += o0; a1 += o1; a2 += o2; }
+        const double o0 = __shfl_down_sync(0xffffffffu, a0, off), o1 = __shfl_down_sync(0xffffffffu, a1, off);
+        if (lane + off < 32) { a0 += o0; a1 += o1; }
     }
-    if (lane == 0) { rsum[warp][0] = a0; rsum[warp][1] = a1; rsum[warp][2] = a2; }
+    if (lane == 0) { rsum[warp][0] = a0; rsum[warp][1] = a1; }
     __syncthreads();
     if (warp == 0) {
         constexpr int NW = kBlock / 32;
         a0 = lane < NW ? rsum[lane][0] : 0.0;
         a1 = lane < NW ? rsum[lane][1] : 0.0;
-        a2 = lane < NW ? rsum[lane][2] : 0.0;
 #pragma unroll
         for (int off = NW / 2; off >= 1; off >>= 1) {
-            const double o0 = __shfl_down_sync(0xffffffffu, a0, off), o1 = __shfl_down_sync(0xffffffffu, a1, off),
-                         o2 = __shfl_down_sync(0xffffffffu, a2, off);
-            if (lane + off < NW) { a0 += o0; a1 += o1; a2 += o2; }
+            const double o0 = __shfl_down_sync(0xffffffffu, a0, off), o1 = __shfl_down_sync(0xffffffffu, a1, off);
+            if (lane + off < NW) { a0 += o0; a1 += o1; }
         }
     }
-    s0 = a0; s1 = a1; s2 = a2;
+    s0 = a0; s1 = a1;
     return true;
 }
 
@@ -949,11 +943,11 @@ __device__ bool reduce_wait(MHead &hd, const MDesc *__restrict__ descs, MState *
         const int ntl = D.ntiles;
         const unsigned tag = hd.st[cs].tick + 1u;
         const TileRec *R = D.recs + (size_t)(blockIdx.x % kRecCopies) * 2 * ntl + (tag & 1u);
-        double s0, s1, s2;
-        if (!sum_records(R, ntl, tag, ctl, hd.rsum, hd.acq, hd.nsolve == 1 ? hd.nacq : -1, s0, s1, s2)) return false;
+        double s0, s1;
+        if (!sum_records(R, ntl, tag, ctl, hd.rsum, hd.acq, hd.nsolve == 1 ? hd.nacq : -1, s0, s1)) return false;
         if (threadIdx.x == 0) {
             MState &S = hd.st[cs];
-            advance_state(S, s0, s1, s2);
+            advance_state(S, s0, s1);
             S.tick = tag;
             if (S.done && hd.owner[cs]) {
                 gstates[hd.sid[cs]] = S;
@@ -1087,11 +1081,11 @@ __device__ bool lead_duties(MHead &hd, const MDesc *__restrict__ descs, MState *
         const int ntl = D.ntiles;
         const unsigned tag = hd.st[cs].tick + 1u;
         const TileRec *R = D.recs + (size_t)(blockIdx.x % kRecCopies) * 2 * ntl + (tag & 1u);
-        double s0, s1, s2;
-        if (!sum_records(R, ntl, tag, ctl, hd.rsum, nullptr, -1, s0, s1, s2)) return false;
+        double s0, s1;
+        if (!sum_records(R, ntl, tag, ctl, hd.rsum, nullptr, -1, s0, s1)) return false;
         if (threadIdx.x == 0) {
             MState &S = hd.st[cs];
-            advance_state(S, s0, s1, s2);
+            advance_state(S, s0, s1);
             S.tick = tag;
             if (S.done) *gstates[hd.sid[cs]] = S;
             Bcast *B = D.bc + (size_t)(tag & 1u) * kBcastCopies;
