@@ -643,6 +643,7 @@ static MDesc mixed_desc(const Solver &sv, int precond, int TY) {  // TY: the sol
     D.ntiles = D.tiles_x * D.tiles_y;
     D.A32 = m.A32;
     D.A64 = sv.A.as<double>();
+    D.A64i = m.A64i;
     D.pre = m.pre;
     D.act = sv.act.as<int32_t>();
     D.b = p.bu;
@@ -752,6 +753,8 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
             return cudaMalloc(p, n);
         };
         CU(alloc((void **)&m.A32, (size_t)NC * nvec * sizeof(float4)));
+        if ((size_t)NC * (size_t)nvec * sizeof(float4) > kStreamBytes)  // streamed matrix: interleaved FP64 copy
+            CU(alloc((void **)&m.A64i, (size_t)NC * nvec * 2 * sizeof(double2)));
         CU(alloc((void **)&m.pre, (size_t)6 * nvec * sizeof(float)));
         CU(alloc((void **)&m.vec, (size_t)16 * nvec * sizeof(float)));
         CU(alloc((void **)&m.state, sizeof(MState)));
@@ -767,8 +770,8 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
         m.ntiles = 0;
     }
     if (m.stale) {  // new matrix: FP32 copy (couplings leaving the grid set to zero)
-        if (NC == 27) k_to_f32<27><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32);
-        else k_to_f32<9><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32);
+        if (NC == 27) k_to_f32<27><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32, m.A64i);
+        else k_to_f32<9><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32, m.A64i);
         CU(cudaGetLastError());
         m.stale = false;
         m.precond = -1;

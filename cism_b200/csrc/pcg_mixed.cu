@@ -76,6 +76,8 @@ struct MDesc {
     int tiles_x, tiles_y, ntiles;
     const float4 *A32;   // [NC][nz][NQ] of (uu, uv, vu, vv): one 16-byte load per coupling
     const double *A64;   // [4][NC][nz][NQ]
+    const double2 *A64i; // [NC][nz][NQ][2] of {uu, uv}, {vu, vv} for streamed matrices (else null): the FP64
+                         // residual's two 16-byte loads per coupling
     const float *pre;    // diag: [2][nz][NQ] inverse diagonal; sia: [2][3][nz][NQ] (1/beta, sb, gamma)
     const int32_t *act;  // [NQ]
     const double *b;     // [2][nz][NQ]
@@ -318,6 +320,13 @@ __device__ __forceinline__ double ld_stream(const double *p, unsigned long long 
     asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(p), "l"(pol));
     return v;
 }
+__device__ __forceinline__ double2 ld_stream(const double2 *p, unsigned long long pol) {
+    double2 v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+        : "=d"(v.x), "=d"(v.y)
+        : "l"(p), "l"(pol));
+    return v;
+}
 
 // Loads of data that other CTAs wrote earlier in the same launch go through L2
 // (ld.global.cg): L1 is not coherent across SMs.
@@ -445,7 +454,9 @@ __device__ __forceinline__ void sia_col(const MDesc &D, float *zc, int NS, int s
 // advanced by this iteration's update, x + alpha64 * dn with dn = sdn[c][k][slot] -- the same
 // FP64 fma its owner applies later, so the residual sees exactly the updated x.
 // Partials: p0 = (b,b), p1 = (r,r).  Loads of kChR items are issued before any store.
-template <int NC>
+// IL: read the interleaved FP64 copy (solves whose matrix streams through L2; a matrix L2
+// keeps between checks reads faster from the four planes).
+template <int NC, bool IL>
 __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, int TY, int i0, int j0, int rpar,
                                               const float *sdn, double alpha64, double &p0, double &p1) {
     const Geom &g = D.g;
@@ -453,6 +464,7 @@ __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, i
     const int NQ = (int)g.NQ;
     const int plane = nz * NQ;
     const int NT = kTX * TY;
+    const double2 *__restrict__ A2 = D.A64i;
     const double *__restrict__ Auu = D.A64;
     const double *__restrict__ Auv = D.A64 + (size_t)NC * plane;
     const double *__restrict__ Avu = D.A64 + (size_t)2 * NC * plane;
@@ -504,10 +516,18 @@ __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, i
                                 x1 = fma(alpha64, (double)sdn[(k + kA) * NS + sn], x1);
                                 x2 = fma(alpha64, (double)sdn[(nz + k + kA) * NS + sn], x2);
                             }
-                            yu[u] = fma(ld_stream(Auu + a, pol), x1, yu[u]);
-                            yu[u] = fma(ld_stream(Auv + a, pol), x2, yu[u]);
-                            yv[u] = fma(ld_stream(Avu + a, pol), x1, yv[u]);
-                            yv[u] = fma(ld_stream(Avv + a, pol), x2, yv[u]);
+                            if (IL) {
+                                const double2 au = ld_stream(A2 + 2 * a, pol), av = ld_stream(A2 + 2 * a + 1, pol);
+                                yu[u] = fma(au.x, x1, yu[u]);
+                                yu[u] = fma(au.y, x2, yu[u]);
+                                yv[u] = fma(av.x, x1, yv[u]);
+                                yv[u] = fma(av.y, x2, yv[u]);
+                            } else {
+                                yu[u] = fma(ld_stream(Auu + a, pol), x1, yu[u]);
+                                yu[u] = fma(ld_stream(Auv + a, pol), x2, yu[u]);
+                                yv[u] = fma(ld_stream(Avu + a, pol), x1, yv[u]);
+                                yv[u] = fma(ld_stream(Avv + a, pol), x2, yv[u]);
+                            }
                         }
                     }
                 }
@@ -556,7 +576,8 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
     }
 
     if (step == MS_INIT) {
-        residual_pass<NC>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
+        if (D.A64i) residual_pass<NC, true>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
+        else residual_pass<NC, false>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
     } else if (step == MS_BC) {
         // update of iteration iter fused with the FP64 check: dn = z + beta d on tile and halo
         // slots (into shared memory, over the z rows), q for the owned columns; the owners'
@@ -605,7 +626,8 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
             }
         }
         __syncthreads();
-        residual_pass<NC>(D, smap, TY, i0, j0, par ^ 1, sdn, S.alpha, p0, p1);
+        if (D.A64i) residual_pass<NC, true>(D, smap, TY, i0, j0, par ^ 1, sdn, S.alpha, p0, p1);
+        else residual_pass<NC, false>(D, smap, TY, i0, j0, par ^ 1, sdn, S.alpha, p0, p1);
         p0 = p1;
         p1 = 0.0;
     } else if (step == MS_FIN) {
@@ -1227,7 +1249,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict
 // array (which the reference skips) are stored as zero so the FP32 stencil loop needs
 // no bounds tests.
 template <int NC>
-__global__ void k_to_f32(Geom g, const double *__restrict__ src, float4 *__restrict__ dst) {
+__global__ void k_to_f32(Geom g, const double *__restrict__ src, float4 *__restrict__ dst,
+                         double2 *__restrict__ dst64) {
     const long long plane = (long long)g.nz * g.NQ;
     const long long n = (long long)NC * plane;  // one float4 (uu, uv, vu, vv) per coupling and node
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
@@ -1239,8 +1262,13 @@ __global__ void k_to_f32(Geom g, const double *__restrict__ src, float4 *__restr
         const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
         const bool in = i + iA >= 0 && i + iA < g.NX && j + jA >= 0 && j + jA < g.NY && k + kA >= 0 && k + kA < g.nz;
         const size_t bs = (size_t)NC * plane;  // FP64 planes [4][NC][nz][NQ]
-        dst[e] = in ? make_float4((float)src[e], (float)src[bs + e], (float)src[2 * bs + e], (float)src[3 * bs + e])
-                    : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const double uu = in ? src[e] : 0.0, uv = in ? src[bs + e] : 0.0;
+        const double vu = in ? src[2 * bs + e] : 0.0, vv = in ? src[3 * bs + e] : 0.0;
+        dst[e] = make_float4((float)uu, (float)uv, (float)vu, (float)vv);
+        if (dst64) {
+            dst64[2 * e] = make_double2(uu, uv);
+            dst64[2 * e + 1] = make_double2(vu, vv);
+        }
     }
 }
 
@@ -1289,6 +1317,7 @@ struct MixedBufs {
     int shape_nc = 0;
     int precond = -1;
     float4 *A32 = nullptr;
+    double2 *A64i = nullptr;   // FP64 matrix interleaved per coupling (k_to_f32)
     float *pre = nullptr, *vec = nullptr;
     int *maps = nullptr;
     int *nbrs = nullptr;
@@ -1303,10 +1332,11 @@ struct MixedBufs {
     int ntiles_cap = 0;
     long long maps_cap = 0;
     void release() {
-        for (void *p : {(void *)A32, (void *)pre, (void *)vec, (void *)recs, (void *)state, (void *)desc,
+        for (void *p : {(void *)A32, (void *)A64i, (void *)pre, (void *)vec, (void *)recs, (void *)state, (void *)desc,
                         (void *)tiles, (void *)ctl, (void *)maps, (void *)nbrs, (void *)bc})
             if (p) cudaFree(p);
         A32 = nullptr;
+        A64i = nullptr;
         pre = vec = nullptr;
         maps = nullptr;
         nbrs = nullptr;

@@ -45,12 +45,14 @@ struct SrvReq {
 };
 
 // Device bytes a request's handle holds at most (the FP64 system, its staging block, the
-// FP64 and FP32 vectors, the FP32 matrix and factors, tile maps and records).
+// FP64 and FP32 vectors, the FP32 matrix, the interleaved FP64 matrix of a streamed solve,
+// the factors, tile maps and records).
 static size_t request_bytes(const cismgpu_request_t &r) {
     const long long NQ = (long long)(r.nx - 1) * (r.ny - 1);
     const long long nvec = NQ * (r.dims == 3 ? r.nz : 1);
     const long long NC = r.dims == 3 ? 27 : 9;
-    const long long per = 4 * NC * 8 + NC * 8 + NVEC * 8 + 4 * NC * 4 + 6 * 4 + 16 * 4;
+    const bool streamed = (size_t)(NC * nvec) * 16 > kStreamBytes;
+    const long long per = 4 * NC * 8 + NC * 8 + NVEC * 8 + 4 * NC * 4 + (streamed ? 4 * NC * 8 : 0) + 6 * 4 + 16 * 4;
     return (size_t)(nvec * per + NQ * 16 + (8 << 20));
 }
 

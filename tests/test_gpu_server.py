@@ -71,7 +71,7 @@ def test_server_budget(gpu_lib):
     request larger than the budget fails with CISMGPU_ENOMEM without stopping the others."""
     P = asm.ssa_random(ewn=61, nsn=57, seed=3)
     big = asm.ssa_random(ewn=150, nsn=140, seed=4)
-    S = cg.Server(hbm_budget_bytes=12 * 10**6, epoch_steps=32)
+    S = cg.Server(hbm_budget_bytes=14 * 10**6, epoch_steps=32)  # one small request (~12.3 MB) at a time
     try:
         ids = [S.submit(P, precond=1, tol=1e-8, maxiters=5000) for _ in range(3)]
         bid = S.submit(big, precond=1, tol=1e-8, maxiters=5000)
