@@ -1014,11 +1014,9 @@ static int run_algorithm(Solver &sv, int alg, int precond, int ncheck, double to
     return fail(CISMGPU_EINVAL, "unknown algorithm");
 }
 
-static int validate(int nx, int ny, int nz, const cismgpu_par_t *par, const void *indx, const void *act,
-                    const void *A0, const void *A1, const void *A2, const void *A3, const void *bu,
-                    const void *bv) {
-    if (!par || !indx || !act || !A0 || !A1 || !A2 || !A3 || !bu || !bv)
-        return fail(CISMGPU_EINVAL, "null pointer argument");
+// Grid sizes and owned bounds every entry point shares.
+static int validate_geom(int nx, int ny, int nz, const cismgpu_par_t *par) {
+    if (!par) return fail(CISMGPU_EINVAL, "null pointer argument");
     if (nx < 6 || ny < 6 || nz < 1 || nz > kMaxNz)
         return fail(CISMGPU_EINVAL, "grid too small or nz outside 1..64");
     if (par->tasks_row * par->tasks_col != 1)
@@ -1027,6 +1025,14 @@ static int validate(int nx, int ny, int nz, const cismgpu_par_t *par, const void
         par->staggered_jlo < 1 || par->staggered_jhi > ny - 1 || par->staggered_jlo > par->staggered_jhi)
         return fail(CISMGPU_EINVAL, "owned vertex bounds outside the array");
     return CISMGPU_OK;
+}
+
+static int validate(int nx, int ny, int nz, const cismgpu_par_t *par, const void *indx, const void *act,
+                    const void *A0, const void *A1, const void *A2, const void *A3, const void *bu,
+                    const void *bv) {
+    if (!par || !indx || !act || !A0 || !A1 || !A2 || !A3 || !bu || !bv)
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    return validate_geom(nx, ny, nz, par);
 }
 
 static int validate_solve_args(int precond, int ncheck, int maxiters) {
@@ -1146,7 +1152,7 @@ static int oneshot_resid_velo(bool is3d, int whichresid, int nx, int ny, int nz,
     std::lock_guard<std::mutex> lk(g_mu);
     g_last_error.clear();
     if (!uvel || !vvel || !usav || !vsav || !resid_velo) return fail(CISMGPU_EINVAL, "null pointer argument");
-    TRY(validate(nx, ny, is3d ? nz : 1, par, uvel, uvel, uvel, uvel, uvel, uvel, uvel, uvel));
+    TRY(validate_geom(nx, ny, is3d ? nz : 1, par));
     if (!g_oneshot) g_oneshot = new Solver();
     Solver &sv = *g_oneshot;
     TRY(sv.init(nullptr));
