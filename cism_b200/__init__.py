@@ -172,9 +172,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_solver_set_system.argtypes = [vp, d, d, d, d, d, d, i32]
     lib.cismgpu_solver_residual_vector.argtypes = [vp, d, d, P(dbl), P(dbl)]
     lib.cismgpu_solver_residual_velocity.argtypes = [vp, i32, P(dbl)]
+    lib.cismgpu_solver_save.argtypes = [vp]
+    lib.cismgpu_solver_restore.argtypes = [vp]
     for f in ("cismgpu_compute_residual_vector_3d", "cismgpu_compute_residual_vector_2d",
               "cismgpu_compute_residual_velocity_3d", "cismgpu_compute_residual_velocity_2d",
-              "cismgpu_solver_set_system", "cismgpu_solver_residual_vector", "cismgpu_solver_residual_velocity"):
+              "cismgpu_solver_set_system", "cismgpu_solver_residual_vector", "cismgpu_solver_residual_velocity",
+              "cismgpu_solver_save", "cismgpu_solver_restore"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -456,6 +459,14 @@ class DeviceSolver:
         _check(self._lib, self._lib.cismgpu_solver_residual_vector(self.handle, pu, pv, ctypes.byref(l2),
                                                                    ctypes.byref(l2r)))
         return ru, rv, l2.value, l2r.value
+
+    def save(self):
+        """Accelerated Picard's saved state: the current velocity and A (not b) on the device."""
+        _check(self._lib, self._lib.cismgpu_solver_save(self.handle))
+
+    def restore(self):
+        """Back to the saved velocity and A; the velocity becomes the next solve's initial guess."""
+        _check(self._lib, self._lib.cismgpu_solver_restore(self.handle))
 
     def residual_velocity(self, whichresid=1):
         """compute_residual_velocity between the last solution and the guess it started from."""

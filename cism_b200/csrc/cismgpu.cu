@@ -111,6 +111,8 @@ struct Solver {
     bool own_stream = false;
     DevBuf A, raw, vec, act, partials, state, map;
     DevBuf tri;       // tridiagonal preconditioner planes (TriPlane), on first use
+    DevBuf A_sav, x_sav;      // accelerated Picard's saved matrix and velocity (cismgpu_solver_save)
+    bool have_sav = false;
     bool x_current = false;   // the x planes hold a solution (a solve ran since the last upload)
     int32_t hindx[27] = {};   // host copy of the uploaded indxA map (27 or 9 entries)
     int32_t hindx2[9] = {};   // indxA_2d: the uploaded map in 2D; in 3D the caller's, else standard
@@ -132,6 +134,9 @@ struct Solver {
     void destroy() {
         A.release(); raw.release(); vec.release(); act.release(); partials.release(); state.release(); map.release();
         tri.release();
+        A_sav.release();
+        x_sav.release();
+        have_sav = false;
         mixed.release();
         if (h_done) cudaFreeHost(h_done);
         if (h_state) cudaFreeHost(h_state);
@@ -1637,6 +1642,40 @@ int cismgpu_solver_residual_vector(cismgpu_solver_t *h, double *resid_u, double 
     if (resid_u) TRY(sv.download(VR_U, VR_V, resid_u, resid_v));
     *L2_norm = l2;
     if (L2_norm_relative) *L2_norm_relative = (l2b > 0.0) ? l2 / l2b : 0.0;
+    return CISMGPU_OK;
+}
+
+int cismgpu_solver_save(cismgpu_solver_t *h) {
+    g_last_error.clear();
+    if (!h) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
+    Solver &sv = h->sv;
+    const size_t abytes = (size_t)4 * sv.NC * sv.nvec * sizeof(double), xbytes = (size_t)2 * sv.nvec * sizeof(double);
+    CU(sv.A_sav.ensure(abytes));
+    CU(sv.x_sav.ensure(xbytes));
+    const Ptrs p = sv.ptrs();
+    CU(cudaMemcpyAsync(sv.A_sav.p, sv.A.p, abytes, cudaMemcpyDeviceToDevice, sv.stream));
+    CU(cudaMemcpyAsync(sv.x_sav.p, sv.x_current ? p.xu : p.x0u, xbytes, cudaMemcpyDeviceToDevice, sv.stream));
+    CU(cudaStreamSynchronize(sv.stream));
+    sv.have_sav = true;
+    return CISMGPU_OK;
+}
+
+int cismgpu_solver_restore(cismgpu_solver_t *h) {
+    g_last_error.clear();
+    if (!h) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
+    Solver &sv = h->sv;
+    if (!sv.have_sav) return fail(CISMGPU_EINVAL, "nothing saved on this handle");
+    const size_t abytes = (size_t)4 * sv.NC * sv.nvec * sizeof(double), xbytes = (size_t)2 * sv.nvec * sizeof(double);
+    const Ptrs p = sv.ptrs();
+    CU(cudaMemcpyAsync(sv.A.p, sv.A_sav.p, abytes, cudaMemcpyDeviceToDevice, sv.stream));
+    CU(cudaMemcpyAsync(p.x0u, sv.x_sav.p, xbytes, cudaMemcpyDeviceToDevice, sv.stream));
+    CU(cudaStreamSynchronize(sv.stream));
+    sv.mixed.stale = true;  // the FP32 copies follow the restored matrix
+    sv.x_current = false;   // the current velocity is the saved one, and the next solve starts from it
     return CISMGPU_OK;
 }
 

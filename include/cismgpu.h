@@ -339,6 +339,15 @@ int cismgpu_solver_residual_vector(cismgpu_solver_t *s, double *resid_u, double 
                                    double *L2_norm_relative);
 int cismgpu_solver_residual_velocity(cismgpu_solver_t *s, int whichresid, double *resid_velo);
 
+/* The saved state of evaluate_accelerated_picard_{2d,3d} (glissade_velo_higher.F90:9898-10184)
+ * on a handle: cismgpu_solver_save keeps a device copy of the current velocity and of A
+ * ("uvel_sav = uvel; Auu_sav = Auu ..."; b is not saved, as there); cismgpu_solver_restore
+ * brings them back ("uvel = uvel_sav; Auu = Auu_sav ...": the restored velocity becomes the
+ * current one and the next solve's initial guess).  The scalar decision between extending,
+ * accepting and restoring stays with the caller.  Restore without a save: CISMGPU_EINVAL. */
+int cismgpu_solver_save(cismgpu_solver_t *s);
+int cismgpu_solver_restore(cismgpu_solver_t *s);
+
 /* Per-kernel CUDA-event timing of the structured matvec launches (off by default).
  * read: total device milliseconds, launch count, and algorithmic bytes per launch
  * (active owned nodes x (4*NC*sizeof(A) + vector streams)). */

@@ -109,3 +109,40 @@ def test_device_resident_picard_steps(gpu_lib, kind):
     # after the solve the residual vector is that of the new solution
     assert S.residual_vector(arrays=False)[2] == gpu_residual_vector(Q, x2[0], x2[1])[2]
     S.close()
+
+
+def test_accelerated_picard_save_restore(gpu_lib):
+    """evaluate_accelerated_picard's saved state on a handle: after save, a new system and a
+    solve, restore brings back the saved velocity and A (b stays the latest, as in the
+    reference); the residual and the next solve equal the one-shot calls on (A1, b2) from x1."""
+    P = problems.slab_3d(seed=46)
+    S = cg.DeviceSolver(P)
+    with pytest.raises(cg.CismGpuError):
+        S.restore()  # nothing saved yet
+    S.solve(cg.ALG_CHRONGEAR, 1, 5, 1e-10, 400)
+    x1 = S.x()
+    S.save()
+    A2 = [a * 1.07 for a in (P.Auu, P.Auv, P.Avu, P.Avv)]
+    b2u, b2v = P.bu * 0.95, P.bv * 0.95
+    S.set_system(*A2, b2u, b2v, x0_from_solution=True)
+    S.solve(cg.ALG_CHRONGEAR, 1, 5, 1e-10, 400)
+    S.restore()
+    Q = problems.slab_3d(seed=46)
+    Q.bu, Q.bv = b2u, b2v
+    ru, rv, l2, l2r = S.residual_vector()
+    want = gpu_residual_vector(Q, x1[0], x1[1])
+    np.testing.assert_array_equal(ru, want[0])
+    np.testing.assert_array_equal(rv, want[1])
+    assert (l2, l2r) == (want[2], want[3])
+    err, nit = S.solve(cg.ALG_CHRONGEAR, 1, 5, 1e-10, 400)
+    xu, xv = x1[0].copy(), x1[1].copy()
+    e2, n2 = cg.pcg_solver_chrongear_3d(Q.nx, Q.ny, Q.nz, Q.par, asm.indxA_2d(), asm.indxA_3d(), Q.active_vertex,
+                                        Q.Auu, Q.Auv, Q.Avu, Q.Avv, b2u, b2v, xu, xv, 1, 5, 1e-10, 400)
+    assert (err, nit) == (e2, n2)
+    np.testing.assert_array_equal(S.x()[0], xu)
+    np.testing.assert_array_equal(S.x()[1], xv)
+    # the mixed solver after a restore works on the restored matrix (its FP32 copy rebuilt)
+    S.restore()
+    em, nm = S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 2000)
+    assert em < 1e-8
+    S.close()
