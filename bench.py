@@ -416,6 +416,23 @@ def dist_setup(args):
     return world, rank, local
 
 
+def max_over_ranks(total_ms, pg, device="cuda"):
+    """The slowest rank's timed region (every rank passes its own, every rank gets the max).
+    pg is torch.distributed (an initialised default group) or None for one process."""
+    if not pg:
+        return float(total_ms)
+    import torch
+    t = torch.tensor([float(total_ms)], device=device, dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, steps, total_ms):
+    """Solves per second of the whole job: every rank (one replica per GPU) solved `steps`
+    systems within the slowest rank's total_ms."""
+    return world * steps / (total_ms / 1e3)
+
+
 # ---------------------------------------------------------------------------
 # reference arm: the CPU restatement on all host cores
 # ---------------------------------------------------------------------------
@@ -546,10 +563,7 @@ def run_ours(args):
     clk = clocks.stop()
     total_ms = t_start.elapsed_time(t_end)
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    if pg:
-        t = torch.tensor([total_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, pg, "cuda")
     prof_ms, prof_n, prof_bytes = S.profile_read()
     S.profile(False)
     xm = S.x()  # the mixed solution, before the FP64 solves below overwrite x
@@ -573,7 +587,7 @@ def run_ours(args):
     den = math.sqrt(float(np.sum(x64[0] ** 2) + np.sum(x64[1] ** 2)))
     err_vs_fp64 = num / den
 
-    value = world * args.steps / (total_ms / 1e3)
+    value = whole_job_rate(world, args.steps, total_ms)
     peak, peak_kind = hbm_peak()
     avg_launch_ms = prof_ms / max(prof_n, 1)
     achieved = prof_bytes / (avg_launch_ms / 1e3) / 1e9 if prof_n else None
