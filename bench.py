@@ -348,7 +348,8 @@ def hbm_peak():
 
 
 def ncu_traffic(kernel_key):
-    """Per-launch DRAM bytes of a kernel from the committed ncu summary (profiles/*.md), or None."""
+    """Per-launch DRAM bytes (dram__bytes_read.sum + write.sum of one ncu capture) of a kernel,
+    as recorded in profiles/traffic.json beside the capture summaries, or None."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as f:
