@@ -49,3 +49,36 @@ def test_built_for_sm100a_only():
     flags = build.flags()
     assert "arch=compute_100a,code=sm_100a" in flags
     assert "--fmad=false" in flags
+
+
+def _header_prototypes():
+    text = ""
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text += re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+    protos = {}
+    for m in re.finditer(r"\b(cismgpu_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        args = m.group(2).strip()
+        protos[m.group(1)] = 0 if args in ("", "void") else args.count(",") + 1
+    return protos
+
+
+def test_fortran_interfaces_match_the_header():
+    """Every bind(C) interface of the Fortran module names a declared C function with the same
+    number of arguments."""
+    src = open(os.path.join(ROOT, "cism_b200", "fortran", "glissade_velo_higher_pcg_gpu.F90")).read()
+    src = "\n".join(line.split("!")[0] for line in src.splitlines())  # drop comments
+    src = re.sub(r"&\s*\n\s*", " ", src)                                 # join continuation lines
+    protos = _header_prototypes()
+    found = re.findall(r"function\s+\w+\s*\(([^)]*)\)\s*bind\(C,\s*name=\"(cismgpu_[a-z0-9_]+)\"\)", src)
+    assert len(found) >= 8
+    for args, cname in found:
+        n = 0 if not args.strip() else args.count(",") + 1
+        assert cname in protos, cname
+        assert protos[cname] == n, (cname, protos[cname], n)
+
+
+def test_status_names_match_the_header():
+    import cism_b200 as cg
+    text = open(os.path.join(ROOT, "include", "cismgpu.h")).read()
+    codes = {int(v): n for n, v in re.findall(r"#define\s+(CISMGPU_(?:OK|E[A-Z0-9_]+))\s+(\d+)", text)}
+    assert codes == cg.STATUS_NAMES
