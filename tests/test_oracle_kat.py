@@ -136,12 +136,15 @@ def test_tridiag_precond_2d_matches_dense_line_solves(bc):
     np.testing.assert_allclose(zv3, wv, rtol=1e-10, atol=1e-12 * np.abs(wv).max())
 
 
+@pytest.mark.parametrize("case", [dict(seed=22, nz=5), dict(seed=24, nz=4, boundary_ice=True, bc="periodic"),
+                                  dict(seed=25, nz=4, boundary_ice=True, bc="outflow")],
+                         ids=["interior", "boundary-periodic", "boundary-outflow"])
 @pytest.mark.parametrize("precond", [3, 4])
-def test_tridiag_precond_3d_matches_dense(precond):
+def test_tridiag_precond_3d_matches_dense(precond, case):
     """Precond 3/4 in 3D: vertically summed couplings (all 27 folded onto the 9 horizontal
     ones), line solves of the summed residual, halo, then the SIA column solve of r plus the
     summed solution on every level (tridiag_solver_local_3d :4524-4658)."""
-    P = problems.slab_3d(seed=22, nz=5)
+    P = problems.slab_3d(**case)
     rng = np.random.default_rng(3)
     ru, rv = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bv.shape)
     st, zu, zv = oracle.precond_apply(P, precond, ru, rv)
@@ -166,8 +169,8 @@ def test_tridiag_precond_3d_matches_dense(precond):
         zsv[j0:j1, i] = _line_solve(sv[4][j0:j1, i], sv[1][j0:j1, i], sv[7][j0:j1, i], rsv[j0:j1, i])
     zsu = oracle.halo(P.nx, P.ny, 1, P.par, zsu)
     zsv = oracle.halo(P.nx, P.ny, 1, P.par, zsv)
-    for j in range(NY):
-        for i in range(NX):
+    for j in J:  # owned columns: halo columns of an outflow grid can hold all-zero rows
+        for i in I:
             for A, r, zs, z in ((P.Auu, ru, zsu, zu), (P.Avv, rv, zsv, zv)):
                 if P.active_vertex[j, i]:
                     T = np.diag(A[j, i, :, 13]) + np.diag(A[j, i, 1:, 4], -1) + np.diag(A[j, i, :-1, 22], 1)
