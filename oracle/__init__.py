@@ -11,7 +11,8 @@ Parity is unpinned against reference outputs (no Fortran compiler here and no
 golden vectors in the reference); see pcg_oracle.cpp's header.
 
 Sum modes: SUM_SEQ (the reference's order), SUM_EXACT (exact, reproducible),
-SUM_DDTREE (restatement of the GPU library's reduction tree).
+SUM_DDTREE (restatement of the GPU library's reduction tree), SUM_REPRO (restatement of
+the reference's reprosum branch, cism_reprosum_mod.F90, as CISM calls it on one rank).
 """
 from __future__ import annotations
 
@@ -21,7 +22,7 @@ import subprocess
 
 import numpy as np
 
-SUM_SEQ, SUM_EXACT, SUM_DDTREE = 0, 1, 2
+SUM_SEQ, SUM_EXACT, SUM_DDTREE, SUM_REPRO = 0, 1, 2, 3
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
@@ -63,6 +64,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_compute_residual_velocity.argtypes = [i, i, i, i, i, P(_Par), d, d, d, d, i]
         L.oracle_compute_residual_velocity.restype = dbl
         L.oracle_exact_sum.argtypes = [d, ctypes.c_long]
+        L.oracle_reprosum.argtypes = [d, ctypes.c_long]
+        L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
         _lib = L
     return _lib
@@ -178,6 +181,12 @@ def residual_velocity(prob, whichresid: int, uvel, vvel, usav, vsav, summode: in
     arrs = [_p(np.ascontiguousarray(a, dtype=np.float64)) for a in (uvel, vvel, usav, vsav)]
     return lib().oracle_compute_residual_velocity(int(is3d), whichresid, prob.nx, prob.ny, prob.nz if is3d else 1,
                                                   ctypes.byref(par), *arrs, summode)
+
+
+def reprosum(a) -> float:
+    """The reference's reproducible sum (cism_reprosum_calc as CISM calls it, one rank)."""
+    a = np.ascontiguousarray(a, dtype=np.float64).ravel()
+    return lib().oracle_reprosum(_p(a), a.size)
 
 
 def exact_sum(a) -> float:

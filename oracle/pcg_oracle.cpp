@@ -54,6 +54,10 @@
 //                       column chunks of 256, warp and block trees); with it the whole solve is
 //                       bit-identical to the GPU, which isolates summation order as the only
 //                       source of difference against ORACLE_SUM_SEQ.
+//   ORACLE_SUM_REPRO  : a restatement of the reference's reprosum branch as CISM calls it on one
+//                       rank and one thread (parallel_reduce_reprosum, parallel_mpi.F90:9618-9725,
+//                       cism_reprosum_calc and cism_reprosum_int, libglimmer/cism_reprosum_mod.F90:
+//                       237-1057 and 1063-1818): the integer-vector fixed-point sum.
 
 #include <cmath>
 #include <cstdint>
@@ -65,7 +69,7 @@
 
 namespace {
 
-enum { ORACLE_SUM_SEQ = 0, ORACLE_SUM_EXACT = 1, ORACLE_SUM_DDTREE = 2 };
+enum { ORACLE_SUM_SEQ = 0, ORACLE_SUM_EXACT = 1, ORACLE_SUM_DDTREE = 2, ORACLE_SUM_REPRO = 3 };
 
 // ---------------------------------------------------------------------------
 // Exact summation: a Kulisch-style fixed-point accumulator over the whole
@@ -261,6 +265,157 @@ typedef std::vector<double> Vec;
 
 // parallel_global_sum_stagger (3D and 2D; nz = 1 for 2D), one field with arr2.
 // Vectors are in Fortran layout (nz, NX, NY), so element (k, q) is at k-1 + nz*q.
+// ---------------------------------------------------------------------------
+// reprosum (libglimmer/cism_reprosum_mod.F90), one field, one rank, one OpenMP thread, called
+// as parallel_reduce_reprosum does (parallel_mpi.F90:9691-9707): no global-max or level hints,
+// so cism_reprosum_calc takes its "recompute" path (:442-525): exponent range of the nonzero
+// summands, arr_max_shift from the summand count, max_levels from the range, then
+// cism_reprosum_int with validate = .false.  Fortran intrinsics on IEEE doubles: exponent(x)
+// and fraction(x) are frexp's exponent and mantissa, scale(x,n) = x*2^n, set_exponent(x,e) =
+// fraction(x)*2^e; digits(1.0_r8) = 53, digits(1_i8) = 63, MINEXPONENT(1.0_r8) = -1021,
+// MAXEXPONENT(1.0_r8) = 1024; int(x,i8) truncates; i8 division truncates toward zero.
+// ---------------------------------------------------------------------------
+inline int f_exponent(double x) { int e; std::frexp(x, &e); return e; }
+inline double f_fraction(double x) { int e; return std::frexp(x, &e); }
+inline double f_set_exponent(double x, int e) { return std::ldexp(f_fraction(x), e); }
+
+double reprosum(const std::vector<double> &arr) {
+    const int kDigR8 = 53, kDigI8 = 63, kMinExp = -1021, kMaxExp = 1024;
+    const long nsummands = (long)arr.size();
+    // exponent extremes of the nonzero summands (:455-487)
+    int lmin = kMaxExp, lmax = kMinExp;
+    for (double x : arr)
+        if (x != 0.0) {
+            const int e = f_exponent(x);
+            lmin = std::min(e, lmin);
+            lmax = std::max(e, lmax);
+        }
+    const int gmax = lmax;
+    const int gmin = std::min(gmax, lmin);
+    long max_nsummands = nsummands / 1 + 1;      // (max_nsummands/omp_nthreads) + 1 (:501)
+    max_nsummands = std::max(max_nsummands, 1L); // max(., tasks*omp_nthreads)
+    const int shift = kDigI8 - (f_exponent((double)max_nsummands) + 1);
+    if (shift < 2) return NAN;                   // mpi_abort in the reference (:505-510)
+    const int max_levels = 2 + (kDigR8 + (gmax - gmin)) / shift;
+    const int extra_levels = (kDigI8 - 1) / shift;
+    const int min_level = -(extra_levels - 1);
+    const int64_t R = (int64_t)1 << shift;       // i8_radix**arr_max_shift
+    // levels min_level..max_levels
+    std::vector<int64_t> lv(max_levels - min_level + 1, 0);
+    auto L = [&](int level) -> int64_t & { return lv[level - min_level]; };
+    // integer expansion of every summand (:1199-1262)
+    for (double x : arr) {
+        if (x == 0.0) continue;
+        const int e = f_exponent(x);
+        const double f = f_fraction(x);
+        int ashift = shift - (gmax - e);
+        int ilevel;
+        if (ashift < 1) {
+            ilevel = (1 + (gmax - e)) / shift;
+            ashift = ilevel * shift - (gmax - e);
+            while (ashift < 1) {
+                ashift += shift;
+                ilevel += 1;
+            }
+        } else {
+            ilevel = 1;
+        }
+        if (ilevel <= max_levels) {
+            double rem = std::ldexp(f, ashift);
+            int64_t v = (int64_t)rem;
+            L(ilevel) += v;
+            rem = rem - (double)v;
+            while (rem != 0.0 && ilevel < max_levels) {
+                ilevel += 1;
+                rem = std::ldexp(rem, shift);
+                v = (int64_t)rem;
+                L(ilevel) += v;
+                rem = rem - (double)v;
+            }
+        }
+    }
+    auto carry = [&]() {  // (:1266-1276, :1361-1371, :1403-1413)
+        for (int l = max_levels; l >= min_level + 1; --l)
+            if ((L(l) < 0 ? -L(l) : L(l)) >= R) {
+                const int64_t ix = L(l) / R;
+                L(l - 1) += ix;
+                L(l) -= ix * R;
+            }
+    };
+    carry();  // per thread
+    carry();  // after the (one-rank) allreduce
+    // sign and same-sign digits (:1373-1401)
+    int ilevel = min_level;
+    while (L(ilevel) == 0 && ilevel < max_levels) ++ilevel;
+    const int64_t sgn = (L(ilevel) < 0) ? -1 : 1;
+    auto fsign = [](int64_t v) -> int64_t { return v < 0 ? -1 : 1; };
+    if (ilevel < max_levels)
+        for (int j = ilevel; j <= max_levels - 1; ++j)
+            if (fsign(L(j)) != fsign(L(j + 1)) || L(j + 1) == 0) {
+                L(j) -= sgn;
+                L(j + 1) += sgn * R;
+            }
+    if (sgn < 0)
+        for (int j = ilevel; j <= max_levels; ++j) L(j) = -L(j);
+    carry();
+    // floating-point pieces of at most 53 digits each (:1415-1487)
+    std::vector<double> sv;
+    bool first = true;
+    int ash = gmax - min_level * shift;
+    int digit_count = 0;
+    int begin_level = min_level;
+    while (begin_level <= max_levels) {
+        int trunc_loc = 0, trunc_level = max_levels;
+        for (int l = begin_level; l <= max_levels; ++l) {
+            int LX;
+            if (first) {
+                if (digit_count == 0) LX = (L(l) != 0) ? f_exponent((double)L(l)) : 0;
+                else LX = shift;
+            } else {
+                LX = (l == begin_level && digit_count != 0) ? 0 : shift;
+            }
+            if (digit_count + LX >= kDigR8) {
+                trunc_level = l;
+                trunc_loc = (digit_count + LX) - kDigR8;
+                break;
+            }
+            digit_count += LX;
+        }
+        first = false;
+        int64_t trunc_rem = 0;
+        if (trunc_loc != 0) {
+            const int64_t P = (int64_t)1 << trunc_loc;
+            int64_t ix = L(trunc_level) / P;
+            ix = ix * P;
+            trunc_rem = L(trunc_level) - ix;
+            L(trunc_level) = ix;
+        }
+        double piece = 0.0;
+        for (int l = begin_level; l <= trunc_level; ++l) {
+            if (L(l) != 0) {
+                const double X = (double)L(l);
+                const int cur = f_exponent(X) + ash;
+                if (cur >= kMinExp) piece = piece + f_set_exponent(X, cur);
+                else piece = piece + std::ldexp(f_set_exponent(X, cur - kMinExp), kMinExp);
+            }
+            if (l < trunc_level || trunc_loc == 0) ash -= shift;
+        }
+        sv.push_back(piece);
+        if (trunc_loc == 0) {
+            digit_count = 0;
+            begin_level = trunc_level + 1;
+        } else {
+            digit_count = trunc_loc;
+            begin_level = trunc_level;
+            L(trunc_level) = trunc_rem;
+        }
+    }
+    // smallest to largest, then the sign (:1489-1495)
+    double sum = 0.0;
+    for (long j = (long)sv.size() - 1; j >= 0; --j) sum = sum + sv[j];
+    return (double)sgn * sum;
+}
+
 double global_sum(const Ctx &c, const Vec &a1, const Vec &a2) {
     const Geom &g = c.g;
     const cismgpu_par_t &p = c.par;
@@ -273,6 +428,15 @@ double global_sum(const Ctx &c, const Vec &a1, const Vec &a2) {
                     local_sum = local_sum + a1[e] + a2[e];
                 }
         return local_sum;  // parallel_reduce_sum on one rank
+    } else if (c.summode == ORACLE_SUM_REPRO) {  // parallel_mpi.F90:6703-6738: arr(count) = arr1 + arr2
+        std::vector<double> arr;
+        for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+            for (int i = p.staggered_ilo; i <= p.staggered_ihi; ++i)
+                for (int k = 1; k <= g.nz; ++k) {
+                    long e = g.v3(k, i, j);
+                    arr.push_back(a1[e] + a2[e]);
+                }
+        return reprosum(arr);
     } else if (c.summode == ORACLE_SUM_EXACT) {
         ExactAcc acc;
         for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
@@ -1071,6 +1235,9 @@ double oracle_compute_residual_velocity(int is3d, int whichresid, int nx, int ny
     Vec u(uvel, uvel + n), v(vvel, vvel + n), us(usav, usav + n), vs(vsav, vsav + n);
     return resid_velocity(c, is3d != 0, whichresid, u, v, us, vs);
 }
+
+// reprosum of n doubles (the reference's reproducible sum, one rank)
+double oracle_reprosum(const double *a, long n) { return reprosum(std::vector<double>(a, a + n)); }
 
 // exact correctly-rounded sum of n doubles
 double oracle_exact_sum(const double *a, long n) {

@@ -248,6 +248,54 @@ def test_residual_velocity_matches_numpy(kind, which):
         assert got == d.max()
 
 
+def test_reprosum_restatement_properties():
+    """The restated reprosum (cism_reprosum_calc/int as CISM calls them, one rank): the exact
+    fixed-point sum converted through 53-digit pieces added smallest first.  It equals the
+    correctly rounded exact sum except where that conversion double-rounds near a tie (at most
+    1 ulp), and it does not depend on the order of the summands."""
+    rng = np.random.default_rng(11)
+    for t in range(300):
+        n = int(rng.integers(1, 2000))
+        if t % 3 == 0:
+            a = rng.standard_normal(n)
+        elif t % 3 == 1:
+            a = rng.standard_normal(n) * np.exp(rng.uniform(-690, 690, n))   # wide exponent range
+        else:
+            a = np.where(rng.random(n) < 0.5, 0.0, rng.standard_normal(n) * 1e7)  # zeros
+        assert oracle.reprosum(a) == oracle.exact_sum(a)
+    # near a tie: 1 + 2^-53 + 2^-106 - tiny rounds up exactly, but the piece 2^-53 + (2^-106 - tiny)
+    # first rounds to 2^-53, and 1 + 2^-53 then rounds to even
+    a = np.array([1.0, 2.0**-53, 2.0**-106, -1e-40])
+    assert oracle.exact_sum(a) == 1.0 + 2.0**-52 and oracle.reprosum(a) == 1.0
+    b = rng.standard_normal(3000) * np.exp(rng.uniform(-200, 200, 3000))
+    assert len({oracle.reprosum(rng.permutation(b)) for _ in range(10)}) == 1
+    assert oracle.reprosum(np.zeros(7)) == 0.0
+
+
+def test_global_sum_repro_mode():
+    """The oracle's SUM_REPRO global sum (the reference's reprosum branch) on owned vertices."""
+    P = problems.slab_3d(seed=13, boundary_ice=True, bc="periodic")
+    rng = np.random.default_rng(12)
+    a1, a2 = rng.standard_normal(P.bu.shape), rng.standard_normal(P.bu.shape)
+    p = P.par
+    sl = (slice(p["staggered_jlo"] - 1, p["staggered_jhi"]), slice(p["staggered_ilo"] - 1, p["staggered_ihi"]))
+    want = oracle.reprosum((a1 + a2)[sl].ravel())
+    assert oracle.global_sum(P.nx, P.ny, P.nz, P.par, a1, a2, oracle.SUM_REPRO) == want
+    assert want == oracle.global_sum(P.nx, P.ny, P.nz, P.par, a1, a2, oracle.SUM_EXACT)
+
+
+@pytest.mark.parametrize("case", ["dome-sia", "slab2d-diag"])
+def test_reprosum_solve_equals_exact_sum_solve(case):
+    """A whole solve with the reference's reprosum sums is bit-identical to the solve with
+    correctly rounded exact sums (no sum of these solves lands on a double-rounding tie)."""
+    P, pc = (asm.dome(), 2) if case == "dome-sia" else (problems.slab_2d(seed=12), 1)
+    r = oracle.pcg("chrongear", P, pc, summode=oracle.SUM_REPRO, maxiters=2000)
+    e = oracle.pcg("chrongear", P, pc, summode=oracle.SUM_EXACT, maxiters=2000)
+    assert r[0] == e[0] == 0 and r[4] == e[4] and r[3] == e[3]
+    np.testing.assert_array_equal(r[1], e[1])
+    np.testing.assert_array_equal(r[2], e[2])
+
+
 def test_exact_sum_is_correctly_rounded():
     rng = np.random.default_rng(7)
     for trial in range(20):
