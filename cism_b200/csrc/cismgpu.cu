@@ -112,6 +112,7 @@ struct Solver {
     DevBuf A, raw, vec, act, partials, state, map;
     DevBuf tri;       // tridiagonal preconditioner planes (TriPlane), on first use
     DevBuf A_sav, x_sav;      // accelerated Picard's saved matrix and velocity (cismgpu_solver_save)
+    DevBuf rsum;              // the reproducible sum's exponent extremes and level sums
     bool have_sav = false;
     bool x_current = false;   // the x planes hold a solution (a solve ran since the last upload)
     int32_t hindx[27] = {};   // host copy of the uploaded indxA map (27 or 9 entries)
@@ -136,6 +137,7 @@ struct Solver {
         tri.release();
         A_sav.release();
         x_sav.release();
+        rsum.release();
         have_sav = false;
         mixed.release();
         if (h_done) cudaFreeHost(h_done);
@@ -1169,6 +1171,10 @@ static int oneshot_resid_velo(bool is3d, int whichresid, int nx, int ny, int nz,
     return sv.residual_velocity(whichresid, VX_U, VX0_U, resid_velo);
 }
 
+}  // namespace cismgpu
+#include "reprosum.cu"
+namespace cismgpu {
+
 static int oneshot_global_sum(int nx, int ny, int nz, const cismgpu_par_t *par, const double *a1, const double *a2,
                               double *sum) {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -1191,6 +1197,7 @@ static int oneshot_global_sum(int nx, int ny, int nz, const cismgpu_par_t *par, 
     SolveState *st = sv.state.as<SolveState>();
     CU(cudaMemcpyAsync(d1, a1, n * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
     CU(cudaMemcpyAsync(d2, a2, n * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
+    if (par->reprosum) return repro_global_sum(sv.stream, g, d1, d2, sv.rsum, sum);  // parallel_mpi.F90:6703-6738
     CU(cudaMemsetAsync(st, 0, sizeof(SolveState), sv.stream));
     k_gsum<true><<<nb, kBlock, 0, sv.stream>>>(g, d1, d2, sv.partials.as<DD>(), &st->ticket[0], &st->err);
     CU(cudaGetLastError());

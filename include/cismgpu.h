@@ -150,10 +150,13 @@ int cismgpu_matvec_structured_2d(int nx, int ny, const cismgpu_par_t *par,
 /* Mirrors parallel_global_sum_stagger(arr1, parallel, arr2)
  * (libglimmer/parallel_mpi.F90: _real8_2d :6537-6658, _real8_3d :6663-6794) on one rank:
  * the sum over locally owned vertices of arr1 + arr2.  Host arrays in the caller's layout
- * (nz, nx-1, ny-1); nz = 1 for 2D fields.  The sum uses the library's fixed
- * double-double reduction tree (the same one every solver uses), so it is independent
- * of the launch and reproducible; it equals the correctly rounded exact sum except in
- * rare near-tie cases.  *sum receives the result. */
+ * (nz, nx-1, ny-1); nz = 1 for 2D fields.  With par->reprosum == 0 the sum uses the
+ * library's fixed double-double reduction tree (the same one every solver uses): launch-
+ * independent and reproducible, the correctly rounded exact sum except in rare near-tie
+ * cases.  With par->reprosum != 0 it is the reference's reproducible sum
+ * (parallel_reduce_reprosum -> cism_reprosum_calc, libglimmer/cism_reprosum_mod.F90:
+ * 237-1818): the integer-vector fixed-point sum, its value independent of the order of the
+ * summands, bit for bit the reference's on one rank.  *sum receives the result. */
 int cismgpu_global_sum_stagger(int nx, int ny, int nz, const cismgpu_par_t *par,
                                const double *arr1, const double *arr2, double *sum);
 

@@ -228,3 +228,23 @@ def test_global_sum_stagger(gpu_lib, nz, bc):
     assert g == oracle.global_sum(nx, ny, nz, par, a1, a2, oracle.SUM_EXACT)
     seq = oracle.global_sum(nx, ny, nz, par, a1, a2, oracle.SUM_SEQ)
     assert abs(g - seq) <= 1e-12 * np.sum(np.abs(a1 + a2))
+
+
+@pytest.mark.parametrize("nz,bc,spread", [(11, "periodic", 20), (1, "outflow", 600), (7, "no_ice", 300)])
+def test_global_sum_reprosum(gpu_lib, nz, bc, spread):
+    """parallel_global_sum_stagger with parallel%reprosum: the reference's integer-vector sum
+    (cism_reprosum_calc as CISM calls it), bit-identical to the oracle's restatement, also for
+    exponent spreads of hundreds of binades, zeros, and a near-tie the reference double-rounds."""
+    nx, ny = 37, 29
+    par = dict(asm.default_par(nx, ny, bc), reprosum=1)
+    rng = np.random.default_rng(nz + spread)
+    a1 = rng.standard_normal((ny - 1, nx - 1, nz)) * np.exp(rng.uniform(-spread, spread, (ny - 1, nx - 1, nz)))
+    a2 = np.where(rng.random((ny - 1, nx - 1, nz)) < 0.3, 0.0, rng.standard_normal((ny - 1, nx - 1, nz)))
+    g = cg.parallel_global_sum_stagger(nx, ny, nz, par, a1, a2)
+    assert g == oracle.global_sum(nx, ny, nz, par, a1, a2, oracle.SUM_REPRO)
+    # a near-tie: 1 + 2^-53 + 2^-106 - 1e-40 on four owned vertices, zeros elsewhere
+    z1, z2 = np.zeros_like(a1), np.zeros_like(a2)
+    j, i = par["staggered_jlo"] - 1, par["staggered_ilo"] - 1
+    z1[j, i, 0], z1[j, i + 1, 0], z1[j + 1, i, 0], z1[j + 1, i + 1, 0] = 1.0, 2.0**-53, 2.0**-106, -1e-40
+    t = cg.parallel_global_sum_stagger(nx, ny, nz, par, z1, z2)
+    assert t == oracle.global_sum(nx, ny, nz, par, z1, z2, oracle.SUM_REPRO) == 1.0
