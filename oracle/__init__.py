@@ -65,6 +65,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_compute_residual_velocity.restype = dbl
         L.oracle_exact_sum.argtypes = [d, ctypes.c_long]
         L.oracle_reprosum.argtypes = [d, ctypes.c_long]
+        L.oracle_check_symmetry.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, P(dbl), P(ctypes.c_long)]
         L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
         _lib = L
@@ -181,6 +182,24 @@ def residual_velocity(prob, whichresid: int, uvel, vvel, usav, vsav, summode: in
     arrs = [_p(np.ascontiguousarray(a, dtype=np.float64)) for a in (uvel, vvel, usav, vsav)]
     return lib().oracle_compute_residual_velocity(int(is3d), whichresid, prob.nx, prob.ny, prob.nz if is3d else 1,
                                                   ctypes.byref(par), *arrs, summode)
+
+
+def check_symmetry(prob, Auu=None, Auv=None, Avu=None, Avv=None):
+    """check_symmetry_assembled_matrix_{2d,3d} on prob's matrix (or the given blocks, prob's
+    layout).  Returns (Auu, Auv, Avu, Avv, maxdiff, nwarn): copies of the blocks, with the 3D
+    check's averages written in (the 2D check changes nothing), the largest asymmetry seen and
+    the number of asymmetry warnings the reference prints."""
+    is3d = prob.kind == "3d"
+    blocks = [np.array(prob.Auu if Auu is None else Auu, dtype=np.float64, copy=True),
+              np.array(prob.Auv if Auv is None else Auv, dtype=np.float64, copy=True),
+              np.array(prob.Avu if Avu is None else Avu, dtype=np.float64, copy=True),
+              np.array(prob.Avv if Avv is None else Avv, dtype=np.float64, copy=True)]
+    md, nw = ctypes.c_double(0.0), ctypes.c_long(0)
+    par = _par(prob.par)
+    lib().oracle_check_symmetry(int(is3d), prob.nx, prob.ny, prob.nz if is3d else 1, ctypes.byref(par),
+                                _p(indx3() if is3d else indx2()), _p(prob.active_vertex), *[_p(b) for b in blocks],
+                                ctypes.byref(md), ctypes.byref(nw))
+    return (*blocks, md.value, nw.value)
 
 
 def reprosum(a) -> float:

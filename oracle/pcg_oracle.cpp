@@ -1093,6 +1093,98 @@ double resid_velocity(const Ctx &c, bool is3d, int whichresid, const Vec &u, con
 // ---------------------------------------------------------------------------
 // C ABI of the oracle (same argument lists as include/cismgpu.h plus a sum mode)
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// check_symmetry_assembled_matrix_{3d,2d} (glissade_velo_higher.F90:10648-10850 and
+// :10854-11117): every owned active row compares each coefficient with its transpose partner
+// (Auu with Auu^T, Auv with Avu^T, Avv with Avv^T, Avu with Auv^T).  A visit whose two values
+// differ raises maxdiff to |val2 - val1| and either averages the pair, when the difference is
+// below eps11 (glimmer_paramets.F90:77, 1e-11) times |diag| of the visited row's block (Auu's
+// diagonal for the Auu and Auv checks, Avv's for Avv and Avu), or prints a warning.  The 3D
+// check writes the averages in place; the 2D check only reports (its averaging is commented
+// out).  nwarn counts the asymmetry warnings.  A partner outside the arrays (an owned row at
+// the array edge) is skipped; the reference would read outside its arrays there.
+// ---------------------------------------------------------------------------
+constexpr double kEps11 = 1.0e-11;
+
+struct SymCheck {
+    double maxdiff = 0.0;
+    long nwarn = 0;
+};
+
+inline void sym_visit(SymCheck &r, double &x1, double &x2, double diag, bool fix) {
+    const double val1 = x1, val2 = x2;
+    if (val2 != val1) {
+        if (std::fabs(val2 - val1) > r.maxdiff) r.maxdiff = std::fabs(val2 - val1);
+        if (std::fabs(val2 - val1) < kEps11 * std::fabs(diag)) {
+            if (fix) {
+                const double avg = 0.5 * (val1 + val2);
+                x1 = avg;
+                x2 = avg;
+            }
+        } else {
+            ++r.nwarn;
+        }
+    }
+}
+
+// :10854-11117, rows in j, i, k order; per row the Auu/Auv loop, then the Avv/Avu loop, each
+// over jA, iA, kA with k+kA inside 1..nz
+SymCheck sym_check3(const Ctx &c, double *Auu, double *Auv, double *Avu, double *Avv) {
+    const Geom &g = c.g;
+    const cismgpu_par_t &p = c.par;
+    SymCheck r;
+    const int md = c.I3(0, 0, 0);
+    for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+        for (int i = p.staggered_ilo; i <= p.staggered_ihi; ++i) {
+            if (!c.act(i, j)) continue;
+            for (int k = 1; k <= g.nz; ++k)
+                for (int pass = 0; pass < 2; ++pass) {
+                    const double diag = pass == 0 ? Auu[g.a3(md, k, i, j)] : Avv[g.a3(md, k, i, j)];
+                    for (int jA = -1; jA <= 1; ++jA)
+                        for (int iA = -1; iA <= 1; ++iA)
+                            for (int kA = -1; kA <= 1; ++kA) {
+                                if (k + kA < 1 || k + kA > g.nz) continue;
+                                if (i + iA < 1 || i + iA > g.NX || j + jA < 1 || j + jA > g.NY) continue;
+                                const long a = g.a3(c.I3(iA, jA, kA), k, i, j);
+                                const long b = g.a3(c.I3(-iA, -jA, -kA), k + kA, i + iA, j + jA);
+                                if (pass == 0) {
+                                    sym_visit(r, Auu[a], Auu[b], diag, true);
+                                    sym_visit(r, Auv[a], Avu[b], diag, true);
+                                } else {
+                                    sym_visit(r, Avv[a], Avv[b], diag, true);
+                                    sym_visit(r, Avu[a], Auv[b], diag, true);
+                                }
+                            }
+                }
+        }
+    return r;
+}
+
+// :10648-10850, jA, iA outer, owned active rows inner; nothing is modified
+SymCheck sym_check2(const Ctx &c, const double *Auu, const double *Auv, const double *Avu, const double *Avv) {
+    const Geom &g = c.g;
+    const cismgpu_par_t &p = c.par;
+    SymCheck r;
+    const int md = c.I2(0, 0);
+    for (int jA = -1; jA <= 1; ++jA)
+        for (int iA = -1; iA <= 1; ++iA) {
+            const int m = c.I2(iA, jA), mm = c.I2(-iA, -jA);
+            for (int j = p.staggered_jlo; j <= p.staggered_jhi; ++j)
+                for (int i = p.staggered_ilo; i <= p.staggered_ihi; ++i) {
+                    if (!c.act(i, j)) continue;
+                    if (i + iA < 1 || i + iA > g.NX || j + jA < 1 || j + jA > g.NY) continue;
+                    const long a = g.a2(i, j, m), b = g.a2(i + iA, j + jA, mm);
+                    double v1, v2;
+                    const double du = Auu[g.a2(i, j, md)], dv = Avv[g.a2(i, j, md)];
+                    sym_visit(r, v1 = Auu[a], v2 = Auu[b], du, false);
+                    sym_visit(r, v1 = Auv[a], v2 = Avu[b], du, false);
+                    sym_visit(r, v1 = Avv[a], v2 = Avv[b], dv, false);
+                    sym_visit(r, v1 = Avu[a], v2 = Auv[b], dv, false);
+                }
+        }
+    return r;
+}
+
 extern "C" {
 
 int oracle_pcg_standard_3d(int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indxA_2d,
@@ -1234,6 +1326,19 @@ double oracle_compute_residual_velocity(int is3d, int whichresid, int nx, int ny
     const long n = c.g.ntot();
     Vec u(uvel, uvel + n), v(vvel, vvel + n), us(usav, usav + n), vs(vsav, vsav + n);
     return resid_velocity(c, is3d != 0, whichresid, u, v, us, vs);
+}
+
+// check_symmetry_assembled_matrix_{3d,2d}: is3d ? (27,nz,nx-1,ny-1) blocks, averaged in
+// place, indx = indxA_3d : (nx-1,ny-1,9) blocks, unchanged, indx = indxA_2d.
+int oracle_check_symmetry(int is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indx,
+                          const int32_t *active_vertex, double *Auu, double *Auv, double *Avu, double *Avv,
+                          double *maxdiff, long *nwarn) {
+    Ctx c{Geom{is3d ? nz : 1, nx - 1, ny - 1}, *par, 0, is3d ? nullptr : indx, is3d ? indx : nullptr,
+          active_vertex};
+    const SymCheck r = is3d ? sym_check3(c, Auu, Auv, Avu, Avv) : sym_check2(c, Auu, Auv, Avu, Avv);
+    *maxdiff = r.maxdiff;
+    *nwarn = r.nwarn;
+    return 0;
 }
 
 // reprosum of n doubles (the reference's reproducible sum, one rank)
