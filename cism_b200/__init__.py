@@ -27,7 +27,9 @@ __all__ = [
     "pcg_solver_standard_2d", "pcg_solver_chrongear_2d", "matvec_multiply_structured_3d",
     "matvec_multiply_structured_2d", "HO_PRECOND_NONE", "HO_PRECOND_DIAG", "HO_PRECOND_SIA",
     "HO_PRECOND_TRIDIAG_LOCAL", "HO_PRECOND_TRIDIAG_GLOBAL", "DeviceSolver", "solve_batch",
-    "ALG_STANDARD", "ALG_CHRONGEAR", "ALG_MIXED_CHRONGEAR",
+    "ALG_STANDARD", "ALG_CHRONGEAR", "ALG_MIXED_CHRONGEAR", "compute_residual_vector_3d",
+    "compute_residual_vector_2d", "compute_residual_velocity_3d", "compute_residual_velocity_2d",
+    "check_symmetry_assembled_matrix_3d", "check_symmetry_assembled_matrix_2d",
 ]
 
 ALG_STANDARD, ALG_CHRONGEAR, ALG_MIXED_CHRONGEAR = 0, 1, 2
@@ -174,10 +176,15 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_solver_residual_velocity.argtypes = [vp, i32, P(dbl)]
     lib.cismgpu_solver_save.argtypes = [vp]
     lib.cismgpu_solver_restore.argtypes = [vp]
+    i64 = ctypes.c_longlong
+    lib.cismgpu_check_symmetry_assembled_matrix_3d.argtypes = [i32, i32, i32, par, d, d, d, d, d, d, P(dbl), P(i64)]
+    lib.cismgpu_check_symmetry_assembled_matrix_2d.argtypes = [i32, i32, par, d, d, d, d, d, d, P(dbl), P(i64)]
+    lib.cismgpu_solver_check_symmetry.argtypes = [vp, P(dbl), P(i64)]
     for f in ("cismgpu_compute_residual_vector_3d", "cismgpu_compute_residual_vector_2d",
               "cismgpu_compute_residual_velocity_3d", "cismgpu_compute_residual_velocity_2d",
               "cismgpu_solver_set_system", "cismgpu_solver_residual_vector", "cismgpu_solver_residual_velocity",
-              "cismgpu_solver_save", "cismgpu_solver_restore"):
+              "cismgpu_solver_save", "cismgpu_solver_restore", "cismgpu_check_symmetry_assembled_matrix_3d",
+              "cismgpu_check_symmetry_assembled_matrix_2d", "cismgpu_solver_check_symmetry"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -390,6 +397,37 @@ def compute_residual_velocity_2d(whichresid, nx, ny, parallel, uvel, vvel, usav,
     return out.value
 
 
+def check_symmetry_assembled_matrix_3d(nx, ny, nz, parallel, indxA_3d, active_vertex, Auu, Auv, Avu, Avv):
+    """Mirrors check_symmetry_assembled_matrix_3d (glissade_velo_higher.F90:10854-11117): the
+    nearly symmetric pairs of the four blocks are averaged in place (the arrays must be
+    writable float64 in the caller's layout).  Returns (maxdiff, nwarn): the largest asymmetry
+    met and the number of asymmetry warnings the reference logs."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    nblk = nv * nz * 27
+    md, nw = ctypes.c_double(0.0), ctypes.c_longlong(0)
+    par = _par(parallel)
+    _check(lib, lib.cismgpu_check_symmetry_assembled_matrix_3d(
+        nx, ny, nz, ctypes.byref(par), _ptr(np.ascontiguousarray(indxA_3d, dtype=np.int32), np.int32, 27),
+        _ptr(active_vertex, np.int32, nv), _ptr(Auu, np.float64, nblk, True), _ptr(Auv, np.float64, nblk, True),
+        _ptr(Avu, np.float64, nblk, True), _ptr(Avv, np.float64, nblk, True), ctypes.byref(md), ctypes.byref(nw)))
+    return md.value, nw.value
+
+
+def check_symmetry_assembled_matrix_2d(nx, ny, parallel, indxA_2d, active_vertex, Auu, Auv, Avu, Avv):
+    """Mirrors check_symmetry_assembled_matrix_2d (glissade_velo_higher.F90:10648-10850), which
+    only reports: returns (maxdiff, nwarn) and leaves the blocks unchanged."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    md, nw = ctypes.c_double(0.0), ctypes.c_longlong(0)
+    par = _par(parallel)
+    _check(lib, lib.cismgpu_check_symmetry_assembled_matrix_2d(
+        nx, ny, ctypes.byref(par), _ptr(np.ascontiguousarray(indxA_2d, dtype=np.int32), np.int32, 9),
+        _ptr(active_vertex, np.int32, nv), _ptr(Auu, np.float64, nv * 9), _ptr(Auv, np.float64, nv * 9),
+        _ptr(Avu, np.float64, nv * 9), _ptr(Avv, np.float64, nv * 9), ctypes.byref(md), ctypes.byref(nw)))
+    return md.value, nw.value
+
+
 class DeviceSolver:
     """A device-resident linear system (cismgpu_solver_create): A, b and x0 live in HBM.
 
@@ -459,6 +497,13 @@ class DeviceSolver:
         _check(self._lib, self._lib.cismgpu_solver_residual_vector(self.handle, pu, pv, ctypes.byref(l2),
                                                                    ctypes.byref(l2r)))
         return ru, rv, l2.value, l2r.value
+
+    def check_symmetry(self):
+        """check_symmetry_assembled_matrix on the resident blocks (3D: the averages go into the
+        device copy the next solve uses); returns (maxdiff, nwarn)."""
+        md, nw = ctypes.c_double(0.0), ctypes.c_longlong(0)
+        _check(self._lib, self._lib.cismgpu_solver_check_symmetry(self.handle, ctypes.byref(md), ctypes.byref(nw)))
+        return md.value, nw.value
 
     def save(self):
         """Accelerated Picard's saved state: the current velocity and A (not b) on the device."""

@@ -286,6 +286,48 @@ struct Solver {
         return CISMGPU_OK;
     }
 
+    // check_symmetry_assembled_matrix_{3d,2d} (glissade_velo_higher.F90:10648-11117) on four
+    // device blocks in layout L: 3D averages the nearly symmetric pairs in place, 2D only
+    // reports.  maxdiff: the largest asymmetry seen; nwarn: the reference's asymmetry warnings.
+    // Leaves the stream synchronized.
+    int sym_check(const SymIdx &L, double *Auu, double *Auv, double *Avu, double *Avv, double *maxdiff,
+                  long long *nwarn) {
+        CU(rsum.ensure(2 * sizeof(unsigned long long)));
+        unsigned long long *out = rsum.as<unsigned long long>();
+        cudaStream_t s = stream;
+        CU(cudaMemsetAsync(out, 0, 2 * sizeof(unsigned long long), s));
+        const long long n = (long long)NC * nvec;
+        const dim3 grid((unsigned)((n + kBlock - 1) / kBlock), 3);
+        if (is3d)
+            k_sym_check<27, true><<<grid, kBlock, 0, s>>>(g, L, act.as<int32_t>(), Auu, Auv, Avu, Avv, out);
+        else
+            k_sym_check<9, false><<<grid, kBlock, 0, s>>>(g, L, act.as<int32_t>(), Auu, Auv, Avu, Avv, out);
+        CU(cudaGetLastError());
+        unsigned long long h[2];
+        CU(cudaMemcpyAsync(h, out, sizeof(h), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        double md;
+        std::memcpy(&md, &h[0], sizeof(md));
+        if (maxdiff) *maxdiff = md;
+        if (nwarn) *nwarn = (long long)h[1];
+        return CISMGPU_OK;
+    }
+
+    // The symmetry check on the resident canonical planes.
+    int check_symmetry(double *maxdiff, long long *nwarn) {
+        SymIdx L{};
+        for (int c = 0; c < 27; ++c) L.map[c] = c + 1;
+        L.n = nvec;
+        L.NQ = g.NQ;
+        L.nz = g.nz;
+        L.raw3 = 0;
+        const size_t bs = (size_t)NC * nvec;
+        double *A0 = A.as<double>();
+        TRY(sym_check(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, maxdiff, nwarn));
+        if (is3d) mixed.stale = true;  // the FP32 copies follow the averaged matrix
+        return CISMGPU_OK;
+    }
+
     // compute_residual_velocity on the device (:10188-10446) between the planes of id_new
     // (uvel, vvel) and id_old (usav, vsav).  Leaves the stream synchronized.
     int residual_velocity(int whichresid, int id_new, int id_old, double *resid_velo) {
@@ -1153,6 +1195,45 @@ static int oneshot_resid_vec(bool is3d, int nx, int ny, int nz, const cismgpu_pa
     return CISMGPU_OK;
 }
 
+// check_symmetry_assembled_matrix_{3d,2d} on the caller's blocks: copied to the device in the
+// caller's own layout, checked there and, in 3D, copied back with the averages written in.
+static int oneshot_symmetry(bool is3d, int nx, int ny, int nz, const cismgpu_par_t *par, const int32_t *indx,
+                            const int32_t *act, double *const blocks[4], double *maxdiff, long long *nwarn) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_error.clear();
+    if (!par || !indx || !act || !blocks[0] || !blocks[1] || !blocks[2] || !blocks[3] || !maxdiff || !nwarn)
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    TRY(validate_geom(nx, ny, is3d ? nz : 1, par));
+    TRY(validate_indx(indx, is3d ? 27 : 9));
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
+    TRY(sv.set_geom(make_geom(nx, ny, is3d ? nz : 1, par), is3d));
+    const Geom &g = sv.g;
+    cudaStream_t s = sv.stream;
+    CU(sv.act.ensure((size_t)g.NQ * sizeof(int32_t)));
+    CU(cudaMemcpyAsync(sv.act.p, act, (size_t)g.NQ * sizeof(int32_t), cudaMemcpyHostToDevice, s));
+    const size_t bs = (size_t)sv.NC * sv.nvec;
+    CU(sv.A.ensure(4 * bs * sizeof(double)));
+    sv.mixed.stale = true;  // the matrix buffer holds the caller's layout until the next upload
+    double *A0 = sv.A.as<double>();
+    for (int b = 0; b < 4; ++b)
+        CU(cudaMemcpyAsync(A0 + b * bs, blocks[b], bs * sizeof(double), cudaMemcpyHostToDevice, s));
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = c < sv.NC ? indx[c] : 1;
+    L.n = sv.nvec;
+    L.NQ = g.NQ;
+    L.nz = g.nz;
+    L.raw3 = is3d ? 1 : 0;
+    TRY(sv.sym_check(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, maxdiff, nwarn));
+    if (is3d) {
+        for (int b = 0; b < 4; ++b)
+            CU(cudaMemcpyAsync(blocks[b], A0 + b * bs, bs * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+    }
+    return CISMGPU_OK;
+}
+
 static int oneshot_resid_velo(bool is3d, int whichresid, int nx, int ny, int nz, const cismgpu_par_t *par,
                               const double *uvel, const double *vvel, const double *usav, const double *vsav,
                               double *resid_velo) {
@@ -1451,6 +1532,24 @@ int cismgpu_compute_residual_velocity_2d(int whichresid, int nx, int ny, const c
     return oneshot_resid_velo(false, whichresid, nx, ny, 1, par, uvel, vvel, usav, vsav, resid_velo);
 }
 
+int cismgpu_check_symmetry_assembled_matrix_3d(int nx, int ny, int nz, const cismgpu_par_t *par,
+                                               const int32_t *indxA_3d, const int32_t *active_vertex, double *Auu,
+                                               double *Auv, double *Avu, double *Avv, double *maxdiff,
+                                               long long *nwarn) {
+    double *const blocks[4] = {Auu, Auv, Avu, Avv};
+    return oneshot_symmetry(true, nx, ny, nz, par, indxA_3d, active_vertex, blocks, maxdiff, nwarn);
+}
+
+int cismgpu_check_symmetry_assembled_matrix_2d(int nx, int ny, const cismgpu_par_t *par, const int32_t *indxA_2d,
+                                               const int32_t *active_vertex, const double *Auu, const double *Auv,
+                                               const double *Avu, const double *Avv, double *maxdiff,
+                                               long long *nwarn) {
+    // the 2D check writes nothing: the blocks stay const through the shared path
+    double *const blocks[4] = {const_cast<double *>(Auu), const_cast<double *>(Auv), const_cast<double *>(Avu),
+                               const_cast<double *>(Avv)};
+    return oneshot_symmetry(false, nx, ny, 1, par, indxA_2d, active_vertex, blocks, maxdiff, nwarn);
+}
+
 int cismgpu_solver_create(cismgpu_solver_t **out, int dims, int nx, int ny, int nz, const cismgpu_par_t *par,
                           const int32_t *indxA, const int32_t *active_vertex, const double *Auu, const double *Auv,
                           const double *Avu, const double *Avv, const double *bu, const double *bv,
@@ -1650,6 +1749,14 @@ int cismgpu_solver_residual_vector(cismgpu_solver_t *h, double *resid_u, double 
     *L2_norm = l2;
     if (L2_norm_relative) *L2_norm_relative = (l2b > 0.0) ? l2 / l2b : 0.0;
     return CISMGPU_OK;
+}
+
+int cismgpu_solver_check_symmetry(cismgpu_solver_t *h, double *maxdiff, long long *nwarn) {
+    g_last_error.clear();
+    if (!h) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
+    return h->sv.check_symmetry(maxdiff, nwarn);
 }
 
 int cismgpu_solver_save(cismgpu_solver_t *h) {

@@ -497,6 +497,109 @@ __global__ void __launch_bounds__(kBlock) k_resid_velo(Geom g, int kmax, int mea
 }
 
 // ---------------------------------------------------------------------------
+// check_symmetry_assembled_matrix_{3d,2d} (glissade_velo_higher.F90:10854-11117 and
+// :10648-10850) pair by pair
+// ---------------------------------------------------------------------------
+// The reference visits every owned active row R and compares each coefficient of offset d
+// with its transpose partner at row R+d, offset -d: Auu with Auu, Auv with Avu (Auu's
+// diagonal in the tolerance), then Avv with Avv, Avu with Auv (Avv's diagonal).  A visit
+// whose values differ raises maxdiff to |val2 - val1| and, when that is below
+// eps11 * |diag of the visited row|, the 3D check averages the pair in place; otherwise it
+// warns.  Every coefficient has exactly one partner, so the in-place loop is a function of
+// each pair alone: a pair is seen from R (if R is owned and active) and from R+d (likewise),
+// it is averaged when either visit's test passes on the original values, the earlier visit
+// warns when its test fails, and the later one when its own fails and the earlier one did not
+// average.  "Earlier" is the reference's loop order: rows j, i, k, then the Auu/Auv loop
+// before the Avv/Avu loop.  One thread owns each pair (the Auv member of an Auv-Avu pair; of
+// an Auu or Avv pair the member with the smaller offset index c < 26 - c), reads both values
+// and writes both, and only the owners write; the diagonals that the tolerance reads are
+// their own partners and are never written, so no thread reads what another writes.
+constexpr double kEps11 = 1.0e-11;  // eps11, libglimmer/glimmer_paramets.F90:77
+
+// Element offsets of coefficient c (canonical offset index (iA+1) + 3(jA+1) + 9(kA+1)) at
+// level k of column q: the canonical planes (map = identity) or the caller's Fortran blocks,
+// (27, nz, NX, NY) in 3D (raw3) or (NX, NY, 9) in 2D, through the caller's indxA map.
+struct SymIdx {
+    int32_t map[27];
+    long long n;  // nz * NQ
+    long long NQ;
+    int nz;
+    int raw3;
+    __device__ __forceinline__ long long at(int c, int k, long long q) const {
+        const long long m = map[c] - 1;
+        return raw3 ? m + 27LL * (k + (long long)nz * q) : m * n + (long long)k * NQ + q;
+    }
+};
+
+// blockIdx.y: 0 Auu-Auu pairs, 1 Auv-Avu pairs, 2 Avv-Avv pairs; x: coefficient c, level k,
+// column q of the pair's first member.  out[0]: maxdiff as the bits of a non-negative double
+// (a NaN difference never wins: "abs(val2 - val1) > maxdiff" is false for it), out[1]: warnings.
+template <int NC, bool FIX>
+__global__ void __launch_bounds__(kBlock) k_sym_check(Geom g, SymIdx L, const int32_t *__restrict__ act,
+                                                      double *Auu, double *Auv, double *Avu, double *Avv,
+                                                      unsigned long long *out) {
+    const long long n = (long long)g.nz * g.NQ;
+    const long long t = (long long)blockIdx.x * kBlock + threadIdx.x;
+    const int kind = blockIdx.y;
+    unsigned long long dbits = 0ull, nw = 0ull;
+    if (t < NC * n) {
+        const int c = (int)(t / n);
+        const long long r = t - (long long)c * n;
+        const int k = (int)(r / g.NQ);
+        const long long q = r - (long long)k * g.NQ;
+        int i, j;
+        col_of(g, q, i, j);
+        const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
+        const int cc = NC - 1 - c, cd = NC / 2;
+        const int kp = k + kA, ip = i + iA, jp = j + jA;
+        // a partner outside the arrays (owned rows at the array edge) is not compared
+        const bool inside = kp >= 0 && kp < g.nz && ip >= 0 && ip < g.NX && jp >= 0 && jp < g.NY;
+        if (inside && (kind == 1 || c <= cc)) {
+            const long long qp = (long long)jp * g.NX + ip;
+            const bool self = kind != 1 && c == cc;  // a diagonal is its own partner
+            const bool visA = owned(g, i, j) && act[q] != 0;
+            const bool visB = !self && owned(g, ip, jp) && act[qp] != 0;
+            double *X = kind == 0 ? Auu : (kind == 1 ? Auv : Avv);
+            double *Y = kind == 0 ? Auu : (kind == 1 ? Avu : Avv);
+            const long long ea = L.at(c, k, q), eb = L.at(cc, kp, qp);
+            const double x = (visA || visB) ? X[ea] : 0.0, y = (visA || visB) ? Y[eb] : 0.0;
+            if (y != x) {  // val2 /= val1, true for a NaN
+                const double d = fabs(__dsub_rn(y, x));
+                if (d > 0.0) dbits = (unsigned long long)__double_as_longlong(d);
+                // visit A from R: Auu's diagonal for the Auu and Auv checks, Avv's for Avv;
+                // visit B from R+d: Auu's for Auu, Avv's for the Avv and Avu checks
+                const double *DA = kind == 2 ? Avv : Auu, *DB = kind == 0 ? Auu : Avv;
+                const bool passA = visA && d < __dmul_rn(kEps11, fabs(DA[L.at(cd, k, q)]));
+                const bool passB = visB && d < __dmul_rn(kEps11, fabs(DB[L.at(cd, kp, qp)]));
+                if (FIX) {
+                    const long long rowA = k + (long long)g.nz * q, rowB = kp + (long long)g.nz * qp;
+                    const bool aFirst = rowA <= rowB;  // equal rows: the Auv check (A) precedes Avu's (B)
+                    const bool v1 = aFirst ? visA : visB, p1 = aFirst ? passA : passB;
+                    const bool v2 = aFirst ? visB : visA, p2 = aFirst ? passB : passA;
+                    nw = (unsigned long long)(v1 && !p1) + (unsigned long long)(v2 && !p2 && !p1);
+                    if (passA || passB) {
+                        const double avg = __dmul_rn(0.5, __dadd_rn(x, y));
+                        X[ea] = avg;
+                        Y[eb] = avg;
+                    }
+                } else {
+                    nw = (unsigned long long)(visA && !passA) + (unsigned long long)(visB && !passB);
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+        dbits = max(dbits, __shfl_down_sync(0xffffffffu, dbits, off));
+        nw += __shfl_down_sync(0xffffffffu, nw, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (dbits) atomicMax(&out[0], dbits);
+        if (nw) atomicAdd(&out[1], nw);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // tridiagonal line preconditioners (precond 3 local, 4 global) on one task
 // ---------------------------------------------------------------------------
 // On one task the global form's solution is its particular solution (tasks_rc = 1,

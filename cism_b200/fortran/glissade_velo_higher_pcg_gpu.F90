@@ -13,6 +13,8 @@
 !   takes these with "use glissade_velo_higher_pcg_gpu, only: gpu_x => x"):
 !     compute_residual_vector_2d   (:9502-9689)    compute_residual_vector_3d   (:9693-9894)
 !     compute_residual_velocity_2d (:10188-10310)  compute_residual_velocity_3d (:10314-10446)
+!     check_symmetry_assembled_matrix_2d (:10648-10850)
+!     check_symmetry_assembled_matrix_3d (:10854-11117)
 !   A nonzero library status is reported the way the reference reports a failed
 !   solve: write_log(message, GM_FATAL).
 !
@@ -40,6 +42,7 @@
               pcg_solver_chrongear_2d, pcg_solver_chrongear_3d, &
               compute_residual_vector_2d, compute_residual_vector_3d, &
               compute_residual_velocity_2d, compute_residual_velocity_3d, &
+              check_symmetry_assembled_matrix_2d, check_symmetry_assembled_matrix_3d, &
               cismgpu_use_mixed_precision
 
     type, bind(C) :: cismgpu_par_t
@@ -162,6 +165,28 @@
          real(c_double), intent(in) :: uvel(*), vvel(*), usav(*), vsav(*)
          real(c_double), intent(out) :: resid_velo
        end function c_resid_velocity_2d
+
+       integer(c_int) function c_check_symmetry_3d(nx, ny, nz, par, indxA_3d, active_vertex, Auu, Auv, Avu, &
+            Avv, maxdiff, nwarn) bind(C, name="cismgpu_check_symmetry_assembled_matrix_3d")
+         import :: c_int, c_double, c_int32_t, c_long_long, cismgpu_par_t
+         integer(c_int), value :: nx, ny, nz
+         type(cismgpu_par_t), intent(in) :: par
+         integer(c_int32_t), intent(in) :: indxA_3d(*), active_vertex(*)
+         real(c_double), intent(inout) :: Auu(*), Auv(*), Avu(*), Avv(*)
+         real(c_double), intent(out) :: maxdiff
+         integer(c_long_long), intent(out) :: nwarn
+       end function c_check_symmetry_3d
+
+       integer(c_int) function c_check_symmetry_2d(nx, ny, par, indxA_2d, active_vertex, Auu, Auv, Avu, Avv, &
+            maxdiff, nwarn) bind(C, name="cismgpu_check_symmetry_assembled_matrix_2d")
+         import :: c_int, c_double, c_int32_t, c_long_long, cismgpu_par_t
+         integer(c_int), value :: nx, ny
+         type(cismgpu_par_t), intent(in) :: par
+         integer(c_int32_t), intent(in) :: indxA_2d(*), active_vertex(*)
+         real(c_double), intent(in) :: Auu(*), Auv(*), Avu(*), Avv(*)
+         real(c_double), intent(out) :: maxdiff
+         integer(c_long_long), intent(out) :: nwarn
+       end function c_check_symmetry_2d
     end interface
 
   contains
@@ -386,5 +411,50 @@
       call check(c_resid_velocity_2d(whichresid, size(uvel,1) + 1, size(uvel,2) + 1, to_c(parallel), &
                                      uvel, vvel, usav, vsav, resid_velo))
     end subroutine compute_residual_velocity_2d
+
+    !-----------------------------------------------------------------------
+    ! The nearly symmetric pairs (|difference| < eps11 * |diagonal|) are averaged in place, as
+    ! in the reference; the reference's per-entry warnings become one log line with their count
+    ! and the largest asymmetry.
+    subroutine check_symmetry_assembled_matrix_3d(nx, ny, nz, parallel, active_vertex, Auu, Auv, Avu, Avv)
+      integer, intent(in) :: nx, ny, nz
+      type(parallel_type), intent(in) :: parallel
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      real(dp), dimension(27,nz,nx-1,ny-1), intent(inout) :: Auu, Auv, Avu, Avv
+      integer(c_int32_t) :: act(nx-1,ny-1), indx3(27)
+      real(c_double) :: maxdiff
+      integer(c_long_long) :: nwarn
+      character(len=160) :: text
+      integer :: m
+      act = merge(1, 0, active_vertex)
+      indx3 = [(m, m = 1, 27)]
+      call check(c_check_symmetry_3d(nx, ny, nz, to_c(parallel), indx3, act, Auu, Auv, Avu, Avv, maxdiff, nwarn))
+      if (nwarn > 0) then
+         write(text, '(a,i0,a,es12.5)') 'Assembled matrix is not symmetric: ', nwarn, &
+              ' warnings, max asymmetry =', maxdiff
+         call write_log(trim(text), GM_WARNING)
+      endif
+    end subroutine check_symmetry_assembled_matrix_3d
+
+    !-----------------------------------------------------------------------
+    subroutine check_symmetry_assembled_matrix_2d(nx, ny, parallel, active_vertex, Auu, Auv, Avu, Avv)
+      integer, intent(in) :: nx, ny
+      type(parallel_type), intent(in) :: parallel
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      real(dp), dimension(nx-1,ny-1,9), intent(inout) :: Auu, Auv, Avu, Avv
+      integer(c_int32_t) :: act(nx-1,ny-1), indx2(9)
+      real(c_double) :: maxdiff
+      integer(c_long_long) :: nwarn
+      character(len=160) :: text
+      integer :: m
+      act = merge(1, 0, active_vertex)
+      indx2 = [(m, m = 1, 9)]
+      call check(c_check_symmetry_2d(nx, ny, to_c(parallel), indx2, act, Auu, Auv, Avu, Avv, maxdiff, nwarn))
+      if (nwarn > 0) then
+         write(text, '(a,i0,a,es12.5)') 'Assembled matrix is not symmetric: ', nwarn, &
+              ' warnings, max asymmetry =', maxdiff
+         call write_log(trim(text), GM_WARNING)
+      endif
+    end subroutine check_symmetry_assembled_matrix_2d
 
   end module glissade_velo_higher_pcg_gpu

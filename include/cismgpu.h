@@ -221,6 +221,27 @@ int cismgpu_compute_residual_velocity_2d(int whichresid, int nx, int ny, const c
                                          const double *uvel, const double *vvel, const double *usav,
                                          const double *vsav, double *resid_velo);
 
+/* Replace check_symmetry_assembled_matrix_3d (glissade_velo_higher.F90:10854-11117) and
+ * check_symmetry_assembled_matrix_2d (:10648-10850), which glissade_velo_higher_solve calls on
+ * the assembled blocks before the solve (:2923-2931, :2704-2711).  Every owned active row
+ * compares each coefficient with its transpose partner (Auu with Auu^T, Auv with Avu^T, Avv
+ * with Avv^T, Avu with Auv^T).  Where the two differ by less than eps11 = 1e-11
+ * (glimmer_paramets.F90:77) times |diagonal| of the visited row's block, the 3D check replaces
+ * both by their average, in place in the caller's arrays; larger differences are reported.
+ * The 2D check reports only (its averaging is commented out in the reference) and leaves the
+ * blocks unchanged.  maxdiff: the largest |difference| met (the reference's maxdiff);
+ * nwarn: the number of asymmetry warnings the reference writes to its log.  indxA_3d /
+ * indxA_2d: the reference's module index maps.  A partner outside the arrays (an owned row on
+ * the array edge, where the reference would read outside its arrays) is not compared. */
+int cismgpu_check_symmetry_assembled_matrix_3d(int nx, int ny, int nz, const cismgpu_par_t *par,
+                                               const int32_t *indxA_3d, const int32_t *active_vertex, double *Auu,
+                                               double *Auv, double *Avu, double *Avv, double *maxdiff,
+                                               long long *nwarn);
+int cismgpu_check_symmetry_assembled_matrix_2d(int nx, int ny, const cismgpu_par_t *par, const int32_t *indxA_2d,
+                                               const int32_t *active_vertex, const double *Auu, const double *Auv,
+                                               const double *Avu, const double *Avv, double *maxdiff,
+                                               long long *nwarn);
+
 /* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps
@@ -350,6 +371,11 @@ int cismgpu_solver_residual_velocity(cismgpu_solver_t *s, int whichresid, double
  * accepting and restoring stays with the caller.  Restore without a save: CISMGPU_EINVAL. */
 int cismgpu_solver_save(cismgpu_solver_t *s);
 int cismgpu_solver_restore(cismgpu_solver_t *s);
+
+/* check_symmetry_assembled_matrix_{3d,2d} (see above) on the handle's resident blocks: in 3D
+ * the averages are written into the device copy that the next solve uses (the caller's host
+ * arrays are not touched); in 2D nothing changes.  maxdiff and nwarn may be NULL. */
+int cismgpu_solver_check_symmetry(cismgpu_solver_t *s, double *maxdiff, long long *nwarn);
 
 /* Per-kernel CUDA-event timing of the structured matvec launches (off by default).
  * read: total device milliseconds, launch count, and algorithmic bytes per launch
