@@ -178,12 +178,13 @@ def first_picard_efvs(flwa: float) -> float:
 
 
 def assemble_bp_3d(thck, usrf, dx, dy, nz, flwa=1.0e-16, beta=None, bc="periodic", name="",
-                   chunk=40000) -> Problem:
+                   chunk=40000, stiffness_only=False) -> Problem:
     """Blatter-Pattyn 3D system for the first Picard iteration.
 
     thck, usrf: cell fields (ny, nx) including the 2-cell halo.
     beta: vertex field (ny-1, nx-1) in Pa yr/m for 'beta local' sliding, or None for a
           no-slip bed (Dirichlet u = v = 0 at k = nz, which_ho_babc = 4).
+    stiffness_only: return the assembled stiffness blocks before any basal condition.
     """
     ny, nx = thck.shape
     NX, NY = nx - 1, ny - 1
@@ -251,7 +252,9 @@ def assemble_bp_3d(thck, usrf, dx, dy, nz, flwa=1.0e-16, beta=None, bc="periodic
     bv = np.where(av[:, :, None], -RHOI * GRAV * dx * dy * dzk / VOL0 * dsdy[:, :, None], 0.0)
 
     m0 = 13
-    if beta is not None:
+    if stiffness_only:
+        pass
+    elif beta is not None:
         lsrf = usrf - thck
         staglsrf = stagger(lsrf, np.ones_like(thck, dtype=bool))
         gx, gy = np.gradient(staglsrf, dy, dx)

@@ -65,6 +65,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_compute_residual_velocity.restype = dbl
         L.oracle_exact_sum.argtypes = [d, ctypes.c_long]
         L.oracle_reprosum.argtypes = [d, ctypes.c_long]
+        L.oracle_assemble_stiffness_3d.argtypes = [i, i, i, i, d, d, d, d, d, d, d, d, d, i, i, dbl, dbl, dbl,
+                                                   d, d, d, d, d]
         L.oracle_check_symmetry.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, P(dbl), P(ctypes.c_long)]
         L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
@@ -200,6 +202,23 @@ def check_symmetry(prob, Auu=None, Auv=None, Avu=None, Avv=None):
                                 _p(indx3() if is3d else indx2()), _p(prob.active_vertex), *[_p(b) for b in blocks],
                                 ctypes.byref(md), ctypes.byref(nw))
     return (*blocks, md.value, nw.value)
+
+
+def assemble_stiffness_3d(nx, ny, nz, sigma, active_cell, xVertex, yVertex, uvel, vvel, stagusrf, stagthck,
+                          flwafact, whichapprox=2, whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8,
+                          n_glen=3.0, nhalo=2):
+    """assemble_stiffness_matrix_3d (glissade_velo_higher.F90:5382-5643) on numpy arrays in
+    the caller's layout as C-order arrays with reversed dimensions: active_cell (ny, nx),
+    vertex fields (ny-1, nx-1), uvel/vvel (ny-1, nx-1, nz), flwafact (ny, nx, nz-1).
+    Returns (status, efvs (ny, nx, nz-1), Auu, Auv, Avu, Avv (ny-1, nx-1, nz, 27))."""
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    efvs = np.zeros((ny, nx, nz - 1))
+    A = [np.zeros((ny - 1, nx - 1, nz, 27)) for _ in range(4)]
+    ins = [f64(sigma), np.ascontiguousarray(active_cell, dtype=np.int32), f64(xVertex), f64(yVertex), f64(uvel),
+           f64(vvel), f64(stagusrf), f64(stagthck), f64(flwafact)]
+    st = lib().oracle_assemble_stiffness_3d(nx, ny, nz, nhalo, *[_p(a) for a in ins], whichapprox, whichefvs,
+                                            efvs_constant, effstrain_min, n_glen, _p(efvs), *[_p(a) for a in A])
+    return (st, efvs, *A)
 
 
 def reprosum(a) -> float:

@@ -1,0 +1,261 @@
+// CPU restatement of the Blatter-Pattyn stiffness assembly -- TEST INFRASTRUCTURE ONLY.
+//
+// assemble_stiffness_matrix_3d (libglissade/glissade_velo_higher.F90:5382-5643) with the
+// routines it calls, loop for loop and in the reference's operation order:
+//   reference element, quadrature points and weights      glissade_velo_higher.F90:314-392
+//   node shift tables ishift/jshift/kshift                  :455-478
+//   get_basis_function_derivatives_3d                       :6508-6732
+//   compute_effective_viscosity                             :7285-7470
+//   compute_element_matrix                                  :8001-8123
+//   element_to_global_matrix_3d                             :8200-8268
+// check_symmetry_element_matrix (:10583-10644) only stops the run on an asymmetric element
+// matrix; the element matrices here are symmetric by construction (each product is formed
+// with the same operands in the same order on both sides of the diagonal, the factors 2 and 4
+// scale exactly), so nothing is restated for it.  Fortran's x**2 is x*x; x**y with a real y is
+// the C library's pow, as gfortran calls it.  Compiled -ffp-contract=off (no FMA).
+//
+// Arrays in the caller's Fortran layout (column-major, 1-based in the comments):
+//   active_cell(nx,ny), xVertex/yVertex/stagusrf/stagthck(nx-1,ny-1), uvel/vvel(nz,nx-1,ny-1),
+//   flwafact/efvs(nz-1,nx,ny), A**(27,nz,nx-1,ny-1).
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <initializer_list>
+
+namespace {
+
+constexpr int kApproxSIA = 0, kApproxSSA = 1;          // glide_types.F90:335-336 (else BP)
+constexpr int kEfvsConstant = 0, kEfvsFlowfact = 1;    // glide_types.F90:240-242 (2: nonlinear)
+constexpr double kVol0 = 1.0e9;                        // glissade_velo_higher.F90:1254
+constexpr double kScyr = 31536000.0;                   // glimmer_physcon.F90:90
+constexpr double kLenScale = 200.0e3;                  // glimmer_paramets.F90:97
+constexpr double kVeloScale = 500.0 / kScyr;           // glimmer_paramets.F90:98
+
+// ishift(7,n), jshift(7,n), kshift(7,n): node n of the element relative to node 7, whose
+// (k,i,j) are the element's; ishift(nr,nc) = ishift(7,nc) - ishift(7,nr) and likewise.
+constexpr int kIsh7[8] = {-1, 0, 0, -1, -1, 0, 0, -1};
+constexpr int kJsh7[8] = {-1, -1, 0, 0, -1, -1, 0, 0};
+constexpr int kKsh7[8] = {1, 1, 1, 1, 0, 0, 0, 0};
+
+struct RefElement {
+    double wqp[8];
+    double dxr[8][8], dyr[8][8], dzr[8][8];  // [p][n]
+    RefElement() {
+        const double r = 1.0 / std::sqrt(3.0);
+        const double xq[8] = {-r, r, r, -r, -r, r, r, -r};
+        const double yq[8] = {-r, -r, r, r, -r, -r, r, r};
+        const double zq[8] = {-r, -r, -r, -r, r, r, r, r};
+        for (int p = 0; p < 8; ++p) {
+            const double x = xq[p], y = yq[p], z = zq[p];
+            wqp[p] = 1.0;
+            dxr[p][0] = -(1.0 - y) * (1.0 - z) / 8.0;
+            dxr[p][1] = (1.0 - y) * (1.0 - z) / 8.0;
+            dxr[p][2] = (1.0 + y) * (1.0 - z) / 8.0;
+            dxr[p][3] = -(1.0 + y) * (1.0 - z) / 8.0;
+            dxr[p][4] = -(1.0 - y) * (1.0 + z) / 8.0;
+            dxr[p][5] = (1.0 - y) * (1.0 + z) / 8.0;
+            dxr[p][6] = (1.0 + y) * (1.0 + z) / 8.0;
+            dxr[p][7] = -(1.0 + y) * (1.0 + z) / 8.0;
+            dyr[p][0] = -(1.0 - x) * (1.0 - z) / 8.0;
+            dyr[p][1] = -(1.0 + x) * (1.0 - z) / 8.0;
+            dyr[p][2] = (1.0 + x) * (1.0 - z) / 8.0;
+            dyr[p][3] = (1.0 - x) * (1.0 - z) / 8.0;
+            dyr[p][4] = -(1.0 - x) * (1.0 + z) / 8.0;
+            dyr[p][5] = -(1.0 + x) * (1.0 + z) / 8.0;
+            dyr[p][6] = (1.0 + x) * (1.0 + z) / 8.0;
+            dyr[p][7] = (1.0 - x) * (1.0 + z) / 8.0;
+            dzr[p][0] = -(1.0 - x) * (1.0 - y) / 8.0;
+            dzr[p][1] = -(1.0 + x) * (1.0 - y) / 8.0;
+            dzr[p][2] = -(1.0 + x) * (1.0 + y) / 8.0;
+            dzr[p][3] = -(1.0 - x) * (1.0 + y) / 8.0;
+            dzr[p][4] = (1.0 - x) * (1.0 - y) / 8.0;
+            dzr[p][5] = (1.0 + x) * (1.0 - y) / 8.0;
+            dzr[p][6] = (1.0 + x) * (1.0 + y) / 8.0;
+            dzr[p][7] = (1.0 - x) * (1.0 + y) / 8.0;
+        }
+    }
+};
+
+const RefElement &ref() {
+    static const RefElement r;
+    return r;
+}
+
+// get_basis_function_derivatives_3d (:6508-6732): Jacobian sums in node order, cofactors,
+// detJ by the first row, Jinv = transpose(cofactor) / detJ, then dphi = Jinv * dphi_r.
+// Returns false for a singular Jacobian (the reference stops with GM_FATAL).
+bool basis_derivs_3d(const double *x, const double *y, const double *z, const double *dxr, const double *dyr,
+                     const double *dzr, double *dx, double *dy, double *dz, double *detJ) {
+    double J[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int n = 0; n < 8; ++n) {
+        J[0][0] = J[0][0] + dxr[n] * x[n];
+        J[0][1] = J[0][1] + dxr[n] * y[n];
+        J[0][2] = J[0][2] + dxr[n] * z[n];
+        J[1][0] = J[1][0] + dyr[n] * x[n];
+        J[1][1] = J[1][1] + dyr[n] * y[n];
+        J[1][2] = J[1][2] + dyr[n] * z[n];
+        J[2][0] = J[2][0] + dzr[n] * x[n];
+        J[2][1] = J[2][1] + dzr[n] * y[n];
+        J[2][2] = J[2][2] + dzr[n] * z[n];
+    }
+    double c[3][3];
+    c[0][0] = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+    c[0][1] = -(J[1][0] * J[2][2] - J[1][2] * J[2][0]);
+    c[0][2] = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+    c[1][0] = -(J[0][1] * J[2][2] - J[0][2] * J[2][1]);
+    c[1][1] = J[0][0] * J[2][2] - J[0][2] * J[2][0];
+    c[1][2] = -(J[0][0] * J[2][1] - J[0][1] * J[2][0]);
+    c[2][0] = J[0][1] * J[1][2] - J[0][2] * J[1][1];
+    c[2][1] = -(J[0][0] * J[1][2] - J[0][2] * J[1][0]);
+    c[2][2] = J[0][0] * J[1][1] - J[0][1] * J[1][0];
+    const double det = J[0][0] * c[0][0] + J[0][1] * c[0][1] + J[0][2] * c[0][2];
+    *detJ = det;
+    if (!(std::fabs(det) > 0.0)) return false;
+    double Ji[3][3];
+    for (int col = 0; col < 3; ++col)
+        for (int row = 0; row < 3; ++row) Ji[row][col] = c[col][row] / det;
+    for (int n = 0; n < 8; ++n) {
+        dx[n] = Ji[0][0] * dxr[n] + Ji[0][1] * dyr[n] + Ji[0][2] * dzr[n];
+        dy[n] = Ji[1][0] * dxr[n] + Ji[1][1] * dyr[n] + Ji[1][2] * dzr[n];
+        dz[n] = Ji[2][0] * dxr[n] + Ji[2][1] * dyr[n] + Ji[2][2] * dzr[n];
+    }
+    return true;
+}
+
+// compute_effective_viscosity (:7285-7470) at one quadrature point of an 8-node element.
+double efvs_qp(int whichefvs, int whichapprox, double efvs_constant, double effstrain_min, double n_glen,
+               const double *dx, const double *dy, const double *dz, const double *u, const double *v,
+               double flwafact) {
+    const double p_effstr = (1.0 - n_glen) / n_glen;
+    if (whichefvs == kEfvsConstant) return efvs_constant;
+    if (whichefvs == kEfvsFlowfact) {
+        const double effstrain = kVeloScale / kLenScale * kScyr;
+        return flwafact * std::pow(effstrain, p_effstr);
+    }
+    double du_dx = 0.0, du_dy = 0.0, du_dz = 0.0, dv_dx = 0.0, dv_dy = 0.0, dv_dz = 0.0, sq;
+    if (whichapprox == kApproxSIA) {
+        for (int n = 0; n < 8; ++n) {
+            du_dz = du_dz + dz[n] * u[n];
+            dv_dz = dv_dz + dz[n] * v[n];
+        }
+        sq = effstrain_min * effstrain_min + 0.25 * (du_dz * du_dz + dv_dz * dv_dz);
+    } else if (whichapprox == kApproxSSA) {
+        for (int n = 0; n < 8; ++n) {
+            du_dx = du_dx + dx[n] * u[n];
+            du_dy = du_dy + dy[n] * u[n];
+            dv_dx = dv_dx + dx[n] * v[n];
+            dv_dy = dv_dy + dy[n] * v[n];
+        }
+        sq = effstrain_min * effstrain_min +
+             (du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * ((dv_dx + du_dy) * (dv_dx + du_dy)));
+    } else {
+        for (int n = 0; n < 8; ++n) {
+            du_dx = du_dx + dx[n] * u[n];
+            du_dy = du_dy + dy[n] * u[n];
+            du_dz = du_dz + dz[n] * u[n];
+            dv_dx = dv_dx + dx[n] * v[n];
+            dv_dy = dv_dy + dy[n] * v[n];
+            dv_dz = dv_dz + dz[n] * v[n];
+        }
+        sq = effstrain_min * effstrain_min +
+             (du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * ((dv_dx + du_dy) * (dv_dx + du_dy))) +
+             0.25 * (du_dz * du_dz + dv_dz * dv_dz);
+    }
+    return flwafact * std::pow(sq, p_effstr / 2.0);
+}
+
+// compute_element_matrix (:8001-8123): K += efvs*wqp*detJ/vol0 * (products), columns outer.
+void element_matrix(int whichapprox, double wqp, double detJ, double efvs, const double *dx, const double *dy,
+                    const double *dz, double Kuu[8][8], double Kuv[8][8], double Kvu[8][8], double Kvv[8][8]) {
+    const double f = efvs * wqp * detJ / kVol0;
+    for (int nc = 0; nc < 8; ++nc)
+        for (int nr = 0; nr < 8; ++nr) {
+            if (whichapprox == kApproxSIA) {
+                Kuu[nr][nc] = Kuu[nr][nc] + f * (dz[nr] * dz[nc]);
+                Kvv[nr][nc] = Kvv[nr][nc] + f * (dz[nr] * dz[nc]);
+            } else if (whichapprox == kApproxSSA) {
+                Kuu[nr][nc] = Kuu[nr][nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc]);
+                Kuv[nr][nc] = Kuv[nr][nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
+                Kvu[nr][nc] = Kvu[nr][nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
+                Kvv[nr][nc] = Kvv[nr][nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc]);
+            } else {
+                Kuu[nr][nc] = Kuu[nr][nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc] + dz[nr] * dz[nc]);
+                Kuv[nr][nc] = Kuv[nr][nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
+                Kvu[nr][nc] = Kvu[nr][nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
+                Kvv[nr][nc] = Kvv[nr][nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc] + dz[nr] * dz[nc]);
+            }
+        }
+}
+
+}  // namespace
+
+extern "C" {
+
+// assemble_stiffness_matrix_3d (:5382-5643): efvs and A zeroed, then every active cell
+// j = nhalo+1..ny-nhalo+1, i = nhalo+1..nx-nhalo+1 (j outer), element k = 1..nz-1: node
+// coordinates, velocity, the eight quadrature points (basis derivatives, viscosity, element
+// matrix), the mean viscosity, and the element matrix summed into A with the standard indxA_3d
+// (m = 1 + (iA+1) + 3(jA+1) + 9(kA+1)).  Returns 0, or 1 for a singular Jacobian (A partly
+// assembled, as far as the reference would have got before stopping), 2 for nhalo < 2 (element
+// vertices outside the arrays).
+int oracle_assemble_stiffness_3d(int nx, int ny, int nz, int nhalo, const double *sigma, const int32_t *active_cell,
+                                 const double *xVertex, const double *yVertex, const double *uvel,
+                                 const double *vvel, const double *stagusrf, const double *stagthck,
+                                 const double *flwafact, int whichapprox, int whichefvs, double efvs_constant,
+                                 double effstrain_min, double n_glen, double *efvs, double *Auu, double *Auv,
+                                 double *Avu, double *Avv) {
+    if (nhalo < 2) return 2;
+    const long NX = nx - 1, NY = ny - 1;
+    const RefElement &R = ref();
+    std::memset(efvs, 0, sizeof(double) * (size_t)(nz - 1) * nx * ny);
+    const size_t na = (size_t)27 * nz * NX * NY;
+    for (double *A : {Auu, Auv, Avu, Avv}) std::memset(A, 0, sizeof(double) * na);
+    auto V = [&](int i, int j) { return (long)(i - 1) + NX * (j - 1); };
+    for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+        for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+            if (!active_cell[(i - 1) + (long)nx * (j - 1)]) continue;
+            for (int k = 1; k <= nz - 1; ++k) {
+                double Kuu[8][8] = {}, Kuv[8][8] = {}, Kvu[8][8] = {}, Kvv[8][8] = {};
+                double x[8], y[8], z[8], u[8], v[8];
+                for (int n = 0; n < 8; ++n) {
+                    const int iN = i + kIsh7[n], jN = j + kJsh7[n], kN = k + kKsh7[n];
+                    const long q = V(iN, jN);
+                    x[n] = xVertex[q];
+                    y[n] = yVertex[q];
+                    z[n] = stagusrf[q] - sigma[kN - 1] * stagthck[q];
+                    u[n] = uvel[(kN - 1) + (long)nz * q];
+                    v[n] = vvel[(kN - 1) + (long)nz * q];
+                }
+                const double ff = flwafact[(k - 1) + (long)(nz - 1) * ((i - 1) + (long)nx * (j - 1))];
+                double eq[8];
+                for (int p = 0; p < 8; ++p) {
+                    double dx[8], dy[8], dz[8], detJ;
+                    if (!basis_derivs_3d(x, y, z, R.dxr[p], R.dyr[p], R.dzr[p], dx, dy, dz, &detJ)) return 1;
+                    eq[p] = efvs_qp(whichefvs, whichapprox, efvs_constant, effstrain_min, n_glen, dx, dy, dz, u, v,
+                                    ff);
+                    element_matrix(whichapprox, R.wqp[p], detJ, eq[p], dx, dy, dz, Kuu, Kuv, Kvu, Kvv);
+                }
+                double &e = efvs[(k - 1) + (long)(nz - 1) * ((i - 1) + (long)nx * (j - 1))];
+                e = 0.0;
+                for (int p = 0; p < 8; ++p) e = e + eq[p];
+                e = e / 8;
+                // element_to_global_matrix_3d (:8200-8268)
+                for (int nr = 0; nr < 8; ++nr) {
+                    const int iR = i + kIsh7[nr], jR = j + kJsh7[nr], kR = k + kKsh7[nr];
+                    for (int nc = 0; nc < 8; ++nc) {
+                        const int kA = kKsh7[nc] - kKsh7[nr], iA = kIsh7[nc] - kIsh7[nr], jA = kJsh7[nc] - kJsh7[nr];
+                        const int m = (iA + 1) + 3 * (jA + 1) + 9 * (kA + 1);
+                        const size_t a = (size_t)m + 27 * ((size_t)(kR - 1) + (size_t)nz * (size_t)V(iR, jR));
+                        Auu[a] = Auu[a] + Kuu[nr][nc];
+                        Auv[a] = Auv[a] + Kuv[nr][nc];
+                        Avu[a] = Avu[a] + Kvu[nr][nc];
+                        Avv[a] = Avv[a] + Kvv[nr][nc];
+                    }
+                }
+            }
+        }
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,156 @@
+"""Known-answer tests of the oracle's restatement of assemble_stiffness_matrix_3d
+(libglissade/glissade_velo_higher.F90:5382-5643).
+
+Checks against independent mathematics and against the package's vectorized numpy
+assembly (a different summation order, so agreement is to roundoff):
+  - at u = 0 the blocks equal the numpy first-Picard assembly to 1e-12 of the largest entry;
+  - the element-by-element scatter makes A exactly symmetric (the symmetry check finds 0);
+  - a velocity linear in x, y and z has constant strain rates on trilinear elements, so
+    every element's viscosity equals the flow law evaluated at those rates;
+  - constant viscosity: a uniform velocity is in the null space of each interior row;
+  - efvs constant and flow-factor options.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from cism_b200 import assembly as asm
+
+N_GLEN = 3.0
+
+
+def geometry(ewn=9, nsn=8, nz=5, seed=0, dx=2000.0):
+    """Cell fields of a sloping slab with a notch (as the solver tests use) and the inputs
+    assemble_stiffness_matrix_3d takes."""
+    rng = np.random.default_rng(seed)
+    nx, ny = ewn + 4, nsn + 4
+    H = 800.0 + 400.0 * rng.random((ny, nx))
+    x = (np.arange(nx) + 0.5) * dx
+    usrf = 2000.0 - x[None, :] * 0.01 + 30.0 * rng.random((ny, nx))
+    ice = np.zeros((ny, nx), dtype=bool)
+    ice[3:ny - 3, 3:nx - 3] = True
+    ice[3:5, 3:5] = False
+    thck = np.where(ice, H, 0.0)
+    usrf = np.where(ice, usrf, usrf - H)
+    ac, av = asm.active_masks(thck)
+    g = dict(nx=nx, ny=ny, nz=nz, dx=dx, thck=thck, usrf=usrf, ac=ac, av=av,
+             sigma=asm.glide_sigma(nz),
+             xVertex=np.broadcast_to(np.arange(nx - 1) * dx, (ny - 1, nx - 1)).copy(),
+             yVertex=np.broadcast_to((np.arange(ny - 1) * dx)[:, None], (ny - 1, nx - 1)).copy(),
+             stagusrf=asm.stagger(usrf, thck > 1.0), stagthck=asm.stagger(thck, thck > 1.0))
+    return g
+
+
+def run(g, uvel=None, vvel=None, flwa=1.0e-16, **kw):
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    shape = (ny - 1, nx - 1, nz)
+    u = np.zeros(shape) if uvel is None else uvel
+    v = np.zeros(shape) if vvel is None else vvel
+    flwafact = np.full((ny, nx, nz - 1), 0.5 * flwa ** (-1.0 / N_GLEN))
+    st, efvs, Auu, Auv, Avu, Avv = oracle.assemble_stiffness_3d(
+        nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], u, v, g["stagusrf"], g["stagthck"], flwafact,
+        **kw)
+    assert st == 0
+    return efvs, Auu, Auv, Avu, Avv
+
+
+def test_first_picard_matches_numpy_assembly():
+    g = geometry(seed=1)
+    efvs, *A = run(g)
+    P = asm.assemble_bp_3d(g["thck"], g["usrf"], g["dx"], g["dx"], g["nz"], stiffness_only=True)
+    scale = max(np.abs(P.Auu).max(), np.abs(P.Avv).max())
+    for got, want in zip(A, (P.Auu, P.Auv, P.Avu, P.Avv)):
+        assert np.abs(got - want).max() <= 1e-12 * scale
+    e0 = asm.first_picard_efvs(1.0e-16)
+    act = g["ac"]
+    assert np.all(np.abs(efvs[act] - e0) <= 1e-14 * e0) and np.all(efvs[~act] == 0.0)
+
+
+def test_scatter_is_exactly_symmetric():
+    """Each element matrix is symmetric bit for bit and every entry sums its elements in the
+    same order as its transpose partner: the assembled blocks are exactly symmetric."""
+    g = geometry(seed=2)
+    rng = np.random.default_rng(3)
+    shape = (g["ny"] - 1, g["nx"] - 1, g["nz"])
+    efvs, *A = run(g, 50.0 * rng.standard_normal(shape), 50.0 * rng.standard_normal(shape))
+    P = asm.Problem("3d", g["nx"], g["ny"], g["nz"], *A, np.zeros(shape), np.zeros(shape),
+                    g["av"].astype(np.int32), asm.default_par(g["nx"], g["ny"]))
+    r = oracle.check_symmetry(P)
+    assert r[4] == 0.0 and r[5] == 0
+    assert np.abs(A[0]).max() > 0.0
+
+
+@pytest.mark.parametrize("approx", [2, 1, 0])
+def test_linear_velocity_gives_the_flow_law_viscosity(approx):
+    """u = a.x, v = b.x (x = (x, y, z) of each node): trilinear elements reproduce linear
+    fields, so the strain rates at every quadrature point are (a, b)."""
+    g = geometry(seed=4)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    X = np.broadcast_to(g["xVertex"][..., None], (ny - 1, nx - 1, nz))
+    Y = np.broadcast_to(g["yVertex"][..., None], (ny - 1, nx - 1, nz))
+    Z = g["stagusrf"][..., None] - g["sigma"][None, None, :] * g["stagthck"][..., None]
+    a = (3.0e-3, -1.0e-3, 2.0e-2)
+    b = (1.5e-3, 2.5e-3, -1.0e-2)
+    u = a[0] * X + a[1] * Y + a[2] * Z
+    v = b[0] * X + b[1] * Y + b[2] * Z
+    flwa = 1.0e-16
+    efvs, *A = run(g, u, v, flwa=flwa, whichapprox=approx)
+    emin = 1.0e-8
+    if approx == 0:
+        sq = emin ** 2 + 0.25 * (a[2] ** 2 + b[2] ** 2)
+    else:
+        sq = emin ** 2 + (a[0] ** 2 + b[1] ** 2 + a[0] * b[1] + 0.25 * (b[0] + a[1]) ** 2)
+        if approx == 2:
+            sq += 0.25 * (a[2] ** 2 + b[2] ** 2)
+    want = 0.5 * flwa ** (-1.0 / N_GLEN) * sq ** ((1.0 - N_GLEN) / N_GLEN / 2.0)
+    act = g["ac"]
+    assert np.all(np.abs(efvs[act] - want) <= 1e-12 * want)
+    if approx == 0:  # SIA: only vertical derivatives, no coupling blocks
+        assert np.all(A[1] == 0.0) and np.all(A[2] == 0.0)
+
+
+def test_constant_viscosity_null_space():
+    """With a constant viscosity, a uniform velocity (u = 1, v = 0) gives zero stress: every
+    row whose 8 surrounding elements all exist sums to zero (to roundoff)."""
+    g = geometry(seed=5)
+    efvs, Auu, Auv, Avu, Avv = run(g, whichefvs=0, efvs_constant=1.0e6)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    ac = g["ac"]
+    full = ac[:-1, :-1] & ac[:-1, 1:] & ac[1:, :-1] & ac[1:, 1:]  # vertex with 4 active cells around
+    rows_u = Auu.sum(axis=-1)
+    rows_v = Avu.sum(axis=-1)
+    scale = np.abs(Auu).max()
+    inner = np.zeros((ny - 1, nx - 1, nz), dtype=bool)
+    inner[full, :] = True
+    assert np.abs(rows_u[inner]).max() <= 1e-12 * scale
+    assert np.abs(rows_v[inner]).max() <= 1e-12 * scale
+    assert np.all(efvs[ac] == 1.0e6)
+
+
+def test_flowfact_viscosity():
+    """whichefvs = 1: efvs = flwafact * (velo_scale / len_scale * scyr)^((1-n)/n)."""
+    g = geometry(seed=6)
+    flwa = 2.0e-17
+    efvs, *A = run(g, flwa=flwa, whichefvs=1)
+    scyr = 31536000.0
+    eff = (500.0 / scyr) / 200.0e3 * scyr
+    want = 0.5 * flwa ** (-1.0 / N_GLEN) * math.pow(eff, (1.0 - N_GLEN) / N_GLEN)
+    assert np.all(efvs[g["ac"]] == want)
+
+
+def test_singular_and_halo_errors():
+    g = geometry(seed=7)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    shape = (ny - 1, nx - 1, nz)
+    ff = np.ones((ny, nx, nz - 1))
+    st = oracle.assemble_stiffness_3d(nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], np.zeros(shape),
+                                      np.zeros(shape), g["stagusrf"], g["stagthck"], ff, nhalo=1)[0]
+    assert st == 2
+    flat = np.zeros_like(g["stagthck"])  # zero thickness everywhere: every element is flat
+    st = oracle.assemble_stiffness_3d(nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], np.zeros(shape),
+                                      np.zeros(shape), g["stagusrf"], flat, ff)[0]
+    assert st == 1
