@@ -29,7 +29,7 @@ __all__ = [
     "HO_PRECOND_TRIDIAG_LOCAL", "HO_PRECOND_TRIDIAG_GLOBAL", "DeviceSolver", "solve_batch",
     "ALG_STANDARD", "ALG_CHRONGEAR", "ALG_MIXED_CHRONGEAR", "compute_residual_vector_3d",
     "compute_residual_vector_2d", "compute_residual_velocity_3d", "compute_residual_velocity_2d",
-    "check_symmetry_assembled_matrix_3d", "check_symmetry_assembled_matrix_2d",
+    "check_symmetry_assembled_matrix_3d", "check_symmetry_assembled_matrix_2d", "assemble_stiffness_matrix_3d",
 ]
 
 ALG_STANDARD, ALG_CHRONGEAR, ALG_MIXED_CHRONGEAR = 0, 1, 2
@@ -180,11 +180,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_check_symmetry_assembled_matrix_3d.argtypes = [i32, i32, i32, par, d, d, d, d, d, d, P(dbl), P(i64)]
     lib.cismgpu_check_symmetry_assembled_matrix_2d.argtypes = [i32, i32, par, d, d, d, d, d, d, P(dbl), P(i64)]
     lib.cismgpu_solver_check_symmetry.argtypes = [vp, P(dbl), P(i64)]
+    lib.cismgpu_assemble_stiffness_matrix_3d.argtypes = [i32, i32, i32, i32, d, d, d, d, d, d, d, d, d, i32, i32,
+                                                         dbl, dbl, dbl, d, d, d, d, d, d]
+    lib.cismgpu_solver_assemble_stiffness_3d.argtypes = [vp, i32, d, d, d, d, d, d, d, d, d, i32, i32, dbl, dbl,
+                                                         dbl, d]
     for f in ("cismgpu_compute_residual_vector_3d", "cismgpu_compute_residual_vector_2d",
               "cismgpu_compute_residual_velocity_3d", "cismgpu_compute_residual_velocity_2d",
               "cismgpu_solver_set_system", "cismgpu_solver_residual_vector", "cismgpu_solver_residual_velocity",
               "cismgpu_solver_save", "cismgpu_solver_restore", "cismgpu_check_symmetry_assembled_matrix_3d",
-              "cismgpu_check_symmetry_assembled_matrix_2d", "cismgpu_solver_check_symmetry"):
+              "cismgpu_check_symmetry_assembled_matrix_2d", "cismgpu_solver_check_symmetry",
+              "cismgpu_assemble_stiffness_matrix_3d", "cismgpu_solver_assemble_stiffness_3d"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -428,6 +433,35 @@ def check_symmetry_assembled_matrix_2d(nx, ny, parallel, indxA_2d, active_vertex
     return md.value, nw.value
 
 
+def _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagusrf, stagthck, flwafact):
+    nv = (nx - 1) * (ny - 1)
+    return [_ptr(np.ascontiguousarray(sigma, dtype=np.float64), np.float64, nz),
+            _ptr(np.ascontiguousarray(active_cell, dtype=np.int32), np.int32, nx * ny),
+            _ptr(xVertex, np.float64, nv), _ptr(yVertex, np.float64, nv)], \
+        [_ptr(stagusrf, np.float64, nv), _ptr(stagthck, np.float64, nv),
+         _ptr(flwafact, np.float64, (nz - 1) * nx * ny)]
+
+
+def assemble_stiffness_matrix_3d(nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel, vvel, stagusrf,
+                                 stagthck, flwafact, whichapprox=2, whichefvs=2, efvs_constant=0.0,
+                                 effstrain_min=1.0e-8, n_glen=3.0, indxA_3d=None):
+    """Mirrors assemble_stiffness_matrix_3d (glissade_velo_higher.F90:5382-5643) on the GPU.
+    Arrays in the caller's layout (C-order numpy with reversed dimensions): active_cell
+    (ny, nx), vertex fields (ny-1, nx-1), uvel/vvel (ny-1, nx-1, nz), flwafact (ny, nx, nz-1).
+    Returns (efvs (ny, nx, nz-1), Auu, Auv, Avu, Avv (ny-1, nx-1, nz, 27))."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    indx = np.arange(1, 28, dtype=np.int32) if indxA_3d is None else np.ascontiguousarray(indxA_3d, dtype=np.int32)
+    efvs = np.zeros((ny, nx, nz - 1))
+    A = [np.zeros((ny - 1, nx - 1, nz, 27)) for _ in range(4)]
+    head, tail = _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagusrf, stagthck, flwafact)
+    _check(lib, lib.cismgpu_assemble_stiffness_matrix_3d(
+        nx, ny, nz, int(nhalo), *head, _ptr(uvel, np.float64, nv * nz), _ptr(vvel, np.float64, nv * nz), *tail,
+        int(whichapprox), int(whichefvs), float(efvs_constant), float(effstrain_min), float(n_glen),
+        _ptr(indx, np.int32, 27), _ptr(efvs, np.float64, efvs.size, True), *[_ptr(a, np.float64, a.size, True) for a in A]))
+    return (efvs, *A)
+
+
 class DeviceSolver:
     """A device-resident linear system (cismgpu_solver_create): A, b and x0 live in HBM.
 
@@ -504,6 +538,23 @@ class DeviceSolver:
         md, nw = ctypes.c_double(0.0), ctypes.c_longlong(0)
         _check(self._lib, self._lib.cismgpu_solver_check_symmetry(self.handle, ctypes.byref(md), ctypes.byref(nw)))
         return md.value, nw.value
+
+    def assemble_stiffness(self, nhalo, sigma, active_cell, xVertex, yVertex, stagusrf, stagthck, flwafact,
+                           uvel=None, vvel=None, whichapprox=2, whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8,
+                           n_glen=3.0):
+        """assemble_stiffness_matrix_3d into the resident blocks (3D handles); uvel = vvel =
+        None uses the handle's current velocity.  Returns efvs (ny, nx, nz-1)."""
+        P = self.problem
+        nx, ny, nz = P.nx, P.ny, P.nz
+        nv = (nx - 1) * (ny - 1)
+        efvs = np.zeros((ny, nx, nz - 1))
+        head, tail = _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagusrf, stagthck, flwafact)
+        pu = None if uvel is None else _ptr(uvel, np.float64, nv * nz)
+        pv = None if vvel is None else _ptr(vvel, np.float64, nv * nz)
+        _check(self._lib, self._lib.cismgpu_solver_assemble_stiffness_3d(
+            self.handle, int(nhalo), *head, pu, pv, *tail, int(whichapprox), int(whichefvs), float(efvs_constant),
+            float(effstrain_min), float(n_glen), _ptr(efvs, np.float64, efvs.size, True)))
+        return efvs
 
     def save(self):
         """Accelerated Picard's saved state: the current velocity and A (not b) on the device."""

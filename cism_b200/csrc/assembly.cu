@@ -1,0 +1,211 @@
+// assembly.cu -- the Blatter-Pattyn stiffness matrix assembled on the device:
+// assemble_stiffness_matrix_3d (libglissade/glissade_velo_higher.F90:5382-5643) with
+// get_basis_function_derivatives_3d (:6508-6732), compute_effective_viscosity (:7285-7470),
+// compute_element_matrix (:8001-8123) and element_to_global_matrix_3d (:8200-8268).
+//
+// The reference loops over the elements (active cells j, i, then layers k) and adds each 8x8
+// element matrix into the 27-point rows of its 8 nodes.  Here one thread owns one matrix row
+// (node k, i, j) and gathers instead: it visits the (up to) 8 elements that contain its node in
+// the reference's element order (j, then i, then k), recomputes each element's quadrature (the
+// element's 8 nodes, Jacobian, basis derivatives, viscosity) and adds the element's row for its
+// node, column by column, to its 4 x 27 accumulators.  Every coefficient thus receives the
+// same terms in the same order as in the reference, with no atomics; the cost is each element
+// evaluated once per node (8 times), which is FP64 ALU work on data read once from HBM.
+// The arithmetic is the reference's operation for operation (the library is built without FMA
+// contraction); only pow (the flow law's (effstrain^2)^((1-n)/2n), and the flow-factor option's
+// power, which the host evaluates once) is CUDA's rather than the host C library's.
+
+namespace cismgpu {
+
+constexpr double kAsmVol0 = 1.0e9;   // vol0, glissade_velo_higher.F90:1254
+constexpr int kAsmBlock = 128;
+
+// The reference element (glissade_velo_higher.F90:314-392): weights and the derivatives of the
+// 8 trilinear basis functions at the 8 Gauss points, filled by the host.
+struct AsmRef {
+    double wqp[8];
+    double dxr[8][8], dyr[8][8], dzr[8][8];  // [p][n]
+};
+__constant__ AsmRef c_asm_ref;
+
+// node n of an element relative to node 7 (ishift(7,n), jshift(7,n), kshift(7,n), :455-478)
+__constant__ int c_ish7[8] = {-1, 0, 0, -1, -1, 0, 0, -1};
+__constant__ int c_jsh7[8] = {-1, -1, 0, 0, -1, -1, 0, 0};
+__constant__ int c_ksh7[8] = {1, 1, 1, 1, 0, 0, 0, 0};
+
+struct AsmArgs {
+    int nx, ny, nz, nhalo;
+    int whichapprox, whichefvs;  // 0 SIA, 1 SSA, else BP; 0 constant, 1 flow factor, 2 nonlinear
+    double efvs_constant, effstrain_min, p_half;  // p_half = (1 - n)/n / 2
+    double flowfact_pow;                          // (velo_scale/len_scale*scyr)^((1-n)/n), host pow
+    const double *sigma;                          // (nz)
+    const int32_t *active_cell;                   // (nx, ny)
+    const double *xv, *yv, *usrf, *thck;          // (nx-1, ny-1)
+    const double *u, *v;                          // (nz, nx-1, ny-1), or level-major planes
+    int vel_planes;                               // 1: u, v are level-major planes (k*NQ + q)
+    const double *flwafact;                       // (nz-1, nx, ny)
+    double *efvs;                                 // (nz-1, nx, ny), zeroed by the host
+    int *singular;                                // set when an element's Jacobian is singular
+};
+
+// The row of node nr of element (ie, je, ke) (1-based) added to the accumulators acc[b][m]:
+// the element's quadrature loop (:5502-5571) restricted to row nr of Kuu, Kuv, Kvu, Kvv.
+// Returns false for a singular Jacobian.  The element's own thread also writes its mean
+// viscosity (:5575-5581).
+__device__ bool asm_element_row(const AsmArgs &a, int ie, int je, int ke, int nr, bool own, double acc[4][27]) {
+    const long long NX = a.nx - 1;
+    double x[8], y[8], z[8], u[8], v[8];
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+        const int iN = ie + c_ish7[n], jN = je + c_jsh7[n], kN = ke + c_ksh7[n];
+        const long long q = (long long)(iN - 1) + NX * (jN - 1);
+        x[n] = a.xv[q];
+        y[n] = a.yv[q];
+        z[n] = a.usrf[q] - a.sigma[kN - 1] * a.thck[q];
+        const long long e = a.vel_planes ? (long long)(kN - 1) * NX * (a.ny - 1) + q : (long long)(kN - 1) + a.nz * q;
+        u[n] = a.u[e];
+        v[n] = a.v[e];
+    }
+    const double ff = a.flwafact[(ke - 1) + (long long)(a.nz - 1) * ((ie - 1) + (long long)a.nx * (je - 1))];
+    double Kuu[8], Kuv[8], Kvu[8], Kvv[8];
+#pragma unroll
+    for (int nc = 0; nc < 8; ++nc) Kuu[nc] = Kuv[nc] = Kvu[nc] = Kvv[nc] = 0.0;
+    double esum = 0.0;
+    for (int p = 0; p < 8; ++p) {
+        const double *dxr = c_asm_ref.dxr[p], *dyr = c_asm_ref.dyr[p], *dzr = c_asm_ref.dzr[p];
+        // get_basis_function_derivatives_3d
+        double J00 = 0.0, J01 = 0.0, J02 = 0.0, J10 = 0.0, J11 = 0.0, J12 = 0.0, J20 = 0.0, J21 = 0.0, J22 = 0.0;
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            J00 = J00 + dxr[n] * x[n];
+            J01 = J01 + dxr[n] * y[n];
+            J02 = J02 + dxr[n] * z[n];
+            J10 = J10 + dyr[n] * x[n];
+            J11 = J11 + dyr[n] * y[n];
+            J12 = J12 + dyr[n] * z[n];
+            J20 = J20 + dzr[n] * x[n];
+            J21 = J21 + dzr[n] * y[n];
+            J22 = J22 + dzr[n] * z[n];
+        }
+        const double c00 = J11 * J22 - J12 * J21, c01 = -(J10 * J22 - J12 * J20), c02 = J10 * J21 - J11 * J20;
+        const double c10 = -(J01 * J22 - J02 * J21), c11 = J00 * J22 - J02 * J20, c12 = -(J00 * J21 - J01 * J20);
+        const double c20 = J01 * J12 - J02 * J11, c21 = -(J00 * J12 - J02 * J10), c22 = J00 * J11 - J01 * J10;
+        const double detJ = J00 * c00 + J01 * c01 + J02 * c02;
+        if (!(fabs(detJ) > 0.0)) return false;
+        // Jinv(row,col) = cofactor(col,row) / detJ
+        const double i00 = c00 / detJ, i01 = c10 / detJ, i02 = c20 / detJ;
+        const double i10 = c01 / detJ, i11 = c11 / detJ, i12 = c21 / detJ;
+        const double i20 = c02 / detJ, i21 = c12 / detJ, i22 = c22 / detJ;
+        double dx[8], dy[8], dz[8];
+#pragma unroll
+        for (int n = 0; n < 8; ++n) {
+            dx[n] = i00 * dxr[n] + i01 * dyr[n] + i02 * dzr[n];
+            dy[n] = i10 * dxr[n] + i11 * dyr[n] + i12 * dzr[n];
+            dz[n] = i20 * dxr[n] + i21 * dyr[n] + i22 * dzr[n];
+        }
+        // compute_effective_viscosity
+        double efvs;
+        if (a.whichefvs == 0) {
+            efvs = a.efvs_constant;
+        } else if (a.whichefvs == 1) {
+            efvs = ff * a.flowfact_pow;
+        } else {
+            double du_dx = 0.0, du_dy = 0.0, du_dz = 0.0, dv_dx = 0.0, dv_dy = 0.0, dv_dz = 0.0, sq;
+            const double em2 = a.effstrain_min * a.effstrain_min;
+            if (a.whichapprox == 0) {
+#pragma unroll
+                for (int n = 0; n < 8; ++n) {
+                    du_dz = du_dz + dz[n] * u[n];
+                    dv_dz = dv_dz + dz[n] * v[n];
+                }
+                sq = em2 + 0.25 * (du_dz * du_dz + dv_dz * dv_dz);
+            } else {
+#pragma unroll
+                for (int n = 0; n < 8; ++n) {
+                    du_dx = du_dx + dx[n] * u[n];
+                    du_dy = du_dy + dy[n] * u[n];
+                    if (a.whichapprox != 1) du_dz = du_dz + dz[n] * u[n];
+                    dv_dx = dv_dx + dx[n] * v[n];
+                    dv_dy = dv_dy + dy[n] * v[n];
+                    if (a.whichapprox != 1) dv_dz = dv_dz + dz[n] * v[n];
+                }
+                const double sh = dv_dx + du_dy;
+                sq = em2 + (du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * (sh * sh));
+                if (a.whichapprox != 1) sq = sq + 0.25 * (du_dz * du_dz + dv_dz * dv_dz);
+            }
+            efvs = ff * pow(sq, a.p_half);
+        }
+        esum = esum + efvs;
+        // compute_element_matrix, row nr
+        const double f = efvs * c_asm_ref.wqp[p] * detJ / kAsmVol0;
+#pragma unroll
+        for (int nc = 0; nc < 8; ++nc) {
+            if (a.whichapprox == 0) {
+                Kuu[nc] = Kuu[nc] + f * (dz[nr] * dz[nc]);
+                Kvv[nc] = Kvv[nc] + f * (dz[nr] * dz[nc]);
+            } else if (a.whichapprox == 1) {
+                Kuu[nc] = Kuu[nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc]);
+                Kuv[nc] = Kuv[nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
+                Kvu[nc] = Kvu[nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
+                Kvv[nc] = Kvv[nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc]);
+            } else {
+                Kuu[nc] = Kuu[nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc] + dz[nr] * dz[nc]);
+                Kuv[nc] = Kuv[nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
+                Kvu[nc] = Kvu[nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
+                Kvv[nc] = Kvv[nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc] + dz[nr] * dz[nc]);
+            }
+        }
+    }
+    if (own) a.efvs[(ke - 1) + (long long)(a.nz - 1) * ((ie - 1) + (long long)a.nx * (je - 1))] = esum / 8;
+    // element_to_global_matrix_3d, row nr
+#pragma unroll
+    for (int nc = 0; nc < 8; ++nc) {
+        const int m = (c_ish7[nc] - c_ish7[nr] + 1) + 3 * (c_jsh7[nc] - c_jsh7[nr] + 1) +
+                      9 * (c_ksh7[nc] - c_ksh7[nr] + 1);
+        acc[0][m] = acc[0][m] + Kuu[nc];
+        acc[1][m] = acc[1][m] + Kuv[nc];
+        acc[2][m] = acc[2][m] + Kvu[nc];
+        acc[3][m] = acc[3][m] + Kvv[nc];
+    }
+    return true;
+}
+
+// One thread per node (k, q = i + NX*j, 0-based): the elements that contain the node, in the
+// reference's element order (j, then i, then k), each valid when its cell is one the reference
+// loops over (nhalo+1..n-nhalo+1), is active, and its layer exists; then the node's 4 x 27
+// coefficients in layout L (every coefficient of every node is written, zero where no element
+// contributes, as the reference zeroes A first).
+__global__ void __launch_bounds__(kAsmBlock) k_assemble3d(AsmArgs a, SymIdx L, double *Auu, double *Auv,
+                                                          double *Avu, double *Avv) {
+    const long long NX = a.nx - 1, NQ = NX * (a.ny - 1);
+    const long long n = (long long)a.nz * NQ;
+    const long long t = (long long)blockIdx.x * kAsmBlock + threadIdx.x;
+    if (t >= n) return;
+    const int k0 = (int)(t / NQ);
+    const long long q = t - (long long)k0 * NQ;
+    const int j0 = (int)(q / NX), i0 = (int)(q - (long long)j0 * NX);
+    const int iR = i0 + 1, jR = j0 + 1, kR = k0 + 1;  // 1-based node
+    double acc[4][27];
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int c = 0; c < 27; ++c) acc[b][c] = 0.0;
+    for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di)
+            for (int dk = 0; dk < 2; ++dk) {
+                const int je = jR + dj, ie = iR + di, ke = kR - 1 + dk;
+                if (ke < 1 || ke > a.nz - 1) continue;
+                if (ie < a.nhalo + 1 || ie > a.nx - a.nhalo + 1 || je < a.nhalo + 1 || je > a.ny - a.nhalo + 1)
+                    continue;
+                if (!a.active_cell[(ie - 1) + (long long)a.nx * (je - 1)]) continue;
+                // node index within the element: shifts (iR-ie, jR-je, kR-ke) = (-di, -dj, 1-dk)
+                const int nr = (dk == 0 ? 0 : 4) + (dj == 0 ? (di == 0 ? 2 : 3) : (di == 0 ? 1 : 0));
+                if (!asm_element_row(a, ie, je, ke, nr, dj == 0 && di == 0 && dk == 1, acc)) atomicExch(a.singular, 1);
+            }
+    double *B[4] = {Auu, Auv, Avu, Avv};
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+        for (int c = 0; c < 27; ++c) B[b][L.at(c, k0, q)] = acc[b][c];
+}
+
+}  // namespace cismgpu

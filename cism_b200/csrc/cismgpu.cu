@@ -19,6 +19,7 @@
 
 #include "pcg_fp64.cu"
 #include "pcg_mixed.cu"
+#include "assembly.cu"
 
 namespace cismgpu {
 
@@ -113,6 +114,7 @@ struct Solver {
     DevBuf tri;       // tridiagonal preconditioner planes (TriPlane), on first use
     DevBuf A_sav, x_sav;      // accelerated Picard's saved matrix and velocity (cismgpu_solver_save)
     DevBuf rsum;              // the reproducible sum's exponent extremes and level sums
+    DevBuf asm_in;            // the stiffness assembly's inputs (geometry, flow factor, velocity, efvs)
     bool have_sav = false;
     bool x_current = false;   // the x planes hold a solution (a solve ran since the last upload)
     int32_t hindx[27] = {};   // host copy of the uploaded indxA map (27 or 9 entries)
@@ -138,6 +140,7 @@ struct Solver {
         A_sav.release();
         x_sav.release();
         rsum.release();
+        asm_in.release();
         have_sav = false;
         mixed.release();
         if (h_done) cudaFreeHost(h_done);
@@ -310,6 +313,90 @@ struct Solver {
         std::memcpy(&md, &h[0], sizeof(md));
         if (maxdiff) *maxdiff = md;
         if (nwarn) *nwarn = (long long)h[1];
+        return CISMGPU_OK;
+    }
+
+    // assemble_stiffness_matrix_3d (glissade_velo_higher.F90:5382-5643) on the device into four
+    // blocks in layout L.  The host arrays are uploaded; u, v null: the velocity planes vel_id,
+    // vel_id+1 (level-major) instead.  efvs (host, may be null) receives the element viscosity.
+    // Leaves the stream synchronized.
+    int assemble3d(const SymIdx &L, double *Auu, double *Auv, double *Avu, double *Avv, int nhalo,
+                   const double *sigma, const int32_t *active_cell, const double *xv, const double *yv,
+                   const double *u, const double *v, int vel_id, const double *usrf, const double *thck,
+                   const double *flwafact, int whichapprox, int whichefvs, double efvs_constant,
+                   double effstrain_min, double n_glen, double *efvs) {
+        static bool ref_ready = false;  // the reference element in constant memory (:314-392)
+        if (!ref_ready) {
+            AsmRef r;
+            const double rs = 1.0 / std::sqrt(3.0);
+            const double xq[8] = {-rs, rs, rs, -rs, -rs, rs, rs, -rs};
+            const double yq[8] = {-rs, -rs, rs, rs, -rs, -rs, rs, rs};
+            const double zq[8] = {-rs, -rs, -rs, -rs, rs, rs, rs, rs};
+            const double sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1}, sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1},
+                         sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};  // node corners of the reference cube
+            for (int p = 0; p < 8; ++p) {
+                r.wqp[p] = 1.0;
+                for (int n = 0; n < 8; ++n) {  // d/dxr of (1 +- x)(1 +- y)(1 +- z)/8, as :362-389
+                    const double fx = sx[n] < 0 ? 1.0 - xq[p] : 1.0 + xq[p];
+                    const double fy = sy[n] < 0 ? 1.0 - yq[p] : 1.0 + yq[p];
+                    const double fz = sz[n] < 0 ? 1.0 - zq[p] : 1.0 + zq[p];
+                    r.dxr[p][n] = sx[n] * fy * fz / 8.0;
+                    r.dyr[p][n] = sy[n] * fx * fz / 8.0;
+                    r.dzr[p][n] = sz[n] * fx * fy / 8.0;
+                }
+            }
+            CU(cudaMemcpyToSymbol(c_asm_ref, &r, sizeof(r)));
+            ref_ready = true;
+        }
+        const int nx = g.NX + 1, ny = g.NY + 1, nz = g.nz;
+        const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny, nel = (size_t)(nz - 1) * ncell;
+        const bool host_vel = u != nullptr;
+        // doubles: sigma, 4 vertex fields, flwafact, efvs, [u, v]; then active_cell and the flag
+        const size_t nd = (size_t)nz + 4 * nq + 2 * nel + (host_vel ? 2 * (size_t)nz * nq : 0);
+        CU(asm_in.ensure(nd * sizeof(double) + ncell * sizeof(int32_t) + 16));
+        double *D = asm_in.as<double>();
+        double *d_sigma = D, *d_xv = D + nz, *d_yv = d_xv + nq, *d_usrf = d_yv + nq, *d_thck = d_usrf + nq;
+        double *d_ff = d_thck + nq, *d_efvs = d_ff + nel, *d_u = d_efvs + nel, *d_v = d_u + (size_t)nz * nq;
+        int32_t *d_act = reinterpret_cast<int32_t *>(D + nd);
+        int *d_sing = reinterpret_cast<int *>(d_act + ncell);
+        cudaStream_t s = stream;
+        auto up = [&](void *dst, const void *src, size_t bytes) {
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+        };
+        CU(up(d_sigma, sigma, nz * sizeof(double)));
+        CU(up(d_xv, xv, nq * sizeof(double)));
+        CU(up(d_yv, yv, nq * sizeof(double)));
+        CU(up(d_usrf, usrf, nq * sizeof(double)));
+        CU(up(d_thck, thck, nq * sizeof(double)));
+        CU(up(d_ff, flwafact, nel * sizeof(double)));
+        CU(up(d_act, active_cell, ncell * sizeof(int32_t)));
+        if (host_vel) {
+            CU(up(d_u, u, (size_t)nz * nq * sizeof(double)));
+            CU(up(d_v, v, (size_t)nz * nq * sizeof(double)));
+        }
+        CU(cudaMemsetAsync(d_efvs, 0, nel * sizeof(double), s));
+        CU(cudaMemsetAsync(d_sing, 0, sizeof(int), s));
+        AsmArgs a;
+        a.nx = nx; a.ny = ny; a.nz = nz; a.nhalo = nhalo;
+        a.whichapprox = whichapprox; a.whichefvs = whichefvs;
+        a.efvs_constant = efvs_constant; a.effstrain_min = effstrain_min;
+        a.p_half = (1.0 - n_glen) / n_glen / 2.0;
+        // HO_EFVS_FLOWFACT: velo_scale / len_scale * scyr (glimmer_paramets.F90:97-98), host pow
+        a.flowfact_pow = std::pow(500.0 / 31536000.0 / 200.0e3 * 31536000.0, (1.0 - n_glen) / n_glen);
+        a.sigma = d_sigma; a.active_cell = d_act; a.xv = d_xv; a.yv = d_yv; a.usrf = d_usrf; a.thck = d_thck;
+        const double *V = vec.as<double>();
+        a.u = host_vel ? d_u : V + (size_t)vel_id * nvec;
+        a.v = host_vel ? d_v : V + (size_t)(vel_id + 1) * nvec;
+        a.vel_planes = host_vel ? 0 : 1;
+        a.flwafact = d_ff; a.efvs = d_efvs; a.singular = d_sing;
+        const long long n = (long long)nz * g.NQ;
+        k_assemble3d<<<(unsigned)((n + kAsmBlock - 1) / kAsmBlock), kAsmBlock, 0, s>>>(a, L, Auu, Auv, Avu, Avv);
+        CU(cudaGetLastError());
+        int sing = 0;
+        CU(cudaMemcpyAsync(&sing, d_sing, sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (efvs) CU(cudaMemcpyAsync(efvs, d_efvs, nel * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (sing) return fail(CISMGPU_EINVAL, "Jacobian matrix is singular (an element of zero volume)");
         return CISMGPU_OK;
     }
 
@@ -1234,6 +1321,56 @@ static int oneshot_symmetry(bool is3d, int nx, int ny, int nz, const cismgpu_par
     return CISMGPU_OK;
 }
 
+static int validate_assembly(int nx, int ny, int nz, int nhalo, int whichefvs, double n_glen, const void *sigma,
+                             const void *act, const void *xv, const void *yv, const void *usrf, const void *thck,
+                             const void *ff) {
+    if (!sigma || !act || !xv || !yv || !usrf || !thck || !ff) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (nx < 6 || ny < 6 || nz < 2 || nz > kMaxNz) return fail(CISMGPU_EINVAL, "grid too small or nz outside 2..64");
+    if (nhalo < 2 || 2 * nhalo >= nx || 2 * nhalo >= ny)
+        return fail(CISMGPU_EINVAL, "nhalo must be >= 2 (element vertices inside the arrays) and fit the grid");
+    if (whichefvs < 0 || whichefvs > 2) return fail(CISMGPU_EINVAL, "whichefvs outside 0..2");
+    if (!(n_glen > 0.0)) return fail(CISMGPU_EINVAL, "n_glen must be positive");
+    return CISMGPU_OK;
+}
+
+// assemble_stiffness_matrix_3d on the caller's host arrays: inputs uploaded, the blocks written
+// on the device in the caller's layout (through its indxA_3d) and copied back.
+static int oneshot_assemble3d(int nx, int ny, int nz, int nhalo, const double *sigma, const int32_t *active_cell,
+                              const double *xv, const double *yv, const double *u, const double *v,
+                              const double *usrf, const double *thck, const double *ff, int whichapprox,
+                              int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
+                              const int32_t *indx, double *efvs, double *const blocks[4]) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_error.clear();
+    TRY(validate_assembly(nx, ny, nz, nhalo, whichefvs, n_glen, sigma, active_cell, xv, yv, usrf, thck, ff));
+    if (!u || !v || !indx || !blocks[0] || !blocks[1] || !blocks[2] || !blocks[3])
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    TRY(validate_indx(indx, 27));
+    cismgpu_par_t par{};
+    par.staggered_ilo = 1; par.staggered_ihi = nx - 1; par.staggered_jlo = 1; par.staggered_jhi = ny - 1;
+    par.tasks_row = par.tasks_col = 1;
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
+    TRY(sv.set_geom(make_geom(nx, ny, nz, &par), true));
+    const size_t bs = (size_t)27 * sv.nvec;
+    CU(sv.A.ensure(4 * bs * sizeof(double)));
+    sv.mixed.stale = true;  // the matrix buffer holds the caller's layout until the next upload
+    double *A0 = sv.A.as<double>();
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = indx[c];
+    L.n = sv.nvec;
+    L.NQ = sv.g.NQ;
+    L.nz = nz;
+    L.raw3 = 1;
+    TRY(sv.assemble3d(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, nhalo, sigma, active_cell, xv, yv, u, v, 0, usrf,
+                      thck, ff, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen, efvs));
+    for (int b = 0; b < 4; ++b)
+        CU(cudaMemcpyAsync(blocks[b], A0 + b * bs, bs * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
+    CU(cudaStreamSynchronize(sv.stream));
+    return CISMGPU_OK;
+}
+
 static int oneshot_resid_velo(bool is3d, int whichresid, int nx, int ny, int nz, const cismgpu_par_t *par,
                               const double *uvel, const double *vvel, const double *usav, const double *vsav,
                               double *resid_velo) {
@@ -1749,6 +1886,48 @@ int cismgpu_solver_residual_vector(cismgpu_solver_t *h, double *resid_u, double 
     *L2_norm = l2;
     if (L2_norm_relative) *L2_norm_relative = (l2b > 0.0) ? l2 / l2b : 0.0;
     return CISMGPU_OK;
+}
+
+int cismgpu_assemble_stiffness_matrix_3d(int nx, int ny, int nz, int nhalo, const double *sigma,
+                                         const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                         const double *uvel, const double *vvel, const double *stagusrf,
+                                         const double *stagthck, const double *flwafact, int whichapprox,
+                                         int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
+                                         const int32_t *indxA_3d, double *efvs, double *Auu, double *Auv,
+                                         double *Avu, double *Avv) {
+    double *const blocks[4] = {Auu, Auv, Avu, Avv};
+    return oneshot_assemble3d(nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel, vvel, stagusrf,
+                              stagthck, flwafact, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen,
+                              indxA_3d, efvs, blocks);
+}
+
+int cismgpu_solver_assemble_stiffness_3d(cismgpu_solver_t *h, int nhalo, const double *sigma,
+                                         const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                         const double *uvel, const double *vvel, const double *stagusrf,
+                                         const double *stagthck, const double *flwafact, int whichapprox,
+                                         int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
+                                         double *efvs) {
+    g_last_error.clear();
+    if (!h) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
+    Solver &sv = h->sv;
+    if (!sv.is3d) return fail(CISMGPU_EINVAL, "the handle holds a 2D system");
+    if ((!uvel) != (!vvel)) return fail(CISMGPU_EINVAL, "give both velocity components or neither");
+    TRY(validate_assembly(sv.g.NX + 1, sv.g.NY + 1, sv.g.nz, nhalo, whichefvs, n_glen, sigma, active_cell, xVertex,
+                          yVertex, stagusrf, stagthck, flwafact));
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = c + 1;
+    L.n = sv.nvec;
+    L.NQ = sv.g.NQ;
+    L.nz = sv.g.nz;
+    L.raw3 = 0;
+    const size_t bs = (size_t)27 * sv.nvec;
+    double *A0 = sv.A.as<double>();
+    sv.mixed.stale = true;  // the FP32 copies follow the new matrix
+    return sv.assemble3d(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, nhalo, sigma, active_cell, xVertex, yVertex, uvel,
+                         vvel, sv.x_current ? VX_U : VX0_U, stagusrf, stagthck, flwafact, whichapprox, whichefvs,
+                         efvs_constant, effstrain_min, n_glen, efvs);
 }
 
 int cismgpu_solver_check_symmetry(cismgpu_solver_t *h, double *maxdiff, long long *nwarn) {

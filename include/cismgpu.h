@@ -242,6 +242,28 @@ int cismgpu_check_symmetry_assembled_matrix_2d(int nx, int ny, const cismgpu_par
                                                const double *Avu, const double *Avv, double *maxdiff,
                                                long long *nwarn);
 
+/* Replaces assemble_stiffness_matrix_3d (glissade_velo_higher.F90:5382-5643): the four
+ * Blatter-Pattyn (whichapprox 2; 1 SSA and 0 SIA forms too) stiffness blocks of the
+ * trilinear hexahedral elements of every active cell j = nhalo+1..ny-nhalo+1,
+ * i = nhalo+1..nx-nhalo+1, layers 1..nz-1, with 8-point Gauss quadrature and the effective
+ * viscosity of whichefvs (0 constant efvs_constant, 1 flow factor, 2 nonlinear from uvel,
+ * vvel with effstrain_min; glide_types.F90:240-242), computed on the GPU.  Arguments are the
+ * reference's (itest, jtest, rtest dropped), in its layouts: sigma(nz), active_cell(nx,ny)
+ * (nonzero = .true.), xVertex, yVertex, stagusrf, stagthck (nx-1,ny-1), uvel, vvel
+ * (nz,nx-1,ny-1), flwafact and efvs (nz-1,nx,ny), A** (27,nz,nx-1,ny-1); n_glen is
+ * glimmer_physcon's n_glen and indxA_3d the module's index map.  nhalo must be >= 2.
+ * Every coefficient is the reference's sum, term for term and in the reference's element
+ * order (so A is exactly symmetric); only the flow law's pow is CUDA's rather than the host
+ * C library's.  A singular element Jacobian (the reference stops with GM_FATAL) returns
+ * CISMGPU_EINVAL.  The basal and Dirichlet conditions and the load vector are not applied. */
+int cismgpu_assemble_stiffness_matrix_3d(int nx, int ny, int nz, int nhalo, const double *sigma,
+                                         const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                         const double *uvel, const double *vvel, const double *stagusrf,
+                                         const double *stagthck, const double *flwafact, int whichapprox,
+                                         int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
+                                         const int32_t *indxA_3d, double *efvs, double *Auu, double *Auv,
+                                         double *Avu, double *Avv);
+
 /* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps
@@ -376,6 +398,18 @@ int cismgpu_solver_restore(cismgpu_solver_t *s);
  * the averages are written into the device copy that the next solve uses (the caller's host
  * arrays are not touched); in 2D nothing changes.  maxdiff and nwarn may be NULL. */
 int cismgpu_solver_check_symmetry(cismgpu_solver_t *s, double *maxdiff, long long *nwarn);
+
+/* cismgpu_assemble_stiffness_matrix_3d (see above) into a 3D handle's resident blocks: the
+ * next solve, residual or check uses the assembled A without it crossing PCIe.  uvel = vvel =
+ * NULL takes the handle's current velocity (the last solution, else the initial guess), so a
+ * Picard loop uploads only the geometry and flow factor.  efvs may be NULL.  The right-hand
+ * side and the boundary conditions are not touched (cismgpu_solver_set_system replaces all). */
+int cismgpu_solver_assemble_stiffness_3d(cismgpu_solver_t *s, int nhalo, const double *sigma,
+                                         const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                         const double *uvel, const double *vvel, const double *stagusrf,
+                                         const double *stagthck, const double *flwafact, int whichapprox,
+                                         int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
+                                         double *efvs);
 
 /* Per-kernel CUDA-event timing of the structured matvec launches (off by default).
  * read: total device milliseconds, launch count, and algorithmic bytes per launch

@@ -1,0 +1,137 @@
+"""assemble_stiffness_matrix_3d (glissade_velo_higher.F90:5382-5643) on the device, through
+the C ABI: one-shot on the caller's arrays and into a device-resident handle.
+
+Bars, against the oracle's restatement on the same inputs:
+  - constant and flow-factor viscosity: bit-exact blocks and efvs (no pow on the device, or
+    the host's pow);
+  - nonlinear viscosity: the flow law's pow is CUDA's, not the host C library's (a few ulp
+    apart), so efvs within 1e-14 relative and every coefficient within 1e-13 of its block's
+    largest; the blocks are still exactly symmetric (each element's terms are shared by the
+    pair in the same order);
+  - a handle's assembly equals the one-shot assembly bit for bit, with the velocity given or
+    taken from the last solution.
+"""
+import numpy as np
+import pytest
+
+import cism_b200 as cg
+import oracle
+from cism_b200 import assembly as asm
+from tests.test_oracle_assembly import geometry
+
+pytestmark = pytest.mark.gpu
+
+BLOCKS = ("Auu", "Auv", "Avu", "Avv")
+
+
+def inputs(g, seed=3, scale=40.0):
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(seed)
+    shape = (ny - 1, nx - 1, nz)
+    u, v = scale * rng.standard_normal(shape), scale * rng.standard_normal(shape)
+    ff = 0.5 * 1.0e-16 ** (-1.0 / 3.0) * (1.0 + 0.2 * rng.random((ny, nx, nz - 1)))
+    return u, v, ff
+
+
+def both(g, u, v, ff, **kw):
+    args = (g["nx"], g["ny"], g["nz"])
+    geo = (g["sigma"], g["ac"].astype(np.int32), g["xVertex"], g["yVertex"])
+    o = oracle.assemble_stiffness_3d(*args, *geo, u, v, g["stagusrf"], g["stagthck"], ff, **kw)
+    assert o[0] == 0
+    d = cg.assemble_stiffness_matrix_3d(*args, 2, *geo, u, v, g["stagusrf"], g["stagthck"], ff, **kw)
+    return o[1:], d
+
+
+@pytest.mark.parametrize("efvs_opt", [0, 1])
+@pytest.mark.parametrize("approx", [2, 1, 0])
+def test_assembly_bitexact_without_pow(gpu_lib, approx, efvs_opt):
+    g = geometry(seed=21)
+    u, v, ff = inputs(g)
+    o, d = both(g, u, v, ff, whichapprox=approx, whichefvs=efvs_opt, efvs_constant=3.0e6)
+    for a, b in zip(o, d):
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("approx", [2, 1, 0])
+def test_assembly_nonlinear_viscosity(gpu_lib, approx):
+    g = geometry(seed=22)
+    u, v, ff = inputs(g)
+    o, d = both(g, u, v, ff, whichapprox=approx)
+    act = g["ac"]
+    rel = np.abs(d[0][act] - o[0][act]) / o[0][act]
+    assert rel.max() <= 1e-14 and np.all(d[0][~act] == 0.0)
+    for a, b in zip(o[1:], d[1:]):
+        scale = max(np.abs(a).max(), 1e-300)
+        assert np.abs(a - b).max() <= 1e-13 * scale
+    P = asm.Problem("3d", g["nx"], g["ny"], g["nz"], *d[1:], np.zeros_like(u), np.zeros_like(u),
+                    g["av"].astype(np.int32), asm.default_par(g["nx"], g["ny"]))
+    r = oracle.check_symmetry(P)
+    assert r[4] == 0.0 and r[5] == 0
+
+
+def test_assembly_permuted_index_map(gpu_lib):
+    """The blocks come back in the caller's layout through its indxA_3d map."""
+    g = geometry(seed=23)
+    u, v, ff = inputs(g)
+    perm = np.random.default_rng(5).permutation(27).astype(np.int32) + 1
+    args = (g["nx"], g["ny"], g["nz"], 2, g["sigma"], g["ac"].astype(np.int32), g["xVertex"], g["yVertex"], u, v,
+            g["stagusrf"], g["stagthck"], ff)
+    base = cg.assemble_stiffness_matrix_3d(*args, whichefvs=0, efvs_constant=1.0e6)
+    got = cg.assemble_stiffness_matrix_3d(*args, whichefvs=0, efvs_constant=1.0e6, indxA_3d=perm)
+    for a, b in zip(base[1:], got[1:]):
+        for c in range(27):
+            np.testing.assert_array_equal(b[..., perm[c] - 1], a[..., c])
+
+
+def _slab_problem(g):
+    """A solvable system on the same grid: the first-Picard slab the solver tests use."""
+    return asm.assemble_bp_3d(g["thck"], g["usrf"], g["dx"], g["dx"], g["nz"],
+                              beta=asm.lognormal_beta((g["ny"] - 1, g["nx"] - 1), 7))
+
+
+def test_assembly_on_handle(gpu_lib):
+    """Into a handle: the resident blocks are the one-shot blocks (checked through the
+    residual of the assembled system), with the velocity given and from the last solution."""
+    g = geometry(seed=24)
+    u, v, ff = inputs(g, scale=10.0)
+    P = _slab_problem(g)
+    geo = (2, g["sigma"], g["ac"].astype(np.int32), g["xVertex"], g["yVertex"], g["stagusrf"], g["stagthck"], ff)
+    s = cg.DeviceSolver(P, x0=(u, v))
+    try:
+        s.solve(cg.ALG_CHRONGEAR, cg.HO_PRECOND_DIAG, 5, 1e-6, 50)  # the slab's own, well-posed system
+        xs = s.x()
+        efvs_x = s.assemble_stiffness(*geo)                 # velocity: the solution, on the device
+        efvs_h = s.assemble_stiffness(*geo, uvel=u, vvel=v)  # velocity from the host
+        ru, rv, l2, _ = s.residual_vector()                 # A(u, v) xs - b
+    finally:
+        s.close()
+    d = cg.assemble_stiffness_matrix_3d(g["nx"], g["ny"], g["nz"], 2, g["sigma"], g["ac"].astype(np.int32),
+                                        g["xVertex"], g["yVertex"], u, v, g["stagusrf"], g["stagthck"], ff)
+    np.testing.assert_array_equal(efvs_h, d[0])
+    Q = _slab_problem(g)
+    for n, a in zip(BLOCKS, d[1:]):
+        setattr(Q, n, a)
+    want = cg.compute_residual_vector_3d(Q.nx, Q.ny, Q.nz, Q.par, asm.indxA_3d(), Q.active_vertex, Q.Auu, Q.Auv,
+                                         Q.Avu, Q.Avv, Q.bu, Q.bv, xs[0], xs[1])
+    np.testing.assert_array_equal(ru, want[0])
+    np.testing.assert_array_equal(rv, want[1])
+    assert l2 == want[2]
+    dx = cg.assemble_stiffness_matrix_3d(g["nx"], g["ny"], g["nz"], 2, g["sigma"], g["ac"].astype(np.int32),
+                                         g["xVertex"], g["yVertex"], xs[0], xs[1], g["stagusrf"], g["stagthck"], ff)
+    np.testing.assert_array_equal(efvs_x, dx[0])
+
+
+def test_assembly_errors(gpu_lib):
+    g = geometry(seed=25)
+    u, v, ff = inputs(g)
+    args = [g["nx"], g["ny"], g["nz"], 2, g["sigma"], g["ac"].astype(np.int32), g["xVertex"], g["yVertex"], u, v,
+            g["stagusrf"], g["stagthck"], ff]
+    bad = list(args)
+    bad[3] = 1  # nhalo < 2: element vertices outside the arrays
+    with pytest.raises(cg.CismGpuError):
+        cg.assemble_stiffness_matrix_3d(*bad)
+    flat = list(args)
+    flat[10] = np.zeros_like(g["stagusrf"])  # every node at z = 0: the Jacobian's z column is zero
+    flat[11] = np.zeros_like(g["stagthck"])
+    with pytest.raises(cg.CismGpuError):
+        cg.assemble_stiffness_matrix_3d(*flat)
