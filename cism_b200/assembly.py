@@ -291,8 +291,10 @@ def assemble_bp_3d(thck, usrf, dx, dy, nz, flwa=1.0e-16, beta=None, bc="periodic
                    av.astype(np.int32), par, name)
 
 
-def assemble_ssa_2d(thck, usrf, dx, dy, beta, flwa=1.0e-16, bc="periodic", name="") -> Problem:
-    """SSA 2D system (9-point blocks) for the first Picard iteration, beta-local sliding."""
+def assemble_ssa_2d(thck, usrf, dx, dy, beta, flwa=1.0e-16, bc="periodic", name="",
+                    stiffness_only=False) -> Problem:
+    """SSA 2D system (9-point blocks) for the first Picard iteration, beta-local sliding.
+    stiffness_only: the assembled stiffness blocks without the basal term."""
     ny, nx = thck.shape
     NX, NY = nx - 1, ny - 1
     ac, av = active_masks(thck)
@@ -329,8 +331,9 @@ def assemble_ssa_2d(thck, usrf, dx, dy, beta, flwa=1.0e-16, bc="periodic", name=
     gx, gy = np.gradient(staglsrf, dy, dx)
     theta = np.arctan(np.sqrt(gx * gx + gy * gy))
     add = np.where(av, dx * dy / VOL0 * beta / np.cos(theta), 0.0)
-    A[0, 4] += add
-    A[3, 4] += add
+    if not stiffness_only:
+        A[0, 4] += add
+        A[3, 4] += add
     dsdx, dsdy = vertex_gradient(usrf, dx, dy)
     bu = np.where(av, -RHOI * GRAV * dx * dy * stagthck / VOL0 * dsdx, 0.0)
     bv = np.where(av, -RHOI * GRAV * dx * dy * stagthck / VOL0 * dsdy, 0.0)

@@ -67,6 +67,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_reprosum.argtypes = [d, ctypes.c_long]
         L.oracle_assemble_stiffness_3d.argtypes = [i, i, i, i, d, d, d, d, d, d, d, d, d, i, i, dbl, dbl, dbl,
                                                    d, d, d, d, d]
+        L.oracle_assemble_stiffness_2d.argtypes = [i, i, i, i, d, d, d, d, d, d, d, d, i, dbl, dbl, dbl, d, d, d, d, d]
         L.oracle_check_symmetry.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, P(dbl), P(ctypes.c_long)]
         L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
@@ -218,6 +219,21 @@ def assemble_stiffness_3d(nx, ny, nz, sigma, active_cell, xVertex, yVertex, uvel
            f64(vvel), f64(stagusrf), f64(stagthck), f64(flwafact)]
     st = lib().oracle_assemble_stiffness_3d(nx, ny, nz, nhalo, *[_p(a) for a in ins], whichapprox, whichefvs,
                                             efvs_constant, effstrain_min, n_glen, _p(efvs), *[_p(a) for a in A])
+    return (st, efvs, *A)
+
+
+def assemble_stiffness_2d(nx, ny, nz, sigma, active_cell, xVertex, yVertex, uvel, vvel, stagthck, flwafact,
+                          whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8, n_glen=3.0, nhalo=2):
+    """assemble_stiffness_matrix_2d (glissade_velo_higher.F90:4961-5378), SSA: vertex fields
+    (ny-1, nx-1), flwafact (ny, nx, nz-1).  Returns (status, efvs (ny, nx, nz-1), Auu, Auv,
+    Avu, Avv (9, ny-1, nx-1))."""
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    efvs = np.zeros((ny, nx, nz - 1))
+    A = [np.zeros((9, ny - 1, nx - 1)) for _ in range(4)]
+    ins = [f64(sigma), np.ascontiguousarray(active_cell, dtype=np.int32), f64(xVertex), f64(yVertex), f64(uvel),
+           f64(vvel), f64(stagthck), f64(flwafact)]
+    st = lib().oracle_assemble_stiffness_2d(nx, ny, nz, nhalo, *[_p(a) for a in ins], whichefvs, efvs_constant,
+                                            effstrain_min, n_glen, _p(efvs), *[_p(a) for a in A])
     return (st, efvs, *A)
 
 

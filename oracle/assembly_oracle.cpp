@@ -22,6 +22,7 @@
 #include <cstdint>
 #include <cstring>
 #include <initializer_list>
+#include <vector>
 
 namespace {
 
@@ -165,6 +166,24 @@ double efvs_qp(int whichefvs, int whichapprox, double efvs_constant, double effs
     return flwafact * std::pow(sq, p_effstr / 2.0);
 }
 
+// compute_effective_viscosity (:7285-7470) for the SSA on a 4-node element (dphi_dz = 0).
+double efvs_qp4(int whichefvs, double efvs_constant, double effstrain_min, double n_glen, const double *dx,
+                const double *dy, const double *u, const double *v, double flwafact) {
+    const double p_effstr = (1.0 - n_glen) / n_glen;
+    if (whichefvs == kEfvsConstant) return efvs_constant;
+    if (whichefvs == kEfvsFlowfact) return flwafact * std::pow(kVeloScale / kLenScale * kScyr, p_effstr);
+    double du_dx = 0.0, du_dy = 0.0, dv_dx = 0.0, dv_dy = 0.0;
+    for (int n = 0; n < 4; ++n) {
+        du_dx = du_dx + dx[n] * u[n];
+        du_dy = du_dy + dy[n] * u[n];
+        dv_dx = dv_dx + dx[n] * v[n];
+        dv_dy = dv_dy + dy[n] * v[n];
+    }
+    const double sq = effstrain_min * effstrain_min +
+                      (du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * ((dv_dx + du_dy) * (dv_dx + du_dy)));
+    return flwafact * std::pow(sq, p_effstr / 2.0);
+}
+
 // compute_element_matrix (:8001-8123): K += efvs*wqp*detJ/vol0 * (products), columns outer.
 void element_matrix(int whichapprox, double wqp, double detJ, double efvs, const double *dx, const double *dy,
                     const double *dz, double Kuu[8][8], double Kuv[8][8], double Kvu[8][8], double Kvv[8][8]) {
@@ -188,9 +207,142 @@ void element_matrix(int whichapprox, double wqp, double detJ, double efvs, const
         }
 }
 
+// The 2D reference element (glissade_velo_higher.F90:528-570): 4 Gauss points, weights 1.
+struct RefElement2 {
+    double phi[4][4], dxr[4][4], dyr[4][4];  // [p][n]
+    RefElement2() {
+        const double r = 1.0 / std::sqrt(3.0);
+        const double xq[4] = {-r, r, r, -r};
+        const double yq[4] = {-r, -r, r, r};
+        for (int p = 0; p < 4; ++p) {
+            const double x = xq[p], y = yq[p];
+            phi[p][0] = (1.0 - x) * (1.0 - y) / 4.0;
+            phi[p][1] = (1.0 + x) * (1.0 - y) / 4.0;
+            phi[p][2] = (1.0 + x) * (1.0 + y) / 4.0;
+            phi[p][3] = (1.0 - x) * (1.0 + y) / 4.0;
+            dxr[p][0] = -(1.0 - y) / 4.0;
+            dxr[p][1] = (1.0 - y) / 4.0;
+            dxr[p][2] = (1.0 + y) / 4.0;
+            dxr[p][3] = -(1.0 + y) / 4.0;
+            dyr[p][0] = -(1.0 - x) / 4.0;
+            dyr[p][1] = -(1.0 + x) / 4.0;
+            dyr[p][2] = (1.0 + x) / 4.0;
+            dyr[p][3] = (1.0 - x) / 4.0;
+        }
+    }
+};
+
+const RefElement2 &ref2() {
+    static const RefElement2 r;
+    return r;
+}
+
+// get_basis_function_derivatives_2d (:6319-6504)
+bool basis_derivs_2d(const double *x, const double *y, const double *dxr, const double *dyr, double *dx, double *dy,
+                     double *detJ) {
+    double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
+    for (int n = 0; n < 4; ++n) {
+        J00 = J00 + dxr[n] * x[n];
+        J01 = J01 + dxr[n] * y[n];
+        J10 = J10 + dyr[n] * x[n];
+        J11 = J11 + dyr[n] * y[n];
+    }
+    const double det = J00 * J11 - J01 * J10;
+    *detJ = det;
+    if (!(std::fabs(det) > 0.0)) return false;
+    const double i00 = J11 / det, i01 = -J01 / det, i10 = -J10 / det, i11 = J00 / det;
+    for (int n = 0; n < 4; ++n) {
+        dx[n] = 0.0 + i00 * dxr[n] + i01 * dyr[n];
+        dy[n] = 0.0 + i10 * dxr[n] + i11 * dyr[n];
+    }
+    return true;
+}
+
+// 2D node n of the element relative to the element's (i, j): ishift(3,n), jshift(3,n)
+constexpr int kIsh3[4] = {-1, 0, 0, -1};
+constexpr int kJsh3[4] = {-1, -1, 0, 0};
+
 }  // namespace
 
 extern "C" {
+
+// assemble_stiffness_matrix_2d (:4961-5378), SSA branch: flwafact averaged over the layers
+// (glissade_vertical_average, glissade_grid_operators.F90:1882-1946, no mask), then every active
+// cell j = nhalo+1..ny-nhalo+1, i = nhalo+1..nx-nhalo+1: 4 quadrature points (basis derivatives,
+// the SSA viscosity at the averaged flow factor, h at the point, the SSA element matrix with
+// h*efvs), efvs(k,i,j) the mean over the points for every layer, and the scatter
+// element_to_global_matrix_2d (:8127-8196) with the standard indxA_2d.  Arrays: uvel/vvel,
+// xVertex, yVertex, stagusrf, stagthck (nx-1,ny-1); flwafact/efvs (nz-1,nx,ny);
+// A** (nx-1,ny-1,9).  Returns 0, 1 (singular Jacobian) or 2 (nhalo < 2).
+int oracle_assemble_stiffness_2d(int nx, int ny, int nz, int nhalo, const double *sigma, const int32_t *active_cell,
+                                 const double *xVertex, const double *yVertex, const double *uvel,
+                                 const double *vvel, const double *stagthck, const double *flwafact, int whichefvs,
+                                 double efvs_constant, double effstrain_min, double n_glen, double *efvs, double *Auu,
+                                 double *Auv, double *Avu, double *Avv) {
+    if (nhalo < 2) return 2;
+    const long NX = nx - 1, NY = ny - 1, NQ = NX * NY;
+    const RefElement2 &R = ref2();
+    std::memset(efvs, 0, sizeof(double) * (size_t)(nz - 1) * nx * ny);
+    for (double *A : {Auu, Auv, Avu, Avv}) std::memset(A, 0, sizeof(double) * 9 * (size_t)NQ);
+    std::vector<double> ff2((size_t)nx * ny, 0.0);
+    for (int j = 1; j <= ny; ++j)
+        for (int i = 1; i <= nx; ++i) {
+            double &f = ff2[(i - 1) + (size_t)nx * (j - 1)];
+            f = 0.0;
+            for (int k = 1; k <= nz - 1; ++k)
+                f = f + flwafact[(k - 1) + (size_t)(nz - 1) * ((i - 1) + (size_t)nx * (j - 1))] * (sigma[k] - sigma[k - 1]);
+        }
+    for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+        for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+            if (!active_cell[(i - 1) + (long)nx * (j - 1)]) continue;
+            double Kuu[4][4] = {}, Kuv[4][4] = {}, Kvu[4][4] = {}, Kvv[4][4] = {};
+            double x[4], y[4], u[4], v[4], h[4];
+            for (int n = 0; n < 4; ++n) {
+                const long q = (long)(i + kIsh3[n] - 1) + NX * (j + kJsh3[n] - 1);
+                x[n] = xVertex[q];
+                y[n] = yVertex[q];
+                u[n] = uvel[q];
+                v[n] = vvel[q];
+                h[n] = stagthck[q];
+            }
+            const double ffc = ff2[(i - 1) + (size_t)nx * (j - 1)];
+            double evert[4];
+            for (int p = 0; p < 4; ++p) {
+                double dx[4], dy[4], detJ;
+                if (!basis_derivs_2d(x, y, R.dxr[p], R.dyr[p], dx, dy, &detJ)) return 1;
+                evert[p] = efvs_qp4(whichefvs, efvs_constant, effstrain_min, n_glen, dx, dy, u, v, ffc);
+                double h_qp = 0.0;
+                for (int n = 0; n < 4; ++n) h_qp = h_qp + R.phi[p][n] * h[n];
+                const double f = h_qp * evert[p] * 1.0 * detJ / kVol0;
+                for (int nc = 0; nc < 4; ++nc)
+                    for (int nr = 0; nr < 4; ++nr) {
+                        Kuu[nr][nc] = Kuu[nr][nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc]);
+                        Kuv[nr][nc] = Kuv[nr][nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
+                        Kvu[nr][nc] = Kvu[nr][nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
+                        Kvv[nr][nc] = Kvv[nr][nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc]);
+                    }
+            }
+            for (int k = 1; k <= nz - 1; ++k) {
+                double &e = efvs[(k - 1) + (long)(nz - 1) * ((i - 1) + (long)nx * (j - 1))];
+                e = 0.0;
+                for (int p = 0; p < 4; ++p) e = e + evert[p];
+                e = e / 4;
+            }
+            for (int nr = 0; nr < 4; ++nr) {
+                const long q = (long)(i + kIsh3[nr] - 1) + NX * (j + kJsh3[nr] - 1);
+                for (int nc = 0; nc < 4; ++nc) {
+                    const int m = (kIsh3[nc] - kIsh3[nr] + 1) + 3 * (kJsh3[nc] - kJsh3[nr] + 1);
+                    const size_t a = (size_t)q + (size_t)NQ * m;
+                    Auu[a] = Auu[a] + Kuu[nr][nc];
+                    Auv[a] = Auv[a] + Kuv[nr][nc];
+                    Avu[a] = Avu[a] + Kvu[nr][nc];
+                    Avv[a] = Avv[a] + Kvv[nr][nc];
+                }
+            }
+        }
+    return 0;
+}
+
 
 // assemble_stiffness_matrix_3d (:5382-5643): efvs and A zeroed, then every active cell
 // j = nhalo+1..ny-nhalo+1, i = nhalo+1..nx-nhalo+1 (j outer), element k = 1..nz-1: node

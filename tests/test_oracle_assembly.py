@@ -154,3 +154,74 @@ def test_singular_and_halo_errors():
     st = oracle.assemble_stiffness_3d(nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], np.zeros(shape),
                                       np.zeros(shape), flat, flat, ff)[0]
     assert st == 1
+
+
+# ---------------------------------------------------------------------------
+# assemble_stiffness_matrix_2d (:4961-5378), SSA
+# ---------------------------------------------------------------------------
+
+def run2(g, uvel=None, vvel=None, flwa=1.0e-16, ff=None, **kw):
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    shape = (ny - 1, nx - 1)
+    u = np.zeros(shape) if uvel is None else uvel
+    v = np.zeros(shape) if vvel is None else vvel
+    if ff is None:
+        ff = np.full((ny, nx, nz - 1), 0.5 * flwa ** (-1.0 / N_GLEN))
+    st, efvs, *A = oracle.assemble_stiffness_2d(nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], u, v,
+                                                g["stagthck"], ff, **kw)
+    assert st == 0
+    return efvs, A
+
+
+def test_ssa_first_picard_matches_numpy_assembly():
+    g = geometry(seed=31)
+    efvs, A = run2(g)
+    P = asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], np.zeros((g["ny"] - 1, g["nx"] - 1)),
+                            stiffness_only=True)
+    scale = max(np.abs(P.Auu).max(), np.abs(P.Avv).max())
+    for got, want in zip(A, (P.Auu, P.Auv, P.Avu, P.Avv)):
+        assert np.abs(got - want).max() <= 1e-13 * scale
+    e0 = asm.first_picard_efvs(1.0e-16)
+    act = g["ac"]
+    assert np.all(np.abs(efvs[act] - e0) <= 1e-14 * e0) and np.all(efvs[~act] == 0.0)
+
+
+def test_ssa_scatter_is_exactly_symmetric():
+    g = geometry(seed=32)
+    rng = np.random.default_rng(4)
+    shape = (g["ny"] - 1, g["nx"] - 1)
+    efvs, A = run2(g, 50.0 * rng.standard_normal(shape), 50.0 * rng.standard_normal(shape))
+    P = asm.Problem("2d", g["nx"], g["ny"], 1, *A, np.zeros(shape), np.zeros(shape), g["av"].astype(np.int32),
+                    asm.default_par(g["nx"], g["ny"]))
+    r = oracle.check_symmetry(P)
+    assert r[4] == 0.0 and r[5] == 0 and np.abs(A[0]).max() > 0.0
+
+
+def test_ssa_linear_velocity_and_layer_averaged_flow_factor():
+    """u, v linear in x and y: constant SSA strain rates, so efvs = the flow law at those rates
+    with the layer average of flwafact (weights sigma(k+1) - sigma(k)), the same in every layer."""
+    g = geometry(seed=33, nz=6)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    a, b = (2.0e-3, -1.5e-3), (0.5e-3, 3.0e-3)
+    u = a[0] * g["xVertex"] + a[1] * g["yVertex"]
+    v = b[0] * g["xVertex"] + b[1] * g["yVertex"]
+    rng = np.random.default_rng(6)
+    layer = 0.5 * 1.0e-16 ** (-1.0 / N_GLEN) * (1.0 + 0.5 * rng.random(nz - 1))
+    ff = np.broadcast_to(layer, (ny, nx, nz - 1)).copy()
+    efvs, A = run2(g, u, v, ff=ff)
+    ff2 = float(np.sum(layer * np.diff(g["sigma"])))
+    sq = 1.0e-16 + (a[0] ** 2 + b[1] ** 2 + a[0] * b[1] + 0.25 * (b[0] + a[1]) ** 2)
+    want = ff2 * sq ** ((1.0 - N_GLEN) / N_GLEN / 2.0)
+    act = g["ac"]
+    assert np.all(np.abs(efvs[act] - want) <= 1e-12 * want)
+    assert np.all(efvs[act] == efvs[act][:, :1])  # every layer the same
+
+
+def test_ssa_constant_viscosity_null_space():
+    g = geometry(seed=34)
+    efvs, (Auu, Auv, Avu, Avv) = run2(g, whichefvs=0, efvs_constant=1.0e6)
+    ac = g["ac"]
+    full = ac[:-1, :-1] & ac[:-1, 1:] & ac[1:, :-1] & ac[1:, 1:]
+    scale = np.abs(Auu).max()
+    assert np.abs(Auu.sum(axis=0)[full]).max() <= 1e-12 * scale
+    assert np.abs(Avu.sum(axis=0)[full]).max() <= 1e-12 * scale
