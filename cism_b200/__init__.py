@@ -30,6 +30,7 @@ __all__ = [
     "ALG_STANDARD", "ALG_CHRONGEAR", "ALG_MIXED_CHRONGEAR", "compute_residual_vector_3d",
     "compute_residual_vector_2d", "compute_residual_velocity_3d", "compute_residual_velocity_2d",
     "check_symmetry_assembled_matrix_3d", "check_symmetry_assembled_matrix_2d", "assemble_stiffness_matrix_3d",
+    "assemble_stiffness_matrix_2d",
 ]
 
 ALG_STANDARD, ALG_CHRONGEAR, ALG_MIXED_CHRONGEAR = 0, 1, 2
@@ -184,12 +185,16 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                                          dbl, dbl, dbl, d, d, d, d, d, d]
     lib.cismgpu_solver_assemble_stiffness_3d.argtypes = [vp, i32, d, d, d, d, d, d, d, d, d, i32, i32, dbl, dbl,
                                                          dbl, d]
+    lib.cismgpu_assemble_stiffness_matrix_2d.argtypes = [i32, i32, i32, i32, d, d, d, d, d, d, d, d, i32, dbl, dbl,
+                                                         dbl, d, d, d, d, d, d]
+    lib.cismgpu_solver_assemble_stiffness_2d.argtypes = [vp, i32, i32, d, d, d, d, d, d, d, d, i32, dbl, dbl, dbl, d]
     for f in ("cismgpu_compute_residual_vector_3d", "cismgpu_compute_residual_vector_2d",
               "cismgpu_compute_residual_velocity_3d", "cismgpu_compute_residual_velocity_2d",
               "cismgpu_solver_set_system", "cismgpu_solver_residual_vector", "cismgpu_solver_residual_velocity",
               "cismgpu_solver_save", "cismgpu_solver_restore", "cismgpu_check_symmetry_assembled_matrix_3d",
               "cismgpu_check_symmetry_assembled_matrix_2d", "cismgpu_solver_check_symmetry",
-              "cismgpu_assemble_stiffness_matrix_3d", "cismgpu_solver_assemble_stiffness_3d"):
+              "cismgpu_assemble_stiffness_matrix_3d", "cismgpu_solver_assemble_stiffness_3d",
+              "cismgpu_assemble_stiffness_matrix_2d", "cismgpu_solver_assemble_stiffness_2d"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -462,6 +467,25 @@ def assemble_stiffness_matrix_3d(nx, ny, nz, nhalo, sigma, active_cell, xVertex,
     return (efvs, *A)
 
 
+def assemble_stiffness_matrix_2d(nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel_2d, vvel_2d,
+                                 stagthck, flwafact, whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8,
+                                 n_glen=3.0, indxA_2d=None):
+    """Mirrors assemble_stiffness_matrix_2d (glissade_velo_higher.F90:4961-5378), SSA, on the
+    GPU.  Vertex fields (ny-1, nx-1), active_cell (ny, nx), flwafact (ny, nx, nz-1).
+    Returns (efvs (ny, nx, nz-1), Auu, Auv, Avu, Avv (9, ny-1, nx-1))."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    indx = np.arange(1, 10, dtype=np.int32) if indxA_2d is None else np.ascontiguousarray(indxA_2d, dtype=np.int32)
+    efvs = np.zeros((ny, nx, nz - 1))
+    A = [np.zeros((9, ny - 1, nx - 1)) for _ in range(4)]
+    head, tail = _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagthck, stagthck, flwafact)
+    _check(lib, lib.cismgpu_assemble_stiffness_matrix_2d(
+        nx, ny, nz, int(nhalo), *head, _ptr(uvel_2d, np.float64, nv), _ptr(vvel_2d, np.float64, nv), tail[1],
+        tail[2], int(whichefvs), float(efvs_constant), float(effstrain_min), float(n_glen), _ptr(indx, np.int32, 9),
+        _ptr(efvs, np.float64, efvs.size, True), *[_ptr(a, np.float64, a.size, True) for a in A]))
+    return (efvs, *A)
+
+
 class DeviceSolver:
     """A device-resident linear system (cismgpu_solver_create): A, b and x0 live in HBM.
 
@@ -542,18 +566,29 @@ class DeviceSolver:
     def assemble_stiffness(self, nhalo, sigma, active_cell, xVertex, yVertex, stagusrf, stagthck, flwafact,
                            uvel=None, vvel=None, whichapprox=2, whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8,
                            n_glen=3.0):
-        """assemble_stiffness_matrix_3d into the resident blocks (3D handles); uvel = vvel =
-        None uses the handle's current velocity.  Returns efvs (ny, nx, nz-1)."""
+        """assemble_stiffness_matrix_3d (3D handles) or _2d (SSA, 2D handles; stagusrf unused)
+        into the resident blocks; uvel = vvel = None uses the handle's current velocity.
+        Returns efvs (ny, nx, nz-1)."""
         P = self.problem
-        nx, ny, nz = P.nx, P.ny, P.nz
+        is3d = P.kind == "3d"
+        nx, ny = P.nx, P.ny
+        nz = P.nz if is3d else len(sigma)  # 2D: the sigma levels of flwafact
         nv = (nx - 1) * (ny - 1)
+        nvel = nv * (nz if is3d else 1)
         efvs = np.zeros((ny, nx, nz - 1))
         head, tail = _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagusrf, stagthck, flwafact)
-        pu = None if uvel is None else _ptr(uvel, np.float64, nv * nz)
-        pv = None if vvel is None else _ptr(vvel, np.float64, nv * nz)
-        _check(self._lib, self._lib.cismgpu_solver_assemble_stiffness_3d(
-            self.handle, int(nhalo), *head, pu, pv, *tail, int(whichapprox), int(whichefvs), float(efvs_constant),
-            float(effstrain_min), float(n_glen), _ptr(efvs, np.float64, efvs.size, True)))
+        pu = None if uvel is None else _ptr(uvel, np.float64, nvel)
+        pv = None if vvel is None else _ptr(vvel, np.float64, nvel)
+        pe = _ptr(efvs, np.float64, efvs.size, True)
+        if is3d:
+            st = self._lib.cismgpu_solver_assemble_stiffness_3d(
+                self.handle, int(nhalo), *head, pu, pv, *tail, int(whichapprox), int(whichefvs), float(efvs_constant),
+                float(effstrain_min), float(n_glen), pe)
+        else:
+            st = self._lib.cismgpu_solver_assemble_stiffness_2d(
+                self.handle, nz, int(nhalo), *head, pu, pv, tail[1], tail[2], int(whichefvs), float(efvs_constant),
+                float(effstrain_min), float(n_glen), pe)
+        _check(self._lib, st)
         return efvs
 
     def save(self):

@@ -208,4 +208,142 @@ __global__ void __launch_bounds__(kAsmBlock) k_assemble3d(AsmArgs a, SymIdx L, d
         for (int c = 0; c < 27; ++c) B[b][L.at(c, k0, q)] = acc[b][c];
 }
 
+// ---------------------------------------------------------------------------
+// assemble_stiffness_matrix_2d (glissade_velo_higher.F90:4961-5378), SSA branch: 4-node
+// quadrilaterals, 4 Gauss points (:528-570), get_basis_function_derivatives_2d (:6319-6504),
+// the SSA viscosity at the layer-averaged flow factor, h at the point, and
+// element_to_global_matrix_2d (:8127-8196).  One thread per vertex, gathering the (up to) 4
+// cells around it in the reference's cell order (j, then i).
+// ---------------------------------------------------------------------------
+struct AsmRef2 {
+    double phi[4][4], dxr[4][4], dyr[4][4];  // [p][n]
+};
+__constant__ AsmRef2 c_asm_ref2;
+__constant__ int c_ish3[4] = {-1, 0, 0, -1};  // ishift(3,n), jshift(3,n), n = 1..4
+__constant__ int c_jsh3[4] = {-1, -1, 0, 0};
+
+// glissade_vertical_average (glissade_grid_operators.F90:1882-1946, no mask) of flwafact
+// (nz-1, nx, ny) into ff2 (nx, ny): sum over k of flwafact(k) * (sigma(k+1) - sigma(k)).
+__global__ void __launch_bounds__(kBlock) k_asm_vertavg(int ncell, int nz, const double *__restrict__ sigma,
+                                                       const double *__restrict__ ff, double *__restrict__ ff2) {
+    const int c = blockIdx.x * kBlock + threadIdx.x;
+    if (c >= ncell) return;
+    double f = 0.0;
+    for (int k = 0; k < nz - 1; ++k) f = f + ff[k + (long long)(nz - 1) * c] * (sigma[k + 1] - sigma[k]);
+    ff2[c] = f;
+}
+
+// Row nr of cell (ie, je)'s element matrix into acc[b][m]; the cell's own thread writes its
+// efvs for every layer (the mean over the 4 points, :5348-5354).
+__device__ bool asm_cell_row(const AsmArgs &a, const double *ff2, int ie, int je, int nr, bool own,
+                             double acc[4][9]) {
+    const long long NX = a.nx - 1;
+    double x[4], y[4], u[4], v[4], h[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        const long long q = (long long)(ie + c_ish3[n] - 1) + NX * (je + c_jsh3[n] - 1);
+        x[n] = a.xv[q];
+        y[n] = a.yv[q];
+        u[n] = a.u[q];
+        v[n] = a.v[q];
+        h[n] = a.thck[q];
+    }
+    const double ffc = ff2[(ie - 1) + (long long)a.nx * (je - 1)];
+    double Kuu[4], Kuv[4], Kvu[4], Kvv[4];
+#pragma unroll
+    for (int nc = 0; nc < 4; ++nc) Kuu[nc] = Kuv[nc] = Kvu[nc] = Kvv[nc] = 0.0;
+    double esum = 0.0;
+    for (int p = 0; p < 4; ++p) {
+        const double *dxr = c_asm_ref2.dxr[p], *dyr = c_asm_ref2.dyr[p];
+        double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            J00 = J00 + dxr[n] * x[n];
+            J01 = J01 + dxr[n] * y[n];
+            J10 = J10 + dyr[n] * x[n];
+            J11 = J11 + dyr[n] * y[n];
+        }
+        const double detJ = J00 * J11 - J01 * J10;
+        if (!(fabs(detJ) > 0.0)) return false;
+        const double i00 = J11 / detJ, i01 = -J01 / detJ, i10 = -J10 / detJ, i11 = J00 / detJ;
+        double dx[4], dy[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            dx[n] = 0.0 + i00 * dxr[n] + i01 * dyr[n];
+            dy[n] = 0.0 + i10 * dxr[n] + i11 * dyr[n];
+        }
+        double efvs;
+        if (a.whichefvs == 0) {
+            efvs = a.efvs_constant;
+        } else if (a.whichefvs == 1) {
+            efvs = ffc * a.flowfact_pow;
+        } else {
+            double du_dx = 0.0, du_dy = 0.0, dv_dx = 0.0, dv_dy = 0.0;
+#pragma unroll
+            for (int n = 0; n < 4; ++n) {
+                du_dx = du_dx + dx[n] * u[n];
+                du_dy = du_dy + dy[n] * u[n];
+                dv_dx = dv_dx + dx[n] * v[n];
+                dv_dy = dv_dy + dy[n] * v[n];
+            }
+            const double sh = dv_dx + du_dy;
+            const double sq = a.effstrain_min * a.effstrain_min +
+                              (du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * (sh * sh));
+            efvs = ffc * pow(sq, a.p_half);
+        }
+        esum = esum + efvs;
+        double h_qp = 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) h_qp = h_qp + c_asm_ref2.phi[p][n] * h[n];
+        const double f = h_qp * efvs * 1.0 * detJ / kAsmVol0;
+#pragma unroll
+        for (int nc = 0; nc < 4; ++nc) {
+            Kuu[nc] = Kuu[nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc]);
+            Kuv[nc] = Kuv[nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
+            Kvu[nc] = Kvu[nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
+            Kvv[nc] = Kvv[nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc]);
+        }
+    }
+    if (own) {
+        const double e = esum / 4;
+        for (int k = 0; k < a.nz - 1; ++k) a.efvs[k + (long long)(a.nz - 1) * ((ie - 1) + (long long)a.nx * (je - 1))] = e;
+    }
+#pragma unroll
+    for (int nc = 0; nc < 4; ++nc) {
+        const int m = (c_ish3[nc] - c_ish3[nr] + 1) + 3 * (c_jsh3[nc] - c_jsh3[nr] + 1);
+        acc[0][m] = acc[0][m] + Kuu[nc];
+        acc[1][m] = acc[1][m] + Kuv[nc];
+        acc[2][m] = acc[2][m] + Kvu[nc];
+        acc[3][m] = acc[3][m] + Kvv[nc];
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(kAsmBlock) k_assemble2d(AsmArgs a, const double *__restrict__ ff2, SymIdx L,
+                                                          double *Auu, double *Auv, double *Avu, double *Avv) {
+    const long long NX = a.nx - 1, NQ = NX * (a.ny - 1);
+    const long long q = (long long)blockIdx.x * kAsmBlock + threadIdx.x;
+    if (q >= NQ) return;
+    const int j0 = (int)(q / NX), i0 = (int)(q - (long long)j0 * NX);
+    const int iR = i0 + 1, jR = j0 + 1;
+    double acc[4][9];
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) acc[b][c] = 0.0;
+    for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+            const int je = jR + dj, ie = iR + di;
+            if (ie < a.nhalo + 1 || ie > a.nx - a.nhalo + 1 || je < a.nhalo + 1 || je > a.ny - a.nhalo + 1) continue;
+            if (!a.active_cell[(ie - 1) + (long long)a.nx * (je - 1)]) continue;
+            // node index within the cell: shifts (iR-ie, jR-je) = (-di, -dj)
+            const int nr = dj == 0 ? (di == 0 ? 2 : 3) : (di == 0 ? 1 : 0);
+            if (!asm_cell_row(a, ff2, ie, je, nr, dj == 0 && di == 0, acc)) atomicExch(a.singular, 1);
+        }
+    double *B[4] = {Auu, Auv, Avu, Avv};
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+        for (int c = 0; c < 9; ++c) B[b][L.at(c, 0, q)] = acc[b][c];
+}
+
 }  // namespace cismgpu

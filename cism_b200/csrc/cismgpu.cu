@@ -316,18 +316,20 @@ struct Solver {
         return CISMGPU_OK;
     }
 
-    // assemble_stiffness_matrix_3d (glissade_velo_higher.F90:5382-5643) on the device into four
-    // blocks in layout L.  The host arrays are uploaded; u, v null: the velocity planes vel_id,
-    // vel_id+1 (level-major) instead.  efvs (host, may be null) receives the element viscosity.
-    // Leaves the stream synchronized.
-    int assemble3d(const SymIdx &L, double *Auu, double *Auv, double *Avu, double *Avv, int nhalo,
-                   const double *sigma, const int32_t *active_cell, const double *xv, const double *yv,
-                   const double *u, const double *v, int vel_id, const double *usrf, const double *thck,
-                   const double *flwafact, int whichapprox, int whichefvs, double efvs_constant,
-                   double effstrain_min, double n_glen, double *efvs) {
-        static bool ref_ready = false;  // the reference element in constant memory (:314-392)
+    // assemble_stiffness_matrix_3d (glissade_velo_higher.F90:5382-5643) or, with three_d false,
+    // the SSA branch of assemble_stiffness_matrix_2d (:4961-5378) on the device into four blocks
+    // in layout L.  nzl: the number of sigma levels (the layers of flwafact and efvs).  The host
+    // arrays are uploaded; u, v null: the velocity planes vel_id, vel_id+1 instead.  efvs (host,
+    // may be null) receives the element viscosity.  Leaves the stream synchronized.
+    int assemble(bool three_d, int nzl, const SymIdx &L, double *Auu, double *Auv, double *Avu, double *Avv,
+                 int nhalo, const double *sigma, const int32_t *active_cell, const double *xv, const double *yv,
+                 const double *u, const double *v, int vel_id, const double *usrf, const double *thck,
+                 const double *flwafact, int whichapprox, int whichefvs, double efvs_constant,
+                 double effstrain_min, double n_glen, double *efvs) {
+        static bool ref_ready = false;  // the reference elements in constant memory (:314-392, :528-570)
         if (!ref_ready) {
             AsmRef r;
+            AsmRef2 r2;
             const double rs = 1.0 / std::sqrt(3.0);
             const double xq[8] = {-rs, rs, rs, -rs, -rs, rs, rs, -rs};
             const double yq[8] = {-rs, -rs, rs, rs, -rs, -rs, rs, rs};
@@ -345,39 +347,51 @@ struct Solver {
                     r.dzr[p][n] = sz[n] * fx * fy / 8.0;
                 }
             }
+            for (int p = 0; p < 4; ++p)  // the square: points and nodes are the cube's first four
+                for (int n = 0; n < 4; ++n) {
+                    const double fx = sx[n] < 0 ? 1.0 - xq[p] : 1.0 + xq[p];
+                    const double fy = sy[n] < 0 ? 1.0 - yq[p] : 1.0 + yq[p];
+                    r2.phi[p][n] = fx * fy / 4.0;
+                    r2.dxr[p][n] = sx[n] * fy / 4.0;
+                    r2.dyr[p][n] = sy[n] * fx / 4.0;
+                }
             CU(cudaMemcpyToSymbol(c_asm_ref, &r, sizeof(r)));
+            CU(cudaMemcpyToSymbol(c_asm_ref2, &r2, sizeof(r2)));
             ref_ready = true;
         }
-        const int nx = g.NX + 1, ny = g.NY + 1, nz = g.nz;
-        const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny, nel = (size_t)(nz - 1) * ncell;
+        const int nx = g.NX + 1, ny = g.NY + 1;
+        const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny, nel = (size_t)(nzl - 1) * ncell;
+        const size_t nvel = three_d ? (size_t)nzl * nq : nq;
         const bool host_vel = u != nullptr;
-        // doubles: sigma, 4 vertex fields, flwafact, efvs, [u, v]; then active_cell and the flag
-        const size_t nd = (size_t)nz + 4 * nq + 2 * nel + (host_vel ? 2 * (size_t)nz * nq : 0);
+        // doubles: sigma, 4 vertex fields, flwafact, efvs, the 2D averaged flow factor, [u, v];
+        // then active_cell and the flag
+        const size_t nd = (size_t)nzl + 4 * nq + 2 * nel + ncell + (host_vel ? 2 * nvel : 0);
         CU(asm_in.ensure(nd * sizeof(double) + ncell * sizeof(int32_t) + 16));
         double *D = asm_in.as<double>();
-        double *d_sigma = D, *d_xv = D + nz, *d_yv = d_xv + nq, *d_usrf = d_yv + nq, *d_thck = d_usrf + nq;
-        double *d_ff = d_thck + nq, *d_efvs = d_ff + nel, *d_u = d_efvs + nel, *d_v = d_u + (size_t)nz * nq;
+        double *d_sigma = D, *d_xv = D + nzl, *d_yv = d_xv + nq, *d_usrf = d_yv + nq, *d_thck = d_usrf + nq;
+        double *d_ff = d_thck + nq, *d_efvs = d_ff + nel, *d_ff2 = d_efvs + nel, *d_u = d_ff2 + ncell,
+               *d_v = d_u + nvel;
         int32_t *d_act = reinterpret_cast<int32_t *>(D + nd);
         int *d_sing = reinterpret_cast<int *>(d_act + ncell);
         cudaStream_t s = stream;
         auto up = [&](void *dst, const void *src, size_t bytes) {
             return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
         };
-        CU(up(d_sigma, sigma, nz * sizeof(double)));
+        CU(up(d_sigma, sigma, nzl * sizeof(double)));
         CU(up(d_xv, xv, nq * sizeof(double)));
         CU(up(d_yv, yv, nq * sizeof(double)));
-        CU(up(d_usrf, usrf, nq * sizeof(double)));
+        if (three_d) CU(up(d_usrf, usrf, nq * sizeof(double)));
         CU(up(d_thck, thck, nq * sizeof(double)));
         CU(up(d_ff, flwafact, nel * sizeof(double)));
         CU(up(d_act, active_cell, ncell * sizeof(int32_t)));
         if (host_vel) {
-            CU(up(d_u, u, (size_t)nz * nq * sizeof(double)));
-            CU(up(d_v, v, (size_t)nz * nq * sizeof(double)));
+            CU(up(d_u, u, nvel * sizeof(double)));
+            CU(up(d_v, v, nvel * sizeof(double)));
         }
         CU(cudaMemsetAsync(d_efvs, 0, nel * sizeof(double), s));
         CU(cudaMemsetAsync(d_sing, 0, sizeof(int), s));
         AsmArgs a;
-        a.nx = nx; a.ny = ny; a.nz = nz; a.nhalo = nhalo;
+        a.nx = nx; a.ny = ny; a.nz = nzl; a.nhalo = nhalo;
         a.whichapprox = whichapprox; a.whichefvs = whichefvs;
         a.efvs_constant = efvs_constant; a.effstrain_min = effstrain_min;
         a.p_half = (1.0 - n_glen) / n_glen / 2.0;
@@ -389,8 +403,15 @@ struct Solver {
         a.v = host_vel ? d_v : V + (size_t)(vel_id + 1) * nvec;
         a.vel_planes = host_vel ? 0 : 1;
         a.flwafact = d_ff; a.efvs = d_efvs; a.singular = d_sing;
-        const long long n = (long long)nz * g.NQ;
-        k_assemble3d<<<(unsigned)((n + kAsmBlock - 1) / kAsmBlock), kAsmBlock, 0, s>>>(a, L, Auu, Auv, Avu, Avv);
+        if (three_d) {
+            const long long n = (long long)nzl * g.NQ;
+            k_assemble3d<<<(unsigned)((n + kAsmBlock - 1) / kAsmBlock), kAsmBlock, 0, s>>>(a, L, Auu, Auv, Avu, Avv);
+        } else {
+            k_asm_vertavg<<<(unsigned)((ncell + kBlock - 1) / kBlock), kBlock, 0, s>>>((int)ncell, nzl, d_sigma, d_ff,
+                                                                                       d_ff2);
+            k_assemble2d<<<(unsigned)((g.NQ + kAsmBlock - 1) / kAsmBlock), kAsmBlock, 0, s>>>(a, d_ff2, L, Auu, Auv,
+                                                                                               Avu, Avv);
+        }
         CU(cudaGetLastError());
         int sing = 0;
         CU(cudaMemcpyAsync(&sing, d_sing, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1333,40 +1354,42 @@ static int validate_assembly(int nx, int ny, int nz, int nhalo, int whichefvs, d
     return CISMGPU_OK;
 }
 
-// assemble_stiffness_matrix_3d on the caller's host arrays: inputs uploaded, the blocks written
-// on the device in the caller's layout (through its indxA_3d) and copied back.
-static int oneshot_assemble3d(int nx, int ny, int nz, int nhalo, const double *sigma, const int32_t *active_cell,
-                              const double *xv, const double *yv, const double *u, const double *v,
-                              const double *usrf, const double *thck, const double *ff, int whichapprox,
-                              int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
-                              const int32_t *indx, double *efvs, double *const blocks[4]) {
+// assemble_stiffness_matrix_3d / _2d (SSA) on the caller's host arrays: inputs uploaded, the
+// blocks written on the device in the caller's layout (through its indxA map) and copied back.
+static int oneshot_assemble(bool three_d, int nx, int ny, int nz, int nhalo, const double *sigma,
+                            const int32_t *active_cell, const double *xv, const double *yv, const double *u,
+                            const double *v, const double *usrf, const double *thck, const double *ff,
+                            int whichapprox, int whichefvs, double efvs_constant, double effstrain_min,
+                            double n_glen, const int32_t *indx, double *efvs, double *const blocks[4]) {
     std::lock_guard<std::mutex> lk(g_mu);
     g_last_error.clear();
-    TRY(validate_assembly(nx, ny, nz, nhalo, whichefvs, n_glen, sigma, active_cell, xv, yv, usrf, thck, ff));
+    TRY(validate_assembly(nx, ny, nz, nhalo, whichefvs, n_glen, sigma, active_cell, xv, yv, three_d ? usrf : thck,
+                          thck, ff));
     if (!u || !v || !indx || !blocks[0] || !blocks[1] || !blocks[2] || !blocks[3])
         return fail(CISMGPU_EINVAL, "null pointer argument");
-    TRY(validate_indx(indx, 27));
+    const int NC = three_d ? 27 : 9;
+    TRY(validate_indx(indx, NC));
     cismgpu_par_t par{};
     par.staggered_ilo = 1; par.staggered_ihi = nx - 1; par.staggered_jlo = 1; par.staggered_jhi = ny - 1;
     par.tasks_row = par.tasks_col = 1;
     if (!g_oneshot) g_oneshot = new Solver();
     Solver &sv = *g_oneshot;
     TRY(sv.init(nullptr));
-    TRY(sv.set_geom(make_geom(nx, ny, nz, &par), true));
-    const size_t bs = (size_t)27 * sv.nvec;
+    TRY(sv.set_geom(make_geom(nx, ny, three_d ? nz : 1, &par), three_d));
+    const size_t bs = (size_t)NC * sv.nvec;
     CU(sv.A.ensure(4 * bs * sizeof(double)));
     sv.mixed.stale = true;  // the matrix buffer holds the caller's layout until the next upload
     double *A0 = sv.A.as<double>();
     SymIdx L{};
-    for (int c = 0; c < 27; ++c) L.map[c] = indx[c];
+    for (int c = 0; c < 27; ++c) L.map[c] = c < NC ? indx[c] : 1;
     L.n = sv.nvec;
     L.NQ = sv.g.NQ;
-    L.nz = nz;
-    L.raw3 = 1;
-    TRY(sv.assemble3d(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, nhalo, sigma, active_cell, xv, yv, u, v, 0, usrf,
-                      thck, ff, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen, efvs));
-    for (int b = 0; b < 4; ++b)
-        CU(cudaMemcpyAsync(blocks[b], A0 + b * bs, bs * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
+    L.nz = sv.g.nz;
+    L.raw3 = three_d ? 1 : 0;
+    TRY(sv.assemble(three_d, nz, L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, nhalo, sigma, active_cell, xv, yv, u, v,
+                    0, usrf, thck, ff, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen, efvs));
+    for (int k = 0; k < 4; ++k)
+        CU(cudaMemcpyAsync(blocks[k], A0 + k * bs, bs * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
     CU(cudaStreamSynchronize(sv.stream));
     return CISMGPU_OK;
 }
@@ -1896,9 +1919,51 @@ int cismgpu_assemble_stiffness_matrix_3d(int nx, int ny, int nz, int nhalo, cons
                                          const int32_t *indxA_3d, double *efvs, double *Auu, double *Auv,
                                          double *Avu, double *Avv) {
     double *const blocks[4] = {Auu, Auv, Avu, Avv};
-    return oneshot_assemble3d(nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel, vvel, stagusrf,
-                              stagthck, flwafact, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen,
-                              indxA_3d, efvs, blocks);
+    return oneshot_assemble(true, nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel, vvel, stagusrf,
+                            stagthck, flwafact, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen, indxA_3d,
+                            efvs, blocks);
+}
+
+int cismgpu_assemble_stiffness_matrix_2d(int nx, int ny, int nz, int nhalo, const double *sigma,
+                                         const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                         const double *uvel_2d, const double *vvel_2d, const double *stagthck,
+                                         const double *flwafact, int whichefvs, double efvs_constant,
+                                         double effstrain_min, double n_glen, const int32_t *indxA_2d, double *efvs,
+                                         double *Auu, double *Auv, double *Avu, double *Avv) {
+    double *const blocks[4] = {Auu, Auv, Avu, Avv};
+    return oneshot_assemble(false, nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel_2d, vvel_2d, nullptr,
+                            stagthck, flwafact, 1, whichefvs, efvs_constant, effstrain_min, n_glen, indxA_2d, efvs,
+                            blocks);
+}
+
+// The handle's assembly: blocks into the resident canonical planes.
+static int solver_assemble(cismgpu_solver_t *h, bool three_d, int nzl, int nhalo, const double *sigma,
+                           const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                           const double *uvel, const double *vvel, const double *stagusrf, const double *stagthck,
+                           const double *flwafact, int whichapprox, int whichefvs, double efvs_constant,
+                           double effstrain_min, double n_glen, double *efvs) {
+    g_last_error.clear();
+    if (!h) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
+    Solver &sv = h->sv;
+    if (sv.is3d != three_d) return fail(CISMGPU_EINVAL, "the handle's dimension differs from the assembly's");
+    if ((!uvel) != (!vvel)) return fail(CISMGPU_EINVAL, "give both velocity components or neither");
+    TRY(validate_assembly(sv.g.NX + 1, sv.g.NY + 1, nzl, nhalo, whichefvs, n_glen, sigma, active_cell, xVertex,
+                          yVertex, three_d ? stagusrf : stagthck, stagthck, flwafact));
+    if (three_d && nzl != sv.g.nz) return fail(CISMGPU_EINVAL, "nz differs from the handle's");
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = c + 1;
+    L.n = sv.nvec;
+    L.NQ = sv.g.NQ;
+    L.nz = sv.g.nz;
+    L.raw3 = 0;
+    const size_t bs = (size_t)sv.NC * sv.nvec;
+    double *A0 = sv.A.as<double>();
+    sv.mixed.stale = true;  // the FP32 copies follow the new matrix
+    return sv.assemble(three_d, nzl, L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, nhalo, sigma, active_cell, xVertex,
+                       yVertex, uvel, vvel, sv.x_current ? VX_U : VX0_U, stagusrf, stagthck, flwafact, whichapprox,
+                       whichefvs, efvs_constant, effstrain_min, n_glen, efvs);
 }
 
 int cismgpu_solver_assemble_stiffness_3d(cismgpu_solver_t *h, int nhalo, const double *sigma,
@@ -1907,27 +1972,18 @@ int cismgpu_solver_assemble_stiffness_3d(cismgpu_solver_t *h, int nhalo, const d
                                          const double *stagthck, const double *flwafact, int whichapprox,
                                          int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
                                          double *efvs) {
-    g_last_error.clear();
-    if (!h) return fail(CISMGPU_EINVAL, "null argument");
-    std::lock_guard<std::mutex> lk(h->mu);
-    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
-    Solver &sv = h->sv;
-    if (!sv.is3d) return fail(CISMGPU_EINVAL, "the handle holds a 2D system");
-    if ((!uvel) != (!vvel)) return fail(CISMGPU_EINVAL, "give both velocity components or neither");
-    TRY(validate_assembly(sv.g.NX + 1, sv.g.NY + 1, sv.g.nz, nhalo, whichefvs, n_glen, sigma, active_cell, xVertex,
-                          yVertex, stagusrf, stagthck, flwafact));
-    SymIdx L{};
-    for (int c = 0; c < 27; ++c) L.map[c] = c + 1;
-    L.n = sv.nvec;
-    L.NQ = sv.g.NQ;
-    L.nz = sv.g.nz;
-    L.raw3 = 0;
-    const size_t bs = (size_t)27 * sv.nvec;
-    double *A0 = sv.A.as<double>();
-    sv.mixed.stale = true;  // the FP32 copies follow the new matrix
-    return sv.assemble3d(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, nhalo, sigma, active_cell, xVertex, yVertex, uvel,
-                         vvel, sv.x_current ? VX_U : VX0_U, stagusrf, stagthck, flwafact, whichapprox, whichefvs,
-                         efvs_constant, effstrain_min, n_glen, efvs);
+    const int nz = h ? h->sv.g.nz : 0;
+    return solver_assemble(h, true, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel, vvel, stagusrf, stagthck,
+                           flwafact, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen, efvs);
+}
+
+int cismgpu_solver_assemble_stiffness_2d(cismgpu_solver_t *h, int nz, int nhalo, const double *sigma,
+                                         const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                         const double *uvel_2d, const double *vvel_2d, const double *stagthck,
+                                         const double *flwafact, int whichefvs, double efvs_constant,
+                                         double effstrain_min, double n_glen, double *efvs) {
+    return solver_assemble(h, false, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel_2d, vvel_2d, nullptr,
+                           stagthck, flwafact, 1, whichefvs, efvs_constant, effstrain_min, n_glen, efvs);
 }
 
 int cismgpu_solver_check_symmetry(cismgpu_solver_t *h, double *maxdiff, long long *nwarn) {

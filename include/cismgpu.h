@@ -264,6 +264,20 @@ int cismgpu_assemble_stiffness_matrix_3d(int nx, int ny, int nz, int nhalo, cons
                                          const int32_t *indxA_3d, double *efvs, double *Auu, double *Auv,
                                          double *Avu, double *Avv);
 
+/* Replaces assemble_stiffness_matrix_2d (glissade_velo_higher.F90:4961-5378) for the SSA
+ * (whichapprox = HO_APPROX_SSA; the L1L2 and DIVA branches are not built): 4-node cells with
+ * 4-point Gauss quadrature, the viscosity of whichefvs at the flow factor averaged over the nz-1
+ * layers (glissade_vertical_average), weighted by the thickness at each point.  uvel_2d,
+ * vvel_2d, xVertex, yVertex, stagthck (nx-1,ny-1); sigma(nz); flwafact and efvs (nz-1,nx,ny),
+ * efvs holding the cell's mean viscosity in every layer; A** (nx-1,ny-1,9) through indxA_2d.
+ * Same arithmetic, order and error behaviour as the 3D call above. */
+int cismgpu_assemble_stiffness_matrix_2d(int nx, int ny, int nz, int nhalo, const double *sigma,
+                                         const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                         const double *uvel_2d, const double *vvel_2d, const double *stagthck,
+                                         const double *flwafact, int whichefvs, double efvs_constant,
+                                         double effstrain_min, double n_glen, const int32_t *indxA_2d, double *efvs,
+                                         double *Auu, double *Auv, double *Avu, double *Avv);
+
 /* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps
@@ -410,6 +424,12 @@ int cismgpu_solver_assemble_stiffness_3d(cismgpu_solver_t *s, int nhalo, const d
                                          const double *stagthck, const double *flwafact, int whichapprox,
                                          int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
                                          double *efvs);
+/* The 2D (SSA) assembly into a 2D handle; nz: the number of sigma levels of flwafact. */
+int cismgpu_solver_assemble_stiffness_2d(cismgpu_solver_t *s, int nz, int nhalo, const double *sigma,
+                                         const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                         const double *uvel_2d, const double *vvel_2d, const double *stagthck,
+                                         const double *flwafact, int whichefvs, double efvs_constant,
+                                         double effstrain_min, double n_glen, double *efvs);
 
 /* Per-kernel CUDA-event timing of the structured matvec launches (off by default).
  * read: total device milliseconds, launch count, and algorithmic bytes per launch

@@ -135,3 +135,79 @@ def test_assembly_errors(gpu_lib):
     flat[11] = np.zeros_like(g["stagthck"])
     with pytest.raises(cg.CismGpuError):
         cg.assemble_stiffness_matrix_3d(*flat)
+
+
+# ---------------------------------------------------------------------------
+# assemble_stiffness_matrix_2d, SSA (:4961-5378)
+# ---------------------------------------------------------------------------
+
+def both2(g, u, v, ff, **kw):
+    args = (g["nx"], g["ny"], g["nz"])
+    geo = (g["sigma"], g["ac"].astype(np.int32), g["xVertex"], g["yVertex"])
+    o = oracle.assemble_stiffness_2d(*args, *geo, u, v, g["stagthck"], ff, **kw)
+    assert o[0] == 0
+    d = cg.assemble_stiffness_matrix_2d(*args, 2, *geo, u, v, g["stagthck"], ff, **kw)
+    return o[1:], d
+
+
+def inputs2(g, seed=4, scale=40.0):
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(seed)
+    u, v = scale * rng.standard_normal((ny - 1, nx - 1)), scale * rng.standard_normal((ny - 1, nx - 1))
+    ff = 0.5 * 1.0e-16 ** (-1.0 / 3.0) * (1.0 + 0.2 * rng.random((ny, nx, nz - 1)))
+    return u, v, ff
+
+
+@pytest.mark.parametrize("efvs_opt", [0, 1])
+def test_ssa_assembly_bitexact_without_pow(gpu_lib, efvs_opt):
+    g = geometry(seed=41, nz=6)
+    u, v, ff = inputs2(g)
+    o, d = both2(g, u, v, ff, whichefvs=efvs_opt, efvs_constant=2.0e6)
+    for a, b in zip(o, d):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_ssa_assembly_nonlinear_viscosity(gpu_lib):
+    g = geometry(seed=42, nz=6)
+    u, v, ff = inputs2(g)
+    o, d = both2(g, u, v, ff)
+    act = g["ac"]
+    assert (np.abs(d[0][act] - o[0][act]) / o[0][act]).max() <= 1e-14 and np.all(d[0][~act] == 0.0)
+    for a, b in zip(o[1:], d[1:]):
+        assert np.abs(a - b).max() <= 1e-13 * np.abs(a).max()
+    shape = (g["ny"] - 1, g["nx"] - 1)
+    P = asm.Problem("2d", g["nx"], g["ny"], 1, *d[1:], np.zeros(shape), np.zeros(shape), g["av"].astype(np.int32),
+                    asm.default_par(g["nx"], g["ny"]))
+    r = oracle.check_symmetry(P)
+    assert r[4] == 0.0 and r[5] == 0
+
+
+def test_ssa_assembly_on_handle(gpu_lib):
+    """A 2D handle: assembly from the host velocity and from the last solution equals the
+    one-shot assembly (efvs bit for bit; the blocks through the residual)."""
+    g = geometry(seed=43, nz=6)
+    u, v, ff = inputs2(g, scale=10.0)
+    P = asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], asm.lognormal_beta((g["ny"] - 1, g["nx"] - 1), 8))
+    geo = (2, g["sigma"], g["ac"].astype(np.int32), g["xVertex"], g["yVertex"], g["stagthck"], g["stagthck"], ff)
+    s = cg.DeviceSolver(P, x0=(u, v))
+    try:
+        s.solve(cg.ALG_CHRONGEAR, cg.HO_PRECOND_DIAG, 5, 1e-6, 50)
+        xs = s.x()
+        efvs_x = s.assemble_stiffness(*geo)
+        efvs_h = s.assemble_stiffness(*geo, uvel=u, vvel=v)
+        ru, rv, l2, _ = s.residual_vector()
+    finally:
+        s.close()
+    args = (g["nx"], g["ny"], g["nz"], 2, g["sigma"], g["ac"].astype(np.int32), g["xVertex"], g["yVertex"])
+    d = cg.assemble_stiffness_matrix_2d(*args, u, v, g["stagthck"], ff)
+    np.testing.assert_array_equal(efvs_h, d[0])
+    Q = asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], asm.lognormal_beta((g["ny"] - 1, g["nx"] - 1), 8))
+    for n, a in zip(BLOCKS, d[1:]):
+        setattr(Q, n, a)
+    want = cg.compute_residual_vector_2d(Q.nx, Q.ny, Q.par, asm.indxA_2d(), Q.active_vertex, Q.Auu, Q.Auv, Q.Avu,
+                                         Q.Avv, Q.bu, Q.bv, xs[0], xs[1])
+    np.testing.assert_array_equal(ru, want[0])
+    np.testing.assert_array_equal(rv, want[1])
+    assert l2 == want[2]
+    dx = cg.assemble_stiffness_matrix_2d(*args, xs[0], xs[1], g["stagthck"], ff)
+    np.testing.assert_array_equal(efvs_x, dx[0])
