@@ -15,6 +15,7 @@
 !     compute_residual_velocity_2d (:10188-10310)  compute_residual_velocity_3d (:10314-10446)
 !     check_symmetry_assembled_matrix_2d (:10648-10850)
 !     check_symmetry_assembled_matrix_3d (:10854-11117)
+!     assemble_stiffness_matrix_3d (:5382-5643), assemble_stiffness_matrix_2d (:4961-5378, SSA)
 !   A nonzero library status is reported the way the reference reports a failed
 !   solve: write_log(message, GM_FATAL).
 !
@@ -43,6 +44,7 @@
               compute_residual_vector_2d, compute_residual_vector_3d, &
               compute_residual_velocity_2d, compute_residual_velocity_3d, &
               check_symmetry_assembled_matrix_2d, check_symmetry_assembled_matrix_3d, &
+              assemble_stiffness_matrix_2d, assemble_stiffness_matrix_3d, &
               cismgpu_use_mixed_precision
 
     type, bind(C) :: cismgpu_par_t
@@ -187,6 +189,30 @@
          real(c_double), intent(out) :: maxdiff
          integer(c_long_long), intent(out) :: nwarn
        end function c_check_symmetry_2d
+
+       integer(c_int) function c_assemble_3d(nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel, vvel, &
+            stagusrf, stagthck, flwafact, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen, indxA_3d, &
+            efvs, Auu, Auv, Avu, Avv) bind(C, name="cismgpu_assemble_stiffness_matrix_3d")
+         import :: c_int, c_double, c_int32_t
+         integer(c_int), value :: nx, ny, nz, nhalo, whichapprox, whichefvs
+         real(c_double), intent(in) :: sigma(*), xVertex(*), yVertex(*), uvel(*), vvel(*), stagusrf(*), &
+              stagthck(*), flwafact(*)
+         integer(c_int32_t), intent(in) :: active_cell(*), indxA_3d(*)
+         real(c_double), value :: efvs_constant, effstrain_min, n_glen
+         real(c_double), intent(out) :: efvs(*), Auu(*), Auv(*), Avu(*), Avv(*)
+       end function c_assemble_3d
+
+       integer(c_int) function c_assemble_2d(nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel_2d, &
+            vvel_2d, stagthck, flwafact, whichefvs, efvs_constant, effstrain_min, n_glen, indxA_2d, efvs, Auu, Auv, &
+            Avu, Avv) bind(C, name="cismgpu_assemble_stiffness_matrix_2d")
+         import :: c_int, c_double, c_int32_t
+         integer(c_int), value :: nx, ny, nz, nhalo, whichefvs
+         real(c_double), intent(in) :: sigma(*), xVertex(*), yVertex(*), uvel_2d(*), vvel_2d(*), stagthck(*), &
+              flwafact(*)
+         integer(c_int32_t), intent(in) :: active_cell(*), indxA_2d(*)
+         real(c_double), value :: efvs_constant, effstrain_min, n_glen
+         real(c_double), intent(out) :: efvs(*), Auu(*), Auv(*), Avu(*), Avv(*)
+       end function c_assemble_2d
     end interface
 
   contains
@@ -456,5 +482,59 @@
          call write_log(trim(text), GM_WARNING)
       endif
     end subroutine check_symmetry_assembled_matrix_2d
+
+    !-----------------------------------------------------------------------
+    ! The reference's argument list (itest, jtest, rtest kept for the call site, unused);
+    ! n_glen is glimmer_physcon's.  The 2D form takes whichapprox and runs the SSA branch; any
+    ! other approximation is reported with GM_FATAL.
+    subroutine assemble_stiffness_matrix_3d(nx, ny, nz, sigma, nhalo, itest, jtest, rtest, active_cell, &
+                                            xVertex, yVertex, uvel, vvel, stagusrf, stagthck, flwafact, &
+                                            whichapprox, whichefvs, efvs, efvs_constant, effstrain_min, &
+                                            Auu, Auv, Avu, Avv)
+      use glimmer_physcon, only: n_glen
+      integer, intent(in) :: nx, ny, nz, nhalo, itest, jtest, rtest, whichapprox, whichefvs
+      real(dp), dimension(nz), intent(in) :: sigma
+      logical, dimension(nx,ny), intent(in) :: active_cell
+      real(dp), dimension(nx-1,ny-1), intent(in) :: xVertex, yVertex, stagusrf, stagthck
+      real(dp), dimension(nz,nx-1,ny-1), intent(in) :: uvel, vvel
+      real(dp), dimension(nz-1,nx,ny), intent(in) :: flwafact
+      real(dp), dimension(nz-1,nx,ny), intent(out) :: efvs
+      real(dp), intent(in) :: efvs_constant, effstrain_min
+      real(dp), dimension(27,nz,nx-1,ny-1), intent(out) :: Auu, Auv, Avu, Avv
+      integer(c_int32_t) :: act(nx,ny), indx3(27)
+      integer :: m
+      act = merge(1, 0, active_cell)
+      indx3 = [(m, m = 1, 27)]
+      call check(c_assemble_3d(nx, ny, nz, nhalo, sigma, act, xVertex, yVertex, uvel, vvel, stagusrf, stagthck, &
+                               flwafact, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen, indx3, &
+                               efvs, Auu, Auv, Avu, Avv))
+    end subroutine assemble_stiffness_matrix_3d
+
+    !-----------------------------------------------------------------------
+    subroutine assemble_stiffness_matrix_2d(nx, ny, nz, sigma, nhalo, itest, jtest, rtest, active_cell, &
+                                            xVertex, yVertex, uvel_2d, vvel_2d, stagthck, flwafact, &
+                                            whichapprox, whichefvs, efvs, efvs_constant, effstrain_min, &
+                                            Auu, Auv, Avu, Avv)
+      use glimmer_physcon, only: n_glen
+      use glide_types, only: HO_APPROX_SSA
+      integer, intent(in) :: nx, ny, nz, nhalo, itest, jtest, rtest, whichapprox, whichefvs
+      real(dp), dimension(nz), intent(in) :: sigma
+      logical, dimension(nx,ny), intent(in) :: active_cell
+      real(dp), dimension(nx-1,ny-1), intent(in) :: xVertex, yVertex, uvel_2d, vvel_2d, stagthck
+      real(dp), dimension(nz-1,nx,ny), intent(in) :: flwafact
+      real(dp), dimension(nz-1,nx,ny), intent(out) :: efvs
+      real(dp), intent(in) :: efvs_constant, effstrain_min
+      real(dp), dimension(nx-1,ny-1,9), intent(out) :: Auu, Auv, Avu, Avv
+      integer(c_int32_t) :: act(nx,ny), indx2(9)
+      integer :: m
+      if (whichapprox /= HO_APPROX_SSA) then
+         call write_log('GPU 2D assembly: only the SSA branch is built', GM_FATAL)
+      endif
+      act = merge(1, 0, active_cell)
+      indx2 = [(m, m = 1, 9)]
+      call check(c_assemble_2d(nx, ny, nz, nhalo, sigma, act, xVertex, yVertex, uvel_2d, vvel_2d, stagthck, &
+                               flwafact, whichefvs, efvs_constant, effstrain_min, n_glen, indx2, efvs, &
+                               Auu, Auv, Avu, Avv))
+    end subroutine assemble_stiffness_matrix_2d
 
   end module glissade_velo_higher_pcg_gpu
