@@ -484,9 +484,9 @@
     end subroutine check_symmetry_assembled_matrix_2d
 
     !-----------------------------------------------------------------------
-    ! The reference's argument list (itest, jtest, rtest kept for the call site, unused);
-    ! n_glen is glimmer_physcon's.  The 2D form takes whichapprox and runs the SSA branch; any
-    ! other approximation is reported with GM_FATAL.
+    ! The reference's argument lists (the diagnostic indices, and in 2D the arguments of the
+    ! L1L2 and DIVA branches, are accepted and unused); n_glen is glimmer_physcon's.  The 2D
+    ! form runs the SSA branch; any other approximation is reported with GM_FATAL.
     subroutine assemble_stiffness_matrix_3d(nx, ny, nz, sigma, nhalo, itest, jtest, rtest, active_cell, &
                                             xVertex, yVertex, uvel, vvel, stagusrf, stagthck, flwafact, &
                                             whichapprox, whichefvs, efvs, efvs_constant, effstrain_min, &
@@ -511,24 +511,33 @@
     end subroutine assemble_stiffness_matrix_3d
 
     !-----------------------------------------------------------------------
-    subroutine assemble_stiffness_matrix_2d(nx, ny, nz, sigma, nhalo, itest, jtest, rtest, active_cell, &
-                                            xVertex, yVertex, uvel_2d, vvel_2d, stagthck, flwafact, &
-                                            whichapprox, whichefvs, efvs, efvs_constant, effstrain_min, &
-                                            Auu, Auv, Avu, Avv)
+    subroutine assemble_stiffness_matrix_2d(nx, ny, nz, sigma, stagsigma, nhalo, itest, jtest, rtest, parallel, &
+                                            active_cell, xVertex, yVertex, uvel_2d, vvel_2d, stagusrf, stagthck, &
+                                            flwa, flwafact, whichapprox, diva_slope_factor_x, diva_slope_factor_y, &
+                                            whichefvs, efvs, efvs_constant, effstrain_min, Auu, Auv, Avu, Avv, &
+                                            dusrf_dx, dusrf_dy, thck, btractx, btracty, omega_k, omega, efvs_qp_3d)
       use glimmer_physcon, only: n_glen
       use glide_types, only: HO_APPROX_SSA
       integer, intent(in) :: nx, ny, nz, nhalo, itest, jtest, rtest, whichapprox, whichefvs
       real(dp), dimension(nz), intent(in) :: sigma
+      real(dp), dimension(nz-1), intent(in) :: stagsigma
+      type(parallel_type), intent(in) :: parallel
       logical, dimension(nx,ny), intent(in) :: active_cell
-      real(dp), dimension(nx-1,ny-1), intent(in) :: xVertex, yVertex, uvel_2d, vvel_2d, stagthck
-      real(dp), dimension(nz-1,nx,ny), intent(in) :: flwafact
+      real(dp), dimension(nx-1,ny-1), intent(in) :: xVertex, yVertex, uvel_2d, vvel_2d, stagusrf, stagthck
+      real(dp), dimension(nz-1,nx,ny), intent(in) :: flwa, flwafact
+      real(dp), dimension(nx,ny), intent(in) :: diva_slope_factor_x, diva_slope_factor_y
       real(dp), dimension(nz-1,nx,ny), intent(out) :: efvs
       real(dp), intent(in) :: efvs_constant, effstrain_min
       real(dp), dimension(nx-1,ny-1,9), intent(out) :: Auu, Auv, Avu, Avv
+      real(dp), dimension(nx-1,ny-1), intent(in), optional :: dusrf_dx, dusrf_dy, btractx, btracty
+      real(dp), dimension(nx,ny), intent(in), optional :: thck
+      real(dp), dimension(nz,nx,ny), intent(out), optional :: omega_k
+      real(dp), dimension(nx,ny), intent(out), optional :: omega
+      real(dp), dimension(nz-1,4,nx,ny), intent(inout), optional :: efvs_qp_3d
       integer(c_int32_t) :: act(nx,ny), indx2(9)
       integer :: m
       if (whichapprox /= HO_APPROX_SSA) then
-         call write_log('GPU 2D assembly: only the SSA branch is built', GM_FATAL)
+         call write_log('GPU 2D assembly: only the SSA branch is built (L1L2 and DIVA are not)', GM_FATAL)
       endif
       act = merge(1, 0, active_cell)
       indx2 = [(m, m = 1, 9)]
