@@ -68,6 +68,10 @@ def lib() -> ctypes.CDLL:
         L.oracle_assemble_stiffness_3d.argtypes = [i, i, i, i, d, d, d, d, d, d, d, d, d, i, i, dbl, dbl, dbl,
                                                    d, d, d, d, d]
         L.oracle_assemble_stiffness_2d.argtypes = [i, i, i, i, d, d, d, d, d, d, d, d, i, dbl, dbl, dbl, d, d, d, d, d]
+        L.oracle_dirichlet_3d.argtypes = [i, i, i, i, d, d, d, d, d, d, d, d, d, d, d]
+        L.oracle_dirichlet_3d.restype = None
+        L.oracle_basal_local_3d.argtypes = [i, i, i, dbl, dbl, d, d, d, d, d, d]
+        L.oracle_basal_local_3d.restype = None
         L.oracle_check_symmetry.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, P(dbl), P(ctypes.c_long)]
         L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
@@ -235,6 +239,30 @@ def assemble_stiffness_2d(nx, ny, nz, sigma, active_cell, xVertex, yVertex, uvel
     st = lib().oracle_assemble_stiffness_2d(nx, ny, nz, nhalo, *[_p(a) for a in ins], whichefvs, efvs_constant,
                                             effstrain_min, n_glen, _p(efvs), *[_p(a) for a in A])
     return (st, efvs, *A)
+
+
+def dirichlet_3d(nx, ny, nz, active_vertex, umask, vmask, uvel, vvel, Auu, Auv, Avu, Avv, bu, bv, nhalo=2):
+    """dirichlet_boundary_conditions_3d (glissade_velo_higher.F90:9305-9498) on copies:
+    masks and velocities (ny-1, nx-1, nz), blocks (ny-1, nx-1, nz, 27).  Returns
+    (Auu, Auv, Avu, Avv, bu, bv)."""
+    out = [np.array(a, dtype=np.float64, copy=True) for a in (Auu, Auv, Avu, Avv, bu, bv)]
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    lib().oracle_dirichlet_3d(nx, ny, nz, nhalo, _p(i32(active_vertex)), _p(i32(umask)), _p(i32(vmask)),
+                              _p(f64(uvel)), _p(f64(vvel)), *[_p(a) for a in out])
+    return tuple(out)
+
+
+def basal_local_3d(nx, ny, nz, dx, dy, active_vertex, beta, lsrf, Auu, Avv):
+    """basal_sliding_bc_3d with HO_ASSEMBLE_BETA_LOCAL (glissade_velo_higher.F90:8815-9129) on
+    copies of the blocks; returns (Auu, Avv, theta (ny-1, nx-1))."""
+    out = [np.array(a, dtype=np.float64, copy=True) for a in (Auu, Avv)]
+    theta = np.zeros((ny - 1, nx - 1))
+    lib().oracle_basal_local_3d(nx, ny, nz, float(dx), float(dy),
+                                _p(np.ascontiguousarray(active_vertex, dtype=np.int32)),
+                                _p(np.ascontiguousarray(beta, dtype=np.float64)),
+                                _p(np.ascontiguousarray(lsrf, dtype=np.float64)), _p(out[0]), _p(out[1]), _p(theta))
+    return out[0], out[1], theta
 
 
 def reprosum(a) -> float:

@@ -411,3 +411,119 @@ int oracle_assemble_stiffness_3d(int nx, int ny, int nz, int nhalo, const double
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Boundary terms of the 3D system (glissade_velo_higher.F90:2848-2898)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+// dirichlet_boundary_conditions_3d (:9305-9498), loop for loop: vertices j = nhalo..ny-nhalo+1,
+// i = nhalo..nx-nhalo+1 that are active, levels k; a u-prescribed node gets b = uvel, a unit
+// diagonal, its u-row zeroed and its column moved to the right-hand side of every neighbour
+// that is not u- (resp. v-) prescribed; then the same for v.  Masks (nz,nx-1,ny-1) int32 with
+// 1 = prescribed; arrays in the caller's layout.
+void oracle_dirichlet_3d(int nx, int ny, int nz, int nhalo, const int32_t *active_vertex, const int32_t *umask,
+                         const int32_t *vmask, const double *uvel, const double *vvel, double *Auu, double *Auv,
+                         double *Avu, double *Avv, double *bu, double *bv) {
+    const long NX = nx - 1;
+    auto V = [&](int k, int i, int j) { return (long)(k - 1) + (long)nz * ((i - 1) + NX * (j - 1)); };
+    auto A = [&](int m, int k, int i, int j) { return (long)(m - 1) + 27L * V(k, i, j); };
+    auto M = [](int iA, int jA, int kA) { return 1 + (iA + 1) + 3 * (jA + 1) + 9 * (kA + 1); };
+    for (int j = nhalo; j <= ny - nhalo + 1; ++j)
+        for (int i = nhalo; i <= nx - nhalo + 1; ++i) {
+            if (!active_vertex[(i - 1) + NX * (j - 1)]) continue;
+            for (int k = 1; k <= nz; ++k) {
+                for (int pass = 0; pass < 2; ++pass) {
+                    const int32_t *mask = pass == 0 ? umask : vmask;
+                    if (mask[V(k, i, j)] != 1) continue;
+                    const double x = pass == 0 ? uvel[V(k, i, j)] : vvel[V(k, i, j)];
+                    (pass == 0 ? bu : bv)[V(k, i, j)] = x;
+                    for (int kA = -1; kA <= 1; ++kA)
+                        for (int jA = -1; jA <= 1; ++jA)
+                            for (int iA = -1; iA <= 1; ++iA) {
+                                if (!(k + kA >= 1 && k + kA <= nz && i + iA >= 1 && i + iA <= nx - 1 && j + jA >= 1 &&
+                                      j + jA <= ny - 1))
+                                    continue;
+                                if (iA == 0 && jA == 0 && kA == 0) {
+                                    const long a = A(M(0, 0, 0), k, i, j);
+                                    if (pass == 0) {
+                                        Auu[a] = 1.0;
+                                        Auv[a] = 0.0;
+                                        Avu[a] = 0.0;
+                                    } else {
+                                        Auv[a] = 0.0;
+                                        Avu[a] = 0.0;
+                                        Avv[a] = 1.0;
+                                    }
+                                    continue;
+                                }
+                                const long a = A(M(iA, jA, kA), k, i, j);
+                                if (pass == 0) {
+                                    Auu[a] = 0.0;
+                                    Auv[a] = 0.0;
+                                } else {
+                                    Avu[a] = 0.0;
+                                    Avv[a] = 0.0;
+                                }
+                                const long e = V(k + kA, i + iA, j + jA);
+                                const long b = A(M(-iA, -jA, -kA), k + kA, i + iA, j + jA);
+                                double *Au = pass == 0 ? Auu : Auv, *Av = pass == 0 ? Avu : Avv;
+                                if (umask[e] != 1) {
+                                    bu[e] = bu[e] - Au[b] * x;
+                                    Au[b] = 0.0;
+                                }
+                                if (vmask[e] != 1) {
+                                    bv[e] = bv[e] - Av[b] * x;
+                                    Av[b] = 0.0;
+                                }
+                            }
+                }
+            }
+        }
+}
+
+// basal_sliding_bc_3d (:8815-9129), HO_ASSEMBLE_BETA_LOCAL: staglsrf = glissade_stagger(lsrf)
+// (glissade_grid_operators.F90:69-157, all four cells), theta = glissade_slope_angle(staglsrf)
+// on the (nx-1, ny-1) grid (:1264-1410: glissade_gradient :309-468 with every edge in the mask,
+// glissade_unstagger :226-305 over the inner cells, atan of the gradient's length; the
+// parallel_halo that follows returns at once for arrays of that size), then at every active
+// vertex the bed diagonal of Auu and Avv (level nz) += dx*dy/vol0 * beta / cos(theta).
+// theta (nx-1,ny-1) is returned too.
+void oracle_basal_local_3d(int nx, int ny, int nz, double dx, double dy, const int32_t *active_vertex,
+                           const double *beta, const double *lsrf, double *Auu, double *Avv, double *theta) {
+    const int NX = nx - 1, NY = ny - 1;
+    std::vector<double> s((size_t)NX * NY), gx((size_t)(NX - 1) * (NY - 1)), gy(gx.size());
+    auto L = [&](int i, int j) { return lsrf[(i - 1) + (long)nx * (j - 1)]; };
+    auto S = [&](int i, int j) -> double & { return s[(i - 1) + (size_t)NX * (j - 1)]; };
+    for (int j = 1; j <= NY; ++j)
+        for (int i = 1; i <= NX; ++i) S(i, j) = (L(i, j + 1) + L(i + 1, j + 1) + L(i, j) + L(i + 1, j)) / 4.0;
+    // glissade_gradient on the (NX, NY) grid: all edge masks true for the edges it reads
+    for (int j = 1; j <= NY - 1; ++j)
+        for (int i = 1; i <= NX - 1; ++i) {
+            const double north = (S(i + 1, j + 1) - S(i, j + 1)) / dx, south = (S(i + 1, j) - S(i, j)) / dx;
+            gx[(i - 1) + (size_t)(NX - 1) * (j - 1)] = (north + south) / 2.0;
+            const double east = (S(i + 1, j + 1) - S(i + 1, j)) / dy, west = (S(i, j + 1) - S(i, j)) / dy;
+            gy[(i - 1) + (size_t)(NX - 1) * (j - 1)] = (east + west) / 2.0;
+        }
+    auto G = [&](const std::vector<double> &g, int i, int j) { return g[(i - 1) + (size_t)(NX - 1) * (j - 1)]; };
+    for (int j = 1; j <= NY; ++j)
+        for (int i = 1; i <= NX; ++i) {
+            double ddx = 0.0, ddy = 0.0;
+            if (i >= 2 && i <= NX - 1 && j >= 2 && j <= NY - 1) {
+                ddx = (G(gx, i, j) + G(gx, i - 1, j) + G(gx, i, j - 1) + G(gx, i - 1, j - 1)) / 4.0;
+                ddy = (G(gy, i, j) + G(gy, i - 1, j) + G(gy, i, j - 1) + G(gy, i - 1, j - 1)) / 4.0;
+            }
+            const double slope = std::sqrt(ddx * ddx + ddy * ddy);
+            theta[(i - 1) + (size_t)NX * (j - 1)] = (slope >= 0.0) ? std::atan(slope) : 0.0;
+        }
+    for (int j = 1; j <= NY; ++j)
+        for (int i = 1; i <= NX; ++i) {
+            const long q = (i - 1) + (long)NX * (j - 1);
+            if (!active_vertex[q]) continue;
+            const long a = 13 + 27L * ((long)(nz - 1) + (long)nz * q);
+            Auu[a] = Auu[a] + dx * dy / kVol0 * beta[q] / std::cos(theta[q]);
+            Avv[a] = Avv[a] + dx * dy / kVol0 * beta[q] / std::cos(theta[q]);
+        }
+}
+
+}  // extern "C"
