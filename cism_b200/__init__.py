@@ -30,7 +30,7 @@ __all__ = [
     "ALG_STANDARD", "ALG_CHRONGEAR", "ALG_MIXED_CHRONGEAR", "compute_residual_vector_3d",
     "compute_residual_vector_2d", "compute_residual_velocity_3d", "compute_residual_velocity_2d",
     "check_symmetry_assembled_matrix_3d", "check_symmetry_assembled_matrix_2d", "assemble_stiffness_matrix_3d",
-    "assemble_stiffness_matrix_2d",
+    "assemble_stiffness_matrix_2d", "dirichlet_boundary_conditions_3d", "basal_sliding_bc_3d",
 ]
 
 ALG_STANDARD, ALG_CHRONGEAR, ALG_MIXED_CHRONGEAR = 0, 1, 2
@@ -188,13 +188,19 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_assemble_stiffness_matrix_2d.argtypes = [i32, i32, i32, i32, d, d, d, d, d, d, d, d, i32, dbl, dbl,
                                                          dbl, d, d, d, d, d, d]
     lib.cismgpu_solver_assemble_stiffness_2d.argtypes = [vp, i32, i32, d, d, d, d, d, d, d, d, i32, dbl, dbl, dbl, d]
+    lib.cismgpu_dirichlet_boundary_conditions_3d.argtypes = [i32, i32, i32, i32, d, d, d, d, d, d, d, d, d, d, d, d]
+    lib.cismgpu_basal_sliding_bc_3d.argtypes = [i32, i32, i32, i32, dbl, dbl, d, d, d, i32, d, d, d]
+    lib.cismgpu_solver_assemble_system_3d.argtypes = [vp, i32, dbl, dbl, d, d, d, d, d, d, d, d, i32, i32, dbl, dbl,
+                                                      dbl, d, d, d, d, d, d, d]
     for f in ("cismgpu_compute_residual_vector_3d", "cismgpu_compute_residual_vector_2d",
               "cismgpu_compute_residual_velocity_3d", "cismgpu_compute_residual_velocity_2d",
               "cismgpu_solver_set_system", "cismgpu_solver_residual_vector", "cismgpu_solver_residual_velocity",
               "cismgpu_solver_save", "cismgpu_solver_restore", "cismgpu_check_symmetry_assembled_matrix_3d",
               "cismgpu_check_symmetry_assembled_matrix_2d", "cismgpu_solver_check_symmetry",
               "cismgpu_assemble_stiffness_matrix_3d", "cismgpu_solver_assemble_stiffness_3d",
-              "cismgpu_assemble_stiffness_matrix_2d", "cismgpu_solver_assemble_stiffness_2d"):
+              "cismgpu_assemble_stiffness_matrix_2d", "cismgpu_solver_assemble_stiffness_2d",
+              "cismgpu_dirichlet_boundary_conditions_3d", "cismgpu_basal_sliding_bc_3d",
+              "cismgpu_solver_assemble_system_3d"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -486,6 +492,36 @@ def assemble_stiffness_matrix_2d(nx, ny, nz, nhalo, sigma, active_cell, xVertex,
     return (efvs, *A)
 
 
+def dirichlet_boundary_conditions_3d(nx, ny, nz, nhalo, active_vertex, umask, vmask, uvel, vvel, Auu, Auv, Avu, Avv,
+                                     bu, bv, indxA_3d=None):
+    """Mirrors dirichlet_boundary_conditions_3d (glissade_velo_higher.F90:9305-9498) on the GPU;
+    the blocks and b (writable float64, caller's layout) are modified in place."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    n = nv * nz
+    indx = np.arange(1, 28, dtype=np.int32) if indxA_3d is None else np.ascontiguousarray(indxA_3d, dtype=np.int32)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    _check(lib, lib.cismgpu_dirichlet_boundary_conditions_3d(
+        nx, ny, nz, int(nhalo), _ptr(i32(active_vertex), np.int32, nv), _ptr(i32(umask), np.int32, n),
+        _ptr(i32(vmask), np.int32, n), _ptr(uvel, np.float64, n), _ptr(vvel, np.float64, n), _ptr(indx, np.int32, 27),
+        *[_ptr(a, np.float64, 27 * n, True) for a in (Auu, Auv, Avu, Avv)], _ptr(bu, np.float64, n, True),
+        _ptr(bv, np.float64, n, True)))
+
+
+def basal_sliding_bc_3d(nx, ny, nz, nhalo, dx, dy, active_vertex, beta, lsrf, Auu, Avv, whichassemble_beta=1,
+                        indxA_3d=None):
+    """Mirrors basal_sliding_bc_3d (glissade_velo_higher.F90:8815-9129), local form, on the GPU:
+    the bed diagonals of the full Auu and Avv blocks are increased in place."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    indx = np.arange(1, 28, dtype=np.int32) if indxA_3d is None else np.ascontiguousarray(indxA_3d, dtype=np.int32)
+    _check(lib, lib.cismgpu_basal_sliding_bc_3d(
+        nx, ny, nz, int(nhalo), float(dx), float(dy), _ptr(np.ascontiguousarray(active_vertex, dtype=np.int32),
+                                                           np.int32, nv),
+        _ptr(beta, np.float64, nv), _ptr(lsrf, np.float64, nx * ny), int(whichassemble_beta), _ptr(indx, np.int32, 27),
+        _ptr(Auu, np.float64, 27 * nv * nz, True), _ptr(Avv, np.float64, 27 * nv * nz, True)))
+
+
 class DeviceSolver:
     """A device-resident linear system (cismgpu_solver_create): A, b and x0 live in HBM.
 
@@ -589,6 +625,28 @@ class DeviceSolver:
                 self.handle, nz, int(nhalo), *head, pu, pv, tail[1], tail[2], int(whichefvs), float(efvs_constant),
                 float(effstrain_min), float(n_glen), pe)
         _check(self._lib, st)
+        return efvs
+
+    def assemble_system(self, nhalo, dx, dy, sigma, active_cell, active_vertex, xVertex, yVertex, stagusrf,
+                        stagthck, flwafact, loadu, loadv, beta=None, lsrf=None, umask=None, vmask=None,
+                        whichapprox=2, whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8, n_glen=3.0):
+        """One Picard iteration's 3D system on the device (cismgpu_solver_assemble_system_3d):
+        stiffness from the current velocity, local basal term, b = load, Dirichlet conditions,
+        staggered halo.  Returns efvs (ny, nx, nz-1)."""
+        P = self.problem
+        nx, ny, nz = P.nx, P.ny, P.nz
+        nv = (nx - 1) * (ny - 1)
+        efvs = np.zeros((ny, nx, nz - 1))
+        head, tail = _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagusrf, stagthck, flwafact)
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        keep = [i32(active_vertex)] + ([i32(umask), i32(vmask)] if umask is not None else [])
+        pm = (_ptr(keep[1], np.int32, nv * nz), _ptr(keep[2], np.int32, nv * nz)) if umask is not None else (None, None)
+        pb = (_ptr(beta, np.float64, nv), _ptr(lsrf, np.float64, nx * ny)) if beta is not None else (None, None)
+        _check(self._lib, self._lib.cismgpu_solver_assemble_system_3d(
+            self.handle, int(nhalo), float(dx), float(dy), head[0], head[1], _ptr(keep[0], np.int32, nv), head[2],
+            head[3], *tail, int(whichapprox), int(whichefvs), float(efvs_constant), float(effstrain_min),
+            float(n_glen), *pb, _ptr(loadu, np.float64, nv * nz), _ptr(loadv, np.float64, nv * nz), *pm,
+            _ptr(efvs, np.float64, efvs.size, True)))
         return efvs
 
     def save(self):

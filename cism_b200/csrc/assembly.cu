@@ -346,4 +346,159 @@ __global__ void __launch_bounds__(kAsmBlock) k_assemble2d(AsmArgs a, const doubl
         for (int c = 0; c < 9; ++c) B[b][L.at(c, 0, q)] = acc[b][c];
 }
 
+// ---------------------------------------------------------------------------
+// Boundary terms of the 3D system (glissade_velo_higher.F90:2848-2898)
+// ---------------------------------------------------------------------------
+// Vector element (k, q) of a (nz, nx-1, ny-1) field: the caller's layout or level-major planes.
+// The Dirichlet pass takes one for b, one for the masks and one for the velocity, which on a
+// handle come from the device planes and the host respectively.
+struct VecIdx {
+    long long NQ;
+    int nz;
+    int planes;
+    __device__ __forceinline__ long long at(int k, long long q) const {
+        return planes ? (long long)k * NQ + q : (long long)k + (long long)nz * q;
+    }
+};
+
+// dirichlet_boundary_conditions_3d (:9305-9498), one thread per node P.  The reference loops
+// over the prescribed nodes R (vertices j = nhalo..ny-nhalo+1, i = nhalo..nx-nhalo+1, active;
+// levels k; u then v) and (a) rewrites R's own row and b(R), (b) moves R's column into the
+// right-hand side of each neighbour P not prescribed in that component and zeroes the
+// coupling.  Every write of (a) and (b) lands in row P or b(P) of a single P, and (b) reads
+// only row P's couplings to R, which nothing else writes: so each P applies, in the
+// reference's order of R (j, then i, then k; u before v), the moves from its prescribed
+// neighbours, and then, when P itself is a visited prescribed node, its own row.  b enters
+// holding the load vector.
+__global__ void __launch_bounds__(kBlock) k_dirichlet3d(int nx, int ny, int nz, int nhalo, SymIdx L, VecIdx Wb,
+                                                        VecIdx Wm, VecIdx Wx,
+                                                        const int32_t *__restrict__ active_vertex,
+                                                        const int32_t *__restrict__ umask,
+                                                        const int32_t *__restrict__ vmask,
+                                                        const double *__restrict__ uvel,
+                                                        const double *__restrict__ vvel, double *Auu, double *Auv,
+                                                        double *Avu, double *Avv, double *bu, double *bv) {
+    const long long NX = nx - 1, NQ = NX * (ny - 1);
+    const long long t = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (t >= (long long)nz * NQ) return;
+    const int k = (int)(t / NQ);
+    const long long q = t - (long long)k * NQ;
+    const int j = (int)(q / NX), i = (int)(q - (long long)j * NX);  // 0-based
+    // a node's own pass runs when its vertex is in the loop range (1-based nhalo..n-nhalo+1)
+    // and active
+    auto visited = [&](int ii, int jj) {
+        return ii >= nhalo - 1 && ii <= nx - nhalo && jj >= nhalo - 1 && jj <= ny - nhalo &&
+               active_vertex[(long long)jj * NX + ii] != 0;
+    };
+    const long long bP = Wb.at(k, q), mP = Wm.at(k, q), xP = Wx.at(k, q);
+    const bool ufree = umask[mP] != 1, vfree = vmask[mP] != 1;
+    double b_u = bu[bP], b_v = bv[bP];
+    for (int ej = -1; ej <= 1; ++ej)
+        for (int ei = -1; ei <= 1; ++ei)
+            for (int ek = -1; ek <= 1; ++ek) {
+                if (ei == 0 && ej == 0 && ek == 0) continue;
+                const int kR = k + ek, iR = i + ei, jR = j + ej;
+                if (kR < 0 || kR >= nz || iR < 0 || iR >= NX || jR < 0 || jR >= ny - 1) continue;
+                if (!visited(iR, jR)) continue;
+                const long long qR = (long long)jR * NX + iR, mR = Wm.at(kR, qR), xR = Wx.at(kR, qR);
+                const int c = (ei + 1) + 3 * (ej + 1) + 9 * (ek + 1);  // row P's coupling to R
+                const long long a = L.at(c, k, q);
+                if (umask[mR] == 1) {
+                    const double x = uvel[xR];
+                    if (ufree) {
+                        b_u = b_u - Auu[a] * x;
+                        Auu[a] = 0.0;
+                    }
+                    if (vfree) {
+                        b_v = b_v - Avu[a] * x;
+                        Avu[a] = 0.0;
+                    }
+                }
+                if (vmask[mR] == 1) {
+                    const double x = vvel[xR];
+                    if (ufree) {
+                        b_u = b_u - Auv[a] * x;
+                        Auv[a] = 0.0;
+                    }
+                    if (vfree) {
+                        b_v = b_v - Avv[a] * x;
+                        Avv[a] = 0.0;
+                    }
+                }
+            }
+    if (visited(i, j)) {
+        for (int pass = 0; pass < 2; ++pass) {
+            if ((pass == 0 ? umask : vmask)[mP] != 1) continue;
+            if (pass == 0) b_u = uvel[xP];
+            else b_v = vvel[xP];
+            for (int c = 0; c < 27; ++c) {
+                const int ei = c % 3 - 1, ej = (c / 3) % 3 - 1, ek = c / 9 - 1;
+                if (k + ek < 0 || k + ek >= nz || i + ei < 0 || i + ei >= NX || j + ej < 0 || j + ej >= ny - 1)
+                    continue;
+                const long long a = L.at(c, k, q);
+                if (c == 13) {
+                    if (pass == 0) {
+                        Auu[a] = 1.0;
+                        Auv[a] = 0.0;
+                        Avu[a] = 0.0;
+                    } else {
+                        Auv[a] = 0.0;
+                        Avu[a] = 0.0;
+                        Avv[a] = 1.0;
+                    }
+                } else if (pass == 0) {
+                    Auu[a] = 0.0;
+                    Auv[a] = 0.0;
+                } else {
+                    Avu[a] = 0.0;
+                    Avv[a] = 0.0;
+                }
+            }
+        }
+    }
+    bu[bP] = b_u;
+    bv[bP] = b_v;
+}
+
+// basal_sliding_bc_3d with HO_ASSEMBLE_BETA_LOCAL (:8840-8875), one thread per vertex: the
+// slope angle of the staggered lower surface (glissade_stagger of lsrf over all four cells,
+// glissade_gradient with every edge, glissade_unstagger over the inner vertices, atan), each
+// intermediate recomputed from its inputs in the reference's operation order, then at an
+// active vertex the bed diagonal (level nz) of Auu and Avv += dx*dy/vol0 * beta / cos(theta).
+__global__ void __launch_bounds__(kBlock) k_basal_local3d(int nx, int ny, int nz, double dx, double dy, SymIdx L,
+                                                          const int32_t *__restrict__ active_vertex,
+                                                          const double *__restrict__ beta,
+                                                          const double *__restrict__ lsrf, double *Auu,
+                                                          double *Avv) {
+    const int NX = nx - 1, NY = ny - 1;
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (q >= (long long)NX * NY) return;
+    if (!active_vertex[q]) return;
+    const int j = (int)(q / NX) + 1, i = (int)(q - (long long)(j - 1) * NX) + 1;  // 1-based
+    auto Lf = [&](int ii, int jj) { return lsrf[(ii - 1) + (long long)nx * (jj - 1)]; };
+    auto S = [&](int ii, int jj) { return (Lf(ii, jj + 1) + Lf(ii + 1, jj + 1) + Lf(ii, jj) + Lf(ii + 1, jj)) / 4.0; };
+    double ddx = 0.0, ddy = 0.0;
+    if (i >= 2 && i <= NX - 1 && j >= 2 && j <= NY - 1) {
+        double gx[4], gy[4];  // at (i,j), (i-1,j), (i,j-1), (i-1,j-1)
+        const int oi[4] = {0, -1, 0, -1}, oj[4] = {0, 0, -1, -1};
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const int a = i + oi[n], b = j + oj[n];
+            const double s00 = S(a, b), s10 = S(a + 1, b), s01 = S(a, b + 1), s11 = S(a + 1, b + 1);
+            const double north = (s11 - s01) / dx, south = (s10 - s00) / dx;
+            gx[n] = (north + south) / 2.0;
+            const double east = (s11 - s10) / dy, west = (s01 - s00) / dy;
+            gy[n] = (east + west) / 2.0;
+        }
+        ddx = (gx[0] + gx[1] + gx[2] + gx[3]) / 4.0;
+        ddy = (gy[0] + gy[1] + gy[2] + gy[3]) / 4.0;
+    }
+    const double slope = sqrt(ddx * ddx + ddy * ddy);
+    const double theta = (slope >= 0.0) ? atan(slope) : 0.0;
+    const double add = dx * dy / kAsmVol0 * beta[q] / cos(theta);
+    const long long a = L.at(13, nz - 1, q);
+    Auu[a] = Auu[a] + add;
+    Avv[a] = Avv[a] + add;
+}
+
 }  // namespace cismgpu

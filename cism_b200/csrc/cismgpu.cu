@@ -115,6 +115,7 @@ struct Solver {
     DevBuf A_sav, x_sav;      // accelerated Picard's saved matrix and velocity (cismgpu_solver_save)
     DevBuf rsum;              // the reproducible sum's exponent extremes and level sums
     DevBuf asm_in;            // the stiffness assembly's inputs (geometry, flow factor, velocity, efvs)
+    DevBuf bc_in;             // the boundary terms' inputs (beta, lsrf, masks, velocity)
     bool have_sav = false;
     bool x_current = false;   // the x planes hold a solution (a solve ran since the last upload)
     int32_t hindx[27] = {};   // host copy of the uploaded indxA map (27 or 9 entries)
@@ -141,6 +142,7 @@ struct Solver {
         x_sav.release();
         rsum.release();
         asm_in.release();
+        bc_in.release();
         have_sav = false;
         mixed.release();
         if (h_done) cudaFreeHost(h_done);
@@ -418,6 +420,55 @@ struct Solver {
         if (efvs) CU(cudaMemcpyAsync(efvs, d_efvs, nel * sizeof(double), cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
         if (sing) return fail(CISMGPU_EINVAL, "Jacobian matrix is singular (an element of zero volume)");
+        return CISMGPU_OK;
+    }
+
+    // The boundary terms of the 3D system on four blocks in layout L and b in layout Wb
+    // (glissade_velo_higher.F90:2848-2891): the local basal term of basal_sliding_bc_3d when
+    // beta is given (lsrf with it), then dirichlet_boundary_conditions_3d when the masks are
+    // given.  Host arrays in the caller's layout; uvel = vvel = null: the velocity planes
+    // vel_id, vel_id+1.  Leaves the stream synchronized.
+    int boundary3d(const SymIdx &L, double *Auu, double *Auv, double *Avu, double *Avv, double *bu, double *bv,
+                   VecIdx Wb, int nhalo, double dx, double dy, const int32_t *active_vertex, const double *beta,
+                   const double *lsrf, const int32_t *umask, const int32_t *vmask, const double *uvel,
+                   const double *vvel, int vel_id) {
+        const int nx = g.NX + 1, ny = g.NY + 1, nz = g.nz;
+        const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny, nn = (size_t)nz * nq;
+        const bool host_vel = uvel != nullptr;
+        // doubles: beta, lsrf, [uvel, vvel]; then int32: active_vertex, umask, vmask
+        const size_t nd = nq + ncell + (host_vel ? 2 * nn : 0);
+        CU(bc_in.ensure(nd * sizeof(double) + (nq + 2 * nn) * sizeof(int32_t)));
+        double *D = bc_in.as<double>();
+        double *d_beta = D, *d_lsrf = D + nq, *d_u = d_lsrf + ncell, *d_v = d_u + nn;
+        int32_t *d_act = reinterpret_cast<int32_t *>(D + nd), *d_um = d_act + nq, *d_vm = d_um + nn;
+        cudaStream_t s = stream;
+        auto up = [&](void *dst, const void *src, size_t bytes) {
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+        };
+        CU(up(d_act, active_vertex, nq * sizeof(int32_t)));
+        if (beta) {
+            CU(up(d_beta, beta, nq * sizeof(double)));
+            CU(up(d_lsrf, lsrf, ncell * sizeof(double)));
+            k_basal_local3d<<<nblocks((long long)nq), kBlock, 0, s>>>(nx, ny, nz, dx, dy, L, d_act, d_beta, d_lsrf,
+                                                                      Auu, Avv);
+            CU(cudaGetLastError());
+        }
+        if (umask) {
+            CU(up(d_um, umask, nn * sizeof(int32_t)));
+            CU(up(d_vm, vmask, nn * sizeof(int32_t)));
+            if (host_vel) {
+                CU(up(d_u, uvel, nn * sizeof(double)));
+                CU(up(d_v, vvel, nn * sizeof(double)));
+            }
+            const double *V = vec.as<double>();
+            const double *xu = host_vel ? d_u : V + (size_t)vel_id * nvec;
+            const double *xv = host_vel ? d_v : V + (size_t)(vel_id + 1) * nvec;
+            const VecIdx Wm{g.NQ, nz, 0}, Wx{g.NQ, nz, host_vel ? 0 : 1};
+            k_dirichlet3d<<<nblocks((long long)nn), kBlock, 0, s>>>(nx, ny, nz, nhalo, L, Wb, Wm, Wx, d_act, d_um,
+                                                                    d_vm, xu, xv, Auu, Auv, Avu, Avv, bu, bv);
+            CU(cudaGetLastError());
+        }
+        CU(cudaStreamSynchronize(s));
         return CISMGPU_OK;
     }
 
@@ -1936,6 +1987,65 @@ int cismgpu_assemble_stiffness_matrix_2d(int nx, int ny, int nz, int nhalo, cons
                             blocks);
 }
 
+// One-shot boundary terms on the caller's 3D blocks (and b): uploaded in the caller's layout,
+// modified on the device, copied back.  which: 0 Dirichlet, 1 local basal term.
+static int oneshot_boundary3d(int which, int nx, int ny, int nz, int nhalo, double dx, double dy,
+                              const int32_t *active_vertex, const double *beta, const double *lsrf,
+                              const int32_t *umask, const int32_t *vmask, const double *uvel, const double *vvel,
+                              const int32_t *indx, double *Auu, double *Auv, double *Avu, double *Avv, double *bu,
+                              double *bv) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_error.clear();
+    if (!active_vertex || !indx || !Auu || !Avv) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (which == 0 && (!umask || !vmask || !uvel || !vvel || !Auv || !Avu || !bu || !bv))
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (which == 1 && (!beta || !lsrf)) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (nx < 6 || ny < 6 || nz < 1 || nz > kMaxNz) return fail(CISMGPU_EINVAL, "grid too small or nz outside 1..64");
+    if (nhalo < 1 || 2 * nhalo >= nx || 2 * nhalo >= ny) return fail(CISMGPU_EINVAL, "nhalo outside the grid");
+    TRY(validate_indx(indx, 27));
+    cismgpu_par_t par{};
+    par.staggered_ilo = 1; par.staggered_ihi = nx - 1; par.staggered_jlo = 1; par.staggered_jhi = ny - 1;
+    par.tasks_row = par.tasks_col = 1;
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
+    TRY(sv.set_geom(make_geom(nx, ny, nz, &par), true));
+    const size_t bs = (size_t)27 * sv.nvec;
+    CU(sv.A.ensure(4 * bs * sizeof(double)));
+    sv.mixed.stale = true;  // the matrix buffer holds the caller's layout until the next upload
+    double *A0 = sv.A.as<double>();
+    double *blk[4] = {A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs};
+    double *host[4] = {Auu, Auv, Avu, Avv};
+    cudaStream_t s = sv.stream;
+    for (int b = 0; b < 4; ++b)
+        if (which == 0 || b == 0 || b == 3)
+            CU(cudaMemcpyAsync(blk[b], host[b], bs * sizeof(double), cudaMemcpyHostToDevice, s));
+    double *V = sv.vec.as<double>();  // b in the caller's layout, in the right-hand-side planes
+    double *dbu = V + (size_t)VB_U * sv.nvec, *dbv = V + (size_t)VB_V * sv.nvec;
+    if (which == 0) {
+        CU(cudaMemcpyAsync(dbu, bu, sv.nvec * sizeof(double), cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(dbv, bv, sv.nvec * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = indx[c];
+    L.n = sv.nvec;
+    L.NQ = sv.g.NQ;
+    L.nz = nz;
+    L.raw3 = 1;
+    const VecIdx Wb{sv.g.NQ, nz, 0};
+    TRY(sv.boundary3d(L, blk[0], blk[1], blk[2], blk[3], dbu, dbv, Wb, nhalo, dx, dy, active_vertex,
+                      which == 1 ? beta : nullptr, lsrf, which == 0 ? umask : nullptr, vmask, uvel, vvel, 0));
+    for (int b = 0; b < 4; ++b)
+        if (which == 0 || b == 0 || b == 3)
+            CU(cudaMemcpyAsync(host[b], blk[b], bs * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (which == 0) {
+        CU(cudaMemcpyAsync(bu, dbu, sv.nvec * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(bv, dbv, sv.nvec * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaStreamSynchronize(s));
+    return CISMGPU_OK;
+}
+
 // The handle's assembly: blocks into the resident canonical planes.
 static int solver_assemble(cismgpu_solver_t *h, bool three_d, int nzl, int nhalo, const double *sigma,
                            const int32_t *active_cell, const double *xVertex, const double *yVertex,
@@ -1984,6 +2094,71 @@ int cismgpu_solver_assemble_stiffness_2d(cismgpu_solver_t *h, int nz, int nhalo,
                                          double effstrain_min, double n_glen, double *efvs) {
     return solver_assemble(h, false, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel_2d, vvel_2d, nullptr,
                            stagthck, flwafact, 1, whichefvs, efvs_constant, effstrain_min, n_glen, efvs);
+}
+
+int cismgpu_dirichlet_boundary_conditions_3d(int nx, int ny, int nz, int nhalo, const int32_t *active_vertex,
+                                             const int32_t *umask_dirichlet, const int32_t *vmask_dirichlet,
+                                             const double *uvel, const double *vvel, const int32_t *indxA_3d,
+                                             double *Auu, double *Auv, double *Avu, double *Avv, double *bu,
+                                             double *bv) {
+    return oneshot_boundary3d(0, nx, ny, nz, nhalo, 0.0, 0.0, active_vertex, nullptr, nullptr, umask_dirichlet,
+                              vmask_dirichlet, uvel, vvel, indxA_3d, Auu, Auv, Avu, Avv, bu, bv);
+}
+
+int cismgpu_basal_sliding_bc_3d(int nx, int ny, int nz, int nhalo, double dx, double dy,
+                                const int32_t *active_vertex, const double *beta, const double *lsrf,
+                                int whichassemble_beta, const int32_t *indxA_3d, double *Auu, double *Avv) {
+    g_last_error.clear();
+    if (whichassemble_beta != 1)
+        return fail(CISMGPU_EUNSUPPORTED, "only the local basal assembly (HO_ASSEMBLE_BETA_LOCAL) is built");
+    return oneshot_boundary3d(1, nx, ny, nz, nhalo, dx, dy, active_vertex, beta, lsrf, nullptr, nullptr, nullptr,
+                              nullptr, indxA_3d, Auu, nullptr, nullptr, Avv, nullptr, nullptr);
+}
+
+int cismgpu_solver_assemble_system_3d(cismgpu_solver_t *h, int nhalo, double dx, double dy, const double *sigma,
+                                      const int32_t *active_cell, const int32_t *active_vertex,
+                                      const double *xVertex, const double *yVertex, const double *stagusrf,
+                                      const double *stagthck, const double *flwafact, int whichapprox,
+                                      int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
+                                      const double *beta, const double *lsrf, const double *loadu,
+                                      const double *loadv, const int32_t *umask_dirichlet,
+                                      const int32_t *vmask_dirichlet, double *efvs) {
+    g_last_error.clear();
+    if (!h) return fail(CISMGPU_EINVAL, "null argument");
+    if (!active_vertex || !loadu || !loadv || (!beta) != (!lsrf) || (!umask_dirichlet) != (!vmask_dirichlet))
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    // the stiffness blocks from the handle's current velocity (takes and releases the lock)
+    TRY(cismgpu_solver_assemble_stiffness_3d(h, nhalo, sigma, active_cell, xVertex, yVertex, nullptr, nullptr,
+                                             stagusrf, stagthck, flwafact, whichapprox, whichefvs, efvs_constant,
+                                             effstrain_min, n_glen, efvs));
+    std::lock_guard<std::mutex> lk(h->mu);
+    Solver &sv = h->sv;
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = c + 1;
+    L.n = sv.nvec;
+    L.NQ = sv.g.NQ;
+    L.nz = sv.g.nz;
+    L.raw3 = 0;
+    const size_t bs = (size_t)27 * sv.nvec;
+    double *A0 = sv.A.as<double>();
+    const Ptrs p = sv.ptrs();
+    TRY(sv.put_vec(VB_U, loadu));  // bu = loadu, bv = loadv (:2868-2869)
+    TRY(sv.put_vec(VB_V, loadv));
+    TRY(sv.boundary3d(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, p.bu, p.bv, VecIdx{sv.g.NQ, sv.g.nz, 1}, nhalo, dx,
+                      dy, active_vertex, beta, lsrf, umask_dirichlet, vmask_dirichlet, nullptr, nullptr,
+                      sv.x_current ? VX_U : VX0_U));
+    // staggered_parallel_halo of the four blocks (every (m, k) plane) and of b (:2893-2904)
+    Geom gA = sv.g;
+    gA.nz = 27 * sv.g.nz;
+    const unsigned hb = nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4));
+    cudaStream_t s = sv.stream;
+    k_halo<<<hb, kBlock, 0, s>>>(gA, A0, A0 + bs, nullptr);
+    k_halo<<<hb, kBlock, 0, s>>>(gA, A0 + 2 * bs, A0 + 3 * bs, nullptr);
+    k_halo<<<hb, kBlock, 0, s>>>(sv.g, p.bu, p.bv, nullptr);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(s));
+    sv.mixed.stale = true;
+    return CISMGPU_OK;
 }
 
 int cismgpu_solver_check_symmetry(cismgpu_solver_t *h, double *maxdiff, long long *nwarn) {

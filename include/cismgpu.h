@@ -278,6 +278,29 @@ int cismgpu_assemble_stiffness_matrix_2d(int nx, int ny, int nz, int nhalo, cons
                                          double effstrain_min, double n_glen, const int32_t *indxA_2d, double *efvs,
                                          double *Auu, double *Auv, double *Avu, double *Avv);
 
+/* Replaces dirichlet_boundary_conditions_3d (glissade_velo_higher.F90:9305-9498): at every
+ * active vertex j = nhalo..ny-nhalo+1, i = nhalo..nx-nhalo+1, level k, with umask_dirichlet = 1
+ * (then likewise vmask_dirichlet), b = uvel (vvel), a unit diagonal, the row zeroed, and the
+ * column moved into the right-hand side of each neighbour not prescribed in that component.
+ * Masks (nz,nx-1,ny-1) int32; velocities and b (nz,nx-1,ny-1); A** (27,nz,nx-1,ny-1) through
+ * indxA_3d.  Right-hand-side moves are summed in the reference's order of the prescribed nodes,
+ * so the result is the reference's bit for bit. */
+int cismgpu_dirichlet_boundary_conditions_3d(int nx, int ny, int nz, int nhalo, const int32_t *active_vertex,
+                                             const int32_t *umask_dirichlet, const int32_t *vmask_dirichlet,
+                                             const double *uvel, const double *vvel, const int32_t *indxA_3d,
+                                             double *Auu, double *Auv, double *Avu, double *Avv, double *bu,
+                                             double *bv);
+
+/* Replaces basal_sliding_bc_3d (glissade_velo_higher.F90:8815-9129) for
+ * whichassemble_beta = HO_ASSEMBLE_BETA_LOCAL (1, CISM's default; the standard finite-element
+ * form returns CISMGPU_EUNSUPPORTED): at every active vertex the bed diagonal (level nz) of Auu
+ * and Avv gains dx*dy/vol0 * beta / cos(theta), theta the slope angle of the lower surface
+ * lsrf(nx,ny) staggered to the vertices (glissade_stagger, glissade_slope_angle).  beta
+ * (nx-1,ny-1); Auu, Avv the full (27,nz,nx-1,ny-1) blocks.  atan and cos are CUDA's. */
+int cismgpu_basal_sliding_bc_3d(int nx, int ny, int nz, int nhalo, double dx, double dy,
+                                const int32_t *active_vertex, const double *beta, const double *lsrf,
+                                int whichassemble_beta, const int32_t *indxA_3d, double *Auu, double *Avv);
+
 /* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps
@@ -424,6 +447,21 @@ int cismgpu_solver_assemble_stiffness_3d(cismgpu_solver_t *s, int nhalo, const d
                                          const double *stagthck, const double *flwafact, int whichapprox,
                                          int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
                                          double *efvs);
+/* One Picard iteration's 3D system on the device, as glissade_velo_higher_solve builds it
+ * (glissade_velo_higher.F90:2829-2904): the stiffness blocks from the handle's current velocity,
+ * the local basal term (beta, lsrf; both NULL for a no-slip bed), b = the load vector
+ * (loadu, loadv), the Dirichlet conditions (masks NULL: none) with the current velocity as the
+ * prescribed values, and the staggered halo of A and b.  Only the 2D fields, the flow factor,
+ * the load and the masks cross PCIe; A is built in HBM. */
+int cismgpu_solver_assemble_system_3d(cismgpu_solver_t *s, int nhalo, double dx, double dy, const double *sigma,
+                                      const int32_t *active_cell, const int32_t *active_vertex,
+                                      const double *xVertex, const double *yVertex, const double *stagusrf,
+                                      const double *stagthck, const double *flwafact, int whichapprox,
+                                      int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
+                                      const double *beta, const double *lsrf, const double *loadu,
+                                      const double *loadv, const int32_t *umask_dirichlet,
+                                      const int32_t *vmask_dirichlet, double *efvs);
+
 /* The 2D (SSA) assembly into a 2D handle; nz: the number of sigma levels of flwafact. */
 int cismgpu_solver_assemble_stiffness_2d(cismgpu_solver_t *s, int nz, int nhalo, const double *sigma,
                                          const int32_t *active_cell, const double *xVertex, const double *yVertex,

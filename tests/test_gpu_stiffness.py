@@ -211,3 +211,94 @@ def test_ssa_assembly_on_handle(gpu_lib):
     assert l2 == want[2]
     dx = cg.assemble_stiffness_matrix_2d(*args, xs[0], xs[1], g["stagthck"], ff)
     np.testing.assert_array_equal(efvs_x, dx[0])
+
+
+# ---------------------------------------------------------------------------
+# Boundary terms and the whole 3D system of one Picard iteration (:2829-2904)
+# ---------------------------------------------------------------------------
+
+def _masks(g, seed=9):
+    from tests.test_oracle_bc import no_slip_mask
+    rng = np.random.default_rng(seed)
+    m = no_slip_mask(g)
+    um, vm = m.copy(), m.copy()
+    um[rng.random(um.shape) < 0.05] = 1
+    vm[rng.random(vm.shape) < 0.05] = 1
+    return um, vm
+
+
+def test_dirichlet_bitexact(gpu_lib):
+    g = geometry(seed=61)
+    S = asm.assemble_bp_3d(g["thck"], g["usrf"], g["dx"], g["dx"], g["nz"], stiffness_only=True)
+    um, vm = _masks(g)
+    rng = np.random.default_rng(2)
+    x = (rng.standard_normal(S.bu.shape), rng.standard_normal(S.bv.shape))
+    want = oracle.dirichlet_3d(g["nx"], g["ny"], g["nz"], g["av"], um, vm, x[0], x[1], S.Auu, S.Auv, S.Avu, S.Avv,
+                               S.bu, S.bv)
+    got = [np.array(a, copy=True) for a in (S.Auu, S.Auv, S.Avu, S.Avv, S.bu, S.bv)]
+    cg.dirichlet_boundary_conditions_3d(g["nx"], g["ny"], g["nz"], 2, g["av"], um, vm, x[0], x[1], *got)
+    for a, b in zip(got, want):
+        np.testing.assert_array_equal(a, b)
+
+
+def test_basal_local(gpu_lib):
+    """atan and cos are CUDA's: the bed diagonals within 1e-15 of their size, the rest exact."""
+    g = geometry(seed=62)
+    S = asm.assemble_bp_3d(g["thck"], g["usrf"], g["dx"], g["dx"], g["nz"], stiffness_only=True)
+    lsrf = g["usrf"] - g["thck"] + 5.0 * np.random.default_rng(3).random(g["thck"].shape)
+    beta = asm.lognormal_beta((g["ny"] - 1, g["nx"] - 1), 5)
+    wu, wv, _ = oracle.basal_local_3d(g["nx"], g["ny"], g["nz"], g["dx"], g["dx"], g["av"], beta, lsrf, S.Auu, S.Avv)
+    Auu, Avv = np.array(S.Auu, copy=True), np.array(S.Avv, copy=True)
+    cg.basal_sliding_bc_3d(g["nx"], g["ny"], g["nz"], 2, g["dx"], g["dx"], g["av"], beta, lsrf, Auu, Avv)
+    for a, b in ((Auu, wu), (Avv, wv)):
+        d = np.abs(a - b)
+        assert d[..., g["nz"] - 1, 13].max() <= 1e-15 * np.abs(b[..., g["nz"] - 1, 13]).max()
+        d[..., g["nz"] - 1, 13] = 0.0
+        assert np.all(d == 0.0)
+    with pytest.raises(cg.CismGpuError):
+        cg.basal_sliding_bc_3d(g["nx"], g["ny"], g["nz"], 2, g["dx"], g["dx"], g["av"], beta, lsrf, Auu, Avv,
+                               whichassemble_beta=0)
+
+
+@pytest.mark.parametrize("bed", ["beta", "no-slip"])
+def test_system_on_handle(gpu_lib, bed):
+    """cismgpu_solver_assemble_system_3d equals the one-shot calls in the reference's sequence
+    (stiffness, basal term, b = load, Dirichlet, staggered halo) bit for bit, seen through the
+    residual of the resident system; against the oracle's sequence within the pow/atan/cos bar."""
+    g = geometry(seed=63)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    P = _slab_problem(g)
+    u, v, ff = inputs(g, scale=10.0)
+    lsrf = g["usrf"] - g["thck"]
+    beta = asm.lognormal_beta((ny - 1, nx - 1), 7) if bed == "beta" else None
+    um, vm = _masks(g) if bed == "no-slip" else (None, None)
+    load = (np.array(P.bu, copy=True), np.array(P.bv, copy=True))
+    geo = (g["sigma"], g["ac"].astype(np.int32), g["av"].astype(np.int32), g["xVertex"], g["yVertex"], g["stagusrf"],
+           g["stagthck"], ff)
+    s = cg.DeviceSolver(P, x0=(u, v))
+    try:
+        efvs_h = s.assemble_system(2, g["dx"], g["dx"], *geo, load[0], load[1], beta=beta, lsrf=lsrf, umask=um,
+                                   vmask=vm)
+        ru, rv, l2, _ = s.residual_vector()
+    finally:
+        s.close()
+    # the same sequence through the one-shot calls
+    efvs, *A = cg.assemble_stiffness_matrix_3d(nx, ny, nz, 2, g["sigma"], g["ac"].astype(np.int32), g["xVertex"],
+                                               g["yVertex"], u, v, g["stagusrf"], g["stagthck"], ff)
+    np.testing.assert_array_equal(efvs_h, efvs)
+    bu, bv = np.array(load[0], copy=True), np.array(load[1], copy=True)
+    if beta is not None:
+        cg.basal_sliding_bc_3d(nx, ny, nz, 2, g["dx"], g["dx"], g["av"], beta, lsrf, A[0], A[3])
+    if um is not None:
+        cg.dirichlet_boundary_conditions_3d(nx, ny, nz, 2, g["av"], um, vm, u, v, *A, bu, bv)
+    Q = _slab_problem(g)
+    from tests import problems
+    for n, a in zip(BLOCKS, A):
+        setattr(Q, n, a)
+    Q.bu, Q.bv = bu, bv
+    Q = problems.halo_blocks_3d(Q)
+    want = cg.compute_residual_vector_3d(nx, ny, nz, Q.par, asm.indxA_3d(), Q.active_vertex, Q.Auu, Q.Auv, Q.Avu,
+                                         Q.Avv, Q.bu, Q.bv, u, v)
+    np.testing.assert_array_equal(ru, want[0])
+    np.testing.assert_array_equal(rv, want[1])
+    assert l2 == want[2]
