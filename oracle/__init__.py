@@ -72,6 +72,10 @@ def lib() -> ctypes.CDLL:
         L.oracle_dirichlet_3d.restype = None
         L.oracle_basal_local_3d.argtypes = [i, i, i, dbl, dbl, d, d, d, d, d, d]
         L.oracle_basal_local_3d.restype = None
+        L.oracle_dirichlet_2d.argtypes = [i, i, i, d, d, d, d, d, d, d, d, d, d, d]
+        L.oracle_dirichlet_2d.restype = None
+        L.oracle_basal_local_2d.argtypes = [i, i, dbl, dbl, d, d, d, d]
+        L.oracle_basal_local_2d.restype = None
         L.oracle_check_symmetry.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, P(dbl), P(ctypes.c_long)]
         L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
@@ -263,6 +267,25 @@ def basal_local_3d(nx, ny, nz, dx, dy, active_vertex, beta, lsrf, Auu, Avv):
                                 _p(np.ascontiguousarray(beta, dtype=np.float64)),
                                 _p(np.ascontiguousarray(lsrf, dtype=np.float64)), _p(out[0]), _p(out[1]), _p(theta))
     return out[0], out[1], theta
+
+
+def dirichlet_2d(nx, ny, active_vertex, umask, vmask, uvel, vvel, Auu, Auv, Avu, Avv, bu, bv, nhalo=2):
+    """dirichlet_boundary_conditions_2d (glissade_velo_higher.F90:9133-9301) on copies: masks,
+    velocities and b (ny-1, nx-1), blocks (9, ny-1, nx-1).  Returns (Auu, Auv, Avu, Avv, bu, bv)."""
+    out = [np.array(a, dtype=np.float64, copy=True) for a in (Auu, Auv, Avu, Avv, bu, bv)]
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    lib().oracle_dirichlet_2d(nx, ny, nhalo, _p(i32(active_vertex)), _p(i32(umask)), _p(i32(vmask)), _p(f64(uvel)),
+                              _p(f64(vvel)), *[_p(a) for a in out])
+    return tuple(out)
+
+
+def basal_local_2d(nx, ny, dx, dy, active_vertex, beta, Auu, Avv):
+    """basal_sliding_bc_2d with HO_ASSEMBLE_BETA_LOCAL on copies; returns (Auu, Avv)."""
+    out = [np.array(a, dtype=np.float64, copy=True) for a in (Auu, Avv)]
+    lib().oracle_basal_local_2d(nx, ny, float(dx), float(dy), _p(np.ascontiguousarray(active_vertex, dtype=np.int32)),
+                                _p(np.ascontiguousarray(beta, dtype=np.float64)), _p(out[0]), _p(out[1]))
+    return out[0], out[1]
 
 
 def reprosum(a) -> float:

@@ -527,3 +527,81 @@ void oracle_basal_local_3d(int nx, int ny, int nz, double dx, double dy, const i
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Boundary terms of the 2D system (glissade_velo_higher.F90:2590-2660)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+// dirichlet_boundary_conditions_2d (:9133-9301), loop for loop: offsets jA, iA outermost, then
+// vertices j = nhalo..ny-nhalo+1, i = nhalo..nx-nhalo+1 that are active; a u-prescribed vertex
+// sets its diagonals Auu, Auv and Avu to 1 (the 2D routine's choice), a v-prescribed one Auv
+// and Avu to 0 and Avv to 1.  Masks (nx-1,ny-1) int32; A** (nx-1,ny-1,9).
+void oracle_dirichlet_2d(int nx, int ny, int nhalo, const int32_t *active_vertex, const int32_t *umask,
+                         const int32_t *vmask, const double *uvel, const double *vvel, double *Auu, double *Auv,
+                         double *Avu, double *Avv, double *bu, double *bv) {
+    const long NX = nx - 1, NQ = NX * (ny - 1);
+    auto V = [&](int i, int j) { return (long)(i - 1) + NX * (j - 1); };
+    auto A = [&](int i, int j, int m) { return V(i, j) + NQ * (m - 1); };
+    auto M = [](int iA, int jA) { return 1 + (iA + 1) + 3 * (jA + 1); };
+    for (int jA = -1; jA <= 1; ++jA)
+        for (int iA = -1; iA <= 1; ++iA) {
+            const int m = M(iA, jA), mm = M(-iA, -jA);
+            for (int j = nhalo; j <= ny - nhalo + 1; ++j)
+                for (int i = nhalo; i <= nx - nhalo + 1; ++i) {
+                    if (!active_vertex[V(i, j)]) continue;
+                    for (int pass = 0; pass < 2; ++pass) {
+                        if ((pass == 0 ? umask : vmask)[V(i, j)] != 1) continue;
+                        const double x = pass == 0 ? uvel[V(i, j)] : vvel[V(i, j)];
+                        (pass == 0 ? bu : bv)[V(i, j)] = x;
+                        if (!(i + iA >= 1 && i + iA <= nx - 1 && j + jA >= 1 && j + jA <= ny - 1)) continue;
+                        if (iA == 0 && jA == 0) {
+                            const long d = A(i, j, M(0, 0));
+                            if (pass == 0) {
+                                Auu[d] = 1.0;
+                                Auv[d] = 1.0;
+                                Avu[d] = 1.0;
+                            } else {
+                                Auv[d] = 0.0;
+                                Avu[d] = 0.0;
+                                Avv[d] = 1.0;
+                            }
+                            continue;
+                        }
+                        const long a = A(i, j, m);
+                        if (pass == 0) {
+                            Auu[a] = 0.0;
+                            Auv[a] = 0.0;
+                        } else {
+                            Avu[a] = 0.0;
+                            Avv[a] = 0.0;
+                        }
+                        const long e = V(i + iA, j + jA), b = A(i + iA, j + jA, mm);
+                        double *Au = pass == 0 ? Auu : Auv, *Av = pass == 0 ? Avu : Avv;
+                        if (umask[e] != 1) {
+                            bu[e] = bu[e] - Au[b] * x;
+                            Au[b] = 0.0;
+                        }
+                        if (vmask[e] != 1) {
+                            bv[e] = bv[e] - Av[b] * x;
+                            Av[b] = 0.0;
+                        }
+                    }
+                }
+        }
+}
+
+// basal_sliding_bc_2d (:8281-8531), HO_ASSEMBLE_BETA_LOCAL: at every active vertex the
+// diagonal of Auu and Avv += (dx*dy/vol0) * beta.
+void oracle_basal_local_2d(int nx, int ny, double dx, double dy, const int32_t *active_vertex, const double *beta,
+                           double *Auu, double *Avv) {
+    const long NQ = (long)(nx - 1) * (ny - 1);
+    for (long q = 0; q < NQ; ++q) {
+        if (!active_vertex[q]) continue;
+        const double increment = (dx * dy / kVol0) * beta[q];
+        Auu[q + 4 * NQ] = Auu[q + 4 * NQ] + increment;
+        Avv[q + 4 * NQ] = Avv[q + 4 * NQ] + increment;
+    }
+}
+
+}  // extern "C"

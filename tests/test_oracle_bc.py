@@ -111,3 +111,71 @@ def test_basal_local_theta_and_diagonal():
     assert np.all(d == 0.0)  # nothing else changes
     np.testing.assert_array_equal(Auu[..., g["nz"] - 1, 13] - S.Auu[..., g["nz"] - 1, 13],
                                   Avv[..., g["nz"] - 1, 13] - S.Avv[..., g["nz"] - 1, 13])
+
+
+# ---------------------------------------------------------------------------
+# 2D: dirichlet_boundary_conditions_2d (:9133-9301), basal_sliding_bc_2d local (:8281-8531)
+# ---------------------------------------------------------------------------
+
+def _ssa(g):
+    return asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], np.zeros((g["ny"] - 1, g["nx"] - 1)),
+                               stiffness_only=True)
+
+
+def test_dirichlet_2d_prescribed_values_keep_the_residual():
+    g = geometry(seed=54)
+    S = _ssa(g)
+    rng = np.random.default_rng(10)
+    m = (rng.random(S.bu.shape) < 0.1).astype(np.int32) * g["av"].astype(np.int32)
+    x = (rng.standard_normal(S.bu.shape), rng.standard_normal(S.bv.shape))
+    out = oracle.dirichlet_2d(g["nx"], g["ny"], g["av"], m, m, x[0], x[1], S.Auu, S.Auv, S.Avu, S.Avv, S.bu, S.bv)
+    P1 = asm.Problem("2d", S.nx, S.ny, 1, *out, S.active_vertex, S.par)
+    r0 = [a - b for a, b in zip(oracle.matvec(S, *x), (S.bu, S.bv))]
+    r1 = [a - b for a, b in zip(oracle.matvec(P1, *x), out[4:])]
+    p = S.par
+    own = np.zeros(S.bu.shape, dtype=bool)
+    own[p["staggered_jlo"] - 1:p["staggered_jhi"], p["staggered_ilo"] - 1:p["staggered_ihi"]] = True
+    act = own & S.active_vertex.astype(bool)
+    for a, b in zip(r0, r1):
+        assert np.all(b[act & (m == 1)] == 0.0)
+        free = act & (m != 1)
+        assert np.abs(a[free] - b[free]).max() <= 1e-9 * np.abs(a[free]).max()
+    assert np.any(m[act] == 1)
+
+
+def test_dirichlet_2d_diagonals():
+    """A u-only prescribed vertex gets unit Auu, Auv and Avu diagonals, a v-only one zero Auv
+    and Avu and a unit Avv; with both, Auu = Avv = 1 and Auv = Avu = 0."""
+    g = geometry(seed=55)
+    S = _ssa(g)
+    av = g["av"].astype(bool)
+    J, I = np.nonzero(av[2:-2, 2:-2])
+    pts = [(J[n] + 2, I[n] + 2) for n in (0, len(J) // 2, len(J) - 1)]
+    um = np.zeros(S.bu.shape, np.int32)
+    vm = np.zeros(S.bu.shape, np.int32)
+    (ju, iu), (jv, iv), (jb, ib) = pts
+    um[ju, iu] = 1
+    vm[jv, iv] = 1
+    um[jb, ib] = vm[jb, ib] = 1
+    z = np.zeros(S.bu.shape)
+    Auu, Auv, Avu, Avv, bu, bv = oracle.dirichlet_2d(g["nx"], g["ny"], g["av"], um, vm, z, z, S.Auu, S.Auv, S.Avu,
+                                                     S.Avv, S.bu, S.bv)
+    assert (Auu[4, ju, iu], Auv[4, ju, iu], Avu[4, ju, iu]) == (1.0, 1.0, 1.0)
+    assert Avv[4, ju, iu] == S.Avv[4, ju, iu]
+    assert (Auv[4, jv, iv], Avu[4, jv, iv], Avv[4, jv, iv]) == (0.0, 0.0, 1.0)
+    assert (Auu[4, jb, ib], Auv[4, jb, ib], Avu[4, jb, ib], Avv[4, jb, ib]) == (1.0, 0.0, 0.0, 1.0)
+    for m in range(9):
+        if m != 4:
+            assert Auu[m, ju, iu] == Auv[m, ju, iu] == 0.0
+            assert Avu[m, jv, iv] == Avv[m, jv, iv] == 0.0
+
+
+def test_basal_local_2d():
+    g = geometry(seed=56)
+    S = _ssa(g)
+    beta = asm.lognormal_beta((g["ny"] - 1, g["nx"] - 1), 6)
+    Auu, Avv = oracle.basal_local_2d(g["nx"], g["ny"], g["dx"], g["dx"], g["av"], beta, S.Auu, S.Avv)
+    inc = np.where(g["av"].astype(bool), (g["dx"] * g["dx"] / 1.0e9) * beta, 0.0)
+    np.testing.assert_array_equal(Auu[4], S.Auu[4] + inc)
+    np.testing.assert_array_equal(Avv[4], S.Avv[4] + inc)
+    np.testing.assert_array_equal(np.delete(Auu, 4, axis=0), np.delete(S.Auu, 4, axis=0))
