@@ -31,6 +31,7 @@ __all__ = [
     "compute_residual_vector_2d", "compute_residual_velocity_3d", "compute_residual_velocity_2d",
     "check_symmetry_assembled_matrix_3d", "check_symmetry_assembled_matrix_2d", "assemble_stiffness_matrix_3d",
     "assemble_stiffness_matrix_2d", "dirichlet_boundary_conditions_3d", "basal_sliding_bc_3d",
+    "dirichlet_boundary_conditions_2d", "basal_sliding_bc_2d",
 ]
 
 ALG_STANDARD, ALG_CHRONGEAR, ALG_MIXED_CHRONGEAR = 0, 1, 2
@@ -192,6 +193,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_basal_sliding_bc_3d.argtypes = [i32, i32, i32, i32, dbl, dbl, d, d, d, i32, d, d, d]
     lib.cismgpu_solver_assemble_system_3d.argtypes = [vp, i32, dbl, dbl, d, d, d, d, d, d, d, d, i32, i32, dbl, dbl,
                                                       dbl, d, d, d, d, d, d, d]
+    lib.cismgpu_dirichlet_boundary_conditions_2d.argtypes = [i32, i32, i32, d, d, d, d, d, d, d, d, d, d, d, d]
+    lib.cismgpu_basal_sliding_bc_2d.argtypes = [i32, i32, i32, dbl, dbl, d, d, i32, d, d, d]
+    lib.cismgpu_solver_assemble_system_2d.argtypes = [vp, i32, i32, dbl, dbl, d, d, d, d, d, d, d, i32, dbl, dbl, dbl,
+                                                      d, d, d, d, d, d]
     for f in ("cismgpu_compute_residual_vector_3d", "cismgpu_compute_residual_vector_2d",
               "cismgpu_compute_residual_velocity_3d", "cismgpu_compute_residual_velocity_2d",
               "cismgpu_solver_set_system", "cismgpu_solver_residual_vector", "cismgpu_solver_residual_velocity",
@@ -200,7 +205,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
               "cismgpu_assemble_stiffness_matrix_3d", "cismgpu_solver_assemble_stiffness_3d",
               "cismgpu_assemble_stiffness_matrix_2d", "cismgpu_solver_assemble_stiffness_2d",
               "cismgpu_dirichlet_boundary_conditions_3d", "cismgpu_basal_sliding_bc_3d",
-              "cismgpu_solver_assemble_system_3d"):
+              "cismgpu_solver_assemble_system_3d", "cismgpu_dirichlet_boundary_conditions_2d",
+              "cismgpu_basal_sliding_bc_2d", "cismgpu_solver_assemble_system_2d"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -522,6 +528,32 @@ def basal_sliding_bc_3d(nx, ny, nz, nhalo, dx, dy, active_vertex, beta, lsrf, Au
         _ptr(Auu, np.float64, 27 * nv * nz, True), _ptr(Avv, np.float64, 27 * nv * nz, True)))
 
 
+def dirichlet_boundary_conditions_2d(nx, ny, nhalo, active_vertex, umask, vmask, uvel, vvel, Auu, Auv, Avu, Avv,
+                                     bu, bv, indxA_2d=None):
+    """Mirrors dirichlet_boundary_conditions_2d (glissade_velo_higher.F90:9133-9301) on the GPU,
+    in place on the (9, ny-1, nx-1) blocks and b."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    indx = np.arange(1, 10, dtype=np.int32) if indxA_2d is None else np.ascontiguousarray(indxA_2d, dtype=np.int32)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    _check(lib, lib.cismgpu_dirichlet_boundary_conditions_2d(
+        nx, ny, int(nhalo), _ptr(i32(active_vertex), np.int32, nv), _ptr(i32(umask), np.int32, nv),
+        _ptr(i32(vmask), np.int32, nv), _ptr(uvel, np.float64, nv), _ptr(vvel, np.float64, nv), _ptr(indx, np.int32, 9),
+        *[_ptr(a, np.float64, 9 * nv, True) for a in (Auu, Auv, Avu, Avv)], _ptr(bu, np.float64, nv, True),
+        _ptr(bv, np.float64, nv, True)))
+
+
+def basal_sliding_bc_2d(nx, ny, nhalo, dx, dy, active_vertex, beta, Auu, Avv, whichassemble_beta=1, indxA_2d=None):
+    """Mirrors basal_sliding_bc_2d (glissade_velo_higher.F90:8281-8531), local form, in place."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    indx = np.arange(1, 10, dtype=np.int32) if indxA_2d is None else np.ascontiguousarray(indxA_2d, dtype=np.int32)
+    _check(lib, lib.cismgpu_basal_sliding_bc_2d(
+        nx, ny, int(nhalo), float(dx), float(dy), _ptr(np.ascontiguousarray(active_vertex, dtype=np.int32), np.int32, nv),
+        _ptr(beta, np.float64, nv), int(whichassemble_beta), _ptr(indx, np.int32, 9), _ptr(Auu, np.float64, 9 * nv, True),
+        _ptr(Avv, np.float64, 9 * nv, True)))
+
+
 class DeviceSolver:
     """A device-resident linear system (cismgpu_solver_create): A, b and x0 live in HBM.
 
@@ -630,10 +662,15 @@ class DeviceSolver:
     def assemble_system(self, nhalo, dx, dy, sigma, active_cell, active_vertex, xVertex, yVertex, stagusrf,
                         stagthck, flwafact, loadu, loadv, beta=None, lsrf=None, umask=None, vmask=None,
                         whichapprox=2, whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8, n_glen=3.0):
-        """One Picard iteration's 3D system on the device (cismgpu_solver_assemble_system_3d):
+        """One Picard iteration's system on the device (cismgpu_solver_assemble_system_3d / _2d):
         stiffness from the current velocity, local basal term, b = load, Dirichlet conditions,
-        staggered halo.  Returns efvs (ny, nx, nz-1)."""
+        staggered halo.  2D handles: stagusrf and lsrf unused, masks (ny-1, nx-1).  Returns efvs
+        (ny, nx, nz-1)."""
         P = self.problem
+        if P.kind != "3d":
+            return self._assemble_system_2d(nhalo, dx, dy, sigma, active_cell, active_vertex, xVertex, yVertex,
+                                            stagthck, flwafact, loadu, loadv, beta, umask, vmask, whichefvs,
+                                            efvs_constant, effstrain_min, n_glen)
         nx, ny, nz = P.nx, P.ny, P.nz
         nv = (nx - 1) * (ny - 1)
         efvs = np.zeros((ny, nx, nz - 1))
@@ -647,6 +684,24 @@ class DeviceSolver:
             head[3], *tail, int(whichapprox), int(whichefvs), float(efvs_constant), float(effstrain_min),
             float(n_glen), *pb, _ptr(loadu, np.float64, nv * nz), _ptr(loadv, np.float64, nv * nz), *pm,
             _ptr(efvs, np.float64, efvs.size, True)))
+        return efvs
+
+    def _assemble_system_2d(self, nhalo, dx, dy, sigma, active_cell, active_vertex, xVertex, yVertex, stagthck,
+                            flwafact, loadu, loadv, beta, umask, vmask, whichefvs, efvs_constant, effstrain_min,
+                            n_glen):
+        P = self.problem
+        nx, ny, nz = P.nx, P.ny, len(sigma)
+        nv = (nx - 1) * (ny - 1)
+        efvs = np.zeros((ny, nx, nz - 1))
+        head, tail = _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagthck, stagthck, flwafact)
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        keep = [i32(active_vertex)] + ([i32(umask), i32(vmask)] if umask is not None else [])
+        pm = (_ptr(keep[1], np.int32, nv), _ptr(keep[2], np.int32, nv)) if umask is not None else (None, None)
+        pb = _ptr(beta, np.float64, nv) if beta is not None else None
+        _check(self._lib, self._lib.cismgpu_solver_assemble_system_2d(
+            self.handle, nz, int(nhalo), float(dx), float(dy), head[0], head[1], _ptr(keep[0], np.int32, nv), head[2],
+            head[3], tail[1], tail[2], int(whichefvs), float(efvs_constant), float(effstrain_min), float(n_glen), pb,
+            _ptr(loadu, np.float64, nv), _ptr(loadv, np.float64, nv), *pm, _ptr(efvs, np.float64, efvs.size, True)))
         return efvs
 
     def save(self):

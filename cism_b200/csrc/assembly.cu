@@ -501,4 +501,108 @@ __global__ void __launch_bounds__(kBlock) k_basal_local3d(int nx, int ny, int nz
     Avv[a] = Avv[a] + add;
 }
 
+// ---------------------------------------------------------------------------
+// Boundary terms of the 2D system (glissade_velo_higher.F90:2590-2660)
+// ---------------------------------------------------------------------------
+// dirichlet_boundary_conditions_2d (:9133-9301), one thread per vertex P.  The reference loops
+// over the offsets (jA, iA) outermost and the prescribed vertices R inside, so the moves into
+// b(P) come in the order of the offset P - R (jA, then iA), u before v for each R; every write
+// lands in row P or b(P) as in 3D.  A u-prescribed vertex's own diagonals Auu, Auv, Avu become
+// 1 (the 2D routine's rule), a v-prescribed one's Auv, Avu 0 and Avv 1, u before v.  Masks,
+// velocities and b in the (nx-1, ny-1) layout; blocks in layout L (NC = 9).
+__global__ void __launch_bounds__(kBlock) k_dirichlet2d(int nx, int ny, int nhalo, SymIdx L,
+                                                        const int32_t *__restrict__ active_vertex,
+                                                        const int32_t *__restrict__ umask,
+                                                        const int32_t *__restrict__ vmask,
+                                                        const double *__restrict__ uvel,
+                                                        const double *__restrict__ vvel, double *Auu, double *Auv,
+                                                        double *Avu, double *Avv, double *bu, double *bv) {
+    const long long NX = nx - 1, NQ = NX * (ny - 1);
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (q >= NQ) return;
+    const int j = (int)(q / NX), i = (int)(q - (long long)j * NX);  // 0-based
+    auto visited = [&](int ii, int jj) {
+        return ii >= nhalo - 1 && ii <= nx - nhalo && jj >= nhalo - 1 && jj <= ny - nhalo &&
+               active_vertex[(long long)jj * NX + ii] != 0;
+    };
+    const bool ufree = umask[q] != 1, vfree = vmask[q] != 1;
+    double b_u = bu[q], b_v = bv[q];
+    for (int jA = -1; jA <= 1; ++jA)
+        for (int iA = -1; iA <= 1; ++iA) {
+            if (iA == 0 && jA == 0) continue;
+            const int iR = i - iA, jR = j - jA;  // P = R + (iA, jA)
+            if (iR < 0 || iR >= NX || jR < 0 || jR >= ny - 1) continue;
+            if (!visited(iR, jR)) continue;
+            const long long qR = (long long)jR * NX + iR;
+            const int c = (-iA + 1) + 3 * (-jA + 1);  // row P's coupling to R
+            const long long a = L.at(c, 0, q);
+            if (umask[qR] == 1) {
+                const double x = uvel[qR];
+                if (ufree) {
+                    b_u = b_u - Auu[a] * x;
+                    Auu[a] = 0.0;
+                }
+                if (vfree) {
+                    b_v = b_v - Avu[a] * x;
+                    Avu[a] = 0.0;
+                }
+            }
+            if (vmask[qR] == 1) {
+                const double x = vvel[qR];
+                if (ufree) {
+                    b_u = b_u - Auv[a] * x;
+                    Auv[a] = 0.0;
+                }
+                if (vfree) {
+                    b_v = b_v - Avv[a] * x;
+                    Avv[a] = 0.0;
+                }
+            }
+        }
+    if (visited(i, j)) {
+        for (int pass = 0; pass < 2; ++pass) {
+            if ((pass == 0 ? umask : vmask)[q] != 1) continue;
+            if (pass == 0) b_u = uvel[q];
+            else b_v = vvel[q];
+            for (int c = 0; c < 9; ++c) {
+                const int ei = c % 3 - 1, ej = c / 3 - 1;
+                if (i + ei < 0 || i + ei >= NX || j + ej < 0 || j + ej >= ny - 1) continue;
+                const long long a = L.at(c, 0, q);
+                if (c == 4) {
+                    if (pass == 0) {
+                        Auu[a] = 1.0;
+                        Auv[a] = 1.0;
+                        Avu[a] = 1.0;
+                    } else {
+                        Auv[a] = 0.0;
+                        Avu[a] = 0.0;
+                        Avv[a] = 1.0;
+                    }
+                } else if (pass == 0) {
+                    Auu[a] = 0.0;
+                    Auv[a] = 0.0;
+                } else {
+                    Avu[a] = 0.0;
+                    Avv[a] = 0.0;
+                }
+            }
+        }
+    }
+    bu[q] = b_u;
+    bv[q] = b_v;
+}
+
+// basal_sliding_bc_2d with HO_ASSEMBLE_BETA_LOCAL (:8325-8336): at every active vertex the
+// diagonal of Auu and Avv += (dx*dy/vol0) * beta.
+__global__ void __launch_bounds__(kBlock) k_basal_local2d(long long NQ, double dx, double dy, SymIdx L,
+                                                          const int32_t *__restrict__ active_vertex,
+                                                          const double *__restrict__ beta, double *Auu, double *Avv) {
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (q >= NQ || !active_vertex[q]) return;
+    const double increment = (dx * dy / kAsmVol0) * beta[q];
+    const long long a = L.at(4, 0, q);
+    Auu[a] = Auu[a] + increment;
+    Avv[a] = Avv[a] + increment;
+}
+
 }  // namespace cismgpu

@@ -472,6 +472,50 @@ struct Solver {
         return CISMGPU_OK;
     }
 
+    // The boundary terms of the 2D system on four blocks in layout L (NC = 9) and b (NQ):
+    // the local basal term of basal_sliding_bc_2d when beta is given, then
+    // dirichlet_boundary_conditions_2d when the masks are given (:2590-2651).  Host arrays in
+    // the (nx-1, ny-1) layout; uvel = vvel = null: the velocity planes vel_id, vel_id+1.
+    // Leaves the stream synchronized.
+    int boundary2d(const SymIdx &L, double *Auu, double *Auv, double *Avu, double *Avv, double *bu, double *bv,
+                   int nhalo, double dx, double dy, const int32_t *active_vertex, const double *beta,
+                   const int32_t *umask, const int32_t *vmask, const double *uvel, const double *vvel, int vel_id) {
+        const int nx = g.NX + 1, ny = g.NY + 1;
+        const size_t nq = (size_t)g.NQ;
+        const bool host_vel = uvel != nullptr;
+        const size_t nd = nq + (host_vel ? 2 * nq : 0);  // beta, [uvel, vvel]; then active, umask, vmask
+        CU(bc_in.ensure(nd * sizeof(double) + 3 * nq * sizeof(int32_t)));
+        double *D = bc_in.as<double>();
+        double *d_beta = D, *d_u = D + nq, *d_v = d_u + nq;
+        int32_t *d_act = reinterpret_cast<int32_t *>(D + nd), *d_um = d_act + nq, *d_vm = d_um + nq;
+        cudaStream_t s = stream;
+        auto up = [&](void *dst, const void *src, size_t bytes) {
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+        };
+        CU(up(d_act, active_vertex, nq * sizeof(int32_t)));
+        if (beta) {
+            CU(up(d_beta, beta, nq * sizeof(double)));
+            k_basal_local2d<<<nblocks((long long)nq), kBlock, 0, s>>>(g.NQ, dx, dy, L, d_act, d_beta, Auu, Avv);
+            CU(cudaGetLastError());
+        }
+        if (umask) {
+            CU(up(d_um, umask, nq * sizeof(int32_t)));
+            CU(up(d_vm, vmask, nq * sizeof(int32_t)));
+            if (host_vel) {
+                CU(up(d_u, uvel, nq * sizeof(double)));
+                CU(up(d_v, vvel, nq * sizeof(double)));
+            }
+            const double *V = vec.as<double>();
+            const double *xu = host_vel ? d_u : V + (size_t)vel_id * nvec;
+            const double *xv = host_vel ? d_v : V + (size_t)(vel_id + 1) * nvec;
+            k_dirichlet2d<<<nblocks((long long)nq), kBlock, 0, s>>>(nx, ny, nhalo, L, d_act, d_um, d_vm, xu, xv, Auu,
+                                                                    Auv, Avu, Avv, bu, bv);
+            CU(cudaGetLastError());
+        }
+        CU(cudaStreamSynchronize(s));
+        return CISMGPU_OK;
+    }
+
     // The symmetry check on the resident canonical planes.
     int check_symmetry(double *maxdiff, long long *nwarn) {
         SymIdx L{};
@@ -2046,6 +2090,63 @@ static int oneshot_boundary3d(int which, int nx, int ny, int nz, int nhalo, doub
     return CISMGPU_OK;
 }
 
+// One-shot 2D boundary terms on the caller's blocks (nx-1,ny-1,9) and b.  which: 0 Dirichlet,
+// 1 local basal term.
+static int oneshot_boundary2d(int which, int nx, int ny, int nhalo, double dx, double dy,
+                              const int32_t *active_vertex, const double *beta, const int32_t *umask,
+                              const int32_t *vmask, const double *uvel, const double *vvel, const int32_t *indx,
+                              double *Auu, double *Auv, double *Avu, double *Avv, double *bu, double *bv) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_error.clear();
+    if (!active_vertex || !indx || !Auu || !Avv) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (which == 0 && (!umask || !vmask || !uvel || !vvel || !Auv || !Avu || !bu || !bv))
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (which == 1 && !beta) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (nx < 6 || ny < 6) return fail(CISMGPU_EINVAL, "grid too small");
+    if (nhalo < 1 || 2 * nhalo >= nx || 2 * nhalo >= ny) return fail(CISMGPU_EINVAL, "nhalo outside the grid");
+    TRY(validate_indx(indx, 9));
+    cismgpu_par_t par{};
+    par.staggered_ilo = 1; par.staggered_ihi = nx - 1; par.staggered_jlo = 1; par.staggered_jhi = ny - 1;
+    par.tasks_row = par.tasks_col = 1;
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
+    TRY(sv.set_geom(make_geom(nx, ny, 1, &par), false));
+    const size_t bs = (size_t)9 * sv.nvec;
+    CU(sv.A.ensure(4 * bs * sizeof(double)));
+    sv.mixed.stale = true;
+    double *A0 = sv.A.as<double>();
+    double *blk[4] = {A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs};
+    double *host[4] = {Auu, Auv, Avu, Avv};
+    cudaStream_t s = sv.stream;
+    for (int b = 0; b < 4; ++b)
+        if (which == 0 || b == 0 || b == 3)
+            CU(cudaMemcpyAsync(blk[b], host[b], bs * sizeof(double), cudaMemcpyHostToDevice, s));
+    double *V = sv.vec.as<double>();
+    double *dbu = V + (size_t)VB_U * sv.nvec, *dbv = V + (size_t)VB_V * sv.nvec;
+    if (which == 0) {
+        CU(cudaMemcpyAsync(dbu, bu, sv.nvec * sizeof(double), cudaMemcpyHostToDevice, s));
+        CU(cudaMemcpyAsync(dbv, bv, sv.nvec * sizeof(double), cudaMemcpyHostToDevice, s));
+    }
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = c < 9 ? indx[c] : 1;
+    L.n = sv.nvec;
+    L.NQ = sv.g.NQ;
+    L.nz = 1;
+    L.raw3 = 0;
+    TRY(sv.boundary2d(L, blk[0], blk[1], blk[2], blk[3], dbu, dbv, nhalo, dx, dy, active_vertex,
+                      which == 1 ? beta : nullptr, which == 0 ? umask : nullptr, vmask, uvel, vvel, 0));
+    for (int b = 0; b < 4; ++b)
+        if (which == 0 || b == 0 || b == 3)
+            CU(cudaMemcpyAsync(host[b], blk[b], bs * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (which == 0) {
+        CU(cudaMemcpyAsync(bu, dbu, sv.nvec * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CU(cudaMemcpyAsync(bv, dbv, sv.nvec * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    CU(cudaStreamSynchronize(s));
+    return CISMGPU_OK;
+}
+
 // The handle's assembly: blocks into the resident canonical planes.
 static int solver_assemble(cismgpu_solver_t *h, bool three_d, int nzl, int nhalo, const double *sigma,
                            const int32_t *active_cell, const double *xVertex, const double *yVertex,
@@ -2150,6 +2251,68 @@ int cismgpu_solver_assemble_system_3d(cismgpu_solver_t *h, int nhalo, double dx,
     // staggered_parallel_halo of the four blocks (every (m, k) plane) and of b (:2893-2904)
     Geom gA = sv.g;
     gA.nz = 27 * sv.g.nz;
+    const unsigned hb = nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4));
+    cudaStream_t s = sv.stream;
+    k_halo<<<hb, kBlock, 0, s>>>(gA, A0, A0 + bs, nullptr);
+    k_halo<<<hb, kBlock, 0, s>>>(gA, A0 + 2 * bs, A0 + 3 * bs, nullptr);
+    k_halo<<<hb, kBlock, 0, s>>>(sv.g, p.bu, p.bv, nullptr);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(s));
+    sv.mixed.stale = true;
+    return CISMGPU_OK;
+}
+
+int cismgpu_dirichlet_boundary_conditions_2d(int nx, int ny, int nhalo, const int32_t *active_vertex,
+                                             const int32_t *umask_dirichlet, const int32_t *vmask_dirichlet,
+                                             const double *uvel, const double *vvel, const int32_t *indxA_2d,
+                                             double *Auu, double *Auv, double *Avu, double *Avv, double *bu,
+                                             double *bv) {
+    return oneshot_boundary2d(0, nx, ny, nhalo, 0.0, 0.0, active_vertex, nullptr, umask_dirichlet, vmask_dirichlet,
+                              uvel, vvel, indxA_2d, Auu, Auv, Avu, Avv, bu, bv);
+}
+
+int cismgpu_basal_sliding_bc_2d(int nx, int ny, int nhalo, double dx, double dy, const int32_t *active_vertex,
+                                const double *beta, int whichassemble_beta, const int32_t *indxA_2d, double *Auu,
+                                double *Avv) {
+    g_last_error.clear();
+    if (whichassemble_beta != 1)
+        return fail(CISMGPU_EUNSUPPORTED, "only the local basal assembly (HO_ASSEMBLE_BETA_LOCAL) is built");
+    return oneshot_boundary2d(1, nx, ny, nhalo, dx, dy, active_vertex, beta, nullptr, nullptr, nullptr, nullptr,
+                              indxA_2d, Auu, nullptr, nullptr, Avv, nullptr, nullptr);
+}
+
+int cismgpu_solver_assemble_system_2d(cismgpu_solver_t *h, int nz, int nhalo, double dx, double dy,
+                                      const double *sigma, const int32_t *active_cell, const int32_t *active_vertex,
+                                      const double *xVertex, const double *yVertex, const double *stagthck,
+                                      const double *flwafact, int whichefvs, double efvs_constant,
+                                      double effstrain_min, double n_glen, const double *beta, const double *loadu,
+                                      const double *loadv, const int32_t *umask_dirichlet,
+                                      const int32_t *vmask_dirichlet, double *efvs) {
+    g_last_error.clear();
+    if (!h) return fail(CISMGPU_EINVAL, "null argument");
+    if (!active_vertex || !loadu || !loadv || (!umask_dirichlet) != (!vmask_dirichlet))
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    TRY(cismgpu_solver_assemble_stiffness_2d(h, nz, nhalo, sigma, active_cell, xVertex, yVertex, nullptr, nullptr,
+                                             stagthck, flwafact, whichefvs, efvs_constant, effstrain_min, n_glen,
+                                             efvs));
+    std::lock_guard<std::mutex> lk(h->mu);
+    Solver &sv = h->sv;
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = c + 1;
+    L.n = sv.nvec;
+    L.NQ = sv.g.NQ;
+    L.nz = 1;
+    L.raw3 = 0;
+    const size_t bs = (size_t)9 * sv.nvec;
+    double *A0 = sv.A.as<double>();
+    const Ptrs p = sv.ptrs();
+    TRY(sv.put_vec(VB_U, loadu));  // bu_2d = loadu_2d, bv_2d = loadv_2d (:2620-2621)
+    TRY(sv.put_vec(VB_V, loadv));
+    TRY(sv.boundary2d(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, p.bu, p.bv, nhalo, dx, dy, active_vertex, beta,
+                      umask_dirichlet, vmask_dirichlet, nullptr, nullptr, sv.x_current ? VX_U : VX0_U));
+    // staggered_parallel_halo of every coefficient plane and of b (:2652-2666)
+    Geom gA = sv.g;
+    gA.nz = 9;
     const unsigned hb = nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4));
     cudaStream_t s = sv.stream;
     k_halo<<<hb, kBlock, 0, s>>>(gA, A0, A0 + bs, nullptr);

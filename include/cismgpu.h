@@ -301,6 +301,21 @@ int cismgpu_basal_sliding_bc_3d(int nx, int ny, int nz, int nhalo, double dx, do
                                 const int32_t *active_vertex, const double *beta, const double *lsrf,
                                 int whichassemble_beta, const int32_t *indxA_3d, double *Auu, double *Avv);
 
+/* Replaces dirichlet_boundary_conditions_2d (glissade_velo_higher.F90:9133-9301) and, for
+ * HO_ASSEMBLE_BETA_LOCAL, basal_sliding_bc_2d (:8281-8531: the diagonal of Auu and Avv at every
+ * active vertex += (dx*dy/vol0) * beta).  Masks, velocities, beta and b (nx-1,ny-1); A**
+ * (nx-1,ny-1,9) through indxA_2d.  As in the reference's 2D routine, a u-prescribed vertex
+ * gets unit diagonals in Auu, Auv and Avu (a v-prescribed one then zero Auv, Avu and unit Avv),
+ * and the moves into b are summed in its order (offsets outermost).  Bit-exact. */
+int cismgpu_dirichlet_boundary_conditions_2d(int nx, int ny, int nhalo, const int32_t *active_vertex,
+                                             const int32_t *umask_dirichlet, const int32_t *vmask_dirichlet,
+                                             const double *uvel, const double *vvel, const int32_t *indxA_2d,
+                                             double *Auu, double *Auv, double *Avu, double *Avv, double *bu,
+                                             double *bv);
+int cismgpu_basal_sliding_bc_2d(int nx, int ny, int nhalo, double dx, double dy, const int32_t *active_vertex,
+                                const double *beta, int whichassemble_beta, const int32_t *indxA_2d, double *Auu,
+                                double *Avv);
+
 /* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps
@@ -459,6 +474,17 @@ int cismgpu_solver_assemble_system_3d(cismgpu_solver_t *s, int nhalo, double dx,
                                       const double *stagthck, const double *flwafact, int whichapprox,
                                       int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
                                       const double *beta, const double *lsrf, const double *loadu,
+                                      const double *loadv, const int32_t *umask_dirichlet,
+                                      const int32_t *vmask_dirichlet, double *efvs);
+
+/* The 2D (SSA) counterpart (glissade_velo_higher.F90:2560-2666): stiffness from the handle's
+ * current velocity, local basal term (beta NULL: none), b = load, Dirichlet (masks (nx-1,ny-1),
+ * NULL: none), staggered halo of A and b.  nz: the sigma levels of flwafact. */
+int cismgpu_solver_assemble_system_2d(cismgpu_solver_t *s, int nz, int nhalo, double dx, double dy,
+                                      const double *sigma, const int32_t *active_cell, const int32_t *active_vertex,
+                                      const double *xVertex, const double *yVertex, const double *stagthck,
+                                      const double *flwafact, int whichefvs, double efvs_constant,
+                                      double effstrain_min, double n_glen, const double *beta, const double *loadu,
                                       const double *loadv, const int32_t *umask_dirichlet,
                                       const int32_t *vmask_dirichlet, double *efvs);
 

@@ -302,3 +302,61 @@ def test_system_on_handle(gpu_lib, bed):
     np.testing.assert_array_equal(ru, want[0])
     np.testing.assert_array_equal(rv, want[1])
     assert l2 == want[2]
+
+
+def test_dirichlet_2d_and_basal_2d_bitexact(gpu_lib):
+    g = geometry(seed=71)
+    nx, ny = g["nx"], g["ny"]
+    S = asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], np.zeros((ny - 1, nx - 1)), stiffness_only=True)
+    rng = np.random.default_rng(71)
+    um = (rng.random(S.bu.shape) < 0.15).astype(np.int32)
+    vm = (rng.random(S.bu.shape) < 0.15).astype(np.int32)
+    x = (rng.standard_normal(S.bu.shape), rng.standard_normal(S.bv.shape))
+    want = oracle.dirichlet_2d(nx, ny, g["av"], um, vm, x[0], x[1], S.Auu, S.Auv, S.Avu, S.Avv, S.bu, S.bv)
+    got = [np.array(a, copy=True) for a in (S.Auu, S.Auv, S.Avu, S.Avv, S.bu, S.bv)]
+    cg.dirichlet_boundary_conditions_2d(nx, ny, 2, g["av"], um, vm, x[0], x[1], *got)
+    for a, b in zip(got, want):
+        np.testing.assert_array_equal(a, b)
+    beta = asm.lognormal_beta((ny - 1, nx - 1), 6)
+    wu, wv = oracle.basal_local_2d(nx, ny, g["dx"], g["dx"], g["av"], beta, S.Auu, S.Avv)
+    Auu, Avv = np.array(S.Auu, copy=True), np.array(S.Avv, copy=True)
+    cg.basal_sliding_bc_2d(nx, ny, 2, g["dx"], g["dx"], g["av"], beta, Auu, Avv)
+    np.testing.assert_array_equal(Auu, wu)
+    np.testing.assert_array_equal(Avv, wv)
+
+
+def test_system_2d_on_handle(gpu_lib):
+    """cismgpu_solver_assemble_system_2d equals the one-shot sequence bit for bit (residual)."""
+    g = geometry(seed=73, nz=6)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    P = asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], asm.lognormal_beta((ny - 1, nx - 1), 8))
+    u, v, ff = inputs2(g, scale=10.0)
+    beta = asm.lognormal_beta((ny - 1, nx - 1), 9)
+    rng = np.random.default_rng(3)
+    um = (rng.random(P.bu.shape) < 0.1).astype(np.int32)
+    load = (np.array(P.bu, copy=True), np.array(P.bv, copy=True))
+    s = cg.DeviceSolver(P, x0=(u, v))
+    try:
+        efvs_h = s.assemble_system(2, g["dx"], g["dx"], g["sigma"], g["ac"].astype(np.int32), g["av"].astype(np.int32),
+                                   g["xVertex"], g["yVertex"], g["stagthck"], g["stagthck"], ff, load[0], load[1],
+                                   beta=beta, umask=um, vmask=um)
+        ru, rv, l2, _ = s.residual_vector()
+    finally:
+        s.close()
+    efvs, *A = cg.assemble_stiffness_matrix_2d(nx, ny, nz, 2, g["sigma"], g["ac"].astype(np.int32), g["xVertex"],
+                                               g["yVertex"], u, v, g["stagthck"], ff)
+    np.testing.assert_array_equal(efvs_h, efvs)
+    bu, bv = np.array(load[0], copy=True), np.array(load[1], copy=True)
+    cg.basal_sliding_bc_2d(nx, ny, 2, g["dx"], g["dx"], g["av"], beta, A[0], A[3])
+    cg.dirichlet_boundary_conditions_2d(nx, ny, 2, g["av"], um, um, u, v, *A, bu, bv)
+    from tests import problems
+    Q = asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], asm.lognormal_beta((ny - 1, nx - 1), 8))
+    for n, a in zip(BLOCKS, A):
+        setattr(Q, n, a)
+    Q.bu, Q.bv = bu, bv
+    Q = problems.halo_blocks_2d(Q)
+    want = cg.compute_residual_vector_2d(nx, ny, Q.par, asm.indxA_2d(), Q.active_vertex, Q.Auu, Q.Auv, Q.Avu, Q.Avv,
+                                         Q.bu, Q.bv, u, v)
+    np.testing.assert_array_equal(ru, want[0])
+    np.testing.assert_array_equal(rv, want[1])
+    assert l2 == want[2]
