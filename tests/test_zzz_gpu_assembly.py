@@ -1,5 +1,8 @@
-"""assemble_stiffness_matrix_3d (glissade_velo_higher.F90:5382-5643) on the device, through
-the C ABI: one-shot on the caller's arrays and into a device-resident handle.
+"""The system assembly of a Picard iteration on the device, through the C ABI:
+assemble_stiffness_matrix_3d / _2d (glissade_velo_higher.F90:5382-5643, :4961-5378), the
+Dirichlet and local basal terms, and the whole 3D and 2D systems on a device-resident handle.
+The file is named to be collected last, so that a failure here under -x leaves every other
+GPU test's result in place.
 
 Bars, against the oracle's restatement on the same inputs:
   - constant and flow-factor viscosity: bit-exact blocks and efvs (no pow on the device, or
