@@ -328,8 +328,10 @@ struct Solver {
                  const double *u, const double *v, int vel_id, const double *usrf, const double *thck,
                  const double *flwafact, int whichapprox, int whichefvs, double efvs_constant,
                  double effstrain_min, double n_glen, double *efvs) {
-        static bool ref_ready = false;  // the reference elements in constant memory (:314-392, :528-570)
-        if (!ref_ready) {
+        // the reference elements in constant memory (:314-392, :528-570), once per process
+        static std::once_flag ref_once;
+        static cudaError_t ref_status = cudaSuccess;
+        std::call_once(ref_once, [] {
             AsmRef r;
             AsmRef2 r2;
             const double rs = 1.0 / std::sqrt(3.0);
@@ -357,10 +359,10 @@ struct Solver {
                     r2.dxr[p][n] = sx[n] * fy / 4.0;
                     r2.dyr[p][n] = sy[n] * fx / 4.0;
                 }
-            CU(cudaMemcpyToSymbol(c_asm_ref, &r, sizeof(r)));
-            CU(cudaMemcpyToSymbol(c_asm_ref2, &r2, sizeof(r2)));
-            ref_ready = true;
-        }
+            ref_status = cudaMemcpyToSymbol(c_asm_ref, &r, sizeof(r));
+            if (ref_status == cudaSuccess) ref_status = cudaMemcpyToSymbol(c_asm_ref2, &r2, sizeof(r2));
+        });
+        CU(ref_status);
         const int nx = g.NX + 1, ny = g.NY + 1;
         const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny, nel = (size_t)(nzl - 1) * ncell;
         const size_t nvel = three_d ? (size_t)nzl * nq : nq;

@@ -82,3 +82,44 @@ def test_status_names_match_the_header():
     text = open(os.path.join(ROOT, "include", "cismgpu.h")).read()
     codes = {int(v): n for n, v in re.findall(r"#define\s+(CISMGPU_(?:OK|E[A-Z0-9_]+))\s+(\d+)", text)}
     assert codes == cg.STATUS_NAMES
+
+
+def test_assembly_entry_points_validate_before_the_device(lib):
+    """The assembly and boundary entry points reject bad arguments with the library's status
+    (4 EINVAL, 3 EUNSUPPORTED) before any device call, so these run without a GPU."""
+    import numpy as np
+    import cism_b200 as cg
+    from tests.test_oracle_assembly import geometry
+    g = geometry(seed=81)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    u = np.zeros((ny - 1, nx - 1, nz))
+    ff = np.ones((ny, nx, nz - 1))
+    act = g["ac"].astype(np.int32)
+    base = [nx, ny, nz, 2, g["sigma"], act, g["xVertex"], g["yVertex"], u, u, g["stagusrf"], g["stagthck"], ff]
+    cases = [(3, 1, {}), (None, None, {"whichefvs": 3}), (None, None, {"n_glen": 0.0})]
+    for idx, val, kw in cases:
+        args = list(base)
+        if idx is not None:
+            args[idx] = val  # nhalo = 1
+        with pytest.raises(cg.CismGpuError) as e:
+            cg.assemble_stiffness_matrix_3d(*args, **kw)
+        assert e.value.status == 4
+    u2 = np.zeros((ny - 1, nx - 1))
+    with pytest.raises(cg.CismGpuError) as e:
+        cg.assemble_stiffness_matrix_2d(nx, ny, nz, 1, g["sigma"], act, g["xVertex"], g["yVertex"], u2, u2,
+                                        g["stagthck"], ff)
+    assert e.value.status == 4
+    A = [np.zeros((ny - 1, nx - 1, nz, 27)) for _ in range(2)]
+    with pytest.raises(cg.CismGpuError) as e:  # the standard finite-element form is not built
+        cg.basal_sliding_bc_3d(nx, ny, nz, 2, 1.0, 1.0, g["av"], np.zeros((ny - 1, nx - 1)), np.zeros((ny, nx)),
+                               *A, whichassemble_beta=0)
+    assert e.value.status == 3
+    A2 = [np.zeros((9, ny - 1, nx - 1)) for _ in range(2)]
+    with pytest.raises(cg.CismGpuError) as e:
+        cg.basal_sliding_bc_2d(nx, ny, 2, 1.0, 1.0, g["av"], np.zeros((ny - 1, nx - 1)), *A2, whichassemble_beta=0)
+    assert e.value.status == 3
+    bad = np.arange(1, 28, dtype=np.int32)
+    bad[5] = 99
+    with pytest.raises(cg.CismGpuError) as e:  # indxA entry outside 1..27
+        cg.assemble_stiffness_matrix_3d(*base, indxA_3d=bad)
+    assert e.value.status == 4
