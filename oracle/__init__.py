@@ -1,9 +1,12 @@
 """CPU oracle for the structured PCG solve -- TEST INFRASTRUCTURE ONLY.
 
-Loads oracle/_build/liboracle.so (built from oracle/pcg_oracle.cpp by
-oracle/Makefile), a loop-for-loop C++ restatement of
-libglissade/glissade_velo_higher_pcg.F90 and the one-rank semantics of
-libglimmer/parallel_mpi.F90's global sum and staggered halo.  Only tests/,
+Loads oracle/_build/liboracle.so (built by oracle/Makefile), loop-for-loop C++
+restatements of:
+- pcg_oracle.cpp: libglissade/glissade_velo_higher_pcg.F90 and the one-rank semantics
+  of libglimmer/parallel_mpi.F90's global sum (incl. reprosum) and staggered halo; the
+  residual routines and the symmetry check of glissade_velo_higher.F90;
+- assembly_oracle.cpp: the stiffness assembly (assemble_stiffness_matrix_3d/_2d) and
+  the Dirichlet and local basal terms of glissade_velo_higher.F90.  Only tests/,
 __graft_entry__.smoke() and bench.py's CPU-baseline arm may use it, and only as
 the checker or the timed CPU baseline.
 
