@@ -16,6 +16,8 @@
 !     check_symmetry_assembled_matrix_2d (:10648-10850)
 !     check_symmetry_assembled_matrix_3d (:10854-11117)
 !     assemble_stiffness_matrix_3d (:5382-5643), assemble_stiffness_matrix_2d (:4961-5378, SSA)
+!     dirichlet_boundary_conditions_3d (:9305-9498), dirichlet_boundary_conditions_2d (:9133-9301)
+!     basal_sliding_bc_3d (:8815-9129), basal_sliding_bc_2d (:8281-8531), local form
 !   A nonzero library status is reported the way the reference reports a failed
 !   solve: write_log(message, GM_FATAL).
 !
@@ -45,6 +47,8 @@
               compute_residual_velocity_2d, compute_residual_velocity_3d, &
               check_symmetry_assembled_matrix_2d, check_symmetry_assembled_matrix_3d, &
               assemble_stiffness_matrix_2d, assemble_stiffness_matrix_3d, &
+              dirichlet_boundary_conditions_2d, dirichlet_boundary_conditions_3d, &
+              basal_sliding_bc_2d, basal_sliding_bc_3d, &
               cismgpu_use_mixed_precision
 
     type, bind(C) :: cismgpu_par_t
@@ -213,6 +217,44 @@
          real(c_double), value :: efvs_constant, effstrain_min, n_glen
          real(c_double), intent(out) :: efvs(*), Auu(*), Auv(*), Avu(*), Avv(*)
        end function c_assemble_2d
+
+       integer(c_int) function c_dirichlet_3d(nx, ny, nz, nhalo, active_vertex, umask, vmask, uvel, vvel, &
+            indxA_3d, Auu, Auv, Avu, Avv, bu, bv) bind(C, name="cismgpu_dirichlet_boundary_conditions_3d")
+         import :: c_int, c_double, c_int32_t
+         integer(c_int), value :: nx, ny, nz, nhalo
+         integer(c_int32_t), intent(in) :: active_vertex(*), umask(*), vmask(*), indxA_3d(*)
+         real(c_double), intent(in) :: uvel(*), vvel(*)
+         real(c_double), intent(inout) :: Auu(*), Auv(*), Avu(*), Avv(*), bu(*), bv(*)
+       end function c_dirichlet_3d
+
+       integer(c_int) function c_dirichlet_2d(nx, ny, nhalo, active_vertex, umask, vmask, uvel, vvel, &
+            indxA_2d, Auu, Auv, Avu, Avv, bu, bv) bind(C, name="cismgpu_dirichlet_boundary_conditions_2d")
+         import :: c_int, c_double, c_int32_t
+         integer(c_int), value :: nx, ny, nhalo
+         integer(c_int32_t), intent(in) :: active_vertex(*), umask(*), vmask(*), indxA_2d(*)
+         real(c_double), intent(in) :: uvel(*), vvel(*)
+         real(c_double), intent(inout) :: Auu(*), Auv(*), Avu(*), Avv(*), bu(*), bv(*)
+       end function c_dirichlet_2d
+
+       integer(c_int) function c_basal_3d(nx, ny, nz, nhalo, dx, dy, active_vertex, beta, lsrf, &
+            whichassemble_beta, indxA_3d, Auu, Avv) bind(C, name="cismgpu_basal_sliding_bc_3d")
+         import :: c_int, c_double, c_int32_t
+         integer(c_int), value :: nx, ny, nz, nhalo, whichassemble_beta
+         real(c_double), value :: dx, dy
+         integer(c_int32_t), intent(in) :: active_vertex(*), indxA_3d(*)
+         real(c_double), intent(in) :: beta(*), lsrf(*)
+         real(c_double), intent(inout) :: Auu(*), Avv(*)
+       end function c_basal_3d
+
+       integer(c_int) function c_basal_2d(nx, ny, nhalo, dx, dy, active_vertex, beta, whichassemble_beta, &
+            indxA_2d, Auu, Avv) bind(C, name="cismgpu_basal_sliding_bc_2d")
+         import :: c_int, c_double, c_int32_t
+         integer(c_int), value :: nx, ny, nhalo, whichassemble_beta
+         real(c_double), value :: dx, dy
+         integer(c_int32_t), intent(in) :: active_vertex(*), indxA_2d(*)
+         real(c_double), intent(in) :: beta(*)
+         real(c_double), intent(inout) :: Auu(*), Avv(*)
+       end function c_basal_2d
     end interface
 
   contains
@@ -545,5 +587,82 @@
                                flwafact, whichefvs, efvs_constant, effstrain_min, n_glen, indx2, efvs, &
                                Auu, Auv, Avu, Avv))
     end subroutine assemble_stiffness_matrix_2d
+
+    !-----------------------------------------------------------------------
+    ! The boundary routines with the reference's argument lists.  basal_sliding_bc_3d receives
+    ! the bed slices Auu(:,nz,:,:), Avv(:,nz,:,:), which the library addresses as one-level
+    ! blocks; the standard finite-element basal form is reported with GM_FATAL.
+    subroutine dirichlet_boundary_conditions_3d(nx, ny, nz, nhalo, active_vertex, umask_dirichlet, &
+                                                vmask_dirichlet, uvel, vvel, Auu, Auv, Avu, Avv, bu, bv)
+      integer, intent(in) :: nx, ny, nz, nhalo
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      integer, dimension(nz,nx-1,ny-1), intent(in) :: umask_dirichlet, vmask_dirichlet
+      real(dp), dimension(nz,nx-1,ny-1), intent(in) :: uvel, vvel
+      real(dp), dimension(27,nz,nx-1,ny-1), intent(inout) :: Auu, Auv, Avu, Avv
+      real(dp), dimension(nz,nx-1,ny-1), intent(inout) :: bu, bv
+      integer(c_int32_t) :: act(nx-1,ny-1), um(nz,nx-1,ny-1), vm(nz,nx-1,ny-1), indx3(27)
+      integer :: m
+      act = merge(1, 0, active_vertex)
+      um = umask_dirichlet
+      vm = vmask_dirichlet
+      indx3 = [(m, m = 1, 27)]
+      call check(c_dirichlet_3d(nx, ny, nz, nhalo, act, um, vm, uvel, vvel, indx3, Auu, Auv, Avu, Avv, bu, bv))
+    end subroutine dirichlet_boundary_conditions_3d
+
+    !-----------------------------------------------------------------------
+    subroutine dirichlet_boundary_conditions_2d(nx, ny, nhalo, active_vertex, umask_dirichlet, vmask_dirichlet, &
+                                                uvel, vvel, Auu, Auv, Avu, Avv, bu, bv)
+      integer, intent(in) :: nx, ny, nhalo
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      integer, dimension(nx-1,ny-1), intent(in) :: umask_dirichlet, vmask_dirichlet
+      real(dp), dimension(nx-1,ny-1), intent(in) :: uvel, vvel
+      real(dp), dimension(nx-1,ny-1,9), intent(inout) :: Auu, Auv, Avu, Avv
+      real(dp), dimension(nx-1,ny-1), intent(inout) :: bu, bv
+      integer(c_int32_t) :: act(nx-1,ny-1), um(nx-1,ny-1), vm(nx-1,ny-1), indx2(9)
+      integer :: m
+      act = merge(1, 0, active_vertex)
+      um = umask_dirichlet
+      vm = vmask_dirichlet
+      indx2 = [(m, m = 1, 9)]
+      call check(c_dirichlet_2d(nx, ny, nhalo, act, um, vm, uvel, vvel, indx2, Auu, Auv, Avu, Avv, bu, bv))
+    end subroutine dirichlet_boundary_conditions_2d
+
+    !-----------------------------------------------------------------------
+    subroutine basal_sliding_bc_3d(nx, ny, nNeighbors, nhalo, parallel, dx, dy, itest, jtest, rtest, &
+                                   active_cell, active_vertex, beta, lsrf, xVertex, yVertex, &
+                                   whichassemble_beta, Auu, Avv)
+      integer, intent(in) :: nx, ny, nNeighbors, nhalo, itest, jtest, rtest, whichassemble_beta
+      type(parallel_type), intent(in) :: parallel
+      real(dp), intent(in) :: dx, dy
+      logical, dimension(nx,ny), intent(in) :: active_cell
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      real(dp), dimension(nx-1,ny-1), intent(in) :: beta, xVertex, yVertex
+      real(dp), dimension(nx,ny), intent(in) :: lsrf
+      real(dp), dimension(nNeighbors,nx-1,ny-1), intent(inout) :: Auu, Avv
+      integer(c_int32_t) :: act(nx-1,ny-1), indx3(27)
+      integer :: m
+      act = merge(1, 0, active_vertex)
+      indx3 = [(m, m = 1, 27)]
+      call check(c_basal_3d(nx, ny, 1, nhalo, dx, dy, act, beta, lsrf, whichassemble_beta, indx3, Auu, Avv))
+    end subroutine basal_sliding_bc_3d
+
+    !-----------------------------------------------------------------------
+    subroutine basal_sliding_bc_2d(nx, ny, nNeighbors, nhalo, parallel, dx, dy, itest, jtest, rtest, &
+                                   active_cell, active_vertex, beta, lsrf, xVertex, yVertex, &
+                                   whichassemble_beta, Auu, Avv)
+      integer, intent(in) :: nx, ny, nNeighbors, nhalo, itest, jtest, rtest, whichassemble_beta
+      type(parallel_type), intent(in) :: parallel
+      real(dp), intent(in) :: dx, dy
+      logical, dimension(nx,ny), intent(in) :: active_cell
+      logical, dimension(nx-1,ny-1), intent(in) :: active_vertex
+      real(dp), dimension(nx-1,ny-1), intent(in) :: beta, xVertex, yVertex
+      real(dp), dimension(nx,ny), intent(in) :: lsrf
+      real(dp), dimension(nx-1,ny-1,nNeighbors), intent(inout) :: Auu, Avv
+      integer(c_int32_t) :: act(nx-1,ny-1), indx2(9)
+      integer :: m
+      act = merge(1, 0, active_vertex)
+      indx2 = [(m, m = 1, 9)]
+      call check(c_basal_2d(nx, ny, nhalo, dx, dy, act, beta, whichassemble_beta, indx2, Auu, Avv))
+    end subroutine basal_sliding_bc_2d
 
   end module glissade_velo_higher_pcg_gpu
