@@ -79,6 +79,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_dirichlet_2d.restype = None
         L.oracle_basal_local_2d.argtypes = [i, i, dbl, dbl, d, d, d, d]
         L.oracle_basal_local_2d.restype = None
+        L.oracle_basal_standard.argtypes = [i, i, i, i, i, d, d, d, d, d, d, d]
         L.oracle_check_symmetry.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, P(dbl), P(ctypes.c_long)]
         L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
@@ -289,6 +290,17 @@ def basal_local_2d(nx, ny, dx, dy, active_vertex, beta, Auu, Avv):
     lib().oracle_basal_local_2d(nx, ny, float(dx), float(dy), _p(np.ascontiguousarray(active_vertex, dtype=np.int32)),
                                 _p(np.ascontiguousarray(beta, dtype=np.float64)), _p(out[0]), _p(out[1]))
     return out[0], out[1]
+
+
+def basal_standard(is3d, nx, ny, nz, active_cell, xVertex, yVertex, beta, lsrf, Auu, Avv, nhalo=2):
+    """basal_sliding_bc_3d / _2d, standard finite-element form (whichassemble_beta = 0), on copies
+    of the blocks (3D (ny-1, nx-1, nz, 27), 2D (9, ny-1, nx-1)).  Returns (status, Auu, Avv)."""
+    out = [np.array(a, dtype=np.float64, copy=True) for a in (Auu, Avv)]
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    st = lib().oracle_basal_standard(int(is3d), nx, ny, nz, nhalo, _p(np.ascontiguousarray(active_cell, dtype=np.int32)),
+                                     _p(f64(xVertex)), _p(f64(yVertex)), _p(f64(beta)),
+                                     _p(f64(np.zeros((ny, nx)) if lsrf is None else lsrf)), _p(out[0]), _p(out[1]))
+    return st, out[0], out[1]
 
 
 def reprosum(a) -> float:

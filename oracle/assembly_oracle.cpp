@@ -605,3 +605,81 @@ void oracle_basal_local_2d(int nx, int ny, double dx, double dy, const int32_t *
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// basal_sliding_bc_3d / _2d, standard finite-element form (whichassemble_beta = 0)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+// basal_sliding_bc_3d (:8876-8960) and basal_sliding_bc_2d (:8337-8410), standard form: every
+// active cell j = nhalo+1..ny-nhalo+1, i = nhalo+1..nx-nhalo+1, 4 Gauss points; beta at the
+// point from the 4 vertex values; the area factor is get_area_scale_factor_curved_2d
+// (:6736-6827, the lower surface staggered over all four cells as z) in 3D and the flat
+// Jacobian of get_basis_function_derivatives_2d in 2D; each point's 4x4 matrix
+// beta_qp*w*detJ/vol0*phi_r*phi_c is added to Auu and Avv (3D: the bed level nz) at once.
+// is3d: blocks (27,nz,nx-1,ny-1), else (nx-1,ny-1,9).  Returns 1 for a singular 2D Jacobian.
+int oracle_basal_standard(int is3d, int nx, int ny, int nz, int nhalo, const int32_t *active_cell,
+                          const double *xVertex, const double *yVertex, const double *beta, const double *lsrf,
+                          double *Auu, double *Avv) {
+    const long NX = nx - 1, NQ = NX * (ny - 1);
+    const RefElement2 &R = ref2();
+    std::vector<double> stag((size_t)NQ, 0.0);
+    if (is3d)
+        for (int j = 1; j <= ny - 1; ++j)
+            for (int i = 1; i <= nx - 1; ++i) {
+                auto L = [&](int ii, int jj) { return lsrf[(ii - 1) + (long)nx * (jj - 1)]; };
+                stag[(i - 1) + NX * (j - 1)] = (L(i, j + 1) + L(i + 1, j + 1) + L(i, j) + L(i + 1, j)) / 4.0;
+            }
+    for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+        for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+            if (!active_cell[(i - 1) + (long)nx * (j - 1)]) continue;
+            double x[4], y[4], z[4], b[4];
+            for (int n = 0; n < 4; ++n) {
+                const long q = (long)(i + kIsh3[n] - 1) + NX * (j + kJsh3[n] - 1);
+                x[n] = xVertex[q];
+                y[n] = yVertex[q];
+                z[n] = stag[q];
+                b[n] = beta[q];
+            }
+            for (int p = 0; p < 4; ++p) {
+                double detJ;
+                if (is3d) {  // get_area_scale_factor_curved_2d
+                    double J11 = 0.0, J12 = 0.0, J13 = 0.0, J21 = 0.0, J22 = 0.0, J23 = 0.0;
+                    for (int n = 0; n < 4; ++n) {
+                        J11 = J11 + R.dxr[p][n] * x[n];
+                        J12 = J12 + R.dxr[p][n] * y[n];
+                        J13 = J13 + R.dxr[p][n] * z[n];
+                        J21 = J21 + R.dyr[p][n] * x[n];
+                        J22 = J22 + R.dyr[p][n] * y[n];
+                        J23 = J23 + R.dyr[p][n] * z[n];
+                    }
+                    const double t1 = (J11 * J22 - J12 * J21);
+                    const double t2 = -(J11 * J23 - J13 * J21);
+                    const double t3 = (J12 * J23 - J13 * J22);
+                    detJ = std::sqrt(t1 * t1 + t2 * t2 + t3 * t3);
+                } else {
+                    double dx[4], dy[4];
+                    if (!basis_derivs_2d(x, y, R.dxr[p], R.dyr[p], dx, dy, &detJ)) return 1;
+                }
+                double beta_qp = 0.0;
+                for (int n = 0; n < 4; ++n) beta_qp = beta_qp + R.phi[p][n] * b[n];
+                double K[4][4] = {};
+                for (int nc = 0; nc < 4; ++nc)
+                    for (int nr = 0; nr < 4; ++nr)
+                        K[nr][nc] = K[nr][nc] + beta_qp * 1.0 * detJ / kVol0 * R.phi[p][nr] * R.phi[p][nc];
+                for (int nr = 0; nr < 4; ++nr) {
+                    const long q = (long)(i + kIsh3[nr] - 1) + NX * (j + kJsh3[nr] - 1);
+                    for (int nc = 0; nc < 4; ++nc) {
+                        const int m = (kIsh3[nc] - kIsh3[nr] + 1) + 3 * (kJsh3[nc] - kJsh3[nr] + 1);  // kA = 0
+                        const size_t a = is3d ? (size_t)(m + 9) + 27 * ((size_t)(nz - 1) + (size_t)nz * q)
+                                              : (size_t)q + (size_t)NQ * m;
+                        Auu[a] = Auu[a] + K[nr][nc];
+                        Avv[a] = Avv[a] + K[nr][nc];
+                    }
+                }
+            }
+        }
+    return 0;
+}
+
+}  // extern "C"
