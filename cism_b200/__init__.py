@@ -190,13 +190,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                                          dbl, d, d, d, d, d, d]
     lib.cismgpu_solver_assemble_stiffness_2d.argtypes = [vp, i32, i32, d, d, d, d, d, d, d, d, i32, dbl, dbl, dbl, d]
     lib.cismgpu_dirichlet_boundary_conditions_3d.argtypes = [i32, i32, i32, i32, d, d, d, d, d, d, d, d, d, d, d, d]
-    lib.cismgpu_basal_sliding_bc_3d.argtypes = [i32, i32, i32, i32, dbl, dbl, d, d, d, i32, d, d, d]
+    lib.cismgpu_basal_sliding_bc_3d.argtypes = [i32, i32, i32, i32, dbl, dbl, d, d, d, d, d, d, i32, d, d, d]
     lib.cismgpu_solver_assemble_system_3d.argtypes = [vp, i32, dbl, dbl, d, d, d, d, d, d, d, d, i32, i32, dbl, dbl,
-                                                      dbl, d, d, d, d, d, d, d]
+                                                      dbl, d, d, i32, d, d, d, d, d]
     lib.cismgpu_dirichlet_boundary_conditions_2d.argtypes = [i32, i32, i32, d, d, d, d, d, d, d, d, d, d, d, d]
-    lib.cismgpu_basal_sliding_bc_2d.argtypes = [i32, i32, i32, dbl, dbl, d, d, i32, d, d, d]
+    lib.cismgpu_basal_sliding_bc_2d.argtypes = [i32, i32, i32, dbl, dbl, d, d, d, d, d, i32, d, d, d]
     lib.cismgpu_solver_assemble_system_2d.argtypes = [vp, i32, i32, dbl, dbl, d, d, d, d, d, d, d, i32, dbl, dbl, dbl,
-                                                      d, d, d, d, d, d]
+                                                      d, i32, d, d, d, d, d]
     for f in ("cismgpu_compute_residual_vector_3d", "cismgpu_compute_residual_vector_2d",
               "cismgpu_compute_residual_velocity_3d", "cismgpu_compute_residual_velocity_2d",
               "cismgpu_solver_set_system", "cismgpu_solver_residual_vector", "cismgpu_solver_residual_velocity",
@@ -514,17 +514,18 @@ def dirichlet_boundary_conditions_3d(nx, ny, nz, nhalo, active_vertex, umask, vm
         _ptr(bv, np.float64, n, True)))
 
 
-def basal_sliding_bc_3d(nx, ny, nz, nhalo, dx, dy, active_vertex, beta, lsrf, Auu, Avv, whichassemble_beta=1,
-                        indxA_3d=None):
-    """Mirrors basal_sliding_bc_3d (glissade_velo_higher.F90:8815-9129), local form, on the GPU:
-    the bed diagonals of the full Auu and Avv blocks are increased in place."""
+def basal_sliding_bc_3d(nx, ny, nz, nhalo, dx, dy, active_cell, active_vertex, beta, lsrf, xVertex, yVertex, Auu,
+                        Avv, whichassemble_beta=1, indxA_3d=None):
+    """Mirrors basal_sliding_bc_3d (glissade_velo_higher.F90:8815-9129) on the GPU (1: local,
+    0: standard form): the bed level of the full Auu and Avv blocks is increased in place."""
     lib = load_library()
     nv = (nx - 1) * (ny - 1)
     indx = np.arange(1, 28, dtype=np.int32) if indxA_3d is None else np.ascontiguousarray(indxA_3d, dtype=np.int32)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
     _check(lib, lib.cismgpu_basal_sliding_bc_3d(
-        nx, ny, nz, int(nhalo), float(dx), float(dy), _ptr(np.ascontiguousarray(active_vertex, dtype=np.int32),
-                                                           np.int32, nv),
-        _ptr(beta, np.float64, nv), _ptr(lsrf, np.float64, nx * ny), int(whichassemble_beta), _ptr(indx, np.int32, 27),
+        nx, ny, nz, int(nhalo), float(dx), float(dy), _ptr(i32(active_cell), np.int32, nx * ny),
+        _ptr(i32(active_vertex), np.int32, nv), _ptr(beta, np.float64, nv), _ptr(lsrf, np.float64, nx * ny),
+        _ptr(xVertex, np.float64, nv), _ptr(yVertex, np.float64, nv), int(whichassemble_beta), _ptr(indx, np.int32, 27),
         _ptr(Auu, np.float64, 27 * nv * nz, True), _ptr(Avv, np.float64, 27 * nv * nz, True)))
 
 
@@ -543,15 +544,19 @@ def dirichlet_boundary_conditions_2d(nx, ny, nhalo, active_vertex, umask, vmask,
         _ptr(bv, np.float64, nv, True)))
 
 
-def basal_sliding_bc_2d(nx, ny, nhalo, dx, dy, active_vertex, beta, Auu, Avv, whichassemble_beta=1, indxA_2d=None):
-    """Mirrors basal_sliding_bc_2d (glissade_velo_higher.F90:8281-8531), local form, in place."""
+def basal_sliding_bc_2d(nx, ny, nhalo, dx, dy, active_cell, active_vertex, beta, xVertex, yVertex, Auu, Avv,
+                        whichassemble_beta=1, indxA_2d=None):
+    """Mirrors basal_sliding_bc_2d (glissade_velo_higher.F90:8281-8531) on the GPU (1: local,
+    0: standard form), in place."""
     lib = load_library()
     nv = (nx - 1) * (ny - 1)
     indx = np.arange(1, 10, dtype=np.int32) if indxA_2d is None else np.ascontiguousarray(indxA_2d, dtype=np.int32)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
     _check(lib, lib.cismgpu_basal_sliding_bc_2d(
-        nx, ny, int(nhalo), float(dx), float(dy), _ptr(np.ascontiguousarray(active_vertex, dtype=np.int32), np.int32, nv),
-        _ptr(beta, np.float64, nv), int(whichassemble_beta), _ptr(indx, np.int32, 9), _ptr(Auu, np.float64, 9 * nv, True),
-        _ptr(Avv, np.float64, 9 * nv, True)))
+        nx, ny, int(nhalo), float(dx), float(dy), _ptr(i32(active_cell), np.int32, nx * ny),
+        _ptr(i32(active_vertex), np.int32, nv), _ptr(beta, np.float64, nv), _ptr(xVertex, np.float64, nv),
+        _ptr(yVertex, np.float64, nv), int(whichassemble_beta), _ptr(indx, np.int32, 9),
+        _ptr(Auu, np.float64, 9 * nv, True), _ptr(Avv, np.float64, 9 * nv, True)))
 
 
 class DeviceSolver:
@@ -661,7 +666,8 @@ class DeviceSolver:
 
     def assemble_system(self, nhalo, dx, dy, sigma, active_cell, active_vertex, xVertex, yVertex, stagusrf,
                         stagthck, flwafact, loadu, loadv, beta=None, lsrf=None, umask=None, vmask=None,
-                        whichapprox=2, whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8, n_glen=3.0):
+                        whichapprox=2, whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8, n_glen=3.0,
+                        whichassemble_beta=1):
         """One Picard iteration's system on the device (cismgpu_solver_assemble_system_3d / _2d):
         stiffness from the current velocity, local basal term, b = load, Dirichlet conditions,
         staggered halo.  2D handles: stagusrf and lsrf unused, masks (ny-1, nx-1).  Returns efvs
@@ -670,7 +676,7 @@ class DeviceSolver:
         if P.kind != "3d":
             return self._assemble_system_2d(nhalo, dx, dy, sigma, active_cell, active_vertex, xVertex, yVertex,
                                             stagthck, flwafact, loadu, loadv, beta, umask, vmask, whichefvs,
-                                            efvs_constant, effstrain_min, n_glen)
+                                            efvs_constant, effstrain_min, n_glen, whichassemble_beta)
         nx, ny, nz = P.nx, P.ny, P.nz
         nv = (nx - 1) * (ny - 1)
         efvs = np.zeros((ny, nx, nz - 1))
@@ -682,13 +688,14 @@ class DeviceSolver:
         _check(self._lib, self._lib.cismgpu_solver_assemble_system_3d(
             self.handle, int(nhalo), float(dx), float(dy), head[0], head[1], _ptr(keep[0], np.int32, nv), head[2],
             head[3], *tail, int(whichapprox), int(whichefvs), float(efvs_constant), float(effstrain_min),
-            float(n_glen), *pb, _ptr(loadu, np.float64, nv * nz), _ptr(loadv, np.float64, nv * nz), *pm,
+            float(n_glen), *pb, int(whichassemble_beta), _ptr(loadu, np.float64, nv * nz),
+            _ptr(loadv, np.float64, nv * nz), *pm,
             _ptr(efvs, np.float64, efvs.size, True)))
         return efvs
 
     def _assemble_system_2d(self, nhalo, dx, dy, sigma, active_cell, active_vertex, xVertex, yVertex, stagthck,
                             flwafact, loadu, loadv, beta, umask, vmask, whichefvs, efvs_constant, effstrain_min,
-                            n_glen):
+                            n_glen, whichassemble_beta=1):
         P = self.problem
         nx, ny, nz = P.nx, P.ny, len(sigma)
         nv = (nx - 1) * (ny - 1)
@@ -701,7 +708,8 @@ class DeviceSolver:
         _check(self._lib, self._lib.cismgpu_solver_assemble_system_2d(
             self.handle, nz, int(nhalo), float(dx), float(dy), head[0], head[1], _ptr(keep[0], np.int32, nv), head[2],
             head[3], tail[1], tail[2], int(whichefvs), float(efvs_constant), float(effstrain_min), float(n_glen), pb,
-            _ptr(loadu, np.float64, nv), _ptr(loadv, np.float64, nv), *pm, _ptr(efvs, np.float64, efvs.size, True)))
+            int(whichassemble_beta), _ptr(loadu, np.float64, nv), _ptr(loadv, np.float64, nv), *pm,
+            _ptr(efvs, np.float64, efvs.size, True)))
         return efvs
 
     def save(self):

@@ -605,4 +605,102 @@ __global__ void __launch_bounds__(kBlock) k_basal_local2d(long long NQ, double d
     Avv[a] = Avv[a] + increment;
 }
 
+// basal_sliding_bc_3d (:8876-8960) / basal_sliding_bc_2d (:8337-8410), standard finite-element
+// form, one thread per vertex: the (up to) 4 active cells around it in the reference's order
+// (j, then i), and for each of the cell's 4 Gauss points the vertex's row of
+// beta_qp*w*detJ/vol0*phi_r*phi_c added to Auu and Avv, point by point as the reference adds
+// them.  3D: the area factor of the lower surface (get_area_scale_factor_curved_2d, :6736-6827,
+// lsrf staggered over all four cells) and the bed level nz; 2D: the flat Jacobian.
+template <bool THREE_D>
+__global__ void __launch_bounds__(kBlock) k_basal_standard(int nx, int ny, int nz, int nhalo, SymIdx L,
+                                                           const int32_t *__restrict__ active_cell,
+                                                           const double *__restrict__ xv,
+                                                           const double *__restrict__ yv,
+                                                           const double *__restrict__ beta,
+                                                           const double *__restrict__ lsrf, double *Auu,
+                                                           double *Avv, int *singular) {
+    const long long NX = nx - 1, NQ = NX * (ny - 1);
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (q >= NQ) return;
+    const int jR = (int)(q / NX) + 1, iR = (int)(q - (long long)(jR - 1) * NX) + 1;  // 1-based
+    auto Lf = [&](int ii, int jj) { return lsrf[(ii - 1) + (long long)nx * (jj - 1)]; };
+    const int base = THREE_D ? 9 : 0;  // indxA_3d(iA, jA, 0) = indxA_2d(iA, jA) + 9
+    const int lev = THREE_D ? nz - 1 : 0;
+    double accU[9], accV[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        accU[c] = Auu[L.at(c + base, lev, q)];
+        accV[c] = Avv[L.at(c + base, lev, q)];
+    }
+    bool any = false;
+    for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+            const int je = jR + dj, ie = iR + di;
+            if (ie < nhalo + 1 || ie > nx - nhalo + 1 || je < nhalo + 1 || je > ny - nhalo + 1) continue;
+            if (!active_cell[(ie - 1) + (long long)nx * (je - 1)]) continue;
+            any = true;
+            const int nr = dj == 0 ? (di == 0 ? 2 : 3) : (di == 0 ? 1 : 0);
+            double x[4], y[4], z[4], b[4];
+#pragma unroll
+            for (int n = 0; n < 4; ++n) {
+                const int iN = ie + c_ish3[n], jN = je + c_jsh3[n];
+                const long long qn = (long long)(iN - 1) + NX * (jN - 1);
+                x[n] = xv[qn];
+                y[n] = yv[qn];
+                b[n] = beta[qn];
+                z[n] = THREE_D ? (Lf(iN, jN + 1) + Lf(iN + 1, jN + 1) + Lf(iN, jN) + Lf(iN + 1, jN)) / 4.0 : 0.0;
+            }
+            for (int p = 0; p < 4; ++p) {
+                const double *dxr = c_asm_ref2.dxr[p], *dyr = c_asm_ref2.dyr[p];
+                double detJ;
+                if (THREE_D) {
+                    double J11 = 0.0, J12 = 0.0, J13 = 0.0, J21 = 0.0, J22 = 0.0, J23 = 0.0;
+#pragma unroll
+                    for (int n = 0; n < 4; ++n) {
+                        J11 = J11 + dxr[n] * x[n];
+                        J12 = J12 + dxr[n] * y[n];
+                        J13 = J13 + dxr[n] * z[n];
+                        J21 = J21 + dyr[n] * x[n];
+                        J22 = J22 + dyr[n] * y[n];
+                        J23 = J23 + dyr[n] * z[n];
+                    }
+                    const double t1 = (J11 * J22 - J12 * J21);
+                    const double t2 = -(J11 * J23 - J13 * J21);
+                    const double t3 = (J12 * J23 - J13 * J22);
+                    detJ = sqrt(t1 * t1 + t2 * t2 + t3 * t3);
+                } else {
+                    double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
+#pragma unroll
+                    for (int n = 0; n < 4; ++n) {
+                        J00 = J00 + dxr[n] * x[n];
+                        J01 = J01 + dxr[n] * y[n];
+                        J10 = J10 + dyr[n] * x[n];
+                        J11 = J11 + dyr[n] * y[n];
+                    }
+                    detJ = J00 * J11 - J01 * J10;
+                    if (!(fabs(detJ) > 0.0)) {
+                        atomicExch(singular, 1);
+                        continue;
+                    }
+                }
+                double beta_qp = 0.0;
+#pragma unroll
+                for (int n = 0; n < 4; ++n) beta_qp = beta_qp + c_asm_ref2.phi[p][n] * b[n];
+#pragma unroll
+                for (int nc = 0; nc < 4; ++nc) {
+                    const double k = 0.0 + beta_qp * 1.0 * detJ / kAsmVol0 * c_asm_ref2.phi[p][nr] * c_asm_ref2.phi[p][nc];
+                    const int m = (c_ish3[nc] - c_ish3[nr] + 1) + 3 * (c_jsh3[nc] - c_jsh3[nr] + 1);
+                    accU[m] = accU[m] + k;
+                    accV[m] = accV[m] + k;
+                }
+            }
+        }
+    if (!any) return;
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+        Auu[L.at(c + base, lev, q)] = accU[c];
+        Avv[L.at(c + base, lev, q)] = accV[c];
+    }
+}
+
 }  // namespace cismgpu

@@ -433,26 +433,40 @@ struct Solver {
     int boundary3d(const SymIdx &L, double *Auu, double *Auv, double *Avu, double *Avv, double *bu, double *bv,
                    VecIdx Wb, int nhalo, double dx, double dy, const int32_t *active_vertex, const double *beta,
                    const double *lsrf, const int32_t *umask, const int32_t *vmask, const double *uvel,
-                   const double *vvel, int vel_id) {
+                   const double *vvel, int vel_id, int assemble_beta = 1, const int32_t *active_cell = nullptr,
+                   const double *xv = nullptr, const double *yv = nullptr) {
         const int nx = g.NX + 1, ny = g.NY + 1, nz = g.nz;
         const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny, nn = (size_t)nz * nq;
         const bool host_vel = uvel != nullptr;
-        // doubles: beta, lsrf, [uvel, vvel]; then int32: active_vertex, umask, vmask
-        const size_t nd = nq + ncell + (host_vel ? 2 * nn : 0);
-        CU(bc_in.ensure(nd * sizeof(double) + (nq + 2 * nn) * sizeof(int32_t)));
+        // doubles: beta, lsrf, xVertex, yVertex, [uvel, vvel]; then int32: active_vertex, umask,
+        // vmask, active_cell, the singular-Jacobian flag
+        const size_t nd = 3 * nq + ncell + (host_vel ? 2 * nn : 0);
+        CU(bc_in.ensure(nd * sizeof(double) + (nq + 2 * nn + ncell + 1) * sizeof(int32_t)));
         double *D = bc_in.as<double>();
-        double *d_beta = D, *d_lsrf = D + nq, *d_u = d_lsrf + ncell, *d_v = d_u + nn;
-        int32_t *d_act = reinterpret_cast<int32_t *>(D + nd), *d_um = d_act + nq, *d_vm = d_um + nn;
+        double *d_beta = D, *d_lsrf = D + nq, *d_xv = d_lsrf + ncell, *d_yv = d_xv + nq, *d_u = d_yv + nq,
+               *d_v = d_u + nn;
+        int32_t *d_act = reinterpret_cast<int32_t *>(D + nd), *d_um = d_act + nq, *d_vm = d_um + nn,
+                *d_cell = d_vm + nn, *d_sing = d_cell + ncell;
         cudaStream_t s = stream;
         auto up = [&](void *dst, const void *src, size_t bytes) {
             return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
         };
         CU(up(d_act, active_vertex, nq * sizeof(int32_t)));
+        CU(cudaMemsetAsync(d_sing, 0, sizeof(int32_t), s));
         if (beta) {
             CU(up(d_beta, beta, nq * sizeof(double)));
             CU(up(d_lsrf, lsrf, ncell * sizeof(double)));
-            k_basal_local3d<<<nblocks((long long)nq), kBlock, 0, s>>>(nx, ny, nz, dx, dy, L, d_act, d_beta, d_lsrf,
-                                                                      Auu, Avv);
+            if (assemble_beta == 1) {
+                k_basal_local3d<<<nblocks((long long)nq), kBlock, 0, s>>>(nx, ny, nz, dx, dy, L, d_act, d_beta,
+                                                                          d_lsrf, Auu, Avv);
+            } else {
+                CU(up(d_cell, active_cell, ncell * sizeof(int32_t)));
+                CU(up(d_xv, xv, nq * sizeof(double)));
+                CU(up(d_yv, yv, nq * sizeof(double)));
+                k_basal_standard<true><<<nblocks((long long)nq), kBlock, 0, s>>>(nx, ny, nz, nhalo, L, d_cell, d_xv,
+                                                                                 d_yv, d_beta, d_lsrf, Auu, Avv,
+                                                                                 d_sing);
+            }
             CU(cudaGetLastError());
         }
         if (umask) {
@@ -470,7 +484,10 @@ struct Solver {
                                                                     d_vm, xu, xv, Auu, Auv, Avu, Avv, bu, bv);
             CU(cudaGetLastError());
         }
+        int sing = 0;
+        CU(cudaMemcpyAsync(&sing, d_sing, sizeof(int), cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
+        if (sing) return fail(CISMGPU_EINVAL, "Jacobian matrix is singular (a basal cell of zero area)");
         return CISMGPU_OK;
     }
 
@@ -481,23 +498,38 @@ struct Solver {
     // Leaves the stream synchronized.
     int boundary2d(const SymIdx &L, double *Auu, double *Auv, double *Avu, double *Avv, double *bu, double *bv,
                    int nhalo, double dx, double dy, const int32_t *active_vertex, const double *beta,
-                   const int32_t *umask, const int32_t *vmask, const double *uvel, const double *vvel, int vel_id) {
+                   const int32_t *umask, const int32_t *vmask, const double *uvel, const double *vvel, int vel_id,
+                   int assemble_beta = 1, const int32_t *active_cell = nullptr, const double *xv = nullptr,
+                   const double *yv = nullptr) {
         const int nx = g.NX + 1, ny = g.NY + 1;
-        const size_t nq = (size_t)g.NQ;
+        const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny;
         const bool host_vel = uvel != nullptr;
-        const size_t nd = nq + (host_vel ? 2 * nq : 0);  // beta, [uvel, vvel]; then active, umask, vmask
-        CU(bc_in.ensure(nd * sizeof(double) + 3 * nq * sizeof(int32_t)));
+        // doubles: beta, xVertex, yVertex, [uvel, vvel]; then int32: active_vertex, umask, vmask,
+        // active_cell, the singular-Jacobian flag
+        const size_t nd = 3 * nq + (host_vel ? 2 * nq : 0);
+        CU(bc_in.ensure(nd * sizeof(double) + (3 * nq + ncell + 1) * sizeof(int32_t)));
         double *D = bc_in.as<double>();
-        double *d_beta = D, *d_u = D + nq, *d_v = d_u + nq;
-        int32_t *d_act = reinterpret_cast<int32_t *>(D + nd), *d_um = d_act + nq, *d_vm = d_um + nq;
+        double *d_beta = D, *d_xv = D + nq, *d_yv = d_xv + nq, *d_u = d_yv + nq, *d_v = d_u + nq;
+        int32_t *d_act = reinterpret_cast<int32_t *>(D + nd), *d_um = d_act + nq, *d_vm = d_um + nq,
+                *d_cell = d_vm + nq, *d_sing = d_cell + ncell;
         cudaStream_t s = stream;
         auto up = [&](void *dst, const void *src, size_t bytes) {
             return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
         };
         CU(up(d_act, active_vertex, nq * sizeof(int32_t)));
+        CU(cudaMemsetAsync(d_sing, 0, sizeof(int32_t), s));
         if (beta) {
             CU(up(d_beta, beta, nq * sizeof(double)));
-            k_basal_local2d<<<nblocks((long long)nq), kBlock, 0, s>>>(g.NQ, dx, dy, L, d_act, d_beta, Auu, Avv);
+            if (assemble_beta == 1) {
+                k_basal_local2d<<<nblocks((long long)nq), kBlock, 0, s>>>(g.NQ, dx, dy, L, d_act, d_beta, Auu, Avv);
+            } else {
+                CU(up(d_cell, active_cell, ncell * sizeof(int32_t)));
+                CU(up(d_xv, xv, nq * sizeof(double)));
+                CU(up(d_yv, yv, nq * sizeof(double)));
+                k_basal_standard<false><<<nblocks((long long)nq), kBlock, 0, s>>>(nx, ny, 1, nhalo, L, d_cell, d_xv,
+                                                                                  d_yv, d_beta, d_beta, Auu, Avv,
+                                                                                  d_sing);
+            }
             CU(cudaGetLastError());
         }
         if (umask) {
@@ -514,7 +546,10 @@ struct Solver {
                                                                     Auv, Avu, Avv, bu, bv);
             CU(cudaGetLastError());
         }
+        int sing = 0;
+        CU(cudaMemcpyAsync(&sing, d_sing, sizeof(int), cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
+        if (sing) return fail(CISMGPU_EINVAL, "Jacobian matrix is singular (a basal cell of zero area)");
         return CISMGPU_OK;
     }
 
@@ -2039,13 +2074,16 @@ static int oneshot_boundary3d(int which, int nx, int ny, int nz, int nhalo, doub
                               const int32_t *active_vertex, const double *beta, const double *lsrf,
                               const int32_t *umask, const int32_t *vmask, const double *uvel, const double *vvel,
                               const int32_t *indx, double *Auu, double *Auv, double *Avu, double *Avv, double *bu,
-                              double *bv) {
+                              double *bv, int assemble_beta = 1, const int32_t *active_cell = nullptr,
+                              const double *xv = nullptr, const double *yv = nullptr) {
     std::lock_guard<std::mutex> lk(g_mu);
     g_last_error.clear();
     if (!active_vertex || !indx || !Auu || !Avv) return fail(CISMGPU_EINVAL, "null pointer argument");
     if (which == 0 && (!umask || !vmask || !uvel || !vvel || !Auv || !Avu || !bu || !bv))
         return fail(CISMGPU_EINVAL, "null pointer argument");
     if (which == 1 && (!beta || !lsrf)) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (which == 1 && assemble_beta == 0 && (!active_cell || !xv || !yv))
+        return fail(CISMGPU_EINVAL, "null pointer argument");
     if (nx < 6 || ny < 6 || nz < 1 || nz > kMaxNz) return fail(CISMGPU_EINVAL, "grid too small or nz outside 1..64");
     if (nhalo < 1 || 2 * nhalo >= nx || 2 * nhalo >= ny) return fail(CISMGPU_EINVAL, "nhalo outside the grid");
     TRY(validate_indx(indx, 27));
@@ -2080,7 +2118,8 @@ static int oneshot_boundary3d(int which, int nx, int ny, int nz, int nhalo, doub
     L.raw3 = 1;
     const VecIdx Wb{sv.g.NQ, nz, 0};
     TRY(sv.boundary3d(L, blk[0], blk[1], blk[2], blk[3], dbu, dbv, Wb, nhalo, dx, dy, active_vertex,
-                      which == 1 ? beta : nullptr, lsrf, which == 0 ? umask : nullptr, vmask, uvel, vvel, 0));
+                      which == 1 ? beta : nullptr, lsrf, which == 0 ? umask : nullptr, vmask, uvel, vvel, 0,
+                      assemble_beta, active_cell, xv, yv));
     for (int b = 0; b < 4; ++b)
         if (which == 0 || b == 0 || b == 3)
             CU(cudaMemcpyAsync(host[b], blk[b], bs * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -2097,13 +2136,17 @@ static int oneshot_boundary3d(int which, int nx, int ny, int nz, int nhalo, doub
 static int oneshot_boundary2d(int which, int nx, int ny, int nhalo, double dx, double dy,
                               const int32_t *active_vertex, const double *beta, const int32_t *umask,
                               const int32_t *vmask, const double *uvel, const double *vvel, const int32_t *indx,
-                              double *Auu, double *Auv, double *Avu, double *Avv, double *bu, double *bv) {
+                              double *Auu, double *Auv, double *Avu, double *Avv, double *bu, double *bv,
+                              int assemble_beta = 1, const int32_t *active_cell = nullptr,
+                              const double *xv = nullptr, const double *yv = nullptr) {
     std::lock_guard<std::mutex> lk(g_mu);
     g_last_error.clear();
     if (!active_vertex || !indx || !Auu || !Avv) return fail(CISMGPU_EINVAL, "null pointer argument");
     if (which == 0 && (!umask || !vmask || !uvel || !vvel || !Auv || !Avu || !bu || !bv))
         return fail(CISMGPU_EINVAL, "null pointer argument");
     if (which == 1 && !beta) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (which == 1 && assemble_beta == 0 && (!active_cell || !xv || !yv))
+        return fail(CISMGPU_EINVAL, "null pointer argument");
     if (nx < 6 || ny < 6) return fail(CISMGPU_EINVAL, "grid too small");
     if (nhalo < 1 || 2 * nhalo >= nx || 2 * nhalo >= ny) return fail(CISMGPU_EINVAL, "nhalo outside the grid");
     TRY(validate_indx(indx, 9));
@@ -2137,7 +2180,8 @@ static int oneshot_boundary2d(int which, int nx, int ny, int nhalo, double dx, d
     L.nz = 1;
     L.raw3 = 0;
     TRY(sv.boundary2d(L, blk[0], blk[1], blk[2], blk[3], dbu, dbv, nhalo, dx, dy, active_vertex,
-                      which == 1 ? beta : nullptr, which == 0 ? umask : nullptr, vmask, uvel, vvel, 0));
+                      which == 1 ? beta : nullptr, which == 0 ? umask : nullptr, vmask, uvel, vvel, 0,
+                      assemble_beta, active_cell, xv, yv));
     for (int b = 0; b < 4; ++b)
         if (which == 0 || b == 0 || b == 3)
             CU(cudaMemcpyAsync(host[b], blk[b], bs * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -2209,13 +2253,15 @@ int cismgpu_dirichlet_boundary_conditions_3d(int nx, int ny, int nz, int nhalo, 
 }
 
 int cismgpu_basal_sliding_bc_3d(int nx, int ny, int nz, int nhalo, double dx, double dy,
-                                const int32_t *active_vertex, const double *beta, const double *lsrf,
+                                const int32_t *active_cell, const int32_t *active_vertex, const double *beta,
+                                const double *lsrf, const double *xVertex, const double *yVertex,
                                 int whichassemble_beta, const int32_t *indxA_3d, double *Auu, double *Avv) {
     g_last_error.clear();
-    if (whichassemble_beta != 1)
-        return fail(CISMGPU_EUNSUPPORTED, "only the local basal assembly (HO_ASSEMBLE_BETA_LOCAL) is built");
+    if (whichassemble_beta != 0 && whichassemble_beta != 1)
+        return fail(CISMGPU_EINVAL, "whichassemble_beta must be 0 (standard) or 1 (local)");
     return oneshot_boundary3d(1, nx, ny, nz, nhalo, dx, dy, active_vertex, beta, lsrf, nullptr, nullptr, nullptr,
-                              nullptr, indxA_3d, Auu, nullptr, nullptr, Avv, nullptr, nullptr);
+                              nullptr, indxA_3d, Auu, nullptr, nullptr, Avv, nullptr, nullptr, whichassemble_beta,
+                              active_cell, xVertex, yVertex);
 }
 
 int cismgpu_solver_assemble_system_3d(cismgpu_solver_t *h, int nhalo, double dx, double dy, const double *sigma,
@@ -2223,13 +2269,15 @@ int cismgpu_solver_assemble_system_3d(cismgpu_solver_t *h, int nhalo, double dx,
                                       const double *xVertex, const double *yVertex, const double *stagusrf,
                                       const double *stagthck, const double *flwafact, int whichapprox,
                                       int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
-                                      const double *beta, const double *lsrf, const double *loadu,
-                                      const double *loadv, const int32_t *umask_dirichlet,
+                                      const double *beta, const double *lsrf, int whichassemble_beta,
+                                      const double *loadu, const double *loadv, const int32_t *umask_dirichlet,
                                       const int32_t *vmask_dirichlet, double *efvs) {
     g_last_error.clear();
     if (!h) return fail(CISMGPU_EINVAL, "null argument");
     if (!active_vertex || !loadu || !loadv || (!beta) != (!lsrf) || (!umask_dirichlet) != (!vmask_dirichlet))
         return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (whichassemble_beta != 0 && whichassemble_beta != 1)
+        return fail(CISMGPU_EINVAL, "whichassemble_beta must be 0 (standard) or 1 (local)");
     // the stiffness blocks from the handle's current velocity (takes and releases the lock)
     TRY(cismgpu_solver_assemble_stiffness_3d(h, nhalo, sigma, active_cell, xVertex, yVertex, nullptr, nullptr,
                                              stagusrf, stagthck, flwafact, whichapprox, whichefvs, efvs_constant,
@@ -2249,7 +2297,7 @@ int cismgpu_solver_assemble_system_3d(cismgpu_solver_t *h, int nhalo, double dx,
     TRY(sv.put_vec(VB_V, loadv));
     TRY(sv.boundary3d(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, p.bu, p.bv, VecIdx{sv.g.NQ, sv.g.nz, 1}, nhalo, dx,
                       dy, active_vertex, beta, lsrf, umask_dirichlet, vmask_dirichlet, nullptr, nullptr,
-                      sv.x_current ? VX_U : VX0_U));
+                      sv.x_current ? VX_U : VX0_U, whichassemble_beta, active_cell, xVertex, yVertex));
     // staggered_parallel_halo of the four blocks (every (m, k) plane) and of b (:2893-2904)
     Geom gA = sv.g;
     gA.nz = 27 * sv.g.nz;
@@ -2273,27 +2321,31 @@ int cismgpu_dirichlet_boundary_conditions_2d(int nx, int ny, int nhalo, const in
                               uvel, vvel, indxA_2d, Auu, Auv, Avu, Avv, bu, bv);
 }
 
-int cismgpu_basal_sliding_bc_2d(int nx, int ny, int nhalo, double dx, double dy, const int32_t *active_vertex,
-                                const double *beta, int whichassemble_beta, const int32_t *indxA_2d, double *Auu,
+int cismgpu_basal_sliding_bc_2d(int nx, int ny, int nhalo, double dx, double dy, const int32_t *active_cell,
+                                const int32_t *active_vertex, const double *beta, const double *xVertex,
+                                const double *yVertex, int whichassemble_beta, const int32_t *indxA_2d, double *Auu,
                                 double *Avv) {
     g_last_error.clear();
-    if (whichassemble_beta != 1)
-        return fail(CISMGPU_EUNSUPPORTED, "only the local basal assembly (HO_ASSEMBLE_BETA_LOCAL) is built");
+    if (whichassemble_beta != 0 && whichassemble_beta != 1)
+        return fail(CISMGPU_EINVAL, "whichassemble_beta must be 0 (standard) or 1 (local)");
     return oneshot_boundary2d(1, nx, ny, nhalo, dx, dy, active_vertex, beta, nullptr, nullptr, nullptr, nullptr,
-                              indxA_2d, Auu, nullptr, nullptr, Avv, nullptr, nullptr);
+                              indxA_2d, Auu, nullptr, nullptr, Avv, nullptr, nullptr, whichassemble_beta, active_cell,
+                              xVertex, yVertex);
 }
 
 int cismgpu_solver_assemble_system_2d(cismgpu_solver_t *h, int nz, int nhalo, double dx, double dy,
                                       const double *sigma, const int32_t *active_cell, const int32_t *active_vertex,
                                       const double *xVertex, const double *yVertex, const double *stagthck,
                                       const double *flwafact, int whichefvs, double efvs_constant,
-                                      double effstrain_min, double n_glen, const double *beta, const double *loadu,
-                                      const double *loadv, const int32_t *umask_dirichlet,
+                                      double effstrain_min, double n_glen, const double *beta, int whichassemble_beta,
+                                      const double *loadu, const double *loadv, const int32_t *umask_dirichlet,
                                       const int32_t *vmask_dirichlet, double *efvs) {
     g_last_error.clear();
     if (!h) return fail(CISMGPU_EINVAL, "null argument");
     if (!active_vertex || !loadu || !loadv || (!umask_dirichlet) != (!vmask_dirichlet))
         return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (whichassemble_beta != 0 && whichassemble_beta != 1)
+        return fail(CISMGPU_EINVAL, "whichassemble_beta must be 0 (standard) or 1 (local)");
     TRY(cismgpu_solver_assemble_stiffness_2d(h, nz, nhalo, sigma, active_cell, xVertex, yVertex, nullptr, nullptr,
                                              stagthck, flwafact, whichefvs, efvs_constant, effstrain_min, n_glen,
                                              efvs));
@@ -2311,7 +2363,8 @@ int cismgpu_solver_assemble_system_2d(cismgpu_solver_t *h, int nz, int nhalo, do
     TRY(sv.put_vec(VB_U, loadu));  // bu_2d = loadu_2d, bv_2d = loadv_2d (:2620-2621)
     TRY(sv.put_vec(VB_V, loadv));
     TRY(sv.boundary2d(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, p.bu, p.bv, nhalo, dx, dy, active_vertex, beta,
-                      umask_dirichlet, vmask_dirichlet, nullptr, nullptr, sv.x_current ? VX_U : VX0_U));
+                      umask_dirichlet, vmask_dirichlet, nullptr, nullptr, sv.x_current ? VX_U : VX0_U,
+                      whichassemble_beta, active_cell, xVertex, yVertex));
     // staggered_parallel_halo of every coefficient plane and of b (:2652-2666)
     Geom gA = sv.g;
     gA.nz = 9;

@@ -236,23 +236,23 @@
          real(c_double), intent(inout) :: Auu(*), Auv(*), Avu(*), Avv(*), bu(*), bv(*)
        end function c_dirichlet_2d
 
-       integer(c_int) function c_basal_3d(nx, ny, nz, nhalo, dx, dy, active_vertex, beta, lsrf, &
-            whichassemble_beta, indxA_3d, Auu, Avv) bind(C, name="cismgpu_basal_sliding_bc_3d")
+       integer(c_int) function c_basal_3d(nx, ny, nz, nhalo, dx, dy, active_cell, active_vertex, beta, lsrf, &
+            xVertex, yVertex, whichassemble_beta, indxA_3d, Auu, Avv) bind(C, name="cismgpu_basal_sliding_bc_3d")
          import :: c_int, c_double, c_int32_t
          integer(c_int), value :: nx, ny, nz, nhalo, whichassemble_beta
          real(c_double), value :: dx, dy
-         integer(c_int32_t), intent(in) :: active_vertex(*), indxA_3d(*)
-         real(c_double), intent(in) :: beta(*), lsrf(*)
+         integer(c_int32_t), intent(in) :: active_cell(*), active_vertex(*), indxA_3d(*)
+         real(c_double), intent(in) :: beta(*), lsrf(*), xVertex(*), yVertex(*)
          real(c_double), intent(inout) :: Auu(*), Avv(*)
        end function c_basal_3d
 
-       integer(c_int) function c_basal_2d(nx, ny, nhalo, dx, dy, active_vertex, beta, whichassemble_beta, &
-            indxA_2d, Auu, Avv) bind(C, name="cismgpu_basal_sliding_bc_2d")
+       integer(c_int) function c_basal_2d(nx, ny, nhalo, dx, dy, active_cell, active_vertex, beta, xVertex, &
+            yVertex, whichassemble_beta, indxA_2d, Auu, Avv) bind(C, name="cismgpu_basal_sliding_bc_2d")
          import :: c_int, c_double, c_int32_t
          integer(c_int), value :: nx, ny, nhalo, whichassemble_beta
          real(c_double), value :: dx, dy
-         integer(c_int32_t), intent(in) :: active_vertex(*), indxA_2d(*)
-         real(c_double), intent(in) :: beta(*)
+         integer(c_int32_t), intent(in) :: active_cell(*), active_vertex(*), indxA_2d(*)
+         real(c_double), intent(in) :: beta(*), xVertex(*), yVertex(*)
          real(c_double), intent(inout) :: Auu(*), Avv(*)
        end function c_basal_2d
     end interface
@@ -591,7 +591,7 @@
     !-----------------------------------------------------------------------
     ! The boundary routines with the reference's argument lists.  basal_sliding_bc_3d receives
     ! the bed slices Auu(:,nz,:,:), Avv(:,nz,:,:), which the library addresses as one-level
-    ! blocks; the standard finite-element basal form is reported with GM_FATAL.
+    ! blocks.
     subroutine dirichlet_boundary_conditions_3d(nx, ny, nz, nhalo, active_vertex, umask_dirichlet, &
                                                 vmask_dirichlet, uvel, vvel, Auu, Auv, Avu, Avv, bu, bv)
       integer, intent(in) :: nx, ny, nz, nhalo
@@ -639,11 +639,13 @@
       real(dp), dimension(nx-1,ny-1), intent(in) :: beta, xVertex, yVertex
       real(dp), dimension(nx,ny), intent(in) :: lsrf
       real(dp), dimension(nNeighbors,nx-1,ny-1), intent(inout) :: Auu, Avv
-      integer(c_int32_t) :: act(nx-1,ny-1), indx3(27)
+      integer(c_int32_t) :: act(nx-1,ny-1), cell(nx,ny), indx3(27)
       integer :: m
       act = merge(1, 0, active_vertex)
+      cell = merge(1, 0, active_cell)
       indx3 = [(m, m = 1, 27)]
-      call check(c_basal_3d(nx, ny, 1, nhalo, dx, dy, act, beta, lsrf, whichassemble_beta, indx3, Auu, Avv))
+      call check(c_basal_3d(nx, ny, 1, nhalo, dx, dy, cell, act, beta, lsrf, xVertex, yVertex, &
+                            whichassemble_beta, indx3, Auu, Avv))
     end subroutine basal_sliding_bc_3d
 
     !-----------------------------------------------------------------------
@@ -658,11 +660,13 @@
       real(dp), dimension(nx-1,ny-1), intent(in) :: beta, xVertex, yVertex
       real(dp), dimension(nx,ny), intent(in) :: lsrf
       real(dp), dimension(nx-1,ny-1,nNeighbors), intent(inout) :: Auu, Avv
-      integer(c_int32_t) :: act(nx-1,ny-1), indx2(9)
+      integer(c_int32_t) :: act(nx-1,ny-1), cell(nx,ny), indx2(9)
       integer :: m
       act = merge(1, 0, active_vertex)
+      cell = merge(1, 0, active_cell)
       indx2 = [(m, m = 1, 9)]
-      call check(c_basal_2d(nx, ny, nhalo, dx, dy, act, beta, whichassemble_beta, indx2, Auu, Avv))
+      call check(c_basal_2d(nx, ny, nhalo, dx, dy, cell, act, beta, xVertex, yVertex, whichassemble_beta, &
+                            indx2, Auu, Avv))
     end subroutine basal_sliding_bc_2d
 
   end module glissade_velo_higher_pcg_gpu

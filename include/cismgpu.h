@@ -291,19 +291,23 @@ int cismgpu_dirichlet_boundary_conditions_3d(int nx, int ny, int nz, int nhalo, 
                                              double *Auu, double *Auv, double *Avu, double *Avv, double *bu,
                                              double *bv);
 
-/* Replaces basal_sliding_bc_3d (glissade_velo_higher.F90:8815-9129) for
- * whichassemble_beta = HO_ASSEMBLE_BETA_LOCAL (1, CISM's default; the standard finite-element
- * form returns CISMGPU_EUNSUPPORTED): at every active vertex the bed diagonal (level nz) of Auu
- * and Avv gains dx*dy/vol0 * beta / cos(theta), theta the slope angle of the lower surface
- * lsrf(nx,ny) staggered to the vertices (glissade_stagger, glissade_slope_angle).  beta
- * (nx-1,ny-1); Auu, Avv the full (27,nz,nx-1,ny-1) blocks.  atan and cos are CUDA's. */
+/* Replaces basal_sliding_bc_3d (glissade_velo_higher.F90:8815-9129).  whichassemble_beta = 1
+ * (HO_ASSEMBLE_BETA_LOCAL, CISM's default): at every active vertex the bed diagonal (level nz)
+ * of Auu and Avv gains dx*dy/vol0 * beta / cos(theta), theta the slope angle of the lower
+ * surface lsrf(nx,ny) staggered to the vertices (glissade_stagger, glissade_slope_angle); atan
+ * and cos are CUDA's.  whichassemble_beta = 0 (standard): per active cell, 4-point quadrature of
+ * beta phi_r phi_c over the lower surface (the curved area factor,
+ * get_area_scale_factor_curved_2d) added to the bed level's 9 horizontal couplings, point by
+ * point in the reference's order (its sqrt is IEEE, so bit-exact).  beta, xVertex, yVertex
+ * (nx-1,ny-1); active_cell (nx,ny); Auu, Avv (27,nz,nx-1,ny-1) (nz = 1 for the bed slices). */
 int cismgpu_basal_sliding_bc_3d(int nx, int ny, int nz, int nhalo, double dx, double dy,
-                                const int32_t *active_vertex, const double *beta, const double *lsrf,
+                                const int32_t *active_cell, const int32_t *active_vertex, const double *beta,
+                                const double *lsrf, const double *xVertex, const double *yVertex,
                                 int whichassemble_beta, const int32_t *indxA_3d, double *Auu, double *Avv);
 
-/* Replaces dirichlet_boundary_conditions_2d (glissade_velo_higher.F90:9133-9301) and, for
- * HO_ASSEMBLE_BETA_LOCAL, basal_sliding_bc_2d (:8281-8531: the diagonal of Auu and Avv at every
- * active vertex += (dx*dy/vol0) * beta).  Masks, velocities, beta and b (nx-1,ny-1); A**
+/* Replaces dirichlet_boundary_conditions_2d (glissade_velo_higher.F90:9133-9301) and
+ * basal_sliding_bc_2d (:8281-8531: local form, the diagonal of Auu and Avv at every active
+ * vertex += (dx*dy/vol0) * beta; standard form, the 4-point quadrature with the flat Jacobian).  Masks, velocities, beta and b (nx-1,ny-1); A**
  * (nx-1,ny-1,9) through indxA_2d.  As in the reference's 2D routine, a u-prescribed vertex
  * gets unit diagonals in Auu, Auv and Avu (a v-prescribed one then zero Auv, Avu and unit Avv),
  * and the moves into b are summed in its order (offsets outermost).  Bit-exact. */
@@ -312,8 +316,9 @@ int cismgpu_dirichlet_boundary_conditions_2d(int nx, int ny, int nhalo, const in
                                              const double *uvel, const double *vvel, const int32_t *indxA_2d,
                                              double *Auu, double *Auv, double *Avu, double *Avv, double *bu,
                                              double *bv);
-int cismgpu_basal_sliding_bc_2d(int nx, int ny, int nhalo, double dx, double dy, const int32_t *active_vertex,
-                                const double *beta, int whichassemble_beta, const int32_t *indxA_2d, double *Auu,
+int cismgpu_basal_sliding_bc_2d(int nx, int ny, int nhalo, double dx, double dy, const int32_t *active_cell,
+                                const int32_t *active_vertex, const double *beta, const double *xVertex,
+                                const double *yVertex, int whichassemble_beta, const int32_t *indxA_2d, double *Auu,
                                 double *Avv);
 
 /* ------------------------------------------------------------------------
@@ -473,8 +478,8 @@ int cismgpu_solver_assemble_system_3d(cismgpu_solver_t *s, int nhalo, double dx,
                                       const double *xVertex, const double *yVertex, const double *stagusrf,
                                       const double *stagthck, const double *flwafact, int whichapprox,
                                       int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
-                                      const double *beta, const double *lsrf, const double *loadu,
-                                      const double *loadv, const int32_t *umask_dirichlet,
+                                      const double *beta, const double *lsrf, int whichassemble_beta,
+                                      const double *loadu, const double *loadv, const int32_t *umask_dirichlet,
                                       const int32_t *vmask_dirichlet, double *efvs);
 
 /* The 2D (SSA) counterpart (glissade_velo_higher.F90:2560-2666): stiffness from the handle's
@@ -484,8 +489,8 @@ int cismgpu_solver_assemble_system_2d(cismgpu_solver_t *s, int nz, int nhalo, do
                                       const double *sigma, const int32_t *active_cell, const int32_t *active_vertex,
                                       const double *xVertex, const double *yVertex, const double *stagthck,
                                       const double *flwafact, int whichefvs, double efvs_constant,
-                                      double effstrain_min, double n_glen, const double *beta, const double *loadu,
-                                      const double *loadv, const int32_t *umask_dirichlet,
+                                      double effstrain_min, double n_glen, const double *beta, int whichassemble_beta,
+                                      const double *loadu, const double *loadv, const int32_t *umask_dirichlet,
                                       const int32_t *vmask_dirichlet, double *efvs);
 
 /* The 2D (SSA) assembly into a 2D handle; nz: the number of sigma levels of flwafact. */

@@ -86,7 +86,7 @@ def test_status_names_match_the_header():
 
 def test_assembly_entry_points_validate_before_the_device(lib):
     """The assembly and boundary entry points reject bad arguments with the library's status
-    (4 EINVAL, 3 EUNSUPPORTED) before any device call, so these run without a GPU."""
+    (4 EINVAL) before any device call, so these run without a GPU."""
     import numpy as np
     import cism_b200 as cg
     from tests.test_oracle_assembly import geometry
@@ -110,14 +110,15 @@ def test_assembly_entry_points_validate_before_the_device(lib):
                                         g["stagthck"], ff)
     assert e.value.status == 4
     A = [np.zeros((ny - 1, nx - 1, nz, 27)) for _ in range(2)]
-    with pytest.raises(cg.CismGpuError) as e:  # the standard finite-element form is not built
-        cg.basal_sliding_bc_3d(nx, ny, nz, 2, 1.0, 1.0, g["av"], np.zeros((ny - 1, nx - 1)), np.zeros((ny, nx)),
-                               *A, whichassemble_beta=0)
-    assert e.value.status == 3
+    with pytest.raises(cg.CismGpuError) as e:  # whichassemble_beta is 0 (standard) or 1 (local)
+        cg.basal_sliding_bc_3d(nx, ny, nz, 2, 1.0, 1.0, act, g["av"], np.zeros((ny - 1, nx - 1)), np.zeros((ny, nx)),
+                               g["xVertex"], g["yVertex"], *A, whichassemble_beta=2)
+    assert e.value.status == 4
     A2 = [np.zeros((9, ny - 1, nx - 1)) for _ in range(2)]
     with pytest.raises(cg.CismGpuError) as e:
-        cg.basal_sliding_bc_2d(nx, ny, 2, 1.0, 1.0, g["av"], np.zeros((ny - 1, nx - 1)), *A2, whichassemble_beta=0)
-    assert e.value.status == 3
+        cg.basal_sliding_bc_2d(nx, ny, 2, 1.0, 1.0, act, g["av"], np.zeros((ny - 1, nx - 1)), g["xVertex"],
+                               g["yVertex"], *A2, whichassemble_beta=2)
+    assert e.value.status == 4
     bad = np.arange(1, 28, dtype=np.int32)
     bad[5] = 99
     with pytest.raises(cg.CismGpuError) as e:  # indxA entry outside 1..27

@@ -252,15 +252,13 @@ def test_basal_local(gpu_lib):
     beta = asm.lognormal_beta((g["ny"] - 1, g["nx"] - 1), 5)
     wu, wv, _ = oracle.basal_local_3d(g["nx"], g["ny"], g["nz"], g["dx"], g["dx"], g["av"], beta, lsrf, S.Auu, S.Avv)
     Auu, Avv = np.array(S.Auu, copy=True), np.array(S.Avv, copy=True)
-    cg.basal_sliding_bc_3d(g["nx"], g["ny"], g["nz"], 2, g["dx"], g["dx"], g["av"], beta, lsrf, Auu, Avv)
+    cg.basal_sliding_bc_3d(g["nx"], g["ny"], g["nz"], 2, g["dx"], g["dx"], g["ac"], g["av"], beta, lsrf, g["xVertex"],
+                           g["yVertex"], Auu, Avv)
     for a, b in ((Auu, wu), (Avv, wv)):
         d = np.abs(a - b)
         assert d[..., g["nz"] - 1, 13].max() <= 1e-15 * np.abs(b[..., g["nz"] - 1, 13]).max()
         d[..., g["nz"] - 1, 13] = 0.0
         assert np.all(d == 0.0)
-    with pytest.raises(cg.CismGpuError):
-        cg.basal_sliding_bc_3d(g["nx"], g["ny"], g["nz"], 2, g["dx"], g["dx"], g["av"], beta, lsrf, Auu, Avv,
-                               whichassemble_beta=0)
 
 
 @pytest.mark.parametrize("bed", ["beta", "no-slip"])
@@ -291,7 +289,8 @@ def test_system_on_handle(gpu_lib, bed):
     np.testing.assert_array_equal(efvs_h, efvs)
     bu, bv = np.array(load[0], copy=True), np.array(load[1], copy=True)
     if beta is not None:
-        cg.basal_sliding_bc_3d(nx, ny, nz, 2, g["dx"], g["dx"], g["av"], beta, lsrf, A[0], A[3])
+        cg.basal_sliding_bc_3d(nx, ny, nz, 2, g["dx"], g["dx"], g["ac"], g["av"], beta, lsrf, g["xVertex"],
+                               g["yVertex"], A[0], A[3])
     if um is not None:
         cg.dirichlet_boundary_conditions_3d(nx, ny, nz, 2, g["av"], um, vm, u, v, *A, bu, bv)
     Q = _slab_problem(g)
@@ -323,7 +322,7 @@ def test_dirichlet_2d_and_basal_2d_bitexact(gpu_lib):
     beta = asm.lognormal_beta((ny - 1, nx - 1), 6)
     wu, wv = oracle.basal_local_2d(nx, ny, g["dx"], g["dx"], g["av"], beta, S.Auu, S.Avv)
     Auu, Avv = np.array(S.Auu, copy=True), np.array(S.Avv, copy=True)
-    cg.basal_sliding_bc_2d(nx, ny, 2, g["dx"], g["dx"], g["av"], beta, Auu, Avv)
+    cg.basal_sliding_bc_2d(nx, ny, 2, g["dx"], g["dx"], g["ac"], g["av"], beta, g["xVertex"], g["yVertex"], Auu, Avv)
     np.testing.assert_array_equal(Auu, wu)
     np.testing.assert_array_equal(Avv, wv)
 
@@ -350,7 +349,7 @@ def test_system_2d_on_handle(gpu_lib):
                                                g["yVertex"], u, v, g["stagthck"], ff)
     np.testing.assert_array_equal(efvs_h, efvs)
     bu, bv = np.array(load[0], copy=True), np.array(load[1], copy=True)
-    cg.basal_sliding_bc_2d(nx, ny, 2, g["dx"], g["dx"], g["av"], beta, A[0], A[3])
+    cg.basal_sliding_bc_2d(nx, ny, 2, g["dx"], g["dx"], g["ac"], g["av"], beta, g["xVertex"], g["yVertex"], A[0], A[3])
     cg.dirichlet_boundary_conditions_2d(nx, ny, 2, g["av"], um, um, u, v, *A, bu, bv)
     from tests import problems
     Q = asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], asm.lognormal_beta((ny - 1, nx - 1), 8))
@@ -363,3 +362,30 @@ def test_system_2d_on_handle(gpu_lib):
     np.testing.assert_array_equal(ru, want[0])
     np.testing.assert_array_equal(rv, want[1])
     assert l2 == want[2]
+
+
+@pytest.mark.parametrize("kind", ["3d", "2d"])
+def test_basal_standard_bitexact(gpu_lib, kind):
+    """The standard finite-element basal form: only IEEE operations (sqrt included), so the
+    blocks equal the oracle's bit for bit, also on top of an assembled stiffness."""
+    g = geometry(seed=64)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    lsrf = g["usrf"] - g["thck"] + 5.0 * np.random.default_rng(4).random(g["thck"].shape)
+    beta = asm.lognormal_beta((ny - 1, nx - 1), 6)
+    if kind == "3d":
+        S = asm.assemble_bp_3d(g["thck"], g["usrf"], g["dx"], g["dx"], nz, stiffness_only=True)
+    else:
+        S = asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], np.zeros((ny - 1, nx - 1)),
+                                stiffness_only=True)
+    st, wu, wv = oracle.basal_standard(kind == "3d", nx, ny, nz, g["ac"], g["xVertex"], g["yVertex"], beta,
+                                       lsrf if kind == "3d" else None, S.Auu, S.Avv)
+    assert st == 0
+    Auu, Avv = np.array(S.Auu, copy=True), np.array(S.Avv, copy=True)
+    if kind == "3d":
+        cg.basal_sliding_bc_3d(nx, ny, nz, 2, g["dx"], g["dx"], g["ac"], g["av"], beta, lsrf, g["xVertex"],
+                               g["yVertex"], Auu, Avv, whichassemble_beta=0)
+    else:
+        cg.basal_sliding_bc_2d(nx, ny, 2, g["dx"], g["dx"], g["ac"], g["av"], beta, g["xVertex"], g["yVertex"], Auu,
+                               Avv, whichassemble_beta=0)
+    np.testing.assert_array_equal(Auu, wu)
+    np.testing.assert_array_equal(Avv, wv)
