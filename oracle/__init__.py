@@ -80,6 +80,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_basal_local_2d.argtypes = [i, i, dbl, dbl, d, d, d, d]
         L.oracle_basal_local_2d.restype = None
         L.oracle_basal_standard.argtypes = [i, i, i, i, i, d, d, d, d, d, d, d]
+        L.oracle_assemble_stiffness_2d_diva.argtypes = [i, i, i, i] + [d] * 14 + [i, dbl, dbl, dbl] + [d] * 8
         L.oracle_check_symmetry.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, P(dbl), P(ctypes.c_long)]
         L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
@@ -301,6 +302,28 @@ def basal_standard(is3d, nx, ny, nz, active_cell, xVertex, yVertex, beta, lsrf, 
                                      _p(f64(xVertex)), _p(f64(yVertex)), _p(f64(beta)),
                                      _p(f64(np.zeros((ny, nx)) if lsrf is None else lsrf)), _p(out[0]), _p(out[1]))
     return st, out[0], out[1]
+
+
+def assemble_stiffness_2d_diva(nx, ny, nz, sigma, stagsigma, active_cell, xVertex, yVertex, uvel, vvel, stagthck,
+                               thck, btractx, btracty, dsfx, dsfy, flwafact, efvs_qp_3d, whichefvs=2,
+                               efvs_constant=0.0, effstrain_min=1.0e-8, n_glen=3.0, nhalo=2):
+    """assemble_stiffness_matrix_2d with HO_APPROX_DIVA: vertex fields (ny-1, nx-1), cell fields
+    (ny, nx), flwafact (ny, nx, nz-1), efvs_qp_3d (ny, nx, 4, nz-1) (a copy is updated).
+    Returns (status, efvs (ny, nx, nz-1), efvs_qp_3d, omega_k (ny, nx, nz), omega (ny, nx),
+    Auu, Auv, Avu, Avv (9, ny-1, nx-1))."""
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    eq = np.array(efvs_qp_3d, dtype=np.float64, copy=True)
+    efvs = np.zeros((ny, nx, nz - 1))
+    ok = np.zeros((ny, nx, nz))
+    om = np.zeros((ny, nx))
+    A = [np.zeros((9, ny - 1, nx - 1)) for _ in range(4)]
+    ins = [f64(sigma), f64(stagsigma), np.ascontiguousarray(active_cell, dtype=np.int32), f64(xVertex), f64(yVertex),
+           f64(uvel), f64(vvel), f64(stagthck), f64(thck), f64(btractx), f64(btracty), f64(dsfx), f64(dsfy),
+           f64(flwafact)]
+    st = lib().oracle_assemble_stiffness_2d_diva(nx, ny, nz, nhalo, *[_p(a) for a in ins], whichefvs, efvs_constant,
+                                                 effstrain_min, n_glen, _p(eq), _p(efvs), _p(ok), _p(om),
+                                                 *[_p(a) for a in A])
+    return (st, efvs, eq, ok, om, *A)
 
 
 def reprosum(a) -> float:

@@ -683,3 +683,150 @@ int oracle_basal_standard(int is3d, int nx, int ny, int nz, int nhalo, const int
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// assemble_stiffness_matrix_2d, DIVA branch
+// ---------------------------------------------------------------------------
+namespace {
+
+// compute_effective_viscosity_diva (:7730-7997), the iterative (non-cubic) form, for one
+// quadrature point of a 4-node cell: efvs(1:nz-1) enters holding the previous iteration's
+// values (0: not yet set) and leaves holding the new ones.
+void efvs_diva(int whichefvs, double efvs_constant, double effstrain_min, double n_glen, int nz,
+               const double *stagsigma, const double *phi, const double *dx, const double *dy, const double *u,
+               const double *v, const double *bx, const double *by, double dsfx, double dsfy, const double *flwafact,
+               double *efvs) {
+    const double p_effstr = (1.0 - n_glen) / n_glen;
+    if (whichefvs == kEfvsConstant) {
+        for (int k = 0; k < nz - 1; ++k) efvs[k] = efvs_constant;
+        return;
+    }
+    if (whichefvs == kEfvsFlowfact) {
+        const double effstrain = kVeloScale / kLenScale * kScyr;
+        for (int k = 0; k < nz - 1; ++k) efvs[k] = flwafact[k] * std::pow(effstrain, p_effstr);
+        return;
+    }
+    double du_dx = 0.0, du_dy = 0.0, dv_dx = 0.0, dv_dy = 0.0, taux = 0.0, tauy = 0.0;
+    for (int n = 0; n < 4; ++n) {
+        du_dx = du_dx + dx[n] * u[n];
+        du_dy = du_dy + dy[n] * u[n];
+        dv_dx = dv_dx + dx[n] * v[n];
+        dv_dy = dv_dy + dy[n] * v[n];
+        taux = taux + phi[n] * bx[n];
+        tauy = tauy + phi[n] * by[n];
+    }
+    for (int k = 0; k < nz - 1; ++k) {
+        if (efvs[k] == 0.0) efvs[k] = flwafact[k] * std::pow(effstrain_min, p_effstr);
+        const double du_dz = taux * stagsigma[k] / (efvs[k] * dsfx);
+        const double dv_dz = tauy * stagsigma[k] / (efvs[k] * dsfy);
+        const double sq = effstrain_min * effstrain_min + du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy +
+                          0.25 * ((dv_dx + du_dy) * (dv_dx + du_dy)) + 0.25 * (du_dz * du_dz) * dsfx +
+                          0.25 * (dv_dz * dv_dz) * dsfy;
+        efvs[k] = flwafact[k] * std::pow(sq, p_effstr / 2.0);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+// assemble_stiffness_matrix_2d (:4961-5378) with whichapprox = HO_APPROX_DIVA: per active cell and
+// Gauss point, the layer viscosities of compute_effective_viscosity_diva from the stored ones
+// (efvs_qp_3d (nz-1,4,nx,ny), updated in place), their sigma-weighted average, the element
+// matrix of the Blatter-Pattyn form with dphi_dz = 0 and h*efvs; efvs(k,i,j) the mean over the
+// points per layer; compute_integrals_diva (:5649-5775) into omega_k (nz,nx,ny) and omega
+// (nx,ny) of active cells.  Returns 0, 1 (singular Jacobian) or 2 (nhalo < 2).
+int oracle_assemble_stiffness_2d_diva(int nx, int ny, int nz, int nhalo, const double *sigma, const double *stagsigma,
+                                      const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                      const double *uvel, const double *vvel, const double *stagthck,
+                                      const double *thck, const double *btractx, const double *btracty,
+                                      const double *dsfx, const double *dsfy, const double *flwafact, int whichefvs,
+                                      double efvs_constant, double effstrain_min, double n_glen, double *efvs_qp_3d,
+                                      double *efvs, double *omega_k, double *omega, double *Auu, double *Auv,
+                                      double *Avu, double *Avv) {
+    if (nhalo < 2) return 2;
+    const long NX = nx - 1, NY = ny - 1, NQ = NX * NY;
+    const RefElement2 &R = ref2();
+    std::memset(efvs, 0, sizeof(double) * (size_t)(nz - 1) * nx * ny);
+    for (double *A : {Auu, Auv, Avu, Avv}) std::memset(A, 0, sizeof(double) * 9 * (size_t)NQ);
+    for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+        for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+            const long cidx = (i - 1) + (long)nx * (j - 1);
+            if (!active_cell[cidx]) continue;
+            double Kuu[4][4] = {}, Kuv[4][4] = {}, Kvu[4][4] = {}, Kvv[4][4] = {};
+            double x[4], y[4], u[4], v[4], h[4], bx[4], by[4];
+            for (int n = 0; n < 4; ++n) {
+                const long q = (long)(i + kIsh3[n] - 1) + NX * (j + kJsh3[n] - 1);
+                x[n] = xVertex[q];
+                y[n] = yVertex[q];
+                u[n] = uvel[q];
+                v[n] = vvel[q];
+                h[n] = stagthck[q];
+                bx[n] = btractx[q];
+                by[n] = btracty[q];
+            }
+            double *eq = efvs_qp_3d + (size_t)(nz - 1) * 4 * cidx;  // (nz-1, 4) of this cell
+            const double *ff = flwafact + (size_t)(nz - 1) * cidx;
+            for (int p = 0; p < 4; ++p) {
+                double dx[4], dy[4], dz[4] = {0.0, 0.0, 0.0, 0.0}, detJ;
+                if (!basis_derivs_2d(x, y, R.dxr[p], R.dyr[p], dx, dy, &detJ)) return 1;
+                efvs_diva(whichefvs, efvs_constant, effstrain_min, n_glen, nz, stagsigma, R.phi[p], dx, dy, u, v, bx, by,
+                          dsfx[cidx], dsfy[cidx], ff, eq + (size_t)(nz - 1) * p);
+                double vavg = 0.0;
+                for (int k = 0; k < nz - 1; ++k) vavg = vavg + eq[(size_t)(nz - 1) * p + k] * (sigma[k + 1] - sigma[k]);
+                double h_qp = 0.0;
+                for (int n = 0; n < 4; ++n) h_qp = h_qp + R.phi[p][n] * h[n];
+                const double f = h_qp * vavg * 1.0 * detJ / kVol0;
+                for (int nc = 0; nc < 4; ++nc)
+                    for (int nr = 0; nr < 4; ++nr) {
+                        Kuu[nr][nc] = Kuu[nr][nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc] + dz[nr] * dz[nc]);
+                        Kuv[nr][nc] = Kuv[nr][nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
+                        Kvu[nr][nc] = Kvu[nr][nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
+                        Kvv[nr][nc] = Kvv[nr][nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc] + dz[nr] * dz[nc]);
+                    }
+            }
+            // compute_integrals_diva: omega_kp per point from the bed up, then means over the points
+            std::vector<double> okp((size_t)nz * 4);
+            for (int p = 0; p < 4; ++p) {
+                okp[(size_t)(nz - 1) * 4 + p] = 0.0;
+                for (int k = nz - 2; k >= 0; --k) {
+                    const double depth = 0.5 * (sigma[k] + sigma[k + 1]);
+                    const double dzk = (sigma[k + 1] - sigma[k]) * thck[cidx];
+                    okp[(size_t)k * 4 + p] = okp[(size_t)(k + 1) * 4 + p] + depth / eq[(size_t)(nz - 1) * p + k] * dzk;
+                }
+            }
+            double *ok = omega_k + (size_t)nz * cidx;
+            for (int k = 0; k < nz; ++k) {
+                double sum = 0.0;
+                for (int p = 0; p < 4; ++p) sum = sum + okp[(size_t)k * 4 + p];
+                ok[k] = sum / 4;
+            }
+            double om = 0.0;
+            for (int k = 0; k < nz - 1; ++k) om = om + 0.5 * (ok[k] + ok[k + 1]) * (sigma[k + 1] - sigma[k]);
+            omega[cidx] = om;
+            for (int k = 0; k < nz - 1; ++k) {
+                double &e = efvs[k + (long)(nz - 1) * cidx];
+                e = 0.0;
+            }
+            for (int p = 0; p < 4; ++p)
+                for (int k = 0; k < nz - 1; ++k) {
+                    double &e = efvs[k + (long)(nz - 1) * cidx];
+                    e = e + eq[(size_t)(nz - 1) * p + k];
+                }
+            for (int k = 0; k < nz - 1; ++k) efvs[k + (long)(nz - 1) * cidx] /= 4;
+            for (int nr = 0; nr < 4; ++nr) {
+                const long q = (long)(i + kIsh3[nr] - 1) + NX * (j + kJsh3[nr] - 1);
+                for (int nc = 0; nc < 4; ++nc) {
+                    const int m = (kIsh3[nc] - kIsh3[nr] + 1) + 3 * (kJsh3[nc] - kJsh3[nr] + 1);
+                    const size_t a = (size_t)q + (size_t)NQ * m;
+                    Auu[a] = Auu[a] + Kuu[nr][nc];
+                    Auv[a] = Auv[a] + Kuv[nr][nc];
+                    Avu[a] = Avu[a] + Kvu[nr][nc];
+                    Avv[a] = Avv[a] + Kvv[nr][nc];
+                }
+            }
+        }
+    return 0;
+}
+
+}  // extern "C"

@@ -225,3 +225,86 @@ def test_ssa_constant_viscosity_null_space():
     scale = np.abs(Auu).max()
     assert np.abs(Auu.sum(axis=0)[full]).max() <= 1e-12 * scale
     assert np.abs(Avu.sum(axis=0)[full]).max() <= 1e-12 * scale
+
+
+# ---------------------------------------------------------------------------
+# assemble_stiffness_matrix_2d, DIVA branch (compute_effective_viscosity_diva :7730-7997,
+# compute_integrals_diva :5649-5775)
+# ---------------------------------------------------------------------------
+
+def diva_inputs(g, seed=0, traction=0.0):
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(seed)
+    sig = g["sigma"]
+    stagsig = 0.5 * (sig[:-1] + sig[1:])
+    bx = np.full((ny - 1, nx - 1), traction)
+    by = np.full((ny - 1, nx - 1), -0.5 * traction)
+    dsf = 1.0 + 0.1 * rng.random((ny, nx))
+    return stagsig, bx, by, dsf, dsf[::-1].copy()
+
+
+def run_diva(g, u, v, ff, eq, traction=0.0, seed=0, **kw):
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    stagsig, bx, by, dsfx, dsfy = diva_inputs(g, seed, traction)
+    out = oracle.assemble_stiffness_2d_diva(nx, ny, nz, g["sigma"], stagsig, g["ac"], g["xVertex"], g["yVertex"], u, v,
+                                            g["stagthck"], g["thck"], bx, by, dsfx, dsfy, ff, eq, **kw)
+    assert out[0] == 0
+    return out[1:], (stagsig, bx, by, dsfx, dsfy)
+
+
+def test_diva_without_traction_is_the_ssa_system():
+    """With zero basal traction the vertical shear terms vanish; with one flow factor in all
+    layers DIVA's layer-averaged viscosity is the SSA's (to roundoff)."""
+    g = geometry(seed=35, nz=6)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(7)
+    u, v = 30 * rng.standard_normal((ny - 1, nx - 1)), 30 * rng.standard_normal((ny - 1, nx - 1))
+    ff = np.full((ny, nx, nz - 1), 0.5 * 1e-16 ** (-1 / 3))
+    (efvs, eq, ok, om, *A), _ = run_diva(g, u, v, ff, np.zeros((ny, nx, 4, nz - 1)))
+    e2, A2 = run2(g, u, v, ff=ff)
+    for a, b in zip(A, A2):
+        assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+    act = g["ac"]
+    assert np.abs(efvs[act] - e2[act]).max() <= 1e-13 * np.abs(e2[act]).max()
+    assert np.all(eq[~act] == 0.0) and np.all(eq[act] > 0.0)
+
+
+def test_diva_layer_viscosity_and_integrals():
+    """Linear velocity and uniform traction: each layer's new viscosity is the flow law at the
+    strain rates plus the vertical shear from the traction and the previous viscosity; omega_k
+    and omega are the integrals of compute_integrals_diva."""
+    g = geometry(seed=36, nz=6)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    a, b = (2.0e-3, -1.0e-3), (0.5e-3, 2.5e-3)
+    u = a[0] * g["xVertex"] + a[1] * g["yVertex"]
+    v = b[0] * g["xVertex"] + b[1] * g["yVertex"]
+    rng = np.random.default_rng(8)
+    layer = 0.5 * 1e-16 ** (-1 / 3) * (1 + 0.5 * rng.random(nz - 1))
+    ff = np.broadcast_to(layer, (ny, nx, nz - 1)).copy()
+    eq0 = np.broadcast_to(2.0e6 * (1 + 0.3 * rng.random(nz - 1)), (ny, nx, 4, nz - 1)).copy()
+    T = 5.0e4
+    (efvs, eq, ok, om, *A), (stagsig, bx, by, dsfx, dsfy) = run_diva(g, u, v, ff, eq0, traction=T, seed=3)
+    act = g["ac"]
+    J, I = np.nonzero(act)
+    for j, i in list(zip(J, I))[:: max(1, len(J) // 7)]:
+        sx, sy = dsfx[j, i], dsfy[j, i]
+        du_dz = T * stagsig / (eq0[j, i, 0] * sx)
+        dv_dz = -0.5 * T * stagsig / (eq0[j, i, 0] * sy)
+        sq = (1e-16 + a[0] ** 2 + b[1] ** 2 + a[0] * b[1] + 0.25 * (b[0] + a[1]) ** 2 + 0.25 * du_dz ** 2 * sx
+              + 0.25 * dv_dz ** 2 * sy)
+        want = layer * sq ** ((1 - 3.0) / 3.0 / 2.0)
+        for p in range(4):
+            assert np.abs(eq[j, i, p] - want).max() <= 1e-12 * want.max()
+        sig = g["sigma"]
+        depth = 0.5 * (sig[:-1] + sig[1:])
+        dz = np.diff(sig) * g["thck"][j, i]
+        okp = np.zeros((4, nz))
+        for p in range(4):
+            for k in range(nz - 2, -1, -1):
+                okp[p, k] = okp[p, k + 1] + depth[k] / eq[j, i, p, k] * dz[k]
+        want_ok = okp.sum(axis=0) / 4
+        assert np.abs(ok[j, i] - want_ok).max() <= 1e-13 * want_ok.max()
+        want_om = np.sum(0.5 * (want_ok[:-1] + want_ok[1:]) * np.diff(sig))
+        assert abs(om[j, i] - want_om) <= 1e-13 * want_om
+        np.testing.assert_allclose(efvs[j, i], eq[j, i].mean(axis=0), rtol=1e-14)
+    assert np.all(ok[~act] == 0.0) and np.all(om[~act] == 0.0)
