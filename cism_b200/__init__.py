@@ -31,7 +31,7 @@ __all__ = [
     "compute_residual_vector_2d", "compute_residual_velocity_3d", "compute_residual_velocity_2d",
     "check_symmetry_assembled_matrix_3d", "check_symmetry_assembled_matrix_2d", "assemble_stiffness_matrix_3d",
     "assemble_stiffness_matrix_2d", "dirichlet_boundary_conditions_3d", "basal_sliding_bc_3d",
-    "dirichlet_boundary_conditions_2d", "basal_sliding_bc_2d",
+    "dirichlet_boundary_conditions_2d", "basal_sliding_bc_2d", "assemble_stiffness_matrix_2d_diva",
 ]
 
 ALG_STANDARD, ALG_CHRONGEAR, ALG_MIXED_CHRONGEAR = 0, 1, 2
@@ -193,6 +193,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_basal_sliding_bc_3d.argtypes = [i32, i32, i32, i32, dbl, dbl, d, d, d, d, d, d, i32, d, d, d]
     lib.cismgpu_solver_assemble_system_3d.argtypes = [vp, i32, dbl, dbl, d, d, d, d, d, d, d, d, i32, i32, dbl, dbl,
                                                       dbl, d, d, i32, d, d, d, d, d]
+    lib.cismgpu_assemble_stiffness_matrix_2d_diva.argtypes = [i32, i32, i32, i32] + [d] * 14 + [i32, dbl, dbl, dbl] + \
+        [d] * 9
+    lib.cismgpu_solver_assemble_stiffness_2d_diva.argtypes = [vp, i32, i32] + [d] * 14 + [i32, dbl, dbl, dbl] + [d] * 4
     lib.cismgpu_dirichlet_boundary_conditions_2d.argtypes = [i32, i32, i32, d, d, d, d, d, d, d, d, d, d, d, d]
     lib.cismgpu_basal_sliding_bc_2d.argtypes = [i32, i32, i32, dbl, dbl, d, d, d, d, d, i32, d, d, d]
     lib.cismgpu_solver_assemble_system_2d.argtypes = [vp, i32, i32, dbl, dbl, d, d, d, d, d, d, d, i32, dbl, dbl, dbl,
@@ -206,7 +209,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
               "cismgpu_assemble_stiffness_matrix_2d", "cismgpu_solver_assemble_stiffness_2d",
               "cismgpu_dirichlet_boundary_conditions_3d", "cismgpu_basal_sliding_bc_3d",
               "cismgpu_solver_assemble_system_3d", "cismgpu_dirichlet_boundary_conditions_2d",
-              "cismgpu_basal_sliding_bc_2d", "cismgpu_solver_assemble_system_2d"):
+              "cismgpu_basal_sliding_bc_2d", "cismgpu_solver_assemble_system_2d",
+              "cismgpu_assemble_stiffness_matrix_2d_diva", "cismgpu_solver_assemble_stiffness_2d_diva"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -529,6 +533,39 @@ def basal_sliding_bc_3d(nx, ny, nz, nhalo, dx, dy, active_cell, active_vertex, b
         _ptr(Auu, np.float64, 27 * nv * nz, True), _ptr(Avv, np.float64, 27 * nv * nz, True)))
 
 
+def _diva_inputs(nx, ny, nz, stagsigma, stagthck, thck, btractx, btracty, dsfx, dsfy):
+    nv, nc = (nx - 1) * (ny - 1), nx * ny
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    return [_ptr(f64(stagsigma), np.float64, nz - 1)], [_ptr(stagthck, np.float64, nv), _ptr(f64(thck), np.float64, nc),
+                                                       _ptr(btractx, np.float64, nv), _ptr(btracty, np.float64, nv),
+                                                       _ptr(f64(dsfx), np.float64, nc), _ptr(f64(dsfy), np.float64, nc)]
+
+
+def assemble_stiffness_matrix_2d_diva(nx, ny, nz, nhalo, sigma, stagsigma, active_cell, xVertex, yVertex, uvel_2d,
+                                      vvel_2d, stagthck, thck, btractx, btracty, dsfx, dsfy, flwafact, efvs_qp_3d,
+                                      whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8, n_glen=3.0,
+                                      indxA_2d=None):
+    """Mirrors assemble_stiffness_matrix_2d with HO_APPROX_DIVA (glissade_velo_higher.F90:4961-5378)
+    on the GPU.  efvs_qp_3d (ny, nx, 4, nz-1), writable float64, is the state, updated in place.
+    Returns (efvs (ny, nx, nz-1), omega_k (ny, nx, nz), omega (ny, nx), Auu, Auv, Avu, Avv)."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    indx = np.arange(1, 10, dtype=np.int32) if indxA_2d is None else np.ascontiguousarray(indxA_2d, dtype=np.int32)
+    efvs = np.zeros((ny, nx, nz - 1))
+    ok = np.zeros((ny, nx, nz))
+    om = np.zeros((ny, nx))
+    A = [np.zeros((9, ny - 1, nx - 1)) for _ in range(4)]
+    head, tail = _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagthck, stagthck, flwafact)
+    ss, dv = _diva_inputs(nx, ny, nz, stagsigma, stagthck, thck, btractx, btracty, dsfx, dsfy)
+    _check(lib, lib.cismgpu_assemble_stiffness_matrix_2d_diva(
+        nx, ny, nz, int(nhalo), head[0], *ss, head[1], head[2], head[3], _ptr(uvel_2d, np.float64, nv),
+        _ptr(vvel_2d, np.float64, nv), *dv, tail[2], int(whichefvs), float(efvs_constant), float(effstrain_min),
+        float(n_glen), _ptr(indx, np.int32, 9), _ptr(efvs_qp_3d, np.float64, (nz - 1) * 4 * nx * ny, True),
+        _ptr(efvs, np.float64, efvs.size, True), _ptr(ok, np.float64, ok.size, True), _ptr(om, np.float64, om.size, True),
+        *[_ptr(a, np.float64, a.size, True) for a in A]))
+    return (efvs, ok, om, *A)
+
+
 def dirichlet_boundary_conditions_2d(nx, ny, nhalo, active_vertex, umask, vmask, uvel, vvel, Auu, Auv, Avu, Avv,
                                      bu, bv, indxA_2d=None):
     """Mirrors dirichlet_boundary_conditions_2d (glissade_velo_higher.F90:9133-9301) on the GPU,
@@ -711,6 +748,29 @@ class DeviceSolver:
             int(whichassemble_beta), _ptr(loadu, np.float64, nv), _ptr(loadv, np.float64, nv), *pm,
             _ptr(efvs, np.float64, efvs.size, True)))
         return efvs
+
+    def assemble_stiffness_diva(self, nz, nhalo, sigma, stagsigma, active_cell, xVertex, yVertex, stagthck, thck,
+                                btractx, btracty, dsfx, dsfy, flwafact, uvel=None, vvel=None, efvs_qp_3d=None,
+                                whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8, n_glen=3.0):
+        """The DIVA assembly into this 2D handle (cismgpu_solver_assemble_stiffness_2d_diva); the
+        layer viscosities stay on the device between calls.  Returns (efvs, omega_k, omega)."""
+        P = self.problem
+        nx, ny = P.nx, P.ny
+        nv = (nx - 1) * (ny - 1)
+        efvs = np.zeros((ny, nx, nz - 1))
+        ok = np.zeros((ny, nx, nz))
+        om = np.zeros((ny, nx))
+        head, tail = _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagthck, stagthck, flwafact)
+        ss, dv = _diva_inputs(nx, ny, nz, stagsigma, stagthck, thck, btractx, btracty, dsfx, dsfy)
+        pu = None if uvel is None else _ptr(uvel, np.float64, nv)
+        pv = None if vvel is None else _ptr(vvel, np.float64, nv)
+        pe = None if efvs_qp_3d is None else _ptr(np.ascontiguousarray(efvs_qp_3d, dtype=np.float64), np.float64,
+                                                  (nz - 1) * 4 * nx * ny)
+        _check(self._lib, self._lib.cismgpu_solver_assemble_stiffness_2d_diva(
+            self.handle, nz, int(nhalo), head[0], *ss, head[1], head[2], head[3], pu, pv, *dv, tail[2], int(whichefvs),
+            float(efvs_constant), float(effstrain_min), float(n_glen), pe, _ptr(efvs, np.float64, efvs.size, True),
+            _ptr(ok, np.float64, ok.size, True), _ptr(om, np.float64, om.size, True)))
+        return efvs, ok, om
 
     def save(self):
         """Accelerated Picard's saved state: the current velocity and A (not b) on the device."""

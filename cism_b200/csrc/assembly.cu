@@ -703,4 +703,174 @@ __global__ void __launch_bounds__(kBlock) k_basal_standard(int nx, int ny, int n
     }
 }
 
+// ---------------------------------------------------------------------------
+// assemble_stiffness_matrix_2d, DIVA branch (:5230-5300 with compute_effective_viscosity_diva
+// :7730-7997, iterative form, and compute_integrals_diva :5649-5775)
+// ---------------------------------------------------------------------------
+// The layer viscosities of each cell's Gauss points are state carried between Picard
+// iterations (efvs_qp_3d(nz-1, 4, nx, ny)).  Every vertex thread recomputes its cells' new
+// viscosities from the previous state; the cell's own thread also writes them, to a second
+// buffer, with the cell's efvs, omega_k and omega, so no thread reads what another writes.
+struct DivaArgs {
+    const double *stagsigma;       // (nz-1)
+    const double *thck;            // (nx, ny) cell thickness
+    const double *bx, *by;         // (nx-1, ny-1) basal traction
+    const double *dsfx, *dsfy;     // (nx, ny) slope factors
+    const double *eq_old;          // (nz-1, 4, nx, ny)
+    double *eq_new, *omega_k, *omega;
+    double init_pow;               // effstrain_min^((1-n)/n), for a state still zero
+};
+
+__device__ bool asm_cell_row_diva(const AsmArgs &a, const DivaArgs &d, int ie, int je, int nr, bool own,
+                                  double acc[4][9]) {
+    const long long NX = a.nx - 1;
+    const int nl = a.nz - 1;
+    double x[4], y[4], u[4], v[4], h[4], bx[4], by[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        const long long q = (long long)(ie + c_ish3[n] - 1) + NX * (je + c_jsh3[n] - 1);
+        x[n] = a.xv[q];
+        y[n] = a.yv[q];
+        u[n] = a.u[q];
+        v[n] = a.v[q];
+        h[n] = a.thck[q];
+        bx[n] = d.bx[q];
+        by[n] = d.by[q];
+    }
+    const long long cidx = (ie - 1) + (long long)a.nx * (je - 1);
+    const double *ff = a.flwafact + (long long)nl * cidx;
+    const double *eo = d.eq_old + (long long)nl * 4 * cidx;
+    double *en = d.eq_new + (long long)nl * 4 * cidx;
+    const double sx = d.dsfx[cidx], sy = d.dsfy[cidx];
+    double Kuu[4], Kuv[4], Kvu[4], Kvv[4];
+#pragma unroll
+    for (int nc = 0; nc < 4; ++nc) Kuu[nc] = Kuv[nc] = Kvu[nc] = Kvv[nc] = 0.0;
+    for (int p = 0; p < 4; ++p) {
+        const double *dxr = c_asm_ref2.dxr[p], *dyr = c_asm_ref2.dyr[p], *phi = c_asm_ref2.phi[p];
+        double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            J00 = J00 + dxr[n] * x[n];
+            J01 = J01 + dxr[n] * y[n];
+            J10 = J10 + dyr[n] * x[n];
+            J11 = J11 + dyr[n] * y[n];
+        }
+        const double detJ = J00 * J11 - J01 * J10;
+        if (!(fabs(detJ) > 0.0)) return false;
+        const double i00 = J11 / detJ, i01 = -J01 / detJ, i10 = -J10 / detJ, i11 = J00 / detJ;
+        double dx[4], dy[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            dx[n] = 0.0 + i00 * dxr[n] + i01 * dyr[n];
+            dy[n] = 0.0 + i10 * dxr[n] + i11 * dyr[n];
+        }
+        double du_dx = 0.0, du_dy = 0.0, dv_dx = 0.0, dv_dy = 0.0, taux = 0.0, tauy = 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            du_dx = du_dx + dx[n] * u[n];
+            du_dy = du_dy + dy[n] * u[n];
+            dv_dx = dv_dx + dx[n] * v[n];
+            dv_dy = dv_dy + dy[n] * v[n];
+            taux = taux + phi[n] * bx[n];
+            tauy = tauy + phi[n] * by[n];
+        }
+        double vavg = 0.0;
+        for (int k = 0; k < nl; ++k) {
+            double e;
+            if (a.whichefvs == 0) {
+                e = a.efvs_constant;
+            } else if (a.whichefvs == 1) {
+                e = ff[k] * a.flowfact_pow;
+            } else {
+                double eold = eo[(long long)nl * p + k];
+                if (eold == 0.0) eold = ff[k] * d.init_pow;
+                const double du_dz = taux * d.stagsigma[k] / (eold * sx);
+                const double dv_dz = tauy * d.stagsigma[k] / (eold * sy);
+                const double sh = dv_dx + du_dy;
+                const double sq = a.effstrain_min * a.effstrain_min + du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy +
+                                  0.25 * (sh * sh) + 0.25 * (du_dz * du_dz) * sx + 0.25 * (dv_dz * dv_dz) * sy;
+                e = ff[k] * pow(sq, a.p_half);
+            }
+            if (own) en[(long long)nl * p + k] = e;
+            vavg = vavg + e * (a.sigma[k + 1] - a.sigma[k]);
+        }
+        double h_qp = 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) h_qp = h_qp + phi[n] * h[n];
+        const double f = h_qp * vavg * 1.0 * detJ / kAsmVol0;
+        const double zero = 0.0 * 0.0;  // dphi_dz(nr)*dphi_dz(nc) of the Blatter-Pattyn form, dphi_dz = 0
+#pragma unroll
+        for (int nc = 0; nc < 4; ++nc) {
+            Kuu[nc] = Kuu[nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc] + zero);
+            Kuv[nc] = Kuv[nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
+            Kvu[nc] = Kvu[nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
+            Kvv[nc] = Kvv[nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc] + zero);
+        }
+    }
+    if (own) {
+        // efvs(k) = the mean over the points; compute_integrals_diva over the new state
+        for (int k = 0; k < nl; ++k) {
+            double e = 0.0;
+            for (int p = 0; p < 4; ++p) e = e + en[(long long)nl * p + k];
+            a.efvs[k + (long long)nl * cidx] = e / 4;
+        }
+        const double tc = d.thck[cidx];
+        double *ok = d.omega_k + (long long)a.nz * cidx;
+        double om = 0.0, prev = 0.0;
+        // omega_k(k) = (sum over p of the integral from the bed to layer k) / 4, from the bed up
+        double okp[4] = {0.0, 0.0, 0.0, 0.0};
+        ok[a.nz - 1] = (((0.0 + okp[0]) + okp[1]) + okp[2] + okp[3]) / 4;
+        for (int k = nl - 1; k >= 0; --k) {
+            const double depth = 0.5 * (a.sigma[k] + a.sigma[k + 1]);
+            const double dzk = (a.sigma[k + 1] - a.sigma[k]) * tc;
+            double sum = 0.0;
+            for (int p = 0; p < 4; ++p) {
+                okp[p] = okp[p] + depth / en[(long long)nl * p + k] * dzk;
+                sum = sum + okp[p];
+            }
+            ok[k] = sum / 4;
+        }
+        for (int k = 0; k < nl; ++k) {
+            prev = 0.5 * (ok[k] + ok[k + 1]);
+            om = om + prev * (a.sigma[k + 1] - a.sigma[k]);
+        }
+        d.omega[cidx] = om;
+    }
+#pragma unroll
+    for (int nc = 0; nc < 4; ++nc) {
+        const int m = (c_ish3[nc] - c_ish3[nr] + 1) + 3 * (c_jsh3[nc] - c_jsh3[nr] + 1);
+        acc[0][m] = acc[0][m] + Kuu[nc];
+        acc[1][m] = acc[1][m] + Kuv[nc];
+        acc[2][m] = acc[2][m] + Kvu[nc];
+        acc[3][m] = acc[3][m] + Kvv[nc];
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(kAsmBlock) k_assemble2d_diva(AsmArgs a, DivaArgs d, SymIdx L, double *Auu,
+                                                               double *Auv, double *Avu, double *Avv) {
+    const long long NX = a.nx - 1, NQ = NX * (a.ny - 1);
+    const long long q = (long long)blockIdx.x * kAsmBlock + threadIdx.x;
+    if (q >= NQ) return;
+    const int j0 = (int)(q / NX), i0 = (int)(q - (long long)j0 * NX);
+    const int iR = i0 + 1, jR = j0 + 1;
+    double acc[4][9];
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) acc[b][c] = 0.0;
+    for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+            const int je = jR + dj, ie = iR + di;
+            if (ie < a.nhalo + 1 || ie > a.nx - a.nhalo + 1 || je < a.nhalo + 1 || je > a.ny - a.nhalo + 1) continue;
+            if (!a.active_cell[(ie - 1) + (long long)a.nx * (je - 1)]) continue;
+            const int nr = dj == 0 ? (di == 0 ? 2 : 3) : (di == 0 ? 1 : 0);
+            if (!asm_cell_row_diva(a, d, ie, je, nr, dj == 0 && di == 0, acc)) atomicExch(a.singular, 1);
+        }
+    double *B[4] = {Auu, Auv, Avu, Avv};
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+        for (int c = 0; c < 9; ++c) B[b][L.at(c, 0, q)] = acc[b][c];
+}
+
 }  // namespace cismgpu

@@ -102,6 +102,46 @@ struct Ptrs {
     double *bu, *bv, *xu, *xv, *ru, *rv, *du, *dv, *qu, *qv, *zu, *zv, *Azu, *Azv, *x0u, *x0v;
 };
 
+// The reference elements of the assembly kernels in constant memory (glissade_velo_higher.F90
+// :314-392, :528-570), once per process.
+static int asm_ref_ready() {
+    static std::once_flag ref_once;
+    static cudaError_t ref_status = cudaSuccess;
+    std::call_once(ref_once, [] {
+        AsmRef r;
+        AsmRef2 r2;
+        const double rs = 1.0 / std::sqrt(3.0);
+        const double xq[8] = {-rs, rs, rs, -rs, -rs, rs, rs, -rs};
+        const double yq[8] = {-rs, -rs, rs, rs, -rs, -rs, rs, rs};
+        const double zq[8] = {-rs, -rs, -rs, -rs, rs, rs, rs, rs};
+        const double sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1}, sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1},
+                     sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};  // node corners of the reference cube
+        for (int p = 0; p < 8; ++p) {
+            r.wqp[p] = 1.0;
+            for (int n = 0; n < 8; ++n) {  // d/dxr of (1 +- x)(1 +- y)(1 +- z)/8, as :362-389
+                const double fx = sx[n] < 0 ? 1.0 - xq[p] : 1.0 + xq[p];
+                const double fy = sy[n] < 0 ? 1.0 - yq[p] : 1.0 + yq[p];
+                const double fz = sz[n] < 0 ? 1.0 - zq[p] : 1.0 + zq[p];
+                r.dxr[p][n] = sx[n] * fy * fz / 8.0;
+                r.dyr[p][n] = sy[n] * fx * fz / 8.0;
+                r.dzr[p][n] = sz[n] * fx * fy / 8.0;
+            }
+        }
+        for (int p = 0; p < 4; ++p)  // the square: points and nodes are the cube's first four
+            for (int n = 0; n < 4; ++n) {
+                const double fx = sx[n] < 0 ? 1.0 - xq[p] : 1.0 + xq[p];
+                const double fy = sy[n] < 0 ? 1.0 - yq[p] : 1.0 + yq[p];
+                r2.phi[p][n] = fx * fy / 4.0;
+                r2.dxr[p][n] = sx[n] * fy / 4.0;
+                r2.dyr[p][n] = sy[n] * fx / 4.0;
+            }
+        ref_status = cudaMemcpyToSymbol(c_asm_ref, &r, sizeof(r));
+        if (ref_status == cudaSuccess) ref_status = cudaMemcpyToSymbol(c_asm_ref2, &r2, sizeof(r2));
+    });
+    CU(ref_status);
+    return CISMGPU_OK;
+}
+
 struct Solver {
     Geom g{};
     bool is3d = false;
@@ -116,6 +156,10 @@ struct Solver {
     DevBuf rsum;              // the reproducible sum's exponent extremes and level sums
     DevBuf asm_in;            // the stiffness assembly's inputs (geometry, flow factor, velocity, efvs)
     DevBuf bc_in;             // the boundary terms' inputs (beta, lsrf, masks, velocity)
+    DevBuf diva_in;           // the DIVA assembly's inputs and outputs
+    DevBuf diva_eq[2];        // DIVA's layer viscosities per Gauss point, previous and new
+    int diva_cur = 0;         // which of diva_eq holds the current state
+    bool diva_valid = false;  // diva_eq[diva_cur] holds a state for this geometry
     bool have_sav = false;
     bool x_current = false;   // the x planes hold a solution (a solve ran since the last upload)
     int32_t hindx[27] = {};   // host copy of the uploaded indxA map (27 or 9 entries)
@@ -143,6 +187,10 @@ struct Solver {
         rsum.release();
         asm_in.release();
         bc_in.release();
+        diva_in.release();
+        diva_eq[0].release();
+        diva_eq[1].release();
+        diva_valid = false;
         have_sav = false;
         mixed.release();
         if (h_done) cudaFreeHost(h_done);
@@ -328,41 +376,7 @@ struct Solver {
                  const double *u, const double *v, int vel_id, const double *usrf, const double *thck,
                  const double *flwafact, int whichapprox, int whichefvs, double efvs_constant,
                  double effstrain_min, double n_glen, double *efvs) {
-        // the reference elements in constant memory (:314-392, :528-570), once per process
-        static std::once_flag ref_once;
-        static cudaError_t ref_status = cudaSuccess;
-        std::call_once(ref_once, [] {
-            AsmRef r;
-            AsmRef2 r2;
-            const double rs = 1.0 / std::sqrt(3.0);
-            const double xq[8] = {-rs, rs, rs, -rs, -rs, rs, rs, -rs};
-            const double yq[8] = {-rs, -rs, rs, rs, -rs, -rs, rs, rs};
-            const double zq[8] = {-rs, -rs, -rs, -rs, rs, rs, rs, rs};
-            const double sx[8] = {-1, 1, 1, -1, -1, 1, 1, -1}, sy[8] = {-1, -1, 1, 1, -1, -1, 1, 1},
-                         sz[8] = {-1, -1, -1, -1, 1, 1, 1, 1};  // node corners of the reference cube
-            for (int p = 0; p < 8; ++p) {
-                r.wqp[p] = 1.0;
-                for (int n = 0; n < 8; ++n) {  // d/dxr of (1 +- x)(1 +- y)(1 +- z)/8, as :362-389
-                    const double fx = sx[n] < 0 ? 1.0 - xq[p] : 1.0 + xq[p];
-                    const double fy = sy[n] < 0 ? 1.0 - yq[p] : 1.0 + yq[p];
-                    const double fz = sz[n] < 0 ? 1.0 - zq[p] : 1.0 + zq[p];
-                    r.dxr[p][n] = sx[n] * fy * fz / 8.0;
-                    r.dyr[p][n] = sy[n] * fx * fz / 8.0;
-                    r.dzr[p][n] = sz[n] * fx * fy / 8.0;
-                }
-            }
-            for (int p = 0; p < 4; ++p)  // the square: points and nodes are the cube's first four
-                for (int n = 0; n < 4; ++n) {
-                    const double fx = sx[n] < 0 ? 1.0 - xq[p] : 1.0 + xq[p];
-                    const double fy = sy[n] < 0 ? 1.0 - yq[p] : 1.0 + yq[p];
-                    r2.phi[p][n] = fx * fy / 4.0;
-                    r2.dxr[p][n] = sx[n] * fy / 4.0;
-                    r2.dyr[p][n] = sy[n] * fx / 4.0;
-                }
-            ref_status = cudaMemcpyToSymbol(c_asm_ref, &r, sizeof(r));
-            if (ref_status == cudaSuccess) ref_status = cudaMemcpyToSymbol(c_asm_ref2, &r2, sizeof(r2));
-        });
-        CU(ref_status);
+        TRY(asm_ref_ready());
         const int nx = g.NX + 1, ny = g.NY + 1;
         const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny, nel = (size_t)(nzl - 1) * ncell;
         const size_t nvel = three_d ? (size_t)nzl * nq : nq;
@@ -460,6 +474,7 @@ struct Solver {
                 k_basal_local3d<<<nblocks((long long)nq), kBlock, 0, s>>>(nx, ny, nz, dx, dy, L, d_act, d_beta,
                                                                           d_lsrf, Auu, Avv);
             } else {
+                TRY(asm_ref_ready());
                 CU(up(d_cell, active_cell, ncell * sizeof(int32_t)));
                 CU(up(d_xv, xv, nq * sizeof(double)));
                 CU(up(d_yv, yv, nq * sizeof(double)));
@@ -523,6 +538,7 @@ struct Solver {
             if (assemble_beta == 1) {
                 k_basal_local2d<<<nblocks((long long)nq), kBlock, 0, s>>>(g.NQ, dx, dy, L, d_act, d_beta, Auu, Avv);
             } else {
+                TRY(asm_ref_ready());
                 CU(up(d_cell, active_cell, ncell * sizeof(int32_t)));
                 CU(up(d_xv, xv, nq * sizeof(double)));
                 CU(up(d_yv, yv, nq * sizeof(double)));
@@ -550,6 +566,90 @@ struct Solver {
         CU(cudaMemcpyAsync(&sing, d_sing, sizeof(int), cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
         if (sing) return fail(CISMGPU_EINVAL, "Jacobian matrix is singular (a basal cell of zero area)");
+        return CISMGPU_OK;
+    }
+
+    // assemble_stiffness_matrix_2d with HO_APPROX_DIVA into four blocks in layout L (NC = 9).
+    // eq_old / eq_new: device buffers of the layer viscosities per Gauss point
+    // (nz-1, 4, nx, ny); eq_new must already hold eq_old's values for the cells the kernel does
+    // not visit.  Host inputs in the reference's layouts; u, v null: the velocity planes
+    // vel_id, vel_id+1.  efvs, omega_k, omega (host, may be null) receive the outputs; omega_k
+    // and omega of cells that are not assembled come back as the caller passed them.
+    int assemble_diva(int nzl, const SymIdx &L, double *Auu, double *Auv, double *Avu, double *Avv, int nhalo,
+                      const double *sigma, const double *stagsigma, const int32_t *active_cell, const double *xv,
+                      const double *yv, const double *u, const double *v, int vel_id, const double *stagthck,
+                      const double *thck, const double *btractx, const double *btracty, const double *dsfx,
+                      const double *dsfy, const double *flwafact, int whichefvs, double efvs_constant,
+                      double effstrain_min, double n_glen, const double *eq_old, double *eq_new, double *efvs,
+                      double *omega_k, double *omega) {
+        TRY(asm_ref_ready());
+        const int nx = g.NX + 1, ny = g.NY + 1;
+        const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny, nel = (size_t)(nzl - 1) * ncell;
+        const bool host_vel = u != nullptr;
+        // doubles: sigma, stagsigma, xv, yv, stagthck, bx, by, thck, dsfx, dsfy, flwafact, efvs,
+        // omega_k, omega, [u, v]; then int32: active_cell, the flag
+        const size_t nd = (size_t)2 * nzl + 5 * nq + 4 * ncell + nel + nel + (size_t)nzl * ncell + ncell +
+                          (host_vel ? 2 * nq : 0);
+        CU(diva_in.ensure(nd * sizeof(double) + (ncell + 1) * sizeof(int32_t)));
+        double *D = diva_in.as<double>();
+        double *d_sigma = D, *d_ss = d_sigma + nzl, *d_xv = d_ss + nzl, *d_yv = d_xv + nq, *d_h = d_yv + nq,
+               *d_bx = d_h + nq, *d_by = d_bx + nq, *d_thck = d_by + nq, *d_sx = d_thck + ncell, *d_sy = d_sx + ncell,
+               *d_ff = d_sy + ncell, *d_efvs = d_ff + nel, *d_ok = d_efvs + nel, *d_om = d_ok + (size_t)nzl * ncell,
+               *d_u = d_om + ncell, *d_v = d_u + nq;
+        int32_t *d_act = reinterpret_cast<int32_t *>(D + nd), *d_sing = d_act + ncell;
+        cudaStream_t s = stream;
+        auto up = [&](void *dst, const void *src, size_t bytes) {
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+        };
+        CU(up(d_sigma, sigma, nzl * sizeof(double)));
+        CU(up(d_ss, stagsigma, (nzl - 1) * sizeof(double)));
+        CU(up(d_xv, xv, nq * sizeof(double)));
+        CU(up(d_yv, yv, nq * sizeof(double)));
+        CU(up(d_h, stagthck, nq * sizeof(double)));
+        CU(up(d_bx, btractx, nq * sizeof(double)));
+        CU(up(d_by, btracty, nq * sizeof(double)));
+        CU(up(d_thck, thck, ncell * sizeof(double)));
+        CU(up(d_sx, dsfx, ncell * sizeof(double)));
+        CU(up(d_sy, dsfy, ncell * sizeof(double)));
+        CU(up(d_ff, flwafact, nel * sizeof(double)));
+        CU(up(d_act, active_cell, ncell * sizeof(int32_t)));
+        if (omega_k) CU(up(d_ok, omega_k, (size_t)nzl * ncell * sizeof(double)));
+        else CU(cudaMemsetAsync(d_ok, 0, (size_t)nzl * ncell * sizeof(double), s));
+        if (omega) CU(up(d_om, omega, ncell * sizeof(double)));
+        else CU(cudaMemsetAsync(d_om, 0, ncell * sizeof(double), s));
+        if (host_vel) {
+            CU(up(d_u, u, nq * sizeof(double)));
+            CU(up(d_v, v, nq * sizeof(double)));
+        }
+        CU(cudaMemsetAsync(d_efvs, 0, nel * sizeof(double), s));
+        CU(cudaMemsetAsync(d_sing, 0, sizeof(int32_t), s));
+        const double p_effstr = (1.0 - n_glen) / n_glen;
+        AsmArgs a;
+        a.nx = nx; a.ny = ny; a.nz = nzl; a.nhalo = nhalo;
+        a.whichapprox = 4; a.whichefvs = whichefvs;
+        a.efvs_constant = efvs_constant; a.effstrain_min = effstrain_min;
+        a.p_half = p_effstr / 2.0;
+        a.flowfact_pow = std::pow(500.0 / 31536000.0 / 200.0e3 * 31536000.0, p_effstr);
+        a.sigma = d_sigma; a.active_cell = d_act; a.xv = d_xv; a.yv = d_yv; a.usrf = d_h; a.thck = d_h;
+        const double *V = vec.as<double>();
+        a.u = host_vel ? d_u : V + (size_t)vel_id * nvec;
+        a.v = host_vel ? d_v : V + (size_t)(vel_id + 1) * nvec;
+        a.vel_planes = 1;
+        a.flwafact = d_ff; a.efvs = d_efvs; a.singular = d_sing;
+        DivaArgs dv;
+        dv.stagsigma = d_ss; dv.thck = d_thck; dv.bx = d_bx; dv.by = d_by; dv.dsfx = d_sx; dv.dsfy = d_sy;
+        dv.eq_old = eq_old; dv.eq_new = eq_new; dv.omega_k = d_ok; dv.omega = d_om;
+        dv.init_pow = std::pow(effstrain_min, p_effstr);  // host pow, as the reference's
+        k_assemble2d_diva<<<(unsigned)((g.NQ + kAsmBlock - 1) / kAsmBlock), kAsmBlock, 0, s>>>(a, dv, L, Auu, Auv,
+                                                                                               Avu, Avv);
+        CU(cudaGetLastError());
+        int sing = 0;
+        CU(cudaMemcpyAsync(&sing, d_sing, sizeof(int), cudaMemcpyDeviceToHost, s));
+        if (efvs) CU(cudaMemcpyAsync(efvs, d_efvs, nel * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (omega_k) CU(cudaMemcpyAsync(omega_k, d_ok, (size_t)nzl * ncell * sizeof(double), cudaMemcpyDeviceToHost, s));
+        if (omega) CU(cudaMemcpyAsync(omega, d_om, ncell * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (sing) return fail(CISMGPU_EINVAL, "Jacobian matrix is singular (an element of zero volume)");
         return CISMGPU_OK;
     }
 
@@ -2193,6 +2293,56 @@ static int oneshot_boundary2d(int which, int nx, int ny, int nhalo, double dx, d
     return CISMGPU_OK;
 }
 
+// assemble_stiffness_matrix_2d with HO_APPROX_DIVA on the caller's host arrays; efvs_qp_3d is
+// the caller's state, read and updated; omega_k and omega change only in assembled cells.
+static int oneshot_assemble_diva(int nx, int ny, int nz, int nhalo, const double *sigma, const double *stagsigma,
+                                 const int32_t *active_cell, const double *xv, const double *yv, const double *u,
+                                 const double *v, const double *stagthck, const double *thck, const double *bx,
+                                 const double *by, const double *dsfx, const double *dsfy, const double *ff,
+                                 int whichefvs, double efvs_constant, double effstrain_min, double n_glen,
+                                 const int32_t *indx, double *efvs_qp_3d, double *efvs, double *omega_k, double *omega,
+                                 double *const blocks[4]) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_error.clear();
+    TRY(validate_assembly(nx, ny, nz, nhalo, whichefvs, n_glen, sigma, active_cell, xv, yv, stagthck, stagthck, ff));
+    if (!stagsigma || !u || !v || !thck || !bx || !by || !dsfx || !dsfy || !indx || !efvs_qp_3d || !blocks[0] ||
+        !blocks[1] || !blocks[2] || !blocks[3])
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    TRY(validate_indx(indx, 9));
+    cismgpu_par_t par{};
+    par.staggered_ilo = 1; par.staggered_ihi = nx - 1; par.staggered_jlo = 1; par.staggered_jhi = ny - 1;
+    par.tasks_row = par.tasks_col = 1;
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
+    TRY(sv.set_geom(make_geom(nx, ny, 1, &par), false));
+    const size_t bs = (size_t)9 * sv.nvec, neq = (size_t)(nz - 1) * 4 * nx * ny;
+    CU(sv.A.ensure(4 * bs * sizeof(double)));
+    sv.mixed.stale = true;
+    CU(sv.diva_eq[0].ensure(neq * sizeof(double)));
+    CU(sv.diva_eq[1].ensure(neq * sizeof(double)));
+    sv.diva_valid = false;  // the one-shot solver's state buffers hold the caller's state only
+    double *eo = sv.diva_eq[0].as<double>(), *en = sv.diva_eq[1].as<double>();
+    cudaStream_t s = sv.stream;
+    CU(cudaMemcpyAsync(eo, efvs_qp_3d, neq * sizeof(double), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(en, eo, neq * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    double *A0 = sv.A.as<double>();
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = c < 9 ? indx[c] : 1;
+    L.n = sv.nvec;
+    L.NQ = sv.g.NQ;
+    L.nz = 1;
+    L.raw3 = 0;
+    TRY(sv.assemble_diva(nz, L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, nhalo, sigma, stagsigma, active_cell, xv, yv,
+                         u, v, 0, stagthck, thck, bx, by, dsfx, dsfy, ff, whichefvs, efvs_constant, effstrain_min,
+                         n_glen, eo, en, efvs, omega_k, omega));
+    for (int k = 0; k < 4; ++k)
+        CU(cudaMemcpyAsync(blocks[k], A0 + k * bs, bs * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(efvs_qp_3d, en, neq * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    return CISMGPU_OK;
+}
+
 // The handle's assembly: blocks into the resident canonical planes.
 static int solver_assemble(cismgpu_solver_t *h, bool three_d, int nzl, int nhalo, const double *sigma,
                            const int32_t *active_cell, const double *xVertex, const double *yVertex,
@@ -2376,6 +2526,70 @@ int cismgpu_solver_assemble_system_2d(cismgpu_solver_t *h, int nz, int nhalo, do
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(s));
     sv.mixed.stale = true;
+    return CISMGPU_OK;
+}
+
+int cismgpu_assemble_stiffness_matrix_2d_diva(int nx, int ny, int nz, int nhalo, const double *sigma,
+                                              const double *stagsigma, const int32_t *active_cell,
+                                              const double *xVertex, const double *yVertex, const double *uvel_2d,
+                                              const double *vvel_2d, const double *stagthck, const double *thck,
+                                              const double *btractx, const double *btracty,
+                                              const double *diva_slope_factor_x, const double *diva_slope_factor_y,
+                                              const double *flwafact, int whichefvs, double efvs_constant,
+                                              double effstrain_min, double n_glen, const int32_t *indxA_2d,
+                                              double *efvs_qp_3d, double *efvs, double *omega_k, double *omega,
+                                              double *Auu, double *Auv, double *Avu, double *Avv) {
+    double *const blocks[4] = {Auu, Auv, Avu, Avv};
+    return oneshot_assemble_diva(nx, ny, nz, nhalo, sigma, stagsigma, active_cell, xVertex, yVertex, uvel_2d, vvel_2d,
+                                 stagthck, thck, btractx, btracty, diva_slope_factor_x, diva_slope_factor_y, flwafact,
+                                 whichefvs, efvs_constant, effstrain_min, n_glen, indxA_2d, efvs_qp_3d, efvs, omega_k,
+                                 omega, blocks);
+}
+
+int cismgpu_solver_assemble_stiffness_2d_diva(cismgpu_solver_t *h, int nz, int nhalo, const double *sigma,
+                                              const double *stagsigma, const int32_t *active_cell,
+                                              const double *xVertex, const double *yVertex, const double *uvel_2d,
+                                              const double *vvel_2d, const double *stagthck, const double *thck,
+                                              const double *btractx, const double *btracty,
+                                              const double *diva_slope_factor_x, const double *diva_slope_factor_y,
+                                              const double *flwafact, int whichefvs, double efvs_constant,
+                                              double effstrain_min, double n_glen, const double *efvs_qp_3d_in,
+                                              double *efvs, double *omega_k, double *omega) {
+    g_last_error.clear();
+    if (!h) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(h->mu);
+    if (h->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch (destroy the batch first)");
+    Solver &sv = h->sv;
+    if (sv.is3d) return fail(CISMGPU_EINVAL, "the handle holds a 3D system");
+    if ((!uvel_2d) != (!vvel_2d)) return fail(CISMGPU_EINVAL, "give both velocity components or neither");
+    const int nx = sv.g.NX + 1, ny = sv.g.NY + 1;
+    TRY(validate_assembly(nx, ny, nz, nhalo, whichefvs, n_glen, sigma, active_cell, xVertex, yVertex, stagthck,
+                          stagthck, flwafact));
+    if (!stagsigma || !thck || !btractx || !btracty || !diva_slope_factor_x || !diva_slope_factor_y)
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    const size_t neq = (size_t)(nz - 1) * 4 * nx * ny;
+    CU(sv.diva_eq[0].ensure(neq * sizeof(double)));
+    CU(sv.diva_eq[1].ensure(neq * sizeof(double)));
+    cudaStream_t s = sv.stream;
+    double *eo = sv.diva_eq[sv.diva_cur].as<double>(), *en = sv.diva_eq[1 - sv.diva_cur].as<double>();
+    if (efvs_qp_3d_in) CU(cudaMemcpyAsync(eo, efvs_qp_3d_in, neq * sizeof(double), cudaMemcpyHostToDevice, s));
+    else if (!sv.diva_valid) CU(cudaMemsetAsync(eo, 0, neq * sizeof(double), s));  // the reference starts at zero
+    CU(cudaMemcpyAsync(en, eo, neq * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = c + 1;
+    L.n = sv.nvec;
+    L.NQ = sv.g.NQ;
+    L.nz = 1;
+    L.raw3 = 0;
+    const size_t bs = (size_t)9 * sv.nvec;
+    double *A0 = sv.A.as<double>();
+    sv.mixed.stale = true;
+    TRY(sv.assemble_diva(nz, L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, nhalo, sigma, stagsigma, active_cell, xVertex,
+                         yVertex, uvel_2d, vvel_2d, sv.x_current ? VX_U : VX0_U, stagthck, thck, btractx, btracty,
+                         diva_slope_factor_x, diva_slope_factor_y, flwafact, whichefvs, efvs_constant, effstrain_min,
+                         n_glen, eo, en, efvs, omega_k, omega));
+    sv.diva_cur = 1 - sv.diva_cur;
+    sv.diva_valid = true;
     return CISMGPU_OK;
 }
 

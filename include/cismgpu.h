@@ -321,6 +321,26 @@ int cismgpu_basal_sliding_bc_2d(int nx, int ny, int nhalo, double dx, double dy,
                                 const double *yVertex, int whichassemble_beta, const int32_t *indxA_2d, double *Auu,
                                 double *Avv);
 
+/* assemble_stiffness_matrix_2d (glissade_velo_higher.F90:4961-5378) with whichapprox =
+ * HO_APPROX_DIVA: per active cell and Gauss point, the layer viscosities of
+ * compute_effective_viscosity_diva (:7730-7997, its iterative form; the cubic form is disabled
+ * in the reference) from the previous ones in efvs_qp_3d (nz-1,4,nx,ny), read and updated, the
+ * basal traction btractx, btracty (nx-1,ny-1) and the slope factors diva_slope_factor_x/_y
+ * (nx,ny); their sigma-weighted average times the thickness in the element matrix; efvs
+ * (nz-1,nx,ny) the mean over the points; compute_integrals_diva (:5649-5775) into omega_k
+ * (nz,nx,ny) and omega (nx,ny) of the assembled cells (the rest unchanged).  thck (nx,ny) is
+ * the cell thickness of the integrals; stagsigma (nz-1).  The flow law's pow is CUDA's. */
+int cismgpu_assemble_stiffness_matrix_2d_diva(int nx, int ny, int nz, int nhalo, const double *sigma,
+                                              const double *stagsigma, const int32_t *active_cell,
+                                              const double *xVertex, const double *yVertex, const double *uvel_2d,
+                                              const double *vvel_2d, const double *stagthck, const double *thck,
+                                              const double *btractx, const double *btracty,
+                                              const double *diva_slope_factor_x, const double *diva_slope_factor_y,
+                                              const double *flwafact, int whichefvs, double efvs_constant,
+                                              double effstrain_min, double n_glen, const int32_t *indxA_2d,
+                                              double *efvs_qp_3d, double *efvs, double *omega_k, double *omega,
+                                              double *Auu, double *Auv, double *Avu, double *Avv);
+
 /* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps
@@ -492,6 +512,20 @@ int cismgpu_solver_assemble_system_2d(cismgpu_solver_t *s, int nz, int nhalo, do
                                       double effstrain_min, double n_glen, const double *beta, int whichassemble_beta,
                                       const double *loadu, const double *loadv, const int32_t *umask_dirichlet,
                                       const int32_t *vmask_dirichlet, double *efvs);
+
+/* The DIVA assembly into a 2D handle.  The layer viscosities per Gauss point stay in HBM
+ * between calls (zero at first, as the reference's); efvs_qp_3d_in non-NULL replaces them
+ * first.  uvel_2d = vvel_2d = NULL: the handle's current velocity.  efvs, omega_k, omega may be
+ * NULL. */
+int cismgpu_solver_assemble_stiffness_2d_diva(cismgpu_solver_t *s, int nz, int nhalo, const double *sigma,
+                                              const double *stagsigma, const int32_t *active_cell,
+                                              const double *xVertex, const double *yVertex, const double *uvel_2d,
+                                              const double *vvel_2d, const double *stagthck, const double *thck,
+                                              const double *btractx, const double *btracty,
+                                              const double *diva_slope_factor_x, const double *diva_slope_factor_y,
+                                              const double *flwafact, int whichefvs, double efvs_constant,
+                                              double effstrain_min, double n_glen, const double *efvs_qp_3d_in,
+                                              double *efvs, double *omega_k, double *omega);
 
 /* The 2D (SSA) assembly into a 2D handle; nz: the number of sigma levels of flwafact. */
 int cismgpu_solver_assemble_stiffness_2d(cismgpu_solver_t *s, int nz, int nhalo, const double *sigma,

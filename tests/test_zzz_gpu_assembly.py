@@ -389,3 +389,96 @@ def test_basal_standard_bitexact(gpu_lib, kind):
                                Avv, whichassemble_beta=0)
     np.testing.assert_array_equal(Auu, wu)
     np.testing.assert_array_equal(Avv, wv)
+
+
+# ---------------------------------------------------------------------------
+# assemble_stiffness_matrix_2d, DIVA branch
+# ---------------------------------------------------------------------------
+
+def _diva_case(seed=37, nz=5, traction=4.0e4):
+    from tests.test_oracle_assembly import diva_inputs
+    g = geometry(seed=seed, nz=nz)
+    nx, ny = g["nx"], g["ny"]
+    rng = np.random.default_rng(seed)
+    u, v = 20 * rng.standard_normal((ny - 1, nx - 1)), 20 * rng.standard_normal((ny - 1, nx - 1))
+    ff = 0.5 * 1e-16 ** (-1 / 3) * (1 + 0.3 * rng.random((ny, nx, nz - 1)))
+    return g, u, v, ff, diva_inputs(g, 2, traction)
+
+
+def _diva_gpu(g, u, v, ff, extra, eq, **kw):
+    stagsig, bx, by, dsfx, dsfy = extra
+    return cg.assemble_stiffness_matrix_2d_diva(g["nx"], g["ny"], g["nz"], 2, g["sigma"], stagsig,
+                                                g["ac"].astype(np.int32), g["xVertex"], g["yVertex"], u, v,
+                                                g["stagthck"], g["thck"], bx, by, dsfx, dsfy, ff, eq, **kw)
+
+
+def _diva_oracle(g, u, v, ff, extra, eq, **kw):
+    stagsig, bx, by, dsfx, dsfy = extra
+    o = oracle.assemble_stiffness_2d_diva(g["nx"], g["ny"], g["nz"], g["sigma"], stagsig, g["ac"], g["xVertex"],
+                                          g["yVertex"], u, v, g["stagthck"], g["thck"], bx, by, dsfx, dsfy, ff, eq, **kw)
+    assert o[0] == 0
+    return o[1:]
+
+
+def test_diva_constant_viscosity_bitexact(gpu_lib):
+    g, u, v, ff, extra = _diva_case()
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    eq = np.zeros((ny, nx, 4, nz - 1))
+    efvs, eq_o, ok_o, om_o, *Ao = _diva_oracle(g, u, v, ff, extra, eq, whichefvs=0, efvs_constant=2.0e6)
+    d = _diva_gpu(g, u, v, ff, extra, eq, whichefvs=0, efvs_constant=2.0e6)
+    np.testing.assert_array_equal(eq, eq_o)
+    for a, b in zip(d, (efvs, ok_o, om_o, *Ao)):
+        np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("start", ["zero", "previous"])
+def test_diva_nonlinear(gpu_lib, start):
+    """The layer viscosities within 1e-14 (pow is CUDA's), the blocks within 1e-13 of their
+    largest, the integrals within 1e-13; from a zero state (the first Picard iteration) and
+    from a previous one."""
+    g, u, v, ff, extra = _diva_case(seed=38)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(1)
+    eq = np.zeros((ny, nx, 4, nz - 1)) if start == "zero" else 1e6 * (1 + rng.random((ny, nx, 4, nz - 1)))
+    eq_gpu = np.array(eq, copy=True)
+    efvs, eq_o, ok_o, om_o, *Ao = _diva_oracle(g, u, v, ff, extra, eq)
+    efvs_d, ok_d, om_d, *Ad = _diva_gpu(g, u, v, ff, extra, eq_gpu)
+    act = g["ac"]
+    assert np.abs(eq_gpu - eq_o).max() <= 1e-14 * np.abs(eq_o).max()
+    assert np.all(eq_gpu[~act] == eq[~act])
+    assert np.abs(efvs_d - efvs).max() <= 1e-14 * np.abs(efvs).max()
+    assert np.abs(ok_d - ok_o).max() <= 1e-13 * np.abs(ok_o).max()
+    assert np.abs(om_d - om_o).max() <= 1e-13 * np.abs(om_o).max()
+    for a, b in zip(Ad, Ao):
+        assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+
+
+def test_diva_state_on_handle(gpu_lib):
+    """Two DIVA assemblies in a row on a handle, the layer viscosities kept on the device, equal
+    the one-shot calls carrying the state on the host, bit for bit."""
+    g, u, v, ff, extra = _diva_case(seed=39)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    stagsig, bx, by, dsfx, dsfy = extra
+    P = asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], asm.lognormal_beta((ny - 1, nx - 1), 8))
+    s = cg.DeviceSolver(P, x0=(u, v))
+    out_h = []
+    try:
+        for it in range(2):
+            out_h.append(s.assemble_stiffness_diva(nz, 2, g["sigma"], stagsig, g["ac"].astype(np.int32), g["xVertex"],
+                                                   g["yVertex"], g["stagthck"], g["thck"], bx, by, dsfx, dsfy, ff,
+                                                   uvel=u * (1 + it), vvel=v * (1 + it)))
+        ru, rv, l2, _ = s.residual_vector()
+    finally:
+        s.close()
+    eq = np.zeros((ny, nx, 4, nz - 1))
+    for it in range(2):
+        d = _diva_gpu(g, u * (1 + it), v * (1 + it), ff, extra, eq)
+        for a, b in zip(out_h[it], d[:3]):
+            np.testing.assert_array_equal(a, b)
+    Q = asm.assemble_ssa_2d(g["thck"], g["usrf"], g["dx"], g["dx"], asm.lognormal_beta((ny - 1, nx - 1), 8))
+    for n, a in zip(BLOCKS, d[3:]):
+        setattr(Q, n, a)
+    want = cg.compute_residual_vector_2d(nx, ny, Q.par, asm.indxA_2d(), Q.active_vertex, Q.Auu, Q.Auv, Q.Avu, Q.Avv,
+                                         Q.bu, Q.bv, u, v)
+    np.testing.assert_array_equal(ru, want[0])
+    np.testing.assert_array_equal(rv, want[1])
