@@ -218,6 +218,20 @@
          real(c_double), intent(out) :: efvs(*), Auu(*), Auv(*), Avu(*), Avv(*)
        end function c_assemble_2d
 
+       integer(c_int) function c_assemble_2d_diva(nx, ny, nz, nhalo, sigma, stagsigma, active_cell, xVertex, &
+            yVertex, uvel_2d, vvel_2d, stagthck, thck, btractx, btracty, dsfx, dsfy, flwafact, whichefvs, &
+            efvs_constant, effstrain_min, n_glen, indxA_2d, efvs_qp_3d, efvs, omega_k, omega, Auu, Auv, Avu, Avv) &
+            bind(C, name="cismgpu_assemble_stiffness_matrix_2d_diva")
+         import :: c_int, c_double, c_int32_t
+         integer(c_int), value :: nx, ny, nz, nhalo, whichefvs
+         real(c_double), intent(in) :: sigma(*), stagsigma(*), xVertex(*), yVertex(*), uvel_2d(*), vvel_2d(*), &
+              stagthck(*), thck(*), btractx(*), btracty(*), dsfx(*), dsfy(*), flwafact(*)
+         integer(c_int32_t), intent(in) :: active_cell(*), indxA_2d(*)
+         real(c_double), value :: efvs_constant, effstrain_min, n_glen
+         real(c_double), intent(inout) :: efvs_qp_3d(*), omega_k(*), omega(*)
+         real(c_double), intent(out) :: efvs(*), Auu(*), Auv(*), Avu(*), Avv(*)
+       end function c_assemble_2d_diva
+
        integer(c_int) function c_dirichlet_3d(nx, ny, nz, nhalo, active_vertex, umask, vmask, uvel, vvel, &
             indxA_3d, Auu, Auv, Avu, Avv, bu, bv) bind(C, name="cismgpu_dirichlet_boundary_conditions_3d")
          import :: c_int, c_double, c_int32_t
@@ -527,8 +541,8 @@
 
     !-----------------------------------------------------------------------
     ! The reference's argument lists (the diagnostic indices, and in 2D the arguments of the
-    ! L1L2 and DIVA branches, are accepted and unused); n_glen is glimmer_physcon's.  The 2D
-    ! form runs the SSA branch; any other approximation is reported with GM_FATAL.
+    ! L1L2 branch, are accepted and unused); n_glen is glimmer_physcon's.  The 2D form runs
+    ! the SSA and DIVA branches; L1L2 is reported with GM_FATAL.
     subroutine assemble_stiffness_matrix_3d(nx, ny, nz, sigma, nhalo, itest, jtest, rtest, active_cell, &
                                             xVertex, yVertex, uvel, vvel, stagusrf, stagthck, flwafact, &
                                             whichapprox, whichefvs, efvs, efvs_constant, effstrain_min, &
@@ -559,7 +573,7 @@
                                             whichefvs, efvs, efvs_constant, effstrain_min, Auu, Auv, Avu, Avv, &
                                             dusrf_dx, dusrf_dy, thck, btractx, btracty, omega_k, omega, efvs_qp_3d)
       use glimmer_physcon, only: n_glen
-      use glide_types, only: HO_APPROX_SSA
+      use glide_types, only: HO_APPROX_SSA, HO_APPROX_DIVA
       integer, intent(in) :: nx, ny, nz, nhalo, itest, jtest, rtest, whichapprox, whichefvs
       real(dp), dimension(nz), intent(in) :: sigma
       real(dp), dimension(nz-1), intent(in) :: stagsigma
@@ -578,14 +592,24 @@
       real(dp), dimension(nz-1,4,nx,ny), intent(inout), optional :: efvs_qp_3d
       integer(c_int32_t) :: act(nx,ny), indx2(9)
       integer :: m
-      if (whichapprox /= HO_APPROX_SSA) then
-         call write_log('GPU 2D assembly: only the SSA branch is built (L1L2 and DIVA are not)', GM_FATAL)
-      endif
       act = merge(1, 0, active_cell)
       indx2 = [(m, m = 1, 9)]
-      call check(c_assemble_2d(nx, ny, nz, nhalo, sigma, act, xVertex, yVertex, uvel_2d, vvel_2d, stagthck, &
-                               flwafact, whichefvs, efvs_constant, effstrain_min, n_glen, indx2, efvs, &
-                               Auu, Auv, Avu, Avv))
+      if (whichapprox == HO_APPROX_DIVA) then
+         if (.not. (present(thck) .and. present(btractx) .and. present(btracty) .and. present(omega_k) .and. &
+                    present(omega) .and. present(efvs_qp_3d))) then
+            call write_log('GPU DIVA assembly: thck, btractx/y, omega_k, omega and efvs_qp_3d are needed', GM_FATAL)
+         endif
+         call check(c_assemble_2d_diva(nx, ny, nz, nhalo, sigma, stagsigma, act, xVertex, yVertex, uvel_2d, &
+                                       vvel_2d, stagthck, thck, btractx, btracty, diva_slope_factor_x, &
+                                       diva_slope_factor_y, flwafact, whichefvs, efvs_constant, effstrain_min, &
+                                       n_glen, indx2, efvs_qp_3d, efvs, omega_k, omega, Auu, Auv, Avu, Avv))
+      elseif (whichapprox == HO_APPROX_SSA) then
+         call check(c_assemble_2d(nx, ny, nz, nhalo, sigma, act, xVertex, yVertex, uvel_2d, vvel_2d, stagthck, &
+                                  flwafact, whichefvs, efvs_constant, effstrain_min, n_glen, indx2, efvs, &
+                                  Auu, Auv, Avu, Avv))
+      else
+         call write_log('GPU 2D assembly: the L1L2 branch is not built', GM_FATAL)
+      endif
     end subroutine assemble_stiffness_matrix_2d
 
     !-----------------------------------------------------------------------

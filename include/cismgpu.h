@@ -265,7 +265,8 @@ int cismgpu_assemble_stiffness_matrix_3d(int nx, int ny, int nz, int nhalo, cons
                                          double *Avu, double *Avv);
 
 /* Replaces assemble_stiffness_matrix_2d (glissade_velo_higher.F90:4961-5378) for the SSA
- * (whichapprox = HO_APPROX_SSA; the L1L2 and DIVA branches are not built): 4-node cells with
+ * (whichapprox = HO_APPROX_SSA; DIVA: cismgpu_assemble_stiffness_matrix_2d_diva below; the L1L2
+ * branch is not built): 4-node cells with
  * 4-point Gauss quadrature, the viscosity of whichefvs at the flow factor averaged over the nz-1
  * layers (glissade_vertical_average), weighted by the thickness at each point.  uvel_2d,
  * vvel_2d, xVertex, yVertex, stagthck (nx-1,ny-1); sigma(nz); flwafact and efvs (nz-1,nx,ny),
