@@ -81,6 +81,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_basal_local_2d.restype = None
         L.oracle_basal_standard.argtypes = [i, i, i, i, i, d, d, d, d, d, d, d]
         L.oracle_assemble_stiffness_2d_diva.argtypes = [i, i, i, i] + [d] * 14 + [i, dbl, dbl, dbl] + [d] * 8
+        L.oracle_basal_diva.argtypes = [i, i, i, dbl, dbl, d, d, d, d, d, d, d, i, d, d]
+        L.oracle_basal_diva.restype = None
         L.oracle_check_symmetry.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, P(dbl), P(ctypes.c_long)]
         L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
@@ -324,6 +326,19 @@ def assemble_stiffness_2d_diva(nx, ny, nz, sigma, stagsigma, active_cell, xVerte
                                                  effstrain_min, n_glen, _p(eq), _p(efvs), _p(ok), _p(om),
                                                  *[_p(a) for a in A])
     return (st, efvs, eq, ok, om, *A)
+
+
+def basal_diva(nx, ny, dx, dy, active_cell, active_vertex, beta_eff_x, beta_eff_y, lsrf, xVertex, yVertex,
+               whichassemble_beta, Auu, Avv, nhalo=2):
+    """basal_sliding_bc_2d_diva (glissade_velo_higher.F90:8535-8811) on copies of the (9, ny-1,
+    nx-1) blocks; returns (Auu, Avv)."""
+    out = [np.array(a, dtype=np.float64, copy=True) for a in (Auu, Avv)]
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    lib().oracle_basal_diva(nx, ny, nhalo, float(dx), float(dy), _p(i32(active_cell)), _p(i32(active_vertex)),
+                            _p(f64(beta_eff_x)), _p(f64(beta_eff_y)), _p(f64(lsrf)), _p(f64(xVertex)), _p(f64(yVertex)),
+                            int(whichassemble_beta), _p(out[0]), _p(out[1]))
+    return out[0], out[1]
 
 
 def reprosum(a) -> float:

@@ -830,3 +830,98 @@ int oracle_assemble_stiffness_2d_diva(int nx, int ny, int nz, int nhalo, const d
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// basal_sliding_bc_2d_diva (:8535-8811), the DIVA basal term with slope correction
+// ---------------------------------------------------------------------------
+extern "C" {
+
+// Local form (whichassemble_beta = 1): theta_x = atan(|dz/dx|), theta_y = atan(|dz/dy|) of the
+// staggered lower surface (glissade_slope_angle's theta_slope_x/_y: the gradient and unstagger
+// of oracle_basal_local_3d), then at active vertices Auu(0,0) += (dx*dy/vol0)*beta_eff_x/cos(theta_x)
+// and Avv(0,0) += (dx*dy/vol0)*beta_eff_y/cos(theta_y).  Standard form (0): per active cell the
+// curved area factor of the staggered lower surface and 4-point quadrature, beta_eff_x into Auu
+// and beta_eff_y into Avv.  Blocks (nx-1,ny-1,9).
+void oracle_basal_diva(int nx, int ny, int nhalo, double dx, double dy, const int32_t *active_cell,
+                       const int32_t *active_vertex, const double *bex, const double *bey, const double *lsrf,
+                       const double *xVertex, const double *yVertex, int whichassemble_beta, double *Auu, double *Avv) {
+    const long NX = nx - 1, NY = ny - 1, NQ = NX * NY;
+    auto L = [&](long i, long j) { return lsrf[(i - 1) + (long)nx * (j - 1)]; };
+    std::vector<double> s((size_t)NQ);
+    for (long j = 1; j <= NY; ++j)
+        for (long i = 1; i <= NX; ++i) s[(i - 1) + NX * (j - 1)] = (L(i, j + 1) + L(i + 1, j + 1) + L(i, j) + L(i + 1, j)) / 4.0;
+    auto S = [&](long i, long j) { return s[(i - 1) + NX * (j - 1)]; };
+    if (whichassemble_beta == 1) {
+        std::vector<double> gx((size_t)(NX - 1) * (NY - 1)), gy(gx.size());
+        for (long j = 1; j <= NY - 1; ++j)
+            for (long i = 1; i <= NX - 1; ++i) {
+                const double north = (S(i + 1, j + 1) - S(i, j + 1)) / dx, south = (S(i + 1, j) - S(i, j)) / dx;
+                gx[(i - 1) + (NX - 1) * (j - 1)] = (north + south) / 2.0;
+                const double east = (S(i + 1, j + 1) - S(i + 1, j)) / dy, west = (S(i, j + 1) - S(i, j)) / dy;
+                gy[(i - 1) + (NX - 1) * (j - 1)] = (east + west) / 2.0;
+            }
+        auto G = [&](const std::vector<double> &g, long i, long j) { return g[(i - 1) + (NX - 1) * (j - 1)]; };
+        for (long j = 1; j <= NY; ++j)
+            for (long i = 1; i <= NX; ++i) {
+                const long q = (i - 1) + NX * (j - 1);
+                if (!active_vertex[q]) continue;
+                double ddx = 0.0, ddy = 0.0;
+                if (i >= 2 && i <= NX - 1 && j >= 2 && j <= NY - 1) {
+                    ddx = (G(gx, i, j) + G(gx, i - 1, j) + G(gx, i, j - 1) + G(gx, i - 1, j - 1)) / 4.0;
+                    ddy = (G(gy, i, j) + G(gy, i - 1, j) + G(gy, i, j - 1) + G(gy, i - 1, j - 1)) / 4.0;
+                }
+                const double tx = std::atan(std::fabs(ddx)), ty = std::atan(std::fabs(ddy));
+                Auu[q + 4 * NQ] = Auu[q + 4 * NQ] + (dx * dy / kVol0) * bex[q] / std::cos(tx);
+                Avv[q + 4 * NQ] = Avv[q + 4 * NQ] + (dx * dy / kVol0) * bey[q] / std::cos(ty);
+            }
+        return;
+    }
+    const RefElement2 &R = ref2();
+    for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+        for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+            if (!active_cell[(i - 1) + (long)nx * (j - 1)]) continue;
+            double x[4], y[4], z[4], bx[4], by[4];
+            for (int n = 0; n < 4; ++n) {
+                const long q = (long)(i + kIsh3[n] - 1) + NX * (j + kJsh3[n] - 1);
+                x[n] = xVertex[q];
+                y[n] = yVertex[q];
+                z[n] = s[q];
+                bx[n] = bex[q];
+                by[n] = bey[q];
+            }
+            for (int p = 0; p < 4; ++p) {
+                double J11 = 0.0, J12 = 0.0, J13 = 0.0, J21 = 0.0, J22 = 0.0, J23 = 0.0;
+                for (int n = 0; n < 4; ++n) {
+                    J11 = J11 + R.dxr[p][n] * x[n];
+                    J12 = J12 + R.dxr[p][n] * y[n];
+                    J13 = J13 + R.dxr[p][n] * z[n];
+                    J21 = J21 + R.dyr[p][n] * x[n];
+                    J22 = J22 + R.dyr[p][n] * y[n];
+                    J23 = J23 + R.dyr[p][n] * z[n];
+                }
+                const double t1 = (J11 * J22 - J12 * J21), t2 = -(J11 * J23 - J13 * J21), t3 = (J12 * J23 - J13 * J22);
+                const double detJ = std::sqrt(t1 * t1 + t2 * t2 + t3 * t3);
+                double bqx = 0.0, bqy = 0.0;
+                for (int n = 0; n < 4; ++n) {
+                    bqx = bqx + R.phi[p][n] * bx[n];
+                    bqy = bqy + R.phi[p][n] * by[n];
+                }
+                double Ku[4][4] = {}, Kv[4][4] = {};
+                for (int nc = 0; nc < 4; ++nc)
+                    for (int nr = 0; nr < 4; ++nr) {
+                        Ku[nr][nc] = Ku[nr][nc] + bqx * 1.0 * detJ / kVol0 * R.phi[p][nr] * R.phi[p][nc];
+                        Kv[nr][nc] = Kv[nr][nc] + bqy * 1.0 * detJ / kVol0 * R.phi[p][nr] * R.phi[p][nc];
+                    }
+                for (int nr = 0; nr < 4; ++nr) {
+                    const long q = (long)(i + kIsh3[nr] - 1) + NX * (j + kJsh3[nr] - 1);
+                    for (int nc = 0; nc < 4; ++nc) {
+                        const int m = (kIsh3[nc] - kIsh3[nr] + 1) + 3 * (kJsh3[nc] - kJsh3[nr] + 1);
+                        Auu[q + NQ * m] = Auu[q + NQ * m] + Ku[nr][nc];
+                        Avv[q + NQ * m] = Avv[q + NQ * m] + Kv[nr][nc];
+                    }
+                }
+            }
+        }
+}
+
+}  // extern "C"

@@ -218,3 +218,52 @@ def test_basal_standard_integrates_beta_over_the_bed():
     J, I = np.nonzero(full)
     j, i = J[len(J) // 2], I[len(I) // 2]
     assert abs(d2[4, j, i] / d2[:, j, i].sum() - 4.0 / 9.0) <= 1e-12
+
+
+# ---------------------------------------------------------------------------
+# basal_sliding_bc_2d_diva (:8535-8811)
+# ---------------------------------------------------------------------------
+
+def numpy_slope_xy(lsrf, dx, dy):
+    """dz/dx and dz/dy of glissade_slope_angle on the staggered lower surface (the chain of
+    numpy_theta without the final atan of the length)."""
+    s = (lsrf[1:, :-1] + lsrf[1:, 1:] + lsrf[:-1, :-1] + lsrf[:-1, 1:]) / 4.0
+    gx = ((s[1:, 1:] - s[1:, :-1]) / dx + (s[:-1, 1:] - s[:-1, :-1]) / dx) / 2.0
+    gy = ((s[1:, 1:] - s[:-1, 1:]) / dy + (s[1:, :-1] - s[:-1, :-1]) / dy) / 2.0
+    ddx = np.zeros_like(s)
+    ddy = np.zeros_like(s)
+    ddx[1:-1, 1:-1] = (gx[1:, 1:] + gx[1:, :-1] + gx[:-1, 1:] + gx[:-1, :-1]) / 4.0
+    ddy[1:-1, 1:-1] = (gy[1:, 1:] + gy[1:, :-1] + gy[:-1, 1:] + gy[:-1, :-1]) / 4.0
+    return ddx, ddy
+
+
+def test_basal_diva_local():
+    g = geometry(seed=58)
+    nx, ny, dx = g["nx"], g["ny"], g["dx"]
+    z2 = np.zeros((9, ny - 1, nx - 1))
+    lsrf = g["usrf"] - g["thck"] + 5.0 * np.random.default_rng(2).random(g["thck"].shape)
+    bex, bey = asm.lognormal_beta((ny - 1, nx - 1), 3), asm.lognormal_beta((ny - 1, nx - 1), 4)
+    Auu, Avv = oracle.basal_diva(nx, ny, dx, dx, g["ac"], g["av"], bex, bey, lsrf, g["xVertex"], g["yVertex"], 1, z2, z2)
+    ddx, ddy = numpy_slope_xy(lsrf, dx, dx)
+    av = g["av"].astype(bool)
+    wu = np.where(av, (dx * dx / 1.0e9) * bex / np.cos(np.arctan(np.abs(ddx))), 0.0)
+    wv = np.where(av, (dx * dx / 1.0e9) * bey / np.cos(np.arctan(np.abs(ddy))), 0.0)
+    assert np.abs(Auu[4] - wu).max() <= 1e-15 * np.abs(wu).max()
+    assert np.abs(Avv[4] - wv).max() <= 1e-15 * np.abs(wv).max()
+    assert np.all(np.delete(Auu, 4, axis=0) == 0.0) and np.all(np.delete(Avv, 4, axis=0) == 0.0)
+
+
+def test_basal_diva_standard_integrates_over_the_bed():
+    g = geometry(seed=59)
+    nx, ny, dx = g["nx"], g["ny"], g["dx"]
+    a, b = -0.015, 0.02
+    xc = (np.arange(nx) - 0.5) * dx
+    yc = (np.arange(ny) - 0.5) * dx
+    lsrf = a * xc[None, :] + b * yc[:, None]
+    z2 = np.zeros((9, ny - 1, nx - 1))
+    bex, bey = np.full((ny - 1, nx - 1), 200.0), np.full((ny - 1, nx - 1), 300.0)
+    Auu, Avv = oracle.basal_diva(nx, ny, dx, dx, g["ac"], g["av"], bex, bey, lsrf, g["xVertex"], g["yVertex"], 0, z2, z2)
+    ncell = int(np.count_nonzero(g["ac"][2:ny - 1, 2:nx - 1]))
+    area = dx * dx * np.sqrt(1 + a * a + b * b) / 1.0e9 * ncell
+    assert abs(Auu.sum() - 200.0 * area) <= 1e-12 * 200.0 * area
+    assert abs(Avv.sum() - 300.0 * area) <= 1e-12 * 300.0 * area
