@@ -32,6 +32,7 @@ __all__ = [
     "check_symmetry_assembled_matrix_3d", "check_symmetry_assembled_matrix_2d", "assemble_stiffness_matrix_3d",
     "assemble_stiffness_matrix_2d", "dirichlet_boundary_conditions_3d", "basal_sliding_bc_3d",
     "dirichlet_boundary_conditions_2d", "basal_sliding_bc_2d", "assemble_stiffness_matrix_2d_diva",
+    "basal_sliding_bc_2d_diva",
 ]
 
 ALG_STANDARD, ALG_CHRONGEAR, ALG_MIXED_CHRONGEAR = 0, 1, 2
@@ -196,6 +197,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_assemble_stiffness_matrix_2d_diva.argtypes = [i32, i32, i32, i32] + [d] * 14 + [i32, dbl, dbl, dbl] + \
         [d] * 9
     lib.cismgpu_solver_assemble_stiffness_2d_diva.argtypes = [vp, i32, i32] + [d] * 14 + [i32, dbl, dbl, dbl] + [d] * 4
+    lib.cismgpu_basal_sliding_bc_2d_diva.argtypes = [i32, i32, i32, dbl, dbl, d, d, d, d, d, d, d, i32, d, d, d]
     lib.cismgpu_dirichlet_boundary_conditions_2d.argtypes = [i32, i32, i32, d, d, d, d, d, d, d, d, d, d, d, d]
     lib.cismgpu_basal_sliding_bc_2d.argtypes = [i32, i32, i32, dbl, dbl, d, d, d, d, d, i32, d, d, d]
     lib.cismgpu_solver_assemble_system_2d.argtypes = [vp, i32, i32, dbl, dbl, d, d, d, d, d, d, d, i32, dbl, dbl, dbl,
@@ -210,7 +212,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
               "cismgpu_dirichlet_boundary_conditions_3d", "cismgpu_basal_sliding_bc_3d",
               "cismgpu_solver_assemble_system_3d", "cismgpu_dirichlet_boundary_conditions_2d",
               "cismgpu_basal_sliding_bc_2d", "cismgpu_solver_assemble_system_2d",
-              "cismgpu_assemble_stiffness_matrix_2d_diva", "cismgpu_solver_assemble_stiffness_2d_diva"):
+              "cismgpu_assemble_stiffness_matrix_2d_diva", "cismgpu_solver_assemble_stiffness_2d_diva",
+              "cismgpu_basal_sliding_bc_2d_diva"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -564,6 +567,22 @@ def assemble_stiffness_matrix_2d_diva(nx, ny, nz, nhalo, sigma, stagsigma, activ
         _ptr(efvs, np.float64, efvs.size, True), _ptr(ok, np.float64, ok.size, True), _ptr(om, np.float64, om.size, True),
         *[_ptr(a, np.float64, a.size, True) for a in A]))
     return (efvs, ok, om, *A)
+
+
+def basal_sliding_bc_2d_diva(nx, ny, nhalo, dx, dy, active_cell, active_vertex, beta_eff_x, beta_eff_y, lsrf,
+                             xVertex, yVertex, Auu, Avv, whichassemble_beta=1, indxA_2d=None):
+    """Mirrors basal_sliding_bc_2d_diva (glissade_velo_higher.F90:8535-8811) on the GPU, in place
+    on the (9, ny-1, nx-1) blocks."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    indx = np.arange(1, 10, dtype=np.int32) if indxA_2d is None else np.ascontiguousarray(indxA_2d, dtype=np.int32)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    _check(lib, lib.cismgpu_basal_sliding_bc_2d_diva(
+        nx, ny, int(nhalo), float(dx), float(dy), _ptr(i32(active_cell), np.int32, nx * ny),
+        _ptr(i32(active_vertex), np.int32, nv), _ptr(beta_eff_x, np.float64, nv), _ptr(beta_eff_y, np.float64, nv),
+        _ptr(np.ascontiguousarray(lsrf, dtype=np.float64), np.float64, nx * ny), _ptr(xVertex, np.float64, nv),
+        _ptr(yVertex, np.float64, nv), int(whichassemble_beta), _ptr(indx, np.int32, 9),
+        _ptr(Auu, np.float64, 9 * nv, True), _ptr(Avv, np.float64, 9 * nv, True)))
 
 
 def dirichlet_boundary_conditions_2d(nx, ny, nhalo, active_vertex, umask, vmask, uvel, vvel, Auu, Auv, Avu, Avv,

@@ -610,13 +610,16 @@ __global__ void __launch_bounds__(kBlock) k_basal_local2d(long long NQ, double d
 // (j, then i), and for each of the cell's 4 Gauss points the vertex's row of
 // beta_qp*w*detJ/vol0*phi_r*phi_c added to Auu and Avv, point by point as the reference adds
 // them.  3D: the area factor of the lower surface (get_area_scale_factor_curved_2d, :6736-6827,
-// lsrf staggered over all four cells) and the bed level nz; 2D: the flat Jacobian.
-template <bool THREE_D>
+// lsrf staggered over all four cells) and the bed level nz; 2D: the flat Jacobian, or with
+// CURVED the area factor as in 3D (basal_sliding_bc_2d_diva :8650-8700, which also takes a
+// separate beta for v, beta_v).
+template <bool THREE_D, bool CURVED>
 __global__ void __launch_bounds__(kBlock) k_basal_standard(int nx, int ny, int nz, int nhalo, SymIdx L,
                                                            const int32_t *__restrict__ active_cell,
                                                            const double *__restrict__ xv,
                                                            const double *__restrict__ yv,
                                                            const double *__restrict__ beta,
+                                                           const double *__restrict__ beta_v,
                                                            const double *__restrict__ lsrf, double *Auu,
                                                            double *Avv, int *singular) {
     const long long NX = nx - 1, NQ = NX * (ny - 1);
@@ -640,7 +643,7 @@ __global__ void __launch_bounds__(kBlock) k_basal_standard(int nx, int ny, int n
             if (!active_cell[(ie - 1) + (long long)nx * (je - 1)]) continue;
             any = true;
             const int nr = dj == 0 ? (di == 0 ? 2 : 3) : (di == 0 ? 1 : 0);
-            double x[4], y[4], z[4], b[4];
+            double x[4], y[4], z[4], b[4], bv[4];
 #pragma unroll
             for (int n = 0; n < 4; ++n) {
                 const int iN = ie + c_ish3[n], jN = je + c_jsh3[n];
@@ -648,12 +651,13 @@ __global__ void __launch_bounds__(kBlock) k_basal_standard(int nx, int ny, int n
                 x[n] = xv[qn];
                 y[n] = yv[qn];
                 b[n] = beta[qn];
-                z[n] = THREE_D ? (Lf(iN, jN + 1) + Lf(iN + 1, jN + 1) + Lf(iN, jN) + Lf(iN + 1, jN)) / 4.0 : 0.0;
+                bv[n] = beta_v[qn];
+                z[n] = CURVED ? (Lf(iN, jN + 1) + Lf(iN + 1, jN + 1) + Lf(iN, jN) + Lf(iN + 1, jN)) / 4.0 : 0.0;
             }
             for (int p = 0; p < 4; ++p) {
                 const double *dxr = c_asm_ref2.dxr[p], *dyr = c_asm_ref2.dyr[p];
                 double detJ;
-                if (THREE_D) {
+                if (CURVED) {
                     double J11 = 0.0, J12 = 0.0, J13 = 0.0, J21 = 0.0, J22 = 0.0, J23 = 0.0;
 #pragma unroll
                     for (int n = 0; n < 4; ++n) {
@@ -683,15 +687,19 @@ __global__ void __launch_bounds__(kBlock) k_basal_standard(int nx, int ny, int n
                         continue;
                     }
                 }
-                double beta_qp = 0.0;
+                double beta_qp = 0.0, beta_qv = 0.0;
 #pragma unroll
-                for (int n = 0; n < 4; ++n) beta_qp = beta_qp + c_asm_ref2.phi[p][n] * b[n];
+                for (int n = 0; n < 4; ++n) {
+                    beta_qp = beta_qp + c_asm_ref2.phi[p][n] * b[n];
+                    beta_qv = beta_qv + c_asm_ref2.phi[p][n] * bv[n];
+                }
 #pragma unroll
                 for (int nc = 0; nc < 4; ++nc) {
-                    const double k = 0.0 + beta_qp * 1.0 * detJ / kAsmVol0 * c_asm_ref2.phi[p][nr] * c_asm_ref2.phi[p][nc];
+                    const double ku = 0.0 + beta_qp * 1.0 * detJ / kAsmVol0 * c_asm_ref2.phi[p][nr] * c_asm_ref2.phi[p][nc];
+                    const double kv = 0.0 + beta_qv * 1.0 * detJ / kAsmVol0 * c_asm_ref2.phi[p][nr] * c_asm_ref2.phi[p][nc];
                     const int m = (c_ish3[nc] - c_ish3[nr] + 1) + 3 * (c_jsh3[nc] - c_jsh3[nr] + 1);
-                    accU[m] = accU[m] + k;
-                    accV[m] = accV[m] + k;
+                    accU[m] = accU[m] + ku;
+                    accV[m] = accV[m] + kv;
                 }
             }
         }
@@ -871,6 +879,43 @@ __global__ void __launch_bounds__(kAsmBlock) k_assemble2d_diva(AsmArgs a, DivaAr
 #pragma unroll
     for (int b = 0; b < 4; ++b)
         for (int c = 0; c < 9; ++c) B[b][L.at(c, 0, q)] = acc[b][c];
+}
+
+// basal_sliding_bc_2d_diva (:8586-8620), local form, one thread per vertex: glissade_slope_angle's
+// theta_x = atan(|dz/dx|), theta_y = atan(|dz/dy|) of the staggered lower surface (the chain of
+// k_basal_local3d), then at an active vertex the diagonal of Auu += (dx*dy/vol0)*beta_eff_x /
+// cos(theta_x) and of Avv += (dx*dy/vol0)*beta_eff_y / cos(theta_y).
+__global__ void __launch_bounds__(kBlock) k_basal_local_diva(int nx, int ny, double dx, double dy, SymIdx L,
+                                                             const int32_t *__restrict__ active_vertex,
+                                                             const double *__restrict__ bex,
+                                                             const double *__restrict__ bey,
+                                                             const double *__restrict__ lsrf, double *Auu,
+                                                             double *Avv) {
+    const int NX = nx - 1, NY = ny - 1;
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (q >= (long long)NX * NY) return;
+    if (!active_vertex[q]) return;
+    const int j = (int)(q / NX) + 1, i = (int)(q - (long long)(j - 1) * NX) + 1;  // 1-based
+    auto Lf = [&](int ii, int jj) { return lsrf[(ii - 1) + (long long)nx * (jj - 1)]; };
+    auto S = [&](int ii, int jj) { return (Lf(ii, jj + 1) + Lf(ii + 1, jj + 1) + Lf(ii, jj) + Lf(ii + 1, jj)) / 4.0; };
+    double ddx = 0.0, ddy = 0.0;
+    if (i >= 2 && i <= NX - 1 && j >= 2 && j <= NY - 1) {
+        double gx[4], gy[4];  // at (i,j), (i-1,j), (i,j-1), (i-1,j-1)
+        const int oi[4] = {0, -1, 0, -1}, oj[4] = {0, 0, -1, -1};
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            const int a = i + oi[n], b = j + oj[n];
+            const double s00 = S(a, b), s10 = S(a + 1, b), s01 = S(a, b + 1), s11 = S(a + 1, b + 1);
+            gx[n] = ((s11 - s01) / dx + (s10 - s00) / dx) / 2.0;
+            gy[n] = ((s11 - s10) / dy + (s01 - s00) / dy) / 2.0;
+        }
+        ddx = (gx[0] + gx[1] + gx[2] + gx[3]) / 4.0;
+        ddy = (gy[0] + gy[1] + gy[2] + gy[3]) / 4.0;
+    }
+    const double tx = atan(fabs(ddx)), ty = atan(fabs(ddy));
+    const long long a = L.at(4, 0, q);
+    Auu[a] = Auu[a] + (dx * dy / kAsmVol0) * bex[q] / cos(tx);
+    Avv[a] = Avv[a] + (dx * dy / kAsmVol0) * bey[q] / cos(ty);
 }
 
 }  // namespace cismgpu

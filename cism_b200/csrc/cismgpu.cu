@@ -478,9 +478,8 @@ struct Solver {
                 CU(up(d_cell, active_cell, ncell * sizeof(int32_t)));
                 CU(up(d_xv, xv, nq * sizeof(double)));
                 CU(up(d_yv, yv, nq * sizeof(double)));
-                k_basal_standard<true><<<nblocks((long long)nq), kBlock, 0, s>>>(nx, ny, nz, nhalo, L, d_cell, d_xv,
-                                                                                 d_yv, d_beta, d_lsrf, Auu, Avv,
-                                                                                 d_sing);
+                k_basal_standard<true, true><<<nblocks((long long)nq), kBlock, 0, s>>>(
+                    nx, ny, nz, nhalo, L, d_cell, d_xv, d_yv, d_beta, d_beta, d_lsrf, Auu, Avv, d_sing);
             }
             CU(cudaGetLastError());
         }
@@ -515,16 +514,19 @@ struct Solver {
                    int nhalo, double dx, double dy, const int32_t *active_vertex, const double *beta,
                    const int32_t *umask, const int32_t *vmask, const double *uvel, const double *vvel, int vel_id,
                    int assemble_beta = 1, const int32_t *active_cell = nullptr, const double *xv = nullptr,
-                   const double *yv = nullptr) {
+                   const double *yv = nullptr, const double *beta_v = nullptr, const double *lsrf = nullptr) {
+        // beta_v given: the DIVA basal term (basal_sliding_bc_2d_diva) with beta for u, beta_v
+        // for v and the lower surface lsrf (nx, ny)
         const int nx = g.NX + 1, ny = g.NY + 1;
         const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny;
-        const bool host_vel = uvel != nullptr;
-        // doubles: beta, xVertex, yVertex, [uvel, vvel]; then int32: active_vertex, umask, vmask,
-        // active_cell, the singular-Jacobian flag
-        const size_t nd = 3 * nq + (host_vel ? 2 * nq : 0);
+        const bool host_vel = uvel != nullptr, diva = beta_v != nullptr;
+        // doubles: beta, xVertex, yVertex, beta_v, lsrf, [uvel, vvel]; then int32: active_vertex,
+        // umask, vmask, active_cell, the singular-Jacobian flag
+        const size_t nd = 4 * nq + ncell + (host_vel ? 2 * nq : 0);
         CU(bc_in.ensure(nd * sizeof(double) + (3 * nq + ncell + 1) * sizeof(int32_t)));
         double *D = bc_in.as<double>();
-        double *d_beta = D, *d_xv = D + nq, *d_yv = d_xv + nq, *d_u = d_yv + nq, *d_v = d_u + nq;
+        double *d_beta = D, *d_xv = D + nq, *d_yv = d_xv + nq, *d_bv = d_yv + nq, *d_lsrf = d_bv + nq,
+               *d_u = d_lsrf + ncell, *d_v = d_u + nq;
         int32_t *d_act = reinterpret_cast<int32_t *>(D + nd), *d_um = d_act + nq, *d_vm = d_um + nq,
                 *d_cell = d_vm + nq, *d_sing = d_cell + ncell;
         cudaStream_t s = stream;
@@ -533,7 +535,23 @@ struct Solver {
         };
         CU(up(d_act, active_vertex, nq * sizeof(int32_t)));
         CU(cudaMemsetAsync(d_sing, 0, sizeof(int32_t), s));
-        if (beta) {
+        if (beta && diva) {
+            CU(up(d_beta, beta, nq * sizeof(double)));
+            CU(up(d_bv, beta_v, nq * sizeof(double)));
+            CU(up(d_lsrf, lsrf, ncell * sizeof(double)));
+            if (assemble_beta == 1) {
+                k_basal_local_diva<<<nblocks((long long)nq), kBlock, 0, s>>>(nx, ny, dx, dy, L, d_act, d_beta, d_bv,
+                                                                             d_lsrf, Auu, Avv);
+            } else {
+                TRY(asm_ref_ready());
+                CU(up(d_cell, active_cell, ncell * sizeof(int32_t)));
+                CU(up(d_xv, xv, nq * sizeof(double)));
+                CU(up(d_yv, yv, nq * sizeof(double)));
+                k_basal_standard<false, true><<<nblocks((long long)nq), kBlock, 0, s>>>(
+                    nx, ny, 1, nhalo, L, d_cell, d_xv, d_yv, d_beta, d_bv, d_lsrf, Auu, Avv, d_sing);
+            }
+            CU(cudaGetLastError());
+        } else if (beta) {
             CU(up(d_beta, beta, nq * sizeof(double)));
             if (assemble_beta == 1) {
                 k_basal_local2d<<<nblocks((long long)nq), kBlock, 0, s>>>(g.NQ, dx, dy, L, d_act, d_beta, Auu, Avv);
@@ -542,9 +560,8 @@ struct Solver {
                 CU(up(d_cell, active_cell, ncell * sizeof(int32_t)));
                 CU(up(d_xv, xv, nq * sizeof(double)));
                 CU(up(d_yv, yv, nq * sizeof(double)));
-                k_basal_standard<false><<<nblocks((long long)nq), kBlock, 0, s>>>(nx, ny, 1, nhalo, L, d_cell, d_xv,
-                                                                                  d_yv, d_beta, d_beta, Auu, Avv,
-                                                                                  d_sing);
+                k_basal_standard<false, false><<<nblocks((long long)nq), kBlock, 0, s>>>(
+                    nx, ny, 1, nhalo, L, d_cell, d_xv, d_yv, d_beta, d_beta, d_beta, Auu, Avv, d_sing);
             }
             CU(cudaGetLastError());
         }
@@ -2238,13 +2255,15 @@ static int oneshot_boundary2d(int which, int nx, int ny, int nhalo, double dx, d
                               const int32_t *vmask, const double *uvel, const double *vvel, const int32_t *indx,
                               double *Auu, double *Auv, double *Avu, double *Avv, double *bu, double *bv,
                               int assemble_beta = 1, const int32_t *active_cell = nullptr,
-                              const double *xv = nullptr, const double *yv = nullptr) {
+                              const double *xv = nullptr, const double *yv = nullptr, const double *beta_v = nullptr,
+                              const double *lsrf = nullptr) {
     std::lock_guard<std::mutex> lk(g_mu);
     g_last_error.clear();
     if (!active_vertex || !indx || !Auu || !Avv) return fail(CISMGPU_EINVAL, "null pointer argument");
     if (which == 0 && (!umask || !vmask || !uvel || !vvel || !Auv || !Avu || !bu || !bv))
         return fail(CISMGPU_EINVAL, "null pointer argument");
     if (which == 1 && !beta) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (beta_v && !lsrf) return fail(CISMGPU_EINVAL, "null pointer argument");
     if (which == 1 && assemble_beta == 0 && (!active_cell || !xv || !yv))
         return fail(CISMGPU_EINVAL, "null pointer argument");
     if (nx < 6 || ny < 6) return fail(CISMGPU_EINVAL, "grid too small");
@@ -2281,7 +2300,7 @@ static int oneshot_boundary2d(int which, int nx, int ny, int nhalo, double dx, d
     L.raw3 = 0;
     TRY(sv.boundary2d(L, blk[0], blk[1], blk[2], blk[3], dbu, dbv, nhalo, dx, dy, active_vertex,
                       which == 1 ? beta : nullptr, which == 0 ? umask : nullptr, vmask, uvel, vvel, 0,
-                      assemble_beta, active_cell, xv, yv));
+                      assemble_beta, active_cell, xv, yv, beta_v, lsrf));
     for (int b = 0; b < 4; ++b)
         if (which == 0 || b == 0 || b == 3)
             CU(cudaMemcpyAsync(host[b], blk[b], bs * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -2481,6 +2500,19 @@ int cismgpu_basal_sliding_bc_2d(int nx, int ny, int nhalo, double dx, double dy,
     return oneshot_boundary2d(1, nx, ny, nhalo, dx, dy, active_vertex, beta, nullptr, nullptr, nullptr, nullptr,
                               indxA_2d, Auu, nullptr, nullptr, Avv, nullptr, nullptr, whichassemble_beta, active_cell,
                               xVertex, yVertex);
+}
+
+int cismgpu_basal_sliding_bc_2d_diva(int nx, int ny, int nhalo, double dx, double dy, const int32_t *active_cell,
+                                     const int32_t *active_vertex, const double *beta_eff_x, const double *beta_eff_y,
+                                     const double *lsrf, const double *xVertex, const double *yVertex,
+                                     int whichassemble_beta, const int32_t *indxA_2d, double *Auu, double *Avv) {
+    g_last_error.clear();
+    if (whichassemble_beta != 0 && whichassemble_beta != 1)
+        return fail(CISMGPU_EINVAL, "whichassemble_beta must be 0 (standard) or 1 (local)");
+    if (!beta_eff_y || !lsrf) return fail(CISMGPU_EINVAL, "null pointer argument");
+    return oneshot_boundary2d(1, nx, ny, nhalo, dx, dy, active_vertex, beta_eff_x, nullptr, nullptr, nullptr, nullptr,
+                              indxA_2d, Auu, nullptr, nullptr, Avv, nullptr, nullptr, whichassemble_beta, active_cell,
+                              xVertex, yVertex, beta_eff_y, lsrf);
 }
 
 int cismgpu_solver_assemble_system_2d(cismgpu_solver_t *h, int nz, int nhalo, double dx, double dy,

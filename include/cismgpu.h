@@ -342,6 +342,16 @@ int cismgpu_assemble_stiffness_matrix_2d_diva(int nx, int ny, int nz, int nhalo,
                                               double *efvs_qp_3d, double *efvs, double *omega_k, double *omega,
                                               double *Auu, double *Auv, double *Avu, double *Avv);
 
+/* Replaces basal_sliding_bc_2d_diva (glissade_velo_higher.F90:8535-8811), the DIVA basal term
+ * with slope correction (CISM's default for DIVA): beta_eff_x into Auu and beta_eff_y into Avv.
+ * Local form (1): the diagonals gain (dx*dy/vol0)*beta_eff/cos(theta) with theta_x = atan|dz/dx|,
+ * theta_y = atan|dz/dy| of the staggered lower surface lsrf(nx,ny) (atan, cos are CUDA's).
+ * Standard form (0): 4-point quadrature with the curved area factor, bit-exact. */
+int cismgpu_basal_sliding_bc_2d_diva(int nx, int ny, int nhalo, double dx, double dy, const int32_t *active_cell,
+                                     const int32_t *active_vertex, const double *beta_eff_x, const double *beta_eff_y,
+                                     const double *lsrf, const double *xVertex, const double *yVertex,
+                                     int whichassemble_beta, const int32_t *indxA_2d, double *Auu, double *Avv);
+
 /* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps

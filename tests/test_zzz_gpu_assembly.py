@@ -482,3 +482,28 @@ def test_diva_state_on_handle(gpu_lib):
                                          Q.bu, Q.bv, u, v)
     np.testing.assert_array_equal(ru, want[0])
     np.testing.assert_array_equal(rv, want[1])
+
+
+@pytest.mark.parametrize("mode", [1, 0])
+def test_basal_diva(gpu_lib, mode):
+    """basal_sliding_bc_2d_diva: the standard form bit-exact; the local form's diagonals within
+    1e-15 of their size (atan and cos are CUDA's), the rest exact."""
+    g = geometry(seed=65)
+    nx, ny, dx = g["nx"], g["ny"], g["dx"]
+    S = asm.assemble_ssa_2d(g["thck"], g["usrf"], dx, dx, np.zeros((ny - 1, nx - 1)), stiffness_only=True)
+    lsrf = g["usrf"] - g["thck"] + 5.0 * np.random.default_rng(4).random(g["thck"].shape)
+    bex, bey = asm.lognormal_beta((ny - 1, nx - 1), 6), asm.lognormal_beta((ny - 1, nx - 1), 7)
+    wu, wv = oracle.basal_diva(nx, ny, dx, dx, g["ac"], g["av"], bex, bey, lsrf, g["xVertex"], g["yVertex"], mode,
+                               S.Auu, S.Avv)
+    Auu, Avv = np.array(S.Auu, copy=True), np.array(S.Avv, copy=True)
+    cg.basal_sliding_bc_2d_diva(nx, ny, 2, dx, dx, g["ac"], g["av"], bex, bey, lsrf, g["xVertex"], g["yVertex"], Auu, Avv,
+                                whichassemble_beta=mode)
+    if mode == 0:
+        np.testing.assert_array_equal(Auu, wu)
+        np.testing.assert_array_equal(Avv, wv)
+    else:
+        for a, b in ((Auu, wu), (Avv, wv)):
+            d = np.abs(a - b)
+            assert d[4].max() <= 1e-15 * np.abs(b[4]).max()
+            d[4] = 0.0
+            assert np.all(d == 0.0)
