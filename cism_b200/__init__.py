@@ -198,6 +198,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         [d] * 9
     lib.cismgpu_solver_assemble_stiffness_2d_diva.argtypes = [vp, i32, i32] + [d] * 14 + [i32, dbl, dbl, dbl] + [d] * 4
     lib.cismgpu_basal_sliding_bc_2d_diva.argtypes = [i32, i32, i32, dbl, dbl, d, d, d, d, d, d, d, i32, d, d, d]
+    lib.cismgpu_solver_assemble_system_2d_diva.argtypes = [vp, i32, i32, dbl, dbl] + [d] * 13 + \
+        [i32, dbl, dbl, dbl, d, d, d, i32] + [d] * 7
     lib.cismgpu_dirichlet_boundary_conditions_2d.argtypes = [i32, i32, i32, d, d, d, d, d, d, d, d, d, d, d, d]
     lib.cismgpu_basal_sliding_bc_2d.argtypes = [i32, i32, i32, dbl, dbl, d, d, d, d, d, i32, d, d, d]
     lib.cismgpu_solver_assemble_system_2d.argtypes = [vp, i32, i32, dbl, dbl, d, d, d, d, d, d, d, i32, dbl, dbl, dbl,
@@ -213,7 +215,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
               "cismgpu_solver_assemble_system_3d", "cismgpu_dirichlet_boundary_conditions_2d",
               "cismgpu_basal_sliding_bc_2d", "cismgpu_solver_assemble_system_2d",
               "cismgpu_assemble_stiffness_matrix_2d_diva", "cismgpu_solver_assemble_stiffness_2d_diva",
-              "cismgpu_basal_sliding_bc_2d_diva"):
+              "cismgpu_basal_sliding_bc_2d_diva", "cismgpu_solver_assemble_system_2d_diva"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -789,6 +791,36 @@ class DeviceSolver:
             self.handle, nz, int(nhalo), head[0], *ss, head[1], head[2], head[3], pu, pv, *dv, tail[2], int(whichefvs),
             float(efvs_constant), float(effstrain_min), float(n_glen), pe, _ptr(efvs, np.float64, efvs.size, True),
             _ptr(ok, np.float64, ok.size, True), _ptr(om, np.float64, om.size, True)))
+        return efvs, ok, om
+
+    def assemble_system_diva(self, nz, nhalo, dx, dy, sigma, stagsigma, active_cell, active_vertex, xVertex, yVertex,
+                             stagthck, thck, btractx, btracty, dsfx, dsfy, flwafact, loadu, loadv, beta_eff_x=None,
+                             beta_eff_y=None, lsrf=None, umask=None, vmask=None, whichassemble_beta=1, whichefvs=2,
+                             efvs_constant=0.0, effstrain_min=1.0e-8, n_glen=3.0):
+        """One Picard iteration's DIVA system on this 2D handle; returns (efvs, omega_k, omega)."""
+        P = self.problem
+        nx, ny = P.nx, P.ny
+        nv = (nx - 1) * (ny - 1)
+        efvs = np.zeros((ny, nx, nz - 1))
+        ok = np.zeros((ny, nx, nz))
+        om = np.zeros((ny, nx))
+        head, tail = _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagthck, stagthck, flwafact)
+        ss, dv = _diva_inputs(nx, ny, nz, stagsigma, stagthck, thck, btractx, btracty, dsfx, dsfy)
+        i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+        keep = [i32(active_vertex)] + ([i32(umask), i32(vmask)] if umask is not None else [])
+        pm = (_ptr(keep[1], np.int32, nv), _ptr(keep[2], np.int32, nv)) if umask is not None else (None, None)
+        if beta_eff_x is not None:
+            lk = np.ascontiguousarray(lsrf, dtype=np.float64)
+            keep.append(lk)
+            pb = (_ptr(beta_eff_x, np.float64, nv), _ptr(beta_eff_y, np.float64, nv), _ptr(lk, np.float64, nx * ny))
+        else:
+            pb = (None, None, None)
+        _check(self._lib, self._lib.cismgpu_solver_assemble_system_2d_diva(
+            self.handle, nz, int(nhalo), float(dx), float(dy), head[0], *ss, head[1], _ptr(keep[0], np.int32, nv),
+            head[2], head[3], *dv, tail[2], int(whichefvs), float(efvs_constant), float(effstrain_min), float(n_glen),
+            *pb, int(whichassemble_beta), _ptr(loadu, np.float64, nv), _ptr(loadv, np.float64, nv), *pm,
+            _ptr(efvs, np.float64, efvs.size, True), _ptr(ok, np.float64, ok.size, True),
+            _ptr(om, np.float64, om.size, True)))
         return efvs, ok, om
 
     def save(self):

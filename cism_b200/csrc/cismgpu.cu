@@ -2625,6 +2625,56 @@ int cismgpu_solver_assemble_stiffness_2d_diva(cismgpu_solver_t *h, int nz, int n
     return CISMGPU_OK;
 }
 
+int cismgpu_solver_assemble_system_2d_diva(
+    cismgpu_solver_t *h, int nz, int nhalo, double dx, double dy, const double *sigma, const double *stagsigma,
+    const int32_t *active_cell, const int32_t *active_vertex, const double *xVertex, const double *yVertex,
+    const double *stagthck, const double *thck, const double *btractx, const double *btracty,
+    const double *diva_slope_factor_x, const double *diva_slope_factor_y, const double *flwafact, int whichefvs,
+    double efvs_constant, double effstrain_min, double n_glen, const double *beta_eff_x, const double *beta_eff_y,
+    const double *lsrf, int whichassemble_beta, const double *loadu, const double *loadv,
+    const int32_t *umask_dirichlet, const int32_t *vmask_dirichlet, double *efvs, double *omega_k, double *omega) {
+    g_last_error.clear();
+    if (!h) return fail(CISMGPU_EINVAL, "null argument");
+    if (!active_vertex || !loadu || !loadv || (!beta_eff_x) != (!beta_eff_y) || (beta_eff_x && !lsrf) ||
+        (!umask_dirichlet) != (!vmask_dirichlet))
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (whichassemble_beta != 0 && whichassemble_beta != 1)
+        return fail(CISMGPU_EINVAL, "whichassemble_beta must be 0 (standard) or 1 (local)");
+    // the DIVA stiffness from the handle's current velocity and its kept layer viscosities
+    TRY(cismgpu_solver_assemble_stiffness_2d_diva(h, nz, nhalo, sigma, stagsigma, active_cell, xVertex, yVertex,
+                                                  nullptr, nullptr, stagthck, thck, btractx, btracty,
+                                                  diva_slope_factor_x, diva_slope_factor_y, flwafact, whichefvs,
+                                                  efvs_constant, effstrain_min, n_glen, nullptr, efvs, omega_k, omega));
+    std::lock_guard<std::mutex> lk(h->mu);
+    Solver &sv = h->sv;
+    SymIdx L{};
+    for (int c = 0; c < 27; ++c) L.map[c] = c + 1;
+    L.n = sv.nvec;
+    L.NQ = sv.g.NQ;
+    L.nz = 1;
+    L.raw3 = 0;
+    const size_t bs = (size_t)9 * sv.nvec;
+    double *A0 = sv.A.as<double>();
+    const Ptrs p = sv.ptrs();
+    TRY(sv.put_vec(VB_U, loadu));
+    TRY(sv.put_vec(VB_V, loadv));
+    // basal_sliding_bc_2d_diva (:2575-2589), b = load, dirichlet_boundary_conditions_2d
+    TRY(sv.boundary2d(L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, p.bu, p.bv, nhalo, dx, dy, active_vertex, beta_eff_x,
+                      umask_dirichlet, vmask_dirichlet, nullptr, nullptr, sv.x_current ? VX_U : VX0_U,
+                      whichassemble_beta, active_cell, xVertex, yVertex, beta_eff_y, lsrf));
+    Geom gA = sv.g;
+    gA.nz = 9;
+    const unsigned hb = nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4));
+    cudaStream_t s = sv.stream;
+    k_halo<<<hb, kBlock, 0, s>>>(gA, A0, A0 + bs, nullptr);
+    k_halo<<<hb, kBlock, 0, s>>>(gA, A0 + 2 * bs, A0 + 3 * bs, nullptr);
+    k_halo<<<hb, kBlock, 0, s>>>(sv.g, p.bu, p.bv, nullptr);
+    CU(cudaGetLastError());
+    CU(cudaStreamSynchronize(s));
+    sv.mixed.stale = true;
+    return CISMGPU_OK;
+}
+
 int cismgpu_solver_check_symmetry(cismgpu_solver_t *h, double *maxdiff, long long *nwarn) {
     g_last_error.clear();
     if (!h) return fail(CISMGPU_EINVAL, "null argument");

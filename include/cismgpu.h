@@ -538,6 +538,18 @@ int cismgpu_solver_assemble_stiffness_2d_diva(cismgpu_solver_t *s, int nz, int n
                                               double effstrain_min, double n_glen, const double *efvs_qp_3d_in,
                                               double *efvs, double *omega_k, double *omega);
 
+/* The DIVA system of one Picard iteration on a 2D handle (:2560-2666 with whichapprox =
+ * HO_APPROX_DIVA): the DIVA stiffness from the current velocity and the kept layer viscosities,
+ * the DIVA basal term (beta_eff_x/_y, lsrf; NULL: none), b = load, Dirichlet, halo. */
+int cismgpu_solver_assemble_system_2d_diva(
+    cismgpu_solver_t *s, int nz, int nhalo, double dx, double dy, const double *sigma, const double *stagsigma,
+    const int32_t *active_cell, const int32_t *active_vertex, const double *xVertex, const double *yVertex,
+    const double *stagthck, const double *thck, const double *btractx, const double *btracty,
+    const double *diva_slope_factor_x, const double *diva_slope_factor_y, const double *flwafact, int whichefvs,
+    double efvs_constant, double effstrain_min, double n_glen, const double *beta_eff_x, const double *beta_eff_y,
+    const double *lsrf, int whichassemble_beta, const double *loadu, const double *loadv,
+    const int32_t *umask_dirichlet, const int32_t *vmask_dirichlet, double *efvs, double *omega_k, double *omega);
+
 /* The 2D (SSA) assembly into a 2D handle; nz: the number of sigma levels of flwafact. */
 int cismgpu_solver_assemble_stiffness_2d(cismgpu_solver_t *s, int nz, int nhalo, const double *sigma,
                                          const int32_t *active_cell, const double *xVertex, const double *yVertex,

@@ -507,3 +507,44 @@ def test_basal_diva(gpu_lib, mode):
             assert d[4].max() <= 1e-15 * np.abs(b[4]).max()
             d[4] = 0.0
             assert np.all(d == 0.0)
+
+
+def test_diva_system_on_handle(gpu_lib):
+    """cismgpu_solver_assemble_system_2d_diva equals the one-shot sequence (DIVA stiffness, DIVA
+    basal term, b = load, Dirichlet, staggered halo) bit for bit, through the residual."""
+    g, u, v, ff, extra = _diva_case(seed=40)
+    nx, ny, nz, dx = g["nx"], g["ny"], g["nz"], g["dx"]
+    stagsig, bx, by, dsfx, dsfy = extra
+    P = asm.assemble_ssa_2d(g["thck"], g["usrf"], dx, dx, asm.lognormal_beta((ny - 1, nx - 1), 8))
+    bex, bey = asm.lognormal_beta((ny - 1, nx - 1), 6), asm.lognormal_beta((ny - 1, nx - 1), 7)
+    lsrf = g["usrf"] - g["thck"]
+    um = (np.random.default_rng(3).random(P.bu.shape) < 0.1).astype(np.int32)
+    load = (np.array(P.bu, copy=True), np.array(P.bv, copy=True))
+    s = cg.DeviceSolver(P, x0=(u, v))
+    try:
+        eh = s.assemble_system_diva(nz, 2, dx, dx, g["sigma"], stagsig, g["ac"].astype(np.int32),
+                                    g["av"].astype(np.int32), g["xVertex"], g["yVertex"], g["stagthck"], g["thck"], bx,
+                                    by, dsfx, dsfy, ff, load[0], load[1], beta_eff_x=bex, beta_eff_y=bey, lsrf=lsrf,
+                                    umask=um, vmask=um)
+        ru, rv, l2, _ = s.residual_vector()
+    finally:
+        s.close()
+    eq = np.zeros((ny, nx, 4, nz - 1))
+    efvs, ok, om, *A = _diva_gpu(g, u, v, ff, extra, eq)
+    for a, b in zip(eh, (efvs, ok, om)):
+        np.testing.assert_array_equal(a, b)
+    bu, bv = np.array(load[0], copy=True), np.array(load[1], copy=True)
+    cg.basal_sliding_bc_2d_diva(nx, ny, 2, dx, dx, g["ac"], g["av"], bex, bey, lsrf, g["xVertex"], g["yVertex"], A[0],
+                                A[3])
+    cg.dirichlet_boundary_conditions_2d(nx, ny, 2, g["av"], um, um, u, v, *A, bu, bv)
+    from tests import problems
+    Q = asm.assemble_ssa_2d(g["thck"], g["usrf"], dx, dx, asm.lognormal_beta((ny - 1, nx - 1), 8))
+    for n, a in zip(BLOCKS, A):
+        setattr(Q, n, a)
+    Q.bu, Q.bv = bu, bv
+    Q = problems.halo_blocks_2d(Q)
+    want = cg.compute_residual_vector_2d(nx, ny, Q.par, asm.indxA_2d(), Q.active_vertex, Q.Auu, Q.Auv, Q.Avu, Q.Avv,
+                                         Q.bu, Q.bv, u, v)
+    np.testing.assert_array_equal(ru, want[0])
+    np.testing.assert_array_equal(rv, want[1])
+    assert l2 == want[2]
