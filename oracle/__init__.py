@@ -83,6 +83,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_assemble_stiffness_2d_diva.argtypes = [i, i, i, i] + [d] * 14 + [i, dbl, dbl, dbl] + [d] * 8
         L.oracle_basal_diva.argtypes = [i, i, i, dbl, dbl, d, d, d, d, d, d, d, i, d, d]
         L.oracle_basal_diva.restype = None
+        L.oracle_assemble_stiffness_2d_l1l2.argtypes = [i, i, i, i] + [d] * 11 + [i, dbl, dbl, dbl] + [d] * 5
         L.oracle_check_symmetry.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, P(dbl), P(ctypes.c_long)]
         L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
@@ -339,6 +340,21 @@ def basal_diva(nx, ny, dx, dy, active_cell, active_vertex, beta_eff_x, beta_eff_
                             _p(f64(beta_eff_x)), _p(f64(beta_eff_y)), _p(f64(lsrf)), _p(f64(xVertex)), _p(f64(yVertex)),
                             int(whichassemble_beta), _p(out[0]), _p(out[1]))
     return out[0], out[1]
+
+
+def assemble_stiffness_2d_l1l2(nx, ny, nz, sigma, active_cell, xVertex, yVertex, uvel, vvel, stagthck, dusrf_dx,
+                               dusrf_dy, flwa, flwafact, whichefvs=2, efvs_constant=0.0, effstrain_min=1.0e-8,
+                               n_glen=3.0, nhalo=2):
+    """assemble_stiffness_matrix_2d with HO_APPROX_L1L2: vertex fields (ny-1, nx-1), flwa and
+    flwafact (ny, nx, nz-1).  Returns (status, efvs (ny, nx, nz-1), Auu, Auv, Avu, Avv)."""
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    efvs = np.zeros((ny, nx, nz - 1))
+    A = [np.zeros((9, ny - 1, nx - 1)) for _ in range(4)]
+    ins = [f64(sigma), np.ascontiguousarray(active_cell, dtype=np.int32), f64(xVertex), f64(yVertex), f64(uvel),
+           f64(vvel), f64(stagthck), f64(dusrf_dx), f64(dusrf_dy), f64(flwa), f64(flwafact)]
+    st = lib().oracle_assemble_stiffness_2d_l1l2(nx, ny, nz, nhalo, *[_p(a) for a in ins], whichefvs, efvs_constant,
+                                                 effstrain_min, n_glen, _p(efvs), *[_p(a) for a in A])
+    return (st, efvs, *A)
 
 
 def reprosum(a) -> float:

@@ -925,3 +925,140 @@ void oracle_basal_diva(int nx, int ny, int nhalo, double dx, double dy, const in
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// assemble_stiffness_matrix_2d, L1L2 branch (compute_effective_viscosity_L1L2 :7474-7726)
+// ---------------------------------------------------------------------------
+namespace {
+constexpr double kRhoi = 910.0, kGrav = 9.81;  // glimmer_physcon.F90:67, :69
+
+// compute_effective_viscosity_L1L2 at one quadrature point of a 4-node cell: per layer the
+// cubic for tau_parallel, then efvs = 1/(2A) (n = 1) or 1/(2A(tau_par^2 + tau_perp^2)) (n = 3).
+// Fortran's a**3 is (a*a)*a, x**(1/3) is pow.  Returns false for another n_glen (GM_FATAL).
+bool efvs_l1l2(int whichefvs, double efvs_constant, double effstrain_min, double n_glen, int nz, const double *sigma,
+               const double *phi, const double *dx, const double *dy, const double *u, const double *v,
+               const double *h, const double *dsdx, const double *dsdy, const double *flwa, const double *flwafact,
+               double *efvs) {
+    const double p_effstr = (1.0 - n_glen) / n_glen;
+    if (whichefvs == kEfvsConstant) {
+        for (int k = 0; k < nz - 1; ++k) efvs[k] = efvs_constant;
+        return true;
+    }
+    if (whichefvs == kEfvsFlowfact) {
+        const double effstrain = kVeloScale / kLenScale * kScyr;
+        for (int k = 0; k < nz - 1; ++k) efvs[k] = flwafact[k] * std::pow(effstrain, p_effstr);
+        return true;
+    }
+    double du_dx = 0.0, du_dy = 0.0, dv_dx = 0.0, dv_dy = 0.0, ds_dx = 0.0, ds_dy = 0.0, thck = 0.0;
+    for (int n = 0; n < 4; ++n) {
+        du_dx = du_dx + dx[n] * u[n];
+        du_dy = du_dy + dy[n] * u[n];
+        dv_dx = dv_dx + dx[n] * v[n];
+        dv_dy = dv_dy + dy[n] * v[n];
+        ds_dx = ds_dx + phi[n] * dsdx[n];
+        ds_dy = ds_dy + phi[n] * dsdy[n];
+        thck = thck + phi[n] * h[n];
+    }
+    const double sq = effstrain_min * effstrain_min + du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy +
+                      0.25 * ((dv_dx + du_dy) * (dv_dx + du_dy));
+    const double effstrain = std::sqrt(sq);
+    for (int k = 0; k < nz - 1; ++k) {
+        const double depth = thck * sigma[k + 1];
+        const double grads = std::sqrt(ds_dx * ds_dx + ds_dy * ds_dy);
+        const double tau_perp = kRhoi * kGrav * depth * grads;
+        const double a = tau_perp * tau_perp;
+        const double b = -effstrain / flwa[k];
+        const double a3 = (a * a) * a;
+        const double c = std::sqrt(b * b / 4.0 + a3 / 27.0);
+        const double rootA = std::pow(-b / 2.0 + c, 1.0 / 3.0);
+        double rootB;
+        if (a3 / 27.0 > 1.0e-6 * (b * b / 4.0)) rootB = -std::pow(b / 2.0 + c, 1.0 / 3.0);
+        else rootB = -a / (3.0 * std::pow(std::fabs(b), 1.0 / 3.0));
+        const double tau_parallel = rootA + rootB;
+        if (std::fabs(n_glen - 1.0) < 1.0e-10) efvs[k] = 1.0 / (2.0 * flwa[k]);
+        else if (std::fabs(n_glen - 3.0) < 1.0e-10)
+            efvs[k] = 1.0 / (2.0 * flwa[k] * (tau_parallel * tau_parallel + tau_perp * tau_perp));
+        else return false;
+    }
+    return true;
+}
+}  // namespace
+
+extern "C" {
+
+// assemble_stiffness_matrix_2d (:4961-5378) with whichapprox = HO_APPROX_L1L2: per Gauss point the
+// layer viscosities of compute_effective_viscosity_L1L2 (surface gradient dusrf_dx/_dy at the
+// vertices, flwa per layer), their sigma-weighted average, the Blatter-Pattyn element matrix with
+// dphi_dz = 0 and h*efvs; efvs(k,i,j) the mean over the points.  Returns 0, 1 (singular Jacobian),
+// 2 (nhalo < 2) or 3 (n_glen neither 1 nor 3, the reference's GM_FATAL).
+int oracle_assemble_stiffness_2d_l1l2(int nx, int ny, int nz, int nhalo, const double *sigma,
+                                      const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                      const double *uvel, const double *vvel, const double *stagthck,
+                                      const double *dusrf_dx, const double *dusrf_dy, const double *flwa,
+                                      const double *flwafact, int whichefvs, double efvs_constant,
+                                      double effstrain_min, double n_glen, double *efvs, double *Auu, double *Auv,
+                                      double *Avu, double *Avv) {
+    if (nhalo < 2) return 2;
+    const long NX = nx - 1, NY = ny - 1, NQ = NX * NY;
+    const RefElement2 &R = ref2();
+    std::memset(efvs, 0, sizeof(double) * (size_t)(nz - 1) * nx * ny);
+    for (double *A : {Auu, Auv, Avu, Avv}) std::memset(A, 0, sizeof(double) * 9 * (size_t)NQ);
+    std::vector<double> eq((size_t)(nz - 1) * 4);
+    for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+        for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+            const long cidx = (i - 1) + (long)nx * (j - 1);
+            if (!active_cell[cidx]) continue;
+            double Kuu[4][4] = {}, Kuv[4][4] = {}, Kvu[4][4] = {}, Kvv[4][4] = {};
+            double x[4], y[4], u[4], v[4], h[4], sx[4], sy[4];
+            for (int n = 0; n < 4; ++n) {
+                const long q = (long)(i + kIsh3[n] - 1) + NX * (j + kJsh3[n] - 1);
+                x[n] = xVertex[q];
+                y[n] = yVertex[q];
+                u[n] = uvel[q];
+                v[n] = vvel[q];
+                h[n] = stagthck[q];
+                sx[n] = dusrf_dx[q];
+                sy[n] = dusrf_dy[q];
+            }
+            const double *fl = flwa + (size_t)(nz - 1) * cidx, *ff = flwafact + (size_t)(nz - 1) * cidx;
+            for (int p = 0; p < 4; ++p) {
+                double dx[4], dy[4], dz[4] = {0.0, 0.0, 0.0, 0.0}, detJ;
+                if (!basis_derivs_2d(x, y, R.dxr[p], R.dyr[p], dx, dy, &detJ)) return 1;
+                double *e = eq.data() + (size_t)(nz - 1) * p;
+                if (!efvs_l1l2(whichefvs, efvs_constant, effstrain_min, n_glen, nz, sigma, R.phi[p], dx, dy, u, v, h,
+                               sx, sy, fl, ff, e))
+                    return 3;
+                double vavg = 0.0;
+                for (int k = 0; k < nz - 1; ++k) vavg = vavg + e[k] * (sigma[k + 1] - sigma[k]);
+                double h_qp = 0.0;
+                for (int n = 0; n < 4; ++n) h_qp = h_qp + R.phi[p][n] * h[n];
+                const double f = h_qp * vavg * 1.0 * detJ / kVol0;
+                for (int nc = 0; nc < 4; ++nc)
+                    for (int nr = 0; nr < 4; ++nr) {
+                        Kuu[nr][nc] = Kuu[nr][nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc] + dz[nr] * dz[nc]);
+                        Kuv[nr][nc] = Kuv[nr][nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
+                        Kvu[nr][nc] = Kvu[nr][nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
+                        Kvv[nr][nc] = Kvv[nr][nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc] + dz[nr] * dz[nc]);
+                    }
+            }
+            for (int k = 0; k < nz - 1; ++k) {
+                double s = 0.0;
+                for (int p = 0; p < 4; ++p) s = s + eq[(size_t)(nz - 1) * p + k];
+                efvs[k + (long)(nz - 1) * cidx] = s / 4;
+            }
+            for (int nr = 0; nr < 4; ++nr) {
+                const long q = (long)(i + kIsh3[nr] - 1) + NX * (j + kJsh3[nr] - 1);
+                for (int nc = 0; nc < 4; ++nc) {
+                    const int m = (kIsh3[nc] - kIsh3[nr] + 1) + 3 * (kJsh3[nc] - kJsh3[nr] + 1);
+                    const size_t a = (size_t)q + (size_t)NQ * m;
+                    Auu[a] = Auu[a] + Kuu[nr][nc];
+                    Auv[a] = Auv[a] + Kuv[nr][nc];
+                    Avu[a] = Avu[a] + Kvu[nr][nc];
+                    Avv[a] = Avv[a] + Kvv[nr][nc];
+                }
+            }
+        }
+    return 0;
+}
+
+}  // extern "C"

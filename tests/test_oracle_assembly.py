@@ -308,3 +308,55 @@ def test_diva_layer_viscosity_and_integrals():
         assert abs(om[j, i] - want_om) <= 1e-13 * want_om
         np.testing.assert_allclose(efvs[j, i], eq[j, i].mean(axis=0), rtol=1e-14)
     assert np.all(ok[~act] == 0.0) and np.all(om[~act] == 0.0)
+
+
+# ---------------------------------------------------------------------------
+# assemble_stiffness_matrix_2d, L1L2 branch (compute_effective_viscosity_L1L2 :7474-7726)
+# ---------------------------------------------------------------------------
+
+def run_l1l2(g, u, v, dsdx, dsdy, flwa, n_glen=3.0, **kw):
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    ff = 0.5 * flwa ** (-1.0 / 3.0)
+    return oracle.assemble_stiffness_2d_l1l2(nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], u, v,
+                                             g["stagthck"], dsdx, dsdy, flwa, ff, n_glen=n_glen, **kw)
+
+
+def test_l1l2_flat_surface_is_glen():
+    """With a flat surface tau_perp = 0, the cubic gives tau_parallel = (effstrain/A)^(1/3) and
+    efvs = 1/(2 A tau_parallel^2), Glen's viscosity 0.5 A^(-1/3) effstrain^(-2/3)."""
+    g = geometry(seed=91, nz=6)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    a, b = (2.0e-3, -1.0e-3), (0.5e-3, 2.5e-3)
+    u = a[0] * g["xVertex"] + a[1] * g["yVertex"]
+    v = b[0] * g["xVertex"] + b[1] * g["yVertex"]
+    layer = 1e-16 * (1 + np.random.default_rng(2).random(nz - 1))
+    flwa = np.broadcast_to(layer, (ny, nx, nz - 1)).copy()
+    z = np.zeros((ny - 1, nx - 1))
+    st, efvs, *A = run_l1l2(g, u, v, z, z, flwa)
+    assert st == 0
+    eff = np.sqrt(1e-16 + a[0] ** 2 + b[1] ** 2 + a[0] * b[1] + 0.25 * (b[0] + a[1]) ** 2)
+    want = 0.5 * layer ** (-1.0 / 3.0) * eff ** (-2.0 / 3.0)
+    act = g["ac"]
+    assert np.abs(efvs[act] - want).max() <= 1e-12 * want.max()
+
+
+def test_l1l2_linear_rheology_and_errors():
+    """n = 1: efvs = 1/(2A) in every layer whatever the flow; another n is the reference's
+    GM_FATAL (status 3)."""
+    g = geometry(seed=92, nz=6)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(3)
+    u, v = rng.standard_normal((ny - 1, nx - 1)), rng.standard_normal((ny - 1, nx - 1))
+    dsdx, dsdy = 0.01 * rng.standard_normal((ny - 1, nx - 1)), 0.01 * rng.standard_normal((ny - 1, nx - 1))
+    flwa = 1e-16 * (1 + rng.random((ny, nx, nz - 1)))
+    st, efvs, *A = run_l1l2(g, u, v, dsdx, dsdy, flwa, n_glen=1.0)
+    assert st == 0
+    act = g["ac"]
+    np.testing.assert_array_equal(efvs[act], (1.0 / (2.0 * flwa))[act])
+    assert run_l1l2(g, u, v, dsdx, dsdy, flwa, n_glen=2.0)[0] == 3
+    st, efvs3, *A3 = run_l1l2(g, u, v, dsdx, dsdy, flwa)  # n = 3 with a sloping surface: below Glen's
+    assert st == 0 and np.all(efvs3[act] > 0.0)
+    P = asm.Problem("2d", nx, ny, 1, *A3, np.zeros_like(u), np.zeros_like(u), g["av"].astype(np.int32),
+                    asm.default_par(nx, ny))
+    r = oracle.check_symmetry(P)
+    assert r[4] == 0.0 and r[5] == 0
