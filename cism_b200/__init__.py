@@ -32,7 +32,7 @@ __all__ = [
     "check_symmetry_assembled_matrix_3d", "check_symmetry_assembled_matrix_2d", "assemble_stiffness_matrix_3d",
     "assemble_stiffness_matrix_2d", "dirichlet_boundary_conditions_3d", "basal_sliding_bc_3d",
     "dirichlet_boundary_conditions_2d", "basal_sliding_bc_2d", "assemble_stiffness_matrix_2d_diva",
-    "basal_sliding_bc_2d_diva",
+    "basal_sliding_bc_2d_diva", "assemble_stiffness_matrix_2d_l1l2",
 ]
 
 ALG_STANDARD, ALG_CHRONGEAR, ALG_MIXED_CHRONGEAR = 0, 1, 2
@@ -198,6 +198,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         [d] * 9
     lib.cismgpu_solver_assemble_stiffness_2d_diva.argtypes = [vp, i32, i32] + [d] * 14 + [i32, dbl, dbl, dbl] + [d] * 4
     lib.cismgpu_basal_sliding_bc_2d_diva.argtypes = [i32, i32, i32, dbl, dbl, d, d, d, d, d, d, d, i32, d, d, d]
+    lib.cismgpu_assemble_stiffness_matrix_2d_l1l2.argtypes = [i32, i32, i32, i32] + [d] * 11 + \
+        [i32, dbl, dbl, dbl] + [d] * 6
     lib.cismgpu_solver_assemble_system_2d_diva.argtypes = [vp, i32, i32, dbl, dbl] + [d] * 13 + \
         [i32, dbl, dbl, dbl, d, d, d, i32] + [d] * 7
     lib.cismgpu_dirichlet_boundary_conditions_2d.argtypes = [i32, i32, i32, d, d, d, d, d, d, d, d, d, d, d, d]
@@ -215,7 +217,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
               "cismgpu_solver_assemble_system_3d", "cismgpu_dirichlet_boundary_conditions_2d",
               "cismgpu_basal_sliding_bc_2d", "cismgpu_solver_assemble_system_2d",
               "cismgpu_assemble_stiffness_matrix_2d_diva", "cismgpu_solver_assemble_stiffness_2d_diva",
-              "cismgpu_basal_sliding_bc_2d_diva", "cismgpu_solver_assemble_system_2d_diva"):
+              "cismgpu_basal_sliding_bc_2d_diva", "cismgpu_solver_assemble_system_2d_diva",
+              "cismgpu_assemble_stiffness_matrix_2d_l1l2"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -569,6 +572,26 @@ def assemble_stiffness_matrix_2d_diva(nx, ny, nz, nhalo, sigma, stagsigma, activ
         _ptr(efvs, np.float64, efvs.size, True), _ptr(ok, np.float64, ok.size, True), _ptr(om, np.float64, om.size, True),
         *[_ptr(a, np.float64, a.size, True) for a in A]))
     return (efvs, ok, om, *A)
+
+
+def assemble_stiffness_matrix_2d_l1l2(nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel_2d, vvel_2d,
+                                      stagthck, dusrf_dx, dusrf_dy, flwa, flwafact, whichefvs=2, efvs_constant=0.0,
+                                      effstrain_min=1.0e-8, n_glen=3.0, indxA_2d=None):
+    """Mirrors assemble_stiffness_matrix_2d with HO_APPROX_L1L2 (glissade_velo_higher.F90:4961-5378)
+    on the GPU.  Returns (efvs (ny, nx, nz-1), Auu, Auv, Avu, Avv (9, ny-1, nx-1))."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    indx = np.arange(1, 10, dtype=np.int32) if indxA_2d is None else np.ascontiguousarray(indxA_2d, dtype=np.int32)
+    efvs = np.zeros((ny, nx, nz - 1))
+    A = [np.zeros((9, ny - 1, nx - 1)) for _ in range(4)]
+    head, tail = _assembly_inputs(nx, ny, nz, sigma, active_cell, xVertex, yVertex, stagthck, stagthck, flwafact)
+    _check(lib, lib.cismgpu_assemble_stiffness_matrix_2d_l1l2(
+        nx, ny, nz, int(nhalo), *head, _ptr(uvel_2d, np.float64, nv), _ptr(vvel_2d, np.float64, nv), tail[1],
+        _ptr(dusrf_dx, np.float64, nv), _ptr(dusrf_dy, np.float64, nv),
+        _ptr(np.ascontiguousarray(flwa, dtype=np.float64), np.float64, (nz - 1) * nx * ny), tail[2], int(whichefvs),
+        float(efvs_constant), float(effstrain_min), float(n_glen), _ptr(indx, np.int32, 9),
+        _ptr(efvs, np.float64, efvs.size, True), *[_ptr(a, np.float64, a.size, True) for a in A]))
+    return (efvs, *A)
 
 
 def basal_sliding_bc_2d_diva(nx, ny, nhalo, dx, dy, active_cell, active_vertex, beta_eff_x, beta_eff_y, lsrf,

@@ -918,4 +918,149 @@ __global__ void __launch_bounds__(kBlock) k_basal_local_diva(int nx, int ny, dou
     Avv[a] = Avv[a] + (dx * dy / kAsmVol0) * bey[q] / cos(ty);
 }
 
+// ---------------------------------------------------------------------------
+// assemble_stiffness_matrix_2d, L1L2 branch (:5225-5250 with compute_effective_viscosity_L1L2
+// :7474-7726): per Gauss point and layer the cubic for tau_parallel (Fortran's a**3 is (a*a)*a,
+// x**(1/3) is pow) and efvs = 1/(2A) for n = 1 or 1/(2A(tau_par^2 + tau_perp^2)) for n = 3 (the
+// host rejects other n).  No state; the cell's own thread sums the layer viscosities over the
+// points into efvs (zeroed by the host), in the reference's order, and divides by 4.
+struct L1l2Args {
+    const double *dsdx, *dsdy;  // (nx-1, ny-1) surface gradient at the vertices
+    const double *flwa;         // (nz-1, nx, ny)
+    int linear;                 // n_glen == 1
+};
+
+__device__ void asm_cell_row_l1l2(const AsmArgs &a, const L1l2Args &l, int ie, int je, int nr, bool own,
+                                  double acc[4][9]) {
+    const long long NX = a.nx - 1;
+    const int nl = a.nz - 1;
+    double x[4], y[4], u[4], v[4], h[4], sx[4], sy[4];
+#pragma unroll
+    for (int n = 0; n < 4; ++n) {
+        const long long q = (long long)(ie + c_ish3[n] - 1) + NX * (je + c_jsh3[n] - 1);
+        x[n] = a.xv[q];
+        y[n] = a.yv[q];
+        u[n] = a.u[q];
+        v[n] = a.v[q];
+        h[n] = a.thck[q];
+        sx[n] = l.dsdx[q];
+        sy[n] = l.dsdy[q];
+    }
+    const long long cidx = (ie - 1) + (long long)a.nx * (je - 1);
+    const double *fl = l.flwa + (long long)nl * cidx, *ff = a.flwafact + (long long)nl * cidx;
+    double *ecell = a.efvs + (long long)nl * cidx;
+    double Kuu[4], Kuv[4], Kvu[4], Kvv[4];
+#pragma unroll
+    for (int nc = 0; nc < 4; ++nc) Kuu[nc] = Kuv[nc] = Kvu[nc] = Kvv[nc] = 0.0;
+    for (int p = 0; p < 4; ++p) {
+        const double *dxr = c_asm_ref2.dxr[p], *dyr = c_asm_ref2.dyr[p], *phi = c_asm_ref2.phi[p];
+        double J00 = 0.0, J01 = 0.0, J10 = 0.0, J11 = 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            J00 = J00 + dxr[n] * x[n];
+            J01 = J01 + dxr[n] * y[n];
+            J10 = J10 + dyr[n] * x[n];
+            J11 = J11 + dyr[n] * y[n];
+        }
+        const double detJ = J00 * J11 - J01 * J10;
+        if (!(fabs(detJ) > 0.0)) {
+            atomicExch(a.singular, 1);
+            return;
+        }
+        const double i00 = J11 / detJ, i01 = -J01 / detJ, i10 = -J10 / detJ, i11 = J00 / detJ;
+        double dx[4], dy[4];
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            dx[n] = 0.0 + i00 * dxr[n] + i01 * dyr[n];
+            dy[n] = 0.0 + i10 * dxr[n] + i11 * dyr[n];
+        }
+        double du_dx = 0.0, du_dy = 0.0, dv_dx = 0.0, dv_dy = 0.0, ds_dx = 0.0, ds_dy = 0.0, thck = 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) {
+            du_dx = du_dx + dx[n] * u[n];
+            du_dy = du_dy + dy[n] * u[n];
+            dv_dx = dv_dx + dx[n] * v[n];
+            dv_dy = dv_dy + dy[n] * v[n];
+            ds_dx = ds_dx + phi[n] * sx[n];
+            ds_dy = ds_dy + phi[n] * sy[n];
+            thck = thck + phi[n] * h[n];
+        }
+        const double sh = dv_dx + du_dy;
+        const double effstrain = sqrt(a.effstrain_min * a.effstrain_min + du_dx * du_dx + dv_dy * dv_dy +
+                                      du_dx * dv_dy + 0.25 * (sh * sh));
+        double vavg = 0.0;
+        for (int k = 0; k < nl; ++k) {
+            double e;
+            if (a.whichefvs == 0) {
+                e = a.efvs_constant;
+            } else if (a.whichefvs == 1) {
+                e = ff[k] * a.flowfact_pow;
+            } else {
+                const double depth = thck * a.sigma[k + 1];
+                const double grads = sqrt(ds_dx * ds_dx + ds_dy * ds_dy);
+                const double tau_perp = 910.0 * 9.81 * depth * grads;  // rhoi*grav, glimmer_physcon.F90:67,69
+                const double aa = tau_perp * tau_perp;
+                const double b = -effstrain / fl[k];
+                const double a3 = (aa * aa) * aa;
+                const double c = sqrt(b * b / 4.0 + a3 / 27.0);
+                const double rootA = pow(-b / 2.0 + c, 1.0 / 3.0);
+                const double rootB = (a3 / 27.0 > 1.0e-6 * (b * b / 4.0)) ? -pow(b / 2.0 + c, 1.0 / 3.0)
+                                                                        : -aa / (3.0 * pow(fabs(b), 1.0 / 3.0));
+                const double tp = rootA + rootB;
+                e = l.linear ? 1.0 / (2.0 * fl[k]) : 1.0 / (2.0 * fl[k] * (tp * tp + tau_perp * tau_perp));
+            }
+            if (own) ecell[k] = ecell[k] + e;
+            vavg = vavg + e * (a.sigma[k + 1] - a.sigma[k]);
+        }
+        double h_qp = 0.0;
+#pragma unroll
+        for (int n = 0; n < 4; ++n) h_qp = h_qp + phi[n] * h[n];
+        const double f = h_qp * vavg * 1.0 * detJ / kAsmVol0;
+        const double zero = 0.0 * 0.0;  // dphi_dz(nr)*dphi_dz(nc) of the Blatter-Pattyn form, dphi_dz = 0
+#pragma unroll
+        for (int nc = 0; nc < 4; ++nc) {
+            Kuu[nc] = Kuu[nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc] + zero);
+            Kuv[nc] = Kuv[nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
+            Kvu[nc] = Kvu[nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
+            Kvv[nc] = Kvv[nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc] + zero);
+        }
+    }
+    if (own)
+        for (int k = 0; k < nl; ++k) ecell[k] = ecell[k] / 4;
+#pragma unroll
+    for (int nc = 0; nc < 4; ++nc) {
+        const int m = (c_ish3[nc] - c_ish3[nr] + 1) + 3 * (c_jsh3[nc] - c_jsh3[nr] + 1);
+        acc[0][m] = acc[0][m] + Kuu[nc];
+        acc[1][m] = acc[1][m] + Kuv[nc];
+        acc[2][m] = acc[2][m] + Kvu[nc];
+        acc[3][m] = acc[3][m] + Kvv[nc];
+    }
+}
+
+__global__ void __launch_bounds__(kAsmBlock) k_assemble2d_l1l2(AsmArgs a, L1l2Args l, SymIdx L, double *Auu,
+                                                               double *Auv, double *Avu, double *Avv) {
+    const long long NX = a.nx - 1, NQ = NX * (a.ny - 1);
+    const long long q = (long long)blockIdx.x * kAsmBlock + threadIdx.x;
+    if (q >= NQ) return;
+    const int j0 = (int)(q / NX), i0 = (int)(q - (long long)j0 * NX);
+    const int iR = i0 + 1, jR = j0 + 1;
+    double acc[4][9];
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) acc[b][c] = 0.0;
+    for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di) {
+            const int je = jR + dj, ie = iR + di;
+            if (ie < a.nhalo + 1 || ie > a.nx - a.nhalo + 1 || je < a.nhalo + 1 || je > a.ny - a.nhalo + 1) continue;
+            if (!a.active_cell[(ie - 1) + (long long)a.nx * (je - 1)]) continue;
+            const int nr = dj == 0 ? (di == 0 ? 2 : 3) : (di == 0 ? 1 : 0);
+            asm_cell_row_l1l2(a, l, ie, je, nr, dj == 0 && di == 0, acc);
+        }
+    double *B[4] = {Auu, Auv, Avu, Avv};
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+        for (int c = 0; c < 9; ++c) B[b][L.at(c, 0, q)] = acc[b][c];
+}
+
 }  // namespace cismgpu

@@ -375,20 +375,22 @@ struct Solver {
                  int nhalo, const double *sigma, const int32_t *active_cell, const double *xv, const double *yv,
                  const double *u, const double *v, int vel_id, const double *usrf, const double *thck,
                  const double *flwafact, int whichapprox, int whichefvs, double efvs_constant,
-                 double effstrain_min, double n_glen, double *efvs) {
+                 double effstrain_min, double n_glen, double *efvs, const double *dsdx = nullptr,
+                 const double *dsdy = nullptr, const double *flwa = nullptr) {
+        // 2D with dsdx given: the L1L2 branch (dsdx, dsdy at the vertices, flwa per layer)
         TRY(asm_ref_ready());
         const int nx = g.NX + 1, ny = g.NY + 1;
         const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny, nel = (size_t)(nzl - 1) * ncell;
         const size_t nvel = three_d ? (size_t)nzl * nq : nq;
-        const bool host_vel = u != nullptr;
-        // doubles: sigma, 4 vertex fields, flwafact, efvs, the 2D averaged flow factor, [u, v];
-        // then active_cell and the flag
-        const size_t nd = (size_t)nzl + 4 * nq + 2 * nel + ncell + (host_vel ? 2 * nvel : 0);
+        const bool host_vel = u != nullptr, l1l2 = !three_d && dsdx != nullptr;
+        // doubles: sigma, 4 vertex fields, flwafact, efvs, the 2D averaged flow factor, [u, v],
+        // [dsdx, dsdy, flwa]; then active_cell and the flag
+        const size_t nd = (size_t)nzl + 4 * nq + 2 * nel + ncell + (host_vel ? 2 * nvel : 0) + (l1l2 ? 2 * nq + nel : 0);
         CU(asm_in.ensure(nd * sizeof(double) + ncell * sizeof(int32_t) + 16));
         double *D = asm_in.as<double>();
         double *d_sigma = D, *d_xv = D + nzl, *d_yv = d_xv + nq, *d_usrf = d_yv + nq, *d_thck = d_usrf + nq;
         double *d_ff = d_thck + nq, *d_efvs = d_ff + nel, *d_ff2 = d_efvs + nel, *d_u = d_ff2 + ncell,
-               *d_v = d_u + nvel;
+               *d_v = d_u + nvel, *d_sx = d_u + (host_vel ? 2 * nvel : 0), *d_sy = d_sx + nq, *d_fl = d_sy + nq;
         int32_t *d_act = reinterpret_cast<int32_t *>(D + nd);
         int *d_sing = reinterpret_cast<int *>(d_act + ncell);
         cudaStream_t s = stream;
@@ -405,6 +407,11 @@ struct Solver {
         if (host_vel) {
             CU(up(d_u, u, nvel * sizeof(double)));
             CU(up(d_v, v, nvel * sizeof(double)));
+        }
+        if (l1l2) {
+            CU(up(d_sx, dsdx, nq * sizeof(double)));
+            CU(up(d_sy, dsdy, nq * sizeof(double)));
+            CU(up(d_fl, flwa, nel * sizeof(double)));
         }
         CU(cudaMemsetAsync(d_efvs, 0, nel * sizeof(double), s));
         CU(cudaMemsetAsync(d_sing, 0, sizeof(int), s));
@@ -424,6 +431,12 @@ struct Solver {
         if (three_d) {
             const long long n = (long long)nzl * g.NQ;
             k_assemble3d<<<(unsigned)((n + kAsmBlock - 1) / kAsmBlock), kAsmBlock, 0, s>>>(a, L, Auu, Auv, Avu, Avv);
+        } else if (l1l2) {
+            L1l2Args l;
+            l.dsdx = d_sx; l.dsdy = d_sy; l.flwa = d_fl;
+            l.linear = std::fabs(n_glen - 1.0) < 1.0e-10;
+            k_assemble2d_l1l2<<<(unsigned)((g.NQ + kAsmBlock - 1) / kAsmBlock), kAsmBlock, 0, s>>>(a, l, L, Auu, Auv,
+                                                                                                   Avu, Avv);
         } else {
             k_asm_vertavg<<<(unsigned)((ncell + kBlock - 1) / kBlock), kBlock, 0, s>>>((int)ncell, nzl, d_sigma, d_ff,
                                                                                        d_ff2);
@@ -1609,7 +1622,9 @@ static int oneshot_assemble(bool three_d, int nx, int ny, int nz, int nhalo, con
                             const int32_t *active_cell, const double *xv, const double *yv, const double *u,
                             const double *v, const double *usrf, const double *thck, const double *ff,
                             int whichapprox, int whichefvs, double efvs_constant, double effstrain_min,
-                            double n_glen, const int32_t *indx, double *efvs, double *const blocks[4]) {
+                            double n_glen, const int32_t *indx, double *efvs, double *const blocks[4],
+                            const double *dsdx = nullptr, const double *dsdy = nullptr,
+                            const double *flwa = nullptr) {
     std::lock_guard<std::mutex> lk(g_mu);
     g_last_error.clear();
     TRY(validate_assembly(nx, ny, nz, nhalo, whichefvs, n_glen, sigma, active_cell, xv, yv, three_d ? usrf : thck,
@@ -1635,8 +1650,12 @@ static int oneshot_assemble(bool three_d, int nx, int ny, int nz, int nhalo, con
     L.NQ = sv.g.NQ;
     L.nz = sv.g.nz;
     L.raw3 = three_d ? 1 : 0;
+    if (dsdx && (!dsdy || !flwa)) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (dsdx && whichefvs == 2 && std::fabs(n_glen - 1.0) >= 1.0e-10 && std::fabs(n_glen - 3.0) >= 1.0e-10)
+        return fail(CISMGPU_EINVAL, "Invalid value of n_glen for L1L2 solver (1 or 3)");
     TRY(sv.assemble(three_d, nz, L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, nhalo, sigma, active_cell, xv, yv, u, v,
-                    0, usrf, thck, ff, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen, efvs));
+                    0, usrf, thck, ff, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen, efvs, dsdx, dsdy,
+                    flwa));
     for (int k = 0; k < 4; ++k)
         CU(cudaMemcpyAsync(blocks[k], A0 + k * bs, bs * sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
     CU(cudaStreamSynchronize(sv.stream));
@@ -2360,6 +2379,23 @@ static int oneshot_assemble_diva(int nx, int ny, int nz, int nhalo, const double
     CU(cudaMemcpyAsync(efvs_qp_3d, en, neq * sizeof(double), cudaMemcpyDeviceToHost, s));
     CU(cudaStreamSynchronize(s));
     return CISMGPU_OK;
+}
+
+int cismgpu_assemble_stiffness_matrix_2d_l1l2(int nx, int ny, int nz, int nhalo, const double *sigma,
+                                              const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                              const double *uvel_2d, const double *vvel_2d, const double *stagthck,
+                                              const double *dusrf_dx, const double *dusrf_dy, const double *flwa,
+                                              const double *flwafact, int whichefvs, double efvs_constant,
+                                              double effstrain_min, double n_glen, const int32_t *indxA_2d,
+                                              double *efvs, double *Auu, double *Auv, double *Avu, double *Avv) {
+    if (!dusrf_dx) {
+        g_last_error.clear();
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    }
+    double *const blocks[4] = {Auu, Auv, Avu, Avv};
+    return oneshot_assemble(false, nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel_2d, vvel_2d, nullptr,
+                            stagthck, flwafact, 3, whichefvs, efvs_constant, effstrain_min, n_glen, indxA_2d, efvs,
+                            blocks, dusrf_dx, dusrf_dy, flwa);
 }
 
 // The handle's assembly: blocks into the resident canonical planes.

@@ -232,6 +232,19 @@
          real(c_double), intent(out) :: efvs(*), Auu(*), Auv(*), Avu(*), Avv(*)
        end function c_assemble_2d_diva
 
+       integer(c_int) function c_assemble_2d_l1l2(nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, &
+            uvel_2d, vvel_2d, stagthck, dusrf_dx, dusrf_dy, flwa, flwafact, whichefvs, efvs_constant, &
+            effstrain_min, n_glen, indxA_2d, efvs, Auu, Auv, Avu, Avv) &
+            bind(C, name="cismgpu_assemble_stiffness_matrix_2d_l1l2")
+         import :: c_int, c_double, c_int32_t
+         integer(c_int), value :: nx, ny, nz, nhalo, whichefvs
+         real(c_double), intent(in) :: sigma(*), xVertex(*), yVertex(*), uvel_2d(*), vvel_2d(*), stagthck(*), &
+              dusrf_dx(*), dusrf_dy(*), flwa(*), flwafact(*)
+         integer(c_int32_t), intent(in) :: active_cell(*), indxA_2d(*)
+         real(c_double), value :: efvs_constant, effstrain_min, n_glen
+         real(c_double), intent(out) :: efvs(*), Auu(*), Auv(*), Avu(*), Avv(*)
+       end function c_assemble_2d_l1l2
+
        integer(c_int) function c_dirichlet_3d(nx, ny, nz, nhalo, active_vertex, umask, vmask, uvel, vvel, &
             indxA_3d, Auu, Auv, Avu, Avv, bu, bv) bind(C, name="cismgpu_dirichlet_boundary_conditions_3d")
          import :: c_int, c_double, c_int32_t
@@ -540,9 +553,8 @@
     end subroutine check_symmetry_assembled_matrix_2d
 
     !-----------------------------------------------------------------------
-    ! The reference's argument lists (the diagnostic indices, and in 2D the arguments of the
-    ! L1L2 branch, are accepted and unused); n_glen is glimmer_physcon's.  The 2D form runs
-    ! the SSA and DIVA branches; L1L2 is reported with GM_FATAL.
+    ! The reference's argument lists (the diagnostic indices are accepted and unused); n_glen
+    ! is glimmer_physcon's.  The 2D form runs the SSA, L1L2 and DIVA branches.
     subroutine assemble_stiffness_matrix_3d(nx, ny, nz, sigma, nhalo, itest, jtest, rtest, active_cell, &
                                             xVertex, yVertex, uvel, vvel, stagusrf, stagthck, flwafact, &
                                             whichapprox, whichefvs, efvs, efvs_constant, effstrain_min, &
@@ -573,7 +585,7 @@
                                             whichefvs, efvs, efvs_constant, effstrain_min, Auu, Auv, Avu, Avv, &
                                             dusrf_dx, dusrf_dy, thck, btractx, btracty, omega_k, omega, efvs_qp_3d)
       use glimmer_physcon, only: n_glen
-      use glide_types, only: HO_APPROX_SSA, HO_APPROX_DIVA
+      use glide_types, only: HO_APPROX_SSA, HO_APPROX_DIVA, HO_APPROX_L1L2
       integer, intent(in) :: nx, ny, nz, nhalo, itest, jtest, rtest, whichapprox, whichefvs
       real(dp), dimension(nz), intent(in) :: sigma
       real(dp), dimension(nz-1), intent(in) :: stagsigma
@@ -607,8 +619,15 @@
          call check(c_assemble_2d(nx, ny, nz, nhalo, sigma, act, xVertex, yVertex, uvel_2d, vvel_2d, stagthck, &
                                   flwafact, whichefvs, efvs_constant, effstrain_min, n_glen, indx2, efvs, &
                                   Auu, Auv, Avu, Avv))
+      elseif (whichapprox == HO_APPROX_L1L2) then
+         if (.not. (present(dusrf_dx) .and. present(dusrf_dy))) then
+            call write_log('GPU L1L2 assembly: dusrf_dx and dusrf_dy are needed', GM_FATAL)
+         endif
+         call check(c_assemble_2d_l1l2(nx, ny, nz, nhalo, sigma, act, xVertex, yVertex, uvel_2d, vvel_2d, &
+                                       stagthck, dusrf_dx, dusrf_dy, flwa, flwafact, whichefvs, efvs_constant, &
+                                       effstrain_min, n_glen, indx2, efvs, Auu, Auv, Avu, Avv))
       else
-         call write_log('GPU 2D assembly: the L1L2 branch is not built', GM_FATAL)
+         call write_log('GPU 2D assembly: whichapprox must be SSA, L1L2 or DIVA', GM_FATAL)
       endif
     end subroutine assemble_stiffness_matrix_2d
 

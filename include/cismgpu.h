@@ -352,6 +352,20 @@ int cismgpu_basal_sliding_bc_2d_diva(int nx, int ny, int nhalo, double dx, doubl
                                      const double *lsrf, const double *xVertex, const double *yVertex,
                                      int whichassemble_beta, const int32_t *indxA_2d, double *Auu, double *Avv);
 
+/* assemble_stiffness_matrix_2d (glissade_velo_higher.F90:4961-5378) with whichapprox =
+ * HO_APPROX_L1L2: per Gauss point and layer the viscosity of compute_effective_viscosity_L1L2
+ * (:7474-7726; the cubic for the parallel stress from the surface gradient dusrf_dx/_dy
+ * (nx-1,ny-1) and flwa (nz-1,nx,ny)), its sigma-weighted average times the thickness in the
+ * element matrix, efvs the mean over the points.  n_glen must be 1 or 3 for the nonlinear
+ * viscosity (the reference's GM_FATAL otherwise: CISMGPU_EINVAL).  pow is CUDA's. */
+int cismgpu_assemble_stiffness_matrix_2d_l1l2(int nx, int ny, int nz, int nhalo, const double *sigma,
+                                              const int32_t *active_cell, const double *xVertex, const double *yVertex,
+                                              const double *uvel_2d, const double *vvel_2d, const double *stagthck,
+                                              const double *dusrf_dx, const double *dusrf_dy, const double *flwa,
+                                              const double *flwafact, int whichefvs, double efvs_constant,
+                                              double effstrain_min, double n_glen, const int32_t *indxA_2d,
+                                              double *efvs, double *Auu, double *Auv, double *Avu, double *Avv);
+
 /* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps

@@ -548,3 +548,36 @@ def test_diva_system_on_handle(gpu_lib):
     np.testing.assert_array_equal(ru, want[0])
     np.testing.assert_array_equal(rv, want[1])
     assert l2 == want[2]
+
+
+# ---------------------------------------------------------------------------
+# assemble_stiffness_matrix_2d, L1L2 branch
+# ---------------------------------------------------------------------------
+
+@pytest.mark.parametrize("n_glen", [3.0, 1.0])
+def test_l1l2(gpu_lib, n_glen):
+    """n = 1 bit-exact (no pow); n = 3 within the pow bar: efvs 1e-14, blocks 1e-13."""
+    g = geometry(seed=93, nz=5)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(3)
+    u, v = 30 * rng.standard_normal((ny - 1, nx - 1)), 30 * rng.standard_normal((ny - 1, nx - 1))
+    dsdx, dsdy = 0.01 * rng.standard_normal((ny - 1, nx - 1)), 0.01 * rng.standard_normal((ny - 1, nx - 1))
+    flwa = 1e-16 * (1 + rng.random((ny, nx, nz - 1)))
+    ff = 0.5 * flwa ** (-1 / 3)
+    st, eo, *Ao = oracle.assemble_stiffness_2d_l1l2(nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], u, v,
+                                                     g["stagthck"], dsdx, dsdy, flwa, ff, n_glen=n_glen)
+    assert st == 0
+    e, *Ad = cg.assemble_stiffness_matrix_2d_l1l2(nx, ny, nz, 2, g["sigma"], g["ac"].astype(np.int32), g["xVertex"],
+                                                  g["yVertex"], u, v, g["stagthck"], dsdx, dsdy, flwa, ff,
+                                                  n_glen=n_glen)
+    if n_glen == 1.0:
+        np.testing.assert_array_equal(e, eo)
+        for a, b in zip(Ad, Ao):
+            np.testing.assert_array_equal(a, b)
+    else:
+        assert np.abs(e - eo).max() <= 1e-14 * np.abs(eo).max()
+        for a, b in zip(Ad, Ao):
+            assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
+    with pytest.raises(cg.CismGpuError):
+        cg.assemble_stiffness_matrix_2d_l1l2(nx, ny, nz, 2, g["sigma"], g["ac"].astype(np.int32), g["xVertex"],
+                                             g["yVertex"], u, v, g["stagthck"], dsdx, dsdy, flwa, ff, n_glen=2.0)
