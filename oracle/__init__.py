@@ -84,6 +84,7 @@ def lib() -> ctypes.CDLL:
         L.oracle_basal_diva.argtypes = [i, i, i, dbl, dbl, d, d, d, d, d, d, d, i, d, d]
         L.oracle_basal_diva.restype = None
         L.oracle_assemble_stiffness_2d_l1l2.argtypes = [i, i, i, i] + [d] * 11 + [i, dbl, dbl, dbl] + [d] * 5
+        L.oracle_load_vector_gravity.argtypes = [i, i, i, i, d, d, dbl, dbl, d, d, d, d, d, d, d, d, i, d, d]
         L.oracle_check_symmetry.argtypes = [i, i, i, i, P(_Par), d, d, d, d, d, d, P(dbl), P(ctypes.c_long)]
         L.oracle_reprosum.restype = dbl
         L.oracle_exact_sum.restype = dbl
@@ -355,6 +356,20 @@ def assemble_stiffness_2d_l1l2(nx, ny, nz, sigma, active_cell, xVertex, yVertex,
     st = lib().oracle_assemble_stiffness_2d_l1l2(nx, ny, nz, nhalo, *[_p(a) for a in ins], whichefvs, efvs_constant,
                                                  effstrain_min, n_glen, _p(efvs), *[_p(a) for a in A])
     return (st, efvs, *A)
+
+
+def load_vector_gravity(nx, ny, nz, sigma, stagwbndsigma, dx, dy, active_cell, active_vertex, xVertex, yVertex,
+                        stagusrf, stagthck, dusrf_dx, dusrf_dy, whichassemble_taud, nhalo=2):
+    """load_vector_gravity (glissade_velo_higher.F90:4228-4449) from zero: vertex fields
+    (ny-1, nx-1), stagwbndsigma (nz+1).  Returns (status, loadu, loadv (ny-1, nx-1, nz))."""
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    lu, lv = np.zeros((ny - 1, nx - 1, nz)), np.zeros((ny - 1, nx - 1, nz))
+    st = lib().oracle_load_vector_gravity(nx, ny, nz, nhalo, _p(f64(sigma)), _p(f64(stagwbndsigma)), float(dx),
+                                          float(dy), _p(i32(active_cell)), _p(i32(active_vertex)), _p(f64(xVertex)),
+                                          _p(f64(yVertex)), _p(f64(stagusrf)), _p(f64(stagthck)), _p(f64(dusrf_dx)),
+                                          _p(f64(dusrf_dy)), int(whichassemble_taud), _p(lu), _p(lv))
+    return st, lu, lv
 
 
 def reprosum(a) -> float:

@@ -1062,3 +1062,87 @@ int oracle_assemble_stiffness_2d_l1l2(int nx, int ny, int nz, int nhalo, const d
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// load_vector_gravity (:4228-4449)
+// ---------------------------------------------------------------------------
+extern "C" {
+
+// Local form (whichassemble_taud = 1): at every active vertex and level k,
+// load -= rhoi*grav*dx*dy*dz/vol0 * dusrf_dx with dz = stagthck*(stagwbndsigma(k) -
+// stagwbndsigma(k-1)).  Standard form (0): per active cell and element, 8-point quadrature of
+// rhoi*grav*w*detJ/vol0 * (ds/dx at the point) * phi_n into each node.  loadu/loadv
+// (nz,nx-1,ny-1) are added to (the reference's caller zeroes them); stagwbndsigma (0:nz).
+// Returns 0, 1 (singular Jacobian) or 2 (nhalo < 2).
+int oracle_load_vector_gravity(int nx, int ny, int nz, int nhalo, const double *sigma, const double *stagwbndsigma,
+                               double dx, double dy, const int32_t *active_cell, const int32_t *active_vertex,
+                               const double *xVertex, const double *yVertex, const double *stagusrf,
+                               const double *stagthck, const double *dusrf_dx, const double *dusrf_dy,
+                               int whichassemble_taud, double *loadu, double *loadv) {
+    const long NX = nx - 1;
+    auto V = [&](int k, int i, int j) { return (long)(k - 1) + (long)nz * ((i - 1) + NX * (j - 1)); };
+    if (whichassemble_taud == 1) {
+        for (int j = 1; j <= ny - 1; ++j)
+            for (int i = 1; i <= nx - 1; ++i) {
+                const long q = (i - 1) + NX * (j - 1);
+                if (!active_vertex[q]) continue;
+                for (int k = 1; k <= nz; ++k) {
+                    const double dz = stagthck[q] * (stagwbndsigma[k] - stagwbndsigma[k - 1]);
+                    loadu[V(k, i, j)] = loadu[V(k, i, j)] - kRhoi * kGrav * dx * dy * dz / kVol0 * dusrf_dx[q];
+                    loadv[V(k, i, j)] = loadv[V(k, i, j)] - kRhoi * kGrav * dx * dy * dz / kVol0 * dusrf_dy[q];
+                }
+            }
+        return 0;
+    }
+    if (nhalo < 2) return 2;
+    const RefElement &R = ref();
+    double phi[8][8];  // phi_3d(n,p) at the Gauss points, :354-361
+    {
+        const double r = 1.0 / std::sqrt(3.0);
+        const double xq[8] = {-r, r, r, -r, -r, r, r, -r}, yq[8] = {-r, -r, r, r, -r, -r, r, r},
+                     zq[8] = {-r, -r, -r, -r, r, r, r, r};
+        for (int p = 0; p < 8; ++p) {
+            const double x = xq[p], y = yq[p], z = zq[p];
+            phi[p][0] = (1.0 - x) * (1.0 - y) * (1.0 - z) / 8.0;
+            phi[p][1] = (1.0 + x) * (1.0 - y) * (1.0 - z) / 8.0;
+            phi[p][2] = (1.0 + x) * (1.0 + y) * (1.0 - z) / 8.0;
+            phi[p][3] = (1.0 - x) * (1.0 + y) * (1.0 - z) / 8.0;
+            phi[p][4] = (1.0 - x) * (1.0 - y) * (1.0 + z) / 8.0;
+            phi[p][5] = (1.0 + x) * (1.0 - y) * (1.0 + z) / 8.0;
+            phi[p][6] = (1.0 + x) * (1.0 + y) * (1.0 + z) / 8.0;
+            phi[p][7] = (1.0 - x) * (1.0 + y) * (1.0 + z) / 8.0;
+        }
+    }
+    for (int j = nhalo + 1; j <= ny - nhalo + 1; ++j)
+        for (int i = nhalo + 1; i <= nx - nhalo + 1; ++i) {
+            if (!active_cell[(i - 1) + (long)nx * (j - 1)]) continue;
+            for (int k = 1; k <= nz - 1; ++k) {
+                double x[8], y[8], z[8], sx[8], sy[8];
+                for (int n = 0; n < 8; ++n) {
+                    const long q = (long)(i + kIsh7[n] - 1) + NX * (j + kJsh7[n] - 1);
+                    x[n] = xVertex[q];
+                    y[n] = yVertex[q];
+                    z[n] = stagusrf[q] - sigma[k + kKsh7[n] - 1] * stagthck[q];
+                    sx[n] = dusrf_dx[q];
+                    sy[n] = dusrf_dy[q];
+                }
+                for (int p = 0; p < 8; ++p) {
+                    double ddx[8], ddy[8], ddz[8], detJ;
+                    if (!basis_derivs_3d(x, y, z, R.dxr[p], R.dyr[p], R.dzr[p], ddx, ddy, ddz, &detJ)) return 1;
+                    double sxq = 0.0, syq = 0.0;
+                    for (int n = 0; n < 8; ++n) {
+                        sxq = sxq + phi[p][n] * sx[n];
+                        syq = syq + phi[p][n] * sy[n];
+                    }
+                    for (int n = 0; n < 8; ++n) {
+                        const long e = V(k + kKsh7[n], i + kIsh7[n], j + kJsh7[n]);
+                        loadu[e] = loadu[e] - kRhoi * kGrav * R.wqp[p] * detJ / kVol0 * sxq * phi[p][n];
+                        loadv[e] = loadv[e] - kRhoi * kGrav * R.wqp[p] * detJ / kVol0 * syq * phi[p][n];
+                    }
+                }
+            }
+        }
+    return 0;
+}
+
+}  // extern "C"

@@ -267,3 +267,53 @@ def test_basal_diva_standard_integrates_over_the_bed():
     area = dx * dx * np.sqrt(1 + a * a + b * b) / 1.0e9 * ncell
     assert abs(Auu.sum() - 200.0 * area) <= 1e-12 * 200.0 * area
     assert abs(Avv.sum() - 300.0 * area) <= 1e-12 * 300.0 * area
+
+
+# ---------------------------------------------------------------------------
+# load_vector_gravity (:4228-4449)
+# ---------------------------------------------------------------------------
+
+def load_geometry(H0=900.0, a=-0.01, b=0.004, nz=5, seed=60):
+    g = geometry(seed=seed, nz=nz)
+    nx, ny, dx = g["nx"], g["ny"], g["dx"]
+    ice = g["thck"] > 0.0
+    thck = np.where(ice, H0, 0.0)
+    xc = (np.arange(nx) - 0.5) * dx
+    yc = (np.arange(ny) - 0.5) * dx
+    usrf = 2000.0 + a * xc[None, :] + b * yc[:, None]
+    ac, av = asm.active_masks(thck)
+    sig = g["sigma"]
+    stagw = np.concatenate([[0.0], 0.5 * (sig[:-1] + sig[1:]), [1.0]])
+    return dict(g, thck=thck, ac=ac, av=av, stagusrf=asm.stagger(usrf, thck > 1.0),
+                stagthck=asm.stagger(thck, thck > 1.0), stagw=stagw, H0=H0, a=a, b=b)
+
+
+def test_load_local_is_the_column_formula():
+    g = load_geometry()
+    nx, ny, nz, dx = g["nx"], g["ny"], g["nz"], g["dx"]
+    rng = np.random.default_rng(5)
+    sx, sy = 0.01 * rng.standard_normal((ny - 1, nx - 1)), 0.01 * rng.standard_normal((ny - 1, nx - 1))
+    st, lu, lv = oracle.load_vector_gravity(nx, ny, nz, g["sigma"], g["stagw"], dx, dx, g["ac"], g["av"], g["xVertex"],
+                                            g["yVertex"], g["stagusrf"], g["stagthck"], sx, sy, 1)
+    assert st == 0
+    dz = g["stagthck"][..., None] * np.diff(g["stagw"])[None, None, :]
+    av = g["av"].astype(bool)[..., None]
+    np.testing.assert_array_equal(lu, np.where(av, 0.0 - 910.0 * 9.81 * dx * dx * dz / 1.0e9 * sx[..., None], 0.0))
+    np.testing.assert_array_equal(lv, np.where(av, 0.0 - 910.0 * 9.81 * dx * dx * dz / 1.0e9 * sy[..., None], 0.0))
+
+
+def test_load_standard_integrates_the_driving_stress():
+    """Constant thickness H0 and a constant surface gradient: summed over all nodes, the
+    standard load is -rhoi*g*(ds/dx)*(ice volume)/vol0, the volume being dx*dy*H0 per active cell
+    (the 2x2x2 Gauss rule integrates the trilinear Jacobian exactly)."""
+    g = load_geometry()
+    nx, ny, nz, dx = g["nx"], g["ny"], g["nz"], g["dx"]
+    sx, sy = np.full((ny - 1, nx - 1), g["a"]), np.full((ny - 1, nx - 1), g["b"])
+    st, lu, lv = oracle.load_vector_gravity(nx, ny, nz, g["sigma"], g["stagw"], dx, dx, g["ac"], g["av"], g["xVertex"],
+                                            g["yVertex"], g["stagusrf"], g["stagthck"], sx, sy, 0)
+    assert st == 0
+    ncell = int(np.count_nonzero(g["ac"][2:ny - 1, 2:nx - 1]))
+    vol = ncell * dx * dx * g["H0"]
+    for load, s in ((lu, g["a"]), (lv, g["b"])):
+        want = -910.0 * 9.81 * s * vol / 1.0e9
+        assert abs(load.sum() - want) <= 1e-11 * abs(want)
