@@ -32,7 +32,7 @@ __all__ = [
     "check_symmetry_assembled_matrix_3d", "check_symmetry_assembled_matrix_2d", "assemble_stiffness_matrix_3d",
     "assemble_stiffness_matrix_2d", "dirichlet_boundary_conditions_3d", "basal_sliding_bc_3d",
     "dirichlet_boundary_conditions_2d", "basal_sliding_bc_2d", "assemble_stiffness_matrix_2d_diva",
-    "basal_sliding_bc_2d_diva", "assemble_stiffness_matrix_2d_l1l2",
+    "basal_sliding_bc_2d_diva", "assemble_stiffness_matrix_2d_l1l2", "load_vector_gravity",
 ]
 
 ALG_STANDARD, ALG_CHRONGEAR, ALG_MIXED_CHRONGEAR = 0, 1, 2
@@ -198,6 +198,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         [d] * 9
     lib.cismgpu_solver_assemble_stiffness_2d_diva.argtypes = [vp, i32, i32] + [d] * 14 + [i32, dbl, dbl, dbl] + [d] * 4
     lib.cismgpu_basal_sliding_bc_2d_diva.argtypes = [i32, i32, i32, dbl, dbl, d, d, d, d, d, d, d, i32, d, d, d]
+    lib.cismgpu_load_vector_gravity.argtypes = [i32, i32, i32, i32, d, d, dbl, dbl, d, d, d, d, d, d, d, d, i32, d, d]
     lib.cismgpu_assemble_stiffness_matrix_2d_l1l2.argtypes = [i32, i32, i32, i32] + [d] * 11 + \
         [i32, dbl, dbl, dbl] + [d] * 6
     lib.cismgpu_solver_assemble_system_2d_diva.argtypes = [vp, i32, i32, dbl, dbl] + [d] * 13 + \
@@ -218,7 +219,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
               "cismgpu_basal_sliding_bc_2d", "cismgpu_solver_assemble_system_2d",
               "cismgpu_assemble_stiffness_matrix_2d_diva", "cismgpu_solver_assemble_stiffness_2d_diva",
               "cismgpu_basal_sliding_bc_2d_diva", "cismgpu_solver_assemble_system_2d_diva",
-              "cismgpu_assemble_stiffness_matrix_2d_l1l2"):
+              "cismgpu_assemble_stiffness_matrix_2d_l1l2", "cismgpu_load_vector_gravity"):
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
@@ -592,6 +593,24 @@ def assemble_stiffness_matrix_2d_l1l2(nx, ny, nz, nhalo, sigma, active_cell, xVe
         float(efvs_constant), float(effstrain_min), float(n_glen), _ptr(indx, np.int32, 9),
         _ptr(efvs, np.float64, efvs.size, True), *[_ptr(a, np.float64, a.size, True) for a in A]))
     return (efvs, *A)
+
+
+def load_vector_gravity(nx, ny, nz, nhalo, sigma, stagwbndsigma, dx, dy, active_cell, active_vertex, xVertex,
+                        yVertex, stagusrf, stagthck, dusrf_dx, dusrf_dy, whichassemble_taud=1):
+    """Mirrors load_vector_gravity (glissade_velo_higher.F90:4228-4449) on the GPU from zero loads;
+    returns (loadu, loadv) of shape (ny-1, nx-1, nz)."""
+    lib = load_library()
+    nv = (nx - 1) * (ny - 1)
+    lu, lv = np.zeros((ny - 1, nx - 1, nz)), np.zeros((ny - 1, nx - 1, nz))
+    f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)
+    i32 = lambda a: np.ascontiguousarray(a, dtype=np.int32)
+    _check(lib, lib.cismgpu_load_vector_gravity(
+        nx, ny, nz, int(nhalo), _ptr(f64(sigma), np.float64, nz), _ptr(f64(stagwbndsigma), np.float64, nz + 1),
+        float(dx), float(dy), _ptr(i32(active_cell), np.int32, nx * ny), _ptr(i32(active_vertex), np.int32, nv),
+        _ptr(xVertex, np.float64, nv), _ptr(yVertex, np.float64, nv), _ptr(stagusrf, np.float64, nv),
+        _ptr(stagthck, np.float64, nv), _ptr(dusrf_dx, np.float64, nv), _ptr(dusrf_dy, np.float64, nv),
+        int(whichassemble_taud), _ptr(lu, np.float64, lu.size, True), _ptr(lv, np.float64, lv.size, True)))
+    return lu, lv
 
 
 def basal_sliding_bc_2d_diva(nx, ny, nhalo, dx, dy, active_cell, active_vertex, beta_eff_x, beta_eff_y, lsrf,

@@ -25,6 +25,7 @@ constexpr int kAsmBlock = 128;
 struct AsmRef {
     double wqp[8];
     double dxr[8][8], dyr[8][8], dzr[8][8];  // [p][n]
+    double phi[8][8];                        // phi_3d(n,p) at [p][n] (:354-361)
 };
 __constant__ AsmRef c_asm_ref;
 
@@ -1061,6 +1062,106 @@ __global__ void __launch_bounds__(kAsmBlock) k_assemble2d_l1l2(AsmArgs a, L1l2Ar
 #pragma unroll
     for (int b = 0; b < 4; ++b)
         for (int c = 0; c < 9; ++c) B[b][L.at(c, 0, q)] = acc[b][c];
+}
+
+// ---------------------------------------------------------------------------
+// load_vector_gravity (:4228-4449)
+// ---------------------------------------------------------------------------
+// Local form (whichassemble_taud = 1, :4283-4304): one thread per vertex and level; at an active
+// vertex load -= rhoi*grav*dx*dy*dz/vol0 * ds/dx with dz = stagthck*(stagwbndsigma(k) -
+// stagwbndsigma(k-1)).  The loads are in the caller's (nz, nx-1, ny-1) layout or planes (W).
+__global__ void __launch_bounds__(kBlock) k_load_local(int nx, int ny, int nz, double dx, double dy, VecIdx W,
+                                                       const int32_t *__restrict__ active_vertex,
+                                                       const double *__restrict__ stagwbndsigma,
+                                                       const double *__restrict__ stagthck,
+                                                       const double *__restrict__ dsdx,
+                                                       const double *__restrict__ dsdy, double *loadu, double *loadv) {
+    const long long NQ = (long long)(nx - 1) * (ny - 1);
+    const long long t = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (t >= (long long)nz * NQ) return;
+    const int k = (int)(t / NQ);
+    const long long q = t - (long long)k * NQ;
+    if (!active_vertex[q]) return;
+    const double dz = stagthck[q] * (stagwbndsigma[k + 1] - stagwbndsigma[k]);
+    const long long e = W.at(k, q);
+    loadu[e] = loadu[e] - 910.0 * 9.81 * dx * dy * dz / kAsmVol0 * dsdx[q];
+    loadv[e] = loadv[e] - 910.0 * 9.81 * dx * dy * dz / kAsmVol0 * dsdy[q];
+}
+
+// Standard form (:4305-4447), one thread per node: the elements containing it in the reference's
+// element order (as k_assemble3d), each element's 8 Gauss points (detJ as
+// get_basis_function_derivatives_3d computes it, ds/dx at the point), and the node's share
+// rhoi*grav*w*detJ/vol0 * (ds/dx) * phi_n subtracted point by point.
+__global__ void __launch_bounds__(kAsmBlock) k_load_standard(AsmArgs a, VecIdx W, const double *__restrict__ dsdx,
+                                                             const double *__restrict__ dsdy, double *loadu,
+                                                             double *loadv) {
+    const long long NX = a.nx - 1, NQ = NX * (a.ny - 1);
+    const long long t = (long long)blockIdx.x * kAsmBlock + threadIdx.x;
+    if (t >= (long long)a.nz * NQ) return;
+    const int k0 = (int)(t / NQ);
+    const long long q = t - (long long)k0 * NQ;
+    const int j0 = (int)(q / NX), i0 = (int)(q - (long long)j0 * NX);
+    const int iR = i0 + 1, jR = j0 + 1, kR = k0 + 1;
+    const long long eP = W.at(k0, q);
+    double lu = loadu[eP], lv = loadv[eP];
+    bool any = false;
+    for (int dj = 0; dj < 2; ++dj)
+        for (int di = 0; di < 2; ++di)
+            for (int dk = 0; dk < 2; ++dk) {
+                const int je = jR + dj, ie = iR + di, ke = kR - 1 + dk;
+                if (ke < 1 || ke > a.nz - 1) continue;
+                if (ie < a.nhalo + 1 || ie > a.nx - a.nhalo + 1 || je < a.nhalo + 1 || je > a.ny - a.nhalo + 1)
+                    continue;
+                if (!a.active_cell[(ie - 1) + (long long)a.nx * (je - 1)]) continue;
+                any = true;
+                const int nr = (dk == 0 ? 0 : 4) + (dj == 0 ? (di == 0 ? 2 : 3) : (di == 0 ? 1 : 0));
+                double x[8], y[8], z[8], sx[8], sy[8];
+#pragma unroll
+                for (int n = 0; n < 8; ++n) {
+                    const int iN = ie + c_ish7[n], jN = je + c_jsh7[n], kN = ke + c_ksh7[n];
+                    const long long qn = (long long)(iN - 1) + NX * (jN - 1);
+                    x[n] = a.xv[qn];
+                    y[n] = a.yv[qn];
+                    z[n] = a.usrf[qn] - a.sigma[kN - 1] * a.thck[qn];
+                    sx[n] = dsdx[qn];
+                    sy[n] = dsdy[qn];
+                }
+                for (int p = 0; p < 8; ++p) {
+                    const double *dxr = c_asm_ref.dxr[p], *dyr = c_asm_ref.dyr[p], *dzr = c_asm_ref.dzr[p];
+                    double J00 = 0.0, J01 = 0.0, J02 = 0.0, J10 = 0.0, J11 = 0.0, J12 = 0.0, J20 = 0.0, J21 = 0.0,
+                           J22 = 0.0;
+#pragma unroll
+                    for (int n = 0; n < 8; ++n) {
+                        J00 = J00 + dxr[n] * x[n];
+                        J01 = J01 + dxr[n] * y[n];
+                        J02 = J02 + dxr[n] * z[n];
+                        J10 = J10 + dyr[n] * x[n];
+                        J11 = J11 + dyr[n] * y[n];
+                        J12 = J12 + dyr[n] * z[n];
+                        J20 = J20 + dzr[n] * x[n];
+                        J21 = J21 + dzr[n] * y[n];
+                        J22 = J22 + dzr[n] * z[n];
+                    }
+                    const double c00 = J11 * J22 - J12 * J21, c01 = -(J10 * J22 - J12 * J20),
+                                 c02 = J10 * J21 - J11 * J20;
+                    const double detJ = J00 * c00 + J01 * c01 + J02 * c02;
+                    if (!(fabs(detJ) > 0.0)) {
+                        atomicExch(a.singular, 1);
+                        continue;
+                    }
+                    double sxq = 0.0, syq = 0.0;
+#pragma unroll
+                    for (int n = 0; n < 8; ++n) {
+                        sxq = sxq + c_asm_ref.phi[p][n] * sx[n];
+                        syq = syq + c_asm_ref.phi[p][n] * sy[n];
+                    }
+                    lu = lu - 910.0 * 9.81 * c_asm_ref.wqp[p] * detJ / kAsmVol0 * sxq * c_asm_ref.phi[p][nr];
+                    lv = lv - 910.0 * 9.81 * c_asm_ref.wqp[p] * detJ / kAsmVol0 * syq * c_asm_ref.phi[p][nr];
+                }
+            }
+    if (!any) return;
+    loadu[eP] = lu;
+    loadv[eP] = lv;
 }
 
 }  // namespace cismgpu

@@ -125,6 +125,7 @@ static int asm_ref_ready() {
                 r.dxr[p][n] = sx[n] * fy * fz / 8.0;
                 r.dyr[p][n] = sy[n] * fx * fz / 8.0;
                 r.dzr[p][n] = sz[n] * fx * fy / 8.0;
+                r.phi[p][n] = fx * fy * fz / 8.0;
             }
         }
         for (int p = 0; p < 4; ++p)  // the square: points and nodes are the cube's first four
@@ -678,6 +679,58 @@ struct Solver {
         if (efvs) CU(cudaMemcpyAsync(efvs, d_efvs, nel * sizeof(double), cudaMemcpyDeviceToHost, s));
         if (omega_k) CU(cudaMemcpyAsync(omega_k, d_ok, (size_t)nzl * ncell * sizeof(double), cudaMemcpyDeviceToHost, s));
         if (omega) CU(cudaMemcpyAsync(omega, d_om, ncell * sizeof(double), cudaMemcpyDeviceToHost, s));
+        CU(cudaStreamSynchronize(s));
+        if (sing) return fail(CISMGPU_EINVAL, "Jacobian matrix is singular (an element of zero volume)");
+        return CISMGPU_OK;
+    }
+
+    // load_vector_gravity (glissade_velo_higher.F90:4228-4449) added into the device loads lu, lv
+    // (layout W).  Host inputs in the reference's layouts.  Leaves the stream synchronized.
+    int load_gravity(VecIdx W, double *lu, double *lv, int nhalo, const double *sigma, const double *stagwbndsigma,
+                     double dx, double dy, const int32_t *active_cell, const int32_t *active_vertex,
+                     const double *xv, const double *yv, const double *stagusrf, const double *stagthck,
+                     const double *dsdx, const double *dsdy, int whichassemble_taud) {
+        TRY(asm_ref_ready());
+        const int nx = g.NX + 1, ny = g.NY + 1, nz = g.nz;
+        const size_t nq = (size_t)g.NQ, ncell = (size_t)nx * ny;
+        // doubles: sigma, stagwbndsigma, xv, yv, stagusrf, stagthck, dsdx, dsdy; then int32:
+        // active_cell, active_vertex, the flag
+        const size_t nd = (size_t)2 * nz + 1 + 6 * nq;
+        CU(asm_in.ensure(nd * sizeof(double) + (ncell + nq + 1) * sizeof(int32_t)));
+        double *D = asm_in.as<double>();
+        double *d_sig = D, *d_sw = d_sig + nz, *d_xv = d_sw + nz + 1, *d_yv = d_xv + nq, *d_us = d_yv + nq,
+               *d_th = d_us + nq, *d_sx = d_th + nq, *d_sy = d_sx + nq;
+        int32_t *d_cell = reinterpret_cast<int32_t *>(D + nd), *d_av = d_cell + ncell, *d_sing = d_av + nq;
+        cudaStream_t s = stream;
+        auto up = [&](void *dst, const void *src, size_t bytes) {
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s);
+        };
+        CU(up(d_sw, stagwbndsigma, (nz + 1) * sizeof(double)));
+        CU(up(d_th, stagthck, nq * sizeof(double)));
+        CU(up(d_sx, dsdx, nq * sizeof(double)));
+        CU(up(d_sy, dsdy, nq * sizeof(double)));
+        CU(up(d_av, active_vertex, nq * sizeof(int32_t)));
+        CU(cudaMemsetAsync(d_sing, 0, sizeof(int32_t), s));
+        if (whichassemble_taud == 1) {
+            k_load_local<<<nblocks((long long)nz * g.NQ), kBlock, 0, s>>>(nx, ny, nz, dx, dy, W, d_av, d_sw, d_th, d_sx,
+                                                                          d_sy, lu, lv);
+        } else {
+            CU(up(d_sig, sigma, nz * sizeof(double)));
+            CU(up(d_xv, xv, nq * sizeof(double)));
+            CU(up(d_yv, yv, nq * sizeof(double)));
+            CU(up(d_us, stagusrf, nq * sizeof(double)));
+            CU(up(d_cell, active_cell, ncell * sizeof(int32_t)));
+            AsmArgs a{};
+            a.nx = nx; a.ny = ny; a.nz = nz; a.nhalo = nhalo;
+            a.sigma = d_sig; a.active_cell = d_cell; a.xv = d_xv; a.yv = d_yv; a.usrf = d_us; a.thck = d_th;
+            a.singular = d_sing;
+            const long long n = (long long)nz * g.NQ;
+            k_load_standard<<<(unsigned)((n + kAsmBlock - 1) / kAsmBlock), kAsmBlock, 0, s>>>(a, W, d_sx, d_sy, lu,
+                                                                                              lv);
+        }
+        CU(cudaGetLastError());
+        int sing = 0;
+        CU(cudaMemcpyAsync(&sing, d_sing, sizeof(int), cudaMemcpyDeviceToHost, s));
         CU(cudaStreamSynchronize(s));
         if (sing) return fail(CISMGPU_EINVAL, "Jacobian matrix is singular (an element of zero volume)");
         return CISMGPU_OK;
@@ -2396,6 +2449,42 @@ int cismgpu_assemble_stiffness_matrix_2d_l1l2(int nx, int ny, int nz, int nhalo,
     return oneshot_assemble(false, nx, ny, nz, nhalo, sigma, active_cell, xVertex, yVertex, uvel_2d, vvel_2d, nullptr,
                             stagthck, flwafact, 3, whichefvs, efvs_constant, effstrain_min, n_glen, indxA_2d, efvs,
                             blocks, dusrf_dx, dusrf_dy, flwa);
+}
+
+int cismgpu_load_vector_gravity(int nx, int ny, int nz, int nhalo, const double *sigma, const double *stagwbndsigma,
+                                double dx, double dy, const int32_t *active_cell, const int32_t *active_vertex,
+                                const double *xVertex, const double *yVertex, const double *stagusrf,
+                                const double *stagthck, const double *dusrf_dx, const double *dusrf_dy,
+                                int whichassemble_taud, double *loadu, double *loadv) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_last_error.clear();
+    if (!stagwbndsigma || !active_vertex || !stagthck || !dusrf_dx || !dusrf_dy || !loadu || !loadv)
+        return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (whichassemble_taud != 0 && whichassemble_taud != 1)
+        return fail(CISMGPU_EINVAL, "whichassemble_taud must be 0 (standard) or 1 (local)");
+    if (whichassemble_taud == 0)
+        TRY(validate_assembly(nx, ny, nz, nhalo, 2, 3.0, sigma, active_cell, xVertex, yVertex, stagusrf, stagthck,
+                              stagthck));
+    else if (nx < 6 || ny < 6 || nz < 1 || nz > kMaxNz)
+        return fail(CISMGPU_EINVAL, "grid too small or nz outside 1..64");
+    cismgpu_par_t par{};
+    par.staggered_ilo = 1; par.staggered_ihi = nx - 1; par.staggered_jlo = 1; par.staggered_jhi = ny - 1;
+    par.tasks_row = par.tasks_col = 1;
+    if (!g_oneshot) g_oneshot = new Solver();
+    Solver &sv = *g_oneshot;
+    TRY(sv.init(nullptr));
+    TRY(sv.set_geom(make_geom(nx, ny, nz, &par), true));
+    double *V = sv.vec.as<double>();  // the loads in the caller's layout, in the right-hand-side planes
+    double *lu = V + (size_t)VB_U * sv.nvec, *lv = V + (size_t)VB_V * sv.nvec;
+    cudaStream_t s = sv.stream;
+    CU(cudaMemcpyAsync(lu, loadu, sv.nvec * sizeof(double), cudaMemcpyHostToDevice, s));
+    CU(cudaMemcpyAsync(lv, loadv, sv.nvec * sizeof(double), cudaMemcpyHostToDevice, s));
+    TRY(sv.load_gravity(VecIdx{sv.g.NQ, nz, 0}, lu, lv, nhalo, sigma, stagwbndsigma, dx, dy, active_cell,
+                        active_vertex, xVertex, yVertex, stagusrf, stagthck, dusrf_dx, dusrf_dy, whichassemble_taud));
+    CU(cudaMemcpyAsync(loadu, lu, sv.nvec * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(loadv, lv, sv.nvec * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CU(cudaStreamSynchronize(s));
+    return CISMGPU_OK;
 }
 
 // The handle's assembly: blocks into the resident canonical planes.

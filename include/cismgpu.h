@@ -366,6 +366,18 @@ int cismgpu_assemble_stiffness_matrix_2d_l1l2(int nx, int ny, int nz, int nhalo,
                                               double effstrain_min, double n_glen, const int32_t *indxA_2d,
                                               double *efvs, double *Auu, double *Auv, double *Avu, double *Avv);
 
+/* Replaces load_vector_gravity (glissade_velo_higher.F90:4228-4449): the gravitational driving
+ * stress added into loadu, loadv (nz,nx-1,ny-1) (the reference's caller zeroes them first).
+ * whichassemble_taud = 1 (local, CISM's default): per active vertex and level
+ * -rhoi*grav*dx*dy*dz/vol0 * dusrf_dx with dz from stagwbndsigma (0:nz) and stagthck;
+ * 0 (standard): 8-point quadrature over the hexahedra of the active cells (nhalo >= 2).
+ * rhoi = 910, grav = 9.81 (glimmer_physcon.F90:67, :69).  Bit-exact. */
+int cismgpu_load_vector_gravity(int nx, int ny, int nz, int nhalo, const double *sigma, const double *stagwbndsigma,
+                                double dx, double dy, const int32_t *active_cell, const int32_t *active_vertex,
+                                const double *xVertex, const double *yVertex, const double *stagusrf,
+                                const double *stagthck, const double *dusrf_dx, const double *dusrf_dy,
+                                int whichassemble_taud, double *loadu, double *loadv);
+
 /* ------------------------------------------------------------------------
  * Device-resident solver handles (no reference counterpart: the reference
  * solvers are stateless calls).  A handle uploads A, b and x0 once and keeps

@@ -581,3 +581,20 @@ def test_l1l2(gpu_lib, n_glen):
     with pytest.raises(cg.CismGpuError):
         cg.assemble_stiffness_matrix_2d_l1l2(nx, ny, nz, 2, g["sigma"], g["ac"].astype(np.int32), g["xVertex"],
                                              g["yVertex"], u, v, g["stagthck"], dsdx, dsdy, flwa, ff, n_glen=2.0)
+
+
+@pytest.mark.parametrize("taud", [1, 0])
+def test_load_vector_gravity_bitexact(gpu_lib, taud):
+    from tests.test_oracle_bc import load_geometry
+    g = load_geometry()
+    nx, ny, nz, dx = g["nx"], g["ny"], g["nz"], g["dx"]
+    rng = np.random.default_rng(5)
+    sx, sy = 0.01 * rng.standard_normal((ny - 1, nx - 1)), 0.01 * rng.standard_normal((ny - 1, nx - 1))
+    args = (nx, ny, nz)
+    st, wu, wv = oracle.load_vector_gravity(*args, g["sigma"], g["stagw"], dx, dx, g["ac"], g["av"], g["xVertex"],
+                                            g["yVertex"], g["stagusrf"], g["stagthck"], sx, sy, taud)
+    assert st == 0
+    lu, lv = cg.load_vector_gravity(*args, 2, g["sigma"], g["stagw"], dx, dx, g["ac"], g["av"], g["xVertex"],
+                                    g["yVertex"], g["stagusrf"], g["stagthck"], sx, sy, whichassemble_taud=taud)
+    np.testing.assert_array_equal(lu, wu)
+    np.testing.assert_array_equal(lv, wv)
