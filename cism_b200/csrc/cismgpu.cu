@@ -1686,6 +1686,9 @@ static int oneshot_assemble(bool three_d, int nx, int ny, int nz, int nhalo, con
         return fail(CISMGPU_EINVAL, "null pointer argument");
     const int NC = three_d ? 27 : 9;
     TRY(validate_indx(indx, NC));
+    if (dsdx && (!dsdy || !flwa)) return fail(CISMGPU_EINVAL, "null pointer argument");
+    if (dsdx && whichefvs == 2 && std::fabs(n_glen - 1.0) >= 1.0e-10 && std::fabs(n_glen - 3.0) >= 1.0e-10)
+        return fail(CISMGPU_EINVAL, "Invalid value of n_glen for L1L2 solver (1 or 3)");
     cismgpu_par_t par{};
     par.staggered_ilo = 1; par.staggered_ihi = nx - 1; par.staggered_jlo = 1; par.staggered_jhi = ny - 1;
     par.tasks_row = par.tasks_col = 1;
@@ -1703,9 +1706,6 @@ static int oneshot_assemble(bool three_d, int nx, int ny, int nz, int nhalo, con
     L.NQ = sv.g.NQ;
     L.nz = sv.g.nz;
     L.raw3 = three_d ? 1 : 0;
-    if (dsdx && (!dsdy || !flwa)) return fail(CISMGPU_EINVAL, "null pointer argument");
-    if (dsdx && whichefvs == 2 && std::fabs(n_glen - 1.0) >= 1.0e-10 && std::fabs(n_glen - 3.0) >= 1.0e-10)
-        return fail(CISMGPU_EINVAL, "Invalid value of n_glen for L1L2 solver (1 or 3)");
     TRY(sv.assemble(three_d, nz, L, A0, A0 + bs, A0 + 2 * bs, A0 + 3 * bs, nhalo, sigma, active_cell, xv, yv, u, v,
                     0, usrf, thck, ff, whichapprox, whichefvs, efvs_constant, effstrain_min, n_glen, efvs, dsdx, dsdy,
                     flwa));

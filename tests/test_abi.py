@@ -124,3 +124,33 @@ def test_assembly_entry_points_validate_before_the_device(lib):
     with pytest.raises(cg.CismGpuError) as e:  # indxA entry outside 1..27
         cg.assemble_stiffness_matrix_3d(*base, indxA_3d=bad)
     assert e.value.status == 4
+
+
+def test_newer_assembly_entry_points_validate_before_the_device(lib):
+    """DIVA, L1L2 and the load vector reject bad arguments (EINVAL) before any device call."""
+    import numpy as np
+    import cism_b200 as cg
+    from tests.test_oracle_assembly import geometry
+    g = geometry(seed=82)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    act = g["ac"].astype(np.int32)
+    z2 = np.zeros((ny - 1, nx - 1))
+    zc = np.zeros((ny, nx))
+    ff = np.ones((ny, nx, nz - 1))
+    with pytest.raises(cg.CismGpuError) as e:  # n_glen must be 1 or 3 for the L1L2 viscosity
+        cg.assemble_stiffness_matrix_2d_l1l2(nx, ny, nz, 2, g["sigma"], act, g["xVertex"], g["yVertex"], z2, z2,
+                                             g["stagthck"], z2, z2, ff, ff, n_glen=2.0)
+    assert e.value.status == 4
+    eq = np.zeros((ny, nx, 4, nz - 1))
+    with pytest.raises(cg.CismGpuError) as e:  # nhalo = 1
+        cg.assemble_stiffness_matrix_2d_diva(nx, ny, nz, 1, g["sigma"], g["sigma"][:-1], act, g["xVertex"],
+                                             g["yVertex"], z2, z2, g["stagthck"], zc, z2, z2, zc, zc, ff, eq)
+    assert e.value.status == 4
+    with pytest.raises(cg.CismGpuError) as e:  # whichassemble_taud is 0 or 1
+        cg.load_vector_gravity(nx, ny, nz, 2, g["sigma"], np.linspace(0, 1, nz + 1), 1.0, 1.0, act, g["av"],
+                               g["xVertex"], g["yVertex"], g["stagusrf"], g["stagthck"], z2, z2, whichassemble_taud=3)
+    assert e.value.status == 4
+    with pytest.raises(cg.CismGpuError) as e:
+        cg.basal_sliding_bc_2d_diva(nx, ny, 2, 1.0, 1.0, act, g["av"], z2, z2, zc, g["xVertex"], g["yVertex"],
+                                    np.zeros((9, ny - 1, nx - 1)), np.zeros((9, ny - 1, nx - 1)), whichassemble_beta=7)
+    assert e.value.status == 4
