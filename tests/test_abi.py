@@ -154,3 +154,48 @@ def test_newer_assembly_entry_points_validate_before_the_device(lib):
         cg.basal_sliding_bc_2d_diva(nx, ny, 2, 1.0, 1.0, act, g["av"], z2, z2, zc, g["xVertex"], g["yVertex"],
                                     np.zeros((9, ny - 1, nx - 1)), np.zeros((9, ny - 1, nx - 1)), whichassemble_beta=7)
     assert e.value.status == 4
+
+
+def test_handle_method_bindings_reach_the_library(lib):
+    """The DeviceSolver assembly methods pass their arguments through ctypes with the C
+    signatures: on a NULL handle the library answers EINVAL (no device call), where a binding
+    mismatch would raise a ctypes or Python error first."""
+    import numpy as np
+    import cism_b200 as cg
+    from cism_b200 import assembly as asm
+    from tests.test_oracle_assembly import geometry
+    g = geometry(seed=83, nz=5)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    act = g["ac"].astype(np.int32)
+    av = g["av"].astype(np.int32)
+    z2, zc = np.zeros((ny - 1, nx - 1)), np.zeros((ny, nx))
+    ff = np.ones((ny, nx, nz - 1))
+    for kind in ("3d", "2d"):
+        s = cg.DeviceSolver.__new__(cg.DeviceSolver)
+        s._lib = cg.load_library()
+        s.handle = None
+        P = asm.Problem(kind, nx, ny, nz if kind == "3d" else 1, None, None, None, None, None, None, av, {})
+        s.problem = P
+        u = np.zeros((ny - 1, nx - 1, nz)) if kind == "3d" else z2
+        load = (u, u)
+        calls = [lambda: s.assemble_stiffness(2, g["sigma"], act, g["xVertex"], g["yVertex"], g["stagusrf"],
+                                              g["stagthck"], ff),
+                 lambda: s.assemble_system(2, 1.0, 1.0, g["sigma"], act, av, g["xVertex"], g["yVertex"],
+                                           g["stagusrf"], g["stagthck"], ff, *load, beta=z2, lsrf=zc,
+                                           umask=np.zeros(u.shape, np.int32), vmask=np.zeros(u.shape, np.int32),
+                                           whichassemble_beta=0)]
+        if kind == "2d":
+            sig = g["sigma"]
+            calls += [lambda: s.assemble_stiffness_diva(nz, 2, sig, sig[:-1], act, g["xVertex"], g["yVertex"],
+                                                        g["stagthck"], zc, z2, z2, zc, zc, ff, uvel=z2, vvel=z2,
+                                                        efvs_qp_3d=np.zeros((ny, nx, 4, nz - 1))),
+                      lambda: s.assemble_system_diva(nz, 2, 1.0, 1.0, sig, sig[:-1], act, av, g["xVertex"],
+                                                     g["yVertex"], g["stagthck"], zc, z2, z2, zc, zc, ff, z2, z2,
+                                                     beta_eff_x=z2, beta_eff_y=z2, lsrf=zc,
+                                                     umask=np.zeros(z2.shape, np.int32),
+                                                     vmask=np.zeros(z2.shape, np.int32))]
+        for call in calls:
+            with pytest.raises(cg.CismGpuError) as e:
+                call()
+            assert e.value.status == 4
+        s.handle = None  # nothing to destroy
