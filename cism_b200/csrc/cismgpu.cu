@@ -143,6 +143,9 @@ static int asm_ref_ready() {
     return CISMGPU_OK;
 }
 
+static int repro_global_sum(cudaStream_t s, const Geom &g, const double *d1, const double *d2, DevBuf &scratch,
+                            double *sum);
+
 struct Solver {
     Geom g{};
     bool is3d = false;
@@ -155,6 +158,8 @@ struct Solver {
     DevBuf tri;       // tridiagonal preconditioner planes (TriPlane), on first use
     DevBuf A_sav, x_sav;      // accelerated Picard's saved matrix and velocity (cismgpu_solver_save)
     DevBuf rsum;              // the reproducible sum's exponent extremes and level sums
+    DevBuf rprod;             // reproducible-sum solves: the two product fields and the flag
+    bool repro = false;       // parallel%reprosum: the FP64 solvers' global sums are reproducible sums
     DevBuf asm_in;            // the stiffness assembly's inputs (geometry, flow factor, velocity, efvs)
     DevBuf bc_in;             // the boundary terms' inputs (beta, lsrf, masks, velocity)
     DevBuf diva_in;           // the DIVA assembly's inputs and outputs
@@ -962,8 +967,43 @@ struct Solver {
         return CISMGPU_OK;
     }
 
+    // One global sum of a reproducible-sum solve: parallel_global_sum_stagger(au*bu, av*bv)
+    // with parallel%reprosum (parallel_mpi.F90:6703-6738), synchronizing the stream.  Non-finite
+    // owned summands give the IEEE sum of those summands (NaN, +Inf or -Inf).
+    int repro_dot(const double *au, const double *bu, const double *av, const double *bv, double *S) {
+        CU(rprod.ensure((size_t)2 * nvec * sizeof(double) + 256));
+        double *o1 = rprod.as<double>(), *o2 = o1 + nvec;
+        int *dflag = reinterpret_cast<int *>(o2 + nvec);
+        CU(cudaMemsetAsync(dflag, 0, sizeof(int), stream));
+        k_repro_products<<<nblocks(g.NQ), kBlock, 0, stream>>>(g, au, bu, av, bv, o1, o2, dflag);
+        CU(cudaGetLastError());
+        int hflag = 0;
+        CU(cudaMemcpyAsync(&hflag, dflag, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        TRY(repro_global_sum(stream, g, o1, o2, rsum, S));  // synchronizes the stream
+        if ((hflag & 1) || (hflag & 6) == 6) *S = std::nan("");
+        else if (hflag & 2) *S = HUGE_VAL;
+        else if (hflag & 4) *S = -HUGE_VAL;
+        return CISMGPU_OK;
+    }
+
+    int repro_epilogue(int epi, int iter, double S0, double S1) {
+        k_epilogue_value<<<1, 1, 0, stream>>>(state.as<SolveState>(), epi, iter, S0, S1);
+        CU(cudaGetLastError());
+        return CISMGPU_OK;
+    }
+
+    // The state's done flag (synchronizes the stream).
+    int read_done(int *done) {
+        CU(cudaMemcpyAsync(h_done, &state.as<SolveState>()->done, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CU(cudaStreamSynchronize(stream));
+        *done = h_done[0];
+        return CISMGPU_OK;
+    }
+
     template <int NCC> int run_standard(int precond, int ncheck, double tol, int maxiters);
     template <int NCC> int run_chrongear(int precond, int ncheck, double tol, int maxiters);
+    template <int NCC> int run_standard_repro(int precond, int ncheck, double tol, int maxiters);
+    template <int NCC> int run_chrongear_repro(int precond, int ncheck, double tol, int maxiters);
     template <int NCC> int run_mixed(int precond, int ncheck, double tol, int maxiters);
 };
 
@@ -1068,6 +1108,127 @@ int Solver::run_chrongear(int precond, int ncheck, double tol, int maxiters) {
             int f = poll.after_check();
             if (f < 0) return fail(CISMGPU_ECUDA, "polling the convergence flag failed");
             if (f) break;
+        }
+    }
+    CU(cudaGetLastError());
+    return CISMGPU_OK;
+}
+
+// pcg_solver_standard_{2d,3d} with parallel%reprosum: the launch sequence of run_standard with
+// each global sum taken by the reproducible sum (parallel_global_sum_stagger :1216, :1325,
+// :1381, :1466 / :441, :631, :687, :754).  The fused kernels run with no epilogue; the sum
+// of the same products then feeds the same scalar epilogue, so alpha, beta and err are the
+// reference's reprosum values.  The host drives the loop: two short stream synchronizations
+// per sum.
+template <int NCC>
+int Solver::run_standard_repro(int precond, int ncheck, double tol, int maxiters) {
+    cudaStream_t s = stream;
+    SolveState *st = state.as<SolveState>();
+    DD *part = partials.as<DD>();
+    const Ptrs p = ptrs();
+    const VecArgs v = vargs();
+    const double *Ad = A.as<double>();
+    const int32_t *ac = act.as<int32_t>();
+    const unsigned nb = nblocks(g.NQ);
+    const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
+    const RedCtx none{part, st, EPI_NONE, 0};
+    const Geom gg = g;
+    double S0 = 0.0;
+
+    k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
+    if (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL)
+        TRY(tri_setup(precond));
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
+    launch_mv<NCC, MV_PLAIN>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr, nullptr, none);
+    k_vec<OP_STD_INIT><<<nb, kBlock, 0, s>>>(gg, v, none);
+    CU(cudaGetLastError());
+    TRY(repro_dot(p.bu, p.bu, p.bv, p.bv, &S0));
+    TRY(repro_epilogue(EPI_L2RHS, 0, S0, 0.0));
+    for (int iter = 1; iter <= maxiters; ++iter) {
+        TRY((apply_precond<NCC, PRE_STD>(precond, p, none, nullptr, nullptr)));
+        TRY(repro_dot(p.ru, p.zu, p.rv, p.zv, &S0));
+        TRY(repro_epilogue(EPI_STD_ETA1, iter, S0, 0.0));
+        k_vec<OP_STD_D><<<nb, kBlock, 0, s>>>(gg, v, none);
+        k_halo<<<hb, kBlock, 0, s>>>(gg, p.du, p.dv, st);
+        launch_mv<NCC, MV_DQ>(s, gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr, none);
+        CU(cudaGetLastError());
+        TRY(repro_dot(p.du, p.qu, p.dv, p.qv, &S0));
+        TRY(repro_epilogue(EPI_STD_ETA2, iter, S0, 0.0));
+        k_vec<OP_XR><<<nb, kBlock, 0, s>>>(gg, v, none);
+        int done = 0;
+        if (is_check(iter, ncheck)) {
+            k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
+            launch_mv<NCC, MV_RESID>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv, none);
+            CU(cudaGetLastError());
+            TRY(repro_dot(p.ru, p.ru, p.rv, p.rv, &S0));
+            TRY(repro_epilogue(EPI_CHECK, iter, S0, 0.0));
+        }
+        TRY(read_done(&done));
+        if (done) break;
+    }
+    CU(cudaGetLastError());
+    return CISMGPU_OK;
+}
+
+// pcg_solver_chrongear_{2d,3d} with parallel%reprosum: the launch sequence of run_chrongear with
+// each global sum taken by the reproducible sum (parallel_global_sum_stagger :1921, :2181
+// and :2447 with two fields, :2572 / :3067, :3258, :3426, :3516); the two fields of one call
+// are summed independently, as cism_reprosum_calc does per field.
+template <int NCC>
+int Solver::run_chrongear_repro(int precond, int ncheck, double tol, int maxiters) {
+    cudaStream_t s = stream;
+    SolveState *st = state.as<SolveState>();
+    DD *part = partials.as<DD>();
+    const Ptrs p = ptrs();
+    const VecArgs v = vargs();
+    const double *Ad = A.as<double>();
+    const int32_t *ac = act.as<int32_t>();
+    const unsigned nb = nblocks(g.NQ);
+    const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
+    const RedCtx none{part, st, EPI_NONE, 0};
+    const Geom gg = g;
+    const bool tri = precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL;
+    if (tri && NCC == 9) maxiters = 100;
+    double S0 = 0.0, S1 = 0.0;
+
+    k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
+    if (tri) TRY(tri_setup(precond));
+    CU(cudaMemsetAsync(p.ru, 0, (size_t)(VAZ_V - VR_U + 1) * nvec * sizeof(double), s));
+    TRY(repro_dot(p.bu, p.bu, p.bv, p.bv, &S0));
+    TRY(repro_epilogue(EPI_L2RHS, 0, S0, 0.0));
+    // first pass
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
+    launch_mv<NCC, MV_PLAIN>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr, nullptr, none);
+    k_vec<OP_CG_INIT><<<nb, kBlock, 0, s>>>(gg, v, none);
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
+    TRY((apply_precond<NCC, PRE_CG_FIRST>(precond, p, none, p.du, p.dv)));
+    launch_mv<NCC, MV_DQ>(s, gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr, none);
+    CU(cudaGetLastError());
+    TRY(repro_dot(p.ru, p.zu, p.rv, p.zv, &S0));
+    TRY(repro_dot(p.du, p.qu, p.dv, p.qv, &S1));
+    TRY(repro_epilogue(EPI_CG_RHO0, 1, S0, 0.0));
+    TRY(repro_epilogue(EPI_CG_FIRST, 1, S1, 0.0));
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.qu, p.qv, st);
+    k_vec<OP_XR><<<nb, kBlock, 0, s>>>(gg, v, none);
+    CU(cudaGetLastError());
+    for (int iter = 2; iter <= maxiters; ++iter) {
+        int done = 0;
+        TRY(read_done(&done));
+        if (done) break;
+        TRY((apply_precond<NCC, PRE_ONLY>(precond, p, none, nullptr, nullptr)));
+        launch_mv<NCC, MV_CG_AZ>(s, gg, Ad, ac, p.zu, p.zv, p.Azu, p.Azv, nullptr, nullptr, p.ru, p.rv, none);
+        CU(cudaGetLastError());
+        TRY(repro_dot(p.ru, p.zu, p.rv, p.zv, &S0));
+        TRY(repro_dot(p.Azu, p.zu, p.Azv, p.zv, &S1));
+        TRY(repro_epilogue(EPI_CG_ITER, iter, S0, S1));
+        k_halo<<<hb, kBlock, 0, s>>>(gg, p.Azu, p.Azv, st);
+        k_vec<OP_CG_UPD><<<nb, kBlock, 0, s>>>(gg, v, none);
+        if (is_check(iter, ncheck)) {
+            launch_mv<NCC, MV_RESID>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv, none);
+            CU(cudaGetLastError());
+            TRY(repro_dot(p.ru, p.ru, p.rv, p.rv, &S0));
+            TRY(repro_epilogue(EPI_CHECK, iter, S0, 0.0));
+            k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
         }
     }
     CU(cudaGetLastError());
@@ -1474,6 +1635,12 @@ enum Algo { ALG_STANDARD = CISMGPU_ALG_STANDARD, ALG_CHRONGEAR = CISMGPU_ALG_CHR
             ALG_MIXED = CISMGPU_ALG_MIXED_CHRONGEAR };
 
 static int run_algorithm(Solver &sv, int alg, int precond, int ncheck, double tol, int maxiters) {
+    if (sv.repro && alg == ALG_STANDARD)
+        return sv.is3d ? sv.run_standard_repro<27>(precond, ncheck, tol, maxiters)
+                       : sv.run_standard_repro<9>(precond, ncheck, tol, maxiters);
+    if (sv.repro && alg == ALG_CHRONGEAR)
+        return sv.is3d ? sv.run_chrongear_repro<27>(precond, ncheck, tol, maxiters)
+                       : sv.run_chrongear_repro<9>(precond, ncheck, tol, maxiters);
     if (alg == ALG_STANDARD)
         return sv.is3d ? sv.run_standard<27>(precond, ncheck, tol, maxiters)
                        : sv.run_standard<9>(precond, ncheck, tol, maxiters);
@@ -1557,6 +1724,7 @@ static int oneshot_solve(int alg, bool is3d, int nx, int ny, int nz, const cismg
     TRY(sv.init(nullptr));
     const double *blocks[4] = {Auu, Auv, Avu, Avv};
     TRY(sv.upload(make_geom(nx, ny, is3d ? nz : 1, par), is3d, indx, act, blocks, bu, bv, xu, xv));
+    sv.repro = par->reprosum != 0;
     if (is3d && indx2)
         for (int c = 0; c < 9; ++c) sv.hindx2[c] = indx2[c];
     TRY(sv.begin_solve());
@@ -2048,6 +2216,7 @@ int cismgpu_solver_create(cismgpu_solver_t **out, int dims, int nx, int ny, int 
     if (!rc) rc = h->sv.upload(make_geom(nx, ny, is3d ? nz : 1, par), is3d, indxA, active_vertex, blocks, bu, bv,
                                xu0, xv0);
     if (!rc && cudaStreamSynchronize(h->sv.stream) != cudaSuccess) rc = fail(CISMGPU_ECUDA, "upload failed");
+    h->sv.repro = par->reprosum != 0;
     if (rc) {
         delete h;
         return rc;

@@ -987,6 +987,46 @@ __global__ void k_vec_out(Geom g, const double *__restrict__ src, double *__rest
     raw[node] = src[(long long)k * g.NQ + q];
 }
 
+// Reproducible-sum solves (parallel%reprosum): the two product fields work2u = au*bu and
+// work2v = av*bv of one parallel_global_sum_stagger call, written in the caller's layout
+// (node k + nz*q) that the reproducible sum reads.  An owned node whose au*bu + av*bv is not
+// finite is recorded in *flag (1 NaN, 2 +Inf, 4 -Inf) and its products are written as zero,
+// so the integer expansion only ever sees finite summands; the host then returns the IEEE
+// sum of the non-finite values instead.
+__global__ void __launch_bounds__(kBlock) k_repro_products(Geom g, const double *__restrict__ au,
+                                                           const double *__restrict__ bu,
+                                                           const double *__restrict__ av,
+                                                           const double *__restrict__ bv, double *__restrict__ o1,
+                                                           double *__restrict__ o2, int *flag) {
+    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
+    if (q >= g.NQ) return;
+    int i, j;
+    col_of(g, q, i, j);
+    const bool own = owned(g, i, j);
+    int f = 0;
+    for (int k = 0; k < g.nz; ++k) {
+        const long long e = (long long)k * g.NQ + q;
+        double p1 = __dmul_rn(au[e], bu[e]);
+        double p2 = __dmul_rn(av[e], bv[e]);
+        if (own) {
+            const double v = __dadd_rn(p1, p2);
+            if (v != v) f |= 1;
+            else if (v == __longlong_as_double(0x7ff0000000000000LL)) f |= 2;
+            else if (v == __longlong_as_double(0xfff0000000000000LL)) f |= 4;
+            if (!(v - v == 0.0)) { p1 = 0.0; p2 = 0.0; }
+        }
+        o1[(long long)k + (long long)g.nz * q] = p1;
+        o2[(long long)k + (long long)g.nz * q] = p2;
+    }
+    if (f) atomicOr(flag, f);
+}
+
+// The scalar epilogue of a sum computed on the host side of the stream (the reproducible sum).
+__global__ void k_epilogue_value(SolveState *st, int epi, int iter, double S0, double S1) {
+    if (st->done) return;
+    epilogue(st, epi, iter, S0, S1);
+}
+
 __global__ void k_init_state(SolveState *st, double tol, int maxiters) {
     st->eta0 = 1.0; st->eta1 = 0.0; st->eta2 = 0.0; st->alpha = 0.0; st->beta = 0.0;
     st->rho_old = 0.0; st->sigma = 0.0; st->rho = 0.0; st->delta = 0.0;

@@ -33,6 +33,19 @@
  * Every call is synchronous: on return xu/xv hold the solution (including the
  * halo values the reference leaves in them), err and niters are set, and the
  * library holds no pointer to caller memory.
+ *
+ * Global sums in the standard and Chronopoulos-Gear solvers: with par->reprosum == 0
+ * every parallel_global_sum_stagger of the reference is the library's fixed double-double
+ * reduction tree (launch-independent, reproducible run to run).  With par->reprosum != 0
+ * (the one-shot solvers and cismgpu_solver_create) each of them is the reference's
+ * reproducible sum (cism_reprosum_calc, libglimmer/cism_reprosum_mod.F90:237-1818, as
+ * parallel_global_sum_stagger's reprosum branch calls it, parallel_mpi.F90:6703-6738), two
+ * fields summed independently where the reference passes nflds = 2 (:1921, :2181, :2447),
+ * so a solve reproduces the reference's reprosum run on one rank bit for bit; the host
+ * then drives the iteration, with two short stream synchronizations per sum.  Non-finite
+ * summands, undefined in the reference, give their IEEE sum (NaN, +Inf or -Inf), so the
+ * NaN breakdown tests behave as without reprosum.  The mixed-precision solver ignores the
+ * flag (its sums are the fixed FP64 tree of its checks).
  */
 #ifndef CISMGPU_H
 #define CISMGPU_H
@@ -74,7 +87,7 @@ typedef struct cismgpu_par {
     int32_t periodic_bc;   /* logical: doubly periodic (also no_penetration, parallel_mpi.F90:2498) */
     int32_t outflow_bc;    /* logical: zero beyond the global boundary                              */
     int32_t no_ice_bc;     /* logical: zero the halo and the last owned row                         */
-    int32_t reprosum;      /* logical: reproducible sums requested                                  */
+    int32_t reprosum;      /* logical: reproducible sums (global sums, FP64 solvers' dot products)  */
     int32_t tasks_row;     /* tasks on this row    (must be 1: whole domain on one GPU)            */
     int32_t tasks_col;     /* tasks on this column (must be 1)                                      */
 } cismgpu_par_t;

@@ -282,6 +282,22 @@ inline double f_set_exponent(double x, int e) { return std::ldexp(f_fraction(x),
 double reprosum(const std::vector<double> &arr) {
     const int kDigR8 = 53, kDigI8 = 63, kMinExp = -1021, kMaxExp = 1024;
     const long nsummands = (long)arr.size();
+    // Non-finite summands: the reference's NaN/Inf handling is commented out
+    // (cism_reprosum_mod.F90:58-62) and int(x, i8) of a NaN or an infinity is processor
+    // dependent, so its result is undefined there.  The library and this restatement both
+    // return the IEEE sum of the non-finite summands (NaN, +Inf or -Inf), which keeps the
+    // solvers' NaN breakdown tests meaningful.
+    {
+        bool nan = false, pinf = false, ninf = false;
+        for (double x : arr) {
+            if (x != x) nan = true;
+            else if (x == HUGE_VAL) pinf = true;
+            else if (x == -HUGE_VAL) ninf = true;
+        }
+        if (nan || (pinf && ninf)) return NAN;
+        if (pinf) return HUGE_VAL;
+        if (ninf) return -HUGE_VAL;
+    }
     // exponent extremes of the nonzero summands (:455-487)
     int lmin = kMaxExp, lmax = kMinExp;
     for (double x : arr)

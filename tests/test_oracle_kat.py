@@ -272,6 +272,16 @@ def test_reprosum_restatement_properties():
     assert oracle.reprosum(np.zeros(7)) == 0.0
 
 
+def test_reprosum_nonfinite_summands():
+    """Non-finite summands, undefined in the reference (its NaN/Inf handling is commented out),
+    give their IEEE sum in the restatement, as in the library's reproducible-sum solves."""
+    assert np.isnan(oracle.reprosum(np.array([1.0, np.nan, 2.0])))
+    assert np.isnan(oracle.reprosum(np.array([np.inf, 3.0, -np.inf])))
+    assert oracle.reprosum(np.array([1.0, np.inf, 1e300])) == np.inf
+    assert oracle.reprosum(np.array([-np.inf, 3.0])) == -np.inf
+    assert oracle.reprosum(np.array([1.0, 2.0**-60])) == 1.0
+
+
 def test_global_sum_repro_mode():
     """The oracle's SUM_REPRO global sum (the reference's reprosum branch) on owned vertices."""
     P = problems.slab_3d(seed=13, boundary_ice=True, bc="periodic")
