@@ -2444,6 +2444,8 @@ static int oneshot_boundary3d(int which, int nx, int ny, int nz, int nhalo, doub
         return fail(CISMGPU_EINVAL, "null pointer argument");
     if (nx < 6 || ny < 6 || nz < 1 || nz > kMaxNz) return fail(CISMGPU_EINVAL, "grid too small or nz outside 1..64");
     if (nhalo < 1 || 2 * nhalo >= nx || 2 * nhalo >= ny) return fail(CISMGPU_EINVAL, "nhalo outside the grid");
+    if (which == 1 && assemble_beta == 0 && nhalo < 2)  // the cells' vertices must lie inside the arrays
+        return fail(CISMGPU_EINVAL, "the standard basal form needs nhalo >= 2");
     TRY(validate_indx(indx, 27));
     cismgpu_par_t par{};
     par.staggered_ilo = 1; par.staggered_ihi = nx - 1; par.staggered_jlo = 1; par.staggered_jhi = ny - 1;
@@ -2509,6 +2511,8 @@ static int oneshot_boundary2d(int which, int nx, int ny, int nhalo, double dx, d
         return fail(CISMGPU_EINVAL, "null pointer argument");
     if (nx < 6 || ny < 6) return fail(CISMGPU_EINVAL, "grid too small");
     if (nhalo < 1 || 2 * nhalo >= nx || 2 * nhalo >= ny) return fail(CISMGPU_EINVAL, "nhalo outside the grid");
+    if (which == 1 && assemble_beta == 0 && nhalo < 2)  // the cells' vertices must lie inside the arrays
+        return fail(CISMGPU_EINVAL, "the standard basal form needs nhalo >= 2");
     TRY(validate_indx(indx, 9));
     cismgpu_par_t par{};
     par.staggered_ilo = 1; par.staggered_ihi = nx - 1; par.staggered_jlo = 1; par.staggered_jhi = ny - 1;

@@ -312,8 +312,10 @@ int cismgpu_dirichlet_boundary_conditions_3d(int nx, int ny, int nz, int nhalo, 
  * and cos are CUDA's.  whichassemble_beta = 0 (standard): per active cell, 4-point quadrature of
  * beta phi_r phi_c over the lower surface (the curved area factor,
  * get_area_scale_factor_curved_2d) added to the bed level's 9 horizontal couplings, point by
- * point in the reference's order (its sqrt is IEEE, so bit-exact).  beta, xVertex, yVertex
- * (nx-1,ny-1); active_cell (nx,ny); Auu, Avv (27,nz,nx-1,ny-1) (nz = 1 for the bed slices). */
+ * point in the reference's order (its sqrt is IEEE, so bit-exact); it reads the vertices of the
+ * cells nhalo+1..n-nhalo+1, so it needs nhalo >= 2 (EINVAL otherwise, as in the 2D forms).
+ * beta, xVertex, yVertex (nx-1,ny-1); active_cell (nx,ny); Auu, Avv (27,nz,nx-1,ny-1) (nz = 1
+ * for the bed slices). */
 int cismgpu_basal_sliding_bc_3d(int nx, int ny, int nz, int nhalo, double dx, double dy,
                                 const int32_t *active_cell, const int32_t *active_vertex, const double *beta,
                                 const double *lsrf, const double *xVertex, const double *yVertex,

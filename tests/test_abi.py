@@ -114,10 +114,18 @@ def test_assembly_entry_points_validate_before_the_device(lib):
         cg.basal_sliding_bc_3d(nx, ny, nz, 2, 1.0, 1.0, act, g["av"], np.zeros((ny - 1, nx - 1)), np.zeros((ny, nx)),
                                g["xVertex"], g["yVertex"], *A, whichassemble_beta=2)
     assert e.value.status == 4
+    with pytest.raises(cg.CismGpuError) as e:  # the standard form reads cell vertices: nhalo >= 2
+        cg.basal_sliding_bc_3d(nx, ny, nz, 1, 1.0, 1.0, act, g["av"], np.zeros((ny - 1, nx - 1)), np.zeros((ny, nx)),
+                               g["xVertex"], g["yVertex"], *A, whichassemble_beta=0)
+    assert e.value.status == 4
     A2 = [np.zeros((9, ny - 1, nx - 1)) for _ in range(2)]
     with pytest.raises(cg.CismGpuError) as e:
         cg.basal_sliding_bc_2d(nx, ny, 2, 1.0, 1.0, act, g["av"], np.zeros((ny - 1, nx - 1)), g["xVertex"],
                                g["yVertex"], *A2, whichassemble_beta=2)
+    assert e.value.status == 4
+    with pytest.raises(cg.CismGpuError) as e:
+        cg.basal_sliding_bc_2d(nx, ny, 1, 1.0, 1.0, act, g["av"], np.zeros((ny - 1, nx - 1)), g["xVertex"],
+                               g["yVertex"], *A2, whichassemble_beta=0)
     assert e.value.status == 4
     bad = np.arange(1, 28, dtype=np.int32)
     bad[5] = 99
