@@ -282,6 +282,25 @@ def test_reprosum_nonfinite_summands():
     assert oracle.reprosum(np.array([1.0, 2.0**-60])) == 1.0
 
 
+def test_reprosum_solve_cases_of_the_device_tests():
+    """The oracle side of the device reprosum-solve tests: the 3D no-slip slab converges with
+    every preconditioner and both algorithms, and the outflow slab breaks down in the first
+    pass (alpha = NaN) with the SIA and tridiagonal preconditioners."""
+    import copy
+    for alg in ("standard", "chrongear"):
+        for pc in range(5):
+            P = copy.copy(problems.slab_3d(seed=5, sliding=False))
+            P.par = dict(P.par, reprosum=1)
+            x0 = problems.random_x0(P, seed=7, scale=10.0)
+            o = oracle.pcg(alg, P, pc, tol=1e-8, maxiters=300, summode=oracle.SUM_REPRO, x0=x0)
+            assert o[0] == 0 and o[3] < 1e-8, (alg, pc, o[0], o[3])
+    for pc in (2, 3, 4):
+        P = problems.slab_3d(seed=3, boundary_ice=True, bc="outflow")
+        x0 = problems.random_x0(P, seed=7, scale=10.0)
+        o = oracle.pcg("chrongear", P, pc, tol=1e-8, maxiters=300, summode=oracle.SUM_REPRO, x0=x0)
+        assert o[0] == 2 and o[4] == 1, (pc, o[0], o[4])  # CISMGPU_EBREAKDOWN_ALPHA
+
+
 def test_global_sum_repro_mode():
     """The oracle's SUM_REPRO global sum (the reference's reprosum branch) on owned vertices."""
     P = problems.slab_3d(seed=13, boundary_ice=True, bc="periodic")
