@@ -223,6 +223,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         getattr(lib, f).restype = ctypes.c_int
     lib.cismgpu_set_oneshot_algorithm.argtypes = [i32]
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
+    lib.cismgpu_set_sum_order.argtypes = [i32]
+    lib.cismgpu_set_sum_order.restype = ctypes.c_int
+    lib.cismgpu_test_set_device_waits.argtypes = [ctypes.c_longlong, ctypes.c_uint]
+    lib.cismgpu_test_set_device_waits.restype = ctypes.c_int
     lib.cismgpu_last_error.restype = ctypes.c_char_p
     lib.cismgpu_version.restype = ctypes.c_char_p
     _lib = lib
@@ -306,6 +310,42 @@ def parallel_global_sum_stagger_noalloc(nx, ny, nz, parallel, arr1_dev: int, arr
     _check(lib, lib.cismgpu_global_sum_stagger_noalloc(nx, ny, nz, ctypes.byref(par), ctypes.c_void_p(arr1_dev),
                                                        ctypes.c_void_p(arr2_dev), ctypes.c_void_p(sum_dev),
                                                        ctypes.c_void_p(stream)))
+
+
+SUM_TREE, SUM_SEQUENTIAL = 0, 1  # CISMGPU_SUM_*
+
+
+def set_sum_order(order: int = SUM_TREE) -> int:
+    """Order of the FP64 solvers' and the global-sum calls' sums when parallel%reprosum is off:
+    SUM_TREE (the library's fixed tree, default) or SUM_SEQUENTIAL (the reference's own
+    sequential order, parallel_mpi.F90:6770, bit for bit; slower).  Process-wide; returns
+    the previous setting."""
+    return int(load_library().cismgpu_set_sum_order(int(order)))
+
+
+class sum_order:
+    """Context manager: `with sum_order(SUM_SEQUENTIAL): ...` restores the previous order on exit."""
+
+    def __init__(self, order: int):
+        self.order = order
+        self.prev = None
+
+    def __enter__(self):
+        self.prev = set_sum_order(self.order)
+        return self
+
+    def __exit__(self, *exc):
+        set_sum_order(self.prev)
+        return False
+
+
+def debug_set_device_waits(wait_cycles: int = 0, withhold_step: int = 0) -> None:
+    """Test hook of the mixed kernels' bounded waits: wait bound in SM cycles (0: the default,
+    about 1 s) and a step whose record tile 0 of every solve does not publish (0: none), so the
+    waits for it run out and the launch ends with CISMGPU_ETIMEOUT.  (0, 0) restores normal
+    operation."""
+    lib = load_library()
+    _check(lib, lib.cismgpu_test_set_device_waits(int(wait_cycles), int(withhold_step)))
 
 
 def set_oneshot_algorithm(algorithm: int = -1) -> int:

@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -992,6 +993,32 @@ struct Solver {
         return CISMGPU_OK;
     }
 
+    // One global sum in the reference's own order, parallel_global_sum_stagger(au*bu, av*bv)
+    // without reprosum (parallel_mpi.F90:6770, :6637), and its scalar epilogue, on the device.
+    int seq_dot(const double *au, const double *bu, const double *av, const double *bv, int epi, int iter) {
+        SeqArgs a{};
+        a.a[0][0] = au; a.b[0][0] = bu;
+        a.a[0][1] = av; a.b[0][1] = bv;
+        k_seq_sum<1, false><<<1, kBlock, 0, stream>>>(g, a, state.as<SolveState>(), epi, EPI_NONE, iter, nullptr);
+        CU(cudaGetLastError());
+        return CISMGPU_OK;
+    }
+
+    // The two-field form (nflds = 2, parallel_mpi.F90:7042, :6904): field 1 = (a1, b1), field 2
+    // = (a2, b2), each summed in the reference's order.  epi2 != EPI_NONE: epilogue epi of S0,
+    // then epi2 of S1; otherwise epi(S0, S1).
+    int seq_dot2(const double *a1u, const double *b1u, const double *a1v, const double *b1v, const double *a2u,
+                 const double *b2u, const double *a2v, const double *b2v, int epi, int epi2, int iter) {
+        SeqArgs a{};
+        a.a[0][0] = a1u; a.b[0][0] = b1u;
+        a.a[0][1] = a1v; a.b[0][1] = b1v;
+        a.a[1][0] = a2u; a.b[1][0] = b2u;
+        a.a[1][1] = a2v; a.b[1][1] = b2v;
+        k_seq_sum<2, false><<<1, kBlock, 0, stream>>>(g, a, state.as<SolveState>(), epi, epi2, iter, nullptr);
+        CU(cudaGetLastError());
+        return CISMGPU_OK;
+    }
+
     // The state's done flag (synchronizes the stream).
     int read_done(int *done) {
         CU(cudaMemcpyAsync(h_done, &state.as<SolveState>()->done, sizeof(int), cudaMemcpyDeviceToHost, stream));
@@ -1004,6 +1031,8 @@ struct Solver {
     template <int NCC> int run_chrongear(int precond, int ncheck, double tol, int maxiters);
     template <int NCC> int run_standard_repro(int precond, int ncheck, double tol, int maxiters);
     template <int NCC> int run_chrongear_repro(int precond, int ncheck, double tol, int maxiters);
+    template <int NCC> int run_standard_seq(int precond, int ncheck, double tol, int maxiters);
+    template <int NCC> int run_chrongear_seq(int precond, int ncheck, double tol, int maxiters);
     template <int NCC> int run_mixed(int precond, int ncheck, double tol, int maxiters);
 };
 
@@ -1229,6 +1258,116 @@ int Solver::run_chrongear_repro(int precond, int ncheck, double tol, int maxiter
             TRY(repro_dot(p.ru, p.ru, p.rv, p.rv, &S0));
             TRY(repro_epilogue(EPI_CHECK, iter, S0, 0.0));
             k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
+        }
+    }
+    CU(cudaGetLastError());
+    return CISMGPU_OK;
+}
+
+// pcg_solver_standard_{2d,3d} with the reference's own summation order: the launch sequence of
+// run_standard, its fused kernels run without their epilogue, and each global sum (:1216,
+// :1325, :1381, :1466 / :441, :631, :687, :754) is k_seq_sum over the same products with
+// the same scalar epilogue.  Everything stays on the device: the host polls the done flag
+// at the checks, with one check period of look-ahead, as in run_standard.
+template <int NCC>
+int Solver::run_standard_seq(int precond, int ncheck, double tol, int maxiters) {
+    cudaStream_t s = stream;
+    SolveState *st = state.as<SolveState>();
+    DD *part = partials.as<DD>();
+    const Ptrs p = ptrs();
+    const VecArgs v = vargs();
+    const double *Ad = A.as<double>();
+    const int32_t *ac = act.as<int32_t>();
+    const unsigned nb = nblocks(g.NQ);
+    const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
+    const RedCtx none{part, st, EPI_NONE, 0};
+    const Geom gg = g;
+    prof_bytes = mv_bytes(0);
+
+    k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
+    if (precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL)
+        TRY(tri_setup(precond));
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
+    launch_mv<NCC, MV_PLAIN>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr, nullptr, none);
+    k_vec<OP_STD_INIT><<<nb, kBlock, 0, s>>>(gg, v, none);
+    CU(cudaGetLastError());
+    TRY(seq_dot(p.bu, p.bu, p.bv, p.bv, EPI_L2RHS, 0));
+    Poller poll(*this);
+    for (int iter = 1; iter <= maxiters; ++iter) {
+        TRY((apply_precond<NCC, PRE_STD>(precond, p, none, nullptr, nullptr)));
+        TRY(seq_dot(p.ru, p.zu, p.rv, p.zv, EPI_STD_ETA1, iter));
+        k_vec<OP_STD_D><<<nb, kBlock, 0, s>>>(gg, v, none);
+        k_halo<<<hb, kBlock, 0, s>>>(gg, p.du, p.dv, st);
+        TRY(timed([&] {
+            launch_mv<NCC, MV_DQ>(s, gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr, none);
+        }));
+        TRY(seq_dot(p.du, p.qu, p.dv, p.qv, EPI_STD_ETA2, iter));
+        k_vec<OP_XR><<<nb, kBlock, 0, s>>>(gg, v, none);
+        if (is_check(iter, ncheck)) {
+            k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
+            launch_mv<NCC, MV_RESID>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv, none);
+            TRY(seq_dot(p.ru, p.ru, p.rv, p.rv, EPI_CHECK, iter));
+            int f = poll.after_check();
+            if (f < 0) return fail(CISMGPU_ECUDA, "polling the convergence flag failed");
+            if (f) break;
+        }
+    }
+    CU(cudaGetLastError());
+    return CISMGPU_OK;
+}
+
+// pcg_solver_chrongear_{2d,3d} with the reference's own summation order: run_chrongear's
+// sequence with each sum (:3074, :3248 and :3413 with two fields, :3516 / :1921, :2181,
+// :2447, :2551) taken by k_seq_sum; the two-field calls sum both fields in one kernel.
+template <int NCC>
+int Solver::run_chrongear_seq(int precond, int ncheck, double tol, int maxiters) {
+    cudaStream_t s = stream;
+    SolveState *st = state.as<SolveState>();
+    DD *part = partials.as<DD>();
+    const Ptrs p = ptrs();
+    const VecArgs v = vargs();
+    const double *Ad = A.as<double>();
+    const int32_t *ac = act.as<int32_t>();
+    const unsigned nb = nblocks(g.NQ);
+    const unsigned hb = nblocks(4LL * g.NX + 4LL * (g.NY - 4));
+    const RedCtx none{part, st, EPI_NONE, 0};
+    const Geom gg = g;
+    prof_bytes = mv_bytes(1);
+    const bool tri = precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL;
+    if (tri && NCC == 9) maxiters = 100;
+
+    k_init_state<<<1, 1, 0, s>>>(st, tol, maxiters);
+    if (tri) TRY(tri_setup(precond));
+    CU(cudaMemsetAsync(p.ru, 0, (size_t)(VAZ_V - VR_U + 1) * nvec * sizeof(double), s));
+    TRY(seq_dot(p.bu, p.bu, p.bv, p.bv, EPI_L2RHS, 0));
+    // first pass
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.xu, p.xv, st);
+    launch_mv<NCC, MV_PLAIN>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, nullptr, nullptr, nullptr, nullptr, none);
+    k_vec<OP_CG_INIT><<<nb, kBlock, 0, s>>>(gg, v, none);
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
+    TRY((apply_precond<NCC, PRE_CG_FIRST>(precond, p, none, p.du, p.dv)));
+    launch_mv<NCC, MV_DQ>(s, gg, Ad, ac, p.du, p.dv, p.qu, p.qv, nullptr, nullptr, nullptr, nullptr, none);
+    TRY(seq_dot2(p.ru, p.zu, p.rv, p.zv, p.du, p.qu, p.dv, p.qv, EPI_CG_RHO0, EPI_CG_FIRST, 1));
+    k_halo<<<hb, kBlock, 0, s>>>(gg, p.qu, p.qv, st);
+    k_vec<OP_XR><<<nb, kBlock, 0, s>>>(gg, v, none);
+    CU(cudaGetLastError());
+    Poller poll(*this);
+    for (int iter = 2; iter <= maxiters; ++iter) {
+        TRY((apply_precond<NCC, PRE_ONLY>(precond, p, none, nullptr, nullptr)));
+        TRY(timed([&] {
+            launch_mv<NCC, MV_CG_AZ>(s, gg, Ad, ac, p.zu, p.zv, p.Azu, p.Azv, nullptr, nullptr, p.ru, p.rv, none);
+        }));
+        TRY(seq_dot2(p.ru, p.zu, p.rv, p.zv, p.Azu, p.zu, p.Azv, p.zv, EPI_CG_ITER, EPI_NONE, iter));
+        k_halo<<<hb, kBlock, 0, s>>>(gg, p.Azu, p.Azv, st);
+        k_vec<OP_CG_UPD><<<nb, kBlock, 0, s>>>(gg, v, none);
+        if (is_check(iter, ncheck)) {
+            launch_mv<NCC, MV_RESID>(s, gg, Ad, ac, p.xu, p.xv, p.zu, p.zv, p.bu, p.bv, p.ru, p.rv, none);
+            TRY(seq_dot(p.ru, p.ru, p.rv, p.rv, EPI_CHECK, iter));
+            k_halo<<<hb, kBlock, 0, s>>>(gg, p.ru, p.rv, st);
+            CU(cudaGetLastError());
+            int f = poll.after_check();
+            if (f < 0) return fail(CISMGPU_ECUDA, "polling the convergence flag failed");
+            if (f) break;
         }
     }
     CU(cudaGetLastError());
@@ -1634,7 +1773,17 @@ int Solver::run_mixed(int precond, int ncheck, double tol, int maxiters) {
 enum Algo { ALG_STANDARD = CISMGPU_ALG_STANDARD, ALG_CHRONGEAR = CISMGPU_ALG_CHRONGEAR,
             ALG_MIXED = CISMGPU_ALG_MIXED_CHRONGEAR };
 
+// Order of the FP64 solvers' global sums when parallel%reprosum is off (cismgpu_set_sum_order).
+static std::atomic<int> g_sum_order{CISMGPU_SUM_TREE};
+
 static int run_algorithm(Solver &sv, int alg, int precond, int ncheck, double tol, int maxiters) {
+    const bool seq = !sv.repro && g_sum_order.load() == CISMGPU_SUM_SEQUENTIAL;
+    if (seq && alg == ALG_STANDARD)
+        return sv.is3d ? sv.run_standard_seq<27>(precond, ncheck, tol, maxiters)
+                       : sv.run_standard_seq<9>(precond, ncheck, tol, maxiters);
+    if (seq && alg == ALG_CHRONGEAR)
+        return sv.is3d ? sv.run_chrongear_seq<27>(precond, ncheck, tol, maxiters)
+                       : sv.run_chrongear_seq<9>(precond, ncheck, tol, maxiters);
     if (sv.repro && alg == ALG_STANDARD)
         return sv.is3d ? sv.run_standard_repro<27>(precond, ncheck, tol, maxiters)
                        : sv.run_standard_repro<9>(precond, ncheck, tol, maxiters);
@@ -1911,6 +2060,8 @@ static int oneshot_global_sum(int nx, int ny, int nz, const cismgpu_par_t *par, 
     g_last_error.clear();
     if (!par || !a1 || !a2 || !sum) return fail(CISMGPU_EINVAL, "null pointer argument");
     if (nx < 6 || ny < 6 || nz < 1) return fail(CISMGPU_EINVAL, "grid too small");
+    if (par->tasks_row * par->tasks_col != 1)
+        return fail(CISMGPU_EUNSUPPORTED, "the whole domain must be on one GPU (tasks_row*tasks_col == 1)");
     if (par->staggered_ilo < 1 || par->staggered_ihi > nx - 1 || par->staggered_ilo > par->staggered_ihi ||
         par->staggered_jlo < 1 || par->staggered_jhi > ny - 1 || par->staggered_jlo > par->staggered_jhi)
         return fail(CISMGPU_EINVAL, "owned vertex bounds outside the array");
@@ -1927,9 +2078,29 @@ static int oneshot_global_sum(int nx, int ny, int nz, const cismgpu_par_t *par, 
     SolveState *st = sv.state.as<SolveState>();
     CU(cudaMemcpyAsync(d1, a1, n * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
     CU(cudaMemcpyAsync(d2, a2, n * sizeof(double), cudaMemcpyHostToDevice, sv.stream));
-    if (par->reprosum) return repro_global_sum(sv.stream, g, d1, d2, sv.rsum, sum);  // parallel_mpi.F90:6703-6738
+    if (par->reprosum) {  // parallel_mpi.F90:6703-6738; non-finite summands give their IEEE sum
+        CU(cudaMemsetAsync(st, 0, sizeof(SolveState), sv.stream));
+        int *dflag = &st->status;
+        const unsigned grid = (unsigned)std::min<long long>((n + kBlock - 1) / kBlock, 1184);
+        k_repro_screen<<<grid, kBlock, 0, sv.stream>>>(g, d1, d2, dflag);
+        CU(cudaGetLastError());
+        int hflag = 0;
+        CU(cudaMemcpyAsync(&hflag, dflag, sizeof(int), cudaMemcpyDeviceToHost, sv.stream));
+        TRY(repro_global_sum(sv.stream, g, d1, d2, sv.rsum, sum));  // synchronizes the stream
+        if ((hflag & 1) || (hflag & 6) == 6) *sum = std::nan("");
+        else if (hflag & 2) *sum = HUGE_VAL;
+        else if (hflag & 4) *sum = -HUGE_VAL;
+        return CISMGPU_OK;
+    }
     CU(cudaMemsetAsync(st, 0, sizeof(SolveState), sv.stream));
-    k_gsum<true><<<nb, kBlock, 0, sv.stream>>>(g, d1, d2, sv.partials.as<DD>(), &st->ticket[0], &st->err);
+    if (g_sum_order.load() == CISMGPU_SUM_SEQUENTIAL) {  // parallel_mpi.F90:6770, :6637
+        SeqArgs sa{};
+        sa.a[0][0] = d1;
+        sa.a[0][1] = d2;
+        k_seq_sum<1, true><<<1, kBlock, 0, sv.stream>>>(g, sa, nullptr, EPI_NONE, EPI_NONE, 0, &st->err);
+    } else {
+        k_gsum<true><<<nb, kBlock, 0, sv.stream>>>(g, d1, d2, sv.partials.as<DD>(), &st->ticket[0], &st->err);
+    }
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(sum, &st->err, sizeof(double), cudaMemcpyDeviceToHost, sv.stream));
     CU(cudaStreamSynchronize(sv.stream));
@@ -3066,6 +3237,20 @@ int cismgpu_set_oneshot_algorithm(int algorithm) {
     const int prev = g_oneshot_alg;
     g_oneshot_alg = (algorithm >= CISMGPU_ALG_STANDARD && algorithm <= CISMGPU_ALG_MIXED_CHRONGEAR) ? algorithm : -1;
     return prev;
+}
+
+int cismgpu_test_set_device_waits(long long wait_cycles, unsigned int withhold_step) {
+    g_last_error.clear();
+    TRY(check_device());
+    const long long w = wait_cycles > 0 ? wait_cycles : kWaitCycles;
+    CU(cudaMemcpyToSymbol(c_wait_cycles, &w, sizeof(w)));
+    CU(cudaMemcpyToSymbol(c_withhold_tag, &withhold_step, sizeof(withhold_step)));
+    return CISMGPU_OK;
+}
+
+int cismgpu_set_sum_order(int order) {
+    const int v = order == CISMGPU_SUM_SEQUENTIAL ? CISMGPU_SUM_SEQUENTIAL : CISMGPU_SUM_TREE;
+    return g_sum_order.exchange(v);
 }
 
 const char *cismgpu_last_error(void) { return g_last_error.c_str(); }

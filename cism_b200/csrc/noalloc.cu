@@ -15,6 +15,12 @@
 // Limits and sharing rules:
 //  * at most CISMGPU_NOALLOC_MAX_COLUMNS vertex columns ((nx-1)*(ny-1)); larger
 //    grids are rejected with CISMGPU_EINVAL before anything is enqueued;
+//  * parallel%reprosum is rejected (CISMGPU_EUNSUPPORTED): the reproducible sum needs
+//    host steps between its kernels, which an asynchronous call cannot take; with the
+//    sequential sum order (cismgpu_set_sum_order) the sum runs in one CTA and uses no
+//    scratch at all;
+//  * the three buffers must be readable by the current device (its own memory, managed
+//    or mapped pinned memory);
 //  * every call on a device shares the one array, so two calls whose kernels
 //    overlap on the GPU (different streams, no ordering between them) race and
 //    give wrong sums; calls on one stream, or otherwise ordered, are safe;
@@ -63,12 +69,20 @@ static int noalloc_scratch(NoAllocScratch **out) {
     return CISMGPU_OK;
 }
 
-// The pointer must be readable by the device: device, managed or mapped pinned memory.
+// The pointer must be readable by the current device: its own device memory, managed memory
+// or mapped pinned memory.  Device memory of another GPU is rejected (the kernel would read
+// it over the peer link, or fault where peer access is off).
 static int noalloc_check_ptr(const void *p, const char *name) {
     cudaPointerAttributes a;
     CU(cudaPointerGetAttributes(&a, p));
     if (a.type == cudaMemoryTypeUnregistered || (a.type == cudaMemoryTypeHost && !a.devicePointer))
         return fail(CISMGPU_EINVAL, std::string(name) + " is not device-accessible memory");
+    if (a.type == cudaMemoryTypeDevice) {
+        int dev = 0;
+        CU(cudaGetDevice(&dev));
+        if (a.device != dev)
+            return fail(CISMGPU_EINVAL, std::string(name) + " is memory of another device than the current one");
+    }
     return CISMGPU_OK;
 }
 
@@ -81,6 +95,11 @@ extern "C" int cismgpu_global_sum_stagger_noalloc(int nx, int ny, int nz, const 
     g_last_error.clear();
     if (!par || !arr1_dev || !arr2_dev || !sum_dev) return fail(CISMGPU_EINVAL, "null pointer argument");
     if (nx < 6 || ny < 6 || nz < 1) return fail(CISMGPU_EINVAL, "grid too small");
+    if (par->tasks_row * par->tasks_col != 1)
+        return fail(CISMGPU_EUNSUPPORTED, "the whole domain must be on one GPU (tasks_row*tasks_col == 1)");
+    if (par->reprosum)
+        return fail(CISMGPU_EUNSUPPORTED, "parallel%reprosum: the reproducible sum needs host steps; "
+                                          "use cismgpu_global_sum_stagger");
     if (par->staggered_ilo < 1 || par->staggered_ihi > nx - 1 || par->staggered_ilo > par->staggered_ihi ||
         par->staggered_jlo < 1 || par->staggered_jhi > ny - 1 || par->staggered_jlo > par->staggered_jhi)
         return fail(CISMGPU_EINVAL, "owned vertex bounds outside the array");
@@ -97,6 +116,14 @@ extern "C" int cismgpu_global_sum_stagger_noalloc(int nx, int ny, int nz, const 
     const cudaStream_t stream = static_cast<cudaStream_t>(cuda_stream);
     const Geom g = make_geom(nx, ny, nz, par);
     const unsigned nb = nblocks(g.NQ);
+    if (g_sum_order.load() == CISMGPU_SUM_SEQUENTIAL) {  // the reference's order; no scratch
+        SeqArgs sa{};
+        sa.a[0][0] = arr1_dev;
+        sa.a[0][1] = arr2_dev;
+        k_seq_sum<1, true><<<1, kBlock, 0, stream>>>(g, sa, nullptr, EPI_NONE, EPI_NONE, 0, sum_dev);
+        CU(cudaGetLastError());
+        return CISMGPU_OK;
+    }
     CU(cudaMemsetAsync(&s->ticket, 0, sizeof(unsigned int), stream));
     k_gsum<true><<<nb, kBlock, 0, stream>>>(g, arr1_dev, arr2_dev, s->partials, &s->ticket, sum_dev);
     CU(cudaGetLastError());

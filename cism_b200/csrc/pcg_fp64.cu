@@ -1027,6 +1027,83 @@ __global__ void k_epilogue_value(SolveState *st, int epi, int iter, double S0, d
     epilogue(st, epi, iter, S0, S1);
 }
 
+// ---------------------------------------------------------------------------
+// Global sums in the reference's own order (parallel_global_sum_stagger without reprosum,
+// parallel_mpi.F90:6770 (3D), :6637 (2D), nflds forms :7042 (3D), :6904 (2D)):
+//   local_sum = local_sum + arr1(k,i,j) + arr2(k,i,j)
+// over owned vertices, j outer, then i, then k, every addition rounded in turn, and the
+// work arrays products rounded first (worku = ru*zu, ...).  A chain of dependent additions
+// has no parallelism, so one thread adds while the other warps of the CTA stage the next
+// chunk of summands in shared memory (two buffers).  With two fields (Chronopoulos-Gear's
+// nflds = 2 calls) the two chains are independent and run interleaved in the same thread.
+// ---------------------------------------------------------------------------
+constexpr int kSeqChunk = 512;  // summands per term per chunk
+
+struct SeqArgs {
+    const double *a[2][2];  // field f: u term a[f][0], v term a[f][1]
+    const double *b[2][2];  // and their second factors (null: the term is a itself)
+};
+
+// FLAYOUT: element (k, q) at k + nz*q (the caller's arrays); otherwise planes k*NQ + q.
+// epi2 != EPI_NONE: the two sums finish two epilogues, epi with S0 then epi2 with S1 (the
+// first pass of Chronopoulos-Gear); otherwise one epilogue epi(S0, S1).  out (optional)
+// receives S0.  One CTA of kBlock threads.
+template <int NF, bool FLAYOUT>
+__global__ void __launch_bounds__(kBlock) k_seq_sum(Geom g, SeqArgs s, SolveState *st, int epi, int epi2, int iter,
+                                                    double *out) {
+    __shared__ double sm[2][NF][2][kSeqChunk];
+    if (st && st->done) return;
+    const long long W = (long long)(g.ihi - g.ilo + 1) * g.nz;  // summands of one owned row j
+    const long long n = (long long)(g.jhi - g.jlo + 1) * W;
+    const long long nchunk = (n + kSeqChunk - 1) / kSeqChunk;
+    // stage chunk c into buffer buf with threads [t0, kBlock)
+    auto stage = [&](long long c, int buf, int t0) {
+        for (int t = threadIdx.x - t0; t < kSeqChunk; t += kBlock - t0) {
+            const long long e = c * kSeqChunk + t;
+            if (e >= n) break;
+            const long long r = e / W, rem = e - r * W;
+            const int i = g.ilo + (int)(rem / g.nz), k = (int)(rem % g.nz), j = g.jlo + (int)r;
+            const long long q = (long long)j * g.NX + i;
+            const long long x = FLAYOUT ? (long long)k + (long long)g.nz * q : (long long)k * g.NQ + q;
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+#pragma unroll
+                for (int h = 0; h < 2; ++h)
+                    sm[buf][f][h][t] = s.b[f][h] ? __dmul_rn(s.a[f][h][x], s.b[f][h][x]) : s.a[f][h][x];
+        }
+    };
+    double s0 = 0.0, s1 = 0.0;
+    if (nchunk > 0) stage(0, 0, 0);
+    __syncthreads();
+    for (long long c = 0; c < nchunk; ++c) {
+        const int buf = (int)(c & 1);
+        if (threadIdx.x >= 32) {
+            if (c + 1 < nchunk) stage(c + 1, buf ^ 1, 32);
+        } else if (threadIdx.x == 0) {
+            const int cnt = (int)min((long long)kSeqChunk, n - c * kSeqChunk);
+            const double *u0 = sm[buf][0][0], *v0 = sm[buf][0][1];
+            const double *u1 = sm[buf][NF - 1][0], *v1 = sm[buf][NF - 1][1];
+#pragma unroll 8
+            for (int t = 0; t < cnt; ++t) {
+                s0 = __dadd_rn(__dadd_rn(s0, u0[t]), v0[t]);
+                if (NF > 1) s1 = __dadd_rn(__dadd_rn(s1, u1[t]), v1[t]);
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (out) *out = s0;
+        if (st) {
+            if (epi2 != EPI_NONE) {
+                epilogue(st, epi, iter, s0, 0.0);
+                if (!st->done) epilogue(st, epi2, iter, s1, 0.0);
+            } else {
+                epilogue(st, epi, iter, s0, s1);
+            }
+        }
+    }
+}
+
 __global__ void k_init_state(SolveState *st, double tol, int maxiters) {
     st->eta0 = 1.0; st->eta1 = 0.0; st->eta2 = 0.0; st->alpha = 0.0; st->beta = 0.0;
     st->rho_old = 0.0; st->sigma = 0.0; st->rho = 0.0; st->delta = 0.0;

@@ -177,6 +177,12 @@ __device__ __forceinline__ int ld_acquire_i(const int *p) {
 }
 
 constexpr long long kWaitCycles = 1LL << 31;  // ~1 s at 2 GHz: a wait longer than this is a failure
+// The wait bound every spin-wait below uses (kWaitCycles unless a test shortened it), and a
+// test hook: with c_withhold_tag != 0, tile 0 of every solve does not publish its record of
+// that step, so the waits for it run out (a flag nothing sets) and the launch ends with
+// CISMGPU_ETIMEOUT.  Both are set by cismgpu_test_set_device_waits; 0 restores the defaults.
+__constant__ long long c_wait_cycles = kWaitCycles;
+__constant__ unsigned c_withhold_tag = 0u;
 
 // ---------------------------------------------------------------------------
 // per-solve state machine, run by thread 0 of every CTA holding the solve
@@ -864,7 +870,8 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
             const unsigned half = (k & 1) ? (unsigned)__double2hiint(pv) : (unsigned)__double2loint(pv);
             TileRec *rp = D.recs + (size_t)c * 2 * D.ntiles + 2 * (size_t)tile + (tag & 1u);
             fence_acq_rel();  // the tile's vector stores (every thread's, via the barrier above) first
-            st_relaxed64(&rp->w[k], ((unsigned long long)tag << 32) | half);
+            if (!(tile == 0 && tag == c_withhold_tag))
+                st_relaxed64(&rp->w[k], ((unsigned long long)tag << 32) | half);
         }
     }
     __syncthreads();
@@ -919,7 +926,7 @@ __device__ bool sum_records(const TileRec *R, int ntl, unsigned tag, MCtl *ctl, 
             __nanosleep(spins < 16 ? 20 : 100);
             if ((++spins & 31u) == 0) {
                 if (*(volatile int *)&ctl->abort) { bad = 1; break; }
-                if (clock64() - t0 > kWaitCycles) {
+                if (clock64() - t0 > c_wait_cycles) {
                     atomicExch(&ctl->abort, 1);
                     bad = 1;
                     break;
@@ -1202,7 +1209,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict
                     __nanosleep(spins < 16 ? 20 : 100);
                     if ((++spins & 31u) == 0) {
                         if (*(volatile int *)&ctl->abort) { st = 2; break; }
-                        if (clock64() - t0 > kWaitCycles) {
+                        if (clock64() - t0 > c_wait_cycles) {
                             atomicExch(&ctl->abort, 1);
                             st = 2;
                             break;

@@ -54,6 +54,30 @@ __global__ void __launch_bounds__(kBlock) k_repro_extremes(Geom g, const double 
     }
 }
 
+// Before a one-shot reproducible sum of caller arrays: an owned summand arr1 + arr2 that is
+// not finite is recorded in *flag (1 NaN, 2 +Inf, 4 -Inf, as k_repro_products) and both of
+// its parts are set to zero in the device copies, so the integer expansion only meets finite
+// values; the caller then returns the IEEE sum of the non-finite summands instead.
+__global__ void __launch_bounds__(kBlock) k_repro_screen(Geom g, double *__restrict__ a1, double *__restrict__ a2,
+                                                         int *flag) {
+    const long long n = (long long)g.nz * g.NQ;
+    int f = 0;
+    for (long long node = (long long)blockIdx.x * kBlock + threadIdx.x; node < n;
+         node += (long long)gridDim.x * kBlock) {
+        const long long q = node / g.nz;
+        const int j = (int)(q / g.NX), i = (int)(q - (long long)j * g.NX);
+        if (!owned(g, i, j)) continue;
+        const double v = __dadd_rn(a1[node], a2[node]);
+        if (v - v == 0.0) continue;
+        if (v != v) f |= 1;
+        else if (v > 0.0) f |= 2;
+        else f |= 4;
+        a1[node] = 0.0;
+        a2[node] = 0.0;
+    }
+    if (f) atomicOr(flag, f);
+}
+
 // Pass 2: the integer expansion of every summand (cism_reprosum_int:1199-1262) into the level
 // sums lv[level - min_level], first in shared memory, then in global memory.  Unsigned 64-bit
 // atomics add two's-complement values exactly; no level sum leaves the int64 range, since

@@ -49,7 +49,7 @@
               assemble_stiffness_matrix_2d, assemble_stiffness_matrix_3d, &
               dirichlet_boundary_conditions_2d, dirichlet_boundary_conditions_3d, &
               basal_sliding_bc_2d, basal_sliding_bc_3d, &
-              cismgpu_use_mixed_precision
+              cismgpu_use_mixed_precision, cismgpu_use_reference_sum_order
 
     type, bind(C) :: cismgpu_par_t
        integer(c_int32_t) :: staggered_ilo, staggered_ihi
@@ -125,6 +125,11 @@
          import :: c_int
          integer(c_int), value :: algorithm
        end function c_set_oneshot_algorithm
+
+       integer(c_int) function c_set_sum_order(order) bind(C, name="cismgpu_set_sum_order")
+         import :: c_int
+         integer(c_int), value :: order
+       end function c_set_sum_order
 
        type(c_ptr) function c_last_error() bind(C, name="cismgpu_last_error")
          import :: c_ptr
@@ -299,6 +304,17 @@
          prev = c_set_oneshot_algorithm(-1_c_int)
       endif
     end subroutine cismgpu_use_mixed_precision
+
+    !-----------------------------------------------------------------------
+    ! .true.: without parallel%reprosum, the FP64 solvers' global sums run in
+    ! the reference's own sequential order (parallel_global_sum_stagger's loop),
+    ! so a solve reproduces the CPU run bit for bit (slower); .false.
+    ! (default): the library's fixed reduction tree.
+    subroutine cismgpu_use_reference_sum_order(on)
+      logical, intent(in) :: on
+      integer(c_int) :: prev
+      prev = c_set_sum_order(merge(1_c_int, 0_c_int, on))
+    end subroutine cismgpu_use_reference_sum_order
 
     function to_c(parallel) result(p)
       type(parallel_type), intent(in) :: parallel

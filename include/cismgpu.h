@@ -36,7 +36,9 @@
  *
  * Global sums in the standard and Chronopoulos-Gear solvers: with par->reprosum == 0
  * every parallel_global_sum_stagger of the reference is the library's fixed double-double
- * reduction tree (launch-independent, reproducible run to run).  With par->reprosum != 0
+ * reduction tree (launch-independent, reproducible run to run), or, after
+ * cismgpu_set_sum_order(CISMGPU_SUM_SEQUENTIAL), the reference's own sequential order, which
+ * reproduces the reference's one-rank solve bit for bit (slower: see cismgpu_set_sum_order).  With par->reprosum != 0
  * (the one-shot solvers and cismgpu_solver_create) each of them is the reference's
  * reproducible sum (cism_reprosum_calc, libglimmer/cism_reprosum_mod.F90:237-1818, as
  * parallel_global_sum_stagger's reprosum branch calls it, parallel_mpi.F90:6703-6738), two
@@ -166,10 +168,14 @@ int cismgpu_matvec_structured_2d(int nx, int ny, const cismgpu_par_t *par,
  * (nz, nx-1, ny-1); nz = 1 for 2D fields.  With par->reprosum == 0 the sum uses the
  * library's fixed double-double reduction tree (the same one every solver uses): launch-
  * independent and reproducible, the correctly rounded exact sum except in rare near-tie
- * cases.  With par->reprosum != 0 it is the reference's reproducible sum
- * (parallel_reduce_reprosum -> cism_reprosum_calc, libglimmer/cism_reprosum_mod.F90:
+ * cases; or, after cismgpu_set_sum_order(CISMGPU_SUM_SEQUENTIAL), the reference's own
+ * sequential order, bit for bit.  With par->reprosum != 0 it is the reference's reproducible
+ * sum (parallel_reduce_reprosum -> cism_reprosum_calc, libglimmer/cism_reprosum_mod.F90:
  * 237-1818): the integer-vector fixed-point sum, its value independent of the order of the
- * summands, bit for bit the reference's on one rank.  *sum receives the result. */
+ * summands, bit for bit the reference's on one rank; an owned summand arr1 + arr2 that is
+ * not finite (undefined in the reference) makes the result the IEEE sum of the non-finite
+ * summands (NaN, +Inf or -Inf).  tasks_row*tasks_col > 1 returns CISMGPU_EUNSUPPORTED.
+ * *sum receives the result. */
 int cismgpu_global_sum_stagger(int nx, int ny, int nz, const cismgpu_par_t *par,
                                const double *arr1, const double *arr2, double *sum);
 
@@ -177,9 +183,13 @@ int cismgpu_global_sum_stagger(int nx, int ny, int nz, const cismgpu_par_t *par,
  * library allocate device memory -- a host whose own allocator has reserved the
  * device, code that must not stall the device mid-step the way cudaMalloc/cudaFree
  * can, or code that only holds device pointers another component gave it.
- * arr1_dev, arr2_dev (layout (nz, nx-1, ny-1)) and sum_dev are device-accessible
- * pointers; the kernel is enqueued on cuda_stream (NULL: the default stream) and
- * *sum_dev is written asynchronously, identical to cismgpu_global_sum_stagger's result.
+ * arr1_dev, arr2_dev (layout (nz, nx-1, ny-1)) and sum_dev are pointers the current
+ * device can read (its own memory, managed or mapped pinned memory; another GPU's memory
+ * returns CISMGPU_EINVAL); the kernel is enqueued on cuda_stream (NULL: the default
+ * stream) and *sum_dev is written asynchronously, identical to cismgpu_global_sum_stagger's
+ * result in the same sum order (cismgpu_set_sum_order).  par->reprosum != 0 returns
+ * CISMGPU_EUNSUPPORTED: the reproducible sum needs host steps this asynchronous call
+ * cannot take; tasks_row*tasks_col > 1 returns CISMGPU_EUNSUPPORTED as everywhere.
  * It allocates nothing: its scratch is a fixed array in the library's device memory,
  * sized for at most CISMGPU_NOALLOC_MAX_COLUMNS vertex columns (nx-1)*(ny-1) (any nz);
  * larger grids return CISMGPU_EINVAL.  All calls on a device share that array: calls
@@ -617,6 +627,39 @@ int cismgpu_solver_destroy(cismgpu_solver_t *s);
  * tolerance implies).  No reference counterpart: a configuration switch of this
  * library.  Returns the previous setting. */
 int cismgpu_set_oneshot_algorithm(int algorithm);
+
+/* Order of the global sums when parallel%reprosum is off.
+ * CISMGPU_SUM_TREE (default): the library's fixed double-double reduction tree, run by many
+ *   CTAs: reproducible run to run and launch-independent, the correctly rounded exact sum
+ *   except in rare near-tie cases.
+ * CISMGPU_SUM_SEQUENTIAL: the reference's own order, parallel_global_sum_stagger's non-reprosum
+ *   loop (libglimmer/parallel_mpi.F90:6770 3D, :6637 2D, nflds forms :7042, :6904):
+ *   local_sum = local_sum + arr1 + arr2 over the owned vertices, j outer, then i, then k, each
+ *   addition rounded in turn, the work arrays' products (worku = ru*zu, ...) rounded first.
+ *   A solve then reproduces the reference's one-rank run bit for bit, whatever the conditioning
+ *   of its trajectory.  The chain of additions runs on one GPU thread (the other threads of its
+ *   CTA stage the summands), so each sum costs one pass at the latency of a dependent FP64 add
+ *   per summand: a mode for parity and reproduction runs, not for speed.
+ * Process-wide; read by the FP64 solvers at each solve (the four one-shot calls and
+ * cismgpu_solver_solve with CISMGPU_ALG_STANDARD / _CHRONGEAR), by cismgpu_global_sum_stagger
+ * and by cismgpu_global_sum_stagger_noalloc.  par->reprosum != 0 takes precedence, as in the
+ * reference.  The mixed-precision solver ignores it.  Any other value selects
+ * CISMGPU_SUM_TREE.  No reference counterpart (the reference has one order per build).
+ * Returns the previous setting. */
+#define CISMGPU_SUM_TREE        0
+#define CISMGPU_SUM_SEQUENTIAL  1
+int cismgpu_set_sum_order(int order);
+
+/* Test hook for the bounded device waits of the mixed-precision kernels (single solves,
+ * batches and serving epochs); no reference counterpart.  Every spin-wait of those kernels
+ * gives up after wait_cycles SM clock cycles (<= 0: the default, 2^31, about 1 s), sets the
+ * launch's abort word, and the launch ends with CISMGPU_ETIMEOUT for every solve it had not
+ * finished; the context stays usable and the next solve starts from a clean state.
+ * withhold_step != 0 makes tile 0 of every solve skip publishing its record of that step
+ * (steps count from 1 in each solve), so the waits for that record run out: a wait on a flag
+ * nothing sets, the way the tests exercise the timeout path without any fault.  (0, 0)
+ * restores normal operation.  Applies to the current device, to launches made after the call. */
+int cismgpu_test_set_device_waits(long long wait_cycles, unsigned int withhold_step);
 
 /* Message for the last nonzero status on the calling thread ("" if none). */
 const char *cismgpu_last_error(void);

@@ -1,14 +1,16 @@
 """Parity of the B200 library against the CPU oracle, called through the C ABI.
 
-Two bars, both on the same seeded inputs:
+Bars, all on the same seeded inputs:
   * bit-exact (x including halo entries, err, niters, status) against the oracle run
     with its restatement of the device reduction tree (oracle.SUM_DDTREE): every
     matvec, preconditioner, halo and vector statement is an exact restatement;
-  * against the reference's own sequential summation order (oracle.SUM_SEQ): with
-    the SIA preconditioner (the reference default) x agrees within 1e-10 relative
-    through convergence; with diagonal or no preconditioning CG trajectories are
-    sensitive to summation order, so the bar there is a converged err < tol on both
-    sides and x within 1e-6 relative.
+  * bit-exact against the reference's own sequential summation order (oracle.SUM_SEQ)
+    when the library sums in that order too (cismgpu_set_sum_order(CISMGPU_SUM_SEQUENTIAL)):
+    the dome at standard/Chronopoulos-Gear x precond 0/1/2 and slabs with ice on the
+    boundary, through convergence;
+  * with the default tree order, against SUM_SEQ: the SIA-preconditioned dome agrees
+    within 1e-10 relative through convergence; diag/none trajectories are sensitive to
+    the summation order, so there both sides converge (err < tol) and x agrees within 1e-6.
 """
 import math
 
@@ -110,6 +112,60 @@ def test_dome_vs_reference_order(gpu_lib, alg, precond):
     assert g[3] < 1e-8 and seq[3] < 1e-8
     bound = 1e-10 if precond == 2 else 1e-6
     assert rel(g[1:3], seq[1:3]) < bound
+
+
+SEQ_DOME = [("standard", 1), ("chrongear", 1), ("standard", 0), ("chrongear", 0), ("standard", 2),
+            ("chrongear", 2)]
+
+
+@pytest.mark.parametrize("alg,precond", SEQ_DOME, ids=[f"{a}-{p}" for a, p in SEQ_DOME])
+def test_dome_bitexact_reference_order(gpu_lib, alg, precond):
+    """The 31x31x11 dome (the reference's CPU case: standard PCG + diagonal precond) with the
+    library summing in the reference's sequential order: x (halo included), err, niters and
+    status identical to the oracle's SUM_SEQ run, the reference's own one-rank arithmetic,
+    through convergence."""
+    P = asm.dome()
+    seq = oracle.pcg(alg, P, precond, maxiters=400, summode=oracle.SUM_SEQ)
+    with cg.sum_order(cg.SUM_SEQUENTIAL):
+        g = gpu_solve(alg, P, precond, maxiters=400)
+    assert seq[0] == 0 and seq[3] < 1e-8
+    assert_bitexact(g, seq)
+    # the default order again afterwards: the tree's result
+    assert_bitexact(gpu_solve(alg, P, precond, maxiters=400),
+                    oracle.pcg(alg, P, precond, maxiters=400, summode=oracle.SUM_DDTREE))
+
+
+SEQ_SLABS = [("3d", "boundary-periodic", dict(seed=2, boundary_ice=True, bc="periodic")),
+             ("3d", "noslip", dict(seed=5, sliding=False)),
+             ("2d", "interior-periodic", dict(seed=1)),
+             ("2d", "boundary-outflow", dict(seed=3, boundary_ice=True, bc="outflow")),
+             ("2d", "boundary-noice", dict(seed=4, boundary_ice=True, bc="no_ice"))]
+
+
+@pytest.mark.parametrize("alg", ["standard", "chrongear"])
+@pytest.mark.parametrize("precond", [1, 3])
+@pytest.mark.parametrize("case", SEQ_SLABS, ids=[f"{c[0]}-{c[1]}" for c in SEQ_SLABS])
+def test_slab_bitexact_reference_order(gpu_lib, alg, precond, case):
+    """3D and 2D slabs with ice on the periodic / outflow / no_ice boundary, diagonal and local
+    tridiagonal preconditioners, random x0: bit-exact against oracle SUM_SEQ in the sequential
+    sum order."""
+    kind, _, kw = case
+    P = problems.slab_3d(**kw) if kind == "3d" else problems.slab_2d(**kw)
+    x0 = problems.random_x0(P, seed=11, scale=10.0)
+    o = oracle.pcg(alg, P, precond, tol=1e-8, maxiters=400, summode=oracle.SUM_SEQ, x0=x0)
+    with cg.sum_order(cg.SUM_SEQUENTIAL):
+        g = gpu_solve(alg, P, precond, tol=1e-8, maxiters=400, x0=x0)
+    assert_bitexact(g, o)
+
+
+def test_reference_order_nan_breakdown(gpu_lib):
+    """A zero right-hand side breaks down with alpha = NaN in the sequential order too."""
+    Z = problems.slab_3d(seed=2)
+    Z.bu[:] = 0.0
+    Z.bv[:] = 0.0
+    with cg.sum_order(cg.SUM_SEQUENTIAL):
+        assert gpu_solve("standard", Z, 1)[0] == oracle.pcg("standard", Z, 1)[0] == 2
+        assert gpu_solve("chrongear", Z, 2)[0] == oracle.pcg("chrongear", Z, 2)[0] == 2
 
 
 def test_dome_trajectory_vs_reference_order(gpu_lib):
@@ -230,6 +286,42 @@ def test_global_sum_stagger(gpu_lib, nz, bc):
     assert abs(g - seq) <= 1e-12 * np.sum(np.abs(a1 + a2))
 
 
+@pytest.mark.parametrize("nz,bc", [(11, "periodic"), (1, "outflow"), (7, "no_ice"), (21, "periodic")])
+def test_global_sum_reference_order(gpu_lib, nz, bc):
+    """parallel_global_sum_stagger in the sequential sum order: bit-identical to the reference's
+    loop (oracle SUM_SEQ), on a grid larger than one staging chunk; the no-allocation entry
+    point gives the same bits on device buffers."""
+    torch = pytest.importorskip("torch")
+    nx, ny = 53, 41
+    par = asm.default_par(nx, ny, bc)
+    rng = np.random.default_rng(100 + nz)
+    a1 = rng.standard_normal((ny - 1, nx - 1, nz)) * np.exp(rng.uniform(-20, 20, (ny - 1, nx - 1, nz)))
+    a2 = rng.standard_normal((ny - 1, nx - 1, nz))
+    seq = oracle.global_sum(nx, ny, nz, par, a1, a2, oracle.SUM_SEQ)
+    with cg.sum_order(cg.SUM_SEQUENTIAL):
+        g = cg.parallel_global_sum_stagger(nx, ny, nz, par, a1, a2)
+        dev = torch.device("cuda:0")
+        t1, t2 = torch.from_numpy(a1).to(dev), torch.from_numpy(a2).to(dev)
+        out = torch.full((1,), float("nan"), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        cg.parallel_global_sum_stagger_noalloc(nx, ny, nz, par, t1.data_ptr(), t2.data_ptr(), out.data_ptr(),
+                                               torch.cuda.current_stream(dev).cuda_stream)
+        torch.cuda.synchronize(dev)
+    assert g == seq
+    assert float(out.cpu()[0]) == seq
+    assert cg.parallel_global_sum_stagger(nx, ny, nz, par, a1, a2) == \
+        oracle.global_sum(nx, ny, nz, par, a1, a2, oracle.SUM_DDTREE)
+
+
+def test_global_sum_multitask_rejected(gpu_lib):
+    nx, ny = 37, 29
+    par = dict(asm.default_par(nx, ny, "periodic"), tasks_row=2)
+    a = np.ones((ny - 1, nx - 1, 1))
+    with pytest.raises(cg.CismGpuError) as e:
+        cg.parallel_global_sum_stagger(nx, ny, 1, par, a, a)
+    assert e.value.status == 3
+
+
 @pytest.mark.parametrize("nz,bc,spread", [(11, "periodic", 20), (1, "outflow", 600), (7, "no_ice", 300)])
 def test_global_sum_reprosum(gpu_lib, nz, bc, spread):
     """parallel_global_sum_stagger with parallel%reprosum: the reference's integer-vector sum
@@ -248,3 +340,32 @@ def test_global_sum_reprosum(gpu_lib, nz, bc, spread):
     z1[j, i, 0], z1[j, i + 1, 0], z1[j + 1, i, 0], z1[j + 1, i + 1, 0] = 1.0, 2.0**-53, 2.0**-106, -1e-40
     t = cg.parallel_global_sum_stagger(nx, ny, nz, par, z1, z2)
     assert t == oracle.global_sum(nx, ny, nz, par, z1, z2, oracle.SUM_REPRO) == 1.0
+
+
+def test_global_sum_reprosum_nonfinite(gpu_lib):
+    """One-shot reproducible sum with non-finite owned summands: the IEEE sum of those summands
+    (NaN for NaN or for +Inf and -Inf together, else the infinity), as the solvers' sums."""
+    nx, ny, nz = 37, 29, 3
+    par = dict(asm.default_par(nx, ny, "periodic"), reprosum=1)
+    rng = np.random.default_rng(5)
+    a1 = rng.standard_normal((ny - 1, nx - 1, nz))
+    a2 = rng.standard_normal((ny - 1, nx - 1, nz))
+    j, i = par["staggered_jlo"] - 1, par["staggered_ilo"] - 1
+    b1 = a1.copy()
+    b1[j, i, 0] = np.inf
+    assert cg.parallel_global_sum_stagger(nx, ny, nz, par, b1, a2) == np.inf
+    b1[j + 1, i, 1] = -np.inf
+    assert math.isnan(cg.parallel_global_sum_stagger(nx, ny, nz, par, b1, a2))
+    c1 = a1.copy()
+    c1[j, i + 2, 2] = np.nan
+    c2 = a2.copy()
+    c2[j + 2, i, 0] = -np.inf
+    assert math.isnan(cg.parallel_global_sum_stagger(nx, ny, nz, par, c1, c2))
+    d2 = a2.copy()
+    d2[j, i, 0] = -np.inf
+    assert cg.parallel_global_sum_stagger(nx, ny, nz, par, a1, d2) == -np.inf
+    # halo summands do not count: a NaN outside the owned range leaves the finite sum
+    e1 = a1.copy()
+    e1[0, 0, 0] = np.nan
+    assert cg.parallel_global_sum_stagger(nx, ny, nz, par, e1, a2) == \
+        oracle.global_sum(nx, ny, nz, par, a1, a2, oracle.SUM_REPRO)

@@ -65,4 +65,14 @@ def test_noalloc_rejects_oversized_and_host_buffers(gpu_lib):
                                                host.ctypes.data_as(ctypes.c_void_p).value, t.data_ptr(),
                                                t.data_ptr(), 0)
     assert e.value.status == 4
+    # parallel%reprosum needs host steps between its kernels: rejected, not summed another way
+    with pytest.raises(cg.CismGpuError) as e:
+        cg.parallel_global_sum_stagger_noalloc(8, 8, 1, dict(asm.default_par(8, 8, "periodic"), reprosum=1),
+                                               t.data_ptr(), t.data_ptr(), t.data_ptr(), 0)
+    assert e.value.status == 3 and "reprosum" in str(e.value)
+    # more than one task: the whole domain must be on this GPU
+    with pytest.raises(cg.CismGpuError) as e:
+        cg.parallel_global_sum_stagger_noalloc(8, 8, 1, dict(asm.default_par(8, 8, "periodic"), tasks_col=2),
+                                               t.data_ptr(), t.data_ptr(), t.data_ptr(), 0)
+    assert e.value.status == 3
     torch.cuda.synchronize(dev)
