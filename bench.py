@@ -1,27 +1,30 @@
-"""Benchmark: solves/sec (and p50/p99 latency) to a 1e-8 FP64 relative residual.
+"""Benchmark: solves/sec (and p50/p99 latency) to a 1e-8 FP64 relative residual, vs the plain
+FP64 GPU PCG.
 
-Workload (default, one GPU): the 401x401-node 2D SSA system, Chronopoulos-Gear PCG
-with the diagonal (Jacobi) preconditioner, first-Picard assembly of a seeded
-smooth random thickness field (500-2000 m) and log-normal basal friction
-(mu = ln 1e3 Pa yr/m, sigma = 1), dx = 1 km.  Synthetic data: the reference runs
-no public dataset for this path.
+Workload (default, one GPU): the batched configuration, 64 uneven 3D Blatter-Pattyn systems
+(sliding ice streams, n ~ U{64..256} vertices per side, 11 levels, each with its own seeded
+log-normal basal friction, first-Picard assembly), Chronopoulos-Gear PCG with the SIA
+preconditioner, tol 1e-8.  Synthetic data: the reference runs no public dataset for this path.
 
-Our arm ("ours"): the mixed-precision persistent Chronopoulos-Gear solver
-(FP32 recurrences, FP64 x, FP64 residual replacement every 5 iterations) on a
-device-resident handle; the plain FP64 GPU PCG (the reference algorithm statement
-by statement, bit-identical to the oracle) is timed beside it on the same handle.
-L2 is flushed (256 MiB write) before every timed solve.
-`e2e` is the same metric through the reference-signature C-ABI call
-(cismgpu_pcg_chrongear_2d) with pinned host buffers: upload of A, b, x0 and the
-download of x inside the timed region.
+Our arm ("ours"): the mixed-precision Chronopoulos-Gear solver (FP32 recurrences, FP64 x, dot
+products and residual replacement every 5 iterations) over all 64 device-resident systems in one
+persistent launch, captured in a CUDA graph; a step is one replay (64 solves from x0 = 0).  Beside
+it in the same line: the plain FP64 GPU PCG (the reference algorithm statement by statement,
+bit-identical to the oracle) one system after another, the mixed solver one system at a time, a
+1-core CPU baseline, and the like-for-like plain FP64 comparison on the 401x401 2D SSA
+configuration (GPU against 1 CPU core).  The inputs (~10 GB of FP32 and ~20 GB of FP64 matrices)
+are larger than L2.  `e2e` is the same metric through the batch API with host buffers: every
+member's A and b uploaded from pinned host memory, the batched solve, every x downloaded.
 
-Reference arm (`--impl reference`): the CPU restatement of the reference PCG
-(oracle/, FP64, reference summation order) on all host cores, one independent
-solve per core; each timed step runs a bounded number of iterations per core and
-is scaled to a full solve by the iteration count of a full solve.
+Reference arm (`--impl reference`): the CPU restatement of the reference PCG (oracle/, FP64,
+the reference's summation order) on all host cores for the same 64 members; each step is a
+bounded sample scaled to full solves by the members' iteration counts (oracle/cfg4_niters.json).
 
-Launch: python bench.py [--gpus N --steps K --warmup W] (torchrun for N > 1:
-each rank solves its own replica, scaling "weak").
+Other workloads: --workload cfg2 (the 401x401 2D SSA system, mixed solver, single solves),
+cfg5 (the served Poisson stream), --mode profile (the commands the ncu summaries capture).
+
+Launch: python bench.py [--gpus N --steps K --warmup W] (torchrun for N > 1: each rank solves
+its own replica of the workload, scaling "weak").
 """
 from __future__ import annotations
 
@@ -104,61 +107,180 @@ def run_profile(args):
 
 
 # ---------------------------------------------------------------------------
-# batched workload: 64 uneven 3D solves in one graph-captured persistent launch
+# batched workload (the default line): 64 uneven 3D solves in one graph-captured launch
 # ---------------------------------------------------------------------------
+CFG4_WORKLOAD = ("cfg4: 64 uneven 3D BP solves, n~U{64..256}^2 x 11 levels, own seeded log-normal beta each, "
+                 "Chronopoulos-Gear + SIA precond, tol 1e-8")
+CFG4_PRECOND, CFG4_MAXIT = 2, 4000
+CFG4_NITERS = os.path.join(ROOT, "oracle", "cfg4_niters.json")
+
+
 def _make_member(args):
     from cism_b200 import assembly as asm
     n, seed = args
     return asm.batch_member(n, seed)
 
 
-def run_batch(args):
-    """64 sliding 3D ice streams, n ~ U{64..256} vertices per side, 11 levels, each with its own
-    seeded log-normal friction; SIA preconditioner, tol 1e-8.  One CUDA-graph replay = one step
-    (all 64 solves from x0 = 0).  Compared with the plain FP64 GPU PCG and with the mixed solver
-    run one system at a time."""
+def cfg4_problems(procs):
+    """The 64 members (seeded sizes and fields), generated in a pool of spawned processes."""
     import multiprocessing as mp
     from cism_b200 import assembly as asm
-    sizes = asm.batch_sizes(args.batch)
+    sizes = asm.batch_sizes(64)
+    with mp.get_context("spawn").Pool(max(1, min(len(sizes), procs))) as pool:
+        return pool.map(_make_member, [(n, s) for s, n in enumerate(sizes)])
+
+
+def cfg4_reference_niters():
+    """Full-solve iteration counts of the reference algorithm (oracle, reference order) per member."""
+    try:
+        with open(CFG4_NITERS) as f:
+            d = json.load(f)
+        return [int(v) for v in d["niters"]]
+    except Exception:
+        return None
+
+
+def active_nodes(P):
+    return int(np.count_nonzero(P.active_vertex)) * (P.nz if P.kind == "3d" else 1)
+
+
+def mixed_bytes(P, niters, ncheck=NCHECK):
+    """Algorithmic HBM bytes of one mixed solve: FP32 iterations x (4*NC*4 + 112 + 24 SIA / +8 diag) and
+    FP64 checks x (4*NC*8 + 40) per active node."""
+    nc = 27 if P.kind == "3d" else 9
+    pre = 24 if P.kind == "3d" else 8
+    checks = int(niters) // ncheck + (1 if niters >= 5 else 0)
+    return active_nodes(P) * (float(niters) * (4 * nc * 4 + 112 + pre) + checks * (4 * nc * 8 + 40))
+
+
+def cpu_cost_sample(P, precond, alg="chrongear", short=2, long=7):
+    """Seconds of the oracle (reference algorithm and order, FP64) for `short` and `long` iterations
+    of one system: their difference gives the cost of an iteration, the rest the set-up."""
+    import oracle
     t0 = time.perf_counter()
-    with mp.get_context("spawn").Pool(min(len(sizes), os.cpu_count() or 1)) as pool:
-        probs = pool.map(_make_member, [(n, s) for s, n in enumerate(sizes)])
-    t_gen = time.perf_counter() - t0
+    oracle.pcg(alg, P, precond, ncheck=NCHECK, tol=0.0, maxiters=short, summode=oracle.SUM_SEQ)
+    t1 = time.perf_counter()
+    oracle.pcg(alg, P, precond, ncheck=NCHECK, tol=0.0, maxiters=long, summode=oracle.SUM_SEQ)
+    t2 = time.perf_counter()
+    per_iter = max((t2 - t1) - (t1 - t0), 1e-9) / (long - short)
+    setup = max((t1 - t0) - short * per_iter, 0.0)
+    return setup, per_iter
+
+
+def cfg4_cpu_baseline(probs, niters):
+    """The oracle on 1 core, a bounded sample: 2 and 7 iterations of every 8th member (by size),
+    per-node set-up and iteration costs scaled to every member's full-solve iteration count."""
+    import oracle
+    oracle.build()
+    order = sorted(range(len(probs)), key=lambda i: active_nodes(probs[i]))
+    pick = order[::8]
+    t0 = time.perf_counter()
+    su = it = nn = 0.0
+    for i in pick:
+        s, p = cpu_cost_sample(probs[i], CFG4_PRECOND)
+        n = active_nodes(probs[i])
+        su, it, nn = su + s, it + p, nn + n
+    dt = time.perf_counter() - t0
+    su_pn, it_pn = su / nn, it / nn
+    total = sum(active_nodes(P) * (su_pn + k * it_pn) for P, k in zip(probs, niters))
+    return {"value": len(probs) / total, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"2 and 7 Chronopoulos-Gear iterations of {len(pick)} of the 64 members ({dt:.1f} s, 1 core, "
+                      "reference algorithm and summation order in FP64), per-node set-up and iteration costs "
+                      "scaled to each member's full-solve iteration count (oracle/cfg4_niters.json)",
+            "solve_s_total": total}
+
+
+def cfg2_side(stream, flush):
+    """The like-for-like plain FP64 comparison on cfg2 (401x401 2D SSA, Chronopoulos-Gear
+    + Jacobi): the FP64 GPU PCG (bit-exact with the oracle) against the oracle on 1 core."""
     import torch
+    import cism_b200 as cg
+    import oracle
+    P = make_problem("cfg2")
+    S = cg.DeviceSolver(P, stream=stream.cuda_stream)
+    try:
+        S.solve(cg.ALG_CHRONGEAR, PRECOND, NCHECK, TOL, 5)  # workspace
+        ms = []
+        for _ in range(3):
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                e, n = S.solve(cg.ALG_CHRONGEAR, PRECOND, NCHECK, TOL, MAXITERS)
+                b.record(stream)
+            stream.synchronize()
+            ms.append(a.elapsed_time(b))
+    finally:
+        S.close()
+    oracle.build()
+    setup, per_iter = cpu_cost_sample(P, PRECOND, short=20, long=220)
+    cpu_s = setup + n * per_iter
+    gpu_s = float(np.median(ms)) / 1e3
+    return {"workload": WORKLOAD, "fp64_gpu_solves_per_s": 1.0 / gpu_s, "fp64_gpu_ms": 1e3 * gpu_s, "niters": n,
+            "err": e, "cpu_1core_solves_per_s": 1.0 / cpu_s,
+            "cpu_sample": "20 and 220 iterations of the oracle (reference algorithm and order, FP64, 1 core), "
+                          f"scaled to {n} iterations", "gpu_over_cpu": cpu_s / gpu_s}
+
+
+def run_cfg4(args):
+    """64 sliding 3D ice streams, n ~ U{64..256} vertices per side, 11 levels, each with its own seeded
+    log-normal friction; SIA preconditioner, tol 1e-8.  A step = one replay of the CUDA graph that runs
+    all 64 solves from x0 = 0 in one persistent launch of the mixed-precision kernel."""
+    import torch
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    t0 = time.perf_counter()
+    probs = cfg4_problems(max(1, (os.cpu_count() or 1) // world))
+    t_gen = time.perf_counter() - t0
     import cism_b200 as cg
     from cism_b200 import build
     build.build()
-    torch.cuda.set_device(0)
+    cg.load_library()
     stream = torch.cuda.Stream()
-    solvers = [cg.DeviceSolver(P) for P in probs]
-    pc, maxit = 2, 4000
-    nodes = sum(int(np.count_nonzero(P.active_vertex)) * P.nz for P in probs)
-    # plain FP64 GPU PCG, one system after another (reference algorithm)
-    fp64_ms, fp64_x, n64 = 0.0, [], []
-    for S in solvers:
-        e, n = S.solve(cg.ALG_CHRONGEAR, pc, NCHECK, TOL, maxit)  # warm
-        torch.cuda.synchronize()
-        t = time.perf_counter()
-        e, n = S.solve(cg.ALG_CHRONGEAR, pc, NCHECK, TOL, maxit)
-        fp64_ms += 1e3 * (time.perf_counter() - t)
-        fp64_x.append(S.x())
-        n64.append(n)
-    # mixed solver, one system at a time
-    one_ms = 0.0
-    for S in solvers:
-        S.solve(cg.ALG_MIXED_CHRONGEAR, pc, NCHECK, TOL, maxit)
-        torch.cuda.synchronize()
-        t = time.perf_counter()
-        S.solve(cg.ALG_MIXED_CHRONGEAR, pc, NCHECK, TOL, maxit)
-        one_ms += 1e3 * (time.perf_counter() - t)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    solvers = [cg.DeviceSolver(P, stream=stream.cuda_stream) for P in probs]
+    pc, maxit, n = CFG4_PRECOND, CFG4_MAXIT, len(probs)
+    nodes = sum(active_nodes(P) for P in probs)
+
+    def timed_each(alg):
+        """Each member alone, one after another (device time by CUDA events on the solve stream)."""
+        ms, out = 0.0, []
+        for S in solvers:
+            S.solve(alg, pc, NCHECK, TOL, 5)  # workspace and FP32 copies of this algorithm
+        for S in solvers:
+            with torch.cuda.stream(stream):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                e, k = S.solve(alg, pc, NCHECK, TOL, maxit)
+                b.record(stream)
+            stream.synchronize()
+            ms += a.elapsed_time(b)
+            out.append((e, k, S.x()))
+        return ms, out
+
+    # plain FP64 GPU PCG (reference algorithm, bit-exact with the oracle), one system after another
+    fp64_ms, fp64 = timed_each(cg.ALG_CHRONGEAR)
+    n64 = [k for _, k, _ in fp64]
+    # the mixed solver one system at a time
+    one_ms, _ = timed_each(cg.ALG_MIXED_CHRONGEAR)
+
+    # the product path: one graph-captured persistent launch over all 64 members
     B = cg.GraphBatch(solvers, precond=pc, ncheck=NCHECK, tol=TOL, maxiters=maxit, stream=stream.cuda_stream)
     for _ in range(max(args.warmup, 3)):
         B.run()
         B.wait()
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
     torch.cuda.synchronize()
+    if pg:
+        pg.barrier()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     t_start, t_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     t_start.record(stream)
@@ -171,43 +293,86 @@ def run_batch(args):
         assert not np.any(sts), sts
     t_end.record(stream)
     stream.synchronize()
+    if pg:
+        pg.barrier()
     clk = clocks.stop()
-    total_ms = t_start.elapsed_time(t_end)
+    total_ms = max_over_ranks(t_start.elapsed_time(t_end), pg, "cuda")
     step_ms = [a.elapsed_time(b) for a, b in evs]
     xb = [S.x() for S in solvers]
     B.close()
-    rel = max(math.sqrt(float(np.sum((a[0] - b[0]) ** 2) + np.sum((a[1] - b[1]) ** 2))) /
-              math.sqrt(float(np.sum(b[0] ** 2) + np.sum(b[1] ** 2))) for a, b in zip(xb, fp64_x))
-    n = len(solvers)
-    value = n * args.steps / (total_ms / 1e3)
-    # algorithmic bytes of one replay: per member, FP32 iterations x 568 B + FP64 checks x 904 B per node
-    by = 0.0
-    for P, it in zip(probs, nits):
-        nn = float(np.count_nonzero(P.active_vertex)) * P.nz
-        checks = int(it) // NCHECK + (1 if it >= 5 else 0)
-        by += nn * (float(it) * (4 * 27 * 4 + 112 + 24) + checks * (4 * 27 * 8 + 40))
+    rel = max(math.sqrt(float(np.sum((a[0] - b[2][0]) ** 2) + np.sum((a[1] - b[2][1]) ** 2))) /
+              math.sqrt(float(np.sum(b[2][0] ** 2) + np.sum(b[2][1] ** 2))) for a, b in zip(xb, fp64))
+    value = whole_job_rate(world, args.steps * n, total_ms)
+    by = sum(mixed_bytes(P, it) for P, it in zip(probs, nits))
     peak, peak_kind = hbm_peak()
-    achieved = by / (np.median(step_ms) / 1e3) / 1e9
+    achieved = by / (float(np.mean(step_ms)) / 1e3) / 1e9
+
+    # end to end through the batch API with host buffers: per step every member's A and b are
+    # uploaded from pinned host memory (cismgpu_solver_set_system), all 64 are solved in one
+    # persistent launch (cismgpu_solver_solve_batch) and every x comes back to host memory
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    host = [tuple(pin(a) for a in (P.Auu, P.Auv, P.Avu, P.Avv, P.bu, P.bv)) for P in probs]
+    xout = [(pin(np.zeros_like(P.bu)), pin(np.zeros_like(P.bv))) for P in probs]
+    e2e_ms = []
+    for k in range(3):
+        torch.cuda.synchronize()
+        ta = time.perf_counter()
+        for S, h in zip(solvers, host):
+            S.set_system(*h, x0_from_solution=False)
+        ee, kk, ss = cg.solve_batch(solvers, cg.ALG_MIXED_CHRONGEAR, pc, NCHECK, TOL, maxit,
+                                    stream=stream.cuda_stream)
+        assert not np.any(ss), ss
+        for S, (xu, xv) in zip(solvers, xout):
+            S.x_into(xu, xv)
+        tb = time.perf_counter()
+        if k > 0:  # the first round re-creates the FP32 copies' workspace
+            e2e_ms.append(1e3 * (tb - ta))
+    h2d = sum(sum(a.nbytes for a in h) for h in host)
+    d2h = sum(xu.nbytes + xv.nbytes for xu, xv in xout)
+    e2e_rate = world * n * 1e3 / float(np.mean(e2e_ms))
+    for S in solvers:
+        S.close()
+
+    if rank != 0:
+        if pg:
+            pg.destroy_process_group()
+        return 0
+    counts = cfg4_reference_niters() or n64
+    cpu = cfg4_cpu_baseline(probs, counts) if world == 1 else None
+    side = cfg2_side(stream, flush) if world == 1 else None
+    fp64_rate = n / (fp64_ms / 1e3)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 recurrences + f64 x/dots/residual", "data": "synthetic",
-        "config": {"workload": f"cfg4: {n} uneven 3D BP solves, n~U{{64..256}}^2 x 11 levels, own log-normal beta each, "
-                               "SIA precond, tol 1e-8", "solver": "one CUDA-graph-captured persistent launch",
-                   "l2": "working set (FP32 matrices ~1.3 GB) larger than L2", "nodes": nodes,
-                   "generation_s": round(t_gen, 1)},
+        "config": {"workload": CFG4_WORKLOAD, "solver": "one CUDA-graph-captured persistent launch (k_mixed_dyn)",
+                   "l2": "inputs larger than L2 (FP32 matrices ~10 GB, FP64 ~20 GB)", "nodes": nodes,
+                   "parallelism": f"replicas x{world}", "generation_s": round(t_gen, 1)},
         "latency_ms": {"p50": float(np.percentile(step_ms, 50)), "p99": float(np.percentile(step_ms, 99))},
-        "niters": {"min": int(np.min(nits)), "max": int(np.max(nits)), "fp64_max": int(max(n64))},
+        "niters": {"min": int(np.min(nits)), "max": int(np.max(nits)), "sum": int(np.sum(nits)),
+                   "fp64_sum": int(sum(n64))},
         "err_max": float(np.max(errs)), "err_vs_fp64_solution_max": rel,
-        "fp64_plain": {"solves_per_s": n / (fp64_ms / 1e3), "ms_for_all": fp64_ms,
+        "fp64_plain": {"solves_per_s": fp64_rate, "ms_for_all": fp64_ms,
                        "solver": "reference Chronopoulos-Gear statement by statement, FP64, one system at a time"},
+        "speedup_vs_fp64_plain": value / world / fp64_rate,
         "mixed_one_at_a_time": {"solves_per_s": n / (one_ms / 1e3), "ms_for_all": one_ms},
-        "speedup_vs_fp64_plain": value / (n / (fp64_ms / 1e3)),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_mixed<27,16> (whole batch in one launch)", "peak_kind": peak_kind},
-        "gpu_launches": 2 * args.steps, "clocks": clk,
+                     "traffic": ncu_traffic("k_mixed_dyn<27,16>:cfg4"), "peak_kind": peak_kind,
+                     "kernel": "k_mixed_dyn<27,16> (the whole batch in one launch; the graph's other kernels are "
+                               "64 halo resets and one result copy)",
+                     "note": "achieved = algorithmic bytes of the replay (FP32 iterations x 568 B + FP64 checks x "
+                             "904 B per active node) / mean replay time by CUDA events; traffic = ncu DRAM bytes"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_rate, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "ms_per_step": float(np.mean(e2e_ms)),
+                "path": "cismgpu_solver_set_system x64 (pinned host A, b) + cismgpu_solver_solve_batch + "
+                        "cismgpu_solver_get_x x64, host wall clock"},
+        "cfg2_fp64_gpu_vs_cpu": side,
+        "gpu_launches": (n + 2) * args.steps, "clocks": clk,
     }
     print(json.dumps(line))
+    if pg:
+        pg.destroy_process_group()
     return 0
 
 
@@ -437,6 +602,78 @@ def whole_job_rate(world, steps, total_ms):
 # ---------------------------------------------------------------------------
 # reference arm: the CPU restatement on all host cores
 # ---------------------------------------------------------------------------
+def _ref_cfg4_worker(args):
+    """One host core's share of the cfg4 members: generate them, then `rounds` samples of each
+    (2 and 7 iterations of the oracle: set-up and per-iteration seconds)."""
+    jobs, rounds = args
+    import oracle
+    from cism_b200 import assembly as asm
+    probs = [(i, asm.batch_member(nn, i)) for i, nn in jobs]
+    out = []
+    for _ in range(rounds):
+        out.append({i: cpu_cost_sample(P, CFG4_PRECOND) for i, P in probs})
+    return out
+
+
+def run_reference(args):
+    """The reference's algorithm on the host cores for the same workload: the C++ restatement of
+    pcg_solver_chrongear_3d (oracle/, FP64, the reference's summation order), one member per core
+    at a time over all cores.  A step is a bounded sample (2 and 7 iterations of every member, all
+    cores busy), scaled to each member's full-solve iteration count; the whole-workload time is the
+    members' summed solve time divided by the cores (64 members on far fewer cores pack evenly)."""
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    if args.workload == "cfg2":
+        return run_reference_cfg2(args)
+    import multiprocessing as mp
+    import oracle
+    from cism_b200 import assembly as asm
+    oracle.build()
+    counts = cfg4_reference_niters()
+    if counts is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/cfg4_niters.json (full-solve iteration counts) "
+                                                               "missing: run oracle/cfg4_niters.py"}))
+        return 0
+    cores = os.cpu_count() or 1
+    sizes = asm.batch_sizes(64)
+    order = sorted(range(len(sizes)), key=lambda i: -sizes[i])
+    shares = [[] for _ in range(cores)]
+    for r, i in enumerate(order):  # snake order: similar work per core
+        c = r % (2 * cores)
+        shares[c if c < cores else 2 * cores - 1 - c].append((i, sizes[i]))
+    rounds = max(args.warmup, 0) + args.steps
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(cores) as pool:
+        res = pool.map(_ref_cfg4_worker, [(sh, rounds) for sh in shares if sh])
+    wall = time.perf_counter() - t0
+    rates, step_s = [], []
+    for r in range(max(args.warmup, 0), rounds):
+        total = 0.0
+        for wres in res:
+            for i, (su, it) in wres[r].items():
+                total += su + counts[i] * it
+        step_s.append(total / cores)
+        rates.append(len(sizes) / (total / cores))
+    value = float(np.median(rates))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * float(np.median(step_s)), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": CFG4_WORKLOAD,
+                   "solver": f"C++ restatement of the reference PCG (oracle/), {cores} cores: FP64, reference "
+                             "summation order, one member per core at a time"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"per step: 2 and 7 Chronopoulos-Gear iterations of each of the 64 members on "
+                                   f"{cores} cores at once, set-up and per-iteration seconds scaled to each member's "
+                                   f"full-solve count (oracle/cfg4_niters.json, {sum(counts)} iterations in all); "
+                                   f"whole run {wall:.0f} s incl. generation"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
 _WORKER_PROBLEM = None
 
 
@@ -451,36 +688,34 @@ def _ref_worker(niters):
     return time.perf_counter() - t0
 
 
-def run_reference(args):
-    world, rank, _ = dist_setup(args)
-    if rank != 0:
-        return 0
+def run_reference_cfg2(args):
+    """cfg2 (--workload cfg2): the C++ restatement on all host cores, one independent solve per core."""
     import multiprocessing as mp
     import oracle
     oracle.build()
+    world = dist_setup(args)[0]
     cores = os.cpu_count() or 1
-    # full-solve iteration count of the reference algorithm (one full solve, untimed)
     P = make_problem()
     st, xu, xv, err, nfull = oracle.pcg("chrongear", P, PRECOND, ncheck=NCHECK, tol=TOL, maxiters=MAXITERS,
                                         summode=oracle.SUM_SEQ)
     sample_iters = 100
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(cores) as pool:
+    with mp.get_context("spawn").Pool(cores) as pool:
         for _ in range(max(args.warmup, 0)):
             pool.map(_ref_worker, [10] * cores)
         rates = []
         t0 = time.perf_counter()
         for _ in range(args.steps):
             times = pool.map(_ref_worker, [sample_iters] * cores)
-            per_iter = max(times) / sample_iters      # all cores run concurrently
-            rates.append(cores / (per_iter * nfull))  # full solves per second, all cores
+            per_iter = max(times) / sample_iters
+            rates.append(cores / (per_iter * nfull))
         wall = time.perf_counter() - t0
     value = float(np.median(rates))
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * wall / max(args.steps, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "solver": "reference PCG restated in C++ (oracle/), FP64, sequential sums"},
+        "config": {"workload": WORKLOAD,
+                   "solver": f"C++ restatement of the reference PCG (oracle/), {cores} cores, FP64, reference order"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                          "sample": f"{sample_iters} Chronopoulos-Gear iterations per core per step, scaled to the "
                                    f"{nfull} iterations of a full solve to 1e-8 (err {err:.2e})"},
@@ -660,21 +895,23 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=None, help="timed steps (default: 5 for cfg4, else 10)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="bench", choices=["bench", "profile"])
-    ap.add_argument("--workload", default="cfg2", choices=["cfg2", "cfg3", "dome", "cfg4", "cfg5"])
+    ap.add_argument("--workload", default="cfg4", choices=["cfg2", "cfg3", "dome", "cfg4", "cfg5"])
     ap.add_argument("--requests", type=int, default=96, help="cfg5: number of requests")
     ap.add_argument("--pool", type=int, default=8, help="cfg5: distinct systems per kind")
     ap.add_argument("--epoch-steps", type=int, default=64, help="cfg5: steps per serving epoch")
     ap.add_argument("--batch", type=int, default=64, help="cfg4: number of systems")
     ap.add_argument("--fp64", action="store_true", help="profile mode: also time one plain FP64 solve")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 5 if args.workload == "cfg4" else 10
     if args.mode == "profile":
         return run_profile(args)
-    if args.workload == "cfg4":
-        return run_batch(args)
+    if args.workload == "cfg4" and args.impl == "ours":
+        return run_cfg4(args)
     if args.workload == "cfg5":
         return run_serve(args)
     if args.impl == "reference":

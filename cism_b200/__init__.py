@@ -927,6 +927,12 @@ class DeviceSolver:
                                                          ctypes.c_void_p(xv.ctypes.data)))
         return xu, xv
 
+    def x_into(self, xu, xv):
+        """The current solution into caller arrays (e.g. pinned host buffers) of the problem's shape."""
+        n = int(np.prod(self._shape))
+        _check(self._lib, self._lib.cismgpu_solver_get_x(self.handle, _ptr(xu, np.float64, n, True),
+                                                         _ptr(xv, np.float64, n, True)))
+
     def profile(self, enable=True):
         _check(self._lib, self._lib.cismgpu_solver_profile(self.handle, int(enable)))
 

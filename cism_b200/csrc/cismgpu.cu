@@ -882,6 +882,10 @@ struct Solver {
             return fail(CISMGPU_EBREAKDOWN_ALPHA, "PCG solver has failed, alpha = NaN");
         if (h_state->status == CISMGPU_EDIVZERO)
             return fail(CISMGPU_EDIVZERO, "divzero in the tridiagonal preconditioner setup");
+        if (h_state->status == CISMGPU_ETIMEOUT)
+            return fail(CISMGPU_ETIMEOUT, "a bounded device wait gave up (the solve was abandoned)");
+        if (h_state->status != CISMGPU_OK)
+            return fail(h_state->status, "solve failed on the device");
         return CISMGPU_OK;
     }
 
