@@ -178,13 +178,16 @@ def first_picard_efvs(flwa: float) -> float:
 
 
 def assemble_bp_3d(thck, usrf, dx, dy, nz, flwa=1.0e-16, beta=None, bc="periodic", name="",
-                   chunk=40000, stiffness_only=False) -> Problem:
+                   chunk=40000, stiffness_only=False, symmetrize=True) -> Problem:
     """Blatter-Pattyn 3D system for the first Picard iteration.
 
     thck, usrf: cell fields (ny, nx) including the 2-cell halo.
     beta: vertex field (ny-1, nx-1) in Pa yr/m for 'beta local' sliding, or None for a
           no-slip bed (Dirichlet u = v = 0 at k = nz, which_ho_babc = 4).
     stiffness_only: return the assembled stiffness blocks before any basal condition.
+    symmetrize: finish with the reference's pre-solve symmetry check (symmetrize_3d), as
+          glissade_velo_higher_solve does; the element sums here run in another order than the
+          reference's scatter, which leaves transpose pairs a rounding apart.
     """
     ny, nx = thck.shape
     NX, NY = nx - 1, ny - 1
@@ -286,9 +289,50 @@ def assemble_bp_3d(thck, usrf, dx, dy, nz, flwa=1.0e-16, beta=None, bc="periodic
         bv[dmask] = 0.0
 
     par = default_par(nx, ny, bc)
+    if symmetrize and not stiffness_only:
+        symmetrize_3d(A, av, par)
     return Problem("3d", nx, ny, nz, np.ascontiguousarray(A[0]), np.ascontiguousarray(A[1]),
                    np.ascontiguousarray(A[2]), np.ascontiguousarray(A[3]), bu, bv,
                    av.astype(np.int32), par, name)
+
+
+def symmetrize_3d(A, active, par, eps11=1.0e-11):
+    """The averaging of check_symmetry_assembled_matrix_3d (glissade_velo_higher.F90:10854-11117),
+    which glissade_velo_higher_solve applies to every assembled 3D system before the solve
+    (:2923-2931; check_symmetry = .true., :197): every coupling of an owned active row and its
+    transpose partner (Auu with Auu, Auv with Avu, Avu with Auv, Avv with Avv, at the neighbour
+    node and the opposite offset) that differ by less than eps11 times the row's diagonal (Auu's
+    for the Auu and Auv entries, Avv's for the Avu and Avv entries) both become 0.5*(val1 + val2).
+    A pair is visited from both of its rows when both are owned and active; each coefficient
+    belongs to one pair, so the in-place loop's result does not depend on its order and the
+    pairs are averaged here all at once.  A: (4, NY, NX, nz, 27) of uu, uv, vu, vv, in place."""
+    _, NY, NX, nz, _ = A.shape
+    own = np.zeros((NY, NX), dtype=bool)
+    jl, jh, il, ih = par["staggered_jlo"] - 1, par["staggered_jhi"], par["staggered_ilo"] - 1, par["staggered_ihi"]
+    own[jl:jh, il:ih] = active[jl:jh, il:ih] != 0
+    orig = A.copy()
+    diag = (np.abs(orig[0][..., 13]), np.abs(orig[3][..., 13]))  # Auu, Avv diagonals (NY, NX, nz)
+    # (block at R, block at the partner, diagonal tested at R, diagonal tested at the partner)
+    groups = ((0, 0, 0, 0), (1, 2, 0, 1), (2, 1, 1, 0), (3, 3, 1, 1))
+    for c in range(27):
+        iA, jA, kA = c % 3 - 1, (c // 3) % 3 - 1, c // 9 - 1
+        cp = 26 - c
+        rj = slice(max(0, -jA), NY - max(0, jA))
+        ri = slice(max(0, -iA), NX - max(0, iA))
+        rk = slice(max(0, -kA), nz - max(0, kA))
+        nj = slice(rj.start + jA, rj.stop + jA)
+        ni = slice(ri.start + iA, ri.stop + iA)
+        nk = slice(rk.start + kA, rk.stop + kA)
+        ownR = own[rj, ri][:, :, None]
+        ownN = own[nj, ni][:, :, None]
+        for bR, bN, dR, dN in groups:
+            v1 = orig[bR][rj, ri, rk, c]
+            v2 = orig[bN][nj, ni, nk, cp]
+            diff = np.abs(v1 - v2)
+            hit = (ownR & (diff < eps11 * diag[dR][rj, ri, rk])) | (ownN & (diff < eps11 * diag[dN][nj, ni, nk]))
+            avg = 0.5 * (v1 + v2)
+            A[bR][rj, ri, rk, c] = np.where(hit, avg, A[bR][rj, ri, rk, c])
+            A[bN][nj, ni, nk, cp] = np.where(hit, avg, A[bN][nj, ni, nk, cp])
 
 
 def assemble_ssa_2d(thck, usrf, dx, dy, beta, flwa=1.0e-16, bc="periodic", name="",
@@ -366,7 +410,7 @@ def _ice_interior(ny, nx):
     return m
 
 
-def dome(ewn=31, nsn=31, nz=11, dx=2000.0, H0=1000.0, R=25000.0, name="dome") -> Problem:
+def dome(ewn=31, nsn=31, nz=11, dx=2000.0, H0=1000.0, R=25000.0, name="dome", symmetrize=True) -> Problem:
     """Parabolic dome H = H0 sqrt(1 - r^2/R^2) on a flat bed, no-slip bed (benchmark cfg 1)."""
     nx, ny = ewn + 2 * NHALO, nsn + 2 * NHALO
     # owned cells are 3..nx-2 (1-based); cell centres at (i - 0.5) dx in vertex coordinates
@@ -379,11 +423,11 @@ def dome(ewn=31, nsn=31, nz=11, dx=2000.0, H0=1000.0, R=25000.0, name="dome") ->
     thck = np.where(r2 < 1.0, H0 * np.sqrt(np.maximum(1.0 - r2, 0.0)), 0.0)
     thck = np.where(_ice_interior(ny, nx), thck, 0.0)
     usrf = thck.copy()
-    return assemble_bp_3d(thck, usrf, dx, dx, nz, flwa=1.0e-16, beta=None, name=name)
+    return assemble_bp_3d(thck, usrf, dx, dx, nz, flwa=1.0e-16, beta=None, name=name, symmetrize=symmetrize)
 
 
 def ice_stream(ewn=201, nsn=201, nz=11, dx=2000.0, H=1500.0, slope_deg=0.5, rough=0.05, seed=3,
-               beta=None, name="ice_stream") -> Problem:
+               beta=None, name="ice_stream", symmetrize=True) -> Problem:
     """Slab ice stream: surface and bed slope slope_deg in x, seeded bed roughness of rough*H."""
     rng = np.random.default_rng(seed)
     nx, ny = ewn + 2 * NHALO, nsn + 2 * NHALO
@@ -394,7 +438,7 @@ def ice_stream(ewn=201, nsn=201, nz=11, dx=2000.0, H=1500.0, slope_deg=0.5, roug
     usrf = np.broadcast_to(usrf0[None, :], (ny, nx)).copy()
     thck = np.where(_ice_interior(ny, nx), usrf - topg, 0.0)
     usrf = np.where(thck > 0, usrf, topg)
-    return assemble_bp_3d(thck, usrf, dx, dx, nz, flwa=1.0e-16, beta=beta, name=name)
+    return assemble_bp_3d(thck, usrf, dx, dx, nz, flwa=1.0e-16, beta=beta, name=name, symmetrize=symmetrize)
 
 
 def ssa_random(ewn=401, nsn=401, dx=1000.0, seed=7, corr_km=20.0, name="ssa") -> Problem:
@@ -415,12 +459,12 @@ def lognormal_beta(shape, seed, mu=math.log(1.0e3), sd=1.0):
     return np.exp(mu + sd * rng.standard_normal(shape))
 
 
-def batch_member(n, seed, nz=11, dx=2000.0) -> Problem:
+def batch_member(n, seed, nz=11, dx=2000.0, symmetrize=True) -> Problem:
     """One member of the batched 3D workload: an n x n x nz ice stream (seeded bed roughness)
     sliding on its own seeded log-normal basal friction field (mu = ln 1e3 Pa yr/m, sigma = 1)."""
     shape = (n + 2 * NHALO - 1, n + 2 * NHALO - 1)
     return ice_stream(ewn=n, nsn=n, nz=nz, dx=dx, seed=seed, beta=lognormal_beta(shape, 1000 + seed),
-                      name=f"member{seed}_{n}")
+                      name=f"member{seed}_{n}", symmetrize=symmetrize)
 
 
 def batch_sizes(count=64, seed=11, lo=64, hi=256):

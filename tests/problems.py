@@ -39,7 +39,11 @@ def halo_blocks_2d(P):
     return P
 
 
-def slab_3d(ewn=9, nsn=8, nz=5, seed=0, bc="periodic", boundary_ice=False, sliding=True, dx=2000.0):
+def slab_3d(ewn=9, nsn=8, nz=5, seed=0, bc="periodic", boundary_ice=False, sliding=True, dx=2000.0,
+            symmetrize=True):
+    """A small 3D slab; with boundary_ice the matrix halo is filled as the reference's staggered halo
+    update does, and (symmetrize) the reference's pre-solve symmetry check runs last, in the
+    reference's order (glissade_velo_higher.F90:2893-2931)."""
     rng = np.random.default_rng(seed)
     nx, ny = ewn + 4, nsn + 4
     H = 800.0 + 400.0 * rng.random((ny, nx))
@@ -54,9 +58,14 @@ def slab_3d(ewn=9, nsn=8, nz=5, seed=0, bc="periodic", boundary_ice=False, slidi
     thck = np.where(ice, H, 0.0)
     usrf = np.where(ice, usrf, usrf - H)
     beta = asm.lognormal_beta((ny - 1, nx - 1), seed + 100) if sliding else None
-    P = asm.assemble_bp_3d(thck, usrf, dx, dx, nz, beta=beta, bc=bc, name=f"slab3d-{bc}-{seed}")
+    P = asm.assemble_bp_3d(thck, usrf, dx, dx, nz, beta=beta, bc=bc, name=f"slab3d-{bc}-{seed}",
+                           symmetrize=symmetrize and not boundary_ice)
     if boundary_ice:
         P = halo_blocks_3d(P)
+        if symmetrize:
+            A = np.stack([P.Auu, P.Auv, P.Avu, P.Avv])
+            asm.symmetrize_3d(A, P.active_vertex, P.par)
+            P.Auu, P.Auv, P.Avu, P.Avv = (np.ascontiguousarray(a) for a in A)
     return P
 
 

@@ -18,9 +18,9 @@ pytestmark = pytest.mark.gpu
 
 BLOCKS = ("Auu", "Auv", "Avu", "Avv")
 CASES = [
-    ("3d-interior", lambda: problems.slab_3d(seed=51)),
-    ("3d-periodic", lambda: problems.slab_3d(seed=52, boundary_ice=True, bc="periodic")),
-    ("3d-outflow", lambda: problems.slab_3d(seed=53, boundary_ice=True, bc="outflow")),
+    ("3d-interior", lambda: problems.slab_3d(seed=51, symmetrize=False)),
+    ("3d-periodic", lambda: problems.slab_3d(seed=52, boundary_ice=True, bc="periodic", symmetrize=False)),
+    ("3d-outflow", lambda: problems.slab_3d(seed=53, boundary_ice=True, bc="outflow", symmetrize=False)),
     ("2d-interior", lambda: problems.slab_2d(seed=54)),
     ("2d-noice", lambda: problems.slab_2d(seed=55, boundary_ice=True, bc="no_ice")),
 ]
@@ -59,7 +59,7 @@ def test_check_symmetry_oneshot_bitexact(gpu_lib, case):
 def test_check_symmetry_oneshot_idempotent(gpu_lib):
     """An interior 3D system has only roundoff asymmetry: one pass averages it all, and a
     second pass finds nothing."""
-    P = problems.slab_3d(seed=56)
+    P = problems.slab_3d(seed=56, symmetrize=False)
     blocks = [np.array(getattr(P, n), copy=True) for n in BLOCKS]
     md, nw = gpu_check(P, blocks)
     assert md > 0.0 and nw == 0
@@ -91,7 +91,7 @@ def test_check_symmetry_on_handle(gpu_lib, case):
 
 
 def test_check_symmetry_errors(gpu_lib):
-    P = problems.slab_3d(seed=57)
+    P = problems.slab_3d(seed=57, symmetrize=False)
     blocks = [np.array(getattr(P, n), copy=True) for n in BLOCKS]
     bad = np.array(asm.indxA_3d(), copy=True)
     bad[0] = 0

@@ -109,7 +109,7 @@ def _symmetrized(P):
 
 
 def test_symmetry_3d_known_answers():
-    P = problems.slab_3d(seed=41)
+    P = problems.slab_3d(seed=41, symmetrize=False)
     S = _symmetrized(P)
     J, I = (P.par["staggered_jlo"] + 1, P.par["staggered_ilo"] + 2)  # an owned active interior row
     assert P.active_vertex[J, I] and P.active_vertex[J, I + 1]
@@ -158,9 +158,9 @@ def test_symmetry_3d_matches_pairwise_form(case):
     pairwise form agree bit for bit (blocks, maxdiff, warning count).  The boundary cases
     carry halo copies whose partners are not transposes, so they also warn by the thousand."""
     if case == "interior":
-        P = problems.slab_3d(seed=42)
+        P = problems.slab_3d(seed=42, symmetrize=False)
     else:
-        P = problems.slab_3d(seed=43, boundary_ice=True, bc=case.split("-")[1])
+        P = problems.slab_3d(seed=43, boundary_ice=True, bc=case.split("-")[1], symmetrize=False)
     rng = np.random.default_rng(7)
     A = _blocks(P)
     for n in BLOCKS:
@@ -206,7 +206,7 @@ def test_symmetry_2d_reports_only():
 def test_symmetry_check_skips_inactive_rows():
     """Rows of inactive vertices are not visited: a coefficient of an inactive row whose
     partner row is inactive too is left as it is, however asymmetric."""
-    P = problems.slab_3d(seed=45)
+    P = problems.slab_3d(seed=45, symmetrize=False)
     S = _symmetrized(P)
     act = P.active_vertex != 0
     j, i, iA, jA = next((j, i, iA, jA) for j, i in zip(*np.nonzero(~act))
@@ -218,3 +218,35 @@ def test_symmetry_check_skips_inactive_rows():
     A["Auu"][j, i, 1, m] = 12345.0
     got, md, nw = _check(P, A)
     assert md == 0.0 and nw == 0 and got["Auu"][j, i, 1, m] == 12345.0
+
+
+@pytest.mark.parametrize("which", ["dome", "member", "slab-periodic", "slab-outflow", "slab-noslip"])
+def test_package_symmetrization_matches_reference_check(which):
+    """The synthetic 3D systems end with the reference's pre-solve symmetry check
+    (cism_b200.assembly.symmetrize_3d, glissade_velo_higher_solve :2923-2931): the vectorized
+    pair averaging gives the oracle's in-place loop result bit for bit, and a second check
+    changes nothing."""
+    from cism_b200 import assembly as asm
+    if which == "dome":
+        make = lambda sym: asm.dome(symmetrize=sym)  # noqa: E731
+    elif which == "member":
+        make = lambda sym: asm.batch_member(30, 5, nz=7, symmetrize=sym)  # noqa: E731
+    elif which == "slab-noslip":
+        make = lambda sym: problems.slab_3d(seed=5, sliding=False, symmetrize=sym)  # noqa: E731
+    else:
+        bc = which.split("-")[1]
+        make = lambda sym: problems.slab_3d(seed=4, bc=bc, boundary_ice=True, symmetrize=sym)  # noqa: E731
+    P, Q = make(True), make(False)
+    ou, ouv, ovu, ov, md, nw = oracle.check_symmetry(Q)
+    np.testing.assert_array_equal(P.Auu, ou)
+    np.testing.assert_array_equal(P.Auv, ouv)
+    np.testing.assert_array_equal(P.Avu, ovu)
+    np.testing.assert_array_equal(P.Avv, ov)
+    ru, ruv, rvu, rv, md2, nw2 = oracle.check_symmetry(P)
+    for a, b in zip((ru, ruv, rvu, rv), (P.Auu, P.Auv, P.Avu, P.Avv)):
+        np.testing.assert_array_equal(a, b)
+    # an assembly with an ice-free outer ring leaves nothing above the tolerance; the slabs with
+    # ice on the boundary take their halo rows from the halo update (periodic copies of the far
+    # side, outflow zeros), which the element sums of the owned rows do not match
+    if not which.startswith("slab-") or which == "slab-noslip":
+        assert nw == 0 and nw2 == 0 and md2 == 0.0
