@@ -71,6 +71,7 @@ def run_profile(args):
     from cism_b200 import build
     build.build()
     torch.zeros(1, device="cuda")  # CUDA context up before any timing
+    cg.set_mixed_layout(cg.MIXED_LAYOUT_FULL if args.layout == "full" else cg.MIXED_LAYOUT_AUTO)
     if args.workload == "cfg4":  # a small batch of cfg4 members through one graph-captured launch
         from cism_b200 import assembly as asm
         sizes = asm.batch_sizes(args.batch)
@@ -144,10 +145,11 @@ def active_nodes(P):
     return int(np.count_nonzero(P.active_vertex)) * (P.nz if P.kind == "3d" else 1)
 
 
-def mixed_bytes(P, niters, ncheck=NCHECK):
+def mixed_bytes(P, niters, ncheck=NCHECK, half=False):
     """Algorithmic HBM bytes of one mixed solve: FP32 iterations x (4*NC*4 + 112 + 24 SIA / +8 diag) and
-    FP64 checks x (4*NC*8 + 40) per active node."""
-    nc = 27 if P.kind == "3d" else 9
+    FP64 checks x (4*NC*8 + 40) per active node, NC the couplings stored per node (27 in 3D, 14 for
+    the symmetric half of an exactly symmetric 3D matrix, 9 in 2D)."""
+    nc = (14 if half else 27) if P.kind == "3d" else 9
     pre = 24 if P.kind == "3d" else 8
     checks = int(niters) // ncheck + (1 if niters >= 5 else 0)
     return active_nodes(P) * (float(niters) * (4 * nc * 4 + 112 + pre) + checks * (4 * nc * 8 + 40))
@@ -299,11 +301,12 @@ def run_cfg4(args):
     total_ms = max_over_ranks(t_start.elapsed_time(t_end), pg, "cuda")
     step_ms = [a.elapsed_time(b) for a, b in evs]
     xb = [S.x() for S in solvers]
+    half = [S.mixed_symmetric_half() for S in solvers]
     B.close()
     rel = max(math.sqrt(float(np.sum((a[0] - b[2][0]) ** 2) + np.sum((a[1] - b[2][1]) ** 2))) /
               math.sqrt(float(np.sum(b[2][0] ** 2) + np.sum(b[2][1] ** 2))) for a, b in zip(xb, fp64))
     value = whole_job_rate(world, args.steps * n, total_ms)
-    by = sum(mixed_bytes(P, it) for P, it in zip(probs, nits))
+    by = sum(mixed_bytes(P, it, half=h) for P, it, h in zip(probs, nits, half))
     peak, peak_kind = hbm_peak()
     achieved = by / (float(np.mean(step_ms)) / 1e3) / 1e9
 
@@ -360,8 +363,11 @@ def run_cfg4(args):
                      "traffic": ncu_traffic("k_mixed_dyn<27,16>:cfg4"), "peak_kind": peak_kind,
                      "kernel": "k_mixed_dyn<27,16> (the whole batch in one launch; the graph's other kernels are "
                                "64 halo resets and one result copy)",
-                     "note": "achieved = algorithmic bytes of the replay (FP32 iterations x 568 B + FP64 checks x "
-                             "904 B per active node) / mean replay time by CUDA events; traffic = ncu DRAM bytes"},
+                     "note": "achieved = algorithmic bytes of the replay (per active node: FP32 iterations x "
+                             "(16 B x stored couplings + 136 B) + FP64 checks x (32 B x stored couplings + 40 B); "
+                             f"{sum(half)} of {n} members stored as the symmetric half, 14 of 27 couplings) / mean "
+                             "replay time by CUDA events; traffic = ncu DRAM bytes"},
+        "algorithmic_bytes_per_step": by,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_rate, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": float(np.mean(e2e_ms)),
@@ -905,6 +911,8 @@ def main():
     ap.add_argument("--epoch-steps", type=int, default=64, help="cfg5: steps per serving epoch")
     ap.add_argument("--batch", type=int, default=64, help="cfg4: number of systems")
     ap.add_argument("--fp64", action="store_true", help="profile mode: also time one plain FP64 solve")
+    ap.add_argument("--layout", default="auto", choices=["auto", "full"],
+                    help="profile mode: mixed matrix layout (auto: symmetric half when exactly symmetric)")
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 5 if args.workload == "cfg4" else 10

@@ -225,6 +225,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_set_oneshot_algorithm.restype = ctypes.c_int
     lib.cismgpu_set_sum_order.argtypes = [i32]
     lib.cismgpu_set_sum_order.restype = ctypes.c_int
+    lib.cismgpu_set_mixed_layout.argtypes = [i32]
+    lib.cismgpu_set_mixed_layout.restype = ctypes.c_int
+    lib.cismgpu_solver_mixed_layout.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+    lib.cismgpu_solver_mixed_layout.restype = ctypes.c_int
     lib.cismgpu_test_set_device_waits.argtypes = [ctypes.c_longlong, ctypes.c_uint]
     lib.cismgpu_test_set_device_waits.restype = ctypes.c_int
     lib.cismgpu_last_error.restype = ctypes.c_char_p
@@ -337,6 +341,17 @@ class sum_order:
     def __exit__(self, *exc):
         set_sum_order(self.prev)
         return False
+
+
+MIXED_LAYOUT_AUTO, MIXED_LAYOUT_FULL = 0, 1  # CISMGPU_MIXED_LAYOUT_*
+
+
+def set_mixed_layout(layout: int = MIXED_LAYOUT_AUTO) -> int:
+    """Matrix layout of the mixed solver's copies: MIXED_LAYOUT_AUTO stores an exactly symmetric 3D
+    matrix as its symmetric half (bit-identical results, about half the matrix bytes);
+    MIXED_LAYOUT_FULL keeps every coupling.  Read when a handle builds its copies; returns the
+    previous setting."""
+    return int(load_library().cismgpu_set_mixed_layout(int(layout)))
 
 
 def debug_set_device_waits(wait_cycles: int = 0, withhold_step: int = 0) -> None:
@@ -926,6 +941,12 @@ class DeviceSolver:
         _check(self._lib, self._lib.cismgpu_solver_get_x(self.handle, ctypes.c_void_p(xu.ctypes.data),
                                                          ctypes.c_void_p(xv.ctypes.data)))
         return xu, xv
+
+    def mixed_symmetric_half(self) -> bool:
+        """True if the mixed copies of this handle hold the symmetric half of the matrix."""
+        v = ctypes.c_int(0)
+        _check(self._lib, self._lib.cismgpu_solver_mixed_layout(self.handle, ctypes.byref(v)))
+        return bool(v.value)
 
     def x_into(self, xu, xv):
         """The current solution into caller arrays (e.g. pinned host buffers) of the problem's shape."""

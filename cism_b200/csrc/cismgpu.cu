@@ -26,6 +26,10 @@ namespace cismgpu {
 
 static thread_local std::string g_last_error;
 
+// cismgpu_set_mixed_layout(CISMGPU_MIXED_LAYOUT_FULL): the mixed solver keeps every coupling even
+// of an exactly symmetric 3D matrix (for layout comparisons); read when a copy is built.
+static std::atomic<bool> g_mixed_full_storage{false};
+
 // CISMGPU_TRACE=1: host-side phase timestamps on stderr (diagnostics only).
 static bool trace_on() {
     static const bool on = [] {
@@ -1405,6 +1409,9 @@ static int tiles_for(const Geom &g, int TY) {
     return ((g.ihi - g.ilo + kTX) / kTX) * ((g.jhi - g.jlo + TY) / TY);
 }
 
+// Couplings per node the mixed kernels read from HBM: 14 with the symmetric half, else NC.
+static int mixed_couplings(const Solver &sv) { return sv.mixed.sym ? 14 : sv.NC; }
+
 static MDesc mixed_desc(const Solver &sv, int precond, int TY) {  // TY: the solve's tile height
     const MixedBufs &m = sv.mixed;
     const long long nvec = sv.nvec;
@@ -1419,7 +1426,8 @@ static MDesc mixed_desc(const Solver &sv, int precond, int TY) {  // TY: the sol
     D.ntiles = D.tiles_x * D.tiles_y;
     D.A32 = m.A32;
     D.A64 = sv.A.as<double>();
-    D.A64i = m.A64i;
+    D.A64i = (m.sym || m.il) ? m.A64i : nullptr;
+    D.sym = m.sym ? 1 : 0;
     D.pre = m.pre;
     D.act = sv.act.as<int32_t>();
     D.b = p.bu;
@@ -1436,7 +1444,7 @@ static MDesc mixed_desc(const Solver &sv, int precond, int TY) {  // TY: the sol
     D.dflag = reinterpret_cast<int *>(m.bc + 2 * kBcastCopies);
     D.maps = m.maps;
     D.nbrs = m.nbrs;
-    D.stream = (size_t)sv.NC * (size_t)nvec * sizeof(float4) > kStreamBytes ? 1 : 0;
+    D.stream = (size_t)mixed_couplings(sv) * (size_t)nvec * sizeof(float4) > kStreamBytes ? 1 : 0;
     return D;
 }
 
@@ -1529,8 +1537,10 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
             return cudaMalloc(p, n);
         };
         CU(alloc((void **)&m.A32, (size_t)NC * nvec * sizeof(float4)));
-        if ((size_t)NC * (size_t)nvec * sizeof(float4) > kStreamBytes)  // streamed matrix: interleaved FP64 copy
+        // the interleaved FP64 copy: for a streamed matrix, and in 3D for the symmetric half
+        if (NC == 27 || (size_t)NC * (size_t)nvec * sizeof(float4) > kStreamBytes)
             CU(alloc((void **)&m.A64i, (size_t)NC * nvec * 2 * sizeof(double2)));
+        CU(alloc((void **)&m.flag, 256));
         CU(alloc((void **)&m.pre, (size_t)6 * nvec * sizeof(float)));
         CU(alloc((void **)&m.vec, (size_t)16 * nvec * sizeof(float)));
         CU(alloc((void **)&m.state, sizeof(MState)));
@@ -1546,7 +1556,20 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
         m.ntiles = 0;
     }
     if (m.stale) {  // new matrix: FP32 copy (couplings leaving the grid set to zero)
-        if (NC == 27) k_to_f32<27><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32, m.A64i);
+        // 3D: an exactly symmetric matrix is stored as its symmetric half (14 of 27 couplings)
+        m.sym = false;
+        if (NC == 27) {
+            CU(cudaMemsetAsync(m.flag, 0, sizeof(int), sv.stream));
+            k_sym_exact3d<<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, sv.act.as<int32_t>(), sv.A.as<double>(), m.flag);
+            CU(cudaGetLastError());
+            int hflag = 1;
+            CU(cudaMemcpyAsync(&hflag, m.flag, sizeof(int), cudaMemcpyDeviceToHost, sv.stream));
+            CU(cudaStreamSynchronize(sv.stream));
+            m.sym = hflag == 0 && !g_mixed_full_storage.load();
+        }
+        m.il = !m.sym && m.A64i != nullptr && (size_t)NC * (size_t)nvec * sizeof(float4) > kStreamBytes;
+        if (m.sym) k_to_half<<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32, m.A64i);
+        else if (NC == 27) k_to_f32<27><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32, m.il ? m.A64i : nullptr);
         else k_to_f32<9><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32, m.A64i);
         CU(cudaGetLastError());
         m.stale = false;
@@ -1717,13 +1740,13 @@ static int mixed_dispatch(bool is3d, int nzm, const MDesc *d, MState *st, const 
 
 static double mixed_iter_bytes(const Solver &sv, int precond) {
     const double pre = precond == 2 ? 24.0 : (precond == 1 ? 8.0 : 0.0);
-    return (double)sv.n_active_owned * sv.g.nz * (4.0 * sv.NC * 4.0 + 40.0 + 32.0 + 40.0 + pre);
+    return (double)sv.n_active_owned * sv.g.nz * (4.0 * mixed_couplings(sv) * 4.0 + 40.0 + 32.0 + 40.0 + pre);
 }
 
 static double mixed_check_bytes(const Solver &sv) {
     // FP64 residual (matrix, x, b, r32) + the fused update (z, d, q, Az loads, q store) + the
     // deferred owner writes of the next step (d, z, x loads, d, x stores)
-    return (double)sv.n_active_owned * sv.g.nz * (4.0 * sv.NC * 8.0 + 16.0 + 16.0 + 8.0 + 20.0 + 28.0);
+    return (double)sv.n_active_owned * sv.g.nz * (4.0 * mixed_couplings(sv) * 8.0 + 16.0 + 16.0 + 8.0 + 20.0 + 28.0);
 }
 
 template <int NCC>
@@ -3249,6 +3272,18 @@ int cismgpu_test_set_device_waits(long long wait_cycles, unsigned int withhold_s
     const long long w = wait_cycles > 0 ? wait_cycles : kWaitCycles;
     CU(cudaMemcpyToSymbol(c_wait_cycles, &w, sizeof(w)));
     CU(cudaMemcpyToSymbol(c_withhold_tag, &withhold_step, sizeof(withhold_step)));
+    return CISMGPU_OK;
+}
+
+int cismgpu_set_mixed_layout(int layout) {
+    return g_mixed_full_storage.exchange(layout == CISMGPU_MIXED_LAYOUT_FULL) ? CISMGPU_MIXED_LAYOUT_FULL
+                                                                               : CISMGPU_MIXED_LAYOUT_AUTO;
+}
+
+int cismgpu_solver_mixed_layout(const cismgpu_solver_t *h, int *symmetric_half) {
+    g_last_error.clear();
+    if (!h || !symmetric_half) return fail(CISMGPU_EINVAL, "null argument");
+    *symmetric_half = (h->sv.mixed.valid && h->sv.mixed.sym) ? 1 : 0;
     return CISMGPU_OK;
 }
 

@@ -90,6 +90,7 @@ struct MDesc {
     const int *maps;     // [ntiles][(kTX+2)*(TY+2)] slot maps (k_slot_maps)
     const int *nbrs;     // [ntiles][kNbrStride] tiles owning the tile's live halo columns (k_tile_nbrs)
     int stream;          // matrix loads evict-first (the FP32 matrix exceeds kStreamBytes)
+    int sym;             // 3D, exactly symmetric: A32 and A64i hold the symmetric half (k_to_half)
 };
 
 struct MState {
@@ -461,8 +462,10 @@ __device__ __forceinline__ void sia_col(const MDesc &D, float *zc, int NS, int s
 // FP64 fma its owner applies later, so the residual sees exactly the updated x.
 // Partials: p0 = (b,b), p1 = (r,r).  Loads of kChR items are issued before any store.
 // IL: read the interleaved FP64 copy (solves whose matrix streams through L2; a matrix L2
-// keeps between checks reads faster from the four planes).
-template <int NC, bool IL>
+// keeps between checks reads faster from the four planes).  HALF (3D, D.sym): the interleaved
+// copy holds the symmetric half only; a lower coupling is read from its transpose partner.
+// The coefficients are the same numbers in either layout, so the result is too.
+template <int NC, bool IL, bool HALF = false>
 __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, int TY, int i0, int j0, int rpar,
                                               const float *sdn, double alpha64, double &p0, double &p1) {
     const Geom &g = D.g;
@@ -522,7 +525,24 @@ __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, i
                                 x1 = fma(alpha64, (double)sdn[(k + kA) * NS + sn], x1);
                                 x2 = fma(alpha64, (double)sdn[(nz + k + kA) * NS + sn], x2);
                             }
-                            if (IL) {
+                            if (HALF) {
+                                double2 au, av;
+                                if (c >= 13) {
+                                    const size_t h = (size_t)(c - 13) * plane + e;
+                                    au = ld_stream(A2 + 2 * h, pol);
+                                    av = ld_stream(A2 + 2 * h + 1, pol);
+                                } else {  // partner n = (k+kA, i+iA, j+jA), coupling 26 - c, blocks swapped
+                                    const size_t h = (size_t)(13 - c) * plane + (size_t)(k + kA) * NQ +
+                                                     (size_t)((j + jA) * g.NX + (i + iA));
+                                    const double2 pu = ld_stream(A2 + 2 * h, pol), pv = ld_stream(A2 + 2 * h + 1, pol);
+                                    au = make_double2(pu.x, pv.x);  // uu, uv(R) = vu(n)
+                                    av = make_double2(pu.y, pv.y);  // vu(R) = uv(n), vv
+                                }
+                                yu[u] = fma(au.x, x1, yu[u]);
+                                yu[u] = fma(au.y, x2, yu[u]);
+                                yv[u] = fma(av.x, x1, yv[u]);
+                                yv[u] = fma(av.y, x2, yv[u]);
+                            } else if (IL) {
                                 const double2 au = ld_stream(A2 + 2 * a, pol), av = ld_stream(A2 + 2 * a + 1, pol);
                                 yu[u] = fma(au.x, x1, yu[u]);
                                 yu[u] = fma(au.y, x2, yu[u]);
@@ -582,7 +602,8 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
     }
 
     if (step == MS_INIT) {
-        if (D.A64i) residual_pass<NC, true>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
+        if (NC == 27 && D.sym) residual_pass<NC, true, true>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
+        else if (D.A64i) residual_pass<NC, true>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
         else residual_pass<NC, false>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
     } else if (step == MS_BC) {
         // update of iteration iter fused with the FP64 check: dn = z + beta d on tile and halo
@@ -632,7 +653,8 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
             }
         }
         __syncthreads();
-        if (D.A64i) residual_pass<NC, true>(D, smap, TY, i0, j0, par ^ 1, sdn, S.alpha, p0, p1);
+        if (NC == 27 && D.sym) residual_pass<NC, true, true>(D, smap, TY, i0, j0, par ^ 1, sdn, S.alpha, p0, p1);
+        else if (D.A64i) residual_pass<NC, true>(D, smap, TY, i0, j0, par ^ 1, sdn, S.alpha, p0, p1);
         else residual_pass<NC, false>(D, smap, TY, i0, j0, par ^ 1, sdn, S.alpha, p0, p1);
         p0 = p1;
         p1 = 0.0;
@@ -815,7 +837,32 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                             zu[u] = szu[(k + OFF) * NS + s];
                             zv[u] = szv[(k + OFF) * NS + s];
                             if (map_live(smap[s])) {
-                                if (resident) {
+                                if (NC == 27 && D.sym) {
+                                    // symmetric half: the diagonal and upper couplings from this node,
+                                    // a lower coupling c from its transpose partner (node n = this
+                                    // node + offset(c), coupling 26 - c, uv and vu swapped); at level
+                                    // 0 a kA = -1 partner row is clamped to level 0, its z row being
+                                    // the zero padding
+#pragma unroll
+                                    for (int c = 0; c < NC; ++c) {
+                                        const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = c / 9 - 1;
+                                        const int zi = (k + OFF + kA) * NS + s + iA + (kTX + 2) * jA;
+                                        const float z1 = szu[zi], z2 = szv[zi];
+                                        float4 a;
+                                        if (c >= 13) {
+                                            a = ld_stream(A4 + (size_t)(c - 13) * plane + e, pol);
+                                        } else {
+                                            const int kk = k + kA < 0 ? 0 : k + kA;
+                                            const float4 pa = ld_stream(A4 + (size_t)(13 - c) * plane + kk * NQ +
+                                                                            (j + jA) * g.NX + (i + iA), pol);
+                                            a = make_float4(pa.x, pa.z, pa.y, pa.w);
+                                        }
+                                        yu[u] = fmaf(a.x, z1, yu[u]);
+                                        yu[u] = fmaf(a.y, z2, yu[u]);
+                                        yv[u] = fmaf(a.z, z1, yv[u]);
+                                        yv[u] = fmaf(a.w, z2, yv[u]);
+                                    }
+                                } else if (resident) {
 #pragma unroll
                                     for (int c = 0; c < NC; ++c) {
                                         const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = (NC == 27) ? c / 9 - 1 : 0;
@@ -1279,6 +1326,62 @@ __global__ void k_to_f32(Geom g, const double *__restrict__ src, float4 *__restr
     }
 }
 
+// Exact symmetry of a 3D system, the condition of the symmetric half storage: every lower
+// coupling c < 13 of an owned active row R equals its transpose partner bit for bit -- Auu with
+// Auu, Auv with Avu, Avu with Auv, Avv with Avv -- at the neighbour node n = R + (iA, jA, kA)
+// and the opposite offset 26 - c.  check_symmetry_assembled_matrix_3d, which the reference runs
+// before every 3D solve (glissade_velo_higher.F90:2923-2931), averages such pairs to equality.
+// A difference, or a partner outside the array, sets *flag.  One thread per column.
+__global__ void k_sym_exact3d(Geom g, const int32_t *__restrict__ act, const double *__restrict__ A, int *flag) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.NQ) return;
+    const int i = (int)(q % g.NX), j = (int)(q / g.NX);
+    if (!owned(g, i, j) || act[q] == 0) return;
+    const long long plane = (long long)g.nz * g.NQ, bs = 27 * plane;
+    int bad = 0;
+    for (int k = 0; k < g.nz && !bad; ++k)
+        for (int c = 0; c < 13; ++c) {
+            const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = c / 9 - 1;
+            const int in = i + iA, jn = j + jA, kn = k + kA;
+            if (kn < 0) continue;  // a coupling leaving the column: zero in both layouts
+            if (in < 0 || in >= g.NX || jn < 0 || jn >= g.NY) { bad = 1; break; }
+            const long long e = (long long)c * plane + (long long)k * g.NQ + q;
+            const long long f = (long long)(26 - c) * plane + (long long)kn * g.NQ + (long long)jn * g.NX + in;
+            if (A[e] != A[f] || A[bs + e] != A[2 * bs + f] || A[2 * bs + e] != A[bs + f] ||
+                A[3 * bs + e] != A[3 * bs + f]) {
+                bad = 1;
+                break;
+            }
+        }
+    if (bad) atomicOr(flag, 1);
+}
+
+// The symmetric half copy (3D): the 14 couplings c = 13..26 (the diagonal and the upper
+// offsets) of every node, FP32 as float4 (uu, uv, vu, vv) in planes [c - 13][nz][NQ] and FP64
+// interleaved as {uu, uv}, {vu, vv}; couplings leaving the array are stored as zero, as in
+// k_to_f32.  The kernels read a lower coupling from its transpose partner.
+__global__ void k_to_half(Geom g, const double *__restrict__ src, float4 *__restrict__ dst,
+                          double2 *__restrict__ dst64) {
+    const long long plane = (long long)g.nz * g.NQ;
+    const long long n = 14 * plane;
+    const size_t bs = (size_t)27 * plane;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const int h = (int)(e / plane), c = 13 + h;
+        const long long r = e % plane;
+        const int k = (int)(r / g.NQ);
+        const long long q = r % g.NQ;
+        const int i = (int)(q % g.NX), j = (int)(q / g.NX);
+        const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = c / 9 - 1;
+        const bool in = i + iA >= 0 && i + iA < g.NX && j + jA >= 0 && j + jA < g.NY && k + kA >= 0 && k + kA < g.nz;
+        const size_t f = (size_t)c * plane + r;
+        const double uu = in ? src[f] : 0.0, uv = in ? src[bs + f] : 0.0;
+        const double vu = in ? src[2 * bs + f] : 0.0, vv = in ? src[3 * bs + f] : 0.0;
+        dst[e] = make_float4((float)uu, (float)uv, (float)vu, (float)vv);
+        dst64[2 * e] = make_double2(uu, uv);
+        dst64[2 * e + 1] = make_double2(vu, vv);
+    }
+}
+
 // diag: inverse of the diagonal coefficient (0 where the diagonal is 0), per component
 // sia : Thomas factors of the column tridiagonal (0,0,-1)/(0,0,0)/(0,0,+1) couplings
 template <int NC>
@@ -1324,7 +1427,10 @@ struct MixedBufs {
     int shape_nc = 0;
     int precond = -1;
     float4 *A32 = nullptr;
-    double2 *A64i = nullptr;   // FP64 matrix interleaved per coupling (k_to_f32)
+    double2 *A64i = nullptr;   // FP64 matrix interleaved per coupling (k_to_f32), or its symmetric half
+    bool sym = false;          // A32 and A64i hold the symmetric half (k_to_half)
+    bool il = false;           // A64i holds the full interleaved FP64 copy (streamed, not symmetric)
+    int *flag = nullptr;       // device word of the symmetry test
     float *pre = nullptr, *vec = nullptr;
     int *maps = nullptr;
     int *nbrs = nullptr;
@@ -1340,10 +1446,13 @@ struct MixedBufs {
     long long maps_cap = 0;
     void release() {
         for (void *p : {(void *)A32, (void *)A64i, (void *)pre, (void *)vec, (void *)recs, (void *)state, (void *)desc,
-                        (void *)tiles, (void *)ctl, (void *)maps, (void *)nbrs, (void *)bc})
+                        (void *)tiles, (void *)ctl, (void *)maps, (void *)nbrs, (void *)bc, (void *)flag})
             if (p) cudaFree(p);
         A32 = nullptr;
         A64i = nullptr;
+        flag = nullptr;
+        sym = false;
+        il = false;
         pre = vec = nullptr;
         maps = nullptr;
         nbrs = nullptr;

@@ -650,6 +650,26 @@ int cismgpu_set_oneshot_algorithm(int algorithm);
 #define CISMGPU_SUM_SEQUENTIAL  1
 int cismgpu_set_sum_order(int order);
 
+/* Matrix layout of the mixed-precision solver's FP32 and FP64 copies (no reference counterpart).
+ * CISMGPU_MIXED_LAYOUT_AUTO (default): a 3D matrix whose every lower coupling of an owned active
+ *   row equals its transpose partner bit for bit (Auu with Auu, Auv with Avu, Avv with Avv at the
+ *   neighbour node and the opposite offset; check_symmetry_assembled_matrix_3d, which the
+ *   reference runs before every 3D solve, glissade_velo_higher.F90:2923-2931, makes it so) is
+ *   stored as its symmetric half: the diagonal and the 13 upper couplings of each node (224 of
+ *   432 FP32 bytes, 448 of 864 FP64), a lower coupling read from its partner.  The coefficients
+ *   are the same numbers either way, so results are bit-identical to the full layout.  Any other
+ *   matrix keeps all 27 couplings.
+ * CISMGPU_MIXED_LAYOUT_FULL: all couplings always.
+ * Process-wide, read whenever a handle builds its mixed copies (first mixed solve after an
+ * upload or a new system).  Returns the previous setting. */
+#define CISMGPU_MIXED_LAYOUT_AUTO 0
+#define CISMGPU_MIXED_LAYOUT_FULL 1
+int cismgpu_set_mixed_layout(int layout);
+
+/* Whether the handle's mixed copies hold the symmetric half (1) or every coupling (0; also
+ * before its first mixed solve). */
+int cismgpu_solver_mixed_layout(const cismgpu_solver_t *s, int *symmetric_half);
+
 /* Test hook for the bounded device waits of the mixed-precision kernels (single solves,
  * batches and serving epochs); no reference counterpart.  Every spin-wait of those kernels
  * gives up after wait_cycles SM clock cycles (<= 0: the default, 2^31, about 1 s), sets the

@@ -13,8 +13,8 @@ The loops these cover are the reference's Chronopoulos-Gear iterations,
 glissade_velo_higher_pcg.F90:2227-2613 (2D) and :3296-3581 (3D).
 
 The x bounds: two solutions whose relative residuals are both below 1e-8 differ by at most
-about cond(A) x 1e-8; the bounds below sit a factor of about 20 above the differences the
-mixed solver showed on these systems.
+about cond(A) x 1e-8; the bounds below sit a factor of 20-30 above the differences the
+mixed solver showed on these systems on a B200 (cfg2 4.5e-10, cfg3 3.1e-12).
 """
 import numpy as np
 import pytest
@@ -28,7 +28,7 @@ from tests.test_gpu_parity import assert_bitexact, gpu_solve
 pytestmark = pytest.mark.gpu
 
 XB_CFG2 = 1e-8
-XB_CFG3 = 1e-8
+XB_CFG3 = 1e-10
 
 
 @pytest.fixture(scope="module")

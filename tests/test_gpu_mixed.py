@@ -198,3 +198,66 @@ def test_mixed_stops_with_updated_x(gpu_lib, maxiters):
     if maxiters % 5 == 0:
         assert abs(true_residual(P, xu, xv) - err) <= 1e-9 * err
         assert abs(true_residual(P, bu, bv) - errs[0]) <= 1e-9 * errs[0]
+
+
+# (name, problem, precond, stored as the symmetric half): the boundary-ice periodic slab takes its
+# halo rows from the far side, so pairs across the periodic seam stay unequal (the reference's check
+# warns about them instead of averaging) and the matrix keeps the full layout
+LAYOUT_CASES = [
+    ("dome", lambda: asm.dome(), 2, True),
+    ("member-sliding", lambda: asm.batch_member(37, seed=9, nz=11), 2, True),
+    ("slab-noslip-diag", lambda: problems.slab_3d(seed=5, sliding=False), 1, True),
+    ("slab-periodic-boundary", lambda: problems.slab_3d(seed=6, boundary_ice=True, bc="periodic", sliding=False), 1,
+     False),
+]
+
+
+def _mixed(P, precond, layout, batch=False):
+    prev = cg.set_mixed_layout(layout)
+    try:
+        S = cg.DeviceSolver(P)
+        try:
+            if batch:
+                errs, nits, sts = cg.solve_batch([S], cg.ALG_MIXED_CHRONGEAR, precond, 5, 1e-8, 4000)
+                assert sts[0] == 0
+                e, n = errs[0], nits[0]
+            else:
+                e, n = S.solve(cg.ALG_MIXED_CHRONGEAR, precond, 5, 1e-8, 4000)
+            return e, n, S.x(), S.mixed_symmetric_half()
+        finally:
+            S.close()
+    finally:
+        cg.set_mixed_layout(prev)
+
+
+@pytest.mark.parametrize("batch", [False, True], ids=["single", "batched"])
+@pytest.mark.parametrize("name,make,precond,sym", LAYOUT_CASES, ids=[c[0] for c in LAYOUT_CASES])
+def test_symmetric_half_layout_bit_identical(gpu_lib, name, make, precond, sym, batch):
+    """An exactly symmetric 3D matrix (the reference symmetrizes every 3D system before its
+    solve) is stored as its symmetric half; the kernels read a lower coupling from its transpose
+    partner, which holds the same number, so err, niters and x equal the full layout's bit for
+    bit, in the single-solve and in the batched kernel."""
+    P = make()
+    half = _mixed(P, precond, cg.MIXED_LAYOUT_AUTO, batch)
+    full = _mixed(P, precond, cg.MIXED_LAYOUT_FULL, batch)
+    assert half[3] is sym and full[3] is False
+    assert half[0] == full[0] and half[1] == full[1] and half[0] < 1e-8
+    np.testing.assert_array_equal(half[2][0], full[2][0])
+    np.testing.assert_array_equal(half[2][1], full[2][1])
+    assert true_residual(P, *half[2]) < 1.0001e-8
+
+
+def test_asymmetric_matrix_keeps_full_layout(gpu_lib):
+    """One lower coupling off its partner by a relative 1e-13 (below the reference check's
+    averaging threshold, but not equal): the matrix keeps every coupling and still solves to the
+    FP64 tolerance against the oracle."""
+    P = asm.dome()
+    p = P.par
+    j, i, k = p["staggered_jlo"] + 12, p["staggered_ilo"] + 14, 4
+    assert P.active_vertex[j, i]
+    P.Auu[j, i, k, 4] *= 1.0 + 1e-13
+    e, n, x, half = _mixed(P, 2, cg.MIXED_LAYOUT_AUTO)
+    assert half is False and e < 1e-8
+    assert true_residual(P, *x) < 1.0001e-8
+    st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, 2, tol=1e-8, maxiters=4000)
+    assert rel(x, (ou, ov), P) < 1e-7
