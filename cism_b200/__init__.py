@@ -152,6 +152,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_server_drain.restype = ctypes.c_int
     lib.cismgpu_server_stats.argtypes = [vp, P(ctypes.c_longlong), P(ctypes.c_size_t), P(i32), P(i32)]
     lib.cismgpu_server_stats.restype = ctypes.c_int
+    lib.cismgpu_server_launch_stats.argtypes = [vp, P(ctypes.c_longlong), P(ctypes.c_longlong)]
+    lib.cismgpu_server_launch_stats.restype = ctypes.c_int
     lib.cismgpu_server_destroy.argtypes = [vp]
     lib.cismgpu_server_destroy.restype = ctypes.c_int
     lib.cismgpu_solver_get_x.argtypes = [vp, d, d]
@@ -1094,6 +1096,12 @@ class Server:
 
     def drain(self):
         _check(self._lib, self._lib.cismgpu_server_drain(self.handle))
+
+    def launch_stats(self):
+        """(kernel launches, launches that held 2D and 3D requests together)."""
+        a, b = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(self._lib, self._lib.cismgpu_server_launch_stats(self.handle, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def stats(self):
         ep, by, ac, qu = ctypes.c_longlong(), ctypes.c_size_t(), ctypes.c_int(), ctypes.c_int()

@@ -1697,9 +1697,26 @@ static int mixed_dyn_launch(const MDesc *d_descs, MState *const *d_states, const
                             const MTile *d_tiles, int ntiles, int TY, MCtl *d_ctl, int max_steps, int grid,
                             cudaStream_t s) {
     const size_t smem = MLayout<NC, NZM>(TY, false).bytes();
+    int TY2 = TY;
     void *args[] = {(void *)&d_descs, (void *)&d_states, (void *)&d_tick0, (void *)&nsolve, (void *)&d_tiles,
-                    (void *)&ntiles, (void *)&TY, (void *)&d_ctl, (void *)&max_steps};
+                    (void *)&ntiles, (void *)&TY, (void *)&TY2, (void *)&d_ctl, (void *)&max_steps};
     CU(cudaLaunchCooperativeKernel((const void *)k_mixed_dyn<NC, NZM>, dim3(grid), dim3(kBlock), args, smem, s));
+    return CISMGPU_OK;
+}
+
+// Shared memory of the 2D + 3D (nz <= 16) dynamic kernel: the larger of the two layouts.
+static size_t mixed_multi_smem(int TY3, int TY2) {
+    return std::max(MLayout<27, 16>(TY3, false).bytes(), MLayout<9, 1>(TY2, false).bytes());
+}
+
+// One launch of 2D and 3D (nz <= 16) solves together: 3D tiles of height at most TY3, 2D at most TY2.
+static int mixed_multi_launch(const MDesc *d_descs, MState *const *d_states, const unsigned *d_tick0, int nsolve,
+                              const MTile *d_tiles, int ntiles, int TY3, int TY2, MCtl *d_ctl, int max_steps,
+                              int grid, cudaStream_t s) {
+    const size_t smem = mixed_multi_smem(TY3, TY2);
+    void *args[] = {(void *)&d_descs, (void *)&d_states, (void *)&d_tick0, (void *)&nsolve, (void *)&d_tiles,
+                    (void *)&ntiles, (void *)&TY3, (void *)&TY2, (void *)&d_ctl, (void *)&max_steps};
+    CU(cudaLaunchCooperativeKernel((const void *)k_mixed_dyn<27, 16, true>, dim3(grid), dim3(kBlock), args, smem, s));
     return CISMGPU_OK;
 }
 
@@ -1707,6 +1724,22 @@ static const void *mixed_dyn_kernel(bool is3d, int nzm) {
     if (!is3d) return (const void *)k_mixed_dyn<9, 1>;
     if (nzm == 16) return (const void *)k_mixed_dyn<27, 16>;
     return (const void *)k_mixed_dyn<27, 32>;
+}
+
+// Co-resident CTAs of a kernel with `smem` dynamic shared memory (sets the kernel's
+// shared-memory attribute; call outside any stream capture).  0 if it does not fit.
+static int coresident_grid(const void *k, size_t smem) {
+    if (smem > 227 * 1024 - 64) return 0;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    int dev = 0, nsm = 0, occ = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kBlock, smem) != cudaSuccess) return 0;
+    return nsm * occ;
+}
+
+static int mixed_multi_grid(int TY3, int TY2) {
+    return coresident_grid((const void *)k_mixed_dyn<27, 16, true>, mixed_multi_smem(TY3, TY2));
 }
 
 // Co-resident CTAs of the dynamic kernel at tile height TY (sets its shared-memory attribute;

@@ -335,6 +335,11 @@ __device__ __forceinline__ double2 ld_stream(const double2 *p, unsigned long lon
     return v;
 }
 
+// Loads of the symmetric half copy: every stored coupling is read twice in a step, by its
+// node and by its transpose partner's node, close together in time.
+__device__ __forceinline__ float4 ld_half(const float4 *p, unsigned long long pol) { return ld_stream(p, pol); }
+__device__ __forceinline__ double2 ld_half(const double2 *p, unsigned long long pol) { return ld_stream(p, pol); }
+
 // Loads of data that other CTAs wrote earlier in the same launch go through L2
 // (ld.global.cg): L1 is not coherent across SMs.
 __device__ __forceinline__ float ldf(const float *p) { return __ldcg(p); }
@@ -529,12 +534,12 @@ __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, i
                                 double2 au, av;
                                 if (c >= 13) {
                                     const size_t h = (size_t)(c - 13) * plane + e;
-                                    au = ld_stream(A2 + 2 * h, pol);
-                                    av = ld_stream(A2 + 2 * h + 1, pol);
+                                    au = ld_half(A2 + 2 * h, pol);
+                                    av = ld_half(A2 + 2 * h + 1, pol);
                                 } else {  // partner n = (k+kA, i+iA, j+jA), coupling 26 - c, blocks swapped
                                     const size_t h = (size_t)(13 - c) * plane + (size_t)(k + kA) * NQ +
                                                      (size_t)((j + jA) * g.NX + (i + iA));
-                                    const double2 pu = ld_stream(A2 + 2 * h, pol), pv = ld_stream(A2 + 2 * h + 1, pol);
+                                    const double2 pu = ld_half(A2 + 2 * h, pol), pv = ld_half(A2 + 2 * h + 1, pol);
                                     au = make_double2(pu.x, pv.x);  // uu, uv(R) = vu(n)
                                     av = make_double2(pu.y, pv.y);  // vu(R) = uv(n), vv
                                 }
@@ -850,10 +855,10 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                                         const float z1 = szu[zi], z2 = szv[zi];
                                         float4 a;
                                         if (c >= 13) {
-                                            a = ld_stream(A4 + (size_t)(c - 13) * plane + e, pol);
+                                            a = ld_half(A4 + (size_t)(c - 13) * plane + e, pol);
                                         } else {
                                             const int kk = k + kA < 0 ? 0 : k + kA;
-                                            const float4 pa = ld_stream(A4 + (size_t)(13 - c) * plane + kk * NQ +
+                                            const float4 pa = ld_half(A4 + (size_t)(13 - c) * plane + kk * NQ +
                                                                             (j + jA) * g.NX + (i + iA), pol);
                                             a = make_float4(pa.x, pa.z, pa.y, pa.w);
                                         }
@@ -1193,11 +1198,14 @@ __device__ bool lead_duties(MHead &hd, const MDesc *__restrict__ descs, MState *
 // in the same fixed order as the single-solve kernel, so every result is bit-identical to
 // solving the system alone with the same tile height.  Stops when all solves are done or
 // after max_steps steps (a serving epoch), after folding in the last step's sums.
-template <int NC, int NZM>
+// MULTI: the launch holds 2D solves and 3D solves of up to NZM levels together (the serving
+// loop's mixed epochs); each work item runs the tile code of its solve's class, 3D tiles laid
+// out for height TYmax and 2D tiles for TY2max in the same dynamic shared memory.
+template <int NC, int NZM, bool MULTI = false>
 __global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict__ descs, MState *const *states,
                                                          const unsigned *__restrict__ ltick0, int nsolve,
                                                          const MTile *__restrict__ tiles, int ntiles, int TYmax,
-                                                         MCtl *ctl, int max_steps) {
+                                                         int TY2max, MCtl *ctl, int max_steps) {
     extern __shared__ __align__(16) unsigned char smem[];
     MHead &hd = *reinterpret_cast<MHead *>(smem);
     __shared__ unsigned long long s_item;
@@ -1281,7 +1289,12 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict
         __syncthreads();
         if (s_flag == 2) return;
         if (s_flag == 1) continue;
-        tile_step<NC, NZM>(s_view, T.tile, false, TYmax, hd, smem);
+        if (MULTI) {
+            if (hd.D.NC == 27) tile_step<27, NZM>(s_view, T.tile, false, TYmax, hd, smem);
+            else tile_step<9, 1>(s_view, T.tile, false, TY2max, hd, smem);
+        } else {
+            tile_step<NC, NZM>(s_view, T.tile, false, TYmax, hd, smem);
+        }
     }
     if (threadIdx.x == 0) s_flag = *(volatile int *)&ctl->abort;
     __syncthreads();

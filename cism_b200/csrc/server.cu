@@ -5,11 +5,13 @@
 //   * admission (its own host thread): in arrival order while the HBM budget allows; an admitted request gets
 //     its own device-resident handle (matrix, FP32 copy, preconditioner, Krylov vectors),
 //     uploaded on the handle's own stream while the GPU runs the current epoch;
-//   * epochs: every active request of a kernel class (2D, 3D nz <= 16, 3D nz <= 32) takes
-//     part in one launch of the dynamic persistent kernel (k_mixed_dyn) for up to
-//     epoch_steps steps; a request's state (scalars in its MState, vectors in its buffers)
-//     stays on the device between epochs, so a request joins and leaves between any two
-//     epochs without restarting anyone;
+//   * epochs: every active request of a kernel class (2D and 3D with nz <= 16 together; 3D
+//     with 16 < nz <= 32) takes part in one launch of the dynamic persistent kernel
+//     (k_mixed_dyn; with 2D and 3D requests both present, its multi-class form, in which
+//     every work item runs its own solve's tile code, so 2D and 3D requests share the SMs in
+//     the same launch) for up to epoch_steps steps; a request's state (scalars in its MState,
+//     vectors in its buffers) stays on the device between epochs, so a request joins and
+//     leaves between any two epochs without restarting anyone;
 //   * retirement: a finished request's x is copied into the caller's arrays, its handle
 //     freed and its bytes returned to the budget.
 // Tile heights and the order of every sum depend on the request only, so a result is
@@ -39,27 +41,26 @@ struct SrvReq {
     double t_submit = 0.0, t_admit = 0.0, t_done = 0.0;  // ms since the server started
     cismgpu_solver *h = nullptr;
     size_t bytes = 0;
-    int cls = 0;       // kernel class: 0 2D, 1 3D nz <= 16, 2 3D nz <= 32
+    int cls = 0;       // kernel class: 0 2D or 3D nz <= 16, 1 3D 16 < nz <= 32
     int TY = 0;
     unsigned tick = 0; // steps completed, as of the last epoch
 };
 
 // Device bytes a request's handle holds at most (the FP64 system, its staging block, the
-// FP64 and FP32 vectors, the FP32 matrix, the interleaved FP64 matrix of a streamed solve,
-// the factors, tile maps and records).
+// FP64 and FP32 vectors, the FP32 matrix, the interleaved FP64 matrix of a 3D or streamed
+// solve, the factors, tile maps and records).
 static size_t request_bytes(const cismgpu_request_t &r) {
     const long long NQ = (long long)(r.nx - 1) * (r.ny - 1);
     const long long nvec = NQ * (r.dims == 3 ? r.nz : 1);
     const long long NC = r.dims == 3 ? 27 : 9;
-    const bool streamed = (size_t)(NC * nvec) * 16 > kStreamBytes;
-    const long long per = 4 * NC * 8 + NC * 8 + NVEC * 8 + 4 * NC * 4 + (streamed ? 4 * NC * 8 : 0) + 6 * 4 + 16 * 4;
+    const bool il = r.dims == 3 || (size_t)(NC * nvec) * 16 > kStreamBytes;
+    const long long per = 4 * NC * 8 + NC * 8 + NVEC * 8 + 4 * NC * 4 + (il ? 4 * NC * 8 : 0) + 6 * 4 + 16 * 4;
     return (size_t)(nvec * per + NQ * 16 + (8 << 20));
 }
 
-static int request_class(const cismgpu_request_t &r) {
-    if (r.dims != 3) return 0;
-    return r.nz <= 16 ? 1 : 2;
-}
+static constexpr int kSrvClasses = 2;
+
+static int request_class(const cismgpu_request_t &r) { return (r.dims == 3 && r.nz > 16) ? 1 : 0; }
 
 }  // namespace cismgpu
 
@@ -76,6 +77,8 @@ struct cismgpu_server {
     long long next_id = 1;
     long long inflight = 0;         // submitted and not yet done
     long long epochs = 0;
+    long long launches = 0;         // kernel launches (one per class and epoch)
+    long long multi_launches = 0;   // launches that held 2D and 3D requests together
     bool stop = false;
     int device = 0;
     std::thread th;                 // epoch loop
@@ -126,12 +129,12 @@ static int srv_admit(SrvReq &r) {
 }
 
 // Launch one epoch of class cls over its active requests (asynchronous on the epoch stream).
-static int srv_launch(cismgpu_server *S, SrvLaunch &L, int cls) {
+// *multi: the launch held 2D and 3D requests together (the multi-class kernel).
+static int srv_launch(cismgpu_server *S, SrvLaunch &L, int cls, bool *multi) {
     const int n = (int)L.members.size();
+    *multi = false;
     if (n == 0) return CISMGPU_OK;
-    const bool is3d = cls != 0;
-    const int nzm = cls == 0 ? 1 : (cls == 1 ? 16 : 32);
-    int TYmax = 1;
+    int TY2 = 1, TY3 = 1, n3 = 0;
     std::vector<MDesc> descs(n);
     std::vector<MState *> sptr(n);
     std::vector<unsigned> tick(n);
@@ -142,10 +145,19 @@ static int srv_launch(cismgpu_server *S, SrvLaunch &L, int cls) {
         descs[t] = mixed_desc(sv, r.rq.precond, r.TY);
         sptr[t] = sv.mixed.state;
         tick[t] = r.tick;
-        TYmax = std::max(TYmax, r.TY);
+        if (sv.is3d) {
+            TY3 = std::max(TY3, r.TY);
+            ++n3;
+        } else {
+            TY2 = std::max(TY2, r.TY);
+        }
         for (int k = 0; k < descs[t].ntiles; ++k) tl.push_back(MTile{t, k});
     }
-    const int grid = mixed_dyn_grid(is3d, nzm, TYmax);
+    const bool is3d = n3 > 0;
+    *multi = n3 > 0 && n3 < n;  // class 0 with both kinds: one multi-class launch
+    const int nzm = cls == 1 ? 32 : 16;
+    const int TYmax = is3d ? TY3 : TY2;
+    const int grid = *multi ? mixed_multi_grid(TY3, TY2) : mixed_dyn_grid(is3d, is3d ? nzm : 1, TYmax);
     if (grid < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM at this tile height");
     if ((long long)n > (long long)grid * kMaxCtaSolves) return fail(CISMGPU_EUNSUPPORTED, "too many requests");
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
@@ -178,9 +190,16 @@ static int srv_launch(cismgpu_server *S, SrvLaunch &L, int cls) {
     std::memcpy(L.h_blk + o_l, tl.data(), tl.size() * sizeof(MTile));
     std::memcpy(L.h_blk + o_c, &c0, sizeof(MCtl));
     CU(cudaMemcpyAsync(base, L.h_blk, o_g, cudaMemcpyHostToDevice, s));
-    TRY(mixed_dyn_dispatch(is3d, nzm, reinterpret_cast<MDesc *>(base + o_d), reinterpret_cast<MState **>(base + o_p),
-                           reinterpret_cast<unsigned *>(base + o_t), n, reinterpret_cast<MTile *>(base + o_l),
-                           (int)tl.size(), TYmax, reinterpret_cast<MCtl *>(base + o_c), S->epoch_steps, grid, s));
+    if (*multi)
+        TRY(mixed_multi_launch(reinterpret_cast<MDesc *>(base + o_d), reinterpret_cast<MState **>(base + o_p),
+                               reinterpret_cast<unsigned *>(base + o_t), n, reinterpret_cast<MTile *>(base + o_l),
+                               (int)tl.size(), TY3, TY2, reinterpret_cast<MCtl *>(base + o_c), S->epoch_steps, grid,
+                               s));
+    else
+        TRY(mixed_dyn_dispatch(is3d, is3d ? nzm : 1, reinterpret_cast<MDesc *>(base + o_d),
+                               reinterpret_cast<MState **>(base + o_p), reinterpret_cast<unsigned *>(base + o_t), n,
+                               reinterpret_cast<MTile *>(base + o_l), (int)tl.size(), TYmax,
+                               reinterpret_cast<MCtl *>(base + o_c), S->epoch_steps, grid, s));
     k_gather_states<<<(n + 127) / 128, 128, 0, s>>>(reinterpret_cast<MState **>(base + o_p),
                                                    reinterpret_cast<MState *>(base + o_g), n);
     CU(cudaGetLastError());
@@ -252,7 +271,7 @@ static void srv_admit_loop(cismgpu_server *S) {
 // ones; requests admitted meanwhile join at the next epoch.
 static void srv_loop(cismgpu_server *S) {
     cudaSetDevice(S->device);
-    SrvLaunch L[3];
+    SrvLaunch L[kSrvClasses];
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(S->mu);
@@ -264,26 +283,30 @@ static void srv_loop(cismgpu_server *S) {
             S->active.insert(S->active.end(), S->ready.begin(), S->ready.end());
             S->ready.clear();
         }
-        for (int c = 0; c < 3; ++c) L[c].members.clear();
+        for (int c = 0; c < kSrvClasses; ++c) L[c].members.clear();
         for (SrvReq *r : S->active) L[r->cls].members.push_back(r);
-        int launched = 0;
-        for (int c = 0; c < 3; ++c) {
+        int launched = 0, multi = 0;
+        for (int c = 0; c < kSrvClasses; ++c) {
             if (L[c].members.empty()) continue;
-            const int rc = srv_launch(S, L[c], c);
+            bool m = false;
+            const int rc = srv_launch(S, L[c], c, &m);
             if (rc) {  // the class cannot run: fail its requests
                 for (SrvReq *r : L[c].members) srv_retire(S, *r, rc, std::nan(""), 0, 0);
                 L[c].members.clear();
             } else {
                 ++launched;
+                multi += m ? 1 : 0;
             }
         }
         if (launched) {
             cudaStreamSynchronize(S->es);
             std::lock_guard<std::mutex> lk(S->mu);
             ++S->epochs;
+            S->launches += launched;
+            S->multi_launches += multi;
         }
         std::vector<SrvReq *> still;
-        for (int c = 0; c < 3; ++c) {
+        for (int c = 0; c < kSrvClasses; ++c) {
             const bool aborted = L[c].h_ctl && !L[c].members.empty() && L[c].h_ctl->abort;
             for (size_t t = 0; t < L[c].members.size(); ++t) {
                 SrvReq *r = L[c].members[t];
@@ -386,6 +409,15 @@ int cismgpu_server_stats(cismgpu_server_t *S, long long *epochs, size_t *bytes_i
     if (bytes_in_use) *bytes_in_use = S->used;
     if (active) *active = (int)S->active.size();
     if (queued) *queued = (int)S->queued.size();
+    return CISMGPU_OK;
+}
+
+int cismgpu_server_launch_stats(cismgpu_server_t *S, long long *launches, long long *multi_class_launches) {
+    using namespace cismgpu;
+    if (!S) return fail(CISMGPU_EINVAL, "null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (launches) *launches = S->launches;
+    if (multi_class_launches) *multi_class_launches = S->multi_launches;
     return CISMGPU_OK;
 }
 

@@ -502,6 +502,9 @@ int cismgpu_server_poll(cismgpu_server_t *s, long long id, int *done, double *er
                         double *latency_ms, double *queue_ms);
 int cismgpu_server_drain(cismgpu_server_t *s);  /* wait until every submitted request is done */
 int cismgpu_server_stats(cismgpu_server_t *s, long long *epochs, size_t *bytes_in_use, int *active, int *queued);
+/* Kernel launches of the serving loop so far (one per kernel class and epoch), and how many of
+ * them held 2D and 3D requests together in one multi-class launch. */
+int cismgpu_server_launch_stats(cismgpu_server_t *s, long long *launches, long long *multi_class_launches);
 int cismgpu_server_destroy(cismgpu_server_t *s); /* finishes the queued requests first */
 
 /* Copy the current solution (caller's Fortran layout, halo entries included) to host memory. */

@@ -1,7 +1,8 @@
 """The continuous-batching serving loop (cismgpu_server_*), called through the C ABI.
 
 Each request's result must be bit-identical whether it is served alone or in a mix
-(requests of different kinds and sizes, submitted while others are on the GPU), must reach
+(requests of different kinds and sizes, submitted while others are on the GPU; 2D and 3D
+requests in the same multi-class launch), must reach
 the FP64 tolerance, and must agree with the FP64 oracle within the accuracy that tolerance
 implies.  Admission respects the HBM budget.
 """
@@ -24,7 +25,7 @@ def mix():
         (asm.batch_member(24, seed=5, nz=7), 2),
         (problems.slab_3d(seed=5, sliding=False), 1),
         (asm.ssa_random(ewn=90, nsn=70, seed=9), 1),
-        (asm.batch_member(31, seed=6, nz=19), 2),   # nz > 16: the third kernel class
+        (asm.batch_member(31, seed=6, nz=19), 2),   # nz > 16: the second kernel class
         (asm.dome(), 2),
     ]
 
@@ -50,6 +51,8 @@ def test_served_alone_equals_mix(gpu_lib):
         ids += [S.submit(P, precond=pc, tol=1e-8, maxiters=5000) for P, pc in cases[3:]]
         S.drain()
         assert S.stats()["epochs"] > 1
+        launches, multi = S.launch_stats()
+        assert multi >= 1 and launches >= S.stats()["epochs"]  # 2D and 3D requests in one launch
         for (P, pc), rid, (au, av, ainfo) in zip(cases, ids, alone):
             xu, xv, info = S.result(rid)
             assert info["status"] == 0 and ainfo["status"] == 0
