@@ -72,10 +72,10 @@ def run_profile(args):
     build.build()
     torch.zeros(1, device="cuda")  # CUDA context up before any timing
     cg.set_mixed_layout(cg.MIXED_LAYOUT_FULL if args.layout == "full" else cg.MIXED_LAYOUT_AUTO)
-    if args.workload == "cfg4":  # a small batch of cfg4 members through one graph-captured launch
+    if args.workload == "cfg4":  # the first --batch members of cfg4 through one graph-captured launch
         from cism_b200 import assembly as asm
-        sizes = asm.batch_sizes(args.batch)
-        solvers = [cg.DeviceSolver(asm.batch_member(n, s)) for s, n in enumerate(sizes)]
+        sizes = asm.batch_sizes(64)[:args.batch]
+        solvers = [cg.DeviceSolver(P) for P in cfg4_problems(os.cpu_count() or 1, args.batch)]
         B = cg.GraphBatch(solvers, precond=2, ncheck=NCHECK, tol=TOL, maxiters=4000)
         for k in range(args.warmup + args.steps):
             t0 = time.perf_counter()
@@ -84,6 +84,7 @@ def run_profile(args):
             wall = time.perf_counter() - t0
         print(f"profile workload=cfg4 batch={len(sizes)} sizes={sizes} niters={list(nits)} err_max={max(errs):.3e} "
               f"wall_ms={1e3 * wall:.1f}")
+        print("tile heights:", cg.tile_table())
         B.close()
         return 0
     P = make_problem(args.workload)
@@ -98,6 +99,7 @@ def run_profile(args):
     torch.cuda.synchronize()
     wall = (time.perf_counter() - t0) / max(args.steps, 1)
     ms, nl, by = S.profile_read()
+    print("tile heights:", cg.tile_table())
     print(f"profile workload={args.workload} precond={pc} niters={n} err={e:.3e} unknowns={P.n_unknowns} "
           f"kernel_ms={ms / max(nl, 1):.3f} wall_ms={1e3 * wall:.3f} GB/s={by / (ms / max(nl, 1) / 1e3) / 1e9:.1f}")
     if args.fp64:
@@ -122,11 +124,12 @@ def _make_member(args):
     return asm.batch_member(n, seed)
 
 
-def cfg4_problems(procs):
-    """The 64 members (seeded sizes and fields), generated in a pool of spawned processes."""
+def cfg4_problems(procs, count=64):
+    """The first `count` of the 64 members (seeded sizes and fields), generated in a pool of spawned
+    processes."""
     import multiprocessing as mp
     from cism_b200 import assembly as asm
-    sizes = asm.batch_sizes(64)
+    sizes = asm.batch_sizes(64)[:count]
     with mp.get_context("spawn").Pool(max(1, min(len(sizes), procs))) as pool:
         return pool.map(_make_member, [(n, s) for s, n in enumerate(sizes)])
 
@@ -374,6 +377,7 @@ def run_cfg4(args):
                 "path": "cismgpu_solver_set_system x64 (pinned host A, b) + cismgpu_solver_solve_batch + "
                         "cismgpu_solver_get_x x64, host wall clock"},
         "cfg2_fp64_gpu_vs_cpu": side,
+        "tile_heights": [ln for ln in cg.tile_table() if ln.startswith("batch:")],
         "gpu_launches": (n + 2) * args.steps, "clocks": clk,
     }
     print(json.dumps(line))

@@ -231,6 +231,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.cismgpu_set_mixed_layout.restype = ctypes.c_int
     lib.cismgpu_solver_mixed_layout.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
     lib.cismgpu_solver_mixed_layout.restype = ctypes.c_int
+    lib.cismgpu_tile_table.argtypes = [ctypes.c_char_p, ctypes.c_size_t]
+    lib.cismgpu_tile_table.restype = ctypes.c_size_t
     lib.cismgpu_test_set_device_waits.argtypes = [ctypes.c_longlong, ctypes.c_uint]
     lib.cismgpu_test_set_device_waits.restype = ctypes.c_int
     lib.cismgpu_last_error.restype = ctypes.c_char_p
@@ -343,6 +345,15 @@ class sum_order:
     def __exit__(self, *exc):
         set_sum_order(self.prev)
         return False
+
+
+def tile_table() -> list:
+    """The mixed solver's tile-height table: one 'key height [# timings]' string per key."""
+    lib = load_library()
+    n = int(lib.cismgpu_tile_table(None, 0))
+    buf = ctypes.create_string_buffer(n)
+    lib.cismgpu_tile_table(buf, n)
+    return [ln for ln in buf.value.decode().split("\n") if ln]
 
 
 MIXED_LAYOUT_AUTO, MIXED_LAYOUT_FULL = 0, 1  # CISMGPU_MIXED_LAYOUT_*

@@ -10,11 +10,16 @@
 #include <cstdio>
 #include <algorithm>
 #include <chrono>
+#include <cctype>
 #include <cmath>
+#include <fstream>
+#include <map>
+#include <sstream>
 #include <cstdlib>
 #include <cstring>
 #include <atomic>
 #include <mutex>
+#include <sys/stat.h>
 #include <string>
 #include <vector>
 
@@ -1500,11 +1505,12 @@ static int mixed_solve_ty(const Geom &g, bool is3d, int nzm) {
 }
 
 // Tile height of a solve in batched and served launches (dynamic kernel): the single-solve
-// height, but at least 4 rows (3D) or 16 rows (2D), so that a tile carries enough work to
-// hide its fixed costs (descriptor, map, broadcast, record).  Depends on the solve only, so a
-// system gives the same bits alone and in any mix.
-static int mixed_batch_ty(const Geom &g, bool is3d, int nzm) {
-    int ty = std::max(mixed_solve_ty(g, is3d, nzm), is3d ? 4 : 16);
+// rule's height, but at least `floor` rows, so that a tile carries enough work to hide its
+// fixed costs (descriptor, map, broadcast, record).  Depends on the solve (and the floor of
+// its dims and nz class) only, so a system gives the same bits alone and in any mix.
+// floor: the least height (batch_floor: tuned per dims and nz class, else 4 rows in 3D and 16 in 2D).
+static int mixed_batch_ty(const Geom &g, bool is3d, int nzm, int floor) {
+    int ty = std::max(mixed_solve_ty(g, is3d, nzm), floor);
     while (ty > 1 && mixed_grid(is3d, nzm, ty) == 0) --ty;
     return ty;
 }
@@ -1782,50 +1788,196 @@ static double mixed_check_bytes(const Solver &sv) {
     return (double)sv.n_active_owned * sv.g.nz * (4.0 * mixed_couplings(sv) * 8.0 + 16.0 + 16.0 + 8.0 + 20.0 + 28.0);
 }
 
-template <int NCC>
-int Solver::run_mixed(int precond, int ncheck, double tol, int maxiters) {
-    trace("run_mixed: begin");
-    const int nzm = mixed_nzm(g, is3d);
-    const int TY = mixed_solve_ty(g, is3d, nzm);
-    trace("run_mixed: tile height chosen");
-    TRY(mixed_prepare(*this, precond, TY));
-    trace("run_mixed: prepared");
-    TRY(mixed_reset(*this, stream));
-    trace("run_mixed: reset enqueued");
-    MixedBufs &m = mixed;
+// One mixed solve at tile height TY on the solver's stream (enqueued; the result lands in the
+// solver's SolveState).  ms: device time of the persistent launch (synchronizes).
+static int mixed_run(Solver &sv, int precond, int ncheck, double tol, int maxiters, int TY, float *ms,
+                     MState *out = nullptr) {
+    const bool is3d = sv.is3d;
+    const int nzm = mixed_nzm(sv.g, is3d);
+    cudaStream_t stream = sv.stream;
+    TRY(mixed_prepare(sv, precond, TY));
+    TRY(mixed_reset(sv, stream));
+    MixedBufs &m = sv.mixed;
     const bool resident = mixed_resident(is3d, nzm, TY, m.ntiles);
-    const MDesc D = mixed_desc(*this, precond, TY);
+    const MDesc D = mixed_desc(sv, precond, TY);
     const MState S0 = mixed_init_state(tol, maxiters, ncheck);
     CU(cudaMemcpyAsync(m.desc, &D, sizeof(MDesc), cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(m.state, &S0, sizeof(MState), cudaMemcpyHostToDevice, stream));
     CU(cudaMemsetAsync(m.ctl, 0, sizeof(MCtl), stream));
     const int max_steps = 4 * maxiters + 16;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
-    if (prof) {
+    if (ms) {
         CU(cudaEventCreate(&e0));
         CU(cudaEventCreate(&e1));
         CU(cudaEventRecord(e0, stream));
     }
-    trace("run_mixed: descriptors copied");
     const int grid = mixed_launch_grid(is3d, nzm, TY, resident, m.ntiles);
     if (grid < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM at this tile height");
     TRY(mixed_dispatch(is3d, nzm, m.desc, m.state, m.tiles, m.ntiles, TY, resident, m.ctl, max_steps, grid, stream));
-    trace("run_mixed: kernel launched");
-    if (prof) CU(cudaEventRecord(e1, stream));
-    k_mstate_to_solve<<<1, 1, 0, stream>>>(m.state, state.as<SolveState>(), m.ctl);
+    if (ms) CU(cudaEventRecord(e1, stream));
+    k_mstate_to_solve<<<1, 1, 0, stream>>>(m.state, sv.state.as<SolveState>(), m.ctl);
     CU(cudaGetLastError());
+    if (out) CU(cudaMemcpyAsync(out, m.state, sizeof(MState), cudaMemcpyDeviceToHost, stream));
+    if (ms) {
+        CU(cudaStreamSynchronize(stream));
+        CU(cudaEventElapsedTime(ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    return CISMGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Tile-height tuner
+// ---------------------------------------------------------------------------
+// The mixed kernels cut a solve's owned vertices into 32 x TY tiles.  TY trades the fixed costs
+// of a tile (slot map, record, broadcast wait) and the halo ring recomputed around it against
+// parallelism (tiles per co-resident CTA) and shared memory per CTA.  The tuner times the
+// candidate heights on the system itself the first time it meets a key, and keeps the winner
+// for the rest of the process and in a cache file, so that a system's tiling -- and with it the
+// order of its sums -- depends on the system alone:
+//  * single solves: key (dims, nz, layout, tile columns, height bucket); every height that fits
+//    on an SM is timed on a short solve of the actual system (kTuneIters iterations, tol 0),
+//    best of two;
+//  * batches and serving: key (dims, nz class): the least height of every member's tiles,
+//    timed on a short launch (kTuneSteps steps) of the first batch that meets the key.
+// The occupancy rule (mixed_solve_ty; batch floors 4 rows in 3D and 16 in 2D) is the default and
+// keeps its place unless a candidate is more than 3 % faster.  The serving loop never times (its
+// launches share the GPU) and uses the table or the default.  CISMGPU_TILE_TUNING=0 turns timing
+// off; the cache file is $CISMGPU_TILE_CACHE, else $HOME/.cache/cismgpu/tiles-<GPU name>.txt.
+constexpr int kTuneIters = 12;
+constexpr int kTuneSteps = 48;
+
+struct TileTuner {
+    std::mutex mu;
+    bool loaded = false;
+    int timing = -1;  // -1 not read yet
+    std::string path;
+    std::map<std::string, int> table;
+    std::vector<std::string> log;  // what was measured in this process, for cismgpu_tile_table
+
+    bool timing_on() {
+        if (timing < 0) {
+            const char *e = std::getenv("CISMGPU_TILE_TUNING");
+            timing = (e && e[0] == '0') ? 0 : 1;
+        }
+        return timing == 1;
+    }
+    void load() {  // caller holds mu
+        if (loaded) return;
+        loaded = true;
+        const char *e = std::getenv("CISMGPU_TILE_CACHE");
+        if (e && e[0]) {
+            path = e;
+        } else {
+            const char *home = std::getenv("HOME");
+            cudaDeviceProp prop;
+            int dev = 0;
+            std::string name = "gpu";
+            if (cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess) name = prop.name;
+            for (char &c : name)
+                if (!std::isalnum((unsigned char)c)) c = '_';
+            if (home && home[0]) path = std::string(home) + "/.cache/cismgpu/tiles-" + name + ".txt";
+        }
+        if (path.empty()) return;
+        std::ifstream f(path);
+        std::string line;
+        while (std::getline(f, line)) {
+            std::istringstream ss(line);
+            std::string key;
+            int v = 0;
+            if (ss >> key >> v && v > 0 && v <= kMaxTY) table[key] = v;
+        }
+    }
+    int get(const std::string &key) {
+        std::lock_guard<std::mutex> lk(mu);
+        load();
+        auto it = table.find(key);
+        return it == table.end() ? 0 : it->second;
+    }
+    void put(const std::string &key, int v, const std::string &note) {
+        std::lock_guard<std::mutex> lk(mu);
+        load();
+        table[key] = v;
+        log.push_back(key + " " + std::to_string(v) + " # " + note);
+        if (path.empty()) return;
+        for (size_t p = path.find('/', 1); p != std::string::npos; p = path.find('/', p + 1))
+            (void)::mkdir(path.substr(0, p).c_str(), 0755);  // the cache directory, best effort
+        std::ofstream f(path, std::ios::app);
+        if (f) f << key << " " << v << " # " << note << "\n";
+    }
+};
+static TileTuner g_tiles;
+
+static std::string tile_key_single(const Solver &sv, int nzm) {
+    const int W = sv.g.ihi - sv.g.ilo + 1, H = sv.g.jhi - sv.g.jlo + 1;
+    const int hb = (int)std::lround(4.0 * std::log2((double)std::max(H, 1)));
+    std::ostringstream k;
+    k << "solve:" << (sv.is3d ? "3d" : "2d") << ":nzm" << nzm << ":nz" << sv.g.nz << ":" << (sv.mixed.sym ? "half" : "full")
+      << ":tx" << (W + kTX - 1) / kTX << ":hb" << hb;
+    return k.str();
+}
+
+static std::string tile_key_batch(bool is3d, int nzm) {
+    return std::string("batch:") + (is3d ? "3d" : "2d") + ":nzm" + std::to_string(nzm);
+}
+
+// The single-solve tile height of sv (prepared with the default height, so its layout is set).
+static int tuned_solve_ty(Solver &sv, int precond, int nzm, int TYdef, int *TY) {
+    const std::string key = tile_key_single(sv, nzm);
+    int v = g_tiles.get(key);
+    if (v > 0 && mixed_grid(sv.is3d, nzm, v, false) > 0) {
+        *TY = v;
+        return CISMGPU_OK;
+    }
+    *TY = TYdef;
+    if (!g_tiles.timing_on()) return CISMGPU_OK;
+    std::vector<int> cand = {TYdef};
+    for (int ty : {1, 2, 3, 4, 6, 8, 12, 16, 24, 32})
+        if (ty != TYdef && ty <= kMaxTY && mixed_grid(sv.is3d, nzm, ty, false) > 0) cand.push_back(ty);
+    float tdef = 0.f, tbest = 0.f;
+    int arg = TYdef;
+    std::ostringstream note;
+    for (int ty : cand) {
+        float t = 0.f, u = 0.f;
+        TRY(mixed_run(sv, precond, 5, 0.0, kTuneIters, ty, &t));
+        TRY(mixed_run(sv, precond, 5, 0.0, kTuneIters, ty, &u));
+        t = std::min(t, u);
+        note << ty << ":" << t << "ms ";
+        if (ty == TYdef) tdef = t;
+        if (ty == TYdef || t < tbest) {
+            tbest = t;
+            arg = ty;
+        }
+    }
+    if (tbest >= 0.97f * tdef) arg = TYdef;  // the default unless a candidate is clearly faster
+    g_tiles.put(key, arg, note.str() + "(default " + std::to_string(TYdef) + ")");
+    *TY = arg;
+    return CISMGPU_OK;
+}
+
+static int batch_floor(bool is3d, int nzm) {
+    const int v = g_tiles.get(tile_key_batch(is3d, nzm));
+    return v > 0 ? v : (is3d ? 4 : 16);
+}
+
+template <int NCC>
+int Solver::run_mixed(int precond, int ncheck, double tol, int maxiters) {
+    trace("run_mixed: begin");
+    const int nzm = mixed_nzm(g, is3d);
+    const int TYdef = mixed_solve_ty(g, is3d, nzm);
+    TRY(mixed_prepare(*this, precond, TYdef));  // the matrix layout, which the key names
+    int TY = TYdef;
+    TRY(tuned_solve_ty(*this, precond, nzm, TYdef, &TY));
+    trace("run_mixed: tile height chosen");
+    MState hs;
+    float ms = 0.f;
+    TRY(mixed_run(*this, precond, ncheck, tol, maxiters, TY, prof ? &ms : nullptr, prof ? &hs : nullptr));
     last_ty = TY;
     if (prof) {
-        MState hs;
-        CU(cudaMemcpyAsync(&hs, m.state, sizeof(MState), cudaMemcpyDeviceToHost, stream));
-        CU(cudaStreamSynchronize(stream));
-        float ms = 0.f;
-        CU(cudaEventElapsedTime(&ms, e0, e1));
         prof_ms += ms;
         prof_n += 1;
         prof_bytes = hs.fp32_matvecs * mixed_iter_bytes(*this, precond) + hs.fp64_matvecs * mixed_check_bytes(*this);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
     }
     return CISMGPU_OK;
 }
@@ -2199,18 +2351,19 @@ struct MixedBatch {
 
 // Prepare every member (FP32 matrix, maps, preconditioner; its own batch tile height), plan
 // the launch and upload the descriptors, initial states and the tile list.
-static int batch_prepare(MixedBatch &B, int precond, int ncheck, double tol, int maxiters) {
+static int batch_prepare(MixedBatch &B, int precond, int ncheck, double tol, int maxiters, int floor = 0) {
     const int n = (int)B.svs.size();
     Solver &s0 = *B.svs[0];
     B.is3d = s0.is3d;
     B.nzm = mixed_nzm(s0.g, s0.is3d);
+    if (floor <= 0) floor = batch_floor(B.is3d, B.nzm);
     std::vector<int> tys(n);
     std::vector<MTile> tl;
     for (int t = 0; t < n; ++t) {
         Solver &sv = *B.svs[t];
         if (sv.is3d != s0.is3d || mixed_nzm(sv.g, sv.is3d) != B.nzm)
             return fail(CISMGPU_EINVAL, "batch members must share dims and the nz class (<=16 or <=32)");
-        tys[t] = mixed_batch_ty(sv.g, sv.is3d, B.nzm);
+        tys[t] = mixed_batch_ty(sv.g, sv.is3d, B.nzm, floor);
         B.TYmax = std::max(B.TYmax, tys[t]);
         TRY(mixed_prepare(sv, precond, tys[t]));
         for (int k = 0; k < tiles_for(sv.g, tys[t]); ++k) tl.push_back(MTile{t, k});
@@ -2278,6 +2431,59 @@ static int batch_enqueue(MixedBatch &B, cudaStream_t s) {
     CU(cudaGetLastError());
     CU(cudaMemcpyAsync(B.h_states, B.d_states, n * sizeof(MState), cudaMemcpyDeviceToHost, s));
     CU(cudaMemcpyAsync(B.h_ctl, B.d_ctl, sizeof(MCtl), cudaMemcpyDeviceToHost, s));
+    return CISMGPU_OK;
+}
+
+// The batch tile floor of the members' dims and nz class, timed on this batch the first time the
+// class is met (the tuner above): each candidate floor runs kTuneSteps steps of the whole batch
+// (tol 0, so no member stops), best of two.  Outside any stream capture.
+static int tune_batch_floor(const std::vector<Solver *> &svs, int precond, int ncheck, cudaStream_t s) {
+    if (svs.empty()) return CISMGPU_OK;
+    const bool is3d = svs[0]->is3d;
+    const int nzm = mixed_nzm(svs[0]->g, is3d);
+    for (Solver *sv : svs)
+        if (sv->is3d != is3d || mixed_nzm(sv->g, sv->is3d) != nzm) return CISMGPU_OK;  // batch_prepare rejects it
+    const std::string key = tile_key_batch(is3d, nzm);
+    if (g_tiles.get(key) > 0 || !g_tiles.timing_on()) return CISMGPU_OK;
+    const int fdef = is3d ? 4 : 16;
+    const std::vector<int> cand = is3d ? std::vector<int>{4, 2, 6, 8} : std::vector<int>{16, 8, 32};
+    float tdef = 0.f, tbest = 0.f;
+    int arg = fdef;
+    std::ostringstream note;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    int rc = CISMGPU_OK;
+    for (int f : cand) {
+        MixedBatch T;
+        T.svs = svs;
+        rc = batch_prepare(T, precond, ncheck, 0.0, 1 << 24, f);
+        if (rc) break;
+        T.max_steps = kTuneSteps;
+        float t = 1e30f;
+        for (int rep = 0; rep < 2 && !rc; ++rep) {
+            if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(CISMGPU_ECUDA, "event record failed");
+            if (!rc) rc = batch_enqueue(T, s);
+            if (!rc && cudaEventRecord(e1, s) != cudaSuccess) rc = fail(CISMGPU_ECUDA, "event record failed");
+            float ms = 0.f;
+            if (!rc && (cudaStreamSynchronize(s) != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess))
+                rc = fail(CISMGPU_ECUDA, "timing a batch tile floor failed");
+            t = std::min(t, ms);
+        }
+        if (rc) break;
+        note << f << ":" << t << "ms ";
+        if (f == fdef) tdef = t;
+        if (f == fdef || t < tbest) {
+            tbest = t;
+            arg = f;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    if (tbest >= 0.97f * tdef) arg = fdef;
+    g_tiles.put(key, arg, note.str() + "(" + std::to_string(svs.size()) + " systems, " +
+                              std::to_string(kTuneSteps) + " steps; default " + std::to_string(fdef) + ")");
     return CISMGPU_OK;
 }
 
@@ -2494,8 +2700,9 @@ int cismgpu_solver_solve_batch(cismgpu_solver_t **solvers, int n, int algorithm,
         if (solvers[t]->in_batch) return fail(CISMGPU_EINVAL, "handle belongs to a graph batch");
         B.svs.push_back(&solvers[t]->sv);
     }
-    TRY(batch_prepare(B, precond, linear_solve_ncheck, tolerance, maxiters));
     cudaStream_t s = cuda_stream ? (cudaStream_t)cuda_stream : B.svs[0]->stream;
+    TRY(tune_batch_floor(B.svs, precond, linear_solve_ncheck, s));
+    TRY(batch_prepare(B, precond, linear_solve_ncheck, tolerance, maxiters));
     TRY(batch_enqueue(B, s));
     CU(cudaStreamSynchronize(s));
     return batch_results(B, errs, niters, statuses);
@@ -2521,6 +2728,8 @@ int cismgpu_batch_create(cismgpu_batch_t **out, cismgpu_solver_t **solvers, int 
             if (solvers[t]->in_batch) rc = fail(CISMGPU_EINVAL, "handle already belongs to a graph batch");
             h->b.svs.push_back(&solvers[t]->sv);
         }
+        if (!rc) rc = tune_batch_floor(h->b.svs, precond, linear_solve_ncheck,
+                                       cuda_stream ? (cudaStream_t)cuda_stream : h->b.svs[0]->stream);
         if (!rc) rc = batch_prepare(h->b, precond, linear_solve_ncheck, tolerance, maxiters);
         if (!rc) {
             if (cuda_stream) {
@@ -3306,6 +3515,26 @@ int cismgpu_test_set_device_waits(long long wait_cycles, unsigned int withhold_s
     CU(cudaMemcpyToSymbol(c_wait_cycles, &w, sizeof(w)));
     CU(cudaMemcpyToSymbol(c_withhold_tag, &withhold_step, sizeof(withhold_step)));
     return CISMGPU_OK;
+}
+
+size_t cismgpu_tile_table(char *buf, size_t len) {
+    std::string out;
+    {
+        std::lock_guard<std::mutex> lk(g_tiles.mu);
+        g_tiles.load();
+        for (const auto &kv : g_tiles.table) {
+            std::string line = kv.first + " " + std::to_string(kv.second);
+            for (const std::string &l : g_tiles.log)
+                if (l.compare(0, kv.first.size() + 1, kv.first + " ") == 0) line = l;
+            out += line + "\n";
+        }
+    }
+    if (buf && len > 0) {
+        const size_t n = std::min(len - 1, out.size());
+        std::memcpy(buf, out.data(), n);
+        buf[n] = '\0';
+    }
+    return out.size() + 1;
 }
 
 int cismgpu_set_mixed_layout(int layout) {

@@ -118,7 +118,7 @@ static int srv_admit(SrvReq &r) {
     r.h = h;
     Solver &sv = h->sv;
     const int nzm = mixed_nzm(sv.g, sv.is3d);
-    r.TY = mixed_batch_ty(sv.g, sv.is3d, nzm);
+    r.TY = mixed_batch_ty(sv.g, sv.is3d, nzm, batch_floor(sv.is3d, nzm));
     TRY(mixed_prepare(sv, q.precond, r.TY));
     TRY(mixed_reset(sv, sv.stream));
     const MState S0 = mixed_init_state(q.tolerance, q.maxiters, q.linear_solve_ncheck);

@@ -669,6 +669,18 @@ int cismgpu_set_sum_order(int order);
 #define CISMGPU_MIXED_LAYOUT_FULL 1
 int cismgpu_set_mixed_layout(int layout);
 
+/* The mixed solver's tile heights (no reference counterpart).  The kernels cut a system's owned
+ * vertices into 32 x TY tiles; a tuner times the candidate heights on the system itself the first
+ * time it meets a key -- single solves: (dims, nz, layout, tile columns, height bucket); batches:
+ * the least height per (dims, nz class), timed on a short launch of the first such batch -- and
+ * keeps the winner for the process and in a cache file ($CISMGPU_TILE_CACHE, else
+ * $HOME/.cache/cismgpu/tiles-<GPU name>.txt), so a system's tiling, and its rounding, depends on
+ * the system alone.  The occupancy rule is the default and stays unless a candidate is more than
+ * 3 % faster; CISMGPU_TILE_TUNING=0 turns timing off; the serving loop uses the table and never
+ * times.  cismgpu_tile_table writes the table, one "key height [# timings]" line per key, into buf
+ * (NUL-terminated, truncated to len) and returns the length it needs. */
+size_t cismgpu_tile_table(char *buf, size_t len);
+
 /* Whether the handle's mixed copies hold the symmetric half (1) or every coupling (0; also
  * before its first mixed solve). */
 int cismgpu_solver_mixed_layout(const cismgpu_solver_t *s, int *symmetric_half);

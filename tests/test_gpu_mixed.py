@@ -261,3 +261,28 @@ def test_asymmetric_matrix_keeps_full_layout(gpu_lib):
     assert true_residual(P, *x) < 1.0001e-8
     st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, 2, tol=1e-8, maxiters=4000)
     assert rel(x, (ou, ov), P) < 1e-7
+
+
+def test_tile_tuner_keeps_a_system_on_one_tiling(gpu_lib):
+    """The tile tuner times candidate heights the first time it meets a system's key and keeps
+    the winner: repeated solves of the system (and of a copy of it) give the same bits, and the
+    table names the key with the height it chose."""
+    P = asm.batch_member(45, seed=12, nz=9)
+    S = cg.DeviceSolver(P)
+    try:
+        a = S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 4000), S.x()
+        b = S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 4000), S.x()
+    finally:
+        S.close()
+    T = cg.DeviceSolver(P)
+    try:
+        c = T.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 4000), T.x()
+    finally:
+        T.close()
+    for r in (b, c):
+        assert r[0] == a[0]
+        np.testing.assert_array_equal(r[1][0], a[1][0])
+        np.testing.assert_array_equal(r[1][1], a[1][1])
+    table = cg.tile_table()
+    keys = [ln.split()[0] for ln in table]
+    assert any(k.startswith("solve:3d:nzm16:nz9:half:") for k in keys), table
