@@ -514,6 +514,96 @@ def run_serve(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# on-device assembly of a Picard iteration's 3D system (the step the upload replaces)
+# ---------------------------------------------------------------------------
+def run_asm3d(args):
+    """cismgpu_solver_assemble_system_3d on the cfg3 grid (201x201 vertices x 11 levels, the ice
+    stream): stiffness with the nonlinear (Glen) viscosity from a velocity field, local basal
+    friction, the gravitational load as b, no-slip Dirichlet rows at the bed, staggered halo.
+    Device time by CUDA events on the handle's stream, against the upload of the same assembled
+    system from pinned host memory (cismgpu_solver_set_system), the host-to-device traffic the
+    on-device assembly removes.  A step is one assembly."""
+    import math as _m
+    import torch
+    import cism_b200 as cg
+    from cism_b200 import assembly as asm
+    from cism_b200 import build
+    build.build()
+    torch.cuda.set_device(0)
+    ewn, nz, dx = 201, 11, 2000.0
+    P = asm.ice_stream(ewn=ewn, nsn=ewn, nz=nz, dx=dx)
+    nx, ny = P.nx, P.ny
+    rng = np.random.default_rng(3)
+    x = (np.arange(nx) + 0.5) * dx
+    usrf0 = 3000.0 - x * _m.tan(_m.radians(0.5))
+    topg = usrf0[None, :] - 1500.0 + 0.05 * 1500.0 * asm.smooth_field((ny, nx), 4.0, rng)
+    usrf = np.broadcast_to(usrf0[None, :], (ny, nx)).copy()
+    thck = np.where(asm._ice_interior(ny, nx), usrf - topg, 0.0)
+    usrf = np.where(thck > 0, usrf, topg)
+    ac, av = asm.active_masks(thck)
+    sigma = asm.glide_sigma(nz)
+    xV = np.broadcast_to(np.arange(nx - 1) * dx, (ny - 1, nx - 1)).copy()
+    yV = np.broadcast_to((np.arange(ny - 1) * dx)[:, None], (ny - 1, nx - 1)).copy()
+    stagusrf, stagthck = asm.stagger(usrf, thck > 1.0), asm.stagger(thck, thck > 1.0)
+    ff = np.full((ny, nx, nz - 1), 0.5 * 1.0e-16 ** (-1.0 / 3.0))
+    beta = asm.lognormal_beta((ny - 1, nx - 1), 7)
+    lsrf = usrf - thck
+    u0 = 30.0 * rng.standard_normal((ny - 1, nx - 1, nz))
+    v0 = 30.0 * rng.standard_normal((ny - 1, nx - 1, nz))
+    stream = torch.cuda.Stream()
+    S = cg.DeviceSolver(P, x0=(u0, v0), stream=stream.cuda_stream)
+    geo = (sigma, ac.astype(np.int32), av.astype(np.int32), xV, yV, stagusrf, stagthck, ff)
+    load = (np.ascontiguousarray(P.bu), np.ascontiguousarray(P.bv))
+
+    def assemble():
+        return S.assemble_system(2, dx, dx, *geo, load[0], load[1], beta=beta, lsrf=lsrf)
+
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    host = [pin(a) for a in (P.Auu, P.Auv, P.Avu, P.Avv, P.bu, P.bv)]
+    for _ in range(max(args.warmup, 3)):
+        assemble()
+        S.set_system(*host, x0_from_solution=False)
+    a_ms, u_ms, w_ms = [], [], []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            t0 = time.perf_counter()
+            e[0].record(stream)
+            assemble()
+            e[1].record(stream)
+            t1 = time.perf_counter()
+            e[2].record(stream)
+            S.set_system(*host, x0_from_solution=False)
+            e[3].record(stream)
+        stream.synchronize()
+        a_ms.append(e[0].elapsed_time(e[1]))
+        u_ms.append(e[2].elapsed_time(e[3]))
+        w_ms.append(1e3 * (t1 - t0))
+    S.close()
+    nodes = int(np.count_nonzero(av)) * nz
+    up_bytes = sum(a.nbytes for a in host)
+    am = float(np.median(a_ms))
+    line = {
+        "metric": "on-device assembly of one Picard iteration's 3D system", "value": 1e3 / am, "unit": "systems/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": am, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"cfg3 grid: {ewn}x{ewn} vertices x {nz} levels ice stream, nonlinear Glen viscosity "
+                               "from a velocity field, local basal friction, gravitational load, staggered halo",
+                   "active_nodes": nodes},
+        "assemble_ms": {"device_median": am, "wall_median": float(np.median(w_ms)),
+                        "note": "CUDA events on the handle's stream around cismgpu_solver_assemble_system_3d "
+                                "(inputs' host-to-device copies, the kernels, the efvs download)"},
+        "upload_ms": {"device_median": float(np.median(u_ms)), "bytes": int(up_bytes),
+                      "GB_per_s": up_bytes / (float(np.median(u_ms)) / 1e3) / 1e9,
+                      "note": "the same system assembled on the host and uploaded from pinned memory "
+                              "(cismgpu_solver_set_system)"},
+        "speedup_vs_upload": float(np.median(u_ms)) / am,
+    }
+    print(json.dumps(line))
+    return 0
+
+
 def hbm_peak():
     try:
         with open(PEAKS) as f:
@@ -909,7 +999,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--mode", default="bench", choices=["bench", "profile"])
-    ap.add_argument("--workload", default="cfg4", choices=["cfg2", "cfg3", "dome", "cfg4", "cfg5"])
+    ap.add_argument("--workload", default="cfg4", choices=["cfg2", "cfg3", "dome", "cfg4", "cfg5", "asm3d"])
     ap.add_argument("--requests", type=int, default=96, help="cfg5: number of requests")
     ap.add_argument("--pool", type=int, default=8, help="cfg5: distinct systems per kind")
     ap.add_argument("--epoch-steps", type=int, default=64, help="cfg5: steps per serving epoch")
@@ -926,6 +1016,8 @@ def main():
         return run_cfg4(args)
     if args.workload == "cfg5":
         return run_serve(args)
+    if args.workload == "asm3d":
+        return run_asm3d(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)
