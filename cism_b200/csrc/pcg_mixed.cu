@@ -1220,6 +1220,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed_dyn(const MDesc *__restrict
             const unsigned long long *src = reinterpret_cast<const unsigned long long *>(states[i]);
             unsigned long long *dst = reinterpret_cast<unsigned long long *>(&hd.st[n]);
             for (int w8 = 0; w8 < (int)(sizeof(MState) / 8); ++w8) dst[w8] = __ldcg(src + w8);
+            // a solve that finished in an earlier launch (the serving loop queues its next epoch
+            // before it has read the previous one) is not running: count it out at once
+            if (hd.st[n].done) atomicSub(&ctl->active, 1);
             ++n;
         }
         hd.nsolve = n;

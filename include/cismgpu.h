@@ -500,7 +500,8 @@ int cismgpu_server_submit(cismgpu_server_t *s, const cismgpu_request_t *req, lon
  * queue_ms: submit to admission. */
 int cismgpu_server_poll(cismgpu_server_t *s, long long id, int *done, double *err, int *niters, int *status,
                         double *latency_ms, double *queue_ms);
-int cismgpu_server_drain(cismgpu_server_t *s);  /* wait until every submitted request is done */
+int cismgpu_server_drain(cismgpu_server_t *s);  /* wait until every submitted request is done and its
+                                                   device memory released */
 int cismgpu_server_stats(cismgpu_server_t *s, long long *epochs, size_t *bytes_in_use, int *active, int *queued);
 /* Kernel launches of the serving loop so far (one per kernel class and epoch), and how many of
  * them held 2D and 3D requests together in one multi-class launch. */
