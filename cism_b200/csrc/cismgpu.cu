@@ -1573,7 +1573,9 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
             CU(cudaStreamSynchronize(sv.stream));
             m.sym = hflag == 0 && !g_mixed_full_storage.load();
         }
-        m.il = !m.sym && m.A64i != nullptr && (size_t)NC * (size_t)nvec * sizeof(float4) > kStreamBytes;
+        // the interleaved FP64 copy: always in 3D (the check steps read it with the x tile in
+        // shared memory), in 2D for a streamed matrix
+        m.il = !m.sym && m.A64i != nullptr && (NC == 27 || (size_t)NC * (size_t)nvec * sizeof(float4) > kStreamBytes);
         if (m.sym) k_to_half<<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32, m.A64i);
         else if (NC == 27) k_to_f32<27><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32, m.il ? m.A64i : nullptr);
         else k_to_f32<9><<<1184, kBlock, 0, sv.stream>>>(g, sv.A.as<double>(), m.A32, m.A64i);

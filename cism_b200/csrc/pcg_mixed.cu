@@ -301,8 +301,17 @@ struct MLayout {
     __host__ __device__ size_t off_z() const { return (off_map() + 4 * (size_t)NS + 15) / 16 * 16; }
     __host__ __device__ size_t off_rt() const { return off_z() + 4 * (size_t)2 * KP * NS; }
     __host__ __device__ size_t off_A() const { return (off_rt() + 4 * (size_t)2 * NZM * NT + 15) / 16 * 16; }
+    // 3D FP64 check steps (up to 16 levels): x (updated by the step's d) of the tile and its halo
+    // ring, all levels with a zero row above and below, [2][KP][NS] doubles over the z and rt regions
+    __host__ __device__ size_t off_x64() const { return off_z(); }
     __host__ __device__ size_t bytes() const {
-        return off_A() + (resA ? 4 * (size_t)4 * NC * NZM * NT : 0);
+        size_t b = off_A() + (resA ? 4 * (size_t)4 * NC * NZM * NT : 0);
+        if (NC == 27 && NZM <= 16) {  // (32 levels keep the per-coupling residual_pass: the tile
+                                      // would halve their occupancy)
+            const size_t bx = off_x64() + 8 * (size_t)2 * KP * NS;
+            if (bx > b) b = bx;
+        }
+        return b;
     }
 };
 
@@ -576,6 +585,169 @@ __device__ __forceinline__ void residual_pass(const MDesc &D, const int *smap, i
     }
 }
 
+// FP64 r = b - A64 x on a 3D tile with x read from the shared-memory tile sx ([2][KP][NS]
+// doubles: level k at row k+1, rows 0 and nz+1 and slots that hold zero are zero), the matrix
+// from the interleaved copy (HALF: its symmetric half, a lower coupling read from its transpose
+// partner).  Every node takes all 27 couplings with no bounds tests: a coupling that leaves the
+// array meets a zero x (and in the full copy a zero coefficient), which adds nothing.  The
+// multiply-adds run in the reference's coupling order, as residual_pass.  Partials: p0 = (b,b),
+// p1 = (r,r); r32 = r on live columns, into buffer rpar.
+template <int NZM, bool HALF>
+__device__ __forceinline__ void residual_tile(const MDesc &D, const int *smap, int TY, int i0, int j0, int rpar,
+                                              const double *sx, double &p0, double &p1) {
+    constexpr int KP = NZM + 2;
+    const Geom &g = D.g;
+    const int nz = g.nz;
+    const int NQ = (int)g.NQ;
+    const int plane = nz * NQ;
+    const int NT = kTX * TY;
+    const int NS = (kTX + 2) * (TY + 2);
+    const double2 *__restrict__ A2 = D.A64i;
+    float *__restrict__ ru32 = D.r[rpar];
+    float *__restrict__ rv32 = D.r[rpar] + plane;
+    const double *sxu = sx, *sxv = sx + KP * NS;
+    const int nitems = NT * nz;
+    const unsigned long long pol = l2_matrix_policy(D.stream != 0);
+#pragma unroll 1
+    for (int base = threadIdx.x; base < nitems; base += kChR * kBlock) {
+        double yu[kChR], yv[kChR], bu[kChR], bv[kChR];
+        int ee[kChR];
+        bool ok[kChR], lv[kChR];
+#pragma unroll
+        for (int u = 0; u < kChR; ++u) {
+            const int it = base + u * kBlock;
+            yu[u] = 0.0; yv[u] = 0.0; bu[u] = 0.0; bv[u] = 0.0;
+            ee[u] = 0; ok[u] = false; lv[u] = false;
+            if (it < nitems) {
+                const int col = it % NT, k = it / NT;
+                const int ti = col % kTX, tj = col / kTX;
+                const int i = i0 + ti, j = j0 + tj;
+                if (i <= g.ihi && j <= g.jhi) {
+                    const int q = j * g.NX + i;
+                    const int s = (ti + 1) + (kTX + 2) * (tj + 1);
+                    const int e = k * NQ + q;
+                    ok[u] = true;
+                    ee[u] = e;
+                    lv[u] = map_live(smap[s]);
+                    bu[u] = D.b[e];
+                    bv[u] = D.b[plane + e];
+                    if (D.act[q] != 0) {
+#pragma unroll
+                        for (int c = 0; c < 27; ++c) {
+                            const int iA = c % 3 - 1, jA = (c / 3) % 3 - 1, kA = c / 9 - 1;
+                            const int zi = (k + 1 + kA) * NS + s + iA + (kTX + 2) * jA;
+                            const double x1 = sxu[zi], x2 = sxv[zi];
+                            double2 au, av;
+                            if (!HALF) {
+                                const size_t h = (size_t)c * plane + e;
+                                au = ld_stream(A2 + 2 * h, pol);
+                                av = ld_stream(A2 + 2 * h + 1, pol);
+                            } else if (c >= 13) {
+                                const size_t h = (size_t)(c - 13) * plane + e;
+                                au = ld_half(A2 + 2 * h, pol);
+                                av = ld_half(A2 + 2 * h + 1, pol);
+                            } else {  // partner n = (k+kA, i+iA, j+jA), coupling 26 - c, blocks swapped
+                                const int kk = k + kA < 0 ? 0 : k + kA;  // level -1: its x row is zero
+                                const size_t h = (size_t)(13 - c) * plane + (size_t)kk * NQ +
+                                                 (size_t)((j + jA) * g.NX + (i + iA));
+                                const double2 pu = ld_half(A2 + 2 * h, pol), pv = ld_half(A2 + 2 * h + 1, pol);
+                                au = make_double2(pu.x, pv.x);
+                                av = make_double2(pu.y, pv.y);
+                            }
+                            yu[u] = fma(au.x, x1, yu[u]);
+                            yu[u] = fma(au.y, x2, yu[u]);
+                            yv[u] = fma(av.x, x1, yv[u]);
+                            yv[u] = fma(av.y, x2, yv[u]);
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kChR; ++u) {
+            if (!ok[u]) continue;
+            const double ru = bu[u] - yu[u], rv = bv[u] - yv[u];
+            p1 += ru * ru + rv * rv;
+            p0 += bu[u] * bu[u] + bv[u] * bv[u];
+            ru32[ee[u]] = lv[u] ? (float)ru : 0.0f;
+            rv32[ee[u]] = lv[u] ? (float)rv : 0.0f;
+        }
+    }
+}
+
+// x of a 3D tile and its halo ring into the shared-memory tile sx ([2][KP][NS] doubles, level k
+// at row k+1, zero rows 0 and nz+1, zero in slots that hold zero); with upd, advanced by this
+// step's d: x + alpha64 * dn, dn = z + beta d (the owner applies the same FP64 fma later, so the
+// residual sees exactly the updated x), and q = Az + beta q written for the owned columns.
+template <int NZM>
+__device__ __forceinline__ void fill_x_tile(const MDesc &D, const int *smap, int TY, int par, bool upd, float beta,
+                                            double alpha64, double *sx) {
+    constexpr int KP = NZM + 2;
+    const Geom &g = D.g;
+    const int nz = g.nz;
+    const int NQ = (int)g.NQ;
+    const int plane = nz * NQ;
+    const int NS = (kTX + 2) * (TY + 2);
+    const float *__restrict__ q_in = D.q[par];
+    const float *__restrict__ az_in = D.Az[par];
+    float *__restrict__ q_out = D.q[par ^ 1];
+    for (int it = threadIdx.x; it < 2 * NS; it += kBlock) {  // zero rows above and below
+        const int c = it >= NS ? 1 : 0, sl = it - c * NS;
+        sx[(c * KP + 0) * NS + sl] = 0.0;
+        sx[(c * KP + nz + 1) * NS + sl] = 0.0;
+    }
+    const int n1 = 2 * NS * nz;
+#pragma unroll 1
+    for (int base = threadIdx.x; base < n1; base += 4 * kBlock) {
+        float zo[4], dol[4], qo[4], az[4];
+        double xo[4];
+        int ee[4], vv[4], ix[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int it = base + u * kBlock;
+            ix[u] = -1;
+            vv[u] = 0;
+            ee[u] = 0;
+            zo[u] = dol[u] = qo[u] = az[u] = 0.0f;
+            xo[u] = 0.0;
+            if (it < n1) {
+                const int k = it / (2 * NS), rem = it - k * 2 * NS;
+                const int c = rem >= NS ? 1 : 0, sl = rem - c * NS;
+                ix[u] = (c * KP + k + 1) * NS + sl;
+                const int v = smap[sl];
+                vv[u] = v;
+                if (map_live(v)) {
+                    const int e = c * plane + k * NQ + map_src(v);
+                    ee[u] = e;
+                    xo[u] = ldd(D.x + e);
+                    if (upd) {
+                        zo[u] = ldf(D.z + e);
+                        dol[u] = ldf(D.d + e);
+                        if (map_mine(v)) {
+                            qo[u] = ldf(q_in + e);
+                            az[u] = ldf(az_in + e);
+                        }
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (ix[u] < 0) continue;
+            const bool live = map_live(vv[u]);
+            double xn = 0.0;
+            if (live) {
+                xn = xo[u];
+                if (upd) {
+                    xn = fma(alpha64, (double)fmaf(beta, dol[u], zo[u]), xn);  // x + alpha (z_i + beta d_{i-1})
+                    if (map_mine(vv[u])) q_out[ee[u]] = fmaf(beta, qo[u], az[u]);  // q_i = Az_i + beta q_{i-1}
+                }
+            }
+            sx[ix[u]] = xn;
+        }
+    }
+}
+
 // One tile of one solve for the solve's current step; publishes the tile's record.
 template <int NC, int NZM>
 __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, MHead &hd, unsigned char *smem) {
@@ -606,7 +778,20 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
         __syncthreads();
     }
 
-    if (step == MS_INIT) {
+    if (NC == 27 && NZM <= 16 && D.A64i && (step == MS_INIT || step == MS_BC)) {
+        // 3D: x of the tile and halo (updated by this step's d in MS_BC) into shared memory, then
+        // the FP64 residual with branch-free couplings
+        double *sx = reinterpret_cast<double *>(smem + ly.off_x64());
+        const bool upd = step == MS_BC;
+        fill_x_tile<NZM>(D, smap, TY, par, upd, upd ? (float)S.beta : 0.0f, upd ? S.alpha : 0.0, sx);
+        __syncthreads();
+        if (D.sym) residual_tile<NZM, true>(D, smap, TY, i0, j0, upd ? par ^ 1 : par, sx, p0, p1);
+        else residual_tile<NZM, false>(D, smap, TY, i0, j0, upd ? par ^ 1 : par, sx, p0, p1);
+        if (upd) {
+            p0 = p1;
+            p1 = 0.0;
+        }
+    } else if (step == MS_INIT) {
         if (NC == 27 && D.sym) residual_pass<NC, true, true>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
         else if (D.A64i) residual_pass<NC, true>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
         else residual_pass<NC, false>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);

@@ -12,11 +12,8 @@
 //     the same launch) for up to epoch_steps steps; a request's state (scalars in its MState,
 //     vectors in its buffers) stays on the device between epochs, so a request joins and
 //     leaves between any two epochs without restarting anyone;
-//   * epochs are pipelined: epoch e is queued before the host reads epoch e-1, so the GPU runs
-//     them back to back with no host synchronization of the stream in between;
-//   * retirement: a finished request's x is copied into the caller's arrays as soon as its
-//     epoch is read; its handle is freed and its bytes returned to the budget once the epoch
-//     queued after it (which still lists it, as a finished solve the kernel skips) completes.
+//   * retirement: a finished request's x is copied into the caller's arrays, its handle
+//     freed and its bytes returned to the budget.
 // Tile heights and the order of every sum depend on the request only, so a result is
 // bit-identical whether the request is served alone or in any mix.
 #pragma once
@@ -212,7 +209,7 @@ static int srv_launch(cismgpu_server *S, SrvLaunch &L, int cls, bool *multi) {
 }
 
 // A request's result: x to the caller's arrays, its status and counters; it is done for the
-// caller (poll and drain see it) from here on.  Its device memory stays until srv_free.
+// caller (poll and drain see it) from here on.
 static void srv_deliver(cismgpu_server *S, SrvReq &r, int status, double err, int niters, int checks) {
     if (r.h) {
         const int rc = cismgpu_solver_get_x(r.h, r.rq.xu, r.rq.xv);
@@ -229,8 +226,7 @@ static void srv_deliver(cismgpu_server *S, SrvReq &r, int status, double err, in
     S->cv.notify_all();
 }
 
-// The handle of a delivered request freed (no launch in flight refers to it) and its bytes
-// returned to the budget.
+// The handle of a delivered request freed and its bytes returned to the budget.
 static void srv_free(cismgpu_server *S, SrvReq &r) {
     if (r.h) {
         cismgpu_solver_destroy(r.h);
@@ -242,7 +238,7 @@ static void srv_free(cismgpu_server *S, SrvReq &r) {
     S->cv.notify_all();
 }
 
-// A request that never reached the GPU (admission failed): delivered and freed at once.
+// Finish a request: delivered, then freed.
 static void srv_retire(cismgpu_server *S, SrvReq &r, int status, double err, int niters, int checks) {
     srv_deliver(S, r, status, err, niters, checks);
     srv_free(S, r);
@@ -287,107 +283,65 @@ static void srv_admit_loop(cismgpu_server *S) {
     }
 }
 
-// Epoch loop, pipelined: epoch e (one launch per kernel class over the active requests) is
-// queued on the epoch stream before the host reads epoch e-1, so the GPU runs epochs back to
-// back and the host never synchronizes the whole stream.  A request that finished in e-1 is
-// therefore also a member of e: the kernel counts it out at once and skips its tiles, its x
-// and status are delivered as soon as e-1 is read, and its handle is freed only after e has
-// completed.  A running request's launch-start tick for e is predicted (every running solve
-// advances exactly epoch_steps steps per epoch) and checked when e-1 is read.  Requests
-// admitted meanwhile join at the next epoch.
-struct SrvEpoch {
-    SrvLaunch L[kSrvClasses];
-    std::vector<unsigned> tick0[kSrvClasses];  // launch-start ticks, per member
-    bool live = false;
-    cudaEvent_t done = nullptr;
-};
-
+// Epoch loop: one epoch per kernel class over the active requests (2D and 3D requests share the
+// class-0 launch), then the finished ones are delivered and freed; requests admitted meanwhile
+// join at the next epoch.  The host waits for each epoch before it queues the next: a pipelined
+// form that queued epoch e before reading e-1 measured slower on the served stream (6.9 against
+// 8.3 solves/s), because a 3D result's layout change is a kernel that cannot start beside a
+// cooperative launch holding every SM, and freeing a finished request's memory synchronizes the
+// device, so the host waited for the queued epoch anyway and every request spent one more epoch
+// as a skipped member.
 static void srv_loop(cismgpu_server *S) {
     cudaSetDevice(S->device);
-    SrvEpoch E[2];
-    for (SrvEpoch &x : E) cudaEventCreateWithFlags(&x.done, cudaEventDisableTiming);
-    std::vector<SrvReq *> to_free;  // delivered; their handles wait for the epoch in flight
-    long long e = 0;
+    SrvLaunch L[kSrvClasses];
     for (;;) {
-        SrvEpoch &prev = E[(e + 1) & 1], &cur = E[e & 1];
         {
             std::unique_lock<std::mutex> lk(S->mu);
             S->cv.wait(lk, [&] {
-                return !S->ready.empty() || !S->active.empty() || prev.live || !to_free.empty() ||
+                return !S->ready.empty() || !S->active.empty() ||
                        (S->stop && S->queued.empty() && S->uploading == 0);
             });
-            if (S->ready.empty() && S->active.empty() && !prev.live && to_free.empty()) break;
+            if (S->ready.empty() && S->active.empty()) break;  // stopping and nothing left
             S->active.insert(S->active.end(), S->ready.begin(), S->ready.end());
             S->ready.clear();
         }
-        // queue epoch e over the active set
-        for (int c = 0; c < kSrvClasses; ++c) {
-            cur.L[c].members.clear();
-            cur.tick0[c].clear();
-        }
-        for (SrvReq *r : S->active) cur.L[r->cls].members.push_back(r);
+        for (int c = 0; c < kSrvClasses; ++c) L[c].members.clear();
+        for (SrvReq *r : S->active) L[r->cls].members.push_back(r);
         int launched = 0, multi = 0;
         for (int c = 0; c < kSrvClasses; ++c) {
-            if (cur.L[c].members.empty()) continue;
-            for (SrvReq *r : cur.L[c].members) cur.tick0[c].push_back(r->tick);
+            if (L[c].members.empty()) continue;
             bool m = false;
-            const int rc = srv_launch(S, cur.L[c], c, &m);
-            if (rc) {  // the class cannot run: fail its requests (after the epoch in flight)
-                for (SrvReq *r : cur.L[c].members) {
-                    srv_deliver(S, *r, rc, std::nan(""), 0, 0);
-                    to_free.push_back(r);
-                }
-                cur.L[c].members.clear();
+            const int rc = srv_launch(S, L[c], c, &m);
+            if (rc) {  // the class cannot run: fail its requests
+                for (SrvReq *r : L[c].members) srv_retire(S, *r, rc, std::nan(""), 0, 0);
+                L[c].members.clear();
             } else {
                 ++launched;
                 multi += m ? 1 : 0;
-                for (SrvReq *r : cur.L[c].members) r->tick += (unsigned)S->epoch_steps;  // predicted
             }
         }
-        cur.live = launched > 0;
-        if (cur.live) {
-            cudaEventRecord(cur.done, S->es);
+        if (launched) {
+            cudaStreamSynchronize(S->es);
             std::lock_guard<std::mutex> lk(S->mu);
             ++S->epochs;
             S->launches += launched;
             S->multi_launches += multi;
         }
-        // read epoch e-1; the epoch before it has completed, so free what waited for it
-        std::vector<SrvReq *> freeable;
-        if (prev.live) {
-            cudaEventSynchronize(prev.done);
-            freeable.swap(to_free);
-            for (int c = 0; c < kSrvClasses; ++c) {
-                const bool aborted = prev.L[c].h_ctl && !prev.L[c].members.empty() && prev.L[c].h_ctl->abort;
-                for (size_t t = 0; t < prev.L[c].members.size(); ++t) {
-                    SrvReq *r = prev.L[c].members[t];
-                    if (r->phase == 2) continue;  // delivered already
-                    const MState &st = prev.L[c].h_states[t];
-                    int status = -1;
-                    if (st.done) status = st.status;
-                    else if (aborted) status = CISMGPU_ETIMEOUT;
-                    else if (st.tick != prev.tick0[c][t] + (unsigned)S->epoch_steps)
-                        status = fail(CISMGPU_ECUDA, "serving epoch did not advance a running request");
-                    if (status < 0) continue;
-                    srv_deliver(S, *r, status, st.err, st.niters, st.checks);
-                    to_free.push_back(r);  // still a member of epoch e
-                }
+        std::vector<SrvReq *> still;
+        for (int c = 0; c < kSrvClasses; ++c) {
+            const bool aborted = L[c].h_ctl && !L[c].members.empty() && L[c].h_ctl->abort;
+            for (size_t t = 0; t < L[c].members.size(); ++t) {
+                SrvReq *r = L[c].members[t];
+                const MState &st = L[c].h_states[t];
+                r->tick = st.tick;
+                if (st.done) srv_retire(S, *r, st.status, st.err, st.niters, st.checks);
+                else if (aborted) srv_retire(S, *r, CISMGPU_ETIMEOUT, st.err, st.niters, st.checks);
+                else still.push_back(r);
             }
-            prev.live = false;
-        } else {  // no epoch before e is in flight, and e holds no delivered request
-            freeable.swap(to_free);
         }
-        {
-            std::lock_guard<std::mutex> lk(S->mu);
-            std::vector<SrvReq *> still;
-            for (SrvReq *r : S->active)
-                if (r->phase != 2) still.push_back(r);
-            S->active.swap(still);
-        }
-        for (SrvReq *r : freeable) srv_free(S, *r);
-        ++e;
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->active.swap(still);
     }
-    for (SrvEpoch &x : E) cudaEventDestroy(x.done);
 }
 
 }  // namespace cismgpu
