@@ -1842,13 +1842,14 @@ static int mixed_run(Solver &sv, int precond, int ncheck, double tol, int maxite
 //    on an SM is timed on a short solve of the actual system (kTuneIters iterations, tol 0),
 //    best of two;
 //  * batches and serving: key (dims, nz class): the least height of every member's tiles,
-//    timed on a short launch (kTuneSteps steps) of the first batch that meets the key.
+//    timed on a launch of kTuneSteps steps of the first batch that meets the key (48 steps
+//    picked a floor that was faster early in the solve and slower over all of it).
 // The occupancy rule (mixed_solve_ty; batch floors 4 rows in 3D and 16 in 2D) is the default and
 // keeps its place unless a candidate is more than 3 % faster.  The serving loop never times (its
 // launches share the GPU) and uses the table or the default.  CISMGPU_TILE_TUNING=0 turns timing
 // off; the cache file is $CISMGPU_TILE_CACHE, else $HOME/.cache/cismgpu/tiles-<GPU name>.txt.
 constexpr int kTuneIters = 12;
-constexpr int kTuneSteps = 48;
+constexpr int kTuneSteps = 400;  // batch floors: long enough to see more than the first check
 
 struct TileTuner {
     std::mutex mu;
@@ -2438,7 +2439,7 @@ static int batch_enqueue(MixedBatch &B, cudaStream_t s) {
 
 // The batch tile floor of the members' dims and nz class, timed on this batch the first time the
 // class is met (the tuner above): each candidate floor runs kTuneSteps steps of the whole batch
-// (tol 0, so no member stops), best of two.  Outside any stream capture.
+// (tol 0, so no member stops).  Outside any stream capture.
 static int tune_batch_floor(const std::vector<Solver *> &svs, int precond, int ncheck, cudaStream_t s) {
     if (svs.empty()) return CISMGPU_OK;
     const bool is3d = svs[0]->is3d;
@@ -2463,7 +2464,7 @@ static int tune_batch_floor(const std::vector<Solver *> &svs, int precond, int n
         if (rc) break;
         T.max_steps = kTuneSteps;
         float t = 1e30f;
-        for (int rep = 0; rep < 2 && !rc; ++rep) {
+        for (int rep = 0; rep < 1 && !rc; ++rep) {
             if (cudaEventRecord(e0, s) != cudaSuccess) rc = fail(CISMGPU_ECUDA, "event record failed");
             if (!rc) rc = batch_enqueue(T, s);
             if (!rc && cudaEventRecord(e1, s) != cudaSuccess) rc = fail(CISMGPU_ECUDA, "event record failed");

@@ -5,8 +5,10 @@
 //   * admission (its own host thread): in arrival order while the HBM budget allows; an admitted request gets
 //     its own device-resident handle (matrix, FP32 copy, preconditioner, Krylov vectors),
 //     uploaded on the handle's own stream while the GPU runs the current epoch;
-//   * epochs: every active request of a kernel class (2D and 3D with nz <= 16 together; 3D
-//     with 16 < nz <= 32) takes part in one launch of the dynamic persistent kernel
+//   * epochs: a large 2D request runs a launch of the single-solve kernel of its own (its FP32
+//     matrix resident in shared memory where its tiles fit one per CTA); every other active
+//     request of a kernel class (2D and 3D with nz <= 16 together; 3D with 16 < nz <= 32) takes
+//     part in one launch of the dynamic persistent kernel
 //     (k_mixed_dyn; with 2D and 3D requests both present, its multi-class form, in which
 //     every work item runs its own solve's tile code, so 2D and 3D requests share the SMs in
 //     the same launch) for up to epoch_steps steps; a request's state (scalars in its MState,
@@ -41,7 +43,10 @@ struct SrvReq {
     double t_submit = 0.0, t_admit = 0.0, t_done = 0.0;  // ms since the server started
     cismgpu_solver *h = nullptr;
     size_t bytes = 0;
-    int cls = 0;       // kernel class: 0 2D or 3D nz <= 16, 1 3D 16 < nz <= 32
+    int cls = 0;       // kernel class: 0 2D or 3D nz <= 16, 1 3D 16 < nz <= 32, 2 large 2D on the
+                       // single-solve kernel
+    MState *h_st = nullptr;  // class 2: pinned copy of the state after each epoch
+    MCtl *h_ctl = nullptr;   // class 2: pinned copy of the launch's control word
     int TY = 0;
     unsigned tick = 0; // steps completed, as of the last epoch
 };
@@ -58,7 +63,9 @@ static size_t request_bytes(const cismgpu_request_t &r) {
     return (size_t)(nvec * per + NQ * 16 + (8 << 20));
 }
 
-static constexpr int kSrvClasses = 2;
+static constexpr int kSrvClasses = 2;       // classes served by the dynamic kernel
+static constexpr long long kSrvResidentMin = 65536;  // owned vertices from which a 2D request runs on
+                                                     // the single-solve kernel
 
 static int request_class(const cismgpu_request_t &r) { return (r.dims == 3 && r.nz > 16) ? 1 : 0; }
 
@@ -119,12 +126,46 @@ static int srv_admit(SrvReq &r) {
     Solver &sv = h->sv;
     const int nzm = mixed_nzm(sv.g, sv.is3d);
     r.TY = mixed_batch_ty(sv.g, sv.is3d, nzm, batch_floor(sv.is3d, nzm));
+    if (!sv.is3d) {
+        // a large 2D system runs its epochs on the single-solve kernel, a launch of its own, with
+        // its FP32 matrix resident in shared memory where the tiles fit one per co-resident CTA
+        // (2D steps are latency-bound: no leader hop, and no matrix stream where resident)
+        const int ty1 = mixed_solve_ty(sv.g, false, 1);
+        const long long owned = (long long)(sv.g.ihi - sv.g.ilo + 1) * (sv.g.jhi - sv.g.jlo + 1);
+        if (owned >= kSrvResidentMin) {
+            r.cls = 2;
+            r.TY = ty1;
+            CU(cudaMallocHost((void **)&r.h_st, sizeof(MState)));
+            CU(cudaMallocHost((void **)&r.h_ctl, sizeof(MCtl)));
+        }
+    }
     TRY(mixed_prepare(sv, q.precond, r.TY));
     TRY(mixed_reset(sv, sv.stream));
     const MState S0 = mixed_init_state(q.tolerance, q.maxiters, q.linear_solve_ncheck);
     CU(cudaMemcpyAsync(sv.mixed.state, &S0, sizeof(MState), cudaMemcpyHostToDevice, sv.stream));
+    if (r.cls == 2) {
+        const MDesc D = mixed_desc(sv, q.precond, r.TY);
+        CU(cudaMemcpyAsync(sv.mixed.desc, &D, sizeof(MDesc), cudaMemcpyHostToDevice, sv.stream));
+    }
     CU(cudaStreamSynchronize(sv.stream));
     r.tick = 0;
+    return CISMGPU_OK;
+}
+
+// One epoch of a class-2 request: the single-solve kernel for up to epoch_steps steps
+// (it resumes exactly where the previous epoch stopped), then its state and control word into
+// the request's pinned copies (asynchronous on the epoch stream).
+static int srv_launch_resident(cismgpu_server *S, SrvReq &r) {
+    Solver &sv = r.h->sv;
+    MixedBufs &m = sv.mixed;
+    cudaStream_t s = S->es;
+    const bool res = mixed_resident(false, 1, r.TY, m.ntiles);
+    const int grid = mixed_launch_grid(false, 1, r.TY, res, m.ntiles);
+    if (grid < 1) return fail(CISMGPU_EUNSUPPORTED, "mixed kernel does not fit on an SM at this tile height");
+    CU(cudaMemsetAsync(m.ctl, 0, sizeof(MCtl), s));
+    TRY(mixed_dispatch(false, 1, m.desc, m.state, m.tiles, m.ntiles, r.TY, res, m.ctl, S->epoch_steps, grid, s));
+    CU(cudaMemcpyAsync(r.h_st, m.state, sizeof(MState), cudaMemcpyDeviceToHost, s));
+    CU(cudaMemcpyAsync(r.h_ctl, m.ctl, sizeof(MCtl), cudaMemcpyDeviceToHost, s));
     return CISMGPU_OK;
 }
 
@@ -232,6 +273,10 @@ static void srv_free(cismgpu_server *S, SrvReq &r) {
         cismgpu_solver_destroy(r.h);
         r.h = nullptr;
     }
+    if (r.h_st) cudaFreeHost(r.h_st);
+    if (r.h_ctl) cudaFreeHost(r.h_ctl);
+    r.h_st = nullptr;
+    r.h_ctl = nullptr;
     std::lock_guard<std::mutex> lk(S->mu);
     S->used -= r.bytes;
     r.bytes = 0;
@@ -306,8 +351,21 @@ static void srv_loop(cismgpu_server *S) {
             S->ready.clear();
         }
         for (int c = 0; c < kSrvClasses; ++c) L[c].members.clear();
-        for (SrvReq *r : S->active) L[r->cls].members.push_back(r);
+        std::vector<SrvReq *> resident;
+        for (SrvReq *r : S->active) {
+            if (r->cls == 2) resident.push_back(r);
+            else L[r->cls].members.push_back(r);
+        }
         int launched = 0, multi = 0;
+        std::vector<SrvReq *> res_run;
+        for (SrvReq *r : resident) {
+            const int rc = srv_launch_resident(S, *r);
+            if (rc) srv_retire(S, *r, rc, std::nan(""), 0, 0);
+            else {
+                res_run.push_back(r);
+                ++launched;
+            }
+        }
         for (int c = 0; c < kSrvClasses; ++c) {
             if (L[c].members.empty()) continue;
             bool m = false;
@@ -328,6 +386,12 @@ static void srv_loop(cismgpu_server *S) {
             S->multi_launches += multi;
         }
         std::vector<SrvReq *> still;
+        for (SrvReq *r : res_run) {
+            const MState &st = *r->h_st;
+            if (st.done) srv_retire(S, *r, st.status, st.err, st.niters, st.checks);
+            else if (r->h_ctl->abort) srv_retire(S, *r, CISMGPU_ETIMEOUT, st.err, st.niters, st.checks);
+            else still.push_back(r);
+        }
         for (int c = 0; c < kSrvClasses; ++c) {
             const bool aborted = L[c].h_ctl && !L[c].members.empty() && L[c].h_ctl->abort;
             for (size_t t = 0; t < L[c].members.size(); ++t) {

@@ -88,3 +88,23 @@ def test_server_budget(gpu_lib):
         assert q[2] > q[0]
     finally:
         S.close()
+
+
+def test_large_2d_request_alone_equals_mix(gpu_lib):
+    """A 2D request large enough for the single-solve kernel's own launches (>= 65536 owned
+    vertices) gives the same bits served alone and served beside 3D and small 2D requests."""
+    big = (asm.ssa_random(ewn=300, nsn=240, seed=21), 1)
+    others = [(asm.batch_member(30, seed=8, nz=7), 2), (asm.ssa_random(ewn=50, nsn=44, seed=22), 1)]
+    au, av, ainfo = serve_alone(*big)
+    S = cg.Server(hbm_budget_bytes=4 * 10**9, epoch_steps=16)
+    try:
+        ids = [S.submit(P, precond=pc, tol=1e-8, maxiters=5000) for P, pc in [big] + others]
+        S.drain()
+        xu, xv, info = S.result(ids[0])
+        assert info["status"] == 0 and ainfo["status"] == 0 and info["err"] < 1e-8
+        assert info["err"] == ainfo["err"] and info["niters"] == ainfo["niters"]
+        np.testing.assert_array_equal(xu, au)
+        np.testing.assert_array_equal(xv, av)
+        assert all(S.poll(i)["status"] == 0 for i in ids)
+    finally:
+        S.close()
