@@ -434,12 +434,12 @@ __global__ void k_tile_nbrs(MDesc D, const int *maps, int *nbrs) {
 // row stride NS; level k at row k+1), FP32.  The column's factors are loaded in one
 // batch first: a load inside the recurrence would cost a memory round trip per level.
 template <int NZM>
-__device__ __forceinline__ void sia_col(const MDesc &D, float *zc, int NS, int s, int q) {
+__device__ __forceinline__ void sia_col(const MDesc &D, float *zc, int NS, int s, int q, int c0, int c1) {
     const int nz = D.g.nz;
     const int NQ = (int)D.g.NQ;
     const int plane = nz * NQ;
     constexpr int KP = NZM + 2;
-    for (int c = 0; c < 2; ++c) {
+    for (int c = c0; c <= c1; ++c) {
         float *z = zc + c * KP * NS + NS + s;  // z[k * NS] is level k
         const float *ib = D.pre + (c * 3 + 0) * plane, *sb = D.pre + (c * 3 + 1) * plane,
                     *gm = D.pre + (c * 3 + 2) * plane;
@@ -983,9 +983,14 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
             }
             __syncthreads();
             if (NC == 27 && D.precond == 2) {  // column tridiagonal solves on tile + halo
-                for (int sl = t; sl < NS; sl += kBlock) {
+                // one (column, component) per thread while they fit the block: the two
+                // components' recurrences then run side by side instead of one after the other
+                const bool split = 2 * NS <= kBlock;
+                const int nit = split ? 2 * NS : NS;
+                for (int it = t; it < nit; it += kBlock) {
+                    const int c = split ? it / NS : 0, sl = split ? it - c * NS : it;
                     const int v = smap[sl];
-                    if (map_live(v)) sia_col<NZM>(D, sz, NS, sl, map_src(v));
+                    if (map_live(v)) sia_col<NZM>(D, sz, NS, sl, map_src(v), c, split ? c : 1);
                 }
                 __syncthreads();
             }
