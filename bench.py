@@ -363,13 +363,14 @@ def run_cfg4(args):
         "speedup_vs_fp64_plain": value / world / fp64_rate,
         "mixed_one_at_a_time": {"solves_per_s": n / (one_ms / 1e3), "ms_for_all": one_ms},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": ncu_traffic("k_mixed_dyn<27,16>:cfg4"), "peak_kind": peak_kind,
+                     "traffic": cfg4_traffic(by), "peak_kind": peak_kind,
                      "kernel": "k_mixed_dyn<27,16> (the whole batch in one launch; the graph's other kernels are "
                                "64 halo resets and one result copy)",
                      "note": "achieved = algorithmic bytes of the replay (per active node: FP32 iterations x "
                              "(16 B x stored couplings + 136 B) + FP64 checks x (32 B x stored couplings + 40 B); "
                              f"{sum(half)} of {n} members stored as the symmetric half, 14 of 27 couplings) / mean "
-                             "replay time by CUDA events; traffic = ncu DRAM bytes"},
+                             "replay time by CUDA events; traffic = ncu DRAM bytes of the 4-member batch "
+                             "(profiles/k_mixed_dyn_cfg4_batch4.md) scaled by algorithmic bytes"},
         "algorithmic_bytes_per_step": by,
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_rate, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
@@ -610,6 +611,16 @@ def hbm_peak():
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM, "fallback"
+
+
+def cfg4_traffic(algorithmic_bytes):
+    """DRAM bytes of one cfg4 replay: the dram__bytes_read.sum + write.sum of an ncu capture of the
+    first 4 members' batch (profiles/traffic.json; the full 64-member launch runs ~6 s, too long to
+    capture), scaled by the ratio of the replay's algorithmic bytes to the capture's."""
+    rec = ncu_traffic("k_mixed_dyn<27,16>:cfg4-batch4")
+    if not isinstance(rec, dict) or not rec.get("algorithmic_bytes"):
+        return None
+    return rec["dram_bytes"] / rec["algorithmic_bytes"] * algorithmic_bytes
 
 
 def ncu_traffic(kernel_key):

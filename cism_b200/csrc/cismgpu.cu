@@ -1469,17 +1469,38 @@ static const void *mixed_kernel(bool is3d, int nzm) {
     return (const void *)k_mixed<27, 32>;
 }
 
-// Co-resident CTAs of the mixed kernel at tile height TY (0 if it does not fit).
-static int mixed_grid(bool is3d, int nzm, int TY, bool resident = false) {
-    const size_t smem = mixed_smem(is3d, nzm, TY, resident);
-    if (smem > 227 * 1024 - 64) return 0;
-    const void *k = mixed_kernel(is3d, nzm);
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
-    int dev = 0, nsm = 0, occ = 0;
+// Co-resident CTAs of kernel k with `smem` bytes of dynamic shared memory (0 if it does not fit).
+// The kernel's dynamic shared-memory limit is raised once per device to the device's opt-in
+// maximum and never lowered: several host threads (the serving loop's admission and epoch threads,
+// solves on handles) size and launch the same kernels with different amounts, and a limit set per
+// call by one thread could drop below the amount another thread is about to launch with.
+static int smem_grid(const void *k, size_t smem) {
+    static std::mutex mu;
+    static std::vector<std::pair<int, const void *>> raised;
+    int dev = 0, nsm = 0, optin = 0, occ = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, k) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+    const long long maxdyn = (long long)optin - (long long)fa.sharedSizeBytes;
+    if ((long long)smem > maxdyn) return 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        const std::pair<int, const void *> key(dev, k);
+        if (std::find(raised.begin(), raised.end(), key) == raised.end()) {
+            if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)maxdyn) != cudaSuccess)
+                return 0;
+            raised.push_back(key);
+        }
+    }
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kBlock, smem) != cudaSuccess) return 0;
     return nsm * occ;
+}
+
+// Co-resident CTAs of the mixed kernel at tile height TY (0 if it does not fit).
+static int mixed_grid(bool is3d, int nzm, int TY, bool resident = false) {
+    return smem_grid(mixed_kernel(is3d, nzm), mixed_smem(is3d, nzm, TY, resident));
 }
 
 // Tile autotuner, per solve (a solve's tiling, and so its rounding, never depends on what
@@ -1734,34 +1755,13 @@ static const void *mixed_dyn_kernel(bool is3d, int nzm) {
     return (const void *)k_mixed_dyn<27, 32>;
 }
 
-// Co-resident CTAs of a kernel with `smem` dynamic shared memory (sets the kernel's
-// shared-memory attribute; call outside any stream capture).  0 if it does not fit.
-static int coresident_grid(const void *k, size_t smem) {
-    if (smem > 227 * 1024 - 64) return 0;
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
-    int dev = 0, nsm = 0, occ = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kBlock, smem) != cudaSuccess) return 0;
-    return nsm * occ;
-}
-
 static int mixed_multi_grid(int TY3, int TY2) {
-    return coresident_grid((const void *)k_mixed_dyn<27, 16, true>, mixed_multi_smem(TY3, TY2));
+    return smem_grid((const void *)k_mixed_dyn<27, 16, true>, mixed_multi_smem(TY3, TY2));
 }
 
-// Co-resident CTAs of the dynamic kernel at tile height TY (sets its shared-memory attribute;
-// call outside any stream capture).
+// Co-resident CTAs of the dynamic kernel at tile height TY (0 if it does not fit).
 static int mixed_dyn_grid(bool is3d, int nzm, int TY) {
-    const size_t smem = mixed_smem(is3d, nzm, TY, false);
-    if (smem > 227 * 1024 - 64) return 0;
-    const void *k = mixed_dyn_kernel(is3d, nzm);
-    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
-    int dev = 0, nsm = 0, occ = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
-    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kBlock, smem) != cudaSuccess) return 0;
-    return nsm * occ;
+    return smem_grid(mixed_dyn_kernel(is3d, nzm), mixed_smem(is3d, nzm, TY, false));
 }
 
 static int mixed_dyn_dispatch(bool is3d, int nzm, const MDesc *d, MState *const *st, const unsigned *tick0, int nsolve,
