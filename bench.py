@@ -231,6 +231,7 @@ def run_cfg4(args):
     """64 sliding 3D ice streams, n ~ U{64..256} vertices per side, 11 levels, each with its own seeded
     log-normal friction; SIA preconditioner, tol 1e-8.  A step = one replay of the CUDA graph that runs
     all 64 solves from x0 = 0 in one persistent launch of the mixed-precision kernel."""
+    import tempfile
     import torch
     world, rank, local = dist_setup(args)
     torch.cuda.set_device(local)
@@ -240,6 +241,10 @@ def run_cfg4(args):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         pg = dist
+    # the tile tuner times this workload's own systems (a table left by earlier processes on the
+    # machine, e.g. small test batches, would otherwise decide the batch tile floor)
+    tile_cache = os.path.join(tempfile.mkdtemp(prefix="cismgpu-bench-"), "tiles.txt")
+    os.environ["CISMGPU_TILE_CACHE"] = tile_cache
     t0 = time.perf_counter()
     probs = cfg4_problems(max(1, (os.cpu_count() or 1) // world))
     t_gen = time.perf_counter() - t0

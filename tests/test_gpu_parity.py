@@ -249,7 +249,7 @@ def test_golden_dense_solutions(gpu_lib):
     data = np.load(os.path.join(os.path.dirname(__file__), "golden", "dense_kat.npz"))
     from tests.test_oracle_kat import owned_active_mask
     for name in ("slab3d", "slab2d"):
-        P = problems.slab_3d(seed=21, nz=4) if name == "slab3d" else problems.slab_2d(seed=22)
+        P = problems.slab_3d(seed=21, nz=4, symmetrize=False) if name == "slab3d" else problems.slab_2d(seed=22)
         m = owned_active_mask(P)
         for alg in ("standard", "chrongear"):
             st, xu, xv, err, nit = gpu_solve(alg, P, 1, tol=1e-10, maxiters=10000)

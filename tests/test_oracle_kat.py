@@ -494,7 +494,7 @@ def test_golden_dense_solutions():
     path = os.path.join(GOLDEN, "dense_kat.npz")
     data = np.load(path)
     for name in ("slab3d", "slab2d"):
-        P = problems.slab_3d(seed=21, nz=4) if name == "slab3d" else problems.slab_2d(seed=22)
+        P = problems.slab_3d(seed=21, nz=4, symmetrize=False) if name == "slab3d" else problems.slab_2d(seed=22)
         np.testing.assert_array_equal(P.bu, data[f"{name}_bu"])  # generator unchanged
         xs_u, xs_v = data[f"{name}_xu"], data[f"{name}_xv"]
         for alg in ("standard", "chrongear"):
