@@ -4,13 +4,14 @@
 // compute_element_matrix (:8001-8123) and element_to_global_matrix_3d (:8200-8268).
 //
 // The reference loops over the elements (active cells j, i, then layers k) and adds each 8x8
-// element matrix into the 27-point rows of its 8 nodes.  Here one thread owns one matrix row
-// (node k, i, j) and gathers instead: it visits the (up to) 8 elements that contain its node in
-// the reference's element order (j, then i, then k), recomputes each element's quadrature (the
-// element's 8 nodes, Jacobian, basis derivatives, viscosity) and adds the element's row for its
-// node, column by column, to its 4 x 27 accumulators.  Every coefficient thus receives the
-// same terms in the same order as in the reference, with no atomics; the cost is each element
-// evaluated once per node (8 times), which is FP64 ALU work on data read once from HBM.
+// element matrix into the 27-point rows of its 8 nodes.  Here the 3D stiffness is built in two
+// kernels per slab of cell rows: k_asm_elements3d evaluates every element's quadrature once
+// (the element's 8 Gauss points on 8 threads, shared through shared memory, then its 8 rows on
+// 8 threads) into a scratch of element matrices that L2 keeps, and k_asm_gather3d has one
+// thread per matrix row (node k, i, j) sum the rows of the (up to) 8 elements that contain its
+// node in the reference's element order (j, then i, then k).  Every coefficient thus receives
+// the same terms in the same order as in the reference, with no atomics.  The 2D kernels keep
+// the gather-and-recompute form (4-point cells, one thread per vertex).
 // The arithmetic is the reference's operation for operation (the library is built without FMA
 // contraction); only pow (the flow law's (effstrain^2)^((1-n)/2n), and the flow-factor option's
 // power, which the host evaluates once) is CUDA's rather than the host C library's.
@@ -49,164 +50,264 @@ struct AsmArgs {
     int *singular;                                // set when an element's Jacobian is singular
 };
 
-// The row of node nr of element (ie, je, ke) (1-based) added to the accumulators acc[b][m]:
-// the element's quadrature loop (:5502-5571) restricted to row nr of Kuu, Kuv, Kvu, Kvv.
-// Returns false for a singular Jacobian.  The element's own thread also writes its mean
-// viscosity (:5575-5581).
-__device__ bool asm_element_row(const AsmArgs &a, int ie, int je, int ke, int nr, bool own, double acc[4][27]) {
-    const long long NX = a.nx - 1;
-    double x[8], y[8], z[8], u[8], v[8];
+// Node n of an element relative to node 7, as constant expressions (the gather below resolves
+// its coupling indices at compile time)
+__host__ __device__ constexpr int ish7(int n) { return (n == 0 || n == 3 || n == 4 || n == 7) ? -1 : 0; }
+__host__ __device__ constexpr int jsh7(int n) { return (n % 4 < 2) ? -1 : 0; }
+__host__ __device__ constexpr int ksh7(int n) { return n < 4 ? 1 : 0; }
+
+// Element matrices are built element by element into a scratch of cell-row slabs, then gathered
+// node by node.  Scratch layout: K[b][nr][nc][e], b = Kuu, Kuv, Kvu, Kvv, row nr and column nc of
+// the 8x8 element matrix, e = (ie-1) + nx*((ke-1) + (nz-1)*(je-je0)) the slab's element index.
+constexpr int kAsmEl = 16;                        // elements per block of k_asm_elements3d
+constexpr int kAsmElThreads = 8 * kAsmEl;         // one thread per (element, Gauss point / row)
+static_assert(kAsmEl == 16, "k_asm_elements3d maps a warp to 2 x 16 elements");
+constexpr size_t kAsmScratchBytes = 64ull << 20;  // slab scratch budget (L2 keeps it between the kernels)
+
+// One Gauss point of one element: the basis-function derivatives, the viscosity and the
+// quadrature factor efvs * w * detJ / vol0 that every entry of the element matrix takes.
+struct AsmPt {
+    double dx[8], dy[8], dz[8];
+    double f, efvs;
+};
+
+// get_basis_function_derivatives_3d (:6508-6732) and compute_effective_viscosity (:7285-7470)
+// at Gauss point p of the element with nodes x, y, z, u, v and flow factor ff.  Returns false
+// for a singular Jacobian.
+__device__ bool asm_point3d(const AsmArgs &a, int p, const double (&x)[8], const double (&y)[8],
+                            const double (&z)[8], const double (&u)[8], const double (&v)[8], double ff, AsmPt &o) {
+    const double *dxr = c_asm_ref.dxr[p], *dyr = c_asm_ref.dyr[p], *dzr = c_asm_ref.dzr[p];
+    double J00 = 0.0, J01 = 0.0, J02 = 0.0, J10 = 0.0, J11 = 0.0, J12 = 0.0, J20 = 0.0, J21 = 0.0, J22 = 0.0;
 #pragma unroll
     for (int n = 0; n < 8; ++n) {
-        const int iN = ie + c_ish7[n], jN = je + c_jsh7[n], kN = ke + c_ksh7[n];
-        const long long q = (long long)(iN - 1) + NX * (jN - 1);
-        x[n] = a.xv[q];
-        y[n] = a.yv[q];
-        z[n] = a.usrf[q] - a.sigma[kN - 1] * a.thck[q];
-        const long long e = a.vel_planes ? (long long)(kN - 1) * NX * (a.ny - 1) + q : (long long)(kN - 1) + a.nz * q;
-        u[n] = a.u[e];
-        v[n] = a.v[e];
+        J00 = J00 + dxr[n] * x[n];
+        J01 = J01 + dxr[n] * y[n];
+        J02 = J02 + dxr[n] * z[n];
+        J10 = J10 + dyr[n] * x[n];
+        J11 = J11 + dyr[n] * y[n];
+        J12 = J12 + dyr[n] * z[n];
+        J20 = J20 + dzr[n] * x[n];
+        J21 = J21 + dzr[n] * y[n];
+        J22 = J22 + dzr[n] * z[n];
     }
-    const double ff = a.flwafact[(ke - 1) + (long long)(a.nz - 1) * ((ie - 1) + (long long)a.nx * (je - 1))];
-    double Kuu[8], Kuv[8], Kvu[8], Kvv[8];
+    const double c00 = J11 * J22 - J12 * J21, c01 = -(J10 * J22 - J12 * J20), c02 = J10 * J21 - J11 * J20;
+    const double c10 = -(J01 * J22 - J02 * J21), c11 = J00 * J22 - J02 * J20, c12 = -(J00 * J21 - J01 * J20);
+    const double c20 = J01 * J12 - J02 * J11, c21 = -(J00 * J12 - J02 * J10), c22 = J00 * J11 - J01 * J10;
+    const double detJ = J00 * c00 + J01 * c01 + J02 * c02;
+    if (!(fabs(detJ) > 0.0)) return false;
+    // Jinv(row,col) = cofactor(col,row) / detJ
+    const double i00 = c00 / detJ, i01 = c10 / detJ, i02 = c20 / detJ;
+    const double i10 = c01 / detJ, i11 = c11 / detJ, i12 = c21 / detJ;
+    const double i20 = c02 / detJ, i21 = c12 / detJ, i22 = c22 / detJ;
 #pragma unroll
-    for (int nc = 0; nc < 8; ++nc) Kuu[nc] = Kuv[nc] = Kvu[nc] = Kvv[nc] = 0.0;
-    double esum = 0.0;
-    for (int p = 0; p < 8; ++p) {
-        const double *dxr = c_asm_ref.dxr[p], *dyr = c_asm_ref.dyr[p], *dzr = c_asm_ref.dzr[p];
-        // get_basis_function_derivatives_3d
-        double J00 = 0.0, J01 = 0.0, J02 = 0.0, J10 = 0.0, J11 = 0.0, J12 = 0.0, J20 = 0.0, J21 = 0.0, J22 = 0.0;
+    for (int n = 0; n < 8; ++n) {
+        o.dx[n] = i00 * dxr[n] + i01 * dyr[n] + i02 * dzr[n];
+        o.dy[n] = i10 * dxr[n] + i11 * dyr[n] + i12 * dzr[n];
+        o.dz[n] = i20 * dxr[n] + i21 * dyr[n] + i22 * dzr[n];
+    }
+    double efvs;
+    if (a.whichefvs == 0) {
+        efvs = a.efvs_constant;
+    } else if (a.whichefvs == 1) {
+        efvs = ff * a.flowfact_pow;
+    } else {
+        double du_dx = 0.0, du_dy = 0.0, du_dz = 0.0, dv_dx = 0.0, dv_dy = 0.0, dv_dz = 0.0, sq;
+        const double em2 = a.effstrain_min * a.effstrain_min;
+        if (a.whichapprox == 0) {
 #pragma unroll
-        for (int n = 0; n < 8; ++n) {
-            J00 = J00 + dxr[n] * x[n];
-            J01 = J01 + dxr[n] * y[n];
-            J02 = J02 + dxr[n] * z[n];
-            J10 = J10 + dyr[n] * x[n];
-            J11 = J11 + dyr[n] * y[n];
-            J12 = J12 + dyr[n] * z[n];
-            J20 = J20 + dzr[n] * x[n];
-            J21 = J21 + dzr[n] * y[n];
-            J22 = J22 + dzr[n] * z[n];
-        }
-        const double c00 = J11 * J22 - J12 * J21, c01 = -(J10 * J22 - J12 * J20), c02 = J10 * J21 - J11 * J20;
-        const double c10 = -(J01 * J22 - J02 * J21), c11 = J00 * J22 - J02 * J20, c12 = -(J00 * J21 - J01 * J20);
-        const double c20 = J01 * J12 - J02 * J11, c21 = -(J00 * J12 - J02 * J10), c22 = J00 * J11 - J01 * J10;
-        const double detJ = J00 * c00 + J01 * c01 + J02 * c02;
-        if (!(fabs(detJ) > 0.0)) return false;
-        // Jinv(row,col) = cofactor(col,row) / detJ
-        const double i00 = c00 / detJ, i01 = c10 / detJ, i02 = c20 / detJ;
-        const double i10 = c01 / detJ, i11 = c11 / detJ, i12 = c21 / detJ;
-        const double i20 = c02 / detJ, i21 = c12 / detJ, i22 = c22 / detJ;
-        double dx[8], dy[8], dz[8];
-#pragma unroll
-        for (int n = 0; n < 8; ++n) {
-            dx[n] = i00 * dxr[n] + i01 * dyr[n] + i02 * dzr[n];
-            dy[n] = i10 * dxr[n] + i11 * dyr[n] + i12 * dzr[n];
-            dz[n] = i20 * dxr[n] + i21 * dyr[n] + i22 * dzr[n];
-        }
-        // compute_effective_viscosity
-        double efvs;
-        if (a.whichefvs == 0) {
-            efvs = a.efvs_constant;
-        } else if (a.whichefvs == 1) {
-            efvs = ff * a.flowfact_pow;
+            for (int n = 0; n < 8; ++n) {
+                du_dz = du_dz + o.dz[n] * u[n];
+                dv_dz = dv_dz + o.dz[n] * v[n];
+            }
+            sq = em2 + 0.25 * (du_dz * du_dz + dv_dz * dv_dz);
         } else {
-            double du_dx = 0.0, du_dy = 0.0, du_dz = 0.0, dv_dx = 0.0, dv_dy = 0.0, dv_dz = 0.0, sq;
-            const double em2 = a.effstrain_min * a.effstrain_min;
-            if (a.whichapprox == 0) {
 #pragma unroll
-                for (int n = 0; n < 8; ++n) {
-                    du_dz = du_dz + dz[n] * u[n];
-                    dv_dz = dv_dz + dz[n] * v[n];
-                }
-                sq = em2 + 0.25 * (du_dz * du_dz + dv_dz * dv_dz);
-            } else {
-#pragma unroll
-                for (int n = 0; n < 8; ++n) {
-                    du_dx = du_dx + dx[n] * u[n];
-                    du_dy = du_dy + dy[n] * u[n];
-                    if (a.whichapprox != 1) du_dz = du_dz + dz[n] * u[n];
-                    dv_dx = dv_dx + dx[n] * v[n];
-                    dv_dy = dv_dy + dy[n] * v[n];
-                    if (a.whichapprox != 1) dv_dz = dv_dz + dz[n] * v[n];
-                }
-                const double sh = dv_dx + du_dy;
-                sq = em2 + (du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * (sh * sh));
-                if (a.whichapprox != 1) sq = sq + 0.25 * (du_dz * du_dz + dv_dz * dv_dz);
+            for (int n = 0; n < 8; ++n) {
+                du_dx = du_dx + o.dx[n] * u[n];
+                du_dy = du_dy + o.dy[n] * u[n];
+                if (a.whichapprox != 1) du_dz = du_dz + o.dz[n] * u[n];
+                dv_dx = dv_dx + o.dx[n] * v[n];
+                dv_dy = dv_dy + o.dy[n] * v[n];
+                if (a.whichapprox != 1) dv_dz = dv_dz + o.dz[n] * v[n];
             }
-            efvs = ff * pow(sq, a.p_half);
+            const double sh = dv_dx + du_dy;
+            sq = em2 + (du_dx * du_dx + dv_dy * dv_dy + du_dx * dv_dy + 0.25 * (sh * sh));
+            if (a.whichapprox != 1) sq = sq + 0.25 * (du_dz * du_dz + dv_dz * dv_dz);
         }
-        esum = esum + efvs;
-        // compute_element_matrix, row nr
-        const double f = efvs * c_asm_ref.wqp[p] * detJ / kAsmVol0;
-#pragma unroll
-        for (int nc = 0; nc < 8; ++nc) {
-            if (a.whichapprox == 0) {
-                Kuu[nc] = Kuu[nc] + f * (dz[nr] * dz[nc]);
-                Kvv[nc] = Kvv[nc] + f * (dz[nr] * dz[nc]);
-            } else if (a.whichapprox == 1) {
-                Kuu[nc] = Kuu[nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc]);
-                Kuv[nc] = Kuv[nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
-                Kvu[nc] = Kvu[nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
-                Kvv[nc] = Kvv[nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc]);
-            } else {
-                Kuu[nc] = Kuu[nc] + f * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc] + dz[nr] * dz[nc]);
-                Kuv[nc] = Kuv[nc] + f * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc]);
-                Kvu[nc] = Kvu[nc] + f * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc]);
-                Kvv[nc] = Kvv[nc] + f * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc] + dz[nr] * dz[nc]);
-            }
-        }
+        efvs = ff * pow(sq, a.p_half);
     }
-    if (own) a.efvs[(ke - 1) + (long long)(a.nz - 1) * ((ie - 1) + (long long)a.nx * (je - 1))] = esum / 8;
-    // element_to_global_matrix_3d, row nr
-#pragma unroll
-    for (int nc = 0; nc < 8; ++nc) {
-        const int m = (c_ish7[nc] - c_ish7[nr] + 1) + 3 * (c_jsh7[nc] - c_jsh7[nr] + 1) +
-                      9 * (c_ksh7[nc] - c_ksh7[nr] + 1);
-        acc[0][m] = acc[0][m] + Kuu[nc];
-        acc[1][m] = acc[1][m] + Kuv[nc];
-        acc[2][m] = acc[2][m] + Kvu[nc];
-        acc[3][m] = acc[3][m] + Kvv[nc];
-    }
+    o.efvs = efvs;
+    o.f = efvs * c_asm_ref.wqp[p] * detJ / kAsmVol0;
     return true;
 }
 
-// One thread per node (k, q = i + NX*j, 0-based): the elements that contain the node, in the
-// reference's element order (j, then i, then k), each valid when its cell is one the reference
-// loops over (nhalo+1..n-nhalo+1), is active, and its layer exists; then the node's 4 x 27
-// coefficients in layout L (every coefficient of every node is written, zero where no element
-// contributes, as the reference zeroes A first).
-__global__ void __launch_bounds__(kAsmBlock) k_assemble3d(AsmArgs a, SymIdx L, double *Auu, double *Auv,
-                                                          double *Avu, double *Avv) {
-    const long long NX = a.nx - 1, NQ = NX * (a.ny - 1);
-    const long long n = (long long)a.nz * NQ;
-    const long long t = (long long)blockIdx.x * kAsmBlock + threadIdx.x;
-    if (t >= n) return;
-    const int k0 = (int)(t / NQ);
-    const long long q = t - (long long)k0 * NQ;
-    const int j0 = (int)(q / NX), i0 = (int)(q - (long long)j0 * NX);
-    const int iR = i0 + 1, jR = j0 + 1, kR = k0 + 1;  // 1-based node
-    double acc[4][27];
+// The element matrices of the cell rows je0 .. je0+nrows-1 (1-based), every layer: the
+// reference's element loop body (:5502-5581), each element's quadrature evaluated once.  A block
+// holds kAsmEl elements.  Phase 1, thread (element, p): the element's nodes and Gauss point p
+// into shared memory.  Phase 2, 8 threads an element: the four 8x8 blocks,
+// compute_element_matrix (:8001-8123) over the points in order, into the scratch K.  An element
+// outside the reference's cell loop (nhalo+1..n-nhalo+1) or inactive writes nothing (the gather
+// never reads it).  Its first thread writes the element's mean viscosity (:5575-5581) when its
+// own node (ie-1, je-1, ke-1) is a vertex with je-1 in [jown0, jown1).
+__global__ void __launch_bounds__(kAsmElThreads) k_asm_elements3d(AsmArgs a, int je0, int nrows, int jown0,
+                                                                  int jown1, double *__restrict__ K, long long ks) {
+    __shared__ AsmPt sp[8][kAsmEl];
+    __shared__ int sval[kAsmEl];
+    const int nzl1 = a.nz - 1;
+    const long long nel = (long long)a.nx * nzl1 * nrows;
+    const long long NX = a.nx - 1;
+    const int tid = threadIdx.x, el = tid % kAsmEl, sub = tid / kAsmEl;
+    const long long e = (long long)blockIdx.x * kAsmEl + el;
+    int ie = 0, je = 0, ke = 0;
+    bool valid = false;
+    if (e < nel) {
+        ie = (int)(e % a.nx) + 1;
+        const long long r = e / a.nx;
+        ke = (int)(r % nzl1) + 1;
+        je = je0 + (int)(r / nzl1);
+        valid = ie >= a.nhalo + 1 && ie <= a.nx - a.nhalo + 1 && je >= a.nhalo + 1 && je <= a.ny - a.nhalo + 1 &&
+                a.active_cell[(ie - 1) + (long long)a.nx * (je - 1)] != 0;
+    }
+    if (sub == 0) sval[el] = valid;
+    if (valid) {  // phase 1: Gauss point p = sub
+        double x[8], y[8], z[8], u[8], v[8];
 #pragma unroll
-    for (int b = 0; b < 4; ++b)
+        for (int n = 0; n < 8; ++n) {
+            const int iN = ie + ish7(n), jN = je + jsh7(n), kN = ke + ksh7(n);
+            const long long q = (long long)(iN - 1) + NX * (jN - 1);
+            x[n] = a.xv[q];
+            y[n] = a.yv[q];
+            z[n] = a.usrf[q] - a.sigma[kN - 1] * a.thck[q];
+            const long long ev = a.vel_planes ? (long long)(kN - 1) * NX * (a.ny - 1) + q : (long long)(kN - 1) + a.nz * q;
+            u[n] = a.u[ev];
+            v[n] = a.v[ev];
+        }
+        const double ff = a.flwafact[(ke - 1) + (long long)nzl1 * ((ie - 1) + (long long)a.nx * (je - 1))];
+        if (!asm_point3d(a, sub, x, y, z, u, v, ff, sp[sub][el])) atomicExch(a.singular, 1);
+    }
+    __syncthreads();
+    if (!valid) return;
+    // phase 2.  The blocks' entries are products the reference forms in an order that makes
+    // Kuu and Kvv symmetric and Kvu the transpose of Kuv bit for bit ((4 a) b and (4 b) a, (2 a) b
+    // and (2 b) a round the same exact product; a b = b a).  Warp w (r = w) takes rows r and
+    // 7 - r of the upper triangle (columns >= the row, 9 entries, written with their mirrors)
+    // of Kuu in its first half-warp and of Kvv in its second, and each thread one row of Kuv
+    // (urow = 2 w + half, written with its transpose in Kvu): 17 entries a thread instead of
+    // 32, warp-uniform, each summed over the points in order, as compute_element_matrix does.
+    // Kvv's entries are Kuu's with dx and dy exchanged: 4 dy dy + dx dx (+ dz dz).
+    const int r = tid / 32, comp = (tid / kAsmEl) % 2, r2 = 7 - r, urow = 2 * r + comp;
+    double U[8], Sa[8], Sb[8];  // Kuv row urow; rows r (columns >= r) and 7 - r (columns >= 7 - r)
 #pragma unroll
-        for (int c = 0; c < 27; ++c) acc[b][c] = 0.0;
-    for (int dj = 0; dj < 2; ++dj)
-        for (int di = 0; di < 2; ++di)
-            for (int dk = 0; dk < 2; ++dk) {
-                const int je = jR + dj, ie = iR + di, ke = kR - 1 + dk;
-                if (ke < 1 || ke > a.nz - 1) continue;
-                if (ie < a.nhalo + 1 || ie > a.nx - a.nhalo + 1 || je < a.nhalo + 1 || je > a.ny - a.nhalo + 1)
-                    continue;
-                if (!a.active_cell[(ie - 1) + (long long)a.nx * (je - 1)]) continue;
-                // node index within the element: shifts (iR-ie, jR-je, kR-ke) = (-di, -dj, 1-dk)
-                const int nr = (dk == 0 ? 0 : 4) + (dj == 0 ? (di == 0 ? 2 : 3) : (di == 0 ? 1 : 0));
-                if (!asm_element_row(a, ie, je, ke, nr, dj == 0 && di == 0 && dk == 1, acc)) atomicExch(a.singular, 1);
+    for (int nc = 0; nc < 8; ++nc) U[nc] = Sa[nc] = Sb[nc] = 0.0;
+    for (int p = 0; p < 8; ++p) {
+        const AsmPt &P = sp[p][el];
+        const double f = P.f;
+        const double *p1 = comp == 0 ? P.dx : P.dy, *p2 = comp == 0 ? P.dy : P.dx;
+        const double a1 = p1[r], a2 = p2[r], az = P.dz[r];
+        const double b1 = p1[r2], b2 = p2[r2], bz = P.dz[r2];
+        const double ux = P.dx[urow], uy = P.dy[urow];
+#pragma unroll
+        for (int nc = 0; nc < 8; ++nc) {
+            const double cx = P.dx[nc], cy = P.dy[nc], cz = P.dz[nc];
+            const double c1 = comp == 0 ? cx : cy, c2 = comp == 0 ? cy : cx;
+            if (a.whichapprox != 0) U[nc] = U[nc] + f * (2.0 * ux * cy + uy * cx);
+            if (a.whichapprox == 0) {
+                if (nc >= r) Sa[nc] = Sa[nc] + f * (az * cz);
+                if (nc >= r2) Sb[nc] = Sb[nc] + f * (bz * cz);
+            } else if (a.whichapprox == 1) {
+                if (nc >= r) Sa[nc] = Sa[nc] + f * (4.0 * a1 * c1 + a2 * c2);
+                if (nc >= r2) Sb[nc] = Sb[nc] + f * (4.0 * b1 * c1 + b2 * c2);
+            } else {
+                if (nc >= r) Sa[nc] = Sa[nc] + f * (4.0 * a1 * c1 + a2 * c2 + az * cz);
+                if (nc >= r2) Sb[nc] = Sb[nc] + f * (4.0 * b1 * c1 + b2 * c2 + bz * cz);
             }
-    double *B[4] = {Auu, Auv, Avu, Avv};
+        }
+    }
+    const int bs = comp == 0 ? 0 : 3;  // Kuu or Kvv
 #pragma unroll
-    for (int b = 0; b < 4; ++b)
-        for (int c = 0; c < 27; ++c) B[b][L.at(c, k0, q)] = acc[b][c];
+    for (int nc = 0; nc < 8; ++nc) {
+        if (nc >= r) {
+            K[(long long)((bs * 8 + r) * 8 + nc) * ks + e] = Sa[nc];
+            if (nc != r) K[(long long)((bs * 8 + nc) * 8 + r) * ks + e] = Sa[nc];
+        }
+        if (nc >= r2) {
+            K[(long long)((bs * 8 + r2) * 8 + nc) * ks + e] = Sb[nc];
+            if (nc != r2) K[(long long)((bs * 8 + nc) * 8 + r2) * ks + e] = Sb[nc];
+        }
+        K[(long long)((1 * 8 + urow) * 8 + nc) * ks + e] = U[nc];  // Kuv(urow, nc)
+        K[(long long)((2 * 8 + nc) * 8 + urow) * ks + e] = U[nc];  // Kvu(nc, urow)
+    }
+    if (sub == 0 && ie - 1 < NX && je - 1 < a.ny - 1 && je - 1 >= jown0 && je - 1 < jown1) {
+        double esum = 0.0;
+        for (int p = 0; p < 8; ++p) esum = esum + sp[p][el].efvs;
+        a.efvs[(ke - 1) + (long long)nzl1 * ((ie - 1) + (long long)a.nx * (je - 1))] = esum / 8;
+    }
+}
+
+// Element slot s = 4 dj + 2 di + dk of a node (the element at cell (i+1+di, j+1+dj), layer k+dk,
+// 1-based node (i, j, k)): the node's row in that element (shifts (-di, -dj, 1-dk) from node 7),
+// and the element column that lands on the node's coupling m, or -1.
+__host__ __device__ constexpr int asm_slot_row(int s) {
+    return ((s % 2) == 0 ? 0 : 4) + ((s / 4) == 0 ? (((s / 2) % 2) == 0 ? 2 : 3) : (((s / 2) % 2) == 0 ? 1 : 0));
+}
+__host__ __device__ constexpr int asm_col_coupling(int nr, int nc) {
+    return (ish7(nc) - ish7(nr) + 1) + 3 * (jsh7(nc) - jsh7(nr) + 1) + 9 * (ksh7(nc) - ksh7(nr) + 1);
+}
+__host__ __device__ constexpr int asm_slot_col(int s, int m) {
+    return asm_col_coupling(asm_slot_row(s), 0) == m ? 0
+         : asm_col_coupling(asm_slot_row(s), 1) == m ? 1
+         : asm_col_coupling(asm_slot_row(s), 2) == m ? 2
+         : asm_col_coupling(asm_slot_row(s), 3) == m ? 3
+         : asm_col_coupling(asm_slot_row(s), 4) == m ? 4
+         : asm_col_coupling(asm_slot_row(s), 5) == m ? 5
+         : asm_col_coupling(asm_slot_row(s), 6) == m ? 6
+         : asm_col_coupling(asm_slot_row(s), 7) == m ? 7 : -1;
+}
+
+// element_to_global_matrix_3d (:8200-8268) as a gather: one thread per node (k0, i0, j0),
+// 0-based, of the vertex rows j0 in [ja, jb), and block b = blockIdx.y, over the (up to) 8
+// elements that contain the node in the reference's element order (j, then i, then k), each
+// valid when its cell is one the reference loops over, is active, and its layer exists.  The coefficient for coupling m of
+// block b sums, in that order, the column of the element's row for the node that lands on m
+// (slot, row and column are compile-time constants: one running sum at a time).
+// Every coefficient of every node in the rows is written, zero where no element contributes
+// (the reference zeroes A first).  je0: the scratch slab's first cell row.
+__global__ void __launch_bounds__(kAsmBlock) k_asm_gather3d(AsmArgs a, SymIdx L, int ja, int jb, int je0,
+                                                            const double *__restrict__ K, long long ks,
+                                                            double *Auu, double *Auv, double *Avu, double *Avv) {
+    const long long NX = a.nx - 1, NQ = NX * (a.ny - 1);
+    const long long nrow = (long long)(jb - ja) * NX;
+    const long long t = (long long)blockIdx.x * kAsmBlock + threadIdx.x;
+    if (t >= (long long)a.nz * nrow) return;
+    const int k0 = (int)(t / nrow);
+    const long long rem = t - (long long)k0 * nrow;
+    const int j0 = ja + (int)(rem / NX), i0 = (int)(rem % NX);
+    const long long q = (long long)j0 * NX + i0;
+    const int iR = i0 + 1, jR = j0 + 1, kR = k0 + 1;
+    const int nzl1 = a.nz - 1;
+    long long es[8];
+    bool ok[8];
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const int dj = s / 4, di = (s / 2) % 2, dk = s % 2;
+        const int je = jR + dj, ie = iR + di, ke = kR - 1 + dk;
+        ok[s] = ke >= 1 && ke <= nzl1 && ie >= a.nhalo + 1 && ie <= a.nx - a.nhalo + 1 && je >= a.nhalo + 1 &&
+                je <= a.ny - a.nhalo + 1 && a.active_cell[(ie - 1) + (long long)a.nx * (je - 1)] != 0;
+        es[s] = (long long)(ie - 1) + (long long)a.nx * ((ke - 1) + (long long)nzl1 * (je - je0));
+    }
+    const int b = blockIdx.y;  // the block: Kuu, Kuv, Kvu, Kvv
+    const double *Kb = K + (long long)(b * 64) * ks;
+    double *Bb = b == 0 ? Auu : b == 1 ? Auv : b == 2 ? Avu : Avv;
+#pragma unroll
+    for (int m = 0; m < 27; ++m) {
+        double acc = 0.0;
+#pragma unroll
+        for (int s = 0; s < 8; ++s) {
+            const int nc = asm_slot_col(s, m);
+            if (nc >= 0 && ok[s]) acc = acc + Kb[(long long)(asm_slot_row(s) * 8 + nc) * ks + es[s]];
+        }
+        Bb[L.at(m, k0, q)] = acc;
+    }
 }
 
 // ---------------------------------------------------------------------------

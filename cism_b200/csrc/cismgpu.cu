@@ -106,6 +106,8 @@ static int check_device() {
 }
 
 static inline unsigned nblocks(long long n, int b = kBlock) { return (unsigned)((n + b - 1) / b); }
+// rows of blocks (levels in parallel) for the halo of a matrix's 27 nz coefficient planes
+constexpr unsigned kHaloPlaneRows = 64;
 static inline bool is_check(int iter, int ncheck) { return (iter % ncheck == 0) || iter == 5; }
 
 struct Ptrs {
@@ -171,6 +173,7 @@ struct Solver {
     DevBuf rprod;             // reproducible-sum solves: the two product fields and the flag
     bool repro = false;       // parallel%reprosum: the FP64 solvers' global sums are reproducible sums
     DevBuf asm_in;            // the stiffness assembly's inputs (geometry, flow factor, velocity, efvs)
+    DevBuf asm_k;             // 3D assembly: element matrices of one slab of cell rows
     DevBuf bc_in;             // the boundary terms' inputs (beta, lsrf, masks, velocity)
     DevBuf diva_in;           // the DIVA assembly's inputs and outputs
     DevBuf diva_eq[2];        // DIVA's layer viscosities per Gauss point, previous and new
@@ -202,6 +205,7 @@ struct Solver {
         x_sav.release();
         rsum.release();
         asm_in.release();
+        asm_k.release();
         bc_in.release();
         diva_in.release();
         diva_eq[0].release();
@@ -263,7 +267,11 @@ struct Solver {
         x_current = false;
         CU(vec.ensure((size_t)NVEC * nvec * sizeof(double)));
         CU(raw.ensure((size_t)nvec * sizeof(double)));
-        CU(partials.ensure((size_t)nblocks(g.NQ) * 2 * sizeof(DD)));
+        // the block partials of a reduction, then one counter per column block (the 3D matvec's
+        // dot products: k_mv_nodes), zero between launches
+        const size_t nbq = nblocks(g.NQ);
+        CU(partials.ensure(nbq * 2 * sizeof(DD) + nbq * sizeof(unsigned)));
+        CU(cudaMemsetAsync(partials.as<DD>() + 2 * nbq, 0, nbq * sizeof(unsigned), stream));
         CU(state.ensure(sizeof(SolveState)));
         return CISMGPU_OK;
     }
@@ -445,8 +453,29 @@ struct Solver {
         a.vel_planes = host_vel ? 0 : 1;
         a.flwafact = d_ff; a.efvs = d_efvs; a.singular = d_sing;
         if (three_d) {
-            const long long n = (long long)nzl * g.NQ;
-            k_assemble3d<<<(unsigned)((n + kAsmBlock - 1) / kAsmBlock), kAsmBlock, 0, s>>>(a, L, Auu, Auv, Avu, Avv);
+            // element matrices by slabs of cell rows into a scratch L2 can keep, each slab then
+            // gathered into the rows of its vertex rows: vertex rows [ja, jb) take the cell rows
+            // ja+1 .. jb+1 (1-based), so consecutive slabs share one cell row
+            const long long per_row = (long long)nx * (nzl - 1);  // elements per cell row
+            const long long row_bytes = per_row * 256 * (long long)sizeof(double);
+            int vrows = (int)g.NY;
+            if (row_bytes > 0) {
+                const long long fit = (long long)(kAsmScratchBytes / (size_t)row_bytes) - 1;
+                vrows = (int)std::max<long long>(1, std::min<long long>(fit, (long long)g.NY));
+            }
+            const long long ks = std::max<long long>(1, per_row * (vrows + 1));
+            CU(asm_k.ensure((size_t)ks * 256 * sizeof(double)));
+            double *K = asm_k.as<double>();
+            for (int ja = 0; ja < (int)g.NY; ja += vrows) {
+                const int jb = std::min((int)g.NY, ja + vrows), nrows = jb - ja + 1;
+                const long long nel = per_row * nrows;
+                if (nel > 0)
+                    k_asm_elements3d<<<(unsigned)((nel + kAsmEl - 1) / kAsmEl), kAsmElThreads, 0, s>>>(
+                        a, ja + 1, nrows, ja, jb, K, ks);
+                const long long nn = (long long)nzl * (jb - ja) * g.NX;
+                k_asm_gather3d<<<dim3((unsigned)((nn + kAsmBlock - 1) / kAsmBlock), 4), kAsmBlock, 0, s>>>(
+                    a, L, ja, jb, ja + 1, K, ks, Auu, Auv, Avu, Avv);
+            }
         } else if (l1l2) {
             L1l2Args l;
             l.dsdx = d_sx; l.dsdy = d_sy; l.flwa = d_fl;
@@ -3213,8 +3242,8 @@ int cismgpu_solver_assemble_system_3d(cismgpu_solver_t *h, int nhalo, double dx,
     gA.nz = 27 * sv.g.nz;
     const unsigned hb = nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4));
     cudaStream_t s = sv.stream;
-    k_halo<<<hb, kBlock, 0, s>>>(gA, A0, A0 + bs, nullptr);
-    k_halo<<<hb, kBlock, 0, s>>>(gA, A0 + 2 * bs, A0 + 3 * bs, nullptr);
+    k_halo<<<dim3(hb, kHaloPlaneRows), kBlock, 0, s>>>(gA, A0, A0 + bs, nullptr);
+    k_halo<<<dim3(hb, kHaloPlaneRows), kBlock, 0, s>>>(gA, A0 + 2 * bs, A0 + 3 * bs, nullptr);
     k_halo<<<hb, kBlock, 0, s>>>(sv.g, p.bu, p.bv, nullptr);
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(s));
@@ -3293,8 +3322,8 @@ int cismgpu_solver_assemble_system_2d(cismgpu_solver_t *h, int nz, int nhalo, do
     gA.nz = 9;
     const unsigned hb = nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4));
     cudaStream_t s = sv.stream;
-    k_halo<<<hb, kBlock, 0, s>>>(gA, A0, A0 + bs, nullptr);
-    k_halo<<<hb, kBlock, 0, s>>>(gA, A0 + 2 * bs, A0 + 3 * bs, nullptr);
+    k_halo<<<dim3(hb, kHaloPlaneRows), kBlock, 0, s>>>(gA, A0, A0 + bs, nullptr);
+    k_halo<<<dim3(hb, kHaloPlaneRows), kBlock, 0, s>>>(gA, A0 + 2 * bs, A0 + 3 * bs, nullptr);
     k_halo<<<hb, kBlock, 0, s>>>(sv.g, p.bu, p.bv, nullptr);
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(s));
@@ -3407,8 +3436,8 @@ int cismgpu_solver_assemble_system_2d_diva(
     gA.nz = 9;
     const unsigned hb = nblocks(4LL * sv.g.NX + 4LL * (sv.g.NY - 4));
     cudaStream_t s = sv.stream;
-    k_halo<<<hb, kBlock, 0, s>>>(gA, A0, A0 + bs, nullptr);
-    k_halo<<<hb, kBlock, 0, s>>>(gA, A0 + 2 * bs, A0 + 3 * bs, nullptr);
+    k_halo<<<dim3(hb, kHaloPlaneRows), kBlock, 0, s>>>(gA, A0, A0 + bs, nullptr);
+    k_halo<<<dim3(hb, kHaloPlaneRows), kBlock, 0, s>>>(gA, A0 + 2 * bs, A0 + 3 * bs, nullptr);
     k_halo<<<hb, kBlock, 0, s>>>(sv.g, p.bu, p.bv, nullptr);
     CU(cudaGetLastError());
     CU(cudaStreamSynchronize(s));

@@ -215,19 +215,56 @@ __device__ __forceinline__ void mv_row(const Geom &g, const double *__restrict__
 
 enum MvMode { MV_PLAIN = 0, MV_RESID, MV_DQ, MV_CG_AZ };
 
+constexpr int kDotChunk = 8;  // levels whose loads a column's dot terms issue together
+
+// The dot terms of column q (modes with dot products), added over k in level order: a chunk's
+// loads together, then its terms in order.  Loads through L2 (__ldcg): the other levels' y and
+// r were written by other CTAs of the same launch.
+template <int MODE>
+__device__ __forceinline__ void col_dots(const Geom &g, long long q, const double *__restrict__ xu,
+                                         const double *__restrict__ xv, const double *__restrict__ yu,
+                                         const double *__restrict__ yv, const double *__restrict__ ru,
+                                         const double *__restrict__ rv, DD &s0, DD &s1) {
+    for (int k0 = 0; k0 < g.nz; k0 += kDotChunk) {
+        double t0[kDotChunk], t1[kDotChunk];
+#pragma unroll
+        for (int u = 0; u < kDotChunk; ++u) {
+            t0[u] = t1[u] = 0.0;
+            if (k0 + u >= g.nz) continue;
+            const long long e = (long long)(k0 + u) * g.NQ + q;
+            if (MODE == MV_RESID) {
+                const double r1 = __ldcg(ru + e), r2 = __ldcg(rv + e);
+                t0[u] = __dadd_rn(__dmul_rn(r1, r1), __dmul_rn(r2, r2));
+            } else if (MODE == MV_DQ) {
+                t0[u] = __dadd_rn(__dmul_rn(__ldcg(xu + e), __ldcg(yu + e)), __dmul_rn(__ldcg(xv + e), __ldcg(yv + e)));
+            } else if (MODE == MV_CG_AZ) {
+                const double z1 = __ldcg(xu + e), z2 = __ldcg(xv + e);
+                t0[u] = __dadd_rn(__dmul_rn(__ldcg(ru + e), z1), __dmul_rn(__ldcg(rv + e), z2));
+                t1[u] = __dadd_rn(__dmul_rn(__ldcg(yu + e), z1), __dmul_rn(__ldcg(yv + e), z2));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kDotChunk; ++u)
+            if (k0 + u < g.nz) {
+                s0 = dd_add_d(s0, t0[u]);
+                if (MODE == MV_CG_AZ) s1 = dd_add_d(s1, t1[u]);
+            }
+    }
+}
+
 // y = A x over owned active columns, 0 elsewhere; optional fused statements:
 //   MV_RESID : r = b - y (whole array); S0 = (r,r)             [:1454-1466, :3504-3516]
 //   MV_DQ    : S0 = (x,y) with x = d, y = q                    [:1376-1381, :3241-3248]
 //   MV_CG_AZ : S0 = (r,z), S1 = (y,z) with x = z, y = Az       [:3401-3413]
-// The structured matvec runs as two kernels in 3D.  k_mv_nodes: one thread per node (column
-// q, level k = blockIdx.y), y = A x with the reference's statements (mv_row), and for MV_RESID
-// also r = b - y: every (column, level) is independent, so a launch has nz * NQ/256 CTAs and
-// enough loads in flight to stream the 108 coefficient planes.  k_mv_dots (modes with dot
-// products): one thread per column adds its terms over k in level order, then the block tree
-// of the 256 columns and the last-CTA tree: the order the reduction has always had.  In 2D a
-// column has one level, so k_mv_nodes adds the terms and reduces itself.
+// k_mv_nodes: one thread per node (column q, level k = blockIdx.y), y = A x with the
+// reference's statements (mv_row), and for MV_RESID also r = b - y: every (column, level) is
+// independent, so a launch has nz * NQ/256 CTAs and enough loads in flight to stream the 108
+// coefficient planes.  Dot products in 3D: the last level block of each column block to
+// finish has one thread per column add its terms over k in level order (col_dots), then the
+// block tree of the 256 columns and the last-CTA tree: the order the reduction has always
+// had.  In 2D a column has one level, so every block adds its terms and reduces.
 template <int NC, int MODE>
-__global__ void __launch_bounds__(kBlock) k_mv_nodes(Geom g, const double *__restrict__ A,
+__global__ void __launch_bounds__(kBlock, 4) k_mv_nodes(Geom g, const double *__restrict__ A,
                                                      const int32_t *__restrict__ act,
                                                      const double *__restrict__ xu, const double *__restrict__ xv,
                                                      double *__restrict__ yu, double *__restrict__ yv,
@@ -272,50 +309,33 @@ __global__ void __launch_bounds__(kBlock) k_mv_nodes(Geom g, const double *__res
         if (MODE == MV_CG_AZ) reduce_and_finish_first<2>(rc, s0, s1);
         else reduce_and_finish_first<1>(rc, s0, s1);
     }
-}
-
-constexpr int kDotChunk = 8;  // levels whose loads k_mv_dots issues together
-
-template <int MODE>
-__global__ void __launch_bounds__(kBlock) k_mv_dots(Geom g, const double *__restrict__ xu,
-                                                    const double *__restrict__ xv, const double *__restrict__ yu,
-                                                    const double *__restrict__ yv, const double *__restrict__ ru,
-                                                    const double *__restrict__ rv, RedCtx rc) {
-    if (rc.st->done) return;
-    const long long q = (long long)blockIdx.x * kBlock + threadIdx.x;
-    DD s0{0.0, 0.0}, s1{0.0, 0.0};
-    if (q < g.NQ) {
-        int i, j;
-        col_of(g, q, i, j);
-        if (owned(g, i, j))
-            for (int k0 = 0; k0 < g.nz; k0 += kDotChunk) {  // a chunk's loads together, then its terms in order
-                double t0[kDotChunk], t1[kDotChunk];
-#pragma unroll
-                for (int u = 0; u < kDotChunk; ++u) {
-                    t0[u] = t1[u] = 0.0;
-                    if (k0 + u >= g.nz) continue;
-                    const long long e = (long long)(k0 + u) * g.NQ + q;
-                    if (MODE == MV_RESID) {
-                        const double r1 = ru[e], r2 = rv[e];
-                        t0[u] = __dadd_rn(__dmul_rn(r1, r1), __dmul_rn(r2, r2));
-                    } else if (MODE == MV_DQ) {
-                        t0[u] = __dadd_rn(__dmul_rn(xu[e], yu[e]), __dmul_rn(xv[e], yv[e]));
-                    } else if (MODE == MV_CG_AZ) {
-                        const double z1 = xu[e], z2 = xv[e];
-                        t0[u] = __dadd_rn(__dmul_rn(ru[e], z1), __dmul_rn(rv[e], z2));
-                        t1[u] = __dadd_rn(__dmul_rn(yu[e], z1), __dmul_rn(yv[e], z2));
-                    }
-                }
-#pragma unroll
-                for (int u = 0; u < kDotChunk; ++u)
-                    if (k0 + u < g.nz) {
-                        s0 = dd_add_d(s0, t0[u]);
-                        if (MODE == MV_CG_AZ) s1 = dd_add_d(s1, t1[u]);
-                    }
-            }
+    if (NC == 27 && MODE != MV_PLAIN) {
+        // the last of the gridDim.y level blocks of column block blockIdx.x to finish adds the
+        // dot terms of its 256 columns over all levels, then the block tree and the last-CTA
+        // tree: the same order as a separate dot pass, without its launch and with the sums of
+        // the early column blocks overlapping the rest of the matvec.  The per-column-block
+        // counters sit after the partials and return to zero here.
+        __shared__ bool lastk;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned *cnt = reinterpret_cast<unsigned *>(rc.partials + 2 * gridDim.x) + blockIdx.x;
+            __threadfence();  // this block's y and r before its count
+            const unsigned t = atomicAdd(cnt, 1u);
+            lastk = t == gridDim.y - 1;
+            if (lastk) *cnt = 0u;
+        }
+        __syncthreads();
+        if (!lastk) return;
+        __threadfence();
+        DD d0{0.0, 0.0}, d1{0.0, 0.0};
+        if (q < g.NQ) {
+            int i, j;
+            col_of(g, q, i, j);
+            if (owned(g, i, j)) col_dots<MODE>(g, q, xu, xv, yu, yv, ru, rv, d0, d1);
+        }
+        if (MODE == MV_CG_AZ) reduce_and_finish_first<2>(rc, d0, d1);
+        else reduce_and_finish_first<1>(rc, d0, d1);
     }
-    if (MODE == MV_RESID || MODE == MV_DQ) reduce_and_finish_first<1>(rc, s0, s1);
-    if (MODE == MV_CG_AZ) reduce_and_finish_first<2>(rc, s0, s1);
 }
 
 // y = A x (+ the statement MODE fuses with it, see MvMode) on stream s.
@@ -325,8 +345,6 @@ inline void launch_mv(cudaStream_t s, const Geom &g, const double *A, const int3
                       double *rv, const RedCtx &rc) {
     const dim3 grid((unsigned)((g.NQ + kBlock - 1) / kBlock), (unsigned)g.nz);
     k_mv_nodes<NC, MODE><<<grid, kBlock, 0, s>>>(g, A, act, xu, xv, yu, yv, bu, bv, ru, rv, rc);
-    if (NC == 27 && MODE != MV_PLAIN)
-        k_mv_dots<MODE><<<grid.x, kBlock, 0, s>>>(g, xu, xv, yu, yv, ru, rv, rc);
 }
 
 // ---------------------------------------------------------------------------
@@ -849,7 +867,9 @@ __global__ void __launch_bounds__(kBlock) k_vec(Geom g, VecArgs v, RedCtx rc) {
 // pi(0)=NX-3, pi(1)=NX-2, pi(NX-1)=2 (identity otherwise): the composite of the
 // east-west exchange on owned rows followed by the north-south exchange on all
 // columns.  Sources are never halo positions, so one pass is race free.  Outflow
-// then zeroes i,j in {0, N-1}; no_ice zeroes i,j in {0,1,N-2,N-1}.
+// then zeroes i,j in {0, N-1}; no_ice zeroes i,j in {0,1,N-2,N-1}.  Levels k run over
+// blockIdx.y, blockIdx.y + gridDim.y, ... (many planes, such as the 27 nz coefficient planes of
+// a block, take a grid with several rows of blocks).
 __device__ __forceinline__ int pmap(int i, int N) {
     if (i == 0) return N - 3;
     if (i == 1) return N - 2;
@@ -880,7 +900,7 @@ __global__ void __launch_bounds__(kBlock) k_halo(Geom g, double *__restrict__ au
     else if (g.no_ice) zero = (i <= 1 || i >= NX - 2 || j <= 1 || j >= NY - 2);
     const long long q = (long long)j * NX + i;
     if (zero) {
-        for (int k = 0; k < g.nz; ++k) {
+        for (int k = blockIdx.y; k < g.nz; k += gridDim.y) {
             au[(long long)k * g.NQ + q] = 0.0;
             av[(long long)k * g.NQ + q] = 0.0;
         }
@@ -890,7 +910,7 @@ __global__ void __launch_bounds__(kBlock) k_halo(Geom g, double *__restrict__ au
         const bool halo = (i <= 1 || i == NX - 1 || j <= 1 || j == NY - 1);
         if (!halo) return;
         const long long s = (long long)pmap(j, NY) * NX + pmap(i, NX);
-        for (int k = 0; k < g.nz; ++k) {
+        for (int k = blockIdx.y; k < g.nz; k += gridDim.y) {
             au[(long long)k * g.NQ + q] = au[(long long)k * g.NQ + s];
             av[(long long)k * g.NQ + q] = av[(long long)k * g.NQ + s];
         }

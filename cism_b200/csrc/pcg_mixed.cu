@@ -165,6 +165,33 @@ __device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
     return v;
 }
 __device__ __forceinline__ void fence_acq_rel() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
+// Bulk copies global -> shared memory (the copy engine, no registers in flight) completing on
+// an mbarrier in the CTA's shared memory.  Addresses 16-byte aligned, sizes multiples of 16.
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long *m, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(m)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *m, unsigned bytes) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}" ::"r"(smem_u32(m)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *m) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(m))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *m, unsigned parity) {
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(m)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
 // The four words of a record, as two 16-byte relaxed loads (each 64-bit element is a
 // single-copy-atomic access).
 __device__ __forceinline__ void ld_rec(const TileRec *rp, unsigned long long (&w)[4]) {
@@ -282,6 +309,7 @@ struct MHead {
     int cur;                   // cache slot described by D
     double red[8][2];
     double rsum[8][2];
+    unsigned long long mbar;   // resident launches: completion of the matrix's bulk copies
     int nacq;                  // >= 0: the CTA reads the halo of acq[0..nacq) only; -1: fence
     int acq[kMaxAcq];
     int ntl;                   // static launches: tile list entries of this CTA
@@ -1293,15 +1321,36 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
         const int tx = T.tile % D.tiles_x, ty = T.tile / D.tiles_x;
         const int i0 = D.g.ilo + tx * kTX, j0 = D.g.jlo + ty * TY;
         const int NN = nz * NT;
-        for (int w = threadIdx.x; w < NC * NN; w += kBlock) {
-            const int it = w % NN, c = w / NN;
-            const int col = it % NT, k = it / NT;
-            const int i = i0 + col % kTX, j = j0 + col / kTX;
-            float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (i <= D.g.ihi && j <= D.g.jhi) a = D.A32[(size_t)c * plane + k * NQ + j * D.g.NX + i];
-            sA[w] = a;
+        // sA[c][k][tj][ti] = A32[c][k][j0+tj][i0+ti]: each (c, k, tj) row of the tile inside the
+        // grid is one bulk copy of ncol float4 (16-byte aligned at both ends); the columns past
+        // ihi and the rows past jhi are zeros stored by the threads (bytes no copy writes)
+        const int ncol = min(kTX, D.g.ihi - i0 + 1), nrow = min(TY, D.g.jhi - j0 + 1);
+        const int nrows = NC * nz * nrow;
+        if (threadIdx.x == 0) {
+            mbar_init(&hd.mbar, 1);
+            mbar_expect_tx(&hd.mbar, (unsigned)(nrows * ncol * 16));
         }
         __syncthreads();
+        for (int r = threadIdx.x; r < nrows; r += kBlock) {
+            const int tj = r % nrow, ck = r / nrow, k = ck % nz, c = ck / nz;
+            bulk_g2s(sA + (size_t)c * NN + k * NT + tj * kTX, D.A32 + (size_t)c * plane + k * NQ + (j0 + tj) * D.g.NX + i0,
+                     (unsigned)(ncol * 16), &hd.mbar);
+        }
+        for (int w = threadIdx.x; w < NC * NN; w += kBlock) {
+            const int col = (w % NN) % NT;
+            if (col % kTX >= ncol || col / kTX >= nrow) sA[w] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+        long long t0 = clock64();
+        bool ok = true;
+        while (!mbar_try_wait(&hd.mbar, 0u))
+            if (clock64() - t0 > c_wait_cycles) { ok = false; break; }
+        if (__syncthreads_or(!ok)) {  // the copies did not land: fail the launch, after one more
+            if (threadIdx.x == 0) atomicExch(&ctl->abort, 1);  // bounded wait for them
+            t0 = clock64();
+            while (!mbar_try_wait(&hd.mbar, 0u) && clock64() - t0 <= c_wait_cycles) {
+            }
+            return;
+        }
     }
     bool finished = false;
     int step = 0;
