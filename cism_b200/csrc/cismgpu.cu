@@ -1479,6 +1479,9 @@ static MDesc mixed_desc(const Solver &sv, int precond, int TY) {  // TY: the sol
     D.maps = m.maps;
     D.nbrs = m.nbrs;
     D.stream = (size_t)mixed_couplings(sv) * (size_t)nvec * sizeof(float4) > kStreamBytes ? 1 : 0;
+    D.tri = m.tri;
+    D.rs = m.tri ? m.tri + 8 * sv.g.NQ : nullptr;
+    D.zs = m.tri ? m.tri + 10 * sv.g.NQ : nullptr;
     return D;
 }
 
@@ -1579,8 +1582,9 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
     if (sv.g.nz > kMixedMaxNz) return fail(CISMGPU_EUNSUPPORTED, "mixed solver supports nz <= 32");
     if (8LL * sv.nvec >= (1LL << 31))  // the kernel indexes vector planes with 32-bit offsets
         return fail(CISMGPU_EUNSUPPORTED, "mixed solver supports nz*(nx-1)*(ny-1) < 2^28");
-    if (!(precond == 0 || precond == 1 || (precond == 2 && sv.is3d)))
-        return fail(CISMGPU_EUNSUPPORTED, "mixed solver preconditioners: 0, 1, or 2 (3D only)");
+    if (!(precond == 0 || precond == 1 || (precond == 2 && sv.is3d) || precond == CISMGPU_PRECOND_TRIDIAG_LOCAL ||
+          precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL))
+        return fail(CISMGPU_EUNSUPPORTED, "mixed solver preconditioners: 0, 1, 2 (3D only), 3 or 4");
     MixedBufs &m = sv.mixed;
     const long long nvec = sv.nvec;
     const int NC = sv.NC;
@@ -1666,19 +1670,46 @@ static int mixed_prepare(Solver &sv, int precond, int TY) {
         m.TY = TY;
     }
     if (m.precond != precond) {
+        const bool tri = precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL;
+        // the 3D line preconditioners start with the SIA column solves (tridiag_solver_local_3d)
+        const int kind = tri ? (NC == 27 ? CISMGPU_PRECOND_SIA : CISMGPU_PRECOND_NONE) : precond;
         if (NC == 27)
-            k_mixed_precond_setup<27><<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, precond, sv.A.as<double>(), m.pre);
+            k_mixed_precond_setup<27><<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, kind, sv.A.as<double>(), m.pre);
         else
-            k_mixed_precond_setup<9><<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, precond, sv.A.as<double>(), m.pre);
+            k_mixed_precond_setup<9><<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, kind, sv.A.as<double>(), m.pre);
         CU(cudaGetLastError());
+        if (tri) {  // the FP64 setup (its zero-pivot check included), then the FP32 factors
+            if (!m.tri) {
+                CU(cudaMalloc((void **)&m.tri, (size_t)12 * g.NQ * sizeof(float)));
+                m.nbytes += (size_t)12 * g.NQ * sizeof(float);
+            }
+            SolveState *st = sv.state.as<SolveState>();
+            k_init_state<<<1, 1, 0, sv.stream>>>(st, 0.0, 0);
+            TRY(sv.tri_setup(precond));
+            k_tri_to_f32<<<nblocks(g.NQ), kBlock, 0, sv.stream>>>(g, sv.tri.as<double>(), m.tri);
+            CU(cudaGetLastError());
+            int hst = 0;
+            CU(cudaMemcpyAsync(&hst, &st->status, sizeof(int), cudaMemcpyDeviceToHost, sv.stream));
+            CU(cudaStreamSynchronize(sv.stream));
+            if (hst == CISMGPU_EDIVZERO) {
+                m.precond = -1;
+                return fail(CISMGPU_EDIVZERO, "tridiagonal preconditioner setup met a zero pivot");
+            }
+        }
         m.precond = precond;
     }
     return CISMGPU_OK;
 }
 
-static MState mixed_init_state(double tol, int maxiters, int ncheck) {
+// precond 3 and 4 take three steps per iteration (MS_UPD, MS_LINES).  The mixed solver runs them to
+// the caller's maxiters: the reference's 2D budget of 100 iterations for these preconditioners
+// (maxiters_tridiag, glissade_velo_higher_pcg.F90:1703-1732, which the FP64 solvers keep) is a
+// heuristic for FP64 iterations, and the FP32 recurrences can need more of them.
+static MState mixed_init_state(double tol, int maxiters, int ncheck, int precond = 0) {
     MState S;
     std::memset(&S, 0, sizeof(S));
+    const bool tri = precond == CISMGPU_PRECOND_TRIDIAG_LOCAL || precond == CISMGPU_PRECOND_TRIDIAG_GLOBAL;
+    S.tri = tri ? 1 : 0;
     S.tol = tol;
     S.maxiters = maxiters;
     S.ncheck = ncheck;
@@ -1831,7 +1862,7 @@ static int mixed_run(Solver &sv, int precond, int ncheck, double tol, int maxite
     MixedBufs &m = sv.mixed;
     const bool resident = mixed_resident(is3d, nzm, TY, m.ntiles);
     const MDesc D = mixed_desc(sv, precond, TY);
-    const MState S0 = mixed_init_state(tol, maxiters, ncheck);
+    const MState S0 = mixed_init_state(tol, maxiters, ncheck, precond);
     CU(cudaMemcpyAsync(m.desc, &D, sizeof(MDesc), cudaMemcpyHostToDevice, stream));
     CU(cudaMemcpyAsync(m.state, &S0, sizeof(MState), cudaMemcpyHostToDevice, stream));
     CU(cudaMemsetAsync(m.ctl, 0, sizeof(MCtl), stream));
@@ -2413,7 +2444,7 @@ static int batch_prepare(MixedBatch &B, int precond, int ncheck, double tol, int
         descs[t] = mixed_desc(*B.svs[t], precond, tys[t]);
         dst[t] = B.svs[t]->state.as<SolveState>();
     }
-    const std::vector<MState> states(n, mixed_init_state(tol, maxiters, ncheck));
+    const std::vector<MState> states(n, mixed_init_state(tol, maxiters, ncheck, precond));
     const std::vector<unsigned> tick0(n, 0u);
     MCtl c0;
     std::memset(&c0, 0, sizeof(c0));

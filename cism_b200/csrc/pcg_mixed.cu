@@ -38,7 +38,11 @@ constexpr int kMixedMaxNz = 32;                  // shared-memory bound of the m
 // replacement together); the owners' in-place d and x writes of that update are deferred
 // to the next step (MS_A_UPD, or MS_FIN when the solve stops there), so that no tile reads
 // a neighbour's half-updated d or x while it recomputes the halo of x.
-enum MStep { MS_INIT = 0, MS_A, MS_MERGED, MS_B, MS_CHECK_UNUSED, MS_DONE, MS_BC, MS_A_UPD, MS_FIN };
+// The tridiagonal line preconditioners (precond 3, 4) need the whole domain's residual before any
+// line is solved, so an iteration takes three steps: MS_UPD (the update alone, the tile's line
+// right-hand sides), MS_LINES (the line solves) and MS_A / MS_A_UPD (the preconditioner, which reads
+// the line solution, then the stencil product and the dots).
+enum MStep { MS_INIT = 0, MS_A, MS_MERGED, MS_B, MS_CHECK_UNUSED, MS_DONE, MS_BC, MS_A_UPD, MS_FIN, MS_UPD, MS_LINES };
 
 // A tile's partial sums of one step (two sums).  Every 64-bit word carries the step number
 // (tag) in its high half and one 32-bit half of a sum in its low half (w[2i] low, w[2i+1]
@@ -91,6 +95,11 @@ struct MDesc {
     const int *nbrs;     // [ntiles][kNbrStride] tiles owning the tile's live halo columns (k_tile_nbrs)
     int stream;          // matrix loads evict-first (the FP32 matrix exceeds kStreamBytes)
     int sym;             // 3D, exactly symmetric: A32 and A64i hold the symmetric half (k_to_half)
+    // precond 3, 4: FP32 line factors [u, v][sub, 1/diag, omega, 1/denom][NQ], the lines' right-hand
+    // sides rs and solution zs [u, v][NQ]; u planes transposed (column i, row j at i*NY + j) so that
+    // the u lines, one per owned row, load and store coalesced
+    const float *tri;
+    float *rs, *zs;
 };
 
 struct MState {
@@ -100,6 +109,8 @@ struct MState {
     int done, status, niters;
     int checks, fp32_matvecs, fp64_matvecs;
     unsigned tick;       // steps completed (the tag of the last records summed)
+    int tri;             // precond 3, 4: iterations take the MS_UPD, MS_LINES steps
+    int after;           // the step that follows MS_LINES
 };
 
 struct MTile { int solve, tile; };
@@ -227,7 +238,8 @@ __device__ void advance_state(MState &S, double S0, double S1) {
             S.done = 1;
             S.step = MS_DONE;
         } else {
-            S.step = MS_A;
+            S.step = S.tri ? MS_LINES : MS_A;
+            S.after = MS_A;
         }
         break;
     case MS_A:       // S0 = (r,z), S1 = (Az,z) of iteration iter
@@ -253,9 +265,19 @@ __device__ void advance_state(MState &S, double S0, double S1) {
         }
         // iteration iter's update comes next: with the FP64 check at check iterations, alone
         // at the last iteration, merged with the next iteration's first half otherwise
-        S.step = is_check_it(S.iter, S.ncheck) ? MS_BC : (S.iter >= S.maxiters ? MS_B : MS_MERGED);
+        S.step = is_check_it(S.iter, S.ncheck) ? MS_BC
+                 : (S.iter >= S.maxiters ? MS_B : (S.tri ? MS_UPD : MS_MERGED));
         break;
     }
+    case MS_UPD:  // line preconditioners: iteration iter's update, then the lines of iter + 1
+        S.par ^= 1;
+        S.iter += 1;
+        S.step = MS_LINES;
+        S.after = MS_A;
+        break;
+    case MS_LINES:
+        S.step = S.after;
+        break;
     case MS_B:  // last iteration without a check
         S.par ^= 1;
         S.niters = S.maxiters;
@@ -275,7 +297,8 @@ __device__ void advance_state(MState &S, double S0, double S1) {
             S.step = MS_FIN;
         } else {
             S.iter += 1;
-            S.step = MS_A_UPD;
+            S.step = S.tri ? MS_LINES : MS_A_UPD;
+            S.after = MS_A_UPD;
         }
         break;
     case MS_FIN:  // the deferred x and d writes are done
@@ -776,6 +799,101 @@ __device__ __forceinline__ void fill_x_tile(const MDesc &D, const int *smap, int
     }
 }
 
+// Line preconditioners (precond 3, 4): the right-hand sides of the line solves for the tile's
+// owned columns, from the residual rb this step wrote -- per column and component the sum over
+// levels in level order (3D, as tridiag_solver_local_3d sums r, glissade_velo_higher_pcg.F90:
+// 4585-4590), r itself in 2D -- with the u component transposed.  rb is read back through L2 after
+// a barrier (this CTA's threads wrote it).
+template <int NC, int NZM>
+__device__ __forceinline__ void tri_rhs(const MDesc &D, int TY, int i0, int j0, const float *rb) {
+    const Geom &g = D.g;
+    const int nz = (NC == 27) ? g.nz : 1;
+    const int NQ = (int)g.NQ, plane = nz * NQ, NT = kTX * TY;
+    for (int it = threadIdx.x; it < 2 * NT; it += kBlock) {
+        const int c = it / NT, col = it - c * NT;
+        const int i = i0 + col % kTX, j = j0 + col / kTX;
+        if (i > g.ihi || j > g.jhi) continue;
+        const int q = j * g.NX + i;
+        const float *r = rb + c * plane + q;
+        float v[NZM];
+#pragma unroll
+        for (int k = 0; k < NZM; ++k) v[k] = (k < nz) ? ldf(r + k * NQ) : 0.0f;
+        float sum = v[0];
+#pragma unroll
+        for (int k = 1; k < NZM; ++k)
+            if (k < nz) sum += v[k];
+        D.rs[c * NQ + (c == 0 ? i * g.NY + j : q)] = sum;
+    }
+}
+
+// The line solves of one step (tridiag_solver_local_2d, :4985-5013 along rows for u, :5041-5069
+// along columns for v), in FP32 with the factors of the FP64 setup: forward elimination
+// gamma_s = (b_s - sub_s gamma_{s-1}) / denom_s (gamma_s0 = b_s0 / diag_s0), then back
+// substitution z_s = gamma_s - omega_s z_{s+1} over the owned range.  One thread per line: u lines
+// over the owned rows, then v lines over the owned columns, spread over the solve's tiles (tile t
+// takes lines t*256 + thread, then + ntiles*256).  Both kinds index their planes s*stride + line
+// (u planes transposed), so a warp's 32 consecutive lines load and store 128 contiguous bytes per
+// position.  Loads of kLineBatch positions are issued before the recurrence runs through them.
+constexpr int kLineBatch = 16;
+__device__ void lines_step(const MDesc &D, int tile) {
+    const Geom &g = D.g;
+    const int NQ = (int)g.NQ;
+    const int nu = g.jhi - g.jlo + 1, nv = g.ihi - g.ilo + 1;
+    for (int L = tile * kBlock + (int)threadIdx.x; L < nu + nv; L += D.ntiles * kBlock) {
+        const bool uline = L < nu;
+        const int l = uline ? g.jlo + L : g.ilo + (L - nu);
+        const int stride = uline ? g.NY : g.NX;
+        const int s0 = uline ? g.ilo : g.jlo, s1 = uline ? g.ihi : g.jhi;
+        const float *__restrict__ F = D.tri + (uline ? 0 : 4) * (size_t)NQ;
+        const float *__restrict__ sub = F, *__restrict__ adr = F + NQ, *__restrict__ om = F + 2 * NQ,
+                                  *__restrict__ den = F + 3 * NQ;
+        const float *b = D.rs + (uline ? 0 : NQ);
+        float *x = D.zs + (uline ? 0 : NQ);
+        float gp = ldf(b + s0 * stride + l) * __ldg(adr + s0 * stride + l);
+        x[s0 * stride + l] = gp;
+#pragma unroll 1
+        for (int s = s0 + 1; s <= s1; s += kLineBatch) {
+            float vb[kLineBatch], vs[kLineBatch], vd[kLineBatch];
+#pragma unroll
+            for (int u = 0; u < kLineBatch; ++u) {
+                vb[u] = vs[u] = vd[u] = 0.0f;
+                if (s + u <= s1) {
+                    const int e = (s + u) * stride + l;
+                    vb[u] = ldf(b + e);
+                    vs[u] = __ldg(sub + e);
+                    vd[u] = __ldg(den + e);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kLineBatch; ++u)
+                if (s + u <= s1) {
+                    gp = fmaf(-vs[u], gp, vb[u]) * vd[u];
+                    x[(s + u) * stride + l] = gp;
+                }
+        }
+        float xn = gp;
+#pragma unroll 1
+        for (int s = s1 - 1; s >= s0; s -= kLineBatch) {
+            float vg[kLineBatch], vo[kLineBatch];
+#pragma unroll
+            for (int u = 0; u < kLineBatch; ++u) {
+                vg[u] = vo[u] = 0.0f;
+                if (s - u >= s0) {
+                    const int e = (s - u) * stride + l;
+                    vg[u] = ldf(x + e);  // this thread's own forward store
+                    vo[u] = __ldg(om + e);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kLineBatch; ++u)
+                if (s - u >= s0) {
+                    xn = fmaf(-vo[u], xn, vg[u]);
+                    x[(s - u) * stride + l] = xn;
+                }
+        }
+    }
+}
+
 // One tile of one solve for the solve's current step; publishes the tile's record.
 template <int NC, int NZM>
 __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, MHead &hd, unsigned char *smem) {
@@ -798,6 +916,7 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
     const int t = threadIdx.x;
     const int step = S.step;
     const int par = S.par;
+    const bool tri = D.precond >= 3;  // the line preconditioners
     double p0 = 0.0, p1 = 0.0;
 
     if (!resident) {  // resident launches keep their single tile's map for the whole launch
@@ -819,10 +938,20 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
             p0 = p1;
             p1 = 0.0;
         }
+        if (tri) {
+            __syncthreads();
+            tri_rhs<NC, NZM>(D, TY, i0, j0, D.r[upd ? par ^ 1 : par]);
+        }
+    } else if (step == MS_LINES) {
+        lines_step(D, tile);
     } else if (step == MS_INIT) {
         if (NC == 27 && D.sym) residual_pass<NC, true, true>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
         else if (D.A64i) residual_pass<NC, true>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
         else residual_pass<NC, false>(D, smap, TY, i0, j0, par, nullptr, 0.0, p0, p1);
+        if (tri) {
+            __syncthreads();
+            tri_rhs<NC, NZM>(D, TY, i0, j0, D.r[par]);
+        }
     } else if (step == MS_BC) {
         // update of iteration iter fused with the FP64 check: dn = z + beta d on tile and halo
         // slots (into shared memory, over the z rows), q for the owned columns; the owners'
@@ -876,6 +1005,10 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
         else residual_pass<NC, false>(D, smap, TY, i0, j0, par ^ 1, sdn, S.alpha, p0, p1);
         p0 = p1;
         p1 = 0.0;
+        if (tri) {
+            __syncthreads();
+            tri_rhs<NC, NZM>(D, TY, i0, j0, D.r[par ^ 1]);
+        }
     } else if (step == MS_FIN) {
         // the deferred owner writes of the last (checked) update
         const float beta = (float)S.beta;
@@ -895,7 +1028,7 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
     } else {
         const float alpha = (float)S.alpha, beta = (float)S.beta;
         const double alpha64 = S.alpha;
-        const bool do_b = (step == MS_MERGED || step == MS_B);
+        const bool do_b = (step == MS_MERGED || step == MS_B || step == MS_UPD);
         const bool do_a = (step == MS_MERGED || step == MS_A || step == MS_A_UPD);
         const bool upd = (step == MS_A_UPD);  // apply the owners' deferred d and x writes
         const int rin = par, rout = do_b ? (par ^ 1) : par;  // buffers holding r_i / r_{i+1}
@@ -943,7 +1076,8 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                         sr[u] = (c * NZM + k) * NT + (li - 1) + kTX * (lj - 1);
                     const int v = smap[sl];
                     vv[u] = v;
-                    const int m = map_live(v) ? map_src(v) : -1;
+                    // an update alone (MS_B, MS_UPD) writes only the tile's own columns
+                    const int m = (map_live(v) && (do_a || map_mine(v))) ? map_src(v) : -1;
                     if (m >= 0) {
                         const int e = c * plane + k * NQ + m;
                         ee[u] = e;
@@ -1001,6 +1135,10 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                 }
             }
         }
+        if (tri && !do_a) {  // MS_UPD: the right-hand sides of the next lines
+            __syncthreads();
+            tri_rhs<NC, NZM>(D, TY, i0, j0, r_out);
+        }
         if (do_a) {
             if (NC == 27) {  // zero padding rows (levels -1 and nz)
                 for (int it = t; it < 2 * NS; it += kBlock) {
@@ -1010,7 +1148,7 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                 }
             }
             __syncthreads();
-            if (NC == 27 && D.precond == 2) {  // column tridiagonal solves on tile + halo
+            if (NC == 27 && (D.precond == 2 || tri)) {  // column tridiagonal solves on tile + halo
                 // one (column, component) per thread while they fit the block: the two
                 // components' recurrences then run side by side instead of one after the other
                 const bool split = 2 * NS <= kBlock;
@@ -1019,6 +1157,21 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
                     const int c = split ? it / NS : 0, sl = split ? it - c * NS : it;
                     const int v = smap[sl];
                     if (map_live(v)) sia_col<NZM>(D, sz, NS, sl, map_src(v), c, split ? c : 1);
+                }
+                __syncthreads();
+            }
+            if (tri) {  // + the line solution of the column (3D: on every level), or z = it (2D)
+                for (int it = t; it < 2 * NS; it += kBlock) {
+                    const int c = it >= NS ? 1 : 0, sl = it - c * NS;
+                    const int v = smap[sl];
+                    if (!map_live(v)) continue;
+                    const int m = map_src(v);
+                    const float zl = (c == 0) ? ldf(D.zs + (m % g.NX) * g.NY + m / g.NX) : ldf(D.zs + NQ + m);
+                    if (NC == 27) {
+                        for (int k = 0; k < nz; ++k) sz[(c * KP + k + OFF) * NS + sl] += zl;
+                    } else {
+                        sz[(c * KP + OFF) * NS + sl] = zl;
+                    }
                 }
                 __syncthreads();
             }
@@ -1289,14 +1442,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_mixed(const MDesc *__restrict__ d
         }
         hd.nsolve = n;
         hd.cur = -1;
-        // one solve: acquire only the tiles whose columns this CTA's halo reads
+        // one solve: acquire only the tiles whose columns this CTA's halo reads (the line
+        // preconditioners read every tile's columns: fence)
         int na = (n == 1) ? 0 : -1;
         for (int w = blockIdx.x; w < ntiles && na >= 0; w += gridDim.x) {
             const MTile T = tiles[w];
             if (T.solve < 0) continue;
             const int *nb = descs[T.solve].nbrs + (size_t)T.tile * kNbrStride;
             const int cnt = nb[0];
-            if (cnt < 0 || na + cnt > kMaxAcq) { na = -1; break; }
+            if (cnt < 0 || na + cnt > kMaxAcq || descs[T.solve].precond >= 3) { na = -1; break; }
             for (int k = 0; k < cnt; ++k) hd.acq[na++] = nb[1 + k];
         }
         hd.nacq = na;
@@ -1673,6 +1827,20 @@ __global__ void k_mixed_precond_setup(Geom g, int precond, const double *__restr
     }
 }
 
+// FP32 factors of the line preconditioners (precond 3, 4) from the FP64 setup's planes (k_tri_coef,
+// k_tri_factor): [u, v][sub, 1/diag, omega, 1/denom][NQ], the u planes transposed (column i, row j
+// at i*NY + j) for the coalesced u lines of lines_step.
+__global__ void k_tri_to_f32(Geom g, const double *__restrict__ T, float *__restrict__ out) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= g.NQ) return;
+    const long long i = q % g.NX, j = q / g.NX, tq = i * g.NY + j;
+    const int f[4] = {TU_SUB, TU_ADR, TU_OM, TU_DEN};
+    for (int k = 0; k < 4; ++k) {
+        out[k * g.NQ + tq] = (float)T[(long long)f[k] * g.NQ + q];
+        out[(4 + k) * g.NQ + q] = (float)T[(long long)(f[k] - TU_SUB + TV_SUB) * g.NQ + q];
+    }
+}
+
 // Device buffers of the mixed solver for one system (owned by the host Solver).
 struct MixedBufs {
     bool valid = false;
@@ -1687,6 +1855,7 @@ struct MixedBufs {
     bool il = false;           // A64i holds the full interleaved FP64 copy (streamed, not symmetric)
     int *flag = nullptr;       // device word of the symmetry test
     float *pre = nullptr, *vec = nullptr;
+    float *tri = nullptr;      // precond 3, 4: line factors [8][NQ], rs [2][NQ], zs [2][NQ]
     int *maps = nullptr;
     int *nbrs = nullptr;
     TileRec *recs = nullptr;
@@ -1701,8 +1870,9 @@ struct MixedBufs {
     long long maps_cap = 0;
     void release() {
         for (void *p : {(void *)A32, (void *)A64i, (void *)pre, (void *)vec, (void *)recs, (void *)state, (void *)desc,
-                        (void *)tiles, (void *)ctl, (void *)maps, (void *)nbrs, (void *)bc, (void *)flag})
+                        (void *)tiles, (void *)ctl, (void *)maps, (void *)nbrs, (void *)bc, (void *)flag, (void *)tri})
             if (p) cudaFree(p);
+        tri = nullptr;
         A32 = nullptr;
         A64i = nullptr;
         flag = nullptr;

@@ -53,14 +53,16 @@ struct SrvReq {
 
 // Device bytes a request's handle holds at most (the FP64 system, its staging block, the
 // FP64 and FP32 vectors, the FP32 matrix, the interleaved FP64 matrix of a 3D or streamed
-// solve, the factors, tile maps and records).
+// solve, the factors, tile maps and records; with the line preconditioners their FP64 setup
+// planes and FP32 factors and work planes).
 static size_t request_bytes(const cismgpu_request_t &r) {
     const long long NQ = (long long)(r.nx - 1) * (r.ny - 1);
     const long long nvec = NQ * (r.dims == 3 ? r.nz : 1);
     const long long NC = r.dims == 3 ? 27 : 9;
     const bool il = r.dims == 3 || (size_t)(NC * nvec) * 16 > kStreamBytes;
     const long long per = 4 * NC * 8 + NC * 8 + NVEC * 8 + 4 * NC * 4 + (il ? 4 * NC * 8 : 0) + 6 * 4 + 16 * 4;
-    return (size_t)(nvec * per + NQ * 16 + (8 << 20));
+    const long long lines = r.precond >= 3 ? NQ * (NTRI * 8 + 12 * 4) : 0;
+    return (size_t)(nvec * per + NQ * 16 + lines + (8 << 20));
 }
 
 static constexpr int kSrvClasses = 2;       // classes served by the dynamic kernel
@@ -141,7 +143,7 @@ static int srv_admit(SrvReq &r) {
     }
     TRY(mixed_prepare(sv, q.precond, r.TY));
     TRY(mixed_reset(sv, sv.stream));
-    const MState S0 = mixed_init_state(q.tolerance, q.maxiters, q.linear_solve_ncheck);
+    const MState S0 = mixed_init_state(q.tolerance, q.maxiters, q.linear_solve_ncheck, q.precond);
     CU(cudaMemcpyAsync(sv.mixed.state, &S0, sizeof(MState), cudaMemcpyHostToDevice, sv.stream));
     if (r.cls == 2) {
         const MDesc D = mixed_desc(sv, q.precond, r.TY);
@@ -441,8 +443,8 @@ int cismgpu_server_submit(cismgpu_server_t *S, const cismgpu_request_t *rq, long
     if (!S || !rq || !id || !rq->par || !rq->xu || !rq->xv) return fail(CISMGPU_EINVAL, "null argument");
     if (rq->dims != 2 && rq->dims != 3) return fail(CISMGPU_EINVAL, "dims must be 2 or 3");
     TRY(validate_solve_args(rq->precond, rq->linear_solve_ncheck, rq->maxiters));
-    if (!(rq->precond == 0 || rq->precond == 1 || (rq->precond == 2 && rq->dims == 3)))
-        return fail(CISMGPU_EUNSUPPORTED, "mixed solver preconditioners: 0, 1, or 2 (3D only)");
+    if (!(rq->precond >= 0 && rq->precond <= 4 && (rq->precond != 2 || rq->dims == 3)))
+        return fail(CISMGPU_EUNSUPPORTED, "mixed solver preconditioners: 0, 1, 2 (3D only), 3 or 4");
     if (rq->dims == 3 && (rq->nz < 1 || rq->nz > kMixedMaxNz)) return fail(CISMGPU_EUNSUPPORTED, "nz must be 1..32");
     SrvReq *r = new SrvReq();
     r->rq = *rq;

@@ -63,7 +63,7 @@ extern "C" {
 #define CISMGPU_OK                0
 #define CISMGPU_EBREAKDOWN_ETA1   1  /* eta1 = (r,z) is NaN   (reference :637, :1331)            */
 #define CISMGPU_EBREAKDOWN_ALPHA  2  /* alpha is NaN           (reference :697, :1391, :2196, :2467, :3263, :3434) */
-#define CISMGPU_EUNSUPPORTED      3  /* tasks_row*tasks_col > 1; mixed solver with precond 3,4   */
+#define CISMGPU_EUNSUPPORTED      3  /* tasks_row*tasks_col > 1; mixed solver with 2D precond 2  */
 #define CISMGPU_EINVAL            4  /* bad sizes, null pointers, inconsistent owned bounds     */
 #define CISMGPU_ECUDA             5  /* CUDA runtime error (message via cismgpu_last_error)     */
 #define CISMGPU_ETIMEOUT          6  /* a bounded device wait gave up                           */
@@ -430,7 +430,12 @@ int cismgpu_solver_create(cismgpu_solver_t **out, int dims, int nx, int ny, int 
 
 /* Solve from the stored x0; err/niters as in the reference calls (for the mixed
  * algorithm: err is the FP64 true relative residual, niters the total inner
- * iterations).  Blocks until the solve has finished. */
+ * iterations).  Blocks until the solve has finished.  The mixed algorithm takes
+ * precond 0, 1, 2 (3D) and the tridiagonal line preconditioners 3 and 4: their
+ * setup is the FP64 one (a zero pivot returns CISMGPU_EDIVZERO, x unchanged), the
+ * line solves run in FP32, and 2D solves run to maxiters (pcg_solver_chrongear_2d's
+ * budget of 100 iterations for these preconditioners, which the FP64 algorithms keep,
+ * counts FP64 iterations; the FP32 recurrences can need more). */
 int cismgpu_solver_solve(cismgpu_solver_t *s, int algorithm, int precond, int linear_solve_ncheck,
                          double tolerance, int maxiters, double *err, int *niters);
 

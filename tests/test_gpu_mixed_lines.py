@@ -1,0 +1,159 @@
+"""The tridiagonal line preconditioners (precond 3 local, 4 global) in the mixed-precision
+persistent kernels: an iteration takes an update step, a line-solve step and a
+preconditioner + stencil step (setup_preconditioner_tridiag_*, tridiag_solver_local_2d/3d,
+glissade_velo_higher_pcg.F90:3737-5100, used by pcg_solver_chrongear_* :1704-1880, :2916-3040).
+
+Every result is checked against the FP64 oracle running the reference algorithm with the same
+preconditioner: the FP64 true residual must reach the tolerance (recomputed on the CPU), x must
+agree with the oracle's solution within the bound of each case, and the iteration count must stay
+close to the FP64 count.  Batched and served results must be bit-identical to each system alone.
+"""
+import time
+
+import numpy as np
+import pytest
+
+import cism_b200 as cg
+import oracle
+from cism_b200 import assembly as asm
+from tests import problems
+from tests.test_gpu_mixed import rel, true_residual
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    ("dome-local", lambda: asm.dome(), 3, 1e-7),
+    ("dome-global", lambda: asm.dome(), 4, 1e-7),
+    ("slab3d-sliding-local", lambda: problems.slab_3d(seed=1, ewn=20, nsn=17), 3, 1e-5),
+    ("slab3d-noslip-local", lambda: problems.slab_3d(seed=5, sliding=False), 3, 1e-6),
+    ("slab3d-periodic-boundary-ice-global",
+     lambda: problems.slab_3d(seed=3, boundary_ice=True, sliding=False), 4, 1e-6),
+    ("slab2d-local", lambda: problems.slab_2d(seed=1), 3, 1e-5),
+    ("slab2d-global", lambda: problems.slab_2d(seed=1), 4, 1e-5),
+    ("slab2d-outflow-local", lambda: problems.slab_2d(seed=2, boundary_ice=True, bc="outflow"), 3, 1e-5),
+]
+
+
+@pytest.mark.parametrize("name,make,precond,xbound", CASES, ids=[c[0] for c in CASES])
+def test_mixed_line_preconditioners(gpu_lib, name, make, precond, xbound):
+    P = make()
+    S = cg.DeviceSolver(P)
+    err, nit = S.solve(cg.ALG_MIXED_CHRONGEAR, precond, 5, 1e-8, 3000)
+    xu, xv = S.x()
+    st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, precond, tol=1e-8, maxiters=3000)
+    assert st == 0 and oerr < 1e-8
+    assert err < 1e-8
+    assert true_residual(P, xu, xv) < 1.5e-8        # independent FP64 residual on the CPU
+    assert rel((xu, xv), (ou, ov), P) < xbound
+    # the small ill-conditioned 2D slabs are sensitive to FP32 rounding (as without a line
+    # preconditioner); the 3D systems stay close to the FP64 count
+    assert nit <= (2.0 if P.kind == "2d" else 1.5) * onit + 10
+
+
+def test_mixed_line_preconditioner_beats_sia_iterations(gpu_lib):
+    """On a sliding 3D member the line preconditioner converges in fewer iterations than the SIA
+    columns alone, as it does in the FP64 oracle (245 against 395)."""
+    P = asm.batch_member(33, seed=2, nz=7)
+    S = cg.DeviceSolver(P)
+    e3, n3 = S.solve(cg.ALG_MIXED_CHRONGEAR, 3, 5, 1e-8, 3000)
+    e2, n2 = S.solve(cg.ALG_MIXED_CHRONGEAR, 2, 5, 1e-8, 3000)
+    assert e3 < 1e-8 and e2 < 1e-8
+    assert n3 < n2
+
+
+def test_mixed_line_preconditioner_2d_runs_to_maxiters(gpu_lib):
+    """pcg_solver_chrongear_2d gives these preconditioners 100 FP64 iterations (:1703-1732), which
+    this SSA system does not converge in; the FP64 standard PCG, which has no such budget, converges
+    in 245.  The mixed solver runs to the caller's maxiters and converges to the same solution."""
+    P = asm.ssa_random(ewn=40, nsn=33, seed=10)
+    st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, 3, tol=1e-8, maxiters=5000)
+    assert st == 0 and onit == 100 and oerr > 1e-8
+    st, su, sv, serr, snit = oracle.pcg("standard", P, 3, tol=1e-8, maxiters=5000)
+    assert st == 0 and serr < 1e-8
+    S = cg.DeviceSolver(P)
+    err, nit = S.solve(cg.ALG_MIXED_CHRONGEAR, 3, 5, 1e-8, 5000)
+    xu, xv = S.x()
+    assert err < 1e-8 and true_residual(P, xu, xv) < 1.5e-8
+    assert nit <= 2 * snit + 10
+    assert rel((xu, xv), (su, sv), P) < 1e-5
+
+
+def test_mixed_line_preconditioner_deterministic(gpu_lib):
+    P = problems.slab_3d(seed=1, ewn=20, nsn=17)
+    S = cg.DeviceSolver(P)
+    a = S.solve(cg.ALG_MIXED_CHRONGEAR, 3, 5, 1e-8, 3000), S.x()
+    b = S.solve(cg.ALG_MIXED_CHRONGEAR, 3, 5, 1e-8, 3000), S.x()
+    assert a[0] == b[0]
+    np.testing.assert_array_equal(a[1][0], b[1][0])
+    np.testing.assert_array_equal(a[1][1], b[1][1])
+
+
+@pytest.mark.parametrize("precond", [3, 4])
+def test_batch_line_preconditioner_equals_alone(gpu_lib, precond):
+    """Uneven 3D members in one dynamic launch with a line preconditioner: bit-identical to each
+    member batched alone, converged, and within the tolerance's accuracy of the FP64 oracle."""
+    probs = [asm.batch_member(n, seed=s, nz=7) for s, n in enumerate((20, 27, 33))]
+    solvers = [cg.DeviceSolver(P) for P in probs]
+    alone = []
+    for S in solvers:
+        errs, nits, sts = cg.solve_batch([S], cg.ALG_MIXED_CHRONGEAR, precond, 5, 1e-8, 3000)
+        assert sts[0] == 0
+        alone.append((errs[0], nits[0], S.x()))
+    errs, nits, sts = cg.solve_batch(solvers, cg.ALG_MIXED_CHRONGEAR, precond, 5, 1e-8, 3000)
+    assert not np.any(sts)
+    for t, (S, P) in enumerate(zip(solvers, probs)):
+        xu, xv = S.x()
+        assert errs[t] < 1e-8 and errs[t] == alone[t][0] and nits[t] == alone[t][1]
+        np.testing.assert_array_equal(xu, alone[t][2][0])
+        np.testing.assert_array_equal(xv, alone[t][2][1])
+    st, ou, ov, oerr, onit = oracle.pcg("chrongear", probs[0], precond, tol=1e-8, maxiters=3000)
+    assert rel(solvers[0].x(), (ou, ov), probs[0]) < 1e-5
+
+
+def test_graph_batch_line_preconditioner_2d(gpu_lib):
+    """A CUDA-graph batch of 2D systems with the global line preconditioner replays bit for bit."""
+    probs = [problems.slab_2d(seed=1), problems.slab_2d(seed=2, boundary_ice=True, bc="outflow")]
+    solvers = [cg.DeviceSolver(P) for P in probs]
+    B = cg.GraphBatch(solvers, precond=4, ncheck=5, tol=1e-8, maxiters=3000)
+    try:
+        B.run()
+        e1, n1, s1 = B.wait()
+        x1 = [S.x() for S in solvers]
+        B.run()
+        e2, n2, s2 = B.wait()
+        assert not np.any(s1) and np.all(e1 < 1e-8)
+        assert list(e1) == list(e2) and list(n1) == list(n2)
+        for S, (u, v) in zip(solvers, x1):
+            xu, xv = S.x()
+            np.testing.assert_array_equal(xu, u)
+            np.testing.assert_array_equal(xv, v)
+    finally:
+        B.close()
+
+
+def test_served_line_preconditioners_alone_equals_mix(gpu_lib):
+    """Requests with line preconditioners served in a mix with diagonal and SIA requests (2D and 3D
+    in the same multi-class launch) give the same bits as each served alone."""
+    from tests.test_gpu_server import serve_alone
+    cases = [
+        (problems.slab_2d(seed=1), 3),
+        (asm.batch_member(24, seed=5, nz=7), 3),
+        (asm.ssa_random(ewn=61, nsn=57, seed=3), 1),
+        (asm.dome(), 4),
+        (asm.batch_member(27, seed=1, nz=7), 2),
+    ]
+    alone = [serve_alone(P, pc) for P, pc in cases]
+    S = cg.Server(hbm_budget_bytes=4 * 10**9, epoch_steps=16)
+    try:
+        ids = [S.submit(P, precond=pc, tol=1e-8, maxiters=5000) for P, pc in cases[:2]]
+        time.sleep(0.02)
+        ids += [S.submit(P, precond=pc, tol=1e-8, maxiters=5000) for P, pc in cases[2:]]
+        S.drain()
+        for (P, pc), rid, (au, av, ainfo) in zip(cases, ids, alone):
+            xu, xv, info = S.result(rid)
+            assert info["status"] == 0 and ainfo["status"] == 0 and info["err"] < 1e-8
+            assert info["err"] == ainfo["err"] and info["niters"] == ainfo["niters"]
+            np.testing.assert_array_equal(xu, au)
+            np.testing.assert_array_equal(xv, av)
+    finally:
+        S.close()
