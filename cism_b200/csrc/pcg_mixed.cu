@@ -503,21 +503,47 @@ __device__ __forceinline__ void sia_col(const MDesc &D, float *zc, int NS, int s
             fgm[k] = in ? __ldg(gm + k * NQ + q) : 0.0f;
         }
         // forward: y_1 = r_1/beta_1; y_k = (r_k - sb_k y_{k-1})/beta_k; back: z_k = y_k - gamma_{k+1} z_{k+1}
-        float prev = z[0] * fib[0];
-        z[0] = prev;
+        if (NZM <= 16) {
+            // the column in registers: its shared-memory loads issue together, and the recurrences
+            // wait on arithmetic alone (the same operations in the same order as below)
+            float zz[NZM];
 #pragma unroll
-        for (int k = 1; k < NZM; ++k)
-            if (k < nz) {
-                prev = (z[k * NS] - fsb[k] * prev) * fib[k];
-                z[k * NS] = prev;
-            }
-        float next = prev;
+            for (int k = 0; k < NZM; ++k) zz[k] = (k < nz) ? z[k * NS] : 0.0f;
+            float prev = zz[0] * fib[0];
+            zz[0] = prev;
 #pragma unroll
-        for (int k = NZM - 2; k >= 0; --k)
-            if (k < nz - 1) {
-                next = z[k * NS] - fgm[k + 1] * next;
-                z[k * NS] = next;
-            }
+            for (int k = 1; k < NZM; ++k)
+                if (k < nz) {
+                    prev = (zz[k] - fsb[k] * prev) * fib[k];
+                    zz[k] = prev;
+                }
+            float next = prev;
+#pragma unroll
+            for (int k = NZM - 2; k >= 0; --k)
+                if (k < nz - 1) {
+                    next = zz[k] - fgm[k + 1] * next;
+                    zz[k] = next;
+                }
+#pragma unroll
+            for (int k = 0; k < NZM; ++k)
+                if (k < nz) z[k * NS] = zz[k];
+        } else {
+            float prev = z[0] * fib[0];
+            z[0] = prev;
+#pragma unroll
+            for (int k = 1; k < NZM; ++k)
+                if (k < nz) {
+                    prev = (z[k * NS] - fsb[k] * prev) * fib[k];
+                    z[k * NS] = prev;
+                }
+            float next = prev;
+#pragma unroll
+            for (int k = NZM - 2; k >= 0; --k)
+                if (k < nz - 1) {
+                    next = z[k * NS] - fgm[k + 1] * next;
+                    z[k * NS] = next;
+                }
+        }
     }
 }
 
@@ -1045,7 +1071,7 @@ __device__ void tile_step(const MState &S, int tile, bool resident, int TYmax, M
 
         // ---- pass 1: update (B) on the tile, new residual (and diag z) on tile + halo ----
         // items (k, c, slot) in the order k, c, slot; kCh1 items' loads are issued together
-        constexpr int kCh1 = (NC == 27) ? 4 : 6;  // items per load batch (register budget)
+        constexpr int kCh1 = 6;  // items per load batch (register budget)
         const int per_k = 2 * NS;
         const int n1 = per_k * nz;
 #pragma unroll 1
