@@ -76,16 +76,24 @@ def run_profile(args):
         from cism_b200 import assembly as asm
         sizes = asm.batch_sizes(64)[:args.batch]
         solvers = [cg.DeviceSolver(P) for P in cfg4_problems(os.cpu_count() or 1, args.batch)]
-        B = cg.GraphBatch(solvers, precond=2, ncheck=NCHECK, tol=TOL, maxiters=4000)
+        B = cg.GraphBatch(solvers, precond=args.precond, ncheck=NCHECK, tol=TOL, maxiters=4000)
         for k in range(args.warmup + args.steps):
             t0 = time.perf_counter()
             B.run()
             errs, nits, sts = B.wait()
             wall = time.perf_counter() - t0
-        print(f"profile workload=cfg4 batch={len(sizes)} sizes={sizes} niters={list(nits)} err_max={max(errs):.3e} "
+        print(f"profile workload=cfg4 batch={len(sizes)} precond={args.precond} sizes={sizes} niters={list(nits)} "
+              f"niters_sum={int(sum(nits))} err_max={max(errs):.3e} "
               f"wall_ms={1e3 * wall:.1f}")
         print("tile heights:", cg.tile_table())
         B.close()
+        if args.fp64:  # the plain FP64 solver on the same members, one after another
+            t0 = time.perf_counter()
+            n64 = 0
+            for S in solvers:
+                e, n = S.solve(cg.ALG_CHRONGEAR, args.precond, NCHECK, TOL, 4000)
+                n64 += n
+            print(f"fp64 plain: precond={args.precond} niters_sum={n64} wall_ms={1e3 * (time.perf_counter() - t0):.1f}")
         return 0
     P = make_problem(args.workload)
     S = cg.DeviceSolver(P)
@@ -1024,6 +1032,7 @@ def main():
     ap.add_argument("--epoch-steps", type=int, default=64, help="cfg5: steps per serving epoch")
     ap.add_argument("--batch", type=int, default=64, help="cfg4: number of systems")
     ap.add_argument("--fp64", action="store_true", help="profile mode: also time one plain FP64 solve")
+    ap.add_argument("--precond", type=int, default=2, help="profile mode, cfg4: preconditioner of the batch")
     ap.add_argument("--layout", default="auto", choices=["auto", "full"],
                     help="profile mode: mixed matrix layout (auto: symmetric half when exactly symmetric)")
     args = ap.parse_args()

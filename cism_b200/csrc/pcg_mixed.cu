@@ -860,8 +860,10 @@ __device__ __forceinline__ void tri_rhs(const MDesc &D, int TY, int i0, int j0, 
 // takes lines t*256 + thread, then + ntiles*256).  Both kinds index their planes s*stride + line
 // (u planes transposed), so a warp's 32 consecutive lines load and store 128 contiguous bytes per
 // position.  Loads of kLineBatch positions are issued before the recurrence runs through them.
+// Not inlined: its batch registers would otherwise raise the register pressure of every step
+// kind (spills in the 2D kernels' hot passes).
 constexpr int kLineBatch = 16;
-__device__ void lines_step(const MDesc &D, int tile) {
+__device__ __noinline__ void lines_step(const MDesc &D, int tile) {
     const Geom &g = D.g;
     const int NQ = (int)g.NQ;
     const int nu = g.jhi - g.jlo + 1, nv = g.ihi - g.ilo + 1;
