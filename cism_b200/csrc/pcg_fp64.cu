@@ -756,7 +756,11 @@ __global__ void k_tri_vsum(Geom g, const double *__restrict__ ru, const double *
 }
 
 // Line solves of tridiag_solver_local_2d (:4985-5013 u, :5041-5069 v) from planes bu, bv into
-// xu, xv, which hold zeros on entry: gamma forward (stored in x), then back substitution.
+// xu, xv, which hold zeros on entry: gamma forward (stored in x), then back substitution.  A
+// line is a chain of dependent operations, so the loads of kTriBatch positions are issued before
+// the chain runs through them (one memory round trip per batch instead of per position); the
+// operations and their order are the reference's.
+constexpr int kTriBatch = 8;
 __global__ void k_tri_lines(Geom g, int global, const double *__restrict__ bu, const double *__restrict__ bv,
                             double *__restrict__ xu, double *__restrict__ xv, const double *__restrict__ T,
                             const SolveState *st) {
@@ -773,22 +777,55 @@ __global__ void k_tri_lines(Geom g, int global, const double *__restrict__ bu, c
     long long e = tri_at(g, along_i, l, s0);
     double gp = __dmul_rn(b[e], adr[e]);
     x[e] = gp;
-    for (int s = s0 + 1; s <= s1; ++s) {
-        e = tri_at(g, along_i, l, s);
-        gp = __dmul_rn(__dsub_rn(b[e], __dmul_rn(sub[e], gp)), den[e]);
-        x[e] = gp;
+    for (int s = s0 + 1; s <= s1; s += kTriBatch) {
+        double vb[kTriBatch], vs[kTriBatch], vd[kTriBatch];
+#pragma unroll
+        for (int u = 0; u < kTriBatch; ++u) {
+            vb[u] = vs[u] = vd[u] = 0.0;
+            if (s + u <= s1) {
+                const long long f = tri_at(g, along_i, l, s + u);
+                vb[u] = b[f];
+                vs[u] = sub[f];
+                vd[u] = den[f];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kTriBatch; ++u)
+            if (s + u <= s1) {
+                gp = __dmul_rn(__dsub_rn(vb[u], __dmul_rn(vs[u], gp)), vd[u]);
+                x[tri_at(g, along_i, l, s + u)] = gp;
+            }
     }
     double xn = gp;
-    for (int s = s1 - 1; s >= s0; --s) {
-        e = tri_at(g, along_i, l, s);
-        xn = __dsub_rn(x[e], __dmul_rn(om[e], xn));
-        x[e] = xn;
+    for (int s = s1 - 1; s >= s0; s -= kTriBatch) {
+        double vx[kTriBatch], vo[kTriBatch];
+#pragma unroll
+        for (int u = 0; u < kTriBatch; ++u) {
+            vx[u] = vo[u] = 0.0;
+            if (s - u >= s0) {
+                const long long f = tri_at(g, along_i, l, s - u);
+                vx[u] = x[f];  // this thread's forward value
+                vo[u] = om[f];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kTriBatch; ++u)
+            if (s - u >= s0) {
+                xn = __dsub_rn(vx[u], __dmul_rn(vo[u], xn));
+                x[tri_at(g, along_i, l, s - u)] = xn;
+            }
     }
     if (!global)
-        for (int s = s0 - 1; s >= 0; --s) {
-            e = tri_at(g, along_i, l, s);
-            xn = __dsub_rn(0.0, __dmul_rn(om[e], xn));
-            x[e] = xn;
+        for (int s = s0 - 1; s >= 0; s -= kTriBatch) {
+            double vo[kTriBatch];
+#pragma unroll
+            for (int u = 0; u < kTriBatch; ++u) vo[u] = (s - u >= 0) ? om[tri_at(g, along_i, l, s - u)] : 0.0;
+#pragma unroll
+            for (int u = 0; u < kTriBatch; ++u)
+                if (s - u >= 0) {
+                    xn = __dsub_rn(0.0, __dmul_rn(vo[u], xn));
+                    x[tri_at(g, along_i, l, s - u)] = xn;
+                }
         }
 }
 
