@@ -326,6 +326,40 @@ def run_cfg4(args):
     peak, peak_kind = hbm_peak()
     achieved = by / (float(np.mean(step_ms)) / 1e3) / 1e9
 
+    # the same members with the tridiagonal line preconditioner (precond 3, local form): the mixed
+    # batch (one graph replay after a warm-up) against the plain FP64 solver one system at a time
+    lines = None
+    if world == 1:
+        BL = cg.GraphBatch(solvers, precond=3, ncheck=NCHECK, tol=TOL, maxiters=maxit, stream=stream.cuda_stream)
+        BL.run()
+        BL.wait()
+        with torch.cuda.stream(stream):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            BL.run()
+            b.record(stream)
+        el, nl, sl = BL.wait()
+        assert not np.any(sl), sl
+        line_ms = a.elapsed_time(b)
+        BL.close()
+        l64_ms, l64_it = 0.0, 0
+        for S in solvers:
+            S.solve(cg.ALG_CHRONGEAR, 3, NCHECK, TOL, 5)  # line factors and workspace
+            with torch.cuda.stream(stream):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                e, k = S.solve(cg.ALG_CHRONGEAR, 3, NCHECK, TOL, maxit)
+                b.record(stream)
+            stream.synchronize()
+            l64_ms += a.elapsed_time(b)
+            l64_it += k
+        lines = {"precond": "3 (tridiagonal line, local form)", "solves_per_s": n / (line_ms / 1e3),
+                 "ms_per_replay": line_ms, "niters_sum": int(np.sum(nl)), "err_max": float(np.max(el)),
+                 "fp64_plain_solves_per_s": n / (l64_ms / 1e3), "fp64_plain_niters_sum": int(l64_it),
+                 "speedup_vs_fp64_plain": l64_ms / line_ms,
+                 "note": "same 64 members; mixed: one graph replay of the batch (CUDA events); FP64: the reference "
+                         "algorithm one system at a time (CUDA events)"}
+
     # end to end through the batch API with host buffers: per step every member's A and b are
     # uploaded from pinned host memory (cismgpu_solver_set_system), all 64 are solved in one
     # persistent launch (cismgpu_solver_solve_batch) and every x comes back to host memory
@@ -391,6 +425,7 @@ def run_cfg4(args):
                 "path": "cismgpu_solver_set_system x64 (pinned host A, b) + cismgpu_solver_solve_batch + "
                         "cismgpu_solver_get_x x64, host wall clock"},
         "cfg2_fp64_gpu_vs_cpu": side,
+        "line_preconditioner": lines,
         "tile_heights": [ln for ln in cg.tile_table() if ln.startswith("batch:")],
         "gpu_launches": (n + 2) * args.steps, "clocks": clk,
     }
