@@ -204,7 +204,7 @@ def cfg4_cpu_baseline(probs, niters):
 
 
 def cfg2_side(stream, flush):
-    """The like-for-like plain FP64 comparison on cfg2 (401x401 2D SSA, Chronopoulos-Gear
+    """The like-for-like plain FP64 comparison on cfg2 (the 401x401 2D SSA system, Chronopoulos-Gear
     + Jacobi): the FP64 GPU PCG (bit-exact with the oracle) against the oracle on 1 core."""
     import torch
     import cism_b200 as cg
