@@ -1,13 +1,19 @@
-"""A second, independent restatement of one reference solver, in plain Python, against the oracle.
+"""A second, independent restatement of reference solvers, in Python, against the oracle.
 
 The oracle (oracle/pcg_oracle.cpp) is a C++ restatement of glissade_velo_higher_pcg.F90.  This file
-restates pcg_solver_standard_2d with the diagonal preconditioner once more, statement by statement
-from the reference source, in Python floats (IEEE binary64, no fused multiply-add, left-to-right
-evaluation as in Fortran): the staggered halo update on one rank (staggered_parallel_halo_real8_2d,
-libglimmer/parallel_mpi.F90:10609-10769), matvec_multiply_structured_2d (:5656-5773), the
-non-reprosum global sum (parallel_global_sum_stagger_real8_2d, parallel_mpi.F90:6620-6637),
-setup_preconditioner_diag_2d (:4199-4243) and the solver loop (:385-808).  Two restatements written
-separately that agree bit for bit at every iteration count rule out transcription slips in either.
+restates pcg_solver_standard_2d (diagonal preconditioner), pcg_solver_chrongear_2d and
+pcg_solver_chrongear_3d (no, diagonal and SIA preconditioners) once more, statement by statement
+from the reference source, in IEEE binary64 with no fused multiply-add and Fortran's left-to-right
+evaluation: the staggered halo update on one rank (staggered_parallel_halo_real8_2d/_3d,
+libglimmer/parallel_mpi.F90:10609-10936), matvec_multiply_structured_2d/_3d (:5656-5773,
+:5528-5652), the non-reprosum global sums (parallel_global_sum_stagger_real8_2d/_3d and their
+two-field forms, parallel_mpi.F90:6620-6637, 6770-6790, 6904, 7042), the diagonal and SIA
+preconditioners (setup_preconditioner_diag_2d/_3d, setup_preconditioner_sia_3d :3647-3733,
+easy_sia_solver and tridiag_solver :5777-5922) and the solver loops.  Element-wise statements use
+numpy arrays (one IEEE operation per element); the 3D matvec runs over all nodes at once but adds
+each node's couplings in the reference's order; the global sums are sequential Python loops.  Two
+restatements written separately that agree bit for bit at every iteration count rule out
+transcription slips in either.
 """
 import math
 
@@ -22,8 +28,9 @@ from tests import problems
 def _halo(a, par):
     """staggered_parallel_halo on one rank: with periodic_bc the exchanges go to the rank itself
     (east/west on the owned rows, then north/south on whole columns); outflow and no_ice zero the
-    edges of the global domain.  lhalo = 2, uhalo = 1.  a is (NY, NX), a[j-1, i-1] = a(i, j)."""
-    NY, NX = a.shape
+    edges of the global domain.  lhalo = 2, uhalo = 1.  a is (NY, NX) or (NY, NX, nz), a[j-1, i-1]
+    = a(i, j) (all levels of the column in 3D, as the 3D routine exchanges whole columns)."""
+    NY, NX = a.shape[:2]
     jlo, jhi = par["staggered_jlo"], par["staggered_jhi"]
     if par["periodic_bc"]:
         rows = slice(jlo - 1, jhi)
@@ -110,6 +117,8 @@ def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8):
         eta0 = eta1
         eta2 = _gsum(P, du * qu, dv * qv)
         alpha = eta1 / eta2
+        if eta1 != eta1 or alpha != alpha:  # eta1 = NaN or alpha = NaN: GM_FATAL
+            return xu, xv, err, -it
         xu = xu + alpha * du
         xv = xv + alpha * dv
         ru = ru - alpha * qu
@@ -123,6 +132,218 @@ def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8):
             if err < tol:
                 niters = it
                 break
+    return xu, xv, err, niters
+
+
+def _gsum2(P, a1, b1, a2, b2):
+    """The two-field form (nflds = 2, parallel_mpi.F90:6904): each field summed on its own."""
+    return _gsum(P, a1, b1), _gsum(P, a2, b2)
+
+
+def _precond(P, precond, ru, rv):
+    if precond == 0:
+        return ru.copy(), rv.copy()
+    adu, adv = P.Auu[_m(0, 0)], P.Avv[_m(0, 0)]
+    return (np.divide(ru, adu, out=np.zeros_like(ru), where=adu != 0.0),
+            np.divide(rv, adv, out=np.zeros_like(rv), where=adv != 0.0))
+
+
+def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8):
+    """pcg_solver_chrongear_2d (:1541-2628) with precond 0 or 1, from x0 = 0: the first pass
+    (:1913-2227), then iterations 2.. with one two-field sum each; returns (xu, xv, err, niters)."""
+    par = P.par
+    bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
+    xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    du, dv = np.zeros_like(bu), np.zeros_like(bv)
+    l2_rhs = math.sqrt(_gsum(P, bu * bu, bv * bv))
+    _halo(xu, par)
+    _halo(xv, par)
+    zu, zv = _matvec(P, xu, xv)
+    ru, rv = bu - zu, bv - zv
+    _halo(ru, par)
+    _halo(rv, par)
+    zu, zv = _precond(P, precond, ru, rv)
+    w1u, w1v = ru * zu, rv * zv
+    du, dv = zu.copy(), zv.copy()
+    qu, qv = _matvec(P, du, dv)
+    rho_old, sigma = _gsum2(P, w1u, w1v, du * qu, dv * qv)
+    _halo(qu, par)
+    _halo(qv, par)
+    alpha = rho_old / sigma
+    if alpha != alpha:  # 'solver has failed, alpha = NaN', GM_FATAL
+        return xu, xv, float("nan"), -1
+    xu = xu + alpha * du
+    xv = xv + alpha * dv
+    ru = ru - alpha * qu
+    rv = rv - alpha * qv
+    niters, err = maxiters, float("nan")
+    for it in range(2, maxiters + 1):
+        zu, zv = _precond(P, precond, ru, rv)
+        azu, azv = _matvec(P, zu, zv)
+        rho, delta = _gsum2(P, ru * zu, rv * zv, azu * zu, azv * zv)
+        _halo(azu, par)
+        _halo(azv, par)
+        beta = rho / rho_old
+        sigma = delta - beta * rho / alpha
+        alpha = rho / sigma
+        rho_old = rho
+        if alpha != alpha:
+            return xu, xv, err, -it
+        du = zu + beta * du
+        dv = zv + beta * dv
+        qu = azu + beta * qu
+        qv = azv + beta * qv
+        xu = xu + alpha * du
+        xv = xv + alpha * dv
+        ru = ru - alpha * qu
+        rv = rv - alpha * qv
+        if it % ncheck == 0 or it == 5:
+            zu, zv = _matvec(P, xu, xv)
+            ru, rv = bu - zu, bv - zv
+            err = math.sqrt(_gsum(P, ru * ru, rv * rv)) / l2_rhs
+            if err < tol:
+                niters = it
+                break
+            _halo(ru, par)
+            _halo(rv, par)
+    return xu, xv, err, niters
+
+
+def _m3(iA, jA, kA):
+    """indxA_3d(iA, jA, kA) - 1 for the standard map (1..27, iA fastest, then jA, then kA)."""
+    return (iA + 1) + 3 * (jA + 1) + 9 * (kA + 1)
+
+
+def _matvec3(P, xu, xv):
+    """matvec_multiply_structured_3d: over owned active columns, every level k, the couplings in the
+    order kA, jA, iA; a coupling that leaves the arrays is skipped.  Arrays are (NY, NX, nz) and the
+    blocks (NY, NX, nz, 27); the nodes are independent, so they are updated together."""
+    par = P.par
+    NY, NX, nz = xu.shape
+    own = np.zeros((NY, NX), dtype=bool)
+    own[par["staggered_jlo"] - 1:par["staggered_jhi"], par["staggered_ilo"] - 1:par["staggered_ihi"]] = True
+    rows = (own & (P.active_vertex != 0))[:, :, None]
+    J, I, K = np.meshgrid(np.arange(NY), np.arange(NX), np.arange(nz), indexing="ij")
+    yu, yv = np.zeros_like(xu), np.zeros_like(xv)
+    for kA in (-1, 0, 1):
+        for jA in (-1, 0, 1):
+            for iA in (-1, 0, 1):
+                m = _m3(iA, jA, kA)
+                jn, i_n, kn = J + jA, I + iA, K + kA
+                ok = rows & (kn >= 0) & (kn < nz) & (i_n >= 0) & (i_n < NX) & (jn >= 0) & (jn < NY)
+                jc, ic, kc = np.clip(jn, 0, NY - 1), np.clip(i_n, 0, NX - 1), np.clip(kn, 0, nz - 1)
+                x1, x2 = xu[jc, ic, kc], xv[jc, ic, kc]
+                nu = (yu + P.Auu[..., m] * x1) + P.Auv[..., m] * x2
+                nv = (yv + P.Avu[..., m] * x1) + P.Avv[..., m] * x2
+                yu = np.where(ok, nu, yu)
+                yv = np.where(ok, nv, yv)
+    return yu, yv
+
+
+def _gsum3(P, a1, a2):
+    """Sequential sum over owned vertices j, i, then levels k: local_sum + arr1 + arr2."""
+    par = P.par
+    l1, l2 = a1.tolist(), a2.tolist()
+    s = 0.0
+    for j in range(par["staggered_jlo"], par["staggered_jhi"] + 1):
+        for i in range(par["staggered_ilo"], par["staggered_ihi"] + 1):
+            c1, c2 = l1[j - 1][i - 1], l2[j - 1][i - 1]
+            for k in range(len(c1)):
+                s = (s + c1[k]) + c2[k]
+    return s
+
+
+def _sia(P, A, r, z):
+    """easy_sia_solver with the SIA matrix of setup_preconditioner_sia_3d (the column couplings
+    (0,0,-1), (0,0,0), (0,0,1) of A): tridiag_solver on every active column (halo included); z
+    keeps its values on inactive columns.  Vectorized over columns, sequential over levels."""
+    nz = r.shape[2]
+    sb, dg, sp = A[..., _m3(0, 0, -1)], A[..., _m3(0, 0, 0)], A[..., _m3(0, 0, 1)]
+    act = P.active_vertex != 0
+    soln = np.zeros_like(r)
+    gamma = np.zeros_like(r)
+    beta = dg[:, :, 0].copy()
+    soln[:, :, 0] = r[:, :, 0] / np.where(act, beta, 1.0)
+    for k in range(1, nz):
+        gamma[:, :, k] = sp[:, :, k - 1] / np.where(act, beta, 1.0)
+        beta = dg[:, :, k] - sb[:, :, k] * gamma[:, :, k]
+        soln[:, :, k] = (r[:, :, k] - sb[:, :, k] * soln[:, :, k - 1]) / np.where(act, beta, 1.0)
+    for k in range(nz - 2, -1, -1):
+        soln[:, :, k] = soln[:, :, k] - gamma[:, :, k + 1] * soln[:, :, k + 1]
+    out = z.copy()
+    out[act] = soln[act]
+    return out
+
+
+def _precond3(P, precond, ru, rv, zu, zv):
+    if precond == 0:
+        return ru.copy(), rv.copy()
+    if precond == 1:
+        adu, adv = P.Auu[..., _m3(0, 0, 0)], P.Avv[..., _m3(0, 0, 0)]
+        return (np.divide(ru, adu, out=np.zeros_like(ru), where=adu != 0.0),
+                np.divide(rv, adv, out=np.zeros_like(rv), where=adv != 0.0))
+    return _sia(P, P.Auu, ru, zu), _sia(P, P.Avv, rv, zv)
+
+
+def pcg_chrongear_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
+    """pcg_solver_chrongear_3d (:2632-3594) with precond 0, 1 or 2, from x0 = 0: the first pass
+    (:3048-3290), then iterations 2.. (:3296-3581); returns (xu, xv, err, niters)."""
+    par = P.par
+    bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
+    xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    du, dv = np.zeros_like(bu), np.zeros_like(bv)
+    qu, qv = np.zeros_like(bu), np.zeros_like(bv)
+    l2_rhs = math.sqrt(_gsum3(P, bu * bu, bv * bv))
+    _halo(xu, par)
+    _halo(xv, par)
+    zu, zv = _matvec3(P, xu, xv)
+    ru, rv = bu - zu, bv - zv
+    _halo(ru, par)
+    _halo(rv, par)
+    zu, zv = _precond3(P, precond, ru, rv, zu, zv)
+    w1u, w1v = ru * zu, rv * zv
+    du, dv = zu.copy(), zv.copy()
+    qu, qv = _matvec3(P, du, dv)
+    rho_old, sigma = _gsum3(P, w1u, w1v), _gsum3(P, du * qu, dv * qv)
+    _halo(qu, par)
+    _halo(qv, par)
+    alpha = rho_old / sigma
+    if alpha != alpha:  # 'solver has failed, alpha = NaN', GM_FATAL
+        return xu, xv, float("nan"), -1
+    xu = xu + alpha * du
+    xv = xv + alpha * dv
+    ru = ru - alpha * qu
+    rv = rv - alpha * qv
+    niters, err = maxiters, float("nan")
+    for it in range(2, maxiters + 1):
+        zu, zv = _precond3(P, precond, ru, rv, zu, zv)
+        azu, azv = _matvec3(P, zu, zv)
+        rho, delta = _gsum3(P, ru * zu, rv * zv), _gsum3(P, azu * zu, azv * zv)
+        _halo(azu, par)
+        _halo(azv, par)
+        beta = rho / rho_old
+        sigma = delta - beta * rho / alpha
+        alpha = rho / sigma
+        rho_old = rho
+        if alpha != alpha:
+            return xu, xv, err, -it
+        du = zu + beta * du
+        dv = zv + beta * dv
+        qu = azu + beta * qu
+        qv = azv + beta * qv
+        xu = xu + alpha * du
+        xv = xv + alpha * dv
+        ru = ru - alpha * qu
+        rv = rv - alpha * qv
+        if it % ncheck == 0 or it == 5:
+            zu, zv = _matvec3(P, xu, xv)
+            ru, rv = bu - zu, bv - zv
+            err = math.sqrt(_gsum3(P, ru * ru, rv * rv)) / l2_rhs
+            if err < tol:
+                niters = it
+                break
+            _halo(ru, par)
+            _halo(rv, par)
     return xu, xv, err, niters
 
 
@@ -141,7 +362,53 @@ def test_second_restatement_matches_oracle(name, make, maxiters):
     P = make()
     xu, xv, err, nit = pcg_standard_2d_diag(P, maxiters)
     st, ou, ov, oerr, onit = oracle.pcg("standard", P, 1, tol=1e-8, maxiters=maxiters, summode=oracle.SUM_SEQ)
-    assert st == 0
+    if st != 0:  # the reference stops with GM_FATAL (a NaN alpha); so must the restatement
+        assert nit < 0
+        return
+    assert nit == onit
+    assert (err == oerr) or (math.isnan(err) and math.isnan(oerr))
+    np.testing.assert_array_equal(xu, ou)
+    np.testing.assert_array_equal(xv, ov)
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("precond", [0, 1])
+@pytest.mark.parametrize("maxiters", [1, 4, 12, 600])
+def test_second_restatement_chrongear_2d(name, make, precond, maxiters):
+    """pcg_solver_chrongear_2d: bit-identical x, err and niters with the oracle's reference-order solve."""
+    P = make()
+    xu, xv, err, nit = pcg_chrongear_2d(P, precond, maxiters)
+    st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, precond, tol=1e-8, maxiters=maxiters,
+                                        summode=oracle.SUM_SEQ)
+    if st != 0:  # the reference stops with GM_FATAL (a NaN alpha); so must the restatement
+        assert nit < 0
+        return
+    assert nit == onit
+    assert (err == oerr) or (math.isnan(err) and math.isnan(oerr))
+    np.testing.assert_array_equal(xu, ou)
+    np.testing.assert_array_equal(xv, ov)
+
+
+CASES3 = [
+    ("slab-periodic-sliding", lambda: problems.slab_3d(seed=1)),
+    ("slab-periodic-boundary-ice", lambda: problems.slab_3d(seed=3, boundary_ice=True, sliding=False)),
+    ("slab-outflow-boundary-ice", lambda: problems.slab_3d(seed=4, boundary_ice=True, bc="outflow", sliding=False)),
+    ("dome", lambda: asm.dome()),
+]
+
+
+@pytest.mark.parametrize("name,make", CASES3, ids=[c[0] for c in CASES3])
+@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("maxiters", [1, 4, 12, 400])
+def test_second_restatement_chrongear_3d(name, make, precond, maxiters):
+    """pcg_solver_chrongear_3d: bit-identical x, err and niters with the oracle's reference-order solve."""
+    P = make()
+    xu, xv, err, nit = pcg_chrongear_3d(P, precond, maxiters)
+    st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, precond, tol=1e-8, maxiters=maxiters,
+                                        summode=oracle.SUM_SEQ)
+    if st != 0:  # the reference stops with GM_FATAL (a NaN alpha); so must the restatement
+        assert nit < 0
+        return
     assert nit == onit
     assert (err == oerr) or (math.isnan(err) and math.isnan(oerr))
     np.testing.assert_array_equal(xu, ou)
