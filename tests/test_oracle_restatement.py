@@ -1,8 +1,8 @@
 """A second, independent restatement of reference solvers, in Python, against the oracle.
 
 The oracle (oracle/pcg_oracle.cpp) is a C++ restatement of glissade_velo_higher_pcg.F90.  This file
-restates pcg_solver_standard_2d (diagonal preconditioner), pcg_solver_chrongear_2d and
-pcg_solver_chrongear_3d (no, diagonal and SIA preconditioners) once more, statement by statement
+restates pcg_solver_standard_2d (diagonal preconditioner), pcg_solver_standard_3d,
+pcg_solver_chrongear_2d and pcg_solver_chrongear_3d (no, diagonal and SIA preconditioners) once more, statement by statement
 from the reference source, in IEEE binary64 with no fused multiply-add and Fortran's left-to-right
 evaluation: the staggered halo update on one rank (staggered_parallel_halo_real8_2d/_3d,
 libglimmer/parallel_mpi.F90:10609-10936), matvec_multiply_structured_2d/_3d (:5656-5773,
@@ -389,6 +389,52 @@ def test_second_restatement_chrongear_2d(name, make, precond, maxiters):
     np.testing.assert_array_equal(xv, ov)
 
 
+def pcg_standard_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
+    """pcg_solver_standard_3d (:827-1537) with precond 0, 1 or 2, from x0 = 0 (the loop :1169-1524);
+    returns (xu, xv, err, niters), niters < 0 where the reference stops with GM_FATAL."""
+    par = P.par
+    bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
+    xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    _halo(xu, par)
+    _halo(xv, par)
+    zu, zv = _matvec3(P, xu, xv)
+    ru, rv = bu - zu, bv - zv
+    niters, eta0, err = maxiters, 1.0, float("nan")
+    du, dv = np.zeros_like(bu), np.zeros_like(bv)
+    zu, zv = np.zeros_like(bu), np.zeros_like(bv)
+    l2_rhs = math.sqrt(_gsum3(P, bu * bu, bv * bv))
+    for it in range(1, maxiters + 1):
+        zu, zv = _precond3(P, precond, ru, rv, zu, zv)
+        eta1 = _gsum3(P, ru * zu, rv * zv)
+        if eta1 != eta1:
+            return xu, xv, err, -it
+        beta = eta1 / eta0
+        du = zu + beta * du
+        dv = zv + beta * dv
+        _halo(du, par)
+        _halo(dv, par)
+        qu, qv = _matvec3(P, du, dv)
+        eta0 = eta1
+        eta2 = _gsum3(P, du * qu, dv * qv)
+        alpha = eta1 / eta2
+        if alpha != alpha:
+            return xu, xv, err, -it
+        xu = xu + alpha * du
+        xv = xv + alpha * dv
+        ru = ru - alpha * qu
+        rv = rv - alpha * qv
+        if it % ncheck == 0 or it == 5:
+            _halo(xu, par)
+            _halo(xv, par)
+            zu, zv = _matvec3(P, xu, xv)
+            ru, rv = bu - zu, bv - zv
+            err = math.sqrt(_gsum3(P, ru * ru, rv * rv)) / l2_rhs
+            if err < tol:
+                niters = it
+                break
+    return xu, xv, err, niters
+
+
 CASES3 = [
     ("slab-periodic-sliding", lambda: problems.slab_3d(seed=1)),
     ("slab-periodic-boundary-ice", lambda: problems.slab_3d(seed=3, boundary_ice=True, sliding=False)),
@@ -407,6 +453,25 @@ def test_second_restatement_chrongear_3d(name, make, precond, maxiters):
     st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, precond, tol=1e-8, maxiters=maxiters,
                                         summode=oracle.SUM_SEQ)
     if st != 0:  # the reference stops with GM_FATAL (a NaN alpha); so must the restatement
+        assert nit < 0
+        return
+    assert nit == onit
+    assert (err == oerr) or (math.isnan(err) and math.isnan(oerr))
+    np.testing.assert_array_equal(xu, ou)
+    np.testing.assert_array_equal(xv, ov)
+
+
+@pytest.mark.parametrize("name,make", CASES3, ids=[c[0] for c in CASES3])
+@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("maxiters", [1, 4, 12, 400])
+def test_second_restatement_standard_3d(name, make, precond, maxiters):
+    """pcg_solver_standard_3d (the dome with the diagonal preconditioner is the reference's own CPU
+    configuration): bit-identical x, err and niters with the oracle's reference-order solve."""
+    P = make()
+    xu, xv, err, nit = pcg_standard_3d(P, precond, maxiters)
+    st, ou, ov, oerr, onit = oracle.pcg("standard", P, precond, tol=1e-8, maxiters=maxiters,
+                                        summode=oracle.SUM_SEQ)
+    if st != 0:  # the reference stops with GM_FATAL (a NaN eta1 or alpha); so must the restatement
         assert nit < 0
         return
     assert nit == onit
