@@ -263,13 +263,14 @@ def _sia(P, A, r, z):
     soln = np.zeros_like(r)
     gamma = np.zeros_like(r)
     beta = dg[:, :, 0].copy()
-    soln[:, :, 0] = r[:, :, 0] / np.where(act, beta, 1.0)
-    for k in range(1, nz):
-        gamma[:, :, k] = sp[:, :, k - 1] / np.where(act, beta, 1.0)
-        beta = dg[:, :, k] - sb[:, :, k] * gamma[:, :, k]
-        soln[:, :, k] = (r[:, :, k] - sb[:, :, k] * soln[:, :, k - 1]) / np.where(act, beta, 1.0)
-    for k in range(nz - 2, -1, -1):
-        soln[:, :, k] = soln[:, :, k] - gamma[:, :, k + 1] * soln[:, :, k + 1]
+    with np.errstate(divide="ignore", invalid="ignore"):  # a zero pivot gives the IEEE result, as in Fortran
+        soln[:, :, 0] = r[:, :, 0] / np.where(act, beta, 1.0)
+        for k in range(1, nz):
+            gamma[:, :, k] = sp[:, :, k - 1] / np.where(act, beta, 1.0)
+            beta = dg[:, :, k] - sb[:, :, k] * gamma[:, :, k]
+            soln[:, :, k] = (r[:, :, k] - sb[:, :, k] * soln[:, :, k - 1]) / np.where(act, beta, 1.0)
+        for k in range(nz - 2, -1, -1):
+            soln[:, :, k] = soln[:, :, k] - gamma[:, :, k + 1] * soln[:, :, k + 1]
     out = z.copy()
     out[act] = soln[act]
     return out
