@@ -2,14 +2,16 @@
 
 The oracle (oracle/pcg_oracle.cpp) is a C++ restatement of glissade_velo_higher_pcg.F90.  This file
 restates pcg_solver_standard_2d (diagonal preconditioner), pcg_solver_standard_3d,
-pcg_solver_chrongear_2d and pcg_solver_chrongear_3d (no, diagonal and SIA preconditioners) once more, statement by statement
+pcg_solver_chrongear_2d and pcg_solver_chrongear_3d (no, diagonal, SIA and local tridiagonal line
+preconditioners) once more, statement by statement
 from the reference source, in IEEE binary64 with no fused multiply-add and Fortran's left-to-right
 evaluation: the staggered halo update on one rank (staggered_parallel_halo_real8_2d/_3d,
 libglimmer/parallel_mpi.F90:10609-10936), matvec_multiply_structured_2d/_3d (:5656-5773,
 :5528-5652), the non-reprosum global sums (parallel_global_sum_stagger_real8_2d/_3d and their
 two-field forms, parallel_mpi.F90:6620-6637, 6770-6790, 6904, 7042), the diagonal and SIA
 preconditioners (setup_preconditioner_diag_2d/_3d, setup_preconditioner_sia_3d :3647-3733,
-easy_sia_solver and tridiag_solver :5777-5922) and the solver loops.  Element-wise statements use
+easy_sia_solver and tridiag_solver :5777-5922, setup_preconditioner_tridiag_local_2d/_3d
+:3737-3830, :4247-4392, tridiag_solver_local_2d/_3d :4917-5100, :4524-4655) and the solver loops.  Element-wise statements use
 numpy arrays (one IEEE operation per element); the 3D matvec runs over all nodes at once but adds
 each node's couplings in the reference's order; the global sums are sequential Python loops.  Two
 restatements written separately that agree bit for bit at every iteration count rule out
@@ -89,12 +91,90 @@ def _gsum(P, a1, a2):
     return s
 
 
-def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8):
-    """pcg_solver_standard_2d, precond = HO_PRECOND_DIAG, from x0 = 0; returns (xu, xv, err, niters)."""
+def _tri_setup_2d(P, U, V):
+    """setup_preconditioner_tridiag_local_2d (:4247-4392) on coefficient planes U = Auu, V = Avv
+    ((9, NY, NX), 0-based m = indxA_2d - 1): u lines along i with the couplings (-1,0), (0,0),
+    (1,0), v lines along j with (0,-1), (0,0), (0,1); a zero diagonal becomes 1 with zero
+    off-diagonals; forward elimination over the owned range; a zero pivot is GM_FATAL (raises)."""
+    par = P.par
+    ilo, ihi, jlo, jhi = par["staggered_ilo"], par["staggered_ihi"], par["staggered_jlo"], par["staggered_jhi"]
+    out = {}
+    for comp, A, offs in (("u", U, ((-1, 0), (0, 0), (1, 0))), ("v", V, ((0, -1), (0, 0), (0, 1)))):
+        sub, dg, sp = (A[_m(*o)].astype(np.float64).copy() for o in offs)
+        zero = dg == 0.0
+        dg[zero], sub[zero], sp[zero] = 1.0, 0.0, 0.0
+        om, den = np.zeros_like(dg), np.zeros_like(dg)
+        lines = range(jlo, jhi + 1) if comp == "u" else range(ilo, ihi + 1)
+        for ln in lines:
+            pos = list(range(ilo, ihi + 1)) if comp == "u" else list(range(jlo, jhi + 1))
+            at = (lambda q: (ln - 1, q - 1)) if comp == "u" else (lambda q: (q - 1, ln - 1))
+            om[at(pos[0])] = float(sp[at(pos[0])]) / float(dg[at(pos[0])])
+            for a, b in zip(pos[:-1], pos[1:]):
+                d = float(dg[at(b)]) - float(sub[at(b)]) * float(om[at(a)])
+                if d == 0.0:
+                    raise ZeroDivisionError("divzero in setup_preconditioner_tridiag_local_2d")
+                den[at(b)] = 1.0 / d
+                om[at(b)] = float(sp[at(b)]) * float(den[at(b)])
+        out[comp] = (1.0 / dg, sub, om, den)
+    return out
+
+
+def _tri_solve_2d(P, T, bu, bv):
+    """tridiag_solver_local_2d (:4917-5100): gamma forward over the owned range, back substitution
+    from the last owned position down to the array's first (omega and gamma are zero below)."""
+    par = P.par
+    ilo, ihi, jlo, jhi = par["staggered_ilo"], par["staggered_ihi"], par["staggered_jlo"], par["staggered_jhi"]
+    res = []
+    for comp, b in (("u", bu), ("v", bv)):
+        adg, sub, om, den = T[comp]
+        x, gam = np.zeros_like(b), np.zeros_like(b)
+        lines = range(jlo, jhi + 1) if comp == "u" else range(ilo, ihi + 1)
+        for ln in lines:
+            lo, hi = (ilo, ihi) if comp == "u" else (jlo, jhi)
+            at = (lambda q: (ln - 1, q - 1)) if comp == "u" else (lambda q: (q - 1, ln - 1))
+            gam[at(lo)] = float(b[at(lo)]) * float(adg[at(lo)])
+            for q in range(lo + 1, hi + 1):
+                gam[at(q)] = (float(b[at(q)]) - float(sub[at(q)]) * float(gam[at(q - 1)])) * float(den[at(q)])
+            x[at(hi)] = gam[at(hi)]
+            for q in range(hi - 1, 0, -1):
+                x[at(q)] = float(gam[at(q)]) - float(om[at(q)]) * float(x[at(q + 1)])
+        res.append(x)
+    return res[0], res[1]
+
+
+def _vsum_planes(P, A):
+    """setup_preconditioner_tridiag_local_3d (:3737-3830): per column the sums over levels of the
+    three vertical offsets of each horizontal coupling, ((s + A(m)) + A(m+9)) + A(m+18); inactive
+    columns get the identity (centre 1, the rest 0)."""
+    nz = A.shape[2]
+    out = np.zeros((9,) + A.shape[:2])
+    for m in range(9):
+        acc = np.zeros(A.shape[:2])
+        for k in range(nz):
+            acc = ((acc + A[:, :, k, m]) + A[:, :, k, m + 9]) + A[:, :, k, m + 18]
+        out[m] = acc
+    inact = P.active_vertex == 0
+    out[:, inact] = 0.0
+    out[4, inact] = 1.0
+    return out
+
+
+def _line_rhs_3d(r):
+    """sum(r(:, i, j)) in level order."""
+    acc = np.zeros(r.shape[:2])
+    for k in range(r.shape[2]):
+        acc = acc + r[:, :, k]
+    return acc
+
+
+def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8, precond=1):
+    """pcg_solver_standard_2d with precond 1 (diagonal) or 3 (local tridiagonal lines, then the
+    halo of z), from x0 = 0; returns (xu, xv, err, niters)."""
     par = P.par
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
     xu, xv = np.zeros_like(bu), np.zeros_like(bv)
     adu, adv = P.Auu[_m(0, 0)], P.Avv[_m(0, 0)]
+    T = _tri_setup_2d(P, P.Auu, P.Avv) if precond == 3 else None
     _halo(xu, par)
     _halo(xv, par)
     zu, zv = _matvec(P, xu, xv)
@@ -105,8 +185,13 @@ def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8):
     l2_rhs = math.sqrt(_gsum(P, bu * bu, bv * bv))
     err = float("nan")
     for it in range(1, maxiters + 1):
-        zu = np.divide(ru, adu, out=np.zeros_like(ru), where=adu != 0.0)
-        zv = np.divide(rv, adv, out=np.zeros_like(rv), where=adv != 0.0)
+        if precond == 3:
+            zu, zv = _tri_solve_2d(P, T, ru, rv)
+            _halo(zu, par)
+            _halo(zv, par)
+        else:
+            zu = np.divide(ru, adu, out=np.zeros_like(ru), where=adu != 0.0)
+            zv = np.divide(rv, adv, out=np.zeros_like(rv), where=adv != 0.0)
         eta1 = _gsum(P, ru * zu, rv * zv)
         beta = eta1 / eta0
         du = zu + beta * du
@@ -140,18 +225,28 @@ def _gsum2(P, a1, b1, a2, b2):
     return _gsum(P, a1, b1), _gsum(P, a2, b2)
 
 
-def _precond(P, precond, ru, rv):
+def _precond(P, precond, ru, rv, T=None):
     if precond == 0:
         return ru.copy(), rv.copy()
+    if precond == 3:
+        zu, zv = _tri_solve_2d(P, T, ru, rv)
+        _halo(zu, P.par)
+        _halo(zv, P.par)
+        return zu, zv
     adu, adv = P.Auu[_m(0, 0)], P.Avv[_m(0, 0)]
     return (np.divide(ru, adu, out=np.zeros_like(ru), where=adu != 0.0),
             np.divide(rv, adv, out=np.zeros_like(rv), where=adv != 0.0))
 
 
 def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8):
-    """pcg_solver_chrongear_2d (:1541-2628) with precond 0 or 1, from x0 = 0: the first pass
-    (:1913-2227), then iterations 2.. with one two-field sum each; returns (xu, xv, err, niters)."""
+    """pcg_solver_chrongear_2d (:1541-2628) with precond 0, 1 or 3, from x0 = 0: the first pass
+    (:1913-2227), then iterations 2.. with one two-field sum each; with the line preconditioner at
+    most 100 iterations (maxiters_tridiag, :1703-1732); returns (xu, xv, err, niters)."""
     par = P.par
+    T = None
+    if precond == 3:
+        T = _tri_setup_2d(P, P.Auu, P.Avv)
+        maxiters = 100
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
     xu, xv = np.zeros_like(bu), np.zeros_like(bv)
     du, dv = np.zeros_like(bu), np.zeros_like(bv)
@@ -162,7 +257,7 @@ def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8):
     ru, rv = bu - zu, bv - zv
     _halo(ru, par)
     _halo(rv, par)
-    zu, zv = _precond(P, precond, ru, rv)
+    zu, zv = _precond(P, precond, ru, rv, T)
     w1u, w1v = ru * zu, rv * zv
     du, dv = zu.copy(), zv.copy()
     qu, qv = _matvec(P, du, dv)
@@ -178,7 +273,7 @@ def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8):
     rv = rv - alpha * qv
     niters, err = maxiters, float("nan")
     for it in range(2, maxiters + 1):
-        zu, zv = _precond(P, precond, ru, rv)
+        zu, zv = _precond(P, precond, ru, rv, T)
         azu, azv = _matvec(P, zu, zv)
         rho, delta = _gsum2(P, ru * zu, rv * zv, azu * zu, azv * zv)
         _halo(azu, par)
@@ -276,9 +371,15 @@ def _sia(P, A, r, z):
     return out
 
 
-def _precond3(P, precond, ru, rv, zu, zv):
+def _precond3(P, precond, ru, rv, zu, zv, T=None):
     if precond == 0:
         return ru.copy(), rv.copy()
+    if precond == 3:  # tridiag_solver_local_3d (:4524-4655)
+        su, sv = _tri_solve_2d(P, T, _line_rhs_3d(ru), _line_rhs_3d(rv))
+        _halo(su, P.par)
+        _halo(sv, P.par)
+        zu, zv = _sia(P, P.Auu, ru, zu), _sia(P, P.Avv, rv, zv)
+        return zu + su[:, :, None], zv + sv[:, :, None]
     if precond == 1:
         adu, adv = P.Auu[..., _m3(0, 0, 0)], P.Avv[..., _m3(0, 0, 0)]
         return (np.divide(ru, adu, out=np.zeros_like(ru), where=adu != 0.0),
@@ -290,6 +391,7 @@ def pcg_chrongear_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
     """pcg_solver_chrongear_3d (:2632-3594) with precond 0, 1 or 2, from x0 = 0: the first pass
     (:3048-3290), then iterations 2.. (:3296-3581); returns (xu, xv, err, niters)."""
     par = P.par
+    T = _tri_setup_2d(P, _vsum_planes(P, P.Auu), _vsum_planes(P, P.Avv)) if precond == 3 else None
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
     xu, xv = np.zeros_like(bu), np.zeros_like(bv)
     du, dv = np.zeros_like(bu), np.zeros_like(bv)
@@ -301,7 +403,7 @@ def pcg_chrongear_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
     ru, rv = bu - zu, bv - zv
     _halo(ru, par)
     _halo(rv, par)
-    zu, zv = _precond3(P, precond, ru, rv, zu, zv)
+    zu, zv = _precond3(P, precond, ru, rv, zu, zv, T)
     w1u, w1v = ru * zu, rv * zv
     du, dv = zu.copy(), zv.copy()
     qu, qv = _matvec3(P, du, dv)
@@ -317,7 +419,7 @@ def pcg_chrongear_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
     rv = rv - alpha * qv
     niters, err = maxiters, float("nan")
     for it in range(2, maxiters + 1):
-        zu, zv = _precond3(P, precond, ru, rv, zu, zv)
+        zu, zv = _precond3(P, precond, ru, rv, zu, zv, T)
         azu, azv = _matvec3(P, zu, zv)
         rho, delta = _gsum3(P, ru * zu, rv * zv), _gsum3(P, azu * zu, azv * zv)
         _halo(azu, par)
@@ -348,6 +450,14 @@ def pcg_chrongear_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
     return xu, xv, err, niters
 
 
+def _run(solver, P, precond, maxiters):
+    """A restated solve; a zero pivot in the line setup (GM_FATAL) comes back as niters = -1."""
+    try:
+        return solver(P, precond, maxiters)
+    except ZeroDivisionError:
+        return None, None, float("nan"), -1
+
+
 CASES = [
     ("slab-periodic", lambda: problems.slab_2d(seed=1)),
     ("slab-outflow-boundary-ice", lambda: problems.slab_2d(seed=2, boundary_ice=True, bc="outflow")),
@@ -373,12 +483,12 @@ def test_second_restatement_matches_oracle(name, make, maxiters):
 
 
 @pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("precond", [0, 1])
+@pytest.mark.parametrize("precond", [0, 1, 3])
 @pytest.mark.parametrize("maxiters", [1, 4, 12, 600])
 def test_second_restatement_chrongear_2d(name, make, precond, maxiters):
     """pcg_solver_chrongear_2d: bit-identical x, err and niters with the oracle's reference-order solve."""
     P = make()
-    xu, xv, err, nit = pcg_chrongear_2d(P, precond, maxiters)
+    xu, xv, err, nit = _run(pcg_chrongear_2d, P, precond, maxiters)
     st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, precond, tol=1e-8, maxiters=maxiters,
                                         summode=oracle.SUM_SEQ)
     if st != 0:  # the reference stops with GM_FATAL (a NaN alpha); so must the restatement
@@ -394,6 +504,7 @@ def pcg_standard_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
     """pcg_solver_standard_3d (:827-1537) with precond 0, 1 or 2, from x0 = 0 (the loop :1169-1524);
     returns (xu, xv, err, niters), niters < 0 where the reference stops with GM_FATAL."""
     par = P.par
+    T = _tri_setup_2d(P, _vsum_planes(P, P.Auu), _vsum_planes(P, P.Avv)) if precond == 3 else None
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
     xu, xv = np.zeros_like(bu), np.zeros_like(bv)
     _halo(xu, par)
@@ -405,7 +516,7 @@ def pcg_standard_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
     zu, zv = np.zeros_like(bu), np.zeros_like(bv)
     l2_rhs = math.sqrt(_gsum3(P, bu * bu, bv * bv))
     for it in range(1, maxiters + 1):
-        zu, zv = _precond3(P, precond, ru, rv, zu, zv)
+        zu, zv = _precond3(P, precond, ru, rv, zu, zv, T)
         eta1 = _gsum3(P, ru * zu, rv * zv)
         if eta1 != eta1:
             return xu, xv, err, -it
@@ -445,12 +556,12 @@ CASES3 = [
 
 
 @pytest.mark.parametrize("name,make", CASES3, ids=[c[0] for c in CASES3])
-@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3])
 @pytest.mark.parametrize("maxiters", [1, 4, 12, 400])
 def test_second_restatement_chrongear_3d(name, make, precond, maxiters):
     """pcg_solver_chrongear_3d: bit-identical x, err and niters with the oracle's reference-order solve."""
     P = make()
-    xu, xv, err, nit = pcg_chrongear_3d(P, precond, maxiters)
+    xu, xv, err, nit = _run(pcg_chrongear_3d, P, precond, maxiters)
     st, ou, ov, oerr, onit = oracle.pcg("chrongear", P, precond, tol=1e-8, maxiters=maxiters,
                                         summode=oracle.SUM_SEQ)
     if st != 0:  # the reference stops with GM_FATAL (a NaN alpha); so must the restatement
@@ -463,16 +574,36 @@ def test_second_restatement_chrongear_3d(name, make, precond, maxiters):
 
 
 @pytest.mark.parametrize("name,make", CASES3, ids=[c[0] for c in CASES3])
-@pytest.mark.parametrize("precond", [0, 1, 2])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3])
 @pytest.mark.parametrize("maxiters", [1, 4, 12, 400])
 def test_second_restatement_standard_3d(name, make, precond, maxiters):
     """pcg_solver_standard_3d (the dome with the diagonal preconditioner is the reference's own CPU
     configuration): bit-identical x, err and niters with the oracle's reference-order solve."""
     P = make()
-    xu, xv, err, nit = pcg_standard_3d(P, precond, maxiters)
+    xu, xv, err, nit = _run(pcg_standard_3d, P, precond, maxiters)
     st, ou, ov, oerr, onit = oracle.pcg("standard", P, precond, tol=1e-8, maxiters=maxiters,
                                         summode=oracle.SUM_SEQ)
     if st != 0:  # the reference stops with GM_FATAL (a NaN eta1 or alpha); so must the restatement
+        assert nit < 0
+        return
+    assert nit == onit
+    assert (err == oerr) or (math.isnan(err) and math.isnan(oerr))
+    np.testing.assert_array_equal(xu, ou)
+    np.testing.assert_array_equal(xv, ov)
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("maxiters", [3, 12, 400])
+def test_second_restatement_standard_2d_lines(name, make, maxiters):
+    """pcg_solver_standard_2d with the local tridiagonal line preconditioner (precond 3)."""
+    P = make()
+    try:
+        xu, xv, err, nit = pcg_standard_2d_diag(P, maxiters, precond=3)
+    except ZeroDivisionError:
+        xu = xv = None
+        err, nit = float("nan"), -1
+    st, ou, ov, oerr, onit = oracle.pcg("standard", P, 3, tol=1e-8, maxiters=maxiters, summode=oracle.SUM_SEQ)
+    if st != 0:
         assert nit < 0
         return
     assert nit == onit
