@@ -673,6 +673,16 @@ __global__ void k_tri_coef(Geom g, const double *__restrict__ A, const int32_t *
                 v[e] = sum;
             }
         }
+        if (NC == 27 && global) {
+            // the global form's staggered halo update of the nine summed planes (:4055-4058): its
+            // outflow / no_ice zeroing, which with no_ice reaches the last owned row and column
+            // (its periodic copies reach only halo positions, which no owned line reads)
+            const int i = (int)(q % g.NX), j = (int)(q / g.NX);
+            bool zero = false;
+            if (g.outflow) zero = (i == 0 || i == g.NX - 1 || j == 0 || j == g.NY - 1);
+            else if (g.no_ice) zero = (i <= 1 || i >= g.NX - 2 || j <= 1 || j >= g.NY - 2);
+            if (zero) v[0] = v[1] = v[2] = 0.0;
+        }
         if (v[1] == 0.0) { v[1] = 1.0; v[0] = 0.0; v[2] = 0.0; }
         double *P = T + (comp ? TV_SUB : TU_SUB) * g.NQ;
         P[0 * g.NQ + q] = v[0];

@@ -772,7 +772,8 @@ int setup_precond(const Ctx &c, bool is3d, int precond, const double *Auu, const
         // vertical sums of the 9 horizontal couplings over the 3 vertical offsets and all
         // levels, raw m, m+9, m+18 (:3809-3821 / :4011-4023); inactive columns: the local form
         // zeroes the 9 sums and sets m = 5 to 1 (:3823-3833), the global form only sets m = 5
-        // to 1 (:4025-4032); its halo update of the sums (:4034-4037) touches no owned entry
+        // to 1 (:4025-4032) and then runs the staggered halo update on each summed plane
+        // (:4055-4058), whose no_ice zeroing reaches the last owned row and column
         const long nq = g.nq();
         Vec su(9 * nq), sv(9 * nq);
         for (int j = 1; j <= g.NY; ++j)
@@ -795,6 +796,18 @@ int setup_precond(const Ctx &c, bool is3d, int precond, const double *Auu, const
                         sv[(m - 1) * nq + g.v2(i, j)] = (m == 5) ? 1.0 : 0.0;
                     }
             }
+        if (global) {
+            Ctx c2 = c;
+            c2.g.nz = 1;  // (NX, NY) planes
+            for (int m = 0; m < 9; ++m) {
+                Vec pu(su.begin() + m * nq, su.begin() + (m + 1) * nq);
+                Vec pv(sv.begin() + m * nq, sv.begin() + (m + 1) * nq);
+                halo(c2, pu);
+                halo(c2, pv);
+                std::copy(pu.begin(), pu.end(), su.begin() + m * nq);
+                std::copy(pv.begin(), pv.end(), sv.begin() + m * nq);
+            }
+        }
         tri_coefs(c, P.tu, true, [&](int i, int j, int m) { return su[(m - 1) * nq + g.v2(i, j)]; });
         tri_coefs(c, P.tv, false, [&](int i, int j, int m) { return sv[(m - 1) * nq + g.v2(i, j)]; });
         int st = tri_factor(c, P.tu, true, global);

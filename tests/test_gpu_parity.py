@@ -79,6 +79,19 @@ def test_3d_bitexact_vs_device_tree_oracle(gpu_lib, alg, precond, case):
     assert_bitexact(g, o)
 
 
+@pytest.mark.parametrize("alg", ["standard", "chrongear"])
+@pytest.mark.parametrize("precond", [3, 4])
+def test_3d_lines_noice_edge_coefficients(gpu_lib, alg, precond):
+    """A no_ice system whose last owned row and column keep nonzero couplings: the global line
+    preconditioner's halo update of its summed planes zeroes those owned entries (the local form
+    keeps them), bit-exact against the oracle through 12 iterations or the breakdown."""
+    from tests.test_oracle_restatement import _no_ice_edge_coefficients
+    P = _no_ice_edge_coefficients()
+    o = oracle.pcg(alg, P, precond, tol=1e-8, maxiters=12, summode=oracle.SUM_DDTREE)
+    g = gpu_solve(alg, P, precond, tol=1e-8, maxiters=12)
+    assert_bitexact(g, o)
+
+
 CASES_2D = [
     ("interior-periodic", dict(seed=1)),
     ("boundary-periodic", dict(seed=2, boundary_ice=True, bc="periodic")),

@@ -91,7 +91,7 @@ def _gsum(P, a1, a2):
     return s
 
 
-def _tri_setup_2d(P, U, V):
+def _tri_setup_2d(P, U, V, glob=False):
     """setup_preconditioner_tridiag_local_2d (:4247-4392) on coefficient planes U = Auu, V = Avv
     ((9, NY, NX), 0-based m = indxA_2d - 1): u lines along i with the couplings (-1,0), (0,0),
     (1,0), v lines along j with (0,-1), (0,0), (0,1); a zero diagonal becomes 1 with zero
@@ -115,11 +115,18 @@ def _tri_setup_2d(P, U, V):
                     raise ZeroDivisionError("divzero in setup_preconditioner_tridiag_local_2d")
                 den[at(b)] = 1.0 / d
                 om[at(b)] = float(sp[at(b)]) * float(den[at(b)])
+            if glob:  # setup_preconditioner_tridiag_global_2d (:4396-4520): the reverse recurrence's check
+                ouh = float(sub[at(pos[-1])]) / float(dg[at(pos[-1])])
+                for q in reversed(pos[:-1]):
+                    duh = float(dg[at(q)]) - float(sp[at(q)]) * ouh
+                    if duh == 0.0:
+                        raise ZeroDivisionError("divzero in setup_preconditioner_tridiag_global_2d")
+                    ouh = float(sub[at(q)]) / duh
         out[comp] = (1.0 / dg, sub, om, den)
     return out
 
 
-def _tri_solve_2d(P, T, bu, bv):
+def _tri_solve_2d(P, T, bu, bv, glob=False):
     """tridiag_solver_local_2d (:4917-5100): gamma forward over the owned range, back substitution
     from the last owned position down to the array's first (omega and gamma are zero below)."""
     par = P.par
@@ -136,13 +143,15 @@ def _tri_solve_2d(P, T, bu, bv):
             for q in range(lo + 1, hi + 1):
                 gam[at(q)] = (float(b[at(q)]) - float(sub[at(q)]) * float(gam[at(q - 1)])) * float(den[at(q)])
             x[at(hi)] = gam[at(hi)]
-            for q in range(hi - 1, 0, -1):
+            # the global form (tridiag_solver_global_2d on one task: the particular solution of the
+            # owned block, zero elsewhere, :5291-5519) stops at the owned range
+            for q in range(hi - 1, (lo - 1) if glob else 0, -1):
                 x[at(q)] = float(gam[at(q)]) - float(om[at(q)]) * float(x[at(q + 1)])
         res.append(x)
     return res[0], res[1]
 
 
-def _vsum_planes(P, A):
+def _vsum_planes(P, A, glob=False):
     """setup_preconditioner_tridiag_local_3d (:3737-3830): per column the sums over levels of the
     three vertical offsets of each horizontal coupling, ((s + A(m)) + A(m+9)) + A(m+18); inactive
     columns get the identity (centre 1, the rest 0)."""
@@ -154,8 +163,13 @@ def _vsum_planes(P, A):
             acc = ((acc + A[:, :, k, m]) + A[:, :, k, m + 9]) + A[:, :, k, m + 18]
         out[m] = acc
     inact = P.active_vertex == 0
-    out[:, inact] = 0.0
-    out[4, inact] = 1.0
+    if glob:  # setup_preconditioner_tridiag_global_3d (:3937-4195): the centre only, then the halo
+        out[4, inact] = 1.0  # update of every summed plane (:4056-4057)
+        for m in range(9):
+            _halo(out[m], P.par)
+    else:
+        out[:, inact] = 0.0
+        out[4, inact] = 1.0
     return out
 
 
@@ -174,7 +188,7 @@ def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8, precond=1):
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
     xu, xv = np.zeros_like(bu), np.zeros_like(bv)
     adu, adv = P.Auu[_m(0, 0)], P.Avv[_m(0, 0)]
-    T = _tri_setup_2d(P, P.Auu, P.Avv) if precond == 3 else None
+    T = _tri_setup_2d(P, P.Auu, P.Avv, glob=precond == 4) if precond in (3, 4) else None
     _halo(xu, par)
     _halo(xv, par)
     zu, zv = _matvec(P, xu, xv)
@@ -185,8 +199,8 @@ def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8, precond=1):
     l2_rhs = math.sqrt(_gsum(P, bu * bu, bv * bv))
     err = float("nan")
     for it in range(1, maxiters + 1):
-        if precond == 3:
-            zu, zv = _tri_solve_2d(P, T, ru, rv)
+        if precond in (3, 4):
+            zu, zv = _tri_solve_2d(P, T, ru, rv, glob=precond == 4)
             _halo(zu, par)
             _halo(zv, par)
         else:
@@ -228,8 +242,8 @@ def _gsum2(P, a1, b1, a2, b2):
 def _precond(P, precond, ru, rv, T=None):
     if precond == 0:
         return ru.copy(), rv.copy()
-    if precond == 3:
-        zu, zv = _tri_solve_2d(P, T, ru, rv)
+    if precond in (3, 4):
+        zu, zv = _tri_solve_2d(P, T, ru, rv, glob=precond == 4)
         _halo(zu, P.par)
         _halo(zv, P.par)
         return zu, zv
@@ -244,8 +258,8 @@ def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8):
     most 100 iterations (maxiters_tridiag, :1703-1732); returns (xu, xv, err, niters)."""
     par = P.par
     T = None
-    if precond == 3:
-        T = _tri_setup_2d(P, P.Auu, P.Avv)
+    if precond in (3, 4):
+        T = _tri_setup_2d(P, P.Auu, P.Avv, glob=precond == 4)
         maxiters = 100
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
     xu, xv = np.zeros_like(bu), np.zeros_like(bv)
@@ -374,8 +388,8 @@ def _sia(P, A, r, z):
 def _precond3(P, precond, ru, rv, zu, zv, T=None):
     if precond == 0:
         return ru.copy(), rv.copy()
-    if precond == 3:  # tridiag_solver_local_3d (:4524-4655)
-        su, sv = _tri_solve_2d(P, T, _line_rhs_3d(ru), _line_rhs_3d(rv))
+    if precond in (3, 4):  # tridiag_solver_local_3d (:4524-4655) / _global_3d (:4662-4913)
+        su, sv = _tri_solve_2d(P, T, _line_rhs_3d(ru), _line_rhs_3d(rv), glob=precond == 4)
         _halo(su, P.par)
         _halo(sv, P.par)
         zu, zv = _sia(P, P.Auu, ru, zu), _sia(P, P.Avv, rv, zv)
@@ -391,7 +405,8 @@ def pcg_chrongear_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
     """pcg_solver_chrongear_3d (:2632-3594) with precond 0, 1 or 2, from x0 = 0: the first pass
     (:3048-3290), then iterations 2.. (:3296-3581); returns (xu, xv, err, niters)."""
     par = P.par
-    T = _tri_setup_2d(P, _vsum_planes(P, P.Auu), _vsum_planes(P, P.Avv)) if precond == 3 else None
+    T = (_tri_setup_2d(P, _vsum_planes(P, P.Auu, precond == 4), _vsum_planes(P, P.Avv, precond == 4),
+                       glob=precond == 4) if precond in (3, 4) else None)
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
     xu, xv = np.zeros_like(bu), np.zeros_like(bv)
     du, dv = np.zeros_like(bu), np.zeros_like(bv)
@@ -483,7 +498,7 @@ def test_second_restatement_matches_oracle(name, make, maxiters):
 
 
 @pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("precond", [0, 1, 3])
+@pytest.mark.parametrize("precond", [0, 1, 3, 4])
 @pytest.mark.parametrize("maxiters", [1, 4, 12, 600])
 def test_second_restatement_chrongear_2d(name, make, precond, maxiters):
     """pcg_solver_chrongear_2d: bit-identical x, err and niters with the oracle's reference-order solve."""
@@ -504,7 +519,8 @@ def pcg_standard_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
     """pcg_solver_standard_3d (:827-1537) with precond 0, 1 or 2, from x0 = 0 (the loop :1169-1524);
     returns (xu, xv, err, niters), niters < 0 where the reference stops with GM_FATAL."""
     par = P.par
-    T = _tri_setup_2d(P, _vsum_planes(P, P.Auu), _vsum_planes(P, P.Avv)) if precond == 3 else None
+    T = (_tri_setup_2d(P, _vsum_planes(P, P.Auu, precond == 4), _vsum_planes(P, P.Avv, precond == 4),
+                       glob=precond == 4) if precond in (3, 4) else None)
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
     xu, xv = np.zeros_like(bu), np.zeros_like(bv)
     _halo(xu, par)
@@ -547,16 +563,30 @@ def pcg_standard_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
     return xu, xv, err, niters
 
 
+def _no_ice_edge_coefficients():
+    """A no_ice slab whose last owned row and column keep nonzero couplings (a matrix that was not
+    halo-updated before the solve): the global line preconditioner's halo update of its summed
+    planes then zeroes owned entries, which the local form does not."""
+    P = problems.slab_3d(seed=3, boundary_ice=True, bc="no_ice", sliding=False)
+    ihi, jhi = P.par["staggered_ihi"], P.par["staggered_jhi"]
+    for name in ("Auu", "Auv", "Avu", "Avv"):
+        A = getattr(P, name)
+        A[:, ihi - 1] = A[:, ihi - 2]
+        A[jhi - 1, :] = A[jhi - 2, :]
+    return P
+
+
 CASES3 = [
     ("slab-periodic-sliding", lambda: problems.slab_3d(seed=1)),
     ("slab-periodic-boundary-ice", lambda: problems.slab_3d(seed=3, boundary_ice=True, sliding=False)),
     ("slab-outflow-boundary-ice", lambda: problems.slab_3d(seed=4, boundary_ice=True, bc="outflow", sliding=False)),
     ("dome", lambda: asm.dome()),
+    ("slab-no-ice-edge-coefficients", _no_ice_edge_coefficients),
 ]
 
 
 @pytest.mark.parametrize("name,make", CASES3, ids=[c[0] for c in CASES3])
-@pytest.mark.parametrize("precond", [0, 1, 2, 3])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("maxiters", [1, 4, 12, 400])
 def test_second_restatement_chrongear_3d(name, make, precond, maxiters):
     """pcg_solver_chrongear_3d: bit-identical x, err and niters with the oracle's reference-order solve."""
@@ -574,7 +604,7 @@ def test_second_restatement_chrongear_3d(name, make, precond, maxiters):
 
 
 @pytest.mark.parametrize("name,make", CASES3, ids=[c[0] for c in CASES3])
-@pytest.mark.parametrize("precond", [0, 1, 2, 3])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("maxiters", [1, 4, 12, 400])
 def test_second_restatement_standard_3d(name, make, precond, maxiters):
     """pcg_solver_standard_3d (the dome with the diagonal preconditioner is the reference's own CPU
@@ -593,16 +623,18 @@ def test_second_restatement_standard_3d(name, make, precond, maxiters):
 
 
 @pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("precond", [3, 4])
 @pytest.mark.parametrize("maxiters", [3, 12, 400])
-def test_second_restatement_standard_2d_lines(name, make, maxiters):
-    """pcg_solver_standard_2d with the local tridiagonal line preconditioner (precond 3)."""
+def test_second_restatement_standard_2d_lines(name, make, precond, maxiters):
+    """pcg_solver_standard_2d with the tridiagonal line preconditioners (3 local, 4 global)."""
     P = make()
     try:
-        xu, xv, err, nit = pcg_standard_2d_diag(P, maxiters, precond=3)
+        xu, xv, err, nit = pcg_standard_2d_diag(P, maxiters, precond=precond)
     except ZeroDivisionError:
         xu = xv = None
         err, nit = float("nan"), -1
-    st, ou, ov, oerr, onit = oracle.pcg("standard", P, 3, tol=1e-8, maxiters=maxiters, summode=oracle.SUM_SEQ)
+    st, ou, ov, oerr, onit = oracle.pcg("standard", P, precond, tol=1e-8, maxiters=maxiters,
+                                        summode=oracle.SUM_SEQ)
     if st != 0:
         assert nit < 0
         return
