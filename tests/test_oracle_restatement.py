@@ -11,7 +11,9 @@ libglimmer/parallel_mpi.F90:10609-10936), matvec_multiply_structured_2d/_3d (:56
 two-field forms, parallel_mpi.F90:6620-6637, 6770-6790, 6904, 7042), the diagonal and SIA
 preconditioners (setup_preconditioner_diag_2d/_3d, setup_preconditioner_sia_3d :3647-3733,
 easy_sia_solver and tridiag_solver :5777-5922, setup_preconditioner_tridiag_local_2d/_3d
-:3737-3830, :4247-4392, tridiag_solver_local_2d/_3d :4917-5100, :4524-4655) and the solver loops.  Element-wise statements use
+:3737-3830, :4247-4392, tridiag_solver_local_2d/_3d :4917-5100, :4524-4655, and the global forms)
+and the solver loops, plus the residual steps of the Picard loop (compute_residual_vector_2d/_3d and
+compute_residual_velocity_2d/_3d, glissade_velo_higher.F90:9502-9894, 10188-10446).  Element-wise statements use
 numpy arrays (one IEEE operation per element); the 3D matvec runs over all nodes at once but adds
 each node's couplings in the reference's order; the global sums are sequential Python loops.  Two
 restatements written separately that agree bit for bit at every iteration count rule out
@@ -642,3 +644,76 @@ def test_second_restatement_standard_2d_lines(name, make, precond, maxiters):
     assert (err == oerr) or (math.isnan(err) and math.isnan(oerr))
     np.testing.assert_array_equal(xu, ou)
     np.testing.assert_array_equal(xv, ov)
+
+
+# ---------------------------------------------------------------------------------------------
+# the residual steps of the Picard loop around the solve
+# ---------------------------------------------------------------------------------------------
+def residual_vector(P, u, v):
+    """compute_residual_vector_2d/_3d (glissade_velo_higher.F90:9502-9689, 9693-9894): A u - b on the
+    owned active vertices (the matvec's statements and order), 0 elsewhere; L2_norm over them, and
+    L2_norm_relative = L2_norm / |b| over the same vertices (0 for a zero b)."""
+    is3d = P.kind == "3d"
+    mv, gs = (_matvec3, _gsum3) if is3d else (_matvec, _gsum)
+    yu, yv = mv(P, u, v)
+    par = P.par
+    own = np.zeros(P.active_vertex.shape, dtype=bool)
+    own[par["staggered_jlo"] - 1:par["staggered_jhi"], par["staggered_ilo"] - 1:par["staggered_ihi"]] = True
+    live = own & (P.active_vertex != 0)
+    if is3d:
+        live = np.broadcast_to(live[:, :, None], yu.shape)
+    ru = np.where(live, yu - P.bu, 0.0)
+    rv = np.where(live, yv - P.bv, 0.0)
+    l2 = math.sqrt(gs(P, np.where(live, ru * ru, 0.0), np.where(live, rv * rv, 0.0)))
+    l2b = math.sqrt(gs(P, np.where(live, P.bu * P.bu, 0.0), np.where(live, P.bv * P.bv, 0.0)))
+    return ru, rv, l2, (l2 / l2b if l2b > 0.0 else 0.0)
+
+
+def residual_velocity(P, which, u, v, us, vs):
+    """compute_residual_velocity_2d/_3d (:10188-10310, :10314-10446): the largest relative speed change
+    over the owned vertices, in 3D without the bed level for HO_RESID_MAXU_NO_UBAS (1); the mean
+    for HO_RESID_MEANU (2); otherwise every level."""
+    par = P.par
+    is3d = P.kind == "3d"
+    nz = u.shape[2] if is3d else 1
+    kmax = nz - 1 if (is3d and which in (1, 2)) else nz
+    res, count = 0.0, 0
+    lu, lv, lus, lvs = u.tolist(), v.tolist(), us.tolist(), vs.tolist()
+    for j in range(par["staggered_jlo"], par["staggered_jhi"] + 1):
+        for i in range(par["staggered_ilo"], par["staggered_ihi"] + 1):
+            for k in range(kmax):
+                g = (lambda a: a[j - 1][i - 1][k]) if is3d else (lambda a: a[j - 1][i - 1])
+                speed = math.sqrt(g(lu) * g(lu) + g(lv) * g(lv))
+                if speed != 0.0:
+                    old = math.sqrt(g(lus) * g(lus) + g(lvs) * g(lvs))
+                    diff = abs((old - speed) / speed)
+                    if which == 2:
+                        count += 1
+                        res = res + diff
+                    elif diff > res:
+                        res = diff
+    if which == 2 and count > 0:
+        res = res / count
+    return res
+
+
+RESID_CASES = CASES + [c for c in CASES3 if c[0] != "slab-no-ice-edge-coefficients"]
+
+
+@pytest.mark.parametrize("name,make", RESID_CASES, ids=[c[0] for c in RESID_CASES])
+def test_second_restatement_residuals(name, make):
+    """The residual vector, its norms and the velocity residuals: bit-identical with the oracle."""
+    P = make()
+    rng = np.random.default_rng(11)
+    u, v = rng.standard_normal(P.bu.shape) * 50.0, rng.standard_normal(P.bv.shape) * 50.0
+    us, vs = u * (1.0 + 0.01 * rng.standard_normal(u.shape)), v * (1.0 + 0.01 * rng.standard_normal(v.shape))
+    u[tuple(ix[:3] for ix in np.nonzero(np.ones(u.shape, dtype=bool)))] = 0.0  # a few zero speeds
+    v[tuple(ix[:3] for ix in np.nonzero(np.ones(v.shape, dtype=bool)))] = 0.0
+    ru, rv, l2, l2r = residual_vector(P, u, v)
+    ou, ov, ol2, ol2r = oracle.residual_vector(P, u, v, summode=oracle.SUM_SEQ)
+    np.testing.assert_array_equal(ru, ou)
+    np.testing.assert_array_equal(rv, ov)
+    assert l2 == ol2 and l2r == ol2r
+    for which in (0, 1, 2):
+        assert residual_velocity(P, which, u, v, us, vs) == \
+            oracle.residual_velocity(P, which, u, v, us, vs, summode=oracle.SUM_SEQ)
