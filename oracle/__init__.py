@@ -11,7 +11,9 @@ __graft_entry__.smoke() and bench.py's CPU-baseline arm may use it, and only as
 the checker or the timed CPU baseline.
 
 Parity is unpinned against reference outputs (no Fortran compiler here and no
-golden vectors in the reference); see pcg_oracle.cpp's header.
+golden vectors in the reference); it is checked against mathematical known answers and,
+bit for bit, against a second restatement of the solver path written separately in Python
+(tests/test_oracle_restatement.py); see pcg_oracle.cpp's header.
 
 Sum modes: SUM_SEQ (the reference's order), SUM_EXACT (exact, reproducible),
 SUM_DDTREE (restatement of the GPU library's reduction tree), SUM_REPRO (restatement of

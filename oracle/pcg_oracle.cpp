@@ -9,7 +9,10 @@
 // this build environment, and the reference ships no golden vectors or
 // known-answer tests for this path.  This restatement is therefore *unpinned*
 // against reference outputs; it is pinned against mathematical known answers
-// (dense solves, dense matvecs, Thomas vs dense) in tests/test_oracle_kat.py.
+// (dense solves, dense matvecs, Thomas vs dense) in tests/test_oracle_kat.py, and
+// against a second restatement of the four solvers, their preconditioners, halo,
+// matvecs, sums and the residual steps, written separately in Python from the
+// reference source (tests/test_oracle_restatement.py), which it equals bit for bit.
 //
 // It restates, loop for loop and in the same floating-point operation order:
 //   libglissade/glissade_velo_higher_pcg.F90
