@@ -717,3 +717,136 @@ def test_second_restatement_residuals(name, make):
     for which in (0, 1, 2):
         assert residual_velocity(P, which, u, v, us, vs) == \
             oracle.residual_velocity(P, which, u, v, us, vs, summode=oracle.SUM_SEQ)
+
+
+# ---------------------------------------------------------------------------------------------
+# assemble_stiffness_matrix_2d, SSA (glissade_velo_higher.F90:4961-5378)
+# ---------------------------------------------------------------------------------------------
+_RSQRT3 = 1.0 / math.sqrt(3.0)
+_XQP = (-_RSQRT3, _RSQRT3, _RSQRT3, -_RSQRT3)  # quadrature points in the reference square (:528-538)
+_YQP = (-_RSQRT3, -_RSQRT3, _RSQRT3, _RSQRT3)
+_ISHIFT = ((0, 1, 1, 0), (-1, 0, 0, -1), (-1, 0, 0, -1), (0, 1, 1, 0))  # rows 1-4, columns 1-4 (:461-468)
+_JSHIFT = ((0, 0, 1, 1), (0, 0, 1, 1), (-1, -1, 0, 0), (-1, -1, 0, 0))  # (:474-481)
+
+
+def _ref_square(p):
+    """phi_2d, dphi_dxr_2d, dphi_dyr_2d at quadrature point p (:555-575)."""
+    x, y = _XQP[p], _YQP[p]
+    phi = ((1.0 - x) * (1.0 - y) / 4.0, (1.0 + x) * (1.0 - y) / 4.0, (1.0 + x) * (1.0 + y) / 4.0,
+           (1.0 - x) * (1.0 + y) / 4.0)
+    dxr = (-(1.0 - y) / 4.0, (1.0 - y) / 4.0, (1.0 + y) / 4.0, -(1.0 + y) / 4.0)
+    dyr = (-(1.0 - x) / 4.0, -(1.0 + x) / 4.0, (1.0 + x) / 4.0, (1.0 - x) / 4.0)
+    return phi, dxr, dyr
+
+
+def assemble_ssa_2d(nx, ny, nz, sigma, active_cell, xv, yv, uvel, vvel, stagthck, flwafact, whichefvs,
+                    efvs_constant, effstrain_min, n_glen, nhalo=2):
+    """The SSA branch: glissade_vertical_average of the flow factor (glissade_grid_operators.F90:
+    1882-1946), then per active cell of the reference's loop (nhalo+1 .. n-nhalo+1) and quadrature
+    point get_basis_function_derivatives_2d (:6319-6504), compute_effective_viscosity (:7285-7470),
+    the thickness at the point and compute_element_matrix (:8001-8123), the cell's viscosity, and
+    element_to_global_matrix_2d (:8127-8196).  Arrays as the oracle's: vertex fields (ny-1, nx-1),
+    cell fields (ny, nx[, nz-1]), blocks (9, ny-1, nx-1)."""
+    vol0 = 1.0e9
+    p_eff = (1.0 - n_glen) / n_glen
+    effstrain_ff = 500.0 / 31536000.0 / 200.0e3 * 31536000.0  # velo_scale / len_scale * scyr
+    ff2 = np.zeros((ny, nx))
+    for j in range(ny):
+        for i in range(nx):
+            acc = 0.0
+            for k in range(nz - 1):
+                acc = acc + float(flwafact[j, i, k]) * (float(sigma[k + 1]) - float(sigma[k]))
+            ff2[j, i] = acc
+    A = [np.zeros((9, ny - 1, nx - 1)) for _ in range(4)]
+    efvs_out = np.zeros((ny, nx, nz - 1))
+    for j in range(nhalo + 1, ny - nhalo + 2):
+        for i in range(nhalo + 1, nx - nhalo + 2):
+            if not active_cell[j - 1, i - 1]:
+                continue
+            verts = [(i + _ISHIFT[2][n], j + _JSHIFT[2][n]) for n in range(4)]  # node n's vertex (1-based)
+            x = [float(xv[jv - 1, iv - 1]) for iv, jv in verts]
+            y = [float(yv[jv - 1, iv - 1]) for iv, jv in verts]
+            u = [float(uvel[jv - 1, iv - 1]) for iv, jv in verts]
+            v = [float(vvel[jv - 1, iv - 1]) for iv, jv in verts]
+            h = [float(stagthck[jv - 1, iv - 1]) for iv, jv in verts]
+            K = [[[0.0] * 4 for _ in range(4)] for _ in range(4)]  # Kuu, Kuv, Kvu, Kvv [nr][nc]
+            evq = [0.0] * 4
+            for p in range(4):
+                phi, dxr, dyr = _ref_square(p)
+                j11 = j12 = j21 = j22 = 0.0
+                for n in range(4):
+                    j11 = j11 + dxr[n] * x[n]
+                    j12 = j12 + dxr[n] * y[n]
+                    j21 = j21 + dyr[n] * x[n]
+                    j22 = j22 + dyr[n] * y[n]
+                det = j11 * j22 - j12 * j21
+                if not abs(det) > 0.0:
+                    raise ZeroDivisionError("Jacobian matrix is singular")
+                i11, i12, i21, i22 = j22 / det, -j12 / det, -j21 / det, j11 / det
+                dx = [(0.0 + i11 * dxr[n]) + i12 * dyr[n] for n in range(4)]
+                dy = [(0.0 + i21 * dxr[n]) + i22 * dyr[n] for n in range(4)]
+                if whichefvs == 0:
+                    ev = efvs_constant
+                elif whichefvs == 1:
+                    ev = float(ff2[j - 1, i - 1]) * effstrain_ff ** p_eff
+                else:
+                    dudx = dudy = dvdx = dvdy = 0.0
+                    for n in range(4):
+                        dudx = dudx + dx[n] * u[n]
+                        dudy = dudy + dy[n] * u[n]
+                        dvdx = dvdx + dx[n] * v[n]
+                        dvdy = dvdy + dy[n] * v[n]
+                    sh = dvdx + dudy
+                    esq = effstrain_min * effstrain_min + \
+                        (((dudx * dudx + dvdy * dvdy) + dudx * dvdy) + 0.25 * (sh * sh))
+                    ev = float(ff2[j - 1, i - 1]) * esq ** (p_eff / 2.0)
+                evq[p] = ev
+                hq = 0.0
+                for n in range(4):
+                    hq = hq + phi[n] * h[n]
+                fac = (hq * ev) * 1.0 * det / vol0
+                for nc in range(4):
+                    for nr in range(4):
+                        K[0][nr][nc] = K[0][nr][nc] + fac * (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc])
+                        K[1][nr][nc] = K[1][nr][nc] + fac * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc])
+                        K[2][nr][nc] = K[2][nr][nc] + fac * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc])
+                        K[3][nr][nc] = K[3][nr][nc] + fac * (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc])
+            acc = 0.0
+            for p in range(4):
+                acc = acc + evq[p]
+            efvs_out[j - 1, i - 1, :] = acc / 4
+            for nr in range(4):
+                iv, jv = i + _ISHIFT[2][nr], j + _JSHIFT[2][nr]
+                for nc in range(4):
+                    m = _m(_ISHIFT[nr][nc], _JSHIFT[nr][nc])
+                    for b in range(4):
+                        A[b][m, jv - 1, iv - 1] = float(A[b][m, jv - 1, iv - 1]) + K[b][nr][nc]
+    return efvs_out, A
+
+
+def _ssa_inputs(seed, velocity):
+    from tests.test_oracle_assembly import geometry
+    g = geometry(seed=seed)
+    rng = np.random.default_rng(seed + 50)
+    shape = (g["ny"] - 1, g["nx"] - 1)
+    u = 40.0 * rng.standard_normal(shape) if velocity else np.zeros(shape)
+    v = 40.0 * rng.standard_normal(shape) if velocity else np.zeros(shape)
+    ff = 0.5 * 1.0e-16 ** (-1.0 / 3.0) * (1.0 + 0.2 * rng.random((g["ny"], g["nx"], g["nz"] - 1)))
+    return g, u, v, ff
+
+
+@pytest.mark.parametrize("whichefvs", [0, 1, 2])
+@pytest.mark.parametrize("seed,velocity", [(31, False), (32, True), (33, True)])
+def test_second_restatement_ssa_assembly(whichefvs, seed, velocity):
+    """assemble_stiffness_matrix_2d (SSA): every coefficient and the cell viscosities bit-identical
+    with the oracle, for constant, flow-factor and nonlinear (Glen) viscosity."""
+    g, u, v, ff = _ssa_inputs(seed, velocity)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    args = (nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], u, v, g["stagthck"], ff)
+    kw = dict(whichefvs=whichefvs, efvs_constant=2.5e6, effstrain_min=1.0e-8, n_glen=3.0)
+    st, oefvs, *oA = oracle.assemble_stiffness_2d(*args, **kw)
+    assert st == 0
+    efvs, A = assemble_ssa_2d(*args, whichefvs, 2.5e6, 1.0e-8, 3.0)
+    np.testing.assert_array_equal(efvs, oefvs)
+    for got, want in zip(A, oA):
+        np.testing.assert_array_equal(got, want)
