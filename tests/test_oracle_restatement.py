@@ -13,7 +13,9 @@ preconditioners (setup_preconditioner_diag_2d/_3d, setup_preconditioner_sia_3d :
 easy_sia_solver and tridiag_solver :5777-5922, setup_preconditioner_tridiag_local_2d/_3d
 :3737-3830, :4247-4392, tridiag_solver_local_2d/_3d :4917-5100, :4524-4655, and the global forms)
 and the solver loops, plus the residual steps of the Picard loop (compute_residual_vector_2d/_3d and
-compute_residual_velocity_2d/_3d, glissade_velo_higher.F90:9502-9894, 10188-10446).  Element-wise statements use
+compute_residual_velocity_2d/_3d, glissade_velo_higher.F90:9502-9894, 10188-10446) and the stiffness
+assembly (assemble_stiffness_matrix_3d :5382-5643, the SSA branch of assemble_stiffness_matrix_2d
+:4961-5378, with the basis-function derivatives, viscosities, element matrices and scatters).  Element-wise statements use
 numpy arrays (one IEEE operation per element); the 3D matvec runs over all nodes at once but adds
 each node's couplings in the reference's order; the global sums are sequential Python loops.  Two
 restatements written separately that agree bit for bit at every iteration count rule out
@@ -847,6 +849,170 @@ def test_second_restatement_ssa_assembly(whichefvs, seed, velocity):
     st, oefvs, *oA = oracle.assemble_stiffness_2d(*args, **kw)
     assert st == 0
     efvs, A = assemble_ssa_2d(*args, whichefvs, 2.5e6, 1.0e-8, 3.0)
+    np.testing.assert_array_equal(efvs, oefvs)
+    for got, want in zip(A, oA):
+        np.testing.assert_array_equal(got, want)
+
+
+# ---------------------------------------------------------------------------------------------
+# assemble_stiffness_matrix_3d (glissade_velo_higher.F90:5382-5643)
+# ---------------------------------------------------------------------------------------------
+_XQ3 = (-_RSQRT3, _RSQRT3, _RSQRT3, -_RSQRT3, -_RSQRT3, _RSQRT3, _RSQRT3, -_RSQRT3)  # (:314-338)
+_YQ3 = (-_RSQRT3, -_RSQRT3, _RSQRT3, _RSQRT3, -_RSQRT3, -_RSQRT3, _RSQRT3, _RSQRT3)
+_ZQ3 = (-_RSQRT3,) * 4 + (_RSQRT3,) * 4
+_I1, _I2 = (0, 1, 1, 0, 0, 1, 1, 0), (-1, 0, 0, -1, -1, 0, 0, -1)  # ishift rows (:461-468)
+_J1, _J3 = (0, 0, 1, 1, 0, 0, 1, 1), (-1, -1, 0, 0, -1, -1, 0, 0)  # jshift rows (:474-481)
+_K1, _K5 = (0, 0, 0, 0, -1, -1, -1, -1), (1, 1, 1, 1, 0, 0, 0, 0)  # kshift rows (:486-493)
+_ISH3 = (_I1, _I2, _I2, _I1, _I1, _I2, _I2, _I1)
+_JSH3 = (_J1, _J1, _J3, _J3, _J1, _J1, _J3, _J3)
+_KSH3 = (_K1, _K1, _K1, _K1, _K5, _K5, _K5, _K5)
+
+
+def _ref_cube(p):
+    """dphi_dxr_3d, dphi_dyr_3d, dphi_dzr_3d at quadrature point p (:355-391)."""
+    x, y, z = _XQ3[p], _YQ3[p], _ZQ3[p]
+    dxr = (-(1.0 - y) * (1.0 - z) / 8.0, (1.0 - y) * (1.0 - z) / 8.0, (1.0 + y) * (1.0 - z) / 8.0,
+           -(1.0 + y) * (1.0 - z) / 8.0, -(1.0 - y) * (1.0 + z) / 8.0, (1.0 - y) * (1.0 + z) / 8.0,
+           (1.0 + y) * (1.0 + z) / 8.0, -(1.0 + y) * (1.0 + z) / 8.0)
+    dyr = (-(1.0 - x) * (1.0 - z) / 8.0, -(1.0 + x) * (1.0 - z) / 8.0, (1.0 + x) * (1.0 - z) / 8.0,
+           (1.0 - x) * (1.0 - z) / 8.0, -(1.0 - x) * (1.0 + z) / 8.0, -(1.0 + x) * (1.0 + z) / 8.0,
+           (1.0 + x) * (1.0 + z) / 8.0, (1.0 - x) * (1.0 + z) / 8.0)
+    dzr = (-(1.0 - x) * (1.0 - y) / 8.0, -(1.0 + x) * (1.0 - y) / 8.0, -(1.0 + x) * (1.0 + y) / 8.0,
+           -(1.0 - x) * (1.0 + y) / 8.0, (1.0 - x) * (1.0 - y) / 8.0, (1.0 + x) * (1.0 - y) / 8.0,
+           (1.0 + x) * (1.0 + y) / 8.0, (1.0 - x) * (1.0 + y) / 8.0)
+    return dxr, dyr, dzr
+
+
+def assemble_3d(nx, ny, nz, sigma, active_cell, xv, yv, uvel, vvel, stagusrf, stagthck, flwafact, whichapprox,
+                whichefvs, efvs_constant, effstrain_min, n_glen, nhalo=2):
+    """Per active cell of the reference's loop and layer k: the element's nodes (ishift/jshift/
+    kshift row 7: nodes 1-4 on level k+1, 5-8 on level k), per quadrature point
+    get_basis_function_derivatives_3d (:6508-6732: Jacobian, cofactors, detJ, Jinv = cofactor^T /
+    detJ), compute_effective_viscosity (:7285-7470, the SIA / SSA / 3D branches) and
+    compute_element_matrix (:8001-8123), the layer's mean viscosity, element_to_global_matrix_3d
+    (:8200-8268).  Arrays as the oracle's."""
+    vol0 = 1.0e9
+    p_eff = (1.0 - n_glen) / n_glen
+    effstrain_ff = 500.0 / 31536000.0 / 200.0e3 * 31536000.0
+    A = [np.zeros((ny - 1, nx - 1, nz, 27)) for _ in range(4)]
+    efvs_out = np.zeros((ny, nx, nz - 1))
+    cubes = [_ref_cube(p) for p in range(8)]
+    for j in range(nhalo + 1, ny - nhalo + 2):
+        for i in range(nhalo + 1, nx - nhalo + 2):
+            if not active_cell[j - 1, i - 1]:
+                continue
+            for k in range(1, nz):
+                nodes = [(i + _ISH3[6][n], j + _JSH3[6][n], k + _KSH3[6][n]) for n in range(8)]
+                x = [float(xv[jn - 1, in_ - 1]) for in_, jn, kn in nodes]
+                y = [float(yv[jn - 1, in_ - 1]) for in_, jn, kn in nodes]
+                z = [float(stagusrf[jn - 1, in_ - 1]) - float(sigma[kn - 1]) * float(stagthck[jn - 1, in_ - 1])
+                     for in_, jn, kn in nodes]
+                u = [float(uvel[jn - 1, in_ - 1, kn - 1]) for in_, jn, kn in nodes]
+                v = [float(vvel[jn - 1, in_ - 1, kn - 1]) for in_, jn, kn in nodes]
+                ff = float(flwafact[j - 1, i - 1, k - 1])
+                K = [[[0.0] * 8 for _ in range(8)] for _ in range(4)]
+                evq = [0.0] * 8
+                for p in range(8):
+                    dxr, dyr, dzr = cubes[p]
+                    J = [[0.0] * 3 for _ in range(3)]
+                    for n in range(8):
+                        for r, d in enumerate((dxr, dyr, dzr)):
+                            J[r][0] = J[r][0] + d[n] * x[n]
+                            J[r][1] = J[r][1] + d[n] * y[n]
+                            J[r][2] = J[r][2] + d[n] * z[n]
+                    c = [[J[1][1] * J[2][2] - J[1][2] * J[2][1], -(J[1][0] * J[2][2] - J[1][2] * J[2][0]),
+                          J[1][0] * J[2][1] - J[1][1] * J[2][0]],
+                         [-(J[0][1] * J[2][2] - J[0][2] * J[2][1]), J[0][0] * J[2][2] - J[0][2] * J[2][0],
+                          -(J[0][0] * J[2][1] - J[0][1] * J[2][0])],
+                         [J[0][1] * J[1][2] - J[0][2] * J[1][1], -(J[0][0] * J[1][2] - J[0][2] * J[1][0]),
+                          J[0][0] * J[1][1] - J[0][1] * J[1][0]]]
+                    det = (J[0][0] * c[0][0] + J[0][1] * c[0][1]) + J[0][2] * c[0][2]
+                    if not abs(det) > 0.0:
+                        raise ZeroDivisionError("Jacobian matrix is singular")
+                    Ji = [[c[col][row] / det for col in range(3)] for row in range(3)]
+                    dx = [(Ji[0][0] * dxr[n] + Ji[0][1] * dyr[n]) + Ji[0][2] * dzr[n] for n in range(8)]
+                    dy = [(Ji[1][0] * dxr[n] + Ji[1][1] * dyr[n]) + Ji[1][2] * dzr[n] for n in range(8)]
+                    dz = [(Ji[2][0] * dxr[n] + Ji[2][1] * dyr[n]) + Ji[2][2] * dzr[n] for n in range(8)]
+                    if whichefvs == 0:
+                        ev = efvs_constant
+                    elif whichefvs == 1:
+                        ev = ff * effstrain_ff ** p_eff
+                    else:
+                        dudx = dudy = dudz = dvdx = dvdy = dvdz = 0.0
+                        for n in range(8):
+                            if whichapprox == 0:
+                                dudz = dudz + dz[n] * u[n]
+                                dvdz = dvdz + dz[n] * v[n]
+                            else:
+                                dudx = dudx + dx[n] * u[n]
+                                dudy = dudy + dy[n] * u[n]
+                                dvdx = dvdx + dx[n] * v[n]
+                                dvdy = dvdy + dy[n] * v[n]
+                                if whichapprox != 1:
+                                    dudz = dudz + dz[n] * u[n]
+                                    dvdz = dvdz + dz[n] * v[n]
+                        em2 = effstrain_min * effstrain_min
+                        sh = dvdx + dudy
+                        if whichapprox == 0:
+                            esq = em2 + 0.25 * (dudz * dudz + dvdz * dvdz)
+                        elif whichapprox == 1:
+                            esq = em2 + (((dudx * dudx + dvdy * dvdy) + dudx * dvdy) + 0.25 * (sh * sh))
+                        else:
+                            esq = (em2 + (((dudx * dudx + dvdy * dvdy) + dudx * dvdy) + 0.25 * (sh * sh))) + \
+                                0.25 * (dudz * dudz + dvdz * dvdz)
+                        ev = ff * esq ** (p_eff / 2.0)
+                    evq[p] = ev
+                    fac = ev * 1.0 * det / vol0
+                    for nc in range(8):
+                        for nr in range(8):
+                            if whichapprox == 0:
+                                t = fac * (dz[nr] * dz[nc])
+                                K[0][nr][nc] = K[0][nr][nc] + t
+                                K[3][nr][nc] = K[3][nr][nc] + t
+                                continue
+                            if whichapprox == 1:
+                                kuu = 4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc]
+                                kvv = 4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc]
+                            else:
+                                kuu = (4.0 * dx[nr] * dx[nc] + dy[nr] * dy[nc]) + dz[nr] * dz[nc]
+                                kvv = (4.0 * dy[nr] * dy[nc] + dx[nr] * dx[nc]) + dz[nr] * dz[nc]
+                            K[0][nr][nc] = K[0][nr][nc] + fac * kuu
+                            K[1][nr][nc] = K[1][nr][nc] + fac * (2.0 * dx[nr] * dy[nc] + dy[nr] * dx[nc])
+                            K[2][nr][nc] = K[2][nr][nc] + fac * (2.0 * dy[nr] * dx[nc] + dx[nr] * dy[nc])
+                            K[3][nr][nc] = K[3][nr][nc] + fac * kvv
+                acc = 0.0
+                for p in range(8):
+                    acc = acc + evq[p]
+                efvs_out[j - 1, i - 1, k - 1] = acc / 8
+                for nr in range(8):
+                    ir, jr, kr = nodes[nr]
+                    for nc in range(8):
+                        m = _m3(_ISH3[nr][nc], _JSH3[nr][nc], _KSH3[nr][nc])
+                        for b in range(4):
+                            A[b][jr - 1, ir - 1, kr - 1, m] = float(A[b][jr - 1, ir - 1, kr - 1, m]) + K[b][nr][nc]
+    return efvs_out, A
+
+
+@pytest.mark.parametrize("whichapprox", [0, 1, 2])
+@pytest.mark.parametrize("whichefvs", [0, 1, 2])
+@pytest.mark.parametrize("seed,velocity", [(41, False), (42, True)])
+def test_second_restatement_3d_assembly(whichapprox, whichefvs, seed, velocity):
+    """assemble_stiffness_matrix_3d (SIA, SSA and Blatter-Pattyn element matrices; constant,
+    flow-factor and Glen viscosity): every coefficient and layer viscosity bit-identical with the
+    oracle."""
+    from tests.test_oracle_assembly import geometry
+    g = geometry(seed=seed)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(seed + 60)
+    shape = (ny - 1, nx - 1, nz)
+    u = 40.0 * rng.standard_normal(shape) if velocity else np.zeros(shape)
+    v = 40.0 * rng.standard_normal(shape) if velocity else np.zeros(shape)
+    ff = 0.5 * 1.0e-16 ** (-1.0 / 3.0) * (1.0 + 0.2 * rng.random((ny, nx, nz - 1)))
+    args = (nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], u, v, g["stagusrf"], g["stagthck"], ff)
+    st, oefvs, *oA = oracle.assemble_stiffness_3d(*args, whichapprox=whichapprox, whichefvs=whichefvs,
+                                                  efvs_constant=2.5e6, effstrain_min=1.0e-8, n_glen=3.0)
+    assert st == 0
+    efvs, A = assemble_3d(*args, whichapprox, whichefvs, 2.5e6, 1.0e-8, 3.0)
     np.testing.assert_array_equal(efvs, oefvs)
     for got, want in zip(A, oA):
         np.testing.assert_array_equal(got, want)
