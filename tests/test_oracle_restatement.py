@@ -1016,3 +1016,74 @@ def test_second_restatement_3d_assembly(whichapprox, whichefvs, seed, velocity):
     np.testing.assert_array_equal(efvs, oefvs)
     for got, want in zip(A, oA):
         np.testing.assert_array_equal(got, want)
+
+
+def _phi3(p):
+    x, y, z = _XQ3[p], _YQ3[p], _ZQ3[p]
+    return ((1.0 - x) * (1.0 - y) * (1.0 - z) / 8.0, (1.0 + x) * (1.0 - y) * (1.0 - z) / 8.0,
+            (1.0 + x) * (1.0 + y) * (1.0 - z) / 8.0, (1.0 - x) * (1.0 + y) * (1.0 - z) / 8.0,
+            (1.0 - x) * (1.0 - y) * (1.0 + z) / 8.0, (1.0 + x) * (1.0 - y) * (1.0 + z) / 8.0,
+            (1.0 + x) * (1.0 + y) * (1.0 + z) / 8.0, (1.0 - x) * (1.0 + y) * (1.0 + z) / 8.0)
+
+
+def load_vector_standard(nx, ny, nz, sigma, active_cell, xv, yv, stagusrf, stagthck, dsx, dsy, nhalo=2):
+    """load_vector_gravity, standard finite-element form (glissade_velo_higher.F90:4341-4449): per
+    element and quadrature point the surface gradient interpolated at the point, and each node's
+    -rhoi*grav*wqp*detJ/vol0*ds*phi added in node order (rhoi = 910, grav = 9.81)."""
+    vol0, rhoi, grav = 1.0e9, 910.0, 9.81
+    lu, lv = np.zeros((ny - 1, nx - 1, nz)), np.zeros((ny - 1, nx - 1, nz))
+    for j in range(nhalo + 1, ny - nhalo + 2):
+        for i in range(nhalo + 1, nx - nhalo + 2):
+            if not active_cell[j - 1, i - 1]:
+                continue
+            for k in range(1, nz):
+                nodes = [(i + _ISH3[6][n], j + _JSH3[6][n], k + _KSH3[6][n]) for n in range(8)]
+                x = [float(xv[jn - 1, in_ - 1]) for in_, jn, kn in nodes]
+                y = [float(yv[jn - 1, in_ - 1]) for in_, jn, kn in nodes]
+                z = [float(stagusrf[jn - 1, in_ - 1]) - float(sigma[kn - 1]) * float(stagthck[jn - 1, in_ - 1])
+                     for in_, jn, kn in nodes]
+                sx = [float(dsx[jn - 1, in_ - 1]) for in_, jn, kn in nodes]
+                sy = [float(dsy[jn - 1, in_ - 1]) for in_, jn, kn in nodes]
+                for p in range(8):
+                    dxr, dyr, dzr = _ref_cube(p)
+                    J = [[0.0] * 3 for _ in range(3)]
+                    for n in range(8):
+                        for r, d in enumerate((dxr, dyr, dzr)):
+                            J[r][0] = J[r][0] + d[n] * x[n]
+                            J[r][1] = J[r][1] + d[n] * y[n]
+                            J[r][2] = J[r][2] + d[n] * z[n]
+                    c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1]
+                    c01 = -(J[1][0] * J[2][2] - J[1][2] * J[2][0])
+                    c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0]
+                    det = (J[0][0] * c00 + J[0][1] * c01) + J[0][2] * c02
+                    phi = _phi3(p)
+                    qx = qy = 0.0
+                    for n in range(8):
+                        qx = qx + phi[n] * sx[n]
+                        qy = qy + phi[n] * sy[n]
+                    for n in range(8):
+                        in_, jn, kn = nodes[n]
+                        lu[jn - 1, in_ - 1, kn - 1] = float(lu[jn - 1, in_ - 1, kn - 1]) - \
+                            rhoi * grav * 1.0 * det / vol0 * qx * phi[n]
+                        lv[jn - 1, in_ - 1, kn - 1] = float(lv[jn - 1, in_ - 1, kn - 1]) - \
+                            rhoi * grav * 1.0 * det / vol0 * qy * phi[n]
+    return lu, lv
+
+
+def test_second_restatement_load_vector_standard():
+    """load_vector_gravity, standard form: bit-identical with the oracle on a rough surface."""
+    from tests.test_oracle_assembly import geometry
+    g = geometry(seed=44)
+    nx, ny, nz, dx = g["nx"], g["ny"], g["nz"], g["dx"]
+    rng = np.random.default_rng(9)
+    sx, sy = 0.01 * rng.standard_normal((ny - 1, nx - 1)), 0.01 * rng.standard_normal((ny - 1, nx - 1))
+    sig = g["sigma"]
+    stagw = np.concatenate([[0.0], 0.5 * (sig[:-1] + sig[1:]), [1.0]])
+    st, ou, ov = oracle.load_vector_gravity(nx, ny, nz, sig, stagw, dx, dx, g["ac"], g["av"], g["xVertex"],
+                                            g["yVertex"], g["stagusrf"], g["stagthck"], sx, sy, 0)
+    assert st == 0
+    lu, lv = load_vector_standard(nx, ny, nz, sig, g["ac"], g["xVertex"], g["yVertex"], g["stagusrf"],
+                                  g["stagthck"], sx, sy)
+    assert np.count_nonzero(lu) > 0
+    np.testing.assert_array_equal(lu, ou)
+    np.testing.assert_array_equal(lv, ov)
