@@ -1087,3 +1087,77 @@ def test_second_restatement_load_vector_standard():
     assert np.count_nonzero(lu) > 0
     np.testing.assert_array_equal(lu, ou)
     np.testing.assert_array_equal(lv, ov)
+
+
+def dirichlet_3d(nx, ny, nz, active_vertex, umask, vmask, uvel, vvel, Auu, Auv, Avu, Avv, bu, bv, nhalo=2):
+    """dirichlet_boundary_conditions_3d (glissade_velo_higher.F90:9305-9498), on copies, in the
+    reference's order: vertices j = nhalo..ny-nhalo+1, i = nhalo..nx-nhalo+1, levels k; a u-prescribed
+    node sets b, a unit diagonal (and zero uv, vu diagonals), zeroes its u row and moves each
+    neighbour's coupling to it into that neighbour's b (kA, jA, iA order); then the same for v."""
+    A = [np.array(a, dtype=np.float64, copy=True) for a in (Auu, Auv, Avu, Avv)]
+    b = [np.array(bu, dtype=np.float64, copy=True), np.array(bv, dtype=np.float64, copy=True)]
+    NX, NY = nx - 1, ny - 1
+    masks = (umask, vmask)
+    vel = (uvel, vvel)
+    c0 = _m3(0, 0, 0)
+    for j in range(nhalo, ny - nhalo + 2):
+        for i in range(nhalo, nx - nhalo + 2):
+            if not active_vertex[j - 1, i - 1]:
+                continue
+            for k in range(1, nz + 1):
+                for comp in (0, 1):  # 0: u prescribed, 1: v prescribed
+                    if masks[comp][j - 1, i - 1, k - 1] != 1:
+                        continue
+                    val = float(vel[comp][j - 1, i - 1, k - 1])
+                    b[comp][j - 1, i - 1, k - 1] = val
+                    for kA in (-1, 0, 1):
+                        for jA in (-1, 0, 1):
+                            for iA in (-1, 0, 1):
+                                kn, jn, in_ = k + kA, j + jA, i + iA
+                                if not (1 <= kn <= nz and 1 <= in_ <= NX and 1 <= jn <= NY):
+                                    continue
+                                if iA == 0 and jA == 0 and kA == 0:
+                                    if comp == 0:
+                                        A[0][j - 1, i - 1, k - 1, c0] = 1.0
+                                        A[1][j - 1, i - 1, k - 1, c0] = 0.0
+                                        A[2][j - 1, i - 1, k - 1, c0] = 0.0
+                                    else:
+                                        A[1][j - 1, i - 1, k - 1, c0] = 0.0
+                                        A[2][j - 1, i - 1, k - 1, c0] = 0.0
+                                        A[3][j - 1, i - 1, k - 1, c0] = 1.0
+                                    continue
+                                m = _m3(iA, jA, kA)
+                                row = (0, 1) if comp == 0 else (2, 3)  # this node's row blocks
+                                A[row[0]][j - 1, i - 1, k - 1, m] = 0.0
+                                A[row[1]][j - 1, i - 1, k - 1, m] = 0.0
+                                mt = _m3(-iA, -jA, -kA)
+                                n = (jn - 1, in_ - 1, kn - 1)
+                                # the neighbour's u row (block uu or uv) and v row (vu or vv) coupling
+                                # to this node's prescribed component
+                                bu_blk, bv_blk = (0, 2) if comp == 0 else (1, 3)
+                                if umask[n] != 1:
+                                    b[0][n] = float(b[0][n]) - float(A[bu_blk][n + (mt,)]) * val
+                                    A[bu_blk][n + (mt,)] = 0.0
+                                if vmask[n] != 1:
+                                    b[1][n] = float(b[1][n]) - float(A[bv_blk][n + (mt,)]) * val
+                                    A[bv_blk][n + (mt,)] = 0.0
+    return (*A, *b)
+
+
+@pytest.mark.parametrize("seed", [51, 52])
+def test_second_restatement_dirichlet_3d(seed):
+    """dirichlet_boundary_conditions_3d with random u-only, v-only and u+v prescribed nodes and
+    nonzero prescribed values: every coefficient and b bit-identical with the oracle."""
+    P = problems.slab_3d(seed=seed, boundary_ice=True, sliding=False)
+    rng = np.random.default_rng(seed)
+    shape = P.bu.shape
+    um = (rng.random(shape) < 0.15).astype(np.int32)
+    vm = (rng.random(shape) < 0.15).astype(np.int32)
+    um[:, :, -1] = 1  # the no-slip bed
+    vm[:, :, -1] = 1
+    uv, vv = rng.standard_normal(shape) * 10.0, rng.standard_normal(shape) * 10.0
+    args = (P.nx, P.ny, P.nz, P.active_vertex, um, vm, uv, vv, P.Auu, P.Auv, P.Avu, P.Avv, P.bu, P.bv)
+    want = oracle.dirichlet_3d(*args)
+    got = dirichlet_3d(*args)
+    for g_, w in zip(got, want):
+        np.testing.assert_array_equal(g_, w)
