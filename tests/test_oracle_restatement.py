@@ -1161,3 +1161,73 @@ def test_second_restatement_dirichlet_3d(seed):
     got = dirichlet_3d(*args)
     for g_, w in zip(got, want):
         np.testing.assert_array_equal(g_, w)
+
+
+def basal_standard_3d(nx, ny, nz, active_cell, xv, yv, beta, lsrf, Auu, Avv, nhalo=2):
+    """basal_sliding_bc_3d, standard finite-element form (glissade_velo_higher.F90:8953-9129): lsrf
+    staggered to the vertices (glissade_stagger, all four cells, glissade_grid_operators.F90:69-157),
+    per active cell and quadrature point the curved area factor (get_area_scale_factor_curved_2d
+    :6736-6827), beta at the point, the 4x4 element matrix and its scatter into the bed layer's
+    horizontal couplings, point by point."""
+    vol0 = 1.0e9
+    A = [np.array(Auu, dtype=np.float64, copy=True), np.array(Avv, dtype=np.float64, copy=True)]
+    sl = np.zeros((ny - 1, nx - 1))
+    for j in range(1, ny):
+        for i in range(1, nx):
+            sl[j - 1, i - 1] = (((float(lsrf[j, i - 1]) + float(lsrf[j, i])) + float(lsrf[j - 1, i - 1])) +
+                                float(lsrf[j - 1, i])) / 4.0
+    for j in range(nhalo + 1, ny - nhalo + 2):
+        for i in range(nhalo + 1, nx - nhalo + 2):
+            if not active_cell[j - 1, i - 1]:
+                continue
+            verts = ((i - 1, j - 1), (i, j - 1), (i, j), (i - 1, j))
+            x = [float(xv[jv - 1, iv - 1]) for iv, jv in verts]
+            y = [float(yv[jv - 1, iv - 1]) for iv, jv in verts]
+            z = [float(sl[jv - 1, iv - 1]) for iv, jv in verts]
+            bb = [float(beta[jv - 1, iv - 1]) for iv, jv in verts]
+            for p in range(4):
+                phi, dxr, dyr = _ref_square(p)
+                j11 = j12 = j13 = j21 = j22 = j23 = 0.0
+                for n in range(4):
+                    j11 = j11 + dxr[n] * x[n]
+                    j12 = j12 + dxr[n] * y[n]
+                    j13 = j13 + dxr[n] * z[n]
+                    j21 = j21 + dyr[n] * x[n]
+                    j22 = j22 + dyr[n] * y[n]
+                    j23 = j23 + dyr[n] * z[n]
+                t1 = j11 * j22 - j12 * j21
+                t2 = -(j11 * j23 - j13 * j21)
+                t3 = j12 * j23 - j13 * j22
+                det = math.sqrt((t1 * t1 + t2 * t2) + t3 * t3)
+                bq = 0.0
+                for n in range(4):
+                    bq = bq + phi[n] * bb[n]
+                K = [[0.0] * 4 for _ in range(4)]
+                for nc in range(4):
+                    for nr in range(4):
+                        K[nr][nc] = K[nr][nc] + bq * 1.0 * det / vol0 * phi[nr] * phi[nc]
+                for nr in range(4):
+                    iv, jv = i + _ISHIFT[2][nr], j + _JSHIFT[2][nr]
+                    for nc in range(4):
+                        m = _m3(_ISHIFT[nr][nc], _JSHIFT[nr][nc], 0)
+                        for a in A:
+                            a[jv - 1, iv - 1, nz - 1, m] = float(a[jv - 1, iv - 1, nz - 1, m]) + K[nr][nc]
+    return A[0], A[1]
+
+
+@pytest.mark.parametrize("seed", [61, 62])
+def test_second_restatement_basal_standard_3d(seed):
+    """The standard (curved) basal friction term: bit-identical bed-layer couplings with the oracle."""
+    from tests.test_oracle_assembly import geometry
+    g = geometry(seed=seed)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(seed)
+    beta = np.exp(np.log(1.0e3) + rng.standard_normal((ny - 1, nx - 1)))
+    lsrf = g["usrf"] - g["thck"] + 20.0 * rng.random((ny, nx))
+    P = problems.slab_3d(seed=seed, ewn=nx - 4, nsn=ny - 4, nz=nz, sliding=False)
+    st, ou, ov = oracle.basal_standard(True, nx, ny, nz, g["ac"], g["xVertex"], g["yVertex"], beta, lsrf, P.Auu, P.Avv)
+    assert st == 0
+    gu, gv = basal_standard_3d(nx, ny, nz, g["ac"], g["xVertex"], g["yVertex"], beta, lsrf, P.Auu, P.Avv)
+    assert not np.array_equal(gu, P.Auu)
+    np.testing.assert_array_equal(gu, ou)
+    np.testing.assert_array_equal(gv, ov)
