@@ -1231,3 +1231,76 @@ def test_second_restatement_basal_standard_3d(seed):
     assert not np.array_equal(gu, P.Auu)
     np.testing.assert_array_equal(gu, ou)
     np.testing.assert_array_equal(gv, ov)
+
+
+def dirichlet_2d(nx, ny, active_vertex, umask, vmask, uvel, vvel, Auu, Auv, Avu, Avv, bu, bv, nhalo=2):
+    """dirichlet_boundary_conditions_2d (glissade_velo_higher.F90:9133-9301), on copies: the offsets
+    (jA, iA) outermost, then the vertices; a u-prescribed vertex sets b and its uu, uv and vu
+    diagonals to 1, a v-prescribed one its uv, vu diagonals to 0 and vv to 1; off the diagonal the
+    vertex's row couplings are zeroed and each neighbour's coupling to it moves into that
+    neighbour's b."""
+    A = [np.array(a, dtype=np.float64, copy=True) for a in (Auu, Auv, Avu, Avv)]
+    b = [np.array(bu, dtype=np.float64, copy=True), np.array(bv, dtype=np.float64, copy=True)]
+    NX, NY = nx - 1, ny - 1
+    c0 = _m(0, 0)
+    for jA in (-1, 0, 1):
+        for iA in (-1, 0, 1):
+            m, mm = _m(iA, jA), _m(-iA, -jA)
+            for j in range(nhalo, ny - nhalo + 2):
+                for i in range(nhalo, nx - nhalo + 2):
+                    if not active_vertex[j - 1, i - 1]:
+                        continue
+                    inb = 1 <= i + iA <= NX and 1 <= j + jA <= NY
+                    n = (j + jA - 1, i + iA - 1)
+                    if umask[j - 1, i - 1] == 1:
+                        val = float(uvel[j - 1, i - 1])
+                        b[0][j - 1, i - 1] = val
+                        if inb:
+                            if iA == 0 and jA == 0:
+                                A[0][c0, j - 1, i - 1] = 1.0
+                                A[1][c0, j - 1, i - 1] = 1.0
+                                A[2][c0, j - 1, i - 1] = 1.0
+                            else:
+                                A[0][m, j - 1, i - 1] = 0.0
+                                A[1][m, j - 1, i - 1] = 0.0
+                                if umask[n] != 1:
+                                    b[0][n] = float(b[0][n]) - float(A[0][(mm,) + n]) * val
+                                    A[0][(mm,) + n] = 0.0
+                                if vmask[n] != 1:
+                                    b[1][n] = float(b[1][n]) - float(A[2][(mm,) + n]) * val
+                                    A[2][(mm,) + n] = 0.0
+                    if vmask[j - 1, i - 1] == 1:
+                        val = float(vvel[j - 1, i - 1])
+                        b[1][j - 1, i - 1] = val
+                        if inb:
+                            if iA == 0 and jA == 0:
+                                A[1][c0, j - 1, i - 1] = 0.0
+                                A[2][c0, j - 1, i - 1] = 0.0
+                                A[3][c0, j - 1, i - 1] = 1.0
+                            else:
+                                A[2][m, j - 1, i - 1] = 0.0
+                                A[3][m, j - 1, i - 1] = 0.0
+                                if umask[n] != 1:
+                                    b[0][n] = float(b[0][n]) - float(A[1][(mm,) + n]) * val
+                                    A[1][(mm,) + n] = 0.0
+                                if vmask[n] != 1:
+                                    b[1][n] = float(b[1][n]) - float(A[3][(mm,) + n]) * val
+                                    A[3][(mm,) + n] = 0.0
+    return (*A, *b)
+
+
+@pytest.mark.parametrize("seed", [71, 72])
+def test_second_restatement_dirichlet_2d(seed):
+    """dirichlet_boundary_conditions_2d with u-only, v-only and u+v prescribed vertices and nonzero
+    values: every coefficient and b bit-identical with the oracle."""
+    P = problems.slab_2d(seed=seed, boundary_ice=True)
+    rng = np.random.default_rng(seed)
+    shape = P.bu.shape
+    um = (rng.random(shape) < 0.2).astype(np.int32)
+    vm = (rng.random(shape) < 0.2).astype(np.int32)
+    uv, vv = rng.standard_normal(shape) * 10.0, rng.standard_normal(shape) * 10.0
+    args = (P.nx, P.ny, P.active_vertex, um, vm, uv, vv, P.Auu, P.Auv, P.Avu, P.Avv, P.bu, P.bv)
+    want = oracle.dirichlet_2d(*args)
+    got = dirichlet_2d(*args)
+    for g_, w in zip(got, want):
+        np.testing.assert_array_equal(g_, w)
