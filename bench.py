@@ -556,6 +556,10 @@ def run_serve(args):
                                      "latency_ms": {"p50": float(np.percentile(latmx, 50)),
                                                     "p99": float(np.percentile(latmx, 99))}},
         "speedup_vs_fp64_plain": value / fp64_rate,
+        "pool_service_ms": [{"system": P.name, "kind": P.kind, "nz": int(P.nz) if P.kind == "3d" else 1,
+                             "precond": pc, "fp64_ms": round(1e3 * a, 2), "mixed_ms": round(1e3 * b, 2),
+                             "requests": int(np.count_nonzero(which == w))}
+                            for w, (P, pc, a, b) in enumerate(zip(probs, pcs, svc64, svcmx))],
         "server": {"epochs": st["epochs"]},
         "clocks": clk,
     }
