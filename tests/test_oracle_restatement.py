@@ -1304,3 +1304,152 @@ def test_second_restatement_dirichlet_2d(seed):
     got = dirichlet_2d(*args)
     for g_, w in zip(got, want):
         np.testing.assert_array_equal(g_, w)
+
+
+def _stagger(var):
+    """glissade_stagger with stagger_margin 0 (glissade_grid_operators.F90:69-157): each vertex the
+    mean of its four cells, summed (i,j+1), (i+1,j+1), (i,j), (i+1,j)."""
+    ny, nx = var.shape
+    s = np.zeros((ny - 1, nx - 1))
+    for j in range(1, ny):
+        for i in range(1, nx):
+            s[j - 1, i - 1] = (((float(var[j, i - 1]) + float(var[j, i])) + float(var[j - 1, i - 1])) +
+                               float(var[j - 1, i])) / 4.0
+    return s
+
+
+def _slope_gradients(field, dx, dy):
+    """glissade_slope_angle's gradient on an (nx, ny) field (glissade_grid_operators.F90:1264-1410):
+    glissade_gradient with gradient_margin 1 and the default all-ones mask (:309-468; every edge it
+    reads is in the mask, so each component is the mean of its two edge differences), then
+    glissade_unstagger with stagger_margin 0 (:226-305) back to the field's points, zero on the
+    outer ring.  Returns (dz_dx, dz_dy), both field-shaped."""
+    ny, nx = field.shape
+    gx = np.zeros((ny - 1, nx - 1))
+    gy = np.zeros((ny - 1, nx - 1))
+    f = lambda i, j: float(field[j - 1, i - 1])
+    for j in range(1, ny):
+        for i in range(1, nx):
+            north = (f(i + 1, j + 1) - f(i, j + 1)) / dx
+            south = (f(i + 1, j) - f(i, j)) / dx
+            gx[j - 1, i - 1] = (north + south) / 2.0
+            east = (f(i + 1, j + 1) - f(i + 1, j)) / dy
+            west = (f(i, j + 1) - f(i, j)) / dy
+            gy[j - 1, i - 1] = (east + west) / 2.0
+    out = []
+    for g in (gx, gy):
+        u = np.zeros((ny, nx))
+        for j in range(2, ny):
+            for i in range(2, nx):
+                u[j - 1, i - 1] = (((float(g[j - 1, i - 1]) + float(g[j - 1, i - 2])) + float(g[j - 2, i - 1])) +
+                                   float(g[j - 2, i - 2])) / 4.0
+        out.append(u)
+    return out[0], out[1]
+
+
+def basal_local_3d(nx, ny, nz, dx, dy, active_vertex, beta, lsrf, Auu, Avv):
+    """basal_sliding_bc_3d with HO_ASSEMBLE_BETA_LOCAL (glissade_velo_higher.F90:8921-8951): theta =
+    atan(sqrt(dz_dx**2 + dz_dy**2)) of the staggered lower surface (glissade_slope_angle called on the
+    (nx-1, ny-1) grid), then at active vertices the bed diagonal of Auu and Avv += dx*dy/vol0 *
+    beta / cos(theta).  Returns (Auu, Avv, theta)."""
+    vol0 = 1.0e9
+    A = [np.array(Auu, dtype=np.float64, copy=True), np.array(Avv, dtype=np.float64, copy=True)]
+    ddx, ddy = _slope_gradients(_stagger(lsrf), dx, dy)
+    theta = np.zeros((ny - 1, nx - 1))
+    for j in range(ny - 1):
+        for i in range(nx - 1):
+            slope = math.sqrt(float(ddx[j, i]) ** 2 + float(ddy[j, i]) ** 2)
+            theta[j, i] = math.atan(slope) if slope >= 0.0 else 0.0
+    c = _m3(0, 0, 0)
+    for j in range(ny - 1):
+        for i in range(nx - 1):
+            if active_vertex[j, i]:
+                for a in A:
+                    a[j, i, nz - 1, c] = float(a[j, i, nz - 1, c]) + dx * dy / vol0 * float(beta[j, i]) / \
+                        math.cos(float(theta[j, i]))
+    return A[0], A[1], theta
+
+
+def basal_local_2d_diva(nx, ny, dx, dy, active_vertex, beta_eff_x, beta_eff_y, lsrf, Auu, Avv):
+    """basal_sliding_bc_2d_diva with HO_ASSEMBLE_BETA_LOCAL (glissade_velo_higher.F90:8641-8680): the
+    directional slope angles theta_x = atan(|dz_dx|), theta_y = atan(|dz_dy|) of the staggered lower
+    surface, then at active vertices Auu(0,0) += (dx*dy/vol0)*beta_eff_x/cos(theta_x) and
+    Avv(0,0) += (dx*dy/vol0)*beta_eff_y/cos(theta_y).  Blocks (9, ny-1, nx-1)."""
+    vol0 = 1.0e9
+    A = [np.array(Auu, dtype=np.float64, copy=True), np.array(Avv, dtype=np.float64, copy=True)]
+    ddx, ddy = _slope_gradients(_stagger(lsrf), dx, dy)
+    c = _m(0, 0)
+    for j in range(ny - 1):
+        for i in range(nx - 1):
+            if not active_vertex[j, i]:
+                continue
+            tx = math.atan(abs(float(ddx[j, i])))
+            ty = math.atan(abs(float(ddy[j, i])))
+            A[0][c, j, i] = float(A[0][c, j, i]) + (dx * dy / vol0) * float(beta_eff_x[j, i]) / math.cos(tx)
+            A[1][c, j, i] = float(A[1][c, j, i]) + (dx * dy / vol0) * float(beta_eff_y[j, i]) / math.cos(ty)
+    return A[0], A[1]
+
+
+def basal_local_2d(nx, ny, dx, dy, active_vertex, beta, Auu, Avv):
+    """basal_sliding_bc_2d with HO_ASSEMBLE_BETA_LOCAL (glissade_velo_higher.F90:8373-8391): at
+    active vertices the diagonal of Auu and Avv += (dx*dy/vol0) * beta, no slope correction."""
+    vol0 = 1.0e9
+    A = [np.array(Auu, dtype=np.float64, copy=True), np.array(Avv, dtype=np.float64, copy=True)]
+    c = _m(0, 0)
+    for j in range(ny - 1):
+        for i in range(nx - 1):
+            if active_vertex[j, i]:
+                inc = (dx * dy / vol0) * float(beta[j, i])
+                for a in A:
+                    a[c, j, i] = float(a[c, j, i]) + inc
+    return A[0], A[1]
+
+
+def _basal_local_inputs(seed, nx, ny):
+    rng = np.random.default_rng(seed)
+    # a rough lower surface: a tilted plane, a bump and noise, so every slope angle differs
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    lsrf = 300.0 - 40.0 * ii + 15.0 * jj + 200.0 * np.sin(0.7 * ii) * np.cos(0.5 * jj) + 30.0 * rng.random((ny, nx))
+    av = rng.random((ny - 1, nx - 1)) < 0.8
+    beta = np.exp(np.log(1.0e3) + rng.standard_normal((ny - 1, nx - 1)))
+    return lsrf, av, beta
+
+
+@pytest.mark.parametrize("seed", [81, 82])
+def test_second_restatement_basal_local_3d(seed):
+    """The local basal friction term (CISM's default assembly of beta): the slope angle and the bed
+    diagonals bit-identical with the oracle, on a grid with unequal dx and dy."""
+    from tests.test_oracle_assembly import geometry
+    g = geometry(seed=seed)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    lsrf, av, beta = _basal_local_inputs(seed, nx, ny)
+    P = problems.slab_3d(seed=seed, ewn=nx - 4, nsn=ny - 4, nz=nz, sliding=False)
+    dx, dy = 1000.0, 1350.0
+    ou, ov, ot = oracle.basal_local_3d(nx, ny, nz, dx, dy, av, beta, lsrf, P.Auu, P.Avv)
+    gu, gv, gt = basal_local_3d(nx, ny, nz, dx, dy, av, beta, lsrf, P.Auu, P.Avv)
+    assert np.count_nonzero(gt) > (nx - 3) * (ny - 3) // 2 and not np.array_equal(gu, P.Auu)
+    np.testing.assert_array_equal(gt, ot)
+    np.testing.assert_array_equal(gu, ou)
+    np.testing.assert_array_equal(gv, ov)
+
+
+@pytest.mark.parametrize("seed", [83, 84])
+def test_second_restatement_basal_local_2d(seed):
+    """The local basal terms of the 2D systems: SSA/L1L2 (beta alone) and DIVA (beta_eff_x and
+    beta_eff_y over the directional slope angles), bit-identical with the oracle."""
+    P = problems.slab_2d(seed=seed, boundary_ice=True)
+    nx, ny = P.nx, P.ny
+    lsrf, av, beta = _basal_local_inputs(seed, nx, ny)
+    bey = beta * np.exp(0.3 * np.random.default_rng(seed + 1).standard_normal(beta.shape))
+    dx, dy = 2000.0, 1500.0
+    ou, ov = oracle.basal_local_2d(nx, ny, dx, dy, av, beta, P.Auu, P.Avv)
+    gu, gv = basal_local_2d(nx, ny, dx, dy, av, beta, P.Auu, P.Avv)
+    assert not np.array_equal(gu, P.Auu)
+    np.testing.assert_array_equal(gu, ou)
+    np.testing.assert_array_equal(gv, ov)
+    zc = np.zeros((ny, nx), dtype=np.int32)
+    zv = np.zeros((ny - 1, nx - 1))
+    ou, ov = oracle.basal_diva(nx, ny, dx, dy, zc, av, beta, bey, lsrf, zv, zv, 1, P.Auu, P.Avv)
+    gu, gv = basal_local_2d_diva(nx, ny, dx, dy, av, beta, bey, lsrf, P.Auu, P.Avv)
+    np.testing.assert_array_equal(gu, ou)
+    np.testing.assert_array_equal(gv, ov)
