@@ -1453,3 +1453,247 @@ def test_second_restatement_basal_local_2d(seed):
     gu, gv = basal_local_2d_diva(nx, ny, dx, dy, av, beta, bey, lsrf, P.Auu, P.Avv)
     np.testing.assert_array_equal(gu, ou)
     np.testing.assert_array_equal(gv, ov)
+
+
+# ---------------------------------------------------------------------------------------------
+# assemble_stiffness_matrix_2d, L1L2 and DIVA (glissade_velo_higher.F90:4961-5378)
+# ---------------------------------------------------------------------------------------------
+_RHOI, _GRAV = 910.0, 9.81  # glimmer_physcon.F90:67, :69
+
+
+def _efvs_l1l2(whichefvs, efvs_constant, effstrain_min, n_glen, nz, sigma, phi, dx, dy, u, v, h, dsdx, dsdy, flwa,
+               flwafact):
+    """compute_effective_viscosity_L1L2 (:7474-7726) at one quadrature point: the layer viscosities
+    from the cubic for tau_parallel, with tau_perp from the surface slope and the depth."""
+    p_eff = (1.0 - n_glen) / n_glen
+    if whichefvs == 0:
+        return [efvs_constant] * (nz - 1)
+    if whichefvs == 1:
+        eff = 500.0 / 31536000.0 / 200.0e3 * 31536000.0
+        return [float(flwafact[k]) * eff ** p_eff for k in range(nz - 1)]
+    dudx = dudy = dvdx = dvdy = dsx = dsy = thck = 0.0
+    for n in range(4):
+        dudx = dudx + dx[n] * u[n]
+        dudy = dudy + dy[n] * u[n]
+        dvdx = dvdx + dx[n] * v[n]
+        dvdy = dvdy + dy[n] * v[n]
+        dsx = dsx + phi[n] * dsdx[n]
+        dsy = dsy + phi[n] * dsdy[n]
+        thck = thck + phi[n] * h[n]
+    sh = dvdx + dudy
+    esq = (((effstrain_min * effstrain_min + dudx * dudx) + dvdy * dvdy) + dudx * dvdy) + 0.25 * (sh * sh)
+    eff = math.sqrt(esq)
+    out = []
+    for k in range(nz - 1):
+        depth = thck * float(sigma[k + 1])
+        grads = math.sqrt(dsx * dsx + dsy * dsy)
+        tperp = ((_RHOI * _GRAV) * depth) * grads
+        a = tperp * tperp
+        b = -eff / float(flwa[k])
+        c = math.sqrt((b * b) / 4.0 + ((a * a) * a) / 27.0)
+        root_a = math.pow(-b / 2.0 + c, 1.0 / 3.0)
+        if ((a * a) * a) / 27.0 > 1.0e-6 * ((b * b) / 4.0):
+            root_b = -math.pow(b / 2.0 + c, 1.0 / 3.0)
+        else:
+            root_b = -a / (3.0 * math.pow(abs(b), 1.0 / 3.0))
+        tpar = root_a + root_b
+        if abs(n_glen - 1.0) < 1.0e-10:
+            out.append(1.0 / (2.0 * float(flwa[k])))
+        elif abs(n_glen - 3.0) < 1.0e-10:
+            out.append(1.0 / ((2.0 * float(flwa[k])) * (tpar * tpar + tperp * tperp)))
+        else:
+            raise ValueError("Invalid value of n_glen for L1L2 solver")
+    return out
+
+
+def _efvs_diva(whichefvs, efvs_constant, effstrain_min, n_glen, nz, stagsigma, phi, dx, dy, u, v, bx, by, sfx, sfy,
+               flwafact, old):
+    """compute_effective_viscosity_diva (:7730-7997), the iterative form (cubic = .false.): the
+    vertical shear of each layer from the basal traction over the layer's previous viscosity."""
+    p_eff = (1.0 - n_glen) / n_glen
+    if whichefvs == 0:
+        return [efvs_constant] * (nz - 1)
+    if whichefvs == 1:
+        eff = 500.0 / 31536000.0 / 200.0e3 * 31536000.0
+        return [float(flwafact[k]) * eff ** p_eff for k in range(nz - 1)]
+    dudx = dudy = dvdx = dvdy = taux = tauy = 0.0
+    for n in range(4):
+        dudx = dudx + dx[n] * u[n]
+        dudy = dudy + dy[n] * u[n]
+        dvdx = dvdx + dx[n] * v[n]
+        dvdy = dvdy + dy[n] * v[n]
+        taux = taux + phi[n] * bx[n]
+        tauy = tauy + phi[n] * by[n]
+    out = list(old)
+    for k in range(nz - 1):
+        if out[k] == 0.0:
+            out[k] = float(flwafact[k]) * effstrain_min ** p_eff
+        dudz = taux * float(stagsigma[k]) / (out[k] * sfx)
+        dvdz = tauy * float(stagsigma[k]) / (out[k] * sfy)
+        sh = dvdx + dudy
+        esq = (((((effstrain_min * effstrain_min + dudx * dudx) + dvdy * dvdy) + dudx * dvdy) + 0.25 * (sh * sh)) +
+               (0.25 * (dudz * dudz)) * sfx) + (0.25 * (dvdz * dvdz)) * sfy
+        out[k] = float(flwafact[k]) * esq ** (p_eff / 2.0)
+    return out
+
+
+def _integrals_diva(nz, sigma, thck, eqp):
+    """compute_integrals_diva (:5649-5775): omega_k at each level, the mean over the points of the
+    integral of depth/efvs from the level to the surface, and omega, its layer-midpoint integral."""
+    okp = [[0.0] * nz for _ in range(4)]
+    for p in range(4):
+        for k in range(nz - 2, -1, -1):
+            depth = 0.5 * (float(sigma[k]) + float(sigma[k + 1]))
+            dz = (float(sigma[k + 1]) - float(sigma[k])) * thck
+            okp[p][k] = okp[p][k + 1] + depth / eqp[p][k] * dz
+    ok = []
+    for k in range(nz):
+        acc = 0.0
+        for p in range(4):
+            acc = acc + okp[p][k]
+        ok.append(acc / 4)
+    om = 0.0
+    for k in range(nz - 1):
+        om = om + 0.5 * (ok[k] + ok[k + 1]) * (float(sigma[k + 1]) - float(sigma[k]))
+    return ok, om
+
+
+def assemble_layered_2d(approx, nx, ny, nz, sigma, active_cell, xv, yv, uvel, vvel, stagthck, flwafact, whichefvs,
+                        efvs_constant, effstrain_min, n_glen, l1l2=None, diva=None, nhalo=2):
+    """The L1L2 and DIVA branches: per active cell and quadrature point the basis derivatives, the
+    layer viscosities, their sigma-weighted average times the thickness at the point into the
+    element matrix of the Blatter-Pattyn form with zero vertical derivatives (compute_element_matrix
+    :8001-8123), the cell's viscosity (the mean over the points), for DIVA the integrals, and
+    element_to_global_matrix_2d.  l1l2 = (dusrf_dx, dusrf_dy, flwa); diva = (stagsigma, thck,
+    btractx, btracty, dsfx, dsfy, efvs_qp_3d)."""
+    vol0 = 1.0e9
+    A = [np.zeros((9, ny - 1, nx - 1)) for _ in range(4)]
+    efvs_out = np.zeros((ny, nx, nz - 1))
+    if diva is not None:
+        stagsigma, thck, btx, bty, dsfx, dsfy, eq_in = diva
+        eq3 = np.array(eq_in, dtype=np.float64, copy=True)
+        omega_k = np.zeros((ny, nx, nz))
+        omega = np.zeros((ny, nx))
+    for j in range(nhalo + 1, ny - nhalo + 2):
+        for i in range(nhalo + 1, nx - nhalo + 2):
+            if not active_cell[j - 1, i - 1]:
+                continue
+            verts = [(i + _ISHIFT[2][n], j + _JSHIFT[2][n]) for n in range(4)]
+            pick = lambda f: [float(f[jv - 1, iv - 1]) for iv, jv in verts]
+            x, y, u, v, h = pick(xv), pick(yv), pick(uvel), pick(vvel), pick(stagthck)
+            if l1l2 is not None:
+                dsdx, dsdy = pick(l1l2[0]), pick(l1l2[1])
+            else:
+                bx, by = pick(btx), pick(bty)
+            K = [[[0.0] * 4 for _ in range(4)] for _ in range(4)]
+            eqp = [None] * 4
+            for p in range(4):
+                phi, dxr, dyr = _ref_square(p)
+                j11 = j12 = j21 = j22 = 0.0
+                for n in range(4):
+                    j11 = j11 + dxr[n] * x[n]
+                    j12 = j12 + dxr[n] * y[n]
+                    j21 = j21 + dyr[n] * x[n]
+                    j22 = j22 + dyr[n] * y[n]
+                det = j11 * j22 - j12 * j21
+                if not abs(det) > 0.0:
+                    raise ZeroDivisionError("Jacobian matrix is singular")
+                i11, i12, i21, i22 = j22 / det, -j12 / det, -j21 / det, j11 / det
+                ddx = [(0.0 + i11 * dxr[n]) + i12 * dyr[n] for n in range(4)]
+                ddy = [(0.0 + i21 * dxr[n]) + i22 * dyr[n] for n in range(4)]
+                if approx == "l1l2":
+                    eqp[p] = _efvs_l1l2(whichefvs, efvs_constant, effstrain_min, n_glen, nz, sigma, phi, ddx, ddy, u,
+                                        v, h, dsdx, dsdy, l1l2[2][j - 1, i - 1], flwafact[j - 1, i - 1])
+                else:
+                    old = [float(eq3[j - 1, i - 1, p, k]) for k in range(nz - 1)]
+                    eqp[p] = _efvs_diva(whichefvs, efvs_constant, effstrain_min, n_glen, nz, stagsigma, phi, ddx, ddy,
+                                        u, v, bx, by, float(dsfx[j - 1, i - 1]), float(dsfy[j - 1, i - 1]),
+                                        flwafact[j - 1, i - 1], old)
+                    eq3[j - 1, i - 1, p, :] = eqp[p]
+                avg = 0.0
+                for k in range(nz - 1):
+                    avg = avg + eqp[p][k] * (float(sigma[k + 1]) - float(sigma[k]))
+                hq = 0.0
+                for n in range(4):
+                    hq = hq + phi[n] * h[n]
+                fac = (hq * avg) * 1.0 * det / vol0
+                for nc in range(4):
+                    for nr in range(4):
+                        zz = 0.0 * 0.0
+                        K[0][nr][nc] = K[0][nr][nc] + fac * ((4.0 * ddx[nr] * ddx[nc] + ddy[nr] * ddy[nc]) + zz)
+                        K[1][nr][nc] = K[1][nr][nc] + fac * (2.0 * ddx[nr] * ddy[nc] + ddy[nr] * ddx[nc])
+                        K[2][nr][nc] = K[2][nr][nc] + fac * (2.0 * ddy[nr] * ddx[nc] + ddx[nr] * ddy[nc])
+                        K[3][nr][nc] = K[3][nr][nc] + fac * ((4.0 * ddy[nr] * ddy[nc] + ddx[nr] * ddx[nc]) + zz)
+            if diva is not None:
+                ok, om = _integrals_diva(nz, sigma, float(thck[j - 1, i - 1]), eqp)
+                omega_k[j - 1, i - 1, :] = ok
+                omega[j - 1, i - 1] = om
+            for k in range(nz - 1):
+                acc = 0.0
+                for p in range(4):
+                    acc = acc + eqp[p][k]
+                efvs_out[j - 1, i - 1, k] = acc / 4
+            for nr in range(4):
+                iv, jv = i + _ISHIFT[2][nr], j + _JSHIFT[2][nr]
+                for nc in range(4):
+                    m = _m(_ISHIFT[nr][nc], _JSHIFT[nr][nc])
+                    for b in range(4):
+                        A[b][m, jv - 1, iv - 1] = float(A[b][m, jv - 1, iv - 1]) + K[b][nr][nc]
+    if diva is not None:
+        return efvs_out, eq3, omega_k, omega, A
+    return efvs_out, A
+
+
+@pytest.mark.parametrize("whichefvs", [0, 1, 2])
+@pytest.mark.parametrize("seed,n_glen", [(41, 3.0), (42, 3.0), (43, 1.0)])
+def test_second_restatement_l1l2_assembly(whichefvs, seed, n_glen):
+    """assemble_stiffness_matrix_2d (L1L2): the layer viscosities of the tau_parallel cubic on a
+    sloping surface and every coefficient, bit-identical with the oracle."""
+    g, u, v, _ = _ssa_inputs(seed, True)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(seed + 7)
+    dsdx = 0.02 * rng.standard_normal((ny - 1, nx - 1))
+    dsdy = 0.02 * rng.standard_normal((ny - 1, nx - 1))
+    dsdx[4:6, :] = 0.0  # the cells between two flat vertex rows take the cubic's first-order branch
+    dsdy[4:6, :] = 0.0
+    flwa = 1.0e-16 * (1.0 + rng.random((ny, nx, nz - 1)))
+    ff = 0.5 * flwa ** (-1.0 / 3.0)
+    st, oefvs, *oA = oracle.assemble_stiffness_2d_l1l2(nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], u,
+                                                       v, g["stagthck"], dsdx, dsdy, flwa, ff, whichefvs=whichefvs,
+                                                       efvs_constant=2.5e6, effstrain_min=1.0e-8, n_glen=n_glen)
+    assert st == 0
+    efvs, A = assemble_layered_2d("l1l2", nx, ny, nz, g["sigma"], g["ac"], g["xVertex"], g["yVertex"], u, v,
+                                  g["stagthck"], ff, whichefvs, 2.5e6, 1.0e-8, n_glen, l1l2=(dsdx, dsdy, flwa))
+    assert np.count_nonzero(efvs) > 0
+    np.testing.assert_array_equal(efvs, oefvs)
+    for got, want in zip(A, oA):
+        np.testing.assert_array_equal(got, want)
+
+
+@pytest.mark.parametrize("whichefvs", [0, 1, 2])
+@pytest.mark.parametrize("seed,traction,first", [(44, 5.0e4, False), (45, 2.0e4, True), (46, 0.0, False)])
+def test_second_restatement_diva_assembly(whichefvs, seed, traction, first):
+    """assemble_stiffness_matrix_2d (DIVA): the point viscosities updated from the stored ones (or
+    from the minimum strain rate on a first call, stored zeros), omega_k, omega, the cell
+    viscosities and every coefficient, bit-identical with the oracle."""
+    g, u, v, ff = _ssa_inputs(seed, True)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(seed + 9)
+    sig = g["sigma"]
+    stagsig = 0.5 * (sig[:-1] + sig[1:])
+    bx = traction * (1.0 + rng.random((ny - 1, nx - 1)))
+    by = -0.5 * traction * (1.0 + rng.random((ny - 1, nx - 1)))
+    dsfx = 1.0 + 0.1 * rng.random((ny, nx))
+    dsfy = 1.0 + 0.1 * rng.random((ny, nx))
+    eq0 = np.zeros((ny, nx, 4, nz - 1)) if first else 2.0e6 * (1.0 + 0.3 * rng.random((ny, nx, 4, nz - 1)))
+    o = oracle.assemble_stiffness_2d_diva(nx, ny, nz, sig, stagsig, g["ac"], g["xVertex"], g["yVertex"], u, v,
+                                          g["stagthck"], g["thck"], bx, by, dsfx, dsfy, ff, eq0, whichefvs=whichefvs,
+                                          efvs_constant=2.5e6, effstrain_min=1.0e-8, n_glen=3.0)
+    assert o[0] == 0
+    got = assemble_layered_2d("diva", nx, ny, nz, sig, g["ac"], g["xVertex"], g["yVertex"], u, v, g["stagthck"], ff,
+                              whichefvs, 2.5e6, 1.0e-8, 3.0,
+                              diva=(stagsig, g["thck"], bx, by, dsfx, dsfy, eq0))
+    efvs, eq, ok, om, A = got
+    assert np.count_nonzero(om) > 0
+    for g_, w in zip((efvs, eq, ok, om, *A), o[1:]):
+        np.testing.assert_array_equal(g_, w)
