@@ -1697,3 +1697,95 @@ def test_second_restatement_diva_assembly(whichefvs, seed, traction, first):
     assert np.count_nonzero(om) > 0
     for g_, w in zip((efvs, eq, ok, om, *A), o[1:]):
         np.testing.assert_array_equal(g_, w)
+
+
+def basal_standard_2d(nx, ny, active_cell, xv, yv, beta_x, beta_y, Auu, Avv, lsrf=None, nhalo=2):
+    """The standard finite-element basal terms of the 2D systems, on copies of the (9, ny-1, nx-1)
+    blocks.  lsrf None: basal_sliding_bc_2d (glissade_velo_higher.F90:8393-8531), one beta, the
+    flat Jacobian determinant of get_basis_function_derivatives_2d (:6319-6504) and Kvv = Kuu.
+    lsrf given: basal_sliding_bc_2d_diva (:8682-8811), beta_eff_x into Auu and beta_eff_y into Avv
+    with the area factor of the staggered lower surface (get_area_scale_factor_curved_2d
+    :6736-6827)."""
+    vol0 = 1.0e9
+    A = [np.array(Auu, dtype=np.float64, copy=True), np.array(Avv, dtype=np.float64, copy=True)]
+    sl = None if lsrf is None else _stagger(lsrf)
+    for j in range(nhalo + 1, ny - nhalo + 2):
+        for i in range(nhalo + 1, nx - nhalo + 2):
+            if not active_cell[j - 1, i - 1]:
+                continue
+            verts = ((i - 1, j - 1), (i, j - 1), (i, j), (i - 1, j))
+            pick = lambda f: [float(f[jv - 1, iv - 1]) for iv, jv in verts]
+            x, y, bx, by = pick(xv), pick(yv), pick(beta_x), pick(beta_y)
+            for p in range(4):
+                phi, dxr, dyr = _ref_square(p)
+                if sl is None:
+                    j11 = j12 = j21 = j22 = 0.0
+                    for n in range(4):
+                        j11 = j11 + dxr[n] * x[n]
+                        j12 = j12 + dxr[n] * y[n]
+                        j21 = j21 + dyr[n] * x[n]
+                        j22 = j22 + dyr[n] * y[n]
+                    det = j11 * j22 - j12 * j21
+                    if not abs(det) > 0.0:
+                        raise ZeroDivisionError("Jacobian matrix is singular")
+                else:
+                    z = pick(sl)
+                    j11 = j12 = j13 = j21 = j22 = j23 = 0.0
+                    for n in range(4):
+                        j11 = j11 + dxr[n] * x[n]
+                        j12 = j12 + dxr[n] * y[n]
+                        j13 = j13 + dxr[n] * z[n]
+                        j21 = j21 + dyr[n] * x[n]
+                        j22 = j22 + dyr[n] * y[n]
+                        j23 = j23 + dyr[n] * z[n]
+                    t1 = j11 * j22 - j12 * j21
+                    t2 = -(j11 * j23 - j13 * j21)
+                    t3 = j12 * j23 - j13 * j22
+                    det = math.sqrt((t1 * t1 + t2 * t2) + t3 * t3)
+                bqx = bqy = 0.0
+                for n in range(4):
+                    bqx = bqx + phi[n] * bx[n]
+                    bqy = bqy + phi[n] * by[n]
+                Ku = [[0.0] * 4 for _ in range(4)]
+                Kv = [[0.0] * 4 for _ in range(4)]
+                for nc in range(4):
+                    for nr in range(4):
+                        Ku[nr][nc] = Ku[nr][nc] + bqx * 1.0 * det / vol0 * phi[nr] * phi[nc]
+                        Kv[nr][nc] = Kv[nr][nc] + bqy * 1.0 * det / vol0 * phi[nr] * phi[nc]
+                if sl is None:
+                    Kv = Ku
+                for nr in range(4):
+                    iv, jv = i + _ISHIFT[2][nr], j + _JSHIFT[2][nr]
+                    for nc in range(4):
+                        m = _m(_ISHIFT[nr][nc], _JSHIFT[nr][nc])
+                        A[0][m, jv - 1, iv - 1] = float(A[0][m, jv - 1, iv - 1]) + Ku[nr][nc]
+                        A[1][m, jv - 1, iv - 1] = float(A[1][m, jv - 1, iv - 1]) + Kv[nr][nc]
+    return A[0], A[1]
+
+
+@pytest.mark.parametrize("seed", [91, 92])
+def test_second_restatement_basal_standard_2d(seed):
+    """The standard basal terms of the SSA/L1L2 systems (one beta, flat element) and of DIVA
+    (beta_eff_x, beta_eff_y, curved lower surface): every coefficient bit-identical with the oracle."""
+    from tests.test_oracle_assembly import geometry
+    g = geometry(seed=seed)
+    nx, ny = g["nx"], g["ny"]
+    rng = np.random.default_rng(seed)
+    shape = (ny - 1, nx - 1)
+    beta = np.exp(np.log(1.0e3) + rng.standard_normal(shape))
+    bey = beta * np.exp(0.3 * rng.standard_normal(shape))
+    lsrf, _, _ = _basal_local_inputs(seed, nx, ny)
+    Auu = rng.standard_normal((9,) + shape)
+    Avv = rng.standard_normal((9,) + shape)
+    st, ou, ov = oracle.basal_standard(False, nx, ny, 2, g["ac"], g["xVertex"], g["yVertex"], beta, None, Auu, Avv)
+    assert st == 0
+    gu, gv = basal_standard_2d(nx, ny, g["ac"], g["xVertex"], g["yVertex"], beta, beta, Auu, Avv)
+    assert not np.array_equal(gu, Auu)
+    np.testing.assert_array_equal(gu, ou)
+    np.testing.assert_array_equal(gv, ov)
+    av = np.ones(shape, dtype=np.int32)
+    ou, ov = oracle.basal_diva(nx, ny, 1.0, 1.0, g["ac"], av, beta, bey, lsrf, g["xVertex"], g["yVertex"], 0, Auu,
+                               Avv)
+    gu, gv = basal_standard_2d(nx, ny, g["ac"], g["xVertex"], g["yVertex"], beta, bey, Auu, Avv, lsrf=lsrf)
+    np.testing.assert_array_equal(gu, ou)
+    np.testing.assert_array_equal(gv, ov)
