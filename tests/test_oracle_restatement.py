@@ -1789,3 +1789,181 @@ def test_second_restatement_basal_standard_2d(seed):
     gu, gv = basal_standard_2d(nx, ny, g["ac"], g["xVertex"], g["yVertex"], beta, bey, Auu, Avv, lsrf=lsrf)
     np.testing.assert_array_equal(gu, ou)
     np.testing.assert_array_equal(gv, ov)
+
+
+# ---------------------------------------------------------------------------------------------
+# The reproducible sum: cism_reprosum_calc / cism_reprosum_int (libglimmer/cism_reprosum_mod.F90)
+# as parallel_reduce_reprosum calls it (parallel_mpi.F90:9637-9730): one field, no bounds given
+# (the recompute path), validation off for the recompute, one task and one thread.
+# ---------------------------------------------------------------------------------------------
+_I8_DIGITS, _R8_DIGITS, _R8_MINEXP, _R8_MAXEXP = 63, 53, -1021, 1024
+
+
+def _exponent(x):
+    """Fortran exponent(): x = fraction * 2**exponent with |fraction| in [0.5, 1); 0 for 0."""
+    return 0 if x == 0.0 else math.frexp(x)[1]
+
+
+def _set_exponent(x, e):
+    return math.ldexp(math.frexp(x)[0], e)
+
+
+def _idiv(a, b):
+    """Fortran integer division of a by b > 0: the quotient truncated toward zero."""
+    q = abs(a) // b
+    return q if a >= 0 else -q
+
+
+def _isign(x):
+    """sign(1_i8, x): +1 for x >= 0."""
+    return -1 if x < 0 else 1
+
+
+def reprosum(arr):
+    arr = [float(v) for v in np.ravel(arr)]
+    n = len(arr)
+    # exponent extremes (cism_reprosum_mod.F90:820-867; one task, so the global ones are the same)
+    tlmin, tlmax = _R8_MAXEXP, _R8_MINEXP
+    for v in arr:
+        if v != 0.0:
+            e = _exponent(v)
+            tlmin, tlmax = min(e, tlmin), max(e, tlmax)
+    gmax = tlmax
+    gmin = min(gmax, tlmin)
+    max_nsummands = max(n // 1 + 1, 1 * 1)
+    ams = _I8_DIGITS - (_exponent(float(max_nsummands)) + 1)  # arr_max_shift
+    assert ams >= 2, "number of summands too large for integer vector algorithm"
+    max_levels = 2 + (_R8_DIGITS + (gmax - gmin)) // ams
+    extra_levels = (_I8_DIGITS - 1) // ams
+    min_level = -(extra_levels - 1)
+    radix_s = 2 ** ams
+    lev = {il: 0 for il in range(min_level, max_levels + 1)}
+    # the integer expansion of every summand (cism_reprosum_int, :1256-1370)
+    for v in arr:
+        if v == 0.0:
+            continue
+        e, frac = _exponent(v), math.frexp(v)[0]
+        shift = ams - (gmax - e)
+        if shift < 1:
+            il = (1 + (gmax - e)) // ams
+            shift = il * ams - (gmax - e)
+            while shift < 1:
+                shift += ams
+                il += 1
+        else:
+            il = 1
+        if il <= max_levels:
+            rem = math.ldexp(frac, shift)
+            k = int(rem)
+            lev[il] += k
+            rem = rem - k
+            while rem != 0.0 and il < max_levels:
+                il += 1
+                rem = math.ldexp(rem, ams)
+                k = int(rem)
+                lev[il] += k
+                rem = rem - k
+
+    def carry(g):
+        for il in range(max_levels, min_level, -1):
+            if abs(g[il]) >= radix_s:
+                q = _idiv(g[il], radix_s)
+                g[il - 1] += q
+                g[il] -= q * radix_s
+
+    carry(lev)       # the thread's own normalisation (:1374-1387)
+    g = dict(lev)    # the global level sums (one task) and their normalisation (:1564-1577)
+    carry(g)
+    il = min_level
+    while g[il] == 0 and il < max_levels:
+        il += 1
+    sgn = -1 if g[il] < 0 else 1
+    if il < max_levels:  # make every level's sign the leading one's (:1596-1645)
+        for jl in range(il, max_levels):
+            if _isign(g[jl]) != _isign(g[jl + 1]) or g[jl + 1] == 0:
+                g[jl] -= sgn
+                g[jl + 1] += sgn * radix_s
+    if sgn < 0:
+        for jl in range(il, max_levels + 1):
+            g[jl] = -g[jl]
+    carry(g)
+    # conversion into pieces of 53 binary digits, added smallest first (:1653-1780)
+    first = True
+    shift = gmax - min_level * ams
+    count = 0
+    begin = min_level
+    pieces = []
+    while begin <= max_levels:
+        tloc, tlev = 0, max_levels
+        for il in range(begin, max_levels + 1):
+            if first:
+                if count == 0:
+                    lx = _exponent(float(g[il])) if g[il] != 0 else 0
+                else:
+                    lx = ams
+            else:
+                lx = 0 if (il == begin and count != 0) else ams
+            if count + lx >= _R8_DIGITS:
+                tlev, tloc = il, (count + lx) - _R8_DIGITS
+                break
+            count += lx
+        first = False
+        if tloc == 0:
+            trem = 0
+        else:
+            q = _idiv(g[tlev], 2 ** tloc) * 2 ** tloc
+            trem = g[tlev] - q
+            g[tlev] = q
+        piece = 0.0
+        for il in range(begin, tlev + 1):
+            if g[il] != 0:
+                x = float(g[il])
+                cur = _exponent(x) + shift
+                if cur >= _R8_MINEXP:
+                    piece = piece + _set_exponent(x, cur)
+                else:
+                    piece = piece + math.ldexp(_set_exponent(x, cur - _R8_MINEXP), _R8_MINEXP)
+            if il < tlev or tloc == 0:
+                shift -= ams
+        pieces.append(piece)
+        if tloc == 0:
+            count, begin = 0, tlev + 1
+        else:
+            count, begin = tloc, tlev
+            g[tlev] = trem
+    total = 0.0
+    for piece in reversed(pieces):
+        total = total + piece
+    return sgn * total
+
+
+def test_second_restatement_reprosum():
+    """The reproducible sum, bit-identical with the oracle's on random arrays (normal values, wide
+    exponent spreads reaching the subnormals, zeros and cancellation), on the near-tie case its
+    conversion double-rounds, independent of the summands' order, and equal to the correctly
+    rounded sum elsewhere."""
+    rng = np.random.default_rng(21)
+    cases = []
+    for t in range(120):
+        n = int(rng.integers(1, 400))
+        if t % 4 == 0:
+            a = rng.standard_normal(n)
+        elif t % 4 == 1:
+            a = rng.standard_normal(n) * np.exp(rng.uniform(-700, 700, n))
+        elif t % 4 == 2:
+            a = np.where(rng.random(n) < 0.5, 0.0, rng.standard_normal(n) * 1e7)
+        else:
+            b = rng.standard_normal(n // 2 + 1) * np.exp(rng.uniform(-40, 40, n // 2 + 1))
+            a = np.concatenate([b, -b[: n // 2] * (1.0 + 2.0**-52)])  # heavy cancellation
+        cases.append(a)
+    cases += [np.array([1.0, 2.0**-53, 2.0**-106, -1e-40]), np.zeros(5), np.array([-3.5]),
+              np.array([5e-324, -1e-320, 2.5e-310]), np.array([1.7e308, -1.6e308, 1e292])]
+    for a in cases:
+        got = reprosum(a)
+        assert got == oracle.reprosum(a), a
+        if a.size == 4 and a[1] == 2.0**-53:
+            assert got == 1.0 and math.fsum(a) == 1.0 + 2.0**-52
+        elif a.size > 5:
+            assert got == math.fsum(a)
+    b = cases[1]
+    assert len({reprosum(rng.permutation(b)) for _ in range(5)}) == 1
