@@ -1967,3 +1967,39 @@ def test_second_restatement_reprosum():
             assert got == math.fsum(a)
     b = cases[1]
     assert len({reprosum(rng.permutation(b)) for _ in range(5)}) == 1
+
+
+def load_vector_local(nx, ny, nz, stagwbndsigma, dx, dy, active_vertex, stagthck, dsx, dsy):
+    """load_vector_gravity, local form (glissade_velo_higher.F90:4311-4342): at every active vertex
+    and level the driving stress over the node's share of the column, -rhoi*grav*dx*dy*dz/vol0 *
+    ds, dz the thickness between the staggered level boundaries."""
+    vol0, rhoi, grav = 1.0e9, 910.0, 9.81
+    lu, lv = np.zeros((ny - 1, nx - 1, nz)), np.zeros((ny - 1, nx - 1, nz))
+    for j in range(ny - 1):
+        for i in range(nx - 1):
+            if not active_vertex[j, i]:
+                continue
+            for k in range(1, nz + 1):
+                dz = float(stagthck[j, i]) * (float(stagwbndsigma[k]) - float(stagwbndsigma[k - 1]))
+                lu[j, i, k - 1] = float(lu[j, i, k - 1]) - rhoi * grav * dx * dy * dz / vol0 * float(dsx[j, i])
+                lv[j, i, k - 1] = float(lv[j, i, k - 1]) - rhoi * grav * dx * dy * dz / vol0 * float(dsy[j, i])
+    return lu, lv
+
+
+def test_second_restatement_load_vector_local():
+    """load_vector_gravity, local form: bit-identical with the oracle, unequal dx and dy."""
+    from tests.test_oracle_assembly import geometry
+    g = geometry(seed=45)
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    rng = np.random.default_rng(10)
+    sx, sy = 0.01 * rng.standard_normal((ny - 1, nx - 1)), 0.01 * rng.standard_normal((ny - 1, nx - 1))
+    sig = g["sigma"]
+    stagw = np.concatenate([[0.0], 0.5 * (sig[:-1] + sig[1:]), [1.0]])
+    dx, dy = 1000.0, 1250.0
+    st, ou, ov = oracle.load_vector_gravity(nx, ny, nz, sig, stagw, dx, dy, g["ac"], g["av"], g["xVertex"],
+                                            g["yVertex"], g["stagusrf"], g["stagthck"], sx, sy, 1)
+    assert st == 0
+    lu, lv = load_vector_local(nx, ny, nz, stagw, dx, dy, g["av"], g["stagthck"], sx, sy)
+    assert np.count_nonzero(lu) > 0
+    np.testing.assert_array_equal(lu, ou)
+    np.testing.assert_array_equal(lv, ov)
