@@ -186,8 +186,8 @@ def _line_rhs_3d(r):
 
 
 def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8, precond=1):
-    """pcg_solver_standard_2d with precond 1 (diagonal) or 3 (local tridiagonal lines, then the
-    halo of z), from x0 = 0; returns (xu, xv, err, niters)."""
+    """pcg_solver_standard_2d with precond 0 (none), 1 (diagonal) or 3/4 (local/global tridiagonal
+    lines, then the halo of z), from x0 = 0; returns (xu, xv, err, niters)."""
     par = P.par
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
     xu, xv = np.zeros_like(bu), np.zeros_like(bv)
@@ -207,6 +207,8 @@ def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8, precond=1):
             zu, zv = _tri_solve_2d(P, T, ru, rv, glob=precond == 4)
             _halo(zu, par)
             _halo(zv, par)
+        elif precond == 0:
+            zu, zv = ru.copy(), rv.copy()
         else:
             zu = np.divide(ru, adu, out=np.zeros_like(ru), where=adu != 0.0)
             zv = np.divide(rv, adv, out=np.zeros_like(rv), where=adv != 0.0)
@@ -627,7 +629,7 @@ def test_second_restatement_standard_3d(name, make, precond, maxiters):
 
 
 @pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
-@pytest.mark.parametrize("precond", [3, 4])
+@pytest.mark.parametrize("precond", [0, 3, 4])
 @pytest.mark.parametrize("maxiters", [3, 12, 400])
 def test_second_restatement_standard_2d_lines(name, make, precond, maxiters):
     """pcg_solver_standard_2d with the tridiagonal line preconditioners (3 local, 4 global)."""
