@@ -185,12 +185,17 @@ def _line_rhs_3d(r):
     return acc
 
 
-def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8, precond=1):
-    """pcg_solver_standard_2d with precond 0 (none), 1 (diagonal) or 3/4 (local/global tridiagonal
-    lines, then the halo of z), from x0 = 0; returns (xu, xv, err, niters)."""
+def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8, precond=1, x0=None):
+    """pcg_solver_standard_2d with precond 0 (none), 1 (diagonal), 3/4 (local/global tridiagonal
+    lines, then the halo of z) or 2, which takes no branch in 2D and leaves z as it is: the zeros
+    set before the loop (:424-428), so the first alpha is 0/0.  From x0 (default 0); returns (xu, xv, err,
+    niters)."""
     par = P.par
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
-    xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    if x0 is None:
+        xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    else:
+        xu, xv = np.array(x0[0], dtype=np.float64, copy=True), np.array(x0[1], dtype=np.float64, copy=True)
     adu, adv = P.Auu[_m(0, 0)], P.Avv[_m(0, 0)]
     T = _tri_setup_2d(P, P.Auu, P.Avv, glob=precond == 4) if precond in (3, 4) else None
     _halo(xu, par)
@@ -200,10 +205,13 @@ def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8, precond=1):
     niters = maxiters
     eta0 = 1.0
     du, dv = np.zeros_like(bu), np.zeros_like(bv)
+    zu, zv = np.zeros_like(bu), np.zeros_like(bv)
     l2_rhs = math.sqrt(_gsum(P, bu * bu, bv * bv))
     err = float("nan")
     for it in range(1, maxiters + 1):
-        if precond in (3, 4):
+        if precond == 2:
+            pass
+        elif precond in (3, 4):
             zu, zv = _tri_solve_2d(P, T, ru, rv, glob=precond == 4)
             _halo(zu, par)
             _halo(zv, par)
@@ -245,9 +253,11 @@ def _gsum2(P, a1, b1, a2, b2):
     return _gsum(P, a1, b1), _gsum(P, a2, b2)
 
 
-def _precond(P, precond, ru, rv, T=None):
+def _precond(P, precond, ru, rv, T=None, z=None):
     if precond == 0:
         return ru.copy(), rv.copy()
+    if precond == 2:  # no branch of the 2D solvers takes it: z keeps its contents
+        return z[0].copy(), z[1].copy()
     if precond in (3, 4):
         zu, zv = _tri_solve_2d(P, T, ru, rv, glob=precond == 4)
         _halo(zu, P.par)
@@ -258,17 +268,22 @@ def _precond(P, precond, ru, rv, T=None):
             np.divide(rv, adv, out=np.zeros_like(rv), where=adv != 0.0))
 
 
-def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8):
-    """pcg_solver_chrongear_2d (:1541-2628) with precond 0, 1 or 3, from x0 = 0: the first pass
+def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8, x0=None):
+    """pcg_solver_chrongear_2d (:1541-2628) with precond 0-4, from x0 (default 0): the first pass
     (:1913-2227), then iterations 2.. with one two-field sum each; with the line preconditioner at
-    most 100 iterations (maxiters_tridiag, :1703-1732); returns (xu, xv, err, niters)."""
+    most 100 iterations (maxiters_tridiag, :1703-1732).  Precond 2 takes no branch: z keeps A x0
+    from the first pass's matvec, later A x from the last convergence check.  Returns (xu, xv,
+    err, niters)."""
     par = P.par
     T = None
     if precond in (3, 4):
         T = _tri_setup_2d(P, P.Auu, P.Avv, glob=precond == 4)
         maxiters = 100
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
-    xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    if x0 is None:
+        xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    else:
+        xu, xv = np.array(x0[0], dtype=np.float64, copy=True), np.array(x0[1], dtype=np.float64, copy=True)
     du, dv = np.zeros_like(bu), np.zeros_like(bv)
     l2_rhs = math.sqrt(_gsum(P, bu * bu, bv * bv))
     _halo(xu, par)
@@ -277,7 +292,7 @@ def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8):
     ru, rv = bu - zu, bv - zv
     _halo(ru, par)
     _halo(rv, par)
-    zu, zv = _precond(P, precond, ru, rv, T)
+    zu, zv = _precond(P, precond, ru, rv, T, (zu, zv))
     w1u, w1v = ru * zu, rv * zv
     du, dv = zu.copy(), zv.copy()
     qu, qv = _matvec(P, du, dv)
@@ -293,7 +308,7 @@ def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8):
     rv = rv - alpha * qv
     niters, err = maxiters, float("nan")
     for it in range(2, maxiters + 1):
-        zu, zv = _precond(P, precond, ru, rv, T)
+        zu, zv = _precond(P, precond, ru, rv, T, (zu, zv))
         azu, azv = _matvec(P, zu, zv)
         rho, delta = _gsum2(P, ru * zu, rv * zv, azu * zu, azv * zv)
         _halo(azu, par)
@@ -2005,3 +2020,30 @@ def test_second_restatement_load_vector_local():
     assert np.count_nonzero(lu) > 0
     np.testing.assert_array_equal(lu, ou)
     np.testing.assert_array_equal(lv, ov)
+
+
+@pytest.mark.parametrize("name,make", CASES, ids=[c[0] for c in CASES])
+@pytest.mark.parametrize("alg", ["standard", "chrongear"])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3, 4])
+def test_second_restatement_2d_from_x0(name, make, alg, precond):
+    """Both 2D solvers from a random starting guess, with every preconditioner value, precond 2
+    included (no branch taken: the standard solver breaks down at once on its zeroed z, the
+    Chronopoulos-Gear solver iterates on z = A x0): bit-identical with the oracle."""
+    P = make()
+    x0 = problems.random_x0(P, seed=8, scale=10.0)
+    try:
+        if alg == "standard":
+            xu, xv, err, nit = pcg_standard_2d_diag(P, 60, precond=precond, x0=x0)
+        else:
+            xu, xv, err, nit = pcg_chrongear_2d(P, precond, 60, x0=x0)
+    except ZeroDivisionError:
+        xu = xv = None
+        err, nit = float("nan"), -1
+    st, ou, ov, oerr, onit = oracle.pcg(alg, P, precond, tol=1e-8, maxiters=60, summode=oracle.SUM_SEQ, x0=x0)
+    if st != 0:
+        assert nit < 0
+        return
+    assert nit == onit
+    assert (err == oerr) or (math.isnan(err) and math.isnan(oerr))
+    np.testing.assert_array_equal(xu, ou)
+    np.testing.assert_array_equal(xv, ov)
