@@ -422,14 +422,17 @@ def _precond3(P, precond, ru, rv, zu, zv, T=None):
     return _sia(P, P.Auu, ru, zu), _sia(P, P.Avv, rv, zv)
 
 
-def pcg_chrongear_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
-    """pcg_solver_chrongear_3d (:2632-3594) with precond 0, 1 or 2, from x0 = 0: the first pass
+def pcg_chrongear_3d(P, precond, maxiters, ncheck=5, tol=1e-8, x0=None):
+    """pcg_solver_chrongear_3d (:2632-3594) with precond 0-4, from x0 (default 0): the first pass
     (:3048-3290), then iterations 2.. (:3296-3581); returns (xu, xv, err, niters)."""
     par = P.par
     T = (_tri_setup_2d(P, _vsum_planes(P, P.Auu, precond == 4), _vsum_planes(P, P.Avv, precond == 4),
                        glob=precond == 4) if precond in (3, 4) else None)
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
-    xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    if x0 is None:
+        xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    else:
+        xu, xv = np.array(x0[0], dtype=np.float64, copy=True), np.array(x0[1], dtype=np.float64, copy=True)
     du, dv = np.zeros_like(bu), np.zeros_like(bv)
     qu, qv = np.zeros_like(bu), np.zeros_like(bv)
     l2_rhs = math.sqrt(_gsum3(P, bu * bu, bv * bv))
@@ -536,14 +539,18 @@ def test_second_restatement_chrongear_2d(name, make, precond, maxiters):
     np.testing.assert_array_equal(xv, ov)
 
 
-def pcg_standard_3d(P, precond, maxiters, ncheck=5, tol=1e-8):
-    """pcg_solver_standard_3d (:827-1537) with precond 0, 1 or 2, from x0 = 0 (the loop :1169-1524);
-    returns (xu, xv, err, niters), niters < 0 where the reference stops with GM_FATAL."""
+def pcg_standard_3d(P, precond, maxiters, ncheck=5, tol=1e-8, x0=None):
+    """pcg_solver_standard_3d (:827-1537) with precond 0-4, from x0 (default 0; the loop
+    :1169-1524); returns (xu, xv, err, niters), niters < 0 where the reference stops with
+    GM_FATAL."""
     par = P.par
     T = (_tri_setup_2d(P, _vsum_planes(P, P.Auu, precond == 4), _vsum_planes(P, P.Avv, precond == 4),
                        glob=precond == 4) if precond in (3, 4) else None)
     bu, bv = P.bu.astype(np.float64), P.bv.astype(np.float64)
-    xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    if x0 is None:
+        xu, xv = np.zeros_like(bu), np.zeros_like(bv)
+    else:
+        xu, xv = np.array(x0[0], dtype=np.float64, copy=True), np.array(x0[1], dtype=np.float64, copy=True)
     _halo(xu, par)
     _halo(xv, par)
     zu, zv = _matvec3(P, xu, xv)
@@ -2040,6 +2047,30 @@ def test_second_restatement_2d_from_x0(name, make, alg, precond):
         xu = xv = None
         err, nit = float("nan"), -1
     st, ou, ov, oerr, onit = oracle.pcg(alg, P, precond, tol=1e-8, maxiters=60, summode=oracle.SUM_SEQ, x0=x0)
+    if st != 0:
+        assert nit < 0
+        return
+    assert nit == onit
+    assert (err == oerr) or (math.isnan(err) and math.isnan(oerr))
+    np.testing.assert_array_equal(xu, ou)
+    np.testing.assert_array_equal(xv, ov)
+
+
+@pytest.mark.parametrize("name,make", CASES3, ids=[c[0] for c in CASES3])
+@pytest.mark.parametrize("alg", ["standard", "chrongear"])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3, 4])
+def test_second_restatement_3d_from_x0(name, make, alg, precond):
+    """Both 3D solvers from a random starting guess (the GPU parity tests' form), with every
+    preconditioner: bit-identical with the oracle through 40 iterations or the breakdown."""
+    P = make()
+    x0 = problems.random_x0(P, seed=7, scale=10.0)
+    solver = pcg_standard_3d if alg == "standard" else pcg_chrongear_3d
+    try:
+        xu, xv, err, nit = solver(P, precond, 40, x0=x0)
+    except ZeroDivisionError:
+        xu = xv = None
+        err, nit = float("nan"), -1
+    st, ou, ov, oerr, onit = oracle.pcg(alg, P, precond, tol=1e-8, maxiters=40, summode=oracle.SUM_SEQ, x0=x0)
     if st != 0:
         assert nit < 0
         return
