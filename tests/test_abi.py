@@ -207,3 +207,94 @@ def test_handle_method_bindings_reach_the_library(lib):
                 call()
             assert e.value.status == 4
         s.handle = None  # nothing to destroy
+
+
+# ---------------------------------------------------------------------------------------------
+# The Fortran module's bind(C) interfaces against the header's prototypes, parameter by parameter.
+# No Fortran compiler is available, so the interfaces are read as text, each dummy argument's C
+# type is derived from its ISO_C_BINDING kind and attributes (value: by value; otherwise a pointer
+# to the kind, as Fortran passes by reference), and g++ checks them against the header's function
+# types with static_asserts.  Integer kinds compare by size and signedness (the ABI), floating
+# kinds and structs exactly, pointees without their const.
+# ---------------------------------------------------------------------------------------------
+_KINDS = {"c_int": ("int", 4), "c_int32_t": ("int", 4), "c_long_long": ("int", 8), "c_int64_t": ("int", 8),
+          "c_size_t": ("uint", 8), "c_double": ("double", 8), "c_float": ("float", 4), "c_char": ("char", 1),
+          "c_ptr": ("ptr", 8), "cismgpu_par_t": ("par", 0)}
+
+
+def _fortran_interfaces():
+    src = open(os.path.join(ROOT, "cism_b200", "fortran", "glissade_velo_higher_pcg_gpu.F90")).read()
+    src = "\n".join(line.split("!")[0] for line in src.splitlines())
+    src = re.sub(r"&\s*\n\s*", " ", src)
+    block = src[src.index("\n    interface"):src.index("end interface")]
+    out = []
+    for m in re.finditer(r"(integer|type|real)\((\w+)\)\s+function\s+\w+\s*\(([^)]*)\)\s*"
+                         r"bind\(C,\s*name=\"(cismgpu_[a-z0-9_]+)\"\)(.*?)end function", block, flags=re.S):
+        _, rkind, args, cname, body = m.groups()
+        names = [a.strip() for a in args.split(",") if a.strip()]
+        decl = {}
+        for line in body.splitlines():
+            d = re.match(r"\s*(integer|real|type|character)\((?:kind=)?(\w+)\)\s*(,[^:]*)?::(.*)", line)
+            if not d:
+                continue
+            attrs = d.group(3) or ""
+            for ent in re.findall(r"(\w+)\s*(\([^)]*\))?", d.group(4)):
+                decl[ent[0].lower()] = (d.group(2), "value" in attrs)
+        out.append((cname, rkind, [(n, *decl[n.lower()]) for n in names]))
+    return out
+
+
+def _cxx_check(kind, value, t):
+    base, size = _KINDS[kind]
+    if kind == "c_ptr":
+        return f"std::is_pointer<{t}>::value" if value else f"std::is_pointer<pointee<{t}>>::value"
+    inner = t if value else f"pointee<{t}>"
+    ptr = "true" if value else f"std::is_pointer<{t}>::value"
+    if base in ("int", "uint"):
+        sign = "true" if base == "int" else "false"
+        return (f"{ptr} && std::is_integral<{inner}>::value && sizeof({inner}) == {size} && "
+                f"std::is_signed<{inner}>::value == {sign}")
+    ctype = {"double": "double", "float": "float", "char": "char", "par": "cismgpu_par_t"}[base]
+    return f"{ptr} && std::is_same<{inner}, {ctype}>::value"
+
+
+def test_fortran_interfaces_match_the_header_types(tmp_path):
+    """Every parameter and result of every bind(C) interface of the Fortran module has the C type
+    of the header's prototype (g++ static_asserts), and the module's bind(C) cismgpu_par_t has the
+    header struct's members, types and offsets."""
+    import shutil
+    import subprocess
+    if not shutil.which("g++"):
+        pytest.skip("no C++ compiler")
+    ifaces = _fortran_interfaces()
+    assert len(ifaces) >= 20
+    lines = ["#include <cstddef>", "#include <cstdint>", "#include <tuple>", "#include <type_traits>",
+             '#include "cismgpu.h"',
+             "template <class P> using pointee = std::remove_cv_t<std::remove_pointer_t<P>>;",
+             "template <class F> struct sig;",
+             "template <class R, class... A> struct sig<R (*)(A...)> {",
+             "  using ret = R; static constexpr int n = sizeof...(A);",
+             "  template <int i> using arg = std::tuple_element_t<i, std::tuple<A...>>; };"]
+    for cname, rkind, args in ifaces:
+        s = f"sig<decltype(&{cname})>"
+        lines.append(f'static_assert({s}::n == {len(args)}, "{cname}: argument count");')
+        lines.append(f'static_assert({_cxx_check(rkind, True, f"{s}::ret")}, "{cname}: result type");')
+        for i, (name, kind, value) in enumerate(args):
+            t = f"{s}::arg<{i}>"
+            lines.append(f'static_assert({_cxx_check(kind, value, t)}, "{cname}: argument {i + 1} ({name})");')
+    src = open(os.path.join(ROOT, "cism_b200", "fortran", "glissade_velo_higher_pcg_gpu.F90")).read()
+    body = re.search(r"type, bind\(C\) :: cismgpu_par_t(.*?)end type", src, flags=re.S).group(1)
+    fields = []
+    for kind, names in re.findall(r"integer\((\w+)\)\s*::\s*([^\n!]*)", body):
+        assert kind == "c_int32_t"
+        fields += [n.strip() for n in names.split(",") if n.strip()]
+    assert len(fields) == 10
+    for k, f in enumerate(fields):
+        lines.append(f'static_assert(offsetof(cismgpu_par_t, {f}) == {4 * k}, "par member {f}");')
+        lines.append(f'static_assert(std::is_same<decltype(cismgpu_par_t::{f}), int32_t>::value, "par {f}");')
+    lines.append(f'static_assert(sizeof(cismgpu_par_t) == {4 * len(fields)}, "par size");')
+    cpp = tmp_path / "fortran_abi_check.cpp"
+    cpp.write_text("\n".join(lines) + "\n")
+    r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(cpp)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-4000:]
