@@ -92,7 +92,7 @@ def _gsum(P, a1, a2):
     for j in range(par["staggered_jlo"], par["staggered_jhi"] + 1):
         for i in range(par["staggered_ilo"], par["staggered_ihi"] + 1):
             s = (s + float(a1[j - 1, i - 1])) + float(a2[j - 1, i - 1])
-    return s
+    return np.float64(s)  # the solvers' scalars then divide as IEEE (inf, NaN), as the reference's do
 
 
 def _tri_setup_2d(P, U, V, glob=False):
@@ -206,7 +206,7 @@ def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8, precond=1, x0=None):
     eta0 = 1.0
     du, dv = np.zeros_like(bu), np.zeros_like(bv)
     zu, zv = np.zeros_like(bu), np.zeros_like(bv)
-    l2_rhs = math.sqrt(_gsum(P, bu * bu, bv * bv))
+    l2_rhs = np.sqrt(_gsum(P, bu * bu, bv * bv))
     err = float("nan")
     for it in range(1, maxiters + 1):
         if precond == 2:
@@ -241,7 +241,7 @@ def pcg_standard_2d_diag(P, maxiters, ncheck=5, tol=1e-8, precond=1, x0=None):
             _halo(xv, par)
             zu, zv = _matvec(P, xu, xv)
             ru, rv = bu - zu, bv - zv
-            err = math.sqrt(_gsum(P, ru * ru, rv * rv)) / l2_rhs
+            err = np.sqrt(_gsum(P, ru * ru, rv * rv)) / l2_rhs
             if err < tol:
                 niters = it
                 break
@@ -285,7 +285,7 @@ def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8, x0=None):
     else:
         xu, xv = np.array(x0[0], dtype=np.float64, copy=True), np.array(x0[1], dtype=np.float64, copy=True)
     du, dv = np.zeros_like(bu), np.zeros_like(bv)
-    l2_rhs = math.sqrt(_gsum(P, bu * bu, bv * bv))
+    l2_rhs = np.sqrt(_gsum(P, bu * bu, bv * bv))
     _halo(xu, par)
     _halo(xv, par)
     zu, zv = _matvec(P, xu, xv)
@@ -330,7 +330,7 @@ def pcg_chrongear_2d(P, precond, maxiters, ncheck=5, tol=1e-8, x0=None):
         if it % ncheck == 0 or it == 5:
             zu, zv = _matvec(P, xu, xv)
             ru, rv = bu - zu, bv - zv
-            err = math.sqrt(_gsum(P, ru * ru, rv * rv)) / l2_rhs
+            err = np.sqrt(_gsum(P, ru * ru, rv * rv)) / l2_rhs
             if err < tol:
                 niters = it
                 break
@@ -380,7 +380,7 @@ def _gsum3(P, a1, a2):
             c1, c2 = l1[j - 1][i - 1], l2[j - 1][i - 1]
             for k in range(len(c1)):
                 s = (s + c1[k]) + c2[k]
-    return s
+    return np.float64(s)
 
 
 def _sia(P, A, r, z):
@@ -435,7 +435,7 @@ def pcg_chrongear_3d(P, precond, maxiters, ncheck=5, tol=1e-8, x0=None):
         xu, xv = np.array(x0[0], dtype=np.float64, copy=True), np.array(x0[1], dtype=np.float64, copy=True)
     du, dv = np.zeros_like(bu), np.zeros_like(bv)
     qu, qv = np.zeros_like(bu), np.zeros_like(bv)
-    l2_rhs = math.sqrt(_gsum3(P, bu * bu, bv * bv))
+    l2_rhs = np.sqrt(_gsum3(P, bu * bu, bv * bv))
     _halo(xu, par)
     _halo(xv, par)
     zu, zv = _matvec3(P, xu, xv)
@@ -480,7 +480,7 @@ def pcg_chrongear_3d(P, precond, maxiters, ncheck=5, tol=1e-8, x0=None):
         if it % ncheck == 0 or it == 5:
             zu, zv = _matvec3(P, xu, xv)
             ru, rv = bu - zu, bv - zv
-            err = math.sqrt(_gsum3(P, ru * ru, rv * rv)) / l2_rhs
+            err = np.sqrt(_gsum3(P, ru * ru, rv * rv)) / l2_rhs
             if err < tol:
                 niters = it
                 break
@@ -558,7 +558,7 @@ def pcg_standard_3d(P, precond, maxiters, ncheck=5, tol=1e-8, x0=None):
     niters, eta0, err = maxiters, 1.0, float("nan")
     du, dv = np.zeros_like(bu), np.zeros_like(bv)
     zu, zv = np.zeros_like(bu), np.zeros_like(bv)
-    l2_rhs = math.sqrt(_gsum3(P, bu * bu, bv * bv))
+    l2_rhs = np.sqrt(_gsum3(P, bu * bu, bv * bv))
     for it in range(1, maxiters + 1):
         zu, zv = _precond3(P, precond, ru, rv, zu, zv, T)
         eta1 = _gsum3(P, ru * zu, rv * zv)
@@ -584,7 +584,7 @@ def pcg_standard_3d(P, precond, maxiters, ncheck=5, tol=1e-8, x0=None):
             _halo(xv, par)
             zu, zv = _matvec3(P, xu, xv)
             ru, rv = bu - zu, bv - zv
-            err = math.sqrt(_gsum3(P, ru * ru, rv * rv)) / l2_rhs
+            err = np.sqrt(_gsum3(P, ru * ru, rv * rv)) / l2_rhs
             if err < tol:
                 niters = it
                 break
@@ -2039,10 +2039,9 @@ def test_second_restatement_2d_from_x0(name, make, alg, precond):
     P = make()
     x0 = problems.random_x0(P, seed=8, scale=10.0)
     try:
-        if alg == "standard":
-            xu, xv, err, nit = pcg_standard_2d_diag(P, 60, precond=precond, x0=x0)
-        else:
-            xu, xv, err, nit = pcg_chrongear_2d(P, precond, 60, x0=x0)
+        with np.errstate(divide="ignore", invalid="ignore"):  # precond 2's first alpha is 0/0
+            xu, xv, err, nit = (pcg_standard_2d_diag(P, 60, precond=precond, x0=x0) if alg == "standard" else
+                                pcg_chrongear_2d(P, precond, 60, x0=x0))
     except ZeroDivisionError:
         xu = xv = None
         err, nit = float("nan"), -1
@@ -2056,7 +2055,10 @@ def test_second_restatement_2d_from_x0(name, make, alg, precond):
     np.testing.assert_array_equal(xv, ov)
 
 
-@pytest.mark.parametrize("name,make", CASES3, ids=[c[0] for c in CASES3])
+CASES3_X0 = [c for c in CASES3 if c[0] != "dome"]  # the dome runs from zero above, at four counts
+
+
+@pytest.mark.parametrize("name,make", CASES3_X0, ids=[c[0] for c in CASES3_X0])
 @pytest.mark.parametrize("alg", ["standard", "chrongear"])
 @pytest.mark.parametrize("precond", [0, 1, 2, 3, 4])
 def test_second_restatement_3d_from_x0(name, make, alg, precond):
@@ -2078,3 +2080,72 @@ def test_second_restatement_3d_from_x0(name, make, alg, precond):
     assert (err == oerr) or (math.isnan(err) and math.isnan(oerr))
     np.testing.assert_array_equal(xu, ou)
     np.testing.assert_array_equal(xv, ov)
+
+
+def _solve_both(alg, P, precond, maxiters, x0):
+    """One solve by this restatement and by the oracle (reference order); the restatement's
+    breakdown (a NaN alpha or eta1, GM_FATAL in the reference) as niters < 0."""
+    is3d = P.kind == "3d"
+    with np.errstate(divide="ignore", invalid="ignore"):
+        if alg == "standard":
+            got = (pcg_standard_3d(P, precond, maxiters, x0=x0) if is3d else
+                   pcg_standard_2d_diag(P, maxiters, precond=precond, x0=x0))
+        else:
+            got = (pcg_chrongear_3d(P, precond, maxiters, x0=x0) if is3d else
+                   pcg_chrongear_2d(P, precond, maxiters, x0=x0))
+    want = oracle.pcg(alg, P, precond, tol=1e-8, maxiters=maxiters, summode=oracle.SUM_SEQ, x0=x0)
+    return got, want
+
+
+def _assert_same(got, want):
+    xu, xv, err, nit = got
+    st, ou, ov, oerr, onit = want
+    if st != 0:
+        assert nit < 0
+        return
+    assert nit == onit
+    assert (err == oerr) or (math.isnan(err) and math.isnan(oerr))
+    np.testing.assert_array_equal(xu, ou)
+    np.testing.assert_array_equal(xv, ov)
+
+
+EDGE = [("2d", lambda: problems.slab_2d(seed=1)), ("3d", lambda: problems.slab_3d(seed=5, sliding=False))]
+
+
+@pytest.mark.parametrize("kind,make", EDGE, ids=[e[0] for e in EDGE])
+@pytest.mark.parametrize("alg", ["standard", "chrongear"])
+@pytest.mark.parametrize("precond", [0, 1, 2, 3])
+def test_second_restatement_zero_rhs(kind, make, alg, precond):
+    """A zero right-hand side.  From x0 = 0 every sum is zero and the first alpha is 0/0: the
+    reference stops with GM_FATAL, and so do both restatements.  From a nonzero x0, |b| = 0 makes
+    every convergence check's err +inf (|r|/0), so the solve runs to maxiters: x, err and niters
+    bit-identical with the oracle."""
+    import dataclasses
+    P = make()
+    Z = dataclasses.replace(P, bu=np.zeros_like(P.bu), bv=np.zeros_like(P.bv))
+    got, want = _solve_both(alg, Z, precond, 12, None)
+    assert want[0] != 0 and got[3] < 0
+    x0 = problems.random_x0(P, seed=9, scale=10.0)
+    got, want = _solve_both(alg, Z, precond, 12, x0)
+    _assert_same(got, want)
+    if want[0] == 0:  # Chronopoulos-Gear 2D gives line-preconditioned solves 100 iterations,
+        cap = 100 if (kind == "2d" and alg == "chrongear" and precond == 3) else 12  # whatever maxiters (:1728-1732)
+        assert want[4] == cap and want[3] == float("inf")
+
+
+@pytest.mark.parametrize("kind,make", EDGE, ids=[e[0] for e in EDGE])
+@pytest.mark.parametrize("alg", ["standard", "chrongear"])
+def test_second_restatement_no_active_vertices(kind, make, alg):
+    """No active vertex: zero rows everywhere, so the matvec is zero.  With the diagonal
+    preconditioner (zero diagonals: z = 0) the first alpha is 0/0; with none, z = r gives alpha =
+    eta1/0 = +inf, x and r turn non-finite and the second iteration meets a NaN (eta1 in the
+    standard solver, alpha in Chronopoulos-Gear).  Both restatements stop where the reference's
+    GM_FATAL checks do, from zero and from a random x0."""
+    import dataclasses
+    P = make()
+    Z = dataclasses.replace(P, active_vertex=np.zeros_like(P.active_vertex), Auu=np.zeros_like(P.Auu),
+                            Auv=np.zeros_like(P.Auv), Avu=np.zeros_like(P.Avu), Avv=np.zeros_like(P.Avv))
+    for x0 in (None, problems.random_x0(P, seed=9, scale=10.0)):
+        for precond in (0, 1):
+            got, want = _solve_both(alg, Z, precond, 12, x0)
+            _assert_same(got, want)
