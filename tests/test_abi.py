@@ -298,3 +298,82 @@ def test_fortran_interfaces_match_the_header_types(tmp_path):
     r = subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), str(cpp)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-4000:]
+
+
+# ---------------------------------------------------------------------------------------------
+# The Python package's ctypes signatures against the header's prototypes.
+# ---------------------------------------------------------------------------------------------
+def _header_signatures():
+    """{name: (return type, [parameter types])} from include/*.h, names and array brackets
+    dropped, whitespace normalised."""
+    text = ""
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text += re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+    text = "\n".join(line for line in text.splitlines() if not line.lstrip().startswith("#"))
+    text = text.replace('extern "C" {', ";")
+    out = {}
+    for m in re.finditer(r"([^;{}]*?)\b(cismgpu_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        ret = " ".join(m.group(1).split()).replace("typedef", "").strip()
+        args = m.group(3).strip()
+        params = []
+        if args not in ("", "void"):
+            for a in args.split(","):
+                a = " ".join(a.split())
+                a = re.sub(r"\b\w+(\[\w*\])?$", lambda mm: "*" if mm.group(1) else "", a).strip()
+                params.append(re.sub(r"\s*\*", " *", a).replace("  ", " ").strip())
+        out[m.group(2)] = (ret, params)
+    return out
+
+
+def _ctype_matches(ctype_text, ct):
+    """Whether ctypes type ct passes the C type ctype_text the same way."""
+    t = ctype_text.replace("const ", "").strip()
+    if t.endswith("*"):
+        if ct is ctypes.c_void_p or (t == "char *" and ct is ctypes.c_char_p):
+            return True
+        if not (isinstance(ct, type) and issubclass(ct, ctypes._Pointer)):
+            return False
+        pointee = t[:-1].strip()
+        if pointee.endswith("*"):  # a handle's address: T **
+            return ct._type_ is ctypes.c_void_p or issubclass(ct._type_, ctypes._Pointer)
+        if pointee in ("cismgpu_par_t", "cismgpu_request_t"):
+            return issubclass(ct._type_, ctypes.Structure)
+        return _ctype_matches(pointee, ct._type_)
+    scalars = {"int": ("i", 4, True), "int32_t": ("i", 4, True), "unsigned int": ("i", 4, False),
+               "long long": ("i", 8, True), "int64_t": ("i", 8, True), "size_t": ("i", 8, False),
+               "double": ("d", 8, True), "float": ("f", 4, True)}
+    if t not in scalars or ct is None or not isinstance(ct, type) or not issubclass(ct, ctypes._SimpleCData):
+        return False
+    kind, size, signed = scalars[t]
+    if ctypes.sizeof(ct) != size:
+        return False
+    if kind != "i":
+        return ct._type_ == kind
+    return ct._type_ in "bhilqBHILQ" and (ct._type_.islower() == signed)
+
+
+def test_python_bindings_match_the_header():
+    """Every function the package binds has the header's parameter count and, parameter by
+    parameter, a ctypes type that passes the C type the same way (pointers as c_void_p or a
+    POINTER of the same pointee, integers by size and signedness); functions returning a pointer
+    or a non-int value declare a restype that carries it."""
+    import cism_b200 as cg
+    lib = cg.load_library()
+    sigs = _header_signatures()
+    checked = 0
+    for name, (ret, params) in sorted(sigs.items()):
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        if fn.argtypes is not None:
+            assert len(fn.argtypes) == len(params), (name, len(fn.argtypes), len(params))
+            for i, (p, ct) in enumerate(zip(params, fn.argtypes)):
+                assert _ctype_matches(p, ct), (name, i + 1, p, ct)
+            checked += 1
+        r = ret.replace("const ", "").strip()
+        if r.endswith("*"):
+            assert fn.restype in (ctypes.c_char_p, ctypes.c_void_p) or (
+                isinstance(fn.restype, type) and issubclass(fn.restype, ctypes._Pointer)), (name, ret, fn.restype)
+        elif r not in ("int", "void") and fn.argtypes is not None:
+            assert _ctype_matches(r, fn.restype), (name, ret, fn.restype)
+    assert checked >= 40, checked
