@@ -1814,34 +1814,6 @@ static int mixed_launch_grid(bool is3d, int nzm, int TY, bool resident, int ntil
     return std::min(grid, ntiles);
 }
 
-// Launch order of a tile list on `grid` CTAs (CTA b takes entries b, b + grid, ...).  With
-// more tiles than CTAs, each CTA gets a contiguous run of the (solve, tile) list, so that it
-// holds tiles of few solves; padding entries have solve = -1.  Fails if a CTA would hold
-// tiles of more than kMaxCtaSolves solves.
-static int mixed_tile_order(const std::vector<MTile> &in, int grid, std::vector<MTile> &out) {
-    const int T = (int)in.size();
-    if (T <= grid) {
-        out = in;
-    } else {
-        const int per = (T + grid - 1) / grid;
-        out.assign((size_t)per * grid, MTile{-1, -1});
-        for (int b = 0; b < grid; ++b) {
-            const long long lo = (long long)b * T / grid, hi = (long long)(b + 1) * T / grid;
-            for (long long w = lo; w < hi; ++w) out[(size_t)(w - lo) * grid + b] = in[(size_t)w];
-        }
-    }
-    for (int b = 0; b < grid; ++b) {
-        std::vector<int> seen;
-        for (size_t w = b; w < out.size(); w += grid) {
-            const int sv = out[w].solve;
-            if (sv >= 0 && std::find(seen.begin(), seen.end(), sv) == seen.end()) seen.push_back(sv);
-        }
-        if ((int)seen.size() > kMaxCtaSolves)
-            return fail(CISMGPU_EUNSUPPORTED, "batch too fragmented for one launch (solves per CTA > 64)");
-    }
-    return CISMGPU_OK;
-}
-
 template <int NC, int NZM>
 static int mixed_launch(const MDesc *d_descs, MState *d_states, const MTile *d_tiles, int ntiles, int TY,
                         int resident, MCtl *d_ctl, int max_steps, int grid, cudaStream_t s) {
