@@ -152,7 +152,6 @@ __device__ bool asm_point3d(const AsmArgs &a, int p, const double (&x)[8], const
 __global__ void __launch_bounds__(kAsmElThreads) k_asm_elements3d(AsmArgs a, int je0, int nrows, int jown0,
                                                                   int jown1, double *__restrict__ K, long long ks) {
     __shared__ AsmPt sp[8][kAsmEl];
-    __shared__ int sval[kAsmEl];
     const int nzl1 = a.nz - 1;
     const long long nel = (long long)a.nx * nzl1 * nrows;
     const long long NX = a.nx - 1;
@@ -168,7 +167,6 @@ __global__ void __launch_bounds__(kAsmElThreads) k_asm_elements3d(AsmArgs a, int
         valid = ie >= a.nhalo + 1 && ie <= a.nx - a.nhalo + 1 && je >= a.nhalo + 1 && je <= a.ny - a.nhalo + 1 &&
                 a.active_cell[(ie - 1) + (long long)a.nx * (je - 1)] != 0;
     }
-    if (sub == 0) sval[el] = valid;
     if (valid) {  // phase 1: Gauss point p = sub
         double x[8], y[8], z[8], u[8], v[8];
 #pragma unroll
@@ -275,7 +273,7 @@ __host__ __device__ constexpr int asm_slot_col(int s, int m) {
 __global__ void __launch_bounds__(kAsmBlock) k_asm_gather3d(AsmArgs a, SymIdx L, int ja, int jb, int je0,
                                                             const double *__restrict__ K, long long ks,
                                                             double *Auu, double *Auv, double *Avu, double *Avv) {
-    const long long NX = a.nx - 1, NQ = NX * (a.ny - 1);
+    const long long NX = a.nx - 1;
     const long long nrow = (long long)(jb - ja) * NX;
     const long long t = (long long)blockIdx.x * kAsmBlock + threadIdx.x;
     if (t >= (long long)a.nz * nrow) return;
