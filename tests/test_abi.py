@@ -377,3 +377,54 @@ def test_python_bindings_match_the_header():
         elif r not in ("int", "void") and fn.argtypes is not None:
             assert _ctype_matches(r, fn.restype), (name, ret, fn.restype)
     assert checked >= 40, checked
+
+
+_C_CALLER = r"""
+#include <stdio.h>
+#include <string.h>
+#include "cismgpu.h"
+int main(void) {
+    const char *v = cismgpu_version();
+    if (!v || !strstr(v, "sm_100a")) return 2;
+    int prev = cismgpu_set_sum_order(CISMGPU_SUM_SEQUENTIAL);
+    if (cismgpu_set_sum_order(prev) != CISMGPU_SUM_SEQUENTIAL) return 3;
+    if (cismgpu_solver_mixed_layout(NULL, NULL) != CISMGPU_EINVAL) return 4;
+    if (strlen(cismgpu_last_error()) == 0) return 5;
+    printf("%s\n", v);
+    return 0;
+}
+"""
+
+
+@pytest.mark.parametrize("lang,std", [("c", "c99"), ("c", "c11"), ("c++", "c++11"), ("c++", "c++17")])
+def test_header_compiles_strictly(tmp_path, lang, std):
+    """include/cismgpu.h is plain C for C callers and C++ callers: no warning under -pedantic."""
+    import shutil
+    import subprocess
+    cc = "gcc" if lang == "c" else "g++"
+    if not shutil.which(cc):
+        pytest.skip(f"no {cc}")
+    src = tmp_path / ("hdr.c" if lang == "c" else "hdr.cpp")
+    src.write_text('#include "cismgpu.h"\nint main(void) { return 0; }\n')
+    r = subprocess.run([cc, f"-std={std}", "-Wall", "-Wextra", "-pedantic", "-Werror", "-fsyntax-only",
+                        "-I", os.path.join(ROOT, "include"), str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
+def test_c_caller_links_and_calls(tmp_path, lib):
+    """A C99 program built against the header links libcismgpu.so and calls its host-side entry
+    points (version, sum order, an argument check and its message) without a GPU."""
+    import shutil
+    import subprocess
+    if not shutil.which("gcc"):
+        pytest.skip("no gcc")
+    libdir = os.path.dirname(build.build())
+    src = tmp_path / "caller.c"
+    src.write_text(_C_CALLER)
+    exe = tmp_path / "caller"
+    r = subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I",
+                        os.path.join(ROOT, "include"), str(src), "-L", libdir, "-lcismgpu",
+                        f"-Wl,-rpath,{libdir}", "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=60)
+    assert run.returncode == 0 and "sm_100a" in run.stdout, (run.returncode, run.stdout, run.stderr)
